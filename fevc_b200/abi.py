@@ -1,0 +1,373 @@
+"""ctypes mirror of ``include/fevc_b200.h``.
+
+The struct layouts are the plugin ABI's (``vckss_rust.h``), so the same
+bindings drive this library and any binary exporting the reference plugin's
+entry points.  ``Engine`` wraps the prepare -> solve -> result lifecycle in the
+way the Stata shim calls it.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+u32, u64, i32, i64, f64 = C.c_uint32, C.c_uint64, C.c_int32, C.c_int64, C.c_double
+dptr = C.POINTER(C.c_double)
+InterruptPoll = C.CFUNCTYPE(C.c_int32, C.c_void_p)
+
+
+class Struct(C.Structure):
+    def as_dict(self):
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = v.as_dict() if isinstance(v, Struct) else v
+        return out
+
+
+class PrepareRequestV1(Struct):
+    _fields_ = [("abi_version", u32), ("struct_size", u32), ("rows", u64), ("cleanup_abandoned", u32),
+                ("reserved", u32)]
+
+
+class PrepareRequestV2(Struct):
+    _fields_ = PrepareRequestV1._fields_ + [("memory_limit_bytes", u64), ("caller_copy_bytes", u64)]
+
+
+class PrepareRequestV3(Struct):
+    _fields_ = [("v2", PrepareRequestV2), ("deletion_mode", u32), ("controls_count", u32), ("reserved_2", u64)]
+
+
+class PrepareRequestV4(Struct):
+    _fields_ = [("v3", PrepareRequestV3), ("implicit_match", u32), ("reserved_3", u32)]
+
+
+class PrepareRequestInterruptV2(Struct):
+    _fields_ = [("options", PrepareRequestV3), ("interrupt_poll", InterruptPoll), ("interrupt_context", C.c_void_p),
+                ("checkpoint_interval", u32), ("reserved", u32)]
+
+
+class PrepareRequestInterruptV3(Struct):
+    _fields_ = [("options", PrepareRequestV4), ("interrupt_poll", InterruptPoll), ("interrupt_context", C.c_void_p),
+                ("checkpoint_interval", u32), ("reserved", u32)]
+
+
+class ColumnsV1(Struct):
+    _fields_ = [("struct_size", u32), ("reserved", u32), ("rows", u64), ("worker", dptr), ("firm", dptr),
+                ("deletion", dptr), ("outcome", dptr), ("frequency", dptr), ("target_weight", dptr)]
+
+
+class ColumnsV2(Struct):
+    _fields_ = [("v1", ColumnsV1), ("controls", C.POINTER(dptr)), ("controls_count", u32), ("reserved_2", u32)]
+
+
+class ColumnsV3(Struct):
+    _fields_ = [("v2", ColumnsV2), ("probe_order", dptr), ("probeorder_supplied", u32), ("reserved_3", u32)]
+
+
+class SolveRequestV1(Struct):
+    _fields_ = [("abi_version", u32), ("struct_size", u32), ("seed", u64), ("probes", u32),
+                ("leverage_batch_width", u32), ("target_batch_width", u32), ("deletion_mode", u32),
+                ("rng_contract", u32), ("solver_route", u32), ("allow_automatic_cmg_setup_fallback", u32),
+                ("exact_dimension_limit", u64), ("cmg_minimum_dimension", u64), ("pcg_tolerance", f64),
+                ("maximum_iterations", u32), ("residual_replacement_interval", u32), ("rank_tolerance", f64),
+                ("block_tolerance", f64), ("cmg_terminal_vertices", u64), ("cmg_dense_vertex_cap", u64),
+                ("cmg_maximum_levels", u64), ("cmg_aggregate_cap", u64), ("cmg_minimum_reduction", f64),
+                ("cmg_jacobi_weight", f64), ("cmg_pre_sweeps", u32), ("cmg_post_sweeps", u32),
+                ("cmg_maximum_edge_complexity", f64), ("cmg_maximum_vertex_complexity", f64),
+                ("cmg_memory_limit_bytes", u64)]
+
+
+class SolveRequestV2(Struct):
+    _fields_ = [("v1", SolveRequestV1), ("algorithm", u32), ("nuisance_mode", u32), ("exact_estimator_limit", u64),
+                ("blocksize_limit", u64)]
+
+
+class SolveRequestV3(Struct):
+    _fields_ = [("v2", SolveRequestV2), ("engine", u32), ("batch_mode", u32), ("stayers_mode", u32),
+                ("target_weight_mode", u32), ("deletion_unit_source", u32), ("probeorder_supplied", u32),
+                ("wallseconds_supplied", u32), ("capability_schema", u32), ("capability_profile", u32),
+                ("frequency_use", u32), ("physical_limit", u64), ("request_signature", u64), ("reserved_3", u64)]
+
+
+class SolveRequestV4(Struct):
+    _fields_ = [("v3", SolveRequestV3), ("leverage_batch_mode", u32), ("target_batch_mode", u32),
+                ("wallseconds", f64), ("reserved_4", u64)]
+
+
+class SolveRequestV5(Struct):
+    _fields_ = [("v4", SolveRequestV4), ("threads", u32), ("tolerance_supplied", u32), ("full_cmg_v2", u32),
+                ("reserved_5", u32)]
+
+
+class SolveRequestInterruptV1(Struct):
+    _fields_ = [("options", SolveRequestV1), ("interrupt_poll", InterruptPoll), ("interrupt_context", C.c_void_p),
+                ("checkpoint_interval", u32), ("reserved", u32)]
+
+
+class Components(Struct):
+    _fields_ = [("worker", f64), ("firm", f64), ("covariance", f64), ("total", f64)]
+
+    def tuple(self):
+        return (self.worker, self.firm, self.covariance, self.total)
+
+
+class ResultV1(Struct):
+    _fields_ = [("struct_size", u32), ("reserved", u32), ("generation", u64), ("plugin", Components),
+                ("correction", Components), ("corrected", Components), ("numerical_mcse", Components)]
+
+
+class PreparationReceiptV2(Struct):
+    _fields_ = [("struct_size", u32), ("reserved", u32)] + [(n, u64) for n in (
+        "generation", "input_rows", "retained_rows", "workers", "firms", "cells", "deletion_units", "target_strata",
+        "memory_limit_bytes", "caller_copy_bytes", "preparation_peak_forecast_bytes", "prepared_resident_bytes",
+        "graph_input_rows", "graph_retained_rows", "graph_input_physical_mass", "graph_retained_physical_mass",
+        "graph_initial_components", "graph_maximum_components", "graph_initial_component_rows",
+        "graph_mover_input_rows", "graph_initial_deletion_edges", "graph_retained_deletion_edges",
+        "graph_insufficient_workers_removed", "graph_articulation_workers_removed", "graph_bridge_units_removed",
+        "graph_bridge_rows_removed", "graph_degree_iterations", "graph_articulation_iterations",
+        "graph_bridge_iterations", "graph_fixed_point_iterations")]
+
+
+class PreparationReceiptV3(Struct):
+    _fields_ = [("v2", PreparationReceiptV2), ("target_weight_sum", f64)]
+
+
+class PreparationReceiptV4(Struct):
+    _fields_ = [("v3", PreparationReceiptV3), ("controls_count", u32), ("deletion_mode", u32)]
+
+
+class RhsReceiptV1(Struct):
+    _fields_ = [("phase", u32), ("side", u32), ("probe", i64), ("route", u32), ("iterations", u32),
+                ("zero_rhs", u32), ("reserved", u32), ("reduced_residual", f64), ("complete_residual", f64)]
+
+
+class SnapshotV1(Struct):
+    _fields_ = [("struct_size", u32), ("state", u32), ("generation", u64), ("last_released_generation", u64)]
+
+
+class FevcbSolveOptionsV1(Struct):
+    _fields_ = [("struct_size", u32), ("block_columns", u32), ("preconditioner", u32), ("keep_unit_detail", u32)]
+
+
+class FevcbSolveTimingsV1(Struct):
+    _fields_ = [("struct_size", u32), ("reserved", u32), ("total_ms", f64), ("fit_ms", f64), ("leverage_ms", f64),
+                ("target_ms", f64), ("setup_ms", f64)] + [(n, u64) for n in (
+                    "block_iterations", "column_iterations", "rhs_columns", "kernel_launches", "h2d_bytes",
+                    "vertices", "edges", "kept_workers", "levels")]
+
+
+SIZES = {
+    PrepareRequestV1: 24, PrepareRequestV2: 40, PrepareRequestV3: 56, PrepareRequestV4: 64,
+    PrepareRequestInterruptV2: 80, PrepareRequestInterruptV3: 88, ColumnsV1: 64, ColumnsV2: 80, ColumnsV3: 96,
+    SolveRequestV1: 176, SolveRequestV2: 200, SolveRequestV3: 264, SolveRequestV4: 288, SolveRequestV5: 304,
+    SolveRequestInterruptV1: 200, ResultV1: 144, PreparationReceiptV2: 248, PreparationReceiptV3: 256,
+    PreparationReceiptV4: 264, RhsReceiptV1: 48, SnapshotV1: 24,
+}
+for _cls, _size in SIZES.items():
+    assert C.sizeof(_cls) == _size, (_cls.__name__, C.sizeof(_cls), _size)
+
+TAG_LEVERAGE = 0x4C45564552414745
+TAG_TARGET = 0x0054415247455401
+
+# Every entry point the header declares, with its ctypes signature.
+SIGNATURES = {
+    "vckss_rust_abi_version": (u32, []),
+    "vckss_rust_backend_version": (C.c_char_p, []),
+    "vckss_rust_capabilities_json": (C.c_char_p, []),
+    "vckss_rust_last_error": (C.c_char_p, []),
+    "vckss_rust_selftest": (i32, []),
+    "vckss_rust_backend_capabilities_v1": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_solve_request_v1": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_solve_request_v2": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_solve_request_v3": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_solve_request_v4": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_solve_request_v5": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_solve_request_interrupt_v1": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_solve_request_interrupt_v5": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_prepare_request_v3": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_prepare_request_interrupt_v1": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_prepare_request_interrupt_v2": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_prepare_request_interrupt_v3": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_prepare_v1": (i32, [C.c_void_p, C.c_void_p, C.POINTER(u64), u32]),
+    "vckss_rust_engine_prepare_v2": (i32, [C.c_void_p, C.c_void_p, C.POINTER(u64), u32]),
+    "vckss_rust_engine_prepare_v3": (i32, [C.c_void_p, C.c_void_p, C.POINTER(u64), u32]),
+    "vckss_rust_engine_prepare_interrupt_v1": (i32, [C.c_void_p, C.c_void_p, C.POINTER(u64), u32]),
+    "vckss_rust_engine_prepare_interrupt_v2": (i32, [C.c_void_p, C.c_void_p, C.POINTER(u64), u32]),
+    "vckss_rust_engine_prepare_interrupt_v4": (i32, [C.c_void_p, C.c_void_p, C.POINTER(u64), u32]),
+    "vckss_rust_engine_centering_v1": (i32, [u64, u32]),
+    "vckss_rust_engine_solve_v1": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_interrupt_v1": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_v5": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_interrupt_v5": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_result_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_preparation_receipt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_preparation_receipt_v2": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_preparation_receipt_v3": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_preparation_receipt_v4": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_retained_mask_v1": (i32, [u64, C.c_void_p, u64]),
+    "vckss_rust_engine_rhs_receipts_v1": (i32, [u64, C.c_void_p, u64]),
+    "vckss_rust_engine_rhs_receipts_v2": (i32, [u64, C.c_void_p, u64]),
+    "vckss_rust_engine_release_v1": (i32, [u64]),
+    "vckss_rust_engine_clear_abandoned_v1": (i32, []),
+    "vckss_rust_engine_snapshot_v1": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_last_error": (C.c_char_p, []),
+    "fevcb_device_count": (i32, []),
+    "fevcb_set_stream": (i32, [C.c_void_p]),
+    "fevcb_engine_solve_options_v1": (i32, [u64, C.c_void_p]),
+    "fevcb_engine_timings_v1": (i32, [u64, C.c_void_p, u32]),
+    "fevcb_engine_resolve_v1": (i32, [u64]),
+    "fevcb_engine_unit_detail_v1": (i32, [u64, u64] + [dptr] * 6 + [u64, dptr, dptr, u64, dptr]),
+    "fevcb_counter_atoms_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64, C.POINTER(i64)]),
+}
+
+LIBRARY_PATH = Path(__file__).resolve().parent / "libfevc_b200.so"
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+        self.message = message
+
+
+def load(path: str | os.PathLike | None = None, *, bind_extensions: bool = True) -> C.CDLL:
+    """Load a library exporting the plugin ABI (default: the in-tree build)."""
+    path = Path(path) if path else LIBRARY_PATH
+    if not path.exists():
+        raise FileNotFoundError(f"{path} is missing; run fevc_b200/build.py (or __graft_entry__.build())")
+    lib = C.CDLL(str(path), mode=os.RTLD_LOCAL | getattr(os, "RTLD_NOW", 2))
+    for name, (res, args) in SIGNATURES.items():
+        if name.startswith("fevcb_") and not bind_extensions:
+            continue
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+def _d(a: np.ndarray):
+    return a.ctypes.data_as(dptr)
+
+
+class Engine:
+    """One prepare/solve/result/release cycle against a plugin-ABI library."""
+
+    def __init__(self, lib: C.CDLL):
+        self.lib = lib
+        self.generation = 0
+        self._keep = []
+
+    def check(self, status: int) -> None:
+        if status != 0:
+            msg = self.lib.vckss_rust_engine_last_error()
+            raise EngineError(status, msg.decode() if msg else "")
+
+    # ---- preparation
+    def prepare(self, panel, *, deletion_mode: int = 1, implicit_match: bool = False, cleanup: bool = True,
+                use_v4: bool | None = None) -> int:
+        cols = [np.ascontiguousarray(x, dtype=np.float64) for x in (
+            panel.worker, panel.firm, panel.deletion, panel.outcome, panel.frequency, panel.target_weight)]
+        controls = [np.ascontiguousarray(c, dtype=np.float64) for c in getattr(panel, "controls", [])]
+        self._keep = cols + controls
+        rows = cols[0].shape[0]
+        c1 = ColumnsV1(C.sizeof(ColumnsV1), 0, rows, *[_d(x) for x in cols])
+        handle = u64(0)
+        if use_v4 is None:
+            use_v4 = bool(controls) or deletion_mode != 1 or implicit_match
+        if not use_v4:
+            req = PrepareRequestV1(1, C.sizeof(PrepareRequestV1), rows, int(cleanup), 0)
+            self.check(self.lib.vckss_rust_engine_prepare_v1(C.byref(req), C.byref(c1), C.byref(handle), 8))
+        else:
+            ctl_array = (dptr * max(1, len(controls)))(*[_d(c) for c in controls])
+            self._keep.append(ctl_array)
+            c2 = ColumnsV2(c1, C.cast(ctl_array, C.POINTER(dptr)) if controls else None, len(controls), 0)
+            c3 = ColumnsV3(c2, None, 0, 0)
+            v2 = PrepareRequestV2(1, C.sizeof(PrepareRequestV4), rows, int(cleanup), 0, 64 << 30, 0)
+            v3 = PrepareRequestV3(v2, deletion_mode, len(controls), 0)
+            v4 = PrepareRequestV4(v3, int(implicit_match), 0)
+            req = PrepareRequestInterruptV3(v4, InterruptPoll(0), None, 4096, 0)
+            self.check(self.lib.vckss_rust_engine_prepare_interrupt_v4(C.byref(req), C.byref(c3), C.byref(handle), 8))
+        self.generation = handle.value
+        return self.generation
+
+    def centering(self, mode: int) -> None:
+        self.check(self.lib.vckss_rust_engine_centering_v1(self.generation, mode))
+
+    def receipt(self) -> dict:
+        r = PreparationReceiptV4()
+        self.check(self.lib.vckss_rust_engine_preparation_receipt_v4(self.generation, C.byref(r), C.sizeof(r)))
+        d = r.v3.v2.as_dict()
+        d["target_weight_sum"] = r.v3.target_weight_sum
+        d["controls_count"] = r.controls_count
+        d["deletion_mode"] = r.deletion_mode
+        return d
+
+    def retained_mask(self, rows: int) -> np.ndarray:
+        out = np.zeros(rows, np.uint8)
+        self.check(self.lib.vckss_rust_engine_retained_mask_v1(self.generation, out.ctypes.data_as(C.c_void_p), rows))
+        return out
+
+    # ---- solve
+    def default_request(self) -> SolveRequestV1:
+        req = SolveRequestV1()
+        self.check(self.lib.vckss_rust_engine_default_solve_request_v1(C.byref(req), C.sizeof(req)))
+        return req
+
+    def solve(self, req: SolveRequestV1) -> None:
+        self.check(self.lib.vckss_rust_engine_solve_v1(self.generation, C.byref(req)))
+
+    def result(self) -> dict:
+        r = ResultV1()
+        self.check(self.lib.vckss_rust_engine_result_v1(self.generation, C.byref(r), C.sizeof(r)))
+        return {k: getattr(r, k).tuple() for k in ("plugin", "correction", "corrected", "numerical_mcse")}
+
+    def rhs_receipts(self, count: int) -> list[dict]:
+        arr = (RhsReceiptV1 * count)()
+        self.check(self.lib.vckss_rust_engine_rhs_receipts_v1(self.generation, arr, count))
+        return [a.as_dict() for a in arr]
+
+    def release(self) -> None:
+        if self.generation:
+            self.check(self.lib.vckss_rust_engine_release_v1(self.generation))
+            self.generation = 0
+
+    # ---- B200 extensions
+    def device_options(self, block_columns: int = 0, preconditioner: int = 0) -> None:
+        o = FevcbSolveOptionsV1(C.sizeof(FevcbSolveOptionsV1), block_columns, preconditioner, 1)
+        self.check(self.lib.fevcb_engine_solve_options_v1(self.generation, C.byref(o)))
+
+    def timings(self) -> dict:
+        t = FevcbSolveTimingsV1()
+        self.check(self.lib.fevcb_engine_timings_v1(self.generation, C.byref(t), C.sizeof(t)))
+        return t.as_dict()
+
+    def resolve(self) -> None:
+        self.check(self.lib.fevcb_engine_resolve_v1(self.generation))
+
+    def unit_detail(self, units: int, cells: int, probes: int) -> dict:
+        names = ("projection_share", "residual_share", "finite_bias", "finite_variance", "residual_mass",
+                 "deleted_mass")
+        arrs = {n: np.zeros(units) for n in names}
+        fitted, omega, draws = np.zeros(cells), np.zeros(cells), np.zeros(4 * probes)
+        self.check(self.lib.fevcb_engine_unit_detail_v1(
+            self.generation, units, *[_d(arrs[n]) for n in names], cells, _d(fitted), _d(omega), probes, _d(draws)))
+        arrs["fitted_cell"] = fitted
+        arrs["cell_correction_weight"] = omega
+        arrs["target_draws"] = draws.reshape(probes, 4)
+        return arrs
+
+
+def device_atoms(lib: C.CDLL, seed: int, tag: int, first_probe: int, columns: int, entity, trials) -> np.ndarray:
+    entity = np.ascontiguousarray(entity, dtype=np.uint64)
+    trials = np.ascontiguousarray(trials, dtype=np.uint64)
+    out = np.zeros(entity.size * columns, np.int64)
+    st = lib.fevcb_counter_atoms_v1(seed, tag, first_probe, columns, entity.ctypes.data_as(C.POINTER(u64)),
+                                    trials.ctypes.data_as(C.POINTER(u64)), entity.size,
+                                    out.ctypes.data_as(C.POINTER(i64)))
+    if st != 0:
+        raise EngineError(st, lib.vckss_rust_engine_last_error().decode())
+    return out.reshape(entity.size, columns)

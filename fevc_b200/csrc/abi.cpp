@@ -1,0 +1,966 @@
+// C ABI of the library: the reference plugin's engine entry points over the
+// host preparation and the device engine.  Semantics follow the reference
+// registry (vckss-plugin/src/context.rs:100-530): one active generation,
+// prepare -> solve -> result -> release, typed status codes with
+// thread-local text (ffi_engine.rs:2469-2498).
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+
+#include "fevc_b200.h"
+#include "counter_rng.h"
+#include "engine.h"
+#include "prep.h"
+
+using namespace fevcb;
+
+namespace {
+
+thread_local std::string g_last_error = "OK";
+
+template <class F>
+int32_t status(F&& f) {
+  try {
+    f();
+    g_last_error = "OK";
+    return OK;
+  } catch (const Error& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return ALLOCATION_FAILED;
+  } catch (const std::exception& e) {
+    g_last_error = std::string("contained exception: ") + e.what();
+    return PANIC;
+  } catch (...) {
+    g_last_error = "contained unknown exception";
+    return PANIC;
+  }
+}
+
+struct Interrupt {
+  VckssInterruptPollV1 poll = nullptr;
+  void* ctx = nullptr;
+  void check(const char* phase) const {
+    if (poll && poll(ctx) != VCKSS_INTERRUPT_CONTINUE) fail(USER_BREAK, phase, "interrupted by the caller");
+  }
+};
+
+enum class State : uint32_t { Empty = 0, Prepared = 1, Solving = 2, Solved = 3, Failed = 4 };
+
+struct Prepared {
+  Compressed problem;
+  JlaPlan plan;
+  bool has_plan = false;
+  GraphReceipt graph;
+  std::vector<uint8_t> retained;
+  uint64_t input_rows = 0;
+  uint64_t memory_limit = 0, caller_copy = 0;
+  uint32_t deletion_mode = VCKSS_DELETION_MATCH;
+  uint32_t controls = 0;
+  Centering centering = Centering::None;
+  FevcbSolveOptionsV1 device_options{sizeof(FevcbSolveOptionsV1), 0, 0, 0};
+  std::shared_ptr<DeviceEngine> device;
+  SolveOptions last_options;
+  bool solved_once = false;
+};
+
+struct Registry {
+  std::mutex mu;
+  uint64_t next = 1, last_released = 0, generation = 0;
+  State state = State::Empty;
+  std::unique_ptr<Prepared> prepared;
+  std::unique_ptr<SolveResult> result;
+  std::string failure;
+
+  Prepared& require(uint64_t g, const char* phase) {
+    if (state == State::Empty || g != generation)
+      fail(STALE_CONTEXT, phase, "generation " + std::to_string(g) + " is not the active context");
+    return *prepared;
+  }
+};
+
+Registry& reg() {
+  static Registry r;
+  return r;
+}
+
+template <class T>
+void require_capacity(const void* p, uint64_t cap, const char* label) {
+  if (!p) fail(INVALID_INPUT, "engine_ffi", std::string(label) + " pointer is null");
+  if (cap < sizeof(T))
+    fail(INVALID_INPUT, "engine_ffi",
+         std::string(label) + " capacity " + std::to_string(cap) + " is below " + std::to_string(sizeof(T)));
+}
+
+template <class T>
+T read_struct(const T* p, const char* label) {
+  if (!p) fail(INVALID_INPUT, "engine_ffi", std::string(label) + " pointer is null");
+  T v;
+  std::memcpy(&v, p, sizeof(T));
+  return v;
+}
+
+void require_abi(uint32_t v) {
+  if (v != VCKSS_RUST_ABI_VERSION_V1) fail(ABI_MISMATCH, "engine_ffi", "unsupported ABI version " + std::to_string(v));
+}
+
+void clear_abandoned(uint32_t flag) {
+  if (flag > 1) fail(INVALID_INPUT, "engine_prepare", "cleanup_abandoned must be zero or one");
+  Registry& r = reg();
+  if (flag && r.state != State::Empty) {
+    r.last_released = std::max(r.last_released, r.generation);
+    r.state = State::Empty;
+    r.prepared.reset();
+    r.result.reset();
+  }
+}
+
+struct PrepareArgs {
+  uint64_t rows;
+  uint32_t cleanup;
+  uint64_t memory_limit = 0, caller_copy = 0;
+  uint32_t deletion_mode = VCKSS_DELETION_MATCH;
+  uint32_t implicit_match = 0;
+  const VckssEngineColumnsV1* v1 = nullptr;
+  const double* const* controls = nullptr;
+  uint32_t controls_count = 0;
+  const double* probe_order = nullptr;
+  Interrupt interrupt;
+};
+
+void prepare_common(const PrepareArgs& a, uint64_t* out, uint32_t cap) {
+  require_capacity<uint64_t>(out, cap, "engine output handle");
+  uint64_t zero = 0;
+  std::memcpy(out, &zero, 8);
+  if (a.rows == 0 || a.rows != a.v1->rows)
+    fail(INVALID_INPUT, "engine_prepare", "request and column row counts must agree and be positive");
+  if (a.v1->reserved != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved preparation fields must be zero");
+  if (a.deletion_mode != VCKSS_DELETION_MATCH && a.deletion_mode != VCKSS_DELETION_OBSERVATION)
+    fail(INVALID_INPUT, "engine_prepare", "unknown deletion mode");
+  if (a.implicit_match && a.deletion_mode != VCKSS_DELETION_MATCH)
+    fail(INVALID_INPUT, "session_prepare", "implicit-match preparation requires match deletion");
+  {
+    std::lock_guard<std::mutex> l(reg().mu);
+    clear_abandoned(a.cleanup);
+    if (reg().state != State::Empty)
+      fail(CONTEXT_POISONED, "context_prepare",
+           "generation " + std::to_string(reg().generation) + " is still active; release it before preparing another context");
+  }
+  a.interrupt.check("engine_prepare_entry");
+  auto prep = std::make_unique<Prepared>();
+  InputColumns in = copy_columns(a.rows, a.v1->worker, a.v1->firm, a.v1->deletion, a.v1->outcome, a.v1->frequency,
+                                 a.v1->target_weight, a.controls, a.controls_count, a.probe_order);
+  a.interrupt.check("engine_ingest");
+  Canonical canon = canonicalize(std::move(in), a.implicit_match != 0);
+  a.interrupt.check("canonicalize_final");
+  if (a.deletion_mode == VCKSS_DELETION_OBSERVATION)
+    prep->retained = select_observation_graph(canon, prep->graph);
+  else if (a.implicit_match)
+    prep->retained = select_implicit_match_graph(canon, prep->graph);
+  else
+    prep->retained = select_match_graph(canon, prep->graph);
+  a.interrupt.check("graph_final");
+  prep->problem = compress(canon, prep->retained, a.implicit_match != 0);
+  a.interrupt.check("compression_final");
+  if (a.deletion_mode == VCKSS_DELETION_MATCH && prep->problem.controls.empty()) {
+    prep->plan = build_plan(prep->problem);
+    prep->has_plan = true;
+  }
+  prep->input_rows = a.rows;
+  prep->memory_limit = a.memory_limit;
+  prep->caller_copy = a.caller_copy;
+  prep->deletion_mode = a.deletion_mode;
+  prep->controls = a.controls_count;
+  a.interrupt.check("engine_prepare_final");
+  std::lock_guard<std::mutex> l(reg().mu);
+  Registry& r = reg();
+  if (r.state != State::Empty) fail(CONTEXT_POISONED, "context_prepare", "another generation became active");
+  r.generation = r.next++;
+  r.state = State::Prepared;
+  r.prepared = std::move(prep);
+  r.result.reset();
+  std::memcpy(out, &r.generation, 8);
+}
+
+SolveOptions options_from_v1(const VckssEngineSolveRequestV1& q) {
+  require_abi(q.abi_version);
+  if (q.deletion_mode != VCKSS_DELETION_MATCH)
+    fail(UNSUPPORTED_FEATURE, "jla_validate", "the compressed JLA engine supports match deletion only");
+  if (q.rng_contract != VCKSS_RNG_COUNTER_V1)
+    fail(UNSUPPORTED_FEATURE, "jla_validate", "the JLA engine supports VCKSS-COUNTER-V1 only");
+  if (q.probes < 2) fail(INVALID_INPUT, "jla_validate", "JLA probe count must be at least two");
+  if (q.leverage_batch_width == 0 || q.target_batch_width == 0)
+    fail(INVALID_INPUT, "jla_validate", "leverage and target batch widths must be positive");
+  if (!(q.rank_tolerance >= 1e-14 && q.rank_tolerance < 0.1))
+    fail(INVALID_INPUT, "jla_validate", "rank tolerance must be finite and lie in [1e-14, 0.1)");
+  if (!(q.block_tolerance >= 1e-14 && q.block_tolerance < 1.0))
+    fail(INVALID_INPUT, "jla_validate", "block tolerance must be finite and lie in [1e-14, 1)");
+  if (!(q.pcg_tolerance > 0.0 && q.pcg_tolerance < 1.0))
+    fail(INVALID_INPUT, "pcg", "PCG tolerance must lie in (0, 1)");
+  if (q.maximum_iterations == 0) fail(INVALID_INPUT, "pcg", "maximum iterations must be positive");
+  if (q.residual_replacement_interval == 0) fail(INVALID_INPUT, "pcg", "residual replacement interval must be positive");
+  if (q.solver_route > VCKSS_ROUTE_CMG_PCG) fail(INVALID_INPUT, "solver_router", "unknown solver route");
+  SolveOptions o;
+  o.seed = q.seed;
+  o.probes = q.probes;
+  o.leverage_batch_width = q.leverage_batch_width;
+  o.target_batch_width = q.target_batch_width;
+  o.pcg_tolerance = q.pcg_tolerance;
+  o.maximum_iterations = q.maximum_iterations;
+  o.residual_replacement_interval = q.residual_replacement_interval;
+  o.rank_tolerance = q.rank_tolerance;
+  o.block_tolerance = q.block_tolerance;
+  return o;
+}
+
+void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr) {
+  Registry& r = reg();
+  std::unique_lock<std::mutex> l(r.mu);
+  Prepared& p = r.require(g, "context_solve");
+  if (r.state != State::Prepared)
+    fail(STALE_CONTEXT, "context_solve", "generation " + std::to_string(g) + " is not in the prepared state");
+  if (!p.has_plan)
+    fail(UNSUPPORTED_FEATURE, "engine_solve", "the compressed JLA solve requires a prepared no-control match plan");
+  r.state = State::Solving;
+  try {
+    intr.check("jla_full_fit");
+    o.centering = p.centering;
+    o.block_columns = int(p.device_options.block_columns);
+    o.preconditioner = int(p.device_options.preconditioner);
+    if (!p.device) p.device = make_device_engine(p.problem, p.plan, o.preconditioner);
+    auto res = std::make_unique<SolveResult>(device_solve(*p.device, p.problem, p.plan, o, true));
+    intr.check("jla_finalize");
+    p.last_options = o;
+    p.solved_once = true;
+    r.result = std::move(res);
+    r.state = State::Solved;
+  } catch (...) {
+    r.state = State::Failed;
+    throw;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t vckss_rust_abi_version(void) { return VCKSS_RUST_ABI_VERSION_V1; }
+
+const char* vckss_rust_backend_version(void) { return "fevc-b200 0.1.0 (sm_100a)"; }
+
+const char* vckss_rust_capabilities_json(void) {
+  return "{\"backend\":\"fevc-b200\",\"abi\":1,\"device\":\"sm_100a\",\"rng\":\"VCKSS-COUNTER-V1\","
+         "\"algorithms\":[\"jla\"],\"deletion\":[\"match\"],\"centering\":[\"none\",\"mean\"],"
+         "\"solver\":\"blocked-pcg-hybrid-laplacian\"}";
+}
+
+const char* vckss_rust_last_error(void) { return g_last_error.c_str(); }
+const char* vckss_rust_engine_last_error(void) { return g_last_error.c_str(); }
+
+int32_t vckss_rust_selftest(void) {
+  return status([] {
+    // frozen Counter-V1 vectors (reference rust/crates/vckss-core/src/rng.rs:366-419)
+    uint64_t b[4];
+    philox_block(philox_key(123456789), 99, 17, 3, TAG_LEVERAGE, b);
+    if (b[0] != 0x9f4b6ea90b26b57dull || b[1] != 0x529b58b961489b78ull || b[2] != 0x9d84fab11898a6a0ull ||
+        b[3] != 0x469459830d836d27ull)
+      fail(RNG_CONTRACT_FAILED, "selftest", "Philox block vector mismatch");
+    int64_t s[4];
+    rademacher_block_sums(philox_key(123), TAG_LEVERAGE, 1, 7, 65, s);
+    if (s[1] != -5) fail(RNG_CONTRACT_FAILED, "selftest", "Rademacher sum vector mismatch");
+  });
+}
+
+int32_t vckss_rust_backend_capabilities_v1(VckssBackendCapabilitiesV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssBackendCapabilitiesV1>(out, cap, "capabilities");
+    VckssBackendCapabilitiesV1 c{};
+    c.struct_size = sizeof(c);
+    c.abi_version = 1;
+    c.core_ready_flags = (1ull << 0) | (1ull << 2) | (1ull << 3) | (1ull << 5) | (1ull << 6) | (1ull << 7);
+    c.support_flags = (1ull << 1) | (1ull << 2) | (1ull << 5) | (1ull << 6);
+    c.deterministic_parallelism = 1;
+    std::memcpy(out, &c, sizeof(c));
+  });
+}
+
+int32_t vckss_rust_engine_default_solve_request_v1(VckssEngineSolveRequestV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEngineSolveRequestV1>(out, cap, "engine default solve request");
+    VckssEngineSolveRequestV1 q{};
+    q.abi_version = 1;
+    q.struct_size = sizeof(q);
+    q.seed = 8675309;
+    q.probes = 200;
+    q.leverage_batch_width = 8;
+    q.target_batch_width = 8;
+    q.deletion_mode = VCKSS_DELETION_MATCH;
+    q.rng_contract = VCKSS_RNG_COUNTER_V1;
+    q.solver_route = VCKSS_ROUTE_AUTO;
+    q.allow_automatic_cmg_setup_fallback = 1;
+    q.exact_dimension_limit = 500;
+    q.cmg_minimum_dimension = 2000;
+    q.pcg_tolerance = 1e-10;
+    q.maximum_iterations = 10000;
+    q.residual_replacement_interval = 100;
+    q.rank_tolerance = 1e-10;
+    q.block_tolerance = 1e-10;
+    // CMG fields carry the reference defaults (vckss-core/src/cmg/hierarchy.rs:38-55)
+    q.cmg_terminal_vertices = 128;
+    q.cmg_dense_vertex_cap = 6144;
+    q.cmg_maximum_levels = 96;
+    q.cmg_aggregate_cap = 8;
+    q.cmg_minimum_reduction = 0.20;
+    q.cmg_jacobi_weight = 2.0 / 3.0;
+    q.cmg_pre_sweeps = 1;
+    q.cmg_post_sweeps = 1;
+    q.cmg_maximum_edge_complexity = 12.0;
+    q.cmg_maximum_vertex_complexity = 5.0;
+    q.cmg_memory_limit_bytes = 2ull << 30;
+    std::memcpy(out, &q, sizeof(q));
+  });
+}
+
+int32_t vckss_rust_engine_default_solve_request_v2(VckssEngineSolveRequestV2* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEngineSolveRequestV2>(out, cap, "V2 engine default solve request");
+    VckssEngineSolveRequestV2 q{};
+    if (vckss_rust_engine_default_solve_request_v1(&q.v1, sizeof(q.v1)) != OK) fail(PANIC, "defaults", "V1 defaults");
+    q.v1.struct_size = sizeof(q);
+    q.algorithm = VCKSS_ALGORITHM_JLA;
+    q.nuisance_mode = VCKSS_NUISANCE_JOINT;
+    q.exact_estimator_limit = 500;
+    q.blocksize_limit = 5000;
+    std::memcpy(out, &q, sizeof(q));
+  });
+}
+
+int32_t vckss_rust_engine_default_solve_request_v3(VckssEngineSolveRequestV3* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEngineSolveRequestV3>(out, cap, "V3 engine default solve request");
+    VckssEngineSolveRequestV3 q{};
+    if (vckss_rust_engine_default_solve_request_v2(&q.v2, sizeof(q.v2)) != OK) fail(PANIC, "defaults", "V2 defaults");
+    q.v2.v1.struct_size = sizeof(q);
+    q.v2.v1.solver_route = VCKSS_ROUTE_DIAGONAL_PCG;
+    q.v2.v1.allow_automatic_cmg_setup_fallback = 0;
+    q.engine = 2;
+    q.batch_mode = 1;
+    q.stayers_mode = 1;
+    q.target_weight_mode = 0;
+    q.deletion_unit_source = 1;
+    q.capability_schema = 2;
+    q.capability_profile = 3;
+    q.frequency_use = 0;
+    q.physical_limit = 50000000;
+    std::memcpy(out, &q, sizeof(q));
+  });
+}
+
+int32_t vckss_rust_engine_default_solve_request_v4(VckssEngineSolveRequestV4* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEngineSolveRequestV4>(out, cap, "V4 engine default solve request");
+    VckssEngineSolveRequestV4 q{};
+    if (vckss_rust_engine_default_solve_request_v3(&q.v3, sizeof(q.v3)) != OK) fail(PANIC, "defaults", "V3 defaults");
+    q.v3.v2.v1.struct_size = sizeof(q);
+    q.v3.v2.v1.solver_route = VCKSS_ROUTE_AUTO;
+    q.v3.v2.v1.leverage_batch_width = 0;
+    q.v3.v2.v1.target_batch_width = 0;
+    q.v3.v2.algorithm = VCKSS_ALGORITHM_AUTO;
+    q.v3.engine = 0;
+    q.v3.batch_mode = 0;
+    q.v3.capability_schema = 3;
+    q.v3.capability_profile = 4;
+    std::memcpy(out, &q, sizeof(q));
+  });
+}
+
+int32_t vckss_rust_engine_default_solve_request_v5(VckssEngineSolveRequestV5* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEngineSolveRequestV5>(out, cap, "V5 engine default solve request");
+    VckssEngineSolveRequestV5 q{};
+    if (vckss_rust_engine_default_solve_request_v4(&q.v4, sizeof(q.v4)) != OK) fail(PANIC, "defaults", "V4 defaults");
+    q.v4.v3.v2.v1.struct_size = sizeof(q);
+    q.threads = 1;
+    std::memcpy(out, &q, sizeof(q));
+  });
+}
+
+int32_t vckss_rust_engine_default_solve_request_interrupt_v1(VckssEngineSolveRequestInterruptV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEngineSolveRequestInterruptV1>(out, cap, "interrupt solve request");
+    VckssEngineSolveRequestInterruptV1 q{};
+    if (vckss_rust_engine_default_solve_request_v1(&q.options, sizeof(q.options)) != OK) fail(PANIC, "defaults", "V1");
+    q.checkpoint_interval = 4096;
+    std::memcpy(out, &q, sizeof(q));
+  });
+}
+
+int32_t vckss_rust_engine_default_solve_request_interrupt_v5(VckssEngineSolveRequestInterruptV5* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEngineSolveRequestInterruptV5>(out, cap, "interrupt V5 solve request");
+    VckssEngineSolveRequestInterruptV5 q{};
+    if (vckss_rust_engine_default_solve_request_v5(&q.options, sizeof(q.options)) != OK) fail(PANIC, "defaults", "V5");
+    q.checkpoint_interval = 4096;
+    std::memcpy(out, &q, sizeof(q));
+  });
+}
+
+int32_t vckss_rust_engine_default_prepare_request_v3(VckssEnginePrepareRequestV3* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEnginePrepareRequestV3>(out, cap, "V3 engine default prepare request");
+    VckssEnginePrepareRequestV3 q{};
+    q.v2.abi_version = 1;
+    q.v2.struct_size = sizeof(q);
+    q.v2.memory_limit_bytes = 4ull << 30;
+    q.deletion_mode = VCKSS_DELETION_MATCH;
+    std::memcpy(out, &q, sizeof(q));
+  });
+}
+
+int32_t vckss_rust_engine_default_prepare_request_interrupt_v1(VckssEnginePrepareRequestInterruptV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEnginePrepareRequestInterruptV1>(out, cap, "interrupt prepare request");
+    VckssEnginePrepareRequestInterruptV1 q{};
+    q.options.abi_version = 1;
+    q.options.struct_size = sizeof(q.options);
+    q.options.memory_limit_bytes = 4ull << 30;
+    q.checkpoint_interval = 4096;
+    std::memcpy(out, &q, sizeof(q));
+  });
+}
+
+int32_t vckss_rust_engine_default_prepare_request_interrupt_v2(VckssEnginePrepareRequestInterruptV2* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEnginePrepareRequestInterruptV2>(out, cap, "V2 interrupt prepare request");
+    VckssEnginePrepareRequestInterruptV2 q{};
+    q.options.v2.abi_version = 1;
+    q.options.v2.struct_size = sizeof(q.options);
+    q.options.v2.memory_limit_bytes = 4ull << 30;
+    q.options.deletion_mode = VCKSS_DELETION_MATCH;
+    q.checkpoint_interval = 4096;
+    std::memcpy(out, &q, sizeof(q));
+  });
+}
+
+int32_t vckss_rust_engine_default_prepare_request_interrupt_v3(VckssEnginePrepareRequestInterruptV3* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEnginePrepareRequestInterruptV3>(out, cap, "V3 interrupt prepare request");
+    VckssEnginePrepareRequestInterruptV3 q{};
+    q.options.v3.v2.abi_version = 1;
+    q.options.v3.v2.struct_size = sizeof(q.options);
+    q.options.v3.v2.memory_limit_bytes = 4ull << 30;
+    q.options.v3.deletion_mode = VCKSS_DELETION_MATCH;
+    q.checkpoint_interval = 4096;
+    std::memcpy(out, &q, sizeof(q));
+  });
+}
+
+int32_t vckss_rust_engine_prepare_v1(const VckssEnginePrepareRequestV1* request, const VckssEngineColumnsV1* columns,
+                                     uint64_t* out, uint32_t cap) {
+  return status([&] {
+    auto q = read_struct(request, "engine prepare request");
+    auto c = read_struct(columns, "engine column descriptor");
+    require_abi(q.abi_version);
+    if (q.reserved != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved preparation fields must be zero");
+    PrepareArgs a{q.rows, q.cleanup_abandoned};
+    a.v1 = &c;
+    prepare_common(a, out, cap);
+  });
+}
+
+int32_t vckss_rust_engine_prepare_v2(const VckssEnginePrepareRequestV2* request, const VckssEngineColumnsV1* columns,
+                                     uint64_t* out, uint32_t cap) {
+  return status([&] {
+    auto q = read_struct(request, "V2 engine prepare request");
+    auto c = read_struct(columns, "engine column descriptor");
+    require_abi(q.abi_version);
+    if (q.reserved != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved preparation fields must be zero");
+    PrepareArgs a{q.rows, q.cleanup_abandoned, q.memory_limit_bytes, q.caller_copy_bytes};
+    a.v1 = &c;
+    prepare_common(a, out, cap);
+  });
+}
+
+static void prepare_v3_impl(const VckssEnginePrepareRequestV3& q, const VckssEngineColumnsV2& c, const double* probe,
+                            uint32_t implicit, const Interrupt& intr, uint64_t* out, uint32_t cap) {
+  require_abi(q.v2.abi_version);
+  if (q.v2.reserved != 0 || q.reserved_2 != 0 || c.reserved_2 != 0)
+    fail(ABI_MISMATCH, "engine_ffi", "reserved V2 column fields must be zero");
+  if (q.controls_count != c.controls_count)
+    fail(INVALID_INPUT, "engine_prepare", "request and descriptor control counts disagree");
+  PrepareArgs a{q.v2.rows, q.v2.cleanup_abandoned, q.v2.memory_limit_bytes, q.v2.caller_copy_bytes};
+  a.deletion_mode = q.deletion_mode;
+  a.implicit_match = implicit;
+  a.v1 = &c.v1;
+  a.controls = c.controls;
+  a.controls_count = c.controls_count;
+  a.probe_order = probe;
+  a.interrupt = intr;
+  prepare_common(a, out, cap);
+}
+
+int32_t vckss_rust_engine_prepare_v3(const VckssEnginePrepareRequestV3* request, const VckssEngineColumnsV2* columns,
+                                     uint64_t* out, uint32_t cap) {
+  return status([&] {
+    auto q = read_struct(request, "V3 engine prepare request");
+    auto c = read_struct(columns, "V2 engine column descriptor");
+    prepare_v3_impl(q, c, nullptr, 0, Interrupt{}, out, cap);
+  });
+}
+
+int32_t vckss_rust_engine_prepare_interrupt_v1(const VckssEnginePrepareRequestInterruptV1* request,
+                                               const VckssEngineColumnsV1* columns, uint64_t* out, uint32_t cap) {
+  return status([&] {
+    auto q = read_struct(request, "interrupt engine prepare request");
+    auto c = read_struct(columns, "engine column descriptor");
+    require_abi(q.options.abi_version);
+    if (q.reserved != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved interrupt fields must be zero");
+    PrepareArgs a{q.options.rows, q.options.cleanup_abandoned, q.options.memory_limit_bytes, q.options.caller_copy_bytes};
+    a.v1 = &c;
+    a.interrupt = Interrupt{q.interrupt_poll, q.interrupt_context};
+    prepare_common(a, out, cap);
+  });
+}
+
+int32_t vckss_rust_engine_prepare_interrupt_v2(const VckssEnginePrepareRequestInterruptV2* request,
+                                               const VckssEngineColumnsV2* columns, uint64_t* out, uint32_t cap) {
+  return status([&] {
+    auto q = read_struct(request, "V2 interrupt engine prepare request");
+    auto c = read_struct(columns, "V2 engine column descriptor");
+    if (q.reserved != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved interrupt fields must be zero");
+    prepare_v3_impl(q.options, c, nullptr, 0, Interrupt{q.interrupt_poll, q.interrupt_context}, out, cap);
+  });
+}
+
+int32_t vckss_rust_engine_prepare_interrupt_v4(const VckssEnginePrepareRequestInterruptV3* request,
+                                               const VckssEngineColumnsV3* columns, uint64_t* out, uint32_t cap) {
+  return status([&] {
+    auto q = read_struct(request, "V3 interrupt engine prepare request");
+    auto c = read_struct(columns, "V3 engine column descriptor");
+    if (q.reserved != 0 || q.options.reserved_3 != 0 || c.reserved_3 != 0)
+      fail(ABI_MISMATCH, "engine_ffi", "reserved V3 fields must be zero");
+    if (q.options.implicit_match > 1) fail(INVALID_INPUT, "engine_prepare", "implicit_match must be zero or one");
+    if (c.probeorder_supplied > 1) fail(INVALID_INPUT, "engine_prepare", "probeorder_supplied must be zero or one");
+    prepare_v3_impl(q.options.v3, c.v2, c.probeorder_supplied ? c.probe_order : nullptr, q.options.implicit_match,
+                    Interrupt{q.interrupt_poll, q.interrupt_context}, out, cap);
+  });
+}
+
+int32_t vckss_rust_engine_centering_v1(uint64_t generation, uint32_t mode) {
+  return status([&] {
+    if (mode > 2) fail(INVALID_INPUT, "centering", "invalid mode");
+    if (mode == 2) fail(UNSUPPORTED_FEATURE, "centering", "Corrected centering is not provided by this backend");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "centering");
+    if (reg().state != State::Prepared) fail(STALE_CONTEXT, "centering", "generation is not in the prepared state");
+    p.centering = Centering(mode);
+  });
+}
+
+int32_t vckss_rust_engine_solve_v1(uint64_t generation, const VckssEngineSolveRequestV1* request) {
+  return status([&] {
+    auto q = read_struct(request, "engine solve request");
+    if (q.struct_size < sizeof(q)) fail(ABI_MISMATCH, "engine_ffi", "solve request struct_size is too small");
+    solve_common(generation, options_from_v1(q), Interrupt{});
+  });
+}
+
+int32_t vckss_rust_engine_solve_interrupt_v1(uint64_t generation, const VckssEngineSolveRequestInterruptV1* request) {
+  return status([&] {
+    auto q = read_struct(request, "interrupt engine solve request");
+    if (q.reserved != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved interrupt fields must be zero");
+    solve_common(generation, options_from_v1(q.options), Interrupt{q.interrupt_poll, q.interrupt_context});
+  });
+}
+
+static SolveOptions options_from_v5(const VckssEngineSolveRequestV5& q) {
+  VckssEngineSolveRequestV1 v1 = q.v4.v3.v2.v1;
+  if (v1.leverage_batch_width == 0) v1.leverage_batch_width = 8;
+  if (v1.target_batch_width == 0) v1.target_batch_width = 8;
+  if (q.v4.v3.v2.algorithm == VCKSS_ALGORITHM_EXACT)
+    fail(UNSUPPORTED_FEATURE, "engine_solve", "the exact estimator is not provided by the device engine");
+  SolveOptions o = options_from_v1(v1);
+  // Without a supplied tolerance the reference full-CMG route solves probes
+  // at 1e-6 (vckss-core/src/full_cmg.rs:29,56-69); the device engine keeps the
+  // request's fit tolerance for every right-hand side, which is never looser.
+  return o;
+}
+
+int32_t vckss_rust_engine_solve_v5(uint64_t generation, const VckssEngineSolveRequestV5* request) {
+  return status([&] {
+    auto q = read_struct(request, "V5 engine solve request");
+    solve_common(generation, options_from_v5(q), Interrupt{});
+  });
+}
+
+int32_t vckss_rust_engine_solve_interrupt_v5(uint64_t generation, const VckssEngineSolveRequestInterruptV5* request) {
+  return status([&] {
+    auto q = read_struct(request, "V5 interrupt engine solve request");
+    if (q.reserved != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved interrupt fields must be zero");
+    solve_common(generation, options_from_v5(q.options), Interrupt{q.interrupt_poll, q.interrupt_context});
+  });
+}
+
+int32_t vckss_rust_engine_result_v1(uint64_t generation, VckssEngineResultV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEngineResultV1>(out, cap, "engine result");
+    std::lock_guard<std::mutex> l(reg().mu);
+    reg().require(generation, "engine_result");
+    if (reg().state != State::Solved || !reg().result)
+      fail(STALE_CONTEXT, "engine_result", "generation has no solved result");
+    const SolveResult& s = *reg().result;
+    VckssEngineResultV1 r{};
+    r.struct_size = sizeof(r);
+    r.generation = generation;
+    r.plugin = {s.plugin.worker, s.plugin.firm, s.plugin.covariance, s.plugin.total};
+    r.correction = {s.correction.worker, s.correction.firm, s.correction.covariance, s.correction.total};
+    r.corrected = {s.corrected.worker, s.corrected.firm, s.corrected.covariance, s.corrected.total};
+    r.numerical_mcse = {s.mcse.worker, s.mcse.firm, s.mcse.covariance, s.mcse.total};
+    std::memcpy(out, &r, sizeof(r));
+  });
+}
+
+static VckssEnginePreparationReceiptV4 receipt_v4(uint64_t generation) {
+  Prepared& p = reg().require(generation, "engine_receipt");
+  const Compressed& c = p.problem;
+  VckssEnginePreparationReceiptV4 r{};
+  auto& v2 = r.v3.v2;
+  v2.generation = generation;
+  v2.input_rows = p.input_rows;
+  v2.retained_rows = c.rows();
+  v2.workers = c.workers;
+  v2.firms = c.firms;
+  v2.cells = c.cells;
+  v2.deletion_units = p.deletion_mode == VCKSS_DELETION_OBSERVATION ? c.physical_total : c.deletion_units;
+  v2.target_strata = p.has_plan ? p.plan.tgt_cell.size() : c.exact_target_strata;
+  v2.memory_limit_bytes = p.memory_limit;
+  v2.caller_copy_bytes = p.caller_copy;
+  uint64_t resident = c.rows() * (4 * 6 + 8 * 3) + c.cells * (4 * 2 + 8 * 3);
+  v2.preparation_peak_forecast_bytes = p.caller_copy + 2 * resident;
+  v2.prepared_resident_bytes = resident;
+  const GraphReceipt& g = p.graph;
+  v2.graph_input_rows = g.input_rows;
+  v2.graph_retained_rows = g.retained_rows;
+  v2.graph_input_physical_mass = g.input_physical_mass;
+  v2.graph_retained_physical_mass = g.retained_physical_mass;
+  v2.graph_initial_components = g.initial_components;
+  v2.graph_maximum_components = g.maximum_components;
+  v2.graph_initial_component_rows = g.initial_component_rows;
+  v2.graph_mover_input_rows = g.mover_input_rows;
+  v2.graph_initial_deletion_edges = g.initial_deletion_edges;
+  v2.graph_retained_deletion_edges = g.retained_deletion_edges;
+  v2.graph_insufficient_workers_removed = g.insufficient_workers_removed;
+  v2.graph_articulation_workers_removed = g.articulation_workers_removed;
+  v2.graph_bridge_units_removed = g.bridge_units_removed;
+  v2.graph_bridge_rows_removed = g.bridge_rows_removed;
+  v2.graph_degree_iterations = g.degree_iterations;
+  v2.graph_articulation_iterations = g.articulation_iterations;
+  v2.graph_bridge_iterations = g.bridge_iterations;
+  v2.graph_fixed_point_iterations = g.fixed_point_iterations;
+  r.v3.target_weight_sum = c.target_total;
+  r.controls_count = p.controls;
+  r.deletion_mode = p.deletion_mode;
+  return r;
+}
+
+int32_t vckss_rust_engine_preparation_receipt_v1(uint64_t generation, VckssEnginePreparationReceiptV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEnginePreparationReceiptV1>(out, cap, "preparation receipt");
+    std::lock_guard<std::mutex> l(reg().mu);
+    auto r4 = receipt_v4(generation);
+    VckssEnginePreparationReceiptV1 r{};
+    r.struct_size = sizeof(r);
+    const auto& v2 = r4.v3.v2;
+    r.generation = v2.generation;
+    r.input_rows = v2.input_rows;
+    r.retained_rows = v2.retained_rows;
+    r.workers = v2.workers;
+    r.firms = v2.firms;
+    r.cells = v2.cells;
+    r.deletion_units = v2.deletion_units;
+    r.target_strata = v2.target_strata;
+    std::memcpy(out, &r, sizeof(r));
+  });
+}
+
+int32_t vckss_rust_engine_preparation_receipt_v2(uint64_t generation, VckssEnginePreparationReceiptV2* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEnginePreparationReceiptV2>(out, cap, "V2 preparation receipt");
+    std::lock_guard<std::mutex> l(reg().mu);
+    auto r = receipt_v4(generation).v3.v2;
+    r.struct_size = sizeof(r);
+    std::memcpy(out, &r, sizeof(r));
+  });
+}
+
+int32_t vckss_rust_engine_preparation_receipt_v3(uint64_t generation, VckssEnginePreparationReceiptV3* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEnginePreparationReceiptV3>(out, cap, "V3 preparation receipt");
+    std::lock_guard<std::mutex> l(reg().mu);
+    auto r = receipt_v4(generation).v3;
+    r.v2.struct_size = sizeof(r);
+    std::memcpy(out, &r, sizeof(r));
+  });
+}
+
+int32_t vckss_rust_engine_preparation_receipt_v4(uint64_t generation, VckssEnginePreparationReceiptV4* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEnginePreparationReceiptV4>(out, cap, "V4 preparation receipt");
+    std::lock_guard<std::mutex> l(reg().mu);
+    auto r = receipt_v4(generation);
+    r.v3.v2.struct_size = sizeof(r);
+    std::memcpy(out, &r, sizeof(r));
+  });
+}
+
+int32_t vckss_rust_engine_retained_mask_v1(uint64_t generation, uint8_t* out, uint64_t cap) {
+  return status([&] {
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_retained");
+    if (!out || cap < p.retained.size())
+      fail(INVALID_INPUT, "engine_retained",
+           "retained-mask capacity " + std::to_string(cap) + " is below required size " + std::to_string(p.retained.size()));
+    std::memcpy(out, p.retained.data(), p.retained.size());
+  });
+}
+
+static void fill_rhs_v1(const RhsReceipt& s, VckssEngineRhsReceiptV1& r, uint32_t route) {
+  r.phase = s.phase;
+  r.side = s.side;
+  r.probe = s.probe;
+  r.route = route;
+  r.iterations = s.iterations;
+  r.zero_rhs = s.zero_rhs;
+  r.reserved = 0;
+  r.reduced_residual = s.reduced_residual;
+  r.complete_residual = s.complete_residual;
+}
+
+int32_t vckss_rust_engine_rhs_receipts_v1(uint64_t generation, VckssEngineRhsReceiptV1* out, uint64_t rows) {
+  return status([&] {
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_rhs_receipts");
+    if (reg().state != State::Solved) fail(STALE_CONTEXT, "engine_rhs_receipts", "generation has no solved result");
+    const auto& rc = reg().result->receipts;
+    if (!out || rows < rc.size())
+      fail(INVALID_INPUT, "engine_rhs_receipts", "RHS receipt capacity is below " + std::to_string(rc.size()));
+    uint32_t route = p.last_options.preconditioner == 1 ? VCKSS_ROUTE_DIAGONAL_PCG : VCKSS_ROUTE_CMG_PCG;
+    for (size_t i = 0; i < rc.size(); ++i) fill_rhs_v1(rc[i], out[i], route);
+  });
+}
+
+int32_t vckss_rust_engine_rhs_receipts_v2(uint64_t generation, VckssEngineRhsReceiptV2* out, uint64_t rows) {
+  return status([&] {
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_rhs_receipts");
+    if (reg().state != State::Solved) fail(STALE_CONTEXT, "engine_rhs_receipts", "generation has no solved result");
+    const auto& rc = reg().result->receipts;
+    if (!out || rows < rc.size())
+      fail(INVALID_INPUT, "engine_rhs_receipts", "RHS receipt capacity is below " + std::to_string(rc.size()));
+    uint32_t route = p.last_options.preconditioner == 1 ? VCKSS_ROUTE_DIAGONAL_PCG : VCKSS_ROUTE_CMG_PCG;
+    double gate = std::max(10.0 * p.last_options.pcg_tolerance, 1e-11);
+    for (size_t i = 0; i < rc.size(); ++i) {
+      VckssEngineRhsReceiptV2 r{};
+      fill_rhs_v1(rc[i], r.v1, route);
+      r.status = rc[i].zero_rhs ? 1 : 2;
+      r.operator_applications = rc[i].iterations + 1;
+      r.preconditioner_applications = rc[i].iterations + 1;
+      r.full_residual_tolerance = gate;
+      r.residual_space = 1;
+      r.solver_dimension = p.device ? device_stats(*p.device).vertices : p.problem.firms;
+      out[i] = r;
+    }
+  });
+}
+
+int32_t vckss_rust_engine_release_v1(uint64_t generation) {
+  return status([&] {
+    std::lock_guard<std::mutex> l(reg().mu);
+    Registry& r = reg();
+    if (r.state != State::Empty && r.generation == generation) {
+      r.state = State::Empty;
+      r.prepared.reset();
+      r.result.reset();
+      r.last_released = std::max(r.last_released, generation);
+      return;
+    }
+    if (r.state == State::Empty && generation <= r.last_released) return;
+    fail(STALE_CONTEXT, "context_release", "generation " + std::to_string(generation) + " is not active");
+  });
+}
+
+int32_t vckss_rust_engine_clear_abandoned_v1(void) {
+  return status([&] {
+    std::lock_guard<std::mutex> l(reg().mu);
+    clear_abandoned(1);
+  });
+}
+
+int32_t vckss_rust_engine_snapshot_v1(VckssEngineSnapshotV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEngineSnapshotV1>(out, cap, "engine snapshot");
+    std::lock_guard<std::mutex> l(reg().mu);
+    VckssEngineSnapshotV1 s{};
+    s.struct_size = sizeof(s);
+    s.state = uint32_t(reg().state);
+    s.generation = reg().state == State::Empty ? 0 : reg().generation;
+    s.last_released_generation = reg().last_released;
+    std::memcpy(out, &s, sizeof(s));
+  });
+}
+
+// ---------------- B200 extensions ----------------
+
+int32_t fevcb_device_count(void) { return device_count(); }
+
+int32_t fevcb_set_stream(void* stream) {
+  return status([&] { set_device_stream(stream); });
+}
+
+int32_t fevcb_engine_solve_options_v1(uint64_t generation, const FevcbSolveOptionsV1* options) {
+  return status([&] {
+    auto o = read_struct(options, "device solve options");
+    if (o.struct_size != sizeof(o)) fail(ABI_MISMATCH, "engine_ffi", "device solve options struct_size mismatch");
+    if (o.block_columns != 0 && o.block_columns != 8 && o.block_columns != 16 && o.block_columns != 32 &&
+        o.block_columns != 64)
+      fail(INVALID_INPUT, "engine_ffi", "block_columns must be 0, 8, 16, 32 or 64");
+    if (o.preconditioner > 2) fail(INVALID_INPUT, "engine_ffi", "preconditioner must be 0, 1 or 2");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_solve_options");
+    if (p.device && o.preconditioner != p.device_options.preconditioner) p.device.reset();
+    p.device_options = o;
+  });
+}
+
+int32_t fevcb_engine_timings_v1(uint64_t generation, FevcbSolveTimingsV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<FevcbSolveTimingsV1>(out, cap, "device timings");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_timings");
+    if (reg().state != State::Solved) fail(STALE_CONTEXT, "engine_timings", "generation has no solved result");
+    const SolveTimings& t = reg().result->timings;
+    FevcbSolveTimingsV1 r{};
+    r.struct_size = sizeof(r);
+    r.total_ms = t.total_ms;
+    r.fit_ms = t.fit_ms;
+    r.leverage_ms = t.leverage_ms;
+    r.target_ms = t.target_ms;
+    r.block_iterations = t.pcg_iterations;
+    r.column_iterations = t.column_iterations;
+    r.rhs_columns = t.rhs_columns;
+    r.kernel_launches = t.kernel_launches;
+    if (p.device) {
+      DeviceStats s = device_stats(*p.device);
+      r.setup_ms = s.setup_ms;
+      r.h2d_bytes = s.h2d_bytes;
+      r.vertices = s.vertices;
+      r.edges = s.edges;
+      r.kept_workers = s.kept_workers;
+      r.levels = s.levels;
+    }
+    std::memcpy(out, &r, sizeof(r));
+  });
+}
+
+int32_t fevcb_engine_resolve_v1(uint64_t generation) {
+  return status([&] {
+    Registry& r = reg();
+    std::lock_guard<std::mutex> l(r.mu);
+    Prepared& p = r.require(generation, "engine_resolve");
+    if (r.state != State::Solved || !p.solved_once || !p.device)
+      fail(STALE_CONTEXT, "engine_resolve", "generation has no solved result to repeat");
+    SolveOptions o = p.last_options;
+    o.block_columns = int(p.device_options.block_columns);
+    auto res = std::make_unique<SolveResult>(device_solve(*p.device, p.problem, p.plan, o, false));
+    r.result = std::move(res);
+  });
+}
+
+int32_t fevcb_engine_unit_detail_v1(uint64_t generation, uint64_t units, double* projection_share,
+                                    double* residual_share, double* finite_bias, double* finite_variance,
+                                    double* residual_mass, double* deleted_mass, uint64_t cells, double* fitted_cell,
+                                    double* cell_correction_weight, uint64_t probes, double* target_draws4) {
+  return status([&] {
+    std::lock_guard<std::mutex> l(reg().mu);
+    reg().require(generation, "engine_unit_detail");
+    if (reg().state != State::Solved) fail(STALE_CONTEXT, "engine_unit_detail", "generation has no solved result");
+    const SolveResult& s = *reg().result;
+    if (s.unit_projection_share.empty()) fail(STALE_CONTEXT, "engine_unit_detail", "unit detail was not retained");
+    if (units != s.unit_projection_share.size() || cells != s.fitted_cell.size() || probes != s.target_draws.size())
+      fail(INVALID_INPUT, "engine_unit_detail", "detail dimensions differ from the solved generation");
+    auto put = [&](double* dst, const std::vector<double>& v) {
+      if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(double));
+    };
+    put(projection_share, s.unit_projection_share);
+    put(residual_share, s.unit_residual_share);
+    put(finite_bias, s.unit_finite_bias);
+    put(finite_variance, s.unit_finite_variance);
+    put(residual_mass, s.unit_residual_mass);
+    put(deleted_mass, s.unit_deleted_mass);
+    put(fitted_cell, s.fitted_cell);
+    put(cell_correction_weight, s.cell_correction_weight);
+    if (target_draws4)
+      for (size_t i = 0; i < s.target_draws.size(); ++i) {
+        target_draws4[4 * i + 0] = s.target_draws[i].worker;
+        target_draws4[4 * i + 1] = s.target_draws[i].firm;
+        target_draws4[4 * i + 2] = s.target_draws[i].covariance;
+        target_draws4[4 * i + 3] = s.target_draws[i].total;
+      }
+  });
+}
+
+int32_t fevcb_engine_problem_view_v1(uint64_t generation, FevcbProblemViewV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<FevcbProblemViewV1>(out, cap, "problem view");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_problem_view");
+    if (!p.has_plan) fail(UNSUPPORTED_FEATURE, "engine_problem_view", "no compressed JLA plan was prepared");
+    const Compressed& c = p.problem;
+    const JlaPlan& j = p.plan;
+    FevcbProblemViewV1 v{};
+    v.struct_size = sizeof(v);
+    v.rows = c.rows();
+    v.workers = c.workers;
+    v.firms = c.firms;
+    v.cells = c.cells;
+    v.units = j.del_cell.size();
+    v.strata = j.tgt_cell.size();
+    v.physical_total = c.physical_total;
+    v.target_total = c.target_total;
+    v.row_worker = c.row_worker.data();
+    v.row_firm = c.row_firm.data();
+    v.row_cell = c.row_cell.data();
+    v.row_outcome = c.outcome.data();
+    v.row_target = c.target.data();
+    v.row_frequency = c.frequency.data();
+    v.cell_worker = c.cell_worker.data();
+    v.cell_firm = c.cell_firm.data();
+    v.cell_weight = c.cell_weight.data();
+    v.cell_outcome_sum = c.cell_outcome_sum.data();
+    v.cell_target_sum = c.cell_target_sum.data();
+    v.unit_cell = j.del_cell.data();
+    v.unit_count = j.del_count.data();
+    v.unit_rank = j.del_rank.data();
+    v.unit_outcome_sum = j.del_outcome_sum.data();
+    v.stratum_cell = j.tgt_cell.data();
+    v.stratum_per_copy = j.tgt_per_copy.data();
+    v.stratum_count = j.tgt_count.data();
+    v.stratum_rank = j.tgt_rank.data();
+    std::memcpy(out, &v, sizeof(v));
+  });
+}
+
+int32_t fevcb_counter_atoms_v1(uint64_t seed, uint64_t domain_tag, uint64_t first_probe, uint32_t columns,
+                               const uint64_t* entity, const uint64_t* trials, uint64_t count, int64_t* out) {
+  return status([&] {
+    if (!entity || !trials || !out || columns == 0 || count == 0)
+      fail(INVALID_INPUT, "counter_rng", "semantic atom request has incompatible dimensions");
+    device_atoms(seed, domain_tag, first_probe, columns, entity, trials, count, out);
+  });
+}
+
+}  // extern "C"

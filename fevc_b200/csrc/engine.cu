@@ -1,0 +1,1005 @@
+// JLA leave-out leverage engine on one B200.
+//
+// Prepared problem (resident in HBM for the life of a generation):
+//   cells      C: worker, firm, weight, outcome sum, target sum; cells of a
+//                 worker are contiguous (compression orders cells by worker)
+//   firm CSR   F: cells of each firm
+//   units      G: deletion units in cell order, with Counter-V1 entity rank
+//                 and trial count (reference plan `DeletionSemanticPlan`)
+//   strata     S: target strata in cell order (reference `TargetSemanticPlan`)
+//   hybrid Laplacian on n = F + kept-worker vertices: workers of small degree
+//                 are eliminated exactly (clique of conductances w_a w_b / d_w,
+//                 the firm Schur complement, reference operator.rs:205-262),
+//                 high-degree workers stay as star vertices (the hybrid graph
+//                 of reference cmg_impl.rs.in:78-364).
+// A solve runs blocks of K right-hand sides through one blocked PCG.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <numeric>
+
+#include "engine.h"
+#include "jla_kernels.cuh"
+#include "multigrid.h"
+
+namespace fevcb {
+
+// ---------------------------------------------------------------------------
+// kernels that are not templated
+
+__global__ void k_finish(const double* __restrict__ partial, int blocks, int width, double* __restrict__ out) {
+  __shared__ double sm[1024];
+  if (width <= int(blockDim.x)) {
+    int groups = blockDim.x / width;
+    int o = threadIdx.x % width, g = threadIdx.x / width;
+    double acc = 0.0;
+    if (g < groups)
+      for (int b = g; b < blocks; b += groups) acc += partial[size_t(b) * width + o];
+    sm[threadIdx.x] = acc;
+    __syncthreads();
+    if (g == 0) {
+      double s = 0.0;
+      for (int k = 0; k < groups; ++k) s += sm[k * width + o];
+      out[o] = s;
+    }
+  } else {
+    for (int oo = threadIdx.x; oo < width; oo += blockDim.x) {
+      double acc = 0.0;
+      for (int b = 0; b < blocks; ++b) acc += partial[size_t(b) * width + oo];
+      out[oo] = acc;
+    }
+  }
+}
+
+__global__ void k_raw_atoms(uint64_t count, const uint64_t* __restrict__ entity, const uint64_t* __restrict__ trials,
+                            PhiloxKey key, uint64_t tag, uint64_t first, uint32_t cols, int64_t* __restrict__ out) {
+  uint64_t blocks = (uint64_t(first % 4) + cols + 3) / 4;
+  uint64_t total = count * blocks;
+  for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += uint64_t(gridDim.x) * blockDim.x) {
+    uint64_t e = t / blocks, b = t % blocks;
+    uint64_t pb = first / 4 + b;
+    int64_t a[4];
+    rademacher_block_sums(key, tag, pb, entity[e], trials[e], a);
+    for (int l = 0; l < 4; ++l) {
+      uint64_t probe = pb * 4 + l;
+      if (probe >= first && probe < first + cols) out[e * cols + (probe - first)] = a[l];
+    }
+  }
+}
+
+__global__ void k_adjust(AdjustParams prm, const uint32_t* __restrict__ unit_ptr, const double* __restrict__ moments,
+                         const double* __restrict__ unit_outcome, const double* __restrict__ unit_count_f,
+                         const double* __restrict__ fitted_cell, double* __restrict__ unit_out,
+                         double* __restrict__ omega, unsigned long long* __restrict__ error) {
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < prm.cells; c += gridDim.x * blockDim.x) {
+    StableSumD w;
+    for (uint32_t g = unit_ptr[c]; g < unit_ptr[c + 1]; ++g) {
+      const double* m = moments + size_t(g) * 5;
+      double P = prm.probes;
+      double total_mean = (m[0] + m[1]) / P;
+      unsigned long long code = 0;
+      if (!isfinite(total_mean) || total_mean <= prm.block_tolerance) code = JLA_CONSTRAINT_FAILED;
+      double projection = (m[0] / P) / total_mean;
+      double residual = (m[1] / P) / total_mean;
+      double p2 = m[2] / P, m2 = m[3] / P, mixed = m[4] / P;
+      double bias = (residual * p2 - projection * m2 + (residual - projection) * mixed) / P;
+      double variance = (residual * residual * p2 + projection * projection * m2 - 2.0 * projection * residual * mixed) / P;
+      if (!code && !(isfinite(projection) && isfinite(residual) && isfinite(bias) && isfinite(variance)))
+        code = JLA_MOMENT_FAILED;
+      if (!code && variance < -100.0 * prm.rank_tolerance) code = JLA_MOMENT_FAILED;
+      variance = fmax(variance, 0.0);
+      double maker = 1.0 - projection;
+      if (!code && maker <= prm.block_tolerance) code = NONESTIMABLE_DELETION;
+      double rec = 1.0 / residual;
+      double rec_res = fabs(residual * rec - 1.0);
+      if (!code && (!isfinite(rec) || !isfinite(rec_res) || rec_res > fmax(100.0 * prm.rank_tolerance, 1.0e-10)))
+        code = BLOCK_INVERSE_FAILED;
+      double n = unit_count_f[g];
+      double residual_outcome = unit_outcome[g] - n * fitted_cell[c];
+      double multiplier = rec + bias * (rec * rec) - variance * (rec * rec * rec);
+      double deleted = residual_outcome * multiplier;
+      if (!code && !(isfinite(residual_outcome) && isfinite(multiplier) && isfinite(deleted))) code = CORRECTION_NONFINITE;
+      if (code) atomicMin(error, (unsigned long long)(g) << 8 | code);
+      w.add((unit_outcome[g] - prm.outcome_mean * n) * deleted);
+      double* o = unit_out + size_t(g) * 6;
+      o[0] = projection;
+      o[1] = residual;
+      o[2] = bias;
+      o[3] = variance;
+      o[4] = residual_outcome;
+      o[5] = deleted;
+    }
+    omega[c] = w.finish();
+  }
+}
+
+// fitted cell value and the plug-in reductions of the full fit (one column)
+__global__ void k_fit_cells(uint32_t cells, const uint32_t* __restrict__ cw, const uint32_t* __restrict__ cf,
+                            const double* __restrict__ alpha, const double* __restrict__ psi,
+                            const double* __restrict__ cell_target, double* __restrict__ fitted, int pass,
+                            const double* __restrict__ means, double* __restrict__ partial) {
+  double v[4][1] = {{0}, {0}, {0}, {0}};
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < cells; base += size_t(gridDim.x) * blockDim.x) {
+    size_t c = base + threadIdx.x;
+    if (c < cells) {
+      double a = alpha[cw[c]], b = psi[cf[c]], t = cell_target[c];
+      if (pass == 0) {
+        fitted[c] = a + b;
+        v[0][0] += t * a;
+        v[1][0] += t * b;
+      } else {
+        double ca = a - means[0], cb = b - means[1];
+        v[0][0] += t * ca * ca;
+        v[1][0] += t * cb * cb;
+        v[2][0] += t * ca * cb;
+        v[3][0] += t * (ca + cb) * (ca + cb);
+      }
+    }
+  }
+  block_reduce_cols<1, 4>(v, partial);
+}
+
+// ---------------------------------------------------------------------------
+// stream handling
+
+static std::mutex g_stream_mu;
+static cudaStream_t g_user_stream = nullptr;
+static bool g_user_stream_set = false;
+
+void set_device_stream(void* s) {
+  std::lock_guard<std::mutex> l(g_stream_mu);
+  g_user_stream = static_cast<cudaStream_t>(s);
+  g_user_stream_set = true;
+}
+
+void* device_stream() {
+  std::lock_guard<std::mutex> l(g_stream_mu);
+  return g_user_stream;
+}
+
+int device_count() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+static int grid_blocks() {
+  static int blocks = 0;
+  if (!blocks) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    blocks = sms * 4;  // four 256-thread blocks per SM for the streaming kernels
+  }
+  return blocks;
+}
+
+// ---------------------------------------------------------------------------
+// Device engine
+
+struct BlockWork;  // per-K workspace (defined below)
+
+struct DeviceEngine {
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  uint32_t W = 0, F = 0, C = 0, G = 0, S = 0, n = 0, kept = 0;
+  double target_total = 0;
+  DeviceStats stats;
+  // cells
+  DBuf<uint32_t> cell_worker, cell_firm, worker_ptr, firm_ptr, firm_cells, kept_worker;
+  DBuf<int32_t> kept_index;
+  DBuf<double> cell_weight, cell_outcome, cell_target, cell_scale, worker_diag, firm_diag;
+  // units (cell order)
+  DBuf<uint32_t> unit_ptr, unit_cell;
+  DBuf<uint64_t> unit_rank, unit_count;
+  DBuf<double> unit_outcome, unit_count_f, unit_sqrt_n;
+  std::vector<uint32_t> unit_group;  // cell-order position -> plan group
+  // strata
+  DBuf<uint32_t> tgt_ptr;
+  DBuf<uint64_t> tgt_rank, tgt_count;
+  DBuf<double> tgt_scale;
+  // hybrid Laplacian
+  DBuf<uint32_t> L_ptr, L_col;
+  DBuf<double> L_val, L_diag, L_dinv;
+  std::unique_ptr<Multigrid> mg;
+  int preconditioner = 1;
+  // solve-long buffers
+  DBuf<double> moments, unit_out, omega, fitted, fit_alpha, partial, small;
+  DBuf<unsigned long long> error;
+  std::map<int, std::unique_ptr<BlockWork>> work;
+  // pinned host scalars
+  int* h_nactive = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  ~DeviceEngine();
+};
+
+DeviceStats device_stats(const DeviceEngine& e) { return e.stats; }
+
+// Per block-width workspace and the captured PCG iteration graph.
+struct BlockWork {
+  int K;
+  DBuf<double> bW, bF, b, x, r, z, p, q, alpha, cell_val, unit_atoms, dir, tot;
+  DBuf<double> st;  // 8 * K doubles of per-column state
+  DBuf<int> ist;    // 2 * K + 2 ints
+  PcgState s;
+  cudaGraphExec_t graph = nullptr;
+  int graph_iters = 0;
+  ~BlockWork() {
+    if (graph) cudaGraphExecDestroy(graph);
+  }
+};
+
+DeviceEngine::~DeviceEngine() {
+  work.clear();
+  if (h_nactive) cudaFreeHost(h_nactive);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+namespace {
+
+constexpr uint32_t ELIMINATE_MAX_DEGREE = 16;
+
+// Host assembly of the hybrid Laplacian (conductances) from the cells.
+void build_hybrid(const Compressed& p, std::vector<uint32_t>& kept_worker, std::vector<int32_t>& kept_index,
+                  std::vector<double>& cell_scale, std::vector<double>& worker_diag, std::vector<uint32_t>& Lptr,
+                  std::vector<uint32_t>& Lcol, std::vector<double>& Lval, std::vector<double>& Ldiag) {
+  size_t W = p.workers, F = p.firms, C = p.cells;
+  worker_diag.assign(W, 0.0);
+  kept_index.assign(W, -1);
+  cell_scale.assign(C, 0.0);
+  const auto& wp = p.worker_index.ptr;
+  for (size_t w = 0; w < W; ++w) {
+    double d = 0.0;
+    for (uint64_t c = wp[w]; c < wp[w + 1]; ++c) d += p.cell_weight[c];
+    if (!(d > 0.0) || !std::isfinite(d))
+      fail(GRAPH_UNIDENTIFIED, "operator", "worker or firm information diagonal is not positive and finite");
+    worker_diag[w] = d;
+    if (wp[w + 1] - wp[w] > ELIMINATE_MAX_DEGREE) {
+      kept_index[w] = int32_t(kept_worker.size());
+      kept_worker.push_back(uint32_t(w));
+    }
+  }
+  size_t n = F + kept_worker.size();
+  // triplets (row, col, value) with row != col
+  std::vector<uint64_t> key;
+  std::vector<double> val;
+  for (size_t w = 0; w < W; ++w) {
+    uint64_t b = wp[w], e = wp[w + 1];
+    if (kept_index[w] >= 0) {
+      uint64_t v = F + kept_index[w];
+      for (uint64_t c = b; c < e; ++c) {
+        uint64_t f = p.cell_firm[c];
+        key.push_back((v << 32) | f);
+        val.push_back(p.cell_weight[c]);
+        key.push_back((f << 32) | v);
+        val.push_back(p.cell_weight[c]);
+      }
+    } else {
+      double d = worker_diag[w];
+      for (uint64_t c = b; c < e; ++c) cell_scale[c] = p.cell_weight[c] / d;
+      for (uint64_t i = b; i < e; ++i)
+        for (uint64_t j = b; j < e; ++j) {
+          if (i == j) continue;
+          key.push_back((uint64_t(p.cell_firm[i]) << 32) | p.cell_firm[j]);
+          val.push_back(p.cell_weight[i] * p.cell_weight[j] / d);
+        }
+    }
+  }
+  std::vector<uint32_t> order(key.size());
+  std::iota(order.begin(), order.end(), 0u);
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b] || (key[a] == key[b] && a < b); });
+  Lptr.assign(n + 1, 0);
+  Lcol.clear();
+  Lval.clear();
+  for (size_t i = 0; i < order.size();) {
+    uint64_t k = key[order[i]];
+    double s = 0.0;
+    while (i < order.size() && key[order[i]] == k) s += val[order[i++]];
+    Lcol.push_back(uint32_t(k & 0xffffffffu));
+    Lval.push_back(s);
+    Lptr[(k >> 32) + 1]++;
+  }
+  for (size_t v = 0; v < n; ++v) Lptr[v + 1] += Lptr[v];
+  Ldiag.assign(n, 0.0);
+  for (size_t v = 0; v < n; ++v) {
+    double s = 0.0;
+    for (uint32_t e = Lptr[v]; e < Lptr[v + 1]; ++e) s += Lval[e];
+    if (!(s > 0.0)) fail(GRAPH_UNIDENTIFIED, "operator", "hybrid Laplacian has an isolated vertex");
+    Ldiag[v] = s;
+  }
+}
+
+}  // namespace
+
+std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaPlan& plan, int preconditioner) {
+  if (device_count() < 1) fail(UNSUPPORTED_FEATURE, "device", "no CUDA device is visible; the engine runs only on a GPU");
+  auto t0 = std::chrono::steady_clock::now();
+  auto e = std::make_shared<DeviceEngine>();
+  {
+    std::lock_guard<std::mutex> l(g_stream_mu);
+    if (g_user_stream_set) {
+      e->stream = g_user_stream;
+    } else {
+      CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+      e->own_stream = true;
+    }
+  }
+  cudaStream_t s = e->stream;
+  uint64_t& h2d = e->stats.h2d_bytes;
+  e->W = uint32_t(p.workers);
+  e->F = uint32_t(p.firms);
+  e->C = uint32_t(p.cells);
+  e->G = uint32_t(plan.del_cell.size());
+  e->S = uint32_t(plan.tgt_cell.size());
+  e->target_total = p.target_total;
+
+  std::vector<uint32_t> wptr(p.worker_index.ptr.begin(), p.worker_index.ptr.end());
+  std::vector<uint32_t> fptr(p.firm_index.ptr.begin(), p.firm_index.ptr.end());
+  upload(e->cell_worker, p.cell_worker, s, h2d);
+  upload(e->cell_firm, p.cell_firm, s, h2d);
+  upload(e->cell_weight, p.cell_weight, s, h2d);
+  upload(e->cell_outcome, p.cell_outcome_sum, s, h2d);
+  upload(e->cell_target, p.cell_target_sum, s, h2d);
+  upload(e->worker_ptr, wptr, s, h2d);
+  upload(e->firm_ptr, fptr, s, h2d);
+  upload(e->firm_cells, p.firm_index.items, s, h2d);
+  {
+    std::vector<double> fd(p.firms, 0.0);
+    for (size_t c = 0; c < p.cells; ++c) fd[p.cell_firm[c]] += p.cell_weight[c];
+    upload(e->firm_diag, fd, s, h2d);
+  }
+
+  // units in cell order (stable within a cell: plan group order)
+  {
+    std::vector<uint32_t> uptr(p.cells + 1, 0);
+    for (uint32_t c : plan.del_cell) uptr[c + 1]++;
+    for (size_t c = 0; c < p.cells; ++c) uptr[c + 1] += uptr[c];
+    std::vector<uint32_t> cur(uptr.begin(), uptr.end() - 1);
+    e->unit_group.assign(plan.del_cell.size(), 0);
+    for (size_t g = 0; g < plan.del_cell.size(); ++g) e->unit_group[cur[plan.del_cell[g]]++] = uint32_t(g);
+    std::vector<uint32_t> ucell(e->G);
+    std::vector<uint64_t> urank(e->G), ucount(e->G);
+    std::vector<double> uout(e->G), ucf(e->G), usq(e->G);
+    for (size_t i = 0; i < e->G; ++i) {
+      uint32_t g = e->unit_group[i];
+      ucell[i] = plan.del_cell[g];
+      urank[i] = plan.del_rank[g];
+      ucount[i] = plan.del_count[g];
+      if (ucount[i] == 0 || ucount[i] > MAX_EXACT_BINARY64_INTEGER || (ucount[i] + 63) / 64 > MAX_WORDS_PER_ATOM)
+        fail(RESOURCE_LIMIT, "jla_validate", "leverage trial preflight failed");
+      uout[i] = plan.del_outcome_sum[g];
+      ucf[i] = double(plan.del_count[g]);
+      usq[i] = std::sqrt(ucf[i]);
+    }
+    upload(e->unit_ptr, uptr, s, h2d);
+    upload(e->unit_cell, ucell, s, h2d);
+    upload(e->unit_rank, urank, s, h2d);
+    upload(e->unit_count, ucount, s, h2d);
+    upload(e->unit_outcome, uout, s, h2d);
+    upload(e->unit_count_f, ucf, s, h2d);
+    upload(e->unit_sqrt_n, usq, s, h2d);
+  }
+  // strata (already in cell order)
+  {
+    std::vector<uint32_t> tptr(p.cells + 1, 0);
+    for (size_t k = 0; k < plan.tgt_cell.size(); ++k) {
+      if (k > 0 && plan.tgt_cell[k] < plan.tgt_cell[k - 1])
+        fail(INTERNAL_INVARIANT_FAILED, "jla_plan", "target strata are not in cell order");
+      tptr[plan.tgt_cell[k] + 1]++;
+      if (plan.tgt_count[k] == 0 || (plan.tgt_count[k] + 63) / 64 > MAX_WORDS_PER_ATOM)
+        fail(RESOURCE_LIMIT, "jla_validate", "target trial preflight failed");
+    }
+    for (size_t c = 0; c < p.cells; ++c) tptr[c + 1] += tptr[c];
+    std::vector<double> scale(plan.tgt_cell.size());
+    for (size_t k = 0; k < scale.size(); ++k) scale[k] = std::sqrt(plan.tgt_per_copy[k] / p.target_total);
+    upload(e->tgt_ptr, tptr, s, h2d);
+    upload(e->tgt_rank, plan.tgt_rank, s, h2d);
+    upload(e->tgt_count, plan.tgt_count, s, h2d);
+    upload(e->tgt_scale, scale, s, h2d);
+  }
+  // hybrid Laplacian
+  {
+    std::vector<uint32_t> kw, Lptr, Lcol;
+    std::vector<int32_t> ki;
+    std::vector<double> cs, wd, Lval, Ld;
+    build_hybrid(p, kw, ki, cs, wd, Lptr, Lcol, Lval, Ld);
+    e->kept = uint32_t(kw.size());
+    e->n = e->F + e->kept;
+    std::vector<double> dinv(Ld.size());
+    for (size_t v = 0; v < Ld.size(); ++v) dinv[v] = 1.0 / Ld[v];
+    upload(e->kept_worker, kw, s, h2d);
+    upload(e->kept_index, ki, s, h2d);
+    upload(e->cell_scale, cs, s, h2d);
+    upload(e->worker_diag, wd, s, h2d);
+    upload(e->L_ptr, Lptr, s, h2d);
+    upload(e->L_col, Lcol, s, h2d);
+    upload(e->L_val, Lval, s, h2d);
+    upload(e->L_diag, Ld, s, h2d);
+    upload(e->L_dinv, dinv, s, h2d);
+    e->stats.vertices = e->n;
+    e->stats.edges = Lcol.size() / 2;
+    e->stats.kept_workers = e->kept;
+    e->preconditioner = preconditioner == 0 ? 1 : preconditioner;
+    if (e->preconditioner == 2) {
+      e->mg = build_multigrid(e->n, Lptr, Lcol, Lval, Ld, s, h2d);
+      e->stats.levels = e->mg->levels();
+    } else {
+      e->stats.levels = 1;
+    }
+  }
+  e->moments.alloc(size_t(e->G) * 5);
+  e->unit_out.alloc(size_t(e->G) * 6);
+  e->omega.alloc(e->C);
+  e->fitted.alloc(e->C);
+  e->fit_alpha.alloc(e->W);
+  e->partial.alloc(size_t(grid_blocks()) * 4 * 128 + 1024);
+  e->small.alloc(1024);
+  e->error.alloc(1);
+  CK(cudaMallocHost(&e->h_nactive, sizeof(int) * 16));
+  CK(cudaEventCreate(&e->ev0));
+  CK(cudaEventCreate(&e->ev1));
+  CK(cudaStreamSynchronize(s));
+  e->stats.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// Blocked PCG on the hybrid Laplacian
+
+namespace {
+
+template <int K>
+BlockWork& get_work(DeviceEngine& e) {
+  auto it = e.work.find(K);
+  if (it != e.work.end()) return *it->second;
+  auto w = std::make_unique<BlockWork>();
+  w->K = K;
+  size_t n = e.n;
+  w->bW.alloc(size_t(e.W) * K);
+  w->bF.alloc(size_t(e.F) * K);
+  w->b.alloc(n * K);
+  w->x.alloc(n * K);
+  w->r.alloc(n * K);
+  w->z.alloc(n * K);
+  w->p.alloc(n * K);
+  w->q.alloc(n * K);
+  w->alpha.alloc(size_t(e.W) * K);
+  w->cell_val.alloc(size_t(e.C) * K);
+  w->unit_atoms.alloc(size_t(e.G) * K);
+  w->dir.alloc(size_t(e.C) * (K > 1 ? K / 2 : 1));
+  w->tot.alloc(4 * K);
+  w->st.alloc(8 * K);
+  w->ist.alloc(2 * K + 4);
+  double* st = w->st.p;
+  int* ist = w->ist.p;
+  w->s = PcgState{st, st + K, st + 2 * K, st + 3 * K, st + 4 * K, st + 5 * K, st + 6 * K,
+                  ist, ist + K, ist + 2 * K, ist + 2 * K + 1};
+  auto& ref = *w;
+  e.work[K] = std::move(w);
+  return ref;
+}
+
+// Initial state: r = b - mean(b), x = 0, z = M^-1 r, p = z, rz, tolerances.
+template <int K>
+__global__ void k_pcg_init_state(const double* __restrict__ sums, int ncols, double tol, double n, PcgState s) {
+  for (int j = threadIdx.x; j < K; j += blockDim.x) {
+    double sum = sums[j], sq = sums[K + j];
+    double mean = sum / n;
+    double bb = fmax(sq - n * mean * mean, 0.0);
+    s.mean[j] = mean;
+    s.bb[j] = bb;
+    s.tol2[j] = tol * tol * bb;
+    s.iters[j] = 0;
+    s.active[j] = (j < ncols && bb > 0.0) ? 1 : 0;
+    s.rr[j] = bb;
+  }
+  if (threadIdx.x == 0) {
+    *s.breakdown = -1;
+    *s.nactive = 0;
+  }
+}
+
+template <int K>
+__global__ void k_center(uint32_t n, const double* __restrict__ b, const double* __restrict__ mean,
+                         double* __restrict__ r, double* __restrict__ x) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  size_t total = size_t(n) * TPR;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
+    size_t i = (t / TPR) * K;
+    int c0 = int(t % TPR) * CPT;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      r[i + c0 + c] = b[i + c0 + c] - mean[c0 + c];
+      x[i + c0 + c] = 0.0;
+    }
+  }
+}
+
+template <int K>
+__global__ void k_set_rz(const double* __restrict__ partial, int blocks, PcgState s, int refine_only) {
+  __shared__ int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  for (int j = threadIdx.x; j < K; j += blockDim.x) {
+    double acc = 0.0;
+    for (int b = 0; b < blocks; ++b) acc += partial[size_t(b) * K + j];
+    s.rz[j] = acc;
+    if (s.active[j]) atomicAdd(&cnt, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *s.nactive = cnt;
+}
+
+template <int K>
+__global__ void k_jacobi(uint32_t n, const double* __restrict__ dinv, const double* __restrict__ r,
+                         double* __restrict__ z, double* __restrict__ p) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  size_t total = size_t(n) * TPR;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
+    size_t v = t / TPR;
+    size_t i = v * K + int(t % TPR) * CPT;
+    double d = dinv[v];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      double zi = d * r[i + c];
+      z[i + c] = zi;
+      if (p) p[i + c] = zi;
+    }
+  }
+}
+
+struct Launch {
+  int grid;
+  cudaStream_t s;
+};
+
+template <int K>
+void apply_preconditioner(DeviceEngine& e, BlockWork& w, Launch L, const double* r, double* z) {
+  if (e.preconditioner == 2) {
+    e.mg->apply(K, r, z, L.s);
+  } else {
+    k_jacobi<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_dinv.p, r, z, nullptr);
+  }
+}
+
+// One PCG iteration (all kernels enqueued on L.s).
+template <int K>
+void pcg_iteration(DeviceEngine& e, BlockWork& w, Launch L) {
+  double* part = e.partial.p;
+  double* part2 = e.partial.p + size_t(L.grid) * 2 * K;
+  k_spmm_dot<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_ptr.p, e.L_col.p, e.L_val.p, e.L_diag.p, w.p.p, w.q.p, part);
+  k_step_alpha<K><<<1, 128, 0, L.s>>>(part, L.grid, w.s);
+  if (e.preconditioner == 2) {
+    k_update_xr<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.p.p, w.q.p, w.x.p, w.r.p, w.s.alpha, part);
+    apply_preconditioner<K>(e, w, L, w.r.p, w.z.p);
+    k_dot<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.r.p, w.z.p, part2);
+    k_step_beta<K, 1><<<1, 128, 0, L.s>>>(part, L.grid, part2, L.grid, w.s);
+  } else {
+    k_update_jacobi<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_dinv.p, w.p.p, w.q.p, w.x.p, w.r.p, w.z.p, w.s.alpha, part);
+    k_step_beta<K, 2><<<1, 128, 0, L.s>>>(part, L.grid, nullptr, 0, w.s);
+  }
+  k_direction<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.z.p, w.p.p, w.s.beta);
+}
+
+constexpr int GRAPH_ITERS = 8;
+
+template <int K>
+void ensure_graph(DeviceEngine& e, BlockWork& w, Launch L) {
+  if (w.graph) return;
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(L.s, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < GRAPH_ITERS; ++i) pcg_iteration<K>(e, w, L);
+  CK(cudaStreamEndCapture(L.s, &g));
+  CK(cudaGraphInstantiate(&w.graph, g, 0));
+  cudaGraphDestroy(g);
+  w.graph_iters = GRAPH_ITERS;
+}
+
+// (Re)start PCG from the current x for the active columns: r = b - mean - L x,
+// z = M^-1 r, p = z, rz.  The mean of b is removed so every residual is
+// orthogonal to the Laplacian null space.
+template <int K>
+void pcg_restart(DeviceEngine& e, BlockWork& w, Launch L, bool fresh) {
+  if (fresh) {
+    k_center<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p, w.s.mean, w.r.p, w.x.p);
+  } else {
+    // r = (b - mean) - L x  via q as scratch
+    k_center<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p, w.s.mean, w.q.p, w.z.p);  // q = b - mean, z = 0
+    k_spmm<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_ptr.p, e.L_col.p, e.L_val.p, e.L_diag.p, w.x.p, w.q.p, w.r.p);
+  }
+  apply_preconditioner<K>(e, w, L, w.r.p, w.z.p);
+  CK(cudaMemcpyAsync(w.p.p, w.z.p, size_t(e.n) * K * sizeof(double), cudaMemcpyDeviceToDevice, L.s));
+  k_dot<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.r.p, w.z.p, e.partial.p);
+  k_set_rz<K><<<1, 128, 0, L.s>>>(e.partial.p, L.grid, w.s, 0);
+  CK_LAUNCH();
+}
+
+struct BlockOutcome {
+  std::vector<int> iters;
+  std::vector<double> reduced, complete;
+  std::vector<int> zero;
+  int block_iterations = 0;
+};
+
+// Solve the K right-hand sides held in w.bW / w.bF (columns >= ncols are zero).
+// On return w.alpha holds the worker solution and w.x[0, F) the firm solution.
+template <int K>
+BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOptions& o, SolveTimings& tm) {
+  Launch L{grid_blocks(), e.stream};
+  BlockOutcome out;
+  // hybrid RHS and its column sums
+  k_hybrid_rhs<K><<<L.grid, THREADS, 0, L.s>>>(e.F, e.kept, e.firm_ptr.p, e.firm_cells.p, e.cell_worker.p,
+                                                e.cell_scale.p, e.kept_worker.p, w.bW.p, w.bF.p, w.b.p, e.partial.p);
+  k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 2 * K, w.tot.p);
+  k_pcg_init_state<K><<<1, 128, 0, L.s>>>(w.tot.p, ncols, o.pcg_tolerance, double(e.n), w.s);
+  pcg_restart<K>(e, w, L, true);
+  ensure_graph<K>(e, w, L);
+  tm.kernel_launches += 6;
+
+  const double gate = std::max(10.0 * o.pcg_tolerance, 1e-11);
+  double tol = o.pcg_tolerance;
+  std::vector<double> h_rr(K), h_bb(K);
+  std::vector<int> h_it(K), h_active(K);
+  int total_iters = 0;
+  for (int ladder = 0;; ++ladder) {
+    for (;;) {
+      CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+      CK(cudaStreamSynchronize(L.s));
+      if (*e.h_nactive == 0) break;
+      if (total_iters >= int(o.maximum_iterations))
+        fail(PCG_MAX_ITERATIONS, "pcg", "blocked PCG reached the iteration limit " + std::to_string(o.maximum_iterations));
+      CK(cudaGraphLaunch(w.graph, L.s));
+      total_iters += w.graph_iters;
+      tm.kernel_launches += size_t(w.graph_iters) * (e.preconditioner == 2 ? 6 + e.mg->launches_per_apply() : 5);
+      tm.spmm_launches += w.graph_iters;
+    }
+    int bd = 0;
+    CK(cudaMemcpyAsync(&bd, w.s.breakdown, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    if (bd >= 0) fail(PCG_CURVATURE_BREAKDOWN, "pcg", "nonpositive curvature in column " + std::to_string(bd));
+
+    // extraction and complete residual
+    k_extract<K><<<L.grid, THREADS, 0, L.s>>>(e.W, e.F, e.worker_ptr.p, e.cell_firm.p, e.cell_weight.p,
+                                              e.worker_diag.p, e.kept_index.p, w.x.p, w.bW.p, w.alpha.p);
+    double* pw = e.partial.p;
+    double* pf = e.partial.p + size_t(L.grid) * 2 * K;
+    k_residual_workers<K><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, e.cell_firm.p, e.cell_weight.p,
+                                                       e.worker_diag.p, w.alpha.p, w.x.p, w.bW.p, pw);
+    k_residual_firms<K><<<L.grid, THREADS, 0, L.s>>>(e.F, e.firm_ptr.p, e.firm_cells.p, e.cell_worker.p,
+                                                     e.cell_weight.p, e.firm_diag.p, w.alpha.p, w.x.p, w.bF.p, pf);
+    k_finish<<<1, 1024, 0, L.s>>>(pw, L.grid, 2 * K, w.tot.p);
+    k_finish<<<1, 1024, 0, L.s>>>(pf, L.grid, 2 * K, w.tot.p + 2 * K);
+    tm.kernel_launches += 5;
+    std::vector<double> tot(4 * K);
+    CK(cudaMemcpyAsync(tot.data(), w.tot.p, 4 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaMemcpyAsync(h_rr.data(), w.s.rr, K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaMemcpyAsync(h_bb.data(), w.s.bb, K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaMemcpyAsync(h_it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    out.complete.assign(K, 0.0);
+    out.reduced.assign(K, 0.0);
+    out.iters.assign(h_it.begin(), h_it.end());
+    out.zero.assign(K, 0);
+    bool again = false;
+    for (int j = 0; j < K; ++j) {
+      double rw = tot[j], bw = tot[K + j], rf = tot[2 * K + j], bf = tot[3 * K + j];
+      double bn = std::sqrt(bw + bf), rn = std::sqrt(rw + rf);
+      out.complete[j] = bn == 0.0 ? rn : rn / bn;
+      out.reduced[j] = h_bb[j] > 0 ? std::sqrt(h_rr[j] / h_bb[j]) : 0.0;
+      out.zero[j] = (j < ncols && bn == 0.0) ? 1 : 0;
+      h_active[j] = (j < ncols && out.complete[j] > gate && h_bb[j] > 0) ? 1 : 0;
+      again |= h_active[j] != 0;
+    }
+    if (!again) break;
+    if (ladder >= 3) {
+      double worst = 0;
+      for (int j = 0; j < ncols; ++j) worst = std::max(worst, out.complete[j]);
+      fail(FULL_RESIDUAL_FAILED, "solver",
+           "complete normal-equation residual " + std::to_string(worst) + " exceeds tolerance " + std::to_string(gate));
+    }
+    // refinement ladder: tighten the reduced tolerance by 10x for failing columns
+    tol *= 0.1;
+    std::vector<double> tol2(K);
+    for (int j = 0; j < K; ++j) tol2[j] = tol * tol * h_bb[j];
+    CK(cudaMemcpyAsync(w.s.tol2, tol2.data(), K * sizeof(double), cudaMemcpyHostToDevice, L.s));
+    CK(cudaMemcpyAsync(w.s.active, h_active.data(), K * sizeof(int), cudaMemcpyHostToDevice, L.s));
+    pcg_restart<K>(e, w, L, false);
+  }
+  out.block_iterations = total_iters;
+  tm.pcg_iterations += total_iters;
+  for (int j = 0; j < ncols; ++j) tm.column_iterations += out.iters[j];
+  tm.rhs_columns += ncols;
+  return out;
+}
+
+Components finish_accounting(double w, double f, double c, double t, const char* phase) {
+  Components r{w, f, c, t};
+  double implied = w + f + 2.0 * c;
+  double scale = std::max({std::fabs(w), std::fabs(f), std::fabs(2.0 * c), std::fabs(t), 1.0});
+  if (!(std::isfinite(w) && std::isfinite(f) && std::isfinite(c) && std::isfinite(t)))
+    fail(CORRECTION_NONFINITE, phase, "variance component is nonfinite");
+  if (std::fabs(t - implied) > 1e-11 * scale)
+    fail(ACCOUNTING_IDENTITY_FAILED, phase, "total component differs from worker + firm + 2 covariance");
+  return r;
+}
+
+template <int K>
+void run_leverage(DeviceEngine& e, const SolveOptions& o, SolveResult& res, uint64_t tag_first_probe_unused) {
+  (void)tag_first_probe_unused;
+  BlockWork& w = get_work<K>(e);
+  Launch L{grid_blocks(), e.stream};
+  PhiloxKey key = philox_key(o.seed);
+  for (uint32_t first = 0; first < o.probes; first += K) {
+    int ncols = int(std::min<uint32_t>(K, o.probes - first));
+    k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p, key,
+                                                     TAG_LEVERAGE, first, ncols, w.unit_atoms.p, w.cell_val.p);
+    k_gather<K><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, w.cell_val.p, w.bW.p);
+    k_gather<K><<<L.grid, THREADS, 0, L.s>>>(e.F, e.firm_ptr.p, e.firm_cells.p, w.cell_val.p, w.bF.p);
+    CK_LAUNCH();
+    res.timings.kernel_launches += 3;
+    BlockOutcome bo = solve_block<K>(e, w, ncols, o, res.timings);
+    k_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.G, ncols, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
+                                              e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.moments.p);
+    CK_LAUNCH();
+    res.timings.kernel_launches += 1;
+    for (int j = 0; j < ncols; ++j)
+      res.receipts.push_back(RhsReceipt{2, 1, int64_t(first + j), uint32_t(bo.iters[j]), uint32_t(bo.zero[j]),
+                                        bo.reduced[j], bo.complete[j]});
+  }
+}
+
+template <int K>
+void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res) {
+  constexpr int H = K / 2;
+  BlockWork& w = get_work<K>(e);
+  Launch L{grid_blocks(), e.stream};
+  PhiloxKey key = philox_key(o.seed);
+  double invT = 1.0 / e.target_total;
+  res.target_draws.assign(o.probes, Components{});
+  std::vector<double> tot(2 * K), sums(2 * K), draws(3 * K);
+  for (uint32_t first = 0; first < o.probes; first += H) {
+    int np = int(std::min<uint32_t>(H, o.probes - first));
+    k_target_direction<H><<<L.grid, THREADS, 0, L.s>>>(e.C, e.tgt_ptr.p, e.tgt_rank.p, e.tgt_count.p,
+                                                       e.tgt_scale.p, key, first, np, w.dir.p);
+    // direction totals: sum_c d and the reference scale sum_c |d| + |sum_c d|
+    k_colsum_abs<H><<<L.grid, THREADS, 0, L.s>>>(e.C, w.dir.p, e.partial.p);
+    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 2 * H, w.tot.p);
+    CK(cudaMemcpyAsync(tot.data(), w.tot.p, 2 * H * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    k_target_scores<K><<<L.grid, THREADS, 0, L.s>>>(e.W, 0, e.worker_ptr.p, nullptr, w.dir.p, e.cell_target.p, invT,
+                                                    w.tot.p, w.bW.p);
+    k_target_scores<K><<<L.grid, THREADS, 0, L.s>>>(e.F, 1, e.firm_ptr.p, e.firm_cells.p, w.dir.p, e.cell_target.p,
+                                                    invT, w.tot.p, w.bF.p);
+    // balance repair (reference `balance_score_with_interrupt`, engine.rs:2812-2846):
+    // the last worker / firm entry becomes minus the sum of the others
+    k_colsum<K><<<L.grid, THREADS, 0, L.s>>>(e.W - 1, w.bW.p, e.partial.p);
+    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, K, w.tot.p + 2 * K);
+    k_colsum<K><<<L.grid, THREADS, 0, L.s>>>(e.F - 1, w.bF.p, e.partial.p);
+    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, K, w.tot.p + 3 * K);
+    std::vector<double> lastW(K), lastF(K), pre(2 * K);
+    CK(cudaMemcpyAsync(pre.data(), w.tot.p + 2 * K, 2 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaMemcpyAsync(lastW.data(), w.bW.p + size_t(e.W - 1) * K, K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaMemcpyAsync(lastF.data(), w.bF.p + size_t(e.F - 1) * K, K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    res.timings.kernel_launches += 9;
+    for (int q = 0; q < K; ++q) {
+      int j = q / 2;
+      if (j >= np) {
+        lastW[q] = 0.0;
+        lastF[q] = 0.0;
+        continue;
+      }
+      double ref = tot[H + j] + std::fabs(tot[j]);
+      if (!std::isfinite(ref) || ref < 0.0)
+        fail(TARGET_CENTERING_FAILED, "jla_target",
+             "target reference scale is invalid at probe " + std::to_string(first + j) + ", side centered");
+      double gate = 4096.0 * 2.220446049250313e-16 * ref;
+      double& last = (q & 1) ? lastF[q] : lastW[q];
+      double repaired = (q & 1) ? -pre[K + q] : -pre[q];
+      if ((ref == 0.0 && repaired != last) || (ref > 0.0 && std::fabs(repaired - last) > gate))
+        fail(TARGET_CENTERING_FAILED, "jla_target",
+             "compatibility repair exceeded roundoff at probe " + std::to_string(first + j) +
+                 ((q & 1) ? ", side Firm" : ", side Worker"));
+      last = repaired;
+    }
+    CK(cudaMemcpyAsync(w.bW.p + size_t(e.W - 1) * K, lastW.data(), K * sizeof(double), cudaMemcpyHostToDevice, L.s));
+    CK(cudaMemcpyAsync(w.bF.p + size_t(e.F - 1) * K, lastF.data(), K * sizeof(double), cudaMemcpyHostToDevice, L.s));
+    BlockOutcome bo = solve_block<K>(e, w, 2 * np, o, res.timings);
+    k_contract<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, e.omega.p, w.alpha.p, w.x.p,
+                                               e.partial.p);
+    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 3 * K, w.tot.p);
+    CK(cudaMemcpyAsync(draws.data(), w.tot.p, 3 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    res.timings.kernel_launches += 2;
+    for (int j = 0; j < np; ++j) {
+      double ww = draws[2 * j], ff = draws[K + 2 * j], cv = draws[2 * K + 2 * j];
+      Components d{ww, ff, cv, ww + ff + 2.0 * cv};
+      if (!(std::isfinite(ww) && std::isfinite(ff) && std::isfinite(cv)))
+        fail(CORRECTION_NONFINITE, "jla_target", "target contraction is nonfinite at probe " + std::to_string(first + j));
+      res.target_draws[first + j] = d;
+      res.receipts.push_back(RhsReceipt{3, 2, int64_t(first + j), uint32_t(bo.iters[2 * j]), uint32_t(bo.zero[2 * j]),
+                                        bo.reduced[2 * j], bo.complete[2 * j]});
+      res.receipts.push_back(RhsReceipt{3, 3, int64_t(first + j), uint32_t(bo.iters[2 * j + 1]),
+                                        uint32_t(bo.zero[2 * j + 1]), bo.reduced[2 * j + 1], bo.complete[2 * j + 1]});
+    }
+  }
+}
+
+double outcome_mean(const Compressed& p, Centering c) {
+  if (c == Centering::None) return 0.0;
+  // reference `centering::mean` (vckss-core/src/centering.rs:6-27)
+  double anchor = p.outcome[0];
+  StableSum s;
+  for (size_t r = 0; r < p.rows(); ++r) s.add((p.outcome[r] - anchor) * (double(p.frequency[r]) / double(p.physical_total)));
+  return anchor + s.finish();
+}
+
+template <int K>
+void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o, SolveResult& res,
+             bool detail) {
+  Launch L{grid_blocks(), e.stream};
+  auto now = [] { return std::chrono::steady_clock::now(); };
+  auto t0 = now();
+  // ---- full fit (one column)
+  {
+    BlockWork& w = get_work<1>(e);
+    k_gather<1><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, e.cell_outcome.p, w.bW.p);
+    k_gather<1><<<L.grid, THREADS, 0, L.s>>>(e.F, e.firm_ptr.p, e.firm_cells.p, e.cell_outcome.p, w.bF.p);
+    BlockOutcome bo = solve_block<1>(e, w, 1, o, res.timings);
+    res.receipts.push_back(RhsReceipt{1, 1, -1, uint32_t(bo.iters[0]), uint32_t(bo.zero[0]), bo.reduced[0], bo.complete[0]});
+    k_fit_cells<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p, e.cell_target.p,
+                                             e.fitted.p, 0, nullptr, e.partial.p);
+    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 4, e.small.p);
+    std::vector<double> m(4);
+    CK(cudaMemcpyAsync(m.data(), e.small.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    double means[2] = {m[0] / p.target_total, m[1] / p.target_total};
+    if (!std::isfinite(means[0]) || !std::isfinite(means[1]))
+      fail(CORRECTION_NONFINITE, "jla_plugin", "centered effect mean is nonfinite");
+    CK(cudaMemcpyAsync(e.small.p + 8, means, 2 * sizeof(double), cudaMemcpyHostToDevice, L.s));
+    k_fit_cells<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p, e.cell_target.p,
+                                             e.fitted.p, 1, e.small.p + 8, e.partial.p);
+    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 4, e.small.p);
+    CK(cudaMemcpyAsync(m.data(), e.small.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    double T = p.target_total;
+    res.plugin = finish_accounting(m[0] / T, m[1] / T, m[2] / T, m[3] / T, "jla_components");
+    res.timings.kernel_launches += 6;
+  }
+  auto t1 = now();
+  // ---- leverage
+  CK(cudaMemsetAsync(e.moments.p, 0, e.moments.bytes(), L.s));
+  run_leverage<K>(e, o, res, 0);
+  // ---- adjustment
+  {
+    AdjustParams prm{e.C, double(o.probes), o.block_tolerance, o.rank_tolerance, outcome_mean(p, o.centering)};
+    unsigned long long init = ~0ull;
+    CK(cudaMemcpyAsync(e.error.p, &init, sizeof(init), cudaMemcpyHostToDevice, L.s));
+    k_adjust<<<L.grid, THREADS, 0, L.s>>>(prm, e.unit_ptr.p, e.moments.p, e.unit_outcome.p, e.unit_count_f.p,
+                                          e.fitted.p, e.unit_out.p, e.omega.p, e.error.p);
+    unsigned long long err = 0;
+    CK(cudaMemcpyAsync(&err, e.error.p, sizeof(err), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    res.timings.kernel_launches += 1;
+    if (err != ~0ull) {
+      uint32_t code = uint32_t(err & 0xff);
+      uint32_t g = e.unit_group[err >> 8];
+      const char* what = code == JLA_CONSTRAINT_FAILED ? "projection/residual mass failed"
+                         : code == NONESTIMABLE_DELETION ? "match residual block is singular"
+                         : code == BLOCK_INVERSE_FAILED  ? "residual inverse gate failed"
+                         : code == JLA_MOMENT_FAILED     ? "finite-projection moment failed"
+                                                         : "match correction is nonfinite";
+      fail(int32_t(code), "jla_leverage", std::string(what) + " at unit " + std::to_string(g) + ", side joint");
+    }
+  }
+  auto t2 = now();
+  // ---- target
+  run_target<K>(e, o, res);
+  auto t3 = now();
+  // ---- components
+  {
+    StableSum s[4];
+    for (auto& d : res.target_draws) {
+      s[0].add(d.worker);
+      s[1].add(d.firm);
+      s[2].add(d.covariance);
+      s[3].add(d.total);
+    }
+    double P = double(o.probes);
+    Components corr{s[0].finish() / P, s[1].finish() / P, s[2].finish() / P, s[3].finish() / P};
+    res.correction = corr;
+    res.corrected = Components{res.plugin.worker - corr.worker, res.plugin.firm - corr.firm,
+                               res.plugin.covariance - corr.covariance, res.plugin.total - corr.total};
+    StableSum q[4];
+    for (auto& d : res.target_draws) {
+      q[0].add((d.worker - corr.worker) * (d.worker - corr.worker));
+      q[1].add((d.firm - corr.firm) * (d.firm - corr.firm));
+      q[2].add((d.covariance - corr.covariance) * (d.covariance - corr.covariance));
+      q[3].add((d.total - corr.total) * (d.total - corr.total));
+    }
+    double den = P * (P - 1.0);
+    res.mcse = Components{std::sqrt(q[0].finish() / den), std::sqrt(q[1].finish() / den), std::sqrt(q[2].finish() / den),
+                          std::sqrt(q[3].finish() / den)};
+  }
+  for (auto& r : res.receipts) {
+    res.max_reduced_residual = std::max(res.max_reduced_residual, r.reduced_residual);
+    res.max_complete_residual = std::max(res.max_complete_residual, r.complete_residual);
+  }
+  if (detail) {
+    std::vector<double> uo(size_t(e.G) * 6);
+    res.fitted_cell.resize(e.C);
+    res.cell_correction_weight.resize(e.C);
+    CK(cudaMemcpyAsync(uo.data(), e.unit_out.p, uo.size() * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaMemcpyAsync(res.fitted_cell.data(), e.fitted.p, e.C * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaMemcpyAsync(res.cell_correction_weight.data(), e.omega.p, e.C * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    size_t G = e.G;
+    res.unit_projection_share.assign(G, 0);
+    res.unit_residual_share.assign(G, 0);
+    res.unit_finite_bias.assign(G, 0);
+    res.unit_finite_variance.assign(G, 0);
+    res.unit_residual_mass.assign(G, 0);
+    res.unit_deleted_mass.assign(G, 0);
+    for (size_t i = 0; i < G; ++i) {
+      uint32_t g = e.unit_group[i];
+      res.unit_projection_share[g] = uo[i * 6 + 0];
+      res.unit_residual_share[g] = uo[i * 6 + 1];
+      res.unit_finite_bias[g] = uo[i * 6 + 2];
+      res.unit_finite_variance[g] = uo[i * 6 + 3];
+      res.unit_residual_mass[g] = uo[i * 6 + 4];
+      res.unit_deleted_mass[g] = uo[i * 6 + 5];
+      res.max_leverage = std::max(res.max_leverage, uo[i * 6 + 0]);
+    }
+  }
+  auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+  res.timings.fit_ms = ms(t0, t1);
+  res.timings.leverage_ms = ms(t1, t2);
+  res.timings.target_ms = ms(t2, t3);
+  res.timings.total_ms = ms(t0, now());
+}
+
+}  // namespace
+
+SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o,
+                         bool want_unit_detail) {
+  if (o.probes < 2) fail(INVALID_INPUT, "jla_validate", "JLA probe count must be at least two");
+  if (o.centering == Centering::Corrected)
+    fail(UNSUPPORTED_FEATURE, "centering", "Corrected centering is not provided by the device engine");
+  SolveResult res;
+  int K = o.block_columns;
+  if (K == 0) K = 32;
+  switch (K) {
+    case 8: run_jla<8>(e, p, plan, o, res, want_unit_detail); break;
+    case 16: run_jla<16>(e, p, plan, o, res, want_unit_detail); break;
+    case 32: run_jla<32>(e, p, plan, o, res, want_unit_detail); break;
+    case 64: run_jla<64>(e, p, plan, o, res, want_unit_detail); break;
+    default: fail(INVALID_INPUT, "jla_validate", "device block width must be 8, 16, 32 or 64");
+  }
+  return res;
+}
+
+void device_atoms(uint64_t seed, uint64_t tag, uint64_t first_probe, uint32_t columns, const uint64_t* entity,
+                  const uint64_t* trials, uint64_t count, int64_t* out) {
+  if (device_count() < 1) fail(UNSUPPORTED_FEATURE, "device", "no CUDA device is visible");
+  for (uint64_t i = 0; i < count; ++i)
+    if (trials[i] == 0 || trials[i] > MAX_EXACT_BINARY64_INTEGER)
+      fail(RNG_CONTRACT_FAILED, "counter_rng", "Rademacher trial count must lie in [1, 2^53]");
+  DBuf<uint64_t> de(count), dt(count);
+  DBuf<int64_t> dout(count * columns);
+  CK(cudaMemcpy(de.p, entity, count * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dt.p, trials, count * 8, cudaMemcpyHostToDevice));
+  k_raw_atoms<<<grid_blocks(), THREADS>>>(count, de.p, dt.p, philox_key(seed), tag, first_probe, columns, dout.p);
+  CK_LAUNCH();
+  CK(cudaMemcpy(out, dout.p, count * columns * 8, cudaMemcpyDeviceToHost));
+}
+
+}  // namespace fevcb

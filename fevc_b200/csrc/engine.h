@@ -1,0 +1,89 @@
+// Device engine: the prepared problem resident in HBM and the JLA solve.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "prep.h"
+
+namespace fevcb {
+
+struct Components {
+  double worker = 0, firm = 0, covariance = 0, total = 0;
+};
+
+enum class Centering : uint32_t { None = 0, Mean = 1, Corrected = 2 };
+
+struct SolveOptions {
+  uint64_t seed = 8675309;
+  uint32_t probes = 200;
+  uint32_t leverage_batch_width = 8;  // reference request field; the device block width is separate
+  uint32_t target_batch_width = 8;
+  double pcg_tolerance = 1e-10;
+  uint32_t maximum_iterations = 10000;
+  uint32_t residual_replacement_interval = 100;
+  double rank_tolerance = 1e-10;
+  double block_tolerance = 1e-10;
+  Centering centering = Centering::None;
+  int block_columns = 0;      // device RHS block width (0 = automatic)
+  int preconditioner = 0;     // 0 automatic, 1 Jacobi, 2 aggregation multigrid
+};
+
+// One receipt per solved right-hand side (reference `JlaRhsReceipt`,
+// vckss-core/src/engine.rs:185-195).
+struct RhsReceipt {
+  uint32_t phase;  // 1 fit, 2 leverage, 3 target
+  uint32_t side;   // 1 joint, 2 worker, 3 firm
+  int64_t probe;   // -1 for the fit
+  uint32_t iterations;
+  uint32_t zero_rhs;
+  double reduced_residual;
+  double complete_residual;
+};
+
+struct SolveTimings {
+  double total_ms = 0, fit_ms = 0, leverage_ms = 0, target_ms = 0;
+  uint64_t pcg_iterations = 0;      // summed over RHS blocks (block iterations)
+  uint64_t column_iterations = 0;   // summed over RHS columns
+  uint64_t rhs_columns = 0;
+  uint64_t kernel_launches = 0;
+  uint64_t spmm_launches = 0;
+  double spmm_ms = 0;               // device time of the SpMM launches (events)
+};
+
+struct SolveResult {
+  Components plugin, correction, corrected, mcse;
+  double weighted_rss = 0;
+  std::vector<double> fitted_cell;
+  std::vector<double> unit_projection_share, unit_residual_share, unit_finite_bias, unit_finite_variance;
+  std::vector<double> unit_residual_mass, unit_deleted_mass, cell_correction_weight;
+  std::vector<Components> target_draws;
+  std::vector<RhsReceipt> receipts;
+  double max_reduced_residual = 0, max_complete_residual = 0, max_leverage = 0;
+  SolveTimings timings;
+};
+
+struct DeviceEngine;  // opaque
+
+struct DeviceStats {
+  uint64_t h2d_bytes = 0;
+  uint64_t vertices = 0, edges = 0, kept_workers = 0, levels = 0;
+  double setup_ms = 0;
+};
+
+// Upload the prepared problem and build the solver.  Throws Error.
+std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaPlan& plan, int preconditioner);
+DeviceStats device_stats(const DeviceEngine& e);
+SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o,
+                         bool want_unit_detail);
+
+// Raw Counter-V1 atoms on the device (tests): out[e * columns + j] for probe first+j.
+void device_atoms(uint64_t seed, uint64_t tag, uint64_t first_probe, uint32_t columns, const uint64_t* entity,
+                  const uint64_t* trials, uint64_t count, int64_t* out);
+
+int device_count();
+void set_device_stream(void* stream);
+void* device_stream();
+
+}  // namespace fevcb

@@ -1,0 +1,344 @@
+// Estimator kernels around the solves: solution extraction, complete
+// normal-equation residuals, leverage moments, the leverage adjustment,
+// target directions / scores / balance repair and the target contraction.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace fevcb {
+
+// Worker solution from the hybrid solution x (firm part = psi):
+//   eliminated worker: alpha_w = (bW[w] - sum_{c in w} w_c psi_f(c)) / d_w
+//   kept worker:       alpha_w = -x[F + kept_index[w]]
+// Cells of a worker are contiguous: [worker_ptr[w], worker_ptr[w+1]).
+template <int K>
+__global__ void k_extract(uint32_t W, uint32_t F, const uint32_t* __restrict__ worker_ptr,
+                          const uint32_t* __restrict__ cell_firm, const double* __restrict__ cell_weight,
+                          const double* __restrict__ worker_diag, const int32_t* __restrict__ kept_index,
+                          const double* __restrict__ x, const double* __restrict__ bW, double* __restrict__ alpha) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  size_t total = size_t(W) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
+    size_t w = t / TPR;
+    int c0 = int(t % TPR) * CPT;
+    int32_t k = kept_index[w];
+    if (k >= 0) {
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) alpha[w * K + c0 + c] = -x[(size_t(F) + k) * K + c0 + c];
+    } else {
+      double acc[CPT];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) acc[c] = bW[w * K + c0 + c];
+      for (uint32_t i = worker_ptr[w]; i < worker_ptr[w + 1]; ++i) {
+        double a = cell_weight[i];
+        size_t fb = size_t(cell_firm[i]) * K + c0;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] -= a * x[fb + c];
+      }
+      double inv = 1.0 / worker_diag[w];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) alpha[w * K + c0 + c] = acc[c] * inv;
+    }
+  }
+}
+
+// Complete residual, worker rows: r_W = bW - d_w alpha_w - sum_c w_c psi_f.
+// partial[blk][0][K] = |r_W|^2, [1] = |bW|^2
+template <int K>
+__global__ void k_residual_workers(uint32_t W, const uint32_t* __restrict__ worker_ptr,
+                                   const uint32_t* __restrict__ cell_firm, const double* __restrict__ cell_weight,
+                                   const double* __restrict__ worker_diag, const double* __restrict__ alpha,
+                                   const double* __restrict__ psi, const double* __restrict__ bW,
+                                   double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  double v[2][CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
+  size_t total = size_t(W) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    if (t < total) {
+      size_t w = t / TPR;
+      int c0 = int(t % TPR) * CPT;
+      double d = worker_diag[w];
+      double acc[CPT];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) acc[c] = bW[w * K + c0 + c] - d * alpha[w * K + c0 + c];
+      for (uint32_t i = worker_ptr[w]; i < worker_ptr[w + 1]; ++i) {
+        double a = cell_weight[i];
+        size_t fb = size_t(cell_firm[i]) * K + c0;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] -= a * psi[fb + c];
+      }
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        double b = bW[w * K + c0 + c];
+        v[0][c] += acc[c] * acc[c];
+        v[1][c] += b * b;
+      }
+    }
+  }
+  block_reduce_cols<K, 2>(v, partial);
+}
+
+// Complete residual, firm rows: r_F = bF - d_f psi_f - sum_c w_c alpha_w.
+template <int K>
+__global__ void k_residual_firms(uint32_t F, const uint32_t* __restrict__ firm_ptr,
+                                 const uint32_t* __restrict__ firm_cells, const uint32_t* __restrict__ cell_worker,
+                                 const double* __restrict__ cell_weight, const double* __restrict__ firm_diag,
+                                 const double* __restrict__ alpha, const double* __restrict__ psi,
+                                 const double* __restrict__ bF, double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  double v[2][CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
+  size_t total = size_t(F) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    if (t < total) {
+      size_t f = t / TPR;
+      int c0 = int(t % TPR) * CPT;
+      double d = firm_diag[f];
+      double acc[CPT];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) acc[c] = bF[f * K + c0 + c] - d * psi[f * K + c0 + c];
+      for (uint32_t i = firm_ptr[f]; i < firm_ptr[f + 1]; ++i) {
+        uint32_t cell = firm_cells[i];
+        double a = cell_weight[cell];
+        size_t wb = size_t(cell_worker[cell]) * K + c0;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] -= a * alpha[wb + c];
+      }
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        double b = bF[f * K + c0 + c];
+        v[0][c] += acc[c] * acc[c];
+        v[1][c] += b * b;
+      }
+    }
+  }
+  block_reduce_cols<K, 2>(v, partial);
+}
+
+// Leverage moments per deletion unit (reference `FiveMoments`,
+// vckss-core/src/engine.rs:354-375, accumulation loop engine.rs:1190-1228):
+//   p = sqrt(n) (alpha_w + psi_f),  m = atom / sqrt(n) - p,
+//   moments[g] += (p^2, m^2, p^4, m^4, p^2 m^2) over the block's columns.
+template <int K>
+__global__ void k_moments(uint32_t units, int ncols, const uint32_t* __restrict__ unit_cell,
+                          const double* __restrict__ unit_sqrt_n, const uint32_t* __restrict__ cell_worker,
+                          const uint32_t* __restrict__ cell_firm, const double* __restrict__ alpha,
+                          const double* __restrict__ psi, const double* __restrict__ unit_atoms,
+                          double* __restrict__ moments) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  size_t total = size_t(units) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    double s[5] = {0, 0, 0, 0, 0};
+    size_t g = t / TPR;
+    int c0 = int(t % TPR) * CPT;
+    if (t < total) {
+      uint32_t cell = unit_cell[g];
+      size_t wb = size_t(cell_worker[cell]) * K + c0, fb = size_t(cell_firm[cell]) * K + c0;
+      double rn = unit_sqrt_n[g];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        if (c0 + c < ncols) {
+          double p = rn * (alpha[wb + c] + psi[fb + c]);
+          double m = unit_atoms[g * K + c0 + c] / rn - p;
+          double p2 = p * p, m2 = m * m;
+          s[0] += p2;
+          s[1] += m2;
+          s[2] += p2 * p2;
+          s[3] += m2 * m2;
+          s[4] += p2 * m2;
+        }
+      }
+    }
+    // combine the TPR threads of one unit (they sit in consecutive lanes)
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+#pragma unroll
+      for (int off = 1; off < TPR; off <<= 1) s[i] += __shfl_xor_sync(0xffffffffu, s[i], off);
+    if (t < total && (t % TPR) == 0) {
+#pragma unroll
+      for (int i = 0; i < 5; ++i) moments[g * 5 + i] += s[i];
+    }
+  }
+}
+
+struct AdjustParams {
+  uint32_t cells;
+  double probes;
+  double block_tolerance;
+  double rank_tolerance;
+  double outcome_mean;
+};
+
+// Leverage adjustment per cell over its deletion units in order (reference
+// `leverage_adjustment_with_interrupt`, vckss-core/src/engine.rs:2269-2410).
+// unit_out[g*6 + {0..5}] = projection, residual, bias, variance,
+// residual_outcome, deleted; omega[c] = cell correction weight.
+// error: atomicMin of (unit position << 8 | error code).
+__global__ void k_adjust(AdjustParams prm, const uint32_t* __restrict__ unit_ptr, const double* __restrict__ moments,
+                         const double* __restrict__ unit_outcome, const double* __restrict__ unit_count_f,
+                         const double* __restrict__ fitted_cell, double* __restrict__ unit_out,
+                         double* __restrict__ omega, unsigned long long* __restrict__ error);
+
+// Target directions for H probes starting at `first` (reference
+// `target_directions_with_interrupt`, engine.rs:2621-2700): per cell
+// d[c*H + j] = sum over the cell's strata of sqrt(per_copy/T) * atom.
+template <int H>
+__global__ void k_target_direction(uint32_t cells, const uint32_t* __restrict__ tgt_ptr,
+                                   const uint64_t* __restrict__ tgt_rank, const uint64_t* __restrict__ tgt_count,
+                                   const double* __restrict__ tgt_scale, PhiloxKey key, uint64_t first, int nprobes,
+                                   double* __restrict__ d) {
+  constexpr int B = (H + 3) / 4;
+  size_t total = size_t(cells) * B;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
+    uint32_t c = uint32_t(t / B);
+    int b = int(t % B);
+    StableSumD acc[4];
+    for (uint32_t s = tgt_ptr[c]; s < tgt_ptr[c + 1]; ++s) {
+      int64_t a[4];
+      rademacher_block_sums(key, TAG_TARGET, first / 4 + b, tgt_rank[s], tgt_count[s], a);
+      double sc = tgt_scale[s];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) acc[l].add(sc * double(a[l]));
+    }
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      int j = 4 * b + l;
+      if (j < H) d[size_t(c) * H + j] = (j < nprobes) ? acc[l].finish() : 0.0;
+    }
+  }
+}
+
+// Worker / firm target scores for the block's 2H right-hand sides:
+// column 2j is the worker side (score_W, 0), column 2j+1 the firm side (0, score_F).
+//   dtil_c = d[c][j] - (cell_target[c] / T) * total[j]
+// side == 0: rows are workers (cells contiguous: ptr = worker_ptr, idx = null)
+// side == 1: rows are firms (ptr = firm_ptr, idx = firm_cells)
+template <int K>
+__global__ void k_target_scores(uint32_t rows, int side, const uint32_t* __restrict__ ptr,
+                                const uint32_t* __restrict__ idx, const double* __restrict__ d,
+                                const double* __restrict__ cell_target, double inv_total,
+                                const double* __restrict__ total, double* __restrict__ out) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR, H = K / 2;
+  size_t N = size_t(rows) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < N; t += stride) {
+    size_t r = t / TPR;
+    int c0 = int(t % TPR) * CPT;
+    double acc[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
+    for (uint32_t i = ptr[r]; i < ptr[r + 1]; ++i) {
+      uint32_t cell = idx ? idx[i] : i;
+      double share = cell_target[cell] * inv_total;
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        int q = c0 + c;
+        if ((q & 1) == side) {
+          int j = q >> 1;
+          acc[c] += d[size_t(cell) * H + j] - share * total[j];
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) out[r * K + c0 + c] = acc[c];
+  }
+}
+
+// Column sums over rows [0, rows) of a K-block (used for the balance repair);
+// partial[blk][K].
+template <int K>
+__global__ void k_colsum(uint32_t rows, const double* __restrict__ x, double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  double v[1][CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) v[0][c] = 0.0;
+  int c0 = int(threadIdx.x % TPR) * CPT;
+  size_t total = size_t(rows) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    if (t < total) {
+      size_t i = (t / TPR) * K + c0;
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) v[0][c] += x[i + c];
+    }
+  }
+  block_reduce_cols<K, 1>(v, partial);
+}
+
+// Column sums and absolute sums over rows of an H-block (target direction
+// totals and the reference scale sum|d| + |sum d| of engine.rs:2667-2683).
+template <int K>
+__global__ void k_colsum_abs(uint32_t rows, const double* __restrict__ x, double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  double v[2][CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
+  int c0 = int(threadIdx.x % TPR) * CPT;
+  size_t total = size_t(rows) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    if (t < total) {
+      size_t i = (t / TPR) * K + c0;
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        v[0][c] += x[i + c];
+        v[1][c] += fabs(x[i + c]);
+      }
+    }
+  }
+  block_reduce_cols<K, 2>(v, partial);
+}
+
+// Target contraction (reference `contract_target_solutions_with_interrupt`,
+// engine.rs:3003-3047): for probe j, u_c = alpha^W_w + psi^W_f (column 2j),
+// v_c = alpha^F_w + psi^F_f (column 2j+1); partial sums of omega u^2,
+// omega v^2, omega u v land in the even column of each pair.
+template <int K>
+__global__ void k_contract(uint32_t cells, const uint32_t* __restrict__ cell_worker,
+                           const uint32_t* __restrict__ cell_firm, const double* __restrict__ omega,
+                           const double* __restrict__ alpha, const double* __restrict__ psi,
+                           double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  double v[3][CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = v[2][c] = 0.0;
+  size_t total = size_t(cells) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    double pred[CPT], wgt = 0.0;
+    int c0 = int(t % TPR) * CPT;
+    if (t < total) {
+      size_t c = t / TPR;
+      wgt = omega[c];
+      size_t wb = size_t(cell_worker[c]) * K + c0, fb = size_t(cell_firm[c]) * K + c0;
+#pragma unroll
+      for (int q = 0; q < CPT; ++q) pred[q] = alpha[wb + q] + psi[fb + q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < CPT; ++q) pred[q] = 0.0;
+    }
+    if (CPT == 1) {
+      double other = __shfl_xor_sync(0xffffffffu, pred[0], 1);
+      if ((c0 & 1) == 0) {
+        v[0][0] += wgt * pred[0] * pred[0];
+        v[1][0] += wgt * other * other;
+        v[2][0] += wgt * pred[0] * other;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q + 1 < CPT; q += 2) {
+        v[0][q] += wgt * pred[q] * pred[q];
+        v[1][q] += wgt * pred[q + 1] * pred[q + 1];
+        v[2][q] += wgt * pred[q] * pred[q + 1];
+      }
+    }
+  }
+  block_reduce_cols<K, 3>(v, partial);
+}
+
+}  // namespace fevcb

@@ -1,0 +1,894 @@
+// Host preparation, restated from the reference's ingest / canonicalize /
+// graph / compress / JLA-plan stages.  Orderings, tie rules, compensated sums
+// and error classes follow the cited reference functions so that retained
+// masks, dimensions, checksums and semantic ranks are bit-identical.
+#include "prep.h"
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+namespace fevcb {
+
+namespace {
+
+constexpr uint32_t MISSING = 0xffffffffu;
+
+std::vector<uint64_t> copy_integer(const double* p, uint64_t rows, const char* label, int32_t code) {
+  if (!p) fail(INVALID_INPUT, "engine_ingest", std::string(label) + " pointer is null");
+  if (reinterpret_cast<uintptr_t>(p) % alignof(double))
+    fail(INVALID_INPUT, "engine_ingest", std::string(label) + " pointer is not aligned for binary64 values");
+  std::vector<uint64_t> out(rows);
+  for (uint64_t r = 0; r < rows; ++r) {
+    double v = p[r];
+    if (!std::isfinite(v) || !(v > 0.0 && v <= double(MAX_EXACT_BINARY64_INTEGER)) || std::trunc(v) != v)
+      fail(code, "engine_ingest",
+           std::string(label) + " must be a positive exact binary64 integer at zero-based row " + std::to_string(r));
+    out[r] = uint64_t(v);
+  }
+  return out;
+}
+
+std::vector<double> copy_finite(const double* p, uint64_t rows, const char* label) {
+  if (!p) fail(INVALID_INPUT, "engine_ingest", std::string(label) + " pointer is null");
+  if (reinterpret_cast<uintptr_t>(p) % alignof(double))
+    fail(INVALID_INPUT, "engine_ingest", std::string(label) + " pointer is not aligned for binary64 values");
+  std::vector<double> out(p, p + rows);
+  for (uint64_t r = 0; r < rows; ++r)
+    if (!std::isfinite(out[r]))
+      fail(INVALID_INPUT, "engine_ingest", std::string(label) + " is nonfinite at zero-based row " + std::to_string(r));
+  return out;
+}
+
+// Reference `redense` (problem.rs:696-745): sorted distinct levels, dense ids.
+std::vector<uint32_t> redense(const std::vector<uint64_t>& values, std::vector<uint64_t>& levels, const char* label) {
+  levels = values;
+  std::sort(levels.begin(), levels.end());
+  levels.erase(std::unique(levels.begin(), levels.end()), levels.end());
+  if (levels.size() > 0xffffffffull)
+    fail(RESOURCE_LIMIT, "canonicalize", std::string(label) + " cardinality exceeds the u32 implementation limit");
+  std::vector<uint32_t> dense(values.size());
+  for (size_t i = 0; i < values.size(); ++i)
+    dense[i] = uint32_t(std::lower_bound(levels.begin(), levels.end(), values[i]) - levels.begin());
+  return dense;
+}
+
+void hash_word(uint64_t& h, uint64_t v) {
+  for (int b = 0; b < 8; ++b) {
+    h ^= (v >> (8 * b)) & 0xff;
+    h *= 0x00000100000001b3ull;
+  }
+}
+
+// Reference `topology_checksum` (problem.rs:1213-1248): FNV-1a over the sorted
+// (worker, firm, deletion, frequency) records, each word little-endian.
+uint64_t topology_checksum(const std::vector<uint32_t>& w, const std::vector<uint32_t>& f,
+                           const std::vector<uint32_t>& d, const std::vector<uint64_t>& q) {
+  size_t n = w.size();
+  std::vector<size_t> order(n);
+  std::iota(order.begin(), order.end(), size_t(0));
+  std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+    if (w[a] != w[b]) return w[a] < w[b];
+    if (f[a] != f[b]) return f[a] < f[b];
+    if (d[a] != d[b]) return d[a] < d[b];
+    return q[a] < q[b];
+  });
+  uint64_t h = 0xcbf29ce484222325ull;
+  for (size_t i : order) {
+    hash_word(h, w[i]);
+    hash_word(h, f[i]);
+    hash_word(h, d[i]);
+    hash_word(h, q[i]);
+  }
+  return h;
+}
+
+size_t count_true(const std::vector<uint8_t>& m) {
+  size_t c = 0;
+  for (uint8_t v : m) c += v;
+  return c;
+}
+
+// Bipartite graph with workers 0..W-1 and firms W..W+F-1 in CSR form.
+struct Graph {
+  size_t nodes = 0, edges = 0;
+  std::vector<uint64_t> ptr;
+  std::vector<uint32_t> to, edge;
+};
+
+Graph make_graph(size_t nodes, const std::vector<uint32_t>& eu, const std::vector<uint32_t>& ev) {
+  Graph g;
+  g.nodes = nodes;
+  g.edges = eu.size();
+  g.ptr.assign(nodes + 1, 0);
+  for (size_t e = 0; e < eu.size(); ++e) {
+    g.ptr[eu[e] + 1]++;
+    g.ptr[ev[e] + 1]++;
+  }
+  for (size_t v = 0; v < nodes; ++v) g.ptr[v + 1] += g.ptr[v];
+  g.to.resize(2 * eu.size());
+  g.edge.resize(2 * eu.size());
+  std::vector<uint64_t> cur(g.ptr.begin(), g.ptr.end() - 1);
+  for (size_t e = 0; e < eu.size(); ++e) {
+    uint64_t a = cur[eu[e]]++, b = cur[ev[e]]++;
+    g.to[a] = ev[e];
+    g.edge[a] = uint32_t(e);
+    g.to[b] = eu[e];
+    g.edge[b] = uint32_t(e);
+  }
+  return g;
+}
+
+void validate_mask(const Canonical& in, const std::vector<uint8_t>& active) {
+  if (active.size() != in.rows()) fail(INVALID_INPUT, "graph", "active mask has the wrong length");
+  if (count_true(active) == 0) fail(GRAPH_EMPTY, "graph", "active graph is empty");
+}
+
+// Reference `coordinate_graph` (graph.rs:707-760): distinct active (worker, firm) pairs.
+Graph coordinate_graph(const Canonical& in, const std::vector<uint8_t>& active) {
+  validate_mask(in, active);
+  std::vector<uint64_t> keys;
+  keys.reserve(in.rows());
+  for (size_t r = 0; r < in.rows(); ++r)
+    if (active[r]) keys.push_back((uint64_t(in.worker[r]) << 32) | in.firm[r]);
+  std::sort(keys.begin(), keys.end());
+  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+  std::vector<uint32_t> eu(keys.size()), ev(keys.size());
+  for (size_t e = 0; e < keys.size(); ++e) {
+    eu[e] = uint32_t(keys[e] >> 32);
+    ev[e] = uint32_t(in.workers + (keys[e] & 0xffffffffu));
+  }
+  return make_graph(in.workers + in.firms, eu, ev);
+}
+
+struct ComponentResult {
+  std::vector<uint8_t> keep;
+  size_t components = 0, retained_rows = 0;
+};
+
+// Reference `largest_component` (graph.rs:619-705): rank components by
+// (firm count, physical mass); a tie for the maximum is an identification error.
+ComponentResult largest_component(const Canonical& in, const std::vector<uint8_t>& active) {
+  Graph g = coordinate_graph(in, active);
+  std::vector<uint32_t> label(g.nodes, MISSING);
+  std::vector<uint32_t> queue;
+  queue.reserve(g.nodes);
+  size_t comps = 0;
+  for (size_t root = 0; root < g.nodes; ++root) {
+    if (g.ptr[root] == g.ptr[root + 1] || label[root] != MISSING) continue;
+    label[root] = uint32_t(comps);
+    queue.clear();
+    queue.push_back(uint32_t(root));
+    for (size_t h = 0; h < queue.size(); ++h) {
+      uint32_t v = queue[h];
+      for (uint64_t a = g.ptr[v]; a < g.ptr[v + 1]; ++a) {
+        uint32_t u = g.to[a];
+        if (label[u] == MISSING) {
+          label[u] = uint32_t(comps);
+          queue.push_back(u);
+        }
+      }
+    }
+    ++comps;
+  }
+  if (comps == 0) fail(GRAPH_EMPTY, "graph", "no connected worker-firm component remains");
+  std::vector<uint64_t> firms(comps, 0), mass(comps, 0);
+  for (size_t f = 0; f < in.firms; ++f) {
+    uint32_t c = label[in.workers + f];
+    if (c != MISSING) firms[c]++;
+  }
+  for (size_t r = 0; r < in.rows(); ++r) {
+    if (!active[r]) continue;
+    uint32_t c = label[in.worker[r]];
+    if (c == MISSING) fail(INTERNAL_INVARIANT_FAILED, "graph", "active row has no connected-component label");
+    mass[c] += in.frequency[r];
+  }
+  size_t best = 0;
+  for (size_t c = 1; c < comps; ++c)
+    if (firms[c] > firms[best] || (firms[c] == firms[best] && mass[c] > mass[best])) best = c;
+  size_t winners = 0;
+  for (size_t c = 0; c < comps; ++c) winners += (firms[c] == firms[best] && mass[c] == mass[best]);
+  if (winners != 1)
+    fail(GRAPH_UNIDENTIFIED, "graph", "multiple connected components tie for largest-component selection");
+  ComponentResult out;
+  out.components = comps;
+  out.keep.resize(in.rows());
+  for (size_t r = 0; r < in.rows(); ++r) {
+    out.keep[r] = active[r] && label[in.worker[r]] == best;
+    out.retained_rows += out.keep[r];
+  }
+  return out;
+}
+
+void intersect(std::vector<uint8_t>& active, const std::vector<uint8_t>& keep) {
+  for (size_t r = 0; r < active.size(); ++r) active[r] &= keep[r];
+}
+
+// Reference `distinct_deletion_counts` (graph.rs:762-781).
+std::vector<uint64_t> distinct_deletion_counts(const Canonical& in, const std::vector<uint8_t>& active) {
+  std::vector<uint8_t> seen(in.deletion_units, 0);
+  std::vector<uint64_t> counts(in.workers, 0);
+  for (size_t r = 0; r < in.rows(); ++r) {
+    if (!active[r] || seen[in.deletion[r]]) continue;
+    seen[in.deletion[r]] = 1;
+    counts[in.worker[r]]++;
+  }
+  return counts;
+}
+
+std::vector<uint64_t> worker_physical_counts(const Canonical& in, const std::vector<uint8_t>& active) {
+  validate_mask(in, active);
+  std::vector<uint64_t> counts(in.workers, 0);
+  for (size_t r = 0; r < in.rows(); ++r)
+    if (active[r]) counts[in.worker[r]] += in.frequency[r];
+  return counts;
+}
+
+// Iterative Tarjan low-link over a CSR multigraph.  The parent arc is skipped
+// by edge identity (not by endpoint), so parallel edges count as cycles.
+// Articulation vertices and bridges are properties of the graph, independent
+// of the traversal order (reference `articulation_vertices` graph.rs:872-936
+// and `bridge_edges` graph.rs:1031-1088).
+void tarjan(const Graph& g, std::vector<uint8_t>* articulation, std::vector<uint8_t>* bridge) {
+  size_t n = g.nodes;
+  std::vector<uint64_t> disc(n, 0), low(n, 0), next(n, 0);
+  std::vector<uint32_t> parent(n, MISSING), parent_edge(n, MISSING), children(n, 0);
+  if (articulation) articulation->assign(n, 0);
+  if (bridge) bridge->assign(g.edges, 0);
+  uint64_t clock = 0;
+  std::vector<uint32_t> stack;
+  for (size_t root = 0; root < n; ++root) {
+    if (g.ptr[root] == g.ptr[root + 1] || disc[root]) continue;
+    disc[root] = low[root] = ++clock;
+    next[root] = g.ptr[root];
+    stack.clear();
+    stack.push_back(uint32_t(root));
+    while (!stack.empty()) {
+      uint32_t v = stack.back();
+      if (next[v] < g.ptr[v + 1]) {
+        uint64_t a = next[v]++;
+        uint32_t u = g.to[a], e = g.edge[a];
+        if (e == parent_edge[v]) continue;
+        if (!disc[u]) {
+          parent[u] = v;
+          parent_edge[u] = e;
+          children[v]++;
+          disc[u] = low[u] = ++clock;
+          next[u] = g.ptr[u];
+          stack.push_back(u);
+        } else {
+          low[v] = std::min(low[v], disc[u]);
+        }
+      } else {
+        stack.pop_back();
+        uint32_t p = parent[v];
+        if (p != MISSING) {
+          if (bridge && low[v] > disc[p]) (*bridge)[parent_edge[v]] = 1;
+          low[p] = std::min(low[p], low[v]);
+          if (articulation && parent[p] != MISSING && low[v] >= disc[p]) (*articulation)[p] = 1;
+        }
+      }
+    }
+    if (articulation) (*articulation)[root] = children[root] > 1;
+  }
+}
+
+std::vector<uint8_t> worker_articulations(const Canonical& in, const std::vector<uint8_t>& active) {
+  Graph g = coordinate_graph(in, active);
+  std::vector<uint8_t> art;
+  tarjan(g, &art, nullptr);
+  art.resize(in.workers);
+  return art;
+}
+
+// Active deletion units as multigraph edges (reference `deletion_bridges`,
+// graph.rs:938-1029); returns the bridge deletion ids.
+std::vector<uint32_t> deletion_bridges(const Canonical& in, const std::vector<uint8_t>& active) {
+  validate_mask(in, active);
+  std::vector<uint32_t> cw(in.deletion_units, MISSING), cf(in.deletion_units, MISSING);
+  for (size_t r = 0; r < in.rows(); ++r) {
+    if (!active[r]) continue;
+    uint32_t d = in.deletion[r];
+    if (cw[d] == MISSING) {
+      cw[d] = in.worker[r];
+      cf[d] = in.firm[r];
+    } else if (cw[d] != in.worker[r] || cf[d] != in.firm[r]) {
+      fail(INTERNAL_INVARIANT_FAILED, "graph", "deletion unit crosses worker-firm coordinates");
+    }
+  }
+  std::vector<uint32_t> ids, eu, ev;
+  for (size_t d = 0; d < in.deletion_units; ++d)
+    if (cw[d] != MISSING) {
+      ids.push_back(uint32_t(d));
+      eu.push_back(cw[d]);
+      ev.push_back(uint32_t(in.workers + cf[d]));
+    }
+  if (ids.empty()) return {};
+  Graph g = make_graph(in.workers + in.firms, eu, ev);
+  std::vector<uint8_t> br;
+  tarjan(g, nullptr, &br);
+  std::vector<uint32_t> out;
+  for (size_t e = 0; e < ids.size(); ++e)
+    if (br[e]) out.push_back(ids[e]);
+  return out;
+}
+
+size_t active_deletion_count(const Canonical& in, const std::vector<uint8_t>& active) {
+  std::vector<uint8_t> seen(in.deletion_units, 0);
+  size_t c = 0;
+  for (size_t r = 0; r < in.rows(); ++r)
+    if (active[r] && !seen[in.deletion[r]]) {
+      seen[in.deletion[r]] = 1;
+      ++c;
+    }
+  return c;
+}
+
+GroupIndex grouped_rows(size_t groups, const std::vector<uint32_t>& row_group) {
+  GroupIndex gi;
+  gi.ptr.assign(groups + 1, 0);
+  for (uint32_t g : row_group) {
+    if (g >= groups) fail(INTERNAL_INVARIANT_FAILED, "compression", "row group exceeds group count");
+    gi.ptr[g + 1]++;
+  }
+  for (size_t g = 0; g < groups; ++g) gi.ptr[g + 1] += gi.ptr[g];
+  std::vector<uint64_t> cur(gi.ptr.begin(), gi.ptr.end() - 1);
+  gi.items.resize(row_group.size());
+  for (size_t r = 0; r < row_group.size(); ++r) gi.items[cur[row_group[r]]++] = uint32_t(r);
+  return gi;
+}
+
+GroupIndex grouped_from_order(size_t groups, const std::vector<uint32_t>& group_of, std::vector<uint32_t>&& order) {
+  GroupIndex gi;
+  gi.ptr.assign(groups + 1, 0);
+  for (uint32_t it : order) gi.ptr[group_of[it] + 1]++;
+  for (size_t g = 0; g < groups; ++g) gi.ptr[g + 1] += gi.ptr[g];
+  gi.items = std::move(order);
+  return gi;
+}
+
+}  // namespace
+
+InputColumns copy_columns(uint64_t rows, const double* worker, const double* firm, const double* deletion,
+                          const double* outcome, const double* frequency, const double* target,
+                          const double* const* controls, uint32_t controls_count, const double* probe_order) {
+  InputColumns c;
+  c.worker = copy_integer(worker, rows, "worker identifier", INVALID_IDENTIFIER);
+  c.firm = copy_integer(firm, rows, "firm identifier", INVALID_IDENTIFIER);
+  c.deletion = copy_integer(deletion, rows, "deletion identifier", INVALID_IDENTIFIER);
+  c.outcome = copy_finite(outcome, rows, "outcome");
+  c.frequency = copy_integer(frequency, rows, "frequency weight", INVALID_WEIGHT);
+  if (!target) fail(INVALID_INPUT, "engine_ingest", "target weight pointer is null");
+  c.target.assign(target, target + rows);
+  for (uint64_t r = 0; r < rows; ++r)
+    if (!std::isfinite(c.target[r]) || c.target[r] < 0.0)
+      fail(INVALID_TARGET_WEIGHT, "engine_ingest",
+           "target weight is negative or nonfinite at zero-based row " + std::to_string(r));
+  if (controls_count == 0) {
+    if (controls) fail(INVALID_INPUT, "engine_prepare", "zero controls require a null control-pointer array");
+  } else {
+    if (!controls) fail(INVALID_INPUT, "engine_prepare", "positive control count requires a control-pointer array");
+    for (uint32_t k = 0; k < controls_count; ++k) c.controls.push_back(copy_finite(controls[k], rows, "control"));
+  }
+  if (probe_order) c.probe_order = copy_finite(probe_order, rows, "probe-order value");
+  return c;
+}
+
+Canonical canonicalize(InputColumns&& in, bool implicit_match) {
+  size_t n = in.worker.size();
+  if (n == 0) fail(INVALID_INPUT, "ingest", "input sample is empty");
+  if (in.firm.size() != n || in.deletion.size() != n || in.outcome.size() != n || in.frequency.size() != n ||
+      in.target.size() != n)
+    fail(INVALID_INPUT, "ingest", "input columns have inconsistent lengths");
+  for (auto& c : in.controls)
+    if (c.size() != n) fail(INVALID_INPUT, "ingest", "input columns have inconsistent lengths");
+  uint64_t physical = 0;
+  double target_total = 0.0;
+  for (size_t r = 0; r < n; ++r) {
+    if (!std::isfinite(in.outcome[r]))
+      fail(INVALID_INPUT, "ingest", "outcome is nonfinite at zero-based row " + std::to_string(r));
+    if (in.frequency[r] == 0) fail(INVALID_WEIGHT, "ingest", "frequency is zero at zero-based row " + std::to_string(r));
+    if (!std::isfinite(in.target[r]) || in.target[r] < 0.0)
+      fail(INVALID_TARGET_WEIGHT, "ingest", "target weight is invalid at zero-based row " + std::to_string(r));
+    for (auto& c : in.controls)
+      if (!std::isfinite(c[r])) fail(INVALID_INPUT, "ingest", "control is nonfinite at zero-based row " + std::to_string(r));
+    physical += in.frequency[r];
+    if (physical < in.frequency[r]) fail(RESOURCE_LIMIT, "ingest", "physical-frequency total overflow");
+    if (physical > MAX_EXACT_BINARY64_INTEGER)
+      fail(RESOURCE_LIMIT, "ingest", "literal physical-frequency total exceeds the exact binary64 integer range");
+    target_total += in.target[r];
+  }
+  if (!std::isfinite(target_total) || target_total <= 0.0)
+    fail(INVALID_TARGET_WEIGHT, "ingest", "target weights must have positive finite total mass");
+
+  Canonical c;
+  std::vector<uint64_t> wl, fl, dl;
+  c.worker = redense(in.worker, wl, "worker");
+  c.firm = redense(in.firm, fl, "firm");
+  c.workers = wl.size();
+  c.firms = fl.size();
+  if (implicit_match) {
+    std::vector<uint64_t> keys(n);
+    for (size_t r = 0; r < n; ++r) keys[r] = uint64_t(c.worker[r]) * c.firms + c.firm[r] + 1;
+    c.deletion = redense(keys, dl, "deletion");
+  } else {
+    c.deletion = redense(in.deletion, dl, "deletion");
+  }
+  c.deletion_units = dl.size();
+  {
+    std::vector<uint32_t> cw(c.deletion_units, MISSING), cf(c.deletion_units, MISSING);
+    for (size_t r = 0; r < n; ++r) {
+      uint32_t d = c.deletion[r];
+      if (cw[d] == MISSING) {
+        cw[d] = c.worker[r];
+        cf[d] = c.firm[r];
+      } else if (cw[d] != c.worker[r] || cf[d] != c.firm[r]) {
+        fail(INVALID_IDENTIFIER, "canonicalize", "each deletion identifier must stay within one worker-firm coordinate");
+      }
+    }
+  }
+  c.topology_checksum = topology_checksum(c.worker, c.firm, c.deletion, in.frequency);
+  c.outcome = std::move(in.outcome);
+  c.frequency = std::move(in.frequency);
+  c.target = std::move(in.target);
+  c.controls = std::move(in.controls);
+  c.probe_order = std::move(in.probe_order);
+  c.physical_total = physical;
+  c.target_total = target_total;
+  return c;
+}
+
+std::vector<uint8_t> select_match_graph(const Canonical& in, GraphReceipt& rc) {
+  if (in.rows() == 0) fail(GRAPH_EMPTY, "graph", "command sample is empty");
+  std::vector<uint8_t> active(in.rows(), 1);
+  rc = GraphReceipt{};
+  rc.input_rows = in.rows();
+  rc.input_physical_mass = in.physical_total;
+
+  ComponentResult initial = largest_component(in, active);
+  rc.initial_components = initial.components;
+  rc.maximum_components = initial.components;
+  rc.initial_component_rows = initial.retained_rows;
+  intersect(active, initial.keep);
+
+  {
+    auto units = distinct_deletion_counts(in, active);
+    for (size_t r = 0; r < in.rows(); ++r)
+      if (active[r]) active[r] = units[in.worker[r]] > 1;
+  }
+  size_t movers = count_true(active);
+  rc.mover_input_rows = movers;
+  if (movers == 0) fail(GRAPH_EMPTY, "graph", "no observations remain in the mover target population");
+  ComponentResult mover = largest_component(in, active);
+  rc.maximum_components = std::max<uint64_t>(rc.maximum_components, mover.components);
+  intersect(active, mover.keep);
+
+  size_t initial_edges = active_deletion_count(in, active);
+  rc.initial_deletion_edges = initial_edges;
+  uint64_t bound = in.workers + initial_edges + 1;
+
+  for (;;) {
+    if (rc.fixed_point_iterations > bound)
+      fail(GRAPH_CERTIFICATE_FAILED, "graph", "sample fixed-point pruning exceeded its finite iteration bound");
+    ComponentResult comp = largest_component(in, active);
+    rc.maximum_components = std::max<uint64_t>(rc.maximum_components, comp.components);
+    intersect(active, comp.keep);
+    if (count_true(active) == 0) fail(GRAPH_EMPTY, "graph", "no component remains after fixed-point pruning");
+
+    auto units = distinct_deletion_counts(in, active);
+    size_t removed = 0;
+    for (size_t w = 0; w < in.workers; ++w) removed += units[w] == 1;
+    if (removed) {
+      for (size_t r = 0; r < in.rows(); ++r)
+        if (active[r] && units[in.worker[r]] == 1) active[r] = 0;
+      rc.insufficient_workers_removed += removed;
+      rc.degree_iterations++;
+      rc.fixed_point_iterations++;
+      continue;
+    }
+    auto art = worker_articulations(in, active);
+    size_t arts = count_true(art);
+    if (arts) {
+      for (size_t r = 0; r < in.rows(); ++r)
+        if (active[r] && art[in.worker[r]]) active[r] = 0;
+      rc.articulation_workers_removed += arts;
+      rc.articulation_iterations++;
+      rc.fixed_point_iterations++;
+      continue;
+    }
+    auto bridges = deletion_bridges(in, active);
+    if (bridges.empty()) break;
+    std::vector<uint8_t> is_bridge(in.deletion_units, 0);
+    for (uint32_t d : bridges) is_bridge[d] = 1;
+    size_t removed_rows = 0;
+    for (size_t r = 0; r < in.rows(); ++r)
+      if (active[r] && is_bridge[in.deletion[r]]) {
+        active[r] = 0;
+        ++removed_rows;
+      }
+    rc.bridge_units_removed += bridges.size();
+    rc.bridge_rows_removed += removed_rows;
+    rc.bridge_iterations++;
+    rc.fixed_point_iterations++;
+  }
+  if (rc.fixed_point_iterations > bound)
+    fail(GRAPH_CERTIFICATE_FAILED, "graph", "sample fixed-point pruning exceeded its finite iteration bound");
+  ComponentResult fin = largest_component(in, active);
+  rc.maximum_components = std::max<uint64_t>(rc.maximum_components, fin.components);
+  intersect(active, fin.keep);
+  if (!deletion_bridges(in, active).empty())
+    fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained deletion-unit multigraph still contains a bridge");
+  if (count_true(worker_articulations(in, active)))
+    fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained graph still contains a worker articulation");
+  {
+    auto units = distinct_deletion_counts(in, active);
+    for (uint64_t u : units)
+      if (u == 1) fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained graph still contains a one-deletion-unit worker");
+  }
+  size_t kept = count_true(active);
+  if (kept == 0) fail(GRAPH_EMPTY, "graph", "no component remains after fixed-point graph pruning");
+  rc.retained_rows = kept;
+  for (size_t r = 0; r < in.rows(); ++r)
+    if (active[r]) rc.retained_physical_mass += in.frequency[r];
+  rc.retained_deletion_edges = active_deletion_count(in, active);
+  return active;
+}
+
+std::vector<uint8_t> select_implicit_match_graph(const Canonical& in, GraphReceipt& rc) {
+  if (in.rows() == 0) fail(GRAPH_EMPTY, "graph_implicit_match", "command sample is empty");
+  std::vector<uint8_t> active(in.rows(), 1);
+  Graph g = coordinate_graph(in, active);
+  auto unsupported = [](const char* m) { fail(UNSUPPORTED_FEATURE, "graph_implicit_match", m); };
+  if (g.edges != in.deletion_units)
+    unsupported("each implicit match deletion unit must identify one distinct worker-firm coordinate");
+  ComponentResult comp = largest_component(in, active);
+  if (comp.components != 1) unsupported("the implicit-match graph shortcut requires one connected component");
+  for (size_t w = 0; w < in.workers; ++w)
+    if (g.ptr[w + 1] - g.ptr[w] <= 1)
+      unsupported("the implicit-match graph shortcut requires every worker to be a mover");
+  std::vector<uint8_t> art, br;
+  tarjan(g, &art, &br);
+  for (size_t w = 0; w < in.workers; ++w)
+    if (art[w]) unsupported("the implicit-match graph shortcut does not admit worker articulations");
+  for (uint8_t b : br)
+    if (b) unsupported("the implicit-match graph shortcut does not admit bridge deletion units");
+  rc = GraphReceipt{};
+  rc.input_rows = rc.retained_rows = in.rows();
+  rc.input_physical_mass = rc.retained_physical_mass = in.physical_total;
+  rc.initial_components = rc.maximum_components = 1;
+  rc.initial_component_rows = rc.mover_input_rows = in.rows();
+  rc.initial_deletion_edges = rc.retained_deletion_edges = g.edges;
+  return active;
+}
+
+std::vector<uint8_t> select_observation_graph(const Canonical& in, GraphReceipt& rc) {
+  if (in.rows() == 0) fail(GRAPH_EMPTY, "graph", "command sample is empty");
+  std::vector<uint8_t> active(in.rows(), 1);
+  rc = GraphReceipt{};
+  rc.input_rows = in.rows();
+  rc.input_physical_mass = in.physical_total;
+  ComponentResult initial = largest_component(in, active);
+  rc.initial_components = rc.maximum_components = initial.components;
+  rc.initial_component_rows = initial.retained_rows;
+  intersect(active, initial.keep);
+  rc.mover_input_rows = count_true(active);
+  rc.initial_deletion_edges = coordinate_graph(in, active).edges;
+  uint64_t bound = in.workers + 1;
+  for (;;) {
+    if (rc.fixed_point_iterations > bound)
+      fail(GRAPH_CERTIFICATE_FAILED, "graph", "observation-deletion pruning exceeded its finite iteration bound");
+    ComponentResult comp = largest_component(in, active);
+    rc.maximum_components = std::max<uint64_t>(rc.maximum_components, comp.components);
+    intersect(active, comp.keep);
+    if (count_true(active) == 0) fail(GRAPH_EMPTY, "graph", "no component remains after observation-deletion pruning");
+    auto physical = worker_physical_counts(in, active);
+    size_t removed = 0;
+    for (uint64_t p : physical) removed += p == 1;
+    if (removed) {
+      for (size_t r = 0; r < in.rows(); ++r)
+        if (active[r] && physical[in.worker[r]] == 1) active[r] = 0;
+      rc.insufficient_workers_removed += removed;
+      rc.degree_iterations++;
+      rc.fixed_point_iterations++;
+      continue;
+    }
+    auto art = worker_articulations(in, active);
+    size_t arts = count_true(art);
+    if (arts == 0) break;
+    for (size_t r = 0; r < in.rows(); ++r)
+      if (active[r] && art[in.worker[r]]) active[r] = 0;
+    rc.articulation_workers_removed += arts;
+    rc.articulation_iterations++;
+    rc.fixed_point_iterations++;
+  }
+  ComponentResult fin = largest_component(in, active);
+  rc.maximum_components = std::max<uint64_t>(rc.maximum_components, fin.components);
+  intersect(active, fin.keep);
+  for (uint64_t p : worker_physical_counts(in, active))
+    if (p == 1)
+      fail(GRAPH_CERTIFICATE_FAILED, "graph", "final observation-deletion graph still contains a physical-singleton worker");
+  if (count_true(worker_articulations(in, active)))
+    fail(GRAPH_CERTIFICATE_FAILED, "graph", "final observation-deletion graph still contains a worker articulation");
+  size_t kept = count_true(active);
+  if (kept == 0) fail(GRAPH_EMPTY, "graph", "no component remains after observation-deletion graph pruning");
+  rc.retained_rows = kept;
+  for (size_t r = 0; r < in.rows(); ++r)
+    if (active[r]) rc.retained_physical_mass += in.frequency[r];
+  rc.retained_deletion_edges = coordinate_graph(in, active).edges;
+  return active;
+}
+
+Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, bool implicit_match) {
+  if (active.size() != in.rows()) fail(INVALID_INPUT, "compression", "active mask has the wrong length");
+  Compressed p;
+  for (size_t r = 0; r < in.rows(); ++r)
+    if (active[r]) p.retained_rows.push_back(r);
+    else if (implicit_match)
+      fail(INTERNAL_INVARIANT_FAILED, "compression", "the certified implicit-match route must retain every row");
+  size_t R = p.retained_rows.size();
+  if (R == 0) fail(GRAPH_EMPTY, "compression", "no rows remain after graph selection");
+
+  auto redense_selected = [&](const std::vector<uint32_t>& values, size_t levels, size_t& count) {
+    std::vector<uint32_t> map(levels, MISSING);
+    if (implicit_match) {
+      for (size_t l = 0; l < levels; ++l) map[l] = uint32_t(l);
+      count = levels;
+      return map;
+    }
+    std::vector<uint8_t> present(levels, 0);
+    for (uint64_t r : p.retained_rows) present[values[r]] = 1;
+    uint32_t next = 0;
+    for (size_t l = 0; l < levels; ++l)
+      if (present[l]) map[l] = next++;
+    count = next;
+    return map;
+  };
+  size_t W, F, D;
+  auto wmap = redense_selected(in.worker, in.workers, W);
+  auto fmap = redense_selected(in.firm, in.firms, F);
+  auto dmap = redense_selected(in.deletion, in.deletion_units, D);
+  p.row_worker.resize(R);
+  p.row_firm.resize(R);
+  p.row_deletion.resize(R);
+  for (size_t i = 0; i < R; ++i) {
+    uint64_t r = p.retained_rows[i];
+    p.row_worker[i] = wmap[in.worker[r]];
+    p.row_firm[i] = fmap[in.firm[r]];
+    p.row_deletion[i] = dmap[in.deletion[r]];
+  }
+  if (F < 2) fail(GRAPH_UNIDENTIFIED, "compression", "retained graph must contain at least two firms");
+  p.workers = W;
+  p.firms = F;
+  p.deletion_units = D;
+
+  // cells: rows sorted by (worker, firm, source row)
+  std::vector<uint32_t> order(R);
+  std::iota(order.begin(), order.end(), 0u);
+  std::vector<uint64_t> key(R);
+  for (size_t i = 0; i < R; ++i) key[i] = (uint64_t(p.row_worker[i]) << 32) | p.row_firm[i];
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+  p.row_cell.assign(R, MISSING);
+  for (size_t cur = 0; cur < R;) {
+    size_t begin = cur;
+    uint64_t k = key[order[cur]];
+    while (cur < R && key[order[cur]] == k) ++cur;
+    uint32_t cell = uint32_t(p.cell_worker.size());
+    KahanSum wsum, ysum, tsum;
+    for (size_t j = begin; j < cur; ++j) {
+      uint32_t lr = order[j];
+      uint64_t src = p.retained_rows[lr];
+      double wt = double(in.frequency[src]);
+      double y = wt * in.outcome[src];
+      if (!std::isfinite(wt) || !std::isfinite(y))
+        fail(INVALID_WEIGHT, "compression", "weighted cell moment is nonfinite");
+      wsum.add(wt);
+      ysum.add(y);
+      tsum.add(in.target[src]);
+      p.row_cell[lr] = cell;
+    }
+    p.cell_worker.push_back(uint32_t(k >> 32));
+    p.cell_firm.push_back(uint32_t(k & 0xffffffffu));
+    p.cell_weight.push_back(wsum.finish());
+    p.cell_outcome_sum.push_back(ysum.finish());
+    p.cell_target_sum.push_back(tsum.finish());
+  }
+  size_t C = p.cell_worker.size();
+  p.cells = C;
+  {
+    std::vector<uint32_t> ord(C);
+    std::iota(ord.begin(), ord.end(), 0u);
+    p.worker_index = grouped_from_order(W, p.cell_worker, std::move(ord));
+    std::vector<uint32_t> ford(C);
+    std::iota(ford.begin(), ford.end(), 0u);
+    std::stable_sort(ford.begin(), ford.end(), [&](uint32_t a, uint32_t b) {
+      if (p.cell_firm[a] != p.cell_firm[b]) return p.cell_firm[a] < p.cell_firm[b];
+      if (p.cell_worker[a] != p.cell_worker[b]) return p.cell_worker[a] < p.cell_worker[b];
+      return a < b;
+    });
+    p.firm_index = grouped_from_order(F, p.cell_firm, std::move(ford));
+  }
+
+  // exact target strata (reference `exact_target_strata`, problem.rs:900-965;
+  // the certified-match variant yields the same order)
+  {
+    auto cmp = [&](uint32_t a, uint32_t b) -> int {
+      uint64_t sa = p.retained_rows[a], sb = p.retained_rows[b];
+      if (p.row_worker[a] != p.row_worker[b]) return p.row_worker[a] < p.row_worker[b] ? -1 : 1;
+      if (p.row_firm[a] != p.row_firm[b]) return p.row_firm[a] < p.row_firm[b] ? -1 : 1;
+      if (p.row_deletion[a] != p.row_deletion[b]) return p.row_deletion[a] < p.row_deletion[b] ? -1 : 1;
+      int c = total_cmp(in.outcome[sa], in.outcome[sb]);
+      if (c) return c;
+      if (in.frequency[sa] != in.frequency[sb]) return in.frequency[sa] < in.frequency[sb] ? -1 : 1;
+      c = total_cmp(in.target[sa], in.target[sb]);
+      if (c) return c;
+      for (auto& ctl : in.controls) {
+        c = total_cmp(ctl[sa], ctl[sb]);
+        if (c) return c;
+      }
+      return 0;
+    };
+    std::vector<uint32_t> tord(R);
+    std::iota(tord.begin(), tord.end(), 0u);
+    std::stable_sort(tord.begin(), tord.end(), [&](uint32_t a, uint32_t b) { return cmp(a, b) < 0; });
+    p.row_target.assign(R, MISSING);
+    uint32_t current = 0;
+    for (size_t i = 0; i < R; ++i) {
+      if (i > 0 && cmp(tord[i - 1], tord[i]) != 0) ++current;
+      p.row_target[tord[i]] = current;
+    }
+    p.exact_target_strata = size_t(current) + 1;
+    p.target_index = grouped_from_order(p.exact_target_strata, p.row_target, std::move(tord));
+  }
+  p.deletion_index = grouped_rows(D, p.row_deletion);
+
+  KahanSum tt;
+  p.outcome.resize(R);
+  p.frequency.resize(R);
+  p.target.resize(R);
+  for (size_t i = 0; i < R; ++i) {
+    uint64_t r = p.retained_rows[i];
+    p.physical_total += in.frequency[r];
+    tt.add(in.target[r]);
+    p.outcome[i] = in.outcome[r];
+    p.frequency[i] = in.frequency[r];
+    p.target[i] = in.target[r];
+  }
+  p.target_total = tt.finish();
+  if (!std::isfinite(p.target_total) || p.target_total <= 0.0)
+    fail(INVALID_TARGET_WEIGHT, "compression", "retained target mass is not positive and finite");
+  p.rows_physical = p.physical_total;
+  for (auto& ctl : in.controls) {
+    std::vector<double> col(R);
+    for (size_t i = 0; i < R; ++i) col[i] = ctl[p.retained_rows[i]];
+    p.controls.push_back(std::move(col));
+  }
+  if (!in.probe_order.empty()) {
+    p.probe_order.resize(R);
+    for (size_t i = 0; i < R; ++i) p.probe_order[i] = in.probe_order[p.retained_rows[i]];
+  }
+  p.topology_checksum = topology_checksum(p.row_worker, p.row_firm, p.row_deletion, p.frequency);
+  return p;
+}
+
+JlaPlan build_plan(const Compressed& p) {
+  size_t R = p.rows();
+  JlaPlan plan;
+  std::vector<double> per_copy(R);
+  for (size_t r = 0; r < R; ++r) {
+    if (p.frequency[r] == 0 || p.frequency[r] > MAX_EXACT_BINARY64_INTEGER)
+      fail(INVALID_WEIGHT, "jla_plan", "frequency must be an exact positive binary64 integer");
+    double v = canonical_zero(p.target[r] / double(p.frequency[r]));
+    if (!std::isfinite(v) || v < 0.0)
+      fail(INVALID_TARGET_WEIGHT, "jla_plan", "per-copy target mass is invalid at zero-based row " + std::to_string(r));
+    per_copy[r] = v;
+  }
+  bool has_order = !p.probe_order.empty();
+  // semantic key (reference `compare_semantic_rows`, jla.rs:523-540)
+  auto sem = [&](uint32_t a, uint32_t b) -> int {
+    if (p.row_worker[a] != p.row_worker[b]) return p.row_worker[a] < p.row_worker[b] ? -1 : 1;
+    if (p.row_firm[a] != p.row_firm[b]) return p.row_firm[a] < p.row_firm[b] ? -1 : 1;
+    if (p.row_deletion[a] != p.row_deletion[b]) return p.row_deletion[a] < p.row_deletion[b] ? -1 : 1;
+    int c = ordered_f64(per_copy[a], per_copy[b]);
+    if (c) return c;
+    c = ordered_f64(p.outcome[a], p.outcome[b]);
+    if (c) return c;
+    if (has_order) return ordered_f64(p.probe_order[a], p.probe_order[b]);
+    return 0;
+  };
+  std::vector<uint32_t> order(R);
+  std::iota(order.begin(), order.end(), 0u);
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    int c = sem(a, b);
+    return c ? c < 0 : a < b;
+  });
+  plan.row_rank.assign(R, 0);
+  uint64_t current = 0;
+  for (size_t i = 0; i < R; ++i) {
+    if (i == 0 || sem(order[i - 1], order[i]) != 0) ++current;
+    plan.row_rank[order[i]] = current;
+  }
+
+  // deletion units (reference `deletion_plan`, jla.rs:574-649)
+  size_t G = p.deletion_index.ptr.size() - 1;
+  plan.del_cell.resize(G);
+  plan.del_count.resize(G);
+  plan.del_rank.resize(G);
+  plan.del_outcome_sum.resize(G);
+  plan.del_target_mass.resize(G);
+  for (size_t g = 0; g < G; ++g) {
+    uint64_t b = p.deletion_index.ptr[g], e = p.deletion_index.ptr[g + 1];
+    if (b == e) fail(INTERNAL_INVARIANT_FAILED, "jla_plan", "deletion unit has no retained row");
+    uint64_t phys = 0, minrank = ~uint64_t(0);
+    uint32_t cell = MISSING;
+    StableSum y, t;
+    for (uint64_t i = b; i < e; ++i) {
+      uint32_t r = p.deletion_index.items[i];
+      phys += p.frequency[r];
+      if (cell == MISSING) cell = p.row_cell[r];
+      else if (cell != p.row_cell[r])
+        fail(INVALID_IDENTIFIER, "jla_plan", "one deletion unit crosses coefficient cells");
+      y.add(double(p.frequency[r]) * p.outcome[r]);
+      t.add(p.target[r]);
+      minrank = std::min(minrank, plan.row_rank[r]);
+    }
+    plan.del_cell[g] = cell;
+    plan.del_count[g] = phys;
+    plan.del_outcome_sum[g] = y.finish();
+    plan.del_target_mass[g] = t.finish();
+    plan.del_rank[g] = minrank;
+  }
+  {
+    std::vector<uint64_t> s = plan.del_rank;
+    std::sort(s.begin(), s.end());
+    if (std::adjacent_find(s.begin(), s.end()) != s.end())
+      fail(INTERNAL_INVARIANT_FAILED, "jla_plan", "deletion-unit semantic ranks are not unique");
+  }
+
+  // target strata (reference `target_plan`, jla.rs:651-790)
+  std::vector<uint32_t> tord(R);
+  std::iota(tord.begin(), tord.end(), 0u);
+  std::sort(tord.begin(), tord.end(), [&](uint32_t a, uint32_t b) {
+    if (p.row_cell[a] != p.row_cell[b]) return p.row_cell[a] < p.row_cell[b];
+    int c = ordered_f64(per_copy[a], per_copy[b]);
+    if (c) return c < 0;
+    if (plan.row_rank[a] != plan.row_rank[b]) return plan.row_rank[a] < plan.row_rank[b];
+    return a < b;
+  });
+  for (size_t cur = 0; cur < R;) {
+    size_t begin = cur;
+    uint32_t cell = p.row_cell[tord[cur]];
+    double pc = canonical_zero(per_copy[tord[cur]]);
+    uint64_t bits;
+    std::memcpy(&bits, &pc, 8);
+    ++cur;
+    while (cur < R) {
+      double v = canonical_zero(per_copy[tord[cur]]);
+      uint64_t vb;
+      std::memcpy(&vb, &v, 8);
+      if (p.row_cell[tord[cur]] != cell || vb != bits) break;
+      ++cur;
+    }
+    uint64_t phys = 0, minrank = ~uint64_t(0);
+    StableSum t;
+    for (size_t j = begin; j < cur; ++j) {
+      uint32_t r = tord[j];
+      phys += p.frequency[r];
+      t.add(p.target[r]);
+      minrank = std::min(minrank, plan.row_rank[r]);
+    }
+    plan.tgt_cell.push_back(cell);
+    plan.tgt_per_copy.push_back(pc);
+    plan.tgt_count.push_back(phys);
+    plan.tgt_mass.push_back(t.finish());
+    plan.tgt_rank.push_back(minrank);
+  }
+  {
+    std::vector<uint64_t> s = plan.tgt_rank;
+    std::sort(s.begin(), s.end());
+    if (std::adjacent_find(s.begin(), s.end()) != s.end())
+      fail(INTERNAL_INVARIANT_FAILED, "jla_plan", "target semantic plan is incomplete or noncanonical");
+  }
+  return plan;
+}
+
+}  // namespace fevcb

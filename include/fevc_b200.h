@@ -1,0 +1,513 @@
+/* fevc-b200: B200-native leave-out leverage engine, C ABI.
+ *
+ * The library exports the plugin entry points of fevc's Rust backend for the
+ * JLA solve path with the same names, struct layouts and status codes, so a
+ * caller written against rust/stata_backend/include/vckss_rust.h (the Stata C
+ * shim rust/stata_backend/cshim/stata_entry.c, or a C harness) links or
+ * dlopens this library unchanged.  Each declaration cites the reference
+ * function it replaces (paths inside the reference project).
+ *
+ * Lifecycle: prepare (host ingest, graph pruning, compression, semantic plan)
+ * -> optional centering -> solve (device) -> result / receipts -> release.
+ * One generation is active at a time; the caller owns all memory; every output
+ * is capacity-checked.  Status codes: 0 OK, 1 USER_BREAK, 10 ABI_MISMATCH,
+ * 11 UNSUPPORTED_FEATURE, 20..23 invalid input, 30..32 graph, 40/41 resources,
+ * 60..64 solver, 70..79 estimator, 80..82 context, 90 invariant, 99 panic
+ * (reference rust/crates/vckss-core/src/error.rs:8-48).
+ *
+ * Entry points prefixed fevcb_ are B200 extensions with no reference
+ * counterpart (device selection, stream binding, timings, raw device atoms).
+ */
+#ifndef FEVC_B200_H
+#define FEVC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VCKSS_RUST_ABI_VERSION_V1 1u
+#define VCKSS_DELETION_MATCH 1u
+#define VCKSS_DELETION_OBSERVATION 2u
+#define VCKSS_RNG_COUNTER_V1 1u
+#define VCKSS_ROUTE_AUTO 0u
+#define VCKSS_ROUTE_EXACT 1u
+#define VCKSS_ROUTE_DIAGONAL_PCG 2u
+#define VCKSS_ROUTE_CMG_PCG 3u
+#define VCKSS_ALGORITHM_AUTO 0u
+#define VCKSS_ALGORITHM_EXACT 1u
+#define VCKSS_ALGORITHM_JLA 2u
+#define VCKSS_NUISANCE_JOINT 1u
+#define VCKSS_NUISANCE_FIXED_OFFSET 2u
+#define VCKSS_INTERRUPT_CONTINUE 0
+#define VCKSS_INTERRUPT_USER_BREAK 1
+
+typedef int32_t (*VckssInterruptPollV1)(void *context);
+
+/* ---- preparation requests (reference vckss_rust.h:261-290) ---- */
+typedef struct VckssEnginePrepareRequestV1 {
+  uint32_t abi_version;
+  uint32_t struct_size;
+  uint64_t rows;
+  uint32_t cleanup_abandoned;
+  uint32_t reserved;
+} VckssEnginePrepareRequestV1;
+
+typedef struct VckssEnginePrepareRequestV2 {
+  uint32_t abi_version;
+  uint32_t struct_size;
+  uint64_t rows;
+  uint32_t cleanup_abandoned;
+  uint32_t reserved;
+  uint64_t memory_limit_bytes;
+  uint64_t caller_copy_bytes;
+} VckssEnginePrepareRequestV2;
+
+typedef struct VckssEnginePrepareRequestV3 {
+  VckssEnginePrepareRequestV2 v2;
+  uint32_t deletion_mode;
+  uint32_t controls_count;
+  uint64_t reserved_2;
+} VckssEnginePrepareRequestV3;
+
+typedef struct VckssEnginePrepareRequestV4 {
+  VckssEnginePrepareRequestV3 v3;
+  uint32_t implicit_match;
+  uint32_t reserved_3;
+} VckssEnginePrepareRequestV4;
+
+typedef struct VckssEnginePrepareRequestInterruptV1 {
+  VckssEnginePrepareRequestV2 options;
+  VckssInterruptPollV1 interrupt_poll;
+  void *interrupt_context;
+  uint32_t checkpoint_interval;
+  uint32_t reserved;
+} VckssEnginePrepareRequestInterruptV1;
+
+typedef struct VckssEnginePrepareRequestInterruptV2 {
+  VckssEnginePrepareRequestV3 options;
+  VckssInterruptPollV1 interrupt_poll;
+  void *interrupt_context;
+  uint32_t checkpoint_interval;
+  uint32_t reserved;
+} VckssEnginePrepareRequestInterruptV2;
+
+typedef struct VckssEnginePrepareRequestInterruptV3 {
+  VckssEnginePrepareRequestV4 options;
+  VckssInterruptPollV1 interrupt_poll;
+  void *interrupt_context;
+  uint32_t checkpoint_interval;
+  uint32_t reserved;
+} VckssEnginePrepareRequestInterruptV3;
+
+/* ---- caller columns, binary64 (reference vckss_rust.h:343-367) ---- */
+typedef struct VckssEngineColumnsV1 {
+  uint32_t struct_size;
+  uint32_t reserved;
+  uint64_t rows;
+  const double *worker;
+  const double *firm;
+  const double *deletion;
+  const double *outcome;
+  const double *frequency;
+  const double *target_weight;
+} VckssEngineColumnsV1;
+
+typedef struct VckssEngineColumnsV2 {
+  VckssEngineColumnsV1 v1;
+  const double *const *controls;
+  uint32_t controls_count;
+  uint32_t reserved_2;
+} VckssEngineColumnsV2;
+
+typedef struct VckssEngineColumnsV3 {
+  VckssEngineColumnsV2 v2;
+  const double *probe_order;
+  uint32_t probeorder_supplied;
+  uint32_t reserved_3;
+} VckssEngineColumnsV3;
+
+/* ---- solve requests (reference vckss_rust.h:501-571) ---- */
+typedef struct VckssEngineSolveRequestV1 {
+  uint32_t abi_version;
+  uint32_t struct_size;
+  uint64_t seed;
+  uint32_t probes;
+  uint32_t leverage_batch_width;
+  uint32_t target_batch_width;
+  uint32_t deletion_mode;
+  uint32_t rng_contract;
+  uint32_t solver_route;
+  uint32_t allow_automatic_cmg_setup_fallback;
+  uint64_t exact_dimension_limit;
+  uint64_t cmg_minimum_dimension;
+  double pcg_tolerance;
+  uint32_t maximum_iterations;
+  uint32_t residual_replacement_interval;
+  double rank_tolerance;
+  double block_tolerance;
+  uint64_t cmg_terminal_vertices;
+  uint64_t cmg_dense_vertex_cap;
+  uint64_t cmg_maximum_levels;
+  uint64_t cmg_aggregate_cap;
+  double cmg_minimum_reduction;
+  double cmg_jacobi_weight;
+  uint32_t cmg_pre_sweeps;
+  uint32_t cmg_post_sweeps;
+  double cmg_maximum_edge_complexity;
+  double cmg_maximum_vertex_complexity;
+  uint64_t cmg_memory_limit_bytes;
+} VckssEngineSolveRequestV1;
+
+typedef struct VckssEngineSolveRequestV2 {
+  VckssEngineSolveRequestV1 v1;
+  uint32_t algorithm;
+  uint32_t nuisance_mode;
+  uint64_t exact_estimator_limit;
+  uint64_t blocksize_limit;
+} VckssEngineSolveRequestV2;
+
+typedef struct VckssEngineSolveRequestV3 {
+  VckssEngineSolveRequestV2 v2;
+  uint32_t engine;
+  uint32_t batch_mode;
+  uint32_t stayers_mode;
+  uint32_t target_weight_mode;
+  uint32_t deletion_unit_source;
+  uint32_t probeorder_supplied;
+  uint32_t wallseconds_supplied;
+  uint32_t capability_schema;
+  uint32_t capability_profile;
+  uint32_t frequency_use;
+  uint64_t physical_limit;
+  uint64_t request_signature;
+  uint64_t reserved_3;
+} VckssEngineSolveRequestV3;
+
+typedef struct VckssEngineSolveRequestV4 {
+  VckssEngineSolveRequestV3 v3;
+  uint32_t leverage_batch_mode;
+  uint32_t target_batch_mode;
+  double wallseconds;
+  uint64_t reserved_4;
+} VckssEngineSolveRequestV4;
+
+typedef struct VckssEngineSolveRequestV5 {
+  VckssEngineSolveRequestV4 v4;
+  uint32_t threads;
+  uint32_t tolerance_supplied;
+  uint32_t full_cmg_v2;
+  uint32_t reserved_5;
+} VckssEngineSolveRequestV5;
+
+typedef struct VckssEngineSolveRequestInterruptV1 {
+  VckssEngineSolveRequestV1 options;
+  VckssInterruptPollV1 interrupt_poll;
+  void *interrupt_context;
+  uint32_t checkpoint_interval;
+  uint32_t reserved;
+} VckssEngineSolveRequestInterruptV1;
+
+typedef struct VckssEngineSolveRequestInterruptV5 {
+  VckssEngineSolveRequestV5 options;
+  VckssInterruptPollV1 interrupt_poll;
+  void *interrupt_context;
+  uint32_t checkpoint_interval;
+  uint32_t reserved;
+} VckssEngineSolveRequestInterruptV5;
+
+/* ---- results and receipts (reference vckss_rust.h:711-768, 1037-1052, 1611-1634) ---- */
+typedef struct VckssComponentVectorV1 {
+  double worker;
+  double firm;
+  double covariance;
+  double total;
+} VckssComponentVectorV1;
+
+typedef struct VckssEngineResultV1 {
+  uint32_t struct_size;
+  uint32_t reserved;
+  uint64_t generation;
+  VckssComponentVectorV1 plugin;
+  VckssComponentVectorV1 correction;
+  VckssComponentVectorV1 corrected;
+  VckssComponentVectorV1 numerical_mcse;
+} VckssEngineResultV1;
+
+typedef struct VckssEnginePreparationReceiptV1 {
+  uint32_t struct_size;
+  uint32_t reserved;
+  uint64_t generation;
+  uint64_t input_rows;
+  uint64_t retained_rows;
+  uint64_t workers;
+  uint64_t firms;
+  uint64_t cells;
+  uint64_t deletion_units;
+  uint64_t target_strata;
+} VckssEnginePreparationReceiptV1;
+
+typedef struct VckssEnginePreparationReceiptV2 {
+  uint32_t struct_size;
+  uint32_t reserved;
+  uint64_t generation;
+  uint64_t input_rows;
+  uint64_t retained_rows;
+  uint64_t workers;
+  uint64_t firms;
+  uint64_t cells;
+  uint64_t deletion_units;
+  uint64_t target_strata;
+  uint64_t memory_limit_bytes;
+  uint64_t caller_copy_bytes;
+  uint64_t preparation_peak_forecast_bytes;
+  uint64_t prepared_resident_bytes;
+  uint64_t graph_input_rows;
+  uint64_t graph_retained_rows;
+  uint64_t graph_input_physical_mass;
+  uint64_t graph_retained_physical_mass;
+  uint64_t graph_initial_components;
+  uint64_t graph_maximum_components;
+  uint64_t graph_initial_component_rows;
+  uint64_t graph_mover_input_rows;
+  uint64_t graph_initial_deletion_edges;
+  uint64_t graph_retained_deletion_edges;
+  uint64_t graph_insufficient_workers_removed;
+  uint64_t graph_articulation_workers_removed;
+  uint64_t graph_bridge_units_removed;
+  uint64_t graph_bridge_rows_removed;
+  uint64_t graph_degree_iterations;
+  uint64_t graph_articulation_iterations;
+  uint64_t graph_bridge_iterations;
+  uint64_t graph_fixed_point_iterations;
+} VckssEnginePreparationReceiptV2;
+
+typedef struct VckssEnginePreparationReceiptV3 {
+  VckssEnginePreparationReceiptV2 v2;
+  double target_weight_sum;
+} VckssEnginePreparationReceiptV3;
+
+typedef struct VckssEnginePreparationReceiptV4 {
+  VckssEnginePreparationReceiptV3 v3;
+  uint32_t controls_count;
+  uint32_t deletion_mode;
+} VckssEnginePreparationReceiptV4;
+
+typedef struct VckssEngineRhsReceiptV1 {
+  uint32_t phase;
+  uint32_t side;
+  int64_t probe;
+  uint32_t route;
+  uint32_t iterations;
+  uint32_t zero_rhs;
+  uint32_t reserved;
+  double reduced_residual;
+  double complete_residual;
+} VckssEngineRhsReceiptV1;
+
+typedef struct VckssEngineRhsReceiptV2 {
+  VckssEngineRhsReceiptV1 v1;
+  uint32_t status;
+  uint32_t residual_replacements;
+  uint64_t operator_applications;
+  uint64_t preconditioner_applications;
+  double full_residual_tolerance;
+  uint32_t residual_space;
+  uint32_t reserved_2;
+  uint64_t solver_dimension;
+} VckssEngineRhsReceiptV2;
+
+typedef struct VckssEngineSnapshotV1 {
+  uint32_t struct_size;
+  uint32_t state;
+  uint64_t generation;
+  uint64_t last_released_generation;
+} VckssEngineSnapshotV1;
+
+typedef struct VckssBackendCapabilitiesV1 {
+  uint32_t struct_size;
+  uint32_t abi_version;
+  uint64_t core_ready_flags;
+  uint64_t support_flags;
+  uint32_t deterministic_parallelism;
+  uint32_t reserved;
+} VckssBackendCapabilitiesV1;
+
+/* ---- library identity (reference ffi_engine.rs / vckss_rust.h:1642-1650) ---- */
+uint32_t vckss_rust_abi_version(void);
+const char *vckss_rust_backend_version(void);
+const char *vckss_rust_capabilities_json(void);
+const char *vckss_rust_last_error(void);
+int32_t vckss_rust_selftest(void);
+int32_t vckss_rust_backend_capabilities_v1(VckssBackendCapabilitiesV1 *output, uint32_t output_capacity_bytes);
+
+/* ---- defaults (reference ffi_engine.rs:1094-1276, 2723-2800) ---- */
+int32_t vckss_rust_engine_default_solve_request_v1(VckssEngineSolveRequestV1 *output, uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_default_solve_request_v2(VckssEngineSolveRequestV2 *output, uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_default_solve_request_v3(VckssEngineSolveRequestV3 *output, uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_default_solve_request_v4(VckssEngineSolveRequestV4 *output, uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_default_solve_request_v5(VckssEngineSolveRequestV5 *output, uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_default_solve_request_interrupt_v1(VckssEngineSolveRequestInterruptV1 *output,
+                                                             uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_default_solve_request_interrupt_v5(VckssEngineSolveRequestInterruptV5 *output,
+                                                             uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_default_prepare_request_v3(VckssEnginePrepareRequestV3 *output, uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_default_prepare_request_interrupt_v1(VckssEnginePrepareRequestInterruptV1 *output,
+                                                               uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_default_prepare_request_interrupt_v2(VckssEnginePrepareRequestInterruptV2 *output,
+                                                               uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_default_prepare_request_interrupt_v3(VckssEnginePrepareRequestInterruptV3 *output,
+                                                               uint32_t output_capacity_bytes);
+
+/* ---- preparation (reference ffi_engine.rs:3270-3316 prepare_v1; 3318-3470 V2/V3; V4 implicit match) ---- */
+int32_t vckss_rust_engine_prepare_v1(const VckssEnginePrepareRequestV1 *request, const VckssEngineColumnsV1 *columns,
+                                     uint64_t *output_handle, uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_prepare_v2(const VckssEnginePrepareRequestV2 *request, const VckssEngineColumnsV1 *columns,
+                                     uint64_t *output_handle, uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_prepare_v3(const VckssEnginePrepareRequestV3 *request, const VckssEngineColumnsV2 *columns,
+                                     uint64_t *output_handle, uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_prepare_interrupt_v1(const VckssEnginePrepareRequestInterruptV1 *request,
+                                               const VckssEngineColumnsV1 *columns, uint64_t *output_handle,
+                                               uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_prepare_interrupt_v2(const VckssEnginePrepareRequestInterruptV2 *request,
+                                               const VckssEngineColumnsV2 *columns, uint64_t *output_handle,
+                                               uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_prepare_interrupt_v4(const VckssEnginePrepareRequestInterruptV3 *request,
+                                               const VckssEngineColumnsV3 *columns, uint64_t *output_handle,
+                                               uint32_t output_capacity_bytes);
+
+/* centering mode 0 None, 1 Mean (2 Corrected is refused) (reference ffi_engine.rs:2446-2467) */
+int32_t vckss_rust_engine_centering_v1(uint64_t generation, uint32_t mode);
+
+/* ---- solve (reference ffi_engine.rs:4474-4500 V1, 4629-4690 V5; body 5892-6000) ---- */
+int32_t vckss_rust_engine_solve_v1(uint64_t generation, const VckssEngineSolveRequestV1 *request);
+int32_t vckss_rust_engine_solve_interrupt_v1(uint64_t generation, const VckssEngineSolveRequestInterruptV1 *request);
+int32_t vckss_rust_engine_solve_v5(uint64_t generation, const VckssEngineSolveRequestV5 *request);
+int32_t vckss_rust_engine_solve_interrupt_v5(uint64_t generation, const VckssEngineSolveRequestInterruptV5 *request);
+
+/* ---- results and receipts (reference ffi_engine.rs:5992-6040 result_v1; 4370-4470 receipts, retained mask) ---- */
+int32_t vckss_rust_engine_result_v1(uint64_t generation, VckssEngineResultV1 *output, uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_preparation_receipt_v1(uint64_t generation, VckssEnginePreparationReceiptV1 *output,
+                                                 uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_preparation_receipt_v2(uint64_t generation, VckssEnginePreparationReceiptV2 *output,
+                                                 uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_preparation_receipt_v3(uint64_t generation, VckssEnginePreparationReceiptV3 *output,
+                                                 uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_preparation_receipt_v4(uint64_t generation, VckssEnginePreparationReceiptV4 *output,
+                                                 uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_retained_mask_v1(uint64_t generation, uint8_t *output, uint64_t output_capacity_bytes);
+int32_t vckss_rust_engine_rhs_receipts_v1(uint64_t generation, VckssEngineRhsReceiptV1 *output,
+                                          uint64_t output_capacity_rows);
+int32_t vckss_rust_engine_rhs_receipts_v2(uint64_t generation, VckssEngineRhsReceiptV2 *output,
+                                          uint64_t output_capacity_rows);
+
+/* ---- cleanup (reference ffi_engine.rs:7146-7200, 2470) ---- */
+int32_t vckss_rust_engine_release_v1(uint64_t generation);
+int32_t vckss_rust_engine_clear_abandoned_v1(void);
+int32_t vckss_rust_engine_snapshot_v1(VckssEngineSnapshotV1 *output, uint32_t output_capacity_bytes);
+const char *vckss_rust_engine_last_error(void);
+
+/* ================= B200 extensions (no reference counterpart) ================= */
+
+/* Device options applied to the next solve of a generation. */
+typedef struct FevcbSolveOptionsV1 {
+  uint32_t struct_size;
+  uint32_t block_columns;   /* right-hand sides per blocked PCG: 0 auto, 8, 16, 32, 64 */
+  uint32_t preconditioner;  /* 0 auto, 1 Jacobi, 2 aggregation multigrid */
+  uint32_t keep_unit_detail;/* 1: keep per-unit leverage arrays for fevcb_engine_unit_detail_v1 */
+} FevcbSolveOptionsV1;
+
+/* Wall and device timings of the last solve. */
+typedef struct FevcbSolveTimingsV1 {
+  uint32_t struct_size;
+  uint32_t reserved;
+  double total_ms;
+  double fit_ms;
+  double leverage_ms;
+  double target_ms;
+  double setup_ms;
+  uint64_t block_iterations;
+  uint64_t column_iterations;
+  uint64_t rhs_columns;
+  uint64_t kernel_launches;
+  uint64_t h2d_bytes;
+  uint64_t vertices;
+  uint64_t edges;
+  uint64_t kept_workers;
+  uint64_t levels;
+} FevcbSolveTimingsV1;
+
+int32_t fevcb_device_count(void);
+/* Bind the CUDA stream (a cudaStream_t) used by generations prepared afterwards; NULL = library-owned stream. */
+int32_t fevcb_set_stream(void *stream);
+int32_t fevcb_engine_solve_options_v1(uint64_t generation, const FevcbSolveOptionsV1 *options);
+int32_t fevcb_engine_timings_v1(uint64_t generation, FevcbSolveTimingsV1 *output, uint32_t output_capacity_bytes);
+/* Re-run the solve of a solved generation with the same request (device-resident inputs). */
+int32_t fevcb_engine_resolve_v1(uint64_t generation);
+/* Per-unit and per-probe detail of the last solve (units in plan order). Arrays may be NULL. */
+int32_t fevcb_engine_unit_detail_v1(uint64_t generation, uint64_t units, double *projection_share,
+                                    double *residual_share, double *finite_bias, double *finite_variance,
+                                    double *residual_mass, double *deleted_mass, uint64_t cells, double *fitted_cell,
+                                    double *cell_correction_weight, uint64_t probes, double *target_draws4);
+/* Read-only view of a prepared generation's compressed problem and semantic
+ * plan (host arrays owned by the library, valid until release). */
+typedef struct FevcbProblemViewV1 {
+  uint32_t struct_size;
+  uint32_t reserved;
+  uint64_t rows, workers, firms, cells, units, strata;
+  uint64_t physical_total;
+  double target_total;
+  const uint32_t *row_worker, *row_firm, *row_cell;
+  const double *row_outcome, *row_target;
+  const uint64_t *row_frequency;
+  const uint32_t *cell_worker, *cell_firm;
+  const double *cell_weight, *cell_outcome_sum, *cell_target_sum;
+  const uint32_t *unit_cell;
+  const uint64_t *unit_count, *unit_rank;
+  const double *unit_outcome_sum;
+  const uint32_t *stratum_cell;
+  const double *stratum_per_copy;
+  const uint64_t *stratum_count, *stratum_rank;
+} FevcbProblemViewV1;
+int32_t fevcb_engine_problem_view_v1(uint64_t generation, FevcbProblemViewV1 *output, uint32_t output_capacity_bytes);
+
+/* Counter-V1 atoms computed on the device: out[e*columns + j] for probe first_probe + j. */
+int32_t fevcb_counter_atoms_v1(uint64_t seed, uint64_t domain_tag, uint64_t first_probe, uint32_t columns,
+                               const uint64_t *entity, const uint64_t *trials, uint64_t count, int64_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__cplusplus)
+static_assert(sizeof(VckssEnginePrepareRequestV1) == 24, "prepare request V1 layout");
+static_assert(sizeof(VckssEnginePrepareRequestV2) == 40, "prepare request V2 layout");
+static_assert(sizeof(VckssEnginePrepareRequestV3) == 56, "prepare request V3 layout");
+static_assert(sizeof(VckssEnginePrepareRequestV4) == 64, "prepare request V4 layout");
+static_assert(sizeof(VckssEnginePrepareRequestInterruptV1) == 64, "interrupt prepare V1 layout");
+static_assert(sizeof(VckssEnginePrepareRequestInterruptV2) == 80, "interrupt prepare V2 layout");
+static_assert(sizeof(VckssEnginePrepareRequestInterruptV3) == 88, "interrupt prepare V3 layout");
+static_assert(sizeof(VckssEngineColumnsV1) == 64, "columns V1 layout");
+static_assert(sizeof(VckssEngineColumnsV2) == 80, "columns V2 layout");
+static_assert(sizeof(VckssEngineColumnsV3) == 96, "columns V3 layout");
+static_assert(sizeof(VckssEngineSolveRequestV1) == 176, "solve request V1 layout");
+static_assert(sizeof(VckssEngineSolveRequestV2) == 200, "solve request V2 layout");
+static_assert(sizeof(VckssEngineSolveRequestV3) == 264, "solve request V3 layout");
+static_assert(sizeof(VckssEngineSolveRequestV4) == 288, "solve request V4 layout");
+static_assert(sizeof(VckssEngineSolveRequestV5) == 304, "solve request V5 layout");
+static_assert(sizeof(VckssEngineSolveRequestInterruptV1) == 200, "interrupt solve V1 layout");
+static_assert(sizeof(VckssEngineSolveRequestInterruptV5) == 328, "interrupt solve V5 layout");
+static_assert(sizeof(VckssEngineResultV1) == 144, "result layout");
+static_assert(sizeof(VckssEnginePreparationReceiptV1) == 72, "preparation receipt V1 layout");
+static_assert(sizeof(VckssEnginePreparationReceiptV2) == 248, "preparation receipt V2 layout");
+static_assert(sizeof(VckssEnginePreparationReceiptV3) == 256, "preparation receipt V3 layout");
+static_assert(sizeof(VckssEnginePreparationReceiptV4) == 264, "preparation receipt V4 layout");
+static_assert(sizeof(VckssEngineRhsReceiptV1) == 48, "RHS receipt V1 layout");
+static_assert(sizeof(VckssEngineRhsReceiptV2) == 96, "RHS receipt V2 layout");
+static_assert(sizeof(VckssEngineSnapshotV1) == 24, "snapshot layout");
+static_assert(sizeof(VckssBackendCapabilitiesV1) == 32, "capabilities layout");
+#endif
+
+#endif /* FEVC_B200_H */

@@ -1,0 +1,491 @@
+/* ORACLE - test infrastructure only.
+ *
+ * Plain-C CPU restatement of the reference's Counter-V1 RNG and its
+ * compressed, no-control, match-deletion JLA estimator.  It is the checker for
+ * the device engine: only the tests, the smoke check and the CPU-baseline leg
+ * of the benchmark load it.  The product never links or calls it.
+ *
+ * Restated reference functions (paths inside the reference project):
+ *   rng            rust/crates/vckss-core/src/rng.rs:73-93, 130-305, 308-335
+ *   full fit       rust/crates/vckss-core/src/operator.rs:269-343 (Schur RHS,
+ *                  worker reconstruction), engine.rs:1107-1134
+ *   plug-in        rust/crates/vckss-core/src/jla.rs:286-364
+ *   leverage       rust/crates/vckss-core/src/engine.rs:1150-1228, 2562-2619
+ *   adjustment     rust/crates/vckss-core/src/engine.rs:2269-2410
+ *   target         rust/crates/vckss-core/src/engine.rs:2621-2879 (directions,
+ *                  transpose, balance repair), 3003-3101 (contraction)
+ *   mean / MCSE    rust/crates/vckss-core/src/engine.rs:3108-3200
+ *   centering mean rust/crates/vckss-core/src/centering.rs:6-27
+ * Linear solves use the firm Schur complement on the zero-sum quotient: a
+ * dense grounded Cholesky factor when the firm count is small, otherwise
+ * Jacobi-preconditioned CG to a tight tolerance.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------ RNG */
+
+static uint64_t splitmix64(uint64_t x) {
+  x += 0x9e3779b97f4a7c15ull;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+  return x ^ (x >> 31);
+}
+
+void oracle_philox_block(uint64_t seed, uint64_t tag, uint64_t probe_block, uint64_t entity, uint64_t word,
+                         uint64_t out[4]) {
+  uint64_t c[4] = {entity, probe_block, word, tag};
+  uint64_t k0 = splitmix64(seed), k1 = splitmix64(seed ^ 0xd1b54a32d192ed03ull);
+  for (int round = 0; round < 10; ++round) {
+    unsigned __int128 p0 = (unsigned __int128)0xd2b74407b1ce6e93ull * c[0];
+    unsigned __int128 p1 = (unsigned __int128)0xca5a826395121157ull * c[2];
+    uint64_t h0 = (uint64_t)(p0 >> 64), l0 = (uint64_t)p0, h1 = (uint64_t)(p1 >> 64), l1 = (uint64_t)p1;
+    uint64_t n[4] = {h1 ^ c[1] ^ k0, l1, h0 ^ c[3] ^ k1, l0};
+    memcpy(c, n, sizeof(c));
+    if (round != 9) {
+      k0 += 0x9e3779b97f4a7c15ull;
+      k1 += 0xbb67ae8584caa73bull;
+    }
+  }
+  memcpy(out, c, sizeof(c));
+}
+
+/* 2 * popcount(selected bits) - trials; returns 0 and sets *ok = 0 on a bad trial count */
+int64_t oracle_rademacher_sum(uint64_t seed, uint64_t tag, uint64_t probe, uint64_t entity, uint64_t trials, int* ok) {
+  if (trials == 0 || trials > (1ull << 53)) {
+    if (ok) *ok = 0;
+    return 0;
+  }
+  if (ok) *ok = 1;
+  uint64_t full = trials / 64, rem = trials % 64, pos = 0, b[4];
+  int lane = (int)(probe % 4);
+  for (uint64_t w = 0; w < full; ++w) {
+    oracle_philox_block(seed, tag, probe / 4, entity, w, b);
+    pos += (uint64_t)__builtin_popcountll(b[lane]);
+  }
+  if (rem) {
+    oracle_philox_block(seed, tag, probe / 4, entity, full, b);
+    pos += (uint64_t)__builtin_popcountll(b[lane] & ((1ull << rem) - 1));
+  }
+  return 2 * (int64_t)pos - (int64_t)trials;
+}
+
+/* -------------------------------------------------------- compensated sums */
+
+typedef struct {
+  double sum, corr;
+} Stable;
+
+static void st_add(Stable* s, double v) {
+  double t = s->sum + v;
+  s->corr += (fabs(s->sum) >= fabs(v)) ? (s->sum - t) + v : (v - t) + s->sum;
+  s->sum = t;
+}
+static double st_fin(const Stable* s) { return s->sum + s->corr; }
+
+/* ---------------------------------------------------------------- problem */
+
+typedef struct {
+  uint64_t rows, workers, firms, cells, units, strata, physical_total;
+  double target_total;
+  const uint32_t *row_worker, *row_firm, *row_cell;
+  const double *row_outcome, *row_target;
+  const uint64_t* row_frequency;
+  const uint32_t *cell_worker, *cell_firm;
+  const double *cell_weight, *cell_outcome_sum, *cell_target_sum;
+  const uint32_t* unit_cell;
+  const uint64_t *unit_count, *unit_rank;
+  const double* unit_outcome_sum;
+  const uint32_t* stratum_cell;
+  const double* stratum_per_copy;
+  const uint64_t *stratum_count, *stratum_rank;
+} OracleProblem;
+
+typedef struct {
+  uint64_t seed;
+  uint32_t probes;
+  uint32_t centering; /* 0 none, 1 mean */
+  double tolerance;   /* CG tolerance when the dense factor is not used */
+  double rank_tolerance, block_tolerance;
+  uint32_t dense_limit; /* use the dense factor when firms <= dense_limit */
+} OracleOptions;
+
+typedef struct {
+  double plugin[4], correction[4], corrected[4], mcse[4];
+  double* fitted_cell;          /* cells */
+  double* projection_share;     /* units */
+  double* residual_share;       /* units */
+  double* finite_bias;          /* units */
+  double* finite_variance;      /* units */
+  double* residual_mass;        /* units */
+  double* deleted_mass;         /* units */
+  double* cell_correction_weight; /* cells */
+  double* target_draws;         /* probes x 4 */
+  uint64_t solves, cg_iterations;
+  int error_code;
+  char error[256];
+} OracleResult;
+
+typedef struct {
+  const OracleProblem* p;
+  double *wdiag, *fdiag;
+  int dense;
+  double* chol; /* (F-1)^2 lower factor of the grounded Schur complement */
+  double tol;
+  uint64_t iterations;
+  double *t_sum, *t_r, *t_z, *t_p, *t_q;
+} Solver;
+
+static void schur_apply(const Solver* s, const double* x, double* y, double* wsum) {
+  const OracleProblem* p = s->p;
+  memset(wsum, 0, p->workers * sizeof(double));
+  for (uint64_t c = 0; c < p->cells; ++c) wsum[p->cell_worker[c]] += p->cell_weight[c] * x[p->cell_firm[c]];
+  for (uint64_t w = 0; w < p->workers; ++w) wsum[w] /= s->wdiag[w];
+  for (uint64_t f = 0; f < p->firms; ++f) y[f] = s->fdiag[f] * x[f];
+  for (uint64_t c = 0; c < p->cells; ++c) y[p->cell_firm[c]] -= p->cell_weight[c] * wsum[p->cell_worker[c]];
+}
+
+static void center(double* v, uint64_t n) {
+  Stable s = {0, 0};
+  for (uint64_t i = 0; i < n; ++i) st_add(&s, v[i]);
+  double m = st_fin(&s) / (double)n;
+  for (uint64_t i = 0; i < n; ++i) v[i] -= m;
+}
+
+static int solver_init(Solver* s, const OracleProblem* p, const OracleOptions* o) {
+  memset(s, 0, sizeof(*s));
+  s->p = p;
+  s->tol = o->tolerance;
+  s->wdiag = calloc(p->workers, sizeof(double));
+  s->fdiag = calloc(p->firms, sizeof(double));
+  s->t_sum = calloc(p->workers, sizeof(double));
+  for (uint64_t c = 0; c < p->cells; ++c) {
+    s->wdiag[p->cell_worker[c]] += p->cell_weight[c];
+    s->fdiag[p->cell_firm[c]] += p->cell_weight[c];
+  }
+  uint64_t F = p->firms;
+  s->dense = F <= o->dense_limit;
+  if (s->dense) {
+    uint64_t m = F - 1;
+    double* A = calloc(m * m, sizeof(double));
+    for (uint64_t f = 0; f < m; ++f) A[f * m + f] = s->fdiag[f];
+    /* subtract sum_w a a^T / d_w over the worker's cells (cells of a worker are contiguous) */
+    uint64_t c = 0;
+    while (c < p->cells) {
+      uint64_t e = c;
+      while (e < p->cells && p->cell_worker[e] == p->cell_worker[c]) ++e;
+      double d = s->wdiag[p->cell_worker[c]];
+      for (uint64_t i = c; i < e; ++i)
+        for (uint64_t j = c; j < e; ++j) {
+          uint64_t fi = p->cell_firm[i], fj = p->cell_firm[j];
+          if (fi < m && fj < m) A[fi * m + fj] -= p->cell_weight[i] * p->cell_weight[j] / d;
+        }
+      c = e;
+    }
+    for (uint64_t j = 0; j < m; ++j) {
+      double dd = A[j * m + j];
+      for (uint64_t k = 0; k < j; ++k) dd -= A[j * m + k] * A[j * m + k];
+      if (!(dd > 0.0)) {
+        free(A);
+        return -1;
+      }
+      dd = sqrt(dd);
+      A[j * m + j] = dd;
+      for (uint64_t i = j + 1; i < m; ++i) {
+        double v = A[i * m + j];
+        for (uint64_t k = 0; k < j; ++k) v -= A[i * m + k] * A[j * m + k];
+        A[i * m + j] = v / dd;
+      }
+    }
+    s->chol = A;
+  } else {
+    s->t_r = calloc(F, sizeof(double));
+    s->t_z = calloc(F, sizeof(double));
+    s->t_p = calloc(F, sizeof(double));
+    s->t_q = calloc(F, sizeof(double));
+  }
+  return 0;
+}
+
+static void solver_free(Solver* s) {
+  free(s->wdiag);
+  free(s->fdiag);
+  free(s->t_sum);
+  free(s->chol);
+  free(s->t_r);
+  free(s->t_z);
+  free(s->t_p);
+  free(s->t_q);
+}
+
+/* Solve the two-way normal equations for (worker_rhs, firm_rhs); firm solution centred. */
+static int solve(Solver* s, const double* bw, const double* bf, double* alpha, double* psi) {
+  const OracleProblem* p = s->p;
+  uint64_t W = p->workers, F = p->firms;
+  /* Schur RHS (operator.rs:269-304) */
+  double* rhs = malloc(F * sizeof(double));
+  memcpy(rhs, bf, F * sizeof(double));
+  for (uint64_t c = 0; c < p->cells; ++c) {
+    uint32_t w = p->cell_worker[c];
+    rhs[p->cell_firm[c]] -= p->cell_weight[c] * (bw[w] / s->wdiag[w]);
+  }
+  center(rhs, F);
+  if (s->dense) {
+    uint64_t m = F - 1;
+    const double* L = s->chol;
+    for (uint64_t i = 0; i < m; ++i) {
+      double v = rhs[i];
+      for (uint64_t k = 0; k < i; ++k) v -= L[i * m + k] * psi[k];
+      psi[i] = v / L[i * m + i];
+    }
+    for (uint64_t ii = m; ii-- > 0;) {
+      double v = psi[ii];
+      for (uint64_t k = ii + 1; k < m; ++k) v -= L[k * m + ii] * psi[k];
+      psi[ii] = v / L[ii * m + ii];
+    }
+    psi[m] = 0.0;
+  } else {
+    double *r = s->t_r, *z = s->t_z, *pp = s->t_p, *q = s->t_q;
+    double bn = 0;
+    for (uint64_t f = 0; f < F; ++f) bn += rhs[f] * rhs[f];
+    bn = sqrt(bn);
+    memset(psi, 0, F * sizeof(double));
+    if (bn > 0) {
+      memcpy(r, rhs, F * sizeof(double));
+      double rz = 0;
+      for (uint64_t f = 0; f < F; ++f) {
+        z[f] = r[f] / s->fdiag[f];
+        rz += r[f] * z[f];
+      }
+      memcpy(pp, z, F * sizeof(double));
+      for (int it = 0; it < 100000; ++it) {
+        schur_apply(s, pp, q, s->t_sum);
+        double pq = 0;
+        for (uint64_t f = 0; f < F; ++f) pq += pp[f] * q[f];
+        if (!(pq > 0)) break;
+        double a = rz / pq, rr = 0, rz2 = 0;
+        for (uint64_t f = 0; f < F; ++f) {
+          psi[f] += a * pp[f];
+          r[f] -= a * q[f];
+          rr += r[f] * r[f];
+        }
+        s->iterations++;
+        if (sqrt(rr) <= s->tol * bn) break;
+        for (uint64_t f = 0; f < F; ++f) {
+          z[f] = r[f] / s->fdiag[f];
+          rz2 += r[f] * z[f];
+        }
+        double b = rz2 / rz;
+        rz = rz2;
+        for (uint64_t f = 0; f < F; ++f) pp[f] = z[f] + b * pp[f];
+      }
+    }
+  }
+  free(rhs);
+  center(psi, F);
+  /* worker reconstruction (operator.rs:311-343) */
+  memcpy(alpha, bw, W * sizeof(double));
+  for (uint64_t c = 0; c < p->cells; ++c) alpha[p->cell_worker[c]] -= p->cell_weight[c] * psi[p->cell_firm[c]];
+  for (uint64_t w = 0; w < W; ++w) alpha[w] /= s->wdiag[w];
+  return 0;
+}
+
+static int set_error(OracleResult* r, int code, const char* msg) {
+  r->error_code = code;
+  strncpy(r->error, msg, sizeof(r->error) - 1);
+  return code;
+}
+
+#define TAG_LEVERAGE 0x4c45564552414745ull
+#define TAG_TARGET 0x0054415247455401ull
+
+int oracle_jla(const OracleProblem* p, const OracleOptions* o, OracleResult* res) {
+  uint64_t W = p->workers, F = p->firms, C = p->cells, G = p->units, S = p->strata, P = o->probes;
+  Solver s;
+  res->error_code = 0;
+  if (solver_init(&s, p, o)) return set_error(res, 82, "grounded Schur factor is not positive definite");
+  double *bw = calloc(W, 8), *bf = calloc(F, 8), *alpha = calloc(W, 8), *psi = calloc(F, 8);
+  double *alpha2 = calloc(W, 8), *psi2 = calloc(F, 8);
+  /* ---- full fit */
+  for (uint64_t c = 0; c < C; ++c) {
+    bw[p->cell_worker[c]] += p->cell_outcome_sum[c];
+    bf[p->cell_firm[c]] += p->cell_outcome_sum[c];
+  }
+  solve(&s, bw, bf, alpha, psi);
+  res->solves++;
+  for (uint64_t c = 0; c < C; ++c) res->fitted_cell[c] = alpha[p->cell_worker[c]] + psi[p->cell_firm[c]];
+  {
+    Stable wm = {0, 0}, fm = {0, 0};
+    for (uint64_t r = 0; r < p->rows; ++r) {
+      st_add(&wm, p->row_target[r] * alpha[p->row_worker[r]]);
+      st_add(&fm, p->row_target[r] * psi[p->row_firm[r]]);
+    }
+    double mw = st_fin(&wm) / p->target_total, mf = st_fin(&fm) / p->target_total;
+    Stable a = {0, 0}, b = {0, 0}, cv = {0, 0}, t = {0, 0};
+    for (uint64_t r = 0; r < p->rows; ++r) {
+      double x = alpha[p->row_worker[r]] - mw, y = psi[p->row_firm[r]] - mf, wt = p->row_target[r];
+      st_add(&a, wt * x * x);
+      st_add(&b, wt * y * y);
+      st_add(&cv, wt * x * y);
+      st_add(&t, wt * (x + y) * (x + y));
+    }
+    res->plugin[0] = st_fin(&a) / p->target_total;
+    res->plugin[1] = st_fin(&b) / p->target_total;
+    res->plugin[2] = st_fin(&cv) / p->target_total;
+    res->plugin[3] = st_fin(&t) / p->target_total;
+  }
+  /* ---- leverage moments, one probe at a time (batch invariant) */
+  Stable* mom = calloc(G * 5, sizeof(Stable));
+  int64_t* atoms = calloc(G > S ? G : S, sizeof(int64_t));
+  for (uint64_t probe = 0; probe < P; ++probe) {
+    memset(bw, 0, W * 8);
+    memset(bf, 0, F * 8);
+    for (uint64_t g = 0; g < G; ++g) {
+      int ok;
+      atoms[g] = oracle_rademacher_sum(o->seed, TAG_LEVERAGE, probe, p->unit_rank[g], p->unit_count[g], &ok);
+      if (!ok) return set_error(res, 70, "Rademacher trial count must lie in [1, 2^53]");
+      uint32_t c = p->unit_cell[g];
+      bw[p->cell_worker[c]] += (double)atoms[g];
+      bf[p->cell_firm[c]] += (double)atoms[g];
+    }
+    solve(&s, bw, bf, alpha, psi);
+    res->solves++;
+    for (uint64_t g = 0; g < G; ++g) {
+      uint32_t c = p->unit_cell[g];
+      double rn = sqrt((double)p->unit_count[g]);
+      double pr = rn * (alpha[p->cell_worker[c]] + psi[p->cell_firm[c]]);
+      double m = (double)atoms[g] / rn - pr, p2 = pr * pr, m2 = m * m;
+      st_add(&mom[g * 5 + 0], p2);
+      st_add(&mom[g * 5 + 1], m2);
+      st_add(&mom[g * 5 + 2], p2 * p2);
+      st_add(&mom[g * 5 + 3], m2 * m2);
+      st_add(&mom[g * 5 + 4], p2 * m2);
+    }
+  }
+  /* ---- adjustment */
+  double mean = 0.0;
+  if (o->centering == 1) {
+    double anchor = p->row_outcome[0];
+    Stable sm = {0, 0};
+    for (uint64_t r = 0; r < p->rows; ++r)
+      st_add(&sm, (p->row_outcome[r] - anchor) * ((double)p->row_frequency[r] / (double)p->physical_total));
+    mean = anchor + st_fin(&sm);
+  }
+  Stable* cw = calloc(C, sizeof(Stable));
+  double Pd = (double)P;
+  for (uint64_t g = 0; g < G; ++g) {
+    double pf = st_fin(&mom[g * 5 + 0]), mf = st_fin(&mom[g * 5 + 1]);
+    double tm = (pf + mf) / Pd;
+    if (!(tm > o->block_tolerance)) return set_error(res, 74, "projection/residual mass failed");
+    double proj = (pf / Pd) / tm, resid = (mf / Pd) / tm;
+    double ps = st_fin(&mom[g * 5 + 2]) / Pd, ms = st_fin(&mom[g * 5 + 3]) / Pd, mx = st_fin(&mom[g * 5 + 4]) / Pd;
+    double bias = (resid * ps - proj * ms + (resid - proj) * mx) / Pd;
+    double var = (resid * resid * ps + proj * proj * ms - 2.0 * proj * resid * mx) / Pd;
+    if (var < -100.0 * o->rank_tolerance) return set_error(res, 73, "finite-projection variance is negative");
+    if (var < 0) var = 0;
+    if (1.0 - proj <= o->block_tolerance) return set_error(res, 75, "match residual block is singular");
+    double rec = 1.0 / resid;
+    uint32_t c = p->unit_cell[g];
+    double ro = p->unit_outcome_sum[g] - (double)p->unit_count[g] * res->fitted_cell[c];
+    double mult = rec + bias * rec * rec - var * rec * rec * rec;
+    double del = ro * mult;
+    st_add(&cw[c], (p->unit_outcome_sum[g] - mean * (double)p->unit_count[g]) * del);
+    res->projection_share[g] = proj;
+    res->residual_share[g] = resid;
+    res->finite_bias[g] = bias;
+    res->finite_variance[g] = var;
+    res->residual_mass[g] = ro;
+    res->deleted_mass[g] = del;
+  }
+  for (uint64_t c = 0; c < C; ++c) res->cell_correction_weight[c] = st_fin(&cw[c]);
+  /* ---- target draws */
+  Stable* dir = calloc(C, sizeof(Stable));
+  double* d = calloc(C, 8);
+  double *sw = calloc(W, 8), *sf = calloc(F, 8), *zw = calloc(W, 8), *zf = calloc(F, 8);
+  for (uint64_t probe = 0; probe < P; ++probe) {
+    memset(dir, 0, C * sizeof(Stable));
+    for (uint64_t k = 0; k < S; ++k) {
+      int ok;
+      int64_t a = oracle_rademacher_sum(o->seed, TAG_TARGET, probe, p->stratum_rank[k], p->stratum_count[k], &ok);
+      if (!ok) return set_error(res, 70, "Rademacher trial count must lie in [1, 2^53]");
+      st_add(&dir[p->stratum_cell[k]], sqrt(p->stratum_per_copy[k] / p->target_total) * (double)a);
+    }
+    Stable tot = {0, 0}, ab = {0, 0};
+    for (uint64_t c = 0; c < C; ++c) {
+      d[c] = st_fin(&dir[c]);
+      st_add(&tot, d[c]);
+      st_add(&ab, fabs(d[c]));
+    }
+    double total = st_fin(&tot), refscale = st_fin(&ab) + fabs(total);
+    for (uint64_t c = 0; c < C; ++c) d[c] -= p->cell_target_sum[c] / p->target_total * total;
+    memset(sw, 0, W * 8);
+    memset(sf, 0, F * 8);
+    for (uint64_t c = 0; c < C; ++c) {
+      sw[p->cell_worker[c]] += d[c];
+      sf[p->cell_firm[c]] += d[c];
+    }
+    /* balance repair of the last entry */
+    double* sides[2] = {sw, sf};
+    uint64_t lens[2] = {W, F};
+    for (int k = 0; k < 2; ++k) {
+      Stable pre = {0, 0};
+      for (uint64_t i = 0; i + 1 < lens[k]; ++i) st_add(&pre, sides[k][i]);
+      double last = -st_fin(&pre), orig = sides[k][lens[k] - 1];
+      if ((refscale == 0.0 && last != orig) || (refscale > 0.0 && fabs(last - orig) > 4096.0 * 2.220446049250313e-16 * refscale))
+        return set_error(res, 77, "compatibility repair exceeded roundoff");
+      sides[k][lens[k] - 1] = last;
+    }
+    memset(zw, 0, W * 8);
+    memset(zf, 0, F * 8);
+    solve(&s, sw, zf, alpha, psi);   /* worker side: (score_W, 0) */
+    solve(&s, zw, sf, alpha2, psi2); /* firm side: (0, score_F) */
+    res->solves += 2;
+    Stable uu = {0, 0}, vv = {0, 0}, uv = {0, 0};
+    for (uint64_t c = 0; c < C; ++c) {
+      double u = alpha[p->cell_worker[c]] + psi[p->cell_firm[c]];
+      double v = alpha2[p->cell_worker[c]] + psi2[p->cell_firm[c]];
+      double wt = res->cell_correction_weight[c];
+      st_add(&uu, wt * u * u);
+      st_add(&vv, wt * v * v);
+      st_add(&uv, wt * u * v);
+    }
+    double a = st_fin(&uu), b = st_fin(&vv), cv = st_fin(&uv);
+    res->target_draws[probe * 4 + 0] = a;
+    res->target_draws[probe * 4 + 1] = b;
+    res->target_draws[probe * 4 + 2] = cv;
+    res->target_draws[probe * 4 + 3] = a + b + 2.0 * cv;
+  }
+  /* ---- mean, corrected, MCSE */
+  for (int k = 0; k < 4; ++k) {
+    Stable m = {0, 0};
+    for (uint64_t q = 0; q < P; ++q) st_add(&m, res->target_draws[q * 4 + k]);
+    res->correction[k] = st_fin(&m) / Pd;
+    res->corrected[k] = res->plugin[k] - res->correction[k];
+    Stable v = {0, 0};
+    for (uint64_t q = 0; q < P; ++q) {
+      double e = res->target_draws[q * 4 + k] - res->correction[k];
+      st_add(&v, e * e);
+    }
+    res->mcse[k] = sqrt(st_fin(&v) / (Pd * (Pd - 1.0)));
+  }
+  res->cg_iterations = s.iterations;
+  free(mom);
+  free(atoms);
+  free(cw);
+  free(dir);
+  free(d);
+  free(sw);
+  free(sf);
+  free(zw);
+  free(zf);
+  free(bw);
+  free(bf);
+  free(alpha);
+  free(psi);
+  free(alpha2);
+  free(psi2);
+  solver_free(&s);
+  return 0;
+}
