@@ -1,0 +1,333 @@
+"""Benchmark: JLA probe solves/s (and time-to-decomposition) on a seeded panel.
+
+A step is one complete leave-out decomposition of the prepared panel: the full
+fit, P leverage probes and 2P target solves (1 + 3P right-hand sides), the
+leverage adjustment, the target contraction and the four components.
+
+* ``value``  device-resident throughput: the prepared problem is in HBM and a
+  step re-runs the solve (``fevcb_engine_resolve_v1``); CUDA events on the
+  library's stream bracket exactly K steps after W warm-up steps.
+* ``e2e``    the same metric through the plugin C ABI a caller uses: each step
+  is ``solve_v1`` + ``result_v1`` on a freshly prepared generation, so the
+  host->device upload of the prepared problem and the device->host result read
+  are inside the timed region (host preparation is outside it and reported
+  separately as ``prepare_s``; prepare + solve is the time-to-decomposition).
+* ``roofline``  the dominant kernel (blocked SpMM on the hybrid Laplacian)
+  timed standalone with CUDA events, L2 flushed before each launch.
+* ``cpu_baseline``  the reference's own CPU implementation (its shipped plugin,
+  staged in oracle/_ref by oracle/build.py; else the C oracle) on a bounded
+  sample of the same panel, all host cores.
+
+``--impl reference`` times the reference plugin alone (rank 0) on the same
+panel and metric and prints its own JSON line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "plain_1m"
+METRIC = "JLA probe solves/s & time-to-decomposition, learned+batched vs plain GPU PCG"
+UNIT = "probe solves/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--probes", type=int, default=200)
+    ap.add_argument("--tolerance", type=float, default=1e-8)
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--precond", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-probes", type=int, default=24)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._thread = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                parts = [p.strip() for p in out.stdout.strip().split(",")]
+                if len(parts) == 7:
+                    self.samples.append(parts)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._thread.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def build_panel(args):
+    from fevc_b200.panel import named_panel
+
+    panel = named_panel(args.workload, args.scale)
+    controls = len(panel.controls)
+    # The device engine runs the compressed (no-control, match-deletion) JLA
+    # estimator; year controls are not yet absorbed, so they are dropped here.
+    panel.controls = []
+    return panel, controls
+
+
+def reference_plugin_path():
+    p = ROOT / "oracle" / "_ref" / "fevc_rust_linux_x64.plugin"
+    return p if p.exists() else None
+
+
+def time_reference(panel, probes, tolerance, steps, warmup):
+    """The reference plugin's V5 full-CMG solve (CMG_FULL_V2) on all host cores."""
+    from fevc_b200 import abi
+
+    lib = abi.load(reference_plugin_path(), bind_extensions=False)
+    threads = os.cpu_count() or 1
+    times, prep_times, res = [], [], None
+    for i in range(warmup + steps):
+        e = abi.Engine(lib)
+        t0 = time.perf_counter()
+        e.prepare(panel)
+        t1 = time.perf_counter()
+        q = e.default_request_v5()
+        q.v4.v3.v2.v1.probes = probes
+        q.v4.v3.v2.algorithm = 2
+        q.v4.v3.v2.v1.pcg_tolerance = tolerance
+        q.threads = threads
+        q.full_cmg_v2 = 1
+        q.tolerance_supplied = 1
+        e.solve_v5(q)
+        res = e.result()
+        t2 = time.perf_counter()
+        e.release()
+        if i >= warmup:
+            times.append(t2 - t1)
+            prep_times.append(t1 - t0)
+    rhs = 1 + 3 * probes
+    return {"rhs_per_s": rhs / float(np.median(times)), "solve_s": float(np.median(times)),
+            "prepare_s": float(np.median(prep_times)), "threads": threads, "components": res}
+
+
+def cpu_baseline(panel, probes, tolerance):
+    if reference_plugin_path() is not None:
+        r = time_reference(panel, probes, tolerance, steps=1, warmup=0)
+        return {"value": round(r["rhs_per_s"], 3), "unit": UNIT, "cores": r["threads"], "kind": "reference",
+                "sample": f"reference plugin CMG_FULL_V2 solve of the same panel with {probes} probes "
+                          f"({1 + 3 * probes} RHS) at tol {tolerance:g}; solve phase {r['solve_s']:.2f} s, "
+                          f"prepare {r['prepare_s']:.2f} s"}
+    return None
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    panel, controls = build_panel(args)
+    if reference_plugin_path() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference plugin not staged (run oracle/build.py)"}))
+        return
+    probes = min(args.probes, args.cpu_probes)
+    r = time_reference(panel, probes, args.tolerance, args.steps, args.warmup)
+    line = {"metric": METRIC, "value": round(r["rhs_per_s"], 4), "unit": UNIT, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1000 * r["solve_s"], 2), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, fevc_b200/panel.py)",
+            "config": {"workload": f"{args.workload} panel, {probes}-probe sample", "probes": probes,
+                       "tolerance": args.tolerance, "year_controls_dropped": controls},
+            "prepare_s": round(r["prepare_s"], 3),
+            "cpu_baseline": {"value": round(r["rhs_per_s"], 4), "unit": UNIT, "cores": r["threads"],
+                             "kind": "reference", "sample": f"{probes} probes ({1 + 3 * probes} RHS) per step"},
+            "e2e": {"value": round(r["rhs_per_s"], 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    from fevc_b200 import abi
+
+    lib = abi.load()
+    stream = torch.cuda.Stream()  # the library launches on this stream; the events below record on it
+    torch.cuda.set_stream(stream)
+    lib.fevcb_set_stream(C.c_void_p(stream.cuda_stream))
+    panel, controls = build_panel(args)
+
+    e = abi.Engine(lib)
+    t0 = time.perf_counter()
+    e.prepare(panel)
+    prepare_s = time.perf_counter() - t0
+    e.device_options(args.block, args.precond)
+    req = e.default_request()
+    req.probes = args.probes
+    req.pcg_tolerance = args.tolerance
+    req.maximum_iterations = 20000
+    t0 = time.perf_counter()
+    e.solve(req)
+    torch.cuda.synchronize()
+    first_solve_s = time.perf_counter() - t0
+    result = e.result()
+    rhs = 1 + 3 * args.probes
+
+    for _ in range(args.warmup):
+        e.resolve()
+    barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            e.resolve()
+        stop.record(stream)
+        barrier()
+    ms = start.elapsed_time(stop)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    timings = e.timings()
+    value = world * rhs * args.steps / (ms / 1000.0)
+
+    # roofline: the blocked SpMM, standalone launches with L2 flushed
+    block = args.block or 32
+    spmm_ms, spmm_bytes = e.kernel_benchmark(1, block, 20)
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = spmm_bytes / (spmm_ms / 1000.0) / 1e9
+    h2d = int(timings["h2d_bytes"])
+    e.release()
+
+    # e2e through the C ABI: solve + result on a fresh generation per step
+    e2e_times = []
+    for i in range(args.e2e_steps + 1):
+        g = abi.Engine(lib)
+        g.prepare(panel)
+        g.device_options(args.block, args.precond)
+        barrier()
+        t0 = time.perf_counter()
+        g.solve(req)
+        g.result()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        g.release()
+        if i > 0:
+            e2e_times.append(t1 - t0)
+    e2e_s = float(np.median(e2e_times))
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * rhs / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(panel, min(args.probes, args.cpu_probes), args.tolerance)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, fevc_b200/panel.py)",
+            "config": {"workload": f"{args.workload} panel ({panel.info['workers']} workers, "
+                                   f"{panel.info['firms']} firms, {panel.info['periods']} periods), "
+                                   f"{args.probes} probes, compressed JLA, match deletion",
+                       "probes": args.probes, "rhs_per_step": rhs, "tolerance": args.tolerance,
+                       "block_columns": block, "preconditioner": "jacobi" if args.precond == 1 else "auto",
+                       "year_controls_dropped": controls, "parallelism": f"replicas x{world}",
+                       "l2": "working set per step larger than L2 (126 MB)",
+                       "retained": {"workers": int(timings["vertices"]) and None}},
+            "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": 144, "seconds_per_step": round(e2e_s, 4)},
+            "time_to_decomposition_s": round(prepare_s + e2e_s, 3), "prepare_s": round(prepare_s, 3),
+            "first_solve_s": round(first_solve_s, 3),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "kernel": f"k_spmm_dot<{block}>", "bytes_per_launch": spmm_bytes,
+                         "ms_per_launch": round(spmm_ms, 5), "peak_source": "measured (MEASURED_PEAKS.json)"},
+            "gpu_launches": int(timings["kernel_launches"]) * args.steps,
+            "solver": {k: timings[k] for k in ("block_iterations", "column_iterations", "rhs_columns",
+                                               "vertices", "edges", "kept_workers", "levels")},
+            "components": {k: [round(x, 10) for x in v] for k, v in result.items()},
+            "clocks": clocks.summary(),
+        }
+        del line["config"]["retained"]
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

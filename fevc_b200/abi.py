@@ -221,8 +221,34 @@ SIGNATURES = {
     "fevcb_engine_timings_v1": (i32, [u64, C.c_void_p, u32]),
     "fevcb_engine_resolve_v1": (i32, [u64]),
     "fevcb_engine_unit_detail_v1": (i32, [u64, u64] + [dptr] * 6 + [u64, dptr, dptr, u64, dptr]),
+    "fevcb_engine_problem_view_v1": (i32, [u64, C.c_void_p, u32]),
+    "fevcb_engine_kernel_benchmark_v1": (i32, [u64, u32, u32, u32, C.POINTER(f64), C.POINTER(f64)]),
     "fevcb_counter_atoms_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64, C.POINTER(i64)]),
 }
+
+def capability_signature_v3(req: SolveRequestV4, controls_count: int) -> int:
+    """Request signature that V4+ solves must carry: FNV-1a over the request's
+    capability fields (reference vckss-plugin/src/ffi_engine.rs:9492-9532,
+    field mapping ffi_engine.rs:10425-10460)."""
+    h = 0xCBF29CE484222325
+
+    def eat(data: bytes):
+        nonlocal h
+        for b in data:
+            h ^= b
+            h = (h * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
+
+    v3, v2, v1 = req.v3, req.v3.v2, req.v3.v2.v1
+    eat(b"VCKSS-REQUEST-CAPABILITY-V3")
+    for v in (v3.capability_schema, v2.algorithm, v1.deletion_mode, v2.nuisance_mode, v1.solver_route,
+              v1.rng_contract, controls_count, v3.frequency_use, v3.engine, v3.batch_mode, v3.stayers_mode,
+              v3.target_weight_mode, v3.deletion_unit_source, v3.probeorder_supplied, v3.wallseconds_supplied,
+              req.leverage_batch_mode, req.target_batch_mode, v1.allow_automatic_cmg_setup_fallback):
+        eat(int(v).to_bytes(4, "little"))
+    eat(int(v3.physical_limit).to_bytes(8, "little"))
+    eat(C.c_uint64.from_buffer_copy(C.c_double(req.wallseconds)).value.to_bytes(8, "little"))
+    return h
+
 
 LIBRARY_PATH = Path(__file__).resolve().parent / "libfevc_b200.so"
 
@@ -320,6 +346,15 @@ class Engine:
     def solve(self, req: SolveRequestV1) -> None:
         self.check(self.lib.vckss_rust_engine_solve_v1(self.generation, C.byref(req)))
 
+    def default_request_v5(self) -> SolveRequestV5:
+        req = SolveRequestV5()
+        self.check(self.lib.vckss_rust_engine_default_solve_request_v5(C.byref(req), C.sizeof(req)))
+        return req
+
+    def solve_v5(self, req: SolveRequestV5, controls_count: int = 0) -> None:
+        req.v4.v3.request_signature = capability_signature_v3(req.v4, controls_count)
+        self.check(self.lib.vckss_rust_engine_solve_v5(self.generation, C.byref(req)))
+
     def result(self) -> dict:
         r = ResultV1()
         self.check(self.lib.vckss_rust_engine_result_v1(self.generation, C.byref(r), C.sizeof(r)))
@@ -347,6 +382,12 @@ class Engine:
 
     def resolve(self) -> None:
         self.check(self.lib.fevcb_engine_resolve_v1(self.generation))
+
+    def kernel_benchmark(self, kernel: int, block_columns: int, launches: int) -> tuple[float, float]:
+        ms, nbytes = f64(0), f64(0)
+        self.check(self.lib.fevcb_engine_kernel_benchmark_v1(self.generation, kernel, block_columns, launches,
+                                                             C.byref(ms), C.byref(nbytes)))
+        return ms.value, nbytes.value
 
     def unit_detail(self, units: int, cells: int, probes: int) -> dict:
         names = ("projection_share", "residual_share", "finite_bias", "finite_variance", "residual_mass",

@@ -954,6 +954,17 @@ int32_t fevcb_engine_problem_view_v1(uint64_t generation, FevcbProblemViewV1* ou
   });
 }
 
+int32_t fevcb_engine_kernel_benchmark_v1(uint64_t generation, uint32_t kernel, uint32_t block_columns,
+                                         uint32_t launches, double* ms, double* bytes) {
+  return status([&] {
+    if (!ms || !bytes) fail(INVALID_INPUT, "benchmark", "output pointers are null");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_kernel_benchmark");
+    if (!p.device) fail(STALE_CONTEXT, "engine_kernel_benchmark", "generation has no device state; solve it first");
+    device_kernel_benchmark(*p.device, int(kernel), int(block_columns), int(launches), ms, bytes);
+  });
+}
+
 int32_t fevcb_counter_atoms_v1(uint64_t seed, uint64_t domain_tag, uint64_t first_probe, uint32_t columns,
                                const uint64_t* entity, const uint64_t* trials, uint64_t count, int64_t* out) {
   return status([&] {

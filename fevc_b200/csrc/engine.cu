@@ -153,8 +153,10 @@ static bool g_user_stream_set = false;
 
 void set_device_stream(void* s) {
   std::lock_guard<std::mutex> l(g_stream_mu);
+  // NULL selects a library-owned non-blocking stream: the legacy default
+  // stream cannot be captured into the PCG iteration graphs.
   g_user_stream = static_cast<cudaStream_t>(s);
-  g_user_stream_set = true;
+  g_user_stream_set = s != nullptr;
 }
 
 void* device_stream() {
@@ -985,6 +987,74 @@ SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& pl
     default: fail(INVALID_INPUT, "jla_validate", "device block width must be 8, 16, 32 or 64");
   }
   return res;
+}
+
+namespace {
+
+template <int K>
+void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, double* bytes) {
+  BlockWork& w = get_work<K>(e);
+  Launch L{grid_blocks(), e.stream};
+  size_t vec = size_t(e.n) * K * sizeof(double);
+  CK(cudaMemsetAsync(w.p.p, 0, vec, L.s));
+  CK(cudaMemsetAsync(w.x.p, 0, vec, L.s));
+  CK(cudaMemsetAsync(w.r.p, 0, vec, L.s));
+  CK(cudaMemsetAsync(w.q.p, 0, vec, L.s));
+  CK(cudaMemsetAsync(w.s.alpha, 0, K * sizeof(double), L.s));
+  DBuf<char> flush(size_t(256) << 20);  // larger than the 126 MB L2
+  double nnz = double(e.L_col.n), n = double(e.n);
+  PhiloxKey key = philox_key(8675309);
+  switch (kernel) {
+    case 1: *bytes = nnz * 12 + n * 8 + (n + 1) * 4 + 2 * n * K * 8; break;
+    case 2: *bytes = n * 8 + 7 * n * K * 8; break;  // dinv; read p q x r; write x r z
+    case 3: *bytes = double(e.G) * (8 + 8 + K * 8) + double(e.C) * (4 + K * 8); break;
+    case 4: *bytes = double(e.G) * (4 + 8 + K * 8 + 5 * 8 * 2) + double(e.G) * 2 * K * 8 + double(e.C) * 8; break;
+    default: fail(INVALID_INPUT, "benchmark", "unknown kernel id");
+  }
+  float total = 0.0f;
+  for (int i = 0; i < launches; ++i) {
+    CK(cudaMemsetAsync(flush.p, i & 0xff, flush.bytes(), L.s));
+    CK(cudaEventRecord(e.ev0, L.s));
+    switch (kernel) {
+      case 1:
+        k_spmm_dot<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_ptr.p, e.L_col.p, e.L_val.p, e.L_diag.p, w.p.p, w.q.p,
+                                                   e.partial.p);
+        break;
+      case 2:
+        k_update_jacobi<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_dinv.p, w.p.p, w.q.p, w.x.p, w.r.p, w.z.p, w.s.alpha,
+                                                        e.partial.p);
+        break;
+      case 3:
+        k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p, key,
+                                                         TAG_LEVERAGE, 0, K, w.unit_atoms.p, w.cell_val.p);
+        break;
+      case 4:
+        k_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.G, K, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
+                                                  e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.moments.p);
+        break;
+    }
+    CK(cudaEventRecord(e.ev1, L.s));
+    CK(cudaEventSynchronize(e.ev1));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, e.ev0, e.ev1));
+    total += t;
+  }
+  CK_LAUNCH();
+  *ms = double(total) / launches;
+}
+
+}  // namespace
+
+void device_kernel_benchmark(DeviceEngine& e, int kernel, int block_columns, int launches, double* ms,
+                             double* bytes) {
+  if (launches < 1) fail(INVALID_INPUT, "benchmark", "launch count must be positive");
+  switch (block_columns) {
+    case 8: kernel_benchmark_k<8>(e, kernel, launches, ms, bytes); break;
+    case 16: kernel_benchmark_k<16>(e, kernel, launches, ms, bytes); break;
+    case 32: kernel_benchmark_k<32>(e, kernel, launches, ms, bytes); break;
+    case 64: kernel_benchmark_k<64>(e, kernel, launches, ms, bytes); break;
+    default: fail(INVALID_INPUT, "benchmark", "block width must be 8, 16, 32 or 64");
+  }
 }
 
 void device_atoms(uint64_t seed, uint64_t tag, uint64_t first_probe, uint32_t columns, const uint64_t* entity,

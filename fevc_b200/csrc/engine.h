@@ -78,6 +78,14 @@ DeviceStats device_stats(const DeviceEngine& e);
 SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o,
                          bool want_unit_detail);
 
+// Time `launches` standalone launches of one hot kernel on the prepared
+// problem with CUDA events (L2 flushed before each launch).  kernel: 1 SpMM
+// with the step-length dot, 2 PCG update with the Jacobi apply, 3 leverage
+// Counter-V1 atoms with the per-cell sums, 4 leverage moments.  Returns the
+// mean device milliseconds per launch and the algorithmic bytes per launch.
+void device_kernel_benchmark(DeviceEngine& e, int kernel, int block_columns, int launches, double* ms_per_launch,
+                             double* bytes_per_launch);
+
 // Raw Counter-V1 atoms on the device (tests): out[e * columns + j] for probe first+j.
 void device_atoms(uint64_t seed, uint64_t tag, uint64_t first_probe, uint32_t columns, const uint64_t* entity,
                   const uint64_t* trials, uint64_t count, int64_t* out);

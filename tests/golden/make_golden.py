@@ -1,0 +1,176 @@
+"""Regenerate the golden fixtures in this directory from the reference plugin.
+
+The reference's shipped Linux plugin (``fevc/fevc_rust_linux_x64.plugin`` in
+the reference checkout) is loaded with dlopen and driven only through its C ABI
+(the same ctypes bindings the tests use for this library).  Every fixture
+records the inputs (or the seeded generator call that reproduces them, with a
+checksum of the generated columns) and the plugin's outputs:
+
+* ``prep_cases.json``   retained masks, preparation receipts and status codes
+                         for panels and adversarial inputs;
+* ``jla_cases.json``     components (plug-in, correction, corrected, MCSE) of
+                         solved panels at a tight diagonal-PCG tolerance.
+
+Run from the repository root:  ``python tests/golden/make_golden.py``.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from fevc_b200 import abi  # noqa: E402
+from fevc_b200.panel import Panel, generate_panel  # noqa: E402
+
+PLUGIN = Path("/root/reference/fevc/fevc_rust_linux_x64.plugin")
+HERE = Path(__file__).resolve().parent
+
+
+def panel_digest(p: Panel) -> str:
+    h = hashlib.sha256()
+    for a in (p.worker, p.firm, p.deletion, p.outcome, p.frequency, p.target_weight, *p.controls):
+        h.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def kat12() -> Panel:
+    """The 12-row design of the reference's shared-atom known-answer test
+    (rust/crates/vckss-core/tests/rust_mata_shared_atoms.rs:39-47), in its
+    permuted row order."""
+    worker = [1, 1, 1, 1, 2, 2, 2, 2, 9, 9, 10, 10]
+    firm = [1, 1, 2, 2, 1, 1, 2, 2, 9, 10, 9, 10]
+    deletion = [11, 12, 21, 22, 31, 32, 41, 42, 91, 92, 93, 94]
+    outcome = [1, 3, 0, 2, -1, 1, 2, -2, 10, 11, 12, 13]
+    frequency = [1, 2, 1, 2, 1, 3, 2, 1, 1, 1, 1, 1]
+    target = [1, 2, 2, 2, 3, 9, 8, 4, 1, 1, 1, 1]
+    order = [7, 2, 8, 5, 0, 9, 3, 11, 10, 1, 6, 4]
+    g = lambda a: np.array([a[r] for r in order], dtype=np.float64)  # noqa: E731
+    return Panel(g(worker), g(firm), g(deletion), g(outcome), g(frequency), g(target))
+
+
+def weighted_panel(seed: int) -> Panel:
+    """A generated panel with literal frequency weights, uneven target weights
+    and several rows per deletion unit (exercises the per-copy mass strata)."""
+    p = generate_panel(1500, 120, 5, move_p=0.25, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    p.frequency = rng.integers(1, 4, p.rows).astype(np.float64)
+    p.target_weight = np.round(rng.uniform(0.5, 3.0, p.rows) * 4) / 4 * p.frequency
+    return p
+
+
+PANELS = {
+    "kat12": dict(build=lambda: kat12(), probes=5),
+    "small_2k": dict(build=lambda: generate_panel(2000, 150, 5, move_p=0.2, seed=11), probes=24),
+    "exact_20k": dict(build=lambda: generate_panel(20000, 1000, 5, seed=20261203), probes=40),
+    "weighted_1500": dict(build=lambda: weighted_panel(5), probes=16),
+    "pareto13_4k": dict(build=lambda: generate_panel(4000, 200, 6, move_p=0.08, pareto_shape=1.3, seed=3), probes=20),
+    "regions_4k": dict(build=lambda: generate_panel(4000, 200, 6, regions=2, cross_p=0.01, seed=4), probes=20),
+}
+
+
+def error_cases():
+    base = kat12()
+
+    def mod(**kw):
+        p = Panel(*(np.array(getattr(base, f), copy=True) for f in
+                    ("worker", "firm", "deletion", "outcome", "frequency", "target_weight")))
+        for k, fn in kw.items():
+            setattr(p, k, fn(getattr(p, k)))
+        return p
+
+    def setv(i, v):
+        def f(a):
+            a[i] = v
+            return a
+        return f
+
+    return {
+        "nonfinite_outcome": mod(outcome=setv(3, np.nan)),
+        "zero_frequency": mod(frequency=setv(2, 0.0)),
+        "fractional_frequency": mod(frequency=setv(2, 1.5)),
+        "negative_target": mod(target_weight=setv(1, -1.0)),
+        "zero_worker_id": mod(worker=setv(0, 0.0)),
+        "fractional_firm_id": mod(firm=setv(0, 1.5)),
+        "deletion_crosses_cells": mod(deletion=setv(0, 12.0)),
+        "all_zero_target": mod(target_weight=lambda a: a * 0.0),
+        # two identical disconnected blocks: largest-component tie
+        "tied_components": Panel(np.array([1, 1, 2, 2, 3, 3, 4, 4], float), np.array([1, 2, 1, 2, 3, 4, 3, 4], float),
+                                 np.arange(1, 9, dtype=float), np.arange(8, dtype=float), np.ones(8), np.ones(8)),
+        # a single firm: nothing identified
+        "single_firm": Panel(np.array([1, 1, 2, 2], float), np.array([1, 1, 1, 1], float),
+                             np.arange(1, 5, dtype=float), np.arange(4, dtype=float), np.ones(4), np.ones(4)),
+    }
+
+
+def prepare_record(lib, panel: Panel) -> dict:
+    e = abi.Engine(lib)
+    try:
+        e.prepare(panel)
+    except abi.EngineError as err:
+        return {"status": err.code}
+    rc = e.receipt()
+    mask = e.retained_mask(panel.rows)
+    e.release()
+    keep = {k: v for k, v in rc.items() if k not in (
+        "generation", "struct_size", "reserved", "memory_limit_bytes", "caller_copy_bytes",
+        "preparation_peak_forecast_bytes", "prepared_resident_bytes")}
+    return {"status": 0, "receipt": keep, "mask_sha256": hashlib.sha256(mask.tobytes()).hexdigest(),
+            "retained": int(mask.sum())}
+
+
+def solve_record(lib, panel: Panel, probes: int, centering: int) -> dict:
+    e = abi.Engine(lib)
+    e.prepare(panel)
+    if centering:
+        e.centering(centering)
+    q = e.default_request()
+    q.probes = probes
+    q.leverage_batch_width = 4
+    q.target_batch_width = 4
+    q.solver_route = 2  # diagonal PCG
+    q.allow_automatic_cmg_setup_fallback = 0
+    q.pcg_tolerance = 1e-13
+    q.maximum_iterations = 20000
+    q.residual_replacement_interval = 50
+    e.solve(q)
+    res = e.result()
+    e.release()
+    return {"seed": int(q.seed), "probes": probes, "centering": centering, "pcg_tolerance": 1e-13,
+            **{k: list(v) for k, v in res.items()}}
+
+
+def main() -> None:
+    if not PLUGIN.exists():
+        raise SystemExit(f"reference plugin not found at {PLUGIN}")
+    lib = abi.load(PLUGIN, bind_extensions=False)
+    prep, jla = {}, {}
+    for name, spec in PANELS.items():
+        panel = spec["build"]()
+        rec = prepare_record(lib, panel)
+        rec["rows"] = panel.rows
+        rec["panel_sha256"] = panel_digest(panel)
+        prep[name] = rec
+        jla[name] = [solve_record(lib, panel, spec["probes"], 0), solve_record(lib, panel, spec["probes"], 1)]
+        print(name, rec["retained"], jla[name][0]["corrected"])
+    errs = {}
+    for name, panel in error_cases().items():
+        rec = prepare_record(lib, panel)
+        rec["columns"] = {f: [float(x) if np.isfinite(x) else str(x) for x in getattr(panel, f)]
+                          for f in ("worker", "firm", "deletion", "outcome", "frequency", "target_weight")}
+        errs[name] = rec
+        print(name, rec["status"])
+    meta = {"generator": "tests/golden/make_golden.py", "reference_plugin_version":
+            lib.vckss_rust_backend_version().decode()}
+    (HERE / "prep_cases.json").write_text(json.dumps({"meta": meta, "panels": prep, "errors": errs}, indent=1))
+    (HERE / "jla_cases.json").write_text(json.dumps({"meta": meta, "panels": jla}, indent=1))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,120 @@
+"""Device engine parity: Counter-V1 atoms bit-exact against the oracle, and the
+four variance components against the reference plugin's golden results and the
+oracle, through the C ABI on a B200."""
+
+import numpy as np
+import pytest
+
+from fevc_b200 import abi
+
+import make_golden
+
+pytestmark = pytest.mark.gpu
+
+# Component tolerance: relative to the largest component magnitude of the case.
+# The device solves to 1e-12 relative reduced residual; the golden results were
+# solved at 1e-13, so agreement is limited by the solves, far inside 1e-6.
+COMPONENT_RTOL = 1e-8
+
+
+def rel(a, b):
+    a, b = np.asarray(a, dtype=float), np.asarray(b, dtype=float)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def solve(lib, panel, *, probes, centering=0, tol=1e-12, block=0, precond=0, seed=8675309):
+    e = abi.Engine(lib)
+    e.prepare(panel)
+    if centering:
+        e.centering(centering)
+    e.device_options(block, precond)
+    req = e.default_request()
+    req.seed = seed
+    req.probes = probes
+    req.pcg_tolerance = tol
+    req.maximum_iterations = 20000
+    e.solve(req)
+    return e
+
+
+def test_device_atoms_match_oracle(lib, oracle_mod):
+    rng = np.random.default_rng(1)
+    entity = rng.integers(1, 2**40, 300, dtype=np.uint64)
+    trials = np.concatenate([rng.integers(1, 70, 250), [64, 65, 128, 129, 1000, 4097] * 8, [1, 2]])[:300]
+    trials = trials.astype(np.uint64)
+    for tag in (abi.TAG_LEVERAGE, abi.TAG_TARGET):
+        for first, cols in ((0, 8), (3, 5), (17, 11)):
+            dev = abi.device_atoms(lib, 987654321, tag, first, cols, entity, trials)
+            for i in range(0, 300, 7):
+                for j in range(cols):
+                    assert dev[i, j] == oracle_mod.rademacher_sum(987654321, tag, first + j, int(entity[i]),
+                                                                  int(trials[i]))
+
+
+@pytest.mark.parametrize("name", list(make_golden.PANELS))
+@pytest.mark.parametrize("which", [0, 1])
+def test_components_match_reference(lib, golden, name, which):
+    rec = golden["jla"]["panels"][name][which]
+    panel = make_golden.PANELS[name]["build"]()
+    e = solve(lib, panel, probes=rec["probes"], centering=rec["centering"], seed=rec["seed"])
+    res = e.result()
+    e.release()
+    for key in ("plugin", "correction", "corrected", "numerical_mcse"):
+        assert rel(res[key], rec[key]) < COMPONENT_RTOL, (key, res[key], rec[key])
+
+
+@pytest.mark.parametrize("name", ["kat12", "small_2k", "weighted_1500"])
+def test_unit_detail_matches_oracle(lib, oracle_mod, name):
+    panel = make_golden.PANELS[name]["build"]()
+    probes = make_golden.PANELS[name]["probes"]
+    e = solve(lib, panel, probes=probes)
+    view = oracle_mod.problem_view(lib, e.generation)
+    ref = oracle_mod.run(view, probes=probes)
+    det = e.unit_detail(view.units, view.cells, probes)
+    e.release()
+    for key in ("projection_share", "residual_share", "finite_bias", "finite_variance", "residual_mass",
+                "deleted_mass", "fitted_cell", "cell_correction_weight", "target_draws"):
+        assert rel(det[key], ref[key]) < 1e-8, key
+
+
+@pytest.mark.parametrize("block", [8, 16, 32, 64])
+def test_block_width_does_not_change_the_result(lib, golden, block):
+    """Probe batching is schedule-invariant (reference engine.rs:4188)."""
+    rec = golden["jla"]["panels"]["exact_20k"][0]
+    e = solve(lib, make_golden.PANELS["exact_20k"]["build"](), probes=rec["probes"], block=block)
+    res = e.result()
+    e.release()
+    assert rel(res["corrected"], rec["corrected"]) < COMPONENT_RTOL
+
+
+def test_receipts_and_resolve(lib):
+    panel = make_golden.PANELS["small_2k"]["build"]()
+    probes = 24
+    e = solve(lib, panel, probes=probes, tol=1e-10)
+    first = e.result()
+    rc = e.rhs_receipts(1 + 3 * probes)
+    assert sum(r["phase"] == 1 for r in rc) == 1
+    assert sum(r["phase"] == 2 for r in rc) == probes
+    assert sum(r["phase"] == 3 for r in rc) == 2 * probes
+    assert max(r["complete_residual"] for r in rc) <= max(10 * 1e-10, 1e-11)
+    e.resolve()
+    again = e.result()
+    t = e.timings()
+    e.release()
+    assert again == first  # same device program, same inputs: bitwise repeatable
+    assert t["kernel_launches"] > 0 and t["rhs_columns"] == 1 + 3 * probes
+
+
+def test_accounting_identity_on_a_larger_panel(lib):
+    from fevc_b200.panel import generate_panel
+
+    panel = generate_panel(200_000, 10_000, 5, seed=99)
+    e = solve(lib, panel, probes=32, tol=1e-8)
+    res = e.result()
+    rc = e.rhs_receipts(1 + 3 * 32)
+    e.release()
+    for key in ("plugin", "correction", "corrected"):
+        w, f, c, t = res[key]
+        assert abs(t - (w + f + 2 * c)) <= 1e-10 * max(abs(w), abs(f), abs(t), 1.0)
+    assert max(r["complete_residual"] for r in rc) <= 1e-7
+    assert 0 < res["plugin"][0] < 1 and 0 < res["plugin"][1] < 1

@@ -1,0 +1,41 @@
+"""The oracle against the reference plugin's solved golden cases
+(tests/golden/jla_cases.json): the four components, the correction and the MCSE."""
+
+import numpy as np
+import pytest
+
+from fevc_b200 import abi
+
+import make_golden
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.mark.parametrize("name", list(make_golden.PANELS))
+@pytest.mark.parametrize("which", [0, 1])
+def test_oracle_matches_reference(lib, oracle_mod, golden, name, which):
+    rec = golden["jla"]["panels"][name][which]
+    panel = make_golden.PANELS[name]["build"]()
+    e = abi.Engine(lib)
+    e.prepare(panel)
+    out = oracle_mod.run(oracle_mod.problem_view(lib, e.generation), seed=rec["seed"], probes=rec["probes"],
+                         centering=rec["centering"])
+    e.release()
+    for key, okey in (("plugin", "plugin"), ("correction", "correction"), ("corrected", "corrected"),
+                      ("numerical_mcse", "mcse")):
+        assert rel(out[okey], rec[key]) < 1e-11, (key, out[okey], rec[key])
+
+
+def test_kat_unit_detail(lib, oracle_mod):
+    """Per-unit shares of the 12-row known-answer design sum to one and the
+    cell weights are finite (reference rust_mata_shared_atoms.rs:108-194)."""
+    e = abi.Engine(lib)
+    e.prepare(make_golden.kat12())
+    out = oracle_mod.run(oracle_mod.problem_view(lib, e.generation), probes=5)
+    e.release()
+    assert np.allclose(out["projection_share"] + out["residual_share"], 1.0, atol=1e-14)
+    assert out["projection_share"].shape == (8,) and out["cell_correction_weight"].shape == (4,)
+    assert np.all(np.isfinite(out["deleted_mass"]))
