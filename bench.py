@@ -318,6 +318,7 @@ def main():
             "gpu_launches": int(timings["kernel_launches"]) * args.steps,
             "solver": {k: timings[k] for k in ("block_iterations", "column_iterations", "rhs_columns",
                                                "vertices", "edges", "kept_workers", "levels")},
+            "phase_ms": {k: round(timings[k], 3) for k in ("fit_ms", "leverage_ms", "target_ms", "total_ms")},
             "components": {k: [round(x, 10) for x in v] for k, v in result.items()},
             "clocks": clocks.summary(),
         }
