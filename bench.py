@@ -254,9 +254,9 @@ def main():
     timings = e.timings()
     value = world * rhs * args.steps / (ms / 1000.0)
 
-    # roofline: the blocked SpMM, standalone launches with L2 flushed
+    # roofline: the persistent blocked PCG kernel, standalone launches with L2 flushed
     block = args.block or 32
-    spmm_ms, spmm_bytes = e.kernel_benchmark(1, block, 20)
+    spmm_ms, spmm_bytes = e.kernel_benchmark(1, block, 10)
     peaks = {}
     try:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -313,7 +313,7 @@ def main():
             "first_solve_s": round(first_solve_s, 3),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": None,
-                         "kernel": f"k_spmm_dot<{block}>", "bytes_per_launch": spmm_bytes,
+                         "kernel": f"k_pcg_persistent<{block}> (20 iterations per launch)", "bytes_per_launch": spmm_bytes,
                          "ms_per_launch": round(spmm_ms, 5), "peak_source": "measured (MEASURED_PEAKS.json)"},
             "gpu_launches": int(timings["kernel_launches"]) * args.steps,
             "solver": {k: timings[k] for k in ("block_iterations", "column_iterations", "rhs_columns",

@@ -26,6 +26,7 @@
 #include "engine.h"
 #include "jla_kernels.cuh"
 #include "multigrid.h"
+#include "persistent.cuh"
 
 namespace fevcb {
 
@@ -213,6 +214,8 @@ struct DeviceEngine {
   DBuf<double> L_val, L_diag, L_dinv;
   std::unique_ptr<Multigrid> mg;
   int preconditioner = 1;
+  Segments lap_seg, firm_seg;
+  int coop_blocks = 0;
   // solve-long buffers
   DBuf<double> moments, unit_out, omega, fitted, fit_alpha, partial, small;
   DBuf<unsigned long long> error;
@@ -228,7 +231,7 @@ DeviceStats device_stats(const DeviceEngine& e) { return e.stats; }
 // Per block-width workspace and the captured PCG iteration graph.
 struct BlockWork {
   int K;
-  DBuf<double> bW, bF, b, x, r, z, p, q, alpha, cell_val, unit_atoms, dir, tot;
+  DBuf<double> bW, bF, b, x, r, z, p, q, alpha, cell_val, unit_atoms, dir, tot, seg_buf, fseg_out;
   DBuf<double> st;  // 8 * K doubles of per-column state
   DBuf<int> ist;    // 2 * K + 2 ints
   PcgState s;
@@ -321,6 +324,28 @@ void build_hybrid(const Compressed& p, std::vector<uint32_t>& kept_worker, std::
   }
 }
 
+// Cut every CSR row into segments of at most SEG items.
+void build_segments(const std::vector<uint32_t>& ptr, Segments& sg, cudaStream_t s, uint64_t& h2d) {
+  size_t rows = ptr.size() - 1;
+  std::vector<uint32_t> row, begin, end, first(rows + 1, 0);
+  for (size_t r = 0; r < rows; ++r) {
+    first[r] = uint32_t(row.size());
+    uint32_t b = ptr[r], e = ptr[r + 1];
+    if (b == e) continue;
+    for (uint32_t x = b; x < e; x += SEG) {
+      row.push_back(uint32_t(r));
+      begin.push_back(x);
+      end.push_back(std::min(e, x + SEG));
+    }
+  }
+  first[rows] = uint32_t(row.size());
+  sg.count = uint32_t(row.size());
+  upload(sg.row, row, s, h2d);
+  upload(sg.begin, begin, s, h2d);
+  upload(sg.end, end, s, h2d);
+  upload(sg.row_first, first, s, h2d);
+}
+
 }  // namespace
 
 std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaPlan& plan, int preconditioner) {
@@ -355,6 +380,7 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   upload(e->worker_ptr, wptr, s, h2d);
   upload(e->firm_ptr, fptr, s, h2d);
   upload(e->firm_cells, p.firm_index.items, s, h2d);
+  build_segments(fptr, e->firm_seg, s, h2d);
   {
     std::vector<double> fd(p.firms, 0.0);
     for (size_t c = 0; c < p.cells; ++c) fd[p.cell_firm[c]] += p.cell_weight[c];
@@ -428,6 +454,7 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     upload(e->L_val, Lval, s, h2d);
     upload(e->L_diag, Ld, s, h2d);
     upload(e->L_dinv, dinv, s, h2d);
+    build_segments(Lptr, e->lap_seg, s, h2d);
     e->stats.vertices = e->n;
     e->stats.edges = Lcol.size() / 2;
     e->stats.kept_workers = e->kept;
@@ -448,6 +475,14 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   e->small.alloc(1024);
   e->error.alloc(1);
   CK(cudaMallocHost(&e->h_nactive, sizeof(int) * 16));
+  {
+    int dev = 0, sms = 0, per = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_persistent<64>, PERSIST_THREADS, 0));
+    if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the persistent PCG kernel cannot be resident on an SM");
+    e->coop_blocks = sms;  // one 1024-thread block per SM
+  }
   CK(cudaEventCreate(&e->ev0));
   CK(cudaEventCreate(&e->ev1));
   CK(cudaStreamSynchronize(s));
@@ -480,6 +515,8 @@ BlockWork& get_work(DeviceEngine& e) {
   w->unit_atoms.alloc(size_t(e.G) * K);
   w->dir.alloc(size_t(e.C) * (K > 1 ? K / 2 : 1));
   w->tot.alloc(4 * K);
+  w->seg_buf.alloc(size_t(e.lap_seg.count) * K);
+  w->fseg_out.alloc(size_t(e.firm_seg.count) * K);
   w->st.alloc(8 * K);
   w->ist.alloc(2 * K + 4);
   double* st = w->st.p;
@@ -574,39 +611,6 @@ void apply_preconditioner(DeviceEngine& e, BlockWork& w, Launch L, const double*
   }
 }
 
-// One PCG iteration (all kernels enqueued on L.s).
-template <int K>
-void pcg_iteration(DeviceEngine& e, BlockWork& w, Launch L) {
-  double* part = e.partial.p;
-  double* part2 = e.partial.p + size_t(L.grid) * 2 * K;
-  k_spmm_dot<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_ptr.p, e.L_col.p, e.L_val.p, e.L_diag.p, w.p.p, w.q.p, part);
-  k_step_alpha<K><<<1, 128, 0, L.s>>>(part, L.grid, w.s);
-  if (e.preconditioner == 2) {
-    k_update_xr<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.p.p, w.q.p, w.x.p, w.r.p, w.s.alpha, part);
-    apply_preconditioner<K>(e, w, L, w.r.p, w.z.p);
-    k_dot<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.r.p, w.z.p, part2);
-    k_step_beta<K, 1><<<1, 128, 0, L.s>>>(part, L.grid, part2, L.grid, w.s);
-  } else {
-    k_update_jacobi<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_dinv.p, w.p.p, w.q.p, w.x.p, w.r.p, w.z.p, w.s.alpha, part);
-    k_step_beta<K, 2><<<1, 128, 0, L.s>>>(part, L.grid, nullptr, 0, w.s);
-  }
-  k_direction<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.z.p, w.p.p, w.s.beta);
-}
-
-constexpr int GRAPH_ITERS = 8;
-
-template <int K>
-void ensure_graph(DeviceEngine& e, BlockWork& w, Launch L) {
-  if (w.graph) return;
-  cudaGraph_t g;
-  CK(cudaStreamBeginCapture(L.s, cudaStreamCaptureModeThreadLocal));
-  for (int i = 0; i < GRAPH_ITERS; ++i) pcg_iteration<K>(e, w, L);
-  CK(cudaStreamEndCapture(L.s, &g));
-  CK(cudaGraphInstantiate(&w.graph, g, 0));
-  cudaGraphDestroy(g);
-  w.graph_iters = GRAPH_ITERS;
-}
-
 // (Re)start PCG from the current x for the active columns: r = b - mean - L x,
 // z = M^-1 r, p = z, rz.  The mean of b is removed so every residual is
 // orthogonal to the Laplacian null space.
@@ -626,6 +630,55 @@ void pcg_restart(DeviceEngine& e, BlockWork& w, Launch L, bool fresh) {
   CK_LAUNCH();
 }
 
+// Run the persistent PCG kernel until every active column converges or
+// `iterations` iterations have run; returns the iterations executed.
+template <int K>
+int pcg_run(DeviceEngine& e, BlockWork& w, Launch L, int iterations) {
+  PersistentPcg<K> a;
+  a.n = e.n;
+  a.ptr = e.L_ptr.p;
+  a.col = e.L_col.p;
+  a.val = e.L_val.p;
+  a.diag = e.L_diag.p;
+  a.dinv = e.L_dinv.p;
+  a.nseg = e.lap_seg.count;
+  a.seg_row = e.lap_seg.row.p;
+  a.seg_begin = e.lap_seg.begin.p;
+  a.seg_end = e.lap_seg.end.p;
+  a.row_first = e.lap_seg.row_first.p;
+  a.seg_buf = w.seg_buf.p;
+  a.x = w.x.p;
+  a.r = w.r.p;
+  a.p = w.p.p;
+  a.partial_a = e.partial.p;
+  a.partial_b = e.partial.p + size_t(e.coop_blocks) * K;
+  a.s = w.s;
+  a.max_iters = iterations;
+  void* args[] = {&a};
+  CK(cudaLaunchCooperativeKernel((const void*)k_pcg_persistent<K>, dim3(e.coop_blocks), dim3(PERSIST_THREADS), args,
+                                 0, L.s));
+  CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+  std::vector<int> it(K);
+  CK(cudaMemcpyAsync(it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost, L.s));
+  CK(cudaStreamSynchronize(L.s));
+  int mx = 0;
+  for (int v : it) mx = std::max(mx, v);
+  return mx;
+}
+
+// Segmented firm-side gather (op as in k_seg_firm) finished per row.
+template <int K, int OP, int MODE>
+void firm_gather(DeviceEngine& e, BlockWork& w, Launch L, const double* coef, const double* src,
+                 const double* total, double inv_total, const double* bF, const double* bW, const double* psi,
+                 double* out, double* partial) {
+  k_seg_firm<K, OP><<<L.grid, THREADS, 0, L.s>>>(e.firm_seg.count, e.firm_seg.begin.p, e.firm_seg.end.p,
+                                                  e.firm_cells.p, e.cell_worker.p, coef, src, total, inv_total,
+                                                  w.fseg_out.p);
+  k_seg_firm_finish<K, MODE><<<L.grid, THREADS, 0, L.s>>>(e.F, e.kept, e.firm_seg.row_first.p, w.fseg_out.p, bF, bW,
+                                                          e.kept_worker.p, e.firm_diag.p, psi, out, partial);
+  CK_LAUNCH();
+}
+
 struct BlockOutcome {
   std::vector<int> iters;
   std::vector<double> reduced, complete;
@@ -639,14 +692,12 @@ template <int K>
 BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOptions& o, SolveTimings& tm) {
   Launch L{grid_blocks(), e.stream};
   BlockOutcome out;
-  // hybrid RHS and its column sums
-  k_hybrid_rhs<K><<<L.grid, THREADS, 0, L.s>>>(e.F, e.kept, e.firm_ptr.p, e.firm_cells.p, e.cell_worker.p,
-                                                e.cell_scale.p, e.kept_worker.p, w.bW.p, w.bF.p, w.b.p, e.partial.p);
+  // hybrid RHS (Schur reduction of the worker block) and its column sums
+  firm_gather<K, 1, 1>(e, w, L, e.cell_scale.p, w.bW.p, nullptr, 0.0, w.bF.p, w.bW.p, nullptr, w.b.p, e.partial.p);
   k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 2 * K, w.tot.p);
   k_pcg_init_state<K><<<1, 128, 0, L.s>>>(w.tot.p, ncols, o.pcg_tolerance, double(e.n), w.s);
   pcg_restart<K>(e, w, L, true);
-  ensure_graph<K>(e, w, L);
-  tm.kernel_launches += 6;
+  tm.kernel_launches += 9;
 
   const double gate = std::max(10.0 * o.pcg_tolerance, 1e-11);
   double tol = o.pcg_tolerance;
@@ -654,17 +705,15 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
   std::vector<int> h_it(K), h_active(K);
   int total_iters = 0;
   for (int ladder = 0;; ++ladder) {
-    for (;;) {
-      CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
-      CK(cudaStreamSynchronize(L.s));
-      if (*e.h_nactive == 0) break;
-      if (total_iters >= int(o.maximum_iterations))
-        fail(PCG_MAX_ITERATIONS, "pcg", "blocked PCG reached the iteration limit " + std::to_string(o.maximum_iterations));
-      CK(cudaGraphLaunch(w.graph, L.s));
-      total_iters += w.graph_iters;
-      tm.kernel_launches += size_t(w.graph_iters) * (e.preconditioner == 2 ? 6 + e.mg->launches_per_apply() : 5);
-      tm.spmm_launches += w.graph_iters;
-    }
+    int budget = int(o.maximum_iterations) - total_iters;
+    if (budget <= 0)
+      fail(PCG_MAX_ITERATIONS, "pcg", "blocked PCG reached the iteration limit " + std::to_string(o.maximum_iterations));
+    int done = pcg_run<K>(e, w, L, budget);
+    tm.kernel_launches += 1;
+    tm.spmm_launches += 1;
+    total_iters = done;
+    if (*e.h_nactive != 0)
+      fail(PCG_MAX_ITERATIONS, "pcg", "blocked PCG reached the iteration limit " + std::to_string(o.maximum_iterations));
     int bd = 0;
     CK(cudaMemcpyAsync(&bd, w.s.breakdown, sizeof(int), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
@@ -677,11 +726,10 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
     double* pf = e.partial.p + size_t(L.grid) * 2 * K;
     k_residual_workers<K><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, e.cell_firm.p, e.cell_weight.p,
                                                        e.worker_diag.p, w.alpha.p, w.x.p, w.bW.p, pw);
-    k_residual_firms<K><<<L.grid, THREADS, 0, L.s>>>(e.F, e.firm_ptr.p, e.firm_cells.p, e.cell_worker.p,
-                                                     e.cell_weight.p, e.firm_diag.p, w.alpha.p, w.x.p, w.bF.p, pf);
+    firm_gather<K, 2, 2>(e, w, L, e.cell_weight.p, w.alpha.p, nullptr, 0.0, w.bF.p, nullptr, w.x.p, nullptr, pf);
     k_finish<<<1, 1024, 0, L.s>>>(pw, L.grid, 2 * K, w.tot.p);
     k_finish<<<1, 1024, 0, L.s>>>(pf, L.grid, 2 * K, w.tot.p + 2 * K);
-    tm.kernel_launches += 5;
+    tm.kernel_launches += 6;
     std::vector<double> tot(4 * K);
     CK(cudaMemcpyAsync(tot.data(), w.tot.p, 4 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaMemcpyAsync(h_rr.data(), w.s.rr, K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
@@ -746,9 +794,8 @@ void run_leverage(DeviceEngine& e, const SolveOptions& o, SolveResult& res, uint
     k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p, key,
                                                      TAG_LEVERAGE, first, ncols, w.unit_atoms.p, w.cell_val.p);
     k_gather<K><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, w.cell_val.p, w.bW.p);
-    k_gather<K><<<L.grid, THREADS, 0, L.s>>>(e.F, e.firm_ptr.p, e.firm_cells.p, w.cell_val.p, w.bF.p);
-    CK_LAUNCH();
-    res.timings.kernel_launches += 3;
+    firm_gather<K, 0, 0>(e, w, L, nullptr, w.cell_val.p, nullptr, 0.0, nullptr, nullptr, nullptr, w.bF.p, nullptr);
+    res.timings.kernel_launches += 4;
     BlockOutcome bo = solve_block<K>(e, w, ncols, o, res.timings);
     k_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.G, ncols, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
                                               e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.moments.p);
@@ -779,8 +826,7 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res) {
     CK(cudaMemcpyAsync(tot.data(), w.tot.p, 2 * H * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     k_target_scores<K><<<L.grid, THREADS, 0, L.s>>>(e.W, 0, e.worker_ptr.p, nullptr, w.dir.p, e.cell_target.p, invT,
                                                     w.tot.p, w.bW.p);
-    k_target_scores<K><<<L.grid, THREADS, 0, L.s>>>(e.F, 1, e.firm_ptr.p, e.firm_cells.p, w.dir.p, e.cell_target.p,
-                                                    invT, w.tot.p, w.bF.p);
+    firm_gather<K, 3, 0>(e, w, L, e.cell_target.p, w.dir.p, w.tot.p, invT, nullptr, nullptr, nullptr, w.bF.p, nullptr);
     // balance repair (reference `balance_score_with_interrupt`, engine.rs:2812-2846):
     // the last worker / firm entry becomes minus the sum of the others
     k_colsum<K><<<L.grid, THREADS, 0, L.s>>>(e.W - 1, w.bW.p, e.partial.p);
@@ -855,7 +901,7 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
   {
     BlockWork& w = get_work<1>(e);
     k_gather<1><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, e.cell_outcome.p, w.bW.p);
-    k_gather<1><<<L.grid, THREADS, 0, L.s>>>(e.F, e.firm_ptr.p, e.firm_cells.p, e.cell_outcome.p, w.bF.p);
+    firm_gather<1, 0, 0>(e, w, L, nullptr, e.cell_outcome.p, nullptr, 0.0, nullptr, nullptr, nullptr, w.bF.p, nullptr);
     BlockOutcome bo = solve_block<1>(e, w, 1, o, res.timings);
     res.receipts.push_back(RhsReceipt{1, 1, -1, uint32_t(bo.iters[0]), uint32_t(bo.zero[0]), bo.reduced[0], bo.complete[0]});
     k_fit_cells<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p, e.cell_target.p,
@@ -992,38 +1038,70 @@ SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& pl
 namespace {
 
 template <int K>
+__global__ void k_fill_pattern(uint32_t n, double* __restrict__ b) {
+  size_t total = size_t(n) * K;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x)
+    b[t] = sin(0.37 * double(t / K) + 1.3 * double(t % K));
+}
+
+template <int K>
 void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, double* bytes) {
   BlockWork& w = get_work<K>(e);
   Launch L{grid_blocks(), e.stream};
-  size_t vec = size_t(e.n) * K * sizeof(double);
-  CK(cudaMemsetAsync(w.p.p, 0, vec, L.s));
-  CK(cudaMemsetAsync(w.x.p, 0, vec, L.s));
-  CK(cudaMemsetAsync(w.r.p, 0, vec, L.s));
-  CK(cudaMemsetAsync(w.q.p, 0, vec, L.s));
-  CK(cudaMemsetAsync(w.s.alpha, 0, K * sizeof(double), L.s));
   DBuf<char> flush(size_t(256) << 20);  // larger than the 126 MB L2
-  double nnz = double(e.L_col.n), n = double(e.n);
+  double nnz = double(e.L_col.n), n = double(e.n), nseg = double(e.lap_seg.count);
   PhiloxKey key = philox_key(8675309);
+  const int iters = 20;
   switch (kernel) {
-    case 1: *bytes = nnz * 12 + n * 8 + (n + 1) * 4 + 2 * n * K * 8; break;
-    case 2: *bytes = n * 8 + 7 * n * K * 8; break;  // dinv; read p q x r; write x r z
+    case 1:
+      // persistent PCG, per launch of `iters` iterations: matrix + segment
+      // tables once per iteration, p read, segment products written and read,
+      // x and r read and written, p read and written
+      *bytes = iters * (nnz * 12 + nseg * 12 + n * (4 + 4 + 8 + 8 + 8) + n * K * 8.0 * 9 + 2 * nseg * K * 8.0);
+      break;
     case 3: *bytes = double(e.G) * (8 + 8 + K * 8) + double(e.C) * (4 + K * 8); break;
     case 4: *bytes = double(e.G) * (4 + 8 + K * 8 + 5 * 8 * 2) + double(e.G) * 2 * K * 8 + double(e.C) * 8; break;
     default: fail(INVALID_INPUT, "benchmark", "unknown kernel id");
   }
   float total = 0.0f;
   for (int i = 0; i < launches; ++i) {
+    if (kernel == 1) {
+      // a fresh, never-converging block (tolerance 0) so every launch runs `iters` iterations
+      k_fill_pattern<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p);
+      k_colsum_abs<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p, e.partial.p);
+      k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 2 * K, w.tot.p);
+      k_pcg_init_state<K><<<1, 128, 0, L.s>>>(w.tot.p, K, 0.0, double(e.n), w.s);
+      pcg_restart<K>(e, w, L, true);
+    }
     CK(cudaMemsetAsync(flush.p, i & 0xff, flush.bytes(), L.s));
     CK(cudaEventRecord(e.ev0, L.s));
     switch (kernel) {
-      case 1:
-        k_spmm_dot<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_ptr.p, e.L_col.p, e.L_val.p, e.L_diag.p, w.p.p, w.q.p,
-                                                   e.partial.p);
+      case 1: {
+        PersistentPcg<K> a;
+        a.n = e.n;
+        a.ptr = e.L_ptr.p;
+        a.col = e.L_col.p;
+        a.val = e.L_val.p;
+        a.diag = e.L_diag.p;
+        a.dinv = e.L_dinv.p;
+        a.nseg = e.lap_seg.count;
+        a.seg_row = e.lap_seg.row.p;
+        a.seg_begin = e.lap_seg.begin.p;
+        a.seg_end = e.lap_seg.end.p;
+        a.row_first = e.lap_seg.row_first.p;
+        a.seg_buf = w.seg_buf.p;
+        a.x = w.x.p;
+        a.r = w.r.p;
+        a.p = w.p.p;
+        a.partial_a = e.partial.p;
+        a.partial_b = e.partial.p + size_t(e.coop_blocks) * K;
+        a.s = w.s;
+        a.max_iters = iters;
+        void* args[] = {&a};
+        CK(cudaLaunchCooperativeKernel((const void*)k_pcg_persistent<K>, dim3(e.coop_blocks), dim3(PERSIST_THREADS),
+                                       args, 0, L.s));
         break;
-      case 2:
-        k_update_jacobi<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_dinv.p, w.p.p, w.q.p, w.x.p, w.r.p, w.z.p, w.s.alpha,
-                                                        e.partial.p);
-        break;
+      }
       case 3:
         k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p, key,
                                                          TAG_LEVERAGE, 0, K, w.unit_atoms.p, w.cell_val.p);
@@ -1041,6 +1119,13 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
   }
   CK_LAUNCH();
   *ms = double(total) / launches;
+  if (kernel == 1) {
+    // report the iterations actually executed (a curvature breakdown would stop early)
+    std::vector<int> it(K);
+    CK(cudaMemcpy(it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost));
+    int mx = *std::max_element(it.begin(), it.end());
+    if (mx != iters) *bytes *= double(mx) / iters;
+  }
 }
 
 }  // namespace

@@ -79,9 +79,9 @@ SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& pl
                          bool want_unit_detail);
 
 // Time `launches` standalone launches of one hot kernel on the prepared
-// problem with CUDA events (L2 flushed before each launch).  kernel: 1 SpMM
-// with the step-length dot, 2 PCG update with the Jacobi apply, 3 leverage
-// Counter-V1 atoms with the per-cell sums, 4 leverage moments.  Returns the
+// problem with CUDA events (L2 flushed before each launch).  kernel: 1 the
+// persistent blocked PCG (20 iterations), 3 leverage Counter-V1 atoms with
+// the per-cell sums, 4 leverage moments.  Returns the
 // mean device milliseconds per launch and the algorithmic bytes per launch.
 void device_kernel_benchmark(DeviceEngine& e, int kernel, int block_columns, int launches, double* ms_per_launch,
                              double* bytes_per_launch);

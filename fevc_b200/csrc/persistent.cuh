@@ -1,0 +1,362 @@
+// Load-balanced row segments and the persistent blocked PCG kernel.
+//
+// Firm sizes are heavy-tailed (Pareto), so a few Laplacian rows and a few
+// firm->cell lists are thousands of entries long.  Every such CSR is cut into
+// segments of at most SEG items; one thread group reduces one segment and
+// multi-segment rows are finished in a second, row-parallel step in a fixed
+// order (deterministic, no atomics).
+//
+// The PCG loop for a block of K right-hand sides runs as ONE cooperative
+// kernel per solve: three grid barriers per iteration (after the SpMM, after
+// the x/r update, after the direction update), per-column step lengths and
+// convergence flags held redundantly in every block's shared memory (each
+// block reduces the same per-block partials in the same order, so all blocks
+// agree bit for bit and leave the loop together).
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "kernels.cuh"
+
+namespace fevcb {
+
+constexpr uint32_t SEG = 32;   // items per segment
+constexpr int PERSIST_THREADS = 1024;
+
+// Row segments of a CSR: segment s covers items [begin[s], end[s]) of row
+// row[s]; the segments of a row are consecutive and rows appear in order.
+struct Segments {
+  uint32_t count = 0;
+  DBuf<uint32_t> row, begin, end;
+  DBuf<uint32_t> row_first;  // first segment of each row (rows + 1 entries)
+};
+
+template <int K, int M>
+__device__ __forceinline__ void block_reduce_cols_big(double (&v)[M][Cols<K>::CPT], double* partial,
+                                                      double (*sm)[M][K]) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+#pragma unroll
+  for (int m = 0; m < M; ++m)
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      double x = v[m][c];
+#pragma unroll
+      for (int off = TPR; off < 32; off <<= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+      v[m][c] = x;
+    }
+  if (lane < TPR) {
+#pragma unroll
+    for (int m = 0; m < M; ++m)
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) sm[warp][m][lane * CPT + c] = v[m][c];
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < M * K; t += blockDim.x) {
+    int m = t / K, c = t % K;
+    double s = 0.0;
+    for (int w = 0; w < warps; ++w) s += sm[w][m][c];
+    partial[size_t(blockIdx.x) * M * K + t] = s;
+  }
+  __syncthreads();
+}
+
+// Every block sums the per-block partials [blocks][M][K] in the same order;
+// result into out[M*K] (shared).  Uses all threads: T/(M*K) lanes per output.
+template <int M, int K>
+__device__ __forceinline__ void redundant_finish(const double* __restrict__ partial, int blocks, double* out,
+                                                 double* scratch /* blockDim doubles */) {
+  constexpr int W = M * K;
+  const int per = blockDim.x / W;  // >= 1 when blockDim >= W
+  const int o = threadIdx.x % W, g = threadIdx.x / W;
+  double acc = 0.0;
+  if (g < per)
+    for (int b = g; b < blocks; b += per) acc += __ldcg(partial + size_t(b) * W + o);
+  scratch[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x < W) {
+    double s = 0.0;
+    for (int k = 0; k < per; ++k) s += scratch[k * W + threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
+template <int K>
+struct PersistentPcg {
+  uint32_t n;
+  const uint32_t* ptr;
+  const uint32_t* col;
+  const double* val;
+  const double* diag;
+  const double* dinv;
+  uint32_t nseg;
+  const uint32_t* seg_row;
+  const uint32_t* seg_begin;
+  const uint32_t* seg_end;
+  const uint32_t* row_first;  // first segment of each row
+  double* seg_buf;            // [nseg][K] segment partial products
+  double* x;
+  double* r;
+  double* p;
+  double* partial_a;  // [grid][1][K]
+  double* partial_b;  // [grid][2][K]
+  PcgState s;
+  int max_iters;
+};
+
+template <int K>
+__global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(PersistentPcg<K> a) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  __shared__ double s_alpha[K], s_beta[K], s_rz[K], s_tol2[K];
+  __shared__ int s_active[K], s_iters[K];
+  __shared__ int s_nactive, s_done;
+  __shared__ double s_fin[2 * K];
+  __shared__ double s_scratch[PERSIST_THREADS];
+  __shared__ double s_red[PERSIST_THREADS / 32][2][K];
+
+  for (int j = threadIdx.x; j < K; j += blockDim.x) {
+    s_rz[j] = a.s.rz[j];
+    s_tol2[j] = a.s.tol2[j];
+    s_active[j] = a.s.active[j];
+    s_iters[j] = a.s.iters[j];
+  }
+  if (threadIdx.x == 0) s_done = 0;
+  __syncthreads();
+
+  const int c0 = int(threadIdx.x % TPR) * CPT;
+  const size_t gid = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) / TPR;
+  const size_t ngroups = size_t(gridDim.x) * blockDim.x / TPR;
+  int it = 0;
+  for (; it < a.max_iters; ++it) {
+    // ---- A: segment products  seg_buf[s] = sum_e a_e p[col_e]  and  p.(L p)
+    double v[1][CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) v[0][c] = 0.0;
+    for (size_t sg = gid; sg < a.nseg; sg += ngroups) {
+      uint32_t row = a.seg_row[sg], b = a.seg_begin[sg], e = a.seg_end[sg];
+      double acc[CPT];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
+      uint32_t i = b;
+      for (; i + 2 <= e; i += 2) {
+        uint32_t j0 = __ldg(a.col + i), j1 = __ldg(a.col + i + 1);
+        double a0 = __ldg(a.val + i), a1 = __ldg(a.val + i + 1);
+        const double* x0 = a.p + size_t(j0) * K + c0;
+        const double* x1 = a.p + size_t(j1) * K + c0;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] += a0 * x0[c] + a1 * x1[c];
+      }
+      if (i < e) {
+        uint32_t j0 = __ldg(a.col + i);
+        double a0 = __ldg(a.val + i);
+        const double* x0 = a.p + size_t(j0) * K + c0;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] += a0 * x0[c];
+      }
+      const double* pr = a.p + size_t(row) * K + c0;
+      bool first = (b == a.ptr[row]);
+      double d = first ? a.diag[row] : 0.0;
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        a.seg_buf[sg * K + c0 + c] = acc[c];
+        v[0][c] += pr[c] * (d * pr[c] - acc[c]);
+      }
+    }
+    block_reduce_cols_big<K, 1>(v, a.partial_a, (double(*)[1][K])s_red);
+    grid.sync();
+
+    // ---- step lengths
+    redundant_finish<1, K>(a.partial_a, gridDim.x, s_fin, s_scratch);
+    for (int j = threadIdx.x; j < K; j += blockDim.x) {
+      double pq = s_fin[j], al = 0.0;
+      if (s_active[j]) {
+        if (!(pq > 0.0) || !isfinite(pq)) {
+          if (blockIdx.x == 0) atomicCAS(a.s.breakdown, -1, j);
+          s_active[j] = 0;
+        } else {
+          al = s_rz[j] / pq;
+        }
+      }
+      s_alpha[j] = al;
+    }
+    __syncthreads();
+
+    // ---- B: q = diag p - sum(segments); x += alpha p; r -= alpha q; z = dinv r
+    double w[2][CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) w[0][c] = w[1][c] = 0.0;
+    for (size_t row = gid; row < a.n; row += ngroups) {
+      uint32_t s0 = a.row_first[row], s1 = a.row_first[row + 1];
+      double dr = a.diag[row], di = a.dinv[row];
+      size_t o = row * K + c0;
+      double q[CPT];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) q[c] = dr * a.p[o + c];
+      for (uint32_t sg = s0; sg < s1; ++sg)
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) q[c] -= a.seg_buf[size_t(sg) * K + c0 + c];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        double al = s_alpha[c0 + c];
+        a.x[o + c] += al * a.p[o + c];
+        double ri = a.r[o + c] - al * q[c];
+        a.r[o + c] = ri;
+        w[0][c] += ri * (di * ri);
+        w[1][c] += ri * ri;
+      }
+    }
+    block_reduce_cols_big<K, 2>(w, a.partial_b, (double(*)[2][K])s_red);
+    grid.sync();
+
+    // ---- convergence and direction coefficients
+    redundant_finish<2, K>(a.partial_b, gridDim.x, s_fin, s_scratch);
+    if (threadIdx.x == 0) s_nactive = 0;
+    __syncthreads();
+    for (int j = threadIdx.x; j < K; j += blockDim.x) {
+      double rz = s_fin[j], rr = s_fin[K + j], be = 0.0;
+      if (s_active[j]) {
+        s_iters[j] += 1;
+        if (rr <= s_tol2[j]) {
+          s_active[j] = 0;
+        } else {
+          be = rz / s_rz[j];
+          s_rz[j] = rz;
+          atomicAdd(&s_nactive, 1);
+        }
+        if (blockIdx.x == 0) a.s.rr[j] = rr;
+      }
+      s_beta[j] = be;
+    }
+    __syncthreads();
+    if (s_nactive == 0) {
+      ++it;
+      break;
+    }
+    // ---- C: p = dinv r + beta p
+    for (size_t row = gid; row < a.n; row += ngroups) {
+      double di = a.dinv[row];
+      size_t o = row * K + c0;
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) a.p[o + c] = di * a.r[o + c] + s_beta[c0 + c] * a.p[o + c];
+    }
+    grid.sync();
+  }
+  if (blockIdx.x == 0) {
+    for (int j = threadIdx.x; j < K; j += blockDim.x) {
+      a.s.rz[j] = s_rz[j];
+      a.s.active[j] = s_active[j];
+      a.s.iters[j] = s_iters[j];
+    }
+    if (threadIdx.x == 0) *a.s.nactive = s_nactive;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Segmented firm-side gathers over the firm->cell lists.
+//   op 0: sum of cell values                      (right-hand side of the firm block)
+//   op 1: sum of cell_scale[c] * bW[w(c)]          (Schur reduction of the worker block)
+//   op 2: sum of cell_weight[c] * alpha[w(c)]      (complete residual, firm rows)
+//   op 3: target firm scores: odd columns q=2j+1 sum d[c][j] - share_c * total[j]
+template <int K, int OP>
+__global__ void k_seg_firm(uint32_t nseg, const uint32_t* __restrict__ seg_begin, const uint32_t* __restrict__ seg_end,
+                           const uint32_t* __restrict__ firm_cells, const uint32_t* __restrict__ cell_worker,
+                           const double* __restrict__ coef, const double* __restrict__ src, const double* __restrict__ total,
+                           double inv_total, double* __restrict__ seg_out) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR, H = K / 2;
+  size_t N = size_t(nseg) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < N; t += stride) {
+    size_t sg = t / TPR;
+    int c0 = int(t % TPR) * CPT;
+    double acc[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
+    for (uint32_t i = seg_begin[sg]; i < seg_end[sg]; ++i) {
+      uint32_t cell = firm_cells[i];
+      if (OP == 0) {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] += src[size_t(cell) * K + c0 + c];
+      } else if (OP == 1 || OP == 2) {
+        double s = coef[cell];
+        if (s != 0.0) {
+          size_t wb = size_t(cell_worker[cell]) * K + c0;
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) acc[c] += s * src[wb + c];
+        }
+      } else {
+        double share = coef[cell] * inv_total;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          int q = c0 + c;
+          if (q & 1) acc[c] += src[size_t(cell) * H + (q >> 1)] - share * total[q >> 1];
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) seg_out[sg * K + c0 + c] = acc[c];
+  }
+}
+
+// Finish a segmented firm gather: rows f < F sum their segments in order.
+//   mode 0: out[f] = sum                              (plain)
+//   mode 1: hybrid RHS  b[f] = bF[f] - sum; kept rows b[F+k] = -bW[kept_worker[k]];
+//           partial (sum b, sum b^2)
+//   mode 2: residual    r = bF - d_f psi_f - sum;    partial (|r|^2, |bF|^2)
+template <int K, int MODE>
+__global__ void k_seg_firm_finish(uint32_t F, uint32_t kept, const uint32_t* __restrict__ row_first,
+                                  const double* __restrict__ seg_out, const double* __restrict__ bF,
+                                  const double* __restrict__ bW, const uint32_t* __restrict__ kept_worker,
+                                  const double* __restrict__ firm_diag, const double* __restrict__ psi,
+                                  double* __restrict__ out, double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  double v[2][CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
+  size_t rows = size_t(F) + (MODE == 1 ? kept : 0);
+  size_t N = rows * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < N; base += stride) {
+    size_t t = base + threadIdx.x;
+    if (t < N) {
+      size_t f = t / TPR;
+      int c0 = int(t % TPR) * CPT;
+      double acc[CPT];
+      if (f < F) {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
+        for (uint32_t sg = row_first[f]; sg < row_first[f + 1]; ++sg)
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) acc[c] += seg_out[size_t(sg) * K + c0 + c];
+        if (MODE == 1) {
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) acc[c] = bF[f * K + c0 + c] - acc[c];
+        } else if (MODE == 2) {
+          double d = firm_diag[f];
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) {
+            double b = bF[f * K + c0 + c];
+            double rres = b - d * psi[f * K + c0 + c] - acc[c];
+            v[0][c] += rres * rres;
+            v[1][c] += b * b;
+          }
+        }
+      } else {
+        size_t wb = size_t(kept_worker[f - F]) * K + c0;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] = -bW[wb + c];
+      }
+      if (MODE != 2) {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          out[f * K + c0 + c] = acc[c];
+          v[0][c] += acc[c];
+          v[1][c] += acc[c] * acc[c];
+        }
+      }
+    }
+  }
+  if (MODE != 0) block_reduce_cols<K, 2>(v, partial);
+}
+
+}  // namespace fevcb

@@ -474,8 +474,8 @@ typedef struct FevcbProblemViewV1 {
 int32_t fevcb_engine_problem_view_v1(uint64_t generation, FevcbProblemViewV1 *output, uint32_t output_capacity_bytes);
 
 /* Time standalone launches of one hot kernel of a solved generation with CUDA
- * events, L2 flushed before each launch.  kernel: 1 SpMM + step-length dot,
- * 2 PCG update + Jacobi apply, 3 leverage atoms + cell sums, 4 leverage moments.
+ * events, L2 flushed before each launch.  kernel: 1 persistent blocked PCG
+ * (20 iterations per launch), 3 leverage atoms + cell sums, 4 leverage moments.
  * Outputs mean milliseconds per launch and algorithmic bytes per launch. */
 int32_t fevcb_engine_kernel_benchmark_v1(uint64_t generation, uint32_t kernel, uint32_t block_columns,
                                          uint32_t launches, double *ms_per_launch, double *bytes_per_launch);
