@@ -255,7 +255,7 @@ def main():
     value = world * rhs * args.steps / (ms / 1000.0)
 
     # roofline: the persistent blocked PCG kernel, standalone launches with L2 flushed
-    block = args.block or 32
+    block = args.block or 64
     spmm_ms, spmm_bytes = e.kernel_benchmark(1, block, 10)
     peaks = {}
     try:

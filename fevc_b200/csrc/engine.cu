@@ -1024,7 +1024,7 @@ SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& pl
     fail(UNSUPPORTED_FEATURE, "centering", "Corrected centering is not provided by the device engine");
   SolveResult res;
   int K = o.block_columns;
-  if (K == 0) K = 32;
+  if (K == 0) K = 64;
   switch (K) {
     case 8: run_jla<8>(e, p, plan, o, res, want_unit_detail); break;
     case 16: run_jla<16>(e, p, plan, o, res, want_unit_detail); break;
