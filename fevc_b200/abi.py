@@ -224,6 +224,8 @@ SIGNATURES = {
     "fevcb_engine_problem_view_v1": (i32, [u64, C.c_void_p, u32]),
     "fevcb_engine_kernel_benchmark_v1": (i32, [u64, u32, u32, u32, C.POINTER(f64), C.POINTER(f64)]),
     "fevcb_counter_atoms_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64, C.POINTER(i64)]),
+    "fevcb_counter_atoms_noalloc_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64,
+                                             C.POINTER(i64)]),
 }
 
 def capability_signature_v3(req: SolveRequestV4, controls_count: int) -> int:
@@ -402,11 +404,15 @@ class Engine:
         return arrs
 
 
-def device_atoms(lib: C.CDLL, seed: int, tag: int, first_probe: int, columns: int, entity, trials) -> np.ndarray:
+def device_atoms(lib: C.CDLL, seed: int, tag: int, first_probe: int, columns: int, entity, trials,
+                 *, no_alloc: bool = False) -> np.ndarray:
+    """Counter-V1 atoms computed on the device (``no_alloc`` selects the
+    entry point that stages through the library's fixed device array)."""
     entity = np.ascontiguousarray(entity, dtype=np.uint64)
     trials = np.ascontiguousarray(trials, dtype=np.uint64)
     out = np.zeros(entity.size * columns, np.int64)
-    st = lib.fevcb_counter_atoms_v1(seed, tag, first_probe, columns, entity.ctypes.data_as(C.POINTER(u64)),
+    fn = lib.fevcb_counter_atoms_noalloc_v1 if no_alloc else lib.fevcb_counter_atoms_v1
+    st = fn(seed, tag, first_probe, columns, entity.ctypes.data_as(C.POINTER(u64)),
                                     trials.ctypes.data_as(C.POINTER(u64)), entity.size,
                                     out.ctypes.data_as(C.POINTER(i64)))
     if st != 0:

@@ -975,3 +975,13 @@ int32_t fevcb_counter_atoms_v1(uint64_t seed, uint64_t domain_tag, uint64_t firs
 }
 
 }  // extern "C"
+
+extern "C" int32_t fevcb_counter_atoms_noalloc_v1(uint64_t seed, uint64_t domain_tag, uint64_t first_probe,
+                                                  uint32_t columns, const uint64_t* entity, const uint64_t* trials,
+                                                  uint64_t count, int64_t* out) {
+  return status([&] {
+    if (!entity || !trials || !out || columns == 0 || count == 0)
+      fail(INVALID_INPUT, "counter_rng", "semantic atom request has incompatible dimensions");
+    device_atoms_noalloc(seed, domain_tag, first_probe, columns, entity, trials, count, out);
+  });
+}

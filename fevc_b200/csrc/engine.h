@@ -90,6 +90,10 @@ void device_kernel_benchmark(DeviceEngine& e, int kernel, int block_columns, int
 void device_atoms(uint64_t seed, uint64_t tag, uint64_t first_probe, uint32_t columns, const uint64_t* entity,
                   const uint64_t* trials, uint64_t count, int64_t* out);
 
+// The same atoms staged through a fixed file-scope device array (no allocation).
+void device_atoms_noalloc(uint64_t seed, uint64_t tag, uint64_t first_probe, uint32_t columns, const uint64_t* entity,
+                          const uint64_t* trials, uint64_t count, int64_t* out);
+
 int device_count();
 void set_device_stream(void* stream);
 void* device_stream();

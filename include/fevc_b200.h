@@ -484,6 +484,20 @@ int32_t fevcb_engine_kernel_benchmark_v1(uint64_t generation, uint32_t kernel, u
 int32_t fevcb_counter_atoms_v1(uint64_t seed, uint64_t domain_tag, uint64_t first_probe, uint32_t columns,
                                const uint64_t *entity, const uint64_t *trials, uint64_t count, int64_t *out);
 
+/* Same result as fevcb_counter_atoms_v1, for callers that cannot allocate
+ * device memory (no counterpart in the reference): a process whose own
+ * framework already holds nearly all device memory, or one that fixes its
+ * device-memory plan at start-up.  Inputs and outputs stay host arrays; the
+ * call stages them in one file-scope 8 MiB device array instead of allocating,
+ * so it calls no cudaMalloc/cudaFree.  Requests needing more than 8 MiB
+ * (2 x count x 8 bytes + count x columns x 8 bytes, each part rounded up to
+ * 256 bytes) are refused with RESOURCE_LIMIT (40).  The first call on a device
+ * looks up the array's device address; make that first call before any stream
+ * capture.  Every call shares the array: calls that overlap on the GPU race
+ * and must be serialised by the caller. */
+int32_t fevcb_counter_atoms_noalloc_v1(uint64_t seed, uint64_t domain_tag, uint64_t first_probe, uint32_t columns,
+                                       const uint64_t *entity, const uint64_t *trials, uint64_t count, int64_t *out);
+
 #ifdef __cplusplus
 }
 #endif
