@@ -310,14 +310,16 @@ class Engine:
             req = PrepareRequestV1(1, C.sizeof(PrepareRequestV1), rows, int(cleanup), 0)
             self.check(self.lib.vckss_rust_engine_prepare_v1(C.byref(req), C.byref(c1), C.byref(handle), 8))
         else:
+            c1.struct_size = C.sizeof(ColumnsV3)
             ctl_array = (dptr * max(1, len(controls)))(*[_d(c) for c in controls])
             self._keep.append(ctl_array)
             c2 = ColumnsV2(c1, C.cast(ctl_array, C.POINTER(dptr)) if controls else None, len(controls), 0)
             c3 = ColumnsV3(c2, None, 0, 0)
-            v2 = PrepareRequestV2(1, C.sizeof(PrepareRequestV4), rows, int(cleanup), 0, 64 << 30, 0)
+            v2 = PrepareRequestV2(1, C.sizeof(PrepareRequestInterruptV3), rows, int(cleanup), 0, 1 << 40,
+                                  rows * (6 + len(controls)) * 8)
             v3 = PrepareRequestV3(v2, deletion_mode, len(controls), 0)
             v4 = PrepareRequestV4(v3, int(implicit_match), 0)
-            req = PrepareRequestInterruptV3(v4, InterruptPoll(0), None, 4096, 0)
+            req = PrepareRequestInterruptV3(v4, InterruptPoll(0), None, 0, 0)
             self.check(self.lib.vckss_rust_engine_prepare_interrupt_v4(C.byref(req), C.byref(c3), C.byref(handle), 8))
         self.generation = handle.value
         return self.generation

@@ -41,9 +41,21 @@ int32_t status(F&& f) {
   }
 }
 
+// Caller interrupt callback (reference `CallbackInterrupt::new`,
+// ffi_engine.rs:1422-1461).  The device engine checkpoints between phases and
+// between right-hand-side blocks, each far more than `interval` items of
+// work, so every checkpoint polls the callback.
 struct Interrupt {
   VckssInterruptPollV1 poll = nullptr;
   void* ctx = nullptr;
+  Interrupt() = default;
+  Interrupt(VckssInterruptPollV1 p, void* c, uint32_t interval, uint32_t reserved, const char* label) : poll(p), ctx(c) {
+    if (reserved != 0) fail(ABI_MISMATCH, "engine_ffi", std::string("reserved interrupt ") + label + " fields must be zero");
+    if (!p && (c || interval != 0))
+      fail(INVALID_INPUT, "engine_interrupt", "a null interrupt callback requires null context and zero interval");
+    if (p && interval == 0)
+      fail(INVALID_INPUT, "engine_interrupt", "a nonnull interrupt callback requires a positive checkpoint interval");
+  }
   void check(const char* phase) const {
     if (poll && poll(ctx) != VCKSS_INTERRUPT_CONTINUE) fail(USER_BREAK, phase, "interrupted by the caller");
   }
@@ -96,9 +108,18 @@ void require_capacity(const void* p, uint64_t cap, const char* label) {
          std::string(label) + " capacity " + std::to_string(cap) + " is below " + std::to_string(sizeof(T)));
 }
 
+// Copy a caller struct after checking the size it reports (reference
+// `copy_request_struct` / `copy_sized_struct`, ffi_engine.rs:10815-10830):
+// requests carry struct_size at byte offset 4, descriptors at offset 0.
 template <class T>
-T read_struct(const T* p, const char* label) {
+T read_struct(const T* p, const char* label, size_t size_offset = 4) {
   if (!p) fail(INVALID_INPUT, "engine_ffi", std::string(label) + " pointer is null");
+  uint32_t reported = 0;
+  std::memcpy(&reported, reinterpret_cast<const char*>(p) + size_offset, 4);
+  if (reported < sizeof(T))
+    fail(ABI_MISMATCH, "engine_ffi",
+         std::string(label) + " size " + std::to_string(reported) + " is below required size " +
+             std::to_string(sizeof(T)));
   T v;
   std::memcpy(&v, p, sizeof(T));
   return v;
@@ -122,6 +143,7 @@ void clear_abandoned(uint32_t flag) {
 struct PrepareArgs {
   uint64_t rows;
   uint32_t cleanup;
+  bool explicit_memory = false;  // V2+ requests carry a memory budget that must be positive
   uint64_t memory_limit = 0, caller_copy = 0;
   uint32_t deletion_mode = VCKSS_DELETION_MATCH;
   uint32_t implicit_match = 0;
@@ -143,6 +165,21 @@ void prepare_common(const PrepareArgs& a, uint64_t* out, uint32_t cap) {
     fail(INVALID_INPUT, "engine_prepare", "unknown deletion mode");
   if (a.implicit_match && a.deletion_mode != VCKSS_DELETION_MATCH)
     fail(INVALID_INPUT, "session_prepare", "implicit-match preparation requires match deletion");
+  if (a.cleanup > 1) fail(INVALID_INPUT, "engine_prepare", "cleanup_abandoned must be zero or one");
+  // the budget must be positive (reference memory.rs:33); forecasting against it is not replicated
+  if (a.explicit_memory && a.memory_limit == 0)
+    fail(INVALID_INPUT, "memory_budget", "an explicit memory budget must be positive");
+  if (a.explicit_memory) {
+    // the declared caller copy must equal the binary64 columns handed over
+    // (reference vckss-plugin/src/session.rs:111-121, 218-232)
+    uint64_t columns = 6 + a.controls_count + (a.probe_order ? 1 : 0);
+    uint64_t expected = a.rows * columns * 8;
+    if (a.caller_copy != expected)
+      fail(INVALID_INPUT, "engine_memory",
+           "declared caller copy is " + std::to_string(a.caller_copy) + " bytes; " +
+               (columns == 6 ? std::string("six") : std::to_string(columns)) + " columns require " +
+               std::to_string(expected) + " bytes");
+  }
   {
     std::lock_guard<std::mutex> l(reg().mu);
     clear_abandoned(a.cleanup);
@@ -394,7 +431,7 @@ int32_t vckss_rust_engine_default_solve_request_interrupt_v1(VckssEngineSolveReq
     require_capacity<VckssEngineSolveRequestInterruptV1>(out, cap, "interrupt solve request");
     VckssEngineSolveRequestInterruptV1 q{};
     if (vckss_rust_engine_default_solve_request_v1(&q.options, sizeof(q.options)) != OK) fail(PANIC, "defaults", "V1");
-    q.checkpoint_interval = 4096;
+    q.options.struct_size = sizeof(q);
     std::memcpy(out, &q, sizeof(q));
   });
 }
@@ -404,7 +441,7 @@ int32_t vckss_rust_engine_default_solve_request_interrupt_v5(VckssEngineSolveReq
     require_capacity<VckssEngineSolveRequestInterruptV5>(out, cap, "interrupt V5 solve request");
     VckssEngineSolveRequestInterruptV5 q{};
     if (vckss_rust_engine_default_solve_request_v5(&q.options, sizeof(q.options)) != OK) fail(PANIC, "defaults", "V5");
-    q.checkpoint_interval = 4096;
+    q.options.v4.v3.v2.v1.struct_size = sizeof(q);
     std::memcpy(out, &q, sizeof(q));
   });
 }
@@ -415,7 +452,6 @@ int32_t vckss_rust_engine_default_prepare_request_v3(VckssEnginePrepareRequestV3
     VckssEnginePrepareRequestV3 q{};
     q.v2.abi_version = 1;
     q.v2.struct_size = sizeof(q);
-    q.v2.memory_limit_bytes = 4ull << 30;
     q.deletion_mode = VCKSS_DELETION_MATCH;
     std::memcpy(out, &q, sizeof(q));
   });
@@ -426,9 +462,7 @@ int32_t vckss_rust_engine_default_prepare_request_interrupt_v1(VckssEnginePrepar
     require_capacity<VckssEnginePrepareRequestInterruptV1>(out, cap, "interrupt prepare request");
     VckssEnginePrepareRequestInterruptV1 q{};
     q.options.abi_version = 1;
-    q.options.struct_size = sizeof(q.options);
-    q.options.memory_limit_bytes = 4ull << 30;
-    q.checkpoint_interval = 4096;
+    q.options.struct_size = sizeof(q);
     std::memcpy(out, &q, sizeof(q));
   });
 }
@@ -438,10 +472,8 @@ int32_t vckss_rust_engine_default_prepare_request_interrupt_v2(VckssEnginePrepar
     require_capacity<VckssEnginePrepareRequestInterruptV2>(out, cap, "V2 interrupt prepare request");
     VckssEnginePrepareRequestInterruptV2 q{};
     q.options.v2.abi_version = 1;
-    q.options.v2.struct_size = sizeof(q.options);
-    q.options.v2.memory_limit_bytes = 4ull << 30;
+    q.options.v2.struct_size = sizeof(q);
     q.options.deletion_mode = VCKSS_DELETION_MATCH;
-    q.checkpoint_interval = 4096;
     std::memcpy(out, &q, sizeof(q));
   });
 }
@@ -451,10 +483,8 @@ int32_t vckss_rust_engine_default_prepare_request_interrupt_v3(VckssEnginePrepar
     require_capacity<VckssEnginePrepareRequestInterruptV3>(out, cap, "V3 interrupt prepare request");
     VckssEnginePrepareRequestInterruptV3 q{};
     q.options.v3.v2.abi_version = 1;
-    q.options.v3.v2.struct_size = sizeof(q.options);
-    q.options.v3.v2.memory_limit_bytes = 4ull << 30;
+    q.options.v3.v2.struct_size = sizeof(q);
     q.options.v3.deletion_mode = VCKSS_DELETION_MATCH;
-    q.checkpoint_interval = 4096;
     std::memcpy(out, &q, sizeof(q));
   });
 }
@@ -463,7 +493,7 @@ int32_t vckss_rust_engine_prepare_v1(const VckssEnginePrepareRequestV1* request,
                                      uint64_t* out, uint32_t cap) {
   return status([&] {
     auto q = read_struct(request, "engine prepare request");
-    auto c = read_struct(columns, "engine column descriptor");
+    auto c = read_struct(columns, "engine column descriptor", 0);
     require_abi(q.abi_version);
     if (q.reserved != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved preparation fields must be zero");
     PrepareArgs a{q.rows, q.cleanup_abandoned};
@@ -476,10 +506,10 @@ int32_t vckss_rust_engine_prepare_v2(const VckssEnginePrepareRequestV2* request,
                                      uint64_t* out, uint32_t cap) {
   return status([&] {
     auto q = read_struct(request, "V2 engine prepare request");
-    auto c = read_struct(columns, "engine column descriptor");
+    auto c = read_struct(columns, "engine column descriptor", 0);
     require_abi(q.abi_version);
     if (q.reserved != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved preparation fields must be zero");
-    PrepareArgs a{q.rows, q.cleanup_abandoned, q.memory_limit_bytes, q.caller_copy_bytes};
+    PrepareArgs a{q.rows, q.cleanup_abandoned, true, q.memory_limit_bytes, q.caller_copy_bytes};
     a.v1 = &c;
     prepare_common(a, out, cap);
   });
@@ -492,7 +522,7 @@ static void prepare_v3_impl(const VckssEnginePrepareRequestV3& q, const VckssEng
     fail(ABI_MISMATCH, "engine_ffi", "reserved V2 column fields must be zero");
   if (q.controls_count != c.controls_count)
     fail(INVALID_INPUT, "engine_prepare", "request and descriptor control counts disagree");
-  PrepareArgs a{q.v2.rows, q.v2.cleanup_abandoned, q.v2.memory_limit_bytes, q.v2.caller_copy_bytes};
+  PrepareArgs a{q.v2.rows, q.v2.cleanup_abandoned, true, q.v2.memory_limit_bytes, q.v2.caller_copy_bytes};
   a.deletion_mode = q.deletion_mode;
   a.implicit_match = implicit;
   a.v1 = &c.v1;
@@ -507,7 +537,7 @@ int32_t vckss_rust_engine_prepare_v3(const VckssEnginePrepareRequestV3* request,
                                      uint64_t* out, uint32_t cap) {
   return status([&] {
     auto q = read_struct(request, "V3 engine prepare request");
-    auto c = read_struct(columns, "V2 engine column descriptor");
+    auto c = read_struct(columns, "V2 engine column descriptor", 0);
     prepare_v3_impl(q, c, nullptr, 0, Interrupt{}, out, cap);
   });
 }
@@ -516,12 +546,12 @@ int32_t vckss_rust_engine_prepare_interrupt_v1(const VckssEnginePrepareRequestIn
                                                const VckssEngineColumnsV1* columns, uint64_t* out, uint32_t cap) {
   return status([&] {
     auto q = read_struct(request, "interrupt engine prepare request");
-    auto c = read_struct(columns, "engine column descriptor");
+    auto c = read_struct(columns, "engine column descriptor", 0);
     require_abi(q.options.abi_version);
-    if (q.reserved != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved interrupt fields must be zero");
-    PrepareArgs a{q.options.rows, q.options.cleanup_abandoned, q.options.memory_limit_bytes, q.options.caller_copy_bytes};
+    PrepareArgs a{q.options.rows, q.options.cleanup_abandoned, true, q.options.memory_limit_bytes,
+                  q.options.caller_copy_bytes};
     a.v1 = &c;
-    a.interrupt = Interrupt{q.interrupt_poll, q.interrupt_context};
+    a.interrupt = Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "prepare");
     prepare_common(a, out, cap);
   });
 }
@@ -530,9 +560,9 @@ int32_t vckss_rust_engine_prepare_interrupt_v2(const VckssEnginePrepareRequestIn
                                                const VckssEngineColumnsV2* columns, uint64_t* out, uint32_t cap) {
   return status([&] {
     auto q = read_struct(request, "V2 interrupt engine prepare request");
-    auto c = read_struct(columns, "V2 engine column descriptor");
-    if (q.reserved != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved interrupt fields must be zero");
-    prepare_v3_impl(q.options, c, nullptr, 0, Interrupt{q.interrupt_poll, q.interrupt_context}, out, cap);
+    auto c = read_struct(columns, "V2 engine column descriptor", 0);
+    prepare_v3_impl(q.options, c, nullptr, 0,
+                    Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "prepare"), out, cap);
   });
 }
 
@@ -540,13 +570,13 @@ int32_t vckss_rust_engine_prepare_interrupt_v4(const VckssEnginePrepareRequestIn
                                                const VckssEngineColumnsV3* columns, uint64_t* out, uint32_t cap) {
   return status([&] {
     auto q = read_struct(request, "V3 interrupt engine prepare request");
-    auto c = read_struct(columns, "V3 engine column descriptor");
-    if (q.reserved != 0 || q.options.reserved_3 != 0 || c.reserved_3 != 0)
-      fail(ABI_MISMATCH, "engine_ffi", "reserved V3 fields must be zero");
+    auto c = read_struct(columns, "V3 engine column descriptor", 0);
+    if (q.options.reserved_3 != 0 || c.reserved_3 != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved V3 fields must be zero");
     if (q.options.implicit_match > 1) fail(INVALID_INPUT, "engine_prepare", "implicit_match must be zero or one");
     if (c.probeorder_supplied > 1) fail(INVALID_INPUT, "engine_prepare", "probeorder_supplied must be zero or one");
     prepare_v3_impl(q.options.v3, c.v2, c.probeorder_supplied ? c.probe_order : nullptr, q.options.implicit_match,
-                    Interrupt{q.interrupt_poll, q.interrupt_context}, out, cap);
+                    Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "prepare"), out,
+                    cap);
   });
 }
 
@@ -572,8 +602,8 @@ int32_t vckss_rust_engine_solve_v1(uint64_t generation, const VckssEngineSolveRe
 int32_t vckss_rust_engine_solve_interrupt_v1(uint64_t generation, const VckssEngineSolveRequestInterruptV1* request) {
   return status([&] {
     auto q = read_struct(request, "interrupt engine solve request");
-    if (q.reserved != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved interrupt fields must be zero");
-    solve_common(generation, options_from_v1(q.options), Interrupt{q.interrupt_poll, q.interrupt_context});
+    solve_common(generation, options_from_v1(q.options),
+                 Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "solve"));
   });
 }
 
@@ -600,8 +630,8 @@ int32_t vckss_rust_engine_solve_v5(uint64_t generation, const VckssEngineSolveRe
 int32_t vckss_rust_engine_solve_interrupt_v5(uint64_t generation, const VckssEngineSolveRequestInterruptV5* request) {
   return status([&] {
     auto q = read_struct(request, "V5 interrupt engine solve request");
-    if (q.reserved != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved interrupt fields must be zero");
-    solve_common(generation, options_from_v5(q.options), Interrupt{q.interrupt_poll, q.interrupt_context});
+    solve_common(generation, options_from_v5(q.options),
+                 Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "solve"));
   });
 }
 
@@ -823,7 +853,7 @@ int32_t fevcb_set_stream(void* stream) {
 
 int32_t fevcb_engine_solve_options_v1(uint64_t generation, const FevcbSolveOptionsV1* options) {
   return status([&] {
-    auto o = read_struct(options, "device solve options");
+    auto o = read_struct(options, "device solve options", 0);
     if (o.struct_size != sizeof(o)) fail(ABI_MISMATCH, "engine_ffi", "device solve options struct_size mismatch");
     if (o.block_columns != 0 && o.block_columns != 8 && o.block_columns != 16 && o.block_columns != 32 &&
         o.block_columns != 64)

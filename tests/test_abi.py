@@ -35,15 +35,30 @@ def test_identity(lib):
     assert b"VCKSS-COUNTER-V1" in lib.vckss_rust_capabilities_json()
 
 
+class PrepareRequestInterruptV1(abi.Struct):
+    _fields_ = [("options", abi.PrepareRequestV2), ("interrupt_poll", abi.InterruptPoll),
+                ("interrupt_context", C.c_void_p), ("checkpoint_interval", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class SolveRequestInterruptV5(abi.Struct):
+    _fields_ = [("options", abi.SolveRequestV5), ("interrupt_poll", abi.InterruptPoll),
+                ("interrupt_context", C.c_void_p), ("checkpoint_interval", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 @pytest.mark.skipif(not PLUGIN.exists(), reason="reference plugin not staged")
-@pytest.mark.parametrize("name,cls", [("v1", abi.SolveRequestV1), ("v2", abi.SolveRequestV2),
-                                      ("v3", abi.SolveRequestV3), ("v4", abi.SolveRequestV4),
-                                      ("v5", abi.SolveRequestV5)])
+@pytest.mark.parametrize("name,cls", [
+    ("solve_request_v1", abi.SolveRequestV1), ("solve_request_v2", abi.SolveRequestV2),
+    ("solve_request_v3", abi.SolveRequestV3), ("solve_request_v4", abi.SolveRequestV4),
+    ("solve_request_v5", abi.SolveRequestV5), ("solve_request_interrupt_v1", abi.SolveRequestInterruptV1),
+    ("solve_request_interrupt_v5", SolveRequestInterruptV5), ("prepare_request_v3", abi.PrepareRequestV3),
+    ("prepare_request_interrupt_v1", PrepareRequestInterruptV1),
+    ("prepare_request_interrupt_v2", abi.PrepareRequestInterruptV2),
+    ("prepare_request_interrupt_v3", abi.PrepareRequestInterruptV3)])
 def test_default_requests_match_reference(lib, name, cls):
     ref = abi.load(PLUGIN, bind_extensions=False)
     a, b = cls(), cls()
-    assert getattr(lib, f"vckss_rust_engine_default_solve_request_{name}")(C.byref(a), C.sizeof(a)) == 0
-    assert getattr(ref, f"vckss_rust_engine_default_solve_request_{name}")(C.byref(b), C.sizeof(b)) == 0
+    assert getattr(lib, f"vckss_rust_engine_default_{name}")(C.byref(a), C.sizeof(a)) == 0
+    assert getattr(ref, f"vckss_rust_engine_default_{name}")(C.byref(b), C.sizeof(b)) == 0
     assert bytes(a) == bytes(b), (a.as_dict(), b.as_dict())
 
 
@@ -118,11 +133,29 @@ def test_interrupt_poll_breaks_preparation(lib):
 
     p = kat12()
     cols = [np.ascontiguousarray(x) for x in (p.worker, p.firm, p.deletion, p.outcome, p.frequency, p.target_weight)]
-    c1 = abi.ColumnsV1(C.sizeof(abi.ColumnsV1), 0, p.rows, *[x.ctypes.data_as(abi.dptr) for x in cols])
+    c1 = abi.ColumnsV1(C.sizeof(abi.ColumnsV3), 0, p.rows, *[x.ctypes.data_as(abi.dptr) for x in cols])
     c3 = abi.ColumnsV3(abi.ColumnsV2(c1, None, 0, 0), None, 0, 0)
-    v2 = abi.PrepareRequestV2(1, C.sizeof(abi.PrepareRequestV4), p.rows, 1, 0, 1 << 30, 0)
+    v2 = abi.PrepareRequestV2(1, C.sizeof(abi.PrepareRequestInterruptV3), p.rows, 1, 0, 1 << 30, p.rows * 6 * 8)
     req = abi.PrepareRequestInterruptV3(abi.PrepareRequestV4(abi.PrepareRequestV3(v2, 1, 0, 0), 0, 0), poll, None,
                                         4096, 0)
     out = C.c_uint64(99)
     assert lib.vckss_rust_engine_prepare_interrupt_v4(C.byref(req), C.byref(c3), C.byref(out), 8) == 1
     assert out.value == 0 and len(calls) == 2
+    # the reference plugin refuses the same request the same way
+    if PLUGIN.exists():
+        ref = abi.load(PLUGIN, bind_extensions=False)
+        calls.clear()
+        assert ref.vckss_rust_engine_prepare_interrupt_v4(C.byref(req), C.byref(c3), C.byref(out), 8) == 1
+
+
+def test_short_struct_size_is_an_abi_mismatch(lib):
+    from make_golden import kat12
+
+    e = abi.Engine(lib)
+    e.prepare(kat12())
+    req = e.default_request()
+    req.struct_size = 100
+    with pytest.raises(abi.EngineError) as err:
+        e.solve(req)
+    assert err.value.code == 10 and "below required size 176" in err.value.message
+    e.release()
