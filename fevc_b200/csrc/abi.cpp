@@ -42,22 +42,30 @@ int32_t status(F&& f) {
 }
 
 // Caller interrupt callback (reference `CallbackInterrupt::new`,
-// ffi_engine.rs:1422-1461).  The device engine checkpoints between phases and
-// between right-hand-side blocks, each far more than `interval` items of
-// work, so every checkpoint polls the callback.
+// ffi_engine.rs:1422-1461).  The callback is polled at the first checkpoint
+// and again once `interval` items of work have passed; each checkpoint here
+// reports the items of work (rows, right-hand sides) done since the last one.
 struct Interrupt {
   VckssInterruptPollV1 poll = nullptr;
   void* ctx = nullptr;
+  uint64_t interval = 0;
+  mutable uint64_t remaining = 0;
   Interrupt() = default;
-  Interrupt(VckssInterruptPollV1 p, void* c, uint32_t interval, uint32_t reserved, const char* label) : poll(p), ctx(c) {
+  Interrupt(VckssInterruptPollV1 p, void* c, uint32_t iv, uint32_t reserved, const char* label)
+      : poll(p), ctx(c), interval(iv) {
     if (reserved != 0) fail(ABI_MISMATCH, "engine_ffi", std::string("reserved interrupt ") + label + " fields must be zero");
     if (!p && (c || interval != 0))
       fail(INVALID_INPUT, "engine_interrupt", "a null interrupt callback requires null context and zero interval");
     if (p && interval == 0)
       fail(INVALID_INPUT, "engine_interrupt", "a nonnull interrupt callback requires a positive checkpoint interval");
   }
-  void check(const char* phase) const {
-    if (poll && poll(ctx) != VCKSS_INTERRUPT_CONTINUE) fail(USER_BREAK, phase, "interrupted by the caller");
+  void check(const char* phase, uint64_t items = 1) const {
+    if (!poll) return;
+    if (remaining == 0) {
+      if (poll(ctx) != VCKSS_INTERRUPT_CONTINUE) fail(USER_BREAK, phase, "interrupted by the caller");
+      remaining = interval;
+    }
+    remaining = items >= remaining ? 0 : remaining - items;
   }
 };
 
@@ -191,18 +199,18 @@ void prepare_common(const PrepareArgs& a, uint64_t* out, uint32_t cap) {
   auto prep = std::make_unique<Prepared>();
   InputColumns in = copy_columns(a.rows, a.v1->worker, a.v1->firm, a.v1->deletion, a.v1->outcome, a.v1->frequency,
                                  a.v1->target_weight, a.controls, a.controls_count, a.probe_order);
-  a.interrupt.check("engine_ingest");
+  a.interrupt.check("engine_ingest", a.rows);
   Canonical canon = canonicalize(std::move(in), a.implicit_match != 0);
-  a.interrupt.check("canonicalize_final");
+  a.interrupt.check("canonicalize_final", a.rows);
   if (a.deletion_mode == VCKSS_DELETION_OBSERVATION)
     prep->retained = select_observation_graph(canon, prep->graph);
   else if (a.implicit_match)
     prep->retained = select_implicit_match_graph(canon, prep->graph);
   else
     prep->retained = select_match_graph(canon, prep->graph);
-  a.interrupt.check("graph_final");
+  a.interrupt.check("graph_final", a.rows);
   prep->problem = compress(canon, prep->retained, a.implicit_match != 0);
-  a.interrupt.check("compression_final");
+  a.interrupt.check("compression_final", a.rows);
   if (a.deletion_mode == VCKSS_DELETION_MATCH && prep->problem.controls.empty()) {
     prep->plan = build_plan(prep->problem);
     prep->has_plan = true;
@@ -212,7 +220,7 @@ void prepare_common(const PrepareArgs& a, uint64_t* out, uint32_t cap) {
   prep->caller_copy = a.caller_copy;
   prep->deletion_mode = a.deletion_mode;
   prep->controls = a.controls_count;
-  a.interrupt.check("engine_prepare_final");
+  a.interrupt.check("engine_prepare_final", a.rows);
   std::lock_guard<std::mutex> l(reg().mu);
   Registry& r = reg();
   if (r.state != State::Empty) fail(CONTEXT_POISONED, "context_prepare", "another generation became active");

@@ -122,8 +122,11 @@ def test_solve_without_gpu_fails_loudly(lib):
 
 
 def test_interrupt_poll_breaks_preparation(lib):
-    from make_golden import kat12
+    """A callback that asks to stop on its second poll ends preparation with
+    USER_BREAK and no generation, as the reference plugin does."""
+    from fevc_b200.panel import generate_panel
 
+    p = generate_panel(3000, 150, 5, seed=1)  # 15,000 rows: several polls at interval 4096
     calls = []
 
     @abi.InterruptPoll
@@ -131,21 +134,19 @@ def test_interrupt_poll_breaks_preparation(lib):
         calls.append(1)
         return 1 if len(calls) >= 2 else 0
 
-    p = kat12()
     cols = [np.ascontiguousarray(x) for x in (p.worker, p.firm, p.deletion, p.outcome, p.frequency, p.target_weight)]
     c1 = abi.ColumnsV1(C.sizeof(abi.ColumnsV3), 0, p.rows, *[x.ctypes.data_as(abi.dptr) for x in cols])
     c3 = abi.ColumnsV3(abi.ColumnsV2(c1, None, 0, 0), None, 0, 0)
     v2 = abi.PrepareRequestV2(1, C.sizeof(abi.PrepareRequestInterruptV3), p.rows, 1, 0, 1 << 30, p.rows * 6 * 8)
     req = abi.PrepareRequestInterruptV3(abi.PrepareRequestV4(abi.PrepareRequestV3(v2, 1, 0, 0), 0, 0), poll, None,
                                         4096, 0)
-    out = C.c_uint64(99)
-    assert lib.vckss_rust_engine_prepare_interrupt_v4(C.byref(req), C.byref(c3), C.byref(out), 8) == 1
-    assert out.value == 0 and len(calls) == 2
-    # the reference plugin refuses the same request the same way
-    if PLUGIN.exists():
-        ref = abi.load(PLUGIN, bind_extensions=False)
+    libs = [lib] + ([abi.load(PLUGIN, bind_extensions=False)] if PLUGIN.exists() else [])
+    for target in libs:
         calls.clear()
-        assert ref.vckss_rust_engine_prepare_interrupt_v4(C.byref(req), C.byref(c3), C.byref(out), 8) == 1
+        out = C.c_uint64(99)
+        assert target.vckss_rust_engine_prepare_interrupt_v4(C.byref(req), C.byref(c3), C.byref(out), 8) == 1
+        assert out.value == 0 and len(calls) == 2
+        target.vckss_rust_engine_clear_abandoned_v1()
 
 
 def test_short_struct_size_is_an_abi_mismatch(lib):
