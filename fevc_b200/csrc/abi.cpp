@@ -211,8 +211,8 @@ void prepare_common(const PrepareArgs& a, uint64_t* out, uint32_t cap) {
   a.interrupt.check("graph_final", a.rows);
   prep->problem = compress(canon, prep->retained, a.implicit_match != 0);
   a.interrupt.check("compression_final", a.rows);
-  if (a.deletion_mode == VCKSS_DELETION_MATCH && prep->problem.controls.empty()) {
-    prep->plan = build_plan(prep->problem);
+  if (a.deletion_mode == VCKSS_DELETION_MATCH) {
+    prep->plan = prep->problem.controls.empty() ? build_plan(prep->problem) : build_generic_plan(prep->problem);
     prep->has_plan = true;
   }
   prep->input_rows = a.rows;
@@ -262,10 +262,12 @@ SolveOptions options_from_v1(const VckssEngineSolveRequestV1& q) {
   return o;
 }
 
-void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr) {
+void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr, bool generic_allowed) {
   Registry& r = reg();
   std::unique_lock<std::mutex> l(r.mu);
   Prepared& p = r.require(g, "context_solve");
+  if (p.has_plan && p.plan.generic && !generic_allowed)
+    fail(UNSUPPORTED_FEATURE, "engine_solve", "the frozen V1 JLA solve requires a prepared no-control match plan");
   if (r.state != State::Prepared)
     fail(STALE_CONTEXT, "context_solve", "generation " + std::to_string(g) + " is not in the prepared state");
   if (!p.has_plan)
@@ -603,7 +605,7 @@ int32_t vckss_rust_engine_solve_v1(uint64_t generation, const VckssEngineSolveRe
   return status([&] {
     auto q = read_struct(request, "engine solve request");
     if (q.struct_size < sizeof(q)) fail(ABI_MISMATCH, "engine_ffi", "solve request struct_size is too small");
-    solve_common(generation, options_from_v1(q), Interrupt{});
+    solve_common(generation, options_from_v1(q), Interrupt{}, false);
   });
 }
 
@@ -611,7 +613,7 @@ int32_t vckss_rust_engine_solve_interrupt_v1(uint64_t generation, const VckssEng
   return status([&] {
     auto q = read_struct(request, "interrupt engine solve request");
     solve_common(generation, options_from_v1(q.options),
-                 Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "solve"));
+                 Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "solve"), false);
   });
 }
 
@@ -621,6 +623,8 @@ static SolveOptions options_from_v5(const VckssEngineSolveRequestV5& q) {
   if (v1.target_batch_width == 0) v1.target_batch_width = 8;
   if (q.v4.v3.v2.algorithm == VCKSS_ALGORITHM_EXACT)
     fail(UNSUPPORTED_FEATURE, "engine_solve", "the exact estimator is not provided by the device engine");
+  if (q.v4.v3.v2.nuisance_mode == VCKSS_NUISANCE_FIXED_OFFSET)
+    fail(UNSUPPORTED_FEATURE, "engine_solve", "fixed-offset nuisance is not provided by the device engine");
   SolveOptions o = options_from_v1(v1);
   // Without a supplied tolerance the reference full-CMG route solves probes
   // at 1e-6 (vckss-core/src/full_cmg.rs:29,56-69); the device engine keeps the
@@ -631,7 +635,7 @@ static SolveOptions options_from_v5(const VckssEngineSolveRequestV5& q) {
 int32_t vckss_rust_engine_solve_v5(uint64_t generation, const VckssEngineSolveRequestV5* request) {
   return status([&] {
     auto q = read_struct(request, "V5 engine solve request");
-    solve_common(generation, options_from_v5(q), Interrupt{});
+    solve_common(generation, options_from_v5(q), Interrupt{}, true);
   });
 }
 
@@ -639,7 +643,7 @@ int32_t vckss_rust_engine_solve_interrupt_v5(uint64_t generation, const VckssEng
   return status([&] {
     auto q = read_struct(request, "V5 interrupt engine solve request");
     solve_common(generation, options_from_v5(q.options),
-                 Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "solve"));
+                 Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "solve"), true);
   });
 }
 

@@ -27,6 +27,7 @@
 #include "jla_kernels.cuh"
 #include "multigrid.h"
 #include "persistent.cuh"
+#include "generic.cuh"
 
 namespace fevcb {
 
@@ -216,6 +217,15 @@ struct DeviceEngine {
   int preconditioner = 1;
   Segments lap_seg, firm_seg;
   int coop_blocks = 0;
+  // generic (controlled) estimator: row-level data and the control geometry
+  bool generic = false;
+  int q = 0;
+  uint32_t rows = 0;
+  DBuf<uint32_t> row_cell, cell_rows_ptr, cell_rows, unit_group_d, group_rows;
+  DBuf<uint64_t> group_ptr;
+  DBuf<double> row_freq, row_y, Qd, Rd, alphaH, psiH, residual, deleted, beta_buf;
+  bool controls_ready = false;
+  std::vector<double> Sinv, Lfac;  // q x q, row-major
   // solve-long buffers
   DBuf<double> moments, unit_out, omega, fitted, fit_alpha, partial, small;
   DBuf<unsigned long long> error;
@@ -434,6 +444,42 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     upload(e->tgt_rank, plan.tgt_rank, s, h2d);
     upload(e->tgt_count, plan.tgt_count, s, h2d);
     upload(e->tgt_scale, scale, s, h2d);
+  }
+  // row-level data of the generic estimator
+  if (plan.generic) {
+    e->generic = true;
+    e->q = int(p.controls.size());
+    if (e->q < 1 || e->q > QMAX)
+      fail(UNSUPPORTED_FEATURE, "generic_jla", "the device engine handles between 1 and 8 control columns");
+    e->rows = uint32_t(p.rows());
+    size_t R = p.rows();
+    std::vector<double> freq(R), Q(R * e->q);
+    for (size_t r = 0; r < R; ++r) {
+      freq[r] = double(p.frequency[r]);
+      for (int k = 0; k < e->q; ++k) Q[r * e->q + k] = p.controls[k][r];
+    }
+    std::vector<uint32_t> cptr(p.cells + 1, 0), crow(R);
+    for (size_t r = 0; r < R; ++r) cptr[p.row_cell[r] + 1]++;
+    for (size_t c = 0; c < p.cells; ++c) cptr[c + 1] += cptr[c];
+    {
+      std::vector<uint32_t> cur(cptr.begin(), cptr.end() - 1);
+      for (size_t r = 0; r < R; ++r) crow[cur[p.row_cell[r]]++] = uint32_t(r);
+    }
+    upload(e->row_cell, p.row_cell, s, h2d);
+    upload(e->row_freq, freq, s, h2d);
+    upload(e->row_y, p.outcome, s, h2d);
+    upload(e->Qd, Q, s, h2d);
+    upload(e->cell_rows_ptr, cptr, s, h2d);
+    upload(e->cell_rows, crow, s, h2d);
+    upload(e->group_ptr, plan.group_ptr, s, h2d);
+    upload(e->group_rows, plan.group_rows, s, h2d);
+    upload(e->unit_group_d, e->unit_group, s, h2d);
+    e->Rd.alloc(R * e->q);
+    e->residual.alloc(R);
+    e->deleted.alloc(R);
+    e->alphaH.alloc(size_t(e->W) * QMAX);
+    e->psiH.alloc(size_t(e->F) * QMAX);
+    e->beta_buf.alloc(QMAX * 128);
   }
   // hybrid Laplacian
   {
@@ -808,7 +854,7 @@ void run_leverage(DeviceEngine& e, const SolveOptions& o, SolveResult& res, uint
 }
 
 template <int K>
-void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res) {
+void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double y_center = 0.0) {
   constexpr int H = K / 2;
   BlockWork& w = get_work<K>(e);
   Launch L{grid_blocks(), e.stream};
@@ -862,12 +908,46 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res) {
     CK(cudaMemcpyAsync(w.bW.p + size_t(e.W - 1) * K, lastW.data(), K * sizeof(double), cudaMemcpyHostToDevice, L.s));
     CK(cudaMemcpyAsync(w.bF.p + size_t(e.F - 1) * K, lastF.data(), K * sizeof(double), cudaMemcpyHostToDevice, L.s));
     BlockOutcome bo = solve_block<K>(e, w, 2 * np, o, res.timings);
-    k_contract<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, e.omega.p, w.alpha.p, w.x.p,
-                                               e.partial.p);
-    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 3 * K, w.tot.p);
-    CK(cudaMemcpyAsync(draws.data(), w.tot.p, 3 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
-    CK(cudaStreamSynchronize(L.s));
-    res.timings.kernel_launches += 2;
+    if (!e.generic) {
+      k_contract<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, e.omega.p, w.alpha.p, w.x.p,
+                                                 e.partial.p);
+      k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 3 * K, w.tot.p);
+      CK(cudaMemcpyAsync(draws.data(), w.tot.p, 3 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+      CK(cudaStreamSynchronize(L.s));
+      res.timings.kernel_launches += 2;
+    } else {
+      // full-model solves: beta = -S^{-1} Q'W X theta_fe per column, then the
+      // row-level contraction over match groups
+      std::vector<double> t(QMAX * K), beta(QMAX * K, 0.0);
+      k_target_control<K><<<L.grid, THREADS, 0, L.s>>>(e.rows, e.q, e.row_cell.p, e.cell_worker.p, e.cell_firm.p,
+                                                       e.row_freq.p, e.Qd.p, w.alpha.p, w.x.p, e.partial.p);
+      k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, QMAX * K, w.tot.p);
+      CK(cudaMemcpyAsync(t.data(), w.tot.p, QMAX * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+      CK(cudaStreamSynchronize(L.s));
+      for (int k = 0; k < e.q; ++k)
+        for (int j = 0; j < K; ++j) {
+          double v = 0.0;
+          for (int l = 0; l < e.q; ++l) v -= e.Sinv[k * e.q + l] * t[l * K + j];
+          beta[k * K + j] = v;
+        }
+      CK(cudaMemcpyAsync(e.beta_buf.p, beta.data(), QMAX * K * sizeof(double), cudaMemcpyHostToDevice, L.s));
+      k_generic_contract<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.q, e.group_ptr.p, e.group_rows.p, e.row_cell.p,
+                                                         e.cell_worker.p, e.cell_firm.p, e.row_freq.p, e.row_y.p,
+                                                         y_center, e.deleted.p, e.Rd.p, e.beta_buf.p, w.alpha.p,
+                                                         w.x.p, e.partial.p);
+      k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 2 * K, w.tot.p);
+      std::vector<double> g2(2 * K);
+      CK(cudaMemcpyAsync(g2.data(), w.tot.p, 2 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+      CK(cudaStreamSynchronize(L.s));
+      res.timings.kernel_launches += 4;
+      // reference draw: covariance = (total - worker - firm) / 2
+      for (int j = 0; j < np; ++j) {
+        double ww = g2[2 * j], ff = g2[2 * j + 1], tt = g2[K + 2 * j];
+        draws[2 * j] = ww;
+        draws[K + 2 * j] = ff;
+        draws[2 * K + 2 * j] = 0.5 * (tt - ww - ff);
+      }
+    }
     for (int j = 0; j < np; ++j) {
       double ww = draws[2 * j], ff = draws[K + 2 * j], cv = draws[2 * K + 2 * j];
       Components d{ww, ff, cv, ww + ff + 2.0 * cv};
@@ -1015,6 +1095,201 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
   res.timings.total_ms = ms(t0, now());
 }
 
+// ---------------------------------------------------------------------------
+// Generic (controlled) estimator, match deletion, joint nuisance.
+
+// Host Cholesky of a small SPD matrix (n x n, row-major) into its lower factor.
+bool host_cholesky(std::vector<double>& a, int n) {
+  for (int j = 0; j < n; ++j) {
+    double d = a[j * n + j];
+    for (int k = 0; k < j; ++k) d -= a[j * n + k] * a[j * n + k];
+    if (!(d > 0.0) || !std::isfinite(d)) return false;
+    d = std::sqrt(d);
+    a[j * n + j] = d;
+    for (int i = j + 1; i < n; ++i) {
+      double v = a[i * n + j];
+      for (int k = 0; k < j; ++k) v -= a[i * n + k] * a[j * n + k];
+      a[i * n + j] = v / d;
+    }
+    for (int k = j + 1; k < n; ++k) a[j * n + k] = 0.0;
+  }
+  return true;
+}
+
+// Control geometry, once per prepared generation: H = (X'WX)^+ X'WQ by one
+// blocked FE solve, the residualised controls R = Q - X H, S = R'WR, S^{-1} and
+// its lower factor (reference `control_geometry`, generic_jla.rs:4407-4537).
+void setup_controls(DeviceEngine& e, const SolveOptions& o, SolveTimings& tm) {
+  if (e.controls_ready) return;
+  Launch L{grid_blocks(), e.stream};
+  BlockWork& w8 = get_work<8>(e);
+  const int q = e.q;
+  k_cell_controls<<<L.grid, THREADS, 0, L.s>>>(e.C, q, e.cell_rows_ptr.p, e.cell_rows.p, e.row_freq.p, e.Qd.p,
+                                               w8.cell_val.p);
+  k_gather<8><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, w8.cell_val.p, w8.bW.p);
+  firm_gather<8, 0, 0>(e, w8, L, nullptr, w8.cell_val.p, nullptr, 0.0, nullptr, nullptr, nullptr, w8.bF.p, nullptr);
+  SolveOptions oc = o;
+  oc.pcg_tolerance = std::min(o.pcg_tolerance, 1e-10);
+  solve_block<8>(e, w8, q, oc, tm);
+  CK(cudaMemcpyAsync(e.alphaH.p, w8.alpha.p, size_t(e.W) * QMAX * sizeof(double), cudaMemcpyDeviceToDevice, L.s));
+  CK(cudaMemcpyAsync(e.psiH.p, w8.x.p, size_t(e.F) * QMAX * sizeof(double), cudaMemcpyDeviceToDevice, L.s));
+  k_residualize<<<L.grid, THREADS, 0, L.s>>>(e.rows, q, e.row_cell.p, e.cell_worker.p, e.cell_firm.p, e.row_freq.p,
+                                             e.Qd.p, e.alphaH.p, e.psiH.p, e.Rd.p, e.partial.p);
+  k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, QMAX * QMAX, e.small.p);
+  std::vector<double> S8(QMAX * QMAX);
+  CK(cudaMemcpyAsync(S8.data(), e.small.p, S8.size() * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+  CK(cudaStreamSynchronize(L.s));
+  tm.kernel_launches += 8;
+  std::vector<double> S(q * q), Lc;
+  for (int i = 0; i < q; ++i)
+    for (int j = 0; j < q; ++j) S[i * q + j] = 0.5 * (S8[i * QMAX + j] + S8[j * QMAX + i]);
+  Lc = S;
+  if (!host_cholesky(Lc, q))
+    fail(SINGULAR_INFORMATION, "generic_jla_control_schur", "the residualised control information is singular");
+  // S^{-1} from the factor, column by column
+  e.Sinv.assign(q * q, 0.0);
+  for (int c = 0; c < q; ++c) {
+    std::vector<double> b(q, 0.0);
+    b[c] = 1.0;
+    for (int i = 0; i < q; ++i) {
+      double v = b[i];
+      for (int k = 0; k < i; ++k) v -= Lc[i * q + k] * b[k];
+      b[i] = v / Lc[i * q + i];
+    }
+    for (int i = q - 1; i >= 0; --i) {
+      double v = b[i];
+      for (int k = i + 1; k < q; ++k) v -= Lc[k * q + i] * b[k];
+      b[i] = v / Lc[i * q + i];
+    }
+    for (int i = 0; i < q; ++i) e.Sinv[i * q + c] = b[i];
+  }
+  for (int i = 0; i < q; ++i)
+    for (int j = 0; j < i; ++j) e.Sinv[i * q + j] = e.Sinv[j * q + i] = 0.5 * (e.Sinv[i * q + j] + e.Sinv[j * q + i]);
+  e.Lfac = e.Sinv;
+  if (!host_cholesky(e.Lfac, q))
+    fail(BLOCK_INVERSE_FAILED, "generic_jla_control_factor", "control inverse square root failed");
+  e.controls_ready = true;
+}
+
+template <int K>
+void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o, SolveResult& res,
+                 bool detail) {
+  Launch L{grid_blocks(), e.stream};
+  auto now = [] { return std::chrono::steady_clock::now(); };
+  auto t0 = now();
+  setup_controls(e, o, res.timings);
+  const int q = e.q;
+  // ---- joint fit: FE solve of y, then beta = S^{-1} R'W y and theta = theta_y - H beta
+  {
+    BlockWork& w = get_work<1>(e);
+    k_gather<1><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, e.cell_outcome.p, w.bW.p);
+    firm_gather<1, 0, 0>(e, w, L, nullptr, e.cell_outcome.p, nullptr, 0.0, nullptr, nullptr, nullptr, w.bF.p, nullptr);
+    BlockOutcome bo = solve_block<1>(e, w, 1, o, res.timings);
+    res.receipts.push_back(RhsReceipt{1, 1, -1, uint32_t(bo.iters[0]), uint32_t(bo.zero[0]), bo.reduced[0], bo.complete[0]});
+    k_row_project<<<L.grid, THREADS, 0, L.s>>>(e.rows, q, e.row_freq.p, e.Rd.p, e.row_y.p, e.partial.p);
+    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, QMAX, e.small.p);
+    std::vector<double> ry(QMAX);
+    CK(cudaMemcpyAsync(ry.data(), e.small.p, QMAX * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    SmallMatrix beta{};
+    for (int k = 0; k < q; ++k) {
+      double v = 0.0;
+      for (int l = 0; l < q; ++l) v += e.Sinv[k * q + l] * ry[l];
+      beta.m[k] = v;
+    }
+    k_apply_beta<<<L.grid, THREADS, 0, L.s>>>(e.W, q, e.alphaH.p, beta, w.alpha.p);
+    k_apply_beta<<<L.grid, THREADS, 0, L.s>>>(e.F, q, e.psiH.p, beta, w.x.p);
+    k_row_residual<<<L.grid, THREADS, 0, L.s>>>(e.rows, q, e.row_cell.p, e.cell_worker.p, e.cell_firm.p, e.row_y.p,
+                                                e.Qd.p, w.alpha.p, w.x.p, beta, e.residual.p);
+    k_fit_cells<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p, e.cell_target.p,
+                                             e.fitted.p, 0, nullptr, e.partial.p);
+    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 4, e.small.p);
+    std::vector<double> m(4);
+    CK(cudaMemcpyAsync(m.data(), e.small.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    double means[2] = {m[0] / p.target_total, m[1] / p.target_total};
+    CK(cudaMemcpyAsync(e.small.p + 8, means, 2 * sizeof(double), cudaMemcpyHostToDevice, L.s));
+    k_fit_cells<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p, e.cell_target.p,
+                                             e.fitted.p, 1, e.small.p + 8, e.partial.p);
+    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 4, e.small.p);
+    CK(cudaMemcpyAsync(m.data(), e.small.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    double T = p.target_total;
+    res.plugin = finish_accounting(m[0] / T, m[1] / T, m[2] / T, m[3] / T, "generic_jla_components");
+    res.timings.kernel_launches += 12;
+  }
+  auto t1 = now();
+  // ---- FE-only leverage probes (reference `match_leverage_moments`)
+  CK(cudaMemsetAsync(e.moments.p, 0, e.moments.bytes(), L.s));
+  run_leverage<K>(e, o, res, 0);
+  // ---- deleted residuals of every match group
+  {
+    GenericAdjustParams prm{};
+    prm.units = e.G;
+    prm.q = q;
+    prm.probes = double(o.probes);
+    prm.block_tolerance = o.block_tolerance;
+    prm.rank_tolerance = o.rank_tolerance;
+    for (int i = 0; i < q; ++i)
+      for (int j = 0; j < q; ++j) prm.factor.m[i * QMAX + j] = e.Lfac[i * q + j];
+    unsigned long long init = ~0ull;
+    CK(cudaMemcpyAsync(e.error.p, &init, sizeof(init), cudaMemcpyHostToDevice, L.s));
+    k_generic_adjust<<<L.grid, THREADS, 0, L.s>>>(prm, e.unit_group_d.p, e.moments.p, e.unit_count_f.p, e.group_ptr.p,
+                                                  e.group_rows.p, e.row_freq.p, e.residual.p, e.Rd.p, e.deleted.p,
+                                                  e.unit_out.p, e.error.p);
+    unsigned long long err = 0;
+    CK(cudaMemcpyAsync(&err, e.error.p, sizeof(err), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    res.timings.kernel_launches += 1;
+    if (err != ~0ull) {
+      uint32_t code = uint32_t(err & 0xff);
+      uint32_t g = e.unit_group[err >> 8];
+      const char* what = code == JLA_CONSTRAINT_FAILED   ? "projection and residual masses are not positive"
+                         : code == NONESTIMABLE_DELETION ? "a match residual block is singular"
+                                                         : "finite-projection moment failed";
+      fail(int32_t(code), "generic_jla_leverage", std::string(what) + " at unit " + std::to_string(g));
+    }
+  }
+  auto t2 = now();
+  // ---- target draws on the full model
+  run_target<K>(e, o, res, outcome_mean(p, o.centering));
+  auto t3 = now();
+  {
+    StableSum s[4];
+    for (auto& d : res.target_draws) {
+      s[0].add(d.worker);
+      s[1].add(d.firm);
+      s[2].add(d.covariance);
+      s[3].add(d.total);
+    }
+    double P = double(o.probes);
+    Components corr{s[0].finish() / P, s[1].finish() / P, s[2].finish() / P, s[3].finish() / P};
+    res.correction = corr;
+    res.corrected = Components{res.plugin.worker - corr.worker, res.plugin.firm - corr.firm,
+                               res.plugin.covariance - corr.covariance, res.plugin.total - corr.total};
+    StableSum qq[4];
+    for (auto& d : res.target_draws) {
+      qq[0].add((d.worker - corr.worker) * (d.worker - corr.worker));
+      qq[1].add((d.firm - corr.firm) * (d.firm - corr.firm));
+      qq[2].add((d.covariance - corr.covariance) * (d.covariance - corr.covariance));
+      qq[3].add((d.total - corr.total) * (d.total - corr.total));
+    }
+    double den = P * (P - 1.0);
+    res.mcse = Components{std::sqrt(qq[0].finish() / den), std::sqrt(qq[1].finish() / den),
+                          std::sqrt(qq[2].finish() / den), std::sqrt(qq[3].finish() / den)};
+  }
+  for (auto& r : res.receipts) {
+    res.max_reduced_residual = std::max(res.max_reduced_residual, r.reduced_residual);
+    res.max_complete_residual = std::max(res.max_complete_residual, r.complete_residual);
+  }
+  (void)detail;
+  auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+  res.timings.fit_ms = ms(t0, t1);
+  res.timings.leverage_ms = ms(t1, t2);
+  res.timings.target_ms = ms(t2, t3);
+  res.timings.total_ms = ms(t0, now());
+}
+
 }  // namespace
 
 SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o,
@@ -1025,6 +1300,16 @@ SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& pl
   SolveResult res;
   int K = o.block_columns;
   if (K == 0) K = 64;
+  if (e.generic) {
+    switch (K) {
+      case 8: run_generic<8>(e, p, plan, o, res, want_unit_detail); break;
+      case 16: run_generic<16>(e, p, plan, o, res, want_unit_detail); break;
+      case 32: run_generic<32>(e, p, plan, o, res, want_unit_detail); break;
+      case 64: run_generic<64>(e, p, plan, o, res, want_unit_detail); break;
+      default: fail(INVALID_INPUT, "jla_validate", "device block width must be 8, 16, 32 or 64");
+    }
+    return res;
+  }
   switch (K) {
     case 8: run_jla<8>(e, p, plan, o, res, want_unit_detail); break;
     case 16: run_jla<16>(e, p, plan, o, res, want_unit_detail); break;

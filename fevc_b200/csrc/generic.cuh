@@ -1,0 +1,382 @@
+// Kernels of the generic (controlled) estimator, match deletion, joint
+// nuisance (reference vckss-core/src/generic_jla.rs).  Controls enter through
+// the exact Frisch-Waugh-Lovell block: with H = (X'WX)^+ X'WQ and the
+// residualised controls R = Q - X H, S = R'WR,
+//   full-model solve of (r_X, 0):  beta = -S^{-1} Q'W X theta_fe,
+//                                   row prediction = x_r'theta_fe + R_r'beta,
+// and each match group's leave-out block is the rank-(1+q) low-rank update of
+// generic_jla.rs:6053-6196 (FE leverage estimated by the JLA moments, control
+// leverage exact).
+#pragma once
+
+#include "kernels.cuh"
+
+namespace fevcb {
+
+constexpr int QMAX = 8;          // controls handled on the device
+constexpr int RMAX = QMAX + 1;   // rank of a match block's low-rank factor
+
+// per-cell sums of frequency-weighted controls: out[c*8 + k] = sum_{r in c} f_r Q[r][k]
+__global__ void k_cell_controls(uint32_t cells, int q, const uint32_t* __restrict__ cell_ptr,
+                                const uint32_t* __restrict__ cell_rows, const double* __restrict__ row_freq,
+                                const double* __restrict__ Q, double* __restrict__ out) {
+  for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
+    double acc[QMAX];
+#pragma unroll
+    for (int k = 0; k < QMAX; ++k) acc[k] = 0.0;
+    for (uint32_t i = cell_ptr[c]; i < cell_ptr[c + 1]; ++i) {
+      uint32_t r = cell_rows[i];
+      double f = row_freq[r];
+      for (int k = 0; k < q; ++k) acc[k] += f * Q[size_t(r) * q + k];
+    }
+#pragma unroll
+    for (int k = 0; k < QMAX; ++k) out[c * QMAX + k] = acc[k];
+  }
+}
+
+// R[r][k] = Q[r][k] - (alphaH[w(r)][k] + psiH[f(r)][k]);  partial[blk][64] = sum f R R'
+__global__ void k_residualize(uint32_t rows, int q, const uint32_t* __restrict__ row_cell,
+                              const uint32_t* __restrict__ cell_worker, const uint32_t* __restrict__ cell_firm,
+                              const double* __restrict__ row_freq, const double* __restrict__ Q,
+                              const double* __restrict__ alphaH, const double* __restrict__ psiH,
+                              double* __restrict__ R, double* __restrict__ partial) {
+  double v[QMAX * QMAX][1];
+#pragma unroll
+  for (int i = 0; i < QMAX * QMAX; ++i) v[i][0] = 0.0;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < rows; base += size_t(gridDim.x) * blockDim.x) {
+    size_t r = base + threadIdx.x;
+    if (r < rows) {
+      uint32_t c = row_cell[r];
+      const double* a = alphaH + size_t(cell_worker[c]) * QMAX;
+      const double* p = psiH + size_t(cell_firm[c]) * QMAX;
+      double f = row_freq[r], x[QMAX];
+#pragma unroll
+      for (int k = 0; k < QMAX; ++k) {
+        x[k] = k < q ? Q[r * q + k] - (a[k] + p[k]) : 0.0;
+        if (k < q) R[r * q + k] = x[k];
+      }
+#pragma unroll
+      for (int i = 0; i < QMAX; ++i)
+#pragma unroll
+        for (int j = 0; j < QMAX; ++j) v[i * QMAX + j][0] += f * x[i] * x[j];
+    }
+  }
+  block_reduce_cols<1, QMAX * QMAX>(v, partial);
+}
+
+// partial[blk][k] = sum_r f_r M[r][k] y_r   (M = R or Q, y = row values)
+__global__ void k_row_project(uint32_t rows, int q, const double* __restrict__ row_freq, const double* __restrict__ M,
+                              const double* __restrict__ y, double* __restrict__ partial) {
+  double v[QMAX][1];
+#pragma unroll
+  for (int k = 0; k < QMAX; ++k) v[k][0] = 0.0;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < rows; base += size_t(gridDim.x) * blockDim.x) {
+    size_t r = base + threadIdx.x;
+    if (r < rows) {
+      double fy = row_freq[r] * y[r];
+#pragma unroll
+      for (int k = 0; k < QMAX; ++k)
+        if (k < q) v[k][0] += fy * M[r * q + k];
+    }
+  }
+  block_reduce_cols<1, QMAX>(v, partial);
+}
+
+struct SmallMatrix {
+  double m[QMAX * QMAX];
+};
+
+// Full-fit correction: alpha -= alphaH beta, psi -= psiH beta (rows = W, then F).
+__global__ void k_apply_beta(uint32_t rows, int q, const double* __restrict__ H, SmallMatrix beta,
+                             double* __restrict__ coef) {
+  for (size_t r = size_t(blockIdx.x) * blockDim.x + threadIdx.x; r < rows; r += size_t(gridDim.x) * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < q; ++k) s += H[r * QMAX + k] * beta.m[k];
+    coef[r] -= s;
+  }
+}
+
+// residual_r = y_r - (alpha_w + psi_f + Q_r'beta)
+__global__ void k_row_residual(uint32_t rows, int q, const uint32_t* __restrict__ row_cell,
+                               const uint32_t* __restrict__ cell_worker, const uint32_t* __restrict__ cell_firm,
+                               const double* __restrict__ y, const double* __restrict__ Q,
+                               const double* __restrict__ alpha, const double* __restrict__ psi, SmallMatrix beta,
+                               double* __restrict__ residual) {
+  for (size_t r = size_t(blockIdx.x) * blockDim.x + threadIdx.x; r < rows; r += size_t(gridDim.x) * blockDim.x) {
+    uint32_t c = row_cell[r];
+    double fit = alpha[cell_worker[c]] + psi[cell_firm[c]];
+    for (int k = 0; k < q; ++k) fit += Q[r * q + k] * beta.m[k];
+    residual[r] = y[r] - fit;
+  }
+}
+
+struct GenericAdjustParams {
+  uint32_t units;
+  int q;
+  double probes, block_tolerance, rank_tolerance;
+  SmallMatrix factor;  // lower factor L of S^{-1} = L L'  (row-major, q x q)
+};
+
+// In-place Cholesky of an SPD matrix a (n x n, row-major, n <= RMAX); returns
+// the smallest pivot (squared diagonal of the factor).
+__device__ __forceinline__ double small_cholesky(double* a, int n) {
+  double minpiv = 1e300;
+  for (int j = 0; j < n; ++j) {
+    double d = a[j * RMAX + j];
+    for (int k = 0; k < j; ++k) d -= a[j * RMAX + k] * a[j * RMAX + k];
+    minpiv = fmin(minpiv, d);
+    if (!(d > 0.0)) return d;
+    double s = sqrt(d);
+    a[j * RMAX + j] = s;
+    for (int i = j + 1; i < n; ++i) {
+      double v = a[i * RMAX + j];
+      for (int k = 0; k < j; ++k) v -= a[i * RMAX + k] * a[j * RMAX + k];
+      a[i * RMAX + j] = v / s;
+    }
+  }
+  return minpiv;
+}
+
+__device__ __forceinline__ void small_solve(const double* l, int n, double* b) {
+  for (int i = 0; i < n; ++i) {
+    double v = b[i];
+    for (int k = 0; k < i; ++k) v -= l[i * RMAX + k] * b[k];
+    b[i] = v / l[i * RMAX + i];
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double v = b[i];
+    for (int k = i + 1; k < n; ++k) v -= l[k * RMAX + i] * b[k];
+    b[i] = v / l[i * RMAX + i];
+  }
+}
+
+// Deleted residuals of every match group (reference `match_deleted_adjustment`,
+// generic_jla.rs:6053-6196).  One thread per group; the group's rows are in
+// semantic-rank order.  Low-rank factor row l:
+//   V[l][0] = sqrt(P) * common_l,  common_l = sqrt(f_r / n_g)
+//   V[l][1+o] = sqrt(f_r) * (R_r' L)_o
+// and (I - V V') X = [sqrt(f) residual, common] is solved directly (width <=
+// rank) or through the rank x rank system I - V'V (width > rank).
+__global__ void k_generic_adjust(GenericAdjustParams prm, const uint32_t* __restrict__ unit_group,
+                                 const double* __restrict__ moments, const double* __restrict__ unit_count_f,
+                                 const uint64_t* __restrict__ group_ptr, const uint32_t* __restrict__ group_rows,
+                                 const double* __restrict__ row_freq, const double* __restrict__ residual,
+                                 const double* __restrict__ R, double* __restrict__ deleted,
+                                 double* __restrict__ unit_out, unsigned long long* __restrict__ error) {
+  const int q = prm.q, rank = 1 + q;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < prm.units; i += gridDim.x * blockDim.x) {
+    uint32_t g = unit_group[i];
+    const double* m = moments + size_t(i) * 5;
+    double P = prm.probes;
+    unsigned long long code = 0;
+    double total_mean = (m[0] + m[1]) / P;
+    if (!isfinite(total_mean) || total_mean <= prm.block_tolerance) code = JLA_CONSTRAINT_FAILED;
+    double proj = (m[0] / P) / total_mean, resid = (m[1] / P) / total_mean;
+    double p4 = m[2] / P, m4 = m[3] / P, mixed = m[4] / P;
+    double bias = (resid * p4 - proj * m4 + (resid - proj) * mixed) / P;
+    double var = (resid * resid * p4 + proj * proj * m4 - 2.0 * proj * resid * mixed) / P;
+    if (!code && !(isfinite(proj) && isfinite(resid) && isfinite(bias) && isfinite(var))) code = JLA_MOMENT_FAILED;
+    if (!code && var < -100.0 * prm.rank_tolerance) code = JLA_MOMENT_FAILED;
+    var = fmax(var, 0.0);
+    double sp = sqrt(fmax(proj, 0.0));
+    double inv_root_n = 1.0 / sqrt(unit_count_f[i]);
+    uint64_t b = group_ptr[g], e = group_ptr[g + 1];
+    int width = int(e - b);
+    auto vrow = [&](uint32_t r, double* v) {
+      double root = sqrt(row_freq[r]);
+      v[0] = sp * root * inv_root_n;
+      for (int o = 0; o < q; ++o) {
+        double s = 0.0;
+        for (int in = o; in < q; ++in) s += R[size_t(r) * q + in] * prm.factor.m[in * QMAX + o];
+        v[1 + o] = root * s;
+      }
+    };
+    double a[RMAX * RMAX];
+    double x0[RMAX], x1[RMAX];
+    double ct = 0.0, ci = 0.0;
+    if (width <= rank) {
+      double V[RMAX][RMAX];
+      for (int l = 0; l < width; ++l) {
+        uint32_t r = group_rows[b + l];
+        vrow(r, V[l]);
+        double root = sqrt(row_freq[r]);
+        x0[l] = root * residual[r];
+        x1[l] = root * inv_root_n;
+      }
+      for (int s = 0; s < width; ++s)
+        for (int t = 0; t < width; ++t) {
+          double v = (s == t) ? 1.0 : 0.0;
+          for (int k = 0; k < rank; ++k) v -= V[s][k] * V[t][k];
+          a[s * RMAX + t] = v;
+        }
+      double piv = small_cholesky(a, width);
+      if (!code && !(piv > prm.block_tolerance)) code = NONESTIMABLE_DELETION;
+      if (!code) {
+        small_solve(a, width, x0);
+        small_solve(a, width, x1);
+      }
+      for (int l = 0; l < width; ++l) {
+        double c = sqrt(row_freq[group_rows[b + l]]) * inv_root_n;
+        ct += c * x0[l];
+        ci += c * x1[l];
+      }
+      for (int l = 0; l < width; ++l) {
+        uint32_t r = group_rows[b + l];
+        deleted[r] = x0[l] + bias * x1[l] * ct - var * x1[l] * ci * ct;
+      }
+    } else {
+      // Woodbury: (I - V V')^{-1} y = y + V (I - V'V)^{-1} V'y
+      double vt0[RMAX], vt1[RMAX], v[RMAX];
+      for (int s = 0; s < rank; ++s) {
+        vt0[s] = vt1[s] = 0.0;
+        for (int t = 0; t < rank; ++t) a[s * RMAX + t] = (s == t) ? 1.0 : 0.0;
+      }
+      for (int l = 0; l < width; ++l) {
+        uint32_t r = group_rows[b + l];
+        vrow(r, v);
+        double root = sqrt(row_freq[r]);
+        double y0 = root * residual[r], y1 = root * inv_root_n;
+        for (int s = 0; s < rank; ++s) {
+          vt0[s] += v[s] * y0;
+          vt1[s] += v[s] * y1;
+          for (int t = 0; t < rank; ++t) a[s * RMAX + t] -= v[s] * v[t];
+        }
+      }
+      double piv = small_cholesky(a, rank);
+      if (!code && !(piv > prm.block_tolerance)) code = NONESTIMABLE_DELETION;
+      if (!code) {
+        small_solve(a, rank, vt0);
+        small_solve(a, rank, vt1);
+      }
+      // two passes over the rows: dots with the common direction, then outputs
+      for (int pass = 0; pass < 2; ++pass) {
+        for (int l = 0; l < width; ++l) {
+          uint32_t r = group_rows[b + l];
+          vrow(r, v);
+          double root = sqrt(row_freq[r]);
+          double t0 = root * residual[r], t1 = root * inv_root_n;
+          for (int s = 0; s < rank; ++s) {
+            t0 += v[s] * vt0[s];
+            t1 += v[s] * vt1[s];
+          }
+          if (pass == 0) {
+            double c = root * inv_root_n;
+            ct += c * t0;
+            ci += c * t1;
+          } else {
+            deleted[r] = t0 + bias * t1 * ct - var * t1 * ci * ct;
+          }
+        }
+      }
+    }
+    if (code) atomicMin(error, (unsigned long long)(i) << 8 | code);
+    double* o = unit_out + size_t(i) * 6;
+    o[0] = proj;
+    o[1] = resid;
+    o[2] = bias;
+    o[3] = var;
+    o[4] = ct;
+    o[5] = ci;
+  }
+}
+
+// Target control correction, right-hand side: partial[blk][k][K] =
+// sum_r f_r Q[r][k] (alpha_w + psi_f)[column]   (k < QMAX)
+template <int K>
+__global__ void k_target_control(uint32_t rows, int q, const uint32_t* __restrict__ row_cell,
+                                 const uint32_t* __restrict__ cell_worker, const uint32_t* __restrict__ cell_firm,
+                                 const double* __restrict__ row_freq, const double* __restrict__ Q,
+                                 const double* __restrict__ alpha, const double* __restrict__ psi,
+                                 double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  double v[QMAX][CPT];
+#pragma unroll
+  for (int k = 0; k < QMAX; ++k)
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) v[k][c] = 0.0;
+  int c0 = int(threadIdx.x % TPR) * CPT;
+  size_t total = size_t(rows) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    if (t < total) {
+      size_t r = t / TPR;
+      uint32_t c = row_cell[r];
+      size_t wb = size_t(cell_worker[c]) * K + c0, fb = size_t(cell_firm[c]) * K + c0;
+      double f = row_freq[r];
+#pragma unroll
+      for (int cc = 0; cc < CPT; ++cc) {
+        double u = f * (alpha[wb + cc] + psi[fb + cc]);
+#pragma unroll
+        for (int k = 0; k < QMAX; ++k)
+          if (k < q) v[k][cc] += u * Q[r * q + k];
+      }
+    }
+  }
+  block_reduce_cols<K, QMAX>(v, partial);
+}
+
+// Generic target draw (reference `target_draw`, generic_jla/statistical_batches.rs:259-347):
+// per match group, first_t = sum_r f y u_t(r), second_t = sum_r sqrt(f) d_r u_t(r),
+// draw_t += first_t * second_t, with u_t(r) = u_fe,t(cell) + R_r' beta_t for the
+// worker side t = 2j, the firm side 2j+1 and their sum (the total).
+// partial[blk][0][K]: worker (even) / firm (odd) draw; [1][K]: total (even columns).
+template <int K>
+__global__ void k_generic_contract(uint32_t groups, int q, const uint64_t* __restrict__ group_ptr,
+                                   const uint32_t* __restrict__ group_rows, const uint32_t* __restrict__ row_cell,
+                                   const uint32_t* __restrict__ cell_worker, const uint32_t* __restrict__ cell_firm,
+                                   const double* __restrict__ row_freq, const double* __restrict__ y, double y_center,
+                                   const double* __restrict__ deleted, const double* __restrict__ R,
+                                   const double* __restrict__ beta /* [QMAX][K] */, const double* __restrict__ alpha,
+                                   const double* __restrict__ psi, double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  static_assert(CPT <= 2, "pairs of columns must sit in one thread or in adjacent lanes");
+  double v[2][CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
+  const int c0 = int(threadIdx.x % TPR) * CPT;
+  double bcol[QMAX][CPT];
+#pragma unroll
+  for (int k = 0; k < QMAX; ++k)
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) bcol[k][c] = k < q ? beta[k * K + c0 + c] : 0.0;
+  size_t total = size_t(groups) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    bool live = t < total;
+    size_t g = live ? t / TPR : 0;
+    uint64_t b = live ? group_ptr[g] : 0, e = live ? group_ptr[g + 1] : 0;
+    uint32_t cell = live ? row_cell[group_rows[b]] : 0;
+    double ufe[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c)
+      ufe[c] = live ? alpha[size_t(cell_worker[cell]) * K + c0 + c] + psi[size_t(cell_firm[cell]) * K + c0 + c] : 0.0;
+    double first[CPT], second[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) first[c] = second[c] = 0.0;
+    // the TPR lanes of a group walk its rows in lock step
+    for (uint64_t i = b; i < e; ++i) {
+      uint32_t r = group_rows[i];
+      double f = row_freq[r], fy = f * (y[r] - y_center), sd = sqrt(f) * deleted[r];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        double u = ufe[c];
+        for (int k = 0; k < q; ++k) u += R[size_t(r) * q + k] * bcol[k][c];
+        first[c] += fy * u;
+        second[c] += sd * u;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) v[0][c] += first[c] * second[c];
+    // the total's sums are the sums of the two sides' (linear in u)
+    if (CPT == 2) {
+      v[1][0] += (first[0] + first[CPT - 1]) * (second[0] + second[CPT - 1]);
+    } else {
+      double fo = __shfl_xor_sync(0xffffffffu, first[0], 1);
+      double so = __shfl_xor_sync(0xffffffffu, second[0], 1);
+      if ((c0 & 1) == 0) v[1][0] += (first[0] + fo) * (second[0] + so);
+    }
+  }
+  block_reduce_cols<K, 2>(v, partial);
+}
+
+}  // namespace fevcb

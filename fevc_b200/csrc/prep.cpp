@@ -892,3 +892,110 @@ JlaPlan build_plan(const Compressed& p) {
 }
 
 }  // namespace fevcb
+
+namespace fevcb {
+
+JlaPlan build_generic_plan(const Compressed& p) {
+  size_t R = p.rows();
+  JlaPlan plan;
+  plan.generic = true;
+  std::vector<double> per_copy(R);
+  for (size_t r = 0; r < R; ++r) per_copy[r] = p.target[r] / double(p.frequency[r]);
+  bool has_order = !p.probe_order.empty();
+  // reference `compare_semantic_rows` (generic_jla.rs:3878-3900): per-copy mass
+  // and outcome by total order (no zero canonicalisation), then the controls
+  // and the probe order with -0.0 mapped to +0.0
+  auto sem = [&](uint32_t a, uint32_t b) -> int {
+    if (p.row_worker[a] != p.row_worker[b]) return p.row_worker[a] < p.row_worker[b] ? -1 : 1;
+    if (p.row_firm[a] != p.row_firm[b]) return p.row_firm[a] < p.row_firm[b] ? -1 : 1;
+    if (p.row_deletion[a] != p.row_deletion[b]) return p.row_deletion[a] < p.row_deletion[b] ? -1 : 1;
+    int c = total_cmp(per_copy[a], per_copy[b]);
+    if (c) return c;
+    c = total_cmp(p.outcome[a], p.outcome[b]);
+    if (c) return c;
+    for (auto& col : p.controls) {
+      c = ordered_f64(col[a], col[b]);
+      if (c) return c;
+    }
+    if (has_order) return ordered_f64(p.probe_order[a], p.probe_order[b]);
+    return 0;
+  };
+  std::vector<uint32_t> order(R);
+  std::iota(order.begin(), order.end(), 0u);
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return sem(a, b) < 0; });
+  plan.row_rank.assign(R, 0);
+  uint64_t current = 0;
+  for (size_t i = 0; i < R; ++i) {
+    if (i == 0 || sem(order[i - 1], order[i]) != 0) ++current;
+    plan.row_rank[order[i]] = current;
+  }
+  // match groups (deletion units), rows stably sorted by rank
+  size_t G = p.deletion_index.ptr.size() - 1;
+  plan.group_ptr.assign(p.deletion_index.ptr.begin(), p.deletion_index.ptr.end());
+  plan.group_rows.assign(p.deletion_index.items.begin(), p.deletion_index.items.end());
+  plan.del_cell.resize(G);
+  plan.del_count.resize(G);
+  plan.del_rank.resize(G);
+  plan.del_outcome_sum.resize(G);
+  plan.del_target_mass.resize(G);
+  for (size_t g = 0; g < G; ++g) {
+    auto b = plan.group_rows.begin() + plan.group_ptr[g], e = plan.group_rows.begin() + plan.group_ptr[g + 1];
+    if (b == e) fail(RESOURCE_LIMIT, "generic_jla_match_plan", "a match block is empty or exceeds blocksize_limit");
+    std::stable_sort(b, e, [&](uint32_t x, uint32_t y) { return plan.row_rank[x] < plan.row_rank[y]; });
+    uint32_t cell = p.row_cell[*b];
+    uint64_t phys = 0, ent = ~uint64_t(0);
+    StableSum y, t;
+    for (auto it = b; it != e; ++it) {
+      if (p.row_cell[*it] != cell)
+        fail(INVALID_IDENTIFIER, "generic_jla_match_plan", "one match deletion unit crosses coefficient cells");
+      phys += p.frequency[*it];
+      ent = std::min(ent, plan.row_rank[*it]);
+      y.add(double(p.frequency[*it]) * p.outcome[*it]);
+      t.add(p.target[*it]);
+    }
+    if (phys == 0 || (phys + 63) / 64 > (uint64_t(1) << 20))
+      fail(RESOURCE_LIMIT, "jla_validate", "match deletion unit trial preflight failed");
+    plan.del_cell[g] = cell;
+    plan.del_count[g] = phys;
+    plan.del_rank[g] = ent;
+    plan.del_outcome_sum[g] = y.finish();
+    plan.del_target_mass[g] = t.finish();
+  }
+  // target strata (reference `target_plan`, generic_jla.rs:3902-3995)
+  std::vector<uint32_t> tord(R);
+  std::iota(tord.begin(), tord.end(), 0u);
+  std::stable_sort(tord.begin(), tord.end(), [&](uint32_t a, uint32_t b) {
+    if (p.row_cell[a] != p.row_cell[b]) return p.row_cell[a] < p.row_cell[b];
+    int c = total_cmp(canonical_zero(per_copy[a]), canonical_zero(per_copy[b]));
+    if (c) return c < 0;
+    return plan.row_rank[a] < plan.row_rank[b];
+  });
+  for (size_t cur = 0; cur < R;) {
+    size_t begin = cur;
+    uint32_t cell = p.row_cell[tord[cur]];
+    double pc = canonical_zero(per_copy[tord[cur]]);
+    uint64_t bits;
+    std::memcpy(&bits, &pc, 8);
+    uint64_t phys = 0, ent = ~uint64_t(0);
+    StableSum t;
+    while (cur < R) {
+      double v = canonical_zero(per_copy[tord[cur]]);
+      uint64_t vb;
+      std::memcpy(&vb, &v, 8);
+      if (p.row_cell[tord[cur]] != cell || vb != bits) break;
+      phys += p.frequency[tord[cur]];
+      t.add(p.target[tord[cur]]);
+      ent = std::min(ent, plan.row_rank[tord[cur]]);
+      ++cur;
+    }
+    (void)begin;
+    plan.tgt_cell.push_back(cell);
+    plan.tgt_per_copy.push_back(pc);
+    plan.tgt_count.push_back(phys);
+    plan.tgt_mass.push_back(t.finish());
+    plan.tgt_rank.push_back(ent);
+  }
+  return plan;
+}
+
+}  // namespace fevcb

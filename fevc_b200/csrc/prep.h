@@ -69,7 +69,11 @@ struct Compressed {
 };
 
 struct JlaPlan {
+  bool generic = false;  // built by build_generic_plan (controls present)
   std::vector<uint64_t> row_rank;
+  // generic plan only: rows of each deletion group in semantic-rank order
+  std::vector<uint64_t> group_ptr;
+  std::vector<uint32_t> group_rows;
   // deletion units
   std::vector<uint32_t> del_cell;
   std::vector<uint64_t> del_count, del_rank;
@@ -105,5 +109,11 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
 // Reference `JlaPlan::build_no_controls_with_certified_match_and_interrupt`
 // (jla.rs:59-108) generalised: controls do not enter the plan's orderings.
 JlaPlan build_plan(const Compressed& p);
+
+// The generic (controlled) estimator's plan: semantic ranks that also order
+// by the control values, match groups with their rows in rank order, and
+// target strata (reference generic_jla.rs:3836-3900 ranks, 4052-4143 match
+// plan, 3902-3995 target plan).
+JlaPlan build_generic_plan(const Compressed& p);
 
 }  // namespace fevcb

@@ -75,6 +75,52 @@ PANELS = {
 }
 
 
+CONTROL_PANELS = {
+    "controls_2k": dict(build=lambda: generate_panel(2000, 150, 5, move_p=0.2, year_controls=True, seed=11), probes=16),
+    "controls_weighted_1500": dict(build=lambda: weighted_controls_panel(6), probes=12),
+    "controls_6p_4k": dict(build=lambda: generate_panel(4000, 200, 6, move_p=0.15, year_controls=True, seed=9),
+                           probes=12),
+}
+
+
+def weighted_controls_panel(seed: int) -> Panel:
+    """Year controls with literal frequencies, uneven target weights and
+    repeated rows per match (multi-row deletion groups)."""
+    p = generate_panel(1500, 120, 5, move_p=0.25, year_controls=True, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    p.frequency = rng.integers(1, 4, p.rows).astype(np.float64)
+    p.target_weight = np.round(rng.uniform(0.5, 3.0, p.rows) * 4) / 4 * p.frequency
+    return p
+
+
+def solve_record_v5(lib, panel: Panel, probes: int, centering: int) -> dict:
+    """The plugin's generic engine (controls) through V5, diagonal PCG at 1e-13."""
+    e = abi.Engine(lib)
+    e.prepare(panel)
+    if centering:
+        e.centering(centering)
+    q = e.default_request_v5()
+    v1 = q.v4.v3.v2.v1
+    v1.probes = probes
+    v1.solver_route = 2
+    v1.pcg_tolerance = 1e-13
+    v1.maximum_iterations = 20000
+    v1.leverage_batch_width = 4
+    v1.target_batch_width = 4
+    q.v4.v3.v2.algorithm = 2
+    q.v4.v3.engine = 2
+    q.v4.v3.batch_mode = 1
+    q.v4.leverage_batch_mode = 1
+    q.v4.target_batch_mode = 1
+    q.threads = 4
+    q.tolerance_supplied = 1
+    e.solve_v5(q, controls_count=len(panel.controls))
+    res = e.result()
+    e.release()
+    return {"seed": int(v1.seed), "probes": probes, "centering": centering, "pcg_tolerance": 1e-13,
+            **{k: list(v) for k, v in res.items()}}
+
+
 def error_cases():
     base = kat12()
 
@@ -159,6 +205,15 @@ def main() -> None:
         prep[name] = rec
         jla[name] = [solve_record(lib, panel, spec["probes"], 0), solve_record(lib, panel, spec["probes"], 1)]
         print(name, rec["retained"], jla[name][0]["corrected"])
+    controls = {}
+    for name, spec in CONTROL_PANELS.items():
+        panel = spec["build"]()
+        rec = prepare_record(lib, panel)
+        rec["rows"] = panel.rows
+        rec["panel_sha256"] = panel_digest(panel)
+        prep[name] = rec
+        controls[name] = [solve_record_v5(lib, panel, spec["probes"], 0), solve_record_v5(lib, panel, spec["probes"], 1)]
+        print(name, rec["retained"], controls[name][0]["corrected"])
     errs = {}
     for name, panel in error_cases().items():
         rec = prepare_record(lib, panel)
@@ -169,7 +224,7 @@ def main() -> None:
     meta = {"generator": "tests/golden/make_golden.py", "reference_plugin_version":
             lib.vckss_rust_backend_version().decode()}
     (HERE / "prep_cases.json").write_text(json.dumps({"meta": meta, "panels": prep, "errors": errs}, indent=1))
-    (HERE / "jla_cases.json").write_text(json.dumps({"meta": meta, "panels": jla}, indent=1))
+    (HERE / "jla_cases.json").write_text(json.dumps({"meta": meta, "panels": jla, "controls": controls}, indent=1))
 
 
 if __name__ == "__main__":

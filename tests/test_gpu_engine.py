@@ -63,6 +63,51 @@ def test_components_match_reference(lib, golden, name, which):
         assert rel(res[key], rec[key]) < COMPONENT_RTOL, (key, res[key], rec[key])
 
 
+def solve_v5(lib, panel, *, probes, centering=0, tol=1e-12, block=0, seed=8675309):
+    e = abi.Engine(lib)
+    e.prepare(panel)
+    if centering:
+        e.centering(centering)
+    e.device_options(block, 0)
+    q = e.default_request_v5()
+    v1 = q.v4.v3.v2.v1
+    v1.seed = seed
+    v1.probes = probes
+    v1.pcg_tolerance = tol
+    v1.maximum_iterations = 20000
+    q.v4.v3.v2.algorithm = 2
+    q.v4.v3.engine = 2
+    q.tolerance_supplied = 1
+    e.solve_v5(q, controls_count=len(panel.controls))
+    return e
+
+
+@pytest.mark.parametrize("name", list(make_golden.CONTROL_PANELS))
+@pytest.mark.parametrize("which", [0, 1])
+def test_components_with_controls_match_reference(lib, golden, name, which):
+    """Year controls through the generic estimator (reference generic_jla.rs,
+    V5 entry with engine = generic)."""
+    rec = golden["jla"]["controls"][name][which]
+    panel = make_golden.CONTROL_PANELS[name]["build"]()
+    e = solve_v5(lib, panel, probes=rec["probes"], centering=rec["centering"], seed=rec["seed"])
+    res = e.result()
+    e.release()
+    for key in ("plugin", "correction", "corrected", "numerical_mcse"):
+        assert rel(res[key], rec[key]) < COMPONENT_RTOL, (key, res[key], rec[key])
+
+
+def test_v1_refuses_controls(lib):
+    panel = make_golden.CONTROL_PANELS["controls_2k"]["build"]()
+    e = abi.Engine(lib)
+    e.prepare(panel)
+    req = e.default_request()
+    req.probes = 4
+    with pytest.raises(abi.EngineError) as err:
+        e.solve(req)
+    e.release()
+    assert err.value.code == 11
+
+
 @pytest.mark.parametrize("name", ["kat12", "small_2k", "weighted_1500"])
 def test_unit_detail_matches_oracle(lib, oracle_mod, name):
     panel = make_golden.PANELS[name]["build"]()

@@ -13,10 +13,13 @@ from fevc_b200.panel import Panel
 import make_golden
 
 
-@pytest.mark.parametrize("name", list(make_golden.PANELS))
+ALL_PANELS = {**make_golden.PANELS, **make_golden.CONTROL_PANELS}
+
+
+@pytest.mark.parametrize("name", list(ALL_PANELS))
 def test_panel_preparation_matches_reference(lib, golden, name):
     rec = golden["prep"]["panels"][name]
-    panel = make_golden.PANELS[name]["build"]()
+    panel = ALL_PANELS[name]["build"]()
     assert make_golden.panel_digest(panel) == rec["panel_sha256"], "panel generator drifted"
     e = abi.Engine(lib)
     e.prepare(panel)
