@@ -678,7 +678,7 @@ static VckssEnginePreparationReceiptV4 receipt_v4(uint64_t generation) {
   v2.firms = c.firms;
   v2.cells = c.cells;
   v2.deletion_units = p.deletion_mode == VCKSS_DELETION_OBSERVATION ? c.physical_total : c.deletion_units;
-  v2.target_strata = p.has_plan ? p.plan.tgt_cell.size() : c.exact_target_strata;
+  v2.target_strata = (p.has_plan && !p.plan.generic) ? p.plan.tgt_cell.size() : c.exact_target_strata;
   v2.memory_limit_bytes = p.memory_limit;
   v2.caller_copy_bytes = p.caller_copy;
   uint64_t resident = c.rows() * (4 * 6 + 8 * 3) + c.cells * (4 * 2 + 8 * 3);
