@@ -8,7 +8,7 @@ leverage adjustment, the target contraction and the four components.
   step re-runs the solve (``fevcb_engine_resolve_v1``); CUDA events on the
   library's stream bracket exactly K steps after W warm-up steps.
 * ``e2e``    the same metric through the plugin C ABI a caller uses: each step
-  is ``solve_v1`` + ``result_v1`` on a freshly prepared generation, so the
+  is ``solve_v5`` + ``result_v1`` on a freshly prepared generation, so the
   host->device upload of the prepared problem and the device->host result read
   are inside the timed region (host preparation is outside it and reported
   separately as ``prepare_s``; prepare + solve is the time-to-decomposition).
@@ -111,11 +111,24 @@ def build_panel(args):
     from fevc_b200.panel import named_panel
 
     panel = named_panel(args.workload, args.scale)
-    controls = len(panel.controls)
-    # The device engine runs the compressed (no-control, match-deletion) JLA
-    # estimator; year controls are not yet absorbed, so they are dropped here.
-    panel.controls = []
-    return panel, controls
+    return panel, len(panel.controls)
+
+
+def v5_request(engine, probes, tolerance, *, reference=False):
+    """A V5 solve request: JLA, match deletion, supplied tolerance.  With
+    controls the generic engine runs; the reference additionally selects its
+    production CMG_FULL_V2 route on all host cores."""
+    q = engine.default_request_v5()
+    v1 = q.v4.v3.v2.v1
+    v1.probes = probes
+    v1.pcg_tolerance = tolerance
+    v1.maximum_iterations = 20000
+    q.v4.v3.v2.algorithm = 2
+    q.tolerance_supplied = 1
+    if reference:
+        q.threads = os.cpu_count() or 1
+        q.full_cmg_v2 = 1
+    return q
 
 
 def reference_plugin_path():
@@ -135,14 +148,8 @@ def time_reference(panel, probes, tolerance, steps, warmup):
         t0 = time.perf_counter()
         e.prepare(panel)
         t1 = time.perf_counter()
-        q = e.default_request_v5()
-        q.v4.v3.v2.v1.probes = probes
-        q.v4.v3.v2.algorithm = 2
-        q.v4.v3.v2.v1.pcg_tolerance = tolerance
-        q.threads = threads
-        q.full_cmg_v2 = 1
-        q.tolerance_supplied = 1
-        e.solve_v5(q)
+        q = v5_request(e, probes, tolerance, reference=True)
+        e.solve_v5(q, controls_count=len(panel.controls))
         res = e.result()
         t2 = time.perf_counter()
         e.release()
@@ -179,7 +186,7 @@ def run_reference(args):
             "ms_per_step": round(1000 * r["solve_s"], 2), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, fevc_b200/panel.py)",
             "config": {"workload": f"{args.workload} panel, {probes}-probe sample", "probes": probes,
-                       "tolerance": args.tolerance, "year_controls_dropped": controls},
+                       "tolerance": args.tolerance, "controls": controls},
             "prepare_s": round(r["prepare_s"], 3),
             "cpu_baseline": {"value": round(r["rhs_per_s"], 4), "unit": UNIT, "cores": r["threads"],
                              "kind": "reference", "sample": f"{probes} probes ({1 + 3 * probes} RHS) per step"},
@@ -224,12 +231,9 @@ def main():
     e.prepare(panel)
     prepare_s = time.perf_counter() - t0
     e.device_options(args.block, args.precond)
-    req = e.default_request()
-    req.probes = args.probes
-    req.pcg_tolerance = args.tolerance
-    req.maximum_iterations = 20000
+    req = v5_request(e, args.probes, args.tolerance)
     t0 = time.perf_counter()
-    e.solve(req)
+    e.solve_v5(req, controls_count=controls)
     torch.cuda.synchronize()
     first_solve_s = time.perf_counter() - t0
     result = e.result()
@@ -275,7 +279,7 @@ def main():
         g.device_options(args.block, args.precond)
         barrier()
         t0 = time.perf_counter()
-        g.solve(req)
+        g.solve_v5(req, controls_count=controls)
         g.result()
         torch.cuda.synchronize()
         t1 = time.perf_counter()
@@ -301,10 +305,10 @@ def main():
             "data": "synthetic (seeded generator, fevc_b200/panel.py)",
             "config": {"workload": f"{args.workload} panel ({panel.info['workers']} workers, "
                                    f"{panel.info['firms']} firms, {panel.info['periods']} periods), "
-                                   f"{args.probes} probes, compressed JLA, match deletion",
+                                   f"{args.probes} probes, {controls} year controls, match deletion",
                        "probes": args.probes, "rhs_per_step": rhs, "tolerance": args.tolerance,
                        "block_columns": block, "preconditioner": "jacobi" if args.precond == 1 else "auto",
-                       "year_controls_dropped": controls, "parallelism": f"replicas x{world}",
+                       "controls": controls, "parallelism": f"replicas x{world}",
                        "l2": "working set per step larger than L2 (126 MB)",
                        "retained": {"workers": int(timings["vertices"]) and None}},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
