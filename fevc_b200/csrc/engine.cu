@@ -517,7 +517,8 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   e->omega.alloc(e->C);
   e->fitted.alloc(e->C);
   e->fit_alpha.alloc(e->W);
-  e->partial.alloc(size_t(grid_blocks()) * 4 * 128 + 1024);
+  // per-block partials: at most QMAX*K (K <= 64) or 64 values per block
+  e->partial.alloc(size_t(grid_blocks()) * QMAX * 128 + 1024);
   e->small.alloc(1024);
   e->error.alloc(1);
   CK(cudaMallocHost(&e->h_nactive, sizeof(int) * 16));
@@ -560,7 +561,8 @@ BlockWork& get_work(DeviceEngine& e) {
   w->cell_val.alloc(size_t(e.C) * K);
   w->unit_atoms.alloc(size_t(e.G) * K);
   w->dir.alloc(size_t(e.C) * (K > 1 ? K / 2 : 1));
-  w->tot.alloc(4 * K);
+  // finished reductions: at most QMAX*K (target control sums) or 4*K values
+  w->tot.alloc(size_t(QMAX + 4) * K);
   w->seg_buf.alloc(size_t(e.lap_seg.count) * K);
   w->fseg_out.alloc(size_t(e.firm_seg.count) * K);
   w->st.alloc(8 * K);
