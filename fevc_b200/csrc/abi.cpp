@@ -83,6 +83,7 @@ struct Prepared {
   uint32_t controls = 0;
   Centering centering = Centering::None;
   FevcbSolveOptionsV1 device_options{sizeof(FevcbSolveOptionsV1), 0, 0, 0};
+  std::vector<double> control_values;  // contiguous copy for the problem view
   std::shared_ptr<DeviceEngine> device;
   SolveOptions last_options;
   bool solved_once = false;
@@ -992,6 +993,12 @@ int32_t fevcb_engine_problem_view_v1(uint64_t generation, FevcbProblemViewV1* ou
     v.stratum_per_copy = j.tgt_per_copy.data();
     v.stratum_count = j.tgt_count.data();
     v.stratum_rank = j.tgt_rank.data();
+    v.controls = c.controls.size();
+    if (!c.controls.empty() && p.control_values.empty())
+      for (auto& col : c.controls) p.control_values.insert(p.control_values.end(), col.begin(), col.end());
+    v.control_values = p.control_values.empty() ? nullptr : p.control_values.data();
+    v.group_ptr = j.generic ? j.group_ptr.data() : nullptr;
+    v.group_rows = j.generic ? j.group_rows.data() : nullptr;
     std::memcpy(out, &v, sizeof(v));
   });
 }

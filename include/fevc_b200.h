@@ -470,6 +470,10 @@ typedef struct FevcbProblemViewV1 {
   const uint32_t *stratum_cell;
   const double *stratum_per_copy;
   const uint64_t *stratum_count, *stratum_rank;
+  uint64_t controls;                 /* control columns (generic plan) */
+  const double *control_values;      /* rows x controls, column-major */
+  const uint64_t *group_ptr;         /* generic plan: rows of each deletion unit ... */
+  const uint32_t *group_rows;        /* ... in semantic-rank order */
 } FevcbProblemViewV1;
 int32_t fevcb_engine_problem_view_v1(uint64_t generation, FevcbProblemViewV1 *output, uint32_t output_capacity_bytes);
 

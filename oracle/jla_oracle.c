@@ -16,6 +16,10 @@
  *                  transpose, balance repair), 3003-3101 (contraction)
  *   mean / MCSE    rust/crates/vckss-core/src/engine.rs:3108-3200
  *   centering mean rust/crates/vckss-core/src/centering.rs:6-27
+ *   generic (controls, match deletion, joint nuisance): control geometry
+ *                  generic_jla.rs:4407-4537, deleted adjustment 6053-6196,
+ *                  target correction 8554-8900, target draw
+ *                  generic_jla/statistical_batches.rs:259-347
  * Linear solves use the firm Schur complement on the zero-sum quotient: a
  * dense grounded Cholesky factor when the firm count is small, otherwise
  * Jacobi-preconditioned CG to a tight tolerance.
@@ -101,6 +105,10 @@ typedef struct {
   const uint32_t* stratum_cell;
   const double* stratum_per_copy;
   const uint64_t *stratum_count, *stratum_rank;
+  uint64_t controls;
+  const double* control_values; /* rows x controls, column-major */
+  const uint64_t* group_ptr;
+  const uint32_t* group_rows;
 } OracleProblem;
 
 typedef struct {
@@ -486,6 +494,326 @@ int oracle_jla(const OracleProblem* p, const OracleOptions* o, OracleResult* res
   free(psi);
   free(alpha2);
   free(psi2);
+  solver_free(&s);
+  return 0;
+}
+
+/* ------------------------------------------------------------ generic path */
+
+static int dense_cholesky(double* a, int n) {
+  for (int j = 0; j < n; ++j) {
+    double d = a[j * n + j];
+    for (int k = 0; k < j; ++k) d -= a[j * n + k] * a[j * n + k];
+    if (!(d > 0.0)) return -1;
+    d = sqrt(d);
+    a[j * n + j] = d;
+    for (int i = j + 1; i < n; ++i) {
+      double v = a[i * n + j];
+      for (int k = 0; k < j; ++k) v -= a[i * n + k] * a[j * n + k];
+      a[i * n + j] = v / d;
+    }
+    for (int k = j + 1; k < n; ++k) a[j * n + k] = 0.0;
+  }
+  return 0;
+}
+
+static void dense_solve(const double* l, int n, double* b) {
+  for (int i = 0; i < n; ++i) {
+    double v = b[i];
+    for (int k = 0; k < i; ++k) v -= l[i * n + k] * b[k];
+    b[i] = v / l[i * n + i];
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double v = b[i];
+    for (int k = i + 1; k < n; ++k) v -= l[k * n + i] * b[k];
+    b[i] = v / l[i * n + i];
+  }
+}
+
+/* Generic estimator: year controls through the FWL block, match deletion,
+ * joint nuisance.  result->target_draws hold (worker, firm, covariance,
+ * total) per probe; per-unit arrays are not filled. */
+int oracle_jla_generic(const OracleProblem* p, const OracleOptions* o, OracleResult* res) {
+  uint64_t W = p->workers, F = p->firms, C = p->cells, G = p->units, S = p->strata, P = o->probes, R = p->rows;
+  int q = (int)p->controls;
+  Solver s;
+  res->error_code = 0;
+  if (q < 1 || !p->group_ptr) return set_error(res, 11, "the generic oracle needs controls and match groups");
+  if (solver_init(&s, p, o)) return set_error(res, 82, "grounded Schur factor is not positive definite");
+  double *bw = calloc(W, 8), *bf = calloc(F, 8), *alpha = calloc(W, 8), *psi = calloc(F, 8);
+  double *alpha2 = calloc(W, 8), *psi2 = calloc(F, 8);
+  double *aH = calloc(W * q, 8), *pH = calloc(F * q, 8), *Rr = calloc(R * q, 8);
+  const double* Q = p->control_values;
+  /* H = (X'WX)^+ X'WQ, one FE solve per control column */
+  for (int k = 0; k < q; ++k) {
+    memset(bw, 0, W * 8);
+    memset(bf, 0, F * 8);
+    for (uint64_t r = 0; r < R; ++r) {
+      double v = (double)p->row_frequency[r] * Q[k * R + r];
+      bw[p->row_worker[r]] += v;
+      bf[p->row_firm[r]] += v;
+    }
+    solve(&s, bw, bf, alpha, psi);
+    for (uint64_t w = 0; w < W; ++w) aH[w * q + k] = alpha[w];
+    for (uint64_t f = 0; f < F; ++f) pH[f * q + k] = psi[f];
+  }
+  /* residualised controls, S = R'WR, S^{-1}, lower factor of S^{-1} */
+  double Sm[64] = {0}, Si[64] = {0}, Lf[64];
+  for (uint64_t r = 0; r < R; ++r) {
+    double f = (double)p->row_frequency[r];
+    for (int k = 0; k < q; ++k)
+      Rr[r * q + k] = Q[k * R + r] - (aH[p->row_worker[r] * q + k] + pH[p->row_firm[r] * q + k]);
+    for (int i = 0; i < q; ++i)
+      for (int j = 0; j < q; ++j) Sm[i * q + j] += f * Rr[r * q + i] * Rr[r * q + j];
+  }
+  double Lc[64];
+  memcpy(Lc, Sm, sizeof(Lc));
+  if (dense_cholesky(Lc, q)) return set_error(res, 82, "residualised control information is singular");
+  for (int c = 0; c < q; ++c) {
+    double b[8] = {0};
+    b[c] = 1.0;
+    dense_solve(Lc, q, b);
+    for (int i = 0; i < q; ++i) Si[i * q + c] = b[i];
+  }
+  memcpy(Lf, Si, sizeof(Lf));
+  if (dense_cholesky(Lf, q)) return set_error(res, 76, "control inverse square root failed");
+  /* joint fit */
+  memset(bw, 0, W * 8);
+  memset(bf, 0, F * 8);
+  for (uint64_t c = 0; c < C; ++c) {
+    bw[p->cell_worker[c]] += p->cell_outcome_sum[c];
+    bf[p->cell_firm[c]] += p->cell_outcome_sum[c];
+  }
+  solve(&s, bw, bf, alpha, psi);
+  double ry[8] = {0}, beta[8] = {0};
+  for (uint64_t r = 0; r < R; ++r)
+    for (int k = 0; k < q; ++k) ry[k] += (double)p->row_frequency[r] * Rr[r * q + k] * p->row_outcome[r];
+  for (int k = 0; k < q; ++k)
+    for (int l = 0; l < q; ++l) beta[k] += Si[k * q + l] * ry[l];
+  for (uint64_t w = 0; w < W; ++w)
+    for (int k = 0; k < q; ++k) alpha[w] -= aH[w * q + k] * beta[k];
+  for (uint64_t f = 0; f < F; ++f)
+    for (int k = 0; k < q; ++k) psi[f] -= pH[f * q + k] * beta[k];
+  double* resid = calloc(R, 8);
+  for (uint64_t r = 0; r < R; ++r) {
+    double fit = alpha[p->row_worker[r]] + psi[p->row_firm[r]];
+    for (int k = 0; k < q; ++k) fit += Q[k * R + r] * beta[k];
+    resid[r] = p->row_outcome[r] - fit;
+  }
+  {
+    /* plug-in over cells with cell target sums (generic_jla.rs:3735-3776) */
+    Stable wm = {0, 0}, fm = {0, 0};
+    for (uint64_t c = 0; c < C; ++c) {
+      st_add(&wm, p->cell_target_sum[c] * alpha[p->cell_worker[c]]);
+      st_add(&fm, p->cell_target_sum[c] * psi[p->cell_firm[c]]);
+    }
+    double mw = st_fin(&wm) / p->target_total, mf = st_fin(&fm) / p->target_total;
+    Stable a = {0, 0}, b = {0, 0}, cv = {0, 0}, t = {0, 0};
+    for (uint64_t c = 0; c < C; ++c) {
+      double x = alpha[p->cell_worker[c]] - mw, y = psi[p->cell_firm[c]] - mf, wt = p->cell_target_sum[c];
+      st_add(&a, wt * x * x);
+      st_add(&b, wt * y * y);
+      st_add(&cv, wt * x * y);
+      st_add(&t, wt * (x + y) * (x + y));
+    }
+    res->plugin[0] = st_fin(&a) / p->target_total;
+    res->plugin[1] = st_fin(&b) / p->target_total;
+    res->plugin[2] = st_fin(&cv) / p->target_total;
+    res->plugin[3] = st_fin(&t) / p->target_total;
+  }
+  /* FE-only leverage moments */
+  Stable* mom = calloc(G * 5, sizeof(Stable));
+  for (uint64_t probe = 0; probe < P; ++probe) {
+    memset(bw, 0, W * 8);
+    memset(bf, 0, F * 8);
+    int64_t* at = calloc(G, sizeof(int64_t));
+    for (uint64_t g = 0; g < G; ++g) {
+      int ok;
+      at[g] = oracle_rademacher_sum(o->seed, TAG_LEVERAGE, probe, p->unit_rank[g], p->unit_count[g], &ok);
+      uint32_t c = p->unit_cell[g];
+      bw[p->cell_worker[c]] += (double)at[g];
+      bf[p->cell_firm[c]] += (double)at[g];
+    }
+    solve(&s, bw, bf, alpha2, psi2);
+    for (uint64_t g = 0; g < G; ++g) {
+      uint32_t c = p->unit_cell[g];
+      double rn = sqrt((double)p->unit_count[g]);
+      double pr = rn * (alpha2[p->cell_worker[c]] + psi2[p->cell_firm[c]]);
+      double m = (double)at[g] / rn - pr, p2 = pr * pr, m2 = m * m;
+      st_add(&mom[g * 5 + 0], p2);
+      st_add(&mom[g * 5 + 1], m2);
+      st_add(&mom[g * 5 + 2], p2 * p2);
+      st_add(&mom[g * 5 + 3], m2 * m2);
+      st_add(&mom[g * 5 + 4], p2 * m2);
+    }
+    free(at);
+  }
+  /* deleted residuals per match group: (I - V V') X = [sqrt(f) e, common] */
+  double* deleted = calloc(R, 8);
+  double Pd = (double)P;
+  for (uint64_t g = 0; g < G; ++g) {
+    double pf = st_fin(&mom[g * 5 + 0]), mf = st_fin(&mom[g * 5 + 1]);
+    double tm = (pf + mf) / Pd;
+    if (!(tm > o->block_tolerance)) return set_error(res, 74, "projection/residual mass failed");
+    double proj = (pf / Pd) / tm, rs = (mf / Pd) / tm;
+    double p4 = st_fin(&mom[g * 5 + 2]) / Pd, m4 = st_fin(&mom[g * 5 + 3]) / Pd, mx = st_fin(&mom[g * 5 + 4]) / Pd;
+    double bias = (rs * p4 - proj * m4 + (rs - proj) * mx) / Pd;
+    double var = (rs * rs * p4 + proj * proj * m4 - 2.0 * proj * rs * mx) / Pd;
+    if (var < 0) var = 0;
+    uint64_t b = p->group_ptr[g], e = p->group_ptr[g + 1];
+    int width = (int)(e - b), rank = 1 + q;
+    double* V = calloc((size_t)width * rank, 8);
+    double* A = calloc((size_t)width * width, 8);
+    double *x0 = calloc(width, 8), *x1 = calloc(width, 8), *cm = calloc(width, 8);
+    double n = (double)p->unit_count[g];
+    for (int l = 0; l < width; ++l) {
+      uint32_t r = p->group_rows[b + l];
+      double root = sqrt((double)p->row_frequency[r]);
+      cm[l] = root / sqrt(n);
+      V[l * rank] = sqrt(proj) * cm[l];
+      for (int oo = 0; oo < q; ++oo) {
+        double v = 0;
+        for (int in = 0; in < q; ++in) v += Rr[r * q + in] * Lf[in * q + oo];
+        V[l * rank + 1 + oo] = root * v;
+      }
+      x0[l] = root * resid[r];
+      x1[l] = cm[l];
+    }
+    for (int i = 0; i < width; ++i)
+      for (int j = 0; j < width; ++j) {
+        double v = i == j ? 1.0 : 0.0;
+        for (int k = 0; k < rank; ++k) v -= V[i * rank + k] * V[j * rank + k];
+        A[i * width + j] = v;
+      }
+    if (dense_cholesky(A, width)) return set_error(res, 75, "a match residual block is singular");
+    dense_solve(A, width, x0);
+    dense_solve(A, width, x1);
+    double ct = 0, ci = 0;
+    for (int l = 0; l < width; ++l) {
+      ct += cm[l] * x0[l];
+      ci += cm[l] * x1[l];
+    }
+    for (int l = 0; l < width; ++l) deleted[p->group_rows[b + l]] = x0[l] + bias * x1[l] * ct - var * x1[l] * ci * ct;
+    free(V);
+    free(A);
+    free(x0);
+    free(x1);
+    free(cm);
+  }
+  double mean = 0.0;
+  if (o->centering == 1) {
+    double anchor = p->row_outcome[0];
+    Stable sm = {0, 0};
+    for (uint64_t r = 0; r < R; ++r)
+      st_add(&sm, (p->row_outcome[r] - anchor) * ((double)p->row_frequency[r] / (double)p->physical_total));
+    mean = anchor + st_fin(&sm);
+  }
+  /* target draws on the full model */
+  Stable* dir = calloc(C, sizeof(Stable));
+  double *d = calloc(C, 8), *sw = calloc(W, 8), *sf = calloc(F, 8), *zw = calloc(W, 8), *zf = calloc(F, 8);
+  for (uint64_t probe = 0; probe < P; ++probe) {
+    memset(dir, 0, C * sizeof(Stable));
+    for (uint64_t k = 0; k < S; ++k) {
+      int ok;
+      int64_t a = oracle_rademacher_sum(o->seed, TAG_TARGET, probe, p->stratum_rank[k], p->stratum_count[k], &ok);
+      st_add(&dir[p->stratum_cell[k]], sqrt(p->stratum_per_copy[k] / p->target_total) * (double)a);
+    }
+    Stable tot = {0, 0};
+    for (uint64_t c = 0; c < C; ++c) {
+      d[c] = st_fin(&dir[c]);
+      st_add(&tot, d[c]);
+    }
+    double total = st_fin(&tot);
+    for (uint64_t c = 0; c < C; ++c) d[c] -= p->cell_target_sum[c] / p->target_total * total;
+    memset(sw, 0, W * 8);
+    memset(sf, 0, F * 8);
+    for (uint64_t c = 0; c < C; ++c) {
+      sw[p->cell_worker[c]] += d[c];
+      sf[p->cell_firm[c]] += d[c];
+    }
+    Stable pre = {0, 0};
+    for (uint64_t i = 0; i + 1 < W; ++i) st_add(&pre, sw[i]);
+    sw[W - 1] = -st_fin(&pre);
+    Stable pre2 = {0, 0};
+    for (uint64_t i = 0; i + 1 < F; ++i) st_add(&pre2, sf[i]);
+    sf[F - 1] = -st_fin(&pre2);
+    memset(zw, 0, W * 8);
+    memset(zf, 0, F * 8);
+    solve(&s, sw, zf, alpha, psi);
+    solve(&s, zw, sf, alpha2, psi2);
+    double bW[8] = {0}, bF[8] = {0};
+    for (uint64_t r = 0; r < R; ++r) {
+      double fr = (double)p->row_frequency[r];
+      double uw = alpha[p->row_worker[r]] + psi[p->row_firm[r]], uf = alpha2[p->row_worker[r]] + psi2[p->row_firm[r]];
+      for (int k = 0; k < q; ++k) {
+        bW[k] += fr * Q[k * R + r] * uw;
+        bF[k] += fr * Q[k * R + r] * uf;
+      }
+    }
+    double betaW[8] = {0}, betaF[8] = {0};
+    for (int k = 0; k < q; ++k)
+      for (int l = 0; l < q; ++l) {
+        betaW[k] -= Si[k * q + l] * bW[l];
+        betaF[k] -= Si[k * q + l] * bF[l];
+      }
+    Stable out[3] = {{0, 0}, {0, 0}, {0, 0}};
+    for (uint64_t g = 0; g < G; ++g) {
+      Stable first[3] = {{0, 0}, {0, 0}, {0, 0}}, second[3] = {{0, 0}, {0, 0}, {0, 0}};
+      for (uint64_t i = p->group_ptr[g]; i < p->group_ptr[g + 1]; ++i) {
+        uint32_t r = p->group_rows[i];
+        double fr = (double)p->row_frequency[r];
+        double u[3];
+        u[0] = alpha[p->row_worker[r]] + psi[p->row_firm[r]];
+        u[1] = alpha2[p->row_worker[r]] + psi2[p->row_firm[r]];
+        for (int k = 0; k < q; ++k) {
+          u[0] += Rr[r * q + k] * betaW[k];
+          u[1] += Rr[r * q + k] * betaF[k];
+        }
+        u[2] = u[0] + u[1];
+        for (int t = 0; t < 3; ++t) {
+          st_add(&first[t], fr * (p->row_outcome[r] - mean) * u[t]);
+          st_add(&second[t], sqrt(fr) * deleted[r] * u[t]);
+        }
+      }
+      for (int t = 0; t < 3; ++t) st_add(&out[t], st_fin(&first[t]) * st_fin(&second[t]));
+    }
+    double ww = st_fin(&out[0]), ff = st_fin(&out[1]), tt = st_fin(&out[2]);
+    res->target_draws[probe * 4 + 0] = ww;
+    res->target_draws[probe * 4 + 1] = ff;
+    res->target_draws[probe * 4 + 2] = 0.5 * (tt - ww - ff);
+    res->target_draws[probe * 4 + 3] = tt;
+  }
+  for (int k = 0; k < 4; ++k) {
+    Stable m = {0, 0};
+    for (uint64_t pp = 0; pp < P; ++pp) st_add(&m, res->target_draws[pp * 4 + k]);
+    res->correction[k] = st_fin(&m) / Pd;
+    res->corrected[k] = res->plugin[k] - res->correction[k];
+    Stable v = {0, 0};
+    for (uint64_t pp = 0; pp < P; ++pp) {
+      double e = res->target_draws[pp * 4 + k] - res->correction[k];
+      st_add(&v, e * e);
+    }
+    res->mcse[k] = sqrt(st_fin(&v) / (Pd * (Pd - 1.0)));
+  }
+  res->cg_iterations = s.iterations;
+  free(bw);
+  free(bf);
+  free(alpha);
+  free(psi);
+  free(alpha2);
+  free(psi2);
+  free(aH);
+  free(pH);
+  free(Rr);
+  free(resid);
+  free(mom);
+  free(deleted);
+  free(dir);
+  free(d);
+  free(sw);
+  free(sf);
+  free(zw);
+  free(zf);
   solver_free(&s);
   return 0;
 }

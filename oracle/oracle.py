@@ -22,7 +22,8 @@ class OracleProblem(C.Structure):
         ("row_outcome", dp), ("row_target", dp), ("row_frequency", u64p), ("cell_worker", u32p),
         ("cell_firm", u32p), ("cell_weight", dp), ("cell_outcome_sum", dp), ("cell_target_sum", dp),
         ("unit_cell", u32p), ("unit_count", u64p), ("unit_rank", u64p), ("unit_outcome_sum", dp),
-        ("stratum_cell", u32p), ("stratum_per_copy", dp), ("stratum_count", u64p), ("stratum_rank", u64p)]
+        ("stratum_cell", u32p), ("stratum_per_copy", dp), ("stratum_count", u64p), ("stratum_rank", u64p),
+        ("controls", C.c_uint64), ("control_values", dp), ("group_ptr", u64p), ("group_rows", u32p)]
 
 
 class ProblemView(C.Structure):
@@ -52,6 +53,8 @@ def library() -> C.CDLL:
         _LIB = C.CDLL(str(_build.build()))
         _LIB.oracle_jla.restype = C.c_int
         _LIB.oracle_jla.argtypes = [C.POINTER(OracleProblem), C.POINTER(OracleOptions), C.POINTER(OracleResult)]
+        _LIB.oracle_jla_generic.restype = C.c_int
+        _LIB.oracle_jla_generic.argtypes = _LIB.oracle_jla.argtypes
         _LIB.oracle_rademacher_sum.restype = C.c_int64
         _LIB.oracle_rademacher_sum.argtypes = [C.c_uint64] * 5 + [C.POINTER(C.c_int)]
         _LIB.oracle_philox_block.restype = None
@@ -99,7 +102,8 @@ def run(problem: OracleProblem, *, seed=8675309, probes=200, centering=0, tolera
     for n, a in arrays.items():
         setattr(res, n, a.ctypes.data_as(dp))
     opt = OracleOptions(seed, probes, centering, tolerance, rank_tolerance, block_tolerance, dense_limit)
-    code = lib.oracle_jla(C.byref(problem), C.byref(opt), C.byref(res))
+    fn = lib.oracle_jla_generic if problem.controls else lib.oracle_jla
+    code = fn(C.byref(problem), C.byref(opt), C.byref(res))
     if code != 0:
         raise RuntimeError(f"oracle failed [{code}]: {res.error.decode()}")
     out = {k: np.array(getattr(res, k)[:]) for k in ("plugin", "correction", "corrected", "mcse")}

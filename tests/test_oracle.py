@@ -29,6 +29,22 @@ def test_oracle_matches_reference(lib, oracle_mod, golden, name, which):
         assert rel(out[okey], rec[key]) < 1e-11, (key, out[okey], rec[key])
 
 
+@pytest.mark.parametrize("name", list(make_golden.CONTROL_PANELS))
+@pytest.mark.parametrize("which", [0, 1])
+def test_generic_oracle_matches_reference(lib, oracle_mod, golden, name, which):
+    """The controlled (generic) estimator's restatement against the plugin."""
+    rec = golden["jla"]["controls"][name][which]
+    panel = make_golden.CONTROL_PANELS[name]["build"]()
+    e = abi.Engine(lib)
+    e.prepare(panel)
+    out = oracle_mod.run(oracle_mod.problem_view(lib, e.generation), seed=rec["seed"], probes=rec["probes"],
+                         centering=rec["centering"])
+    e.release()
+    for key, okey in (("plugin", "plugin"), ("correction", "correction"), ("corrected", "corrected"),
+                      ("numerical_mcse", "mcse")):
+        assert rel(out[okey], rec[key]) < 1e-10, (key, out[okey], rec[key])
+
+
 def test_kat_unit_detail(lib, oracle_mod):
     """Per-unit shares of the 12-row known-answer design sum to one and the
     cell weights are finite (reference rust_mata_shared_atoms.rs:108-194)."""
