@@ -350,9 +350,14 @@ class Engine:
     def solve(self, req: SolveRequestV1) -> None:
         self.check(self.lib.vckss_rust_engine_solve_v1(self.generation, C.byref(req)))
 
-    def default_request_v5(self) -> SolveRequestV5:
+    def default_request_v5(self, deletion_mode: int = 1) -> SolveRequestV5:
+        """The library's default V5 request; deletion_mode 2 also sets the
+        observation-row deletion-unit source its capability check requires."""
         req = SolveRequestV5()
         self.check(self.lib.vckss_rust_engine_default_solve_request_v5(C.byref(req), C.sizeof(req)))
+        if deletion_mode == 2:
+            req.v4.v3.v2.v1.deletion_mode = 2
+            req.v4.v3.deletion_unit_source = 3
         return req
 
     def solve_v5(self, req: SolveRequestV5, controls_count: int = 0) -> None:

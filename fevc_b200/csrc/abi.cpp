@@ -30,13 +30,13 @@ int32_t status(F&& f) {
     g_last_error = e.what();
     return e.code;
   } catch (const std::bad_alloc&) {
-    g_last_error = "host allocation failed";
+    g_last_error = "ALLOCATION_FAILED [host]: host allocation failed";
     return ALLOCATION_FAILED;
   } catch (const std::exception& e) {
-    g_last_error = std::string("contained exception: ") + e.what();
+    g_last_error = std::string("PANIC [ffi]: contained exception: ") + e.what();
     return PANIC;
   } catch (...) {
-    g_last_error = "contained unknown exception";
+    g_last_error = "PANIC [ffi]: contained unknown exception";
     return PANIC;
   }
 }
@@ -212,10 +212,11 @@ void prepare_common(const PrepareArgs& a, uint64_t* out, uint32_t cap) {
   a.interrupt.check("graph_final", a.rows);
   prep->problem = compress(canon, prep->retained, a.implicit_match != 0);
   a.interrupt.check("compression_final", a.rows);
-  if (a.deletion_mode == VCKSS_DELETION_MATCH) {
+  if (a.deletion_mode == VCKSS_DELETION_MATCH)
     prep->plan = prep->problem.controls.empty() ? build_plan(prep->problem) : build_generic_plan(prep->problem);
-    prep->has_plan = true;
-  }
+  else
+    prep->plan = build_generic_plan(prep->problem, Deletion::Observation);
+  prep->has_plan = true;
   prep->input_rows = a.rows;
   prep->memory_limit = a.memory_limit;
   prep->caller_copy = a.caller_copy;
@@ -232,9 +233,10 @@ void prepare_common(const PrepareArgs& a, uint64_t* out, uint32_t cap) {
   std::memcpy(out, &r.generation, 8);
 }
 
-SolveOptions options_from_v1(const VckssEngineSolveRequestV1& q) {
+SolveOptions options_from_v1(const VckssEngineSolveRequestV1& q, bool observation_allowed = false) {
   require_abi(q.abi_version);
-  if (q.deletion_mode != VCKSS_DELETION_MATCH)
+  if (q.deletion_mode != VCKSS_DELETION_MATCH &&
+      !(observation_allowed && q.deletion_mode == VCKSS_DELETION_OBSERVATION))
     fail(UNSUPPORTED_FEATURE, "jla_validate", "the compressed JLA engine supports match deletion only");
   if (q.rng_contract != VCKSS_RNG_COUNTER_V1)
     fail(UNSUPPORTED_FEATURE, "jla_validate", "the JLA engine supports VCKSS-COUNTER-V1 only");
@@ -260,6 +262,7 @@ SolveOptions options_from_v1(const VckssEngineSolveRequestV1& q) {
   o.residual_replacement_interval = q.residual_replacement_interval;
   o.rank_tolerance = q.rank_tolerance;
   o.block_tolerance = q.block_tolerance;
+  o.deletion_mode = q.deletion_mode;
   return o;
 }
 
@@ -273,6 +276,8 @@ void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr, bool generi
     fail(STALE_CONTEXT, "context_solve", "generation " + std::to_string(g) + " is not in the prepared state");
   if (!p.has_plan)
     fail(UNSUPPORTED_FEATURE, "engine_solve", "the compressed JLA solve requires a prepared no-control match plan");
+  if (o.deletion_mode != p.deletion_mode)
+    fail(INVALID_INPUT, "engine_solve", "solve deletion mode differs from the prepared graph mode");
   r.state = State::Solving;
   try {
     intr.check("jla_full_fit");
@@ -626,7 +631,7 @@ static SolveOptions options_from_v5(const VckssEngineSolveRequestV5& q) {
     fail(UNSUPPORTED_FEATURE, "engine_solve", "the exact estimator is not provided by the device engine");
   if (q.v4.v3.v2.nuisance_mode == VCKSS_NUISANCE_FIXED_OFFSET)
     fail(UNSUPPORTED_FEATURE, "engine_solve", "fixed-offset nuisance is not provided by the device engine");
-  SolveOptions o = options_from_v1(v1);
+  SolveOptions o = options_from_v1(v1, true);
   // Without a supplied tolerance the reference full-CMG route solves probes
   // at 1e-6 (vckss-core/src/full_cmg.rs:29,56-69); the device engine keeps the
   // request's fit tolerance for every right-hand side, which is never looser.
@@ -999,6 +1004,9 @@ int32_t fevcb_engine_problem_view_v1(uint64_t generation, FevcbProblemViewV1* ou
     v.control_values = p.control_values.empty() ? nullptr : p.control_values.data();
     v.group_ptr = j.generic ? j.group_ptr.data() : nullptr;
     v.group_rows = j.generic ? j.group_rows.data() : nullptr;
+    v.row_rank = j.generic ? j.row_rank.data() : nullptr;
+    v.row_copy_offset = j.observation ? j.row_copy_offset.data() : nullptr;
+    v.deletion_mode = p.deletion_mode;
     std::memcpy(out, &v, sizeof(v));
   });
 }

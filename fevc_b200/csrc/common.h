@@ -50,10 +50,55 @@ enum Code : int32_t {
   PANIC = 99,
 };
 
+// Status-code names as the plugin prints them (reference
+// vckss-core/src/error.rs:52-95).
+inline const char* code_name(int32_t c) {
+  switch (c) {
+    case OK: return "OK";
+    case USER_BREAK: return "USER_BREAK";
+    case ABI_MISMATCH: return "ABI_MISMATCH";
+    case UNSUPPORTED_FEATURE: return "UNSUPPORTED_FEATURE";
+    case INVALID_INPUT: return "INVALID_INPUT";
+    case INVALID_IDENTIFIER: return "INVALID_IDENTIFIER";
+    case INVALID_WEIGHT: return "INVALID_WEIGHT";
+    case INVALID_TARGET_WEIGHT: return "INVALID_TARGET_WEIGHT";
+    case GRAPH_EMPTY: return "GRAPH_EMPTY";
+    case GRAPH_UNIDENTIFIED: return "GRAPH_UNIDENTIFIED";
+    case GRAPH_CERTIFICATE_FAILED: return "GRAPH_CERTIFICATE_FAILED";
+    case RESOURCE_LIMIT: return "RESOURCE_LIMIT";
+    case ALLOCATION_FAILED: return "ALLOCATION_FAILED";
+    case CMG_SETUP_FAILED: return "CMG_SETUP_FAILED";
+    case CMG_APPLY_FAILED: return "CMG_APPLY_FAILED";
+    case PCG_CURVATURE_BREAKDOWN: return "PCG_BREAKDOWN_CURVATURE";
+    case PCG_PRECONDITIONER_BREAKDOWN: return "PCG_BREAKDOWN_PRECONDITIONER";
+    case PCG_STAGNATION: return "PCG_STAGNATION";
+    case PCG_MAX_ITERATIONS: return "PCG_MAXITER";
+    case FULL_RESIDUAL_FAILED: return "FULL_RESIDUAL_FAILED";
+    case RNG_CONTRACT_FAILED: return "RNG_CONTRACT_FAILED";
+    case CORRECTION_NONFINITE: return "CORRECTION_NONFINITE";
+    case ACCOUNTING_IDENTITY_FAILED: return "ACCOUNTING_IDENTITY_FAILED";
+    case JLA_MOMENT_FAILED: return "JLA_MOMENT_FAILED";
+    case JLA_CONSTRAINT_FAILED: return "JLA_CONSTRAINT_FAILED";
+    case NONESTIMABLE_DELETION: return "NONESTIMABLE_DELETION";
+    case BLOCK_INVERSE_FAILED: return "BLOCK_INVERSE_FAILED";
+    case TARGET_CENTERING_FAILED: return "TARGET_CENTERING_FAILED";
+    case TARGET_IDENTITY_FAILED: return "TARGET_IDENTITY_FAILED";
+    case NONFINITE_CORRECTED_TARGET: return "NONFINITE_CORRECTED_TARGET";
+    case STALE_CONTEXT: return "STALE_CONTEXT";
+    case CONTEXT_POISONED: return "CONTEXT_POISONED";
+    case SINGULAR_INFORMATION: return "SINGULAR_INFORMATION";
+    case INTERNAL_INVARIANT_FAILED: return "INTERNAL_INVARIANT_FAILED";
+    case PANIC: return "PANIC";
+    default: return "UNKNOWN";
+  }
+}
+
+// An error carries its status code; its text reads "NAME [phase]: message"
+// like the plugin's last-error string (reference error.rs:125-135).
 struct Error : std::runtime_error {
   int32_t code;
   Error(int32_t c, const std::string& phase, const std::string& msg)
-      : std::runtime_error(phase + ": " + msg), code(c) {}
+      : std::runtime_error(std::string(code_name(c)) + " [" + phase + "]: " + msg), code(c) {}
 };
 
 [[noreturn]] inline void fail(int32_t code, const char* phase, const std::string& msg) {

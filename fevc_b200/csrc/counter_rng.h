@@ -112,4 +112,26 @@ FEVCB_HD void rademacher_block_sums(PhiloxKey key, uint64_t tag, uint64_t probe_
   for (int l = 0; l < 4; ++l) out[l] = 2 * pos[l] - (int64_t)trials;
 }
 
+// Rademacher sums over the copy range [offset, offset + trials) of one entity:
+// copy c draws bit c % 64 of word c / 64 (+1 for a set bit, -1 otherwise),
+// for the four probes 4 * probe_block + lane.  offset = 0 reproduces
+// rademacher_block_sums.
+FEVCB_HD void rademacher_range_block_sums(PhiloxKey key, uint64_t tag, uint64_t probe_block, uint64_t entity,
+                                          uint64_t offset, uint64_t trials, int64_t out[4]) {
+  int64_t pos[4] = {0, 0, 0, 0};
+  uint64_t b[4];
+  uint64_t c = offset, end = offset + trials;
+  while (c < end) {
+    uint64_t word = c >> 6, lo = c & 63, hi = end - (word << 6);
+    if (hi > 64) hi = 64;
+    uint64_t mask = (hi == 64 ? ~uint64_t(0) : ((uint64_t(1) << hi) - 1)) & ~((uint64_t(1) << lo) - 1);
+    philox_block(key, entity, probe_block, word, tag, b);
+#pragma unroll
+    for (int l = 0; l < 4; ++l) pos[l] += popcount64(b[l] & mask);
+    c = (word << 6) + hi;
+  }
+#pragma unroll
+  for (int l = 0; l < 4; ++l) out[l] = 2 * pos[l] - (int64_t)trials;
+}
+
 }  // namespace fevcb

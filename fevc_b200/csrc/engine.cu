@@ -28,6 +28,7 @@
 #include "multigrid.h"
 #include "persistent.cuh"
 #include "generic.cuh"
+#include "observation.cuh"
 
 namespace fevcb {
 
@@ -226,6 +227,12 @@ struct DeviceEngine {
   DBuf<double> row_freq, row_y, Qd, Rd, alphaH, psiH, residual, deleted, beta_buf;
   bool controls_ready = false;
   std::vector<double> Sinv, Lfac;  // q x q, row-major
+  // leave-observation-out: rows are the units; per-row class rank and first
+  // copy number, physical copy offsets, and the probe accumulators
+  bool observation = false;
+  uint64_t physical = 0;
+  DBuf<uint64_t> unit_offset, row_rank_d, row_copy_offset, row_phys;
+  DBuf<double> obs_row_acc, obs_copy_acc, control_lev, obs_out;
   // solve-long buffers
   DBuf<double> moments, unit_out, omega, fitted, fit_alpha, partial, small;
   DBuf<unsigned long long> error;
@@ -397,8 +404,39 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     upload(e->firm_diag, fd, s, h2d);
   }
 
-  // units in cell order (stable within a cell: plan group order)
-  {
+  // units in cell order (stable within a cell: plan group order); for
+  // leave-observation-out every row is a unit, keyed by its class rank and
+  // the number of its first copy inside the class
+  if (plan.observation) {
+    e->observation = true;
+    size_t R = p.rows();
+    e->G = uint32_t(R);
+    std::vector<uint32_t> uptr(p.cells + 1, 0);
+    for (size_t r = 0; r < R; ++r) uptr[p.row_cell[r] + 1]++;
+    for (size_t c = 0; c < p.cells; ++c) uptr[c + 1] += uptr[c];
+    std::vector<uint32_t> cur(uptr.begin(), uptr.end() - 1), order(R);
+    for (size_t r = 0; r < R; ++r) order[cur[p.row_cell[r]]++] = uint32_t(r);
+    std::vector<uint64_t> urank(R), ucount(R), uoff(R), phys(R + 1, 0);
+    for (size_t i = 0; i < R; ++i) {
+      uint32_t r = order[i];
+      urank[i] = plan.row_rank[r];
+      ucount[i] = p.frequency[r];
+      uoff[i] = plan.row_copy_offset[r];
+    }
+    for (size_t r = 0; r < R; ++r) phys[r + 1] = phys[r] + p.frequency[r];
+    e->physical = phys[R];
+    upload(e->unit_ptr, uptr, s, h2d);
+    upload(e->unit_rank, urank, s, h2d);
+    upload(e->unit_count, ucount, s, h2d);
+    upload(e->unit_offset, uoff, s, h2d);
+    upload(e->row_rank_d, plan.row_rank, s, h2d);
+    upload(e->row_copy_offset, plan.row_copy_offset, s, h2d);
+    upload(e->row_phys, phys, s, h2d);
+    e->obs_row_acc.alloc(R * 4);
+    e->obs_copy_acc.alloc(size_t(e->physical) * 4);
+    e->control_lev.alloc(R);
+    e->obs_out.alloc(R * 2);
+  } else {
     std::vector<uint32_t> uptr(p.cells + 1, 0);
     for (uint32_t c : plan.del_cell) uptr[c + 1]++;
     for (size_t c = 0; c < p.cells; ++c) uptr[c + 1] += uptr[c];
@@ -449,8 +487,8 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   if (plan.generic) {
     e->generic = true;
     e->q = int(p.controls.size());
-    if (e->q < 1 || e->q > QMAX)
-      fail(UNSUPPORTED_FEATURE, "generic_jla", "the device engine handles between 1 and 8 control columns");
+    if (e->q < (plan.observation ? 0 : 1) || e->q > QMAX)
+      fail(UNSUPPORTED_FEATURE, "generic_jla", "the device engine handles at most 8 control columns");
     e->rows = uint32_t(p.rows());
     size_t R = p.rows();
     std::vector<double> freq(R), Q(R * e->q);
@@ -512,8 +550,10 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
       e->stats.levels = 1;
     }
   }
-  e->moments.alloc(size_t(e->G) * 5);
-  e->unit_out.alloc(size_t(e->G) * 6);
+  if (!e->observation) {
+    e->moments.alloc(size_t(e->G) * 5);
+    e->unit_out.alloc(size_t(e->G) * 6);
+  }
   e->omega.alloc(e->C);
   e->fitted.alloc(e->C);
   e->fit_alpha.alloc(e->W);
@@ -559,7 +599,7 @@ BlockWork& get_work(DeviceEngine& e) {
   w->q.alloc(n * K);
   w->alpha.alloc(size_t(e.W) * K);
   w->cell_val.alloc(size_t(e.C) * K);
-  w->unit_atoms.alloc(size_t(e.G) * K);
+  if (!e.observation) w->unit_atoms.alloc(size_t(e.G) * K);
   w->dir.alloc(size_t(e.C) * (K > 1 ? K / 2 : 1));
   // finished reductions: at most QMAX*K (target control sums) or 4*K values
   w->tot.alloc(size_t(QMAX + 4) * K);
@@ -839,14 +879,21 @@ void run_leverage(DeviceEngine& e, const SolveOptions& o, SolveResult& res, uint
   PhiloxKey key = philox_key(o.seed);
   for (uint32_t first = 0; first < o.probes; first += K) {
     int ncols = int(std::min<uint32_t>(K, o.probes - first));
-    k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p, key,
-                                                     TAG_LEVERAGE, first, ncols, w.unit_atoms.p, w.cell_val.p);
+    k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p,
+                                                     e.observation ? e.unit_offset.p : nullptr, key,
+                                                     TAG_LEVERAGE, first, ncols,
+                                                     e.observation ? nullptr : w.unit_atoms.p, w.cell_val.p);
     k_gather<K><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, w.cell_val.p, w.bW.p);
     firm_gather<K, 0, 0>(e, w, L, nullptr, w.cell_val.p, nullptr, 0.0, nullptr, nullptr, nullptr, w.bF.p, nullptr);
     res.timings.kernel_launches += 4;
     BlockOutcome bo = solve_block<K>(e, w, ncols, o, res.timings);
-    k_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.G, ncols, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
-                                              e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.moments.p);
+    if (e.observation)
+      k_obs_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.rows, ncols, e.row_cell.p, e.cell_worker.p, e.cell_firm.p,
+                                                    e.row_rank_d.p, e.row_copy_offset.p, e.row_phys.p, key, first,
+                                                    w.alpha.p, w.x.p, e.obs_row_acc.p, e.obs_copy_acc.p);
+    else
+      k_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.G, ncols, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
+                                                e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.moments.p);
     CK_LAUNCH();
     res.timings.kernel_launches += 1;
     for (int j = 0; j < ncols; ++j)
@@ -920,12 +967,14 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
     } else {
       // full-model solves: beta = -S^{-1} Q'W X theta_fe per column, then the
       // row-level contraction over match groups
-      std::vector<double> t(QMAX * K), beta(QMAX * K, 0.0);
-      k_target_control<K><<<L.grid, THREADS, 0, L.s>>>(e.rows, e.q, e.row_cell.p, e.cell_worker.p, e.cell_firm.p,
-                                                       e.row_freq.p, e.Qd.p, w.alpha.p, w.x.p, e.partial.p);
-      k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, QMAX * K, w.tot.p);
-      CK(cudaMemcpyAsync(t.data(), w.tot.p, QMAX * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
-      CK(cudaStreamSynchronize(L.s));
+      std::vector<double> t(QMAX * K, 0.0), beta(QMAX * K, 0.0);
+      if (e.q > 0) {
+        k_target_control<K><<<L.grid, THREADS, 0, L.s>>>(e.rows, e.q, e.row_cell.p, e.cell_worker.p, e.cell_firm.p,
+                                                         e.row_freq.p, e.Qd.p, w.alpha.p, w.x.p, e.partial.p);
+        k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, QMAX * K, w.tot.p);
+        CK(cudaMemcpyAsync(t.data(), w.tot.p, QMAX * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+        CK(cudaStreamSynchronize(L.s));
+      }
       for (int k = 0; k < e.q; ++k)
         for (int j = 0; j < K; ++j) {
           double v = 0.0;
@@ -933,10 +982,15 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
           beta[k * K + j] = v;
         }
       CK(cudaMemcpyAsync(e.beta_buf.p, beta.data(), QMAX * K * sizeof(double), cudaMemcpyHostToDevice, L.s));
-      k_generic_contract<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.q, e.group_ptr.p, e.group_rows.p, e.row_cell.p,
-                                                         e.cell_worker.p, e.cell_firm.p, e.row_freq.p, e.row_y.p,
-                                                         y_center, e.deleted.p, e.Rd.p, e.beta_buf.p, w.alpha.p,
-                                                         w.x.p, e.partial.p);
+      if (e.observation)
+        k_generic_contract<K, true><<<L.grid, THREADS, 0, L.s>>>(
+            e.rows, e.q, nullptr, nullptr, e.row_cell.p, e.cell_worker.p, e.cell_firm.p, e.row_freq.p, e.row_y.p,
+            y_center, e.deleted.p, e.Rd.p, e.beta_buf.p, w.alpha.p, w.x.p, e.partial.p);
+      else
+        k_generic_contract<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.q, e.group_ptr.p, e.group_rows.p, e.row_cell.p,
+                                                           e.cell_worker.p, e.cell_firm.p, e.row_freq.p, e.row_y.p,
+                                                           y_center, e.deleted.p, e.Rd.p, e.beta_buf.p, w.alpha.p,
+                                                           w.x.p, e.partial.p);
       k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 2 * K, w.tot.p);
       std::vector<double> g2(2 * K);
       CK(cudaMemcpyAsync(g2.data(), w.tot.p, 2 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
@@ -1123,6 +1177,12 @@ bool host_cholesky(std::vector<double>& a, int n) {
 // its lower factor (reference `control_geometry`, generic_jla.rs:4407-4537).
 void setup_controls(DeviceEngine& e, const SolveOptions& o, SolveTimings& tm) {
   if (e.controls_ready) return;
+  if (e.q == 0) {  // leave-observation-out without controls: no geometry
+    e.Sinv.clear();
+    e.Lfac.clear();
+    e.controls_ready = true;
+    return;
+  }
   Launch L{grid_blocks(), e.stream};
   BlockWork& w8 = get_work<8>(e);
   const int q = e.q;
@@ -1221,9 +1281,46 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     res.timings.kernel_launches += 12;
   }
   auto t1 = now();
-  // ---- FE-only leverage probes (reference `match_leverage_moments`)
-  CK(cudaMemsetAsync(e.moments.p, 0, e.moments.bytes(), L.s));
+  // ---- FE-only leverage probes (reference `match_leverage_moments`,
+  // `observation_and_match_leverage_moments`)
+  if (e.observation) {
+    CK(cudaMemsetAsync(e.obs_row_acc.p, 0, e.obs_row_acc.bytes(), L.s));
+    CK(cudaMemsetAsync(e.obs_copy_acc.p, 0, e.obs_copy_acc.bytes(), L.s));
+  } else {
+    CK(cudaMemsetAsync(e.moments.p, 0, e.moments.bytes(), L.s));
+  }
   run_leverage<K>(e, o, res, 0);
+  if (e.observation) {
+    // ---- deleted residual of every row from its copies
+    unsigned long long init = ~0ull;
+    CK(cudaMemcpyAsync(e.error.p, &init, sizeof(init), cudaMemcpyHostToDevice, L.s));
+    if (q > 0) {
+      SmallMatrix sinv{};
+      for (int i = 0; i < q; ++i)
+        for (int j = 0; j < q; ++j) sinv.m[i * QMAX + j] = e.Sinv[i * q + j];
+      k_control_leverage<<<L.grid, THREADS, 0, L.s>>>(e.rows, q, e.Rd.p, sinv, o.rank_tolerance, e.control_lev.p,
+                                                      e.error.p);
+      res.timings.kernel_launches += 1;
+    }
+    ObservationAdjustParams prm{e.rows, double(o.probes), o.block_tolerance, o.rank_tolerance};
+    k_obs_adjust<<<L.grid, THREADS, 0, L.s>>>(prm, e.row_phys.p, e.obs_row_acc.p, e.obs_copy_acc.p,
+                                              q > 0 ? e.control_lev.p : nullptr, e.residual.p, e.deleted.p,
+                                              e.obs_out.p, e.error.p);
+    unsigned long long err = 0;
+    CK(cudaMemcpyAsync(&err, e.error.p, sizeof(err), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    res.timings.kernel_launches += 1;
+    if (err != ~0ull) {
+      uint32_t code = uint32_t(err & 0xff);
+      uint64_t row = err >> 8;
+      const char* what = code == JLA_CONSTRAINT_FAILED   ? "projection and residual masses are not positive"
+                         : code == NONESTIMABLE_DELETION ? "estimated residual leverage is nonpositive"
+                         : code == BLOCK_INVERSE_FAILED  ? "finite-projection observation inverse is nonpositive"
+                         : code == CORRECTION_NONFINITE  ? "observation deleted residual is nonfinite"
+                                                         : "finite-projection moment failed";
+      fail(int32_t(code), "generic_jla_observation_adjustment", std::string(what) + " at row " + std::to_string(row));
+    }
+  } else {
   // ---- deleted residuals of every match group
   {
     GenericAdjustParams prm{};
@@ -1251,6 +1348,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
                                                          : "finite-projection moment failed";
       fail(int32_t(code), "generic_jla_leverage", std::string(what) + " at unit " + std::to_string(g));
     }
+  }
   }
   auto t2 = now();
   // ---- target draws on the full model
@@ -1346,8 +1444,16 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
       // x and r read and written, p read and written
       *bytes = iters * (nnz * 12 + nseg * 12 + n * (4 + 4 + 8 + 8 + 8) + n * K * 8.0 * 9 + 2 * nseg * K * 8.0);
       break;
-    case 3: *bytes = double(e.G) * (8 + 8 + K * 8) + double(e.C) * (4 + K * 8); break;
-    case 4: *bytes = double(e.G) * (4 + 8 + K * 8 + 5 * 8 * 2) + double(e.G) * 2 * K * 8 + double(e.C) * 8; break;
+    case 3:
+      *bytes = double(e.G) * (8 + 8 + (e.observation ? 8 : K * 8)) + double(e.C) * (4 + K * 8);
+      break;
+    case 4:
+      if (e.observation)  // per row: cell, offsets, rank, two coefficient rows, row sums; per copy: its sums
+        *bytes = double(e.rows) * (4 + 8 + 8 + 8 + 2 * K * 8 + 4 * 8 * 2) + double(e.physical) * 4 * 8 * 2 +
+                 double(e.C) * 8;
+      else
+        *bytes = double(e.G) * (4 + 8 + K * 8 + 5 * 8 * 2) + double(e.G) * 2 * K * 8 + double(e.C) * 8;
+      break;
     default: fail(INVALID_INPUT, "benchmark", "unknown kernel id");
   }
   float total = 0.0f;
@@ -1390,12 +1496,19 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
         break;
       }
       case 3:
-        k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p, key,
-                                                         TAG_LEVERAGE, 0, K, w.unit_atoms.p, w.cell_val.p);
+        k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p,
+                                                     e.observation ? e.unit_offset.p : nullptr, key,
+                                                         TAG_LEVERAGE, 0, K,
+                                                         e.observation ? nullptr : w.unit_atoms.p, w.cell_val.p);
         break;
       case 4:
-        k_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.G, K, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
-                                                  e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.moments.p);
+        if (e.observation)
+          k_obs_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.rows, K, e.row_cell.p, e.cell_worker.p, e.cell_firm.p,
+                                                        e.row_rank_d.p, e.row_copy_offset.p, e.row_phys.p, key, 0,
+                                                        w.alpha.p, w.x.p, e.obs_row_acc.p, e.obs_copy_acc.p);
+        else
+          k_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.G, K, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
+                                                    e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.moments.p);
         break;
     }
     CK(cudaEventRecord(e.ev1, L.s));

@@ -28,6 +28,7 @@ struct SolveOptions {
   Centering centering = Centering::None;
   int block_columns = 0;      // device RHS block width (0 = automatic)
   int preconditioner = 0;     // 0 automatic, 1 Jacobi, 2 aggregation multigrid
+  uint32_t deletion_mode = 1;  // 1 match, 2 observation (must equal the prepared mode)
 };
 
 // One receipt per solved right-hand side (reference `JlaRhsReceipt`,

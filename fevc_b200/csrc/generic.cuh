@@ -320,7 +320,10 @@ __global__ void k_target_control(uint32_t rows, int q, const uint32_t* __restric
 // draw_t += first_t * second_t, with u_t(r) = u_fe,t(cell) + R_r' beta_t for the
 // worker side t = 2j, the firm side 2j+1 and their sum (the total).
 // partial[blk][0][K]: worker (even) / firm (odd) draw; [1][K]: total (even columns).
-template <int K>
+// OBS: leave-observation-out, every row its own unit and the draw adds
+// f y d u^2 (reference `target_contraction`, generic_jla.rs:8926-8937);
+// group_ptr and group_rows are then unused and `groups` counts rows.
+template <int K, bool OBS = false>
 __global__ void k_generic_contract(uint32_t groups, int q, const uint64_t* __restrict__ group_ptr,
                                    const uint32_t* __restrict__ group_rows, const uint32_t* __restrict__ row_cell,
                                    const uint32_t* __restrict__ cell_worker, const uint32_t* __restrict__ cell_firm,
@@ -344,8 +347,8 @@ __global__ void k_generic_contract(uint32_t groups, int q, const uint64_t* __res
     size_t t = base + threadIdx.x;
     bool live = t < total;
     size_t g = live ? t / TPR : 0;
-    uint64_t b = live ? group_ptr[g] : 0, e = live ? group_ptr[g + 1] : 0;
-    uint32_t cell = live ? row_cell[group_rows[b]] : 0;
+    uint64_t b = live ? (OBS ? g : group_ptr[g]) : 0, e = live ? (OBS ? g + 1 : group_ptr[g + 1]) : 0;
+    uint32_t cell = live ? row_cell[OBS ? uint32_t(b) : group_rows[b]] : 0;
     double ufe[CPT];
 #pragma unroll
     for (int c = 0; c < CPT; ++c)
@@ -355,12 +358,14 @@ __global__ void k_generic_contract(uint32_t groups, int q, const uint64_t* __res
     for (int c = 0; c < CPT; ++c) first[c] = second[c] = 0.0;
     // the TPR lanes of a group walk its rows in lock step
     for (uint64_t i = b; i < e; ++i) {
-      uint32_t r = group_rows[i];
-      double f = row_freq[r], fy = f * (y[r] - y_center), sd = sqrt(f) * deleted[r];
+      uint32_t r = OBS ? uint32_t(i) : group_rows[i];
+      double f = row_freq[r], fy = f * (y[r] - y_center), sd = OBS ? deleted[r] : sqrt(f) * deleted[r];
 #pragma unroll
       for (int c = 0; c < CPT; ++c) {
         double u = ufe[c];
-        for (int k = 0; k < q; ++k) u += R[size_t(r) * q + k] * bcol[k][c];
+#pragma unroll
+        for (int k = 0; k < QMAX; ++k)
+          if (k < q) u += R[size_t(r) * q + k] * bcol[k][c];
         first[c] += fy * u;
         second[c] += sd * u;
       }

@@ -21,8 +21,9 @@ __global__ void k_finish(const double* __restrict__ partial, int blocks, int wid
 template <int K>
 __global__ void k_leverage_atoms(uint32_t cells, const uint32_t* __restrict__ unit_ptr,
                                  const uint64_t* __restrict__ unit_rank, const uint64_t* __restrict__ unit_count,
-                                 PhiloxKey key, uint64_t tag, uint64_t first, int ncols,
-                                 double* __restrict__ unit_atoms, double* __restrict__ cell_atoms) {
+                                 const uint64_t* __restrict__ unit_offset, PhiloxKey key, uint64_t tag,
+                                 uint64_t first, int ncols, double* __restrict__ unit_atoms,
+                                 double* __restrict__ cell_atoms) {
   constexpr int B = (K + 3) / 4;  // probe blocks per row
   size_t total = size_t(cells) * B;
   for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
@@ -31,13 +32,16 @@ __global__ void k_leverage_atoms(uint32_t cells, const uint32_t* __restrict__ un
     double acc[4] = {0, 0, 0, 0};
     for (uint32_t g = unit_ptr[c]; g < unit_ptr[c + 1]; ++g) {
       int64_t a[4];
-      rademacher_block_sums(key, tag, first / 4 + b, unit_rank[g], unit_count[g], a);
+      if (unit_offset)
+        rademacher_range_block_sums(key, tag, first / 4 + b, unit_rank[g], unit_offset[g], unit_count[g], a);
+      else
+        rademacher_block_sums(key, tag, first / 4 + b, unit_rank[g], unit_count[g], a);
 #pragma unroll
       for (int l = 0; l < 4; ++l) {
         int j = 4 * b + l;
         if (j < K) {
           double v = (j < ncols) ? double(a[l]) : 0.0;
-          unit_atoms[size_t(g) * K + j] = v;
+          if (unit_atoms) unit_atoms[size_t(g) * K + j] = v;
           acc[l] += v;
         }
       }

@@ -1,0 +1,218 @@
+// Leave-observation-out statistics of the generic estimator.
+//
+// Every retained row r with frequency f_r holds f_r physical copies.  A probe j
+// draws one Rademacher sign a_j(c) per copy c (Counter-V1 word of the row's
+// class rank, bit = the copy's number inside its class), the FE-only solve of
+// the right-hand side sum_c a_j(c) x_c returns the prediction P_j(r) at every
+// row, and the deleted residual of a copy needs, over the probes,
+//   per row:  sum_j P_j^2,  sum_j P_j^4
+//   per copy: sum_j a_j(c) P_j,  sum_j a_j(c) P_j^3
+// (reference `observation_and_match_leverage_moments`, generic_jla.rs:5540-5881,
+// `observation_moments` / `observation_correlations`,
+// generic_jla/statistical_batches.rs:79-205).  The five projection/residual
+// moments of a copy follow from these four because a_j^2 = 1.
+#pragma once
+
+#include "counter_rng.h"
+#include "device.cuh"
+#include "generic.cuh"
+
+namespace fevcb {
+
+__device__ __forceinline__ void neumaier_add(double& sum, double& corr, double v) {
+  double t = sum + v;
+  corr += (fabs(sum) >= fabs(v)) ? (sum - t) + v : (v - t) + sum;
+  sum = t;
+}
+
+// One probe block of K columns (first a multiple of 4; columns >= ncols carry a
+// zero prediction).  TPR lanes share a row, each holding CPT columns.
+// row_acc[r][4] = (sum P^2, its compensation, sum P^4, its compensation);
+// copy_acc[c][4] = (sum a P, compensation, sum a P^3, compensation), c the
+// copy's physical index (rows in row order, copies consecutive).
+template <int K>
+__global__ void k_obs_moments(uint32_t rows, int ncols, const uint32_t* __restrict__ row_cell,
+                              const uint32_t* __restrict__ cell_worker, const uint32_t* __restrict__ cell_firm,
+                              const uint64_t* __restrict__ row_rank, const uint64_t* __restrict__ row_copy_offset,
+                              const uint64_t* __restrict__ row_phys, PhiloxKey key, uint64_t first,
+                              const double* __restrict__ alpha, const double* __restrict__ psi,
+                              double* __restrict__ row_acc, double* __restrict__ copy_acc) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  static_assert(CPT <= 4, "the columns of one thread must fall in one Philox block");
+  const int c0 = int(threadIdx.x % TPR) * CPT;
+  // all columns of this lane sit in one probe block: (first + c0) / 4
+  const uint64_t pblock = (first + uint64_t(c0)) >> 2;
+  const int lane0 = int((first + uint64_t(c0)) & 3);
+  size_t total = size_t(rows) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    bool live = t < total;
+    uint32_t r = live ? uint32_t(t / TPR) : 0;
+    double P[CPT];
+    double s2 = 0.0, s4 = 0.0;
+    uint64_t ncopy = 0, off = 0, ph = 0, ent = 0;
+    if (live) {
+      uint32_t cell = row_cell[r];
+      size_t wi = size_t(cell_worker[cell]) * K, fi = size_t(cell_firm[cell]) * K;
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        P[c] = (c0 + c < ncols) ? alpha[wi + c0 + c] + psi[fi + c0 + c] : 0.0;
+        double p2 = P[c] * P[c];
+        s2 += p2;
+        s4 += p2 * p2;
+      }
+      ph = row_phys[r];
+      ncopy = row_phys[r + 1] - ph;
+      off = row_copy_offset[r];
+      ent = row_rank[r];
+    } else {
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) P[c] = 0.0;
+    }
+#pragma unroll
+    for (int o = TPR / 2; o > 0; o >>= 1) {
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      s4 += __shfl_xor_sync(0xffffffffu, s4, o);
+    }
+    if (live && c0 == 0) {
+      double* a = row_acc + size_t(r) * 4;
+      neumaier_add(a[0], a[1], s2);
+      neumaier_add(a[2], a[3], s4);
+    }
+    // copies: the warp walks the longest row of its groups in lock step
+    uint64_t most = ncopy;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      uint64_t other = __shfl_xor_sync(0xffffffffu, most, o);
+      most = other > most ? other : most;
+    }
+    uint64_t word_at = ~uint64_t(0), bits[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) bits[c] = 0;
+    for (uint64_t i = 0; i < most; ++i) {
+      double f1 = 0.0, f3 = 0.0;
+      bool mine = live && i < ncopy;
+      if (mine) {
+        uint64_t cn = off + i, word = cn >> 6;
+        if (word != word_at) {
+          uint64_t blk[4];
+          philox_block(key, ent, pblock, word, TAG_LEVERAGE, blk);
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) {
+            int l = (lane0 + c) & 3;  // select without a dynamically indexed array
+            bits[c] = l == 0 ? blk[0] : l == 1 ? blk[1] : l == 2 ? blk[2] : blk[3];
+          }
+          word_at = word;
+        }
+        int bit = int(cn & 63);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          double a = ((bits[c] >> bit) & 1) ? 1.0 : -1.0;
+          double p = P[c];
+          f1 += a * p;
+          f3 += a * p * p * p;
+        }
+      }
+#pragma unroll
+      for (int o = TPR / 2; o > 0; o >>= 1) {
+        f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+        f3 += __shfl_xor_sync(0xffffffffu, f3, o);
+      }
+      if (mine && c0 == 0) {
+        double* a = copy_acc + size_t(ph + i) * 4;
+        neumaier_add(a[0], a[1], f1);
+        neumaier_add(a[2], a[3], f3);
+      }
+    }
+  }
+}
+
+// Analytic control leverage of one copy of each row, R_r' S^{-1} R_r, clipped
+// at zero; below -100 rank_tolerance or nonfinite is a moment failure
+// (reference `control_geometry`, generic_jla.rs:4493-4523).
+__global__ void k_control_leverage(uint32_t rows, int q, const double* __restrict__ R, SmallMatrix sinv,
+                                   double rank_tolerance, double* __restrict__ leverage,
+                                   unsigned long long* __restrict__ error) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+    StableSumD v;
+    for (int i = 0; i < q; ++i)
+      for (int j = 0; j < q; ++j) v.add(R[size_t(r) * q + i] * sinv.m[i * QMAX + j] * R[size_t(r) * q + j]);
+    double x = v.finish();
+    if (!isfinite(x) || x < -100.0 * rank_tolerance) atomicMin(error, (unsigned long long)r << 8 | JLA_MOMENT_FAILED);
+    leverage[r] = fmax(x, 0.0);
+  }
+}
+
+struct ObservationAdjustParams {
+  uint32_t rows;
+  double probes, block_tolerance, rank_tolerance;
+};
+
+// Deleted residual of every row: the mean over its copies of the
+// finite-projection inverse 1/t + bias/t^2 - var/t^3, t = residual share -
+// control leverage, times the row's full-fit residual (reference
+// `observation_deleted_adjustment`, generic_jla.rs:5893-6018, with
+// `FiveMoments::finite`, generic_jla.rs:467-516).  out[r][2] = (mean total
+// leverage, maximum total leverage over the copies).
+__global__ void k_obs_adjust(ObservationAdjustParams prm, const uint64_t* __restrict__ row_phys,
+                             const double* __restrict__ row_acc, const double* __restrict__ copy_acc,
+                             const double* __restrict__ control_leverage, const double* __restrict__ residual,
+                             double* __restrict__ deleted, double* __restrict__ out,
+                             unsigned long long* __restrict__ error) {
+  const double P = prm.probes;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < prm.rows; r += gridDim.x * blockDim.x) {
+    const double pf = row_acc[size_t(r) * 4] + row_acc[size_t(r) * 4 + 1];
+    const double ps = row_acc[size_t(r) * 4 + 2] + row_acc[size_t(r) * 4 + 3];
+    const double lev_c = control_leverage ? control_leverage[r] : 0.0;
+    unsigned long long code = 0;
+    StableSumD inv_sum, lev_sum;
+    double lev_max = 0.0;
+    uint64_t b = row_phys[r], e = row_phys[r + 1];
+    for (uint64_t c = b; c < e && !code; ++c) {
+      const double* a = copy_acc + size_t(c) * 4;
+      double first = a[0] + a[1], third = a[2] + a[3];
+      double m_proj = pf, m_res = P + pf - 2.0 * first, m_p4 = ps;
+      double m_r4 = P + 6.0 * pf + ps - 4.0 * first - 4.0 * third, m_mix = pf + ps - 2.0 * third;
+      double total = (m_proj + m_res) / P;
+      if (!isfinite(total) || total <= prm.block_tolerance) {
+        code = JLA_CONSTRAINT_FAILED;
+        break;
+      }
+      double proj = (m_proj / P) / total, res = (m_res / P) / total;
+      double p4 = m_p4 / P, m4 = m_r4 / P, mixed = m_mix / P;
+      double bias = (res * p4 - proj * m4 + (res - proj) * mixed) / P;
+      double var = (res * res * p4 + proj * proj * m4 - 2.0 * proj * res * mixed) / P;
+      if (!(isfinite(proj) && isfinite(res) && isfinite(bias) && isfinite(var)) || var < -100.0 * prm.rank_tolerance) {
+        code = JLA_MOMENT_FAILED;
+        break;
+      }
+      var = fmax(var, 0.0);
+      double tr = res - lev_c;
+      if (!isfinite(tr) || tr <= prm.block_tolerance) {
+        code = NONESTIMABLE_DELETION;
+        break;
+      }
+      double rc = 1.0 / tr;
+      double inverse = rc + bias * rc * rc - var * rc * rc * rc;
+      if (!isfinite(inverse) || inverse <= 0.0) {
+        code = BLOCK_INVERSE_FAILED;
+        break;
+      }
+      inv_sum.add(inverse);
+      double tl = proj + lev_c;
+      lev_sum.add(tl);
+      lev_max = fmax(lev_max, tl);
+    }
+    double f = double(e - b);
+    double d = code ? 0.0 : residual[r] * (inv_sum.finish() / f);
+    if (!code && !isfinite(d)) code = CORRECTION_NONFINITE;
+    if (code) atomicMin(error, (unsigned long long)r << 8 | code);
+    deleted[r] = d;
+    if (out) {
+      out[size_t(r) * 2] = lev_sum.finish() / f;
+      out[size_t(r) * 2 + 1] = lev_max;
+    }
+  }
+}
+
+}  // namespace fevcb

@@ -895,13 +895,86 @@ JlaPlan build_plan(const Compressed& p) {
 
 namespace fevcb {
 
-JlaPlan build_generic_plan(const Compressed& p) {
+void build_target_strata(const Compressed& p, const std::vector<double>& per_copy, JlaPlan& plan);
+
+// Leave-observation-out units.  Semantic ranks order rows by worker, firm,
+// per-copy target mass and outcome (total order, -0.0 folded into +0.0 for
+// the mass), then the controls and the probe order; the deletion identifier
+// takes no part (reference `observation_row_ranks` / `compare_observation_rows`,
+// generic_jla.rs:4267-4334).  Rows of one rank form a class whose physical
+// copies are numbered consecutively in row order: copy c of the class draws
+// bit c % 64 of Counter-V1 word c / 64 for entity = rank (reference
+// `observation_classes`, generic_jla.rs:4158-4215, `observation_addresses`,
+// generic_jla/statistical_batches.rs:15-54, `rademacher_copy`,
+// generic_jla.rs:10322-10329).
+static void build_observation_units(const Compressed& p, const std::vector<double>& per_copy, JlaPlan& plan) {
+  size_t R = p.rows();
+  bool has_order = !p.probe_order.empty();
+  auto sem = [&](uint32_t a, uint32_t b) -> int {
+    if (p.row_worker[a] != p.row_worker[b]) return p.row_worker[a] < p.row_worker[b] ? -1 : 1;
+    if (p.row_firm[a] != p.row_firm[b]) return p.row_firm[a] < p.row_firm[b] ? -1 : 1;
+    int c = total_cmp(canonical_zero(per_copy[a]), canonical_zero(per_copy[b]));
+    if (c) return c;
+    c = total_cmp(p.outcome[a], p.outcome[b]);
+    if (c) return c;
+    for (auto& col : p.controls) {
+      c = ordered_f64(col[a], col[b]);
+      if (c) return c;
+    }
+    if (has_order) return ordered_f64(p.probe_order[a], p.probe_order[b]);
+    return 0;
+  };
+  std::vector<uint32_t> order(R);
+  std::iota(order.begin(), order.end(), 0u);
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return sem(a, b) < 0; });
+  plan.row_rank.assign(R, 0);
+  uint64_t current = 0;
+  for (size_t i = 0; i < R; ++i) {
+    if (i == 0 || sem(order[i - 1], order[i]) != 0) ++current;
+    plan.row_rank[order[i]] = current;
+  }
+  // classes: rows sorted by (rank, row); the stable sort above already holds
+  // equal ranks in row order
+  plan.row_copy_offset.assign(R, 0);
+  plan.group_ptr.assign(1, 0);
+  plan.group_rows.assign(order.begin(), order.end());
+  for (size_t i = 0; i < R;) {
+    size_t j = i;
+    uint64_t phys = 0;
+    StableSum y, t;
+    while (j < R && plan.row_rank[order[j]] == plan.row_rank[order[i]]) {
+      uint32_t r = order[j];
+      plan.row_copy_offset[r] = phys;
+      phys += p.frequency[r];
+      y.add(double(p.frequency[r]) * p.outcome[r]);
+      t.add(p.target[r]);
+      ++j;
+    }
+    if (phys == 0 || (phys + 63) / 64 > (uint64_t(1) << 20))
+      fail(RESOURCE_LIMIT, "generic_jla_rng_preflight", "observation class has an invalid physical trial count");
+    plan.group_ptr.push_back(j);
+    plan.del_cell.push_back(p.row_cell[order[i]]);
+    plan.del_count.push_back(phys);
+    plan.del_rank.push_back(plan.row_rank[order[i]]);
+    plan.del_outcome_sum.push_back(y.finish());
+    plan.del_target_mass.push_back(t.finish());
+    i = j;
+  }
+}
+
+JlaPlan build_generic_plan(const Compressed& p, Deletion deletion) {
   size_t R = p.rows();
   JlaPlan plan;
   plan.generic = true;
   std::vector<double> per_copy(R);
   for (size_t r = 0; r < R; ++r) per_copy[r] = p.target[r] / double(p.frequency[r]);
   bool has_order = !p.probe_order.empty();
+  if (deletion == Deletion::Observation) {
+    plan.observation = true;
+    build_observation_units(p, per_copy, plan);
+    build_target_strata(p, per_copy, plan);
+    return plan;
+  }
   // reference `compare_semantic_rows` (generic_jla.rs:3878-3900): per-copy mass
   // and outcome by total order (no zero canonicalisation), then the controls
   // and the probe order with -0.0 mapped to +0.0
@@ -961,7 +1034,15 @@ JlaPlan build_generic_plan(const Compressed& p) {
     plan.del_outcome_sum[g] = y.finish();
     plan.del_target_mass[g] = t.finish();
   }
-  // target strata (reference `target_plan`, generic_jla.rs:3902-3995)
+  build_target_strata(p, per_copy, plan);
+  return plan;
+}
+
+// Target strata of the generic estimator: rows grouped by (cell, per-copy
+// target mass), each stratum keyed by its smallest semantic rank (reference
+// `target_plan`, generic_jla.rs:3902-3995).
+void build_target_strata(const Compressed& p, const std::vector<double>& per_copy, JlaPlan& plan) {
+  size_t R = p.rows();
   std::vector<uint32_t> tord(R);
   std::iota(tord.begin(), tord.end(), 0u);
   std::stable_sort(tord.begin(), tord.end(), [&](uint32_t a, uint32_t b) {
@@ -995,7 +1076,6 @@ JlaPlan build_generic_plan(const Compressed& p) {
     plan.tgt_mass.push_back(t.finish());
     plan.tgt_rank.push_back(ent);
   }
-  return plan;
 }
 
 }  // namespace fevcb

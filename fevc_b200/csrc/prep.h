@@ -69,9 +69,13 @@ struct Compressed {
 };
 
 struct JlaPlan {
-  bool generic = false;  // built by build_generic_plan (controls present)
+  bool generic = false;      // built by build_generic_plan
+  bool observation = false;  // leave-observation-out units (classes of equal rank)
   std::vector<uint64_t> row_rank;
+  // observation plan only: first Counter-V1 copy index of each row in its class
+  std::vector<uint64_t> row_copy_offset;
   // generic plan only: rows of each deletion group in semantic-rank order
+  // (observation plan: rows of each class in row order)
   std::vector<uint64_t> group_ptr;
   std::vector<uint32_t> group_rows;
   // deletion units
@@ -110,10 +114,11 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
 // (jla.rs:59-108) generalised: controls do not enter the plan's orderings.
 JlaPlan build_plan(const Compressed& p);
 
-// The generic (controlled) estimator's plan: semantic ranks that also order
-// by the control values, match groups with their rows in rank order, and
-// target strata (reference generic_jla.rs:3836-3900 ranks, 4052-4143 match
-// plan, 3902-3995 target plan).
-JlaPlan build_generic_plan(const Compressed& p);
+// The generic estimator's plan: semantic ranks that also order by the control
+// values, the deletion units (match groups with their rows in rank order, or
+// observation classes), and target strata (reference generic_jla.rs:3836-3900
+// match ranks, 4052-4143 match plan, 4158-4334 observation classes,
+// 3902-3995 target plan).
+JlaPlan build_generic_plan(const Compressed& p, Deletion deletion = Deletion::Match);
 
 }  // namespace fevcb

@@ -473,7 +473,10 @@ typedef struct FevcbProblemViewV1 {
   uint64_t controls;                 /* control columns (generic plan) */
   const double *control_values;      /* rows x controls, column-major */
   const uint64_t *group_ptr;         /* generic plan: rows of each deletion unit ... */
-  const uint32_t *group_rows;        /* ... in semantic-rank order */
+  const uint32_t *group_rows;        /* ... in semantic-rank order (observation: class rows in row order) */
+  const uint64_t *row_rank;          /* generic plan: semantic rank of every row */
+  const uint64_t *row_copy_offset;   /* observation plan: number of the row's first copy in its class */
+  uint64_t deletion_mode;            /* VCKSS_DELETION_MATCH or VCKSS_DELETION_OBSERVATION */
 } FevcbProblemViewV1;
 int32_t fevcb_engine_problem_view_v1(uint64_t generation, FevcbProblemViewV1 *output, uint32_t output_capacity_bytes);
 

@@ -109,6 +109,9 @@ typedef struct {
   const double* control_values; /* rows x controls, column-major */
   const uint64_t* group_ptr;
   const uint32_t* group_rows;
+  const uint64_t* row_rank;        /* generic plans: semantic rank of every row */
+  const uint64_t* row_copy_offset; /* not read: the oracle numbers copies itself */
+  uint64_t deletion_mode;          /* 1 match, 2 observation */
 } OracleProblem;
 
 typedef struct {
@@ -533,12 +536,136 @@ static void dense_solve(const double* l, int n, double* b) {
 /* Generic estimator: year controls through the FWL block, match deletion,
  * joint nuisance.  result->target_draws hold (worker, firm, covariance,
  * total) per probe; per-unit arrays are not filled. */
+/* ---------------------------------------------- leave-observation-out */
+
+static const uint64_t* g_rank_for_sort;
+static int by_rank_then_row(const void* a, const void* b) {
+  uint32_t x = *(const uint32_t*)a, y = *(const uint32_t*)b;
+  if (g_rank_for_sort[x] != g_rank_for_sort[y]) return g_rank_for_sort[x] < g_rank_for_sort[y] ? -1 : 1;
+  return x < y ? -1 : (x > y);
+}
+
+/* sign of copy `copy` of `entity`: bit copy % 64 of word copy / 64
+ * (reference `rademacher_copy`, generic_jla.rs:10322-10329) */
+static double copy_sign(uint64_t seed, uint64_t probe, uint64_t entity, uint64_t copy) {
+  uint64_t b[4];
+  oracle_philox_block(seed, TAG_LEVERAGE, probe / 4, entity, copy / 64, b);
+  return ((b[probe % 4] >> (copy % 64)) & 1) ? 1.0 : -1.0;
+}
+
+/* Leverage probes with one sign per physical copy, the per-row and per-copy
+ * moment sums, and the deleted residual of every row (reference
+ * `observation_classes` generic_jla.rs:4158-4215,
+ * `observation_and_match_leverage_moments` 5540-5881,
+ * `observation_deleted_adjustment` 5893-6018, control leverage 4493-4523). */
+static int observation_deleted(const OracleProblem* p, const OracleOptions* o, Solver* s, int q, const double* Rr,
+                               const double* Si, const double* resid, double* deleted, OracleResult* res) {
+  uint64_t W = p->workers, F = p->firms, R = p->rows, P = o->probes;
+  double Pd = (double)P;
+  /* classes: rows sorted by (rank, row); copies numbered through the class */
+  uint32_t* order = malloc(R * sizeof(uint32_t));
+  for (uint64_t r = 0; r < R; ++r) order[r] = (uint32_t)r;
+  g_rank_for_sort = p->row_rank;
+  qsort(order, R, sizeof(uint32_t), by_rank_then_row);
+  uint64_t *off = calloc(R, 8), *phys = calloc(R + 1, 8);
+  for (uint64_t i = 0, run = 0; i < R; ++i) {
+    if (i > 0 && p->row_rank[order[i]] != p->row_rank[order[i - 1]]) run = 0;
+    off[order[i]] = run;
+    run += p->row_frequency[order[i]];
+  }
+  for (uint64_t r = 0; r < R; ++r) phys[r + 1] = phys[r] + p->row_frequency[r];
+  uint64_t N = phys[R];
+  Stable *p2 = calloc(R, sizeof(Stable)), *p4 = calloc(R, sizeof(Stable));
+  Stable *c1 = calloc(N, sizeof(Stable)), *c3 = calloc(N, sizeof(Stable));
+  double *bw = calloc(W, 8), *bf = calloc(F, 8), *al = calloc(W, 8), *ps = calloc(F, 8);
+  for (uint64_t probe = 0; probe < P; ++probe) {
+    memset(bw, 0, W * 8);
+    memset(bf, 0, F * 8);
+    for (uint64_t r = 0; r < R; ++r) {
+      double a = 0.0;
+      for (uint64_t i = 0; i < p->row_frequency[r]; ++i) a += copy_sign(o->seed, probe, p->row_rank[r], off[r] + i);
+      bw[p->row_worker[r]] += a;
+      bf[p->row_firm[r]] += a;
+    }
+    solve(s, bw, bf, al, ps);
+    for (uint64_t r = 0; r < R; ++r) {
+      double pr = al[p->row_worker[r]] + ps[p->row_firm[r]];
+      st_add(&p2[r], pr * pr);
+      st_add(&p4[r], pr * pr * pr * pr);
+      for (uint64_t i = 0; i < p->row_frequency[r]; ++i) {
+        double sg = copy_sign(o->seed, probe, p->row_rank[r], off[r] + i);
+        st_add(&c1[phys[r] + i], sg * pr);
+        st_add(&c3[phys[r] + i], sg * pr * pr * pr);
+      }
+    }
+  }
+  int code = 0;
+  for (uint64_t r = 0; r < R && !code; ++r) {
+    Stable lv = {0, 0};
+    for (int i = 0; i < q; ++i)
+      for (int j = 0; j < q; ++j) st_add(&lv, Rr[r * q + i] * Si[i * q + j] * Rr[r * q + j]);
+    double lev = st_fin(&lv);
+    if (!isfinite(lev) || lev < -100.0 * o->rank_tolerance) {
+      code = set_error(res, 73, "analytic control leverage is negative or nonfinite");
+      break;
+    }
+    lev = lev > 0.0 ? lev : 0.0;
+    double pf = st_fin(&p2[r]), pq = st_fin(&p4[r]);
+    Stable inv = {0, 0};
+    for (uint64_t i = 0; i < p->row_frequency[r]; ++i) {
+      double first = st_fin(&c1[phys[r] + i]), third = st_fin(&c3[phys[r] + i]);
+      double mp = pf, mr = Pd + pf - 2.0 * first, m4p = pq;
+      double m4r = Pd + 6.0 * pf + pq - 4.0 * first - 4.0 * third, mx = pf + pq - 2.0 * third;
+      double total = (mp + mr) / Pd;
+      if (!isfinite(total) || total <= o->block_tolerance) {
+        code = set_error(res, 74, "projection and residual masses are not positive");
+        break;
+      }
+      double proj = (mp / Pd) / total, rs = (mr / Pd) / total;
+      double q4 = m4p / Pd, r4 = m4r / Pd, mix = mx / Pd;
+      double bias = (rs * q4 - proj * r4 + (rs - proj) * mix) / Pd;
+      double var = (rs * rs * q4 + proj * proj * r4 - 2.0 * proj * rs * mix) / Pd;
+      if (var < -100.0 * o->rank_tolerance) {
+        code = set_error(res, 73, "finite-projection variance is negative");
+        break;
+      }
+      if (var < 0) var = 0;
+      double tr = rs - lev;
+      if (!isfinite(tr) || tr <= o->block_tolerance) {
+        code = set_error(res, 75, "estimated residual leverage is nonpositive");
+        break;
+      }
+      double rc = 1.0 / tr, v = rc + bias * rc * rc - var * rc * rc * rc;
+      if (!isfinite(v) || v <= 0.0) {
+        code = set_error(res, 76, "finite-projection observation inverse is nonpositive");
+        break;
+      }
+      st_add(&inv, v);
+    }
+    deleted[r] = resid[r] * (st_fin(&inv) / (double)p->row_frequency[r]);
+  }
+  free(order);
+  free(off);
+  free(phys);
+  free(p2);
+  free(p4);
+  free(c1);
+  free(c3);
+  free(bw);
+  free(bf);
+  free(al);
+  free(ps);
+  return code;
+}
+
 int oracle_jla_generic(const OracleProblem* p, const OracleOptions* o, OracleResult* res) {
   uint64_t W = p->workers, F = p->firms, C = p->cells, G = p->units, S = p->strata, P = o->probes, R = p->rows;
   int q = (int)p->controls;
   Solver s;
   res->error_code = 0;
-  if (q < 1 || !p->group_ptr) return set_error(res, 11, "the generic oracle needs controls and match groups");
+  const int observation = p->deletion_mode == 2;
+  if (observation ? !p->row_rank : (q < 1 || !p->group_ptr))
+    return set_error(res, 11, "the generic oracle needs controls and match groups, or observation ranks");
   if (solver_init(&s, p, o)) return set_error(res, 82, "grounded Schur factor is not positive definite");
   double *bw = calloc(W, 8), *bf = calloc(F, 8), *alpha = calloc(W, 8), *psi = calloc(F, 8);
   double *alpha2 = calloc(W, 8), *psi2 = calloc(F, 8);
@@ -621,8 +748,16 @@ int oracle_jla_generic(const OracleProblem* p, const OracleOptions* o, OracleRes
     res->plugin[2] = st_fin(&cv) / p->target_total;
     res->plugin[3] = st_fin(&t) / p->target_total;
   }
+  double* deleted = calloc(R, 8);
+  double Pd = (double)P;
+  Stable* mom = NULL;
+  if (observation) {
+    int err = observation_deleted(p, o, &s, q, Rr, Si, resid, deleted, res);
+    if (err) return err;
+    goto target;
+  }
   /* FE-only leverage moments */
-  Stable* mom = calloc(G * 5, sizeof(Stable));
+  mom = calloc(G * 5, sizeof(Stable));
   for (uint64_t probe = 0; probe < P; ++probe) {
     memset(bw, 0, W * 8);
     memset(bf, 0, F * 8);
@@ -649,8 +784,6 @@ int oracle_jla_generic(const OracleProblem* p, const OracleOptions* o, OracleRes
     free(at);
   }
   /* deleted residuals per match group: (I - V V') X = [sqrt(f) e, common] */
-  double* deleted = calloc(R, 8);
-  double Pd = (double)P;
   for (uint64_t g = 0; g < G; ++g) {
     double pf = st_fin(&mom[g * 5 + 0]), mf = st_fin(&mom[g * 5 + 1]);
     double tm = (pf + mf) / Pd;
@@ -700,6 +833,7 @@ int oracle_jla_generic(const OracleProblem* p, const OracleOptions* o, OracleRes
     free(x1);
     free(cm);
   }
+target:;
   double mean = 0.0;
   if (o->centering == 1) {
     double anchor = p->row_outcome[0];
@@ -757,7 +891,22 @@ int oracle_jla_generic(const OracleProblem* p, const OracleOptions* o, OracleRes
         betaF[k] -= Si[k * q + l] * bF[l];
       }
     Stable out[3] = {{0, 0}, {0, 0}, {0, 0}};
-    for (uint64_t g = 0; g < G; ++g) {
+    if (observation) {
+      /* f y d u^2 per row (reference `target_contraction`, generic_jla.rs:8926-8937) */
+      for (uint64_t r = 0; r < R; ++r) {
+        double fr = (double)p->row_frequency[r];
+        double u[3];
+        u[0] = alpha[p->row_worker[r]] + psi[p->row_firm[r]];
+        u[1] = alpha2[p->row_worker[r]] + psi2[p->row_firm[r]];
+        for (int k = 0; k < q; ++k) {
+          u[0] += Rr[r * q + k] * betaW[k];
+          u[1] += Rr[r * q + k] * betaF[k];
+        }
+        u[2] = u[0] + u[1];
+        for (int t = 0; t < 3; ++t) st_add(&out[t], fr * (p->row_outcome[r] - mean) * deleted[r] * u[t] * u[t]);
+      }
+    }
+    for (uint64_t g = 0; g < (observation ? 0 : G); ++g) {
       Stable first[3] = {{0, 0}, {0, 0}, {0, 0}}, second[3] = {{0, 0}, {0, 0}, {0, 0}};
       for (uint64_t i = p->group_ptr[g]; i < p->group_ptr[g + 1]; ++i) {
         uint32_t r = p->group_rows[i];

@@ -23,7 +23,8 @@ class OracleProblem(C.Structure):
         ("cell_firm", u32p), ("cell_weight", dp), ("cell_outcome_sum", dp), ("cell_target_sum", dp),
         ("unit_cell", u32p), ("unit_count", u64p), ("unit_rank", u64p), ("unit_outcome_sum", dp),
         ("stratum_cell", u32p), ("stratum_per_copy", dp), ("stratum_count", u64p), ("stratum_rank", u64p),
-        ("controls", C.c_uint64), ("control_values", dp), ("group_ptr", u64p), ("group_rows", u32p)]
+        ("controls", C.c_uint64), ("control_values", dp), ("group_ptr", u64p), ("group_rows", u32p),
+        ("row_rank", u64p), ("row_copy_offset", u64p), ("deletion_mode", C.c_uint64)]
 
 
 class ProblemView(C.Structure):
@@ -102,7 +103,7 @@ def run(problem: OracleProblem, *, seed=8675309, probes=200, centering=0, tolera
     for n, a in arrays.items():
         setattr(res, n, a.ctypes.data_as(dp))
     opt = OracleOptions(seed, probes, centering, tolerance, rank_tolerance, block_tolerance, dense_limit)
-    fn = lib.oracle_jla_generic if problem.controls else lib.oracle_jla
+    fn = lib.oracle_jla_generic if (problem.controls or problem.deletion_mode == 2) else lib.oracle_jla
     code = fn(C.byref(problem), C.byref(opt), C.byref(res))
     if code != 0:
         raise RuntimeError(f"oracle failed [{code}]: {res.error.decode()}")

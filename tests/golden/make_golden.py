@@ -93,13 +93,43 @@ def weighted_controls_panel(seed: int) -> Panel:
     return p
 
 
-def solve_record_v5(lib, panel: Panel, probes: int, centering: int) -> dict:
-    """The plugin's generic engine (controls) through V5, diagonal PCG at 1e-13."""
+def duplicated_rows_panel(seed: int, controls: bool) -> Panel:
+    """Literal frequencies plus repeated rows: about a sixth of the rows appear
+    again with the same worker, firm, outcome, controls and per-copy target
+    mass (some with another frequency), so leave-observation-out classes hold
+    several rows whose copies are numbered through the class."""
+    p = generate_panel(1500, 120, 5, move_p=0.25, year_controls=controls, seed=seed)
+    rng = np.random.default_rng(seed + 2)
+    p.frequency = rng.integers(1, 4, p.rows).astype(np.float64)
+    per_copy = np.round(rng.uniform(0.5, 3.0, p.rows) * 4) / 4
+    p.target_weight = per_copy * p.frequency
+    pick = np.sort(rng.choice(p.rows, p.rows // 6, replace=False))
+    freq = p.frequency[pick].copy()
+    refreq = rng.random(pick.size) < 0.4
+    freq[refreq] = rng.integers(1, 5, int(refreq.sum()))
+    cat = lambda a, b: np.concatenate([a, b])
+    return Panel(cat(p.worker, p.worker[pick]), cat(p.firm, p.firm[pick]), cat(p.deletion, p.deletion[pick]),
+                 cat(p.outcome, p.outcome[pick]), cat(p.frequency, freq), cat(p.target_weight, per_copy[pick] * freq),
+                 [cat(c, c[pick]) for c in p.controls])
+
+
+OBSERVATION_PANELS = {
+    "obs_2k": dict(build=lambda: generate_panel(2000, 150, 5, move_p=0.2, seed=11), probes=16),
+    "obs_controls_2k": dict(build=lambda: generate_panel(2000, 150, 5, move_p=0.2, year_controls=True, seed=11),
+                            probes=16),
+    "obs_duplicates_1500": dict(build=lambda: duplicated_rows_panel(8, False), probes=12),
+    "obs_controls_duplicates_1500": dict(build=lambda: duplicated_rows_panel(9, True), probes=12),
+}
+
+
+def solve_record_v5(lib, panel: Panel, probes: int, centering: int, deletion_mode: int = 1) -> dict:
+    """The plugin's generic engine (controls or leave-observation-out) through
+    V5, diagonal PCG at 1e-13."""
     e = abi.Engine(lib)
-    e.prepare(panel)
+    e.prepare(panel, deletion_mode=deletion_mode)
     if centering:
         e.centering(centering)
-    q = e.default_request_v5()
+    q = e.default_request_v5(deletion_mode)
     v1 = q.v4.v3.v2.v1
     v1.probes = probes
     v1.solver_route = 2
@@ -155,10 +185,10 @@ def error_cases():
     }
 
 
-def prepare_record(lib, panel: Panel) -> dict:
+def prepare_record(lib, panel: Panel, deletion_mode: int = 1) -> dict:
     e = abi.Engine(lib)
     try:
-        e.prepare(panel)
+        e.prepare(panel, deletion_mode=deletion_mode)
     except abi.EngineError as err:
         return {"status": err.code}
     rc = e.receipt()
@@ -214,6 +244,17 @@ def main() -> None:
         prep[name] = rec
         controls[name] = [solve_record_v5(lib, panel, spec["probes"], 0), solve_record_v5(lib, panel, spec["probes"], 1)]
         print(name, rec["retained"], controls[name][0]["corrected"])
+    observation = {}
+    for name, spec in OBSERVATION_PANELS.items():
+        panel = spec["build"]()
+        rec = prepare_record(lib, panel, 2)
+        rec["rows"] = panel.rows
+        rec["panel_sha256"] = panel_digest(panel)
+        rec["deletion_mode"] = 2
+        prep[name] = rec
+        observation[name] = [solve_record_v5(lib, panel, spec["probes"], 0, 2),
+                             solve_record_v5(lib, panel, spec["probes"], 1, 2)]
+        print(name, rec["retained"], observation[name][0]["corrected"])
     errs = {}
     for name, panel in error_cases().items():
         rec = prepare_record(lib, panel)
@@ -224,7 +265,8 @@ def main() -> None:
     meta = {"generator": "tests/golden/make_golden.py", "reference_plugin_version":
             lib.vckss_rust_backend_version().decode()}
     (HERE / "prep_cases.json").write_text(json.dumps({"meta": meta, "panels": prep, "errors": errs}, indent=1))
-    (HERE / "jla_cases.json").write_text(json.dumps({"meta": meta, "panels": jla, "controls": controls}, indent=1))
+    (HERE / "jla_cases.json").write_text(json.dumps({"meta": meta, "panels": jla, "controls": controls,
+                                                        "observation": observation}, indent=1))
 
 
 if __name__ == "__main__":

@@ -96,6 +96,64 @@ def test_components_with_controls_match_reference(lib, golden, name, which):
         assert rel(res[key], rec[key]) < COMPONENT_RTOL, (key, res[key], rec[key])
 
 
+def solve_observation(lib, panel, *, probes, centering=0, tol=1e-12, block=0, seed=8675309):
+    e = abi.Engine(lib)
+    e.prepare(panel, deletion_mode=2)
+    if centering:
+        e.centering(centering)
+    e.device_options(block, 0)
+    q = e.default_request_v5(2)
+    v1 = q.v4.v3.v2.v1
+    v1.seed = seed
+    v1.probes = probes
+    v1.pcg_tolerance = tol
+    v1.maximum_iterations = 20000
+    q.v4.v3.v2.algorithm = 2
+    q.v4.v3.engine = 2
+    q.tolerance_supplied = 1
+    e.solve_v5(q, controls_count=len(panel.controls))
+    return e
+
+
+@pytest.mark.parametrize("name", list(make_golden.OBSERVATION_PANELS))
+@pytest.mark.parametrize("which", [0, 1])
+def test_observation_components_match_reference(lib, golden, name, which):
+    """Leave-observation-out through the generic estimator (reference
+    generic_jla.rs:5540-6018, V5 entry with deletion = observation)."""
+    rec = golden["jla"]["observation"][name][which]
+    panel = make_golden.OBSERVATION_PANELS[name]["build"]()
+    e = solve_observation(lib, panel, probes=rec["probes"], centering=rec["centering"], seed=rec["seed"])
+    res = e.result()
+    e.release()
+    for key in ("plugin", "correction", "corrected", "numerical_mcse"):
+        assert rel(res[key], rec[key]) < COMPONENT_RTOL, (key, res[key], rec[key])
+
+
+@pytest.mark.parametrize("block", [8, 16, 32, 64])
+def test_observation_block_width_does_not_change_the_result(lib, oracle_mod, block):
+    """Per-copy signs regroup across probe blocks of every width; the oracle
+    restates the per-probe loop."""
+    panel = make_golden.OBSERVATION_PANELS["obs_controls_duplicates_1500"]["build"]()
+    e = solve_observation(lib, panel, probes=20, block=block)
+    res = e.result()
+    ref = oracle_mod.run(oracle_mod.problem_view(lib, e.generation), probes=20)
+    e.release()
+    for key, okey in (("plugin", "plugin"), ("correction", "correction"), ("corrected", "corrected")):
+        assert rel(res[key], ref[okey]) < COMPONENT_RTOL, (key, res[key], ref[okey])
+
+
+def test_v1_refuses_observation(lib):
+    panel = make_golden.OBSERVATION_PANELS["obs_2k"]["build"]()
+    e = abi.Engine(lib)
+    e.prepare(panel, deletion_mode=2)
+    req = e.default_request()
+    req.probes = 4
+    with pytest.raises(abi.EngineError) as err:
+        e.solve(req)
+    e.release()
+    assert err.value.code == 11
+
+
 def test_v1_refuses_controls(lib):
     panel = make_golden.CONTROL_PANELS["controls_2k"]["build"]()
     e = abi.Engine(lib)

@@ -45,6 +45,41 @@ def test_generic_oracle_matches_reference(lib, oracle_mod, golden, name, which):
         assert rel(out[okey], rec[key]) < 1e-10, (key, out[okey], rec[key])
 
 
+@pytest.mark.parametrize("name", list(make_golden.OBSERVATION_PANELS))
+@pytest.mark.parametrize("which", [0, 1])
+def test_observation_oracle_matches_reference(lib, oracle_mod, golden, name, which):
+    """Leave-observation-out (one Rademacher sign per physical copy, classes of
+    equal semantic rank) restated against the plugin's generic engine."""
+    rec = golden["jla"]["observation"][name][which]
+    panel = make_golden.OBSERVATION_PANELS[name]["build"]()
+    e = abi.Engine(lib)
+    e.prepare(panel, deletion_mode=2)
+    out = oracle_mod.run(oracle_mod.problem_view(lib, e.generation), seed=rec["seed"], probes=rec["probes"],
+                         centering=rec["centering"])
+    e.release()
+    for key, okey in (("plugin", "plugin"), ("correction", "correction"), ("corrected", "corrected"),
+                      ("numerical_mcse", "mcse")):
+        assert rel(out[okey], rec[key]) < 1e-10, (key, out[okey], rec[key])
+
+
+def test_observation_classes_number_copies_through_the_class(lib, oracle_mod):
+    """Rows of equal semantic rank share one class entity; their copies are
+    numbered consecutively in row order (reference generic_jla.rs:4158-4215)."""
+    panel = make_golden.OBSERVATION_PANELS["obs_duplicates_1500"]["build"]()
+    e = abi.Engine(lib)
+    e.prepare(panel, deletion_mode=2)
+    v = oracle_mod.problem_view(lib, e.generation)
+    rank = np.ctypeslib.as_array(v.row_rank, shape=(v.rows,)).copy()
+    off = np.ctypeslib.as_array(v.row_copy_offset, shape=(v.rows,)).copy()
+    freq = np.ctypeslib.as_array(v.row_frequency, shape=(v.rows,)).copy()
+    e.release()
+    assert v.deletion_mode == 2
+    assert len(np.unique(rank)) < v.rows  # the panel repeats rows
+    for r_ in np.unique(rank)[:400]:
+        rows = np.flatnonzero(rank == r_)
+        assert np.array_equal(off[rows], np.concatenate([[0], np.cumsum(freq[rows])[:-1]]))
+
+
 def test_kat_unit_detail(lib, oracle_mod):
     """Per-unit shares of the 12-row known-answer design sum to one and the
     cell weights are finite (reference rust_mata_shared_atoms.rs:108-194)."""

@@ -13,16 +13,18 @@ from fevc_b200.panel import Panel
 import make_golden
 
 
-ALL_PANELS = {**make_golden.PANELS, **make_golden.CONTROL_PANELS}
+ALL_PANELS = {**make_golden.PANELS, **make_golden.CONTROL_PANELS, **make_golden.OBSERVATION_PANELS}
 
 
 @pytest.mark.parametrize("name", list(ALL_PANELS))
 def test_panel_preparation_matches_reference(lib, golden, name):
+    """Match panels through the match-deletion graph; leave-observation-out
+    panels through the observation graph (reference graph.rs:82-243)."""
     rec = golden["prep"]["panels"][name]
     panel = ALL_PANELS[name]["build"]()
     assert make_golden.panel_digest(panel) == rec["panel_sha256"], "panel generator drifted"
     e = abi.Engine(lib)
-    e.prepare(panel)
+    e.prepare(panel, deletion_mode=rec.get("deletion_mode", 1))
     receipt = e.receipt()
     mask = e.retained_mask(panel.rows)
     e.release()
