@@ -174,6 +174,54 @@ TAG_LEVERAGE = 0x4C45564552414745
 TAG_TARGET = 0x0054415247455401
 
 # Every entry point the header declares, with its ctypes signature.
+class FullCmgReceiptV1(C.Structure):
+    """The plugin's VckssFullCmgReceiptV1 (vckss_rust.h:1458-1509, 400 bytes)."""
+    _fields_ = ([("struct_size", u32), ("schema_version", u32), ("generation", u64), ("backend_identity", u32),
+                 ("platform_os", u32), ("platform_arch", u32), ("batch_strategy_mask", u32),
+                 ("cmg_source_commit", C.c_uint8 * 40), ("threads_requested", u32), ("threads_used", u32)]
+                + [(n, u64) for n in ("maximum_concurrency", "vertices", "edges", "hierarchy_levels",
+                                      "terminal_vertices", "graph_copy_bytes", "hierarchy_bytes", "plan_bytes",
+                                      "workspace_bytes_each", "workspace_pool_bytes", "admitted_peak_bytes")]
+                + [(n, f64) for n in ("fit_effective_tolerance", "probe_effective_tolerance",
+                                      "fit_initial_inner_tolerance", "probe_initial_inner_tolerance")]
+                + [(n, u64) for n in ("refinement_attempts", "refined_columns", "batch_calls", "rhs_count",
+                                      "serial_batches", "planned_batches", "across_rhs_batches", "total_iterations",
+                                      "total_operator_applications", "total_preconditioner_applications")]
+                + [(n, f64) for n in ("maximum_reduced_residual", "maximum_complete_residual")]
+                + [(n, u64) for n in ("graph_ns", "hierarchy_plan_ns", "rhs_ns", "solve_ns", "extraction_ns",
+                                      "preparation_peak_bytes", "prepared_persistent_bytes",
+                                      "non_cmg_command_peak_bytes", "pre_rng_forecast_bytes", "actual_retained_bytes",
+                                      "allocator_allowance_bytes", "maximum_batch_rhs", "workspace_count")])
+
+
+assert C.sizeof(FullCmgReceiptV1) == 400
+
+
+class CmgSummaryV1(C.Structure):
+    _fields_ = [("struct_size", u32), ("eliminate_max_degree", u32), ("vertices", u64), ("edges", u64),
+                ("hierarchy_levels", u64), ("terminal_vertices", u64), ("terminal_reason", u32), ("reserved", u32),
+                ("level_vertices", u64 * 32), ("level_edges", u64 * 32), ("level_repeat", u32 * 32)]
+
+
+assert C.sizeof(CmgSummaryV1) == 688
+
+
+def cmg_aggregate(lib, ptr: np.ndarray, col: np.ndarray, weight: np.ndarray, threshold: float = 0.125):
+    """One CMG forest-aggregation step (host): (labels, aggregate count)."""
+    n = len(ptr) - 1
+    ptr = np.ascontiguousarray(ptr, dtype=np.uint32)
+    col = np.ascontiguousarray(col, dtype=np.uint32)
+    weight = np.ascontiguousarray(weight, dtype=np.float64)
+    labels = np.zeros(n, dtype=np.uint32)
+    count = u32(0)
+    up = C.POINTER(u32)
+    st = lib.fevcb_cmg_aggregate_v1(n, ptr.ctypes.data_as(up), col.ctypes.data_as(up), weight.ctypes.data_as(dptr),
+                                    threshold, labels.ctypes.data_as(up), C.byref(count))
+    if st != 0:
+        raise EngineError(st, lib.vckss_rust_engine_last_error().decode())
+    return labels, int(count.value)
+
+
 SIGNATURES = {
     "vckss_rust_abi_version": (u32, []),
     "vckss_rust_backend_version": (C.c_char_p, []),
@@ -223,6 +271,9 @@ SIGNATURES = {
     "fevcb_engine_unit_detail_v1": (i32, [u64, u64] + [dptr] * 6 + [u64, dptr, dptr, u64, dptr]),
     "fevcb_engine_problem_view_v1": (i32, [u64, C.c_void_p, u32]),
     "fevcb_engine_kernel_benchmark_v1": (i32, [u64, u32, u32, u32, C.POINTER(f64), C.POINTER(f64)]),
+    "fevcb_engine_cmg_summary_v1": (i32, [u64, u32, C.c_void_p, u32]),
+    "fevcb_cmg_aggregate_v1": (i32, [u32, C.POINTER(u32), C.POINTER(u32), C.POINTER(f64), f64, C.POINTER(u32),
+                                     C.POINTER(u32)]),
     "fevcb_counter_atoms_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64, C.POINTER(i64)]),
     "fevcb_counter_atoms_noalloc_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64,
                                              C.POINTER(i64)]),
@@ -397,6 +448,17 @@ class Engine:
         self.check(self.lib.fevcb_engine_kernel_benchmark_v1(self.generation, kernel, block_columns, launches,
                                                              C.byref(ms), C.byref(nbytes)))
         return ms.value, nbytes.value
+
+    def cmg_summary(self, eliminate_max_degree: int = 0) -> dict:
+        """Host-built CMG hierarchy of this generation (no GPU needed)."""
+        out = CmgSummaryV1()
+        self.check(self.lib.fevcb_engine_cmg_summary_v1(self.generation, eliminate_max_degree, C.byref(out),
+                                                        C.sizeof(out)))
+        L = int(out.hierarchy_levels)
+        return {"vertices": int(out.vertices), "edges": int(out.edges), "hierarchy_levels": L,
+                "terminal_vertices": int(out.terminal_vertices), "terminal_reason": int(out.terminal_reason),
+                "level_vertices": list(out.level_vertices[:L]), "level_edges": list(out.level_edges[:L]),
+                "level_repeat": list(out.level_repeat[:max(L - 1, 0)])}
 
     def unit_detail(self, units: int, cells: int, probes: int) -> dict:
         names = ("projection_share", "residual_share", "finite_bias", "finite_variance", "residual_mass",

@@ -12,6 +12,8 @@
 #include "fevc_b200.h"
 #include "counter_rng.h"
 #include "engine.h"
+#include "cmg_host.h"
+#include "hybrid.h"
 #include "prep.h"
 
 using namespace fevcb;
@@ -85,6 +87,7 @@ struct Prepared {
   FevcbSolveOptionsV1 device_options{sizeof(FevcbSolveOptionsV1), 0, 0, 0};
   std::vector<double> control_values;  // contiguous copy for the problem view
   std::shared_ptr<DeviceEngine> device;
+  int device_preconditioner = 0;  // preconditioner the device engine was built with
   SolveOptions last_options;
   bool solved_once = false;
 };
@@ -263,6 +266,7 @@ SolveOptions options_from_v1(const VckssEngineSolveRequestV1& q, bool observatio
   o.rank_tolerance = q.rank_tolerance;
   o.block_tolerance = q.block_tolerance;
   o.deletion_mode = q.deletion_mode;
+  o.solver_route = q.solver_route;
   return o;
 }
 
@@ -283,8 +287,15 @@ void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr, bool generi
     intr.check("jla_full_fit");
     o.centering = p.centering;
     o.block_columns = int(p.device_options.block_columns);
+    // the device option wins; otherwise the request's route picks the
+    // preconditioner (CMG route -> aggregation multigrid, else Jacobi)
     o.preconditioner = int(p.device_options.preconditioner);
-    if (!p.device) p.device = make_device_engine(p.problem, p.plan, o.preconditioner);
+    if (o.preconditioner == 0) o.preconditioner = o.solver_route == VCKSS_ROUTE_CMG_PCG ? 2 : 1;
+    if (p.device && p.device_preconditioner != o.preconditioner) p.device.reset();
+    if (!p.device) {
+      p.device = make_device_engine(p.problem, p.plan, o.preconditioner);
+      p.device_preconditioner = o.preconditioner;
+    }
     auto res = std::make_unique<SolveResult>(device_solve(*p.device, p.problem, p.plan, o, true));
     intr.check("jla_finalize");
     p.last_options = o;
@@ -1008,6 +1019,56 @@ int32_t fevcb_engine_problem_view_v1(uint64_t generation, FevcbProblemViewV1* ou
     v.row_copy_offset = j.observation ? j.row_copy_offset.data() : nullptr;
     v.deletion_mode = p.deletion_mode;
     std::memcpy(out, &v, sizeof(v));
+  });
+}
+
+int32_t fevcb_engine_cmg_summary_v1(uint64_t generation, uint32_t eliminate_max_degree, FevcbCmgSummaryV1* out,
+                                    uint32_t cap) {
+  return status([&] {
+    require_capacity<FevcbCmgSummaryV1>(out, cap, "CMG summary");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_cmg_summary");
+    uint32_t degree = eliminate_max_degree ? eliminate_max_degree : ELIMINATE_MAX_DEGREE;
+    std::vector<uint32_t> kw, Lptr, Lcol;
+    std::vector<int32_t> ki;
+    std::vector<double> cs, wd, Lval, Ld;
+    build_hybrid(p.problem, degree, kw, ki, cs, wd, Lptr, Lcol, Lval, Ld);
+    MultigridReport rep;
+    build_cmg_hierarchy(uint32_t(Ld.size()), Lptr, Lcol, Lval, Ld, MultigridOptions(), rep);
+    FevcbCmgSummaryV1 v{};
+    v.struct_size = sizeof(v);
+    v.eliminate_max_degree = degree;
+    v.vertices = Ld.size();
+    v.edges = Lcol.size() / 2;
+    v.hierarchy_levels = rep.vertices.size();
+    v.terminal_vertices = rep.vertices.empty() ? 0 : rep.vertices.back();
+    v.terminal_reason = uint32_t(rep.terminal_reason);
+    for (size_t i = 0; i < rep.vertices.size() && i < 32; ++i) {
+      v.level_vertices[i] = rep.vertices[i];
+      v.level_edges[i] = rep.nonzeros[i] / 2;
+    }
+    for (size_t i = 0; i < rep.repeat.size() && i < 32; ++i) v.level_repeat[i] = uint32_t(rep.repeat[i]);
+    std::memcpy(out, &v, sizeof(v));
+  });
+}
+
+int32_t fevcb_cmg_aggregate_v1(uint32_t n, const uint32_t* ptr, const uint32_t* col, const double* val,
+                               double threshold, uint32_t* labels, uint32_t* aggregates) {
+  return status([&] {
+    if (!ptr || !labels || !aggregates || (n > 0 && ptr[n] > 0 && (!col || !val)))
+      fail(INVALID_INPUT, "cmg_aggregate", "null graph or output pointer");
+    if (!(threshold >= 0.0 && threshold <= 1.0))
+      fail(INVALID_INPUT, "cmg_aggregate", "low effective degree threshold must lie in [0, 1]");
+    std::vector<uint32_t> P(ptr, ptr + n + 1), Cc(col, col + ptr[n]);
+    std::vector<double> V(val, val + ptr[n]), D(n, 0.0);
+    for (uint32_t v = 0; v < n; ++v)
+      for (uint32_t e = P[v]; e < P[v + 1]; ++e) {
+        if (Cc[e] >= n || !(V[e] > 0.0)) fail(INVALID_INPUT, "cmg_aggregate", "invalid edge");
+        D[v] += V[e];
+      }
+    std::vector<uint32_t> out;
+    *aggregates = forest_aggregation(n, P, Cc, V, D, threshold, out);
+    std::copy(out.begin(), out.end(), labels);
   });
 }
 

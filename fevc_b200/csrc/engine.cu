@@ -25,6 +25,7 @@
 
 #include "engine.h"
 #include "jla_kernels.cuh"
+#include "hybrid.h"
 #include "multigrid.h"
 #include "persistent.cuh"
 #include "generic.cuh"
@@ -269,100 +270,6 @@ DeviceEngine::~DeviceEngine() {
 
 namespace {
 
-constexpr uint32_t ELIMINATE_MAX_DEGREE = 16;
-
-// Host assembly of the hybrid Laplacian (conductances) from the cells.
-void build_hybrid(const Compressed& p, std::vector<uint32_t>& kept_worker, std::vector<int32_t>& kept_index,
-                  std::vector<double>& cell_scale, std::vector<double>& worker_diag, std::vector<uint32_t>& Lptr,
-                  std::vector<uint32_t>& Lcol, std::vector<double>& Lval, std::vector<double>& Ldiag) {
-  size_t W = p.workers, F = p.firms, C = p.cells;
-  worker_diag.assign(W, 0.0);
-  kept_index.assign(W, -1);
-  cell_scale.assign(C, 0.0);
-  const auto& wp = p.worker_index.ptr;
-  for (size_t w = 0; w < W; ++w) {
-    double d = 0.0;
-    for (uint64_t c = wp[w]; c < wp[w + 1]; ++c) d += p.cell_weight[c];
-    if (!(d > 0.0) || !std::isfinite(d))
-      fail(GRAPH_UNIDENTIFIED, "operator", "worker or firm information diagonal is not positive and finite");
-    worker_diag[w] = d;
-    if (wp[w + 1] - wp[w] > ELIMINATE_MAX_DEGREE) {
-      kept_index[w] = int32_t(kept_worker.size());
-      kept_worker.push_back(uint32_t(w));
-    }
-  }
-  size_t n = F + kept_worker.size();
-  // triplets (row, col, value) with row != col
-  std::vector<uint64_t> key;
-  std::vector<double> val;
-  for (size_t w = 0; w < W; ++w) {
-    uint64_t b = wp[w], e = wp[w + 1];
-    if (kept_index[w] >= 0) {
-      uint64_t v = F + kept_index[w];
-      for (uint64_t c = b; c < e; ++c) {
-        uint64_t f = p.cell_firm[c];
-        key.push_back((v << 32) | f);
-        val.push_back(p.cell_weight[c]);
-        key.push_back((f << 32) | v);
-        val.push_back(p.cell_weight[c]);
-      }
-    } else {
-      double d = worker_diag[w];
-      for (uint64_t c = b; c < e; ++c) cell_scale[c] = p.cell_weight[c] / d;
-      for (uint64_t i = b; i < e; ++i)
-        for (uint64_t j = b; j < e; ++j) {
-          if (i == j) continue;
-          key.push_back((uint64_t(p.cell_firm[i]) << 32) | p.cell_firm[j]);
-          val.push_back(p.cell_weight[i] * p.cell_weight[j] / d);
-        }
-    }
-  }
-  std::vector<uint32_t> order(key.size());
-  std::iota(order.begin(), order.end(), 0u);
-  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b] || (key[a] == key[b] && a < b); });
-  Lptr.assign(n + 1, 0);
-  Lcol.clear();
-  Lval.clear();
-  for (size_t i = 0; i < order.size();) {
-    uint64_t k = key[order[i]];
-    double s = 0.0;
-    while (i < order.size() && key[order[i]] == k) s += val[order[i++]];
-    Lcol.push_back(uint32_t(k & 0xffffffffu));
-    Lval.push_back(s);
-    Lptr[(k >> 32) + 1]++;
-  }
-  for (size_t v = 0; v < n; ++v) Lptr[v + 1] += Lptr[v];
-  Ldiag.assign(n, 0.0);
-  for (size_t v = 0; v < n; ++v) {
-    double s = 0.0;
-    for (uint32_t e = Lptr[v]; e < Lptr[v + 1]; ++e) s += Lval[e];
-    if (!(s > 0.0)) fail(GRAPH_UNIDENTIFIED, "operator", "hybrid Laplacian has an isolated vertex");
-    Ldiag[v] = s;
-  }
-}
-
-// Cut every CSR row into segments of at most SEG items.
-void build_segments(const std::vector<uint32_t>& ptr, Segments& sg, cudaStream_t s, uint64_t& h2d) {
-  size_t rows = ptr.size() - 1;
-  std::vector<uint32_t> row, begin, end, first(rows + 1, 0);
-  for (size_t r = 0; r < rows; ++r) {
-    first[r] = uint32_t(row.size());
-    uint32_t b = ptr[r], e = ptr[r + 1];
-    if (b == e) continue;
-    for (uint32_t x = b; x < e; x += SEG) {
-      row.push_back(uint32_t(r));
-      begin.push_back(x);
-      end.push_back(std::min(e, x + SEG));
-    }
-  }
-  first[rows] = uint32_t(row.size());
-  sg.count = uint32_t(row.size());
-  upload(sg.row, row, s, h2d);
-  upload(sg.begin, begin, s, h2d);
-  upload(sg.end, end, s, h2d);
-  upload(sg.row_first, first, s, h2d);
-}
-
 }  // namespace
 
 std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaPlan& plan, int preconditioner) {
@@ -524,7 +431,7 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     std::vector<uint32_t> kw, Lptr, Lcol;
     std::vector<int32_t> ki;
     std::vector<double> cs, wd, Lval, Ld;
-    build_hybrid(p, kw, ki, cs, wd, Lptr, Lcol, Lval, Ld);
+    build_hybrid(p, ELIMINATE_MAX_DEGREE, kw, ki, cs, wd, Lptr, Lcol, Lval, Ld);
     e->kept = uint32_t(kw.size());
     e->n = e->F + e->kept;
     std::vector<double> dinv(Ld.size());
@@ -754,6 +661,60 @@ int pcg_run(DeviceEngine& e, BlockWork& w, Launch L, int iterations) {
   return mx;
 }
 
+// Multigrid-preconditioned blocked PCG: one iteration is q = L p with p.q,
+// the step length, x/r update with r.r, z = M^{-1} r (the CMG cycle), r.z,
+// the direction coefficient and convergence, and p = z + beta p.  `chunk`
+// iterations are captured once as a CUDA graph and replayed; the host reads
+// the active-column count between replays.  Returns the largest per-column
+// iteration count, as pcg_run does.
+template <int K>
+void mg_iteration(DeviceEngine& e, BlockWork& w, Launch L, cudaStream_t s) {
+  double* pa = e.partial.p;
+  double* pb = e.partial.p + size_t(L.grid) * K;
+  k_spmm_dot<K><<<L.grid, THREADS, 0, s>>>(e.n, e.L_ptr.p, e.L_col.p, e.L_val.p, e.L_diag.p, w.p.p, w.q.p, pa);
+  k_step_alpha<K><<<1, 128, 0, s>>>(pa, L.grid, w.s);
+  k_update_xr<K><<<L.grid, THREADS, 0, s>>>(e.n, w.p.p, w.q.p, w.x.p, w.r.p, w.s.alpha, pa);
+  e.mg->apply(K, w.r.p, w.z.p, s);
+  k_dot<K><<<L.grid, THREADS, 0, s>>>(e.n, w.r.p, w.z.p, pb);
+  k_step_beta<K, 1><<<1, 128, 0, s>>>(pa, L.grid, pb, L.grid, w.s);
+  k_direction<K><<<L.grid, THREADS, 0, s>>>(e.n, w.z.p, w.p.p, w.s.beta);
+}
+
+constexpr int MG_GRAPH_ITERATIONS = 4;
+
+template <int K>
+int pcg_run_mg(DeviceEngine& e, BlockWork& w, Launch L, int iterations, SolveTimings& tm) {
+  if (!w.graph) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(L.s, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < MG_GRAPH_ITERATIONS; ++i) mg_iteration<K>(e, w, L, L.s);
+    cudaError_t end = cudaStreamEndCapture(L.s, &g);
+    CK(end);
+    cudaError_t inst = cudaGraphInstantiate(&w.graph, g, 0);
+    cudaGraphDestroy(g);
+    CK(inst);
+    w.graph_iters = MG_GRAPH_ITERATIONS;
+  }
+  const int per_iteration = 6 + e.mg->launches_per_apply();
+  int executed = 0;
+  CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+  CK(cudaStreamSynchronize(L.s));
+  while (*e.h_nactive > 0 && executed < iterations) {
+    CK(cudaGraphLaunch(w.graph, L.s));
+    executed += w.graph_iters;
+    tm.kernel_launches += uint64_t(w.graph_iters) * per_iteration;
+    tm.spmm_launches += w.graph_iters;
+    CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+  }
+  std::vector<int> it(K);
+  CK(cudaMemcpyAsync(it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost, L.s));
+  CK(cudaStreamSynchronize(L.s));
+  int mx = 0;
+  for (int v : it) mx = std::max(mx, v);
+  return mx;
+}
+
 // Segmented firm-side gather (op as in k_seg_firm) finished per row.
 template <int K, int OP, int MODE>
 void firm_gather(DeviceEngine& e, BlockWork& w, Launch L, const double* coef, const double* src,
@@ -796,9 +757,14 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
     int budget = int(o.maximum_iterations) - total_iters;
     if (budget <= 0)
       fail(PCG_MAX_ITERATIONS, "pcg", "blocked PCG reached the iteration limit " + std::to_string(o.maximum_iterations));
-    int done = pcg_run<K>(e, w, L, budget);
-    tm.kernel_launches += 1;
-    tm.spmm_launches += 1;
+    int done;
+    if (e.preconditioner == 2) {
+      done = pcg_run_mg<K>(e, w, L, budget, tm);
+    } else {
+      done = pcg_run<K>(e, w, L, budget);
+      tm.kernel_launches += 1;
+      tm.spmm_launches += 1;
+    }
     total_iters = done;
     if (*e.h_nactive != 0)
       fail(PCG_MAX_ITERATIONS, "pcg", "blocked PCG reached the iteration limit " + std::to_string(o.maximum_iterations));

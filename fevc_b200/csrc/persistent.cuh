@@ -31,6 +31,28 @@ struct Segments {
   DBuf<uint32_t> row_first;  // first segment of each row (rows + 1 entries)
 };
 
+// Cut every CSR row into segments of at most SEG items.
+inline void build_segments(const std::vector<uint32_t>& ptr, Segments& sg, cudaStream_t s, uint64_t& h2d) {
+  size_t rows = ptr.size() - 1;
+  std::vector<uint32_t> row, begin, end, first(rows + 1, 0);
+  for (size_t r = 0; r < rows; ++r) {
+    first[r] = uint32_t(row.size());
+    uint32_t b = ptr[r], e = ptr[r + 1];
+    if (b == e) continue;
+    for (uint32_t x = b; x < e; x += SEG) {
+      row.push_back(uint32_t(r));
+      begin.push_back(x);
+      end.push_back(std::min(e, x + SEG));
+    }
+  }
+  first[rows] = uint32_t(row.size());
+  sg.count = uint32_t(row.size());
+  upload(sg.row, row, s, h2d);
+  upload(sg.begin, begin, s, h2d);
+  upload(sg.end, end, s, h2d);
+  upload(sg.row_first, first, s, h2d);
+}
+
 template <int K, int M>
 __device__ __forceinline__ void block_reduce_cols_big(double (&v)[M][Cols<K>::CPT], double* partial,
                                                       double (*sm)[M][K]) {

@@ -480,6 +480,33 @@ typedef struct FevcbProblemViewV1 {
 } FevcbProblemViewV1;
 int32_t fevcb_engine_problem_view_v1(uint64_t generation, FevcbProblemViewV1 *output, uint32_t output_capacity_bytes);
 
+/* The combinatorial aggregation hierarchy of a prepared generation, built on
+ * the host only (no GPU needed): the hybrid Laplacian with workers of at most
+ * `eliminate_max_degree` cells eliminated (0: the device engine's 16; 4: the
+ * reference's rule, whose vertex and edge counts and hierarchy the plugin's
+ * VckssFullCmgReceiptV1 reports) and its CMG levels. */
+typedef struct FevcbCmgSummaryV1 {
+  uint32_t struct_size;
+  uint32_t eliminate_max_degree;
+  uint64_t vertices;          /* hybrid vertices (firms + kept workers) */
+  uint64_t edges;             /* undirected hybrid edges */
+  uint64_t hierarchy_levels;
+  uint64_t terminal_vertices;
+  uint32_t terminal_reason;   /* 1 direct, 2 full contraction, 3 stagnated vertices, 4 fill, 5 level cap */
+  uint32_t reserved;
+  uint64_t level_vertices[32];
+  uint64_t level_edges[32];
+  uint32_t level_repeat[32];
+} FevcbCmgSummaryV1;
+int32_t fevcb_engine_cmg_summary_v1(uint64_t generation, uint32_t eliminate_max_degree, FevcbCmgSummaryV1 *output,
+                                    uint32_t output_capacity_bytes);
+
+/* One CMG forest-aggregation step on a Laplacian given as CSR of positive
+ * off-diagonal conductances (both directions, diagonal = row sums), host only:
+ * labels[v] is the aggregate of vertex v (first-occurrence numbering). */
+int32_t fevcb_cmg_aggregate_v1(uint32_t vertices, const uint32_t *row_ptr, const uint32_t *col, const double *weight,
+                               double low_degree_threshold, uint32_t *labels, uint32_t *aggregates);
+
 /* Time standalone launches of one hot kernel of a solved generation with CUDA
  * events, L2 flushed before each launch.  kernel: 1 persistent blocked PCG
  * (20 iterations per launch), 3 leverage atoms + cell sums, 4 leverage moments.
@@ -511,6 +538,7 @@ int32_t fevcb_counter_atoms_noalloc_v1(uint64_t seed, uint64_t domain_tag, uint6
 
 #if defined(__cplusplus)
 static_assert(sizeof(VckssEnginePrepareRequestV1) == 24, "prepare request V1 layout");
+static_assert(sizeof(FevcbCmgSummaryV1) == 688, "CMG summary layout");
 static_assert(sizeof(VckssEnginePrepareRequestV2) == 40, "prepare request V2 layout");
 static_assert(sizeof(VckssEnginePrepareRequestV3) == 56, "prepare request V3 layout");
 static_assert(sizeof(VckssEnginePrepareRequestV4) == 64, "prepare request V4 layout");

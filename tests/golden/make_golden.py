@@ -16,6 +16,7 @@ Run from the repository root:  ``python tests/golden/make_golden.py``.
 
 from __future__ import annotations
 
+import ctypes as C
 import hashlib
 import json
 import sys
@@ -151,6 +152,37 @@ def solve_record_v5(lib, panel: Panel, probes: int, centering: int, deletion_mod
             **{k: list(v) for k, v in res.items()}}
 
 
+CMG_PANELS = {
+    **{k: PANELS[k] for k in ("kat12", "small_2k", "exact_20k", "weighted_1500", "pareto13_4k", "regions_4k")},
+    "cmg_60k": dict(build=lambda: generate_panel(60000, 6000, 5, seed=61), probes=4),
+    "cmg_pareto_40k": dict(build=lambda: generate_panel(40000, 4000, 6, move_p=0.08, pareto_shape=1.3, seed=62),
+                           probes=4),
+    "cmg_regions_60k": dict(build=lambda: generate_panel(60000, 6000, 6, regions=2, cross_p=0.002, seed=63),
+                            probes=4),
+}
+
+
+def cmg_record(lib, panel: Panel) -> dict:
+    """The plugin's hybrid graph and CMG hierarchy as its full-CMG receipt
+    reports them, after a 4-probe CMG_FULL_V2 solve."""
+    e = abi.Engine(lib)
+    e.prepare(panel)
+    q = e.default_request_v5()
+    v1 = q.v4.v3.v2.v1
+    v1.probes = 4
+    v1.pcg_tolerance = 1e-8
+    v1.solver_route = 3
+    q.v4.v3.v2.algorithm = 2
+    q.threads = 4
+    q.tolerance_supplied = 1
+    q.full_cmg_v2 = 1
+    e.solve_v5(q)
+    r = abi.FullCmgReceiptV1()
+    e.check(lib.vckss_rust_engine_full_cmg_receipt_v1(e.generation, C.byref(r), C.sizeof(r)))
+    e.release()
+    return {k: int(getattr(r, k)) for k in ("vertices", "edges", "hierarchy_levels", "terminal_vertices")}
+
+
 def error_cases():
     base = kat12()
 
@@ -222,10 +254,26 @@ def solve_record(lib, panel: Panel, probes: int, centering: int) -> dict:
             **{k: list(v) for k, v in res.items()}}
 
 
+def write_cmg_cases(lib, meta: dict) -> None:
+    lib.vckss_rust_engine_full_cmg_receipt_v1.restype = C.c_int32
+    lib.vckss_rust_engine_full_cmg_receipt_v1.argtypes = [C.c_uint64, C.c_void_p, C.c_uint32]
+    cmg = {}
+    for name, spec in CMG_PANELS.items():
+        panel = spec["build"]()
+        cmg[name] = {"panel_sha256": panel_digest(panel), **cmg_record(lib, panel)}
+        print(name, cmg[name])
+    (HERE / "cmg_cases.json").write_text(json.dumps({"meta": meta, "panels": cmg}, indent=1))
+
+
 def main() -> None:
+    """All fixtures; with the argument ``cmg`` only cmg_cases.json."""
     if not PLUGIN.exists():
         raise SystemExit(f"reference plugin not found at {PLUGIN}")
     lib = abi.load(PLUGIN, bind_extensions=False)
+    if sys.argv[1:] == ["cmg"]:
+        write_cmg_cases(lib, {"generator": "tests/golden/make_golden.py cmg", "reference_plugin_version":
+                              lib.vckss_rust_backend_version().decode()})
+        return
     prep, jla = {}, {}
     for name, spec in PANELS.items():
         panel = spec["build"]()
@@ -255,6 +303,7 @@ def main() -> None:
         observation[name] = [solve_record_v5(lib, panel, spec["probes"], 0, 2),
                              solve_record_v5(lib, panel, spec["probes"], 1, 2)]
         print(name, rec["retained"], observation[name][0]["corrected"])
+    write_cmg_cases(lib, meta)
     errs = {}
     for name, panel in error_cases().items():
         rec = prepare_record(lib, panel)
@@ -267,6 +316,7 @@ def main() -> None:
     (HERE / "prep_cases.json").write_text(json.dumps({"meta": meta, "panels": prep, "errors": errs}, indent=1))
     (HERE / "jla_cases.json").write_text(json.dumps({"meta": meta, "panels": jla, "controls": controls,
                                                         "observation": observation}, indent=1))
+
 
 
 if __name__ == "__main__":
