@@ -153,6 +153,10 @@ class FevcbSolveOptionsV1(Struct):
     _fields_ = [("struct_size", u32), ("block_columns", u32), ("preconditioner", u32), ("keep_unit_detail", u32)]
 
 
+class FevcbSolveOptionsV2(Struct):
+    _fields_ = [("v1", FevcbSolveOptionsV1), ("precision", u32), ("reserved", u32)]
+
+
 class FevcbSolveTimingsV1(Struct):
     _fields_ = [("struct_size", u32), ("reserved", u32), ("total_ms", f64), ("fit_ms", f64), ("leverage_ms", f64),
                 ("target_ms", f64), ("setup_ms", f64)] + [(n, u64) for n in (
@@ -431,8 +435,11 @@ class Engine:
             self.generation = 0
 
     # ---- B200 extensions
-    def device_options(self, block_columns: int = 0, preconditioner: int = 0) -> None:
-        o = FevcbSolveOptionsV1(C.sizeof(FevcbSolveOptionsV1), block_columns, preconditioner, 1)
+    def device_options(self, block_columns: int = 0, preconditioner: int = 0, precision: int = 0) -> None:
+        """Device solve options: block width, preconditioner (1 Jacobi, 2 CMG)
+        and precision (1: single-precision inner PCG, double refinement)."""
+        o = FevcbSolveOptionsV2(FevcbSolveOptionsV1(C.sizeof(FevcbSolveOptionsV2), block_columns, preconditioner, 1),
+                                precision, 0)
         self.check(self.lib.fevcb_engine_solve_options_v1(self.generation, C.byref(o)))
 
     def timings(self) -> dict:

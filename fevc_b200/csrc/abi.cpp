@@ -88,6 +88,7 @@ struct Prepared {
   std::vector<double> control_values;  // contiguous copy for the problem view
   std::shared_ptr<DeviceEngine> device;
   int device_preconditioner = 0;  // preconditioner the device engine was built with
+  uint32_t precision = 0;         // device option: 1 mixed-precision inner solves
   SolveOptions last_options;
   bool solved_once = false;
 };
@@ -287,6 +288,7 @@ void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr, bool generi
     intr.check("jla_full_fit");
     o.centering = p.centering;
     o.block_columns = int(p.device_options.block_columns);
+    o.precision = int(p.precision);
     // the device option wins; otherwise the request's route picks the
     // preconditioner (CMG route -> aggregation multigrid, else Jacobi)
     o.preconditioner = int(p.device_options.preconditioner);
@@ -883,15 +885,21 @@ int32_t fevcb_set_stream(void* stream) {
 int32_t fevcb_engine_solve_options_v1(uint64_t generation, const FevcbSolveOptionsV1* options) {
   return status([&] {
     auto o = read_struct(options, "device solve options", 0);
-    if (o.struct_size != sizeof(o)) fail(ABI_MISMATCH, "engine_ffi", "device solve options struct_size mismatch");
+    if (o.struct_size != sizeof(FevcbSolveOptionsV1) && o.struct_size != sizeof(FevcbSolveOptionsV2))
+      fail(ABI_MISMATCH, "engine_ffi", "device solve options struct_size mismatch");
+    FevcbSolveOptionsV2 o2{};
+    std::memcpy(&o2, options, o.struct_size);
     if (o.block_columns != 0 && o.block_columns != 8 && o.block_columns != 16 && o.block_columns != 32 &&
         o.block_columns != 64)
       fail(INVALID_INPUT, "engine_ffi", "block_columns must be 0, 8, 16, 32 or 64");
     if (o.preconditioner > 2) fail(INVALID_INPUT, "engine_ffi", "preconditioner must be 0, 1 or 2");
+    if (o2.precision > 1) fail(INVALID_INPUT, "engine_ffi", "precision must be 0 (double) or 1 (mixed)");
+    if (o2.reserved != 0) fail(INVALID_INPUT, "engine_ffi", "reserved fields must be zero");
     std::lock_guard<std::mutex> l(reg().mu);
     Prepared& p = reg().require(generation, "engine_solve_options");
     if (p.device && o.preconditioner != p.device_options.preconditioner) p.device.reset();
     p.device_options = o;
+    p.precision = o2.precision;
   });
 }
 
@@ -934,6 +942,7 @@ int32_t fevcb_engine_resolve_v1(uint64_t generation) {
       fail(STALE_CONTEXT, "engine_resolve", "generation has no solved result to repeat");
     SolveOptions o = p.last_options;
     o.block_columns = int(p.device_options.block_columns);
+    o.precision = int(p.precision);
     auto res = std::make_unique<SolveResult>(device_solve(*p.device, p.problem, p.plan, o, false));
     r.result = std::move(res);
   });

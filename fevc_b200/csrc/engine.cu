@@ -215,6 +215,7 @@ struct DeviceEngine {
   // hybrid Laplacian
   DBuf<uint32_t> L_ptr, L_col;
   DBuf<double> L_val, L_diag, L_dinv;
+  DBuf<float> L_val32, L_diag32, L_dinv32;  // single-precision copies for mixed-precision solves
   std::unique_ptr<Multigrid> mg;
   int preconditioner = 1;
   Segments lap_seg, firm_seg;
@@ -253,6 +254,12 @@ struct BlockWork {
   DBuf<double> st;  // 8 * K doubles of per-column state
   DBuf<int> ist;    // 2 * K + 2 ints
   PcgState s;
+  // mixed precision: single-precision inner iterate, residual, direction and
+  // segment products, and the inner solve's per-column state
+  DBuf<float> x32, r32, p32, seg32;
+  DBuf<double> st_in;
+  DBuf<int> ist_in;
+  PcgState s_in{};
   cudaGraphExec_t graph = nullptr;
   int graph_iters = 0;
   ~BlockWork() {
@@ -661,6 +668,186 @@ int pcg_run(DeviceEngine& e, BlockWork& w, Launch L, int iterations) {
   return mx;
 }
 
+// ---------------------------------------------------------------------------
+// Mixed precision: the inner blocked PCG runs in single precision on the
+// correction e of L e = r (r the FP64 reduced residual of the current x),
+// products, dots and step lengths in double; x += e and the residual
+// recomputation are FP64 (iterative refinement).  Each refinement cycle asks
+// the inner solve for a reduction of MIXED_INNER_REDUCTION or the outer
+// tolerance, whichever is looser.
+
+constexpr double MIXED_INNER_REDUCTION = 1e-5;
+constexpr int MIXED_MAX_CYCLES = 12;
+
+__global__ void k_to_float(size_t n, const double* __restrict__ src, float* __restrict__ dst) {
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    dst[i] = float(src[i]);
+}
+
+// r32 = r64, e32 = 0, p32 = D^{-1} r32; partial (r.z, r.r) of the single-precision values
+template <int K>
+__global__ void k_mixed_begin(uint32_t n, const double* __restrict__ r64, const float* __restrict__ dinv,
+                              float* __restrict__ r32, float* __restrict__ x32, float* __restrict__ p32,
+                              double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  double v[2][CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
+  int c0 = int(threadIdx.x % TPR) * CPT;
+  size_t total = size_t(n) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    if (t < total) {
+      size_t row = t / TPR, i = row * K + c0;
+      float d = dinv[row];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        float r = float(r64[i + c]);
+        float z = d * r;
+        r32[i + c] = r;
+        x32[i + c] = 0.0f;
+        p32[i + c] = z;
+        v[0][c] += double(r) * double(z);
+        v[1][c] += double(r) * double(r);
+      }
+    }
+  }
+  block_reduce_cols<K, 2>(v, partial);
+}
+
+// Per column: the outer residual r.r decides whether the column still
+// iterates; the inner target is max(reduction^2 r.r, outer target).
+template <int K>
+__global__ void k_mixed_state(const double* __restrict__ partial, int blocks, PcgState outer, PcgState inner,
+                              double reduction2) {
+  __shared__ int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  for (int j = threadIdx.x; j < K; j += blockDim.x) {
+    double rz = 0.0, rr = 0.0;
+    for (int b = 0; b < blocks; ++b) {
+      rz += partial[size_t(b) * 2 * K + j];
+      rr += partial[size_t(b) * 2 * K + K + j];
+    }
+    outer.rr[j] = rr;
+    int act = outer.active[j] && rr > outer.tol2[j];
+    outer.active[j] = act;
+    inner.active[j] = act;
+    inner.rz[j] = rz;
+    inner.tol2[j] = fmax(reduction2 * rr, outer.tol2[j]);
+    if (act) atomicAdd(&cnt, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *outer.nactive = cnt;
+    *inner.nactive = cnt;
+    *inner.breakdown = -1;
+  }
+}
+
+// x64 += e32 for every column (inactive columns carry e = 0)
+__global__ void k_mixed_add(size_t n, const float* __restrict__ e, double* __restrict__ x) {
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    x[i] += double(e[i]);
+}
+
+// outer iteration counts and breakdown from the inner state
+template <int K>
+__global__ void k_mixed_finish(PcgState outer, PcgState inner) {
+  for (int j = threadIdx.x; j < K; j += blockDim.x) outer.iters[j] = inner.iters[j];
+  if (threadIdx.x == 0 && *inner.breakdown >= 0) atomicCAS(outer.breakdown, -1, *inner.breakdown);
+}
+
+void ensure_single_precision_matrix(DeviceEngine& e) {
+  if (e.L_val32.p) return;
+  e.L_val32.alloc(e.L_val.n);
+  e.L_diag32.alloc(e.L_diag.n);
+  e.L_dinv32.alloc(e.L_dinv.n);
+  int g = grid_blocks();
+  k_to_float<<<g, THREADS, 0, e.stream>>>(e.L_val.n, e.L_val.p, e.L_val32.p);
+  k_to_float<<<g, THREADS, 0, e.stream>>>(e.L_diag.n, e.L_diag.p, e.L_diag32.p);
+  k_to_float<<<g, THREADS, 0, e.stream>>>(e.L_dinv.n, e.L_dinv.p, e.L_dinv32.p);
+  CK_LAUNCH();
+}
+
+template <int K>
+void ensure_mixed_work(DeviceEngine& e, BlockWork& w) {
+  if (w.x32.p) return;
+  size_t n = size_t(e.n) * K;
+  w.x32.alloc(n);
+  w.r32.alloc(n);
+  w.p32.alloc(n);
+  w.seg32.alloc(size_t(e.lap_seg.count) * K);
+  w.st_in.alloc(8 * K);
+  w.ist_in.alloc(2 * K + 4);
+  double* st = w.st_in.p;
+  int* ist = w.ist_in.p;
+  w.s_in = PcgState{st, st + K, st + 2 * K, st + 3 * K, st + 4 * K, st + 5 * K, st + 6 * K,
+                    ist, ist + K, ist + 2 * K, ist + 2 * K + 1};
+}
+
+// Refinement cycles from the state pcg_restart leaves (x64, r64 = b - mean -
+// L x64, outer tolerances and active columns).  Returns the largest
+// per-column inner iteration count; leaves the count of columns above the
+// outer tolerance in e.h_nactive.
+template <int K>
+int pcg_run_mixed(DeviceEngine& e, BlockWork& w, Launch L, int iterations, SolveTimings& tm) {
+  ensure_single_precision_matrix(e);
+  ensure_mixed_work<K>(e, w);
+  const size_t nk = size_t(e.n) * K;
+  CK(cudaMemcpyAsync(w.s_in.iters, w.s.iters, K * sizeof(int), cudaMemcpyDeviceToDevice, L.s));
+  int done = 0;
+  for (int cycle = 0; cycle < MIXED_MAX_CYCLES; ++cycle) {
+    k_mixed_begin<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.r.p, e.L_dinv32.p, w.r32.p, w.x32.p, w.p32.p, e.partial.p);
+    k_mixed_state<K><<<1, 128, 0, L.s>>>(e.partial.p, L.grid, w.s, w.s_in,
+                                         MIXED_INNER_REDUCTION * MIXED_INNER_REDUCTION);
+    CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    tm.kernel_launches += 2;
+    if (*e.h_nactive == 0 || done >= iterations) break;
+    PersistentPcg<K, float> a;
+    a.n = e.n;
+    a.ptr = e.L_ptr.p;
+    a.col = e.L_col.p;
+    a.val = e.L_val32.p;
+    a.diag = e.L_diag32.p;
+    a.dinv = e.L_dinv32.p;
+    a.nseg = e.lap_seg.count;
+    a.seg_row = e.lap_seg.row.p;
+    a.seg_begin = e.lap_seg.begin.p;
+    a.seg_end = e.lap_seg.end.p;
+    a.row_first = e.lap_seg.row_first.p;
+    a.seg_buf = w.seg32.p;
+    a.x = w.x32.p;
+    a.r = w.r32.p;
+    a.p = w.p32.p;
+    a.partial_a = e.partial.p;
+    a.partial_b = e.partial.p + size_t(e.coop_blocks) * K;
+    a.s = w.s_in;
+    a.max_iters = iterations - done;
+    void* args[] = {&a};
+    CK(cudaLaunchCooperativeKernel((const void*)k_pcg_persistent<K, float>, dim3(e.coop_blocks),
+                                   dim3(PERSIST_THREADS), args, 0, L.s));
+    std::vector<int> it(K);
+    CK(cudaMemcpyAsync(it.data(), w.s_in.iters, K * sizeof(int), cudaMemcpyDeviceToHost, L.s));
+    // x += e; r = (b - mean) - L x in double
+    k_mixed_add<<<L.grid, THREADS, 0, L.s>>>(nk, w.x32.p, w.x.p);
+    k_center<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p, w.s.mean, w.q.p, w.z.p);
+    k_spmm<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_ptr.p, e.L_col.p, e.L_val.p, e.L_diag.p, w.x.p, w.q.p, w.r.p);
+    CK(cudaStreamSynchronize(L.s));
+    tm.kernel_launches += 4;
+    tm.spmm_launches += 2;
+    int mx = 0;
+    for (int v : it) mx = std::max(mx, v);
+    done = mx;
+  }
+  k_mixed_finish<K><<<1, 128, 0, L.s>>>(w.s, w.s_in);
+  CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+  CK(cudaStreamSynchronize(L.s));
+  tm.kernel_launches += 1;
+  return done;
+}
+
 // Multigrid-preconditioned blocked PCG: one iteration is q = L p with p.q,
 // the step length, x/r update with r.r, z = M^{-1} r (the CMG cycle), r.z,
 // the direction coefficient and convergence, and p = z + beta p.  `chunk`
@@ -760,6 +947,8 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
     int done;
     if (e.preconditioner == 2) {
       done = pcg_run_mg<K>(e, w, L, budget, tm);
+    } else if (o.precision == 1) {
+      done = pcg_run_mixed<K>(e, w, L, budget, tm);
     } else {
       done = pcg_run<K>(e, w, L, budget);
       tm.kernel_launches += 1;

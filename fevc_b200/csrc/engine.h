@@ -30,6 +30,7 @@ struct SolveOptions {
   int preconditioner = 0;     // 0 automatic, 1 Jacobi, 2 aggregation multigrid
   uint32_t deletion_mode = 1;  // 1 match, 2 observation (must equal the prepared mode)
   uint32_t solver_route = 0;   // the request's route: 2 diagonal PCG, 3 CMG PCG, 0 automatic
+  int precision = 0;           // 0 double, 1 single-precision inner solves with double refinement
 };
 
 // One receipt per solved right-hand side (reference `JlaRhsReceipt`,

@@ -104,31 +104,35 @@ __device__ __forceinline__ void redundant_finish(const double* __restrict__ part
   __syncthreads();
 }
 
-template <int K>
+// V is the storage type of the Laplacian values and of the iteration vectors
+// x, r, p and the segment products: double for the FP64 solve, float for the
+// inner solve of mixed-precision refinement.  Products, dots and step
+// lengths are formed in double either way.
+template <int K, typename V = double>
 struct PersistentPcg {
   uint32_t n;
   const uint32_t* ptr;
   const uint32_t* col;
-  const double* val;
-  const double* diag;
-  const double* dinv;
+  const V* val;
+  const V* diag;
+  const V* dinv;
   uint32_t nseg;
   const uint32_t* seg_row;
   const uint32_t* seg_begin;
   const uint32_t* seg_end;
   const uint32_t* row_first;  // first segment of each row
-  double* seg_buf;            // [nseg][K] segment partial products
-  double* x;
-  double* r;
-  double* p;
+  V* seg_buf;                 // [nseg][K] segment partial products
+  V* x;
+  V* r;
+  V* p;
   double* partial_a;  // [grid][1][K]
   double* partial_b;  // [grid][2][K]
   PcgState s;
   int max_iters;
 };
 
-template <int K>
-__global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(PersistentPcg<K> a) {
+template <int K, typename V = double>
+__global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(PersistentPcg<K, V> a) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
   constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
@@ -165,26 +169,27 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(Persisten
       uint32_t i = b;
       for (; i + 2 <= e; i += 2) {
         uint32_t j0 = __ldg(a.col + i), j1 = __ldg(a.col + i + 1);
-        double a0 = __ldg(a.val + i), a1 = __ldg(a.val + i + 1);
-        const double* x0 = a.p + size_t(j0) * K + c0;
-        const double* x1 = a.p + size_t(j1) * K + c0;
+        double a0 = double(__ldg(a.val + i)), a1 = double(__ldg(a.val + i + 1));
+        const V* x0 = a.p + size_t(j0) * K + c0;
+        const V* x1 = a.p + size_t(j1) * K + c0;
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) acc[c] += a0 * x0[c] + a1 * x1[c];
+        for (int c = 0; c < CPT; ++c) acc[c] += a0 * double(x0[c]) + a1 * double(x1[c]);
       }
       if (i < e) {
         uint32_t j0 = __ldg(a.col + i);
-        double a0 = __ldg(a.val + i);
-        const double* x0 = a.p + size_t(j0) * K + c0;
+        double a0 = double(__ldg(a.val + i));
+        const V* x0 = a.p + size_t(j0) * K + c0;
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) acc[c] += a0 * x0[c];
+        for (int c = 0; c < CPT; ++c) acc[c] += a0 * double(x0[c]);
       }
-      const double* pr = a.p + size_t(row) * K + c0;
+      const V* pr = a.p + size_t(row) * K + c0;
       bool first = (b == a.ptr[row]);
-      double d = first ? a.diag[row] : 0.0;
+      double d = first ? double(a.diag[row]) : 0.0;
 #pragma unroll
       for (int c = 0; c < CPT; ++c) {
-        a.seg_buf[sg * K + c0 + c] = acc[c];
-        v[0][c] += pr[c] * (d * pr[c] - acc[c]);
+        a.seg_buf[sg * K + c0 + c] = V(acc[c]);
+        double pc = double(pr[c]);
+        v[0][c] += pc * (d * pc - acc[c]);
       }
     }
     block_reduce_cols_big<K, 1>(v, a.partial_a, (double(*)[1][K])s_red);
@@ -212,20 +217,21 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(Persisten
     for (int c = 0; c < CPT; ++c) w[0][c] = w[1][c] = 0.0;
     for (size_t row = gid; row < a.n; row += ngroups) {
       uint32_t s0 = a.row_first[row], s1 = a.row_first[row + 1];
-      double dr = a.diag[row], di = a.dinv[row];
+      double dr = double(a.diag[row]), di = double(a.dinv[row]);
       size_t o = row * K + c0;
       double q[CPT];
 #pragma unroll
-      for (int c = 0; c < CPT; ++c) q[c] = dr * a.p[o + c];
+      for (int c = 0; c < CPT; ++c) q[c] = dr * double(a.p[o + c]);
       for (uint32_t sg = s0; sg < s1; ++sg)
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) q[c] -= a.seg_buf[size_t(sg) * K + c0 + c];
+        for (int c = 0; c < CPT; ++c) q[c] -= double(a.seg_buf[size_t(sg) * K + c0 + c]);
 #pragma unroll
       for (int c = 0; c < CPT; ++c) {
         double al = s_alpha[c0 + c];
-        a.x[o + c] += al * a.p[o + c];
-        double ri = a.r[o + c] - al * q[c];
-        a.r[o + c] = ri;
+        a.x[o + c] = V(double(a.x[o + c]) + al * double(a.p[o + c]));
+        V rv = V(double(a.r[o + c]) - al * q[c]);
+        a.r[o + c] = rv;
+        double ri = double(rv);
         w[0][c] += ri * (di * ri);
         w[1][c] += ri * ri;
       }
@@ -259,10 +265,11 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(Persisten
     }
     // ---- C: p = dinv r + beta p
     for (size_t row = gid; row < a.n; row += ngroups) {
-      double di = a.dinv[row];
+      double di = double(a.dinv[row]);
       size_t o = row * K + c0;
 #pragma unroll
-      for (int c = 0; c < CPT; ++c) a.p[o + c] = di * a.r[o + c] + s_beta[c0 + c] * a.p[o + c];
+      for (int c = 0; c < CPT; ++c)
+        a.p[o + c] = V(di * double(a.r[o + c]) + s_beta[c0 + c] * double(a.p[o + c]));
     }
     grid.sync();
   }

@@ -419,6 +419,13 @@ typedef struct FevcbSolveOptionsV1 {
   uint32_t keep_unit_detail;/* 1: keep per-unit leverage arrays for fevcb_engine_unit_detail_v1 */
 } FevcbSolveOptionsV1;
 
+/* Prefix-extended options (struct_size 24), accepted by the same entry. */
+typedef struct FevcbSolveOptionsV2 {
+  FevcbSolveOptionsV1 v1;
+  uint32_t precision;       /* 0 double; 1 single-precision inner PCG with double iterative refinement */
+  uint32_t reserved;
+} FevcbSolveOptionsV2;
+
 /* Wall and device timings of the last solve. */
 typedef struct FevcbSolveTimingsV1 {
   uint32_t struct_size;
@@ -539,6 +546,7 @@ int32_t fevcb_counter_atoms_noalloc_v1(uint64_t seed, uint64_t domain_tag, uint6
 #if defined(__cplusplus)
 static_assert(sizeof(VckssEnginePrepareRequestV1) == 24, "prepare request V1 layout");
 static_assert(sizeof(FevcbCmgSummaryV1) == 688, "CMG summary layout");
+static_assert(sizeof(FevcbSolveOptionsV2) == 24, "device options V2 layout");
 static_assert(sizeof(VckssEnginePrepareRequestV2) == 40, "prepare request V2 layout");
 static_assert(sizeof(VckssEnginePrepareRequestV3) == 56, "prepare request V3 layout");
 static_assert(sizeof(VckssEnginePrepareRequestV4) == 64, "prepare request V4 layout");

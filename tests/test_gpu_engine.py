@@ -221,3 +221,48 @@ def test_accounting_identity_on_a_larger_panel(lib):
         assert abs(t - (w + f + 2 * c)) <= 1e-10 * max(abs(w), abs(f), abs(t), 1.0)
     assert max(r["complete_residual"] for r in rc) <= 1e-7
     assert 0 < res["plugin"][0] < 1 and 0 < res["plugin"][1] < 1
+
+
+def solve_precision(lib, panel, *, probes, precision, centering=0, tol=1e-12, seed=8675309):
+    e = abi.Engine(lib)
+    e.prepare(panel)
+    if centering:
+        e.centering(centering)
+    e.device_options(0, 1, precision)
+    req = e.default_request()
+    req.seed = seed
+    req.probes = probes
+    req.pcg_tolerance = tol
+    req.maximum_iterations = 20000
+    e.solve(req)
+    return e
+
+
+@pytest.mark.parametrize("name", ["small_2k", "exact_20k", "weighted_1500", "regions_4k"])
+def test_mixed_precision_matches_reference(lib, golden, name):
+    """Single-precision inner PCG with double refinement reaches the same
+    FP64 complete-residual gate, so the components agree with the plugin's."""
+    rec = golden["jla"]["panels"][name][1]
+    panel = make_golden.PANELS[name]["build"]()
+    e = solve_precision(lib, panel, probes=rec["probes"], precision=1, centering=rec["centering"], seed=rec["seed"])
+    res = e.result()
+    rc = e.rhs_receipts(1 + 3 * rec["probes"])
+    e.release()
+    for key in ("plugin", "correction", "corrected", "numerical_mcse"):
+        assert rel(res[key], rec[key]) < COMPONENT_RTOL, (key, res[key], rec[key])
+    assert max(r["complete_residual"] for r in rc) <= max(10 * 1e-12, 1e-11)
+
+
+def test_mixed_precision_agrees_with_double_at_scale(lib):
+    from fevc_b200.panel import generate_panel
+
+    panel = generate_panel(200_000, 10_000, 5, seed=99)
+    out = {}
+    for precision in (0, 1):
+        e = solve_precision(lib, panel, probes=32, precision=precision, tol=1e-8)
+        out[precision] = e.result()
+        rc = e.rhs_receipts(1 + 3 * 32)
+        e.release()
+        assert max(r["complete_residual"] for r in rc) <= 1e-7
+    for key in ("plugin", "correction", "corrected"):
+        assert rel(out[1][key], out[0][key]) < 1e-6, key
