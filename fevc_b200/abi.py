@@ -158,7 +158,7 @@ class FevcbSolveOptionsV2(Struct):
 
 
 class FevcbSolveTimingsV1(Struct):
-    _fields_ = [("struct_size", u32), ("reserved", u32), ("total_ms", f64), ("fit_ms", f64), ("leverage_ms", f64),
+    _fields_ = [("struct_size", u32), ("fallbacks", u32), ("total_ms", f64), ("fit_ms", f64), ("leverage_ms", f64),
                 ("target_ms", f64), ("setup_ms", f64)] + [(n, u64) for n in (
                     "block_iterations", "column_iterations", "rhs_columns", "kernel_launches", "h2d_bytes",
                     "vertices", "edges", "kept_workers", "levels")]
@@ -276,6 +276,17 @@ SIGNATURES = {
     "fevcb_engine_problem_view_v1": (i32, [u64, C.c_void_p, u32]),
     "fevcb_engine_kernel_benchmark_v1": (i32, [u64, u32, u32, u32, C.POINTER(f64), C.POINTER(f64)]),
     "fevcb_engine_cmg_summary_v1": (i32, [u64, u32, C.c_void_p, u32]),
+    "fevcb_learned_param_count_v1": (i32, [C.POINTER(u64)]),
+    "fevcb_learned_initial_params_v1": (i32, [u64, C.POINTER(C.c_float), u64]),
+    "fevcb_learned_install_v1": (i32, [C.POINTER(C.c_float), u64]),
+    "fevcb_learned_trainer_create_v1": (i32, [u64, C.POINTER(u64)]),
+    "fevcb_learned_trainer_destroy_v1": (i32, [u64]),
+    "fevcb_learned_trainer_add_panel_v1": (i32, [u64, u64, u32, u64]),
+    "fevcb_learned_trainer_train_v1": (i32, [u64, u32, f64, C.POINTER(f64)]),
+    "fevcb_learned_trainer_gradient_v1": (i32, [u64, u32, C.POINTER(f64), C.POINTER(C.c_float), u64]),
+    "fevcb_learned_trainer_params_v1": (i32, [u64, C.POINTER(C.c_float), u64]),
+    "fevcb_learned_trainer_set_params_v1": (i32, [u64, C.POINTER(C.c_float), u64]),
+    "fevcb_learned_trainer_dump_v1": (i32, [u64, u32, C.c_void_p, u32]),
     "fevcb_cmg_aggregate_v1": (i32, [u32, C.POINTER(u32), C.POINTER(u32), C.POINTER(f64), f64, C.POINTER(u32),
                                      C.POINTER(u32)]),
     "fevcb_counter_atoms_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64, C.POINTER(i64)]),

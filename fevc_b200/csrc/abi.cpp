@@ -4,7 +4,9 @@
 // prepare -> solve -> result -> release, typed status codes with
 // thread-local text (ffi_engine.rs:2469-2498).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -14,6 +16,7 @@
 #include "engine.h"
 #include "cmg_host.h"
 #include "hybrid.h"
+#include "learned.h"
 #include "prep.h"
 
 using namespace fevcb;
@@ -892,7 +895,7 @@ int32_t fevcb_engine_solve_options_v1(uint64_t generation, const FevcbSolveOptio
     if (o.block_columns != 0 && o.block_columns != 8 && o.block_columns != 16 && o.block_columns != 32 &&
         o.block_columns != 64)
       fail(INVALID_INPUT, "engine_ffi", "block_columns must be 0, 8, 16, 32 or 64");
-    if (o.preconditioner > 2) fail(INVALID_INPUT, "engine_ffi", "preconditioner must be 0, 1 or 2");
+    if (o.preconditioner > 3) fail(INVALID_INPUT, "engine_ffi", "preconditioner must be 0, 1, 2 or 3");
     if (o2.precision > 1) fail(INVALID_INPUT, "engine_ffi", "precision must be 0 (double) or 1 (mixed)");
     if (o2.reserved != 0) fail(INVALID_INPUT, "engine_ffi", "reserved fields must be zero");
     std::lock_guard<std::mutex> l(reg().mu);
@@ -920,6 +923,7 @@ int32_t fevcb_engine_timings_v1(uint64_t generation, FevcbSolveTimingsV1* out, u
     r.column_iterations = t.column_iterations;
     r.rhs_columns = t.rhs_columns;
     r.kernel_launches = t.kernel_launches;
+    r.fallbacks = uint32_t(t.fallbacks);
     if (p.device) {
       DeviceStats s = device_stats(*p.device);
       r.setup_ms = s.setup_ms;
@@ -1057,6 +1061,151 @@ int32_t fevcb_engine_cmg_summary_v1(uint64_t generation, uint32_t eliminate_max_
       v.level_edges[i] = rep.nonzeros[i] / 2;
     }
     for (size_t i = 0; i < rep.repeat.size() && i < 32; ++i) v.level_repeat[i] = uint32_t(rep.repeat[i]);
+    std::memcpy(out, &v, sizeof(v));
+  });
+}
+
+namespace {
+std::mutex g_learned_mu;
+std::map<uint64_t, std::unique_ptr<GnnTrainer>> g_trainers;
+std::map<uint64_t, GnnTrainer::Dump> g_dumps;
+uint64_t g_next_trainer = 1;
+
+GnnTrainer& trainer(uint64_t h) {
+  auto it = g_trainers.find(h);
+  if (it == g_trainers.end()) fail(STALE_CONTEXT, "learned_train", "unknown trainer handle");
+  return *it->second;
+}
+
+void require_count(uint64_t count) {
+  if (count != gnn_param_count())
+    fail(INVALID_INPUT, "learned", "parameter count must be " + std::to_string(gnn_param_count()));
+}
+}  // namespace
+
+int32_t fevcb_learned_param_count_v1(uint64_t* count) {
+  return status([&] {
+    if (!count) fail(INVALID_INPUT, "learned", "null output");
+    *count = gnn_param_count();
+  });
+}
+
+int32_t fevcb_learned_initial_params_v1(uint64_t seed, float* params, uint64_t count) {
+  return status([&] {
+    if (!params) fail(INVALID_INPUT, "learned", "null output");
+    require_count(count);
+    auto p = gnn_initial_params(seed);
+    std::copy(p.begin(), p.end(), params);
+  });
+}
+
+int32_t fevcb_learned_install_v1(const float* params, uint64_t count) {
+  return status([&] {
+    if (!params) fail(INVALID_INPUT, "learned", "null parameters");
+    require_count(count);
+    std::vector<float> p(params, params + count);
+    for (float x : p)
+      if (!std::isfinite(x)) fail(INVALID_INPUT, "learned", "parameters must be finite");
+    set_learned_params(std::move(p));
+  });
+}
+
+int32_t fevcb_learned_trainer_create_v1(uint64_t seed, uint64_t* handle) {
+  return status([&] {
+    if (!handle) fail(INVALID_INPUT, "learned_train", "null handle output");
+    if (device_count() < 1) fail(UNSUPPORTED_FEATURE, "device", "no CUDA device is visible; training runs on a GPU");
+    std::lock_guard<std::mutex> l(g_learned_mu);
+    uint64_t h = g_next_trainer++;
+    g_trainers[h] = make_gnn_trainer(seed);
+    *handle = h;
+  });
+}
+
+int32_t fevcb_learned_trainer_destroy_v1(uint64_t handle) {
+  return status([&] {
+    std::lock_guard<std::mutex> l(g_learned_mu);
+    trainer(handle);
+    g_trainers.erase(handle);
+    g_dumps.erase(handle);
+  });
+}
+
+int32_t fevcb_learned_trainer_add_panel_v1(uint64_t handle, uint64_t generation, uint32_t columns, uint64_t seed) {
+  return status([&] {
+    std::vector<uint32_t> kw, Lptr, Lcol;
+    std::vector<int32_t> ki;
+    std::vector<double> cs, wd, Lval, Ld;
+    {
+      std::lock_guard<std::mutex> l(reg().mu);
+      Prepared& p = reg().require(generation, "learned_add_panel");
+      build_hybrid(p.problem, ELIMINATE_MAX_DEGREE, kw, ki, cs, wd, Lptr, Lcol, Lval, Ld);
+    }
+    std::lock_guard<std::mutex> l(g_learned_mu);
+    trainer(handle).add_graph(uint32_t(Ld.size()), Lptr, Lcol, Lval, Ld, int(columns), seed);
+  });
+}
+
+int32_t fevcb_learned_trainer_train_v1(uint64_t handle, uint32_t steps, double lr, double* losses) {
+  return status([&] {
+    if (!(lr > 0.0 && lr < 1.0)) fail(INVALID_INPUT, "learned_train", "learning rate must lie in (0, 1)");
+    std::lock_guard<std::mutex> l(g_learned_mu);
+    auto out = trainer(handle).train(int(steps), lr);
+    if (losses) std::copy(out.begin(), out.end(), losses);
+  });
+}
+
+int32_t fevcb_learned_trainer_gradient_v1(uint64_t handle, uint32_t graph, double* loss, float* gradient,
+                                          uint64_t count) {
+  return status([&] {
+    if (!loss || !gradient) fail(INVALID_INPUT, "learned_train", "null output");
+    require_count(count);
+    std::lock_guard<std::mutex> l(g_learned_mu);
+    GnnTrainer& t = trainer(handle);
+    if (graph >= uint32_t(t.graphs())) fail(INVALID_INPUT, "learned_train", "graph index out of range");
+    std::vector<float> g;
+    *loss = t.gradient(int(graph), g);
+    std::copy(g.begin(), g.end(), gradient);
+  });
+}
+
+int32_t fevcb_learned_trainer_params_v1(uint64_t handle, float* params, uint64_t count) {
+  return status([&] {
+    if (!params) fail(INVALID_INPUT, "learned_train", "null output");
+    require_count(count);
+    std::lock_guard<std::mutex> l(g_learned_mu);
+    auto& p = trainer(handle).params();
+    std::copy(p.begin(), p.end(), params);
+  });
+}
+
+int32_t fevcb_learned_trainer_set_params_v1(uint64_t handle, const float* params, uint64_t count) {
+  return status([&] {
+    if (!params) fail(INVALID_INPUT, "learned_train", "null parameters");
+    require_count(count);
+    std::lock_guard<std::mutex> l(g_learned_mu);
+    gnn_trainer_set_params(trainer(handle), std::vector<float>(params, params + count));
+  });
+}
+
+int32_t fevcb_learned_trainer_dump_v1(uint64_t handle, uint32_t graph, FevcbLearnedDumpV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<FevcbLearnedDumpV1>(out, cap, "learned dump");
+    std::lock_guard<std::mutex> l(g_learned_mu);
+    GnnTrainer& t = trainer(handle);
+    if (graph >= uint32_t(t.graphs())) fail(INVALID_INPUT, "learned_train", "graph index out of range");
+    GnnTrainer::Dump& d = g_dumps[handle] = t.dump(int(graph));
+    FevcbLearnedDumpV1 v{};
+    v.struct_size = sizeof(v);
+    v.pairs = d.pairs;
+    v.vertices = d.n;
+    v.row_ptr = d.ptr.data();
+    v.col = d.col.data();
+    v.weight = d.val.data();
+    v.diagonal = d.diag.data();
+    v.features = d.X.data();
+    v.basis = d.Y.data();
+    v.error = d.E.data();
+    v.energy = d.ELE.data();
     std::memcpy(out, &v, sizeof(v));
   });
 }

@@ -26,6 +26,7 @@
 #include "engine.h"
 #include "jla_kernels.cuh"
 #include "hybrid.h"
+#include "learned.h"
 #include "multigrid.h"
 #include "persistent.cuh"
 #include "generic.cuh"
@@ -168,6 +169,19 @@ void* device_stream() {
   return g_user_stream;
 }
 
+static std::mutex g_learned_params_mu;
+static std::vector<float> g_learned_params;
+
+void set_learned_params(std::vector<float> params) {
+  std::lock_guard<std::mutex> l(g_learned_params_mu);
+  g_learned_params = std::move(params);
+}
+
+static std::vector<float> learned_params() {
+  std::lock_guard<std::mutex> l(g_learned_params_mu);
+  return g_learned_params;
+}
+
 int device_count() {
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess) {
@@ -217,6 +231,7 @@ struct DeviceEngine {
   DBuf<double> L_val, L_diag, L_dinv;
   DBuf<float> L_val32, L_diag32, L_dinv32;  // single-precision copies for mixed-precision solves
   std::unique_ptr<Multigrid> mg;
+  std::unique_ptr<LearnedPreconditioner> learned;
   int preconditioner = 1;
   Segments lap_seg, firm_seg;
   int coop_blocks = 0;
@@ -257,6 +272,7 @@ struct BlockWork {
   // mixed precision: single-precision inner iterate, residual, direction and
   // segment products, and the inner solve's per-column state
   DBuf<float> x32, r32, p32, seg32;
+  DBuf<double> zold;  // flexible PCG: the previous preconditioned residual
   DBuf<double> st_in;
   DBuf<int> ist_in;
   PcgState s_in{};
@@ -460,6 +476,12 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     if (e->preconditioner == 2) {
       e->mg = build_multigrid(e->n, Lptr, Lcol, Lval, Ld, s, h2d);
       e->stats.levels = e->mg->levels();
+    } else if (e->preconditioner == 3) {
+      std::vector<float> params = learned_params();
+      if (params.empty())
+        fail(UNSUPPORTED_FEATURE, "learned_preconditioner", "no network parameters are installed");
+      e->learned = build_learned(params, e->n, Lptr, Lcol, Lval, Ld, s, h2d);
+      e->stats.levels = 1;
     } else {
       e->stats.levels = 1;
     }
@@ -608,6 +630,8 @@ template <int K>
 void apply_preconditioner(DeviceEngine& e, BlockWork& w, Launch L, const double* r, double* z) {
   if (e.preconditioner == 2) {
     e.mg->apply(K, r, z, L.s);
+  } else if (e.preconditioner == 3) {
+    e.learned->apply(K, r, z, L.s);
   } else {
     k_jacobi<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_dinv.p, r, z, nullptr);
   }
@@ -902,6 +926,163 @@ int pcg_run_mg(DeviceEngine& e, BlockWork& w, Launch L, int iterations, SolveTim
   return mx;
 }
 
+// ---------------------------------------------------------------------------
+// Flexible PCG with the learned polynomial preconditioner: the direction
+// coefficient is beta = r'(z - z_old) / (r_old' z_old) (Polak-Ribiere), which
+// tolerates a preconditioner that is not symmetric.  Iterations are captured
+// as a CUDA graph like the multigrid loop.  A block whose columns have not
+// converged after LEARNED_CAP iterations, or that meets a nonpositive
+// curvature, is finished from its current iterate by the Jacobi PCG.
+
+constexpr int LEARNED_CAP = 300;
+
+template <int K>
+__global__ void __launch_bounds__(THREADS) k_dot2(uint32_t n, const double* __restrict__ r,
+                                                  const double* __restrict__ z, const double* __restrict__ zold,
+                                                  double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  double v[2][CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
+  int c0 = int(threadIdx.x % TPR) * CPT;
+  size_t total = size_t(n) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    if (t < total) {
+      size_t i = (t / TPR) * K + c0;
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        v[0][c] += r[i + c] * z[i + c];
+        v[1][c] += r[i + c] * zold[i + c];
+      }
+    }
+  }
+  block_reduce_cols<K, 2>(v, partial);
+}
+
+template <int K>
+__global__ void k_step_beta_flexible(const double* __restrict__ partial_rr, int blocks,
+                                     const double* __restrict__ partial2, PcgState s) {
+  __shared__ int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  for (int j = threadIdx.x; j < K; j += blockDim.x) {
+    double rr = 0.0, rz = 0.0, rzo = 0.0;
+    for (int b = 0; b < blocks; ++b) {
+      rr += partial_rr[size_t(b) * K + j];
+      rz += partial2[size_t(b) * 2 * K + j];
+      rzo += partial2[size_t(b) * 2 * K + K + j];
+    }
+    double be = 0.0;
+    if (s.active[j]) {
+      s.iters[j] += 1;
+      s.rr[j] = rr;
+      if (rr <= s.tol2[j]) {
+        s.active[j] = 0;
+      } else {
+        be = (rz - rzo) / s.rz[j];
+        s.rz[j] = rz;
+        atomicAdd(&cnt, 1);
+      }
+    }
+    s.beta[j] = be;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *s.nactive = cnt;
+}
+
+// p = z + beta p; z_old = z
+template <int K>
+__global__ void __launch_bounds__(THREADS) k_direction_flexible(uint32_t n, const double* __restrict__ z,
+                                                                double* __restrict__ p, double* __restrict__ zold,
+                                                                const double* __restrict__ beta) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  int c0 = int(threadIdx.x % TPR) * CPT;
+  double be[CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) be[c] = beta[c0 + c];
+  size_t total = size_t(n) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
+    size_t i = (t / TPR) * K + c0;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      double zi = z[i + c];
+      p[i + c] = zi + be[c] * p[i + c];
+      zold[i + c] = zi;
+    }
+  }
+}
+
+template <int K>
+void learned_iteration(DeviceEngine& e, BlockWork& w, Launch L, cudaStream_t s) {
+  double* pa = e.partial.p;
+  double* pb = e.partial.p + size_t(L.grid) * K;
+  k_spmm_dot<K><<<L.grid, THREADS, 0, s>>>(e.n, e.L_ptr.p, e.L_col.p, e.L_val.p, e.L_diag.p, w.p.p, w.q.p, pa);
+  k_step_alpha<K><<<1, 128, 0, s>>>(pa, L.grid, w.s);
+  k_update_xr<K><<<L.grid, THREADS, 0, s>>>(e.n, w.p.p, w.q.p, w.x.p, w.r.p, w.s.alpha, pa);
+  e.learned->apply(K, w.r.p, w.z.p, s);
+  k_dot2<K><<<L.grid, THREADS, 0, s>>>(e.n, w.r.p, w.z.p, w.zold.p, pb);
+  k_step_beta_flexible<K><<<1, 128, 0, s>>>(pa, L.grid, pb, w.s);
+  k_direction_flexible<K><<<L.grid, THREADS, 0, s>>>(e.n, w.z.p, w.p.p, w.zold.p, w.s.beta);
+}
+
+// Reset the breakdown flag and reactivate the columns above their tolerance.
+template <int K>
+__global__ void k_reactivate(PcgState s) {
+  for (int j = threadIdx.x; j < K; j += blockDim.x)
+    s.active[j] = (s.bb[j] > 0.0 && s.rr[j] > s.tol2[j]) ? 1 : 0;
+  if (threadIdx.x == 0) *s.breakdown = -1;
+}
+
+template <int K>
+int pcg_run_learned(DeviceEngine& e, BlockWork& w, Launch L, int iterations, SolveTimings& tm) {
+  if (!w.zold.p) w.zold.alloc(size_t(e.n) * K);
+  CK(cudaMemcpyAsync(w.zold.p, w.z.p, size_t(e.n) * K * sizeof(double), cudaMemcpyDeviceToDevice, L.s));
+  if (!w.graph) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(L.s, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < MG_GRAPH_ITERATIONS; ++i) learned_iteration<K>(e, w, L, L.s);
+    cudaError_t end = cudaStreamEndCapture(L.s, &g);
+    CK(end);
+    cudaError_t inst = cudaGraphInstantiate(&w.graph, g, 0);
+    cudaGraphDestroy(g);
+    CK(inst);
+    w.graph_iters = MG_GRAPH_ITERATIONS;
+  }
+  const int per_iteration = 6 + e.learned->launches_per_apply();
+  const int cap = std::min(iterations, LEARNED_CAP);
+  int executed = 0, bd = -1;
+  CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+  CK(cudaStreamSynchronize(L.s));
+  while (*e.h_nactive > 0 && executed < cap) {
+    CK(cudaGraphLaunch(w.graph, L.s));
+    executed += w.graph_iters;
+    tm.kernel_launches += uint64_t(w.graph_iters) * per_iteration;
+    tm.spmm_launches += w.graph_iters;
+    CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaMemcpyAsync(&bd, w.s.breakdown, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    if (bd >= 0) break;
+  }
+  std::vector<int> it(K);
+  CK(cudaMemcpyAsync(it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost, L.s));
+  CK(cudaStreamSynchronize(L.s));
+  int mx = 0;
+  for (int v : it) mx = std::max(mx, v);
+  if (*e.h_nactive > 0 || bd >= 0) {
+    // fallback: finish from the current iterate with Jacobi PCG
+    tm.fallbacks += 1;
+    k_reactivate<K><<<1, 128, 0, L.s>>>(w.s);
+    int saved = e.preconditioner;
+    e.preconditioner = 1;
+    pcg_restart<K>(e, w, L, false);
+    mx = pcg_run<K>(e, w, L, std::max(1, iterations - mx));
+    e.preconditioner = saved;
+    tm.kernel_launches += 8;
+  }
+  return mx;
+}
+
 // Segmented firm-side gather (op as in k_seg_firm) finished per row.
 template <int K, int OP, int MODE>
 void firm_gather(DeviceEngine& e, BlockWork& w, Launch L, const double* coef, const double* src,
@@ -947,6 +1128,8 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
     int done;
     if (e.preconditioner == 2) {
       done = pcg_run_mg<K>(e, w, L, budget, tm);
+    } else if (e.preconditioner == 3) {
+      done = pcg_run_learned<K>(e, w, L, budget, tm);
     } else if (o.precision == 1) {
       done = pcg_run_mixed<K>(e, w, L, budget, tm);
     } else {

@@ -53,6 +53,7 @@ struct SolveTimings {
   uint64_t kernel_launches = 0;
   uint64_t spmm_launches = 0;
   double spmm_ms = 0;               // device time of the SpMM launches (events)
+  uint64_t fallbacks = 0;           // learned-preconditioner blocks finished by the Jacobi fallback
 };
 
 struct SolveResult {
@@ -98,6 +99,8 @@ void device_atoms_noalloc(uint64_t seed, uint64_t tag, uint64_t first_probe, uin
                           const uint64_t* trials, uint64_t count, int64_t* out);
 
 int device_count();
+// Network parameters used by preconditioner 3 (learned) for engines built afterwards.
+void set_learned_params(std::vector<float> params);
 void set_device_stream(void* stream);
 void* device_stream();
 

@@ -415,7 +415,7 @@ const char *vckss_rust_engine_last_error(void);
 typedef struct FevcbSolveOptionsV1 {
   uint32_t struct_size;
   uint32_t block_columns;   /* right-hand sides per blocked PCG: 0 auto, 8, 16, 32, 64 */
-  uint32_t preconditioner;  /* 0 auto, 1 Jacobi, 2 aggregation multigrid */
+  uint32_t preconditioner;  /* 0 auto, 1 Jacobi, 2 aggregation multigrid, 3 learned (flexible PCG) */
   uint32_t keep_unit_detail;/* 1: keep per-unit leverage arrays for fevcb_engine_unit_detail_v1 */
 } FevcbSolveOptionsV1;
 
@@ -429,7 +429,7 @@ typedef struct FevcbSolveOptionsV2 {
 /* Wall and device timings of the last solve. */
 typedef struct FevcbSolveTimingsV1 {
   uint32_t struct_size;
-  uint32_t reserved;
+  uint32_t fallbacks;       /* learned-preconditioner blocks finished by the Jacobi fallback */
   double total_ms;
   double fit_ms;
   double leverage_ms;
@@ -508,6 +508,38 @@ typedef struct FevcbCmgSummaryV1 {
 int32_t fevcb_engine_cmg_summary_v1(uint64_t generation, uint32_t eliminate_max_degree, FevcbCmgSummaryV1 *output,
                                     uint32_t output_capacity_bytes);
 
+/* Learned preconditioner (no counterpart in the reference).  A trainer holds
+ * training graphs (the hybrid Laplacians of prepared generations) with
+ * residual/error pairs that CMG-PCG generates on the device, and trains the
+ * graph network with the library's own forward and backward kernels.
+ * fevcb_learned_install_v1 makes a parameter vector the network of
+ * preconditioner 3 (device solve option) for later solves. */
+int32_t fevcb_learned_param_count_v1(uint64_t *count);
+int32_t fevcb_learned_initial_params_v1(uint64_t seed, float *params, uint64_t count);
+int32_t fevcb_learned_install_v1(const float *params, uint64_t count);
+int32_t fevcb_learned_trainer_create_v1(uint64_t seed, uint64_t *handle);
+int32_t fevcb_learned_trainer_destroy_v1(uint64_t handle);
+int32_t fevcb_learned_trainer_add_panel_v1(uint64_t handle, uint64_t generation, uint32_t columns, uint64_t seed);
+int32_t fevcb_learned_trainer_train_v1(uint64_t handle, uint32_t steps, double learning_rate, double *losses);
+int32_t fevcb_learned_trainer_gradient_v1(uint64_t handle, uint32_t graph, double *loss, float *gradient,
+                                          uint64_t count);
+int32_t fevcb_learned_trainer_params_v1(uint64_t handle, float *params, uint64_t count);
+int32_t fevcb_learned_trainer_set_params_v1(uint64_t handle, const float *params, uint64_t count);
+/* Host copies of one training graph (valid until the next call on the trainer). */
+typedef struct FevcbLearnedDumpV1 {
+  uint32_t struct_size;
+  uint32_t pairs;
+  uint64_t vertices;
+  const uint32_t *row_ptr, *col;
+  const double *weight, *diagonal;
+  const float *features;  /* vertices x 8 */
+  const float *basis;     /* 4 x vertices x pairs */
+  const float *error;     /* vertices x pairs */
+  const float *energy;    /* pairs: e' L e */
+} FevcbLearnedDumpV1;
+int32_t fevcb_learned_trainer_dump_v1(uint64_t handle, uint32_t graph, FevcbLearnedDumpV1 *output,
+                                      uint32_t output_capacity_bytes);
+
 /* One CMG forest-aggregation step on a Laplacian given as CSR of positive
  * off-diagonal conductances (both directions, diagonal = row sums), host only:
  * labels[v] is the aggregate of vertex v (first-occurrence numbering). */
@@ -547,6 +579,7 @@ int32_t fevcb_counter_atoms_noalloc_v1(uint64_t seed, uint64_t domain_tag, uint6
 static_assert(sizeof(VckssEnginePrepareRequestV1) == 24, "prepare request V1 layout");
 static_assert(sizeof(FevcbCmgSummaryV1) == 688, "CMG summary layout");
 static_assert(sizeof(FevcbSolveOptionsV2) == 24, "device options V2 layout");
+static_assert(sizeof(FevcbLearnedDumpV1) == 80, "learned dump layout");
 static_assert(sizeof(VckssEnginePrepareRequestV2) == 40, "prepare request V2 layout");
 static_assert(sizeof(VckssEnginePrepareRequestV3) == 56, "prepare request V3 layout");
 static_assert(sizeof(VckssEnginePrepareRequestV4) == 64, "prepare request V4 layout");
