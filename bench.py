@@ -18,6 +18,12 @@ leverage adjustment, the target contraction and the four components.
   staged in oracle/_ref by oracle/build.py; else the C oracle) on a bounded
   sample of the same panel, all host cores.
 
+* ``forms``  the other solver forms on the same panel, one device-resident
+  step each: the plain GPU CMG-PCG form (FP64, one target probe per solve, a
+  bounded probe sample), the blocked CMG-PCG, the learned flexible PCG (with
+  the committed network parameters) and the mixed-precision solve;
+  ``speedup_vs_plain_gpu_cmg_pcg`` is ``value`` over the plain form's rate.
+
 ``--impl reference`` times the reference plugin alone (rank 0) on the same
 panel and metric and prints its own JSON line.
 """
@@ -59,6 +65,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-probes", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true")
+    ap.add_argument("--plain-probes", type=int, default=8)
     return ap.parse_args()
 
 
@@ -169,6 +177,56 @@ def cpu_baseline(panel, probes, tolerance):
                           f"({1 + 3 * probes} RHS) at tol {tolerance:g}; solve phase {r['solve_s']:.2f} s, "
                           f"prepare {r['prepare_s']:.2f} s"}
     return None
+
+
+def time_form(lib, panel, controls, probes, tolerance, block, precond, precision, stream, barrier):
+    """One device-resident step of a solver form: (ms, RHS/s, column iterations per RHS)."""
+    import torch
+
+    from fevc_b200 import abi
+
+    e = abi.Engine(lib)
+    e.prepare(panel)
+    e.device_options(block, precond, precision)
+    e.solve_v5(v5_request(e, probes, tolerance), controls_count=controls)
+    barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    e.resolve()
+    stop.record(stream)
+    barrier()
+    ms = start.elapsed_time(stop)
+    t = e.timings()
+    res = e.result()
+    e.release()
+    rhs = 1 + 3 * probes
+    return {"ms_per_step": round(ms, 3), "value": round(rhs / (ms / 1000.0), 3), "unit": UNIT, "probes": probes,
+            "iterations_per_rhs": round(t["column_iterations"] / max(t["rhs_columns"], 1), 3),
+            "fallbacks": t["fallbacks"], "corrected": [round(x, 10) for x in res["corrected"]]}
+
+
+def time_forms(lib, panel, controls, args, stream, barrier):
+    from fevc_b200 import learned
+
+    forms = {}
+    plain_probes = min(args.probes, args.plain_probes)
+    forms["plain_gpu_cmg_pcg"] = {
+        **time_form(lib, panel, controls, plain_probes, args.tolerance, 2, 2, 0, stream, barrier),
+        "form": "FP64 CMG-PCG, one target probe (two right-hand sides) per solve, "
+                f"bounded sample of {plain_probes} probes"}
+    params = learned.load_params()
+    if params is not None:
+        learned.install(lib, params)
+        forms["learned_flexible_pcg"] = {
+            **time_form(lib, panel, controls, args.probes, args.tolerance, 64, 3, 0, stream, barrier),
+            "form": "graph-network polynomial preconditioner in flexible PCG, blocks of 64 (learned_params.f32)"}
+    forms["mixed_precision"] = {
+        **time_form(lib, panel, controls, args.probes, args.tolerance, 64, 1, 1, stream, barrier),
+        "form": "single-precision inner PCG with double refinement, blocks of 64"}
+    forms["cmg_blocked"] = {
+        **time_form(lib, panel, controls, args.probes, args.tolerance, 64, 2, 0, stream, barrier),
+        "form": "FP64 CMG-PCG, blocks of 64"}
+    return forms
 
 
 def run_reference(args):
@@ -293,6 +351,13 @@ def main():
         e2e_s = float(t.item())
     e2e_value = world * rhs / e2e_s
 
+    # the other solver forms on the same panel (device-resident, one timed step
+    # each): the plain GPU CMG-PCG form on a bounded probe sample, the learned
+    # flexible PCG and the mixed-precision solve
+    forms = {}
+    if not args.no_forms:
+        forms = time_forms(lib, panel, controls, args, stream, barrier)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(panel, min(args.probes, args.cpu_probes), args.tolerance)
@@ -327,6 +392,10 @@ def main():
             "clocks": clocks.summary(),
         }
         del line["config"]["retained"]
+        if forms:
+            line["forms"] = forms
+            plain = forms["plain_gpu_cmg_pcg"]["value"]
+            line["speedup_vs_plain_gpu_cmg_pcg"] = round(value / plain, 2) if plain else None
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line))

@@ -892,9 +892,9 @@ int32_t fevcb_engine_solve_options_v1(uint64_t generation, const FevcbSolveOptio
       fail(ABI_MISMATCH, "engine_ffi", "device solve options struct_size mismatch");
     FevcbSolveOptionsV2 o2{};
     std::memcpy(&o2, options, o.struct_size);
-    if (o.block_columns != 0 && o.block_columns != 8 && o.block_columns != 16 && o.block_columns != 32 &&
-        o.block_columns != 64)
-      fail(INVALID_INPUT, "engine_ffi", "block_columns must be 0, 8, 16, 32 or 64");
+    if (o.block_columns != 0 && o.block_columns != 2 && o.block_columns != 8 && o.block_columns != 16 &&
+        o.block_columns != 32 && o.block_columns != 64)
+      fail(INVALID_INPUT, "engine_ffi", "block_columns must be 0, 2, 8, 16, 32 or 64");
     if (o.preconditioner > 3) fail(INVALID_INPUT, "engine_ffi", "preconditioner must be 0, 1, 2 or 3");
     if (o2.precision > 1) fail(INVALID_INPUT, "engine_ffi", "precision must be 0 (double) or 1 (mixed)");
     if (o2.reserved != 0) fail(INVALID_INPUT, "engine_ffi", "reserved fields must be zero");

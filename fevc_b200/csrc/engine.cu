@@ -1740,20 +1740,22 @@ SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& pl
   if (K == 0) K = 64;
   if (e.generic) {
     switch (K) {
+      case 2: run_generic<2>(e, p, plan, o, res, want_unit_detail); break;
       case 8: run_generic<8>(e, p, plan, o, res, want_unit_detail); break;
       case 16: run_generic<16>(e, p, plan, o, res, want_unit_detail); break;
       case 32: run_generic<32>(e, p, plan, o, res, want_unit_detail); break;
       case 64: run_generic<64>(e, p, plan, o, res, want_unit_detail); break;
-      default: fail(INVALID_INPUT, "jla_validate", "device block width must be 8, 16, 32 or 64");
+      default: fail(INVALID_INPUT, "jla_validate", "device block width must be 2, 8, 16, 32 or 64");
     }
     return res;
   }
   switch (K) {
+    case 2: run_jla<2>(e, p, plan, o, res, want_unit_detail); break;
     case 8: run_jla<8>(e, p, plan, o, res, want_unit_detail); break;
     case 16: run_jla<16>(e, p, plan, o, res, want_unit_detail); break;
     case 32: run_jla<32>(e, p, plan, o, res, want_unit_detail); break;
     case 64: run_jla<64>(e, p, plan, o, res, want_unit_detail); break;
-    default: fail(INVALID_INPUT, "jla_validate", "device block width must be 8, 16, 32 or 64");
+    default: fail(INVALID_INPUT, "jla_validate", "device block width must be 2, 8, 16, 32 or 64");
   }
   return res;
 }

@@ -193,11 +193,15 @@ __global__ void k_target_direction(uint32_t cells, const uint32_t* __restrict__ 
                                    const uint64_t* __restrict__ tgt_rank, const uint64_t* __restrict__ tgt_count,
                                    const double* __restrict__ tgt_scale, PhiloxKey key, uint64_t first, int nprobes,
                                    double* __restrict__ d) {
-  constexpr int B = (H + 3) / 4;
+  // probe first + j sits in lane (first + j) % 4 of Philox block (first + j) / 4;
+  // a block of H probes starting off a multiple of four spans one more block
+  constexpr int B = (H + 3) / 4 + 1;
+  const int off = int(first % 4);
   size_t total = size_t(cells) * B;
   for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
     uint32_t c = uint32_t(t / B);
     int b = int(t % B);
+    if (4 * b - off >= H) continue;  // no column of this block
     StableSumD acc[4];
     for (uint32_t s = tgt_ptr[c]; s < tgt_ptr[c + 1]; ++s) {
       int64_t a[4];
@@ -208,8 +212,8 @@ __global__ void k_target_direction(uint32_t cells, const uint32_t* __restrict__ 
     }
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
-      int j = 4 * b + l;
-      if (j < H) d[size_t(c) * H + j] = (j < nprobes) ? acc[l].finish() : 0.0;
+      int j = 4 * b + l - off;
+      if (j >= 0 && j < H) d[size_t(c) * H + j] = (j < nprobes) ? acc[l].finish() : 0.0;
     }
   }
 }

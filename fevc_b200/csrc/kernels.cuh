@@ -24,11 +24,15 @@ __global__ void k_leverage_atoms(uint32_t cells, const uint32_t* __restrict__ un
                                  const uint64_t* __restrict__ unit_offset, PhiloxKey key, uint64_t tag,
                                  uint64_t first, int ncols, double* __restrict__ unit_atoms,
                                  double* __restrict__ cell_atoms) {
-  constexpr int B = (K + 3) / 4;  // probe blocks per row
+  // probe first + j sits in lane (first + j) % 4 of Philox block (first + j) / 4;
+  // a block of K probes starting off a multiple of four spans one more block
+  constexpr int B = (K + 3) / 4 + 1;
+  const int off = int(first % 4);
   size_t total = size_t(cells) * B;
   for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
     uint32_t c = uint32_t(t / B);
     int b = int(t % B);
+    if (4 * b - off >= K) continue;  // no column of this block
     double acc[4] = {0, 0, 0, 0};
     for (uint32_t g = unit_ptr[c]; g < unit_ptr[c + 1]; ++g) {
       int64_t a[4];
@@ -38,8 +42,8 @@ __global__ void k_leverage_atoms(uint32_t cells, const uint32_t* __restrict__ un
         rademacher_block_sums(key, tag, first / 4 + b, unit_rank[g], unit_count[g], a);
 #pragma unroll
       for (int l = 0; l < 4; ++l) {
-        int j = 4 * b + l;
-        if (j < K) {
+        int j = 4 * b + l - off;
+        if (j >= 0 && j < K) {
           double v = (j < ncols) ? double(a[l]) : 0.0;
           if (unit_atoms) unit_atoms[size_t(g) * K + j] = v;
           acc[l] += v;
@@ -48,8 +52,8 @@ __global__ void k_leverage_atoms(uint32_t cells, const uint32_t* __restrict__ un
     }
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
-      int j = 4 * b + l;
-      if (j < K) cell_atoms[size_t(c) * K + j] = acc[l];
+      int j = 4 * b + l - off;
+      if (j >= 0 && j < K) cell_atoms[size_t(c) * K + j] = acc[l];
     }
   }
 }

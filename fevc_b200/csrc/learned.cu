@@ -530,6 +530,7 @@ class PolyPreconditioner final : public LearnedPreconditioner {
   void apply(int K, const double* r, double* z, cudaStream_t s) override {
     switch (K) {
       case 1: run<1>(r, z, s); break;
+      case 2: run<2>(r, z, s); break;
       case 8: run<8>(r, z, s); break;
       case 16: run<16>(r, z, s); break;
       case 32: run<32>(r, z, s); break;

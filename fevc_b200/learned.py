@@ -153,3 +153,28 @@ def train_default(lib, panels: int = 24, steps: int = 600, lr: float = 3e-3, col
             t.add_panel(panel, columns=columns, seed=100 + i)
         losses = t.train(steps, lr)
         return t.params, losses
+
+
+def main() -> None:
+    """Train on seeded panels on the GPU and write the parameter file."""
+    import argparse
+
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--panels", type=int, default=64)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--columns", type=int, default=16)
+    ap.add_argument("--workers", type=int, default=20_000)
+    ap.add_argument("--firms", type=int, default=1_500)
+    ap.add_argument("--out", default=str(PARAMS_FILE))
+    args = ap.parse_args()
+    lib = abi.load()
+    params, losses = train_default(lib, args.panels, args.steps, args.lr, args.columns, args.workers, args.firms)
+    save_params(params, Path(args.out))
+    k = max(1, len(losses) // 20)
+    print({"panels": args.panels, "steps": args.steps, "first_loss": float(np.mean(losses[:k])),
+           "last_loss": float(np.mean(losses[-k:])), "out": args.out})
+
+
+if __name__ == "__main__":
+    main()

@@ -414,7 +414,7 @@ const char *vckss_rust_engine_last_error(void);
 /* Device options applied to the next solve of a generation. */
 typedef struct FevcbSolveOptionsV1 {
   uint32_t struct_size;
-  uint32_t block_columns;   /* right-hand sides per blocked PCG: 0 auto, 8, 16, 32, 64 */
+  uint32_t block_columns;   /* right-hand sides per blocked PCG: 0 auto, 2 (one target probe per solve), 8, 16, 32, 64 */
   uint32_t preconditioner;  /* 0 auto, 1 Jacobi, 2 aggregation multigrid, 3 learned (flexible PCG) */
   uint32_t keep_unit_detail;/* 1: keep per-unit leverage arrays for fevcb_engine_unit_detail_v1 */
 } FevcbSolveOptionsV1;

@@ -35,11 +35,13 @@ def solve(lib, panel, *, probes, route, centering=0, tol=1e-12, block=0, seed=86
     return e
 
 
-@pytest.mark.parametrize("name", ["small_2k", "exact_20k", "weighted_1500", "regions_4k"])
-def test_cmg_route_matches_reference(lib, golden, name):
+@pytest.mark.parametrize("name,block", [("small_2k", 0), ("exact_20k", 0), ("weighted_1500", 0), ("regions_4k", 0),
+                                        ("small_2k", 2)])
+def test_cmg_route_matches_reference(lib, golden, name, block):
+    """Block 2 is the plain form: one target probe (two right-hand sides) per solve."""
     rec = golden["jla"]["panels"][name][1]
     panel = make_golden.PANELS[name]["build"]()
-    e = solve(lib, panel, probes=rec["probes"], route=3, centering=rec["centering"], seed=rec["seed"])
+    e = solve(lib, panel, probes=rec["probes"], route=3, centering=rec["centering"], seed=rec["seed"], block=block)
     res = e.result()
     e.release()
     for key in ("plugin", "correction", "corrected", "numerical_mcse"):

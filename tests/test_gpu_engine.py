@@ -180,7 +180,7 @@ def test_unit_detail_matches_oracle(lib, oracle_mod, name):
         assert rel(det[key], ref[key]) < 1e-8, key
 
 
-@pytest.mark.parametrize("block", [8, 16, 32, 64])
+@pytest.mark.parametrize("block", [2, 8, 16, 32, 64])
 def test_block_width_does_not_change_the_result(lib, golden, block):
     """Probe batching is schedule-invariant (reference engine.rs:4188)."""
     rec = golden["jla"]["panels"]["exact_20k"][0]
