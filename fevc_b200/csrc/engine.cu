@@ -272,7 +272,7 @@ struct BlockWork {
   // mixed precision: single-precision inner iterate, residual, direction and
   // segment products, and the inner solve's per-column state
   DBuf<float> x32, r32, p32, seg32;
-  DBuf<double> zold;  // flexible PCG: the previous preconditioned residual
+  DBuf<double> y1, y2;  // polynomial preconditioner: D^{-1} A powers of the residual
   DBuf<double> st_in;
   DBuf<int> ist_in;
   PcgState s_in{};
@@ -504,6 +504,8 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_persistent<64>, PERSIST_THREADS, 0));
     if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the persistent PCG kernel cannot be resident on an SM");
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_persistent_poly<64>, PERSIST_THREADS, 0));
+    if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the persistent polynomial PCG kernel cannot be resident on an SM");
     e->coop_blocks = sms;  // one 1024-thread block per SM
   }
   CK(cudaEventCreate(&e->ev0));
@@ -927,104 +929,13 @@ int pcg_run_mg(DeviceEngine& e, BlockWork& w, Launch L, int iterations, SolveTim
 }
 
 // ---------------------------------------------------------------------------
-// Flexible PCG with the learned polynomial preconditioner: the direction
-// coefficient is beta = r'(z - z_old) / (r_old' z_old) (Polak-Ribiere), which
-// tolerates a preconditioner that is not symmetric.  Iterations are captured
-// as a CUDA graph like the multigrid loop.  A block whose columns have not
-// converged after LEARNED_CAP iterations, or that meets a nonpositive
-// curvature, is finished from its current iterate by the Jacobi PCG.
+// PCG with the learned polynomial preconditioner: the network's pooled
+// coefficients define one symmetric degree-3 polynomial per graph, applied
+// inside the persistent kernel (k_pcg_persistent_poly).  A block whose
+// columns have not converged after LEARNED_CAP iterations, or that meets a
+// nonpositive curvature, is finished from its current iterate by Jacobi PCG.
 
 constexpr int LEARNED_CAP = 300;
-
-template <int K>
-__global__ void __launch_bounds__(THREADS) k_dot2(uint32_t n, const double* __restrict__ r,
-                                                  const double* __restrict__ z, const double* __restrict__ zold,
-                                                  double* __restrict__ partial) {
-  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
-  double v[2][CPT];
-#pragma unroll
-  for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
-  int c0 = int(threadIdx.x % TPR) * CPT;
-  size_t total = size_t(n) * TPR, stride = size_t(gridDim.x) * blockDim.x;
-  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
-    size_t t = base + threadIdx.x;
-    if (t < total) {
-      size_t i = (t / TPR) * K + c0;
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) {
-        v[0][c] += r[i + c] * z[i + c];
-        v[1][c] += r[i + c] * zold[i + c];
-      }
-    }
-  }
-  block_reduce_cols<K, 2>(v, partial);
-}
-
-template <int K>
-__global__ void k_step_beta_flexible(const double* __restrict__ partial_rr, int blocks,
-                                     const double* __restrict__ partial2, PcgState s) {
-  __shared__ int cnt;
-  if (threadIdx.x == 0) cnt = 0;
-  __syncthreads();
-  for (int j = threadIdx.x; j < K; j += blockDim.x) {
-    double rr = 0.0, rz = 0.0, rzo = 0.0;
-    for (int b = 0; b < blocks; ++b) {
-      rr += partial_rr[size_t(b) * K + j];
-      rz += partial2[size_t(b) * 2 * K + j];
-      rzo += partial2[size_t(b) * 2 * K + K + j];
-    }
-    double be = 0.0;
-    if (s.active[j]) {
-      s.iters[j] += 1;
-      s.rr[j] = rr;
-      if (rr <= s.tol2[j]) {
-        s.active[j] = 0;
-      } else {
-        be = (rz - rzo) / s.rz[j];
-        s.rz[j] = rz;
-        atomicAdd(&cnt, 1);
-      }
-    }
-    s.beta[j] = be;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) *s.nactive = cnt;
-}
-
-// p = z + beta p; z_old = z
-template <int K>
-__global__ void __launch_bounds__(THREADS) k_direction_flexible(uint32_t n, const double* __restrict__ z,
-                                                                double* __restrict__ p, double* __restrict__ zold,
-                                                                const double* __restrict__ beta) {
-  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
-  int c0 = int(threadIdx.x % TPR) * CPT;
-  double be[CPT];
-#pragma unroll
-  for (int c = 0; c < CPT; ++c) be[c] = beta[c0 + c];
-  size_t total = size_t(n) * TPR, stride = size_t(gridDim.x) * blockDim.x;
-  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
-    size_t i = (t / TPR) * K + c0;
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-      double zi = z[i + c];
-      p[i + c] = zi + be[c] * p[i + c];
-      zold[i + c] = zi;
-    }
-  }
-}
-
-template <int K>
-void learned_iteration(DeviceEngine& e, BlockWork& w, Launch L, cudaStream_t s) {
-  double* pa = e.partial.p;
-  double* pb = e.partial.p + size_t(L.grid) * K;
-  k_spmm_dot<K><<<L.grid, THREADS, 0, s>>>(e.n, e.L_ptr.p, e.L_col.p, e.L_val.p, e.L_diag.p, w.p.p, w.q.p, pa);
-  k_step_alpha<K><<<1, 128, 0, s>>>(pa, L.grid, w.s);
-  k_update_xr<K><<<L.grid, THREADS, 0, s>>>(e.n, w.p.p, w.q.p, w.x.p, w.r.p, w.s.alpha, pa);
-  e.learned->apply(K, w.r.p, w.z.p, s);
-  k_dot2<K><<<L.grid, THREADS, 0, s>>>(e.n, w.r.p, w.z.p, w.zold.p, pb);
-  k_step_beta_flexible<K><<<1, 128, 0, s>>>(pa, L.grid, pb, w.s);
-  k_direction_flexible<K><<<L.grid, THREADS, 0, s>>>(e.n, w.z.p, w.p.p, w.zold.p, w.s.beta);
-}
 
 // Reset the breakdown flag and reactivate the columns above their tolerance.
 template <int K>
@@ -1036,35 +947,48 @@ __global__ void k_reactivate(PcgState s) {
 
 template <int K>
 int pcg_run_learned(DeviceEngine& e, BlockWork& w, Launch L, int iterations, SolveTimings& tm) {
-  if (!w.zold.p) w.zold.alloc(size_t(e.n) * K);
-  CK(cudaMemcpyAsync(w.zold.p, w.z.p, size_t(e.n) * K * sizeof(double), cudaMemcpyDeviceToDevice, L.s));
-  if (!w.graph) {
-    cudaGraph_t g = nullptr;
-    CK(cudaStreamBeginCapture(L.s, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < MG_GRAPH_ITERATIONS; ++i) learned_iteration<K>(e, w, L, L.s);
-    cudaError_t end = cudaStreamEndCapture(L.s, &g);
-    CK(end);
-    cudaError_t inst = cudaGraphInstantiate(&w.graph, g, 0);
-    cudaGraphDestroy(g);
-    CK(inst);
-    w.graph_iters = MG_GRAPH_ITERATIONS;
+  if (!w.y1.p) {
+    w.y1.alloc(size_t(e.n) * K);
+    w.y2.alloc(size_t(e.n) * K);
   }
-  const int per_iteration = 6 + e.learned->launches_per_apply();
-  const int cap = std::min(iterations, LEARNED_CAP);
-  int executed = 0, bd = -1;
-  CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
-  CK(cudaStreamSynchronize(L.s));
-  while (*e.h_nactive > 0 && executed < cap) {
-    CK(cudaGraphLaunch(w.graph, L.s));
-    executed += w.graph_iters;
-    tm.kernel_launches += uint64_t(w.graph_iters) * per_iteration;
-    tm.spmm_launches += w.graph_iters;
-    CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
-    CK(cudaMemcpyAsync(&bd, w.s.breakdown, sizeof(int), cudaMemcpyDeviceToHost, L.s));
-    CK(cudaStreamSynchronize(L.s));
-    if (bd >= 0) break;
-  }
+  const double* c = e.learned->scalar_coefficients();
+  PersistentPoly<K> P;
+  PersistentPcg<K>& a = P.a;
+  a.n = e.n;
+  a.ptr = e.L_ptr.p;
+  a.col = e.L_col.p;
+  a.val = e.L_val.p;
+  a.diag = e.L_diag.p;
+  a.dinv = e.L_dinv.p;
+  a.nseg = e.lap_seg.count;
+  a.seg_row = e.lap_seg.row.p;
+  a.seg_begin = e.lap_seg.begin.p;
+  a.seg_end = e.lap_seg.end.p;
+  a.row_first = e.lap_seg.row_first.p;
+  a.seg_buf = w.seg_buf.p;
+  a.x = w.x.p;
+  a.r = w.r.p;
+  a.p = w.p.p;
+  a.partial_a = e.partial.p;
+  a.partial_b = e.partial.p + size_t(e.coop_blocks) * K;
+  a.s = w.s;
+  a.max_iters = std::min(iterations, LEARNED_CAP);
+  P.y1 = w.y1.p;
+  P.y2 = w.y2.p;
+  P.z = w.z.p;
+  P.c0 = c[0];
+  P.c1 = c[1];
+  P.c2 = c[2];
+  P.c3 = c[3];
+  void* args[] = {&P};
+  CK(cudaLaunchCooperativeKernel((const void*)k_pcg_persistent_poly<K>, dim3(e.coop_blocks), dim3(PERSIST_THREADS),
+                                 args, 0, L.s));
+  tm.kernel_launches += 1;
+  tm.spmm_launches += 1;
+  int bd = -1;
   std::vector<int> it(K);
+  CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+  CK(cudaMemcpyAsync(&bd, w.s.breakdown, sizeof(int), cudaMemcpyDeviceToHost, L.s));
   CK(cudaMemcpyAsync(it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost, L.s));
   CK(cudaStreamSynchronize(L.s));
   int mx = 0;

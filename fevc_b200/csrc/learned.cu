@@ -524,8 +524,10 @@ class PolyPreconditioner final : public LearnedPreconditioner {
   DBuf<double> dinv;
   std::map<int, std::pair<DBuf<double>, DBuf<double>>> scratch;
 
+  double scalars[GNN_OUT] = {0, 0, 0, 0};
   int launches_per_apply() const override { return GNN_OUT - 1; }
   const float* coefficients() const override { return g.C.p; }
+  const double* scalar_coefficients() const override { return scalars; }
 
   void apply(int K, const double* r, double* z, cudaStream_t s) override {
     switch (K) {
@@ -579,7 +581,10 @@ std::unique_ptr<LearnedPreconditioner> build_learned(const std::vector<float>& p
   p.bf.alloc(params.size());
   refresh_bf16(p, s);
   forward(pc->g, p, s);
+  float c[GNN_OUT];
+  CK(cudaMemcpyAsync(c, pc->g.C.p, sizeof(c), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  for (int k = 0; k < GNN_OUT; ++k) pc->scalars[k] = double(c[k]);
   // the activations are not needed after inference
   for (int l = 0; l < GNN_LAYERS; ++l) {
     pc->g.S[l].release();

@@ -51,6 +51,8 @@ class LearnedPreconditioner {
   virtual void apply(int K, const double* r, double* z, cudaStream_t s) = 0;
   virtual int launches_per_apply() const = 0;
   virtual const float* coefficients() const = 0;  // device, n x GNN_OUT
+  // the pooled coefficients c_0..c_3 (every vertex carries the same ones)
+  virtual const double* scalar_coefficients() const = 0;
 };
 
 std::unique_ptr<LearnedPreconditioner> build_learned(const std::vector<float>& params, uint32_t n,
