@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--cpu-probes", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true")
+    ap.add_argument("--sharded", action="store_true", help="use the probe-sharded path at any N (launch with torchrun)")
     ap.add_argument("--plain-probes", type=int, default=8)
     return ap.parse_args()
 
@@ -264,7 +265,7 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dist = None
-    if world > 1:
+    if world > 1 or args.sharded:
         import datetime
 
         import torch.distributed as dist
@@ -289,22 +290,43 @@ def main():
     e.prepare(panel)
     prepare_s = time.perf_counter() - t0
     e.device_options(args.block, args.precond)
-    req = v5_request(e, args.probes, args.tolerance)
+    # N ranks: every rank contributes `probes` probes to one decomposition of
+    # probes x N (weak scaling); the leverage accumulators are all-reduced and
+    # the target draws gathered over NCCL (fevc_b200/sharded.py)
+    total_probes = args.probes * world
+    req = v5_request(e, total_probes, args.tolerance)
+    rhs = 1 + 3 * args.probes  # right-hand sides this rank solves per step
+    collectives = None
+    use_shards = world > 1 or args.sharded
+    if use_shards:
+        from fevc_b200 import sharded
+
+        collectives = sharded.torch_collectives(torch.device("cuda", local))
+
+        def step(engine):
+            backend = sharded.DeviceBackend(engine, req, controls)
+            return sharded.solve_sharded(backend, total_probes, rank, world, *collectives)
+    else:
+        def step(engine):
+            engine.resolve()
+
     t0 = time.perf_counter()
-    e.solve_v5(req, controls_count=controls)
+    if use_shards:
+        result = step(e)
+    else:
+        e.solve_v5(req, controls_count=controls)
+        result = e.result()
     torch.cuda.synchronize()
     first_solve_s = time.perf_counter() - t0
-    result = e.result()
-    rhs = 1 + 3 * args.probes
 
     for _ in range(args.warmup):
-        e.resolve()
+        step(e)
     barrier()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
         start.record(stream)
         for _ in range(args.steps):
-            e.resolve()
+            step(e)
         stop.record(stream)
         barrier()
     ms = start.elapsed_time(stop)
@@ -337,7 +359,10 @@ def main():
         g.device_options(args.block, args.precond)
         barrier()
         t0 = time.perf_counter()
-        g.solve_v5(req, controls_count=controls)
+        if use_shards:
+            step(g)
+        else:
+            g.solve_v5(req, controls_count=controls)
         g.result()
         torch.cuda.synchronize()
         t1 = time.perf_counter()
@@ -355,7 +380,7 @@ def main():
     # each): the plain GPU CMG-PCG form on a bounded probe sample, the learned
     # flexible PCG and the mixed-precision solve
     forms = {}
-    if not args.no_forms:
+    if not args.no_forms and world == 1:
         forms = time_forms(lib, panel, controls, args, stream, barrier)
 
     cpu = None
@@ -370,10 +395,14 @@ def main():
             "data": "synthetic (seeded generator, fevc_b200/panel.py)",
             "config": {"workload": f"{args.workload} panel ({panel.info['workers']} workers, "
                                    f"{panel.info['firms']} firms, {panel.info['periods']} periods), "
-                                   f"{args.probes} probes, {controls} year controls, match deletion",
-                       "probes": args.probes, "rhs_per_step": rhs, "tolerance": args.tolerance,
+                                   f"{total_probes} probes, {controls} year controls, match deletion",
+                       "probes": total_probes, "rhs_per_step": rhs * world, "tolerance": args.tolerance,
                        "block_columns": block, "preconditioner": "jacobi" if args.precond == 1 else "auto",
-                       "controls": controls, "parallelism": f"replicas x{world}",
+                       "controls": controls,
+                       "parallelism": (f"probe-sharded x{world}: {args.probes} probes per GPU, "
+                                       f"{total_probes} in the decomposition; NCCL all-reduce of the "
+                                       "leverage accumulators and gather of the draws") if use_shards
+                       else "single GPU",
                        "l2": "working set per step larger than L2 (126 MB)",
                        "retained": {"workers": int(timings["vertices"]) and None}},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
@@ -388,7 +417,7 @@ def main():
             "solver": {k: timings[k] for k in ("block_iterations", "column_iterations", "rhs_columns",
                                                "vertices", "edges", "kept_workers", "levels")},
             "phase_ms": {k: round(timings[k], 3) for k in ("fit_ms", "leverage_ms", "target_ms", "total_ms")},
-            "components": {k: [round(x, 10) for x in v] for k, v in result.items()},
+            "components": {k: [round(float(x), 10) for x in v] for k, v in result.items()},
             "clocks": clocks.summary(),
         }
         del line["config"]["retained"]

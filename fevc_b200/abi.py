@@ -276,6 +276,10 @@ SIGNATURES = {
     "fevcb_engine_problem_view_v1": (i32, [u64, C.c_void_p, u32]),
     "fevcb_engine_kernel_benchmark_v1": (i32, [u64, u32, u32, u32, C.POINTER(f64), C.POINTER(f64)]),
     "fevcb_engine_cmg_summary_v1": (i32, [u64, u32, C.c_void_p, u32]),
+    "fevcb_engine_shard_size_v1": (i32, [u64, C.POINTER(u64)]),
+    "fevcb_engine_shard_leverage_v1": (i32, [u64, C.c_void_p, u32, u32, C.POINTER(f64), u64]),
+    "fevcb_engine_shard_target_v1": (i32, [u64, C.c_void_p, u32, u32, C.POINTER(f64), u64, C.POINTER(f64)]),
+    "fevcb_engine_shard_finish_v1": (i32, [u64, C.c_void_p, C.POINTER(f64)]),
     "fevcb_learned_param_count_v1": (i32, [C.POINTER(u64)]),
     "fevcb_learned_initial_params_v1": (i32, [u64, C.POINTER(C.c_float), u64]),
     "fevcb_learned_install_v1": (i32, [C.POINTER(C.c_float), u64]),

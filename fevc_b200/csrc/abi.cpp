@@ -91,6 +91,8 @@ struct Prepared {
   std::vector<double> control_values;  // contiguous copy for the problem view
   std::shared_ptr<DeviceEngine> device;
   int device_preconditioner = 0;  // preconditioner the device engine was built with
+  Components shard_plugin;        // plug-in components of the last shard
+  SolveTimings shard_timings;     // solver counts of the shards since the last finish
   uint32_t precision = 0;         // device option: 1 mixed-precision inner solves
   SolveOptions last_options;
   bool solved_once = false;
@@ -1062,6 +1064,132 @@ int32_t fevcb_engine_cmg_summary_v1(uint64_t generation, uint32_t eliminate_max_
     }
     for (size_t i = 0; i < rep.repeat.size() && i < 32; ++i) v.level_repeat[i] = uint32_t(rep.repeat[i]);
     std::memcpy(out, &v, sizeof(v));
+  });
+}
+
+namespace {
+// Shared preamble of the shard entries: options, device engine, checks.
+SolveOptions shard_options(Prepared& p, const VckssEngineSolveRequestV5* request, uint32_t begin, uint32_t end) {
+  auto q = read_struct(request, "V5 engine solve request");
+  SolveOptions o = options_from_v5(q);
+  if (p.has_plan && p.plan.generic && q.v4.v3.v2.algorithm == VCKSS_ALGORITHM_EXACT)
+    fail(UNSUPPORTED_FEATURE, "shard", "the exact estimator is not sharded");
+  if (!p.has_plan) fail(UNSUPPORTED_FEATURE, "shard", "no JLA plan was prepared");
+  if (o.deletion_mode != p.deletion_mode)
+    fail(INVALID_INPUT, "engine_solve", "solve deletion mode differs from the prepared graph mode");
+  if (begin % 4 != 0 || begin >= end || end > o.probes)
+    fail(INVALID_INPUT, "shard", "probe range must start on a multiple of four and lie inside the probes");
+  o.centering = p.centering;
+  o.block_columns = int(p.device_options.block_columns);
+  o.precision = int(p.precision);
+  o.preconditioner = int(p.device_options.preconditioner);
+  if (o.preconditioner == 0) o.preconditioner = o.solver_route == VCKSS_ROUTE_CMG_PCG ? 2 : 1;
+  if (p.device && p.device_preconditioner != o.preconditioner) p.device.reset();
+  if (!p.device) {
+    p.device = make_device_engine(p.problem, p.plan, o.preconditioner);
+    p.device_preconditioner = o.preconditioner;
+  }
+  o.probe_begin = begin;
+  o.probe_end = end;
+  return o;
+}
+}  // namespace
+
+int32_t fevcb_engine_shard_size_v1(uint64_t generation, uint64_t* count) {
+  return status([&] {
+    if (!count) fail(INVALID_INPUT, "shard", "null output");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_shard");
+    if (!p.has_plan) fail(UNSUPPORTED_FEATURE, "shard", "no JLA plan was prepared");
+    *count = shard_accumulator_count(p.problem, p.plan);
+  });
+}
+
+int32_t fevcb_engine_shard_leverage_v1(uint64_t generation, const VckssEngineSolveRequestV5* request,
+                                       uint32_t begin, uint32_t end, double* acc, uint64_t count) {
+  return status([&] {
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_shard");
+    if (!acc || count != shard_accumulator_count(p.problem, p.plan))
+      fail(INVALID_INPUT, "shard", "accumulator buffer has the wrong length");
+    SolveOptions o = shard_options(p, request, begin, end);
+    o.shard_phase = 1;
+    SolveResult res = device_solve(*p.device, p.problem, p.plan, o, false);
+    std::copy(res.shard_accumulators.begin(), res.shard_accumulators.end(), acc);
+    {
+      SolveTimings& t = p.shard_timings;
+      t.kernel_launches += res.timings.kernel_launches;
+      t.rhs_columns += res.timings.rhs_columns;
+      t.column_iterations += res.timings.column_iterations;
+      t.pcg_iterations += res.timings.pcg_iterations;
+      t.fit_ms += res.timings.fit_ms;
+      t.leverage_ms += res.timings.leverage_ms;
+      t.target_ms += res.timings.target_ms;
+    }
+
+  });
+}
+
+int32_t fevcb_engine_shard_target_v1(uint64_t generation, const VckssEngineSolveRequestV5* request, uint32_t begin,
+                                     uint32_t end, const double* acc, uint64_t count, double* draws) {
+  return status([&] {
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_shard");
+    if (!acc || !draws || count != shard_accumulator_count(p.problem, p.plan))
+      fail(INVALID_INPUT, "shard", "accumulator or draw buffer is missing or has the wrong length");
+    if (!p.device) fail(STALE_CONTEXT, "shard", "run the leverage shard first");
+    SolveOptions o = shard_options(p, request, begin, end);
+    o.shard_phase = 2;
+    o.shard_input = acc;
+    SolveResult res = device_solve(*p.device, p.problem, p.plan, o, false);
+    for (uint32_t j = begin; j < end; ++j) {
+      const Components& d = res.target_draws[j];
+      draws[size_t(j - begin) * 4 + 0] = d.worker;
+      draws[size_t(j - begin) * 4 + 1] = d.firm;
+      draws[size_t(j - begin) * 4 + 2] = d.covariance;
+      draws[size_t(j - begin) * 4 + 3] = d.total;
+    }
+    p.shard_plugin = res.plugin;
+    {
+      SolveTimings& t = p.shard_timings;
+      t.kernel_launches += res.timings.kernel_launches;
+      t.rhs_columns += res.timings.rhs_columns;
+      t.column_iterations += res.timings.column_iterations;
+      t.pcg_iterations += res.timings.pcg_iterations;
+      t.fit_ms += res.timings.fit_ms;
+      t.leverage_ms += res.timings.leverage_ms;
+      t.target_ms += res.timings.target_ms;
+    }
+  });
+}
+
+int32_t fevcb_engine_shard_finish_v1(uint64_t generation, const VckssEngineSolveRequestV5* request,
+                                     const double* draws) {
+  return status([&] {
+    Registry& r = reg();
+    std::lock_guard<std::mutex> l(r.mu);
+    Prepared& p = r.require(generation, "engine_shard");
+    if (!draws) fail(INVALID_INPUT, "shard", "draws are missing");
+    auto q = read_struct(request, "V5 engine solve request");
+    SolveOptions o = options_from_v5(q);
+    if (!p.device) fail(STALE_CONTEXT, "shard", "no shard of this generation has run");
+    auto res = std::make_unique<SolveResult>();
+    res->plugin = p.shard_plugin;
+    res->target_draws.resize(o.probes);
+    for (uint32_t j = 0; j < o.probes; ++j) {
+      const double* d = draws + size_t(j) * 4;
+      if (!(std::isfinite(d[0]) && std::isfinite(d[1]) && std::isfinite(d[2]) && std::isfinite(d[3])))
+        fail(CORRECTION_NONFINITE, "jla_target", "a target draw is nonfinite");
+      res->target_draws[j] = Components{d[0], d[1], d[2], d[3]};
+    }
+    finish_draws(*res, o.probes);
+    res->timings = p.shard_timings;
+    res->timings.total_ms = res->timings.fit_ms + res->timings.leverage_ms + res->timings.target_ms;
+    p.shard_timings = SolveTimings();
+    o.centering = p.centering;
+    p.last_options = o;
+    r.result = std::move(res);
+    r.state = State::Solved;
   });
 }
 

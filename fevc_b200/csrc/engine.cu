@@ -244,6 +244,7 @@ struct DeviceEngine {
   DBuf<double> row_freq, row_y, Qd, Rd, alphaH, psiH, residual, deleted, beta_buf;
   bool controls_ready = false;
   std::vector<double> Sinv, Lfac;  // q x q, row-major
+  Components shard_plugin;  // the fit's plug-in components, kept between shard phases
   // leave-observation-out: rows are the units; per-row class rank and first
   // copy number, physical copy offsets, and the probe accumulators
   bool observation = false;
@@ -1139,8 +1140,9 @@ void run_leverage(DeviceEngine& e, const SolveOptions& o, SolveResult& res, uint
   BlockWork& w = get_work<K>(e);
   Launch L{grid_blocks(), e.stream};
   PhiloxKey key = philox_key(o.seed);
-  for (uint32_t first = 0; first < o.probes; first += K) {
-    int ncols = int(std::min<uint32_t>(K, o.probes - first));
+  const uint32_t end = o.probe_end ? o.probe_end : o.probes;
+  for (uint32_t first = o.probe_begin; first < end; first += K) {
+    int ncols = int(std::min<uint32_t>(K, end - first));
     k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p,
                                                      e.observation ? e.unit_offset.p : nullptr, key,
                                                      TAG_LEVERAGE, first, ncols,
@@ -1173,8 +1175,9 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
   double invT = 1.0 / e.target_total;
   res.target_draws.assign(o.probes, Components{});
   std::vector<double> tot(2 * K), sums(2 * K), draws(3 * K);
-  for (uint32_t first = 0; first < o.probes; first += H) {
-    int np = int(std::min<uint32_t>(H, o.probes - first));
+  const uint32_t end = o.probe_end ? o.probe_end : o.probes;
+  for (uint32_t first = o.probe_begin; first < end; first += H) {
+    int np = int(std::min<uint32_t>(H, end - first));
     k_target_direction<H><<<L.grid, THREADS, 0, L.s>>>(e.C, e.tgt_ptr.p, e.tgt_rank.p, e.tgt_count.p,
                                                        e.tgt_scale.p, key, first, np, w.dir.p);
     // direction totals: sum_c d and the reference scale sum_c |d| + |sum_c d|
@@ -1289,14 +1292,45 @@ double outcome_mean(const Compressed& p, Centering c) {
   return anchor + s.finish();
 }
 
+// Leverage accumulators of a shard: match units' five moment sums, or the
+// leave-observation-out per-row and per-copy sums.
+void shard_download(DeviceEngine& e, SolveResult& res) {
+  if (e.observation) {
+    res.shard_accumulators.resize(e.obs_row_acc.n + e.obs_copy_acc.n);
+    CK(cudaMemcpyAsync(res.shard_accumulators.data(), e.obs_row_acc.p, e.obs_row_acc.bytes(), cudaMemcpyDeviceToHost,
+                       e.stream));
+    CK(cudaMemcpyAsync(res.shard_accumulators.data() + e.obs_row_acc.n, e.obs_copy_acc.p, e.obs_copy_acc.bytes(),
+                       cudaMemcpyDeviceToHost, e.stream));
+  } else {
+    res.shard_accumulators.resize(size_t(e.G) * 5);
+    CK(cudaMemcpyAsync(res.shard_accumulators.data(), e.moments.p, size_t(e.G) * 5 * sizeof(double),
+                       cudaMemcpyDeviceToHost, e.stream));
+  }
+  CK(cudaStreamSynchronize(e.stream));
+}
+
+void shard_upload(DeviceEngine& e, const double* in) {
+  if (!in) fail(INVALID_INPUT, "shard", "the summed leverage accumulators are missing");
+  if (e.observation) {
+    CK(cudaMemcpyAsync(e.obs_row_acc.p, in, e.obs_row_acc.bytes(), cudaMemcpyHostToDevice, e.stream));
+    CK(cudaMemcpyAsync(e.obs_copy_acc.p, in + e.obs_row_acc.n, e.obs_copy_acc.bytes(), cudaMemcpyHostToDevice,
+                       e.stream));
+  } else {
+    CK(cudaMemcpyAsync(e.moments.p, in, size_t(e.G) * 5 * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+  }
+  CK(cudaStreamSynchronize(e.stream));
+}
+
 template <int K>
 void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o, SolveResult& res,
              bool detail) {
   Launch L{grid_blocks(), e.stream};
   auto now = [] { return std::chrono::steady_clock::now(); };
   auto t0 = now();
-  // ---- full fit (one column)
-  {
+  // ---- full fit (one column); a phase-2 shard reuses the fit of its phase 1
+  if (o.shard_phase == 2) {
+    res.plugin = e.shard_plugin;
+  } else {
     BlockWork& w = get_work<1>(e);
     k_gather<1><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, e.cell_outcome.p, w.bW.p);
     firm_gather<1, 0, 0>(e, w, L, nullptr, e.cell_outcome.p, nullptr, 0.0, nullptr, nullptr, nullptr, w.bF.p, nullptr);
@@ -1319,12 +1353,21 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
     CK(cudaStreamSynchronize(L.s));
     double T = p.target_total;
     res.plugin = finish_accounting(m[0] / T, m[1] / T, m[2] / T, m[3] / T, "jla_components");
+    e.shard_plugin = res.plugin;
     res.timings.kernel_launches += 6;
   }
   auto t1 = now();
   // ---- leverage
-  CK(cudaMemsetAsync(e.moments.p, 0, e.moments.bytes(), L.s));
-  run_leverage<K>(e, o, res, 0);
+  if (o.shard_phase != 2) {
+    CK(cudaMemsetAsync(e.moments.p, 0, e.moments.bytes(), L.s));
+    run_leverage<K>(e, o, res, 0);
+  }
+  if (o.shard_phase == 1) {
+    shard_download(e, res);
+    res.timings.fit_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    return;
+  }
+  if (o.shard_phase == 2) shard_upload(e, o.shard_input);
   // ---- adjustment
   {
     AdjustParams prm{e.C, double(o.probes), o.block_tolerance, o.rank_tolerance, outcome_mean(p, o.centering)};
@@ -1351,31 +1394,12 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
   // ---- target
   run_target<K>(e, o, res);
   auto t3 = now();
-  // ---- components
-  {
-    StableSum s[4];
-    for (auto& d : res.target_draws) {
-      s[0].add(d.worker);
-      s[1].add(d.firm);
-      s[2].add(d.covariance);
-      s[3].add(d.total);
-    }
-    double P = double(o.probes);
-    Components corr{s[0].finish() / P, s[1].finish() / P, s[2].finish() / P, s[3].finish() / P};
-    res.correction = corr;
-    res.corrected = Components{res.plugin.worker - corr.worker, res.plugin.firm - corr.firm,
-                               res.plugin.covariance - corr.covariance, res.plugin.total - corr.total};
-    StableSum q[4];
-    for (auto& d : res.target_draws) {
-      q[0].add((d.worker - corr.worker) * (d.worker - corr.worker));
-      q[1].add((d.firm - corr.firm) * (d.firm - corr.firm));
-      q[2].add((d.covariance - corr.covariance) * (d.covariance - corr.covariance));
-      q[3].add((d.total - corr.total) * (d.total - corr.total));
-    }
-    double den = P * (P - 1.0);
-    res.mcse = Components{std::sqrt(q[0].finish() / den), std::sqrt(q[1].finish() / den), std::sqrt(q[2].finish() / den),
-                          std::sqrt(q[3].finish() / den)};
+  if (o.shard_phase == 2) {
+    res.timings.target_ms = std::chrono::duration<double, std::milli>(t3 - t2).count();
+    return;
   }
+  // ---- components
+  finish_draws(res, o.probes);
   for (auto& r : res.receipts) {
     res.max_reduced_residual = std::max(res.max_reduced_residual, r.reduced_residual);
     res.max_complete_residual = std::max(res.max_complete_residual, r.complete_residual);
@@ -1504,7 +1528,9 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
   setup_controls(e, o, res.timings);
   const int q = e.q;
   // ---- joint fit: FE solve of y, then beta = S^{-1} R'W y and theta = theta_y - H beta
-  {
+  if (o.shard_phase == 2) {
+    res.plugin = e.shard_plugin;
+  } else {
     BlockWork& w = get_work<1>(e);
     k_gather<1><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, e.cell_outcome.p, w.bW.p);
     firm_gather<1, 0, 0>(e, w, L, nullptr, e.cell_outcome.p, nullptr, 0.0, nullptr, nullptr, nullptr, w.bF.p, nullptr);
@@ -1540,18 +1566,27 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     CK(cudaStreamSynchronize(L.s));
     double T = p.target_total;
     res.plugin = finish_accounting(m[0] / T, m[1] / T, m[2] / T, m[3] / T, "generic_jla_components");
+    e.shard_plugin = res.plugin;
     res.timings.kernel_launches += 12;
   }
   auto t1 = now();
   // ---- FE-only leverage probes (reference `match_leverage_moments`,
   // `observation_and_match_leverage_moments`)
-  if (e.observation) {
-    CK(cudaMemsetAsync(e.obs_row_acc.p, 0, e.obs_row_acc.bytes(), L.s));
-    CK(cudaMemsetAsync(e.obs_copy_acc.p, 0, e.obs_copy_acc.bytes(), L.s));
-  } else {
-    CK(cudaMemsetAsync(e.moments.p, 0, e.moments.bytes(), L.s));
+  if (o.shard_phase != 2) {
+    if (e.observation) {
+      CK(cudaMemsetAsync(e.obs_row_acc.p, 0, e.obs_row_acc.bytes(), L.s));
+      CK(cudaMemsetAsync(e.obs_copy_acc.p, 0, e.obs_copy_acc.bytes(), L.s));
+    } else {
+      CK(cudaMemsetAsync(e.moments.p, 0, e.moments.bytes(), L.s));
+    }
+    run_leverage<K>(e, o, res, 0);
   }
-  run_leverage<K>(e, o, res, 0);
+  if (o.shard_phase == 1) {
+    shard_download(e, res);
+    res.timings.fit_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    return;
+  }
+  if (o.shard_phase == 2) shard_upload(e, o.shard_input);
   if (e.observation) {
     // ---- deleted residual of every row from its copies
     unsigned long long init = ~0ull;
@@ -1616,30 +1651,11 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
   // ---- target draws on the full model
   run_target<K>(e, o, res, outcome_mean(p, o.centering));
   auto t3 = now();
-  {
-    StableSum s[4];
-    for (auto& d : res.target_draws) {
-      s[0].add(d.worker);
-      s[1].add(d.firm);
-      s[2].add(d.covariance);
-      s[3].add(d.total);
-    }
-    double P = double(o.probes);
-    Components corr{s[0].finish() / P, s[1].finish() / P, s[2].finish() / P, s[3].finish() / P};
-    res.correction = corr;
-    res.corrected = Components{res.plugin.worker - corr.worker, res.plugin.firm - corr.firm,
-                               res.plugin.covariance - corr.covariance, res.plugin.total - corr.total};
-    StableSum qq[4];
-    for (auto& d : res.target_draws) {
-      qq[0].add((d.worker - corr.worker) * (d.worker - corr.worker));
-      qq[1].add((d.firm - corr.firm) * (d.firm - corr.firm));
-      qq[2].add((d.covariance - corr.covariance) * (d.covariance - corr.covariance));
-      qq[3].add((d.total - corr.total) * (d.total - corr.total));
-    }
-    double den = P * (P - 1.0);
-    res.mcse = Components{std::sqrt(qq[0].finish() / den), std::sqrt(qq[1].finish() / den),
-                          std::sqrt(qq[2].finish() / den), std::sqrt(qq[3].finish() / den)};
+  if (o.shard_phase == 2) {
+    res.timings.target_ms = std::chrono::duration<double, std::milli>(t3 - t2).count();
+    return;
   }
+  finish_draws(res, o.probes);
   for (auto& r : res.receipts) {
     res.max_reduced_residual = std::max(res.max_reduced_residual, r.reduced_residual);
     res.max_complete_residual = std::max(res.max_complete_residual, r.complete_residual);
@@ -1653,6 +1669,37 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
 }
 
 }  // namespace
+
+void finish_draws(SolveResult& res, uint32_t probes) {
+  if (res.target_draws.size() != probes) fail(INTERNAL_INVARIANT_FAILED, "jla_target", "target draws are incomplete");
+  StableSum s[4];
+  for (auto& d : res.target_draws) {
+    s[0].add(d.worker);
+    s[1].add(d.firm);
+    s[2].add(d.covariance);
+    s[3].add(d.total);
+  }
+  double P = double(probes);
+  Components corr{s[0].finish() / P, s[1].finish() / P, s[2].finish() / P, s[3].finish() / P};
+  res.correction = corr;
+  res.corrected = Components{res.plugin.worker - corr.worker, res.plugin.firm - corr.firm,
+                             res.plugin.covariance - corr.covariance, res.plugin.total - corr.total};
+  StableSum q[4];
+  for (auto& d : res.target_draws) {
+    q[0].add((d.worker - corr.worker) * (d.worker - corr.worker));
+    q[1].add((d.firm - corr.firm) * (d.firm - corr.firm));
+    q[2].add((d.covariance - corr.covariance) * (d.covariance - corr.covariance));
+    q[3].add((d.total - corr.total) * (d.total - corr.total));
+  }
+  double den = P * (P - 1.0);
+  res.mcse = Components{std::sqrt(q[0].finish() / den), std::sqrt(q[1].finish() / den),
+                        std::sqrt(q[2].finish() / den), std::sqrt(q[3].finish() / den)};
+}
+
+uint64_t shard_accumulator_count(const Compressed& p, const JlaPlan& plan) {
+  if (plan.observation) return uint64_t(p.rows()) * 4 + p.physical_total * 4;
+  return uint64_t(plan.del_cell.size()) * 5;
+}
 
 SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o,
                          bool want_unit_detail) {

@@ -31,6 +31,15 @@ struct SolveOptions {
   uint32_t deletion_mode = 1;  // 1 match, 2 observation (must equal the prepared mode)
   uint32_t solver_route = 0;   // the request's route: 2 diagonal PCG, 3 CMG PCG, 0 automatic
   int precision = 0;           // 0 double, 1 single-precision inner solves with double refinement
+  // Probe sharding across devices: the leverage and target probes handled
+  // here are [probe_begin, probe_end) of the request's probes (end 0: all).
+  // Phase 1 runs the fit and the leverage probes and returns the leverage
+  // accumulators; phase 2 starts from accumulators summed over all shards
+  // (shard_input), runs the adjustment and the target probes and returns
+  // their draws.  Phase 0 is the whole solve.
+  int shard_phase = 0;
+  uint32_t probe_begin = 0, probe_end = 0;
+  const double* shard_input = nullptr;
 };
 
 // One receipt per solved right-hand side (reference `JlaRhsReceipt`,
@@ -66,7 +75,14 @@ struct SolveResult {
   std::vector<RhsReceipt> receipts;
   double max_reduced_residual = 0, max_complete_residual = 0, max_leverage = 0;
   SolveTimings timings;
+  std::vector<double> shard_accumulators;  // phase 1 output
 };
+
+// Number of leverage accumulators a shard exchanges (match units: 5 moment
+// sums each; leave-observation-out: 4 sums per row and 4 per physical copy).
+uint64_t shard_accumulator_count(const Compressed& p, const JlaPlan& plan);
+// Correction, corrected components and MCSE from all probes' target draws.
+void finish_draws(SolveResult& res, uint32_t probes);
 
 struct DeviceEngine;  // opaque
 

@@ -508,6 +508,29 @@ typedef struct FevcbCmgSummaryV1 {
 int32_t fevcb_engine_cmg_summary_v1(uint64_t generation, uint32_t eliminate_max_degree, FevcbCmgSummaryV1 *output,
                                     uint32_t output_capacity_bytes);
 
+/* Probe sharding across devices (no counterpart in the reference: its
+ * plugin runs on one host).  Every device prepares the same panel; each solves
+ * a contiguous range of the request's probes (ranges start on multiples of
+ * four, one Counter-V1 block):
+ *   1. fevcb_engine_shard_leverage_v1: the fit and the range's leverage probes;
+ *      writes the leverage accumulators (fevcb_engine_shard_size_v1 doubles);
+ *   2. the caller sums the accumulators over all devices (an all-reduce);
+ *   3. fevcb_engine_shard_target_v1: the adjustment from the summed
+ *      accumulators and the range's target probes; writes 4 doubles per probe
+ *      (worker, firm, covariance, total draws);
+ *   4. the caller gathers all probes' draws; fevcb_engine_shard_finish_v1
+ *      publishes the components as the generation's result (result_v1).
+ * The result equals the single-device solve of the same request. */
+int32_t fevcb_engine_shard_size_v1(uint64_t generation, uint64_t *accumulators);
+int32_t fevcb_engine_shard_leverage_v1(uint64_t generation, const VckssEngineSolveRequestV5 *request,
+                                       uint32_t probe_begin, uint32_t probe_end, double *accumulators,
+                                       uint64_t count);
+int32_t fevcb_engine_shard_target_v1(uint64_t generation, const VckssEngineSolveRequestV5 *request,
+                                     uint32_t probe_begin, uint32_t probe_end, const double *accumulators,
+                                     uint64_t count, double *draws);
+int32_t fevcb_engine_shard_finish_v1(uint64_t generation, const VckssEngineSolveRequestV5 *request,
+                                     const double *draws);
+
 /* Learned preconditioner (no counterpart in the reference).  A trainer holds
  * training graphs (the hybrid Laplacians of prepared generations) with
  * residual/error pairs that CMG-PCG generates on the device, and trains the

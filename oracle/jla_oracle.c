@@ -121,6 +121,14 @@ typedef struct {
   double tolerance;   /* CG tolerance when the dense factor is not used */
   double rank_tolerance, block_tolerance;
   uint32_t dense_limit; /* use the dense factor when firms <= dense_limit */
+  /* probe sharding (compressed estimator): probes [probe_begin, probe_end)
+   * (end 0: all); phase 1 stops after the leverage moments and writes their
+   * sums (units x 5) to shard_io; phase 2 reads the summed moments from
+   * shard_io, writes the range's target draws and skips the components */
+  uint32_t probe_begin, probe_end;
+  int32_t phase;
+  uint32_t reserved;
+  double* shard_io;
 } OracleOptions;
 
 typedef struct {
@@ -350,7 +358,10 @@ int oracle_jla(const OracleProblem* p, const OracleOptions* o, OracleResult* res
   /* ---- leverage moments, one probe at a time (batch invariant) */
   Stable* mom = calloc(G * 5, sizeof(Stable));
   int64_t* atoms = calloc(G > S ? G : S, sizeof(int64_t));
-  for (uint64_t probe = 0; probe < P; ++probe) {
+  const uint64_t pb = o->probe_begin, pe = o->probe_end ? o->probe_end : P;
+  if (o->phase == 2)
+    for (uint64_t i = 0; i < G * 5; ++i) mom[i].sum = o->shard_io[i];
+  for (uint64_t probe = pb; probe < (o->phase == 2 ? pb : pe); ++probe) {
     memset(bw, 0, W * 8);
     memset(bf, 0, F * 8);
     for (uint64_t g = 0; g < G; ++g) {
@@ -374,6 +385,19 @@ int oracle_jla(const OracleProblem* p, const OracleOptions* o, OracleResult* res
       st_add(&mom[g * 5 + 3], m2 * m2);
       st_add(&mom[g * 5 + 4], p2 * m2);
     }
+  }
+  if (o->phase == 1) {
+    for (uint64_t i = 0; i < G * 5; ++i) o->shard_io[i] = st_fin(&mom[i]);
+    free(mom);
+    free(atoms);
+    free(bw);
+    free(bf);
+    free(alpha);
+    free(psi);
+    free(alpha2);
+    free(psi2);
+    solver_free(&s);
+    return 0;
   }
   /* ---- adjustment */
   double mean = 0.0;
@@ -415,7 +439,7 @@ int oracle_jla(const OracleProblem* p, const OracleOptions* o, OracleResult* res
   Stable* dir = calloc(C, sizeof(Stable));
   double* d = calloc(C, 8);
   double *sw = calloc(W, 8), *sf = calloc(F, 8), *zw = calloc(W, 8), *zf = calloc(F, 8);
-  for (uint64_t probe = 0; probe < P; ++probe) {
+  for (uint64_t probe = pb; probe < pe; ++probe) {
     memset(dir, 0, C * sizeof(Stable));
     for (uint64_t k = 0; k < S; ++k) {
       int ok;
@@ -469,7 +493,7 @@ int oracle_jla(const OracleProblem* p, const OracleOptions* o, OracleResult* res
     res->target_draws[probe * 4 + 3] = a + b + 2.0 * cv;
   }
   /* ---- mean, corrected, MCSE */
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < (o->phase == 2 ? 0 : 4); ++k) {
     Stable m = {0, 0};
     for (uint64_t q = 0; q < P; ++q) st_add(&m, res->target_draws[q * 4 + k]);
     res->correction[k] = st_fin(&m) / Pd;

@@ -33,7 +33,9 @@ class ProblemView(C.Structure):
 
 class OracleOptions(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("probes", C.c_uint32), ("centering", C.c_uint32), ("tolerance", C.c_double),
-                ("rank_tolerance", C.c_double), ("block_tolerance", C.c_double), ("dense_limit", C.c_uint32)]
+                ("rank_tolerance", C.c_double), ("block_tolerance", C.c_double), ("dense_limit", C.c_uint32),
+                ("probe_begin", C.c_uint32), ("probe_end", C.c_uint32), ("phase", C.c_int32),
+                ("reserved", C.c_uint32), ("shard_io", dp)]
 
 
 class OracleResult(C.Structure):
@@ -102,7 +104,8 @@ def run(problem: OracleProblem, *, seed=8675309, probes=200, centering=0, tolera
     res = OracleResult()
     for n, a in arrays.items():
         setattr(res, n, a.ctypes.data_as(dp))
-    opt = OracleOptions(seed, probes, centering, tolerance, rank_tolerance, block_tolerance, dense_limit)
+    opt = OracleOptions(seed, probes, centering, tolerance, rank_tolerance, block_tolerance, dense_limit, 0, 0, 0, 0,
+                        None)
     fn = lib.oracle_jla_generic if (problem.controls or problem.deletion_mode == 2) else lib.oracle_jla
     code = fn(C.byref(problem), C.byref(opt), C.byref(res))
     if code != 0:
@@ -113,3 +116,30 @@ def run(problem: OracleProblem, *, seed=8675309, probes=200, centering=0, tolera
     out["solves"] = res.solves
     out["cg_iterations"] = res.cg_iterations
     return out
+
+
+def shard(problem: OracleProblem, *, phase: int, probe_begin: int, probe_end: int, io: np.ndarray, seed=8675309,
+          probes=200, centering=0, tolerance=1e-13, rank_tolerance=1e-10, block_tolerance=1e-10,
+          dense_limit=3000) -> dict:
+    """One phase of a probe shard of the compressed estimator: phase 1 writes
+    the range's leverage moment sums into `io` (units x 5); phase 2 reads the
+    summed moments from `io` and returns the range's target draws and the
+    plug-in components."""
+    lib = library()
+    G, Cn, P = problem.units, problem.cells, probes
+    arrays = {n: np.zeros(G) for n in ("projection_share", "residual_share", "finite_bias", "finite_variance",
+                                       "residual_mass", "deleted_mass")}
+    arrays["fitted_cell"] = np.zeros(Cn)
+    arrays["cell_correction_weight"] = np.zeros(Cn)
+    arrays["target_draws"] = np.zeros(4 * P)
+    res = OracleResult()
+    for n, a in arrays.items():
+        setattr(res, n, a.ctypes.data_as(dp))
+    io = np.ascontiguousarray(io, dtype=np.float64)
+    opt = OracleOptions(seed, probes, centering, tolerance, rank_tolerance, block_tolerance, dense_limit,
+                        probe_begin, probe_end, phase, 0, io.ctypes.data_as(dp))
+    code = lib.oracle_jla(C.byref(problem), C.byref(opt), C.byref(res))
+    if code != 0:
+        raise RuntimeError(f"oracle failed [{code}]: {res.error.decode()}")
+    draws = arrays["target_draws"].reshape(P, 4)[probe_begin:probe_end].copy()
+    return {"io": io, "draws": draws, "plugin": np.array(res.plugin[:])}
