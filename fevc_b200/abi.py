@@ -103,6 +103,46 @@ class SolveRequestV5(Struct):
                 ("reserved_5", u32)]
 
 
+class SolveRequestInterruptV4(Struct):
+    _fields_ = [("options", SolveRequestV4), ("interrupt_poll", InterruptPoll), ("interrupt_context", C.c_void_p),
+                ("checkpoint_interval", u32), ("reserved", u32)]
+
+
+class SolveRequestV6(Struct):
+    _fields_ = [("v4", SolveRequestV4), ("execution_mode", u32), ("threads", u32), ("reserved_6", u64)]
+
+
+class SolveRequestV7(Struct):
+    _fields_ = [("v6", SolveRequestV6), ("component_batch_mode", u32), ("reserved_7", u32)]
+
+
+class SolveRequestV8(Struct):
+    _fields_ = [("v7", SolveRequestV7), ("resolved_execution_mode", u32), ("tolerance_supplied", u32)]
+
+
+class SolveRequestInterruptV8(Struct):
+    _fields_ = [("options", SolveRequestV8), ("interrupt_poll", InterruptPoll), ("interrupt_context", C.c_void_p),
+                ("checkpoint_interval", u32), ("reserved", u32)]
+
+
+class CapabilityRequestV1(Struct):
+    _fields_ = [(n, u32) for n in ("abi_version", "struct_size", "request_schema", "algorithm", "deletion_mode",
+                                   "nuisance_mode", "solver_route", "rng_contract", "controls_count",
+                                   "frequency_use")] + [("reserved", u64)]
+
+
+class CapabilityRequestV2(Struct):
+    _fields_ = [("v1", CapabilityRequestV1)] + [(n, u32) for n in (
+        "engine", "batch_mode", "stayers_mode", "target_weight_mode", "deletion_unit_source", "probeorder_supplied",
+        "wallseconds_supplied", "reserved_2")] + [("physical_limit", u64)]
+
+
+class CapabilityRequestV3(Struct):
+    _fields_ = [("v2", CapabilityRequestV2), ("leverage_batch_mode", u32), ("target_batch_mode", u32),
+                ("allow_automatic_cmg_setup_fallback", u32), ("reserved_3", u32), ("wallseconds", f64),
+                ("reserved_4", u64)]
+
+
 class SolveRequestInterruptV1(Struct):
     _fields_ = [("options", SolveRequestV1), ("interrupt_poll", InterruptPoll), ("interrupt_context", C.c_void_p),
                 ("checkpoint_interval", u32), ("reserved", u32)]
@@ -165,6 +205,7 @@ class FevcbSolveTimingsV1(Struct):
 
 
 SIZES = {
+    SolveRequestInterruptV4: 312, SolveRequestV8: 320, SolveRequestInterruptV8: 344, CapabilityRequestV3: 120,
     PrepareRequestV1: 24, PrepareRequestV2: 40, PrepareRequestV3: 56, PrepareRequestV4: 64,
     PrepareRequestInterruptV2: 80, PrepareRequestInterruptV3: 88, ColumnsV1: 64, ColumnsV2: 80, ColumnsV3: 96,
     SolveRequestV1: 176, SolveRequestV2: 200, SolveRequestV3: 264, SolveRequestV4: 288, SolveRequestV5: 304,
@@ -255,6 +296,14 @@ SIGNATURES = {
     "vckss_rust_engine_solve_interrupt_v1": (i32, [u64, C.c_void_p]),
     "vckss_rust_engine_solve_v5": (i32, [u64, C.c_void_p]),
     "vckss_rust_engine_solve_interrupt_v5": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_v4": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_interrupt_v4": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_default_solve_request_v8": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_solve_request_interrupt_v8": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_solve_v8": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_interrupt_v8": (i32, [u64, C.c_void_p]),
+    "vckss_rust_backend_request_capability_v3": (i32, [C.c_void_p, C.c_void_p, u32]),
+    "vckss_rust_engine_full_cmg_receipt_v1": (i32, [u64, C.c_void_p, u32]),
     "vckss_rust_engine_result_v1": (i32, [u64, C.c_void_p, u32]),
     "vckss_rust_engine_preparation_receipt_v1": (i32, [u64, C.c_void_p, u32]),
     "vckss_rust_engine_preparation_receipt_v2": (i32, [u64, C.c_void_p, u32]),

@@ -276,7 +276,180 @@ SolveOptions options_from_v1(const VckssEngineSolveRequestV1& q, bool observatio
   return o;
 }
 
-void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr, bool generic_allowed) {
+// ---- request capability (restated from vckss-plugin/src/ffi_engine.rs:9304-9532)
+
+VckssBackendRequestCapabilityRequestV3 capability_request_for_solve(const VckssEngineSolveRequestV4& q,
+                                                                    uint32_t controls_count) {
+  VckssBackendRequestCapabilityRequestV3 c{};
+  c.v2.v1.abi_version = q.v3.v2.v1.abi_version;
+  c.v2.v1.struct_size = sizeof(c);
+  c.v2.v1.request_schema = q.v3.capability_schema;
+  c.v2.v1.algorithm = q.v3.v2.algorithm;
+  c.v2.v1.deletion_mode = q.v3.v2.v1.deletion_mode;
+  c.v2.v1.nuisance_mode = q.v3.v2.nuisance_mode;
+  c.v2.v1.solver_route = q.v3.v2.v1.solver_route;
+  c.v2.v1.rng_contract = q.v3.v2.v1.rng_contract;
+  c.v2.v1.controls_count = controls_count;
+  c.v2.v1.frequency_use = q.v3.frequency_use;
+  c.v2.engine = q.v3.engine;
+  c.v2.batch_mode = q.v3.batch_mode;
+  c.v2.stayers_mode = q.v3.stayers_mode;
+  c.v2.target_weight_mode = q.v3.target_weight_mode;
+  c.v2.deletion_unit_source = q.v3.deletion_unit_source;
+  c.v2.probeorder_supplied = q.v3.probeorder_supplied;
+  c.v2.wallseconds_supplied = q.v3.wallseconds_supplied;
+  c.v2.physical_limit = q.v3.physical_limit;
+  c.leverage_batch_mode = q.leverage_batch_mode;
+  c.target_batch_mode = q.target_batch_mode;
+  c.allow_automatic_cmg_setup_fallback = q.v3.v2.v1.allow_automatic_cmg_setup_fallback;
+  c.wallseconds = q.wallseconds;
+  return c;
+}
+
+// FNV-1a over the schema tag, the capability fields (little-endian u32),
+// the physical limit and the bits of the wall-seconds value.
+uint64_t capability_signature(const VckssBackendRequestCapabilityRequestV3& c) {
+  uint64_t h = 0xcbf29ce484222325ull;
+  auto eat = [&](const void* data, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(data);
+    for (size_t i = 0; i < n; ++i) {
+      h ^= b[i];
+      h *= 0x100000001b3ull;
+    }
+  };
+  static const char tag[] = "VCKSS-REQUEST-CAPABILITY-V3";
+  eat(tag, sizeof(tag) - 1);
+  const uint32_t fields[] = {c.v2.v1.request_schema, c.v2.v1.algorithm, c.v2.v1.deletion_mode, c.v2.v1.nuisance_mode,
+                             c.v2.v1.solver_route, c.v2.v1.rng_contract, c.v2.v1.controls_count,
+                             c.v2.v1.frequency_use, c.v2.engine, c.v2.batch_mode, c.v2.stayers_mode,
+                             c.v2.target_weight_mode, c.v2.deletion_unit_source, c.v2.probeorder_supplied,
+                             c.v2.wallseconds_supplied, c.leverage_batch_mode, c.target_batch_mode,
+                             c.allow_automatic_cmg_setup_fallback};
+  for (uint32_t f : fields) eat(&f, 4);  // little-endian host
+  eat(&c.v2.physical_limit, 8);
+  uint64_t bits;
+  std::memcpy(&bits, &c.wallseconds, 8);
+  eat(&bits, 8);
+  return h;
+}
+
+uint32_t capability_reason(const VckssBackendRequestCapabilityRequestV3& c) {
+  const auto& v = c.v2.v1;
+  const auto& r = c.v2;
+  auto known_batch = [](uint32_t m) { return m == VCKSS_BATCH_MODE_AUTO || m == VCKSS_BATCH_MODE_EXPLICIT; };
+  uint32_t summary = (c.leverage_batch_mode == VCKSS_BATCH_MODE_AUTO && c.target_batch_mode == VCKSS_BATCH_MODE_AUTO)
+                         ? VCKSS_BATCH_MODE_AUTO
+                     : (c.leverage_batch_mode == VCKSS_BATCH_MODE_EXPLICIT &&
+                        c.target_batch_mode == VCKSS_BATCH_MODE_EXPLICIT)
+                         ? VCKSS_BATCH_MODE_EXPLICIT
+                         : VCKSS_BATCH_MODE_INDEPENDENT;
+  bool source_matches = (v.deletion_mode == VCKSS_DELETION_MATCH &&
+                         (r.deletion_unit_source == VCKSS_DELETION_SOURCE_CELL_DEFAULT ||
+                          r.deletion_unit_source == VCKSS_DELETION_SOURCE_MATCH_ID_EXPLICIT)) ||
+                        (v.deletion_mode == VCKSS_DELETION_OBSERVATION &&
+                         r.deletion_unit_source == VCKSS_DELETION_SOURCE_OBSERVATION_ROW);
+  const bool all_stayers = r.stayers_mode == VCKSS_STAYERS_ALL;
+  if (v.request_schema != VCKSS_REQUEST_CAPABILITY_SCHEMA_V3) return VCKSS_REQUEST_REASON_UNKNOWN_SCHEMA;
+  if (v.algorithm > VCKSS_ALGORITHM_JLA) return VCKSS_REQUEST_REASON_UNKNOWN_ALGORITHM;
+  if (v.deletion_mode != VCKSS_DELETION_MATCH && v.deletion_mode != VCKSS_DELETION_OBSERVATION)
+    return VCKSS_REQUEST_REASON_UNKNOWN_DELETION;
+  if (v.nuisance_mode != VCKSS_NUISANCE_JOINT && v.nuisance_mode != VCKSS_NUISANCE_FIXED_OFFSET)
+    return VCKSS_REQUEST_REASON_UNKNOWN_NUISANCE;
+  if (v.solver_route > VCKSS_ROUTE_CMG_PCG) return VCKSS_REQUEST_REASON_UNKNOWN_SOLVER_ROUTE;
+  if (v.rng_contract != VCKSS_RNG_NONE && v.rng_contract != VCKSS_RNG_COUNTER_V1)
+    return VCKSS_REQUEST_REASON_UNKNOWN_RNG_CONTRACT;
+  if (v.frequency_use != VCKSS_REQUEST_FREQUENCY_UNIT && v.frequency_use != VCKSS_REQUEST_FREQUENCY_LITERAL)
+    return VCKSS_REQUEST_REASON_UNKNOWN_FREQUENCY_USE;
+  if (r.engine > VCKSS_ENGINE_GENERIC) return VCKSS_REQUEST_REASON_UNKNOWN_ENGINE;
+  if (!known_batch(c.leverage_batch_mode) || !known_batch(c.target_batch_mode))
+    return VCKSS_REQUEST_REASON_UNKNOWN_BATCH_MODE;
+  if (r.batch_mode > VCKSS_BATCH_MODE_INDEPENDENT || r.batch_mode != summary)
+    return VCKSS_REQUEST_REASON_BATCH_SUMMARY_MISMATCH;
+  if (r.stayers_mode != VCKSS_STAYERS_MOVERS && r.stayers_mode != VCKSS_STAYERS_ALL)
+    return VCKSS_REQUEST_REASON_UNKNOWN_STAYERS_MODE;
+  if (r.target_weight_mode > VCKSS_TARGET_WEIGHT_STORED_ROW_EXPLICIT)
+    return VCKSS_REQUEST_REASON_UNKNOWN_TARGET_WEIGHT_MODE;
+  if (r.deletion_unit_source < VCKSS_DELETION_SOURCE_CELL_DEFAULT ||
+      r.deletion_unit_source > VCKSS_DELETION_SOURCE_OBSERVATION_ROW)
+    return VCKSS_REQUEST_REASON_UNKNOWN_DELETION_UNIT_SOURCE;
+  if (!source_matches) return VCKSS_REQUEST_REASON_DELETION_UNIT_SOURCE_MISMATCH;
+  if (r.probeorder_supplied > 1) return VCKSS_REQUEST_REASON_PROBEORDER_UNSUPPORTED;
+  if (r.wallseconds_supplied > 1 || (r.wallseconds_supplied == 0 && c.wallseconds != 0.0) ||
+      (r.wallseconds_supplied == 1 && (!std::isfinite(c.wallseconds) || c.wallseconds <= 0.0)))
+    return VCKSS_REQUEST_REASON_WALLSECONDS_VALUE;
+  if (c.allow_automatic_cmg_setup_fallback > 1 ||
+      (c.allow_automatic_cmg_setup_fallback == 1 && v.solver_route != VCKSS_ROUTE_AUTO))
+    return VCKSS_REQUEST_REASON_FALLBACK_ROUTE_MISMATCH;
+  if (r.physical_limit == 0 || r.physical_limit > MAX_EXACT_BINARY64_INTEGER)
+    return VCKSS_REQUEST_REASON_PHYSICAL_LIMIT;
+  if (v.controls_count > 32) return VCKSS_REQUEST_REASON_CONTROLS_LIMIT;
+  if (v.algorithm == VCKSS_ALGORITHM_EXACT) {
+    if (r.engine == VCKSS_ENGINE_COMPRESSED) return VCKSS_REQUEST_REASON_EXACT_ENGINE;
+    if (all_stayers && v.deletion_mode != VCKSS_DELETION_MATCH) return VCKSS_REQUEST_REASON_STAYERS_MODE_UNSUPPORTED;
+    if (all_stayers && r.probeorder_supplied != 0) return VCKSS_REQUEST_REASON_PROBEORDER_UNSUPPORTED;
+    if (all_stayers && r.wallseconds_supplied != 0) return VCKSS_REQUEST_REASON_WALLSECONDS_UNSUPPORTED;
+    if (v.rng_contract != VCKSS_RNG_NONE) return VCKSS_REQUEST_REASON_EXACT_RNG;
+    if (v.solver_route != VCKSS_ROUTE_AUTO && v.solver_route != VCKSS_ROUTE_EXACT)
+      return VCKSS_REQUEST_REASON_EXACT_SOLVER_ROUTE;
+    return VCKSS_REQUEST_REASON_SUPPORTED;
+  }
+  if (all_stayers && v.deletion_mode != VCKSS_DELETION_MATCH) return VCKSS_REQUEST_REASON_STAYERS_MODE_UNSUPPORTED;
+  if (all_stayers && r.engine == VCKSS_ENGINE_COMPRESSED)
+    return VCKSS_REQUEST_REASON_COMPRESSED_SCIENTIFIC_INELIGIBILITY;
+  if (all_stayers && r.probeorder_supplied != 0) return VCKSS_REQUEST_REASON_PROBEORDER_UNSUPPORTED;
+  if (all_stayers && r.wallseconds_supplied != 0) return VCKSS_REQUEST_REASON_WALLSECONDS_UNSUPPORTED;
+  if (v.algorithm == VCKSS_ALGORITHM_AUTO) {
+    if (v.rng_contract != VCKSS_RNG_COUNTER_V1) return VCKSS_REQUEST_REASON_AUTO_RNG;
+    if (v.solver_route != VCKSS_ROUTE_AUTO) return VCKSS_REQUEST_REASON_EXACT_SOLVER_ROUTE;
+    if (r.engine == VCKSS_ENGINE_COMPRESSED) return VCKSS_REQUEST_REASON_AUTO_ENGINE_COMPRESSED;
+    return VCKSS_REQUEST_REASON_SUPPORTED;
+  }
+  if (v.rng_contract != VCKSS_RNG_COUNTER_V1) return VCKSS_REQUEST_REASON_JLA_RNG;
+  if (v.solver_route == VCKSS_ROUTE_EXACT) return VCKSS_REQUEST_REASON_JLA_GENERIC_SOLVER_ROUTE;
+  if (r.engine == VCKSS_ENGINE_COMPRESSED &&
+      (v.deletion_mode != VCKSS_DELETION_MATCH || v.controls_count != 0))
+    return VCKSS_REQUEST_REASON_COMPRESSED_SCIENTIFIC_INELIGIBILITY;
+  return VCKSS_REQUEST_REASON_SUPPORTED;
+}
+
+// The V4+ solve gate (reference ffi_engine.rs:4808-4839): the request's
+// probe-order declaration must match the prepared input, and its profile and
+// signature must be those the capability receipt reports for it.
+void reconcile_capability(const Prepared& p, const VckssEngineSolveRequestV4& q) {
+  if (q.v3.probeorder_supplied != (p.problem.probe_order.empty() ? 0u : 1u))
+    fail(INVALID_INPUT, "engine_solve", "solve probe-order declaration differs from prepared input");
+  auto c = capability_request_for_solve(q, uint32_t(p.problem.controls.size()));
+  uint32_t reason = capability_reason(c);
+  uint32_t profile = reason == VCKSS_REQUEST_REASON_SUPPORTED ? VCKSS_REQUEST_PROFILE_PLANNED_V1
+                                                               : VCKSS_REQUEST_PROFILE_NONE;
+  if (reason != VCKSS_REQUEST_REASON_SUPPORTED || profile != q.v3.capability_profile ||
+      capability_signature(c) != q.v3.request_signature)
+    fail(UNSUPPORTED_FEATURE, "engine_solve", "V4 solve does not reconcile with its V3 capability receipt");
+}
+
+SolveOptions options_from_v4(const VckssEngineSolveRequestV4& q) {
+  // preamble of the reference's V4 solve (ffi_engine.rs:4727-4766)
+  if (q.v3.v2.v1.struct_size < sizeof(VckssEngineSolveRequestV4))
+    fail(ABI_MISMATCH, "engine_ffi", "V4 solve request reports a short structure size");
+  if (q.v3.reserved_3 != 0 || q.reserved_4 != 0)
+    fail(ABI_MISMATCH, "engine_ffi", "reserved V4 solve request fields must be zero");
+  if (q.v3.capability_schema != VCKSS_REQUEST_CAPABILITY_SCHEMA_V3 ||
+      q.v3.capability_profile != VCKSS_REQUEST_PROFILE_PLANNED_V1)
+    fail(UNSUPPORTED_FEATURE, "engine_solve", "V4 solve requires the planned-command V3 capability profile");
+  if (q.v3.v2.algorithm != VCKSS_ALGORITHM_EXACT && q.v3.v2.v1.probes < 2)
+    fail(INVALID_INPUT, "engine_solve", "JLA-capable V4 requests require at least two probes");
+  VckssEngineSolveRequestV1 v1 = q.v3.v2.v1;
+  if (v1.leverage_batch_width == 0) v1.leverage_batch_width = 8;
+  if (v1.target_batch_width == 0) v1.target_batch_width = 8;
+  if (q.v3.v2.algorithm == VCKSS_ALGORITHM_EXACT)
+    fail(UNSUPPORTED_FEATURE, "engine_solve", "the exact estimator is not provided by the device engine");
+  if (q.v3.v2.nuisance_mode == VCKSS_NUISANCE_FIXED_OFFSET)
+    fail(UNSUPPORTED_FEATURE, "engine_solve", "fixed-offset nuisance is not provided by the device engine");
+  return options_from_v1(v1, true);
+}
+
+void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr, bool generic_allowed,
+                  const VckssEngineSolveRequestV4* v4 = nullptr) {
   Registry& r = reg();
   std::unique_lock<std::mutex> l(r.mu);
   Prepared& p = r.require(g, "context_solve");
@@ -286,6 +459,7 @@ void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr, bool generi
     fail(STALE_CONTEXT, "context_solve", "generation " + std::to_string(g) + " is not in the prepared state");
   if (!p.has_plan)
     fail(UNSUPPORTED_FEATURE, "engine_solve", "the compressed JLA solve requires a prepared no-control match plan");
+  if (v4) reconcile_capability(p, *v4);
   if (o.deletion_mode != p.deletion_mode)
     fail(INVALID_INPUT, "engine_solve", "solve deletion mode differs from the prepared graph mode");
   r.state = State::Solving;
@@ -642,14 +816,7 @@ int32_t vckss_rust_engine_solve_interrupt_v1(uint64_t generation, const VckssEng
 }
 
 static SolveOptions options_from_v5(const VckssEngineSolveRequestV5& q) {
-  VckssEngineSolveRequestV1 v1 = q.v4.v3.v2.v1;
-  if (v1.leverage_batch_width == 0) v1.leverage_batch_width = 8;
-  if (v1.target_batch_width == 0) v1.target_batch_width = 8;
-  if (q.v4.v3.v2.algorithm == VCKSS_ALGORITHM_EXACT)
-    fail(UNSUPPORTED_FEATURE, "engine_solve", "the exact estimator is not provided by the device engine");
-  if (q.v4.v3.v2.nuisance_mode == VCKSS_NUISANCE_FIXED_OFFSET)
-    fail(UNSUPPORTED_FEATURE, "engine_solve", "fixed-offset nuisance is not provided by the device engine");
-  SolveOptions o = options_from_v1(v1, true);
+  SolveOptions o = options_from_v4(q.v4);
   // Without a supplied tolerance the reference full-CMG route solves probes
   // at 1e-6 (vckss-core/src/full_cmg.rs:29,56-69); the device engine keeps the
   // request's fit tolerance for every right-hand side, which is never looser.
@@ -659,7 +826,7 @@ static SolveOptions options_from_v5(const VckssEngineSolveRequestV5& q) {
 int32_t vckss_rust_engine_solve_v5(uint64_t generation, const VckssEngineSolveRequestV5* request) {
   return status([&] {
     auto q = read_struct(request, "V5 engine solve request");
-    solve_common(generation, options_from_v5(q), Interrupt{}, true);
+    solve_common(generation, options_from_v5(q), Interrupt{}, true, &q.v4);
   });
 }
 
@@ -667,7 +834,167 @@ int32_t vckss_rust_engine_solve_interrupt_v5(uint64_t generation, const VckssEng
   return status([&] {
     auto q = read_struct(request, "V5 interrupt engine solve request");
     solve_common(generation, options_from_v5(q.options),
-                 Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "solve"), true);
+                 Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "solve"), true,
+                 &q.options.v4);
+  });
+}
+
+int32_t vckss_rust_engine_solve_v4(uint64_t generation, const VckssEngineSolveRequestV4* request) {
+  return status([&] {
+    auto q = read_struct(request, "V4 engine solve request");
+    require_abi(q.v3.v2.v1.abi_version);
+    solve_common(generation, options_from_v4(q), Interrupt{}, true, &q);
+  });
+}
+
+int32_t vckss_rust_engine_solve_interrupt_v4(uint64_t generation, const VckssEngineSolveRequestInterruptV4* request) {
+  return status([&] {
+    auto q = read_struct(request, "V4 interrupt engine solve request");
+    require_abi(q.options.v3.v2.v1.abi_version);
+    solve_common(generation, options_from_v4(q.options),
+                 Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "solve"), true,
+                 &q.options);
+  });
+}
+
+int32_t vckss_rust_engine_default_solve_request_v8(VckssEngineSolveRequestV8* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEngineSolveRequestV8>(out, cap, "V8 engine default solve request");
+    VckssEngineSolveRequestV8 q{};
+    if (vckss_rust_engine_default_solve_request_v4(&q.v7.v6.v4, sizeof(q.v7.v6.v4)) != OK)
+      fail(PANIC, "defaults", "V4 defaults");
+    auto& v4 = q.v7.v6.v4;
+    v4.v3.v2.v1.struct_size = sizeof(q);
+    v4.v3.v2.v1.solver_route = VCKSS_ROUTE_DIAGONAL_PCG;
+    v4.v3.v2.algorithm = VCKSS_ALGORITHM_JLA;
+    v4.v3.engine = VCKSS_ENGINE_GENERIC;
+    q.v7.v6.execution_mode = 3;
+    q.v7.v6.threads = 1;
+    q.resolved_execution_mode = 3;
+    std::memcpy(out, &q, sizeof(q));
+  });
+}
+
+int32_t vckss_rust_engine_default_solve_request_interrupt_v8(VckssEngineSolveRequestInterruptV8* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEngineSolveRequestInterruptV8>(out, cap, "V8 interrupt default solve request");
+    VckssEngineSolveRequestInterruptV8 q{};
+    if (vckss_rust_engine_default_solve_request_v8(&q.options, sizeof(q.options)) != OK)
+      fail(PANIC, "defaults", "V8 defaults");
+    q.options.v7.v6.v4.v3.v2.v1.struct_size = sizeof(q);
+    std::memcpy(out, &q, sizeof(q));
+  });
+}
+
+int32_t vckss_rust_engine_solve_v8(uint64_t generation, const VckssEngineSolveRequestV8* request) {
+  return status([&] {
+    auto q = read_struct(request, "V8 engine solve request");
+    require_abi(q.v7.v6.v4.v3.v2.v1.abi_version);
+    solve_common(generation, options_from_v4(q.v7.v6.v4), Interrupt{}, true, &q.v7.v6.v4);
+  });
+}
+
+int32_t vckss_rust_engine_solve_interrupt_v8(uint64_t generation, const VckssEngineSolveRequestInterruptV8* request) {
+  return status([&] {
+    auto q = read_struct(request, "V8 interrupt engine solve request");
+    require_abi(q.options.v7.v6.v4.v3.v2.v1.abi_version);
+    solve_common(generation, options_from_v4(q.options.v7.v6.v4),
+                 Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "solve"), true,
+                 &q.options.v7.v6.v4);
+  });
+}
+
+int32_t vckss_rust_backend_request_capability_v3(const VckssBackendRequestCapabilityRequestV3* request,
+                                                 VckssBackendRequestCapabilityReceiptV3* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssBackendRequestCapabilityReceiptV3>(out, cap, "V3 request capability receipt");
+    if (!request) fail(INVALID_INPUT, "engine_ffi", "V3 request capability pointer is null");
+    VckssBackendRequestCapabilityRequestV3 c;
+    std::memcpy(&c, request, sizeof(c));
+    require_abi(c.v2.v1.abi_version);
+    if (c.v2.v1.struct_size < sizeof(c))
+      fail(ABI_MISMATCH, "engine_ffi", "V3 request capability reports a short structure size");
+    if (c.v2.v1.reserved != 0 || c.v2.reserved_2 != 0 || c.reserved_3 != 0 || c.reserved_4 != 0)
+      fail(ABI_MISMATCH, "engine_ffi", "reserved V3 request capability fields must be zero");
+    uint32_t reason = capability_reason(c);
+    VckssBackendRequestCapabilityReceiptV3 r{};
+    auto& r1 = r.v2.v1;
+    r1.struct_size = sizeof(r);
+    r1.abi_version = VCKSS_RUST_ABI_VERSION_V1;
+    r1.request_schema = c.v2.v1.request_schema;
+    r1.supported = reason == VCKSS_REQUEST_REASON_SUPPORTED;
+    r1.reason_code = reason;
+    r1.profile_code = reason == VCKSS_REQUEST_REASON_SUPPORTED ? VCKSS_REQUEST_PROFILE_PLANNED_V1
+                                                               : VCKSS_REQUEST_PROFILE_NONE;
+    r1.algorithm = c.v2.v1.algorithm;
+    r1.deletion_mode = c.v2.v1.deletion_mode;
+    r1.nuisance_mode = c.v2.v1.nuisance_mode;
+    r1.solver_route = c.v2.v1.solver_route;
+    r1.rng_contract = c.v2.v1.rng_contract;
+    r1.controls_count = c.v2.v1.controls_count;
+    r1.frequency_use = c.v2.v1.frequency_use;
+    r1.request_signature = capability_signature(c);
+    r.v2.engine = c.v2.engine;
+    r.v2.batch_mode = c.v2.batch_mode;
+    r.v2.stayers_mode = c.v2.stayers_mode;
+    r.v2.target_weight_mode = c.v2.target_weight_mode;
+    r.v2.deletion_unit_source = c.v2.deletion_unit_source;
+    r.v2.probeorder_supplied = c.v2.probeorder_supplied;
+    r.v2.wallseconds_supplied = c.v2.wallseconds_supplied;
+    r.v2.physical_limit = c.v2.physical_limit;
+    r.leverage_batch_mode = c.leverage_batch_mode;
+    r.target_batch_mode = c.target_batch_mode;
+    r.allow_automatic_cmg_setup_fallback = c.allow_automatic_cmg_setup_fallback;
+    r.wallseconds = c.wallseconds;
+    r.algorithm_resolution_deferred = c.v2.v1.algorithm == VCKSS_ALGORITHM_AUTO;
+    r.engine_resolution_deferred = c.v2.v1.algorithm == VCKSS_ALGORITHM_AUTO ||
+                                   (c.v2.v1.algorithm == VCKSS_ALGORITHM_JLA &&
+                                    c.v2.engine == VCKSS_ENGINE_AUTO_OR_UNSPECIFIED);
+    r.route_resolution_deferred = c.v2.v1.algorithm != VCKSS_ALGORITHM_EXACT &&
+                                  c.v2.v1.solver_route == VCKSS_ROUTE_AUTO;
+    r.leverage_batch_resolution_deferred = c.leverage_batch_mode == VCKSS_BATCH_MODE_AUTO;
+    r.target_batch_resolution_deferred = c.target_batch_mode == VCKSS_BATCH_MODE_AUTO;
+    r.wall_advisory_only = 1;
+    std::memcpy(out, &r, sizeof(r));
+  });
+}
+
+int32_t vckss_rust_engine_full_cmg_receipt_v1(uint64_t generation, VckssFullCmgReceiptV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssFullCmgReceiptV1>(out, cap, "full-CMG receipt");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_full_cmg_receipt");
+    if (reg().state != State::Solved || !reg().result || !p.device)
+      fail(STALE_CONTEXT, "engine_full_cmg_receipt", "generation has no solved result");
+    const SolveResult& s = *reg().result;
+    DeviceStats st = device_stats(*p.device);
+    VckssFullCmgReceiptV1 r{};
+    r.struct_size = sizeof(r);
+    r.schema_version = 1;
+    r.generation = generation;
+    static const char id[] = "fevc-b200 device engine";
+    std::memcpy(r.cmg_source_commit, id, sizeof(id) - 1);
+    r.threads_requested = 1;
+    r.threads_used = 1;
+    r.maximum_concurrency = 1;
+    r.vertices = st.vertices;
+    r.edges = st.edges;
+    r.hierarchy_levels = st.levels;
+    r.terminal_vertices = st.terminal_vertices;
+    r.fit_effective_tolerance = p.last_options.pcg_tolerance;
+    r.probe_effective_tolerance = p.last_options.pcg_tolerance;
+    r.fit_initial_inner_tolerance = p.last_options.pcg_tolerance;
+    r.probe_initial_inner_tolerance = p.last_options.pcg_tolerance;
+    r.rhs_count = s.timings.rhs_columns;
+    r.batch_calls = s.timings.pcg_iterations ? s.receipts.size() : 0;
+    r.total_iterations = s.timings.column_iterations;
+    r.total_operator_applications = s.timings.column_iterations;
+    r.total_preconditioner_applications = s.timings.column_iterations + s.timings.rhs_columns;
+    r.maximum_reduced_residual = s.max_reduced_residual;
+    r.maximum_complete_residual = s.max_complete_residual;
+    r.solve_ns = uint64_t(s.timings.total_ms * 1e6);
+    r.maximum_batch_rhs = uint64_t(p.last_options.block_columns ? p.last_options.block_columns : 64);
+    std::memcpy(out, &r, sizeof(r));
   });
 }
 

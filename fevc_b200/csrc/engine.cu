@@ -471,12 +471,14 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     upload(e->L_dinv, dinv, s, h2d);
     build_segments(Lptr, e->lap_seg, s, h2d);
     e->stats.vertices = e->n;
+    e->stats.terminal_vertices = e->n;
     e->stats.edges = Lcol.size() / 2;
     e->stats.kept_workers = e->kept;
     e->preconditioner = preconditioner == 0 ? 1 : preconditioner;
     if (e->preconditioner == 2) {
       e->mg = build_multigrid(e->n, Lptr, Lcol, Lval, Ld, s, h2d);
       e->stats.levels = e->mg->levels();
+      e->stats.terminal_vertices = e->mg->report().vertices.back();
     } else if (e->preconditioner == 3) {
       std::vector<float> params = learned_params();
       if (params.empty())

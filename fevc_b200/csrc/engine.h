@@ -88,7 +88,7 @@ struct DeviceEngine;  // opaque
 
 struct DeviceStats {
   uint64_t h2d_bytes = 0;
-  uint64_t vertices = 0, edges = 0, kept_workers = 0, levels = 0;
+  uint64_t vertices = 0, edges = 0, kept_workers = 0, levels = 0, terminal_vertices = 0;
   double setup_ms = 0;
 };
 

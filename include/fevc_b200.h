@@ -36,11 +36,61 @@ extern "C" {
 #define VCKSS_ROUTE_EXACT 1u
 #define VCKSS_ROUTE_DIAGONAL_PCG 2u
 #define VCKSS_ROUTE_CMG_PCG 3u
+#define VCKSS_REQUEST_CAPABILITY_SCHEMA_V3 3u
+#define VCKSS_REQUEST_FREQUENCY_UNIT 0u
+#define VCKSS_REQUEST_FREQUENCY_LITERAL 1u
+#define VCKSS_REQUEST_PROFILE_NONE 0u
+#define VCKSS_REQUEST_PROFILE_PLANNED_V1 4u
 #define VCKSS_ALGORITHM_AUTO 0u
 #define VCKSS_ALGORITHM_EXACT 1u
 #define VCKSS_ALGORITHM_JLA 2u
 #define VCKSS_NUISANCE_JOINT 1u
 #define VCKSS_NUISANCE_FIXED_OFFSET 2u
+#define VCKSS_RNG_NONE 0u
+#define VCKSS_ENGINE_AUTO_OR_UNSPECIFIED 0u
+#define VCKSS_ENGINE_COMPRESSED 1u
+#define VCKSS_ENGINE_GENERIC 2u
+#define VCKSS_BATCH_MODE_AUTO 0u
+#define VCKSS_BATCH_MODE_EXPLICIT 1u
+#define VCKSS_BATCH_MODE_INDEPENDENT 2u
+#define VCKSS_STAYERS_MOVERS 1u
+#define VCKSS_STAYERS_ALL 2u
+#define VCKSS_TARGET_WEIGHT_FREQUENCY_DEFAULT 0u
+#define VCKSS_TARGET_WEIGHT_STORED_ROW_EXPLICIT 1u
+#define VCKSS_DELETION_SOURCE_CELL_DEFAULT 1u
+#define VCKSS_DELETION_SOURCE_MATCH_ID_EXPLICIT 2u
+#define VCKSS_DELETION_SOURCE_OBSERVATION_ROW 3u
+/* request capability reason codes (reference vckss_rust.h:89-124) */
+#define VCKSS_REQUEST_REASON_SUPPORTED 0u
+#define VCKSS_REQUEST_REASON_UNKNOWN_SCHEMA 1u
+#define VCKSS_REQUEST_REASON_UNKNOWN_ALGORITHM 2u
+#define VCKSS_REQUEST_REASON_UNKNOWN_DELETION 4u
+#define VCKSS_REQUEST_REASON_UNKNOWN_NUISANCE 5u
+#define VCKSS_REQUEST_REASON_UNKNOWN_SOLVER_ROUTE 6u
+#define VCKSS_REQUEST_REASON_UNKNOWN_RNG_CONTRACT 7u
+#define VCKSS_REQUEST_REASON_UNKNOWN_FREQUENCY_USE 8u
+#define VCKSS_REQUEST_REASON_CONTROLS_LIMIT 9u
+#define VCKSS_REQUEST_REASON_EXACT_RNG 10u
+#define VCKSS_REQUEST_REASON_EXACT_SOLVER_ROUTE 11u
+#define VCKSS_REQUEST_REASON_JLA_RNG 15u
+#define VCKSS_REQUEST_REASON_UNKNOWN_ENGINE 16u
+#define VCKSS_REQUEST_REASON_EXACT_ENGINE 17u
+#define VCKSS_REQUEST_REASON_JLA_GENERIC_SOLVER_ROUTE 19u
+#define VCKSS_REQUEST_REASON_UNKNOWN_BATCH_MODE 20u
+#define VCKSS_REQUEST_REASON_UNKNOWN_STAYERS_MODE 21u
+#define VCKSS_REQUEST_REASON_UNKNOWN_TARGET_WEIGHT_MODE 22u
+#define VCKSS_REQUEST_REASON_UNKNOWN_DELETION_UNIT_SOURCE 23u
+#define VCKSS_REQUEST_REASON_PROBEORDER_UNSUPPORTED 24u
+#define VCKSS_REQUEST_REASON_WALLSECONDS_UNSUPPORTED 25u
+#define VCKSS_REQUEST_REASON_PHYSICAL_LIMIT 26u
+#define VCKSS_REQUEST_REASON_DELETION_UNIT_SOURCE_MISMATCH 27u
+#define VCKSS_REQUEST_REASON_STAYERS_MODE_UNSUPPORTED 29u
+#define VCKSS_REQUEST_REASON_BATCH_SUMMARY_MISMATCH 30u
+#define VCKSS_REQUEST_REASON_WALLSECONDS_VALUE 31u
+#define VCKSS_REQUEST_REASON_FALLBACK_ROUTE_MISMATCH 32u
+#define VCKSS_REQUEST_REASON_AUTO_RNG 33u
+#define VCKSS_REQUEST_REASON_AUTO_ENGINE_COMPRESSED 34u
+#define VCKSS_REQUEST_REASON_COMPRESSED_SCIENTIFIC_INELIGIBILITY 35u
 #define VCKSS_INTERRUPT_CONTINUE 0
 #define VCKSS_INTERRUPT_USER_BREAK 1
 
@@ -218,6 +268,183 @@ typedef struct VckssEngineSolveRequestInterruptV5 {
   uint32_t reserved;
 } VckssEngineSolveRequestInterruptV5;
 
+typedef struct VckssEngineSolveRequestInterruptV4 {
+  VckssEngineSolveRequestV4 options;
+  VckssInterruptPollV1 interrupt_poll;
+  void *interrupt_context;
+  uint32_t checkpoint_interval;
+  uint32_t reserved;
+} VckssEngineSolveRequestInterruptV4;
+
+/* V6-V8 extend V4 (reference vckss_rust.h:577-660). */
+typedef struct VckssEngineSolveRequestV6 {
+  VckssEngineSolveRequestV4 v4;
+  uint32_t execution_mode;
+  uint32_t threads;
+  uint64_t reserved_6;
+} VckssEngineSolveRequestV6;
+
+typedef struct VckssEngineSolveRequestV7 {
+  VckssEngineSolveRequestV6 v6;
+  uint32_t component_batch_mode;
+  uint32_t reserved_7;
+} VckssEngineSolveRequestV7;
+
+typedef struct VckssEngineSolveRequestV8 {
+  VckssEngineSolveRequestV7 v7;
+  uint32_t resolved_execution_mode;
+  uint32_t tolerance_supplied;
+} VckssEngineSolveRequestV8;
+
+typedef struct VckssEngineSolveRequestInterruptV8 {
+  VckssEngineSolveRequestV8 options;
+  VckssInterruptPollV1 interrupt_poll;
+  void *interrupt_context;
+  uint32_t checkpoint_interval;
+  uint32_t reserved;
+} VckssEngineSolveRequestInterruptV8;
+
+/* ---- request capability (reference vckss_rust.h:177-259) ---- */
+typedef struct VckssBackendRequestCapabilityRequestV1 {
+  uint32_t abi_version;
+  uint32_t struct_size;
+  uint32_t request_schema;
+  uint32_t algorithm;
+  uint32_t deletion_mode;
+  uint32_t nuisance_mode;
+  uint32_t solver_route;
+  uint32_t rng_contract;
+  uint32_t controls_count;
+  uint32_t frequency_use;
+  uint64_t reserved;
+} VckssBackendRequestCapabilityRequestV1;
+
+typedef struct VckssBackendRequestCapabilityReceiptV1 {
+  uint32_t struct_size;
+  uint32_t abi_version;
+  uint32_t request_schema;
+  uint32_t supported;
+  uint32_t reason_code;
+  uint32_t profile_code;
+  uint32_t algorithm;
+  uint32_t deletion_mode;
+  uint32_t nuisance_mode;
+  uint32_t solver_route;
+  uint32_t rng_contract;
+  uint32_t controls_count;
+  uint32_t frequency_use;
+  uint32_t reserved;
+  uint64_t request_signature;
+} VckssBackendRequestCapabilityReceiptV1;
+
+typedef struct VckssBackendRequestCapabilityRequestV2 {
+  VckssBackendRequestCapabilityRequestV1 v1;
+  uint32_t engine;
+  uint32_t batch_mode;
+  uint32_t stayers_mode;
+  uint32_t target_weight_mode;
+  uint32_t deletion_unit_source;
+  uint32_t probeorder_supplied;
+  uint32_t wallseconds_supplied;
+  uint32_t reserved_2;
+  uint64_t physical_limit;
+} VckssBackendRequestCapabilityRequestV2;
+
+typedef struct VckssBackendRequestCapabilityReceiptV2 {
+  VckssBackendRequestCapabilityReceiptV1 v1;
+  uint32_t engine;
+  uint32_t batch_mode;
+  uint32_t stayers_mode;
+  uint32_t target_weight_mode;
+  uint32_t deletion_unit_source;
+  uint32_t probeorder_supplied;
+  uint32_t wallseconds_supplied;
+  uint32_t reserved_2;
+  uint64_t physical_limit;
+} VckssBackendRequestCapabilityReceiptV2;
+
+typedef struct VckssBackendRequestCapabilityRequestV3 {
+  VckssBackendRequestCapabilityRequestV2 v2;
+  uint32_t leverage_batch_mode;
+  uint32_t target_batch_mode;
+  uint32_t allow_automatic_cmg_setup_fallback;
+  uint32_t reserved_3;
+  double wallseconds;
+  uint64_t reserved_4;
+} VckssBackendRequestCapabilityRequestV3;
+
+typedef struct VckssBackendRequestCapabilityReceiptV3 {
+  VckssBackendRequestCapabilityReceiptV2 v2;
+  uint32_t leverage_batch_mode;
+  uint32_t target_batch_mode;
+  uint32_t allow_automatic_cmg_setup_fallback;
+  uint32_t reserved_3;
+  double wallseconds;
+  uint32_t algorithm_resolution_deferred;
+  uint32_t engine_resolution_deferred;
+  uint32_t route_resolution_deferred;
+  uint32_t leverage_batch_resolution_deferred;
+  uint32_t target_batch_resolution_deferred;
+  uint32_t wall_advisory_only;
+  uint64_t reserved_4;
+} VckssBackendRequestCapabilityReceiptV3;
+
+/* ---- full-CMG receipt (reference vckss_rust.h:1458-1509): this library
+ * fills it from the device solve (hybrid graph, hierarchy when the CMG route
+ * ran, right-hand-side and iteration totals, residual maxima). ---- */
+typedef struct VckssFullCmgReceiptV1 {
+  uint32_t struct_size;
+  uint32_t schema_version;
+  uint64_t generation;
+  uint32_t backend_identity;
+  uint32_t platform_os;
+  uint32_t platform_arch;
+  uint32_t batch_strategy_mask;
+  uint8_t cmg_source_commit[40];
+  uint32_t threads_requested;
+  uint32_t threads_used;
+  uint64_t maximum_concurrency;
+  uint64_t vertices;
+  uint64_t edges;
+  uint64_t hierarchy_levels;
+  uint64_t terminal_vertices;
+  uint64_t graph_copy_bytes;
+  uint64_t hierarchy_bytes;
+  uint64_t plan_bytes;
+  uint64_t workspace_bytes_each;
+  uint64_t workspace_pool_bytes;
+  uint64_t admitted_peak_bytes;
+  double fit_effective_tolerance;
+  double probe_effective_tolerance;
+  double fit_initial_inner_tolerance;
+  double probe_initial_inner_tolerance;
+  uint64_t refinement_attempts;
+  uint64_t refined_columns;
+  uint64_t batch_calls;
+  uint64_t rhs_count;
+  uint64_t serial_batches;
+  uint64_t planned_batches;
+  uint64_t across_rhs_batches;
+  uint64_t total_iterations;
+  uint64_t total_operator_applications;
+  uint64_t total_preconditioner_applications;
+  double maximum_reduced_residual;
+  double maximum_complete_residual;
+  uint64_t graph_ns;
+  uint64_t hierarchy_plan_ns;
+  uint64_t rhs_ns;
+  uint64_t solve_ns;
+  uint64_t extraction_ns;
+  uint64_t preparation_peak_bytes;
+  uint64_t prepared_persistent_bytes;
+  uint64_t non_cmg_command_peak_bytes;
+  uint64_t pre_rng_forecast_bytes;
+  uint64_t actual_retained_bytes;
+  uint64_t allocator_allowance_bytes;
+  uint64_t maximum_batch_rhs;
+  uint64_t workspace_count;
+} VckssFullCmgReceiptV1;
+
 /* ---- results and receipts (reference vckss_rust.h:711-768, 1037-1052, 1611-1634) ---- */
 typedef struct VckssComponentVectorV1 {
   double worker;
@@ -386,6 +613,24 @@ int32_t vckss_rust_engine_solve_v1(uint64_t generation, const VckssEngineSolveRe
 int32_t vckss_rust_engine_solve_interrupt_v1(uint64_t generation, const VckssEngineSolveRequestInterruptV1 *request);
 int32_t vckss_rust_engine_solve_v5(uint64_t generation, const VckssEngineSolveRequestV5 *request);
 int32_t vckss_rust_engine_solve_interrupt_v5(uint64_t generation, const VckssEngineSolveRequestInterruptV5 *request);
+/* V4 and V8 solves (reference vckss_rust.h:1603-1609, 1945-1950): V4 and
+ * later requests must carry the request signature and profile that
+ * vckss_rust_backend_request_capability_v3 reports for them. */
+int32_t vckss_rust_engine_solve_v4(uint64_t generation, const VckssEngineSolveRequestV4 *request);
+int32_t vckss_rust_engine_solve_interrupt_v4(uint64_t generation, const VckssEngineSolveRequestInterruptV4 *request);
+int32_t vckss_rust_engine_default_solve_request_v8(VckssEngineSolveRequestV8 *output, uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_default_solve_request_interrupt_v8(VckssEngineSolveRequestInterruptV8 *output,
+                                                            uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_solve_v8(uint64_t generation, const VckssEngineSolveRequestV8 *request);
+int32_t vckss_rust_engine_solve_interrupt_v8(uint64_t generation, const VckssEngineSolveRequestInterruptV8 *request);
+/* Classify a request and compute its signature (reference vckss_rust.h:1661-1665;
+ * vckss-plugin/src/ffi_engine.rs:2629-2719, 9304-9532). */
+int32_t vckss_rust_backend_request_capability_v3(const VckssBackendRequestCapabilityRequestV3 *request,
+                                                 VckssBackendRequestCapabilityReceiptV3 *output,
+                                                 uint32_t output_capacity_bytes);
+/* Reference vckss_rust.h:2121-2125. */
+int32_t vckss_rust_engine_full_cmg_receipt_v1(uint64_t generation, VckssFullCmgReceiptV1 *output,
+                                              uint32_t output_capacity_bytes);
 
 /* ---- results and receipts (reference ffi_engine.rs:5992-6040 result_v1; 4370-4470 receipts, retained mask) ---- */
 int32_t vckss_rust_engine_result_v1(uint64_t generation, VckssEngineResultV1 *output, uint32_t output_capacity_bytes);
@@ -601,6 +846,12 @@ int32_t fevcb_counter_atoms_noalloc_v1(uint64_t seed, uint64_t domain_tag, uint6
 #if defined(__cplusplus)
 static_assert(sizeof(VckssEnginePrepareRequestV1) == 24, "prepare request V1 layout");
 static_assert(sizeof(FevcbCmgSummaryV1) == 688, "CMG summary layout");
+static_assert(sizeof(VckssEngineSolveRequestInterruptV4) == 312, "interrupt V4 solve layout");
+static_assert(sizeof(VckssEngineSolveRequestV8) == 320, "V8 solve layout");
+static_assert(sizeof(VckssEngineSolveRequestInterruptV8) == 344, "interrupt V8 solve layout");
+static_assert(sizeof(VckssBackendRequestCapabilityRequestV3) == 120, "V3 capability request layout");
+static_assert(sizeof(VckssBackendRequestCapabilityReceiptV3) == 160, "V3 capability receipt layout");
+static_assert(sizeof(VckssFullCmgReceiptV1) == 400, "full-CMG receipt layout");
 static_assert(sizeof(FevcbSolveOptionsV2) == 24, "device options V2 layout");
 static_assert(sizeof(FevcbLearnedDumpV1) == 80, "learned dump layout");
 static_assert(sizeof(VckssEnginePrepareRequestV2) == 40, "prepare request V2 layout");

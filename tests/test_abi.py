@@ -50,6 +50,7 @@ class SolveRequestInterruptV5(abi.Struct):
     ("solve_request_v1", abi.SolveRequestV1), ("solve_request_v2", abi.SolveRequestV2),
     ("solve_request_v3", abi.SolveRequestV3), ("solve_request_v4", abi.SolveRequestV4),
     ("solve_request_v5", abi.SolveRequestV5), ("solve_request_interrupt_v1", abi.SolveRequestInterruptV1),
+    ("solve_request_v8", abi.SolveRequestV8), ("solve_request_interrupt_v8", abi.SolveRequestInterruptV8),
     ("solve_request_interrupt_v5", SolveRequestInterruptV5), ("prepare_request_v3", abi.PrepareRequestV3),
     ("prepare_request_interrupt_v1", PrepareRequestInterruptV1),
     ("prepare_request_interrupt_v2", abi.PrepareRequestInterruptV2),
@@ -160,3 +161,91 @@ def test_short_struct_size_is_an_abi_mismatch(lib):
         e.solve(req)
     assert err.value.code == 10 and "below required size 176" in err.value.message
     e.release()
+
+
+def capability_requests():
+    """A grid of V3 capability requests: the default solve request's fields
+    and single-field variations across valid and invalid values."""
+    base = dict(abi_version=1, request_schema=3, algorithm=2, deletion_mode=1, nuisance_mode=1, solver_route=0,
+                rng_contract=1, controls_count=0, frequency_use=0, engine=0, batch_mode=0, stayers_mode=1,
+                target_weight_mode=0, deletion_unit_source=1, probeorder_supplied=0, wallseconds_supplied=0,
+                physical_limit=1 << 40, leverage_batch_mode=0, target_batch_mode=0,
+                allow_automatic_cmg_setup_fallback=0, wallseconds=0.0)
+    variations = dict(request_schema=[1, 2, 4], algorithm=[0, 1, 3], deletion_mode=[0, 2, 3], nuisance_mode=[0, 2, 3],
+                      solver_route=[1, 2, 3, 4], rng_contract=[0, 2], controls_count=[4, 32, 33],
+                      frequency_use=[1, 2], engine=[1, 2, 3], batch_mode=[1, 2, 3], stayers_mode=[0, 2, 3],
+                      target_weight_mode=[1, 2], deletion_unit_source=[0, 2, 3, 4], probeorder_supplied=[1, 2],
+                      wallseconds_supplied=[1, 2], physical_limit=[0, (1 << 53) + 1],
+                      leverage_batch_mode=[1, 2], target_batch_mode=[1], allow_automatic_cmg_setup_fallback=[1, 2],
+                      wallseconds=[5.0, -1.0])
+    yield base
+    for k, vals in variations.items():
+        for v in vals:
+            yield {**base, k: v}
+    # combinations that reach the algorithm-specific branches
+    for alg in (0, 1, 2):
+        for route in (0, 1, 2, 3):
+            for engine in (0, 1, 2):
+                for deletion, source in ((1, 1), (2, 3)):
+                    for rng in (0, 1):
+                        for stayers in (1, 2):
+                            yield {**base, "algorithm": alg, "solver_route": route, "engine": engine,
+                                   "deletion_mode": deletion, "deletion_unit_source": source, "rng_contract": rng,
+                                   "stayers_mode": stayers, "controls_count": 4 if engine == 1 else 0}
+
+
+def make_capability_request(d):
+    r = abi.CapabilityRequestV3()
+    v1, v2 = r.v2.v1, r.v2
+    v1.struct_size = C.sizeof(r)
+    for k in ("abi_version", "request_schema", "algorithm", "deletion_mode", "nuisance_mode", "solver_route",
+              "rng_contract", "controls_count", "frequency_use"):
+        setattr(v1, k, d[k])
+    for k in ("engine", "batch_mode", "stayers_mode", "target_weight_mode", "deletion_unit_source",
+              "probeorder_supplied", "wallseconds_supplied", "physical_limit"):
+        setattr(v2, k, d[k])
+    for k in ("leverage_batch_mode", "target_batch_mode", "allow_automatic_cmg_setup_fallback", "wallseconds"):
+        setattr(r, k, d[k])
+    return r
+
+
+@pytest.mark.skipif(not PLUGIN.exists(), reason="reference plugin not staged")
+def test_request_capability_receipts_match_reference(lib):
+    """Reason, profile, signature and every receipt byte equal the plugin's."""
+    ref = abi.load(PLUGIN, bind_extensions=False)
+    ref.vckss_rust_backend_request_capability_v3.restype = C.c_int32
+    n = 0
+    for d in capability_requests():
+        req = make_capability_request(d)
+        a, b = (C.c_uint8 * 160)(), (C.c_uint8 * 160)()
+        sa = lib.vckss_rust_backend_request_capability_v3(C.byref(req), a, 160)
+        sb = ref.vckss_rust_backend_request_capability_v3(C.byref(req), b, 160)
+        assert sa == sb, d
+        assert bytes(a) == bytes(b), d
+        n += 1
+    assert n > 100
+
+
+@pytest.mark.skipif(not PLUGIN.exists(), reason="reference plugin not staged")
+def test_v4_solve_refuses_an_unreconciled_request(lib):
+    """A V4 solve whose signature does not match its capability receipt is
+    refused (11) before any work, by both libraries; so is a profile of zero."""
+    from make_golden import kat12
+
+    for L in (lib, abi.load(PLUGIN, bind_extensions=False)):
+        for mutate in ("signature", "profile"):
+            e = abi.Engine(L)
+            e.prepare(kat12())
+            q = abi.SolveRequestV4()
+            assert L.vckss_rust_engine_default_solve_request_v4(C.byref(q), C.sizeof(q)) == 0
+            q.v3.v2.v1.probes = 4
+            q.v3.v2.algorithm = 2
+            q.v3.request_signature = abi.capability_signature_v3(q, 0)
+            if mutate == "signature":
+                q.v3.request_signature ^= 1
+            else:
+                q.v3.capability_profile = 0
+            st = L.vckss_rust_engine_solve_v4(e.generation, C.byref(q))
+            msg = L.vckss_rust_engine_last_error().decode()
+            e.release()
+            assert st == 11 and ("reconcile" in msg or "capability profile" in msg), (L, mutate, st, msg)
