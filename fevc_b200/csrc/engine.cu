@@ -242,6 +242,8 @@ struct DeviceEngine {
   DBuf<uint32_t> row_cell, cell_rows_ptr, cell_rows, unit_group_d, group_rows;
   DBuf<uint64_t> group_ptr;
   DBuf<double> row_freq, row_y, Qd, Rd, alphaH, psiH, residual, deleted, beta_buf;
+  DBuf<double> cellQ;       // per cell, sum of f Q over its rows (C x QMAX)
+  DBuf<double> unit_sums;   // per match unit, the target-contraction sums (units x 2 (1 + q))
   bool controls_ready = false;
   std::vector<double> Sinv, Lfac;  // q x q, row-major
   Components shard_plugin;  // the fit's plug-in components, kept between shard phases
@@ -1236,8 +1238,8 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
       // row-level contraction over match groups
       std::vector<double> t(QMAX * K, 0.0), beta(QMAX * K, 0.0);
       if (e.q > 0) {
-        k_target_control<K><<<L.grid, THREADS, 0, L.s>>>(e.rows, e.q, e.row_cell.p, e.cell_worker.p, e.cell_firm.p,
-                                                         e.row_freq.p, e.Qd.p, w.alpha.p, w.x.p, e.partial.p);
+        k_target_control_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.q, e.cell_worker.p, e.cell_firm.p,
+                                                               e.cellQ.p, w.alpha.p, w.x.p, e.partial.p);
         k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, QMAX * K, w.tot.p);
         CK(cudaMemcpyAsync(t.data(), w.tot.p, QMAX * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
         CK(cudaStreamSynchronize(L.s));
@@ -1254,10 +1256,9 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
             e.rows, e.q, nullptr, nullptr, e.row_cell.p, e.cell_worker.p, e.cell_firm.p, e.row_freq.p, e.row_y.p,
             y_center, e.deleted.p, e.Rd.p, e.beta_buf.p, w.alpha.p, w.x.p, e.partial.p);
       else
-        k_generic_contract<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.q, e.group_ptr.p, e.group_rows.p, e.row_cell.p,
-                                                           e.cell_worker.p, e.cell_firm.p, e.row_freq.p, e.row_y.p,
-                                                           y_center, e.deleted.p, e.Rd.p, e.beta_buf.p, w.alpha.p,
-                                                           w.x.p, e.partial.p);
+        k_generic_contract_units<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.q, e.unit_cell.p, e.cell_worker.p,
+                                                                 e.cell_firm.p, e.unit_sums.p, e.beta_buf.p,
+                                                                 w.alpha.p, w.x.p, e.partial.p);
       k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 2 * K, w.tot.p);
       std::vector<double> g2(2 * K);
       CK(cudaMemcpyAsync(g2.data(), w.tot.p, 2 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
@@ -1476,6 +1477,8 @@ void setup_controls(DeviceEngine& e, const SolveOptions& o, SolveTimings& tm) {
   const int q = e.q;
   k_cell_controls<<<L.grid, THREADS, 0, L.s>>>(e.C, q, e.cell_rows_ptr.p, e.cell_rows.p, e.row_freq.p, e.Qd.p,
                                                w8.cell_val.p);
+  e.cellQ.alloc(size_t(e.C) * QMAX);
+  CK(cudaMemcpyAsync(e.cellQ.p, w8.cell_val.p, size_t(e.C) * QMAX * sizeof(double), cudaMemcpyDeviceToDevice, L.s));
   k_gather<8><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, w8.cell_val.p, w8.bW.p);
   firm_gather<8, 0, 0>(e, w8, L, nullptr, w8.cell_val.p, nullptr, 0.0, nullptr, nullptr, nullptr, w8.bF.p, nullptr);
   SolveOptions oc = o;
@@ -1647,6 +1650,11 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
                                                          : "finite-projection moment failed";
       fail(int32_t(code), "generic_jla_leverage", std::string(what) + " at unit " + std::to_string(g));
     }
+    if (!e.unit_sums.p) e.unit_sums.alloc(size_t(e.G) * 2 * (1 + QMAX));
+    k_unit_target_sums<<<L.grid, THREADS, 0, L.s>>>(e.G, q, e.unit_group_d.p, e.group_ptr.p, e.group_rows.p,
+                                                    e.row_freq.p, e.row_y.p, outcome_mean(p, o.centering),
+                                                    e.deleted.p, e.Rd.p, e.unit_sums.p);
+    res.timings.kernel_launches += 1;
   }
   }
   auto t2 = now();

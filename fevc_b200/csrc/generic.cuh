@@ -280,41 +280,6 @@ __global__ void k_generic_adjust(GenericAdjustParams prm, const uint32_t* __rest
   }
 }
 
-// Target control correction, right-hand side: partial[blk][k][K] =
-// sum_r f_r Q[r][k] (alpha_w + psi_f)[column]   (k < QMAX)
-template <int K>
-__global__ void k_target_control(uint32_t rows, int q, const uint32_t* __restrict__ row_cell,
-                                 const uint32_t* __restrict__ cell_worker, const uint32_t* __restrict__ cell_firm,
-                                 const double* __restrict__ row_freq, const double* __restrict__ Q,
-                                 const double* __restrict__ alpha, const double* __restrict__ psi,
-                                 double* __restrict__ partial) {
-  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
-  double v[QMAX][CPT];
-#pragma unroll
-  for (int k = 0; k < QMAX; ++k)
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) v[k][c] = 0.0;
-  int c0 = int(threadIdx.x % TPR) * CPT;
-  size_t total = size_t(rows) * TPR, stride = size_t(gridDim.x) * blockDim.x;
-  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
-    size_t t = base + threadIdx.x;
-    if (t < total) {
-      size_t r = t / TPR;
-      uint32_t c = row_cell[r];
-      size_t wb = size_t(cell_worker[c]) * K + c0, fb = size_t(cell_firm[c]) * K + c0;
-      double f = row_freq[r];
-#pragma unroll
-      for (int cc = 0; cc < CPT; ++cc) {
-        double u = f * (alpha[wb + cc] + psi[fb + cc]);
-#pragma unroll
-        for (int k = 0; k < QMAX; ++k)
-          if (k < q) v[k][cc] += u * Q[r * q + k];
-      }
-    }
-  }
-  block_reduce_cols<K, QMAX>(v, partial);
-}
-
 // Generic target draw (reference `target_draw`, generic_jla/statistical_batches.rs:259-347):
 // per match group, first_t = sum_r f y u_t(r), second_t = sum_r sqrt(f) d_r u_t(r),
 // draw_t += first_t * second_t, with u_t(r) = u_fe,t(cell) + R_r' beta_t for the
@@ -373,6 +338,139 @@ __global__ void k_generic_contract(uint32_t groups, int q, const uint64_t* __res
 #pragma unroll
     for (int c = 0; c < CPT; ++c) v[0][c] += first[c] * second[c];
     // the total's sums are the sums of the two sides' (linear in u)
+    if (CPT == 2) {
+      v[1][0] += (first[0] + first[CPT - 1]) * (second[0] + second[CPT - 1]);
+    } else {
+      double fo = __shfl_xor_sync(0xffffffffu, first[0], 1);
+      double so = __shfl_xor_sync(0xffffffffu, second[0], 1);
+      if ((c0 & 1) == 0) v[1][0] += (first[0] + fo) * (second[0] + so);
+    }
+  }
+  block_reduce_cols<K, 2>(v, partial);
+}
+
+// Cell-level control sums of the target solutions: partial[blk][k][col] =
+// sum over cells of CQ[c][k] u_c(col), CQ[c][k] = sum over the cell's rows of
+// f Q_rk (computed once with the control geometry) and u_c = alpha_w + psi_f;
+// one term per cell (the control correction of the full-model target solves,
+// reference generic_jla.rs:8554-8900).
+template <int K>
+__global__ void k_target_control_cells(uint32_t cells, int q, const uint32_t* __restrict__ cell_worker,
+                                       const uint32_t* __restrict__ cell_firm, const double* __restrict__ CQ,
+                                       const double* __restrict__ alpha, const double* __restrict__ psi,
+                                       double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  double v[QMAX][CPT];
+#pragma unroll
+  for (int k = 0; k < QMAX; ++k)
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) v[k][c] = 0.0;
+  int c0 = int(threadIdx.x % TPR) * CPT;
+  size_t total = size_t(cells) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    if (t < total) {
+      size_t c = t / TPR;
+      size_t wb = size_t(cell_worker[c]) * K + c0, fb = size_t(cell_firm[c]) * K + c0;
+      double cq[QMAX];
+#pragma unroll
+      for (int k = 0; k < QMAX; ++k) cq[k] = k < q ? CQ[c * QMAX + k] : 0.0;
+#pragma unroll
+      for (int cc = 0; cc < CPT; ++cc) {
+        double u = alpha[wb + cc] + psi[fb + cc];
+#pragma unroll
+        for (int k = 0; k < QMAX; ++k) v[k][cc] += u * cq[k];
+      }
+    }
+  }
+  block_reduce_cols<K, QMAX>(v, partial);
+}
+
+// Per match unit (units in cell order), the sums the target contraction
+// needs over the unit's rows, with S = 1 + q entries each:
+//   out[i][0][0] = sum f (y - y_center),       out[i][0][1 + k] = sum f (y - y_center) R_rk
+//   out[i][1][0] = sum sqrt(f) d,              out[i][1][1 + k] = sum sqrt(f) d R_rk
+// (d the deleted residual).  Every row of a unit lies in one cell, so a
+// unit's draw terms are affine in the cell's FE solution and in beta.
+__global__ void k_unit_target_sums(uint32_t units, int q, const uint32_t* __restrict__ unit_group,
+                                   const uint64_t* __restrict__ group_ptr, const uint32_t* __restrict__ group_rows,
+                                   const double* __restrict__ row_freq, const double* __restrict__ y, double y_center,
+                                   const double* __restrict__ deleted, const double* __restrict__ R,
+                                   double* __restrict__ out) {
+  const int S = 1 + q;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < units; i += size_t(gridDim.x) * blockDim.x) {
+    uint32_t g = unit_group[i];
+    double a[RMAX], b[RMAX];
+#pragma unroll
+    for (int k = 0; k < RMAX; ++k) a[k] = b[k] = 0.0;
+    for (uint64_t j = group_ptr[g]; j < group_ptr[g + 1]; ++j) {
+      uint32_t r = group_rows[j];
+      double f = row_freq[r], fy = f * (y[r] - y_center), sd = sqrt(f) * deleted[r];
+      a[0] += fy;
+      b[0] += sd;
+#pragma unroll
+      for (int k = 0; k < QMAX; ++k)
+        if (k < q) {
+          double rk = R[size_t(r) * q + k];
+          a[1 + k] += fy * rk;
+          b[1 + k] += sd * rk;
+        }
+    }
+    double* o = out + i * size_t(2 * S);
+    for (int k = 0; k < S; ++k) {
+      o[k] = a[k];
+      o[S + k] = b[k];
+    }
+  }
+}
+
+// Target draws from the unit sums: first = u_fe A0 + sum_k beta_k A_k,
+// second = u_fe B0 + sum_k beta_k B_k, draw += first * second; the total
+// side sums the worker and firm columns (linear in u).  partial layout as in
+// k_generic_contract.
+template <int K>
+__global__ void k_generic_contract_units(uint32_t units, int q, const uint32_t* __restrict__ unit_cell,
+                                         const uint32_t* __restrict__ cell_worker,
+                                         const uint32_t* __restrict__ cell_firm, const double* __restrict__ sums,
+                                         const double* __restrict__ beta /* [QMAX][K] */,
+                                         const double* __restrict__ alpha, const double* __restrict__ psi,
+                                         double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  static_assert(CPT <= 2, "pairs of columns must sit in one thread or in adjacent lanes");
+  const int S = 1 + q;
+  double v[2][CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
+  const int c0 = int(threadIdx.x % TPR) * CPT;
+  double bcol[QMAX][CPT];
+#pragma unroll
+  for (int k = 0; k < QMAX; ++k)
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) bcol[k][c] = k < q ? beta[k * K + c0 + c] : 0.0;
+  size_t total = size_t(units) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    bool live = t < total;
+    size_t i = live ? t / TPR : 0;
+    uint32_t cell = live ? unit_cell[i] : 0;
+    const double* o = sums + i * size_t(2 * S);
+    double first[CPT], second[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      double ufe = live ? alpha[size_t(cell_worker[cell]) * K + c0 + c] + psi[size_t(cell_firm[cell]) * K + c0 + c]
+                        : 0.0;
+      double f1 = live ? ufe * o[0] : 0.0, s1 = live ? ufe * o[S] : 0.0;
+#pragma unroll
+      for (int k = 0; k < QMAX; ++k)
+        if (live && k < q) {
+          f1 += bcol[k][c] * o[1 + k];
+          s1 += bcol[k][c] * o[S + 1 + k];
+        }
+      first[c] = f1;
+      second[c] = s1;
+    }
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) v[0][c] += first[c] * second[c];
     if (CPT == 2) {
       v[1][0] += (first[0] + first[CPT - 1]) * (second[0] + second[CPT - 1]);
     } else {
