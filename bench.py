@@ -341,6 +341,8 @@ def main():
     # roofline: the persistent blocked PCG kernel, standalone launches with L2 flushed
     block = args.block or 64
     spmm_ms, spmm_bytes = e.kernel_benchmark(1, block, 10)
+    # the same iterations in the three-barrier form, for comparison
+    tb_ms, tb_bytes = e.kernel_benchmark(5, block, 10)
     peaks = {}
     try:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -353,7 +355,7 @@ def main():
 
     # e2e through the C ABI: solve + result on a fresh generation per step
     e2e_times = []
-    for i in range(args.e2e_steps + 1):
+    for i in range(max(args.e2e_steps, 1) + 1):
         g = abi.Engine(lib)
         g.prepare(panel)
         g.device_options(args.block, args.precond)
@@ -411,8 +413,10 @@ def main():
             "first_solve_s": round(first_solve_s, 3),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": None,
-                         "kernel": f"k_pcg_persistent<{block}> (20 iterations per launch)", "bytes_per_launch": spmm_bytes,
-                         "ms_per_launch": round(spmm_ms, 5), "peak_source": "measured (MEASURED_PEAKS.json)"},
+                         "kernel": f"k_pcg_persistent_cg<{block}> (two grid barriers per iteration, "
+                                   "20 iterations per launch)", "bytes_per_launch": spmm_bytes,
+                         "ms_per_launch": round(spmm_ms, 5), "peak_source": "measured (MEASURED_PEAKS.json)",
+                         "three_barrier_ms_per_launch": round(tb_ms, 5)},
             "gpu_launches": int(timings["kernel_launches"]) * args.steps,
             "solver": {k: timings[k] for k in ("block_iterations", "column_iterations", "rhs_columns",
                                                "vertices", "edges", "kept_workers", "levels")},

@@ -274,7 +274,7 @@ struct BlockWork {
   PcgState s;
   // mixed precision: single-precision inner iterate, residual, direction and
   // segment products, and the inner solve's per-column state
-  DBuf<float> x32, r32, p32, seg32;
+  DBuf<float> x32, r32, p32, ap32, seg32;
   DBuf<double> y1, y2;  // polynomial preconditioner: D^{-1} A powers of the residual
   DBuf<double> st_in;
   DBuf<int> ist_in;
@@ -509,6 +509,10 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_persistent<64>, PERSIST_THREADS, 0));
     if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the persistent PCG kernel cannot be resident on an SM");
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_persistent_cg<64>, PERSIST_THREADS, 0));
+    if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the two-barrier persistent PCG kernel cannot be resident on an SM");
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_persistent_cg<64, float>, PERSIST_THREADS, 0));
+    if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the single-precision persistent PCG kernel cannot be resident on an SM");
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_persistent_poly<64>, PERSIST_THREADS, 0));
     if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the persistent polynomial PCG kernel cannot be resident on an SM");
     e->coop_blocks = sms;  // one 1024-thread block per SM
@@ -663,10 +667,10 @@ void pcg_restart(DeviceEngine& e, BlockWork& w, Launch L, bool fresh) {
   CK_LAUNCH();
 }
 
-// Run the persistent PCG kernel until every active column converges or
-// `iterations` iterations have run; returns the iterations executed.
+// Arguments of the persistent Jacobi PCG kernels over the hybrid Laplacian
+// (double values) for block workspace w.
 template <int K>
-int pcg_run(DeviceEngine& e, BlockWork& w, Launch L, int iterations) {
+PersistentPcg<K> persistent_args(DeviceEngine& e, BlockWork& w, int iterations) {
   PersistentPcg<K> a;
   a.n = e.n;
   a.ptr = e.L_ptr.p;
@@ -683,13 +687,23 @@ int pcg_run(DeviceEngine& e, BlockWork& w, Launch L, int iterations) {
   a.x = w.x.p;
   a.r = w.r.p;
   a.p = w.p.p;
+  a.ap = w.q.p;
   a.partial_a = e.partial.p;
   a.partial_b = e.partial.p + size_t(e.coop_blocks) * K;
   a.s = w.s;
   a.max_iters = iterations;
+  return a;
+}
+
+// Run the persistent (two-barrier) PCG kernel until every active column
+// converges or `iterations` iterations have run; returns the iterations
+// executed.
+template <int K>
+int pcg_run(DeviceEngine& e, BlockWork& w, Launch L, int iterations) {
+  PersistentPcg<K> a = persistent_args<K>(e, w, iterations);
   void* args[] = {&a};
-  CK(cudaLaunchCooperativeKernel((const void*)k_pcg_persistent<K>, dim3(e.coop_blocks), dim3(PERSIST_THREADS), args,
-                                 0, L.s));
+  CK(cudaLaunchCooperativeKernel((const void*)k_pcg_persistent_cg<K>, dim3(e.coop_blocks), dim3(PERSIST_THREADS),
+                                 args, 0, L.s));
   CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
   std::vector<int> it(K);
   CK(cudaMemcpyAsync(it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost, L.s));
@@ -808,6 +822,7 @@ void ensure_mixed_work(DeviceEngine& e, BlockWork& w) {
   w.x32.alloc(n);
   w.r32.alloc(n);
   w.p32.alloc(n);
+  w.ap32.alloc(n);
   w.seg32.alloc(size_t(e.lap_seg.count) * K);
   w.st_in.alloc(8 * K);
   w.ist_in.alloc(2 * K + 4);
@@ -852,12 +867,13 @@ int pcg_run_mixed(DeviceEngine& e, BlockWork& w, Launch L, int iterations, Solve
     a.x = w.x32.p;
     a.r = w.r32.p;
     a.p = w.p32.p;
+    a.ap = w.ap32.p;
     a.partial_a = e.partial.p;
     a.partial_b = e.partial.p + size_t(e.coop_blocks) * K;
     a.s = w.s_in;
     a.max_iters = iterations - done;
     void* args[] = {&a};
-    CK(cudaLaunchCooperativeKernel((const void*)k_pcg_persistent<K, float>, dim3(e.coop_blocks),
+    CK(cudaLaunchCooperativeKernel((const void*)k_pcg_persistent_cg<K, float>, dim3(e.coop_blocks),
                                    dim3(PERSIST_THREADS), args, 0, L.s));
     std::vector<int> it(K);
     CK(cudaMemcpyAsync(it.data(), w.s_in.iters, K * sizeof(int), cudaMemcpyDeviceToHost, L.s));
@@ -1760,9 +1776,12 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
   const int iters = 20;
   switch (kernel) {
     case 1:
+    case 5:
       // persistent PCG, per launch of `iters` iterations: matrix + segment
-      // tables once per iteration, p read, segment products written and read,
-      // x and r read and written, p read and written
+      // tables once per iteration, nine passes over n x K vectors (two-barrier
+      // form: r gathered; r, p, A p, x read and written; three-barrier form:
+      // p gathered; p, x, r read, x, r written; r, p read, p written) and the
+      // segment products written and read
       *bytes = iters * (nnz * 12 + nseg * 12 + n * (4 + 4 + 8 + 8 + 8) + n * K * 8.0 * 9 + 2 * nseg * K * 8.0);
       break;
     case 3:
@@ -1779,7 +1798,7 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
   }
   float total = 0.0f;
   for (int i = 0; i < launches; ++i) {
-    if (kernel == 1) {
+    if (kernel == 1 || kernel == 5) {
       // a fresh, never-converging block (tolerance 0) so every launch runs `iters` iterations
       k_fill_pattern<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p);
       k_colsum_abs<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p, e.partial.p);
@@ -1790,30 +1809,12 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
     CK(cudaMemsetAsync(flush.p, i & 0xff, flush.bytes(), L.s));
     CK(cudaEventRecord(e.ev0, L.s));
     switch (kernel) {
-      case 1: {
-        PersistentPcg<K> a;
-        a.n = e.n;
-        a.ptr = e.L_ptr.p;
-        a.col = e.L_col.p;
-        a.val = e.L_val.p;
-        a.diag = e.L_diag.p;
-        a.dinv = e.L_dinv.p;
-        a.nseg = e.lap_seg.count;
-        a.seg_row = e.lap_seg.row.p;
-        a.seg_begin = e.lap_seg.begin.p;
-        a.seg_end = e.lap_seg.end.p;
-        a.row_first = e.lap_seg.row_first.p;
-        a.seg_buf = w.seg_buf.p;
-        a.x = w.x.p;
-        a.r = w.r.p;
-        a.p = w.p.p;
-        a.partial_a = e.partial.p;
-        a.partial_b = e.partial.p + size_t(e.coop_blocks) * K;
-        a.s = w.s;
-        a.max_iters = iters;
+      case 1:
+      case 5: {
+        PersistentPcg<K> a = persistent_args<K>(e, w, iters);
         void* args[] = {&a};
-        CK(cudaLaunchCooperativeKernel((const void*)k_pcg_persistent<K>, dim3(e.coop_blocks), dim3(PERSIST_THREADS),
-                                       args, 0, L.s));
+        const void* fn = kernel == 1 ? (const void*)k_pcg_persistent_cg<K> : (const void*)k_pcg_persistent<K>;
+        CK(cudaLaunchCooperativeKernel(fn, dim3(e.coop_blocks), dim3(PERSIST_THREADS), args, 0, L.s));
         break;
       }
       case 3:
@@ -1840,7 +1841,7 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
   }
   CK_LAUNCH();
   *ms = double(total) / launches;
-  if (kernel == 1) {
+  if (kernel == 1 || kernel == 5) {
     // report the iterations actually executed (a curvature breakdown would stop early)
     std::vector<int> it(K);
     CK(cudaMemcpy(it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost));

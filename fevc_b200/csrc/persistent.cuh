@@ -125,11 +125,91 @@ struct PersistentPcg {
   V* x;
   V* r;
   V* p;
-  double* partial_a;  // [grid][1][K]
+  V* ap;              // A p (the two-barrier kernel only)
+  double* partial_a;  // [grid][1][K]; the two-barrier kernel: [2][grid][3][K]
   double* partial_b;  // [grid][2][K]
   PcgState s;
   int max_iters;
 };
+
+// Columns c0 .. c0+CPT-1 of vertex j of a vertex-interleaved block, as one
+// vector load where the width allows (c0 is a multiple of CPT).  The block is
+// rewritten between grid barriers, so these are plain coherent loads (no
+// read-only path, no __restrict__ on y).
+template <int K, typename V>
+__device__ __forceinline__ void load_cols(const V* y, uint32_t j, int c0, double (&out)[Cols<K>::CPT]) {
+  constexpr int CPT = Cols<K>::CPT;
+  const V* src = y + size_t(j) * K + c0;
+  if constexpr (CPT == 2 && sizeof(V) == 8) {
+    double2 v = *reinterpret_cast<const double2*>(src);
+    out[0] = v.x;
+    out[1] = v.y;
+  } else if constexpr (CPT == 2 && sizeof(V) == 4) {
+    float2 v = *reinterpret_cast<const float2*>(src);
+    out[0] = v.x;
+    out[1] = v.y;
+  } else {
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) out[c] = double(src[c]);
+  }
+}
+
+// acc[c] = sum_{i in [b, e)} val_i * (dinv[col_i] if SCALE) * y[col_i][c0 + c],
+// summed in item order.  When a warp holds one segment (TPR = 32) the warp
+// loads the segment's columns and values once, coalesced, and broadcasts them
+// by shuffle, so the gathers of four to eight items are issued back to back
+// instead of each waiting for its own index load.
+template <int K, typename V, bool SCALE>
+__device__ __forceinline__ void segment_gather(const uint32_t* __restrict__ col, const V* __restrict__ val,
+                                               const V* __restrict__ dinv, const V* y, uint32_t b,
+                                               uint32_t e, int c0, double (&acc)[Cols<K>::CPT]) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
+  if constexpr (TPR == 32) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t cnt = e - b;  // <= SEG = 32, the same for the whole warp
+    uint32_t my_j = 0;
+    double my_a = 0.0;
+    if (uint32_t(lane) < cnt) {
+      my_j = __ldg(col + b + lane);
+      my_a = double(__ldg(val + b + lane));
+      if (SCALE) my_a *= double(__ldg(dinv + my_j));
+    }
+    // items in flight per lane: 16-byte loads four at a time, narrower ones eight
+    constexpr int U = (CPT * sizeof(V) >= 16) ? 4 : 8;
+    uint32_t i = 0;
+    for (; i + U <= cnt; i += U) {
+      double xv[U][CPT];
+#pragma unroll
+      for (int u = 0; u < U; ++u) load_cols<K, V>(y, __shfl_sync(0xffffffffu, my_j, int(i) + u), c0, xv[u]);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        double av = __shfl_sync(0xffffffffu, my_a, int(i) + u);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] += av * xv[u][c];
+      }
+    }
+    for (; i < cnt; ++i) {
+      uint32_t j = __shfl_sync(0xffffffffu, my_j, int(i));
+      double a = __shfl_sync(0xffffffffu, my_a, int(i));
+      double xv[CPT];
+      load_cols<K, V>(y, j, c0, xv);
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) acc[c] += a * xv[c];
+    }
+  } else {
+    for (uint32_t i = b; i < e; ++i) {
+      uint32_t j = __ldg(col + i);
+      double a = double(__ldg(val + i));
+      if (SCALE) a *= double(__ldg(dinv + j));
+      double xv[CPT];
+      load_cols<K, V>(y, j, c0, xv);
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) acc[c] += a * xv[c];
+    }
+  }
+}
 
 template <int K, typename V = double>
 __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(PersistentPcg<K, V> a) {
@@ -276,6 +356,195 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(Persisten
   if (blockIdx.x == 0) {
     for (int j = threadIdx.x; j < K; j += blockDim.x) {
       a.s.rz[j] = s_rz[j];
+      a.s.active[j] = s_active[j];
+      a.s.iters[j] = s_iters[j];
+    }
+    if (threadIdx.x == 0) *a.s.nactive = s_nactive;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Two grid barriers per iteration: Jacobi PCG in the Chronopoulos-Gear form
+// (A. T. Chronopoulos and C. W. Gear, "s-step iterative methods for symmetric
+// linear systems", J. Comput. Appl. Math. 25 (1989)).  With u = D^{-1} r and
+// w = A u, the direction p and its image s = A p are both carried by
+// recurrence,
+//   beta_i  = gamma_i / gamma_{i-1},     gamma_i = r_i.u_i,  delta_i = u_i.w_i
+//   alpha_i = gamma_i / (delta_i - beta_i gamma_i / alpha_{i-1})
+//   p_i = u_i + beta_i p_{i-1},   s_i = w_i + beta_i s_{i-1}
+//   x_{i+1} = x_i + alpha_i p_i,  r_{i+1} = r_i - alpha_i s_i,
+// so one sparse product (w = A u) and ONE fused reduction (gamma, r.r, delta)
+// serve an iteration:
+//   phase F (rows):     w from the segment products; p, s, x, r; gamma and r.r
+//                       of the new residual                       | barrier
+//   phase S (segments): products of u = D^{-1} r (scaled on the fly) and
+//                       delta = u.(A u)                           | barrier
+// The reductions of an iteration are read after the second barrier and the
+// next ones written after it, so they alternate between two buffers.  The
+// first iteration of every launch starts from p = u (beta = 0); the iteration
+// count and the convergence test on r.r are those of the three-barrier form.
+template <int K, typename V>
+__device__ __forceinline__ void cg_products(const PersistentPcg<K, V>& a, size_t gid, size_t ngroups, int c0,
+                                            double* partial, double (*sm)[1][K]) {
+  constexpr int CPT = Cols<K>::CPT;
+  double v[1][CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) v[0][c] = 0.0;
+  for (size_t sg = gid; sg < a.nseg; sg += ngroups) {
+    uint32_t row = a.seg_row[sg], b = a.seg_begin[sg], e = a.seg_end[sg];
+    double acc[CPT];
+    segment_gather<K, V, true>(a.col, a.val, a.dinv, a.r, b, e, c0, acc);
+    double rr_[CPT];
+    load_cols<K, V>(a.r, row, c0, rr_);
+    double di = double(a.dinv[row]);
+    double d = (b == a.ptr[row]) ? double(a.diag[row]) : 0.0;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      a.seg_buf[sg * K + c0 + c] = V(acc[c]);
+      double u = di * rr_[c];
+      v[0][c] += u * (d * u - acc[c]);
+    }
+  }
+  block_reduce_cols_big<K, 1>(v, partial, sm);
+}
+
+template <int K, typename V = double>
+__global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent_cg(PersistentPcg<K, V> a) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  __shared__ double s_alpha[K], s_beta[K], s_gamma[K], s_tol2[K];
+  __shared__ int s_active[K], s_iters[K];
+  __shared__ int s_nactive;
+  __shared__ double s_fin[3 * K];
+  __shared__ double s_scratch[PERSIST_THREADS];
+  __shared__ double s_red[PERSIST_THREADS / 32][2][K];
+
+  for (int j = threadIdx.x; j < K; j += blockDim.x) {
+    s_tol2[j] = a.s.tol2[j];
+    s_active[j] = a.s.active[j];
+    s_iters[j] = a.s.iters[j];
+    s_alpha[j] = 0.0;
+    s_gamma[j] = 0.0;
+  }
+  if (threadIdx.x == 0) s_nactive = 0;
+  __syncthreads();
+
+  const int c0 = int(threadIdx.x % TPR) * CPT;
+  const size_t gid = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) / TPR;
+  const size_t ngroups = size_t(gridDim.x) * blockDim.x / TPR;
+  const size_t G = gridDim.x;
+  // reduction buffers of parity q: (gamma, r.r) at base(q), delta at base(q) + 2 G K
+  auto base = [&](int q) { return a.partial_a + size_t(q) * 3 * G * K; };
+
+  // ---- prologue: gamma and r.r of the starting residual, products of u and delta
+  {
+    double w[2][CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) w[0][c] = w[1][c] = 0.0;
+    for (size_t row = gid; row < a.n; row += ngroups) {
+      double di = double(a.dinv[row]);
+      double rv[CPT];
+      load_cols<K, V>(a.r, uint32_t(row), c0, rv);
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        w[0][c] += rv[c] * (di * rv[c]);
+        w[1][c] += rv[c] * rv[c];
+      }
+    }
+    block_reduce_cols_big<K, 2>(w, base(0), (double(*)[2][K])s_red);
+    cg_products<K, V>(a, gid, ngroups, c0, base(0) + 2 * G * K, (double(*)[1][K])s_red);
+  }
+  grid.sync();
+
+  int par = 0, it = 0;
+  for (;; ++it) {
+    // ---- step lengths from the reductions of parity `par`
+    redundant_finish<2, K>(base(par), gridDim.x, s_fin, s_scratch);
+    redundant_finish<1, K>(base(par) + 2 * G * K, gridDim.x, s_fin + 2 * K, s_scratch);
+    if (threadIdx.x == 0) s_nactive = 0;
+    __syncthreads();
+    for (int j = threadIdx.x; j < K; j += blockDim.x) {
+      double g = s_fin[j], rr = s_fin[K + j], dl = s_fin[2 * K + j];
+      double al = 0.0, be = 0.0;
+      if (s_active[j] && it > 0) {
+        // the update of the previous iteration is done: count it, test r.r
+        s_iters[j] += 1;
+        if (blockIdx.x == 0) a.s.rr[j] = rr;
+        if (rr <= s_tol2[j]) s_active[j] = 0;
+      }
+      if (s_active[j]) {
+        double den = dl;
+        if (it > 0) {
+          be = g / s_gamma[j];
+          den = dl - be * g / s_alpha[j];
+        }
+        if (!(den > 0.0) || !isfinite(den)) {
+          if (blockIdx.x == 0) atomicCAS(a.s.breakdown, -1, j);
+          s_active[j] = 0;
+          be = 0.0;
+        } else {
+          al = g / den;
+          s_gamma[j] = g;
+          s_alpha[j] = al;
+          atomicAdd(&s_nactive, 1);
+        }
+      }
+      s_fin[j] = al;      // this iteration's step length
+      s_beta[j] = be;
+    }
+    __syncthreads();
+    if (s_nactive == 0 || it >= a.max_iters) break;
+    par ^= 1;
+
+    // ---- F: w = diag u - sum(segments); p, s, x, r; gamma and r.r of the new r
+    {
+      double w2[2][CPT];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) w2[0][c] = w2[1][c] = 0.0;
+      for (size_t row = gid; row < a.n; row += ngroups) {
+        uint32_t s0 = a.row_first[row], s1 = a.row_first[row + 1];
+        double dr = double(a.diag[row]), di = double(a.dinv[row]);
+        size_t o = row * K + c0;
+        double wv[CPT], rv[CPT];
+        load_cols<K, V>(a.r, uint32_t(row), c0, rv);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) wv[c] = dr * (di * rv[c]);
+        for (uint32_t sg = s0; sg < s1; ++sg) {
+          double sv[CPT];
+          load_cols<K, V>(a.seg_buf, sg, c0, sv);
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) wv[c] -= sv[c];
+        }
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          double al = s_fin[c0 + c], be = s_beta[c0 + c];
+          // the first update of a launch reads no earlier p, s (never initialised)
+          double pn = di * rv[c], sn = wv[c];
+          if (it > 0) {
+            pn += be * double(a.p[o + c]);
+            sn += be * double(a.ap[o + c]);
+          }
+          a.p[o + c] = V(pn);
+          a.ap[o + c] = V(sn);
+          a.x[o + c] = V(double(a.x[o + c]) + al * pn);
+          V rn = V(rv[c] - al * sn);
+          a.r[o + c] = rn;
+          double ri = double(rn);
+          w2[0][c] += ri * (di * ri);
+          w2[1][c] += ri * ri;
+        }
+      }
+      block_reduce_cols_big<K, 2>(w2, base(par), (double(*)[2][K])s_red);
+    }
+    grid.sync();
+    // ---- S: products of the new u and delta
+    cg_products<K, V>(a, gid, ngroups, c0, base(par) + 2 * G * K, (double(*)[1][K])s_red);
+    grid.sync();
+  }
+  if (blockIdx.x == 0) {
+    for (int j = threadIdx.x; j < K; j += blockDim.x) {
+      a.s.rz[j] = s_gamma[j];
       a.s.active[j] = s_active[j];
       a.s.iters[j] = s_iters[j];
     }
