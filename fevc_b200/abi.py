@@ -318,6 +318,7 @@ SIGNATURES = {
     "vckss_rust_engine_last_error": (C.c_char_p, []),
     "fevcb_device_count": (i32, []),
     "fevcb_set_stream": (i32, [C.c_void_p]),
+    "fevcb_device_cache_trim_v1": (i32, [C.POINTER(u64), C.POINTER(u64)]),
     "fevcb_engine_solve_options_v1": (i32, [u64, C.c_void_p]),
     "fevcb_engine_timings_v1": (i32, [u64, C.c_void_p, u32]),
     "fevcb_engine_resolve_v1": (i32, [u64]),

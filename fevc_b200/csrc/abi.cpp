@@ -1214,6 +1214,14 @@ int32_t fevcb_set_stream(void* stream) {
   return status([&] { set_device_stream(stream); });
 }
 
+int32_t fevcb_device_cache_trim_v1(uint64_t* freed_bytes, uint64_t* cached_bytes) {
+  return status([&] {
+    uint64_t freed = device_cache_trim();
+    if (freed_bytes) *freed_bytes = freed;
+    if (cached_bytes) *cached_bytes = device_cache_bytes();
+  });
+}
+
 int32_t fevcb_engine_solve_options_v1(uint64_t generation, const FevcbSolveOptionsV1* options) {
   return status([&] {
     auto o = read_struct(options, "device solve options", 0);

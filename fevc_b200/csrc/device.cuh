@@ -21,6 +21,13 @@ inline void check_cuda(cudaError_t e, const char* what) {
 #define CK(x) ::fevcb::check_cuda((x), #x)
 #define CK_LAUNCH() ::fevcb::check_cuda(cudaGetLastError(), "kernel launch")
 
+// Device memory behind DBuf (devmem.cu): released blocks are cached per
+// device and reused; device_cache_trim returns them to the driver.
+void* device_acquire(size_t bytes);
+void device_release(void* p);
+size_t device_cache_trim();
+size_t device_cache_bytes();
+
 // Owned device allocation.
 template <class T>
 struct DBuf {
@@ -41,14 +48,14 @@ struct DBuf {
   }
   ~DBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) device_release(p);
     p = nullptr;
     n = 0;
   }
   void alloc(size_t count) {
     release();
     if (count == 0) count = 1;
-    CK(cudaMalloc(&p, count * sizeof(T)));
+    p = static_cast<T*>(device_acquire(count * sizeof(T)));
     n = count;
   }
   size_t bytes() const { return n * sizeof(T); }

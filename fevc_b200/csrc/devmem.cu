@@ -1,0 +1,126 @@
+// Process-wide cache of device allocations behind DBuf.
+//
+// A prepared generation holds a few GB of device buffers (the hybrid
+// Laplacian, per-cell and per-unit tables, and per block width the K-column
+// workspaces).  Callers release a generation and prepare the next one for
+// every new sample, so fresh cudaMalloc / cudaFree pairs would sit on every
+// solve's path; cudaFree also synchronises the device.  Released blocks are
+// therefore kept per device and handed out again to requests of a similar
+// size (a cached block is reused for a request of at least 4/5 of its size).
+// The cache is bounded (DEVICE_CACHE_LIMIT bytes per device, the largest
+// blocks freed first), is trimmed and the allocation retried when cudaMalloc
+// fails, and fevcb_device_cache_trim_v1 empties it on request.
+//
+// A block is released only once no queued work can still touch it: the
+// owners (DeviceEngine, the trainer) synchronise their stream before their
+// buffers go, and within one owner the reuse is stream-ordered.
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <unordered_map>
+
+#include "device.cuh"
+
+namespace fevcb {
+
+namespace {
+
+constexpr size_t DEVICE_CACHE_LIMIT = size_t(16) << 30;
+constexpr int MAX_DEVICES = 64;
+
+size_t round_request(size_t bytes) {
+  // 512-byte granules below 1 MiB, 1 MiB granules above
+  if (bytes < (size_t(1) << 20)) return (bytes + 511) & ~size_t(511);
+  return (bytes + (size_t(1) << 20) - 1) & ~((size_t(1) << 20) - 1);
+}
+
+struct DeviceCache {
+  std::multimap<size_t, void*> free_blocks;  // size -> block
+  std::unordered_map<void*, size_t> live;    // block -> size
+  size_t cached = 0;
+};
+
+std::mutex g_mu;
+DeviceCache g_cache[MAX_DEVICES];
+
+int current_device() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) {
+    cudaGetLastError();
+    return 0;
+  }
+  return dev;
+}
+
+size_t trim_locked(DeviceCache& c, size_t keep) {
+  size_t freed = 0;
+  while (c.cached > keep && !c.free_blocks.empty()) {
+    auto it = std::prev(c.free_blocks.end());  // largest first
+    cudaFree(it->second);
+    c.cached -= it->first;
+    freed += it->first;
+    c.free_blocks.erase(it);
+  }
+  return freed;
+}
+
+}  // namespace
+
+void* device_acquire(size_t bytes) {
+  const size_t want = round_request(bytes);
+  const int dev = current_device();
+  std::lock_guard<std::mutex> l(g_mu);
+  DeviceCache& c = g_cache[dev];
+  auto it = c.free_blocks.lower_bound(want);
+  if (it != c.free_blocks.end() && want >= it->first - it->first / 5) {
+    void* p = it->second;
+    size_t have = it->first;
+    c.free_blocks.erase(it);
+    c.cached -= have;
+    c.live[p] = have;
+    return p;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, want);
+  if (e == cudaErrorMemoryAllocation && c.cached > 0) {
+    cudaGetLastError();
+    trim_locked(c, 0);
+    e = cudaMalloc(&p, want);
+  }
+  check_cuda(e, "cudaMalloc");
+  c.live[p] = want;
+  return p;
+}
+
+void device_release(void* p) {
+  if (!p) return;
+  const int dev = current_device();
+  std::lock_guard<std::mutex> l(g_mu);
+  DeviceCache& c = g_cache[dev];
+  auto it = c.live.find(p);
+  if (it == c.live.end()) {
+    // allocated on another device: return it to the driver
+    cudaFree(p);
+    return;
+  }
+  size_t have = it->second;
+  c.live.erase(it);
+  c.free_blocks.emplace(have, p);
+  c.cached += have;
+  if (c.cached > DEVICE_CACHE_LIMIT) trim_locked(c, DEVICE_CACHE_LIMIT);
+}
+
+size_t device_cache_trim() {
+  const int dev = current_device();
+  std::lock_guard<std::mutex> l(g_mu);
+  return trim_locked(g_cache[dev], 0);
+}
+
+size_t device_cache_bytes() {
+  const int dev = current_device();
+  std::lock_guard<std::mutex> l(g_mu);
+  return g_cache[dev].cached;
+}
+
+}  // namespace fevcb

@@ -17,6 +17,9 @@
 
 #include <algorithm>
 #include <chrono>
+#include <exception>
+#include <thread>
+#include <functional>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -37,28 +40,39 @@ namespace fevcb {
 // ---------------------------------------------------------------------------
 // kernels that are not templated
 
+// out[o] = sum over b of partial[b][o] for o < width, summed in a fixed order.
+// Block x handles FINISH_COLS columns with blockDim / FINISH_COLS lanes each.
+constexpr int FINISH_COLS = 16;
+constexpr int FINISH_THREADS = 1024;
 __global__ void k_finish(const double* __restrict__ partial, int blocks, int width, double* __restrict__ out) {
-  __shared__ double sm[1024];
-  if (width <= int(blockDim.x)) {
-    int groups = blockDim.x / width;
-    int o = threadIdx.x % width, g = threadIdx.x / width;
-    double acc = 0.0;
-    if (g < groups)
-      for (int b = g; b < blocks; b += groups) acc += partial[size_t(b) * width + o];
-    sm[threadIdx.x] = acc;
-    __syncthreads();
-    if (g == 0) {
-      double s = 0.0;
-      for (int k = 0; k < groups; ++k) s += sm[k * width + o];
-      out[o] = s;
+  __shared__ double sm[FINISH_THREADS];
+  const int groups = blockDim.x / FINISH_COLS;
+  const int o = blockIdx.x * FINISH_COLS + threadIdx.x % FINISH_COLS, g = threadIdx.x / FINISH_COLS;
+  double acc = 0.0;
+  if (o < width) {
+    // four independent partial sums keep four loads in flight per thread
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int b = g;
+    for (; b + 3 * groups < blocks; b += 4 * groups) {
+      a0 += partial[size_t(b) * width + o];
+      a1 += partial[size_t(b + groups) * width + o];
+      a2 += partial[size_t(b + 2 * groups) * width + o];
+      a3 += partial[size_t(b + 3 * groups) * width + o];
     }
-  } else {
-    for (int oo = threadIdx.x; oo < width; oo += blockDim.x) {
-      double acc = 0.0;
-      for (int b = 0; b < blocks; ++b) acc += partial[size_t(b) * width + oo];
-      out[oo] = acc;
-    }
+    for (; b < blocks; b += groups) a0 += partial[size_t(b) * width + o];
+    acc = (a0 + a1) + (a2 + a3);
   }
+  sm[threadIdx.x] = acc;
+  __syncthreads();
+  if (g == 0 && o < width) {
+    double sum = 0.0;
+    for (int k = 0; k < groups; ++k) sum += sm[k * FINISH_COLS + threadIdx.x];
+    out[o] = sum;
+  }
+}
+
+void finish(const double* partial, int blocks, int width, double* out, cudaStream_t s) {
+  k_finish<<<(width + FINISH_COLS - 1) / FINISH_COLS, FINISH_THREADS, 0, s>>>(partial, blocks, width, out);
 }
 
 __global__ void k_raw_atoms(uint64_t count, const uint64_t* __restrict__ entity, const uint64_t* __restrict__ trials,
@@ -197,7 +211,7 @@ static int grid_blocks() {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    blocks = sms * 4;  // four 256-thread blocks per SM for the streaming kernels
+    blocks = sms * 8;  // eight 256-thread blocks per SM (full occupancy at 32 registers)
   }
   return blocks;
 }
@@ -229,7 +243,9 @@ struct DeviceEngine {
   // hybrid Laplacian
   DBuf<uint32_t> L_ptr, L_col;
   DBuf<double> L_val, L_diag, L_dinv;
+  DBuf<double> L_vald;                      // L_val[e] * L_dinv[L_col[e]] (A D^{-1})
   DBuf<float> L_val32, L_diag32, L_dinv32;  // single-precision copies for mixed-precision solves
+  DBuf<float> L_vald32;
   std::unique_ptr<Multigrid> mg;
   std::unique_ptr<LearnedPreconditioner> learned;
   int preconditioner = 1;
@@ -287,6 +303,8 @@ struct BlockWork {
 };
 
 DeviceEngine::~DeviceEngine() {
+  // the buffers go back to the device cache: no queued work may still use them
+  if (stream) cudaStreamSynchronize(stream);
   work.clear();
   if (h_nactive) cudaFreeHost(h_nactive);
   if (ev0) cudaEventDestroy(ev0);
@@ -297,6 +315,36 @@ DeviceEngine::~DeviceEngine() {
 namespace {
 
 }  // namespace
+
+// out[e] = val[e] * dinv[col[e]]: the Laplacian's off-diagonal entries scaled
+// by the inverse diagonal of their column (A D^{-1}).
+__global__ void k_scale_by_col(size_t nnz, const uint32_t* __restrict__ col, const double* __restrict__ val,
+                               const double* __restrict__ dinv, double* __restrict__ out) {
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nnz; i += size_t(gridDim.x) * blockDim.x)
+    out[i] = val[i] * dinv[col[i]];
+}
+
+// Run the tasks on their own threads, bound to the calling thread's device;
+// the first exception (by task order) is rethrown after all have finished.
+void run_parallel(const std::vector<std::function<void()>>& tasks) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::vector<std::exception_ptr> errors(tasks.size());
+  std::vector<std::thread> threads;
+  threads.reserve(tasks.size());
+  for (size_t i = 0; i < tasks.size(); ++i)
+    threads.emplace_back([&, i] {
+      try {
+        CK(cudaSetDevice(dev));
+        tasks[i]();
+      } catch (...) {
+        errors[i] = std::current_exception();
+      }
+    });
+  for (auto& t : threads) t.join();
+  for (auto& err : errors)
+    if (err) std::rethrow_exception(err);
+}
 
 std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaPlan& plan, int preconditioner) {
   if (device_count() < 1) fail(UNSUPPORTED_FEATURE, "device", "no CUDA device is visible; the engine runs only on a GPU");
@@ -312,7 +360,6 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     }
   }
   cudaStream_t s = e->stream;
-  uint64_t& h2d = e->stats.h2d_bytes;
   e->W = uint32_t(p.workers);
   e->F = uint32_t(p.firms);
   e->C = uint32_t(p.cells);
@@ -320,177 +367,203 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   e->S = uint32_t(plan.tgt_cell.size());
   e->target_total = p.target_total;
 
-  std::vector<uint32_t> wptr(p.worker_index.ptr.begin(), p.worker_index.ptr.end());
-  std::vector<uint32_t> fptr(p.firm_index.ptr.begin(), p.firm_index.ptr.end());
-  upload(e->cell_worker, p.cell_worker, s, h2d);
-  upload(e->cell_firm, p.cell_firm, s, h2d);
-  upload(e->cell_weight, p.cell_weight, s, h2d);
-  upload(e->cell_outcome, p.cell_outcome_sum, s, h2d);
-  upload(e->cell_target, p.cell_target_sum, s, h2d);
-  upload(e->worker_ptr, wptr, s, h2d);
-  upload(e->firm_ptr, fptr, s, h2d);
-  upload(e->firm_cells, p.firm_index.items, s, h2d);
-  build_segments(fptr, e->firm_seg, s, h2d);
-  {
-    std::vector<double> fd(p.firms, 0.0);
-    for (size_t c = 0; c < p.cells; ++c) fd[p.cell_firm[c]] += p.cell_weight[c];
-    upload(e->firm_diag, fd, s, h2d);
-  }
-
-  // units in cell order (stable within a cell: plan group order); for
-  // leave-observation-out every row is a unit, keyed by its class rank and
-  // the number of its first copy inside the class
-  if (plan.observation) {
-    e->observation = true;
-    size_t R = p.rows();
-    e->G = uint32_t(R);
-    std::vector<uint32_t> uptr(p.cells + 1, 0);
-    for (size_t r = 0; r < R; ++r) uptr[p.row_cell[r] + 1]++;
-    for (size_t c = 0; c < p.cells; ++c) uptr[c + 1] += uptr[c];
-    std::vector<uint32_t> cur(uptr.begin(), uptr.end() - 1), order(R);
-    for (size_t r = 0; r < R; ++r) order[cur[p.row_cell[r]]++] = uint32_t(r);
-    std::vector<uint64_t> urank(R), ucount(R), uoff(R), phys(R + 1, 0);
-    for (size_t i = 0; i < R; ++i) {
-      uint32_t r = order[i];
-      urank[i] = plan.row_rank[r];
-      ucount[i] = p.frequency[r];
-      uoff[i] = plan.row_copy_offset[r];
-    }
-    for (size_t r = 0; r < R; ++r) phys[r + 1] = phys[r] + p.frequency[r];
-    e->physical = phys[R];
-    upload(e->unit_ptr, uptr, s, h2d);
-    upload(e->unit_rank, urank, s, h2d);
-    upload(e->unit_count, ucount, s, h2d);
-    upload(e->unit_offset, uoff, s, h2d);
-    upload(e->row_rank_d, plan.row_rank, s, h2d);
-    upload(e->row_copy_offset, plan.row_copy_offset, s, h2d);
-    upload(e->row_phys, phys, s, h2d);
-    e->obs_row_acc.alloc(R * 4);
-    e->obs_copy_acc.alloc(size_t(e->physical) * 4);
-    e->control_lev.alloc(R);
-    e->obs_out.alloc(R * 2);
-  } else {
-    std::vector<uint32_t> uptr(p.cells + 1, 0);
-    for (uint32_t c : plan.del_cell) uptr[c + 1]++;
-    for (size_t c = 0; c < p.cells; ++c) uptr[c + 1] += uptr[c];
-    std::vector<uint32_t> cur(uptr.begin(), uptr.end() - 1);
-    e->unit_group.assign(plan.del_cell.size(), 0);
-    for (size_t g = 0; g < plan.del_cell.size(); ++g) e->unit_group[cur[plan.del_cell[g]]++] = uint32_t(g);
-    std::vector<uint32_t> ucell(e->G);
-    std::vector<uint64_t> urank(e->G), ucount(e->G);
-    std::vector<double> uout(e->G), ucf(e->G), usq(e->G);
-    for (size_t i = 0; i < e->G; ++i) {
-      uint32_t g = e->unit_group[i];
-      ucell[i] = plan.del_cell[g];
-      urank[i] = plan.del_rank[g];
-      ucount[i] = plan.del_count[g];
-      if (ucount[i] == 0 || ucount[i] > MAX_EXACT_BINARY64_INTEGER || (ucount[i] + 63) / 64 > MAX_WORDS_PER_ATOM)
-        fail(RESOURCE_LIMIT, "jla_validate", "leverage trial preflight failed");
-      uout[i] = plan.del_outcome_sum[g];
-      ucf[i] = double(plan.del_count[g]);
-      usq[i] = std::sqrt(ucf[i]);
-    }
-    upload(e->unit_ptr, uptr, s, h2d);
-    upload(e->unit_cell, ucell, s, h2d);
-    upload(e->unit_rank, urank, s, h2d);
-    upload(e->unit_count, ucount, s, h2d);
-    upload(e->unit_outcome, uout, s, h2d);
-    upload(e->unit_count_f, ucf, s, h2d);
-    upload(e->unit_sqrt_n, usq, s, h2d);
-  }
-  // strata (already in cell order)
-  {
-    std::vector<uint32_t> tptr(p.cells + 1, 0);
-    for (size_t k = 0; k < plan.tgt_cell.size(); ++k) {
-      if (k > 0 && plan.tgt_cell[k] < plan.tgt_cell[k - 1])
-        fail(INTERNAL_INVARIANT_FAILED, "jla_plan", "target strata are not in cell order");
-      tptr[plan.tgt_cell[k] + 1]++;
-      if (plan.tgt_count[k] == 0 || (plan.tgt_count[k] + 63) / 64 > MAX_WORDS_PER_ATOM)
-        fail(RESOURCE_LIMIT, "jla_validate", "target trial preflight failed");
-    }
-    for (size_t c = 0; c < p.cells; ++c) tptr[c + 1] += tptr[c];
-    std::vector<double> scale(plan.tgt_cell.size());
-    for (size_t k = 0; k < scale.size(); ++k) scale[k] = std::sqrt(plan.tgt_per_copy[k] / p.target_total);
-    upload(e->tgt_ptr, tptr, s, h2d);
-    upload(e->tgt_rank, plan.tgt_rank, s, h2d);
-    upload(e->tgt_count, plan.tgt_count, s, h2d);
-    upload(e->tgt_scale, scale, s, h2d);
-  }
-  // row-level data of the generic estimator
-  if (plan.generic) {
-    e->generic = true;
-    e->q = int(p.controls.size());
-    if (e->q < (plan.observation ? 0 : 1) || e->q > QMAX)
-      fail(UNSUPPORTED_FEATURE, "generic_jla", "the device engine handles at most 8 control columns");
-    e->rows = uint32_t(p.rows());
-    size_t R = p.rows();
-    std::vector<double> freq(R), Q(R * e->q);
-    for (size_t r = 0; r < R; ++r) {
-      freq[r] = double(p.frequency[r]);
-      for (int k = 0; k < e->q; ++k) Q[r * e->q + k] = p.controls[k][r];
-    }
-    std::vector<uint32_t> cptr(p.cells + 1, 0), crow(R);
-    for (size_t r = 0; r < R; ++r) cptr[p.row_cell[r] + 1]++;
-    for (size_t c = 0; c < p.cells; ++c) cptr[c + 1] += cptr[c];
+  // Four independent host builders, each uploading what it builds: cells and
+  // the firm segments; deletion units and then the generic row data (which
+  // reads the unit order); target strata; the hybrid Laplacian with its
+  // preconditioner.  They run on their own threads (bound to this device);
+  // their uploads share the engine's stream and fill disjoint buffers.
+  uint64_t task_h2d[4] = {0, 0, 0, 0};
+  (void)grid_blocks();  // initialise the cached grid size before the threads use it
+  auto cells_task = [&] {
+    uint64_t& h2d = task_h2d[0];
+    std::vector<uint32_t> wptr(p.worker_index.ptr.begin(), p.worker_index.ptr.end());
+    std::vector<uint32_t> fptr(p.firm_index.ptr.begin(), p.firm_index.ptr.end());
+    upload(e->cell_worker, p.cell_worker, s, h2d);
+    upload(e->cell_firm, p.cell_firm, s, h2d);
+    upload(e->cell_weight, p.cell_weight, s, h2d);
+    upload(e->cell_outcome, p.cell_outcome_sum, s, h2d);
+    upload(e->cell_target, p.cell_target_sum, s, h2d);
+    upload(e->worker_ptr, wptr, s, h2d);
+    upload(e->firm_ptr, fptr, s, h2d);
+    upload(e->firm_cells, p.firm_index.items, s, h2d);
+    build_segments(fptr, e->firm_seg, s, h2d);
     {
-      std::vector<uint32_t> cur(cptr.begin(), cptr.end() - 1);
-      for (size_t r = 0; r < R; ++r) crow[cur[p.row_cell[r]]++] = uint32_t(r);
+      std::vector<double> fd(p.firms, 0.0);
+      for (size_t c = 0; c < p.cells; ++c) fd[p.cell_firm[c]] += p.cell_weight[c];
+      upload(e->firm_diag, fd, s, h2d);
     }
-    upload(e->row_cell, p.row_cell, s, h2d);
-    upload(e->row_freq, freq, s, h2d);
-    upload(e->row_y, p.outcome, s, h2d);
-    upload(e->Qd, Q, s, h2d);
-    upload(e->cell_rows_ptr, cptr, s, h2d);
-    upload(e->cell_rows, crow, s, h2d);
-    upload(e->group_ptr, plan.group_ptr, s, h2d);
-    upload(e->group_rows, plan.group_rows, s, h2d);
-    upload(e->unit_group_d, e->unit_group, s, h2d);
-    e->Rd.alloc(R * e->q);
-    e->residual.alloc(R);
-    e->deleted.alloc(R);
-    e->alphaH.alloc(size_t(e->W) * QMAX);
-    e->psiH.alloc(size_t(e->F) * QMAX);
-    e->beta_buf.alloc(QMAX * 128);
-  }
-  // hybrid Laplacian
-  {
-    std::vector<uint32_t> kw, Lptr, Lcol;
-    std::vector<int32_t> ki;
-    std::vector<double> cs, wd, Lval, Ld;
-    build_hybrid(p, ELIMINATE_MAX_DEGREE, kw, ki, cs, wd, Lptr, Lcol, Lval, Ld);
-    e->kept = uint32_t(kw.size());
-    e->n = e->F + e->kept;
-    std::vector<double> dinv(Ld.size());
-    for (size_t v = 0; v < Ld.size(); ++v) dinv[v] = 1.0 / Ld[v];
-    upload(e->kept_worker, kw, s, h2d);
-    upload(e->kept_index, ki, s, h2d);
-    upload(e->cell_scale, cs, s, h2d);
-    upload(e->worker_diag, wd, s, h2d);
-    upload(e->L_ptr, Lptr, s, h2d);
-    upload(e->L_col, Lcol, s, h2d);
-    upload(e->L_val, Lval, s, h2d);
-    upload(e->L_diag, Ld, s, h2d);
-    upload(e->L_dinv, dinv, s, h2d);
-    build_segments(Lptr, e->lap_seg, s, h2d);
-    e->stats.vertices = e->n;
-    e->stats.terminal_vertices = e->n;
-    e->stats.edges = Lcol.size() / 2;
-    e->stats.kept_workers = e->kept;
-    e->preconditioner = preconditioner == 0 ? 1 : preconditioner;
-    if (e->preconditioner == 2) {
-      e->mg = build_multigrid(e->n, Lptr, Lcol, Lval, Ld, s, h2d);
-      e->stats.levels = e->mg->levels();
-      e->stats.terminal_vertices = e->mg->report().vertices.back();
-    } else if (e->preconditioner == 3) {
-      std::vector<float> params = learned_params();
-      if (params.empty())
-        fail(UNSUPPORTED_FEATURE, "learned_preconditioner", "no network parameters are installed");
-      e->learned = build_learned(params, e->n, Lptr, Lcol, Lval, Ld, s, h2d);
-      e->stats.levels = 1;
+
+  };
+  auto units_task = [&] {
+    uint64_t& h2d = task_h2d[1];
+    // units in cell order (stable within a cell: plan group order); for
+    // leave-observation-out every row is a unit, keyed by its class rank and
+    // the number of its first copy inside the class
+    if (plan.observation) {
+      e->observation = true;
+      size_t R = p.rows();
+      e->G = uint32_t(R);
+      std::vector<uint32_t> uptr(p.cells + 1, 0);
+      for (size_t r = 0; r < R; ++r) uptr[p.row_cell[r] + 1]++;
+      for (size_t c = 0; c < p.cells; ++c) uptr[c + 1] += uptr[c];
+      std::vector<uint32_t> cur(uptr.begin(), uptr.end() - 1), order(R);
+      for (size_t r = 0; r < R; ++r) order[cur[p.row_cell[r]]++] = uint32_t(r);
+      std::vector<uint64_t> urank(R), ucount(R), uoff(R), phys(R + 1, 0);
+      for (size_t i = 0; i < R; ++i) {
+        uint32_t r = order[i];
+        urank[i] = plan.row_rank[r];
+        ucount[i] = p.frequency[r];
+        uoff[i] = plan.row_copy_offset[r];
+      }
+      for (size_t r = 0; r < R; ++r) phys[r + 1] = phys[r] + p.frequency[r];
+      e->physical = phys[R];
+      upload(e->unit_ptr, uptr, s, h2d);
+      upload(e->unit_rank, urank, s, h2d);
+      upload(e->unit_count, ucount, s, h2d);
+      upload(e->unit_offset, uoff, s, h2d);
+      upload(e->row_rank_d, plan.row_rank, s, h2d);
+      upload(e->row_copy_offset, plan.row_copy_offset, s, h2d);
+      upload(e->row_phys, phys, s, h2d);
+      e->obs_row_acc.alloc(R * 4);
+      e->obs_copy_acc.alloc(size_t(e->physical) * 4);
+      e->control_lev.alloc(R);
+      e->obs_out.alloc(R * 2);
     } else {
-      e->stats.levels = 1;
+      std::vector<uint32_t> uptr(p.cells + 1, 0);
+      for (uint32_t c : plan.del_cell) uptr[c + 1]++;
+      for (size_t c = 0; c < p.cells; ++c) uptr[c + 1] += uptr[c];
+      std::vector<uint32_t> cur(uptr.begin(), uptr.end() - 1);
+      e->unit_group.assign(plan.del_cell.size(), 0);
+      for (size_t g = 0; g < plan.del_cell.size(); ++g) e->unit_group[cur[plan.del_cell[g]]++] = uint32_t(g);
+      std::vector<uint32_t> ucell(e->G);
+      std::vector<uint64_t> urank(e->G), ucount(e->G);
+      std::vector<double> uout(e->G), ucf(e->G), usq(e->G);
+      for (size_t i = 0; i < e->G; ++i) {
+        uint32_t g = e->unit_group[i];
+        ucell[i] = plan.del_cell[g];
+        urank[i] = plan.del_rank[g];
+        ucount[i] = plan.del_count[g];
+        if (ucount[i] == 0 || ucount[i] > MAX_EXACT_BINARY64_INTEGER || (ucount[i] + 63) / 64 > MAX_WORDS_PER_ATOM)
+          fail(RESOURCE_LIMIT, "jla_validate", "leverage trial preflight failed");
+        uout[i] = plan.del_outcome_sum[g];
+        ucf[i] = double(plan.del_count[g]);
+        usq[i] = std::sqrt(ucf[i]);
+      }
+      upload(e->unit_ptr, uptr, s, h2d);
+      upload(e->unit_cell, ucell, s, h2d);
+      upload(e->unit_rank, urank, s, h2d);
+      upload(e->unit_count, ucount, s, h2d);
+      upload(e->unit_outcome, uout, s, h2d);
+      upload(e->unit_count_f, ucf, s, h2d);
+      upload(e->unit_sqrt_n, usq, s, h2d);
     }
-  }
+    // row-level data of the generic estimator
+    if (plan.generic) {
+      e->generic = true;
+      e->q = int(p.controls.size());
+      if (e->q < (plan.observation ? 0 : 1) || e->q > QMAX)
+        fail(UNSUPPORTED_FEATURE, "generic_jla", "the device engine handles at most 8 control columns");
+      e->rows = uint32_t(p.rows());
+      size_t R = p.rows();
+      std::vector<double> freq(R), Q(R * e->q);
+      for (size_t r = 0; r < R; ++r) {
+        freq[r] = double(p.frequency[r]);
+        for (int k = 0; k < e->q; ++k) Q[r * e->q + k] = p.controls[k][r];
+      }
+      std::vector<uint32_t> cptr(p.cells + 1, 0), crow(R);
+      for (size_t r = 0; r < R; ++r) cptr[p.row_cell[r] + 1]++;
+      for (size_t c = 0; c < p.cells; ++c) cptr[c + 1] += cptr[c];
+      {
+        std::vector<uint32_t> cur(cptr.begin(), cptr.end() - 1);
+        for (size_t r = 0; r < R; ++r) crow[cur[p.row_cell[r]]++] = uint32_t(r);
+      }
+      upload(e->row_cell, p.row_cell, s, h2d);
+      upload(e->row_freq, freq, s, h2d);
+      upload(e->row_y, p.outcome, s, h2d);
+      upload(e->Qd, Q, s, h2d);
+      upload(e->cell_rows_ptr, cptr, s, h2d);
+      upload(e->cell_rows, crow, s, h2d);
+      upload(e->group_ptr, plan.group_ptr, s, h2d);
+      upload(e->group_rows, plan.group_rows, s, h2d);
+      upload(e->unit_group_d, e->unit_group, s, h2d);
+      e->Rd.alloc(R * e->q);
+      e->residual.alloc(R);
+      e->deleted.alloc(R);
+      e->alphaH.alloc(size_t(e->W) * QMAX);
+      e->psiH.alloc(size_t(e->F) * QMAX);
+      e->beta_buf.alloc(QMAX * 128);
+    }
+  };
+  auto strata_task = [&] {
+    uint64_t& h2d = task_h2d[2];
+    // strata (already in cell order)
+    {
+      std::vector<uint32_t> tptr(p.cells + 1, 0);
+      for (size_t k = 0; k < plan.tgt_cell.size(); ++k) {
+        if (k > 0 && plan.tgt_cell[k] < plan.tgt_cell[k - 1])
+          fail(INTERNAL_INVARIANT_FAILED, "jla_plan", "target strata are not in cell order");
+        tptr[plan.tgt_cell[k] + 1]++;
+        if (plan.tgt_count[k] == 0 || (plan.tgt_count[k] + 63) / 64 > MAX_WORDS_PER_ATOM)
+          fail(RESOURCE_LIMIT, "jla_validate", "target trial preflight failed");
+      }
+      for (size_t c = 0; c < p.cells; ++c) tptr[c + 1] += tptr[c];
+      std::vector<double> scale(plan.tgt_cell.size());
+      for (size_t k = 0; k < scale.size(); ++k) scale[k] = std::sqrt(plan.tgt_per_copy[k] / p.target_total);
+      upload(e->tgt_ptr, tptr, s, h2d);
+      upload(e->tgt_rank, plan.tgt_rank, s, h2d);
+      upload(e->tgt_count, plan.tgt_count, s, h2d);
+      upload(e->tgt_scale, scale, s, h2d);
+    }
+  };
+  auto hybrid_task = [&] {
+    uint64_t& h2d = task_h2d[3];
+    // hybrid Laplacian
+    {
+      std::vector<uint32_t> kw, Lptr, Lcol;
+      std::vector<int32_t> ki;
+      std::vector<double> cs, wd, Lval, Ld;
+      build_hybrid(p, ELIMINATE_MAX_DEGREE, kw, ki, cs, wd, Lptr, Lcol, Lval, Ld);
+      e->kept = uint32_t(kw.size());
+      e->n = e->F + e->kept;
+      std::vector<double> dinv(Ld.size());
+      for (size_t v = 0; v < Ld.size(); ++v) dinv[v] = 1.0 / Ld[v];
+      upload(e->kept_worker, kw, s, h2d);
+      upload(e->kept_index, ki, s, h2d);
+      upload(e->cell_scale, cs, s, h2d);
+      upload(e->worker_diag, wd, s, h2d);
+      upload(e->L_ptr, Lptr, s, h2d);
+      upload(e->L_col, Lcol, s, h2d);
+      upload(e->L_val, Lval, s, h2d);
+      upload(e->L_diag, Ld, s, h2d);
+      upload(e->L_dinv, dinv, s, h2d);
+      e->L_vald.alloc(Lval.size());
+      if (!Lval.empty())
+        k_scale_by_col<<<grid_blocks(), THREADS, 0, s>>>(Lval.size(), e->L_col.p, e->L_val.p, e->L_dinv.p,
+                                                         e->L_vald.p);
+      CK_LAUNCH();
+      build_segments(Lptr, e->lap_seg, s, h2d);
+      e->stats.vertices = e->n;
+      e->stats.terminal_vertices = e->n;
+      e->stats.edges = Lcol.size() / 2;
+      e->stats.kept_workers = e->kept;
+      e->preconditioner = preconditioner == 0 ? 1 : preconditioner;
+      if (e->preconditioner == 2) {
+        e->mg = build_multigrid(e->n, Lptr, Lcol, Lval, Ld, s, h2d);
+        e->stats.levels = e->mg->levels();
+        e->stats.terminal_vertices = e->mg->report().vertices.back();
+      } else if (e->preconditioner == 3) {
+        std::vector<float> params = learned_params();
+        if (params.empty())
+          fail(UNSUPPORTED_FEATURE, "learned_preconditioner", "no network parameters are installed");
+        e->learned = build_learned(params, e->n, Lptr, Lcol, Lval, Ld, s, h2d);
+        e->stats.levels = 1;
+      } else {
+        e->stats.levels = 1;
+      }
+    }
+  };
+  run_parallel({cells_task, units_task, strata_task, hybrid_task});
+  for (uint64_t b : task_h2d) e->stats.h2d_bytes += b;
   if (!e->observation) {
     e->moments.alloc(size_t(e->G) * 5);
     e->unit_out.alloc(size_t(e->G) * 6);
@@ -599,19 +672,55 @@ __global__ void k_center(uint32_t n, const double* __restrict__ b, const double*
   }
 }
 
+// rz = sum of the per-block partials [blocks][K]; the count of active columns.
+// One block of SET_RZ_THREADS threads, blockDim / K lanes per column.
+constexpr int SET_RZ_THREADS = 1024;
 template <int K>
-__global__ void k_set_rz(const double* __restrict__ partial, int blocks, PcgState s, int refine_only) {
+__global__ void k_set_rz(const double* __restrict__ partial, int blocks, PcgState s) {
+  __shared__ double sm[SET_RZ_THREADS];
   __shared__ int cnt;
   if (threadIdx.x == 0) cnt = 0;
+  const int groups = blockDim.x / K, o = threadIdx.x % K, g = threadIdx.x / K;
+  double acc = 0.0;
+  if (g < groups)
+    for (int b = g; b < blocks; b += groups) acc += partial[size_t(b) * K + o];
+  sm[threadIdx.x] = acc;
   __syncthreads();
-  for (int j = threadIdx.x; j < K; j += blockDim.x) {
-    double acc = 0.0;
-    for (int b = 0; b < blocks; ++b) acc += partial[size_t(b) * K + j];
-    s.rz[j] = acc;
-    if (s.active[j]) atomicAdd(&cnt, 1);
+  if (g == 0) {
+    double sum = 0.0;
+    for (int k = 0; k < groups; ++k) sum += sm[k * K + o];
+    s.rz[o] = sum;
+    if (s.active[o]) atomicAdd(&cnt, 1);
   }
   __syncthreads();
   if (threadIdx.x == 0) *s.nactive = cnt;
+}
+
+// Jacobi start of the three-barrier kernel: p = D^{-1} r, partial r.p.
+template <int K>
+__global__ void __launch_bounds__(THREADS) k_jacobi_start(uint32_t n, const double* __restrict__ dinv,
+                                                          const double* __restrict__ r, double* __restrict__ p,
+                                                          double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  double v[1][CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) v[0][c] = 0.0;
+  const int c0 = int(threadIdx.x % TPR) * CPT;
+  size_t total = size_t(n) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    if (t < total) {
+      size_t vtx = t / TPR, i = vtx * K + c0;
+      double d = dinv[vtx];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        double z = d * r[i + c];
+        p[i + c] = z;
+        v[0][c] += r[i + c] * z;
+      }
+    }
+  }
+  block_reduce_cols<K, 1>(v, partial);
 }
 
 template <int K>
@@ -649,10 +758,11 @@ void apply_preconditioner(DeviceEngine& e, BlockWork& w, Launch L, const double*
 }
 
 // (Re)start PCG from the current x for the active columns: r = b - mean - L x,
-// z = M^-1 r, p = z, rz.  The mean of b is removed so every residual is
-// orthogonal to the Laplacian null space.
+// and, for the preconditioned forms that take them from here, z = M^-1 r,
+// p = z, rz (the two-barrier Jacobi kernel forms its own from r).  The mean of
+// b is removed so every residual is orthogonal to the Laplacian null space.
 template <int K>
-void pcg_restart(DeviceEngine& e, BlockWork& w, Launch L, bool fresh) {
+void pcg_restart(DeviceEngine& e, BlockWork& w, Launch L, bool fresh, bool directions) {
   if (fresh) {
     k_center<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p, w.s.mean, w.r.p, w.x.p);
   } else {
@@ -660,11 +770,30 @@ void pcg_restart(DeviceEngine& e, BlockWork& w, Launch L, bool fresh) {
     k_center<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p, w.s.mean, w.q.p, w.z.p);  // q = b - mean, z = 0
     k_spmm<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_ptr.p, e.L_col.p, e.L_val.p, e.L_diag.p, w.x.p, w.q.p, w.r.p);
   }
-  apply_preconditioner<K>(e, w, L, w.r.p, w.z.p);
-  CK(cudaMemcpyAsync(w.p.p, w.z.p, size_t(e.n) * K * sizeof(double), cudaMemcpyDeviceToDevice, L.s));
-  k_dot<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.r.p, w.z.p, e.partial.p);
-  k_set_rz<K><<<1, 128, 0, L.s>>>(e.partial.p, L.grid, w.s, 0);
+  if (!directions) {
+    CK_LAUNCH();
+    return;
+  }
+  if (e.preconditioner == 2 || e.preconditioner == 3) {
+    apply_preconditioner<K>(e, w, L, w.r.p, w.z.p);
+    CK(cudaMemcpyAsync(w.p.p, w.z.p, size_t(e.n) * K * sizeof(double), cudaMemcpyDeviceToDevice, L.s));
+    k_dot<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.r.p, w.z.p, e.partial.p);
+  } else {
+    k_jacobi_start<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_dinv.p, w.r.p, w.p.p, e.partial.p);
+  }
+  k_set_rz<K><<<1, SET_RZ_THREADS, 0, L.s>>>(e.partial.p, L.grid, w.s);
   CK_LAUNCH();
+}
+
+// The persistent Jacobi PCG form for a block of K columns stored as V: the
+// two-barrier kernel when a warp holds one segment and a vertex's columns
+// take at most 256 bytes (the block stays in L2 and barrier latency
+// dominates); otherwise the three-barrier kernel, whose phase order re-reads
+// r and p while they are still in L2 (measured on the 64-column double
+// block: 2.40 ms against 2.53 ms per 20 iterations).
+template <int K, typename V>
+constexpr bool two_barrier_form() {
+  return Cols<K>::TPR == 32 && K * sizeof(V) <= 256;
 }
 
 // Arguments of the persistent Jacobi PCG kernels over the hybrid Laplacian
@@ -683,6 +812,8 @@ PersistentPcg<K> persistent_args(DeviceEngine& e, BlockWork& w, int iterations) 
   a.seg_begin = e.lap_seg.begin.p;
   a.seg_end = e.lap_seg.end.p;
   a.row_first = e.lap_seg.row_first.p;
+  a.seg_flag = e.lap_seg.row_flag.p;
+  a.vald = e.L_vald.p;
   a.seg_buf = w.seg_buf.p;
   a.x = w.x.p;
   a.r = w.r.p;
@@ -702,8 +833,9 @@ template <int K>
 int pcg_run(DeviceEngine& e, BlockWork& w, Launch L, int iterations) {
   PersistentPcg<K> a = persistent_args<K>(e, w, iterations);
   void* args[] = {&a};
-  CK(cudaLaunchCooperativeKernel((const void*)k_pcg_persistent_cg<K>, dim3(e.coop_blocks), dim3(PERSIST_THREADS),
-                                 args, 0, L.s));
+  const void* fn = two_barrier_form<K, double>() ? (const void*)k_pcg_persistent_cg<K>
+                                                 : (const void*)k_pcg_persistent<K>;
+  CK(cudaLaunchCooperativeKernel(fn, dim3(e.coop_blocks), dim3(PERSIST_THREADS), args, 0, L.s));
   CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
   std::vector<int> it(K);
   CK(cudaMemcpyAsync(it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost, L.s));
@@ -808,7 +940,9 @@ void ensure_single_precision_matrix(DeviceEngine& e) {
   e.L_val32.alloc(e.L_val.n);
   e.L_diag32.alloc(e.L_diag.n);
   e.L_dinv32.alloc(e.L_dinv.n);
+  e.L_vald32.alloc(e.L_vald.n);
   int g = grid_blocks();
+  k_to_float<<<g, THREADS, 0, e.stream>>>(e.L_vald.n, e.L_vald.p, e.L_vald32.p);
   k_to_float<<<g, THREADS, 0, e.stream>>>(e.L_val.n, e.L_val.p, e.L_val32.p);
   k_to_float<<<g, THREADS, 0, e.stream>>>(e.L_diag.n, e.L_diag.p, e.L_diag32.p);
   k_to_float<<<g, THREADS, 0, e.stream>>>(e.L_dinv.n, e.L_dinv.p, e.L_dinv32.p);
@@ -863,6 +997,8 @@ int pcg_run_mixed(DeviceEngine& e, BlockWork& w, Launch L, int iterations, Solve
     a.seg_begin = e.lap_seg.begin.p;
     a.seg_end = e.lap_seg.end.p;
     a.row_first = e.lap_seg.row_first.p;
+    a.seg_flag = e.lap_seg.row_flag.p;
+    a.vald = e.L_vald32.p;
     a.seg_buf = w.seg32.p;
     a.x = w.x32.p;
     a.r = w.r32.p;
@@ -873,7 +1009,9 @@ int pcg_run_mixed(DeviceEngine& e, BlockWork& w, Launch L, int iterations, Solve
     a.s = w.s_in;
     a.max_iters = iterations - done;
     void* args[] = {&a};
-    CK(cudaLaunchCooperativeKernel((const void*)k_pcg_persistent_cg<K, float>, dim3(e.coop_blocks),
+    const void* fn = two_barrier_form<K, float>() ? (const void*)k_pcg_persistent_cg<K, float>
+                                                  : (const void*)k_pcg_persistent<K, float>;
+    CK(cudaLaunchCooperativeKernel(fn, dim3(e.coop_blocks),
                                    dim3(PERSIST_THREADS), args, 0, L.s));
     std::vector<int> it(K);
     CK(cudaMemcpyAsync(it.data(), w.s_in.iters, K * sizeof(int), cudaMemcpyDeviceToHost, L.s));
@@ -1020,7 +1158,7 @@ int pcg_run_learned(DeviceEngine& e, BlockWork& w, Launch L, int iterations, Sol
     k_reactivate<K><<<1, 128, 0, L.s>>>(w.s);
     int saved = e.preconditioner;
     e.preconditioner = 1;
-    pcg_restart<K>(e, w, L, false);
+    pcg_restart<K>(e, w, L, false, !two_barrier_form<K, double>());
     mx = pcg_run<K>(e, w, L, std::max(1, iterations - mx));
     e.preconditioner = saved;
     tm.kernel_launches += 8;
@@ -1056,10 +1194,14 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
   BlockOutcome out;
   // hybrid RHS (Schur reduction of the worker block) and its column sums
   firm_gather<K, 1, 1>(e, w, L, e.cell_scale.p, w.bW.p, nullptr, 0.0, w.bF.p, w.bW.p, nullptr, w.b.p, e.partial.p);
-  k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 2 * K, w.tot.p);
+  finish(e.partial.p, L.grid, 2 * K, w.tot.p, L.s);
   k_pcg_init_state<K><<<1, 128, 0, L.s>>>(w.tot.p, ncols, o.pcg_tolerance, double(e.n), w.s);
-  pcg_restart<K>(e, w, L, true);
-  tm.kernel_launches += 9;
+  // the multigrid and learned forms and the three-barrier Jacobi kernel take
+  // p and r.z from the restart
+  const bool directions = e.preconditioner == 2 || e.preconditioner == 3 ||
+                          (o.precision != 1 && !two_barrier_form<K, double>());
+  pcg_restart<K>(e, w, L, true, directions);
+  tm.kernel_launches += directions ? 9 : 5;
 
   const double gate = std::max(10.0 * o.pcg_tolerance, 1e-11);
   double tol = o.pcg_tolerance;
@@ -1091,16 +1233,15 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
     if (bd >= 0) fail(PCG_CURVATURE_BREAKDOWN, "pcg", "nonpositive curvature in column " + std::to_string(bd));
 
     // extraction and complete residual
-    k_extract<K><<<L.grid, THREADS, 0, L.s>>>(e.W, e.F, e.worker_ptr.p, e.cell_firm.p, e.cell_weight.p,
-                                              e.worker_diag.p, e.kept_index.p, w.x.p, w.bW.p, w.alpha.p);
     double* pw = e.partial.p;
     double* pf = e.partial.p + size_t(L.grid) * 2 * K;
-    k_residual_workers<K><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, e.cell_firm.p, e.cell_weight.p,
-                                                       e.worker_diag.p, w.alpha.p, w.x.p, w.bW.p, pw);
+    k_extract_residual<K><<<L.grid, THREADS, 0, L.s>>>(e.W, e.F, e.worker_ptr.p, e.cell_firm.p, e.cell_weight.p,
+                                                       e.worker_diag.p, e.kept_index.p, w.x.p, w.bW.p, w.alpha.p,
+                                                       pw);
     firm_gather<K, 2, 2>(e, w, L, e.cell_weight.p, w.alpha.p, nullptr, 0.0, w.bF.p, nullptr, w.x.p, nullptr, pf);
-    k_finish<<<1, 1024, 0, L.s>>>(pw, L.grid, 2 * K, w.tot.p);
-    k_finish<<<1, 1024, 0, L.s>>>(pf, L.grid, 2 * K, w.tot.p + 2 * K);
-    tm.kernel_launches += 6;
+    finish(pw, L.grid, 2 * K, w.tot.p, L.s);
+    finish(pf, L.grid, 2 * K, w.tot.p + 2 * K, L.s);
+    tm.kernel_launches += 5;
     std::vector<double> tot(4 * K);
     CK(cudaMemcpyAsync(tot.data(), w.tot.p, 4 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaMemcpyAsync(h_rr.data(), w.s.rr, K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
@@ -1134,7 +1275,7 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
     for (int j = 0; j < K; ++j) tol2[j] = tol * tol * h_bb[j];
     CK(cudaMemcpyAsync(w.s.tol2, tol2.data(), K * sizeof(double), cudaMemcpyHostToDevice, L.s));
     CK(cudaMemcpyAsync(w.s.active, h_active.data(), K * sizeof(int), cudaMemcpyHostToDevice, L.s));
-    pcg_restart<K>(e, w, L, false);
+    pcg_restart<K>(e, w, L, false, directions);
   }
   out.block_iterations = total_iters;
   tm.pcg_iterations += total_iters;
@@ -1202,7 +1343,7 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
                                                        e.tgt_scale.p, key, first, np, w.dir.p);
     // direction totals: sum_c d and the reference scale sum_c |d| + |sum_c d|
     k_colsum_abs<H><<<L.grid, THREADS, 0, L.s>>>(e.C, w.dir.p, e.partial.p);
-    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 2 * H, w.tot.p);
+    finish(e.partial.p, L.grid, 2 * H, w.tot.p, L.s);
     CK(cudaMemcpyAsync(tot.data(), w.tot.p, 2 * H * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     k_target_scores<K><<<L.grid, THREADS, 0, L.s>>>(e.W, 0, e.worker_ptr.p, nullptr, w.dir.p, e.cell_target.p, invT,
                                                     w.tot.p, w.bW.p);
@@ -1210,9 +1351,9 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
     // balance repair (reference `balance_score_with_interrupt`, engine.rs:2812-2846):
     // the last worker / firm entry becomes minus the sum of the others
     k_colsum<K><<<L.grid, THREADS, 0, L.s>>>(e.W - 1, w.bW.p, e.partial.p);
-    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, K, w.tot.p + 2 * K);
+    finish(e.partial.p, L.grid, K, w.tot.p + 2 * K, L.s);
     k_colsum<K><<<L.grid, THREADS, 0, L.s>>>(e.F - 1, w.bF.p, e.partial.p);
-    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, K, w.tot.p + 3 * K);
+    finish(e.partial.p, L.grid, K, w.tot.p + 3 * K, L.s);
     std::vector<double> lastW(K), lastF(K), pre(2 * K);
     CK(cudaMemcpyAsync(pre.data(), w.tot.p + 2 * K, 2 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaMemcpyAsync(lastW.data(), w.bW.p + size_t(e.W - 1) * K, K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
@@ -1245,7 +1386,7 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
     if (!e.generic) {
       k_contract<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, e.omega.p, w.alpha.p, w.x.p,
                                                  e.partial.p);
-      k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 3 * K, w.tot.p);
+      finish(e.partial.p, L.grid, 3 * K, w.tot.p, L.s);
       CK(cudaMemcpyAsync(draws.data(), w.tot.p, 3 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
       CK(cudaStreamSynchronize(L.s));
       res.timings.kernel_launches += 2;
@@ -1256,7 +1397,7 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
       if (e.q > 0) {
         k_target_control_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.q, e.cell_worker.p, e.cell_firm.p,
                                                                e.cellQ.p, w.alpha.p, w.x.p, e.partial.p);
-        k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, QMAX * K, w.tot.p);
+        finish(e.partial.p, L.grid, QMAX * K, w.tot.p, L.s);
         CK(cudaMemcpyAsync(t.data(), w.tot.p, QMAX * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
         CK(cudaStreamSynchronize(L.s));
       }
@@ -1275,7 +1416,7 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
         k_generic_contract_units<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.q, e.unit_cell.p, e.cell_worker.p,
                                                                  e.cell_firm.p, e.unit_sums.p, e.beta_buf.p,
                                                                  w.alpha.p, w.x.p, e.partial.p);
-      k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 2 * K, w.tot.p);
+      finish(e.partial.p, L.grid, 2 * K, w.tot.p, L.s);
       std::vector<double> g2(2 * K);
       CK(cudaMemcpyAsync(g2.data(), w.tot.p, 2 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
       CK(cudaStreamSynchronize(L.s));
@@ -1357,7 +1498,7 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
     res.receipts.push_back(RhsReceipt{1, 1, -1, uint32_t(bo.iters[0]), uint32_t(bo.zero[0]), bo.reduced[0], bo.complete[0]});
     k_fit_cells<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p, e.cell_target.p,
                                              e.fitted.p, 0, nullptr, e.partial.p);
-    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 4, e.small.p);
+    finish(e.partial.p, L.grid, 4, e.small.p, L.s);
     std::vector<double> m(4);
     CK(cudaMemcpyAsync(m.data(), e.small.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
@@ -1367,7 +1508,7 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
     CK(cudaMemcpyAsync(e.small.p + 8, means, 2 * sizeof(double), cudaMemcpyHostToDevice, L.s));
     k_fit_cells<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p, e.cell_target.p,
                                              e.fitted.p, 1, e.small.p + 8, e.partial.p);
-    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 4, e.small.p);
+    finish(e.partial.p, L.grid, 4, e.small.p, L.s);
     CK(cudaMemcpyAsync(m.data(), e.small.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
     double T = p.target_total;
@@ -1504,7 +1645,7 @@ void setup_controls(DeviceEngine& e, const SolveOptions& o, SolveTimings& tm) {
   CK(cudaMemcpyAsync(e.psiH.p, w8.x.p, size_t(e.F) * QMAX * sizeof(double), cudaMemcpyDeviceToDevice, L.s));
   k_residualize<<<L.grid, THREADS, 0, L.s>>>(e.rows, q, e.row_cell.p, e.cell_worker.p, e.cell_firm.p, e.row_freq.p,
                                              e.Qd.p, e.alphaH.p, e.psiH.p, e.Rd.p, e.partial.p);
-  k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, QMAX * QMAX, e.small.p);
+  finish(e.partial.p, L.grid, QMAX * QMAX, e.small.p, L.s);
   std::vector<double> S8(QMAX * QMAX);
   CK(cudaMemcpyAsync(S8.data(), e.small.p, S8.size() * sizeof(double), cudaMemcpyDeviceToHost, L.s));
   CK(cudaStreamSynchronize(L.s));
@@ -1558,7 +1699,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     BlockOutcome bo = solve_block<1>(e, w, 1, o, res.timings);
     res.receipts.push_back(RhsReceipt{1, 1, -1, uint32_t(bo.iters[0]), uint32_t(bo.zero[0]), bo.reduced[0], bo.complete[0]});
     k_row_project<<<L.grid, THREADS, 0, L.s>>>(e.rows, q, e.row_freq.p, e.Rd.p, e.row_y.p, e.partial.p);
-    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, QMAX, e.small.p);
+    finish(e.partial.p, L.grid, QMAX, e.small.p, L.s);
     std::vector<double> ry(QMAX);
     CK(cudaMemcpyAsync(ry.data(), e.small.p, QMAX * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
@@ -1574,7 +1715,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
                                                 e.Qd.p, w.alpha.p, w.x.p, beta, e.residual.p);
     k_fit_cells<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p, e.cell_target.p,
                                              e.fitted.p, 0, nullptr, e.partial.p);
-    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 4, e.small.p);
+    finish(e.partial.p, L.grid, 4, e.small.p, L.s);
     std::vector<double> m(4);
     CK(cudaMemcpyAsync(m.data(), e.small.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
@@ -1582,7 +1723,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     CK(cudaMemcpyAsync(e.small.p + 8, means, 2 * sizeof(double), cudaMemcpyHostToDevice, L.s));
     k_fit_cells<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p, e.cell_target.p,
                                              e.fitted.p, 1, e.small.p + 8, e.partial.p);
-    k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 4, e.small.p);
+    finish(e.partial.p, L.grid, 4, e.small.p, L.s);
     CK(cudaMemcpyAsync(m.data(), e.small.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
     double T = p.target_total;
@@ -1777,6 +1918,7 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
   switch (kernel) {
     case 1:
     case 5:
+    case 6:
       // persistent PCG, per launch of `iters` iterations: matrix + segment
       // tables once per iteration, nine passes over n x K vectors (two-barrier
       // form: r gathered; r, p, A p, x read and written; three-barrier form:
@@ -1798,22 +1940,25 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
   }
   float total = 0.0f;
   for (int i = 0; i < launches; ++i) {
-    if (kernel == 1 || kernel == 5) {
+    if (kernel == 1 || kernel == 5 || kernel == 6) {
       // a fresh, never-converging block (tolerance 0) so every launch runs `iters` iterations
       k_fill_pattern<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p);
       k_colsum_abs<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p, e.partial.p);
-      k_finish<<<1, 1024, 0, L.s>>>(e.partial.p, L.grid, 2 * K, w.tot.p);
+      finish(e.partial.p, L.grid, 2 * K, w.tot.p, L.s);
       k_pcg_init_state<K><<<1, 128, 0, L.s>>>(w.tot.p, K, 0.0, double(e.n), w.s);
-      pcg_restart<K>(e, w, L, true);
+      pcg_restart<K>(e, w, L, true, kernel == 5);
     }
     CK(cudaMemsetAsync(flush.p, i & 0xff, flush.bytes(), L.s));
     CK(cudaEventRecord(e.ev0, L.s));
     switch (kernel) {
       case 1:
-      case 5: {
+      case 5:
+      case 6: {
         PersistentPcg<K> a = persistent_args<K>(e, w, iters);
         void* args[] = {&a};
-        const void* fn = kernel == 1 ? (const void*)k_pcg_persistent_cg<K> : (const void*)k_pcg_persistent<K>;
+        const void* fn = kernel == 1   ? (const void*)k_pcg_persistent_cg<K>
+                         : kernel == 5 ? (const void*)k_pcg_persistent<K>
+                                       : (const void*)k_pcg_persistent_cg<K, double, true>;
         CK(cudaLaunchCooperativeKernel(fn, dim3(e.coop_blocks), dim3(PERSIST_THREADS), args, 0, L.s));
         break;
       }
@@ -1841,7 +1986,7 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
   }
   CK_LAUNCH();
   *ms = double(total) / launches;
-  if (kernel == 1 || kernel == 5) {
+  if (kernel == 1 || kernel == 5 || kernel == 6) {
     // report the iterations actually executed (a curvature breakdown would stop early)
     std::vector<int> it(K);
     CK(cudaMemcpy(it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost));

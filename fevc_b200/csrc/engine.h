@@ -115,6 +115,10 @@ void device_atoms_noalloc(uint64_t seed, uint64_t tag, uint64_t first_probe, uin
                           const uint64_t* trials, uint64_t count, int64_t* out);
 
 int device_count();
+// Device allocations released by finished generations stay cached for the
+// next one (devmem.cu); the trim returns them to the driver (bytes freed).
+size_t device_cache_trim();
+size_t device_cache_bytes();
 // Network parameters used by preconditioner 3 (learned) for engines built afterwards.
 void set_learned_params(std::vector<float> params);
 void set_device_stream(void* stream);

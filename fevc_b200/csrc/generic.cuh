@@ -442,6 +442,50 @@ __global__ void k_generic_contract_units(uint32_t units, int q, const uint32_t* 
 #pragma unroll
   for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
   const int c0 = int(threadIdx.x % TPR) * CPT;
+  if constexpr (TPR == 32 && CPT == 2) {
+    // one warp per unit: the units' workers and firms are loaded 32 at a time
+    // lane-parallel and broadcast, beta sits in shared memory
+    __shared__ double sbeta[QMAX][K];
+    for (int t = threadIdx.x; t < QMAX * K; t += blockDim.x) sbeta[t / K][t % K] = t / K < q ? beta[t] : 0.0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const size_t nwarps = size_t(gridDim.x) * blockDim.x / 32;
+    for (size_t i0 = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32 * 32; i0 < units; i0 += nwarps * 32) {
+      const int cnt = int(units - i0 < 32 ? units - i0 : 32);
+      uint32_t my_w = 0, my_f = 0;
+      if (lane < cnt) {
+        uint32_t cell = unit_cell[i0 + lane];
+        my_w = cell_worker[cell];
+        my_f = cell_firm[cell];
+      }
+#pragma unroll 4
+      for (int u = 0; u < cnt; ++u) {
+        const uint32_t wk = __shfl_sync(0xffffffffu, my_w, u), fm = __shfl_sync(0xffffffffu, my_f, u);
+        const double* o = sums + (i0 + u) * size_t(2 * S);
+        double av[2], pv[2];
+        load_cols<K, double>(alpha, wk, c0, av);
+        load_cols<K, double>(psi, fm, c0, pv);
+        double first[2], second[2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          double ufe = av[c] + pv[c];
+          double f1 = ufe * o[0], s1 = ufe * o[S];
+          for (int k = 0; k < q; ++k) {
+            double bk = sbeta[k][c0 + c];
+            f1 += bk * o[1 + k];
+            s1 += bk * o[S + 1 + k];
+          }
+          first[c] = f1;
+          second[c] = s1;
+        }
+#pragma unroll
+        for (int c = 0; c < 2; ++c) v[0][c] += first[c] * second[c];
+        v[1][0] += (first[0] + first[1]) * (second[0] + second[1]);
+      }
+    }
+    block_reduce_cols<K, 2>(v, partial);
+    return;
+  }
   double bcol[QMAX][CPT];
 #pragma unroll
   for (int k = 0; k < QMAX; ++k)

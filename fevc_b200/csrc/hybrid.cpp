@@ -5,6 +5,7 @@
 #include <numeric>
 
 #include "common.h"
+#include "radix.h"
 
 namespace fevcb {
 
@@ -55,18 +56,20 @@ void build_hybrid(const Compressed& p, uint32_t max_degree, std::vector<uint32_t
         }
     }
   }
+  if (key.size() > 0xffffffffull) fail(RESOURCE_LIMIT, "operator", "hybrid Laplacian has too many entries");
   std::vector<uint32_t> order(key.size());
   std::iota(order.begin(), order.end(), 0u);
-  // duplicate conductances of one edge add in worker order, as the
-  // reference's edge map does (vckss-core/src/cmg_impl.rs.in:634-660)
-  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b] || (key[a] == key[b] && a < b); });
+  // entries ordered by (row, column); duplicate conductances of one edge keep
+  // their generation (worker) order and add in it, as the reference's edge
+  // map does (vckss-core/src/cmg_impl.rs.in:634-660): the radix sort is stable
+  radix_sort_pairs(key, order);
   Lptr.assign(n + 1, 0);
   Lcol.clear();
   Lval.clear();
   for (size_t i = 0; i < order.size();) {
-    uint64_t k = key[order[i]];
+    uint64_t k = key[i];
     double s = 0.0;
-    while (i < order.size() && key[order[i]] == k) s += val[order[i++]];
+    while (i < order.size() && key[i] == k) s += val[order[i++]];
     Lcol.push_back(uint32_t(k & 0xffffffffu));
     Lval.push_back(s);
     Lptr[(k >> 32) + 1]++;

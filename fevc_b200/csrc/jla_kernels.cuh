@@ -7,49 +7,20 @@
 
 namespace fevcb {
 
-// Worker solution from the hybrid solution x (firm part = psi):
-//   eliminated worker: alpha_w = (bW[w] - sum_{c in w} w_c psi_f(c)) / d_w
+// Worker solution from the hybrid solution x (firm part = psi) and the
+// complete residual of the worker rows, in one pass over each worker's cells:
+//   s_w = sum_{c in w} w_c psi_f(c)
+//   eliminated worker: alpha_w = (bW[w] - s_w) / d_w
 //   kept worker:       alpha_w = -x[F + kept_index[w]]
+//   r_W = (bW[w] - s_w) - d_w alpha_w   (rounding-level for eliminated workers)
 // Cells of a worker are contiguous: [worker_ptr[w], worker_ptr[w+1]).
+// partial[blk][0][K] = |r_W|^2, [1] = |bW|^2.
 template <int K>
-__global__ void k_extract(uint32_t W, uint32_t F, const uint32_t* __restrict__ worker_ptr,
-                          const uint32_t* __restrict__ cell_firm, const double* __restrict__ cell_weight,
-                          const double* __restrict__ worker_diag, const int32_t* __restrict__ kept_index,
-                          const double* __restrict__ x, const double* __restrict__ bW, double* __restrict__ alpha) {
-  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
-  size_t total = size_t(W) * TPR, stride = size_t(gridDim.x) * blockDim.x;
-  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
-    size_t w = t / TPR;
-    int c0 = int(t % TPR) * CPT;
-    int32_t k = kept_index[w];
-    if (k >= 0) {
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) alpha[w * K + c0 + c] = -x[(size_t(F) + k) * K + c0 + c];
-    } else {
-      double acc[CPT];
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) acc[c] = bW[w * K + c0 + c];
-      for (uint32_t i = worker_ptr[w]; i < worker_ptr[w + 1]; ++i) {
-        double a = cell_weight[i];
-        size_t fb = size_t(cell_firm[i]) * K + c0;
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) acc[c] -= a * x[fb + c];
-      }
-      double inv = 1.0 / worker_diag[w];
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) alpha[w * K + c0 + c] = acc[c] * inv;
-    }
-  }
-}
-
-// Complete residual, worker rows: r_W = bW - d_w alpha_w - sum_c w_c psi_f.
-// partial[blk][0][K] = |r_W|^2, [1] = |bW|^2
-template <int K>
-__global__ void k_residual_workers(uint32_t W, const uint32_t* __restrict__ worker_ptr,
+__global__ void k_extract_residual(uint32_t W, uint32_t F, const uint32_t* __restrict__ worker_ptr,
                                    const uint32_t* __restrict__ cell_firm, const double* __restrict__ cell_weight,
-                                   const double* __restrict__ worker_diag, const double* __restrict__ alpha,
-                                   const double* __restrict__ psi, const double* __restrict__ bW,
-                                   double* __restrict__ partial) {
+                                   const double* __restrict__ worker_diag, const int32_t* __restrict__ kept_index,
+                                   const double* __restrict__ x, const double* __restrict__ bW,
+                                   double* __restrict__ alpha, double* __restrict__ partial) {
   constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
   double v[2][CPT];
 #pragma unroll
@@ -57,63 +28,42 @@ __global__ void k_residual_workers(uint32_t W, const uint32_t* __restrict__ work
   size_t total = size_t(W) * TPR, stride = size_t(gridDim.x) * blockDim.x;
   for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
     size_t t = base + threadIdx.x;
+    // with one warp per worker (TPR = 32) the whole warp is live or not
     if (t < total) {
       size_t w = t / TPR;
       int c0 = int(t % TPR) * CPT;
-      double d = worker_diag[w];
-      double acc[CPT];
+      double acc[CPT], b[CPT];
 #pragma unroll
-      for (int c = 0; c < CPT; ++c) acc[c] = bW[w * K + c0 + c] - d * alpha[w * K + c0 + c];
-      for (uint32_t i = worker_ptr[w]; i < worker_ptr[w + 1]; ++i) {
-        double a = cell_weight[i];
-        size_t fb = size_t(cell_firm[i]) * K + c0;
+      for (int c = 0; c < CPT; ++c) acc[c] = b[c] = bW[w * K + c0 + c];
+      if constexpr (TPR == 32) {
+        // the worker's cells 32 at a time, loaded lane-parallel; acc -= w_c psi
+        const int lane = threadIdx.x & 31;
+        for (uint32_t i0 = worker_ptr[w], i1 = worker_ptr[w + 1]; i0 < i1; i0 += 32) {
+          uint32_t cnt = i1 - i0 < 32 ? i1 - i0 : 32, my_j = 0;
+          double my_a = 0.0;
+          if (uint32_t(lane) < cnt) {
+            my_j = cell_firm[i0 + lane];
+            my_a = -cell_weight[i0 + lane];
+          }
+          warp_gather<K, double>(my_j, my_a, cnt, x, c0, acc);
+        }
+      } else {
+        for (uint32_t i = worker_ptr[w]; i < worker_ptr[w + 1]; ++i) {
+          double a = cell_weight[i];
+          size_t fb = size_t(cell_firm[i]) * K + c0;
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) acc[c] -= a * psi[fb + c];
+          for (int c = 0; c < CPT; ++c) acc[c] -= a * x[fb + c];
+        }
       }
+      int32_t k = kept_index[w];
+      double d = worker_diag[w], inv = 1.0 / d;
 #pragma unroll
       for (int c = 0; c < CPT; ++c) {
-        double b = bW[w * K + c0 + c];
-        v[0][c] += acc[c] * acc[c];
-        v[1][c] += b * b;
-      }
-    }
-  }
-  block_reduce_cols<K, 2>(v, partial);
-}
-
-// Complete residual, firm rows: r_F = bF - d_f psi_f - sum_c w_c alpha_w.
-template <int K>
-__global__ void k_residual_firms(uint32_t F, const uint32_t* __restrict__ firm_ptr,
-                                 const uint32_t* __restrict__ firm_cells, const uint32_t* __restrict__ cell_worker,
-                                 const double* __restrict__ cell_weight, const double* __restrict__ firm_diag,
-                                 const double* __restrict__ alpha, const double* __restrict__ psi,
-                                 const double* __restrict__ bF, double* __restrict__ partial) {
-  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
-  double v[2][CPT];
-#pragma unroll
-  for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
-  size_t total = size_t(F) * TPR, stride = size_t(gridDim.x) * blockDim.x;
-  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
-    size_t t = base + threadIdx.x;
-    if (t < total) {
-      size_t f = t / TPR;
-      int c0 = int(t % TPR) * CPT;
-      double d = firm_diag[f];
-      double acc[CPT];
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) acc[c] = bF[f * K + c0 + c] - d * psi[f * K + c0 + c];
-      for (uint32_t i = firm_ptr[f]; i < firm_ptr[f + 1]; ++i) {
-        uint32_t cell = firm_cells[i];
-        double a = cell_weight[cell];
-        size_t wb = size_t(cell_worker[cell]) * K + c0;
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) acc[c] -= a * alpha[wb + c];
-      }
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) {
-        double b = bF[f * K + c0 + c];
-        v[0][c] += acc[c] * acc[c];
-        v[1][c] += b * b;
+        double al = k >= 0 ? -x[(size_t(F) + k) * K + c0 + c] : acc[c] * inv;
+        alpha[w * K + c0 + c] = al;
+        double r = acc[c] - d * al;
+        v[0][c] += r * r;
+        v[1][c] += b[c] * b[c];
       }
     }
   }
@@ -131,6 +81,56 @@ __global__ void k_moments(uint32_t units, int ncols, const uint32_t* __restrict_
                           const double* __restrict__ psi, const double* __restrict__ unit_atoms,
                           double* __restrict__ moments) {
   constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  if constexpr (TPR == 32) {
+    // one warp per unit: 32 units' cells, workers, firms and sqrt(n) loaded
+    // lane-parallel and broadcast, so a unit waits on its row loads only
+    const int lane = threadIdx.x & 31, c0 = lane * CPT;
+    const size_t nwarps = size_t(gridDim.x) * blockDim.x / 32;
+    for (size_t i0 = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32 * 32; i0 < units; i0 += nwarps * 32) {
+      const int cnt = int(units - i0 < 32 ? units - i0 : 32);
+      uint32_t my_w = 0, my_f = 0;
+      double my_rn = 1.0;
+      if (lane < cnt) {
+        uint32_t cell = unit_cell[i0 + lane];
+        my_w = cell_worker[cell];
+        my_f = cell_firm[cell];
+        my_rn = unit_sqrt_n[i0 + lane];
+      }
+#pragma unroll 2
+      for (int u = 0; u < cnt; ++u) {
+        const size_t g = i0 + size_t(u);
+        const uint32_t wk = __shfl_sync(0xffffffffu, my_w, u), fm = __shfl_sync(0xffffffffu, my_f, u);
+        const double rn = __shfl_sync(0xffffffffu, my_rn, u);
+        double av[CPT], pv[CPT], at[CPT];
+        load_cols<K, double>(alpha, wk, c0, av);
+        load_cols<K, double>(psi, fm, c0, pv);
+        load_cols<K, double>(unit_atoms, uint32_t(g), c0, at);
+        double sm[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          if (c0 + c < ncols) {
+            double p = rn * (av[c] + pv[c]);
+            double m = at[c] / rn - p;
+            double p2 = p * p, m2 = m * m;
+            sm[0] += p2;
+            sm[1] += m2;
+            sm[2] += p2 * p2;
+            sm[3] += m2 * m2;
+            sm[4] += p2 * m2;
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+#pragma unroll
+          for (int off = 1; off < 32; off <<= 1) sm[i] += __shfl_xor_sync(0xffffffffu, sm[i], off);
+        if (lane == 0) {
+#pragma unroll
+          for (int i = 0; i < 5; ++i) moments[g * 5 + i] += sm[i];
+        }
+      }
+    }
+    return;
+  }
   size_t total = size_t(units) * TPR, stride = size_t(gridDim.x) * blockDim.x;
   for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
     size_t t = base + threadIdx.x;

@@ -211,6 +211,58 @@ __global__ void k_spmm(uint32_t n, const uint32_t* __restrict__ ptr, const uint3
 
 // ---------------------------------------------------------------------------
 // Per-column PCG state, one array of K entries each.
+// Columns c0 .. c0+CPT-1 of vertex j of a vertex-interleaved block, as one
+// vector load where the width allows (c0 is a multiple of CPT).  The block is
+// rewritten between grid barriers, so these are plain coherent loads (no
+// read-only path, no __restrict__ on y).
+template <int K, typename V>
+__device__ __forceinline__ void load_cols(const V* y, uint32_t j, int c0, double (&out)[Cols<K>::CPT]) {
+  constexpr int CPT = Cols<K>::CPT;
+  const V* src = y + size_t(j) * K + c0;
+  if constexpr (CPT == 2 && sizeof(V) == 8) {
+    double2 v = *reinterpret_cast<const double2*>(src);
+    out[0] = v.x;
+    out[1] = v.y;
+  } else if constexpr (CPT == 2 && sizeof(V) == 4) {
+    float2 v = *reinterpret_cast<const float2*>(src);
+    out[0] = v.x;
+    out[1] = v.y;
+  } else {
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) out[c] = double(src[c]);
+  }
+}
+
+// acc[c] += sum_{i < cnt} a_i y[j_i][c0 + c] in item order, where lane i of the
+// warp holds (j_i, a_i); the whole warp calls it with the same cnt <= 32.
+template <int K, typename V>
+__device__ __forceinline__ void warp_gather(uint32_t my_j, double my_a, uint32_t cnt, const V* y, int c0,
+                                            double (&acc)[Cols<K>::CPT]) {
+  constexpr int CPT = Cols<K>::CPT;
+  // items in flight per lane: 16-byte loads four at a time, narrower ones eight
+  constexpr int U = (CPT * sizeof(V) >= 16) ? 4 : 8;
+  uint32_t i = 0;
+  for (; i + U <= cnt; i += U) {
+    double xv[U][CPT];
+#pragma unroll
+    for (int u = 0; u < U; ++u) load_cols<K, V>(y, __shfl_sync(0xffffffffu, my_j, int(i) + u), c0, xv[u]);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      double av = __shfl_sync(0xffffffffu, my_a, int(i) + u);
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) acc[c] += av * xv[u][c];
+    }
+  }
+  for (; i < cnt; ++i) {
+    uint32_t j = __shfl_sync(0xffffffffu, my_j, int(i));
+    double a = __shfl_sync(0xffffffffu, my_a, int(i));
+    double xv[CPT];
+    load_cols<K, V>(y, j, c0, xv);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) acc[c] += a * xv[c];
+  }
+}
+
 struct PcgState {
   double* rz;     // r.z of the current iterate
   double* rr;     // r.r

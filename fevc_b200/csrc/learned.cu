@@ -645,6 +645,7 @@ class Trainer final : public GnnTrainer {
     CK(cudaStreamSynchronize(s));
   }
   ~Trainer() override {
+    if (s) cudaStreamSynchronize(s);  // no queued work may touch the buffers released below
     graphs_.clear();
     if (s) cudaStreamDestroy(s);
   }

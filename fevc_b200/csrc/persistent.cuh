@@ -29,18 +29,23 @@ struct Segments {
   uint32_t count = 0;
   DBuf<uint32_t> row, begin, end;
   DBuf<uint32_t> row_first;  // first segment of each row (rows + 1 entries)
+  DBuf<uint32_t> row_flag;   // row | SEG_FIRST when the segment opens its row
 };
+
+constexpr uint32_t SEG_FIRST = 0x80000000u;
 
 // Cut every CSR row into segments of at most SEG items.
 inline void build_segments(const std::vector<uint32_t>& ptr, Segments& sg, cudaStream_t s, uint64_t& h2d) {
   size_t rows = ptr.size() - 1;
-  std::vector<uint32_t> row, begin, end, first(rows + 1, 0);
+  if (rows >= SEG_FIRST) fail(RESOURCE_LIMIT, "segments", "segmented CSR has too many rows");
+  std::vector<uint32_t> row, begin, end, flag, first(rows + 1, 0);
   for (size_t r = 0; r < rows; ++r) {
     first[r] = uint32_t(row.size());
     uint32_t b = ptr[r], e = ptr[r + 1];
     if (b == e) continue;
     for (uint32_t x = b; x < e; x += SEG) {
       row.push_back(uint32_t(r));
+      flag.push_back(uint32_t(r) | (x == b ? SEG_FIRST : 0u));
       begin.push_back(x);
       end.push_back(std::min(e, x + SEG));
     }
@@ -51,6 +56,7 @@ inline void build_segments(const std::vector<uint32_t>& ptr, Segments& sg, cudaS
   upload(sg.begin, begin, s, h2d);
   upload(sg.end, end, s, h2d);
   upload(sg.row_first, first, s, h2d);
+  upload(sg.row_flag, flag, s, h2d);
 }
 
 template <int K, int M>
@@ -121,38 +127,18 @@ struct PersistentPcg {
   const uint32_t* seg_begin;
   const uint32_t* seg_end;
   const uint32_t* row_first;  // first segment of each row
+  const uint32_t* seg_flag = nullptr;  // row | SEG_FIRST (the two-barrier kernel)
+  const V* vald = nullptr;             // val[e] * dinv[col[e]] (the two-barrier kernel)
   V* seg_buf;                 // [nseg][K] segment partial products
   V* x;
   V* r;
   V* p;
-  V* ap;              // A p (the two-barrier kernel only)
+  V* ap = nullptr;    // A p (the two-barrier kernel only)
   double* partial_a;  // [grid][1][K]; the two-barrier kernel: [2][grid][3][K]
   double* partial_b;  // [grid][2][K]
   PcgState s;
   int max_iters;
 };
-
-// Columns c0 .. c0+CPT-1 of vertex j of a vertex-interleaved block, as one
-// vector load where the width allows (c0 is a multiple of CPT).  The block is
-// rewritten between grid barriers, so these are plain coherent loads (no
-// read-only path, no __restrict__ on y).
-template <int K, typename V>
-__device__ __forceinline__ void load_cols(const V* y, uint32_t j, int c0, double (&out)[Cols<K>::CPT]) {
-  constexpr int CPT = Cols<K>::CPT;
-  const V* src = y + size_t(j) * K + c0;
-  if constexpr (CPT == 2 && sizeof(V) == 8) {
-    double2 v = *reinterpret_cast<const double2*>(src);
-    out[0] = v.x;
-    out[1] = v.y;
-  } else if constexpr (CPT == 2 && sizeof(V) == 4) {
-    float2 v = *reinterpret_cast<const float2*>(src);
-    out[0] = v.x;
-    out[1] = v.y;
-  } else {
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) out[c] = double(src[c]);
-  }
-}
 
 // acc[c] = sum_{i in [b, e)} val_i * (dinv[col_i] if SCALE) * y[col_i][c0 + c],
 // summed in item order.  When a warp holds one segment (TPR = 32) the warp
@@ -176,28 +162,7 @@ __device__ __forceinline__ void segment_gather(const uint32_t* __restrict__ col,
       my_a = double(__ldg(val + b + lane));
       if (SCALE) my_a *= double(__ldg(dinv + my_j));
     }
-    // items in flight per lane: 16-byte loads four at a time, narrower ones eight
-    constexpr int U = (CPT * sizeof(V) >= 16) ? 4 : 8;
-    uint32_t i = 0;
-    for (; i + U <= cnt; i += U) {
-      double xv[U][CPT];
-#pragma unroll
-      for (int u = 0; u < U; ++u) load_cols<K, V>(y, __shfl_sync(0xffffffffu, my_j, int(i) + u), c0, xv[u]);
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        double av = __shfl_sync(0xffffffffu, my_a, int(i) + u);
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) acc[c] += av * xv[u][c];
-      }
-    }
-    for (; i < cnt; ++i) {
-      uint32_t j = __shfl_sync(0xffffffffu, my_j, int(i));
-      double a = __shfl_sync(0xffffffffu, my_a, int(i));
-      double xv[CPT];
-      load_cols<K, V>(y, j, c0, xv);
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) acc[c] += a * xv[c];
-    }
+    warp_gather<K, V>(my_j, my_a, cnt, y, c0, acc);
   } else {
     for (uint32_t i = b; i < e; ++i) {
       uint32_t j = __ldg(col + i);
@@ -383,32 +348,197 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(Persisten
 // next ones written after it, so they alternate between two buffers.  The
 // first iteration of every launch starts from p = u (beta = 0); the iteration
 // count and the convergence test on r.r are those of the three-barrier form.
-template <int K, typename V>
+// Phase S.  With one warp per segment (TPR = 32) every warp owns a
+// contiguous run of segments: their (row, begin, end) are loaded lane-parallel
+// and broadcast, the next segment's columns and scaled values (A D^{-1}) are
+// loaded while the current segment's gathers are in flight, so a segment costs
+// about one memory latency instead of four dependent ones.
+template <int K, typename V, bool CONTIG>
 __device__ __forceinline__ void cg_products(const PersistentPcg<K, V>& a, size_t gid, size_t ngroups, int c0,
                                             double* partial, double (*sm)[1][K]) {
-  constexpr int CPT = Cols<K>::CPT;
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
   double v[1][CPT];
 #pragma unroll
   for (int c = 0; c < CPT; ++c) v[0][c] = 0.0;
-  for (size_t sg = gid; sg < a.nseg; sg += ngroups) {
-    uint32_t row = a.seg_row[sg], b = a.seg_begin[sg], e = a.seg_end[sg];
-    double acc[CPT];
-    segment_gather<K, V, true>(a.col, a.val, a.dinv, a.r, b, e, c0, acc);
-    double rr_[CPT];
-    load_cols<K, V>(a.r, row, c0, rr_);
-    double di = double(a.dinv[row]);
-    double d = (b == a.ptr[row]) ? double(a.diag[row]) : 0.0;
+  if constexpr (TPR == 32 && !CONTIG) {
+    // grid-strided segments (consecutive segments run side by side across the
+    // grid); scaled values and the row flag save the dinv and row-pointer loads
+    const int lane = threadIdx.x & 31;
+    for (size_t sg = gid; sg < a.nseg; sg += ngroups) {
+      const uint32_t flag = __ldg(a.seg_flag + sg), b = __ldg(a.seg_begin + sg), e = __ldg(a.seg_end + sg);
+      const uint32_t row = flag & ~SEG_FIRST;
+      uint32_t my_j = 0;
+      double my_a = 0.0;
+      if (uint32_t(lane) < e - b) {
+        my_j = __ldg(a.col + b + lane);
+        my_a = double(__ldg(a.vald + b + lane));
+      }
+      double rr_[CPT];
+      load_cols<K, V>(a.r, row, c0, rr_);
+      const double di = double(__ldg(a.dinv + row));
+      const double d = (flag & SEG_FIRST) ? double(__ldg(a.diag + row)) : 0.0;
+      double acc[CPT];
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-      a.seg_buf[sg * K + c0 + c] = V(acc[c]);
-      double u = di * rr_[c];
-      v[0][c] += u * (d * u - acc[c]);
+      for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
+      warp_gather<K, V>(my_j, my_a, e - b, a.r, c0, acc);
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        a.seg_buf[sg * K + c0 + c] = V(acc[c]);
+        double u = di * rr_[c];
+        v[0][c] += u * (d * u - acc[c]);
+      }
+    }
+  } else if constexpr (TPR == 32) {
+    const int lane = threadIdx.x & 31;
+    const size_t lo = gid * a.nseg / ngroups, hi = (gid + 1) * a.nseg / ngroups;
+    for (size_t base = lo; base < hi; base += 32) {
+      const int cnt = int(hi - base < 32 ? hi - base : 32);
+      uint32_t m_flag = 0, m_b = 0, m_e = 0;
+      if (lane < cnt) {
+        m_flag = __ldg(a.seg_flag + base + lane);
+        m_b = __ldg(a.seg_begin + base + lane);
+        m_e = __ldg(a.seg_end + base + lane);
+      }
+      uint32_t b = __shfl_sync(0xffffffffu, m_b, 0), e = __shfl_sync(0xffffffffu, m_e, 0);
+      uint32_t my_j = 0;
+      double my_a = 0.0;
+      if (uint32_t(lane) < e - b) {
+        my_j = __ldg(a.col + b + lane);
+        my_a = double(__ldg(a.vald + b + lane));
+      }
+      for (int k = 0; k < cnt; ++k) {
+        const uint32_t flag = __shfl_sync(0xffffffffu, m_flag, k);
+        const uint32_t row = flag & ~SEG_FIRST;
+        // the next segment's items, in flight during this segment's gathers
+        uint32_t nb = __shfl_sync(0xffffffffu, m_b, (k + 1) & 31), ne = __shfl_sync(0xffffffffu, m_e, (k + 1) & 31);
+        uint32_t nx_j = 0;
+        double nx_a = 0.0;
+        if (k + 1 < cnt && uint32_t(lane) < ne - nb) {
+          nx_j = __ldg(a.col + nb + lane);
+          nx_a = double(__ldg(a.vald + nb + lane));
+        }
+        double rr_[CPT];
+        load_cols<K, V>(a.r, row, c0, rr_);
+        const double di = double(__ldg(a.dinv + row));
+        const double d = (flag & SEG_FIRST) ? double(__ldg(a.diag + row)) : 0.0;
+        double acc[CPT];
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
+        warp_gather<K, V>(my_j, my_a, e - b, a.r, c0, acc);
+        const size_t sg = base + size_t(k);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          a.seg_buf[sg * K + c0 + c] = V(acc[c]);
+          double u = di * rr_[c];
+          v[0][c] += u * (d * u - acc[c]);
+        }
+        b = nb;
+        e = ne;
+        my_j = nx_j;
+        my_a = nx_a;
+      }
+    }
+  } else {
+    for (size_t sg = gid; sg < a.nseg; sg += ngroups) {
+      uint32_t row = a.seg_row[sg], b = a.seg_begin[sg], e = a.seg_end[sg];
+      double acc[CPT];
+      segment_gather<K, V, true>(a.col, a.val, a.dinv, a.r, b, e, c0, acc);
+      double rr_[CPT];
+      load_cols<K, V>(a.r, row, c0, rr_);
+      double di = double(a.dinv[row]);
+      double d = (b == a.ptr[row]) ? double(a.diag[row]) : 0.0;
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        a.seg_buf[sg * K + c0 + c] = V(acc[c]);
+        double u = di * rr_[c];
+        v[0][c] += u * (d * u - acc[c]);
+      }
     }
   }
   block_reduce_cols_big<K, 1>(v, partial, sm);
 }
 
-template <int K, typename V = double>
+// Phase F for one row: w = diag u - sum(segments); p = u + beta p,
+// s = w + beta s, x += alpha p, r -= alpha s; gamma and r.r of the new r.
+template <int K, typename V>
+__device__ __forceinline__ void cg_update_row(const PersistentPcg<K, V>& a, size_t row, uint32_t s0, uint32_t s1,
+                                              double dr, double di, int c0, bool carry, const double* s_alpha_it,
+                                              const double* s_beta, double (&w2)[2][Cols<K>::CPT]) {
+  constexpr int CPT = Cols<K>::CPT;
+  const size_t o = row * K + c0;
+  double wv[CPT], rv[CPT], pv[CPT], sv0[CPT], xv[CPT];
+  load_cols<K, V>(a.r, uint32_t(row), c0, rv);
+  load_cols<K, V>(a.x, uint32_t(row), c0, xv);
+  if (carry) {
+    // the first update of a launch reads no earlier p, s (never initialised)
+    load_cols<K, V>(a.p, uint32_t(row), c0, pv);
+    load_cols<K, V>(a.ap, uint32_t(row), c0, sv0);
+  }
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) wv[c] = dr * (di * rv[c]);
+  for (uint32_t sg = s0; sg < s1; ++sg) {
+    double sv[CPT];
+    load_cols<K, V>(a.seg_buf, sg, c0, sv);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) wv[c] -= sv[c];
+  }
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) {
+    double al = s_alpha_it[c0 + c], be = s_beta[c0 + c];
+    double pn = di * rv[c], sn = wv[c];
+    if (carry) {
+      pn += be * pv[c];
+      sn += be * sv0[c];
+    }
+    a.p[o + c] = V(pn);
+    a.ap[o + c] = V(sn);
+    a.x[o + c] = V(xv[c] + al * pn);
+    V rn = V(rv[c] - al * sn);
+    a.r[o + c] = rn;
+    double ri = double(rn);
+    w2[0][c] += ri * (di * ri);
+    w2[1][c] += ri * ri;
+  }
+}
+
+template <int K, typename V, bool CONTIG>
+__device__ __forceinline__ void cg_update(const PersistentPcg<K, V>& a, size_t gid, size_t ngroups, int c0,
+                                          bool carry, const double* s_alpha_it, const double* s_beta,
+                                          double* partial, double (*sm)[2][K]) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  double w2[2][CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) w2[0][c] = w2[1][c] = 0.0;
+  if constexpr (TPR == 32 && CONTIG) {
+    // a contiguous run of rows per warp; row scalars loaded lane-parallel
+    const int lane = threadIdx.x & 31;
+    const size_t lo = gid * a.n / ngroups, hi = (gid + 1) * a.n / ngroups;
+    for (size_t base = lo; base < hi; base += 32) {
+      const int cnt = int(hi - base < 32 ? hi - base : 32);
+      uint32_t m_s0 = 0, m_s1 = 0;
+      double m_dr = 0.0, m_di = 0.0;
+      if (lane < cnt) {
+        m_s0 = __ldg(a.row_first + base + lane);
+        m_s1 = __ldg(a.row_first + base + lane + 1);
+        m_dr = double(__ldg(a.diag + base + lane));
+        m_di = double(__ldg(a.dinv + base + lane));
+      }
+      for (int k = 0; k < cnt; ++k)
+        cg_update_row<K, V>(a, base + size_t(k), __shfl_sync(0xffffffffu, m_s0, k),
+                            __shfl_sync(0xffffffffu, m_s1, k), __shfl_sync(0xffffffffu, m_dr, k),
+                            __shfl_sync(0xffffffffu, m_di, k), c0, carry, s_alpha_it, s_beta, w2);
+    }
+  } else {
+    for (size_t row = gid; row < a.n; row += ngroups)
+      cg_update_row<K, V>(a, row, a.row_first[row], a.row_first[row + 1], double(a.diag[row]),
+                          double(a.dinv[row]), c0, carry, s_alpha_it, s_beta, w2);
+  }
+  block_reduce_cols_big<K, 2>(w2, partial, sm);
+}
+
+// CONTIG: every warp owns a contiguous run of segments and of rows (loaded
+// lane-parallel, next segment prefetched) instead of the grid-strided order.
+template <int K, typename V = double, bool CONTIG = false>
 __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent_cg(PersistentPcg<K, V> a) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
@@ -453,7 +583,7 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent_cg(Persis
       }
     }
     block_reduce_cols_big<K, 2>(w, base(0), (double(*)[2][K])s_red);
-    cg_products<K, V>(a, gid, ngroups, c0, base(0) + 2 * G * K, (double(*)[1][K])s_red);
+    cg_products<K, V, CONTIG>(a, gid, ngroups, c0, base(0) + 2 * G * K, (double(*)[1][K])s_red);
   }
   grid.sync();
 
@@ -498,48 +628,10 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent_cg(Persis
     par ^= 1;
 
     // ---- F: w = diag u - sum(segments); p, s, x, r; gamma and r.r of the new r
-    {
-      double w2[2][CPT];
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) w2[0][c] = w2[1][c] = 0.0;
-      for (size_t row = gid; row < a.n; row += ngroups) {
-        uint32_t s0 = a.row_first[row], s1 = a.row_first[row + 1];
-        double dr = double(a.diag[row]), di = double(a.dinv[row]);
-        size_t o = row * K + c0;
-        double wv[CPT], rv[CPT];
-        load_cols<K, V>(a.r, uint32_t(row), c0, rv);
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) wv[c] = dr * (di * rv[c]);
-        for (uint32_t sg = s0; sg < s1; ++sg) {
-          double sv[CPT];
-          load_cols<K, V>(a.seg_buf, sg, c0, sv);
-#pragma unroll
-          for (int c = 0; c < CPT; ++c) wv[c] -= sv[c];
-        }
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-          double al = s_fin[c0 + c], be = s_beta[c0 + c];
-          // the first update of a launch reads no earlier p, s (never initialised)
-          double pn = di * rv[c], sn = wv[c];
-          if (it > 0) {
-            pn += be * double(a.p[o + c]);
-            sn += be * double(a.ap[o + c]);
-          }
-          a.p[o + c] = V(pn);
-          a.ap[o + c] = V(sn);
-          a.x[o + c] = V(double(a.x[o + c]) + al * pn);
-          V rn = V(rv[c] - al * sn);
-          a.r[o + c] = rn;
-          double ri = double(rn);
-          w2[0][c] += ri * (di * ri);
-          w2[1][c] += ri * ri;
-        }
-      }
-      block_reduce_cols_big<K, 2>(w2, base(par), (double(*)[2][K])s_red);
-    }
+    cg_update<K, V, CONTIG>(a, gid, ngroups, c0, it > 0, s_fin, s_beta, base(par), (double(*)[2][K])s_red);
     grid.sync();
     // ---- S: products of the new u and delta
-    cg_products<K, V>(a, gid, ngroups, c0, base(par) + 2 * G * K, (double(*)[1][K])s_red);
+    cg_products<K, V, CONTIG>(a, gid, ngroups, c0, base(par) + 2 * G * K, (double(*)[1][K])s_red);
     grid.sync();
   }
   if (blockIdx.x == 0) {
@@ -811,12 +903,42 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent_poly(Pers
 //   op 1: sum of cell_scale[c] * bW[w(c)]          (Schur reduction of the worker block)
 //   op 2: sum of cell_weight[c] * alpha[w(c)]      (complete residual, firm rows)
 //   op 3: target firm scores: odd columns q=2j+1 sum d[c][j] - share_c * total[j]
+// With one warp per segment (TPR = 32) ops 0-2 load the segment's cells, their
+// coefficients and workers lane-parallel and gather by shuffle (warp_gather):
+// one index round trip per segment instead of one per cell; an op-1 cell with
+// a zero coefficient adds an exact zero.
 template <int K, int OP>
 __global__ void k_seg_firm(uint32_t nseg, const uint32_t* __restrict__ seg_begin, const uint32_t* __restrict__ seg_end,
                            const uint32_t* __restrict__ firm_cells, const uint32_t* __restrict__ cell_worker,
                            const double* __restrict__ coef, const double* __restrict__ src, const double* __restrict__ total,
                            double inv_total, double* __restrict__ seg_out) {
   constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR, H = K / 2;
+  if constexpr (TPR == 32 && OP <= 2) {
+    const int lane = threadIdx.x & 31, c0 = lane * CPT;
+    const size_t nwarps = size_t(gridDim.x) * blockDim.x / 32;
+    for (size_t sg = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; sg < nseg; sg += nwarps) {
+      const uint32_t b = seg_begin[sg], e = seg_end[sg];
+      uint32_t my_j = 0;
+      double my_a = 0.0;
+      if (uint32_t(lane) < e - b) {
+        uint32_t cell = firm_cells[b + lane];
+        if (OP == 0) {
+          my_j = cell;
+          my_a = 1.0;
+        } else {
+          my_a = coef[cell];
+          my_j = cell_worker[cell];
+        }
+      }
+      double acc[CPT];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
+      warp_gather<K, double>(my_j, my_a, e - b, src, c0, acc);
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) seg_out[sg * K + c0 + c] = acc[c];
+    }
+    return;
+  }
   size_t N = size_t(nseg) * TPR, stride = size_t(gridDim.x) * blockDim.x;
   for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < N; t += stride) {
     size_t sg = t / TPR;

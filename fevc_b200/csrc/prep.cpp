@@ -4,6 +4,8 @@
 // masks, dimensions, checksums and semantic ranks are bit-identical.
 #include "prep.h"
 
+#include "radix.h"
+
 #include <algorithm>
 #include <cstring>
 #include <numeric>
@@ -40,16 +42,42 @@ std::vector<double> copy_finite(const double* p, uint64_t rows, const char* labe
   return out;
 }
 
-// Reference `redense` (problem.rs:696-745): sorted distinct levels, dense ids.
+// Reference `redense` (problem.rs:696-745): sorted distinct levels, dense ids
+// (a level's id is its rank among the distinct values).  Identifiers that span
+// a range no wider than a few times the row count are relabelled through a
+// presence table over the range; wider ones are radix sorted.
 std::vector<uint32_t> redense(const std::vector<uint64_t>& values, std::vector<uint64_t>& levels, const char* label) {
-  levels = values;
-  std::sort(levels.begin(), levels.end());
-  levels.erase(std::unique(levels.begin(), levels.end()), levels.end());
+  size_t n = values.size();
+  if (n > 0xffffffffull) fail(RESOURCE_LIMIT, "canonicalize", "row count exceeds the u32 implementation limit");
+  levels.clear();
+  std::vector<uint32_t> dense(n);
+  if (n == 0) return dense;
+  uint64_t lo = values[0], hi = values[0];
+  for (uint64_t v : values) {
+    lo = std::min(lo, v);
+    hi = std::max(hi, v);
+  }
+  if (hi - lo < 4 * uint64_t(n) + 1024) {
+    std::vector<uint32_t> id(size_t(hi - lo) + 1, MISSING);
+    for (uint64_t v : values) id[v - lo] = 0;
+    for (size_t k = 0; k < id.size(); ++k)
+      if (id[k] != MISSING) {
+        id[k] = uint32_t(levels.size());
+        levels.push_back(lo + k);
+      }
+    for (size_t i = 0; i < n; ++i) dense[i] = id[values[i] - lo];
+  } else {
+    std::vector<uint64_t> key(values);
+    std::vector<uint32_t> row(n);
+    std::iota(row.begin(), row.end(), 0u);
+    radix_sort_pairs(key, row);
+    for (size_t i = 0; i < n; ++i) {
+      if (i == 0 || key[i] != key[i - 1]) levels.push_back(key[i]);
+      dense[row[i]] = uint32_t(levels.size() - 1);
+    }
+  }
   if (levels.size() > 0xffffffffull)
     fail(RESOURCE_LIMIT, "canonicalize", std::string(label) + " cardinality exceeds the u32 implementation limit");
-  std::vector<uint32_t> dense(values.size());
-  for (size_t i = 0; i < values.size(); ++i)
-    dense[i] = uint32_t(std::lower_bound(levels.begin(), levels.end(), values[i]) - levels.begin());
   return dense;
 }
 
@@ -61,24 +89,68 @@ void hash_word(uint64_t& h, uint64_t v) {
 }
 
 // Reference `topology_checksum` (problem.rs:1213-1248): FNV-1a over the sorted
-// (worker, firm, deletion, frequency) records, each word little-endian.
+// (worker, firm, deletion, frequency) records, each word little-endian.  A
+// deletion unit lies in one (worker, firm) coordinate, so the record order is
+// the units ordered by (worker, firm, unit) with each unit's rows ordered by
+// frequency; the units are radix sorted and the rows bucketed by unit.  When
+// the inputs break that property the records are sorted directly.
 uint64_t topology_checksum(const std::vector<uint32_t>& w, const std::vector<uint32_t>& f,
                            const std::vector<uint32_t>& d, const std::vector<uint64_t>& q) {
   size_t n = w.size();
-  std::vector<size_t> order(n);
-  std::iota(order.begin(), order.end(), size_t(0));
-  std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
-    if (w[a] != w[b]) return w[a] < w[b];
-    if (f[a] != f[b]) return f[a] < f[b];
-    if (d[a] != d[b]) return d[a] < d[b];
-    return q[a] < q[b];
-  });
   uint64_t h = 0xcbf29ce484222325ull;
-  for (size_t i : order) {
+  auto record = [&](size_t i) {
     hash_word(h, w[i]);
     hash_word(h, f[i]);
     hash_word(h, d[i]);
     hash_word(h, q[i]);
+  };
+  uint32_t units = 0;
+  for (uint32_t x : d) units = std::max(units, x + 1);
+  std::vector<uint32_t> uw(units, MISSING), uf(units, MISSING);
+  bool functional = true;
+  for (size_t i = 0; i < n && functional; ++i) {
+    uint32_t u = d[i];
+    if (uw[u] == MISSING) {
+      uw[u] = w[i];
+      uf[u] = f[i];
+    } else if (uw[u] != w[i] || uf[u] != f[i]) {
+      functional = false;
+    }
+  }
+  if (!functional) {
+    std::vector<size_t> order(n);
+    std::iota(order.begin(), order.end(), size_t(0));
+    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+      if (w[a] != w[b]) return w[a] < w[b];
+      if (f[a] != f[b]) return f[a] < f[b];
+      if (d[a] != d[b]) return d[a] < d[b];
+      return q[a] < q[b];
+    });
+    for (size_t i : order) record(i);
+    return h;
+  }
+  // units present, in (worker, firm, unit) order (LSD radix keeps unit order on ties)
+  std::vector<uint64_t> ukey;
+  std::vector<uint32_t> uid;
+  for (uint32_t u = 0; u < units; ++u)
+    if (uw[u] != MISSING) {
+      ukey.push_back((uint64_t(uw[u]) << 32) | uf[u]);
+      uid.push_back(u);
+    }
+  radix_sort_pairs(ukey, uid);
+  // rows bucketed by unit
+  std::vector<uint64_t> ptr(size_t(units) + 1, 0);
+  for (uint32_t x : d) ptr[x + 1]++;
+  for (uint32_t u = 0; u < units; ++u) ptr[u + 1] += ptr[u];
+  std::vector<uint32_t> rows(n);
+  {
+    std::vector<uint64_t> cur(ptr.begin(), ptr.end() - 1);
+    for (size_t i = 0; i < n; ++i) rows[cur[d[i]]++] = uint32_t(i);
+  }
+  for (uint32_t u : uid) {
+    auto b = rows.begin() + ptr[u], e = rows.begin() + ptr[u + 1];
+    if (e - b > 1) std::sort(b, e, [&](uint32_t a, uint32_t c) { return q[a] < q[c]; });
+    for (auto it = b; it != e; ++it) record(*it);
   }
   return h;
 }
@@ -124,20 +196,21 @@ void validate_mask(const Canonical& in, const std::vector<uint8_t>& active) {
   if (count_true(active) == 0) fail(GRAPH_EMPTY, "graph", "active graph is empty");
 }
 
-// Reference `coordinate_graph` (graph.rs:707-760): distinct active (worker, firm) pairs.
+// Reference `coordinate_graph` (graph.rs:707-760): distinct active (worker,
+// firm) pairs, in (worker, firm) order.  The distinct pairs of all rows are
+// indexed once at canonicalisation (Canonical::coord), so a mask selects its
+// edges with one pass over the rows.
 Graph coordinate_graph(const Canonical& in, const std::vector<uint8_t>& active) {
   validate_mask(in, active);
-  std::vector<uint64_t> keys;
-  keys.reserve(in.rows());
+  std::vector<uint8_t> used(in.coord_worker.size(), 0);
   for (size_t r = 0; r < in.rows(); ++r)
-    if (active[r]) keys.push_back((uint64_t(in.worker[r]) << 32) | in.firm[r]);
-  std::sort(keys.begin(), keys.end());
-  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
-  std::vector<uint32_t> eu(keys.size()), ev(keys.size());
-  for (size_t e = 0; e < keys.size(); ++e) {
-    eu[e] = uint32_t(keys[e] >> 32);
-    ev[e] = uint32_t(in.workers + (keys[e] & 0xffffffffu));
-  }
+    if (active[r]) used[in.coord[r]] = 1;
+  std::vector<uint32_t> eu, ev;
+  for (size_t c = 0; c < used.size(); ++c)
+    if (used[c]) {
+      eu.push_back(in.coord_worker[c]);
+      ev.push_back(uint32_t(in.workers + in.coord_firm[c]));
+    }
   return make_graph(in.workers + in.firms, eu, ev);
 }
 
@@ -428,6 +501,35 @@ Canonical canonicalize(InputColumns&& in, bool implicit_match) {
     }
   }
   c.topology_checksum = topology_checksum(c.worker, c.firm, c.deletion, in.frequency);
+  {
+    // distinct (worker, firm) coordinates in (worker, firm) order: rows
+    // bucketed by worker, each worker's rows ordered by firm
+    std::vector<uint64_t> ptr(c.workers + 1, 0);
+    for (uint32_t w : c.worker) ptr[w + 1]++;
+    for (size_t w = 0; w < c.workers; ++w) ptr[w + 1] += ptr[w];
+    std::vector<uint32_t> rows(n);
+    {
+      std::vector<uint64_t> cur(ptr.begin(), ptr.end() - 1);
+      for (size_t r = 0; r < n; ++r) rows[cur[c.worker[r]]++] = uint32_t(r);
+    }
+    c.coord.resize(n);
+    c.coord_worker.reserve(n);
+    c.coord_firm.reserve(n);
+    for (size_t w = 0; w < c.workers; ++w) {
+      auto b = rows.begin() + ptr[w], e = rows.begin() + ptr[w + 1];
+      if (e - b > 1) std::sort(b, e, [&](uint32_t x, uint32_t y) { return c.firm[x] < c.firm[y]; });
+      uint32_t last = MISSING;
+      for (auto it = b; it != e; ++it) {
+        uint32_t f = c.firm[*it];
+        if (f != last) {
+          c.coord_worker.push_back(uint32_t(w));
+          c.coord_firm.push_back(f);
+          last = f;
+        }
+        c.coord[*it] = uint32_t(c.coord_worker.size() - 1);
+      }
+    }
+  }
   c.outcome = std::move(in.outcome);
   c.frequency = std::move(in.frequency);
   c.target = std::move(in.target);
@@ -485,8 +587,7 @@ std::vector<uint8_t> select_match_graph(const Canonical& in, GraphReceipt& rc) {
       rc.degree_iterations++;
       rc.fixed_point_iterations++;
       continue;
-    }
-    auto art = worker_articulations(in, active);
+    } auto art = worker_articulations(in, active);
     size_t arts = count_true(art);
     if (arts) {
       for (size_t r = 0; r < in.rows(); ++r)
@@ -517,8 +618,7 @@ std::vector<uint8_t> select_match_graph(const Canonical& in, GraphReceipt& rc) {
   rc.maximum_components = std::max<uint64_t>(rc.maximum_components, fin.components);
   intersect(active, fin.keep);
   if (!deletion_bridges(in, active).empty())
-    fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained deletion-unit multigraph still contains a bridge");
-  if (count_true(worker_articulations(in, active)))
+    fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained deletion-unit multigraph still contains a bridge"); if (count_true(worker_articulations(in, active)))
     fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained graph still contains a worker articulation");
   {
     auto units = distinct_deletion_counts(in, active);
@@ -591,8 +691,7 @@ std::vector<uint8_t> select_observation_graph(const Canonical& in, GraphReceipt&
       rc.degree_iterations++;
       rc.fixed_point_iterations++;
       continue;
-    }
-    auto art = worker_articulations(in, active);
+    } auto art = worker_articulations(in, active);
     size_t arts = count_true(art);
     if (arts == 0) break;
     for (size_t r = 0; r < in.rows(); ++r)

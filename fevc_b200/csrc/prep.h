@@ -24,6 +24,9 @@ struct InputColumns {
 struct Canonical {
   std::vector<uint32_t> worker, firm, deletion;
   size_t workers = 0, firms = 0, deletion_units = 0;
+  // distinct (worker, firm) coordinates in (worker, firm) order and the
+  // coordinate of every row
+  std::vector<uint32_t> coord, coord_worker, coord_firm;
   std::vector<double> outcome, target;
   std::vector<uint64_t> frequency;
   std::vector<std::vector<double>> controls;

@@ -694,6 +694,10 @@ typedef struct FevcbSolveTimingsV1 {
 int32_t fevcb_device_count(void);
 /* Bind the CUDA stream (a cudaStream_t) used by generations prepared afterwards; NULL = library-owned stream. */
 int32_t fevcb_set_stream(void *stream);
+/* Device buffers of released generations stay cached (at most 16 GiB per
+ * device) for the next generation; this returns the current device's cached
+ * blocks to the driver.  Either pointer may be NULL. */
+int32_t fevcb_device_cache_trim_v1(uint64_t *freed_bytes, uint64_t *cached_bytes);
 int32_t fevcb_engine_solve_options_v1(uint64_t generation, const FevcbSolveOptionsV1 *options);
 int32_t fevcb_engine_timings_v1(uint64_t generation, FevcbSolveTimingsV1 *output, uint32_t output_capacity_bytes);
 /* Re-run the solve of a solved generation with the same request (device-resident inputs). */
