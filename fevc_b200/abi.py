@@ -348,6 +348,104 @@ SIGNATURES = {
                                              C.POINTER(i64)]),
 }
 
+# Reference entry points outside the replaced solve path: schema probes,
+# the session last-error alias and UNSUPPORTED_FEATURE returns (csrc/abi_unsupported.cpp).
+UNSUPPORTED_SIGNATURES = {
+    "vckss_rust_backend_request_capability_v1": (i32, [C.c_void_p, C.c_void_p, u32]),
+    "vckss_rust_backend_request_capability_v2": (i32, [C.c_void_p, C.c_void_p, u32]),
+    "vckss_rust_centering_schema_v1": (u32, []),
+    "vckss_rust_component_inference_interface_version": (u32, []),
+    "vckss_rust_engine_admit_prepare_memory_v1": (i32, [C.c_void_p, C.c_void_p, u32]),
+    "vckss_rust_engine_admit_prepare_probe_order_v1": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_admit_prepare_v2": (i32, [C.c_void_p]),
+    "vckss_rust_engine_admit_prepare_v3": (i32, [C.c_void_p]),
+    "vckss_rust_engine_admit_prepare_v4": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_augment_component_inference_interrupt_v1": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_augment_component_inference_interrupt_v2": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_augment_component_inference_interrupt_v3": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_augment_component_inference_interrupt_v4": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_augment_component_inference_interrupt_v5": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_augment_match_component_inference_interrupt_v1": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_augment_match_component_inference_interrupt_v2": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_augment_match_component_inference_interrupt_v3": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_augment_match_component_inference_interrupt_v4": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_augment_match_component_inference_interrupt_v5": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_augment_projection_interrupt_v1": (i32, [u64, C.c_void_p, C.c_void_p]),
+    "vckss_rust_engine_augment_stayers_interrupt_v1": (i32, [u64, C.c_void_p, C.c_void_p]),
+    "vckss_rust_engine_augment_stayers_v1": (i32, [u64, C.c_void_p, C.c_void_p]),
+    "vckss_rust_engine_component_batch_receipt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_component_inference_augmentation_receipt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_component_inference_result_v2": (i32, [u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u32]),
+    "vckss_rust_engine_component_inference_result_v3": (i32, [u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u32]),
+    "vckss_rust_engine_component_inference_result_v4": (i32, [u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u32]),
+    "vckss_rust_engine_component_inference_result_v5": (i32, [u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u32]),
+    "vckss_rust_engine_component_inference_unit_receipt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_component_inference_unit_receipt_v2": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_default_component_inference_augmentation_request_interrupt_v1": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_projection_augmentation_request_interrupt_v1": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_solve_request_interrupt_v2": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_solve_request_interrupt_v3": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_solve_request_interrupt_v4": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_solve_request_interrupt_v6": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_solve_request_interrupt_v7": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_solve_request_v6": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_default_stayer_augmentation_request_interrupt_v1": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_exact_execution_receipt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_execution_plan_receipt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_full_cmg_model_receipt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_generic_execution_receipt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_generic_execution_receipt_v2": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_leaveout_residual_diagnostic_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_memory_forecast_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_memory_policy_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_numerical_cmg_work_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_numerical_preflight_v1": (i32, [C.c_void_p]),
+    "vckss_rust_engine_numerical_preflight_v2": (i32, [C.c_void_p]),
+    "vckss_rust_engine_numerical_result_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_numerical_rhs_v1": (i32, [u64, C.c_void_p, u64, C.c_void_p]),
+    "vckss_rust_engine_performance_receipt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_prepare_interrupt_v3": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u32]),
+    "vckss_rust_engine_prepare_memory_interrupt_v1": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, u32]),
+    "vckss_rust_engine_projection_augmentation_receipt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_projection_result_receipt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_projection_result_v1": (i32, [u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u32]),
+    "vckss_rust_engine_repeat_measurement_diagnostic_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_repeat_measurement_leading_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_solve_exact_execution_interrupt_v1": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_exact_execution_v1": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_exact_legacy_execution_interrupt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_solve_exact_resolved_execution_interrupt_v2": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_exact_resolved_execution_v2": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_interrupt_v2": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_interrupt_v3": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_interrupt_v6": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_interrupt_v7": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_numerical_generic_legacy_v2": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_numerical_interrupt_v1": (i32, [u64, C.c_void_p, C.c_void_p, C.c_void_p, u32]),
+    "vckss_rust_engine_solve_numerical_interrupt_v2": (i32, [u64, C.c_void_p, C.c_void_p, C.c_void_p, u32]),
+    "vckss_rust_engine_solve_numerical_legacy_v2": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_numerical_v1": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_v2": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_v3": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_solve_v6": (i32, [u64, C.c_void_p]),
+    "vckss_rust_engine_stayer_augmentation_receipt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_stayer_hybrid_result_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_exact_execution_schema_v1": (u32, []),
+    "vckss_rust_exact_legacy_execution_schema_v1": (u32, []),
+    "vckss_rust_exact_resolved_execution_schema_v2": (u32, []),
+    "vckss_rust_numerical_schema_v1": (u32, []),
+    "vckss_rust_numerical_schema_v2": (u32, []),
+    "vckss_rust_projection_centering_schema_v1": (u32, []),
+    "vckss_rust_report_call_v1": (i32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "vckss_rust_session_clear_abandoned_v1": (i32, []),
+    "vckss_rust_session_last_error": (C.c_char_p, []),
+    "vckss_rust_session_preparation_receipt_v1": (i32, [u64, C.c_void_p]),
+    "vckss_rust_session_prepare_v1": (i32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "vckss_rust_session_release_v1": (i32, [u64]),
+    "vckss_rust_session_snapshot_v1": (i32, [C.c_void_p]),
+}
+SIGNATURES.update(UNSUPPORTED_SIGNATURES)
+
 def capability_signature_v3(req: SolveRequestV4, controls_count: int) -> int:
     """Request signature that V4+ solves must carry: FNV-1a over the request's
     capability fields (reference vckss-plugin/src/ffi_engine.rs:9492-9532,

@@ -491,6 +491,16 @@ void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr, bool generi
 
 }  // namespace
 
+namespace fevcb {
+// Reference entry points outside the replaced solve path (abi_unsupported.cpp).
+int32_t unsupported_entry(const char* name) {
+  return status([&] {
+    fail(UNSUPPORTED_FEATURE, "engine_ffi",
+         std::string(name) + " is outside the B200 engine's solve path and is not provided");
+  });
+}
+}  // namespace fevcb
+
 extern "C" {
 
 uint32_t vckss_rust_abi_version(void) { return VCKSS_RUST_ABI_VERSION_V1; }

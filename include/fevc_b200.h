@@ -845,6 +845,247 @@ int32_t fevcb_counter_atoms_v1(uint64_t seed, uint64_t domain_tag, uint64_t firs
 int32_t fevcb_counter_atoms_noalloc_v1(uint64_t seed, uint64_t domain_tag, uint64_t first_probe, uint32_t columns,
                                        const uint64_t *entity, const uint64_t *trials, uint64_t count, int64_t *out);
 
+
+/* ---------------------------------------------------------------------------
+ * The rest of the reference ABI (rust/stata_backend/include/vckss_rust.h).
+ * These entry points sit outside the solve path this library replaces: the
+ * schema probes report what is available (centering 1; numerical, exact
+ * execution, projection and component inference 0, i.e. absent), session
+ * last-error text is the engine's, and every other call returns
+ * VCKSS_UNSUPPORTED_FEATURE (11) with its name in the last-error text.
+ * Their argument structs are only passed through, so they are declared
+ * incomplete here. */
+typedef struct VckssColumnsV1 VckssColumnsV1;
+typedef struct VckssComponentBatchReceiptV1 VckssComponentBatchReceiptV1;
+typedef struct VckssComponentInferenceAugmentationReceiptV1 VckssComponentInferenceAugmentationReceiptV1;
+typedef struct VckssComponentInferenceAugmentationRequestInterruptV1 VckssComponentInferenceAugmentationRequestInterruptV1;
+typedef struct VckssComponentInferenceResultReceiptV2 VckssComponentInferenceResultReceiptV2;
+typedef struct VckssComponentInferenceResultReceiptV3 VckssComponentInferenceResultReceiptV3;
+typedef struct VckssComponentInferenceResultReceiptV4 VckssComponentInferenceResultReceiptV4;
+typedef struct VckssComponentInferenceResultReceiptV5 VckssComponentInferenceResultReceiptV5;
+typedef struct VckssComponentInferenceUnitReceiptV1 VckssComponentInferenceUnitReceiptV1;
+typedef struct VckssComponentInferenceUnitReceiptV2 VckssComponentInferenceUnitReceiptV2;
+typedef struct VckssEnginePerformanceReceiptV1 VckssEnginePerformanceReceiptV1;
+typedef struct VckssEngineSolveRequestInterruptV2 VckssEngineSolveRequestInterruptV2;
+typedef struct VckssEngineSolveRequestInterruptV3 VckssEngineSolveRequestInterruptV3;
+typedef struct VckssEngineSolveRequestInterruptV6 VckssEngineSolveRequestInterruptV6;
+typedef struct VckssEngineSolveRequestInterruptV7 VckssEngineSolveRequestInterruptV7;
+typedef struct VckssExactExecutionReceiptV1 VckssExactExecutionReceiptV1;
+typedef struct VckssExactExecutionRequestInterruptV1 VckssExactExecutionRequestInterruptV1;
+typedef struct VckssExactExecutionRequestV1 VckssExactExecutionRequestV1;
+typedef struct VckssExecutionPlanReceiptV1 VckssExecutionPlanReceiptV1;
+typedef struct VckssFullCmgModelReceiptV1 VckssFullCmgModelReceiptV1;
+typedef struct VckssGenericExecutionReceiptV1 VckssGenericExecutionReceiptV1;
+typedef struct VckssGenericExecutionReceiptV2 VckssGenericExecutionReceiptV2;
+typedef struct VckssLeaveoutResidualDiagnosticV1 VckssLeaveoutResidualDiagnosticV1;
+typedef struct VckssMemoryForecastV1 VckssMemoryForecastV1;
+typedef struct VckssMemoryPolicyV1 VckssMemoryPolicyV1;
+typedef struct VckssNumericalRequestV1 VckssNumericalRequestV1;
+typedef struct VckssNumericalRequestV2 VckssNumericalRequestV2;
+typedef struct VckssNumericalResultV1 VckssNumericalResultV1;
+typedef struct VckssNumericalRhsV1 VckssNumericalRhsV1;
+typedef struct VckssPreparationReceiptV1 VckssPreparationReceiptV1;
+typedef struct VckssPrepareRequestV1 VckssPrepareRequestV1;
+typedef int32_t (*VckssProgressOperationV1)(void *);
+typedef struct VckssProgressOptionsV1 VckssProgressOptionsV1;
+typedef struct VckssProjectionAugmentationReceiptV1 VckssProjectionAugmentationReceiptV1;
+typedef struct VckssProjectionAugmentationRequestInterruptV1 VckssProjectionAugmentationRequestInterruptV1;
+typedef struct VckssProjectionColumnsV1 VckssProjectionColumnsV1;
+typedef struct VckssProjectionResultReceiptV1 VckssProjectionResultReceiptV1;
+typedef struct VckssRepeatMeasurementDiagnosticV1 VckssRepeatMeasurementDiagnosticV1;
+typedef struct VckssRepeatMeasurementLeadingV1 VckssRepeatMeasurementLeadingV1;
+typedef struct VckssSessionSnapshotV1 VckssSessionSnapshotV1;
+typedef struct VckssStayerAugmentationColumnsV1 VckssStayerAugmentationColumnsV1;
+typedef struct VckssStayerAugmentationReceiptV1 VckssStayerAugmentationReceiptV1;
+typedef struct VckssStayerAugmentationRequestInterruptV1 VckssStayerAugmentationRequestInterruptV1;
+typedef struct VckssStayerAugmentationRequestV1 VckssStayerAugmentationRequestV1;
+typedef struct VckssStayerHybridResultV1 VckssStayerHybridResultV1;
+
+/* vckss_rust.h:1651 */
+int32_t vckss_rust_backend_request_capability_v1(const VckssBackendRequestCapabilityRequestV1 *request, VckssBackendRequestCapabilityReceiptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1656 */
+int32_t vckss_rust_backend_request_capability_v2(const VckssBackendRequestCapabilityRequestV2 *request, VckssBackendRequestCapabilityReceiptV2 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:12 */
+uint32_t vckss_rust_centering_schema_v1(void);
+/* vckss_rust.h:1864 */
+uint32_t vckss_rust_component_inference_interface_version(void);
+/* vckss_rust.h:2311 */
+int32_t vckss_rust_engine_admit_prepare_memory_v1(const VckssEnginePrepareRequestV4 *, const VckssMemoryPolicyV1 *, uint32_t);
+/* vckss_rust.h:1761 */
+int32_t vckss_rust_engine_admit_prepare_probe_order_v1(const VckssEnginePrepareRequestV3 *request, uint32_t probeorder_supplied);
+/* vckss_rust.h:1755 */
+int32_t vckss_rust_engine_admit_prepare_v2(const VckssEnginePrepareRequestV2 *request);
+/* vckss_rust.h:1758 */
+int32_t vckss_rust_engine_admit_prepare_v3(const VckssEnginePrepareRequestV3 *request);
+/* vckss_rust.h:1765 */
+int32_t vckss_rust_engine_admit_prepare_v4(const VckssEnginePrepareRequestV4 *request, uint32_t probeorder_supplied);
+/* vckss_rust.h:1830 */
+int32_t vckss_rust_engine_augment_component_inference_interrupt_v1(uint64_t generation, const VckssComponentInferenceAugmentationRequestInterruptV1 *request);
+/* vckss_rust.h:1865 */
+int32_t vckss_rust_engine_augment_component_inference_interrupt_v2(uint64_t generation, const VckssComponentInferenceAugmentationRequestInterruptV1 *request);
+/* vckss_rust.h:1874 */
+int32_t vckss_rust_engine_augment_component_inference_interrupt_v3(uint64_t generation, const VckssComponentInferenceAugmentationRequestInterruptV1 *request);
+/* vckss_rust.h:1883 */
+int32_t vckss_rust_engine_augment_component_inference_interrupt_v4(uint64_t generation, const VckssComponentInferenceAugmentationRequestInterruptV1 *request, uint32_t gram_probes);
+/* vckss_rust.h:1893 */
+int32_t vckss_rust_engine_augment_component_inference_interrupt_v5(uint64_t generation, const VckssComponentInferenceAugmentationRequestInterruptV1 *request, uint32_t gram_probes);
+/* vckss_rust.h:1834 */
+int32_t vckss_rust_engine_augment_match_component_inference_interrupt_v1(uint64_t generation, const VckssComponentInferenceAugmentationRequestInterruptV1 *request);
+/* vckss_rust.h:1869 */
+int32_t vckss_rust_engine_augment_match_component_inference_interrupt_v2(uint64_t generation, const VckssComponentInferenceAugmentationRequestInterruptV1 *request);
+/* vckss_rust.h:1878 */
+int32_t vckss_rust_engine_augment_match_component_inference_interrupt_v3(uint64_t generation, const VckssComponentInferenceAugmentationRequestInterruptV1 *request);
+/* vckss_rust.h:1888 */
+int32_t vckss_rust_engine_augment_match_component_inference_interrupt_v4(uint64_t generation, const VckssComponentInferenceAugmentationRequestInterruptV1 *request, uint32_t gram_probes);
+/* vckss_rust.h:1898 */
+int32_t vckss_rust_engine_augment_match_component_inference_interrupt_v5(uint64_t generation, const VckssComponentInferenceAugmentationRequestInterruptV1 *request, uint32_t gram_probes);
+/* vckss_rust.h:1820 */
+int32_t vckss_rust_engine_augment_projection_interrupt_v1(uint64_t generation, const VckssProjectionAugmentationRequestInterruptV1 *request, const VckssProjectionColumnsV1 *columns);
+/* vckss_rust.h:1810 */
+int32_t vckss_rust_engine_augment_stayers_interrupt_v1(uint64_t generation, const VckssStayerAugmentationRequestInterruptV1 *request, const VckssStayerAugmentationColumnsV1 *columns);
+/* vckss_rust.h:1805 */
+int32_t vckss_rust_engine_augment_stayers_v1(uint64_t generation, const VckssStayerAugmentationRequestV1 *request, const VckssStayerAugmentationColumnsV1 *columns);
+/* vckss_rust.h:1599 */
+int32_t vckss_rust_engine_component_batch_receipt_v1(uint64_t generation, VckssComponentBatchReceiptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1903 */
+int32_t vckss_rust_engine_component_inference_augmentation_receipt_v1(uint64_t generation, VckssComponentInferenceAugmentationReceiptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1999 */
+int32_t vckss_rust_engine_component_inference_result_v2(uint64_t generation, double *primitive_covariance, uint64_t primitive_covariance_capacity, double *covariance, uint64_t covariance_capacity, double *trace_mcse, uint64_t trace_mcse_capacity, double *spectrum, uint64_t spectrum_capacity, double *q1, uint64_t q1_capacity, double *variance_summary, uint64_t variance_summary_capacity, double *fold_diagnostics, uint64_t fold_diagnostics_capacity, double *cv_diagnostics, uint64_t cv_diagnostics_capacity, VckssComponentInferenceResultReceiptV2 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:2020 */
+int32_t vckss_rust_engine_component_inference_result_v3(uint64_t generation, double *primitive_covariance, uint64_t primitive_covariance_capacity, double *covariance, uint64_t covariance_capacity, double *trace_mcse, uint64_t trace_mcse_capacity, double *spectrum, uint64_t spectrum_capacity, double *q1, uint64_t q1_capacity, double *variance_summary, uint64_t variance_summary_capacity, double *fold_diagnostics, uint64_t fold_diagnostics_capacity, double *cv_diagnostics, uint64_t cv_diagnostics_capacity, VckssComponentInferenceResultReceiptV3 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:2041 */
+int32_t vckss_rust_engine_component_inference_result_v4(uint64_t generation, double *primitive_covariance, uint64_t primitive_covariance_capacity, double *covariance, uint64_t covariance_capacity, double *trace_mcse, uint64_t trace_mcse_capacity, double *spectrum, uint64_t spectrum_capacity, double *q1, uint64_t q1_capacity, double *variance_summary, uint64_t variance_summary_capacity, double *fold_diagnostics, uint64_t fold_diagnostics_capacity, double *cv_diagnostics, uint64_t cv_diagnostics_capacity, VckssComponentInferenceResultReceiptV4 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:2062 */
+int32_t vckss_rust_engine_component_inference_result_v5(uint64_t generation, double *primitive, uint64_t primitive_capacity, double *covariance, uint64_t covariance_capacity, double *mcse, uint64_t mcse_capacity, double *spectrum, uint64_t spectrum_capacity, double *q1, uint64_t q1_capacity, double *summaries, uint64_t summaries_capacity, double *folds, uint64_t folds_capacity, double *cv, uint64_t cv_capacity, double *targets, uint64_t targets_capacity, VckssComponentInferenceResultReceiptV5 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1838 */
+int32_t vckss_rust_engine_component_inference_unit_receipt_v1(uint64_t generation, VckssComponentInferenceUnitReceiptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1843 */
+int32_t vckss_rust_engine_component_inference_unit_receipt_v2(uint64_t generation, VckssComponentInferenceUnitReceiptV2 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1725 */
+int32_t vckss_rust_engine_default_component_inference_augmentation_request_interrupt_v1(VckssComponentInferenceAugmentationRequestInterruptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1721 */
+int32_t vckss_rust_engine_default_projection_augmentation_request_interrupt_v1(VckssProjectionAugmentationRequestInterruptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1733 */
+int32_t vckss_rust_engine_default_solve_request_interrupt_v2(VckssEngineSolveRequestInterruptV2 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1737 */
+int32_t vckss_rust_engine_default_solve_request_interrupt_v3(VckssEngineSolveRequestInterruptV3 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1741 */
+int32_t vckss_rust_engine_default_solve_request_interrupt_v4(VckssEngineSolveRequestInterruptV4 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1586 */
+int32_t vckss_rust_engine_default_solve_request_interrupt_v6(VckssEngineSolveRequestInterruptV6 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1595 */
+int32_t vckss_rust_engine_default_solve_request_interrupt_v7(VckssEngineSolveRequestInterruptV7 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1584 */
+int32_t vckss_rust_engine_default_solve_request_v6(VckssEngineSolveRequestV6 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1717 */
+int32_t vckss_rust_engine_default_stayer_augmentation_request_interrupt_v1(VckssStayerAugmentationRequestInterruptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:707 */
+int32_t vckss_rust_engine_exact_execution_receipt_v1(uint64_t generation, VckssExactExecutionReceiptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:2106 */
+int32_t vckss_rust_engine_execution_plan_receipt_v1(uint64_t generation, VckssExecutionPlanReceiptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1524 */
+int32_t vckss_rust_engine_full_cmg_model_receipt_v1(uint64_t generation, VckssFullCmgModelReceiptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1592 */
+int32_t vckss_rust_engine_generic_execution_receipt_v1(uint64_t generation, VckssGenericExecutionReceiptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1564 */
+int32_t vckss_rust_engine_generic_execution_receipt_v2(uint64_t, VckssGenericExecutionReceiptV2 *, uint32_t);
+/* vckss_rust.h:1848 */
+int32_t vckss_rust_engine_leaveout_residual_diagnostic_v1(uint64_t generation, VckssLeaveoutResidualDiagnosticV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:2332 */
+int32_t vckss_rust_engine_memory_forecast_v1(uint64_t, VckssMemoryForecastV1 *, uint32_t);
+/* vckss_rust.h:2316 */
+int32_t vckss_rust_engine_memory_policy_v1(uint64_t, VckssMemoryPolicyV1 *, uint32_t);
+/* vckss_rust.h:2381 */
+int32_t vckss_rust_engine_numerical_cmg_work_v1(uint64_t, VckssFullCmgModelReceiptV1 *, uint32_t);
+/* vckss_rust.h:2376 */
+int32_t vckss_rust_engine_numerical_preflight_v1(const VckssNumericalRequestV1 *);
+/* vckss_rust.h:2355 */
+int32_t vckss_rust_engine_numerical_preflight_v2(const VckssNumericalRequestV2 *);
+/* vckss_rust.h:2380 */
+int32_t vckss_rust_engine_numerical_result_v1(uint64_t, VckssNumericalResultV1 *, uint32_t);
+/* vckss_rust.h:2382 */
+int32_t vckss_rust_engine_numerical_rhs_v1(uint64_t, VckssNumericalRhsV1 *, uint64_t, uint64_t *);
+/* vckss_rust.h:2116 */
+int32_t vckss_rust_engine_performance_receipt_v1(uint64_t generation, VckssEnginePerformanceReceiptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1793 */
+int32_t vckss_rust_engine_prepare_interrupt_v3(const VckssEnginePrepareRequestInterruptV2 *request, const VckssEngineColumnsV3 *columns, uint64_t *output_handle, uint32_t output_capacity_bytes);
+/* vckss_rust.h:2313 */
+int32_t vckss_rust_engine_prepare_memory_interrupt_v1(const VckssEnginePrepareRequestInterruptV3 *, const VckssEngineColumnsV3 *, const VckssMemoryPolicyV1 *, uint64_t *, uint32_t);
+/* vckss_rust.h:1825 */
+int32_t vckss_rust_engine_projection_augmentation_receipt_v1(uint64_t generation, VckssProjectionAugmentationReceiptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1994 */
+int32_t vckss_rust_engine_projection_result_receipt_v1(uint64_t generation, VckssProjectionResultReceiptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1983 */
+int32_t vckss_rust_engine_projection_result_v1(uint64_t generation, double *coefficients, uint64_t coefficients_capacity, double *covariance, uint64_t covariance_capacity, double *naive_covariance, uint64_t naive_covariance_capacity, VckssProjectionResultReceiptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1853 */
+int32_t vckss_rust_engine_repeat_measurement_diagnostic_v1(uint64_t generation, VckssRepeatMeasurementDiagnosticV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1858 */
+int32_t vckss_rust_engine_repeat_measurement_leading_v1(uint64_t generation, VckssRepeatMeasurementLeadingV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:705 */
+int32_t vckss_rust_engine_solve_exact_execution_interrupt_v1(uint64_t generation, const VckssExactExecutionRequestInterruptV1 *request);
+/* vckss_rust.h:703 */
+int32_t vckss_rust_engine_solve_exact_execution_v1(uint64_t generation, const VckssExactExecutionRequestV1 *request);
+/* vckss_rust.h:693 */
+int32_t vckss_rust_engine_solve_exact_legacy_execution_interrupt_v1(uint64_t generation, const VckssEngineSolveRequestInterruptV2 *request, uint32_t threads);
+/* vckss_rust.h:701 */
+int32_t vckss_rust_engine_solve_exact_resolved_execution_interrupt_v2(uint64_t generation, const VckssExactExecutionRequestInterruptV1 *request);
+/* vckss_rust.h:699 */
+int32_t vckss_rust_engine_solve_exact_resolved_execution_v2(uint64_t generation, const VckssExactExecutionRequestV1 *request);
+/* vckss_rust.h:1957 */
+int32_t vckss_rust_engine_solve_interrupt_v2(uint64_t generation, const VckssEngineSolveRequestInterruptV2 *request);
+/* vckss_rust.h:1961 */
+int32_t vckss_rust_engine_solve_interrupt_v3(uint64_t generation, const VckssEngineSolveRequestInterruptV3 *request);
+/* vckss_rust.h:1590 */
+int32_t vckss_rust_engine_solve_interrupt_v6(uint64_t generation, const VckssEngineSolveRequestInterruptV6 *request);
+/* vckss_rust.h:1597 */
+int32_t vckss_rust_engine_solve_interrupt_v7(uint64_t generation, const VckssEngineSolveRequestInterruptV7 *request);
+/* vckss_rust.h:2352 */
+int32_t vckss_rust_engine_solve_numerical_generic_legacy_v2(uint64_t generation, const VckssEngineSolveRequestInterruptV3 *request);
+/* vckss_rust.h:2378 */
+int32_t vckss_rust_engine_solve_numerical_interrupt_v1(uint64_t, const VckssNumericalRequestV1 *, VckssInterruptPollV1, void *, uint32_t);
+/* vckss_rust.h:2356 */
+int32_t vckss_rust_engine_solve_numerical_interrupt_v2(uint64_t, const VckssNumericalRequestV2 *, VckssInterruptPollV1, void *, uint32_t);
+/* vckss_rust.h:2350 */
+int32_t vckss_rust_engine_solve_numerical_legacy_v2(uint64_t generation, const VckssEngineSolveRequestInterruptV2 *request);
+/* vckss_rust.h:2377 */
+int32_t vckss_rust_engine_solve_numerical_v1(uint64_t, const VckssNumericalRequestV1 *);
+/* vckss_rust.h:1937 */
+int32_t vckss_rust_engine_solve_v2(uint64_t generation, const VckssEngineSolveRequestV2 *request);
+/* vckss_rust.h:1941 */
+int32_t vckss_rust_engine_solve_v3(uint64_t generation, const VckssEngineSolveRequestV3 *request);
+/* vckss_rust.h:1588 */
+int32_t vckss_rust_engine_solve_v6(uint64_t generation, const VckssEngineSolveRequestV6 *request);
+/* vckss_rust.h:1815 */
+int32_t vckss_rust_engine_stayer_augmentation_receipt_v1(uint64_t generation, VckssStayerAugmentationReceiptV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:1978 */
+int32_t vckss_rust_engine_stayer_hybrid_result_v1(uint64_t generation, VckssStayerHybridResultV1 *output, uint32_t output_capacity_bytes);
+/* vckss_rust.h:691 */
+uint32_t vckss_rust_exact_execution_schema_v1(void);
+/* vckss_rust.h:692 */
+uint32_t vckss_rust_exact_legacy_execution_schema_v1(void);
+/* vckss_rust.h:698 */
+uint32_t vckss_rust_exact_resolved_execution_schema_v2(void);
+/* vckss_rust.h:2375 */
+uint32_t vckss_rust_numerical_schema_v1(void);
+/* vckss_rust.h:2348 */
+uint32_t vckss_rust_numerical_schema_v2(void);
+/* vckss_rust.h:13 */
+uint32_t vckss_rust_projection_centering_schema_v1(void);
+/* vckss_rust.h:316 */
+int32_t vckss_rust_report_call_v1(const VckssProgressOptionsV1 *, VckssProgressOperationV1, void *);
+/* vckss_rust.h:1677 */
+int32_t vckss_rust_session_clear_abandoned_v1(void);
+/* vckss_rust.h:1679 */
+const char *vckss_rust_session_last_error(void);
+/* vckss_rust.h:1672 */
+int32_t vckss_rust_session_preparation_receipt_v1(uint64_t generation, VckssPreparationReceiptV1 *output);
+/* vckss_rust.h:1667 */
+int32_t vckss_rust_session_prepare_v1(const VckssPrepareRequestV1 *request, const VckssColumnsV1 *columns, uint64_t *output_handle);
+/* vckss_rust.h:1676 */
+int32_t vckss_rust_session_release_v1(uint64_t generation);
+/* vckss_rust.h:1678 */
+int32_t vckss_rust_session_snapshot_v1(VckssSessionSnapshotV1 *output);
+
 #ifdef __cplusplus
 }
 #endif

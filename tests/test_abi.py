@@ -249,3 +249,23 @@ def test_v4_solve_refuses_an_unreconciled_request(lib):
             msg = L.vckss_rust_engine_last_error().decode()
             e.release()
             assert st == 11 and ("reconcile" in msg or "capability profile" in msg), (L, mutate, st, msg)
+
+
+def test_entry_points_outside_the_solve_path(lib):
+    """Every other reference entry point exists: schema probes report what is
+    available and the rest return UNSUPPORTED_FEATURE naming the call."""
+    assert lib.vckss_rust_centering_schema_v1() == 1
+    for probe in ("numerical_schema_v1", "numerical_schema_v2", "exact_execution_schema_v1",
+                  "exact_legacy_execution_schema_v1", "exact_resolved_execution_schema_v2",
+                  "projection_centering_schema_v1", "component_inference_interface_version"):
+        assert getattr(lib, "vckss_rust_" + probe)() == 0, probe
+    called = 0
+    for name, (res, args) in abi.UNSUPPORTED_SIGNATURES.items():
+        if res is not abi.i32:
+            continue
+        zeros = [None if a is C.c_void_p else 0 for a in args]
+        assert getattr(lib, name)(*zeros) == 11, name
+        assert name[len("vckss_rust_"):].encode() in lib.vckss_rust_engine_last_error(), name
+        assert lib.vckss_rust_session_last_error() == lib.vckss_rust_engine_last_error()
+        called += 1
+    assert called >= 80
