@@ -219,6 +219,199 @@ TAG_LEVERAGE = 0x4C45564552414745
 TAG_TARGET = 0x0054415247455401
 
 # Every entry point the header declares, with its ctypes signature.
+# Detailed receipts V1-V7 (vckss_rust.h:1084-1439); layouts as in include/fevc_b200.h.
+
+
+class EngineDetailedReceiptV1(Struct):
+    _fields_ = [
+        ("struct_size", u32), ("reserved", u32), ("generation", u64), ("seed", u64), ("probes_requested", u32),
+        ("leverage_probes_accepted", u32), ("target_probes_accepted", u32), ("solver_requested", u32),
+        ("solver_selected", u32), ("solver_fallback", u32), ("solver_fallback_error", i32),
+        ("solver_dimension", u64), ("leverage_batch_width", u64), ("target_batch_width", u64),
+        ("rank_tolerance", f64), ("block_tolerance", f64), ("full_residual_tolerance", f64),
+        ("full_fit_route", u32), ("full_fit_iterations", u32), ("full_fit_reduced_residual", f64),
+        ("full_fit_complete_residual", f64), ("full_fit_zero_rhs", u32), ("reserved_1", u32),
+        ("leverage_rhs_count", u64), ("target_rhs_count", u64), ("max_reduced_residual", f64),
+        ("max_complete_residual", f64), ("max_leverage", f64), ("max_reciprocal_residual", f64),
+        ("accounting_residual", f64), ("topology_checksum", u64), ("cmg_levels", u64), ("cmg_fine_vertices", u64),
+        ("cmg_fine_edges", u64), ("cmg_terminal_vertices", u64), ("cmg_edge_complexity", f64),
+        ("cmg_vertex_complexity", f64), ("cmg_structural_bytes", u64), ("cmg_workspace_bytes", u64),
+        ("cmg_dense_factor_bytes", u64)
+    ]
+
+
+class EngineDetailedReceiptV2(Struct):
+    _fields_ = [
+        ("struct_size", u32), ("reserved", u32), ("generation", u64), ("seed", u64), ("probes_requested", u32),
+        ("leverage_probes_accepted", u32), ("target_probes_accepted", u32), ("solver_requested", u32),
+        ("solver_selected", u32), ("solver_fallback", u32), ("solver_fallback_error", i32),
+        ("solver_dimension", u64), ("leverage_batch_width", u64), ("target_batch_width", u64),
+        ("rank_tolerance", f64), ("block_tolerance", f64), ("full_residual_tolerance", f64),
+        ("full_fit_route", u32), ("full_fit_iterations", u32), ("full_fit_reduced_residual", f64),
+        ("full_fit_complete_residual", f64), ("full_fit_zero_rhs", u32), ("reserved_1", u32),
+        ("leverage_rhs_count", u64), ("target_rhs_count", u64), ("max_reduced_residual", f64),
+        ("max_complete_residual", f64), ("max_leverage", f64), ("max_reciprocal_residual", f64),
+        ("accounting_residual", f64), ("topology_checksum", u64), ("cmg_levels", u64), ("cmg_fine_vertices", u64),
+        ("cmg_fine_edges", u64), ("cmg_terminal_vertices", u64), ("cmg_edge_complexity", f64),
+        ("cmg_vertex_complexity", f64), ("cmg_structural_bytes", u64), ("cmg_workspace_bytes", u64),
+        ("cmg_dense_factor_bytes", u64), ("full_fit_weighted_rss", f64), ("memory_limit_bytes", u64),
+        ("caller_copy_bytes", u64), ("preparation_peak_forecast_bytes", u64), ("prepared_resident_bytes", u64),
+        ("solver_setup_forecast_bytes", u64), ("leverage_phase_forecast_bytes", u64),
+        ("target_phase_forecast_bytes", u64), ("result_forecast_bytes", u64), ("solve_peak_forecast_bytes", u64),
+        ("command_peak_forecast_bytes", u64)
+    ]
+
+
+class EngineDetailedReceiptV3(Struct):
+    _fields_ = [
+        ("v2", EngineDetailedReceiptV2), ("rng_contract", u32), ("reserved_2", u32), ("rhs_receipt_rows", u64),
+        ("caller_result_copy_bytes", u64)
+    ]
+
+
+class EngineDetailedReceiptV4(Struct):
+    _fields_ = [
+        ("v3", EngineDetailedReceiptV3), ("algorithm_requested", u32), ("algorithm_selected", u32),
+        ("deletion_mode", u32), ("nuisance_mode", u32), ("parameters", u64), ("full_parameters", u64),
+        ("correction_parameters", u64), ("information_rcond", f64), ("inverse_relres", f64),
+        ("exact_peak_forecast_bytes", u64)
+    ]
+
+
+class EngineDetailedReceiptV5(Struct):
+    _fields_ = [
+        ("v4", EngineDetailedReceiptV4), ("applicability_flags", u64), ("working_fit_complete_residual", f64),
+        ("inverse_sqrt_relres", f64), ("maker_relres", f64), ("control_basis_relres", f64),
+        ("control_basis_forward_error", f64), ("deletion_rank_gap", f64), ("firm_zero_sum_residual", f64),
+        ("fit_peak_forecast_bytes", u64), ("correction_peak_forecast_bytes", u64),
+        ("actual_accounting_residual", f64)
+    ]
+
+
+class EngineDetailedReceiptV6(Struct):
+    _fields_ = [
+        ("v5", EngineDetailedReceiptV5), ("engine_requested", u32), ("engine_selected", u32),
+        ("generic_applicability_flags", u64), ("controls_count", u32), ("rhs_receipt_schema", u32),
+        ("control_projection_rhs_count", u64), ("control_rank_rcond", f64),
+        ("control_rank_smallest_generalized_eigenvalue_lower", f64),
+        ("control_rank_largest_generalized_eigenvalue_upper", f64), ("control_rank_projection_error_bound", f64),
+        ("control_rank_normalization_error_bound", f64),
+        ("control_rank_fe_information_eigenvalue_lower_bound", f64),
+        ("control_rank_maximum_projection_residual", f64), ("control_rank_effective_tolerance", f64),
+        ("control_rank_projection_pcg_tolerance", f64), ("control_rank_projection_residual_gate", f64),
+        ("generic_control_basis_relres", f64), ("generic_control_basis_forward_error", f64),
+        ("generic_control_schur_rcond", f64), ("generic_control_schur_relres", f64),
+        ("generic_deletion_rank_gap", f64), ("full_joint_fit_complete_residual", f64),
+        ("generic_working_fit_complete_residual", f64), ("generic_maker_relres", f64),
+        ("canonicalization_peak_forecast_bytes", u64), ("generic_fit_peak_forecast_bytes", u64),
+        ("geometry_peak_forecast_bytes", u64), ("generic_leverage_peak_forecast_bytes", u64),
+        ("generic_target_peak_forecast_bytes", u64), ("maker_peak_forecast_bytes", u64),
+        ("generic_result_forecast_bytes", u64), ("generic_peak_forecast_bytes", u64),
+        ("rhs_v2_caller_copy_bytes", u64), ("capability_schema", u32), ("capability_profile", u32),
+        ("batch_mode", u32), ("stayers_mode", u32), ("target_weight_mode", u32), ("deletion_unit_source", u32),
+        ("probeorder_supplied", u32), ("wallseconds_supplied", u32), ("frequency_use", u32), ("reserved_6", u32),
+        ("physical_limit", u64), ("request_signature", u64)
+    ]
+
+
+class EstimatorResolutionReceiptV1(Struct):
+    _fields_ = [
+        ("algorithm_schema", u32), ("algorithm_requested", u32), ("algorithm_selected", u32),
+        ("algorithm_reason", u32), ("engine_schema", u32), ("engine_requested", u32), ("engine_selected", u32),
+        ("engine_reason", u32), ("compressed_eligibility", u32), ("resolved_before_rng", u32),
+        ("opportunistic_engine_fallback_allowed", u32), ("reserved", u32), ("identified_complexity", u64),
+        ("exact_limit", u64), ("rng_draws_before_resolution", u64), ("counter_atoms_before_resolution", u64)
+    ]
+
+
+class SolverExecutionReceiptV1(Struct):
+    _fields_ = [
+        ("schema_version", u32), ("requested_route", u32), ("selected_route", u32), ("fallback_used", u32),
+        ("fallback_error", i32), ("full_setup_complete", u32), ("fe_setup_complete", u32),
+        ("fe_hierarchy_reused", u32), ("plan_frozen_before_rng", u32), ("auto_route_contract", u32),
+        ("threads_requested", u32), ("threads_used", u32), ("parallel_regions", u32), ("applicability", u32),
+        ("reserved_1", u32), ("reserved_2", u32), ("planned_rhs", u64), ("auto_firm_threshold", u64),
+        ("auto_rhs_threshold", u64), ("full_solver_dimension", u64), ("fe_solver_dimension", u64),
+        ("logical_atoms_before_plan_freeze", u64), ("unique_words_before_plan_freeze", u64),
+        ("physical_trials_before_plan_freeze", u64)
+    ]
+
+
+class BatchPhasePlanReceiptV1(Struct):
+    _fields_ = [
+        ("request_mode", u32), ("selection_reason", u32), ("applicability", u32), ("reserved", u32),
+        ("requested_width", u64), ("selected_width", u64), ("probe_width_cap", u64), ("declared_threads", u64),
+        ("thread_width_cap", u64), ("route_width_cap", u64), ("effective_width_cap", u64),
+        ("hard_memory_bytes", u64), ("width_one_forecast_bytes", u64), ("selected_forecast_bytes", u64)
+    ]
+
+
+class BatchExecutionReceiptV1(Struct):
+    _fields_ = [
+        ("schema_version", u32), ("deterministic", u32), ("width_invariance_required", u32),
+        ("arithmetic_contract", u32), ("whole_command_admitted", u32), ("applicability", u32),
+        ("non_batched_peak_bytes", u64), ("selected_command_peak_bytes", u64),
+        ("leverage", BatchPhasePlanReceiptV1), ("target", BatchPhasePlanReceiptV1)
+    ]
+
+
+class WallExecutionReceiptV1(Struct):
+    _fields_ = [
+        ("schema_version", u32), ("model_code", u32), ("status", u32), ("routing_effect", u32),
+        ("requested_applicable", u32), ("forecast_applicable", u32), ("advisory_applicable", u32),
+        ("margin_applicable", u32), ("requested_seconds", f64), ("forecast_seconds", f64),
+        ("advisory_seconds", f64), ("advisory_margin_fraction", f64), ("preparation_work", u64),
+        ("engine_setup_work", u64), ("full_fit_work", u64), ("leverage_work", u64), ("target_work", u64),
+        ("result_export_work", u64), ("total_work", u64)
+    ]
+
+
+class CounterPhaseExecutionReceiptV1(Struct):
+    _fields_ = [
+        ("planned_logical_atoms", u64), ("actual_logical_atoms", u64), ("planned_unique_packed_words", u64),
+        ("actual_unique_packed_words", u64), ("planned_physical_trials", u64), ("actual_physical_trials", u64),
+        ("planned_generator_work", u64), ("actual_generator_work", u64)
+    ]
+
+
+class CounterExecutionReceiptV1(Struct):
+    _fields_ = [
+        ("schema_version", u32), ("rng_contract", u32), ("generator_work_applicable", u32), ("completed", u32),
+        ("leverage", CounterPhaseExecutionReceiptV1), ("target", CounterPhaseExecutionReceiptV1),
+        ("total", CounterPhaseExecutionReceiptV1), ("logical_atoms_before_plan_freeze", u64),
+        ("unique_words_before_plan_freeze", u64), ("physical_trials_before_plan_freeze", u64)
+    ]
+
+
+class ExecutionMemoryReceiptV1(Struct):
+    _fields_ = [
+        ("schema_version", u32), ("applicability", u32), ("peak_phase", u32), ("reserved", u32),
+        ("hard_limit_bytes", u64), ("prepared_persistent_bytes", u64), ("setup_peak_bytes", u64),
+        ("fit_peak_bytes", u64), ("correction_peak_bytes", u64), ("leverage_peak_bytes", u64),
+        ("target_peak_bytes", u64), ("result_peak_bytes", u64), ("non_batched_peak_bytes", u64),
+        ("command_peak_bytes", u64), ("shared_cmg_persistent_bytes", u64),
+        ("full_control_block_persistent_bytes", u64), ("setup_transient_bytes", u64),
+        ("cmg_preconditioner_workspace_bytes", u64), ("cmg_aggregated_cell_capacity_bytes", u64),
+        ("cmg_group_index_bytes", u64), ("cmg_hybrid_graph_bytes", u64), ("retained_nq_bytes", u64),
+        ("retained_q2_bytes", u64)
+    ]
+
+
+class ExecutionPlanReceiptV1(Struct):
+    _fields_ = [
+        ("struct_size", u32), ("schema_version", u32), ("generation", u64), ("applicability_flags", u64),
+        ("contract_flags", u64), ("request_signature", u64), ("resolution", EstimatorResolutionReceiptV1),
+        ("solver", SolverExecutionReceiptV1), ("batch", BatchExecutionReceiptV1),
+        ("wall", WallExecutionReceiptV1), ("counter", CounterExecutionReceiptV1),
+        ("memory", ExecutionMemoryReceiptV1)
+    ]
+
+
+class EngineDetailedReceiptV7(Struct):
+    _fields_ = [
+        ("v6", EngineDetailedReceiptV6), ("execution", ExecutionPlanReceiptV1)
+    ]
+
 class FullCmgReceiptV1(C.Structure):
     """The plugin's VckssFullCmgReceiptV1 (vckss_rust.h:1458-1509, 400 bytes)."""
     _fields_ = ([("struct_size", u32), ("schema_version", u32), ("generation", u64), ("backend_identity", u32),
@@ -347,6 +540,7 @@ SIGNATURES = {
     "fevcb_counter_atoms_noalloc_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64,
                                              C.POINTER(i64)]),
 }
+SIGNATURES.update({f"vckss_rust_engine_detailed_receipt_v{k}": (i32, [u64, C.c_void_p, u32]) for k in range(1, 8)})
 
 # Reference entry points outside the replaced solve path: schema probes,
 # the session last-error alias and UNSUPPORTED_FEATURE returns (csrc/abi_unsupported.cpp).
@@ -604,6 +798,13 @@ class Engine:
         o = FevcbSolveOptionsV2(FevcbSolveOptionsV1(C.sizeof(FevcbSolveOptionsV2), block_columns, preconditioner, 1),
                                 precision, 0)
         self.check(self.lib.fevcb_engine_solve_options_v1(self.generation, C.byref(o)))
+
+    def detailed_receipt(self, version: int = 7):
+        cls = globals()[f"EngineDetailedReceiptV{version}"]
+        out = cls()
+        self.check(getattr(self.lib, f"vckss_rust_engine_detailed_receipt_v{version}")(
+            self.generation, C.byref(out), C.sizeof(out)))
+        return out
 
     def timings(self) -> dict:
         t = FevcbSolveTimingsV1()

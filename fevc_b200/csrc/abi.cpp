@@ -96,6 +96,8 @@ struct Prepared {
   uint32_t precision = 0;         // device option: 1 mixed-precision inner solves
   SolveOptions last_options;
   bool solved_once = false;
+  uint32_t solve_version = 0;                // request version of the last solve: 1, 4, 5 or 8
+  VckssEngineSolveRequestV4 last_request{};  // the last V4+ request (capability and batch fields)
 };
 
 struct Registry {
@@ -449,7 +451,7 @@ SolveOptions options_from_v4(const VckssEngineSolveRequestV4& q) {
 }
 
 void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr, bool generic_allowed,
-                  const VckssEngineSolveRequestV4* v4 = nullptr) {
+                  const VckssEngineSolveRequestV4* v4 = nullptr, uint32_t version = 1) {
   Registry& r = reg();
   std::unique_lock<std::mutex> l(r.mu);
   Prepared& p = r.require(g, "context_solve");
@@ -477,10 +479,13 @@ void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr, bool generi
       p.device = make_device_engine(p.problem, p.plan, o.preconditioner);
       p.device_preconditioner = o.preconditioner;
     }
-    auto res = std::make_unique<SolveResult>(device_solve(*p.device, p.problem, p.plan, o, true));
+    // per-unit detail stays on the device until a caller asks for it
+    auto res = std::make_unique<SolveResult>(device_solve(*p.device, p.problem, p.plan, o, false));
     intr.check("jla_finalize");
     p.last_options = o;
     p.solved_once = true;
+    p.solve_version = version;
+    p.last_request = v4 ? *v4 : VckssEngineSolveRequestV4{};
     r.result = std::move(res);
     r.state = State::Solved;
   } catch (...) {
@@ -489,6 +494,170 @@ void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr, bool generi
   }
 }
 
+
+// Detailed receipt of the last solve (reference `detailed_receipt` ..
+// `detailed_receipt_v6` and the execution plan, vckss-plugin/src/
+// ffi_engine.rs:7443-8100, 6297-6330).  Filled: the request and what this
+// engine did with it (seed, probes, widths, tolerances, routes, counts, the
+// fit, residual maxima, maximum leverage, accounting, topology checksum, the
+// CMG structure, the capability fields); the reference's CPU memory, thread
+// and wall forecasts have no counterpart here and stay zero.
+VckssEngineDetailedReceiptV7 detailed_receipt(uint64_t g, const Prepared& p, const SolveResult& res) {
+  const SolveOptions& o = p.last_options;
+  const VckssEngineSolveRequestV3& q3 = p.last_request.v3;
+  VckssEngineDetailedReceiptV7 d{};
+  VckssEngineDetailedReceiptV2& v2 = d.v6.v5.v4.v3.v2;
+  DeviceStats st = p.device ? device_stats(*p.device) : DeviceStats{};
+  const uint32_t route = o.preconditioner == 2 ? VCKSS_ROUTE_CMG_PCG : VCKSS_ROUTE_DIAGONAL_PCG;
+  v2.struct_size = sizeof(VckssEngineDetailedReceiptV2);
+  v2.generation = g;
+  v2.seed = o.seed;
+  v2.probes_requested = o.probes;
+  v2.leverage_probes_accepted = o.probes;
+  v2.target_probes_accepted = o.probes;
+  v2.solver_requested = o.solver_route;
+  v2.solver_selected = route;
+  v2.solver_fallback = res.timings.fallbacks ? 1 : 0;
+  // the grounded firm quotient F - 1; the generic estimator's joint system
+  // keeps all F firms and adds the control block
+  v2.solver_dimension = p.plan.generic ? p.problem.firms + p.controls : p.problem.firms - 1;
+  v2.leverage_batch_width = o.leverage_batch_width;
+  v2.target_batch_width = o.target_batch_width;
+  v2.rank_tolerance = o.rank_tolerance;
+  v2.block_tolerance = o.block_tolerance;
+  v2.full_residual_tolerance = std::max(10.0 * o.pcg_tolerance, 1e-11);
+  uint64_t lev = 0, tgt = 0;
+  for (const RhsReceipt& r : res.receipts) {
+    if (r.phase == 1) {
+      v2.full_fit_route = route;
+      v2.full_fit_iterations = r.iterations;
+      v2.full_fit_reduced_residual = r.reduced_residual;
+      v2.full_fit_complete_residual = r.complete_residual;
+      v2.full_fit_zero_rhs = r.zero_rhs;
+    }
+    lev += r.phase == 2;
+    tgt += r.phase == 3;
+  }
+  v2.leverage_rhs_count = lev;
+  v2.target_rhs_count = tgt;
+  v2.max_reduced_residual = res.max_reduced_residual;
+  v2.max_complete_residual = res.max_complete_residual;
+  v2.max_leverage = res.max_leverage;
+  // |M (1/M) - 1| over the units' residual shares (reference engine.rs:2347-2382)
+  for (double share : res.unit_residual_share)
+    if (share > 0.0) v2.max_reciprocal_residual = std::max(v2.max_reciprocal_residual, std::fabs(share * (1.0 / share) - 1.0));
+  // scaled |total - worker - firm - 2 cov| over the plug-in, correction,
+  // corrected components and every draw (reference engine.rs:3227-3317)
+  auto identity = [](const Components& c) {
+    double scale = std::max({std::fabs(c.worker), std::fabs(c.firm), std::fabs(c.covariance), std::fabs(c.total), 1.0});
+    return std::fabs(c.total - c.worker - c.firm - 2.0 * c.covariance) / scale;
+  };
+  v2.accounting_residual = std::max({identity(res.plugin), identity(res.correction), identity(res.corrected)});
+  for (const Components& dr : res.target_draws) v2.accounting_residual = std::max(v2.accounting_residual, identity(dr));
+  v2.topology_checksum = p.problem.topology_checksum;
+  if (o.preconditioner == 2) {
+    v2.cmg_levels = st.levels;
+    v2.cmg_fine_vertices = st.vertices;
+    v2.cmg_fine_edges = st.edges;
+    v2.cmg_terminal_vertices = st.terminal_vertices;
+  }
+  v2.full_fit_weighted_rss = res.weighted_rss;
+  v2.memory_limit_bytes = p.memory_limit;
+  v2.caller_copy_bytes = p.caller_copy;
+  v2.prepared_resident_bytes = st.h2d_bytes;
+  VckssEngineDetailedReceiptV3& v3 = d.v6.v5.v4.v3;
+  v3.rng_contract = VCKSS_RNG_COUNTER_V1;
+  v3.rhs_receipt_rows = res.receipts.size();
+  v3.caller_result_copy_bytes = p.plan.generic ? 0 : res.receipts.size() * 14 * 8;
+  VckssEngineDetailedReceiptV4& v4 = d.v6.v5.v4;
+  v4.algorithm_requested = p.solve_version >= 4 ? q3.v2.algorithm : VCKSS_ALGORITHM_JLA;
+  v4.algorithm_selected = VCKSS_ALGORITHM_JLA;
+  v4.deletion_mode = p.deletion_mode;
+  v4.nuisance_mode = p.solve_version >= 4 ? q3.v2.nuisance_mode : 0;
+  v4.parameters = p.problem.workers + p.problem.firms - 1 + p.controls;
+  v4.full_parameters = v4.parameters;
+  v4.correction_parameters = v4.parameters;
+  VckssEngineDetailedReceiptV5& v5 = d.v6.v5;
+  v5.working_fit_complete_residual = v2.full_fit_complete_residual;
+  v5.actual_accounting_residual = v2.accounting_residual;
+  VckssEngineDetailedReceiptV6& v6 = d.v6;
+  v6.engine_requested = p.solve_version >= 4 ? q3.engine : VCKSS_ENGINE_AUTO_OR_UNSPECIFIED;
+  v6.engine_selected = p.plan.generic ? VCKSS_ENGINE_GENERIC : VCKSS_ENGINE_COMPRESSED;
+  v6.controls_count = p.controls;
+  v6.rhs_receipt_schema = p.plan.generic ? 2 : 1;
+  if (p.solve_version >= 4) {
+    v6.capability_schema = q3.capability_schema;
+    v6.capability_profile = q3.capability_profile;
+    v6.batch_mode = q3.batch_mode;
+    v6.stayers_mode = q3.stayers_mode;
+    v6.target_weight_mode = q3.target_weight_mode;
+    v6.deletion_unit_source = q3.deletion_unit_source;
+    v6.probeorder_supplied = q3.probeorder_supplied;
+    v6.wallseconds_supplied = q3.wallseconds_supplied;
+    v6.frequency_use = q3.frequency_use;
+    v6.physical_limit = q3.physical_limit;
+    v6.request_signature = q3.request_signature;
+  }
+  // execution plan (V5 and V8 solves)
+  VckssExecutionPlanReceiptV1& x = d.execution;
+  x.struct_size = sizeof(VckssExecutionPlanReceiptV1);
+  x.schema_version = 1;
+  x.generation = g;
+  x.request_signature = v6.request_signature;
+  x.resolution.algorithm_schema = 1;
+  x.resolution.algorithm_requested = v4.algorithm_requested;
+  x.resolution.algorithm_selected = VCKSS_ALGORITHM_JLA;
+  x.resolution.engine_schema = 1;
+  x.resolution.engine_requested = v6.engine_requested;
+  x.resolution.engine_selected = v6.engine_selected;
+  x.resolution.resolved_before_rng = 1;
+  x.solver.schema_version = 1;
+  x.solver.requested_route = o.solver_route;
+  x.solver.selected_route = route;
+  x.solver.fallback_used = v2.solver_fallback;
+  x.solver.full_setup_complete = 1;
+  x.solver.fe_setup_complete = 1;
+  x.solver.plan_frozen_before_rng = 1;
+  x.solver.threads_requested = 1;
+  x.solver.threads_used = 1;
+  x.solver.planned_rhs = 1 + 3 * uint64_t(o.probes);
+  x.solver.full_solver_dimension = v2.solver_dimension;
+  x.solver.fe_solver_dimension = p.plan.generic ? p.problem.firms : p.problem.firms - 1;
+  x.batch.schema_version = 1;
+  x.batch.deterministic = 1;
+  x.batch.leverage.requested_width = o.leverage_batch_width;
+  x.batch.leverage.selected_width = o.block_columns ? uint64_t(o.block_columns) : 64;
+  x.batch.target.requested_width = o.target_batch_width;
+  x.batch.target.selected_width = x.batch.leverage.selected_width;
+  x.wall.schema_version = 1;
+  x.counter.schema_version = 1;
+  x.counter.rng_contract = VCKSS_RNG_COUNTER_V1;
+  x.counter.completed = 1;
+  x.memory.schema_version = 1;
+  x.memory.hard_limit_bytes = p.memory_limit;
+  x.memory.prepared_persistent_bytes = st.h2d_bytes;
+  return d;
+}
+
+template <class T>
+void write_receipt_prefix(const VckssEngineDetailedReceiptV7& d, T* out) {
+  static_assert(sizeof(T) <= sizeof(VckssEngineDetailedReceiptV7), "receipt prefix");
+  std::memcpy(out, &d, sizeof(T));
+}
+
+// The solved result a detailed receipt describes, with the quantities the
+// solve leaves on the device (weighted RSS, the units' residual shares) read.
+const SolveResult& solved_result(uint64_t g, Prepared*& p, const char* phase) {
+  p = &reg().require(g, phase);
+  if (reg().state != State::Solved || !reg().result) fail(STALE_CONTEXT, phase, "generation has no solved result");
+  SolveResult& res = *reg().result;
+  if (p->device && !res.weighted_rss_ready) {
+    res.weighted_rss = device_weighted_rss(*p->device, p->problem);
+    res.weighted_rss_ready = true;
+  }
+  if (p->device && !p->plan.generic) device_unit_detail(*p->device, res);
+  return res;
+}
 }  // namespace
 
 namespace fevcb {
@@ -836,7 +1005,7 @@ static SolveOptions options_from_v5(const VckssEngineSolveRequestV5& q) {
 int32_t vckss_rust_engine_solve_v5(uint64_t generation, const VckssEngineSolveRequestV5* request) {
   return status([&] {
     auto q = read_struct(request, "V5 engine solve request");
-    solve_common(generation, options_from_v5(q), Interrupt{}, true, &q.v4);
+    solve_common(generation, options_from_v5(q), Interrupt{}, true, &q.v4, 5);
   });
 }
 
@@ -845,7 +1014,7 @@ int32_t vckss_rust_engine_solve_interrupt_v5(uint64_t generation, const VckssEng
     auto q = read_struct(request, "V5 interrupt engine solve request");
     solve_common(generation, options_from_v5(q.options),
                  Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "solve"), true,
-                 &q.options.v4);
+                 &q.options.v4, 5);
   });
 }
 
@@ -853,7 +1022,7 @@ int32_t vckss_rust_engine_solve_v4(uint64_t generation, const VckssEngineSolveRe
   return status([&] {
     auto q = read_struct(request, "V4 engine solve request");
     require_abi(q.v3.v2.v1.abi_version);
-    solve_common(generation, options_from_v4(q), Interrupt{}, true, &q);
+    solve_common(generation, options_from_v4(q), Interrupt{}, true, &q, 4);
   });
 }
 
@@ -863,7 +1032,7 @@ int32_t vckss_rust_engine_solve_interrupt_v4(uint64_t generation, const VckssEng
     require_abi(q.options.v3.v2.v1.abi_version);
     solve_common(generation, options_from_v4(q.options),
                  Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "solve"), true,
-                 &q.options);
+                 &q.options, 4);
   });
 }
 
@@ -900,7 +1069,7 @@ int32_t vckss_rust_engine_solve_v8(uint64_t generation, const VckssEngineSolveRe
   return status([&] {
     auto q = read_struct(request, "V8 engine solve request");
     require_abi(q.v7.v6.v4.v3.v2.v1.abi_version);
-    solve_common(generation, options_from_v4(q.v7.v6.v4), Interrupt{}, true, &q.v7.v6.v4);
+    solve_common(generation, options_from_v4(q.v7.v6.v4), Interrupt{}, true, &q.v7.v6.v4, 8);
   });
 }
 
@@ -910,7 +1079,7 @@ int32_t vckss_rust_engine_solve_interrupt_v8(uint64_t generation, const VckssEng
     require_abi(q.options.v7.v6.v4.v3.v2.v1.abi_version);
     solve_common(generation, options_from_v4(q.options.v7.v6.v4),
                  Interrupt(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "solve"), true,
-                 &q.options.v7.v6.v4);
+                 &q.options.v7.v6.v4, 8);
   });
 }
 
@@ -966,6 +1135,50 @@ int32_t vckss_rust_backend_request_capability_v3(const VckssBackendRequestCapabi
     r.target_batch_resolution_deferred = c.target_batch_mode == VCKSS_BATCH_MODE_AUTO;
     r.wall_advisory_only = 1;
     std::memcpy(out, &r, sizeof(r));
+  });
+}
+
+int32_t vckss_rust_engine_detailed_receipt_v1(uint64_t generation, VckssEngineDetailedReceiptV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEngineDetailedReceiptV1>(out, cap, "engine detailed receipt");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared* p = nullptr;
+    const SolveResult& res = solved_result(generation, p, "engine_detailed_receipt");
+    if (p->plan.generic)
+      fail(UNSUPPORTED_FEATURE, "engine_detailed_receipt", "the V1 receipt describes a no-control match solve");
+    VckssEngineDetailedReceiptV7 d = detailed_receipt(generation, *p, res);
+    d.v6.v5.v4.v3.v2.struct_size = sizeof(VckssEngineDetailedReceiptV1);
+    write_receipt_prefix(d, out);
+  });
+}
+
+#define FEVCB_DETAILED_RECEIPT(N, TYPE, LABEL)                                                   \
+  int32_t vckss_rust_engine_detailed_receipt_v##N(uint64_t generation, TYPE* out, uint32_t cap) { \
+    return status([&] {                                                                          \
+      require_capacity<TYPE>(out, cap, LABEL);                                                   \
+      std::lock_guard<std::mutex> l(reg().mu);                                                   \
+      Prepared* p = nullptr;                                                                     \
+      const SolveResult& res = solved_result(generation, p, "engine_detailed_receipt");          \
+      write_receipt_prefix(detailed_receipt(generation, *p, res), out);                          \
+    });                                                                                          \
+  }
+FEVCB_DETAILED_RECEIPT(2, VckssEngineDetailedReceiptV2, "V2 engine detailed receipt")
+FEVCB_DETAILED_RECEIPT(3, VckssEngineDetailedReceiptV3, "V3 engine detailed receipt")
+FEVCB_DETAILED_RECEIPT(4, VckssEngineDetailedReceiptV4, "V4 engine detailed receipt")
+FEVCB_DETAILED_RECEIPT(5, VckssEngineDetailedReceiptV5, "V5 engine detailed receipt")
+FEVCB_DETAILED_RECEIPT(6, VckssEngineDetailedReceiptV6, "V6 engine detailed receipt")
+#undef FEVCB_DETAILED_RECEIPT
+
+int32_t vckss_rust_engine_detailed_receipt_v7(uint64_t generation, VckssEngineDetailedReceiptV7* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssEngineDetailedReceiptV7>(out, cap, "V7 engine detailed receipt");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared* p = nullptr;
+    const SolveResult& res = solved_result(generation, p, "engine_detailed_receipt");
+    if (p->solve_version != 5 && p->solve_version != 8)
+      fail(UNSUPPORTED_FEATURE, "engine_detailed_receipt",
+           "the V7 execution-plan receipt is unavailable for a legacy solve");
+    write_receipt_prefix(detailed_receipt(generation, *p, res), out);
   });
 }
 
@@ -1173,8 +1386,16 @@ int32_t vckss_rust_engine_rhs_receipts_v2(uint64_t generation, VckssEngineRhsRec
       r.operator_applications = rc[i].iterations + 1;
       r.preconditioner_applications = rc[i].iterations + 1;
       r.full_residual_tolerance = gate;
-      r.residual_space = 1;
-      r.solver_dimension = p.device ? device_stats(*p.device).vertices : p.problem.firms;
+      // residual space and solver dimension by phase (reference
+      // generic_rhs_receipt_value, vckss-plugin/src/ffi_engine.rs:8900-8960):
+      // the generic joint fit and (joint nuisance) targets carry the control
+      // block; leverage and control projections solve the firm system; the
+      // no-control estimator solves the grounded quotient
+      const uint64_t F = p.problem.firms, q = p.controls;
+      const bool joint = rc[i].phase == 1 || (rc[i].phase == 3 && p.last_request.v3.v2.nuisance_mode == 1);
+      r.residual_space = (p.plan.generic && joint) ? VCKSS_RESIDUAL_SPACE_WORKER_FIRM_CONTROL
+                                                   : VCKSS_RESIDUAL_SPACE_WORKER_FIRM;
+      r.solver_dimension = !p.plan.generic ? F - 1 : (joint ? F + q : F);
       out[i] = r;
     }
   });
@@ -1305,8 +1526,9 @@ int32_t fevcb_engine_unit_detail_v1(uint64_t generation, uint64_t units, double*
                                     double* cell_correction_weight, uint64_t probes, double* target_draws4) {
   return status([&] {
     std::lock_guard<std::mutex> l(reg().mu);
-    reg().require(generation, "engine_unit_detail");
+    Prepared& p = reg().require(generation, "engine_unit_detail");
     if (reg().state != State::Solved) fail(STALE_CONTEXT, "engine_unit_detail", "generation has no solved result");
+    if (p.device && reg().result->unit_projection_share.empty()) device_unit_detail(*p.device, *reg().result);
     const SolveResult& s = *reg().result;
     if (s.unit_projection_share.empty()) fail(STALE_CONTEXT, "engine_unit_detail", "unit detail was not retained");
     if (units != s.unit_projection_share.size() || cells != s.fitted_cell.size() || probes != s.target_draws.size())

@@ -94,7 +94,9 @@ __global__ void k_raw_atoms(uint64_t count, const uint64_t* __restrict__ entity,
 __global__ void k_adjust(AdjustParams prm, const uint32_t* __restrict__ unit_ptr, const double* __restrict__ moments,
                          const double* __restrict__ unit_outcome, const double* __restrict__ unit_count_f,
                          const double* __restrict__ fitted_cell, double* __restrict__ unit_out,
-                         double* __restrict__ omega, unsigned long long* __restrict__ error) {
+                         double* __restrict__ omega, unsigned long long* __restrict__ error,
+                         unsigned long long* __restrict__ max_leverage) {
+  double lev_max = 0.0;  // the largest projection share (the reported maximum leverage)
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < prm.cells; c += gridDim.x * blockDim.x) {
     StableSumD w;
     for (uint32_t g = unit_ptr[c]; g < unit_ptr[c + 1]; ++g) {
@@ -132,9 +134,11 @@ __global__ void k_adjust(AdjustParams prm, const uint32_t* __restrict__ unit_ptr
       o[3] = variance;
       o[4] = residual_outcome;
       o[5] = deleted;
+      lev_max = fmax(lev_max, projection);
     }
     omega[c] = w.finish();
   }
+  warp_max_into(lev_max, max_leverage);
 }
 
 // fitted cell value and the plug-in reductions of the full fit (one column)
@@ -251,6 +255,7 @@ struct DeviceEngine {
   int preconditioner = 1;
   Segments lap_seg, firm_seg;
   int coop_blocks = 0;
+  std::vector<RhsReceipt> control_receipts;  // the control projections' solves (generic estimator)
   // generic (controlled) estimator: row-level data and the control geometry
   bool generic = false;
   int q = 0;
@@ -574,7 +579,7 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   // per-block partials: at most QMAX*K (K <= 64) or 64 values per block
   e->partial.alloc(size_t(grid_blocks()) * QMAX * 128 + 1024);
   e->small.alloc(1024);
-  e->error.alloc(1);
+  e->error.alloc(2);  // [0] first failing unit << 8 | code, [1] maximum leverage (double bits)
   CK(cudaMallocHost(&e->h_nactive, sizeof(int) * 16));
   {
     int dev = 0, sms = 0, per = 0;
@@ -595,6 +600,58 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   CK(cudaStreamSynchronize(s));
   e->stats.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return e;
+}
+
+// Per-unit detail of the last solve without controls (shares, bias, variance,
+// masses), the fitted cells and the cell correction weights; they stay on the
+// device after a solve and are read when a caller asks for them.
+void device_unit_detail(DeviceEngine& e, SolveResult& res) {
+  if (e.generic || e.observation)
+    fail(UNSUPPORTED_FEATURE, "engine_unit_detail", "unit detail is kept for solves without controls");
+  if (!res.unit_projection_share.empty()) return;
+  cudaStream_t st = e.stream;
+  std::vector<double> uo(size_t(e.G) * 6);
+  res.fitted_cell.resize(e.C);
+  res.cell_correction_weight.resize(e.C);
+  CK(cudaMemcpyAsync(uo.data(), e.unit_out.p, uo.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(res.fitted_cell.data(), e.fitted.p, e.C * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(res.cell_correction_weight.data(), e.omega.p, e.C * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  size_t G = e.G;
+  res.unit_projection_share.assign(G, 0);
+  res.unit_residual_share.assign(G, 0);
+  res.unit_finite_bias.assign(G, 0);
+  res.unit_finite_variance.assign(G, 0);
+  res.unit_residual_mass.assign(G, 0);
+  res.unit_deleted_mass.assign(G, 0);
+  for (size_t i = 0; i < G; ++i) {
+    uint32_t g = e.unit_group[i];
+    res.unit_projection_share[g] = uo[i * 6 + 0];
+    res.unit_residual_share[g] = uo[i * 6 + 1];
+    res.unit_finite_bias[g] = uo[i * 6 + 2];
+    res.unit_finite_variance[g] = uo[i * 6 + 3];
+    res.unit_residual_mass[g] = uo[i * 6 + 4];
+    res.unit_deleted_mass[g] = uo[i * 6 + 5];
+  }
+}
+
+// Weighted residual sum of squares of the last solve's full fit, in row order
+// with a compensated sum: sum_r f_r (y_r - fitted cell)^2 without controls
+// (reference `full_fit_weighted_rss_with_interrupt`, engine.rs:2218-2252),
+// sum_r f_r (y_r - alpha - psi - Q_r'beta)^2 with them (generic_jla.rs:2079-2088).
+double device_weighted_rss(DeviceEngine& e, const Compressed& p) {
+  std::vector<double> v(e.generic ? size_t(e.rows) : size_t(e.C));
+  CK(cudaMemcpyAsync(v.data(), e.generic ? e.residual.p : e.fitted.p, v.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost, e.stream));
+  CK(cudaStreamSynchronize(e.stream));
+  double sum = 0.0, comp = 0.0;
+  for (size_t r = 0; r < p.rows(); ++r) {
+    double resid = e.generic ? v[r] : p.outcome[r] - v[p.row_cell[r]];
+    double x = double(p.frequency[r]) * resid * resid, t = sum + x;
+    comp += std::fabs(sum) >= std::fabs(x) ? (sum - t) + x : (x - t) + sum;
+    sum = t;
+  }
+  return sum + comp;
 }
 
 // ---------------------------------------------------------------------------
@@ -1531,13 +1588,15 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
   // ---- adjustment
   {
     AdjustParams prm{e.C, double(o.probes), o.block_tolerance, o.rank_tolerance, outcome_mean(p, o.centering)};
-    unsigned long long init = ~0ull;
-    CK(cudaMemcpyAsync(e.error.p, &init, sizeof(init), cudaMemcpyHostToDevice, L.s));
+    unsigned long long init[2] = {~0ull, 0ull};
+    CK(cudaMemcpyAsync(e.error.p, init, sizeof(init), cudaMemcpyHostToDevice, L.s));
     k_adjust<<<L.grid, THREADS, 0, L.s>>>(prm, e.unit_ptr.p, e.moments.p, e.unit_outcome.p, e.unit_count_f.p,
-                                          e.fitted.p, e.unit_out.p, e.omega.p, e.error.p);
-    unsigned long long err = 0;
-    CK(cudaMemcpyAsync(&err, e.error.p, sizeof(err), cudaMemcpyDeviceToHost, L.s));
+                                          e.fitted.p, e.unit_out.p, e.omega.p, e.error.p, e.error.p + 1);
+    unsigned long long got[2] = {0, 0};
+    CK(cudaMemcpyAsync(got, e.error.p, sizeof(got), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
+    const unsigned long long err = got[0];
+    std::memcpy(&res.max_leverage, &got[1], sizeof(double));
     res.timings.kernel_launches += 1;
     if (err != ~0ull) {
       uint32_t code = uint32_t(err & 0xff);
@@ -1564,32 +1623,7 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
     res.max_reduced_residual = std::max(res.max_reduced_residual, r.reduced_residual);
     res.max_complete_residual = std::max(res.max_complete_residual, r.complete_residual);
   }
-  if (detail) {
-    std::vector<double> uo(size_t(e.G) * 6);
-    res.fitted_cell.resize(e.C);
-    res.cell_correction_weight.resize(e.C);
-    CK(cudaMemcpyAsync(uo.data(), e.unit_out.p, uo.size() * sizeof(double), cudaMemcpyDeviceToHost, L.s));
-    CK(cudaMemcpyAsync(res.fitted_cell.data(), e.fitted.p, e.C * sizeof(double), cudaMemcpyDeviceToHost, L.s));
-    CK(cudaMemcpyAsync(res.cell_correction_weight.data(), e.omega.p, e.C * sizeof(double), cudaMemcpyDeviceToHost, L.s));
-    CK(cudaStreamSynchronize(L.s));
-    size_t G = e.G;
-    res.unit_projection_share.assign(G, 0);
-    res.unit_residual_share.assign(G, 0);
-    res.unit_finite_bias.assign(G, 0);
-    res.unit_finite_variance.assign(G, 0);
-    res.unit_residual_mass.assign(G, 0);
-    res.unit_deleted_mass.assign(G, 0);
-    for (size_t i = 0; i < G; ++i) {
-      uint32_t g = e.unit_group[i];
-      res.unit_projection_share[g] = uo[i * 6 + 0];
-      res.unit_residual_share[g] = uo[i * 6 + 1];
-      res.unit_finite_bias[g] = uo[i * 6 + 2];
-      res.unit_finite_variance[g] = uo[i * 6 + 3];
-      res.unit_residual_mass[g] = uo[i * 6 + 4];
-      res.unit_deleted_mass[g] = uo[i * 6 + 5];
-      res.max_leverage = std::max(res.max_leverage, uo[i * 6 + 0]);
-    }
-  }
+  if (detail) device_unit_detail(e, res);
   auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
   res.timings.fit_ms = ms(t0, t1);
   res.timings.leverage_ms = ms(t1, t2);
@@ -1640,7 +1674,13 @@ void setup_controls(DeviceEngine& e, const SolveOptions& o, SolveTimings& tm) {
   firm_gather<8, 0, 0>(e, w8, L, nullptr, w8.cell_val.p, nullptr, 0.0, nullptr, nullptr, nullptr, w8.bF.p, nullptr);
   SolveOptions oc = o;
   oc.pcg_tolerance = std::min(o.pcg_tolerance, 1e-10);
-  solve_block<8>(e, w8, q, oc, tm);
+  BlockOutcome bo = solve_block<8>(e, w8, q, oc, tm);
+  // one receipt per control projection (phase 5, joint side, probe = the
+  // control's index), reported with every solve of this engine
+  e.control_receipts.clear();
+  for (int k = 0; k < q; ++k)
+    e.control_receipts.push_back(
+        RhsReceipt{5, 0, k, uint32_t(bo.iters[k]), uint32_t(bo.zero[k]), bo.reduced[k], bo.complete[k]});
   CK(cudaMemcpyAsync(e.alphaH.p, w8.alpha.p, size_t(e.W) * QMAX * sizeof(double), cudaMemcpyDeviceToDevice, L.s));
   CK(cudaMemcpyAsync(e.psiH.p, w8.x.p, size_t(e.F) * QMAX * sizeof(double), cudaMemcpyDeviceToDevice, L.s));
   k_residualize<<<L.grid, THREADS, 0, L.s>>>(e.rows, q, e.row_cell.p, e.cell_worker.p, e.cell_firm.p, e.row_freq.p,
@@ -1688,6 +1728,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
   auto now = [] { return std::chrono::steady_clock::now(); };
   auto t0 = now();
   setup_controls(e, o, res.timings);
+  res.receipts.insert(res.receipts.begin(), e.control_receipts.begin(), e.control_receipts.end());
   const int q = e.q;
   // ---- joint fit: FE solve of y, then beta = S^{-1} R'W y and theta = theta_y - H beta
   if (o.shard_phase == 2) {
@@ -1751,8 +1792,8 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
   if (o.shard_phase == 2) shard_upload(e, o.shard_input);
   if (e.observation) {
     // ---- deleted residual of every row from its copies
-    unsigned long long init = ~0ull;
-    CK(cudaMemcpyAsync(e.error.p, &init, sizeof(init), cudaMemcpyHostToDevice, L.s));
+    unsigned long long init[2] = {~0ull, 0ull};
+    CK(cudaMemcpyAsync(e.error.p, init, sizeof(init), cudaMemcpyHostToDevice, L.s));
     if (q > 0) {
       SmallMatrix sinv{};
       for (int i = 0; i < q; ++i)
@@ -1764,10 +1805,12 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     ObservationAdjustParams prm{e.rows, double(o.probes), o.block_tolerance, o.rank_tolerance};
     k_obs_adjust<<<L.grid, THREADS, 0, L.s>>>(prm, e.row_phys.p, e.obs_row_acc.p, e.obs_copy_acc.p,
                                               q > 0 ? e.control_lev.p : nullptr, e.residual.p, e.deleted.p,
-                                              e.obs_out.p, e.error.p);
-    unsigned long long err = 0;
-    CK(cudaMemcpyAsync(&err, e.error.p, sizeof(err), cudaMemcpyDeviceToHost, L.s));
+                                              e.obs_out.p, e.error.p, e.error.p + 1);
+    unsigned long long got[2] = {0, 0};
+    CK(cudaMemcpyAsync(got, e.error.p, sizeof(got), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
+    const unsigned long long err = got[0];
+    std::memcpy(&res.max_leverage, &got[1], sizeof(double));
     res.timings.kernel_launches += 1;
     if (err != ~0ull) {
       uint32_t code = uint32_t(err & 0xff);
@@ -1790,14 +1833,16 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     prm.rank_tolerance = o.rank_tolerance;
     for (int i = 0; i < q; ++i)
       for (int j = 0; j < q; ++j) prm.factor.m[i * QMAX + j] = e.Lfac[i * q + j];
-    unsigned long long init = ~0ull;
-    CK(cudaMemcpyAsync(e.error.p, &init, sizeof(init), cudaMemcpyHostToDevice, L.s));
+    unsigned long long init[2] = {~0ull, 0ull};
+    CK(cudaMemcpyAsync(e.error.p, init, sizeof(init), cudaMemcpyHostToDevice, L.s));
     k_generic_adjust<<<L.grid, THREADS, 0, L.s>>>(prm, e.unit_group_d.p, e.moments.p, e.unit_count_f.p, e.group_ptr.p,
                                                   e.group_rows.p, e.row_freq.p, e.residual.p, e.Rd.p, e.deleted.p,
-                                                  e.unit_out.p, e.error.p);
-    unsigned long long err = 0;
-    CK(cudaMemcpyAsync(&err, e.error.p, sizeof(err), cudaMemcpyDeviceToHost, L.s));
+                                                  e.unit_out.p, e.error.p, e.error.p + 1);
+    unsigned long long got[2] = {0, 0};
+    CK(cudaMemcpyAsync(got, e.error.p, sizeof(got), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
+    const unsigned long long err = got[0];
+    std::memcpy(&res.max_leverage, &got[1], sizeof(double));
     res.timings.kernel_launches += 1;
     if (err != ~0ull) {
       uint32_t code = uint32_t(err & 0xff);

@@ -68,6 +68,7 @@ struct SolveTimings {
 struct SolveResult {
   Components plugin, correction, corrected, mcse;
   double weighted_rss = 0;
+  bool weighted_rss_ready = false;  // computed on request (device_weighted_rss)
   std::vector<double> fitted_cell;
   std::vector<double> unit_projection_share, unit_residual_share, unit_finite_bias, unit_finite_variance;
   std::vector<double> unit_residual_mass, unit_deleted_mass, cell_correction_weight;
@@ -97,6 +98,12 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
 DeviceStats device_stats(const DeviceEngine& e);
 SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o,
                          bool want_unit_detail);
+
+// Per-unit detail of the last solve without controls, read from the device
+// on request (solves keep it there).
+void device_unit_detail(DeviceEngine& e, SolveResult& res);
+// Weighted residual sum of squares of the last solve's full fit, computed on request.
+double device_weighted_rss(DeviceEngine& e, const Compressed& p);
 
 // Time `launches` standalone launches of one hot kernel on the prepared
 // problem with CUDA events (L2 flushed before each launch).  kernel: 1 the

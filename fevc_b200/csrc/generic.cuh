@@ -150,6 +150,64 @@ __device__ __forceinline__ void small_solve(const double* l, int n, double* b) {
   }
 }
 
+// Lower bound of the smallest eigenvalue of the symmetric n x n matrix a
+// (row stride RMAX): cyclic Jacobi rotations to an off-diagonal norm of at most
+// 64 eps n max(|a|_F, 1), then the smallest diagonal entry minus the terminal
+// off-diagonal norm and an accumulated rounding term gamma(64 (sweeps+1) n)
+// max(|a|_F, 1), gamma(k) = k eps / (1 - k eps) (reference
+// `symmetric_eigen_extremes` / `symmetric_spectrum`, vckss-core/src/dense.rs:
+// 36-55, 206-310, 505-527).  Returns NaN if the rotations do not converge.
+__device__ inline double sym_smallest_lower(const double* a, int n) {
+  double w[RMAX * RMAX];
+  double norm2 = 0.0;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      double v = (j < i) ? 0.5 * (a[i * RMAX + j] + a[j * RMAX + i]) : (j > i ? 0.5 * (a[j * RMAX + i] + a[i * RMAX + j]) : a[i * RMAX + i]);
+      w[i * RMAX + j] = v;
+      norm2 += v * v;
+    }
+  const double eps = 2.220446049250313e-16, norm = sqrt(norm2);
+  const double converge = 64.0 * eps * fmax(double(n), 1.0) * fmax(norm, 1.0);
+  auto off_norm = [&] {
+    double sum = 0.0;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j)
+        if (i != j) sum += w[i * RMAX + j] * w[i * RMAX + j];
+    return sqrt(sum);
+  };
+  double off = off_norm();
+  int sweeps = 0;
+  for (int sweep = 0; sweep < 128 && off > converge; ++sweep) {
+    for (int l = 0; l < n; ++l)
+      for (int r = l + 1; r < n; ++r) {
+        double cross = w[l * RMAX + r];
+        if (cross == 0.0) continue;
+        double dl = w[l * RMAX + l], dr = w[r * RMAX + r];
+        double tau = (dr - dl) / (2.0 * cross);
+        double t = copysign(1.0, tau) / (fabs(tau) + sqrt(1.0 + tau * tau));
+        double c = 1.0 / sqrt(1.0 + t * t), sn = t * c;
+        for (int k = 0; k < n; ++k) {
+          if (k == l || k == r) continue;
+          double kl = w[k * RMAX + l], kr = w[k * RMAX + r];
+          double nl = c * kl - sn * kr, nr = sn * kl + c * kr;
+          w[k * RMAX + l] = w[l * RMAX + k] = nl;
+          w[k * RMAX + r] = w[r * RMAX + k] = nr;
+        }
+        w[l * RMAX + l] = dl - t * cross;
+        w[r * RMAX + r] = dr + t * cross;
+        w[l * RMAX + r] = w[r * RMAX + l] = 0.0;
+      }
+    sweeps = sweep + 1;
+    off = off_norm();
+  }
+  if (!(off <= converge)) return nan("");
+  double ops = 64.0 * double(sweeps + 1) * fmax(double(n), 1.0), prod = ops * eps;
+  double bound = off + prod / (1.0 - prod) * fmax(norm, 1.0);
+  double lo = w[0];
+  for (int i = 1; i < n; ++i) lo = fmin(lo, w[i * RMAX + i]);
+  return lo - bound;
+}
+
 // Deleted residuals of every match group (reference `match_deleted_adjustment`,
 // generic_jla.rs:6053-6196).  One thread per group; the group's rows are in
 // semantic-rank order.  Low-rank factor row l:
@@ -162,8 +220,13 @@ __global__ void k_generic_adjust(GenericAdjustParams prm, const uint32_t* __rest
                                  const uint64_t* __restrict__ group_ptr, const uint32_t* __restrict__ group_rows,
                                  const double* __restrict__ row_freq, const double* __restrict__ residual,
                                  const double* __restrict__ R, double* __restrict__ deleted,
-                                 double* __restrict__ unit_out, unsigned long long* __restrict__ error) {
+                                 double* __restrict__ unit_out, unsigned long long* __restrict__ error,
+                                 unsigned long long* __restrict__ max_leverage) {
   const int q = prm.q, rank = 1 + q;
+  // the largest leverage over the groups, 1 - (lower bound of the smallest
+  // eigenvalue of the maker I - V V'), as the reference's maker action reports
+  // it (generic_jla.rs:9097-9305)
+  double lev_max = 0.0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < prm.units; i += gridDim.x * blockDim.x) {
     uint32_t g = unit_group[i];
     const double* m = moments + size_t(i) * 5;
@@ -209,6 +272,7 @@ __global__ void k_generic_adjust(GenericAdjustParams prm, const uint32_t* __rest
           for (int k = 0; k < rank; ++k) v -= V[s][k] * V[t][k];
           a[s * RMAX + t] = v;
         }
+      lev_max = fmax(lev_max, 1.0 - sym_smallest_lower(a, width));
       double piv = small_cholesky(a, width);
       if (!code && !(piv > prm.block_tolerance)) code = NONESTIMABLE_DELETION;
       if (!code) {
@@ -242,6 +306,7 @@ __global__ void k_generic_adjust(GenericAdjustParams prm, const uint32_t* __rest
           for (int t = 0; t < rank; ++t) a[s * RMAX + t] -= v[s] * v[t];
         }
       }
+      lev_max = fmax(lev_max, 1.0 - fmin(sym_smallest_lower(a, rank), 1.0));
       double piv = small_cholesky(a, rank);
       if (!code && !(piv > prm.block_tolerance)) code = NONESTIMABLE_DELETION;
       if (!code) {
@@ -278,6 +343,7 @@ __global__ void k_generic_adjust(GenericAdjustParams prm, const uint32_t* __rest
     o[4] = ct;
     o[5] = ci;
   }
+  warp_max_into(lev_max, max_leverage);
 }
 
 // Generic target draw (reference `target_draw`, generic_jla/statistical_batches.rs:259-347):

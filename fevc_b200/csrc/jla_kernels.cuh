@@ -183,7 +183,8 @@ struct AdjustParams {
 __global__ void k_adjust(AdjustParams prm, const uint32_t* __restrict__ unit_ptr, const double* __restrict__ moments,
                          const double* __restrict__ unit_outcome, const double* __restrict__ unit_count_f,
                          const double* __restrict__ fitted_cell, double* __restrict__ unit_out,
-                         double* __restrict__ omega, unsigned long long* __restrict__ error);
+                         double* __restrict__ omega, unsigned long long* __restrict__ error,
+                         unsigned long long* __restrict__ max_leverage);
 
 // Target directions for H probes starting at `first` (reference
 // `target_directions_with_interrupt`, engine.rs:2621-2700): per cell

@@ -263,6 +263,14 @@ __device__ __forceinline__ void warp_gather(uint32_t my_j, double my_a, uint32_t
   }
 }
 
+// Warp-combined maximum of non-negative doubles into *slot (the bit patterns
+// of non-negative doubles order like the values).
+__device__ __forceinline__ void warp_max_into(double v, unsigned long long* slot) {
+  v = fmax(v, 0.0);
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(slot, (unsigned long long)__double_as_longlong(v));
+}
+
 struct PcgState {
   double* rz;     // r.z of the current iterate
   double* rr;     // r.r

@@ -158,8 +158,9 @@ __global__ void k_obs_adjust(ObservationAdjustParams prm, const uint64_t* __rest
                              const double* __restrict__ row_acc, const double* __restrict__ copy_acc,
                              const double* __restrict__ control_leverage, const double* __restrict__ residual,
                              double* __restrict__ deleted, double* __restrict__ out,
-                             unsigned long long* __restrict__ error) {
+                             unsigned long long* __restrict__ error, unsigned long long* __restrict__ max_leverage) {
   const double P = prm.probes;
+  double lev_all = 0.0;  // the largest total leverage of any copy
   for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < prm.rows; r += gridDim.x * blockDim.x) {
     const double pf = row_acc[size_t(r) * 4] + row_acc[size_t(r) * 4 + 1];
     const double ps = row_acc[size_t(r) * 4 + 2] + row_acc[size_t(r) * 4 + 3];
@@ -212,7 +213,9 @@ __global__ void k_obs_adjust(ObservationAdjustParams prm, const uint64_t* __rest
       out[size_t(r) * 2] = lev_sum.finish() / f;
       out[size_t(r) * 2 + 1] = lev_max;
     }
+    lev_all = fmax(lev_all, lev_max);
   }
+  warp_max_into(lev_all, max_leverage);
 }
 
 }  // namespace fevcb

@@ -36,6 +36,8 @@ extern "C" {
 #define VCKSS_ROUTE_EXACT 1u
 #define VCKSS_ROUTE_DIAGONAL_PCG 2u
 #define VCKSS_ROUTE_CMG_PCG 3u
+#define VCKSS_RESIDUAL_SPACE_WORKER_FIRM 1u
+#define VCKSS_RESIDUAL_SPACE_WORKER_FIRM_CONTROL 2u
 #define VCKSS_REQUEST_CAPABILITY_SCHEMA_V3 3u
 #define VCKSS_REQUEST_FREQUENCY_UNIT 0u
 #define VCKSS_REQUEST_FREQUENCY_LITERAL 1u
@@ -846,6 +848,378 @@ int32_t fevcb_counter_atoms_noalloc_v1(uint64_t seed, uint64_t domain_tag, uint6
                                        const uint64_t *entity, const uint64_t *trials, uint64_t count, int64_t *out);
 
 
+/* Detailed receipts V1-V7 (vckss_rust.h:1084-1439): the same layouts; the fields
+ * this engine fills are listed at fevcb::fill_detailed_receipt (abi.cpp). */
+typedef struct VckssEngineDetailedReceiptV1 {
+  uint32_t struct_size;
+  uint32_t reserved;
+  uint64_t generation;
+  uint64_t seed;
+  uint32_t probes_requested;
+  uint32_t leverage_probes_accepted;
+  uint32_t target_probes_accepted;
+  uint32_t solver_requested;
+  uint32_t solver_selected;
+  uint32_t solver_fallback;
+  int32_t solver_fallback_error;
+  uint64_t solver_dimension;
+  uint64_t leverage_batch_width;
+  uint64_t target_batch_width;
+  double rank_tolerance;
+  double block_tolerance;
+  double full_residual_tolerance;
+  uint32_t full_fit_route;
+  uint32_t full_fit_iterations;
+  double full_fit_reduced_residual;
+  double full_fit_complete_residual;
+  uint32_t full_fit_zero_rhs;
+  uint32_t reserved_1;
+  uint64_t leverage_rhs_count;
+  uint64_t target_rhs_count;
+  double max_reduced_residual;
+  double max_complete_residual;
+  double max_leverage;
+  double max_reciprocal_residual;
+  double accounting_residual;
+  uint64_t topology_checksum;
+  uint64_t cmg_levels;
+  uint64_t cmg_fine_vertices;
+  uint64_t cmg_fine_edges;
+  uint64_t cmg_terminal_vertices;
+  double cmg_edge_complexity;
+  double cmg_vertex_complexity;
+  uint64_t cmg_structural_bytes;
+  uint64_t cmg_workspace_bytes;
+  uint64_t cmg_dense_factor_bytes;
+} VckssEngineDetailedReceiptV1;
+
+typedef struct VckssEngineDetailedReceiptV2 {
+  uint32_t struct_size;
+  uint32_t reserved;
+  uint64_t generation;
+  uint64_t seed;
+  uint32_t probes_requested;
+  uint32_t leverage_probes_accepted;
+  uint32_t target_probes_accepted;
+  uint32_t solver_requested;
+  uint32_t solver_selected;
+  uint32_t solver_fallback;
+  int32_t solver_fallback_error;
+  uint64_t solver_dimension;
+  uint64_t leverage_batch_width;
+  uint64_t target_batch_width;
+  double rank_tolerance;
+  double block_tolerance;
+  double full_residual_tolerance;
+  uint32_t full_fit_route;
+  uint32_t full_fit_iterations;
+  double full_fit_reduced_residual;
+  double full_fit_complete_residual;
+  uint32_t full_fit_zero_rhs;
+  uint32_t reserved_1;
+  uint64_t leverage_rhs_count;
+  uint64_t target_rhs_count;
+  double max_reduced_residual;
+  double max_complete_residual;
+  double max_leverage;
+  double max_reciprocal_residual;
+  double accounting_residual;
+  uint64_t topology_checksum;
+  uint64_t cmg_levels;
+  uint64_t cmg_fine_vertices;
+  uint64_t cmg_fine_edges;
+  uint64_t cmg_terminal_vertices;
+  double cmg_edge_complexity;
+  double cmg_vertex_complexity;
+  uint64_t cmg_structural_bytes;
+  uint64_t cmg_workspace_bytes;
+  uint64_t cmg_dense_factor_bytes;
+  double full_fit_weighted_rss;
+  uint64_t memory_limit_bytes;
+  uint64_t caller_copy_bytes;
+  uint64_t preparation_peak_forecast_bytes;
+  uint64_t prepared_resident_bytes;
+  uint64_t solver_setup_forecast_bytes;
+  uint64_t leverage_phase_forecast_bytes;
+  uint64_t target_phase_forecast_bytes;
+  uint64_t result_forecast_bytes;
+  uint64_t solve_peak_forecast_bytes;
+  uint64_t command_peak_forecast_bytes;
+} VckssEngineDetailedReceiptV2;
+
+typedef struct VckssEngineDetailedReceiptV3 {
+  VckssEngineDetailedReceiptV2 v2;
+  uint32_t rng_contract;
+  uint32_t reserved_2;
+  uint64_t rhs_receipt_rows;
+  uint64_t caller_result_copy_bytes;
+} VckssEngineDetailedReceiptV3;
+
+typedef struct VckssEngineDetailedReceiptV4 {
+  VckssEngineDetailedReceiptV3 v3;
+  uint32_t algorithm_requested;
+  uint32_t algorithm_selected;
+  uint32_t deletion_mode;
+  uint32_t nuisance_mode;
+  uint64_t parameters;
+  uint64_t full_parameters;
+  uint64_t correction_parameters;
+  double information_rcond;
+  double inverse_relres;
+  uint64_t exact_peak_forecast_bytes;
+} VckssEngineDetailedReceiptV4;
+
+typedef struct VckssEngineDetailedReceiptV5 {
+  VckssEngineDetailedReceiptV4 v4;
+  uint64_t applicability_flags;
+  double working_fit_complete_residual;
+  double inverse_sqrt_relres;
+  double maker_relres;
+  double control_basis_relres;
+  double control_basis_forward_error;
+  double deletion_rank_gap;
+  double firm_zero_sum_residual;
+  uint64_t fit_peak_forecast_bytes;
+  uint64_t correction_peak_forecast_bytes;
+  double actual_accounting_residual;
+} VckssEngineDetailedReceiptV5;
+
+typedef struct VckssEngineDetailedReceiptV6 {
+  VckssEngineDetailedReceiptV5 v5;
+  uint32_t engine_requested;
+  uint32_t engine_selected;
+  uint64_t generic_applicability_flags;
+  uint32_t controls_count;
+  uint32_t rhs_receipt_schema;
+  uint64_t control_projection_rhs_count;
+  double control_rank_rcond;
+  double control_rank_smallest_generalized_eigenvalue_lower;
+  double control_rank_largest_generalized_eigenvalue_upper;
+  double control_rank_projection_error_bound;
+  double control_rank_normalization_error_bound;
+  double control_rank_fe_information_eigenvalue_lower_bound;
+  double control_rank_maximum_projection_residual;
+  double control_rank_effective_tolerance;
+  double control_rank_projection_pcg_tolerance;
+  double control_rank_projection_residual_gate;
+  double generic_control_basis_relres;
+  double generic_control_basis_forward_error;
+  double generic_control_schur_rcond;
+  double generic_control_schur_relres;
+  double generic_deletion_rank_gap;
+  double full_joint_fit_complete_residual;
+  double generic_working_fit_complete_residual;
+  double generic_maker_relres;
+  uint64_t canonicalization_peak_forecast_bytes;
+  uint64_t generic_fit_peak_forecast_bytes;
+  uint64_t geometry_peak_forecast_bytes;
+  uint64_t generic_leverage_peak_forecast_bytes;
+  uint64_t generic_target_peak_forecast_bytes;
+  uint64_t maker_peak_forecast_bytes;
+  uint64_t generic_result_forecast_bytes;
+  uint64_t generic_peak_forecast_bytes;
+  uint64_t rhs_v2_caller_copy_bytes;
+  uint32_t capability_schema;
+  uint32_t capability_profile;
+  uint32_t batch_mode;
+  uint32_t stayers_mode;
+  uint32_t target_weight_mode;
+  uint32_t deletion_unit_source;
+  uint32_t probeorder_supplied;
+  uint32_t wallseconds_supplied;
+  uint32_t frequency_use;
+  uint32_t reserved_6;
+  uint64_t physical_limit;
+  uint64_t request_signature;
+} VckssEngineDetailedReceiptV6;
+
+typedef struct VckssEstimatorResolutionReceiptV1 {
+  uint32_t algorithm_schema;
+  uint32_t algorithm_requested;
+  uint32_t algorithm_selected;
+  uint32_t algorithm_reason;
+  uint32_t engine_schema;
+  uint32_t engine_requested;
+  uint32_t engine_selected;
+  uint32_t engine_reason;
+  uint32_t compressed_eligibility;
+  uint32_t resolved_before_rng;
+  uint32_t opportunistic_engine_fallback_allowed;
+  uint32_t reserved;
+  uint64_t identified_complexity;
+  uint64_t exact_limit;
+  uint64_t rng_draws_before_resolution;
+  uint64_t counter_atoms_before_resolution;
+} VckssEstimatorResolutionReceiptV1;
+
+typedef struct VckssSolverExecutionReceiptV1 {
+  uint32_t schema_version;
+  uint32_t requested_route;
+  uint32_t selected_route;
+  uint32_t fallback_used;
+  int32_t fallback_error;
+  uint32_t full_setup_complete;
+  uint32_t fe_setup_complete;
+  uint32_t fe_hierarchy_reused;
+  uint32_t plan_frozen_before_rng;
+  uint32_t auto_route_contract;
+  uint32_t threads_requested;
+  uint32_t threads_used;
+  uint32_t parallel_regions;
+  uint32_t applicability;
+  uint32_t reserved_1;
+  uint32_t reserved_2;
+  uint64_t planned_rhs;
+  uint64_t auto_firm_threshold;
+  uint64_t auto_rhs_threshold;
+  uint64_t full_solver_dimension;
+  uint64_t fe_solver_dimension;
+  uint64_t logical_atoms_before_plan_freeze;
+  uint64_t unique_words_before_plan_freeze;
+  uint64_t physical_trials_before_plan_freeze;
+} VckssSolverExecutionReceiptV1;
+
+typedef struct VckssBatchPhasePlanReceiptV1 {
+  uint32_t request_mode;
+  uint32_t selection_reason;
+  uint32_t applicability;
+  uint32_t reserved;
+  uint64_t requested_width;
+  uint64_t selected_width;
+  uint64_t probe_width_cap;
+  uint64_t declared_threads;
+  uint64_t thread_width_cap;
+  uint64_t route_width_cap;
+  uint64_t effective_width_cap;
+  uint64_t hard_memory_bytes;
+  uint64_t width_one_forecast_bytes;
+  uint64_t selected_forecast_bytes;
+} VckssBatchPhasePlanReceiptV1;
+
+typedef struct VckssBatchExecutionReceiptV1 {
+  uint32_t schema_version;
+  uint32_t deterministic;
+  uint32_t width_invariance_required;
+  uint32_t arithmetic_contract;
+  uint32_t whole_command_admitted;
+  uint32_t applicability;
+  uint64_t non_batched_peak_bytes;
+  uint64_t selected_command_peak_bytes;
+  VckssBatchPhasePlanReceiptV1 leverage;
+  VckssBatchPhasePlanReceiptV1 target;
+} VckssBatchExecutionReceiptV1;
+
+typedef struct VckssWallExecutionReceiptV1 {
+  uint32_t schema_version;
+  uint32_t model_code;
+  uint32_t status;
+  uint32_t routing_effect;
+  uint32_t requested_applicable;
+  uint32_t forecast_applicable;
+  uint32_t advisory_applicable;
+  uint32_t margin_applicable;
+  double requested_seconds;
+  double forecast_seconds;
+  double advisory_seconds;
+  double advisory_margin_fraction;
+  uint64_t preparation_work;
+  uint64_t engine_setup_work;
+  uint64_t full_fit_work;
+  uint64_t leverage_work;
+  uint64_t target_work;
+  uint64_t result_export_work;
+  uint64_t total_work;
+} VckssWallExecutionReceiptV1;
+
+typedef struct VckssCounterPhaseExecutionReceiptV1 {
+  uint64_t planned_logical_atoms;
+  uint64_t actual_logical_atoms;
+  uint64_t planned_unique_packed_words;
+  uint64_t actual_unique_packed_words;
+  uint64_t planned_physical_trials;
+  uint64_t actual_physical_trials;
+  uint64_t planned_generator_work;
+  uint64_t actual_generator_work;
+} VckssCounterPhaseExecutionReceiptV1;
+
+typedef struct VckssCounterExecutionReceiptV1 {
+  uint32_t schema_version;
+  uint32_t rng_contract;
+  uint32_t generator_work_applicable;
+  uint32_t completed;
+  VckssCounterPhaseExecutionReceiptV1 leverage;
+  VckssCounterPhaseExecutionReceiptV1 target;
+  VckssCounterPhaseExecutionReceiptV1 total;
+  uint64_t logical_atoms_before_plan_freeze;
+  uint64_t unique_words_before_plan_freeze;
+  uint64_t physical_trials_before_plan_freeze;
+} VckssCounterExecutionReceiptV1;
+
+typedef struct VckssExecutionMemoryReceiptV1 {
+  uint32_t schema_version;
+  uint32_t applicability;
+  uint32_t peak_phase;
+  uint32_t reserved;
+  uint64_t hard_limit_bytes;
+  uint64_t prepared_persistent_bytes;
+  uint64_t setup_peak_bytes;
+  uint64_t fit_peak_bytes;
+  uint64_t correction_peak_bytes;
+  uint64_t leverage_peak_bytes;
+  uint64_t target_peak_bytes;
+  uint64_t result_peak_bytes;
+  uint64_t non_batched_peak_bytes;
+  uint64_t command_peak_bytes;
+  uint64_t shared_cmg_persistent_bytes;
+  uint64_t full_control_block_persistent_bytes;
+  uint64_t setup_transient_bytes;
+  uint64_t cmg_preconditioner_workspace_bytes;
+  uint64_t cmg_aggregated_cell_capacity_bytes;
+  uint64_t cmg_group_index_bytes;
+  uint64_t cmg_hybrid_graph_bytes;
+  uint64_t retained_nq_bytes;
+  uint64_t retained_q2_bytes;
+} VckssExecutionMemoryReceiptV1;
+
+typedef struct VckssExecutionPlanReceiptV1 {
+  uint32_t struct_size;
+  uint32_t schema_version;
+  uint64_t generation;
+  uint64_t applicability_flags;
+  uint64_t contract_flags;
+  uint64_t request_signature;
+  VckssEstimatorResolutionReceiptV1 resolution;
+  VckssSolverExecutionReceiptV1 solver;
+  VckssBatchExecutionReceiptV1 batch;
+  VckssWallExecutionReceiptV1 wall;
+  VckssCounterExecutionReceiptV1 counter;
+  VckssExecutionMemoryReceiptV1 memory;
+} VckssExecutionPlanReceiptV1;
+
+typedef struct VckssEngineDetailedReceiptV7 {
+  VckssEngineDetailedReceiptV6 v6;
+  VckssExecutionPlanReceiptV1 execution;
+} VckssEngineDetailedReceiptV7;
+
+/* Detailed receipts of the last solve (vckss_rust.h:2093-2116).  V1 needs a
+ * no-control match solve; V7 a V5 or V8 solve (its execution plan).  Fields
+ * of the reference's CPU memory and thread model this engine has no
+ * counterpart for are zero. */
+int32_t vckss_rust_engine_detailed_receipt_v1(uint64_t generation, VckssEngineDetailedReceiptV1 *output,
+                                              uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_detailed_receipt_v2(uint64_t generation, VckssEngineDetailedReceiptV2 *output,
+                                              uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_detailed_receipt_v3(uint64_t generation, VckssEngineDetailedReceiptV3 *output,
+                                              uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_detailed_receipt_v4(uint64_t generation, VckssEngineDetailedReceiptV4 *output,
+                                              uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_detailed_receipt_v5(uint64_t generation, VckssEngineDetailedReceiptV5 *output,
+                                              uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_detailed_receipt_v6(uint64_t generation, VckssEngineDetailedReceiptV6 *output,
+                                              uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_detailed_receipt_v7(uint64_t generation, VckssEngineDetailedReceiptV7 *output,
+                                              uint32_t output_capacity_bytes);
+
 /* ---------------------------------------------------------------------------
  * The rest of the reference ABI (rust/stata_backend/include/vckss_rust.h).
  * These entry points sit outside the solve path this library replaces: the
@@ -1126,6 +1500,15 @@ static_assert(sizeof(VckssEngineRhsReceiptV1) == 48, "RHS receipt V1 layout");
 static_assert(sizeof(VckssEngineRhsReceiptV2) == 96, "RHS receipt V2 layout");
 static_assert(sizeof(VckssEngineSnapshotV1) == 24, "snapshot layout");
 static_assert(sizeof(VckssBackendCapabilitiesV1) == 32, "capabilities layout");
+static_assert(sizeof(VckssEngineDetailedReceiptV1) == 272, "detailed receipt V1 layout");
+static_assert(sizeof(VckssEngineDetailedReceiptV2) == 360, "detailed receipt V2 layout");
+static_assert(sizeof(VckssEngineDetailedReceiptV3) == 384, "detailed receipt V3 layout");
+static_assert(sizeof(VckssEngineDetailedReceiptV4) == 448, "detailed receipt V4 layout");
+static_assert(sizeof(VckssEngineDetailedReceiptV5) == 536, "detailed receipt V5 layout");
+static_assert(sizeof(VckssEngineDetailedReceiptV6) == 840, "detailed receipt V6 layout");
+static_assert(sizeof(VckssExecutionPlanReceiptV1) == 1000, "execution plan receipt layout");
+static_assert(sizeof(VckssEngineDetailedReceiptV7) == 1840, "detailed receipt V7 layout");
+static_assert(offsetof(VckssEngineDetailedReceiptV7, execution) == 840, "detailed receipt V7 extension offset");
 #endif
 
 #endif /* FEVC_B200_H */

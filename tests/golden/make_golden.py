@@ -254,6 +254,56 @@ def solve_record(lib, panel: Panel, probes: int, centering: int) -> dict:
             **{k: list(v) for k, v in res.items()}}
 
 
+# Detailed receipts V7 of V5 solves: the request-side and count fields the B200
+# engine reports the same way (tests/test_gpu_receipts.py lists them).
+RECEIPT_PANELS = {
+    "match_small_2k": dict(build=lambda: PANELS["small_2k"]["build"](), probes=8, deletion_mode=1),
+    "controls": dict(build=lambda: CONTROL_PANELS[next(iter(CONTROL_PANELS))]["build"](), probes=8,
+                     deletion_mode=1),
+    "observation": dict(build=lambda: OBSERVATION_PANELS[next(iter(OBSERVATION_PANELS))]["build"](), probes=8,
+                        deletion_mode=2),
+}
+
+
+def receipt_request(e, probes: int, deletion_mode: int, controls: int):
+    q = e.default_request_v5(deletion_mode)
+    v1 = q.v4.v3.v2.v1
+    v1.probes = probes
+    v1.solver_route = 2
+    v1.pcg_tolerance = 1e-13
+    v1.maximum_iterations = 20000
+    v1.leverage_batch_width = 4
+    v1.target_batch_width = 4
+    q.v4.v3.v2.algorithm = 2
+    q.v4.v3.engine = 2 if (controls or deletion_mode == 2) else 0
+    q.v4.v3.batch_mode = 1
+    q.v4.leverage_batch_mode = 1
+    q.v4.target_batch_mode = 1
+    q.threads = 4
+    q.tolerance_supplied = 1
+    return q
+
+
+def receipt_record(lib, panel: Panel, probes: int, deletion_mode: int) -> dict:
+    e = abi.Engine(lib)
+    e.prepare(panel, deletion_mode=deletion_mode)
+    q = receipt_request(e, probes, deletion_mode, len(panel.controls))
+    e.solve_v5(q, controls_count=len(panel.controls))
+    r = e.detailed_receipt(7)
+    e.release()
+    return {"probes": probes, "deletion_mode": deletion_mode, "receipt": r.as_dict()}
+
+
+def write_receipt_cases(lib, meta: dict) -> None:
+    cases = {}
+    for name, spec in RECEIPT_PANELS.items():
+        panel = spec["build"]()
+        cases[name] = {"panel_sha256": panel_digest(panel),
+                       **receipt_record(lib, panel, spec["probes"], spec["deletion_mode"])}
+        print(name, cases[name]["receipt"]["v6"]["v5"]["v4"]["v3"]["v2"]["topology_checksum"])
+    (HERE / "receipt_cases.json").write_text(json.dumps({"meta": meta, "panels": cases}, indent=1))
+
+
 def write_cmg_cases(lib, meta: dict) -> None:
     lib.vckss_rust_engine_full_cmg_receipt_v1.restype = C.c_int32
     lib.vckss_rust_engine_full_cmg_receipt_v1.argtypes = [C.c_uint64, C.c_void_p, C.c_uint32]
@@ -266,13 +316,18 @@ def write_cmg_cases(lib, meta: dict) -> None:
 
 
 def main() -> None:
-    """All fixtures; with the argument ``cmg`` only cmg_cases.json."""
+    """All fixtures; with the argument ``cmg`` only cmg_cases.json, with
+    ``receipts`` only receipt_cases.json."""
     if not PLUGIN.exists():
         raise SystemExit(f"reference plugin not found at {PLUGIN}")
     lib = abi.load(PLUGIN, bind_extensions=False)
     if sys.argv[1:] == ["cmg"]:
         write_cmg_cases(lib, {"generator": "tests/golden/make_golden.py cmg", "reference_plugin_version":
                               lib.vckss_rust_backend_version().decode()})
+        return
+    if sys.argv[1:] == ["receipts"]:
+        write_receipt_cases(lib, {"generator": "tests/golden/make_golden.py receipts",
+                                  "reference_plugin_version": lib.vckss_rust_backend_version().decode()})
         return
     prep, jla = {}, {}
     for name, spec in PANELS.items():
