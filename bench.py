@@ -325,8 +325,10 @@ def main():
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
         start.record(stream)
+        torch.cuda.nvtx.range_push("timed")  # ncu --nvtx-include "timed/" selects these launches
         for _ in range(args.steps):
             step(e)
+        torch.cuda.nvtx.range_pop()
         stop.record(stream)
         barrier()
     ms = start.elapsed_time(stop)
@@ -340,15 +342,29 @@ def main():
 
     # roofline: the persistent blocked PCG kernel, standalone launches with L2 flushed
     block = args.block or 64
+    torch.cuda.nvtx.range_push("roofline")  # the roofline kernel's standalone launches
     spmm_ms, spmm_bytes = e.kernel_benchmark(1, block, 10)
-    # the same iterations in the three-barrier form, for comparison
-    tb_ms, tb_bytes = e.kernel_benchmark(5, block, 10)
+    torch.cuda.nvtx.range_pop()
+    # the same iterations in both persistent forms, for comparison
+    three_ms, _ = e.kernel_benchmark(5, block, 10)
+    two_ms, _ = e.kernel_benchmark(6, block, 10)
+    two_barrier = block == 32  # the form the solver picks at this width (double, one warp per segment)
     peaks = {}
     try:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
+    # DRAM traffic per launch of this kernel from the committed ncu capture
+    # (profiles/roofline_traffic.json), when it covers this kernel and workload
+    roof_kernel = f"k_pcg_persistent_cg<{block}, double>" if block == 32 else f"k_pcg_persistent<{block}, double>"
+    traffic = None
+    try:
+        rec = json.loads((ROOT / "profiles" / "roofline_traffic.json").read_text()).get(roof_kernel)
+        if rec and rec.get("workload") == args.workload and args.scale == 1.0:
+            traffic = float(rec["bytes_per_launch"])
+    except Exception:
+        pass
     achieved = spmm_bytes / (spmm_ms / 1000.0) / 1e9
     h2d = int(timings["h2d_bytes"])
     e.release()
@@ -412,11 +428,15 @@ def main():
             "time_to_decomposition_s": round(prepare_s + e2e_s, 3), "prepare_s": round(prepare_s, 3),
             "first_solve_s": round(first_solve_s, 3),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": None,
-                         "kernel": f"k_pcg_persistent_cg<{block}> (two grid barriers per iteration, "
-                                   "20 iterations per launch)", "bytes_per_launch": spmm_bytes,
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "kernel": (f"k_pcg_persistent_cg<{block}, double> (two grid barriers per iteration"
+                                    if two_barrier else
+                                    f"k_pcg_persistent<{block}, double> (three grid barriers per iteration")
+                                   + ", 20 iterations per launch, L2 flushed before each)",
+                         "bytes_per_launch": spmm_bytes,
                          "ms_per_launch": round(spmm_ms, 5), "peak_source": "measured (MEASURED_PEAKS.json)",
-                         "three_barrier_ms_per_launch": round(tb_ms, 5)},
+                         "three_barrier_ms_per_launch": round(three_ms, 5),
+                         "two_barrier_ms_per_launch": round(two_ms, 5)},
             "gpu_launches": int(timings["kernel_launches"]) * args.steps,
             "solver": {k: timings[k] for k in ("block_iterations", "column_iterations", "rhs_columns",
                                                "vertices", "edges", "kept_workers", "levels")},

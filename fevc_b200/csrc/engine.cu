@@ -1991,7 +1991,7 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
       k_colsum_abs<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p, e.partial.p);
       finish(e.partial.p, L.grid, 2 * K, w.tot.p, L.s);
       k_pcg_init_state<K><<<1, 128, 0, L.s>>>(w.tot.p, K, 0.0, double(e.n), w.s);
-      pcg_restart<K>(e, w, L, true, kernel == 5);
+      pcg_restart<K>(e, w, L, true, kernel == 5 || (kernel == 1 && !two_barrier_form<K, double>()));
     }
     CK(cudaMemsetAsync(flush.p, i & 0xff, flush.bytes(), L.s));
     CK(cudaEventRecord(e.ev0, L.s));
@@ -2001,9 +2001,9 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
       case 6: {
         PersistentPcg<K> a = persistent_args<K>(e, w, iters);
         void* args[] = {&a};
-        const void* fn = kernel == 1   ? (const void*)k_pcg_persistent_cg<K>
-                         : kernel == 5 ? (const void*)k_pcg_persistent<K>
-                                       : (const void*)k_pcg_persistent_cg<K, double, true>;
+        // 1: the form the solver uses at this width; 5: three barriers; 6: two barriers
+        const bool two = kernel == 6 || (kernel == 1 && two_barrier_form<K, double>());
+        const void* fn = two ? (const void*)k_pcg_persistent_cg<K> : (const void*)k_pcg_persistent<K>;
         CK(cudaLaunchCooperativeKernel(fn, dim3(e.coop_blocks), dim3(PERSIST_THREADS), args, 0, L.s));
         break;
       }

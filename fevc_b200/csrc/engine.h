@@ -107,8 +107,9 @@ double device_weighted_rss(DeviceEngine& e, const Compressed& p);
 
 // Time `launches` standalone launches of one hot kernel on the prepared
 // problem with CUDA events (L2 flushed before each launch).  kernel: 1 the
-// persistent blocked PCG (20 iterations), 3 leverage Counter-V1 atoms with
-// the per-cell sums, 4 leverage moments.  Returns the
+// persistent blocked PCG form used at this width (20 iterations), 3 leverage
+// Counter-V1 atoms with the per-cell sums, 4 leverage moments, 5 / 6 the
+// three- / two-barrier persistent PCG.  Returns the
 // mean device milliseconds per launch and the algorithmic bytes per launch.
 void device_kernel_benchmark(DeviceEngine& e, int kernel, int block_columns, int launches, double* ms_per_launch,
                              double* bytes_per_launch);

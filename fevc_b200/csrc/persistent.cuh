@@ -7,9 +7,10 @@
 // order (deterministic, no atomics).
 //
 // The PCG loop for a block of K right-hand sides runs as ONE cooperative
-// kernel per solve: three grid barriers per iteration (after the SpMM, after
-// the x/r update, after the direction update), per-column step lengths and
-// convergence flags held redundantly in every block's shared memory (each
+// kernel per solve, in one of two forms: three grid barriers per iteration
+// (after the SpMM, after the x/r update, after the direction update), or two
+// (Chronopoulos-Gear recurrences, below).  Per-column step lengths and
+// convergence flags are held redundantly in every block's shared memory (each
 // block reduces the same per-block partials in the same order, so all blocks
 // agree bit for bit and leave the loop together).
 #pragma once
@@ -353,16 +354,17 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(Persisten
 // and broadcast, the next segment's columns and scaled values (A D^{-1}) are
 // loaded while the current segment's gathers are in flight, so a segment costs
 // about one memory latency instead of four dependent ones.
-template <int K, typename V, bool CONTIG>
+template <int K, typename V>
 __device__ __forceinline__ void cg_products(const PersistentPcg<K, V>& a, size_t gid, size_t ngroups, int c0,
                                             double* partial, double (*sm)[1][K]) {
   constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
   double v[1][CPT];
 #pragma unroll
   for (int c = 0; c < CPT; ++c) v[0][c] = 0.0;
-  if constexpr (TPR == 32 && !CONTIG) {
-    // grid-strided segments (consecutive segments run side by side across the
-    // grid); scaled values and the row flag save the dinv and row-pointer loads
+  if constexpr (TPR == 32) {
+    // one warp per segment, grid-strided (consecutive segments run side by
+    // side across the grid); the warp loads the segment's columns and scaled
+    // values (A D^{-1}) lane-parallel, the row flag saves the row-pointer load
     const int lane = threadIdx.x & 31;
     for (size_t sg = gid; sg < a.nseg; sg += ngroups) {
       const uint32_t flag = __ldg(a.seg_flag + sg), b = __ldg(a.seg_begin + sg), e = __ldg(a.seg_end + sg);
@@ -386,56 +388,6 @@ __device__ __forceinline__ void cg_products(const PersistentPcg<K, V>& a, size_t
         a.seg_buf[sg * K + c0 + c] = V(acc[c]);
         double u = di * rr_[c];
         v[0][c] += u * (d * u - acc[c]);
-      }
-    }
-  } else if constexpr (TPR == 32) {
-    const int lane = threadIdx.x & 31;
-    const size_t lo = gid * a.nseg / ngroups, hi = (gid + 1) * a.nseg / ngroups;
-    for (size_t base = lo; base < hi; base += 32) {
-      const int cnt = int(hi - base < 32 ? hi - base : 32);
-      uint32_t m_flag = 0, m_b = 0, m_e = 0;
-      if (lane < cnt) {
-        m_flag = __ldg(a.seg_flag + base + lane);
-        m_b = __ldg(a.seg_begin + base + lane);
-        m_e = __ldg(a.seg_end + base + lane);
-      }
-      uint32_t b = __shfl_sync(0xffffffffu, m_b, 0), e = __shfl_sync(0xffffffffu, m_e, 0);
-      uint32_t my_j = 0;
-      double my_a = 0.0;
-      if (uint32_t(lane) < e - b) {
-        my_j = __ldg(a.col + b + lane);
-        my_a = double(__ldg(a.vald + b + lane));
-      }
-      for (int k = 0; k < cnt; ++k) {
-        const uint32_t flag = __shfl_sync(0xffffffffu, m_flag, k);
-        const uint32_t row = flag & ~SEG_FIRST;
-        // the next segment's items, in flight during this segment's gathers
-        uint32_t nb = __shfl_sync(0xffffffffu, m_b, (k + 1) & 31), ne = __shfl_sync(0xffffffffu, m_e, (k + 1) & 31);
-        uint32_t nx_j = 0;
-        double nx_a = 0.0;
-        if (k + 1 < cnt && uint32_t(lane) < ne - nb) {
-          nx_j = __ldg(a.col + nb + lane);
-          nx_a = double(__ldg(a.vald + nb + lane));
-        }
-        double rr_[CPT];
-        load_cols<K, V>(a.r, row, c0, rr_);
-        const double di = double(__ldg(a.dinv + row));
-        const double d = (flag & SEG_FIRST) ? double(__ldg(a.diag + row)) : 0.0;
-        double acc[CPT];
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
-        warp_gather<K, V>(my_j, my_a, e - b, a.r, c0, acc);
-        const size_t sg = base + size_t(k);
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-          a.seg_buf[sg * K + c0 + c] = V(acc[c]);
-          double u = di * rr_[c];
-          v[0][c] += u * (d * u - acc[c]);
-        }
-        b = nb;
-        e = ne;
-        my_j = nx_j;
-        my_a = nx_a;
       }
     }
   } else {
@@ -501,7 +453,7 @@ __device__ __forceinline__ void cg_update_row(const PersistentPcg<K, V>& a, size
   }
 }
 
-template <int K, typename V, bool CONTIG>
+template <int K, typename V>
 __device__ __forceinline__ void cg_update(const PersistentPcg<K, V>& a, size_t gid, size_t ngroups, int c0,
                                           bool carry, const double* s_alpha_it, const double* s_beta,
                                           double* partial, double (*sm)[2][K]) {
@@ -509,36 +461,13 @@ __device__ __forceinline__ void cg_update(const PersistentPcg<K, V>& a, size_t g
   double w2[2][CPT];
 #pragma unroll
   for (int c = 0; c < CPT; ++c) w2[0][c] = w2[1][c] = 0.0;
-  if constexpr (TPR == 32 && CONTIG) {
-    // a contiguous run of rows per warp; row scalars loaded lane-parallel
-    const int lane = threadIdx.x & 31;
-    const size_t lo = gid * a.n / ngroups, hi = (gid + 1) * a.n / ngroups;
-    for (size_t base = lo; base < hi; base += 32) {
-      const int cnt = int(hi - base < 32 ? hi - base : 32);
-      uint32_t m_s0 = 0, m_s1 = 0;
-      double m_dr = 0.0, m_di = 0.0;
-      if (lane < cnt) {
-        m_s0 = __ldg(a.row_first + base + lane);
-        m_s1 = __ldg(a.row_first + base + lane + 1);
-        m_dr = double(__ldg(a.diag + base + lane));
-        m_di = double(__ldg(a.dinv + base + lane));
-      }
-      for (int k = 0; k < cnt; ++k)
-        cg_update_row<K, V>(a, base + size_t(k), __shfl_sync(0xffffffffu, m_s0, k),
-                            __shfl_sync(0xffffffffu, m_s1, k), __shfl_sync(0xffffffffu, m_dr, k),
-                            __shfl_sync(0xffffffffu, m_di, k), c0, carry, s_alpha_it, s_beta, w2);
-    }
-  } else {
-    for (size_t row = gid; row < a.n; row += ngroups)
-      cg_update_row<K, V>(a, row, a.row_first[row], a.row_first[row + 1], double(a.diag[row]),
-                          double(a.dinv[row]), c0, carry, s_alpha_it, s_beta, w2);
-  }
+  for (size_t row = gid; row < a.n; row += ngroups)
+    cg_update_row<K, V>(a, row, a.row_first[row], a.row_first[row + 1], double(a.diag[row]), double(a.dinv[row]), c0,
+                        carry, s_alpha_it, s_beta, w2);
   block_reduce_cols_big<K, 2>(w2, partial, sm);
 }
 
-// CONTIG: every warp owns a contiguous run of segments and of rows (loaded
-// lane-parallel, next segment prefetched) instead of the grid-strided order.
-template <int K, typename V = double, bool CONTIG = false>
+template <int K, typename V = double>
 __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent_cg(PersistentPcg<K, V> a) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
@@ -583,7 +512,7 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent_cg(Persis
       }
     }
     block_reduce_cols_big<K, 2>(w, base(0), (double(*)[2][K])s_red);
-    cg_products<K, V, CONTIG>(a, gid, ngroups, c0, base(0) + 2 * G * K, (double(*)[1][K])s_red);
+    cg_products<K, V>(a, gid, ngroups, c0, base(0) + 2 * G * K, (double(*)[1][K])s_red);
   }
   grid.sync();
 
@@ -628,10 +557,10 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent_cg(Persis
     par ^= 1;
 
     // ---- F: w = diag u - sum(segments); p, s, x, r; gamma and r.r of the new r
-    cg_update<K, V, CONTIG>(a, gid, ngroups, c0, it > 0, s_fin, s_beta, base(par), (double(*)[2][K])s_red);
+    cg_update<K, V>(a, gid, ngroups, c0, it > 0, s_fin, s_beta, base(par), (double(*)[2][K])s_red);
     grid.sync();
     // ---- S: products of the new u and delta
-    cg_products<K, V, CONTIG>(a, gid, ngroups, c0, base(par) + 2 * G * K, (double(*)[1][K])s_red);
+    cg_products<K, V>(a, gid, ngroups, c0, base(par) + 2 * G * K, (double(*)[1][K])s_red);
     grid.sync();
   }
   if (blockIdx.x == 0) {

@@ -821,10 +821,10 @@ int32_t fevcb_cmg_aggregate_v1(uint32_t vertices, const uint32_t *row_ptr, const
                                double low_degree_threshold, uint32_t *labels, uint32_t *aggregates);
 
 /* Time standalone launches of one hot kernel of a solved generation with CUDA
- * events, L2 flushed before each launch.  kernel: 1 persistent blocked PCG
- * (two grid barriers per iteration, 20 iterations per launch), 3 leverage
- * atoms + cell sums, 4 leverage moments, 5 persistent blocked PCG in the
- * three-barrier form (20 iterations per launch).
+ * events, L2 flushed before each launch.  kernel: 1 the persistent blocked
+ * PCG form the solver uses at this block width (20 iterations per launch),
+ * 3 leverage atoms + cell sums, 4 leverage moments, 5 the three-barrier and
+ * 6 the two-barrier persistent PCG (20 iterations per launch).
  * Outputs mean milliseconds per launch and algorithmic bytes per launch. */
 int32_t fevcb_engine_kernel_benchmark_v1(uint64_t generation, uint32_t kernel, uint32_t block_columns,
                                          uint32_t launches, double *ms_per_launch, double *bytes_per_launch);
