@@ -96,6 +96,8 @@ struct Prepared {
   uint32_t precision = 0;         // device option: 1 mixed-precision inner solves
   SolveOptions last_options;
   bool solved_once = false;
+  uint64_t topology_checksum = 0;            // of the compressed problem, computed on request
+  bool checksum_ready = false;
   uint32_t solve_version = 0;                // request version of the last solve: 1, 4, 5 or 8
   VckssEngineSolveRequestV4 last_request{};  // the last V4+ request (capability and batch fields)
 };
@@ -554,7 +556,7 @@ VckssEngineDetailedReceiptV7 detailed_receipt(uint64_t g, const Prepared& p, con
   };
   v2.accounting_residual = std::max({identity(res.plugin), identity(res.correction), identity(res.corrected)});
   for (const Components& dr : res.target_draws) v2.accounting_residual = std::max(v2.accounting_residual, identity(dr));
-  v2.topology_checksum = p.problem.topology_checksum;
+  v2.topology_checksum = p.topology_checksum;
   if (o.preconditioner == 2) {
     v2.cmg_levels = st.levels;
     v2.cmg_fine_vertices = st.vertices;
@@ -656,6 +658,10 @@ const SolveResult& solved_result(uint64_t g, Prepared*& p, const char* phase) {
     res.weighted_rss_ready = true;
   }
   if (p->device && !p->plan.generic) device_unit_detail(*p->device, res);
+  if (!p->checksum_ready) {
+    p->topology_checksum = compressed_topology_checksum(p->problem);
+    p->checksum_ready = true;
+  }
   return res;
 }
 }  // namespace

@@ -1964,6 +1964,7 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
     case 1:
     case 5:
     case 6:
+    case 7:
       // persistent PCG, per launch of `iters` iterations: matrix + segment
       // tables once per iteration, nine passes over n x K vectors (two-barrier
       // form: r gathered; r, p, A p, x read and written; three-barrier form:
@@ -1985,25 +1986,29 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
   }
   float total = 0.0f;
   for (int i = 0; i < launches; ++i) {
-    if (kernel == 1 || kernel == 5 || kernel == 6) {
+    if (kernel == 1 || kernel >= 5) {
       // a fresh, never-converging block (tolerance 0) so every launch runs `iters` iterations
       k_fill_pattern<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p);
       k_colsum_abs<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p, e.partial.p);
       finish(e.partial.p, L.grid, 2 * K, w.tot.p, L.s);
       k_pcg_init_state<K><<<1, 128, 0, L.s>>>(w.tot.p, K, 0.0, double(e.n), w.s);
-      pcg_restart<K>(e, w, L, true, kernel == 5 || (kernel == 1 && !two_barrier_form<K, double>()));
+      pcg_restart<K>(e, w, L, true, kernel == 5 || kernel == 7 || (kernel == 1 && !two_barrier_form<K, double>()));
     }
     CK(cudaMemsetAsync(flush.p, i & 0xff, flush.bytes(), L.s));
     CK(cudaEventRecord(e.ev0, L.s));
     switch (kernel) {
       case 1:
       case 5:
-      case 6: {
+      case 6:
+      case 7: {
         PersistentPcg<K> a = persistent_args<K>(e, w, iters);
         void* args[] = {&a};
-        // 1: the form the solver uses at this width; 5: three barriers; 6: two barriers
+        // 1: the form the solver uses at this width; 5: three barriers; 6: two
+        // barriers; 7: three barriers with the warp-broadcast gather
         const bool two = kernel == 6 || (kernel == 1 && two_barrier_form<K, double>());
-        const void* fn = two ? (const void*)k_pcg_persistent_cg<K> : (const void*)k_pcg_persistent<K>;
+        const void* fn = kernel == 7 ? (const void*)k_pcg_persistent<K, double, true>
+                         : two      ? (const void*)k_pcg_persistent_cg<K>
+                                    : (const void*)k_pcg_persistent<K>;
         CK(cudaLaunchCooperativeKernel(fn, dim3(e.coop_blocks), dim3(PERSIST_THREADS), args, 0, L.s));
         break;
       }
@@ -2031,7 +2036,7 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
   }
   CK_LAUNCH();
   *ms = double(total) / launches;
-  if (kernel == 1 || kernel == 5 || kernel == 6) {
+  if (kernel == 1 || kernel >= 5) {
     // report the iterations actually executed (a curvature breakdown would stop early)
     std::vector<int> it(K);
     CK(cudaMemcpy(it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost));

@@ -177,7 +177,9 @@ __device__ __forceinline__ void segment_gather(const uint32_t* __restrict__ col,
   }
 }
 
-template <int K, typename V = double>
+// WARP_GATHER: with one warp per segment, load the segment's columns and
+// values lane-parallel and gather by shuffle (warp_gather) in phase A.
+template <int K, typename V = double, bool WARP_GATHER = false>
 __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(PersistentPcg<K, V> a) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
@@ -213,6 +215,17 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(Persisten
 #pragma unroll
       for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
       uint32_t i = b;
+      if constexpr (WARP_GATHER && TPR == 32) {
+        const int lane = threadIdx.x & 31;
+        uint32_t my_j = 0;
+        double my_a = 0.0;
+        if (uint32_t(lane) < e - b) {
+          my_j = __ldg(a.col + b + lane);
+          my_a = double(__ldg(a.val + b + lane));
+        }
+        warp_gather<K, V>(my_j, my_a, e - b, a.p, c0, acc);
+        i = e;
+      }
       for (; i + 2 <= e; i += 2) {
         uint32_t j0 = __ldg(a.col + i), j1 = __ldg(a.col + i + 1);
         double a0 = double(__ldg(a.val + i)), a1 = double(__ldg(a.val + i + 1));

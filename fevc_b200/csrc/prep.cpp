@@ -7,6 +7,9 @@
 #include "radix.h"
 
 #include <algorithm>
+#include <functional>
+#include <exception>
+#include <thread>
 #include <cstring>
 #include <numeric>
 
@@ -161,11 +164,16 @@ size_t count_true(const std::vector<uint8_t>& m) {
   return c;
 }
 
-// Bipartite graph with workers 0..W-1 and firms W..W+F-1 in CSR form.
+// Bipartite graph with workers 0..W-1 and firms W..W+F-1 in CSR form; an arc
+// holds its head and its undirected edge id together (one cache line per
+// visit in the traversals).
+struct Arc {
+  uint32_t to, edge;
+};
 struct Graph {
   size_t nodes = 0, edges = 0;
   std::vector<uint64_t> ptr;
-  std::vector<uint32_t> to, edge;
+  std::vector<Arc> arc;
 };
 
 Graph make_graph(size_t nodes, const std::vector<uint32_t>& eu, const std::vector<uint32_t>& ev) {
@@ -178,15 +186,11 @@ Graph make_graph(size_t nodes, const std::vector<uint32_t>& eu, const std::vecto
     g.ptr[ev[e] + 1]++;
   }
   for (size_t v = 0; v < nodes; ++v) g.ptr[v + 1] += g.ptr[v];
-  g.to.resize(2 * eu.size());
-  g.edge.resize(2 * eu.size());
+  g.arc.resize(2 * eu.size());
   std::vector<uint64_t> cur(g.ptr.begin(), g.ptr.end() - 1);
   for (size_t e = 0; e < eu.size(); ++e) {
-    uint64_t a = cur[eu[e]]++, b = cur[ev[e]]++;
-    g.to[a] = ev[e];
-    g.edge[a] = uint32_t(e);
-    g.to[b] = eu[e];
-    g.edge[b] = uint32_t(e);
+    g.arc[cur[eu[e]]++] = Arc{ev[e], uint32_t(e)};
+    g.arc[cur[ev[e]]++] = Arc{eu[e], uint32_t(e)};
   }
   return g;
 }
@@ -235,7 +239,7 @@ ComponentResult largest_component(const Canonical& in, const std::vector<uint8_t
     for (size_t h = 0; h < queue.size(); ++h) {
       uint32_t v = queue[h];
       for (uint64_t a = g.ptr[v]; a < g.ptr[v + 1]; ++a) {
-        uint32_t u = g.to[a];
+        uint32_t u = g.arc[a].to;
         if (label[u] == MISSING) {
           label[u] = uint32_t(comps);
           queue.push_back(u);
@@ -302,47 +306,63 @@ std::vector<uint64_t> worker_physical_counts(const Canonical& in, const std::vec
 // Articulation vertices and bridges are properties of the graph, independent
 // of the traversal order (reference `articulation_vertices` graph.rs:872-936
 // and `bridge_edges` graph.rs:1031-1088).
-void tarjan(const Graph& g, std::vector<uint8_t>* articulation, std::vector<uint8_t>* bridge) {
-  size_t n = g.nodes;
-  std::vector<uint64_t> disc(n, 0), low(n, 0), next(n, 0);
-  std::vector<uint32_t> parent(n, MISSING), parent_edge(n, MISSING), children(n, 0);
+// edge_on: optional per-edge mask; masked-off edges are absent and a vertex
+// with no edge left is not part of the graph.
+void tarjan(const Graph& g, std::vector<uint8_t>* articulation, std::vector<uint8_t>* bridge,
+            const std::vector<uint8_t>* edge_on = nullptr) {
+  // per-vertex DFS state in one record (discovery time, low link, parent,
+  // parent edge, next arc): a visit touches one cache line
+  struct Node {
+    uint32_t disc = 0, low = 0, parent = MISSING, parent_edge = MISSING;
+    uint64_t next = 0;
+  };
+  const size_t n = g.nodes;
+  if (n >= MISSING) fail(RESOURCE_LIMIT, "graph", "graph has too many vertices");
+  std::vector<Node> st(n);
   if (articulation) articulation->assign(n, 0);
   if (bridge) bridge->assign(g.edges, 0);
-  uint64_t clock = 0;
+  uint32_t clock = 0;
   std::vector<uint32_t> stack;
   for (size_t root = 0; root < n; ++root) {
-    if (g.ptr[root] == g.ptr[root + 1] || disc[root]) continue;
-    disc[root] = low[root] = ++clock;
-    next[root] = g.ptr[root];
+    if (st[root].disc) continue;
+    bool has_edge = false;
+    for (uint64_t a = g.ptr[root]; a < g.ptr[root + 1] && !has_edge; ++a)
+      has_edge = !edge_on || (*edge_on)[g.arc[a].edge];
+    if (!has_edge) continue;
+    st[root].disc = st[root].low = ++clock;
+    st[root].next = g.ptr[root];
+    uint32_t root_children = 0;
     stack.clear();
     stack.push_back(uint32_t(root));
     while (!stack.empty()) {
       uint32_t v = stack.back();
-      if (next[v] < g.ptr[v + 1]) {
-        uint64_t a = next[v]++;
-        uint32_t u = g.to[a], e = g.edge[a];
-        if (e == parent_edge[v]) continue;
-        if (!disc[u]) {
-          parent[u] = v;
-          parent_edge[u] = e;
-          children[v]++;
-          disc[u] = low[u] = ++clock;
-          next[u] = g.ptr[u];
-          stack.push_back(u);
+      Node& sv = st[v];
+      if (sv.next < g.ptr[v + 1]) {
+        const Arc arc = g.arc[sv.next++];
+        if (arc.edge == sv.parent_edge || (edge_on && !(*edge_on)[arc.edge])) continue;
+        Node& su = st[arc.to];
+        if (!su.disc) {
+          su.parent = v;
+          su.parent_edge = arc.edge;
+          root_children += v == root;
+          su.disc = su.low = ++clock;
+          su.next = g.ptr[arc.to];
+          stack.push_back(arc.to);
         } else {
-          low[v] = std::min(low[v], disc[u]);
+          sv.low = std::min(sv.low, su.disc);
         }
       } else {
         stack.pop_back();
-        uint32_t p = parent[v];
+        uint32_t p = sv.parent;
         if (p != MISSING) {
-          if (bridge && low[v] > disc[p]) (*bridge)[parent_edge[v]] = 1;
-          low[p] = std::min(low[p], low[v]);
-          if (articulation && parent[p] != MISSING && low[v] >= disc[p]) (*articulation)[p] = 1;
+          Node& sp = st[p];
+          if (bridge && sv.low > sp.disc) (*bridge)[sv.parent_edge] = 1;
+          sp.low = std::min(sp.low, sv.low);
+          if (articulation && sp.parent != MISSING && sv.low >= sp.disc) (*articulation)[p] = 1;
         }
       }
     }
-    if (articulation) (*articulation)[root] = children[root] > 1;
+    if (articulation) (*articulation)[root] = root_children > 1;
   }
 }
 
@@ -386,6 +406,221 @@ std::vector<uint32_t> deletion_bridges(const Canonical& in, const std::vector<ui
   return out;
 }
 
+// Run independent tasks on their own threads; after all finish the first
+// exception in task order is rethrown (the error a sequential run reports).
+void run_tasks(const std::vector<std::function<void()>>& tasks) {
+  std::vector<std::exception_ptr> err(tasks.size());
+  std::vector<std::thread> th;
+  for (size_t i = 1; i < tasks.size(); ++i)
+    th.emplace_back([&, i] {
+      try {
+        tasks[i]();
+      } catch (...) {
+        err[i] = std::current_exception();
+      }
+    });
+  try {
+    if (!tasks.empty()) tasks[0]();
+  } catch (...) {
+    err[0] = std::current_exception();
+  }
+  for (auto& t : th) t.join();
+  for (auto& e : err)
+    if (e) std::rethrow_exception(e);
+}
+
+// Run two independent tasks on two threads; the first exception (a's first)
+// is rethrown after both finish.
+template <class A, class B>
+void run_side_by_side(A&& a, B&& b) {
+  std::exception_ptr ea, eb;
+  std::thread t([&] {
+    try {
+      b();
+    } catch (...) {
+      eb = std::current_exception();
+    }
+  });
+  try {
+    a();
+  } catch (...) {
+    ea = std::current_exception();
+  }
+  t.join();
+  if (ea) std::rethrow_exception(ea);
+  if (eb) std::rethrow_exception(eb);
+}
+
+// Deletion units of the canonical input (each lies in one worker-firm
+// coordinate, which canonicalisation checked): worker, firm, coordinate, row
+// count and physical mass.
+struct UnitTable {
+  std::vector<uint32_t> worker, firm, coord;
+  std::vector<uint64_t> rows, mass;
+};
+
+UnitTable unit_table(const Canonical& in) {
+  const size_t D = in.deletion_units;
+  UnitTable u;
+  u.worker.assign(D, MISSING);
+  u.firm.assign(D, MISSING);
+  u.coord.assign(D, MISSING);
+  u.rows.assign(D, 0);
+  u.mass.assign(D, 0);
+  for (size_t r = 0; r < in.rows(); ++r) {
+    uint32_t d = in.deletion[r];
+    if (u.worker[d] == MISSING) {
+      u.worker[d] = in.worker[r];
+      u.firm[d] = in.firm[r];
+      u.coord[d] = in.coord[r];
+    }
+    u.rows[d] += 1;
+    u.mass[d] += in.frequency[r];
+  }
+  return u;
+}
+
+uint64_t active_rows(const UnitTable& u, const std::vector<uint8_t>& act) {
+  uint64_t n = 0;
+  for (size_t d = 0; d < act.size(); ++d)
+    if (act[d]) n += u.rows[d];
+  return n;
+}
+
+// The coordinate graph of all rows (edge id = coordinate) and the deletion
+// multigraph of all units (edge id = unit), built once; the fixed point masks
+// edges off instead of rebuilding (`coordinate_graph` of the active rows has
+// exactly the coordinates of the active units).
+struct UnitGraphs {
+  Graph coords, units;
+  std::vector<uint8_t> coord_on;
+};
+
+UnitGraphs unit_graphs(const Canonical& in, const UnitTable& u) {
+  UnitGraphs g;
+  std::vector<uint32_t> eu(in.coord_worker.size()), ev(in.coord_worker.size());
+  for (size_t c = 0; c < eu.size(); ++c) {
+    eu[c] = in.coord_worker[c];
+    ev[c] = uint32_t(in.workers + in.coord_firm[c]);
+  }
+  g.coords = make_graph(in.workers + in.firms, eu, ev);
+  eu.resize(u.worker.size());
+  ev.resize(u.worker.size());
+  for (size_t d = 0; d < u.worker.size(); ++d) {
+    eu[d] = u.worker[d];
+    ev[d] = uint32_t(in.workers + u.firm[d]);
+  }
+  g.units = make_graph(in.workers + in.firms, eu, ev);
+  g.coord_on.assign(in.coord_worker.size(), 0);
+  return g;
+}
+
+// coordinates with an active unit
+void mark_coords(const UnitTable& u, const std::vector<uint8_t>& act, UnitGraphs& g) {
+  std::fill(g.coord_on.begin(), g.coord_on.end(), 0);
+  bool any = false;
+  for (size_t d = 0; d < act.size(); ++d)
+    if (act[d]) {
+      g.coord_on[u.coord[d]] = 1;
+      any = true;
+    }
+  if (!any) fail(GRAPH_EMPTY, "graph", "active graph is empty");
+}
+
+struct UnitComponents {
+  std::vector<uint8_t> keep;  // per unit
+  size_t components = 0;
+  uint64_t retained_rows = 0;
+};
+
+// `largest_component` over the active units' rows: components by (firm count,
+// physical mass), a tie for the maximum is an identification error.
+UnitComponents unit_largest_component(const Canonical& in, const UnitTable& u, const std::vector<uint8_t>& act,
+                                      UnitGraphs& gs) {
+  mark_coords(u, act, gs);
+  const Graph& g = gs.coords;
+  const std::vector<uint8_t>& on = gs.coord_on;
+  std::vector<uint32_t> label(g.nodes, MISSING), queue;
+  queue.reserve(g.nodes);
+  size_t comps = 0;
+  for (size_t root = 0; root < g.nodes; ++root) {
+    if (label[root] != MISSING) continue;
+    bool has_edge = false;
+    for (uint64_t a = g.ptr[root]; a < g.ptr[root + 1] && !has_edge; ++a) has_edge = on[g.arc[a].edge];
+    if (!has_edge) continue;
+    label[root] = uint32_t(comps);
+    queue.clear();
+    queue.push_back(uint32_t(root));
+    for (size_t h = 0; h < queue.size(); ++h) {
+      uint32_t v = queue[h];
+      for (uint64_t a = g.ptr[v]; a < g.ptr[v + 1]; ++a)
+        if (on[g.arc[a].edge] && label[g.arc[a].to] == MISSING) {
+          label[g.arc[a].to] = uint32_t(comps);
+          queue.push_back(g.arc[a].to);
+        }
+    }
+    ++comps;
+  }
+  if (comps == 0) fail(GRAPH_EMPTY, "graph", "no connected worker-firm component remains");
+  std::vector<uint64_t> firms(comps, 0), mass(comps, 0);
+  for (size_t f = 0; f < in.firms; ++f) {
+    uint32_t c = label[in.workers + f];
+    if (c != MISSING) firms[c]++;
+  }
+  for (size_t d = 0; d < act.size(); ++d) {
+    if (!act[d]) continue;
+    uint32_t c = label[u.worker[d]];
+    if (c == MISSING) fail(INTERNAL_INVARIANT_FAILED, "graph", "active row has no connected-component label");
+    mass[c] += u.mass[d];
+  }
+  size_t best = 0;
+  for (size_t c = 1; c < comps; ++c)
+    if (firms[c] > firms[best] || (firms[c] == firms[best] && mass[c] > mass[best])) best = c;
+  size_t winners = 0;
+  for (size_t c = 0; c < comps; ++c) winners += (firms[c] == firms[best] && mass[c] == mass[best]);
+  if (winners != 1)
+    fail(GRAPH_UNIDENTIFIED, "graph", "multiple connected components tie for largest-component selection");
+  UnitComponents out;
+  out.components = comps;
+  out.keep.resize(act.size());
+  for (size_t d = 0; d < act.size(); ++d) {
+    out.keep[d] = act[d] && label[u.worker[d]] == best;
+    if (out.keep[d]) out.retained_rows += u.rows[d];
+  }
+  return out;
+}
+
+// `worker_articulations` of the active units' coordinate graph.
+std::vector<uint8_t> unit_articulations(const Canonical& in, const UnitTable& u, const std::vector<uint8_t>& act,
+                                        UnitGraphs& gs) {
+  mark_coords(u, act, gs);
+  std::vector<uint8_t> art;
+  tarjan(gs.coords, &art, nullptr, &gs.coord_on);
+  art.resize(in.workers);
+  return art;
+}
+
+// `distinct_deletion_counts`: active units per worker.
+std::vector<uint64_t> unit_counts(const Canonical& in, const UnitTable& u, const std::vector<uint8_t>& act) {
+  std::vector<uint64_t> counts(in.workers, 0);
+  for (size_t d = 0; d < act.size(); ++d)
+    if (act[d]) counts[u.worker[d]]++;
+  return counts;
+}
+
+// `deletion_bridges`: the active units as multigraph edges, bridges by id.
+std::vector<uint32_t> unit_bridges(const std::vector<uint8_t>& act, const UnitGraphs& gs) {
+  bool any = false;
+  for (uint8_t a : act) any |= a != 0;
+  if (!any) fail(GRAPH_EMPTY, "graph", "active graph is empty");
+  std::vector<uint8_t> br;
+  tarjan(gs.units, nullptr, &br, &act);
+  std::vector<uint32_t> out;
+  for (size_t d = 0; d < act.size(); ++d)
+    if (act[d] && br[d]) out.push_back(uint32_t(d));
+  return out;
+}
+
 size_t active_deletion_count(const Canonical& in, const std::vector<uint8_t>& active) {
   std::vector<uint8_t> seen(in.deletion_units, 0);
   size_t c = 0;
@@ -426,24 +661,34 @@ InputColumns copy_columns(uint64_t rows, const double* worker, const double* fir
                           const double* outcome, const double* frequency, const double* target,
                           const double* const* controls, uint32_t controls_count, const double* probe_order) {
   InputColumns c;
-  c.worker = copy_integer(worker, rows, "worker identifier", INVALID_IDENTIFIER);
-  c.firm = copy_integer(firm, rows, "firm identifier", INVALID_IDENTIFIER);
-  c.deletion = copy_integer(deletion, rows, "deletion identifier", INVALID_IDENTIFIER);
-  c.outcome = copy_finite(outcome, rows, "outcome");
-  c.frequency = copy_integer(frequency, rows, "frequency weight", INVALID_WEIGHT);
-  if (!target) fail(INVALID_INPUT, "engine_ingest", "target weight pointer is null");
-  c.target.assign(target, target + rows);
-  for (uint64_t r = 0; r < rows; ++r)
-    if (!std::isfinite(c.target[r]) || c.target[r] < 0.0)
-      fail(INVALID_TARGET_WEIGHT, "engine_ingest",
-           "target weight is negative or nonfinite at zero-based row " + std::to_string(r));
-  if (controls_count == 0) {
-    if (controls) fail(INVALID_INPUT, "engine_prepare", "zero controls require a null control-pointer array");
-  } else {
-    if (!controls) fail(INVALID_INPUT, "engine_prepare", "positive control count requires a control-pointer array");
-    for (uint32_t k = 0; k < controls_count; ++k) c.controls.push_back(copy_finite(controls[k], rows, "control"));
-  }
-  if (probe_order) c.probe_order = copy_finite(probe_order, rows, "probe-order value");
+  c.controls.resize(controls_count);
+  // every column is copied and checked on its own thread; the error reported
+  // is the one of the first failing column in this order
+  std::vector<std::function<void()>> tasks = {
+      [&] { c.worker = copy_integer(worker, rows, "worker identifier", INVALID_IDENTIFIER); },
+      [&] { c.firm = copy_integer(firm, rows, "firm identifier", INVALID_IDENTIFIER); },
+      [&] { c.deletion = copy_integer(deletion, rows, "deletion identifier", INVALID_IDENTIFIER); },
+      [&] { c.outcome = copy_finite(outcome, rows, "outcome"); },
+      [&] { c.frequency = copy_integer(frequency, rows, "frequency weight", INVALID_WEIGHT); },
+      [&] {
+        if (!target) fail(INVALID_INPUT, "engine_ingest", "target weight pointer is null");
+        c.target.assign(target, target + rows);
+        for (uint64_t r = 0; r < rows; ++r)
+          if (!std::isfinite(c.target[r]) || c.target[r] < 0.0)
+            fail(INVALID_TARGET_WEIGHT, "engine_ingest",
+                 "target weight is negative or nonfinite at zero-based row " + std::to_string(r));
+      },
+      [&] {
+        if (controls_count == 0 && controls)
+          fail(INVALID_INPUT, "engine_prepare", "zero controls require a null control-pointer array");
+        if (controls_count > 0 && !controls)
+          fail(INVALID_INPUT, "engine_prepare", "positive control count requires a control-pointer array");
+      }};
+  if (controls)
+    for (uint32_t k = 0; k < controls_count; ++k)
+      tasks.push_back([&, k] { c.controls[k] = copy_finite(controls[k], rows, "control"); });
+  if (probe_order) tasks.push_back([&] { c.probe_order = copy_finite(probe_order, rows, "probe-order value"); });
+  run_tasks(tasks);
   return c;
 }
 
@@ -476,16 +721,18 @@ Canonical canonicalize(InputColumns&& in, bool implicit_match) {
 
   Canonical c;
   std::vector<uint64_t> wl, fl, dl;
-  c.worker = redense(in.worker, wl, "worker");
-  c.firm = redense(in.firm, fl, "firm");
+  // the three identifier columns are relabelled side by side (the implicit
+  // match keys need the dense worker and firm ids first)
+  std::vector<std::function<void()>> tasks = {[&] { c.worker = redense(in.worker, wl, "worker"); },
+                                              [&] { c.firm = redense(in.firm, fl, "firm"); }};
+  if (!implicit_match) tasks.push_back([&] { c.deletion = redense(in.deletion, dl, "deletion"); });
+  run_tasks(tasks);
   c.workers = wl.size();
   c.firms = fl.size();
   if (implicit_match) {
     std::vector<uint64_t> keys(n);
     for (size_t r = 0; r < n; ++r) keys[r] = uint64_t(c.worker[r]) * c.firms + c.firm[r] + 1;
     c.deletion = redense(keys, dl, "deletion");
-  } else {
-    c.deletion = redense(in.deletion, dl, "deletion");
   }
   c.deletion_units = dl.size();
   {
@@ -500,7 +747,6 @@ Canonical canonicalize(InputColumns&& in, bool implicit_match) {
       }
     }
   }
-  c.topology_checksum = topology_checksum(c.worker, c.firm, c.deletion, in.frequency);
   {
     // distinct (worker, firm) coordinates in (worker, firm) order: rows
     // bucketed by worker, each worker's rows ordered by firm
@@ -542,71 +788,86 @@ Canonical canonicalize(InputColumns&& in, bool implicit_match) {
 
 std::vector<uint8_t> select_match_graph(const Canonical& in, GraphReceipt& rc) {
   if (in.rows() == 0) fail(GRAPH_EMPTY, "graph", "command sample is empty");
-  std::vector<uint8_t> active(in.rows(), 1);
+  // Every step of the match fixed point keeps or drops whole deletion units
+  // (components and movers by worker, articulation workers, bridge units), so
+  // it runs on the units; the row mask is read off at the end.
+  const UnitTable u = unit_table(in);
+  UnitGraphs gs = unit_graphs(in, u);
+  const size_t D = u.worker.size();
+  std::vector<uint8_t> act(D, 1);
   rc = GraphReceipt{};
   rc.input_rows = in.rows();
   rc.input_physical_mass = in.physical_total;
 
-  ComponentResult initial = largest_component(in, active);
+  UnitComponents initial = unit_largest_component(in, u, act, gs);
   rc.initial_components = initial.components;
   rc.maximum_components = initial.components;
   rc.initial_component_rows = initial.retained_rows;
-  intersect(active, initial.keep);
+  act.swap(initial.keep);
 
   {
-    auto units = distinct_deletion_counts(in, active);
-    for (size_t r = 0; r < in.rows(); ++r)
-      if (active[r]) active[r] = units[in.worker[r]] > 1;
+    auto units = unit_counts(in, u, act);
+    for (size_t d = 0; d < D; ++d)
+      if (act[d]) act[d] = units[u.worker[d]] > 1;
   }
-  size_t movers = count_true(active);
+  uint64_t movers = active_rows(u, act);
   rc.mover_input_rows = movers;
   if (movers == 0) fail(GRAPH_EMPTY, "graph", "no observations remain in the mover target population");
-  ComponentResult mover = largest_component(in, active);
+  UnitComponents mover = unit_largest_component(in, u, act, gs);
   rc.maximum_components = std::max<uint64_t>(rc.maximum_components, mover.components);
-  intersect(active, mover.keep);
+  act.swap(mover.keep);
 
-  size_t initial_edges = active_deletion_count(in, active);
+  size_t initial_edges = count_true(act);
   rc.initial_deletion_edges = initial_edges;
   uint64_t bound = in.workers + initial_edges + 1;
 
+  // A step that only removed workers with one unit (leaves of one connected
+  // coordinate graph) cannot split it: the next component pass would keep
+  // everything and report one component, so it is skipped.
+  bool connected = false;
   for (;;) {
     if (rc.fixed_point_iterations > bound)
       fail(GRAPH_CERTIFICATE_FAILED, "graph", "sample fixed-point pruning exceeded its finite iteration bound");
-    ComponentResult comp = largest_component(in, active);
-    rc.maximum_components = std::max<uint64_t>(rc.maximum_components, comp.components);
-    intersect(active, comp.keep);
-    if (count_true(active) == 0) fail(GRAPH_EMPTY, "graph", "no component remains after fixed-point pruning");
+    if (!connected) {
+      UnitComponents comp = unit_largest_component(in, u, act, gs);
+      rc.maximum_components = std::max<uint64_t>(rc.maximum_components, comp.components);
+      act.swap(comp.keep);
+    }
+    connected = false;
+    if (count_true(act) == 0) fail(GRAPH_EMPTY, "graph", "no component remains after fixed-point pruning");
 
-    auto units = distinct_deletion_counts(in, active);
+    auto units = unit_counts(in, u, act);
     size_t removed = 0;
     for (size_t w = 0; w < in.workers; ++w) removed += units[w] == 1;
     if (removed) {
-      for (size_t r = 0; r < in.rows(); ++r)
-        if (active[r] && units[in.worker[r]] == 1) active[r] = 0;
+      for (size_t d = 0; d < D; ++d)
+        if (act[d] && units[u.worker[d]] == 1) act[d] = 0;
       rc.insufficient_workers_removed += removed;
       rc.degree_iterations++;
       rc.fixed_point_iterations++;
+      connected = true;
       continue;
-    } auto art = worker_articulations(in, active);
+    }
+    // articulation workers and bridge units of the same state, side by side;
+    // the bridges are used only when there is no articulation
+    std::vector<uint8_t> art;
+    std::vector<uint32_t> bridges;
+    run_side_by_side([&] { art = unit_articulations(in, u, act, gs); }, [&] { bridges = unit_bridges(act, gs); });
     size_t arts = count_true(art);
     if (arts) {
-      for (size_t r = 0; r < in.rows(); ++r)
-        if (active[r] && art[in.worker[r]]) active[r] = 0;
+      for (size_t d = 0; d < D; ++d)
+        if (act[d] && art[u.worker[d]]) act[d] = 0;
       rc.articulation_workers_removed += arts;
       rc.articulation_iterations++;
       rc.fixed_point_iterations++;
       continue;
     }
-    auto bridges = deletion_bridges(in, active);
     if (bridges.empty()) break;
-    std::vector<uint8_t> is_bridge(in.deletion_units, 0);
-    for (uint32_t d : bridges) is_bridge[d] = 1;
-    size_t removed_rows = 0;
-    for (size_t r = 0; r < in.rows(); ++r)
-      if (active[r] && is_bridge[in.deletion[r]]) {
-        active[r] = 0;
-        ++removed_rows;
-      }
+    uint64_t removed_rows = 0;
+    for (uint32_t d : bridges) {
+      act[d] = 0;
+      removed_rows += u.rows[d];
+    }
     rc.bridge_units_removed += bridges.size();
     rc.bridge_rows_removed += removed_rows;
     rc.bridge_iterations++;
@@ -614,23 +875,31 @@ std::vector<uint8_t> select_match_graph(const Canonical& in, GraphReceipt& rc) {
   }
   if (rc.fixed_point_iterations > bound)
     fail(GRAPH_CERTIFICATE_FAILED, "graph", "sample fixed-point pruning exceeded its finite iteration bound");
-  ComponentResult fin = largest_component(in, active);
+  UnitComponents fin = unit_largest_component(in, u, act, gs);
   rc.maximum_components = std::max<uint64_t>(rc.maximum_components, fin.components);
-  intersect(active, fin.keep);
-  if (!deletion_bridges(in, active).empty())
-    fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained deletion-unit multigraph still contains a bridge"); if (count_true(worker_articulations(in, active)))
-    fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained graph still contains a worker articulation");
+  act.swap(fin.keep);
   {
-    auto units = distinct_deletion_counts(in, active);
-    for (uint64_t u : units)
-      if (u == 1) fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained graph still contains a one-deletion-unit worker");
+    std::vector<uint8_t> art;
+    std::vector<uint32_t> bridges;
+    run_side_by_side([&] { art = unit_articulations(in, u, act, gs); }, [&] { bridges = unit_bridges(act, gs); });
+    if (!bridges.empty())
+      fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained deletion-unit multigraph still contains a bridge");
+    if (count_true(art))
+      fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained graph still contains a worker articulation");
   }
-  size_t kept = count_true(active);
+  {
+    auto units = unit_counts(in, u, act);
+    for (uint64_t c : units)
+      if (c == 1) fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained graph still contains a one-deletion-unit worker");
+  }
+  uint64_t kept = active_rows(u, act);
   if (kept == 0) fail(GRAPH_EMPTY, "graph", "no component remains after fixed-point graph pruning");
   rc.retained_rows = kept;
-  for (size_t r = 0; r < in.rows(); ++r)
-    if (active[r]) rc.retained_physical_mass += in.frequency[r];
-  rc.retained_deletion_edges = active_deletion_count(in, active);
+  for (size_t d = 0; d < D; ++d)
+    if (act[d]) rc.retained_physical_mass += u.mass[d];
+  rc.retained_deletion_edges = count_true(act);
+  std::vector<uint8_t> active(in.rows());
+  for (size_t r = 0; r < in.rows(); ++r) active[r] = act[in.deletion[r]];
   return active;
 }
 
@@ -691,7 +960,8 @@ std::vector<uint8_t> select_observation_graph(const Canonical& in, GraphReceipt&
       rc.degree_iterations++;
       rc.fixed_point_iterations++;
       continue;
-    } auto art = worker_articulations(in, active);
+    }
+    auto art = worker_articulations(in, active);
     size_t arts = count_true(art);
     if (arts == 0) break;
     for (size_t r = 0; r < in.rows(); ++r)
@@ -865,8 +1135,11 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
     p.probe_order.resize(R);
     for (size_t i = 0; i < R; ++i) p.probe_order[i] = in.probe_order[p.retained_rows[i]];
   }
-  p.topology_checksum = topology_checksum(p.row_worker, p.row_firm, p.row_deletion, p.frequency);
   return p;
+}
+
+uint64_t compressed_topology_checksum(const Compressed& p) {
+  return topology_checksum(p.row_worker, p.row_firm, p.row_deletion, p.frequency);
 }
 
 JlaPlan build_plan(const Compressed& p) {

@@ -33,7 +33,6 @@ struct Canonical {
   std::vector<double> probe_order;
   uint64_t physical_total = 0;
   double target_total = 0.0;
-  uint64_t topology_checksum = 0;
   size_t rows() const { return worker.size(); }
 };
 
@@ -67,7 +66,6 @@ struct Compressed {
   GroupIndex worker_index, firm_index, deletion_index, target_index;
   uint64_t physical_total = 0;
   double target_total = 0.0;
-  uint64_t topology_checksum = 0;
   size_t rows() const { return row_worker.size(); }
 };
 
@@ -112,6 +110,10 @@ std::vector<uint8_t> select_observation_graph(const Canonical& in, GraphReceipt&
 
 // Reference `compress_with_implicit_match_and_interrupt` (problem.rs:206-606).
 Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, bool implicit_match);
+// Reference `topology_checksum` of the compressed problem (problem.rs:1213-1248):
+// FNV-1a over its sorted (worker, firm, deletion, frequency) records; computed
+// on request (the detailed receipt reports it).
+uint64_t compressed_topology_checksum(const Compressed& p);
 
 // Reference `JlaPlan::build_no_controls_with_certified_match_and_interrupt`
 // (jla.rs:59-108) generalised: controls do not enter the plan's orderings.
