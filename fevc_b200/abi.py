@@ -512,6 +512,7 @@ SIGNATURES = {
     "fevcb_device_count": (i32, []),
     "fevcb_set_stream": (i32, [C.c_void_p]),
     "fevcb_device_cache_trim_v1": (i32, [C.POINTER(u64), C.POINTER(u64)]),
+    "fevcb_engine_hybrid_check_v1": (i32, [u64, C.POINTER(u32)]),
     "fevcb_engine_solve_options_v1": (i32, [u64, C.c_void_p]),
     "fevcb_engine_timings_v1": (i32, [u64, C.c_void_p, u32]),
     "fevcb_engine_resolve_v1": (i32, [u64]),

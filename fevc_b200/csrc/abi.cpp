@@ -1453,6 +1453,16 @@ int32_t fevcb_set_stream(void* stream) {
   return status([&] { set_device_stream(stream); });
 }
 
+int32_t fevcb_engine_hybrid_check_v1(uint64_t generation, uint32_t* identical) {
+  return status([&] {
+    if (!identical) fail(INVALID_INPUT, "engine_hybrid_check", "output pointer is null");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_hybrid_check");
+    if (!p.device) fail(STALE_CONTEXT, "engine_hybrid_check", "generation has no device state; solve it first");
+    *identical = device_hybrid_matches_host(*p.device, p.problem) ? 1u : 0u;
+  });
+}
+
 int32_t fevcb_device_cache_trim_v1(uint64_t* freed_bytes, uint64_t* cached_bytes) {
   return status([&] {
     uint64_t freed = device_cache_trim();

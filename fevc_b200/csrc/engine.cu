@@ -19,6 +19,7 @@
 #include <chrono>
 #include <exception>
 #include <thread>
+#include <type_traits>
 #include <functional>
 #include <cmath>
 #include <cstring>
@@ -32,6 +33,7 @@
 #include "learned.h"
 #include "multigrid.h"
 #include "persistent.cuh"
+#include "hybrid_device.cuh"
 #include "generic.cuh"
 #include "observation.cuh"
 
@@ -372,12 +374,12 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   e->S = uint32_t(plan.tgt_cell.size());
   e->target_total = p.target_total;
 
-  // Four independent host builders, each uploading what it builds: cells and
+  // Three independent host builders, each uploading what it builds: cells and
   // the firm segments; deletion units and then the generic row data (which
-  // reads the unit order); target strata; the hybrid Laplacian with its
-  // preconditioner.  They run on their own threads (bound to this device);
-  // their uploads share the engine's stream and fill disjoint buffers.
-  uint64_t task_h2d[4] = {0, 0, 0, 0};
+  // reads the unit order); target strata.  They run on their own threads
+  // (bound to this device); their uploads share the engine's stream and fill
+  // disjoint buffers.  The hybrid Laplacian is then assembled on the device.
+  uint64_t task_h2d[3] = {0, 0, 0};
   (void)grid_blocks();  // initialise the cached grid size before the threads use it
   auto cells_task = [&] {
     uint64_t& h2d = task_h2d[0];
@@ -520,55 +522,57 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
       upload(e->tgt_scale, scale, s, h2d);
     }
   };
-  auto hybrid_task = [&] {
-    uint64_t& h2d = task_h2d[3];
-    // hybrid Laplacian
-    {
-      std::vector<uint32_t> kw, Lptr, Lcol;
-      std::vector<int32_t> ki;
-      std::vector<double> cs, wd, Lval, Ld;
-      build_hybrid(p, ELIMINATE_MAX_DEGREE, kw, ki, cs, wd, Lptr, Lcol, Lval, Ld);
-      e->kept = uint32_t(kw.size());
-      e->n = e->F + e->kept;
-      std::vector<double> dinv(Ld.size());
-      for (size_t v = 0; v < Ld.size(); ++v) dinv[v] = 1.0 / Ld[v];
-      upload(e->kept_worker, kw, s, h2d);
-      upload(e->kept_index, ki, s, h2d);
-      upload(e->cell_scale, cs, s, h2d);
-      upload(e->worker_diag, wd, s, h2d);
-      upload(e->L_ptr, Lptr, s, h2d);
-      upload(e->L_col, Lcol, s, h2d);
-      upload(e->L_val, Lval, s, h2d);
-      upload(e->L_diag, Ld, s, h2d);
-      upload(e->L_dinv, dinv, s, h2d);
-      e->L_vald.alloc(Lval.size());
-      if (!Lval.empty())
-        k_scale_by_col<<<grid_blocks(), THREADS, 0, s>>>(Lval.size(), e->L_col.p, e->L_val.p, e->L_dinv.p,
-                                                         e->L_vald.p);
-      CK_LAUNCH();
-      build_segments(Lptr, e->lap_seg, s, h2d);
-      e->stats.vertices = e->n;
-      e->stats.terminal_vertices = e->n;
-      e->stats.edges = Lcol.size() / 2;
-      e->stats.kept_workers = e->kept;
-      e->preconditioner = preconditioner == 0 ? 1 : preconditioner;
+  run_parallel({cells_task, units_task, strata_task});
+  for (uint64_t b : task_h2d) e->stats.h2d_bytes += b;
+  // hybrid Laplacian, assembled on the device from the uploaded cells
+  {
+    DeviceHybrid h;
+    assemble_hybrid(e->W, e->F, e->C, ELIMINATE_MAX_DEGREE, e->worker_ptr.p, e->cell_firm.p, e->cell_weight.p, h,
+                    e->lap_seg, grid_blocks(), s);
+    e->kept = h.kept;
+    e->n = h.n;
+    e->kept_worker = std::move(h.kept_worker);
+    e->kept_index = std::move(h.kept_index);
+    e->cell_scale = std::move(h.cell_scale);
+    e->worker_diag = std::move(h.worker_diag);
+    e->L_ptr = std::move(h.ptr);
+    e->L_col = std::move(h.col);
+    e->L_val = std::move(h.val);
+    e->L_diag = std::move(h.diag);
+    e->L_dinv = std::move(h.dinv);
+    const size_t nnz = e->L_val.n;
+    e->L_vald.alloc(nnz);
+    if (nnz)
+      k_scale_by_col<<<grid_blocks(), THREADS, 0, s>>>(nnz, e->L_col.p, e->L_val.p, e->L_dinv.p, e->L_vald.p);
+    CK_LAUNCH();
+    e->stats.vertices = e->n;
+    e->stats.terminal_vertices = e->n;
+    e->stats.edges = nnz / 2;
+    e->stats.kept_workers = e->kept;
+    e->preconditioner = preconditioner == 0 ? 1 : preconditioner;
+    e->stats.levels = 1;
+    if (e->preconditioner == 2 || e->preconditioner == 3) {
+      // the CMG hierarchy and the network features are built on the host
+      std::vector<uint32_t> Lptr(e->n + 1), Lcol(nnz);
+      std::vector<double> Lval(nnz), Ld(e->n);
+      CK(cudaMemcpyAsync(Lptr.data(), e->L_ptr.p, Lptr.size() * 4, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(Lcol.data(), e->L_col.p, nnz * 4, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(Lval.data(), e->L_val.p, nnz * 8, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(Ld.data(), e->L_diag.p, e->n * 8, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      uint64_t& h2d = e->stats.h2d_bytes;
       if (e->preconditioner == 2) {
         e->mg = build_multigrid(e->n, Lptr, Lcol, Lval, Ld, s, h2d);
         e->stats.levels = e->mg->levels();
         e->stats.terminal_vertices = e->mg->report().vertices.back();
-      } else if (e->preconditioner == 3) {
+      } else {
         std::vector<float> params = learned_params();
         if (params.empty())
           fail(UNSUPPORTED_FEATURE, "learned_preconditioner", "no network parameters are installed");
         e->learned = build_learned(params, e->n, Lptr, Lcol, Lval, Ld, s, h2d);
-        e->stats.levels = 1;
-      } else {
-        e->stats.levels = 1;
       }
     }
-  };
-  run_parallel({cells_task, units_task, strata_task, hybrid_task});
-  for (uint64_t b : task_h2d) e->stats.h2d_bytes += b;
+  }
   if (!e->observation) {
     e->moments.alloc(size_t(e->G) * 5);
     e->unit_out.alloc(size_t(e->G) * 6);
@@ -600,6 +604,40 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   CK(cudaStreamSynchronize(s));
   e->stats.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return e;
+}
+
+// Compare the device-assembled hybrid Laplacian, its segments and the worker
+// reconstruction arrays with the host builder's (hybrid.cpp), bit for bit.
+bool device_hybrid_matches_host(DeviceEngine& e, const Compressed& p) {
+  std::vector<uint32_t> kw, Lptr, Lcol;
+  std::vector<int32_t> ki;
+  std::vector<double> cs, wd, Lval, Ld;
+  build_hybrid(p, ELIMINATE_MAX_DEGREE, kw, ki, cs, wd, Lptr, Lcol, Lval, Ld);
+  auto same = [&](const auto& host, const auto& dev, size_t count) {
+    using T = typename std::decay_t<decltype(host)>::value_type;
+    if (host.size() != count || dev.n < count) return false;
+    std::vector<T> d(count);
+    if (count) CK(cudaMemcpy(d.data(), dev.p, count * sizeof(T), cudaMemcpyDeviceToHost));
+    return count == 0 || std::memcmp(d.data(), host.data(), count * sizeof(T)) == 0;
+  };
+  std::vector<uint32_t> row, begin, end, flag, first(Lptr.size(), 0);
+  for (size_t r = 0; r + 1 < Lptr.size(); ++r) {
+    first[r] = uint32_t(row.size());
+    for (uint32_t x = Lptr[r]; x < Lptr[r + 1]; x += SEG) {
+      row.push_back(uint32_t(r));
+      begin.push_back(x);
+      end.push_back(std::min(Lptr[r + 1], x + SEG));
+      flag.push_back(uint32_t(r) | (x == Lptr[r] ? SEG_FIRST : 0u));
+    }
+  }
+  first.back() = uint32_t(row.size());
+  CK(cudaStreamSynchronize(e.stream));
+  return e.kept == kw.size() && same(kw, e.kept_worker, kw.size()) && same(ki, e.kept_index, ki.size()) &&
+         same(cs, e.cell_scale, cs.size()) && same(wd, e.worker_diag, wd.size()) && same(Lptr, e.L_ptr, Lptr.size()) &&
+         same(Lcol, e.L_col, Lcol.size()) && same(Lval, e.L_val, Lval.size()) && same(Ld, e.L_diag, Ld.size()) &&
+         e.lap_seg.count == row.size() && same(row, e.lap_seg.row, row.size()) &&
+         same(begin, e.lap_seg.begin, begin.size()) && same(end, e.lap_seg.end, end.size()) &&
+         same(flag, e.lap_seg.row_flag, flag.size()) && same(first, e.lap_seg.row_first, first.size());
 }
 
 // Per-unit detail of the last solve without controls (shares, bias, variance,
@@ -2004,9 +2042,9 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
         PersistentPcg<K> a = persistent_args<K>(e, w, iters);
         void* args[] = {&a};
         // 1: the form the solver uses at this width; 5: three barriers; 6: two
-        // barriers; 7: three barriers with the warp-broadcast gather
+        // barriers; 7: three barriers with per-lane index loads in the gather
         const bool two = kernel == 6 || (kernel == 1 && two_barrier_form<K, double>());
-        const void* fn = kernel == 7 ? (const void*)k_pcg_persistent<K, double, true>
+        const void* fn = kernel == 7 ? (const void*)k_pcg_persistent<K, double, false>
                          : two      ? (const void*)k_pcg_persistent_cg<K>
                                     : (const void*)k_pcg_persistent<K>;
         CK(cudaLaunchCooperativeKernel(fn, dim3(e.coop_blocks), dim3(PERSIST_THREADS), args, 0, L.s));

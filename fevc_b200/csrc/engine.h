@@ -99,6 +99,10 @@ DeviceStats device_stats(const DeviceEngine& e);
 SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o,
                          bool want_unit_detail);
 
+// The device-assembled hybrid Laplacian (and segments, reconstruction arrays)
+// equals the host builder's bit for bit.
+bool device_hybrid_matches_host(DeviceEngine& e, const Compressed& p);
+
 // Per-unit detail of the last solve without controls, read from the device
 // on request (solves keep it there).
 void device_unit_detail(DeviceEngine& e, SolveResult& res);

@@ -696,6 +696,10 @@ typedef struct FevcbSolveTimingsV1 {
 int32_t fevcb_device_count(void);
 /* Bind the CUDA stream (a cudaStream_t) used by generations prepared afterwards; NULL = library-owned stream. */
 int32_t fevcb_set_stream(void *stream);
+/* Whether the hybrid Laplacian the device assembled for a solved generation
+ * (with its row segments and worker reconstruction arrays) equals the host
+ * builder's bit for bit: *identical = 1 or 0. */
+int32_t fevcb_engine_hybrid_check_v1(uint64_t generation, uint32_t *identical);
 /* Device buffers of released generations stay cached (at most 16 GiB per
  * device) for the next generation; this returns the current device's cached
  * blocks to the driver.  Either pointer may be NULL. */
@@ -824,7 +828,8 @@ int32_t fevcb_cmg_aggregate_v1(uint32_t vertices, const uint32_t *row_ptr, const
  * events, L2 flushed before each launch.  kernel: 1 the persistent blocked
  * PCG form the solver uses at this block width (20 iterations per launch),
  * 3 leverage atoms + cell sums, 4 leverage moments, 5 the three-barrier and
- * 6 the two-barrier persistent PCG (20 iterations per launch).
+ * 6 the two-barrier persistent PCG, 7 the three-barrier form with per-lane
+ * index loads in its gather (20 iterations per launch).
  * Outputs mean milliseconds per launch and algorithmic bytes per launch. */
 int32_t fevcb_engine_kernel_benchmark_v1(uint64_t generation, uint32_t kernel, uint32_t block_columns,
                                          uint32_t launches, double *ms_per_launch, double *bytes_per_launch);

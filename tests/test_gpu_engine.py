@@ -2,6 +2,8 @@
 four variance components against the reference plugin's golden results and the
 oracle, through the C ABI on a B200."""
 
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -266,3 +268,29 @@ def test_mixed_precision_agrees_with_double_at_scale(lib):
         assert max(r["complete_residual"] for r in rc) <= 1e-7
     for key in ("plugin", "correction", "corrected"):
         assert rel(out[1][key], out[0][key]) < 1e-6, key
+
+
+@pytest.mark.parametrize("name", ["small_2k", "pareto13_4k", "regions_4k"])
+def test_device_hybrid_assembly_equals_the_host_builder(lib, name):
+    """The hybrid Laplacian assembled on the device (clique emission, stable
+    radix sort, per-run sequential sums) equals hybrid.cpp's bit for bit."""
+    panel = make_golden.PANELS[name]["build"]()
+    e = solve(lib, panel, probes=4)
+    same = abi.u32(0)
+    e.check(lib.fevcb_engine_hybrid_check_v1(e.generation, C.byref(same)))
+    e.release()
+    assert same.value == 1
+
+
+def test_device_hybrid_assembly_with_star_workers(lib):
+    """Workers with more than sixteen cells stay as star vertices: 24 periods
+    with frequent moves give the device assembly kept workers to place."""
+    from fevc_b200.panel import generate_panel
+
+    panel = generate_panel(3000, 300, 24, move_p=0.6, seed=77)
+    e = solve(lib, panel, probes=4)
+    same = abi.u32(0)
+    e.check(lib.fevcb_engine_hybrid_check_v1(e.generation, C.byref(same)))
+    kept = e.timings()["kept_workers"]
+    e.release()
+    assert kept > 0 and same.value == 1
