@@ -5,6 +5,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <utility>
+#include <mutex>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -61,12 +64,41 @@ struct DBuf {
   size_t bytes() const { return n * sizeof(T); }
 };
 
+// Pinned staging of uploads (devmem.cu).  While a thread has a stager bound
+// (HostStager::Bind), upload() copies into pinned blocks from a process-wide
+// cache and the DMA runs asynchronously; the owner synchronises the stream
+// and then finish()es the stager, which returns the blocks.  Without one,
+// uploads copy from pageable memory.
+class HostStager {
+ public:
+  ~HostStager();
+  void* take(size_t bytes);  // a pinned block held until finish()
+  void finish();             // call after the uploads' stream has synchronised
+  struct Bind {
+    explicit Bind(HostStager* s);
+    ~Bind();
+    HostStager* prev;
+  };
+
+ private:
+  std::mutex mu_;
+  std::vector<std::pair<void*, size_t>> blocks_;
+};
+HostStager* bound_stager();
+
 template <class T>
 void upload(DBuf<T>& d, const std::vector<T>& h, cudaStream_t s, uint64_t& counter) {
   d.alloc(h.size());
   if (!h.empty()) {
-    CK(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
-    counter += h.size() * sizeof(T);
+    const size_t bytes = h.size() * sizeof(T);
+    if (HostStager* st = bound_stager()) {
+      void* pin = st->take(bytes);
+      std::memcpy(pin, h.data(), bytes);
+      CK(cudaMemcpyAsync(d.p, pin, bytes, cudaMemcpyHostToDevice, s));
+    } else {
+      CK(cudaMemcpyAsync(d.p, h.data(), bytes, cudaMemcpyHostToDevice, s));
+    }
+    counter += bytes;
   }
 }
 

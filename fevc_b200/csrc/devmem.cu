@@ -123,4 +123,77 @@ size_t device_cache_bytes() {
   return g_cache[dev].cached;
 }
 
+// ---------------------------------------------------------------------------
+// Pinned host blocks for staged uploads, cached like the device blocks
+// (bounded at PINNED_CACHE_LIMIT bytes; a cached block serves requests of at
+// least 4/5 of its size).
+
+namespace {
+
+constexpr size_t PINNED_CACHE_LIMIT = size_t(2) << 30;
+
+std::mutex g_pin_mu;
+std::multimap<size_t, void*> g_pin_free;
+size_t g_pin_cached = 0;
+thread_local HostStager* t_stager = nullptr;
+
+void* pinned_acquire(size_t bytes, size_t& have) {
+  const size_t want = round_request(bytes);
+  {
+    std::lock_guard<std::mutex> l(g_pin_mu);
+    auto it = g_pin_free.lower_bound(want);
+    if (it != g_pin_free.end() && want >= it->first - it->first / 5) {
+      void* p = it->second;
+      have = it->first;
+      g_pin_cached -= have;
+      g_pin_free.erase(it);
+      return p;
+    }
+  }
+  void* p = nullptr;
+  check_cuda(cudaHostAlloc(&p, want, cudaHostAllocDefault), "cudaHostAlloc");
+  have = want;
+  return p;
+}
+
+void pinned_release(void* p, size_t have) {
+  std::lock_guard<std::mutex> l(g_pin_mu);
+  g_pin_free.emplace(have, p);
+  g_pin_cached += have;
+  while (g_pin_cached > PINNED_CACHE_LIMIT && !g_pin_free.empty()) {
+    auto it = std::prev(g_pin_free.end());
+    cudaFreeHost(it->second);
+    g_pin_cached -= it->first;
+    g_pin_free.erase(it);
+  }
+}
+
+}  // namespace
+
+void* HostStager::take(size_t bytes) {
+  size_t have = 0;
+  void* p = pinned_acquire(bytes, have);
+  std::lock_guard<std::mutex> l(mu_);
+  blocks_.emplace_back(p, have);
+  return p;
+}
+
+void HostStager::finish() {
+  std::lock_guard<std::mutex> l(mu_);
+  for (auto& b : blocks_) pinned_release(b.first, b.second);
+  blocks_.clear();
+}
+
+HostStager::~HostStager() {
+  // blocks still held here (an error path) may be in flight: wait, then free
+  // them instead of reusing them
+  if (!blocks_.empty()) cudaDeviceSynchronize();
+  for (auto& b : blocks_) cudaFreeHost(b.first);
+}
+
+HostStager::Bind::Bind(HostStager* s) : prev(t_stager) { t_stager = s; }
+HostStager::Bind::~Bind() { t_stager = prev; }
+
+HostStager* bound_stager() { return t_stager; }
+
 }  // namespace fevcb

@@ -333,7 +333,7 @@ __global__ void k_scale_by_col(size_t nnz, const uint32_t* __restrict__ col, con
 
 // Run the tasks on their own threads, bound to the calling thread's device;
 // the first exception (by task order) is rethrown after all have finished.
-void run_parallel(const std::vector<std::function<void()>>& tasks) {
+void run_parallel(const std::vector<std::function<void()>>& tasks, HostStager* stager = nullptr) {
   int dev = 0;
   CK(cudaGetDevice(&dev));
   std::vector<std::exception_ptr> errors(tasks.size());
@@ -343,6 +343,7 @@ void run_parallel(const std::vector<std::function<void()>>& tasks) {
     threads.emplace_back([&, i] {
       try {
         CK(cudaSetDevice(dev));
+        HostStager::Bind bind(stager);  // uploads of this task go through pinned blocks
         tasks[i]();
       } catch (...) {
         errors[i] = std::current_exception();
@@ -374,12 +375,13 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   e->S = uint32_t(plan.tgt_cell.size());
   e->target_total = p.target_total;
 
-  // Three independent host builders, each uploading what it builds: cells and
-  // the firm segments; deletion units and then the generic row data (which
-  // reads the unit order); target strata.  They run on their own threads
-  // (bound to this device); their uploads share the engine's stream and fill
-  // disjoint buffers.  The hybrid Laplacian is then assembled on the device.
-  uint64_t task_h2d[3] = {0, 0, 0};
+  // Independent host builders, each uploading what it builds: cells and the
+  // firm segments; deletion units; target strata; and for the generic
+  // estimator the row data, the rows of every cell and the match groups.
+  // They run on their own threads (bound to this device); their uploads share
+  // the engine's stream and fill disjoint buffers.  The hybrid Laplacian is
+  // then assembled on the device.
+  uint64_t task_h2d[6] = {0, 0, 0, 0, 0, 0};
   (void)grid_blocks();  // initialise the cached grid size before the threads use it
   auto cells_task = [&] {
     uint64_t& h2d = task_h2d[0];
@@ -464,42 +466,49 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
       upload(e->unit_count_f, ucf, s, h2d);
       upload(e->unit_sqrt_n, usq, s, h2d);
     }
-    // row-level data of the generic estimator
-    if (plan.generic) {
-      e->generic = true;
-      e->q = int(p.controls.size());
-      if (e->q < (plan.observation ? 0 : 1) || e->q > QMAX)
-        fail(UNSUPPORTED_FEATURE, "generic_jla", "the device engine handles at most 8 control columns");
-      e->rows = uint32_t(p.rows());
-      size_t R = p.rows();
-      std::vector<double> freq(R), Q(R * e->q);
-      for (size_t r = 0; r < R; ++r) {
-        freq[r] = double(p.frequency[r]);
-        for (int k = 0; k < e->q; ++k) Q[r * e->q + k] = p.controls[k][r];
-      }
-      std::vector<uint32_t> cptr(p.cells + 1, 0), crow(R);
-      for (size_t r = 0; r < R; ++r) cptr[p.row_cell[r] + 1]++;
-      for (size_t c = 0; c < p.cells; ++c) cptr[c + 1] += cptr[c];
-      {
-        std::vector<uint32_t> cur(cptr.begin(), cptr.end() - 1);
-        for (size_t r = 0; r < R; ++r) crow[cur[p.row_cell[r]]++] = uint32_t(r);
-      }
-      upload(e->row_cell, p.row_cell, s, h2d);
-      upload(e->row_freq, freq, s, h2d);
-      upload(e->row_y, p.outcome, s, h2d);
-      upload(e->Qd, Q, s, h2d);
-      upload(e->cell_rows_ptr, cptr, s, h2d);
-      upload(e->cell_rows, crow, s, h2d);
-      upload(e->group_ptr, plan.group_ptr, s, h2d);
-      upload(e->group_rows, plan.group_rows, s, h2d);
-      upload(e->unit_group_d, e->unit_group, s, h2d);
-      e->Rd.alloc(R * e->q);
-      e->residual.alloc(R);
-      e->deleted.alloc(R);
-      e->alphaH.alloc(size_t(e->W) * QMAX);
-      e->psiH.alloc(size_t(e->F) * QMAX);
-      e->beta_buf.alloc(QMAX * 128);
+    if (plan.generic) upload(e->unit_group_d, e->unit_group, s, h2d);
+  };
+  // row-level data of the generic estimator, in three pieces
+  const size_t R = p.rows();
+  if (plan.generic) {
+    e->generic = true;
+    e->q = int(p.controls.size());
+    if (e->q < (plan.observation ? 0 : 1) || e->q > QMAX)
+      fail(UNSUPPORTED_FEATURE, "generic_jla", "the device engine handles at most 8 control columns");
+    e->rows = uint32_t(R);
+  }
+  auto rows_task = [&] {  // per-row cell, frequency, outcome, controls (row-major)
+    uint64_t& h2d = task_h2d[3];
+    std::vector<double> freq(R), Q(R * e->q);
+    for (size_t r = 0; r < R; ++r) {
+      freq[r] = double(p.frequency[r]);
+      for (int k = 0; k < e->q; ++k) Q[r * e->q + k] = p.controls[k][r];
     }
+    upload(e->row_cell, p.row_cell, s, h2d);
+    upload(e->row_freq, freq, s, h2d);
+    upload(e->row_y, p.outcome, s, h2d);
+    upload(e->Qd, Q, s, h2d);
+    e->Rd.alloc(R * e->q);
+    e->residual.alloc(R);
+    e->deleted.alloc(R);
+  };
+  auto cell_rows_task = [&] {  // rows of every cell (stable counting sort)
+    uint64_t& h2d = task_h2d[4];
+    std::vector<uint32_t> cptr(p.cells + 1, 0), crow(R);
+    for (size_t r = 0; r < R; ++r) cptr[p.row_cell[r] + 1]++;
+    for (size_t c = 0; c < p.cells; ++c) cptr[c + 1] += cptr[c];
+    std::vector<uint32_t> cur(cptr.begin(), cptr.end() - 1);
+    for (size_t r = 0; r < R; ++r) crow[cur[p.row_cell[r]]++] = uint32_t(r);
+    upload(e->cell_rows_ptr, cptr, s, h2d);
+    upload(e->cell_rows, crow, s, h2d);
+  };
+  auto groups_task = [&] {  // match groups (rows by semantic rank) and work buffers
+    uint64_t& h2d = task_h2d[5];
+    upload(e->group_ptr, plan.group_ptr, s, h2d);
+    upload(e->group_rows, plan.group_rows, s, h2d);
+    e->alphaH.alloc(size_t(e->W) * QMAX);
+    e->psiH.alloc(size_t(e->F) * QMAX);
+    e->beta_buf.alloc(QMAX * 128);
   };
   auto strata_task = [&] {
     uint64_t& h2d = task_h2d[2];
@@ -522,7 +531,14 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
       upload(e->tgt_scale, scale, s, h2d);
     }
   };
-  run_parallel({cells_task, units_task, strata_task});
+  std::vector<std::function<void()>> tasks = {cells_task, units_task, strata_task};
+  if (plan.generic) {
+    tasks.push_back(rows_task);
+    tasks.push_back(cell_rows_task);
+    tasks.push_back(groups_task);
+  }
+  HostStager stager;
+  run_parallel(tasks, &stager);
   for (uint64_t b : task_h2d) e->stats.h2d_bytes += b;
   // hybrid Laplacian, assembled on the device from the uploaded cells
   {
@@ -602,6 +618,7 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   CK(cudaEventCreate(&e->ev0));
   CK(cudaEventCreate(&e->ev1));
   CK(cudaStreamSynchronize(s));
+  stager.finish();  // every staged upload has completed
   e->stats.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return e;
 }
