@@ -59,7 +59,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
         src, obj = CSRC / name, BUILD / (name + ".o")
         objs.append(obj)
         if _stale(obj, src):
-            jobs.append([nvcc, "-x", "c++", "-std=c++17", "-O3", "-Xcompiler", "-fPIC,-Wall",
+            jobs.append([nvcc, "-x", "c++", "-std=c++17", "-O3", "-Xcompiler", "-fPIC,-Wall,-fopenmp",
                          f"-I{CSRC}", f"-I{INCLUDE}", "-c", str(src), "-o", str(obj)])
     for name in CU_SOURCES:
         src, obj = CSRC / name, BUILD / (name + ".o")
@@ -77,7 +77,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
     if jobs or not LIB.exists():
         tmp = LIB.with_suffix(".so.tmp")
         _run([nvcc, GENCODE, "-shared", "-cudart", "static", "-o", str(tmp)] + [str(o) for o in objs]
-             + ["-Xlinker", "--no-undefined"])
+             + ["-Xcompiler", "-fopenmp", "-Xlinker", "--no-undefined"])
         os.replace(tmp, LIB)
     return LIB
 

