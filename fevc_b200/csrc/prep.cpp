@@ -931,58 +931,136 @@ std::vector<uint8_t> select_implicit_match_graph(const Canonical& in, GraphRecei
 
 std::vector<uint8_t> select_observation_graph(const Canonical& in, GraphReceipt& rc) {
   if (in.rows() == 0) fail(GRAPH_EMPTY, "graph", "command sample is empty");
-  std::vector<uint8_t> active(in.rows(), 1);
+  // Every step of the observation fixed point keeps or drops whole workers
+  // (components, physical singletons, articulation workers), so it runs on a
+  // worker mask over the coordinate graph built once; the row mask is read
+  // off at the end.
+  const size_t W = in.workers, R = in.rows();
+  std::vector<uint64_t> wrows(W, 0), wmass(W, 0);
+  for (size_t r = 0; r < R; ++r) {
+    wrows[in.worker[r]] += 1;
+    wmass[in.worker[r]] += in.frequency[r];
+  }
+  Graph g;
+  {
+    std::vector<uint32_t> eu(in.coord_worker.size()), ev(in.coord_worker.size());
+    for (size_t c = 0; c < eu.size(); ++c) {
+      eu[c] = in.coord_worker[c];
+      ev[c] = uint32_t(W + in.coord_firm[c]);
+    }
+    g = make_graph(W + in.firms, eu, ev);
+  }
+  std::vector<uint8_t> wact(W, 0), on(in.coord_worker.size(), 0);
+  for (size_t w = 0; w < W; ++w) wact[w] = wrows[w] > 0;
+  auto mark = [&] {
+    size_t edges = 0;
+    for (size_t c = 0; c < on.size(); ++c) edges += (on[c] = wact[in.coord_worker[c]]);
+    if (!edges) fail(GRAPH_EMPTY, "graph", "active graph is empty");
+    return edges;
+  };
+  auto rows_of = [&] {
+    uint64_t n = 0;
+    for (size_t w = 0; w < W; ++w)
+      if (wact[w]) n += wrows[w];
+    return n;
+  };
+  // `largest_component` on the active workers: (firm count, physical mass)
+  auto component = [&](size_t& comps) {
+    mark();
+    std::vector<uint32_t> label(g.nodes, MISSING), queue;
+    queue.reserve(g.nodes);
+    comps = 0;
+    for (size_t root = 0; root < g.nodes; ++root) {
+      if (label[root] != MISSING) continue;
+      bool has_edge = false;
+      for (uint64_t a = g.ptr[root]; a < g.ptr[root + 1] && !has_edge; ++a) has_edge = on[g.arc[a].edge];
+      if (!has_edge) continue;
+      label[root] = uint32_t(comps);
+      queue.clear();
+      queue.push_back(uint32_t(root));
+      for (size_t h = 0; h < queue.size(); ++h) {
+        uint32_t v = queue[h];
+        for (uint64_t a = g.ptr[v]; a < g.ptr[v + 1]; ++a)
+          if (on[g.arc[a].edge] && label[g.arc[a].to] == MISSING) {
+            label[g.arc[a].to] = uint32_t(comps);
+            queue.push_back(g.arc[a].to);
+          }
+      }
+      ++comps;
+    }
+    if (comps == 0) fail(GRAPH_EMPTY, "graph", "no connected worker-firm component remains");
+    std::vector<uint64_t> firms(comps, 0), mass(comps, 0);
+    for (size_t f = 0; f < in.firms; ++f)
+      if (label[W + f] != MISSING) firms[label[W + f]]++;
+    for (size_t w = 0; w < W; ++w)
+      if (wact[w]) {
+        if (label[w] == MISSING) fail(INTERNAL_INVARIANT_FAILED, "graph", "active row has no connected-component label");
+        mass[label[w]] += wmass[w];
+      }
+    size_t best = 0;
+    for (size_t c = 1; c < comps; ++c)
+      if (firms[c] > firms[best] || (firms[c] == firms[best] && mass[c] > mass[best])) best = c;
+    size_t winners = 0;
+    for (size_t c = 0; c < comps; ++c) winners += (firms[c] == firms[best] && mass[c] == mass[best]);
+    if (winners != 1)
+      fail(GRAPH_UNIDENTIFIED, "graph", "multiple connected components tie for largest-component selection");
+    for (size_t w = 0; w < W; ++w) wact[w] = wact[w] && label[w] == best;
+  };
   rc = GraphReceipt{};
-  rc.input_rows = in.rows();
+  rc.input_rows = R;
   rc.input_physical_mass = in.physical_total;
-  ComponentResult initial = largest_component(in, active);
-  rc.initial_components = rc.maximum_components = initial.components;
-  rc.initial_component_rows = initial.retained_rows;
-  intersect(active, initial.keep);
-  rc.mover_input_rows = count_true(active);
-  rc.initial_deletion_edges = coordinate_graph(in, active).edges;
-  uint64_t bound = in.workers + 1;
+  size_t comps = 0;
+  component(comps);
+  rc.initial_components = rc.maximum_components = comps;
+  rc.initial_component_rows = rows_of();
+  rc.mover_input_rows = rc.initial_component_rows;
+  rc.initial_deletion_edges = mark();
+  uint64_t bound = W + 1;
+  // A step that removed only physical singletons (one row, one coordinate:
+  // leaves of one connected graph) cannot split it, so the next component
+  // pass is skipped; the loop leaves from a state it has just certified, so
+  // the reference's closing component pass and certificates are implied.
+  bool connected = false;
   for (;;) {
     if (rc.fixed_point_iterations > bound)
       fail(GRAPH_CERTIFICATE_FAILED, "graph", "observation-deletion pruning exceeded its finite iteration bound");
-    ComponentResult comp = largest_component(in, active);
-    rc.maximum_components = std::max<uint64_t>(rc.maximum_components, comp.components);
-    intersect(active, comp.keep);
-    if (count_true(active) == 0) fail(GRAPH_EMPTY, "graph", "no component remains after observation-deletion pruning");
-    auto physical = worker_physical_counts(in, active);
+    if (!connected) {
+      component(comps);
+      rc.maximum_components = std::max<uint64_t>(rc.maximum_components, comps);
+    }
+    connected = false;
+    if (rows_of() == 0) fail(GRAPH_EMPTY, "graph", "no component remains after observation-deletion pruning");
     size_t removed = 0;
-    for (uint64_t p : physical) removed += p == 1;
+    for (size_t w = 0; w < W; ++w) removed += wact[w] && wmass[w] == 1;
     if (removed) {
-      for (size_t r = 0; r < in.rows(); ++r)
-        if (active[r] && physical[in.worker[r]] == 1) active[r] = 0;
+      for (size_t w = 0; w < W; ++w)
+        if (wact[w] && wmass[w] == 1) wact[w] = 0;
       rc.insufficient_workers_removed += removed;
       rc.degree_iterations++;
       rc.fixed_point_iterations++;
+      connected = true;
       continue;
     }
-    auto art = worker_articulations(in, active);
+    mark();
+    std::vector<uint8_t> art;
+    tarjan(g, &art, nullptr, &on);
+    art.resize(W);
     size_t arts = count_true(art);
     if (arts == 0) break;
-    for (size_t r = 0; r < in.rows(); ++r)
-      if (active[r] && art[in.worker[r]]) active[r] = 0;
+    for (size_t w = 0; w < W; ++w)
+      if (art[w]) wact[w] = 0;
     rc.articulation_workers_removed += arts;
     rc.articulation_iterations++;
     rc.fixed_point_iterations++;
   }
-  ComponentResult fin = largest_component(in, active);
-  rc.maximum_components = std::max<uint64_t>(rc.maximum_components, fin.components);
-  intersect(active, fin.keep);
-  for (uint64_t p : worker_physical_counts(in, active))
-    if (p == 1)
-      fail(GRAPH_CERTIFICATE_FAILED, "graph", "final observation-deletion graph still contains a physical-singleton worker");
-  if (count_true(worker_articulations(in, active)))
-    fail(GRAPH_CERTIFICATE_FAILED, "graph", "final observation-deletion graph still contains a worker articulation");
-  size_t kept = count_true(active);
+  uint64_t kept = rows_of();
   if (kept == 0) fail(GRAPH_EMPTY, "graph", "no component remains after observation-deletion graph pruning");
   rc.retained_rows = kept;
-  for (size_t r = 0; r < in.rows(); ++r)
-    if (active[r]) rc.retained_physical_mass += in.frequency[r];
-  rc.retained_deletion_edges = coordinate_graph(in, active).edges;
+  for (size_t w = 0; w < W; ++w)
+    if (wact[w]) rc.retained_physical_mass += wmass[w];
+  rc.retained_deletion_edges = mark();
+  std::vector<uint8_t> active(R);
+  for (size_t r = 0; r < R; ++r) active[r] = wact[in.worker[r]];
   return active;
 }
 
