@@ -2020,6 +2020,7 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
     case 5:
     case 6:
     case 7:
+    case 8:
       // persistent PCG, per launch of `iters` iterations: matrix + segment
       // tables once per iteration, nine passes over n x K vectors (two-barrier
       // form: r gathered; r, p, A p, x read and written; three-barrier form:
@@ -2047,7 +2048,7 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
       k_colsum_abs<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p, e.partial.p);
       finish(e.partial.p, L.grid, 2 * K, w.tot.p, L.s);
       k_pcg_init_state<K><<<1, 128, 0, L.s>>>(w.tot.p, K, 0.0, double(e.n), w.s);
-      pcg_restart<K>(e, w, L, true, kernel == 5 || kernel == 7 || (kernel == 1 && !two_barrier_form<K, double>()));
+      pcg_restart<K>(e, w, L, true, kernel == 5 || kernel == 7 || kernel == 8 || (kernel == 1 && !two_barrier_form<K, double>()));
     }
     CK(cudaMemsetAsync(flush.p, i & 0xff, flush.bytes(), L.s));
     CK(cudaEventRecord(e.ev0, L.s));
@@ -2055,15 +2056,18 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
       case 1:
       case 5:
       case 6:
-      case 7: {
+      case 7:
+      case 8: {
         PersistentPcg<K> a = persistent_args<K>(e, w, iters);
         void* args[] = {&a};
         // 1: the form the solver uses at this width; 5: three barriers; 6: two
-        // barriers; 7: three barriers with per-lane index loads in the gather
+        // barriers; 7: three barriers with per-lane index loads in the gather;
+        // 8: three barriers, warp gather without pipelining
         const bool two = kernel == 6 || (kernel == 1 && two_barrier_form<K, double>());
-        const void* fn = kernel == 7 ? (const void*)k_pcg_persistent<K, double, false>
-                         : two      ? (const void*)k_pcg_persistent_cg<K>
-                                    : (const void*)k_pcg_persistent<K>;
+        const void* fn = kernel == 7   ? (const void*)k_pcg_persistent<K, double, false>
+                         : kernel == 8 ? (const void*)k_pcg_persistent<K, double, true, false>
+                         : two         ? (const void*)k_pcg_persistent_cg<K>
+                                       : (const void*)k_pcg_persistent<K>;
         CK(cudaLaunchCooperativeKernel(fn, dim3(e.coop_blocks), dim3(PERSIST_THREADS), args, 0, L.s));
         break;
       }
