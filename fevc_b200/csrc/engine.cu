@@ -926,6 +926,14 @@ PersistentPcg<K> persistent_args(DeviceEngine& e, BlockWork& w, int iterations) 
   a.row_first = e.lap_seg.row_first.p;
   a.seg_flag = e.lap_seg.row_flag.p;
   a.vald = e.L_vald.p;
+  a.ord_id = e.lap_seg.ord_id.p;
+  a.ord_flag = e.lap_seg.ord_flag.p;
+  a.ord_begin = e.lap_seg.ord_begin.p;
+  a.ord_end = e.lap_seg.ord_end.p;
+  a.heavy_rows = e.lap_seg.heavy_rows.p;
+  a.light_rows = e.lap_seg.light_rows.p;
+  a.nheavy = e.lap_seg.nheavy;
+  a.nlight = e.lap_seg.nlight;
   a.seg_buf = w.seg_buf.p;
   a.x = w.x.p;
   a.r = w.r.p;

@@ -150,6 +150,75 @@ T read_back(const T* p, cudaStream_t s) {
   return v;
 }
 
+__global__ void k_seg_len(uint32_t count, const uint32_t* __restrict__ begin, const uint32_t* __restrict__ end,
+                          uint32_t* __restrict__ len, uint32_t* __restrict__ idx) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    len[i] = end[i] - begin[i];
+    idx[i] = i;
+  }
+}
+
+__global__ void k_seg_gather(uint32_t count, const uint32_t* __restrict__ id, const uint32_t* __restrict__ flag,
+                             const uint32_t* __restrict__ begin, const uint32_t* __restrict__ end,
+                             uint32_t* __restrict__ oflag, uint32_t* __restrict__ obegin, uint32_t* __restrict__ oend) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    uint32_t j = id[i];
+    oflag[i] = flag[j];
+    obegin[i] = begin[j];
+    oend[i] = end[j];
+  }
+}
+
+__global__ void k_row_classes(uint32_t n, const uint32_t* __restrict__ first, uint32_t threshold,
+                              uint32_t* __restrict__ rows, uint8_t* __restrict__ heavy, uint8_t* __restrict__ light) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    bool h = first[v + 1] - first[v] > threshold;
+    rows[v] = v;
+    heavy[v] = h ? 1 : 0;
+    light[v] = h ? 0 : 1;
+  }
+}
+
+// Work orders of the persistent PCG: segments by decreasing length (the
+// product phase deals them out round-robin, so warps get similar totals) and
+// the rows split into those with more than HEAVY_SEGMENTS segments and the
+// rest (stable selections, row order kept).
+inline void order_segments(Segments& seg, uint32_t n, int grid, cudaStream_t s) {
+  const uint32_t m = seg.count;
+  DBuf<uint32_t> len(m), idx(m), len2(m);
+  seg.ord_id.alloc(m);
+  k_seg_len<<<grid, THREADS, 0, s>>>(m, seg.begin.p, seg.end.p, len.p, idx.p);
+  CK_LAUNCH();
+  if (m) {
+    size_t bytes = 0;
+    CK(cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, len.p, len2.p, idx.p, seg.ord_id.p, m, 0, 6, s));
+    DBuf<char> tmp(bytes);
+    CK(cub::DeviceRadixSort::SortPairsDescending(tmp.p, bytes, len.p, len2.p, idx.p, seg.ord_id.p, m, 0, 6, s));
+  }
+  seg.ord_flag.alloc(m);
+  seg.ord_begin.alloc(m);
+  seg.ord_end.alloc(m);
+  k_seg_gather<<<grid, THREADS, 0, s>>>(m, seg.ord_id.p, seg.row_flag.p, seg.begin.p, seg.end.p, seg.ord_flag.p,
+                                        seg.ord_begin.p, seg.ord_end.p);
+  CK_LAUNCH();
+  DBuf<uint32_t> rows(n), count(2);
+  DBuf<uint8_t> heavy(n), light(n);
+  k_row_classes<<<grid, THREADS, 0, s>>>(n, seg.row_first.p, HEAVY_SEGMENTS, rows.p, heavy.p, light.p);
+  CK_LAUNCH();
+  seg.heavy_rows.alloc(n);
+  seg.light_rows.alloc(n);
+  size_t bytes = 0;
+  CK(cub::DeviceSelect::Flagged(nullptr, bytes, rows.p, heavy.p, seg.heavy_rows.p, count.p, n, s));
+  DBuf<char> tmp(bytes);
+  CK(cub::DeviceSelect::Flagged(tmp.p, bytes, rows.p, heavy.p, seg.heavy_rows.p, count.p, n, s));
+  CK(cub::DeviceSelect::Flagged(tmp.p, bytes, rows.p, light.p, seg.light_rows.p, count.p + 1, n, s));
+  uint32_t got[2] = {0, 0};
+  CK(cudaMemcpyAsync(got, count.p, sizeof(got), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));  // the temporaries above are released on return
+  seg.nheavy = got[0];
+  seg.nlight = got[1];
+}
+
 struct DeviceHybrid {
   uint32_t n = 0, kept = 0;
   DBuf<uint32_t> kept_worker, ptr, col;
@@ -229,6 +298,7 @@ inline void assemble_hybrid(uint32_t W, uint32_t F, uint32_t C, uint32_t max_deg
                                           seg.row_flag.p);
   CK_LAUNCH();
   seg.row_first = std::move(first);
+  order_segments(seg, uint32_t(n), grid, s);
   CK(cudaStreamSynchronize(s));  // the temporaries above are released on return
 }
 

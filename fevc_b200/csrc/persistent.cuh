@@ -31,7 +31,16 @@ struct Segments {
   DBuf<uint32_t> row, begin, end;
   DBuf<uint32_t> row_first;  // first segment of each row (rows + 1 entries)
   DBuf<uint32_t> row_flag;   // row | SEG_FIRST when the segment opens its row
+  // work order of the product phase: segments by decreasing length (ties by
+  // index), as id / flag / begin / end in that order
+  DBuf<uint32_t> ord_id, ord_flag, ord_begin, ord_end;
+  // rows with more than HEAVY_SEGMENTS segments (summed by a whole block in
+  // the row pass) and the others, each in row order
+  DBuf<uint32_t> heavy_rows, light_rows;
+  uint32_t nheavy = 0, nlight = 0;
 };
+
+constexpr uint32_t HEAVY_SEGMENTS = 8;
 
 constexpr uint32_t SEG_FIRST = 0x80000000u;
 
@@ -130,6 +139,14 @@ struct PersistentPcg {
   const uint32_t* row_first;  // first segment of each row
   const uint32_t* seg_flag = nullptr;  // row | SEG_FIRST (the two-barrier kernel)
   const V* vald = nullptr;             // val[e] * dinv[col[e]] (the two-barrier kernel)
+  // balanced work orders (three-barrier kernel; null: plain strides)
+  const uint32_t* ord_id = nullptr;
+  const uint32_t* ord_flag = nullptr;
+  const uint32_t* ord_begin = nullptr;
+  const uint32_t* ord_end = nullptr;
+  const uint32_t* heavy_rows = nullptr;
+  const uint32_t* light_rows = nullptr;
+  uint32_t nheavy = 0, nlight = 0;
   V* seg_buf;                 // [nseg][K] segment partial products
   V* x;
   V* r;
@@ -218,18 +235,25 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(Persisten
 #pragma unroll
     for (int c = 0; c < CPT; ++c) v[0][c] = 0.0;
     if constexpr (PIPE && WARP_GATHER && TPR == 32) {
+      // segments in the balanced order (decreasing length) when it is given
+      const bool ord = a.ord_id != nullptr;
+      const uint32_t* mf = ord ? a.ord_flag : a.seg_flag;
+      const uint32_t* mb = ord ? a.ord_begin : a.seg_begin;
+      const uint32_t* me = ord ? a.ord_end : a.seg_end;
       const int lane = threadIdx.x & 31;
       const size_t s0 = gid;
-      uint32_t f1 = 0, b1 = 0, e1 = 0, f2 = 0, b2 = 0, e2 = 0;
+      uint32_t f1 = 0, b1 = 0, e1 = 0, f2 = 0, b2 = 0, e2 = 0, id1 = 0, id2 = 0;
       if (s0 < a.nseg) {
-        f1 = __ldg(a.seg_flag + s0);
-        b1 = __ldg(a.seg_begin + s0);
-        e1 = __ldg(a.seg_end + s0);
+        f1 = __ldg(mf + s0);
+        b1 = __ldg(mb + s0);
+        e1 = __ldg(me + s0);
+        id1 = ord ? __ldg(a.ord_id + s0) : uint32_t(s0);
       }
       if (s0 + ngroups < a.nseg) {
-        f2 = __ldg(a.seg_flag + s0 + ngroups);
-        b2 = __ldg(a.seg_begin + s0 + ngroups);
-        e2 = __ldg(a.seg_end + s0 + ngroups);
+        f2 = __ldg(mf + s0 + ngroups);
+        b2 = __ldg(mb + s0 + ngroups);
+        e2 = __ldg(me + s0 + ngroups);
+        id2 = ord ? __ldg(a.ord_id + s0 + ngroups) : uint32_t(s0 + ngroups);
       }
       uint32_t my_j = 0;
       double my_a = 0.0;
@@ -245,11 +269,12 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(Persisten
           nj = __ldg(a.col + b2 + lane);
           na = double(__ldg(a.val + b2 + lane));
         }
-        uint32_t f3 = 0, b3 = 0, e3 = 0;
+        uint32_t f3 = 0, b3 = 0, e3 = 0, id3 = 0;
         if (s3 < a.nseg) {
-          f3 = __ldg(a.seg_flag + s3);
-          b3 = __ldg(a.seg_begin + s3);
-          e3 = __ldg(a.seg_end + s3);
+          f3 = __ldg(mf + s3);
+          b3 = __ldg(mb + s3);
+          e3 = __ldg(me + s3);
+          id3 = ord ? __ldg(a.ord_id + s3) : uint32_t(s3);
         }
         const uint32_t row = f1 & ~SEG_FIRST;
         const double d = (f1 & SEG_FIRST) ? double(__ldg(a.diag + row)) : 0.0;
@@ -261,15 +286,17 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(Persisten
         load_cols<K, V>(a.p, row, c0, pr);
 #pragma unroll
         for (int c = 0; c < CPT; ++c) {
-          a.seg_buf[sg * K + c0 + c] = V(acc[c]);
+          a.seg_buf[size_t(id1) * K + c0 + c] = V(acc[c]);
           v[0][c] += pr[c] * (d * pr[c] - acc[c]);
         }
         f1 = f2;
         b1 = b2;
         e1 = e2;
+        id1 = id2;
         f2 = f3;
         b2 = b3;
         e2 = e3;
+        id2 = id3;
         my_j = nj;
         my_a = na;
       }
@@ -339,7 +366,49 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent(Persisten
     double w[2][CPT];
 #pragma unroll
     for (int c = 0; c < CPT; ++c) w[0][c] = w[1][c] = 0.0;
-    for (size_t row = gid; row < a.n; row += ngroups) {
+    // rows with many segments: one block each, its warps take strided shares
+    // of the segments, warp 0 combines them in warp order and updates the row
+    const bool balanced = TPR == 32 && a.heavy_rows != nullptr;
+    if (balanced) {
+      const int warp = int(threadIdx.x >> 5), nw = int(blockDim.x >> 5);
+      double(*hs)[K] = reinterpret_cast<double(*)[K]>(&s_red[0][0][0]);
+      for (uint32_t h = blockIdx.x; h < a.nheavy; h += gridDim.x) {
+        const uint32_t row = a.heavy_rows[h];
+        const uint32_t s0 = a.row_first[row], s1 = a.row_first[row + 1];
+        double part[CPT];
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) part[c] = 0.0;
+        for (uint32_t sg = s0 + uint32_t(warp); sg < s1; sg += uint32_t(nw)) {
+          double sv[CPT];
+          load_cols<K, V>(a.seg_buf, sg, c0, sv);
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) part[c] += sv[c];
+        }
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) hs[warp][c0 + c] = part[c];
+        __syncthreads();
+        if (warp == 0) {
+          const double dr = double(a.diag[row]), di = double(a.dinv[row]);
+          const size_t o = size_t(row) * K + c0;
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) {
+            double q = dr * double(a.p[o + c]);
+            for (int u = 0; u < nw; ++u) q -= hs[u][c0 + c];
+            double al = s_alpha[c0 + c];
+            a.x[o + c] = V(double(a.x[o + c]) + al * double(a.p[o + c]));
+            V rv = V(double(a.r[o + c]) - al * q);
+            a.r[o + c] = rv;
+            double ri = double(rv);
+            w[0][c] += ri * (di * ri);
+            w[1][c] += ri * ri;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    const size_t nrows = balanced ? a.nlight : a.n;
+    for (size_t li = gid; li < nrows; li += ngroups) {
+      const size_t row = balanced ? a.light_rows[li] : li;
       uint32_t s0 = a.row_first[row], s1 = a.row_first[row + 1];
       double dr = double(a.diag[row]), di = double(a.dinv[row]);
       size_t o = row * K + c0;
