@@ -2048,7 +2048,7 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
       break;
     default: fail(INVALID_INPUT, "benchmark", "unknown kernel id");
   }
-  float total = 0.0f;
+  std::vector<float> times;
   for (int i = 0; i < launches; ++i) {
     if (kernel == 1 || kernel >= 5) {
       // a fresh, never-converging block (tolerance 0) so every launch runs `iters` iterations
@@ -2099,10 +2099,13 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
     CK(cudaEventSynchronize(e.ev1));
     float t = 0;
     CK(cudaEventElapsedTime(&t, e.ev0, e.ev1));
-    total += t;
+    times.push_back(t);
   }
   CK_LAUNCH();
-  *ms = double(total) / launches;
+  // the median launch: one launch delayed by something outside this process
+  // (another context time-sliced onto the device) does not move it
+  std::sort(times.begin(), times.end());
+  *ms = launches % 2 ? times[launches / 2] : 0.5 * (double(times[launches / 2 - 1]) + times[launches / 2]);
   if (kernel == 1 || kernel >= 5) {
     // report the iterations actually executed (a curvature breakdown would stop early)
     std::vector<int> it(K);

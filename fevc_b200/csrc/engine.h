@@ -114,7 +114,7 @@ double device_weighted_rss(DeviceEngine& e, const Compressed& p);
 // persistent blocked PCG form used at this width (20 iterations), 3 leverage
 // Counter-V1 atoms with the per-cell sums, 4 leverage moments, 5 / 6 the
 // three- / two-barrier persistent PCG.  Returns the
-// mean device milliseconds per launch and the algorithmic bytes per launch.
+// median device milliseconds per launch and the algorithmic bytes per launch.
 void device_kernel_benchmark(DeviceEngine& e, int kernel, int block_columns, int launches, double* ms_per_launch,
                              double* bytes_per_launch);
 

@@ -831,7 +831,7 @@ int32_t fevcb_cmg_aggregate_v1(uint32_t vertices, const uint32_t *row_ptr, const
  * 6 the two-barrier persistent PCG, 7 the three-barrier form with per-lane
  * index loads in its gather, 8 the three-barrier form without the pipelined
  * product phase (20 iterations per launch).
- * Outputs mean milliseconds per launch and algorithmic bytes per launch. */
+ * Outputs the median milliseconds per launch and algorithmic bytes per launch. */
 int32_t fevcb_engine_kernel_benchmark_v1(uint64_t generation, uint32_t kernel, uint32_t block_columns,
                                          uint32_t launches, double *ms_per_launch, double *bytes_per_launch);
 
