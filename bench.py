@@ -123,11 +123,18 @@ def build_panel(args):
     return panel, len(panel.controls)
 
 
-def v5_request(engine, probes, tolerance, *, reference=False):
-    """A V5 solve request: JLA, match deletion, supplied tolerance.  With
-    controls the generic engine runs; the reference additionally selects its
-    production CMG_FULL_V2 route on all host cores."""
-    q = engine.default_request_v5()
+def deletion_mode(panel) -> int:
+    """1 leave-match-out, 2 leave-observation-out (the learned_10m panel)."""
+    return 2 if panel.info.get("deletion") == "observation" else 1
+
+
+def v5_request(engine, probes, tolerance, *, reference=False, deletion=1):
+    """A V5 solve request: JLA, the panel's deletion mode, supplied tolerance.
+    With controls the generic engine runs; the reference additionally selects
+    its production CMG_FULL_V2 route on all host cores."""
+    q = engine.default_request_v5(deletion)
+    if deletion == 2:
+        q.v4.v3.engine = 2  # leave-observation-out runs the generic engine
     v1 = q.v4.v3.v2.v1
     v1.probes = probes
     v1.pcg_tolerance = tolerance
@@ -155,9 +162,9 @@ def time_reference(panel, probes, tolerance, steps, warmup):
     for i in range(warmup + steps):
         e = abi.Engine(lib)
         t0 = time.perf_counter()
-        e.prepare(panel)
+        e.prepare(panel, deletion_mode=deletion_mode(panel))
         t1 = time.perf_counter()
-        q = v5_request(e, probes, tolerance, reference=True)
+        q = v5_request(e, probes, tolerance, reference=True, deletion=deletion_mode(panel))
         e.solve_v5(q, controls_count=len(panel.controls))
         res = e.result()
         t2 = time.perf_counter()
@@ -187,9 +194,9 @@ def time_form(lib, panel, controls, probes, tolerance, block, precond, precision
     from fevc_b200 import abi
 
     e = abi.Engine(lib)
-    e.prepare(panel)
+    e.prepare(panel, deletion_mode=deletion_mode(panel))
     e.device_options(block, precond, precision)
-    e.solve_v5(v5_request(e, probes, tolerance), controls_count=controls)
+    e.solve_v5(v5_request(e, probes, tolerance, deletion=deletion_mode(panel)), controls_count=controls)
     barrier()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(stream)
@@ -287,14 +294,14 @@ def main():
 
     e = abi.Engine(lib)
     t0 = time.perf_counter()
-    e.prepare(panel)
+    e.prepare(panel, deletion_mode=deletion_mode(panel))
     prepare_s = time.perf_counter() - t0
     e.device_options(args.block, args.precond)
     # N ranks: every rank contributes `probes` probes to one decomposition of
     # probes x N (weak scaling); the leverage accumulators are all-reduced and
     # the target draws gathered over NCCL (fevc_b200/sharded.py)
     total_probes = args.probes * world
-    req = v5_request(e, total_probes, args.tolerance)
+    req = v5_request(e, total_probes, args.tolerance, deletion=deletion_mode(panel))
     rhs = 1 + 3 * args.probes  # right-hand sides this rank solves per step
     collectives = None
     use_shards = world > 1 or args.sharded
@@ -373,7 +380,7 @@ def main():
     e2e_times = []
     for i in range(max(args.e2e_steps, 1) + 1):
         g = abi.Engine(lib)
-        g.prepare(panel)
+        g.prepare(panel, deletion_mode=deletion_mode(panel))
         g.device_options(args.block, args.precond)
         barrier()
         t0 = time.perf_counter()
@@ -413,7 +420,8 @@ def main():
             "data": "synthetic (seeded generator, fevc_b200/panel.py)",
             "config": {"workload": f"{args.workload} panel ({panel.info['workers']} workers, "
                                    f"{panel.info['firms']} firms, {panel.info['periods']} periods), "
-                                   f"{total_probes} probes, {controls} year controls, match deletion",
+                                   f"{total_probes} probes, {controls} year controls, "
+                                   f"{'observation' if deletion_mode(panel) == 2 else 'match'} deletion",
                        "probes": total_probes, "rhs_per_step": rhs * world, "tolerance": args.tolerance,
                        "block_columns": block, "preconditioner": "jacobi" if args.precond == 1 else "auto",
                        "controls": controls,
