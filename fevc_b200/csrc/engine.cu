@@ -1233,25 +1233,8 @@ int pcg_run_learned(DeviceEngine& e, BlockWork& w, Launch L, int iterations, Sol
   const double* c = e.learned->scalar_coefficients();
   PersistentPoly<K> P;
   PersistentPcg<K>& a = P.a;
-  a.n = e.n;
-  a.ptr = e.L_ptr.p;
-  a.col = e.L_col.p;
-  a.val = e.L_val.p;
-  a.diag = e.L_diag.p;
-  a.dinv = e.L_dinv.p;
-  a.nseg = e.lap_seg.count;
-  a.seg_row = e.lap_seg.row.p;
-  a.seg_begin = e.lap_seg.begin.p;
-  a.seg_end = e.lap_seg.end.p;
-  a.row_first = e.lap_seg.row_first.p;
-  a.seg_buf = w.seg_buf.p;
-  a.x = w.x.p;
-  a.r = w.r.p;
-  a.p = w.p.p;
-  a.partial_a = e.partial.p;
-  a.partial_b = e.partial.p + size_t(e.coop_blocks) * K;
-  a.s = w.s;
-  a.max_iters = std::min(iterations, LEARNED_CAP);
+  // matrix, balanced segment order, x, r, p, partials and state as for the Jacobi kernel
+  a = persistent_args<K>(e, w, std::min(iterations, LEARNED_CAP));
   P.y1 = w.y1.p;
   P.y2 = w.y2.p;
   P.z = w.z.p;

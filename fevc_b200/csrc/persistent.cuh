@@ -739,39 +739,42 @@ struct PersistentPoly {
   double c0, c1, c2, c3;
 };
 
-// Segment products of a vector (PRE: y0 = r / d on the fly)
+// The k-th segment of the work order: its id (the slot of its product), row,
+// whether it is the row's first segment, and its entries [b, e).  With the
+// balanced order (segments in decreasing length) when it is given, else in
+// storage order.
+template <int K>
+__device__ __forceinline__ void ordered_segment(const PersistentPcg<K>& a, size_t k, uint32_t& id, uint32_t& row,
+                                                bool& first, uint32_t& b, uint32_t& e) {
+  if (a.ord_id != nullptr) {
+    id = __ldg(a.ord_id + k);
+    const uint32_t f = __ldg(a.ord_flag + k);
+    row = f & ~SEG_FIRST;
+    first = (f & SEG_FIRST) != 0;
+    b = __ldg(a.ord_begin + k);
+    e = __ldg(a.ord_end + k);
+  } else {
+    id = uint32_t(k);
+    row = a.seg_row[k];
+    b = a.seg_begin[k];
+    e = a.seg_end[k];
+    first = b == a.ptr[row];
+  }
+}
+
+// Segment products of a vector (R_OVER_D: of y0 = r / d, scaled on the fly)
 template <int K, bool R_OVER_D>
 __device__ __forceinline__ void poly_products(const PersistentPcg<K>& a, const double* __restrict__ y, size_t gid,
                                               size_t ngroups, int c0) {
   constexpr int CPT = Cols<K>::CPT;
-  for (size_t sg = gid; sg < a.nseg; sg += ngroups) {
-    uint32_t b = a.seg_begin[sg], e = a.seg_end[sg];
+  for (size_t k = gid; k < a.nseg; k += ngroups) {
+    uint32_t id, row, b, e;
+    bool first;
+    ordered_segment<K>(a, k, id, row, first, b, e);
     double acc[CPT];
+    segment_gather<K, double, R_OVER_D>(a.col, a.val, a.dinv, y, b, e, c0, acc);
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
-    uint32_t i = b;
-    for (; i + 2 <= e; i += 2) {
-      uint32_t j0 = __ldg(a.col + i), j1 = __ldg(a.col + i + 1);
-      double a0 = __ldg(a.val + i), a1 = __ldg(a.val + i + 1);
-      if (R_OVER_D) {
-        a0 *= __ldg(a.dinv + j0);
-        a1 *= __ldg(a.dinv + j1);
-      }
-      const double* x0 = y + size_t(j0) * K + c0;
-      const double* x1 = y + size_t(j1) * K + c0;
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) acc[c] += a0 * x0[c] + a1 * x1[c];
-    }
-    if (i < e) {
-      uint32_t j0 = __ldg(a.col + i);
-      double a0 = __ldg(a.val + i);
-      if (R_OVER_D) a0 *= __ldg(a.dinv + j0);
-      const double* x0 = y + size_t(j0) * K + c0;
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) acc[c] += a0 * x0[c];
-    }
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) a.seg_buf[sg * K + c0 + c] = acc[c];
+    for (int c = 0; c < CPT; ++c) a.seg_buf[size_t(id) * K + c0 + c] = acc[c];
   }
 }
 
@@ -807,23 +810,17 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent_poly(Pers
       double v[1][CPT];
 #pragma unroll
       for (int c = 0; c < CPT; ++c) v[0][c] = 0.0;
-      for (size_t sg = gid; sg < a.nseg; sg += ngroups) {
-        uint32_t row = a.seg_row[sg], b = a.seg_begin[sg], e = a.seg_end[sg];
+      for (size_t k = gid; k < a.nseg; k += ngroups) {
+        uint32_t id, row, b, e;
+        bool first;
+        ordered_segment<K>(a, k, id, row, first, b, e);
         double acc[CPT];
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
-        for (uint32_t i = b; i < e; ++i) {
-          uint32_t j0 = __ldg(a.col + i);
-          double a0 = __ldg(a.val + i);
-          const double* x0 = a.p + size_t(j0) * K + c0;
-#pragma unroll
-          for (int c = 0; c < CPT; ++c) acc[c] += a0 * x0[c];
-        }
+        segment_gather<K, double, false>(a.col, a.val, a.dinv, a.p, b, e, c0, acc);
         const double* pr = a.p + size_t(row) * K + c0;
-        double d = (b == a.ptr[row]) ? a.diag[row] : 0.0;
+        const double d = first ? a.diag[row] : 0.0;
 #pragma unroll
         for (int c = 0; c < CPT; ++c) {
-          a.seg_buf[sg * K + c0 + c] = acc[c];
+          a.seg_buf[size_t(id) * K + c0 + c] = acc[c];
           v[0][c] += pr[c] * (d * pr[c] - acc[c]);
         }
       }
