@@ -276,6 +276,10 @@ struct DeviceEngine {
   uint64_t physical = 0;
   DBuf<uint64_t> unit_offset, row_rank_d, row_copy_offset, row_phys;
   DBuf<double> obs_row_acc, obs_copy_acc, control_lev, obs_out;
+  // leave-observation-out target sums per cell (cells x (1 + q)) and the
+  // cell-independent quadratic form sum_r w_r R_r R_r' (q x q, upper triangle)
+  DBuf<double> obs_cell_sums, obs_s2;
+  std::vector<double> obs_S2;
   // solve-long buffers
   DBuf<double> moments, unit_out, omega, fitted, fit_alpha, partial, small;
   DBuf<unsigned long long> error;
@@ -1512,9 +1516,9 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
         }
       CK(cudaMemcpyAsync(e.beta_buf.p, beta.data(), QMAX * K * sizeof(double), cudaMemcpyHostToDevice, L.s));
       if (e.observation)
-        k_generic_contract<K, true><<<L.grid, THREADS, 0, L.s>>>(
-            e.rows, e.q, nullptr, nullptr, e.row_cell.p, e.cell_worker.p, e.cell_firm.p, e.row_freq.p, e.row_y.p,
-            y_center, e.deleted.p, e.Rd.p, e.beta_buf.p, w.alpha.p, w.x.p, e.partial.p);
+        k_obs_contract_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.q, e.cell_worker.p, e.cell_firm.p,
+                                                             e.obs_cell_sums.p, e.beta_buf.p, w.alpha.p, w.x.p,
+                                                             e.partial.p);
       else
         k_generic_contract_units<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.q, e.unit_cell.p, e.cell_worker.p,
                                                                  e.cell_firm.p, e.unit_sums.p, e.beta_buf.p,
@@ -1524,6 +1528,24 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
       CK(cudaMemcpyAsync(g2.data(), w.tot.p, 2 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
       CK(cudaStreamSynchronize(L.s));
       res.timings.kernel_launches += 4;
+      if (e.observation && e.q > 0) {
+        // the cell-independent beta' S2 beta terms of every column and of the total
+        auto quad = [&](int ja, int jb) {
+          double acc = 0.0;
+          for (int k = 0; k < e.q; ++k)
+            for (int l = k; l < e.q; ++l) {
+              const double bk = beta[k * K + ja] + (jb >= 0 ? beta[k * K + jb] : 0.0);
+              const double bl = beta[l * K + ja] + (jb >= 0 ? beta[l * K + jb] : 0.0);
+              acc += (l == k ? 1.0 : 2.0) * e.obs_S2[k * QMAX + l] * bk * bl;
+            }
+          return acc;
+        };
+        for (int j = 0; j < np; ++j) {
+          g2[2 * j] += quad(2 * j, -1);
+          g2[2 * j + 1] += quad(2 * j + 1, -1);
+          g2[K + 2 * j] += quad(2 * j, 2 * j + 1);
+        }
+      }
       // reference draw: covariance = (total - worker - firm) / 2
       for (int j = 0; j < np; ++j) {
         double ww = g2[2 * j], ff = g2[2 * j + 1], tt = g2[K + 2 * j];
@@ -1868,6 +1890,19 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
                                                          : "finite-projection moment failed";
       fail(int32_t(code), "generic_jla_observation_adjustment", std::string(what) + " at row " + std::to_string(row));
     }
+    // the target contraction's per-cell sums of the deleted residuals
+    if (!e.obs_cell_sums.p) {
+      e.obs_cell_sums.alloc(size_t(e.C) * (1 + QMAX));
+      e.obs_s2.alloc(QMAX * QMAX);
+    }
+    k_obs_cell_target_sums<<<L.grid, THREADS, 0, L.s>>>(e.C, q, e.cell_rows_ptr.p, e.cell_rows.p, e.row_freq.p,
+                                                        e.row_y.p, outcome_mean(p, o.centering), e.deleted.p,
+                                                        e.Rd.p, e.obs_cell_sums.p, e.partial.p);
+    finish(e.partial.p, L.grid, QMAX * QMAX, e.obs_s2.p, L.s);
+    e.obs_S2.assign(QMAX * QMAX, 0.0);
+    CK(cudaMemcpyAsync(e.obs_S2.data(), e.obs_s2.p, QMAX * QMAX * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    res.timings.kernel_launches += 2;
   } else {
   // ---- deleted residuals of every match group
   {

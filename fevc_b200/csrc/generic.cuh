@@ -415,6 +415,128 @@ __global__ void k_generic_contract(uint32_t groups, int q, const uint64_t* __res
   block_reduce_cols<K, 2>(v, partial);
 }
 
+// Leave-observation-out target sums per cell.  Every row of a cell shares the
+// cell's FE solution u_c, so the row draw f (y - y_center) d u_r^2 with
+// u_r = u_c + R_r' beta sums over the cell's rows to
+//   S0 u_c^2 + 2 u_c (S1' beta) + beta' S2_c beta,
+// w_r = f (y - y_center) d:  S0 = sum w_r,  S1_k = sum w_r R_rk,  S2_c = sum w_r R_r R_r'.
+// out[c][0] = S0, out[c][1 + k] = S1_k (stride 1 + q); the beta' S2 beta terms
+// do not depend on the cell and are summed over all rows once:
+// partial[blk][k * q + l] for k <= l (the rest zero), reduced by k_finish.
+// Algebraically the row sum of `k_generic_contract<K, true>` (reference
+// `target_contraction`, generic_jla.rs:8926-8937), read once per solve instead
+// of once per target block.
+__global__ void k_obs_cell_target_sums(uint32_t cells, int q, const uint32_t* __restrict__ cell_rows_ptr,
+                                       const uint32_t* __restrict__ cell_rows, const double* __restrict__ row_freq,
+                                       const double* __restrict__ y, double y_center,
+                                       const double* __restrict__ deleted, const double* __restrict__ R,
+                                       double* __restrict__ out, double* __restrict__ partial) {
+  __shared__ double s_red[THREADS / 32][QMAX * QMAX];
+  double s2[QMAX * (QMAX + 1) / 2];
+#pragma unroll
+  for (int k = 0; k < QMAX * (QMAX + 1) / 2; ++k) s2[k] = 0.0;
+  for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
+    double s0 = 0.0, s1[QMAX];
+#pragma unroll
+    for (int k = 0; k < QMAX; ++k) s1[k] = 0.0;
+    for (uint32_t i = cell_rows_ptr[c]; i < cell_rows_ptr[c + 1]; ++i) {
+      const uint32_t r = cell_rows[i];
+      const double w = row_freq[r] * (y[r] - y_center) * deleted[r];
+      s0 += w;
+      double rr[QMAX];
+#pragma unroll
+      for (int k = 0; k < QMAX; ++k) rr[k] = k < q ? R[size_t(r) * q + k] : 0.0;
+      int t = 0;
+#pragma unroll
+      for (int k = 0; k < QMAX; ++k) {
+        s1[k] += w * rr[k];
+#pragma unroll
+        for (int l = k; l < QMAX; ++l, ++t) s2[t] += w * rr[k] * rr[l];
+      }
+    }
+    double* o = out + c * size_t(1 + q);
+    o[0] = s0;
+    for (int k = 0; k < q; ++k) o[1 + k] = s1[k];
+  }
+  // deterministic block sum of s2: warps by shuffle, then across warps
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int t = 0;
+#pragma unroll
+  for (int k = 0; k < QMAX; ++k)
+#pragma unroll
+    for (int l = k; l < QMAX; ++l, ++t) {
+      double v = s2[t];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) s_red[warp][k * QMAX + l] = v;
+    }
+  __syncthreads();
+  for (int i = threadIdx.x; i < QMAX * QMAX; i += blockDim.x) {
+    double v = 0.0;
+    for (int wi = 0; wi < int(blockDim.x >> 5); ++wi) v += s_red[wi][i];
+    const int k = i / QMAX, l = i % QMAX;
+    partial[size_t(blockIdx.x) * QMAX * QMAX + i] = (l >= k && k < q && l < q) ? v : 0.0;
+  }
+}
+
+// Leave-observation-out target draws over cells from k_obs_cell_target_sums:
+// draw_col += S0 u^2 + 2 u (S1' beta_col) per cell, the total side with
+// u = u_worker + u_firm and beta = beta_worker + beta_firm (the sum of the two
+// columns); the cell-independent beta' S2 beta terms are added by the host.
+// partial layout as in k_generic_contract.
+template <int K>
+__global__ void k_obs_contract_cells(uint32_t cells, int q, const uint32_t* __restrict__ cell_worker,
+                                     const uint32_t* __restrict__ cell_firm, const double* __restrict__ sums,
+                                     const double* __restrict__ beta /* [QMAX][K] */, const double* __restrict__ alpha,
+                                     const double* __restrict__ psi, double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  static_assert(CPT <= 2, "pairs of columns must sit in one thread or in adjacent lanes");
+  double v[2][CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
+  const int c0 = int(threadIdx.x % TPR) * CPT;
+  double bcol[QMAX][CPT];
+#pragma unroll
+  for (int k = 0; k < QMAX; ++k)
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) bcol[k][c] = k < q ? beta[k * K + c0 + c] : 0.0;
+  size_t total = size_t(cells) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    size_t t = base + threadIdx.x;
+    bool live = t < total;
+    size_t c = live ? t / TPR : 0;
+    double u[CPT], b1[CPT], s0 = 0.0;
+#pragma unroll
+    for (int cc = 0; cc < CPT; ++cc) u[cc] = b1[cc] = 0.0;
+    if (live) {
+      const double* sc = sums + c * size_t(1 + q);
+      s0 = sc[0];
+      size_t wb = size_t(cell_worker[c]) * K + c0, fb = size_t(cell_firm[c]) * K + c0;
+#pragma unroll
+      for (int cc = 0; cc < CPT; ++cc) u[cc] = alpha[wb + cc] + psi[fb + cc];
+#pragma unroll
+      for (int k = 0; k < QMAX; ++k)
+        if (k < q) {
+          const double s1 = sc[1 + k];
+#pragma unroll
+          for (int cc = 0; cc < CPT; ++cc) b1[cc] += s1 * bcol[k][cc];
+        }
+    }
+#pragma unroll
+    for (int cc = 0; cc < CPT; ++cc) v[0][cc] += s0 * u[cc] * u[cc] + 2.0 * u[cc] * b1[cc];
+    if (CPT == 2) {
+      const double uu = u[0] + u[CPT - 1], bb = b1[0] + b1[CPT - 1];
+      v[1][0] += s0 * uu * uu + 2.0 * uu * bb;
+    } else {
+      const double uo = __shfl_xor_sync(0xffffffffu, u[0], 1);
+      const double bo = __shfl_xor_sync(0xffffffffu, b1[0], 1);
+      const double uu = u[0] + uo, bb = b1[0] + bo;
+      if ((c0 & 1) == 0) v[1][0] += s0 * uu * uu + 2.0 * uu * bb;
+    }
+  }
+  block_reduce_cols<K, 2>(v, partial);
+}
+
 // Cell-level control sums of the target solutions: partial[blk][k][col] =
 // sum over cells of CQ[c][k] u_c(col), CQ[c][k] = sum over the cell's rows of
 // f Q_rk (computed once with the control geometry) and u_c = alpha_w + psi_f;

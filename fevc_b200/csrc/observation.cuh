@@ -26,7 +26,9 @@ __device__ __forceinline__ void neumaier_add(double& sum, double& corr, double v
 }
 
 // One probe block of K columns (first a multiple of 4; columns >= ncols carry a
-// zero prediction).  TPR lanes share a row, each holding CPT columns.
+// zero prediction).  Each lane holds the four columns of one Counter-V1 block
+// (K / 4 lanes per row, 32 / (K / 4) rows per warp), so every Philox block a
+// copy needs is computed once.
 // row_acc[r][4] = (sum P^2, its compensation, sum P^4, its compensation);
 // copy_acc[c][4] = (sum a P, compensation, sum a P^3, compensation), c the
 // copy's physical index (rows in row order, copies consecutive).
@@ -37,25 +39,26 @@ __global__ void k_obs_moments(uint32_t rows, int ncols, const uint32_t* __restri
                               const uint64_t* __restrict__ row_phys, PhiloxKey key, uint64_t first,
                               const double* __restrict__ alpha, const double* __restrict__ psi,
                               double* __restrict__ row_acc, double* __restrict__ copy_acc) {
-  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
-  static_assert(CPT <= 4, "the columns of one thread must fall in one Philox block");
-  const int c0 = int(threadIdx.x % TPR) * CPT;
+  constexpr int CPL = K >= 4 ? 4 : K;  // columns per lane
+  constexpr int LPR = K / CPL;         // lanes per row
+  static_assert(K % CPL == 0 && LPR <= 32 && 32 % LPR == 0, "rows must tile a warp");
+  const int c0 = int(threadIdx.x % LPR) * CPL;
   // all columns of this lane sit in one probe block: (first + c0) / 4
   const uint64_t pblock = (first + uint64_t(c0)) >> 2;
   const int lane0 = int((first + uint64_t(c0)) & 3);
-  size_t total = size_t(rows) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  size_t total = size_t(rows) * LPR, stride = size_t(gridDim.x) * blockDim.x;
   for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
     size_t t = base + threadIdx.x;
     bool live = t < total;
-    uint32_t r = live ? uint32_t(t / TPR) : 0;
-    double P[CPT];
+    uint32_t r = live ? uint32_t(t / LPR) : 0;
+    double P[CPL];
     double s2 = 0.0, s4 = 0.0;
     uint64_t ncopy = 0, off = 0, ph = 0, ent = 0;
     if (live) {
       uint32_t cell = row_cell[r];
       size_t wi = size_t(cell_worker[cell]) * K, fi = size_t(cell_firm[cell]) * K;
 #pragma unroll
-      for (int c = 0; c < CPT; ++c) {
+      for (int c = 0; c < CPL; ++c) {
         P[c] = (c0 + c < ncols) ? alpha[wi + c0 + c] + psi[fi + c0 + c] : 0.0;
         double p2 = P[c] * P[c];
         s2 += p2;
@@ -67,10 +70,10 @@ __global__ void k_obs_moments(uint32_t rows, int ncols, const uint32_t* __restri
       ent = row_rank[r];
     } else {
 #pragma unroll
-      for (int c = 0; c < CPT; ++c) P[c] = 0.0;
+      for (int c = 0; c < CPL; ++c) P[c] = 0.0;
     }
 #pragma unroll
-    for (int o = TPR / 2; o > 0; o >>= 1) {
+    for (int o = LPR / 2; o > 0; o >>= 1) {
       s2 += __shfl_xor_sync(0xffffffffu, s2, o);
       s4 += __shfl_xor_sync(0xffffffffu, s4, o);
     }
@@ -79,16 +82,16 @@ __global__ void k_obs_moments(uint32_t rows, int ncols, const uint32_t* __restri
       neumaier_add(a[0], a[1], s2);
       neumaier_add(a[2], a[3], s4);
     }
-    // copies: the warp walks the longest row of its groups in lock step
+    // copies: the warp walks the longest row of its rows in lock step
     uint64_t most = ncopy;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       uint64_t other = __shfl_xor_sync(0xffffffffu, most, o);
       most = other > most ? other : most;
     }
-    uint64_t word_at = ~uint64_t(0), bits[CPT];
+    uint64_t word_at = ~uint64_t(0), bits[CPL];
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) bits[c] = 0;
+    for (int c = 0; c < CPL; ++c) bits[c] = 0;
     for (uint64_t i = 0; i < most; ++i) {
       double f1 = 0.0, f3 = 0.0;
       bool mine = live && i < ncopy;
@@ -98,7 +101,7 @@ __global__ void k_obs_moments(uint32_t rows, int ncols, const uint32_t* __restri
           uint64_t blk[4];
           philox_block(key, ent, pblock, word, TAG_LEVERAGE, blk);
 #pragma unroll
-          for (int c = 0; c < CPT; ++c) {
+          for (int c = 0; c < CPL; ++c) {
             int l = (lane0 + c) & 3;  // select without a dynamically indexed array
             bits[c] = l == 0 ? blk[0] : l == 1 ? blk[1] : l == 2 ? blk[2] : blk[3];
           }
@@ -106,7 +109,7 @@ __global__ void k_obs_moments(uint32_t rows, int ncols, const uint32_t* __restri
         }
         int bit = int(cn & 63);
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) {
+        for (int c = 0; c < CPL; ++c) {
           double a = ((bits[c] >> bit) & 1) ? 1.0 : -1.0;
           double p = P[c];
           f1 += a * p;
@@ -114,7 +117,7 @@ __global__ void k_obs_moments(uint32_t rows, int ncols, const uint32_t* __restri
         }
       }
 #pragma unroll
-      for (int o = TPR / 2; o > 0; o >>= 1) {
+      for (int o = LPR / 2; o > 0; o >>= 1) {
         f1 += __shfl_xor_sync(0xffffffffu, f1, o);
         f3 += __shfl_xor_sync(0xffffffffu, f3, o);
       }
