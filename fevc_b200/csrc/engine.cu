@@ -1123,6 +1123,14 @@ int pcg_run_mixed(DeviceEngine& e, BlockWork& w, Launch L, int iterations, Solve
     a.row_first = e.lap_seg.row_first.p;
     a.seg_flag = e.lap_seg.row_flag.p;
     a.vald = e.L_vald32.p;
+    a.ord_id = e.lap_seg.ord_id.p;
+    a.ord_flag = e.lap_seg.ord_flag.p;
+    a.ord_begin = e.lap_seg.ord_begin.p;
+    a.ord_end = e.lap_seg.ord_end.p;
+    a.heavy_rows = e.lap_seg.heavy_rows.p;
+    a.light_rows = e.lap_seg.light_rows.p;
+    a.nheavy = e.lap_seg.nheavy;
+    a.nlight = e.lap_seg.nlight;
     a.seg_buf = w.seg32.p;
     a.x = w.x32.p;
     a.r = w.r32.p;
@@ -1133,8 +1141,11 @@ int pcg_run_mixed(DeviceEngine& e, BlockWork& w, Launch L, int iterations, Solve
     a.s = w.s_in;
     a.max_iters = iterations - done;
     void* args[] = {&a};
-    const void* fn = two_barrier_form<K, float>() ? (const void*)k_pcg_persistent_cg<K, float>
-                                                  : (const void*)k_pcg_persistent<K, float>;
+    // one warp per segment (K = 64): the balanced three-barrier form with
+    // warp-broadcast gathers and the pipelined product phase, as in double
+    const void* fn = Cols<K>::TPR == 32          ? (const void*)k_pcg_persistent<K, float, true, true>
+                     : two_barrier_form<K, float>() ? (const void*)k_pcg_persistent_cg<K, float>
+                                                    : (const void*)k_pcg_persistent<K, float>;
     CK(cudaLaunchCooperativeKernel(fn, dim3(e.coop_blocks),
                                    dim3(PERSIST_THREADS), args, 0, L.s));
     std::vector<int> it(K);
