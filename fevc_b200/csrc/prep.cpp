@@ -7,6 +7,8 @@
 #include "radix.h"
 
 #include <algorithm>
+#include <omp.h>
+#include <atomic>
 #include <parallel/algorithm>
 #include <functional>
 #include <exception>
@@ -173,6 +175,33 @@ size_t count_true(const std::vector<uint8_t>& m) {
   size_t c = 0;
   for (uint8_t v : m) c += v;
   return c;
+}
+
+// Indices of the true entries in increasing order (chunks counted and filled
+// on all host cores).
+std::vector<uint64_t> active_indices(const std::vector<uint8_t>& m) {
+  const size_t n = m.size();
+  const int threads = n >= (size_t(1) << 20) ? std::max(1, omp_get_max_threads()) : 1;
+  std::vector<size_t> count(size_t(threads) + 1, 0);
+  std::vector<uint64_t> out;
+#pragma omp parallel num_threads(threads)
+  {
+    const int t = omp_get_thread_num();
+    const size_t b = n * t / threads, e = n * (t + 1) / threads;
+    size_t c = 0;
+    for (size_t i = b; i < e; ++i) c += m[i] != 0;
+    count[t + 1] = c;
+#pragma omp barrier
+#pragma omp single
+    {
+      for (int u = 0; u < threads; ++u) count[u + 1] += count[u];
+      out.resize(count[threads]);
+    }
+    size_t at = count[t];
+    for (size_t i = b; i < e; ++i)
+      if (m[i]) out[at++] = i;
+  }
+  return out;
 }
 
 // Bipartite graph with workers 0..W-1 and firms W..W+F-1 in CSR form; an arc
@@ -941,20 +970,32 @@ std::vector<uint8_t> select_observation_graph(const Canonical& in, GraphReceipt&
     wrows[in.worker[r]] += 1;
     wmass[in.worker[r]] += in.frequency[r];
   }
+  // Workers with one firm (leaves) are left out of the traversed graph: a
+  // leaf shares its firm's component, is never an articulation point and
+  // changes no other worker's articulation status.  Firms reached only by
+  // leaves form components of their own, added after the traversal.
+  std::vector<uint32_t> degree(W, 0), leaf_firm(W, MISSING);
+  for (size_t c = 0; c < in.coord_worker.size(); ++c) degree[in.coord_worker[c]]++;
+  for (size_t c = 0; c < in.coord_worker.size(); ++c)
+    if (degree[in.coord_worker[c]] == 1) leaf_firm[in.coord_worker[c]] = in.coord_firm[c];
   Graph g;
+  std::vector<uint32_t> edge_worker;  // worker of each traversed edge
   {
-    std::vector<uint32_t> eu(in.coord_worker.size()), ev(in.coord_worker.size());
-    for (size_t c = 0; c < eu.size(); ++c) {
-      eu[c] = in.coord_worker[c];
-      ev[c] = uint32_t(W + in.coord_firm[c]);
-    }
+    std::vector<uint32_t> eu, ev;
+    for (size_t c = 0; c < in.coord_worker.size(); ++c)
+      if (degree[in.coord_worker[c]] > 1) {
+        eu.push_back(in.coord_worker[c]);
+        ev.push_back(uint32_t(W + in.coord_firm[c]));
+      }
+    edge_worker = eu;
     g = make_graph(W + in.firms, eu, ev);
   }
-  std::vector<uint8_t> wact(W, 0), on(in.coord_worker.size(), 0);
+  std::vector<uint8_t> wact(W, 0), on(edge_worker.size(), 0);
   for (size_t w = 0; w < W; ++w) wact[w] = wrows[w] > 0;
   auto mark = [&] {
     size_t edges = 0;
-    for (size_t c = 0; c < on.size(); ++c) edges += (on[c] = wact[in.coord_worker[c]]);
+    for (size_t c = 0; c < in.coord_worker.size(); ++c) edges += wact[in.coord_worker[c]];
+    for (size_t e = 0; e < on.size(); ++e) on[e] = wact[edge_worker[e]];
     if (!edges) fail(GRAPH_EMPTY, "graph", "active graph is empty");
     return edges;
   };
@@ -988,6 +1029,12 @@ std::vector<uint8_t> select_observation_graph(const Canonical& in, GraphReceipt&
       }
       ++comps;
     }
+    for (size_t w = 0; w < W; ++w)
+      if (wact[w] && degree[w] == 1) {
+        uint32_t& fl = label[W + leaf_firm[w]];
+        if (fl == MISSING) fl = uint32_t(comps++);  // a firm with leaves only
+        label[w] = fl;
+      }
     if (comps == 0) fail(GRAPH_EMPTY, "graph", "no connected worker-firm component remains");
     std::vector<uint64_t> firms(comps, 0), mass(comps, 0);
     for (size_t f = 0; f < in.firms; ++f)
@@ -1067,10 +1114,9 @@ std::vector<uint8_t> select_observation_graph(const Canonical& in, GraphReceipt&
 Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, bool implicit_match) {
   if (active.size() != in.rows()) fail(INVALID_INPUT, "compression", "active mask has the wrong length");
   Compressed p;
-  for (size_t r = 0; r < in.rows(); ++r)
-    if (active[r]) p.retained_rows.push_back(r);
-    else if (implicit_match)
-      fail(INTERNAL_INVARIANT_FAILED, "compression", "the certified implicit-match route must retain every row");
+  if (implicit_match && count_true(active) != in.rows())
+    fail(INTERNAL_INVARIANT_FAILED, "compression", "the certified implicit-match route must retain every row");
+  p.retained_rows = active_indices(active);
   size_t R = p.retained_rows.size();
   if (R == 0) fail(GRAPH_EMPTY, "compression", "no rows remain after graph selection");
 
@@ -1082,7 +1128,8 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
       return map;
     }
     std::vector<uint8_t> present(levels, 0);
-    for (uint64_t r : p.retained_rows) present[values[r]] = 1;
+#pragma omp parallel for schedule(static) if (R >= 65536)
+    for (size_t i = 0; i < R; ++i) present[values[p.retained_rows[i]]] = 1;
     uint32_t next = 0;
     for (size_t l = 0; l < levels; ++l)
       if (present[l]) map[l] = next++;
@@ -1096,6 +1143,7 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
   p.row_worker.resize(R);
   p.row_firm.resize(R);
   p.row_deletion.resize(R);
+#pragma omp parallel for schedule(static) if (R >= 65536)
   for (size_t i = 0; i < R; ++i) {
     uint64_t r = p.retained_rows[i];
     p.row_worker[i] = wmap[in.worker[r]];
@@ -1108,49 +1156,67 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
   p.deletion_units = D;
 
   // cells: rows sorted by (worker, firm, source row)
+  // stable radix sort of the (worker, firm) keys: equal keys keep row order
   std::vector<uint32_t> order(R);
   std::iota(order.begin(), order.end(), 0u);
   std::vector<uint64_t> key(R);
+#pragma omp parallel for schedule(static) if (R >= 65536)
   for (size_t i = 0; i < R; ++i) key[i] = (uint64_t(p.row_worker[i]) << 32) | p.row_firm[i];
-  sort_rows(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+  {
+    std::vector<uint64_t> sorted_key = key;
+    radix_sort_pairs(sorted_key, order);
+  }
   p.row_cell.assign(R, MISSING);
-  for (size_t cur = 0; cur < R;) {
-    size_t begin = cur;
-    uint64_t k = key[order[cur]];
-    while (cur < R && key[order[cur]] == k) ++cur;
-    uint32_t cell = uint32_t(p.cell_worker.size());
+  // cell boundaries in the sorted order, then every cell's Kahan sums (in row
+  // order, as a sequential walk would take them) independently
+  std::vector<size_t> cell_start;
+  for (size_t i = 0; i < R; ++i)
+    if (i == 0 || key[order[i]] != key[order[i - 1]]) cell_start.push_back(i);
+  const size_t NC = cell_start.size();
+  cell_start.push_back(R);
+  p.cell_worker.resize(NC);
+  p.cell_firm.resize(NC);
+  p.cell_weight.resize(NC);
+  p.cell_outcome_sum.resize(NC);
+  p.cell_target_sum.resize(NC);
+  std::atomic<bool> bad_moment{false};
+#pragma omp parallel for schedule(static) if (NC >= 65536)
+  for (size_t cell = 0; cell < NC; ++cell) {
+    const uint64_t k = key[order[cell_start[cell]]];
     KahanSum wsum, ysum, tsum;
-    for (size_t j = begin; j < cur; ++j) {
+    for (size_t j = cell_start[cell]; j < cell_start[cell + 1]; ++j) {
       uint32_t lr = order[j];
       uint64_t src = p.retained_rows[lr];
       double wt = double(in.frequency[src]);
       double y = wt * in.outcome[src];
-      if (!std::isfinite(wt) || !std::isfinite(y))
-        fail(INVALID_WEIGHT, "compression", "weighted cell moment is nonfinite");
+      if (!std::isfinite(wt) || !std::isfinite(y)) bad_moment = true;
       wsum.add(wt);
       ysum.add(y);
       tsum.add(in.target[src]);
-      p.row_cell[lr] = cell;
+      p.row_cell[lr] = uint32_t(cell);
     }
-    p.cell_worker.push_back(uint32_t(k >> 32));
-    p.cell_firm.push_back(uint32_t(k & 0xffffffffu));
-    p.cell_weight.push_back(wsum.finish());
-    p.cell_outcome_sum.push_back(ysum.finish());
-    p.cell_target_sum.push_back(tsum.finish());
+    p.cell_worker[cell] = uint32_t(k >> 32);
+    p.cell_firm[cell] = uint32_t(k & 0xffffffffu);
+    p.cell_weight[cell] = wsum.finish();
+    p.cell_outcome_sum[cell] = ysum.finish();
+    p.cell_target_sum[cell] = tsum.finish();
   }
+  if (bad_moment) fail(INVALID_WEIGHT, "compression", "weighted cell moment is nonfinite");
   size_t C = p.cell_worker.size();
   p.cells = C;
   {
     std::vector<uint32_t> ord(C);
     std::iota(ord.begin(), ord.end(), 0u);
     p.worker_index = grouped_from_order(W, p.cell_worker, std::move(ord));
-    std::vector<uint32_t> ford(C);
-    std::iota(ford.begin(), ford.end(), 0u);
-    sort_rows(ford.begin(), ford.end(), [&](uint32_t a, uint32_t b) {
-      if (p.cell_firm[a] != p.cell_firm[b]) return p.cell_firm[a] < p.cell_firm[b];
-      if (p.cell_worker[a] != p.cell_worker[b]) return p.cell_worker[a] < p.cell_worker[b];
-      return a < b;
-    });
+    // cells are numbered in (worker, firm) order, so a stable counting sort by
+    // firm gives the (firm, worker, cell) order
+    std::vector<uint32_t> fptr(F + 1, 0), ford(C);
+    for (size_t c = 0; c < C; ++c) fptr[p.cell_firm[c] + 1]++;
+    for (size_t f = 0; f < F; ++f) fptr[f + 1] += fptr[f];
+    {
+      std::vector<uint32_t> at(fptr.begin(), fptr.end() - 1);
+      for (size_t c = 0; c < C; ++c) ford[at[p.cell_firm[c]]++] = uint32_t(c);
+    }
     p.firm_index = grouped_from_order(F, p.cell_firm, std::move(ford));
   }
 
@@ -1173,9 +1239,20 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
       }
       return 0;
     };
-    std::vector<uint32_t> tord(R);
-    std::iota(tord.begin(), tord.end(), 0u);
-    sort_rows(tord.begin(), tord.end(), [&](uint32_t a, uint32_t b) { return cmp(a, b) < 0; });
+    // the comparison leads with (worker, firm), the cell key: `order` already
+    // holds the rows by cell with ties in row order, so a stable sort inside
+    // every cell gives the stable sort of all rows
+    std::vector<uint32_t> tord = order;
+    {
+      std::vector<size_t> cell_begin(C + 1, 0);
+      for (size_t i = 0; i < R; ++i) cell_begin[p.row_cell[i] + 1]++;
+      for (size_t c = 0; c < C; ++c) cell_begin[c + 1] += cell_begin[c];
+#pragma omp parallel for schedule(dynamic, 4096) if (C >= 65536)
+      for (size_t c = 0; c < C; ++c)
+        if (cell_begin[c + 1] - cell_begin[c] > 1)
+          std::stable_sort(tord.begin() + cell_begin[c], tord.begin() + cell_begin[c + 1],
+                           [&](uint32_t a, uint32_t b) { return cmp(a, b) < 0; });
+    }
     p.row_target.assign(R, MISSING);
     uint32_t current = 0;
     for (size_t i = 0; i < R; ++i) {
@@ -1191,13 +1268,17 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
   p.outcome.resize(R);
   p.frequency.resize(R);
   p.target.resize(R);
+#pragma omp parallel for schedule(static) if (R >= 65536)
   for (size_t i = 0; i < R; ++i) {
     uint64_t r = p.retained_rows[i];
-    p.physical_total += in.frequency[r];
-    tt.add(in.target[r]);
     p.outcome[i] = in.outcome[r];
     p.frequency[i] = in.frequency[r];
     p.target[i] = in.target[r];
+  }
+  // the totals in row order
+  for (size_t i = 0; i < R; ++i) {
+    p.physical_total += p.frequency[i];
+    tt.add(p.target[i]);
   }
   p.target_total = tt.finish();
   if (!std::isfinite(p.target_total) || p.target_total <= 0.0)
@@ -1205,6 +1286,7 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
   p.rows_physical = p.physical_total;
   for (auto& ctl : in.controls) {
     std::vector<double> col(R);
+#pragma omp parallel for schedule(static) if (R >= 65536)
     for (size_t i = 0; i < R; ++i) col[i] = ctl[p.retained_rows[i]];
     p.controls.push_back(std::move(col));
   }
