@@ -1438,6 +1438,29 @@ void build_target_strata(const Compressed& p, const std::vector<double>& per_cop
 // `observation_classes`, generic_jla.rs:4158-4215, `observation_addresses`,
 // generic_jla/statistical_batches.rs:15-54, `rademacher_copy`,
 // generic_jla.rs:10322-10329).
+// Rows grouped by cell, in row order inside each cell (a stable counting
+// sort), and the cell offsets.  Cells are numbered in (worker, firm) order,
+// so a comparison that leads with (worker, firm) or with the cell sorts all
+// rows stably when every cell's range is stable-sorted by the rest of it.
+static std::vector<uint32_t> rows_by_cell(const Compressed& p, std::vector<size_t>& begin) {
+  const size_t R = p.rows(), C = p.cells;
+  begin.assign(C + 1, 0);
+  for (size_t r = 0; r < R; ++r) begin[p.row_cell[r] + 1]++;
+  for (size_t c = 0; c < C; ++c) begin[c + 1] += begin[c];
+  std::vector<uint32_t> order(R);
+  std::vector<size_t> at(begin.begin(), begin.end() - 1);
+  for (size_t r = 0; r < R; ++r) order[at[p.row_cell[r]]++] = uint32_t(r);
+  return order;
+}
+
+template <class Less>
+static void sort_within_cells(std::vector<uint32_t>& order, const std::vector<size_t>& begin, Less less) {
+  const size_t C = begin.size() - 1;
+#pragma omp parallel for schedule(dynamic, 4096) if (C >= 65536)
+  for (size_t c = 0; c < C; ++c)
+    if (begin[c + 1] - begin[c] > 1) std::stable_sort(order.begin() + begin[c], order.begin() + begin[c + 1], less);
+}
+
 static void build_observation_units(const Compressed& p, const std::vector<double>& per_copy, JlaPlan& plan) {
   size_t R = p.rows();
   bool has_order = !p.probe_order.empty();
@@ -1455,9 +1478,9 @@ static void build_observation_units(const Compressed& p, const std::vector<doubl
     if (has_order) return ordered_f64(p.probe_order[a], p.probe_order[b]);
     return 0;
   };
-  std::vector<uint32_t> order(R);
-  std::iota(order.begin(), order.end(), 0u);
-  sort_rows(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return sem(a, b) < 0; });
+  std::vector<size_t> cell_begin;
+  std::vector<uint32_t> order = rows_by_cell(p, cell_begin);
+  sort_within_cells(order, cell_begin, [&](uint32_t a, uint32_t b) { return sem(a, b) < 0; });
   plan.row_rank.assign(R, 0);
   uint64_t current = 0;
   for (size_t i = 0; i < R; ++i) {
@@ -1574,10 +1597,9 @@ JlaPlan build_generic_plan(const Compressed& p, Deletion deletion) {
 // `target_plan`, generic_jla.rs:3902-3995).
 void build_target_strata(const Compressed& p, const std::vector<double>& per_copy, JlaPlan& plan) {
   size_t R = p.rows();
-  std::vector<uint32_t> tord(R);
-  std::iota(tord.begin(), tord.end(), 0u);
-  sort_rows(tord.begin(), tord.end(), [&](uint32_t a, uint32_t b) {
-    if (p.row_cell[a] != p.row_cell[b]) return p.row_cell[a] < p.row_cell[b];
+  std::vector<size_t> cell_begin;
+  std::vector<uint32_t> tord = rows_by_cell(p, cell_begin);
+  sort_within_cells(tord, cell_begin, [&](uint32_t a, uint32_t b) {
     int c = total_cmp(canonical_zero(per_copy[a]), canonical_zero(per_copy[b]));
     if (c) return c < 0;
     return plan.row_rank[a] < plan.row_rank[b];
