@@ -102,6 +102,26 @@ void upload(DBuf<T>& d, const std::vector<T>& h, cudaStream_t s, uint64_t& count
   }
 }
 
+// Upload n elements written by fill(T* dst) straight into a pinned staging
+// block (when a stager is bound) to d.p + offset: no intermediate host vector,
+// no second copy.  d must already hold offset + n elements.
+template <class T, class Fill>
+void upload_fill(DBuf<T>& d, size_t offset, size_t n, Fill fill, cudaStream_t s, uint64_t& counter) {
+  if (n == 0) return;
+  const size_t bytes = n * sizeof(T);
+  if (HostStager* st = bound_stager()) {
+    T* pin = static_cast<T*>(st->take(bytes));
+    fill(pin);
+    CK(cudaMemcpyAsync(d.p + offset, pin, bytes, cudaMemcpyHostToDevice, s));
+  } else {
+    std::vector<T> h(n);
+    fill(h.data());
+    CK(cudaMemcpyAsync(d.p + offset, h.data(), bytes, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));  // the host vector goes out of scope
+  }
+  counter += bytes;
+}
+
 // Column layout of a block of K right-hand sides stored vertex-interleaved
 // (value of column j at vertex i is x[i*K + j]).  A row is handled by TPR
 // threads, each owning CPT consecutive columns, so a warp touches whole

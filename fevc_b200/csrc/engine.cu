@@ -385,7 +385,7 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   // They run on their own threads (bound to this device); their uploads share
   // the engine's stream and fill disjoint buffers.  The hybrid Laplacian is
   // then assembled on the device.
-  uint64_t task_h2d[6] = {0, 0, 0, 0, 0, 0};
+  uint64_t task_h2d[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   (void)grid_blocks();  // initialise the cached grid size before the threads use it
   auto cells_task = [&] {
     uint64_t& h2d = task_h2d[0];
@@ -481,20 +481,28 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
       fail(UNSUPPORTED_FEATURE, "generic_jla", "the device engine handles at most 8 control columns");
     e->rows = uint32_t(R);
   }
-  auto rows_task = [&] {  // per-row cell, frequency, outcome, controls (row-major)
+  auto rows_task = [&] {  // per-row cell, frequency and outcome
     uint64_t& h2d = task_h2d[3];
-    std::vector<double> freq(R), Q(R * e->q);
-    for (size_t r = 0; r < R; ++r) {
-      freq[r] = double(p.frequency[r]);
-      for (int k = 0; k < e->q; ++k) Q[r * e->q + k] = p.controls[k][r];
-    }
     upload(e->row_cell, p.row_cell, s, h2d);
-    upload(e->row_freq, freq, s, h2d);
+    e->row_freq.alloc(R);
+    upload_fill(e->row_freq, 0, R, [&](double* d) {
+      for (size_t r = 0; r < R; ++r) d[r] = double(p.frequency[r]);
+    }, s, h2d);
     upload(e->row_y, p.outcome, s, h2d);
-    upload(e->Qd, Q, s, h2d);
-    e->Rd.alloc(R * e->q);
-    e->residual.alloc(R);
-    e->deleted.alloc(R);
+  };
+  // the controls row-major (r * q + k), transposed straight into pinned
+  // blocks by two tasks over halves of the rows
+  auto controls_task = [&](int half) {
+    return [&, half] {
+      uint64_t& h2d = task_h2d[6 + half];
+      const size_t q = size_t(e->q), b = half ? R / 2 : 0, end = half ? R : R / 2;
+      upload_fill(e->Qd, b * q, (end - b) * q, [&](double* d) {
+        for (size_t k = 0; k < q; ++k) {
+          const double* col = p.controls[k].data();
+          for (size_t r = b; r < end; ++r) d[(r - b) * q + k] = col[r];
+        }
+      }, s, h2d);
+    };
   };
   auto cell_rows_task = [&] {  // rows of every cell (stable counting sort)
     uint64_t& h2d = task_h2d[4];
@@ -537,7 +545,13 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   };
   std::vector<std::function<void()>> tasks = {cells_task, units_task, strata_task};
   if (plan.generic) {
+    e->Qd.alloc(R * e->q);
+    e->Rd.alloc(R * e->q);
+    e->residual.alloc(R);
+    e->deleted.alloc(R);
     tasks.push_back(rows_task);
+    tasks.push_back(controls_task(0));
+    tasks.push_back(controls_task(1));
     tasks.push_back(cell_rows_task);
     tasks.push_back(groups_task);
   }
