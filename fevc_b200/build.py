@@ -65,7 +65,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
         src, obj = CSRC / name, BUILD / (name + ".o")
         objs.append(obj)
         if _stale(obj, src):
-            cmd = [nvcc, GENCODE, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC",
+            cmd = [nvcc, GENCODE, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp",
                    "--expt-relaxed-constexpr", f"-I{CSRC}", f"-I{INCLUDE}", "-c", str(src), "-o", str(obj)]
             if ptxas_info:
                 cmd.insert(1, "-Xptxas=-v")

@@ -421,19 +421,26 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
       for (size_t c = 0; c < p.cells; ++c) uptr[c + 1] += uptr[c];
       std::vector<uint32_t> cur(uptr.begin(), uptr.end() - 1), order(R);
       for (size_t r = 0; r < R; ++r) order[cur[p.row_cell[r]]++] = uint32_t(r);
-      std::vector<uint64_t> urank(R), ucount(R), uoff(R), phys(R + 1, 0);
-      for (size_t i = 0; i < R; ++i) {
-        uint32_t r = order[i];
-        urank[i] = plan.row_rank[r];
-        ucount[i] = p.frequency[r];
-        uoff[i] = plan.row_copy_offset[r];
-      }
+      std::vector<uint64_t> phys(R + 1, 0);
       for (size_t r = 0; r < R; ++r) phys[r + 1] = phys[r] + p.frequency[r];
       e->physical = phys[R];
       upload(e->unit_ptr, uptr, s, h2d);
-      upload(e->unit_rank, urank, s, h2d);
-      upload(e->unit_count, ucount, s, h2d);
-      upload(e->unit_offset, uoff, s, h2d);
+      // unit arrays written straight into pinned staging blocks
+      e->unit_rank.alloc(R);
+      e->unit_count.alloc(R);
+      e->unit_offset.alloc(R);
+      upload_fill(e->unit_rank, 0, R, [&](uint64_t* d) {
+#pragma omp parallel for schedule(static) if (R >= 65536)
+        for (size_t i = 0; i < R; ++i) d[i] = plan.row_rank[order[i]];
+      }, s, h2d);
+      upload_fill(e->unit_count, 0, R, [&](uint64_t* d) {
+#pragma omp parallel for schedule(static) if (R >= 65536)
+        for (size_t i = 0; i < R; ++i) d[i] = p.frequency[order[i]];
+      }, s, h2d);
+      upload_fill(e->unit_offset, 0, R, [&](uint64_t* d) {
+#pragma omp parallel for schedule(static) if (R >= 65536)
+        for (size_t i = 0; i < R; ++i) d[i] = plan.row_copy_offset[order[i]];
+      }, s, h2d);
       upload(e->row_rank_d, plan.row_rank, s, h2d);
       upload(e->row_copy_offset, plan.row_copy_offset, s, h2d);
       upload(e->row_phys, phys, s, h2d);
@@ -448,27 +455,39 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
       std::vector<uint32_t> cur(uptr.begin(), uptr.end() - 1);
       e->unit_group.assign(plan.del_cell.size(), 0);
       for (size_t g = 0; g < plan.del_cell.size(); ++g) e->unit_group[cur[plan.del_cell[g]]++] = uint32_t(g);
-      std::vector<uint32_t> ucell(e->G);
-      std::vector<uint64_t> urank(e->G), ucount(e->G);
-      std::vector<double> uout(e->G), ucf(e->G), usq(e->G);
-      for (size_t i = 0; i < e->G; ++i) {
-        uint32_t g = e->unit_group[i];
-        ucell[i] = plan.del_cell[g];
-        urank[i] = plan.del_rank[g];
-        ucount[i] = plan.del_count[g];
-        if (ucount[i] == 0 || ucount[i] > MAX_EXACT_BINARY64_INTEGER || (ucount[i] + 63) / 64 > MAX_WORDS_PER_ATOM)
+      const size_t G = e->G;
+      const std::vector<uint32_t>& ug = e->unit_group;
+      for (size_t g = 0; g < G; ++g) {
+        const uint64_t n = plan.del_count[g];
+        if (n == 0 || n > MAX_EXACT_BINARY64_INTEGER || (n + 63) / 64 > MAX_WORDS_PER_ATOM)
           fail(RESOURCE_LIMIT, "jla_validate", "leverage trial preflight failed");
-        uout[i] = plan.del_outcome_sum[g];
-        ucf[i] = double(plan.del_count[g]);
-        usq[i] = std::sqrt(ucf[i]);
       }
       upload(e->unit_ptr, uptr, s, h2d);
-      upload(e->unit_cell, ucell, s, h2d);
-      upload(e->unit_rank, urank, s, h2d);
-      upload(e->unit_count, ucount, s, h2d);
-      upload(e->unit_outcome, uout, s, h2d);
-      upload(e->unit_count_f, ucf, s, h2d);
-      upload(e->unit_sqrt_n, usq, s, h2d);
+      // unit arrays in cell order, written straight into pinned staging blocks
+      e->unit_cell.alloc(G);
+      e->unit_rank.alloc(G);
+      e->unit_count.alloc(G);
+      e->unit_outcome.alloc(G);
+      e->unit_count_f.alloc(G);
+      e->unit_sqrt_n.alloc(G);
+      upload_fill(e->unit_cell, 0, G, [&](uint32_t* d) {
+        for (size_t i = 0; i < G; ++i) d[i] = plan.del_cell[ug[i]];
+      }, s, h2d);
+      upload_fill(e->unit_rank, 0, G, [&](uint64_t* d) {
+        for (size_t i = 0; i < G; ++i) d[i] = plan.del_rank[ug[i]];
+      }, s, h2d);
+      upload_fill(e->unit_count, 0, G, [&](uint64_t* d) {
+        for (size_t i = 0; i < G; ++i) d[i] = plan.del_count[ug[i]];
+      }, s, h2d);
+      upload_fill(e->unit_outcome, 0, G, [&](double* d) {
+        for (size_t i = 0; i < G; ++i) d[i] = plan.del_outcome_sum[ug[i]];
+      }, s, h2d);
+      upload_fill(e->unit_count_f, 0, G, [&](double* d) {
+        for (size_t i = 0; i < G; ++i) d[i] = double(plan.del_count[ug[i]]);
+      }, s, h2d);
+      upload_fill(e->unit_sqrt_n, 0, G, [&](double* d) {
+        for (size_t i = 0; i < G; ++i) d[i] = std::sqrt(double(plan.del_count[ug[i]]));
+      }, s, h2d);
     }
     if (plan.generic) upload(e->unit_group_d, e->unit_group, s, h2d);
   };
