@@ -111,10 +111,16 @@ void device_release(void* p) {
   if (c.cached > DEVICE_CACHE_LIMIT) trim_locked(c, DEVICE_CACHE_LIMIT);
 }
 
+size_t pinned_cache_trim();
+
 size_t device_cache_trim() {
   const int dev = current_device();
-  std::lock_guard<std::mutex> l(g_mu);
-  return trim_locked(g_cache[dev], 0);
+  size_t freed = 0;
+  {
+    std::lock_guard<std::mutex> l(g_mu);
+    freed = trim_locked(g_cache[dev], 0);
+  }
+  return freed + pinned_cache_trim();
 }
 
 size_t device_cache_bytes() {
@@ -130,7 +136,9 @@ size_t device_cache_bytes() {
 
 namespace {
 
-constexpr size_t PINNED_CACHE_LIMIT = size_t(2) << 30;
+// large enough to hold the staging blocks of one 50M-row generation, so
+// repeated decompositions pin no new host memory
+constexpr size_t PINNED_CACHE_LIMIT = size_t(8) << 30;
 
 std::mutex g_pin_mu;
 std::multimap<size_t, void*> g_pin_free;
@@ -169,6 +177,19 @@ void pinned_release(void* p, size_t have) {
 }
 
 }  // namespace
+
+// Free every cached pinned block (bytes freed).
+size_t pinned_cache_trim() {
+  std::lock_guard<std::mutex> l(g_pin_mu);
+  size_t freed = 0;
+  for (auto& b : g_pin_free) {
+    cudaFreeHost(b.second);
+    freed += b.first;
+  }
+  g_pin_free.clear();
+  g_pin_cached = 0;
+  return freed;
+}
 
 void* HostStager::take(size_t bytes) {
   size_t have = 0;

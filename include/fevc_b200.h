@@ -701,8 +701,10 @@ int32_t fevcb_set_stream(void *stream);
  * builder's bit for bit: *identical = 1 or 0. */
 int32_t fevcb_engine_hybrid_check_v1(uint64_t generation, uint32_t *identical);
 /* Device buffers of released generations stay cached (at most 16 GiB per
- * device) for the next generation; this returns the current device's cached
- * blocks to the driver.  Either pointer may be NULL. */
+ * device) for the next generation, and so do the pinned host blocks that
+ * stage uploads (at most 8 GiB per process); this returns the current
+ * device's cached blocks and the pinned blocks to the driver (freed_bytes
+ * counts both).  Either pointer may be NULL. */
 int32_t fevcb_device_cache_trim_v1(uint64_t *freed_bytes, uint64_t *cached_bytes);
 int32_t fevcb_engine_solve_options_v1(uint64_t generation, const FevcbSolveOptionsV1 *options);
 int32_t fevcb_engine_timings_v1(uint64_t generation, FevcbSolveTimingsV1 *output, uint32_t output_capacity_bytes);
