@@ -1485,7 +1485,7 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
   Launch L{grid_blocks(), e.stream};
   PhiloxKey key = philox_key(o.seed);
   double invT = 1.0 / e.target_total;
-  res.target_draws.assign(o.probes, Components{});
+  if (res.target_draws.size() != o.probes) res.target_draws.assign(o.probes, Components{});
   std::vector<double> tot(2 * K), sums(2 * K), draws(3 * K);
   const uint32_t end = o.probe_end ? o.probe_end : o.probes;
   for (uint32_t first = o.probe_begin; first < end; first += H) {
@@ -1612,6 +1612,65 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
   }
 }
 
+// Probe blocks: full blocks at width K, and a last partial block at the
+// narrowest width that holds it (8, 16 or 32 columns) when that is narrower
+// than K.  Every column is its own PCG, so the results do not depend on the
+// width a column is solved at; a narrow last block costs a fraction of a
+// full-width one.
+inline int tail_width(uint32_t cols, int K) {
+  for (int k : {8, 16, 32})
+    if (k < K && uint32_t(k) >= cols) return k;
+  return 0;
+}
+
+// Splits [probe_begin, probe_end) into the full blocks of `per` probes and
+// the rest; `tail` is the width for the rest (0: run it all at width K).
+inline bool split_probes(const SolveOptions& o, uint32_t per, int K, int cols_per_probe, SolveOptions& head,
+                         SolveOptions& tail, int& width) {
+  const uint32_t begin = o.probe_begin, end = o.probe_end ? o.probe_end : o.probes;
+  const uint32_t full = end > begin ? (end - begin) / per * per : 0, rest = end > begin ? end - begin - full : 0;
+  width = rest ? tail_width(rest * uint32_t(cols_per_probe), K) : 0;
+  if (!width) return false;
+  head = o;
+  tail = o;
+  head.probe_end = begin + full;
+  tail.probe_begin = begin + full;
+  tail.probe_end = end;
+  return true;
+}
+
+template <int K>
+void run_leverage_blocks(DeviceEngine& e, const SolveOptions& o, SolveResult& res) {
+  SolveOptions head, tail;
+  int width = 0;
+  if (K < 16 || !split_probes(o, K, K, 1, head, tail, width)) {
+    run_leverage<K>(e, o, res, 0);
+    return;
+  }
+  if (head.probe_end > head.probe_begin) run_leverage<K>(e, head, res, 0);
+  switch (width) {
+    case 8: run_leverage<8>(e, tail, res, 0); break;
+    case 16: run_leverage<16>(e, tail, res, 0); break;
+    default: run_leverage<32>(e, tail, res, 0); break;
+  }
+}
+
+template <int K>
+void run_target_blocks(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double y_center = 0.0) {
+  SolveOptions head, tail;
+  int width = 0;
+  if (K < 16 || !split_probes(o, K / 2, K, 2, head, tail, width)) {
+    run_target<K>(e, o, res, y_center);
+    return;
+  }
+  if (head.probe_end > head.probe_begin) run_target<K>(e, head, res, y_center);
+  switch (width) {
+    case 8: run_target<8>(e, tail, res, y_center); break;
+    case 16: run_target<16>(e, tail, res, y_center); break;
+    default: run_target<32>(e, tail, res, y_center); break;
+  }
+}
+
 double outcome_mean(const Compressed& p, Centering c) {
   if (c == Centering::None) return 0.0;
   // reference `centering::mean` (vckss-core/src/centering.rs:6-27)
@@ -1689,7 +1748,7 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
   // ---- leverage
   if (o.shard_phase != 2) {
     CK(cudaMemsetAsync(e.moments.p, 0, e.moments.bytes(), L.s));
-    run_leverage<K>(e, o, res, 0);
+    run_leverage_blocks<K>(e, o, res);
   }
   if (o.shard_phase == 1) {
     shard_download(e, res);
@@ -1723,7 +1782,7 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
   }
   auto t2 = now();
   // ---- target
-  run_target<K>(e, o, res);
+  run_target_blocks<K>(e, o, res);
   auto t3 = now();
   if (o.shard_phase == 2) {
     res.timings.target_ms = std::chrono::duration<double, std::milli>(t3 - t2).count();
@@ -1894,7 +1953,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     } else {
       CK(cudaMemsetAsync(e.moments.p, 0, e.moments.bytes(), L.s));
     }
-    run_leverage<K>(e, o, res, 0);
+    run_leverage_blocks<K>(e, o, res);
   }
   if (o.shard_phase == 1) {
     shard_download(e, res);
@@ -1986,7 +2045,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
   }
   auto t2 = now();
   // ---- target draws on the full model
-  run_target<K>(e, o, res, outcome_mean(p, o.centering));
+  run_target_blocks<K>(e, o, res, outcome_mean(p, o.centering));
   auto t3 = now();
   if (o.shard_phase == 2) {
     res.timings.target_ms = std::chrono::duration<double, std::milli>(t3 - t2).count();
