@@ -107,9 +107,21 @@ __device__ __forceinline__ void redundant_finish(const double* __restrict__ part
   constexpr int W = M * K;
   const int per = blockDim.x / W;  // >= 1 when blockDim >= W
   const int o = threadIdx.x % W, g = threadIdx.x / W;
+  // the loads of U partials are issued before their sum, so a thread waits
+  // for one L2 round trip per U blocks instead of one per block
+  constexpr int U = 8;
   double acc = 0.0;
   if (g < per)
-    for (int b = g; b < blocks; b += per) acc += __ldcg(partial + size_t(b) * W + o);
+    for (int b0 = g; b0 < blocks; b0 += U * per) {
+      double v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int b = b0 + u * per;
+        v[u] = b < blocks ? __ldcg(partial + size_t(b) * W + o) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) acc += v[u];
+    }
   scratch[threadIdx.x] = acc;
   __syncthreads();
   if (threadIdx.x < W) {
