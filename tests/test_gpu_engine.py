@@ -192,6 +192,23 @@ def test_block_width_does_not_change_the_result(lib, golden, block):
     assert rel(res["corrected"], rec["corrected"]) < COMPONENT_RTOL
 
 
+@pytest.mark.parametrize("probes", [72, 100])
+def test_last_partial_block_at_a_narrower_width(lib, probes):
+    """At width 64, a last partial probe block is solved at the narrowest
+    width that holds it (72 probes: leverage 64 + 8 at width 8, target
+    64 + 8 probes with the last 16 right-hand sides at width 16; 100 probes:
+    64 + 36 at width 64, target 96 + 4 at width 8).  Every column is its own
+    PCG, so the components equal those of a solve at width 8 throughout."""
+    panel = make_golden.CONTROL_PANELS[next(iter(make_golden.CONTROL_PANELS))]["build"]()
+    out = []
+    for block in (64, 8):
+        e = solve_v5(lib, panel, probes=probes, block=block)
+        out.append(e.result())
+        e.release()
+    for key in ("plugin", "correction", "corrected", "numerical_mcse"):
+        assert rel(out[0][key], out[1][key]) < 1e-10, (key, out[0][key], out[1][key])
+
+
 def test_receipts_and_resolve(lib):
     panel = make_golden.PANELS["small_2k"]["build"]()
     probes = 24
