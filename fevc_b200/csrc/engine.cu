@@ -1378,10 +1378,9 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
     total_iters = done;
     if (*e.h_nactive != 0)
       fail(PCG_MAX_ITERATIONS, "pcg", "blocked PCG reached the iteration limit " + std::to_string(o.maximum_iterations));
-    int bd = 0;
-    CK(cudaMemcpyAsync(&bd, w.s.breakdown, sizeof(int), cudaMemcpyDeviceToHost, L.s));
-    CK(cudaStreamSynchronize(L.s));
-    if (bd >= 0) fail(PCG_CURVATURE_BREAKDOWN, "pcg", "nonpositive curvature in column " + std::to_string(bd));
+    // the breakdown flag comes back with the extraction results (one host
+    // round trip per pass); nothing below is used before it is checked
+    CK(cudaMemcpyAsync(e.h_nactive + 1, w.s.breakdown, sizeof(int), cudaMemcpyDeviceToHost, L.s));
 
     // extraction and complete residual
     double* pw = e.partial.p;
@@ -1399,6 +1398,8 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
     CK(cudaMemcpyAsync(h_bb.data(), w.s.bb, K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaMemcpyAsync(h_it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
+    if (const int bd = e.h_nactive[1]; bd >= 0)
+      fail(PCG_CURVATURE_BREAKDOWN, "pcg", "nonpositive curvature in column " + std::to_string(bd));
     out.complete.assign(K, 0.0);
     out.reduced.assign(K, 0.0);
     out.iters.assign(h_it.begin(), h_it.end());
