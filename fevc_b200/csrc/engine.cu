@@ -1371,13 +1371,25 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
     } else if (o.precision == 1) {
       done = pcg_run_mixed<K>(e, w, L, budget, tm);
     } else {
-      done = pcg_run<K>(e, w, L, budget);
+      // the Jacobi kernel's active count and iterations come back with the
+      // extraction results below (no host round trip of its own)
+      PersistentPcg<K> a = persistent_args<K>(e, w, budget);
+      void* args[] = {&a};
+      const void* fn = two_barrier_form<K, double>() ? (const void*)k_pcg_persistent_cg<K>
+                                                     : (const void*)k_pcg_persistent<K>;
+      CK(cudaLaunchCooperativeKernel(fn, dim3(e.coop_blocks), dim3(PERSIST_THREADS), args, 0, L.s));
+      CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+      done = -1;
       tm.kernel_launches += 1;
       tm.spmm_launches += 1;
     }
-    total_iters = done;
-    if (*e.h_nactive != 0)
-      fail(PCG_MAX_ITERATIONS, "pcg", "blocked PCG reached the iteration limit " + std::to_string(o.maximum_iterations));
+    const bool deferred = done < 0;
+    if (!deferred) {
+      total_iters = done;
+      if (*e.h_nactive != 0)
+        fail(PCG_MAX_ITERATIONS, "pcg",
+             "blocked PCG reached the iteration limit " + std::to_string(o.maximum_iterations));
+    }
     // the breakdown flag comes back with the extraction results (one host
     // round trip per pass); nothing below is used before it is checked
     CK(cudaMemcpyAsync(e.h_nactive + 1, w.s.breakdown, sizeof(int), cudaMemcpyDeviceToHost, L.s));
@@ -1398,6 +1410,12 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
     CK(cudaMemcpyAsync(h_bb.data(), w.s.bb, K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaMemcpyAsync(h_it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
+    if (deferred) {
+      total_iters = *std::max_element(h_it.begin(), h_it.end());
+      if (*e.h_nactive != 0)
+        fail(PCG_MAX_ITERATIONS, "pcg",
+             "blocked PCG reached the iteration limit " + std::to_string(o.maximum_iterations));
+    }
     if (const int bd = e.h_nactive[1]; bd >= 0)
       fail(PCG_CURVATURE_BREAKDOWN, "pcg", "nonpositive curvature in column " + std::to_string(bd));
     out.complete.assign(K, 0.0);
