@@ -13,6 +13,12 @@
 // and it keeps the previous call's contents; calls that overlap on the GPU
 // (from several host threads, or several processes sharing a context) race on
 // it and must be serialised by the caller.
+//
+// The call's copies and its kernel run on the stream bound by fevcb_set_stream
+// (the legacy default stream when none is bound), and the call returns once
+// that stream has finished them.  The array's device address is looked up on
+// the first call on each device and kept for the life of the process, so the
+// entry point must not be used again on a device after cudaDeviceReset.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -20,6 +26,7 @@
 
 #include "counter_rng.h"
 #include "device.cuh"
+#include "engine.h"
 
 namespace fevcb {
 
@@ -65,6 +72,7 @@ size_t noalloc_scratch_bytes() { return NOALLOC_SCRATCH_BYTES; }
 
 void device_atoms_noalloc(uint64_t seed, uint64_t tag, uint64_t first_probe, uint32_t columns, const uint64_t* entity,
                           const uint64_t* trials, uint64_t count, int64_t* out) {
+  if (device_count() < 1) fail(UNSUPPORTED_FEATURE, "device", "no CUDA device is visible");
   if (count == 0 || columns == 0) fail(INVALID_INPUT, "counter_rng", "semantic atom request has incompatible dimensions");
   if (count > NOALLOC_SCRATCH_BYTES || columns > NOALLOC_SCRATCH_BYTES)
     fail(RESOURCE_LIMIT, "noalloc", "request exceeds the fixed scratch array");
@@ -82,16 +90,19 @@ void device_atoms_noalloc(uint64_t seed, uint64_t tag, uint64_t first_probe, uin
   uint64_t* d_entity = reinterpret_cast<uint64_t*>(base);
   uint64_t* d_trials = reinterpret_cast<uint64_t*>(base + in_bytes);
   int64_t* d_out = reinterpret_cast<int64_t*>(base + 2 * in_bytes);
-  CK(cudaMemcpy(d_entity, entity, count * sizeof(uint64_t), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(d_trials, trials, count * sizeof(uint64_t), cudaMemcpyHostToDevice));
+  cudaStream_t s = static_cast<cudaStream_t>(device_stream());
+  CK(cudaMemcpyAsync(d_entity, entity, count * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_trials, trials, count * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
   // the array keeps the previous call's atoms: clear the output region first
-  CK(cudaMemset(d_out, 0, out_bytes));
+  CK(cudaMemsetAsync(d_out, 0, out_bytes, s));
   int dev = 0, sms = 148;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  k_raw_atoms<<<sms * 4, THREADS>>>(count, d_entity, d_trials, philox_key(seed), tag, first_probe, columns, d_out);
+  k_raw_atoms<<<sms * 4, THREADS, 0, s>>>(count, d_entity, d_trials, philox_key(seed), tag, first_probe, columns,
+                                          d_out);
   CK_LAUNCH();
-  CK(cudaMemcpy(out, d_out, out_bytes, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpyAsync(out, d_out, out_bytes, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
 }
 
 }  // namespace fevcb

@@ -848,10 +848,15 @@ int32_t fevcb_counter_atoms_v1(uint64_t seed, uint64_t domain_tag, uint64_t firs
  * call stages them in one file-scope 8 MiB device array instead of allocating,
  * so it calls no cudaMalloc/cudaFree.  Requests needing more than 8 MiB
  * (2 x count x 8 bytes + count x columns x 8 bytes, each part rounded up to
- * 256 bytes) are refused with RESOURCE_LIMIT (40).  The first call on a device
- * looks up the array's device address; make that first call before any stream
- * capture.  Every call shares the array: calls that overlap on the GPU race
- * and must be serialised by the caller. */
+ * 256 bytes) are refused with RESOURCE_LIMIT (40); without a visible device
+ * the call returns UNSUPPORTED_FEATURE (11), as fevcb_counter_atoms_v1 does.
+ * The copies and the kernel run on the stream bound by fevcb_set_stream (the
+ * legacy default stream when none is bound) and the call returns after that
+ * stream has finished them.  The first call on a device looks up the array's
+ * device address and keeps it for the life of the process: make that first
+ * call before any stream capture, and do not call again on a device after
+ * cudaDeviceReset.  Every call shares the array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
 int32_t fevcb_counter_atoms_noalloc_v1(uint64_t seed, uint64_t domain_tag, uint64_t first_probe, uint32_t columns,
                                        const uint64_t *entity, const uint64_t *trials, uint64_t count, int64_t *out);
 
