@@ -687,7 +687,7 @@ const char* vckss_rust_capabilities_json(void) {
          "\"algorithms\":[\"jla\"],\"engines\":[\"compressed\",\"generic\"],"
          "\"deletion\":[\"match\",\"observation\"],\"controls\":8,\"centering\":[\"none\",\"mean\"],"
          "\"solver\":\"blocked-pcg-hybrid-laplacian\","
-         "\"preconditioners\":[\"jacobi\",\"cmg\",\"learned\"],\"precision\":[\"f64\",\"mixed\"]}";
+         "\"preconditioners\":[\"jacobi\",\"cmg\",\"learned\",\"polynomial\"],\"precision\":[\"f64\",\"mixed\"]}";
 }
 
 const char* vckss_rust_last_error(void) { return g_last_error.c_str(); }
@@ -1372,7 +1372,8 @@ int32_t vckss_rust_engine_rhs_receipts_v1(uint64_t generation, VckssEngineRhsRec
     const auto& rc = reg().result->receipts;
     if (!out || rows < rc.size())
       fail(INVALID_INPUT, "engine_rhs_receipts", "RHS receipt capacity is below " + std::to_string(rc.size()));
-    uint32_t route = p.last_options.preconditioner == 1 ? VCKSS_ROUTE_DIAGONAL_PCG : VCKSS_ROUTE_CMG_PCG;
+    uint32_t route = (p.last_options.preconditioner == 1 || p.last_options.preconditioner == 4)
+                         ? VCKSS_ROUTE_DIAGONAL_PCG : VCKSS_ROUTE_CMG_PCG;
     for (size_t i = 0; i < rc.size(); ++i) fill_rhs_v1(rc[i], out[i], route);
   });
 }
@@ -1385,7 +1386,8 @@ int32_t vckss_rust_engine_rhs_receipts_v2(uint64_t generation, VckssEngineRhsRec
     const auto& rc = reg().result->receipts;
     if (!out || rows < rc.size())
       fail(INVALID_INPUT, "engine_rhs_receipts", "RHS receipt capacity is below " + std::to_string(rc.size()));
-    uint32_t route = p.last_options.preconditioner == 1 ? VCKSS_ROUTE_DIAGONAL_PCG : VCKSS_ROUTE_CMG_PCG;
+    uint32_t route = (p.last_options.preconditioner == 1 || p.last_options.preconditioner == 4)
+                         ? VCKSS_ROUTE_DIAGONAL_PCG : VCKSS_ROUTE_CMG_PCG;
     double gate = std::max(10.0 * p.last_options.pcg_tolerance, 1e-11);
     for (size_t i = 0; i < rc.size(); ++i) {
       VckssEngineRhsReceiptV2 r{};
@@ -1481,7 +1483,7 @@ int32_t fevcb_engine_solve_options_v1(uint64_t generation, const FevcbSolveOptio
     if (o.block_columns != 0 && o.block_columns != 2 && o.block_columns != 8 && o.block_columns != 16 &&
         o.block_columns != 32 && o.block_columns != 64)
       fail(INVALID_INPUT, "engine_ffi", "block_columns must be 0, 2, 8, 16, 32 or 64");
-    if (o.preconditioner > 3) fail(INVALID_INPUT, "engine_ffi", "preconditioner must be 0, 1, 2 or 3");
+    if (o.preconditioner > 4) fail(INVALID_INPUT, "engine_ffi", "preconditioner must be 0, 1, 2, 3 or 4");
     if (o2.precision > 1) fail(INVALID_INPUT, "engine_ffi", "precision must be 0 (double) or 1 (mixed)");
     if (o2.reserved != 0) fail(INVALID_INPUT, "engine_ffi", "reserved fields must be zero");
     std::lock_guard<std::mutex> l(reg().mu);

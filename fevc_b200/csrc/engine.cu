@@ -33,6 +33,7 @@
 #include "learned.h"
 #include "multigrid.h"
 #include "persistent.cuh"
+#include "flex.cuh"
 #include "hybrid_device.cuh"
 #include "generic.cuh"
 #include "observation.cuh"
@@ -252,6 +253,11 @@ struct DeviceEngine {
   DBuf<double> L_vald;                      // L_val[e] * L_dinv[L_col[e]] (A D^{-1})
   DBuf<float> L_val32, L_diag32, L_dinv32;  // single-precision copies for mixed-precision solves
   DBuf<float> L_vald32;
+  // vertex-weighted degree-1 polynomial preconditioner z = wa r + ws A (ws r)
+  // (preconditioner 4: the uniform first-order Neumann weights), FP64 and
+  // single-precision copies, and the weighted values val[e] * ws[col[e]]
+  DBuf<double> flex_wa, flex_ws, flex_valw;
+  DBuf<float> flex_wa32, flex_ws32, flex_valw32;
   std::unique_ptr<Multigrid> mg;
   std::unique_ptr<LearnedPreconditioner> learned;
   int preconditioner = 1;
@@ -299,13 +305,9 @@ struct BlockWork {
   DBuf<double> st;  // 8 * K doubles of per-column state
   DBuf<int> ist;    // 2 * K + 2 ints
   PcgState s;
-  // mixed precision: single-precision inner iterate, residual, direction and
-  // segment products, and the inner solve's per-column state
-  DBuf<float> x32, r32, p32, ap32, seg32;
-  DBuf<double> y1, y2;  // polynomial preconditioner: D^{-1} A powers of the residual
-  DBuf<double> st_in;
-  DBuf<int> ist_in;
-  PcgState s_in{};
+  // mixed precision (flex.cuh): increment of x since the last residual
+  // replacement, residual, direction and preconditioned residual
+  DBuf<float> x32, r32, p32, z32;
   cudaGraphExec_t graph = nullptr;
   int graph_iters = 0;
   ~BlockWork() {
@@ -333,6 +335,33 @@ __global__ void k_scale_by_col(size_t nnz, const uint32_t* __restrict__ col, con
                                const double* __restrict__ dinv, double* __restrict__ out) {
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nnz; i += size_t(gridDim.x) * blockDim.x)
     out[i] = val[i] * dinv[col[i]];
+}
+
+// Uniform first-order Neumann weights of the degree-1 polynomial
+// preconditioner: wa = a / d, ws = s / d at every vertex (a > s^2 keeps it
+// positive definite).
+__global__ void k_flex_uniform_weights(uint32_t n, const double* __restrict__ diag, double a, double s,
+                                       double* __restrict__ wa, double* __restrict__ ws) {
+  for (size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += size_t(gridDim.x) * blockDim.x) {
+    wa[v] = a / diag[v];
+    ws[v] = s / diag[v];
+  }
+}
+
+// Learned weights: wa = a / d, ws = s / d from the network's (a, s) per vertex.
+__global__ void k_flex_learned_weights(uint32_t n, const double* __restrict__ diag, const float* __restrict__ as,
+                                       double* __restrict__ wa, double* __restrict__ ws) {
+  for (size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += size_t(gridDim.x) * blockDim.x) {
+    wa[v] = double(as[2 * v]) / diag[v];
+    ws[v] = double(as[2 * v + 1]) / diag[v];
+  }
+}
+
+// valw[e] = val[e] * ws[col[e]]
+__global__ void k_flex_weighted_values(size_t nnz, const uint32_t* __restrict__ col, const double* __restrict__ val,
+                                       const double* __restrict__ ws, double* __restrict__ valw) {
+  for (size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x; e < nnz; e += size_t(gridDim.x) * blockDim.x)
+    valw[e] = val[e] * ws[col[e]];
 }
 
 // Run the tasks on their own threads, bound to the calling thread's device;
@@ -604,6 +633,13 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     e->stats.kept_workers = e->kept;
     e->preconditioner = preconditioner == 0 ? 1 : preconditioner;
     e->stats.levels = 1;
+    if (e->preconditioner == 4) {
+      e->flex_wa.alloc(e->n);
+      e->flex_ws.alloc(e->n);
+      k_flex_uniform_weights<<<grid_blocks(), THREADS, 0, s>>>(e->n, e->L_diag.p, FLEX_NEUMANN_A, FLEX_NEUMANN_S,
+                                                              e->flex_wa.p, e->flex_ws.p);
+      CK_LAUNCH();
+    }
     if (e->preconditioner == 2 || e->preconditioner == 3) {
       // the CMG hierarchy and the network features are built on the host
       std::vector<uint32_t> Lptr(e->n + 1), Lcol(nnz);
@@ -623,7 +659,19 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
         if (params.empty())
           fail(UNSUPPORTED_FEATURE, "learned_preconditioner", "no network parameters are installed");
         e->learned = build_learned(params, e->n, Lptr, Lcol, Lval, Ld, s, h2d);
+        e->flex_wa.alloc(e->n);
+        e->flex_ws.alloc(e->n);
+        k_flex_learned_weights<<<grid_blocks(), THREADS, 0, s>>>(e->n, e->L_diag.p, e->learned->weights(),
+                                                                e->flex_wa.p, e->flex_ws.p);
+        CK_LAUNCH();
       }
+    }
+    if (e->flex_ws.p) {
+      e->flex_valw.alloc(nnz);
+      if (nnz)
+        k_flex_weighted_values<<<grid_blocks(), THREADS, 0, s>>>(nnz, e->L_col.p, e->L_val.p, e->flex_ws.p,
+                                                                 e->flex_valw.p);
+      CK_LAUNCH();
     }
   }
   if (!e->observation) {
@@ -648,8 +696,8 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the two-barrier persistent PCG kernel cannot be resident on an SM");
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_persistent_cg<64, float>, PERSIST_THREADS, 0));
     if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the single-precision persistent PCG kernel cannot be resident on an SM");
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_persistent_poly<64>, PERSIST_THREADS, 0));
-    if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the persistent polynomial PCG kernel cannot be resident on an SM");
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_flex<64, float, true>, PERSIST_THREADS, 0));
+    if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the mixed-precision persistent PCG kernel cannot be resident on an SM");
     e->coop_blocks = sms;  // one 1024-thread block per SM
   }
   CK(cudaEventCreate(&e->ev0));
@@ -899,8 +947,6 @@ template <int K>
 void apply_preconditioner(DeviceEngine& e, BlockWork& w, Launch L, const double* r, double* z) {
   if (e.preconditioner == 2) {
     e.mg->apply(K, r, z, L.s);
-  } else if (e.preconditioner == 3) {
-    e.learned->apply(K, r, z, L.s);
   } else {
     k_jacobi<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_dinv.p, r, z, nullptr);
   }
@@ -923,7 +969,7 @@ void pcg_restart(DeviceEngine& e, BlockWork& w, Launch L, bool fresh, bool direc
     CK_LAUNCH();
     return;
   }
-  if (e.preconditioner == 2 || e.preconditioner == 3) {
+  if (e.preconditioner == 2) {
     apply_preconditioner<K>(e, w, L, w.r.p, w.z.p);
     CK(cudaMemcpyAsync(w.p.p, w.z.p, size_t(e.n) * K * sizeof(double), cudaMemcpyDeviceToDevice, L.s));
     k_dot<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.r.p, w.z.p, e.partial.p);
@@ -1003,93 +1049,11 @@ int pcg_run(DeviceEngine& e, BlockWork& w, Launch L, int iterations) {
 }
 
 // ---------------------------------------------------------------------------
-// Mixed precision: the inner blocked PCG runs in single precision on the
-// correction e of L e = r (r the FP64 reduced residual of the current x),
-// products, dots and step lengths in double; x += e and the residual
-// recomputation are FP64 (iterative refinement).  Each refinement cycle asks
-// the inner solve for a reduction of MIXED_INNER_REDUCTION or the outer
-// tolerance, whichever is looser.
-
-constexpr double MIXED_INNER_REDUCTION = 1e-5;
-constexpr int MIXED_MAX_CYCLES = 12;
+// Single-precision copies of the Laplacian for the mixed-precision solve.
 
 __global__ void k_to_float(size_t n, const double* __restrict__ src, float* __restrict__ dst) {
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
     dst[i] = float(src[i]);
-}
-
-// r32 = r64, e32 = 0, p32 = D^{-1} r32; partial (r.z, r.r) of the single-precision values
-template <int K>
-__global__ void k_mixed_begin(uint32_t n, const double* __restrict__ r64, const float* __restrict__ dinv,
-                              float* __restrict__ r32, float* __restrict__ x32, float* __restrict__ p32,
-                              double* __restrict__ partial) {
-  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
-  double v[2][CPT];
-#pragma unroll
-  for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
-  int c0 = int(threadIdx.x % TPR) * CPT;
-  size_t total = size_t(n) * TPR, stride = size_t(gridDim.x) * blockDim.x;
-  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
-    size_t t = base + threadIdx.x;
-    if (t < total) {
-      size_t row = t / TPR, i = row * K + c0;
-      float d = dinv[row];
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) {
-        float r = float(r64[i + c]);
-        float z = d * r;
-        r32[i + c] = r;
-        x32[i + c] = 0.0f;
-        p32[i + c] = z;
-        v[0][c] += double(r) * double(z);
-        v[1][c] += double(r) * double(r);
-      }
-    }
-  }
-  block_reduce_cols<K, 2>(v, partial);
-}
-
-// Per column: the outer residual r.r decides whether the column still
-// iterates; the inner target is max(reduction^2 r.r, outer target).
-template <int K>
-__global__ void k_mixed_state(const double* __restrict__ partial, int blocks, PcgState outer, PcgState inner,
-                              double reduction2) {
-  __shared__ int cnt;
-  if (threadIdx.x == 0) cnt = 0;
-  __syncthreads();
-  for (int j = threadIdx.x; j < K; j += blockDim.x) {
-    double rz = 0.0, rr = 0.0;
-    for (int b = 0; b < blocks; ++b) {
-      rz += partial[size_t(b) * 2 * K + j];
-      rr += partial[size_t(b) * 2 * K + K + j];
-    }
-    outer.rr[j] = rr;
-    int act = outer.active[j] && rr > outer.tol2[j];
-    outer.active[j] = act;
-    inner.active[j] = act;
-    inner.rz[j] = rz;
-    inner.tol2[j] = fmax(reduction2 * rr, outer.tol2[j]);
-    if (act) atomicAdd(&cnt, 1);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    *outer.nactive = cnt;
-    *inner.nactive = cnt;
-    *inner.breakdown = -1;
-  }
-}
-
-// x64 += e32 for every column (inactive columns carry e = 0)
-__global__ void k_mixed_add(size_t n, const float* __restrict__ e, double* __restrict__ x) {
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
-    x[i] += double(e[i]);
-}
-
-// outer iteration counts and breakdown from the inner state
-template <int K>
-__global__ void k_mixed_finish(PcgState outer, PcgState inner) {
-  for (int j = threadIdx.x; j < K; j += blockDim.x) outer.iters[j] = inner.iters[j];
-  if (threadIdx.x == 0 && *inner.breakdown >= 0) atomicCAS(outer.breakdown, -1, *inner.breakdown);
 }
 
 void ensure_single_precision_matrix(DeviceEngine& e) {
@@ -1106,99 +1070,115 @@ void ensure_single_precision_matrix(DeviceEngine& e) {
   CK_LAUNCH();
 }
 
+
+// ---------------------------------------------------------------------------
+// The single-kernel PCG of flex.cuh for blocks of 32 or 64 columns: Jacobi or
+// the vertex-weighted polynomial stage (preconditioners 3 and 4), in FP32
+// storage with FP64 residual replacement (precision 1) or in FP64.
+
 template <int K>
-void ensure_mixed_work(DeviceEngine& e, BlockWork& w) {
-  if (w.x32.p) return;
-  size_t n = size_t(e.n) * K;
-  w.x32.alloc(n);
-  w.r32.alloc(n);
-  w.p32.alloc(n);
-  w.ap32.alloc(n);
-  w.seg32.alloc(size_t(e.lap_seg.count) * K);
-  w.st_in.alloc(8 * K);
-  w.ist_in.alloc(2 * K + 4);
-  double* st = w.st_in.p;
-  int* ist = w.ist_in.p;
-  w.s_in = PcgState{st, st + K, st + 2 * K, st + 3 * K, st + 4 * K, st + 5 * K, st + 6 * K,
-                    ist, ist + K, ist + 2 * K, ist + 2 * K + 1};
+constexpr bool flex_width() {
+  return Cols<K>::TPR == 32 && K <= 64;
 }
 
-// Refinement cycles from the state pcg_restart leaves (x64, r64 = b - mean -
-// L x64, outer tolerances and active columns).  Returns the largest
-// per-column inner iteration count; leaves the count of columns above the
-// outer tolerance in e.h_nactive.
-template <int K>
-int pcg_run_mixed(DeviceEngine& e, BlockWork& w, Launch L, int iterations, SolveTimings& tm) {
-  ensure_single_precision_matrix(e);
-  ensure_mixed_work<K>(e, w);
-  const size_t nk = size_t(e.n) * K;
-  CK(cudaMemcpyAsync(w.s_in.iters, w.s.iters, K * sizeof(int), cudaMemcpyDeviceToDevice, L.s));
-  int done = 0;
-  for (int cycle = 0; cycle < MIXED_MAX_CYCLES; ++cycle) {
-    k_mixed_begin<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.r.p, e.L_dinv32.p, w.r32.p, w.x32.p, w.p32.p, e.partial.p);
-    k_mixed_state<K><<<1, 128, 0, L.s>>>(e.partial.p, L.grid, w.s, w.s_in,
-                                         MIXED_INNER_REDUCTION * MIXED_INNER_REDUCTION);
-    CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
-    CK(cudaStreamSynchronize(L.s));
-    tm.kernel_launches += 2;
-    if (*e.h_nactive == 0 || done >= iterations) break;
-    PersistentPcg<K, float> a;
-    a.n = e.n;
-    a.ptr = e.L_ptr.p;
-    a.col = e.L_col.p;
+inline bool flex_form(const DeviceEngine& e, const SolveOptions& o) {
+  return o.precision == 1 || e.preconditioner == 3 || e.preconditioner == 4;
+}
+
+void ensure_flex_weights32(DeviceEngine& e) {
+  if (e.flex_wa32.p || !e.flex_wa.p) return;
+  e.flex_wa32.alloc(e.flex_wa.n);
+  e.flex_ws32.alloc(e.flex_ws.n);
+  e.flex_valw32.alloc(e.flex_valw.n);
+  int g = grid_blocks();
+  k_to_float<<<g, THREADS, 0, e.stream>>>(e.flex_wa.n, e.flex_wa.p, e.flex_wa32.p);
+  k_to_float<<<g, THREADS, 0, e.stream>>>(e.flex_ws.n, e.flex_ws.p, e.flex_ws32.p);
+  k_to_float<<<g, THREADS, 0, e.stream>>>(e.flex_valw.n, e.flex_valw.p, e.flex_valw32.p);
+  CK_LAUNCH();
+}
+
+template <int K, typename V, bool POLY>
+void launch_flex_v(DeviceEngine& e, BlockWork& w, Launch L, int iterations, bool fresh) {
+  constexpr bool F32 = std::is_same_v<V, float>;
+  FlexPcg<K, V> a{};
+  a.n = e.n;
+  a.col = e.L_col.p;
+  a.val64 = e.L_val.p;
+  a.diag64 = e.L_diag.p;
+  if constexpr (F32) {
     a.val = e.L_val32.p;
     a.diag = e.L_diag32.p;
     a.dinv = e.L_dinv32.p;
-    a.nseg = e.lap_seg.count;
-    a.seg_row = e.lap_seg.row.p;
-    a.seg_begin = e.lap_seg.begin.p;
-    a.seg_end = e.lap_seg.end.p;
-    a.row_first = e.lap_seg.row_first.p;
-    a.seg_flag = e.lap_seg.row_flag.p;
-    a.vald = e.L_vald32.p;
-    a.ord_id = e.lap_seg.ord_id.p;
-    a.ord_flag = e.lap_seg.ord_flag.p;
-    a.ord_begin = e.lap_seg.ord_begin.p;
-    a.ord_end = e.lap_seg.ord_end.p;
-    a.heavy_rows = e.lap_seg.heavy_rows.p;
-    a.light_rows = e.lap_seg.light_rows.p;
-    a.nheavy = e.lap_seg.nheavy;
-    a.nlight = e.lap_seg.nlight;
-    a.seg_buf = w.seg32.p;
-    a.x = w.x32.p;
+    a.wa = e.flex_wa32.p;
+    a.ws = e.flex_ws32.p;
+    a.valw = e.flex_valw32.p;
+    a.xi = w.x32.p;
     a.r = w.r32.p;
     a.p = w.p32.p;
-    a.ap = w.ap32.p;
-    a.partial_a = e.partial.p;
-    a.partial_b = e.partial.p + size_t(e.coop_blocks) * K;
-    a.s = w.s_in;
-    a.max_iters = iterations - done;
-    void* args[] = {&a};
-    // one warp per segment (K = 64): the balanced three-barrier form with
-    // warp-broadcast gathers and the pipelined product phase, as in double
-    const void* fn = Cols<K>::TPR == 32          ? (const void*)k_pcg_persistent<K, float, true, true>
-                     : two_barrier_form<K, float>() ? (const void*)k_pcg_persistent_cg<K, float>
-                                                    : (const void*)k_pcg_persistent<K, float>;
-    CK(cudaLaunchCooperativeKernel(fn, dim3(e.coop_blocks),
-                                   dim3(PERSIST_THREADS), args, 0, L.s));
-    std::vector<int> it(K);
-    CK(cudaMemcpyAsync(it.data(), w.s_in.iters, K * sizeof(int), cudaMemcpyDeviceToHost, L.s));
-    // x += e; r = (b - mean) - L x in double
-    k_mixed_add<<<L.grid, THREADS, 0, L.s>>>(nk, w.x32.p, w.x.p);
-    k_center<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p, w.s.mean, w.q.p, w.z.p);
-    k_spmm<K><<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_ptr.p, e.L_col.p, e.L_val.p, e.L_diag.p, w.x.p, w.q.p, w.r.p);
-    CK(cudaStreamSynchronize(L.s));
-    tm.kernel_launches += 4;
-    tm.spmm_launches += 2;
-    int mx = 0;
-    for (int v : it) mx = std::max(mx, v);
-    done = mx;
+    a.z = w.z32.p;
+  } else {
+    a.val = e.L_val.p;
+    a.diag = e.L_diag.p;
+    a.dinv = e.L_dinv.p;
+    a.wa = e.flex_wa.p;
+    a.ws = e.flex_ws.p;
+    a.valw = e.flex_valw.p;
+    a.xi = w.q.p;
+    a.r = w.r.p;
+    a.p = w.p.p;
+    a.z = w.z.p;
   }
-  k_mixed_finish<K><<<1, 128, 0, L.s>>>(w.s, w.s_in);
-  CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
-  CK(cudaStreamSynchronize(L.s));
-  tm.kernel_launches += 1;
-  return done;
+  a.nseg = e.lap_seg.count;
+  a.ord_id = e.lap_seg.ord_id.p;
+  a.ord_flag = e.lap_seg.ord_flag.p;
+  a.ord_begin = e.lap_seg.ord_begin.p;
+  a.ord_end = e.lap_seg.ord_end.p;
+  a.row_first = e.lap_seg.row_first.p;
+  a.heavy_rows = e.lap_seg.heavy_rows.p;
+  a.light_rows = e.lap_seg.light_rows.p;
+  a.nheavy = e.lap_seg.nheavy;
+  a.nlight = e.lap_seg.nlight;
+  a.seg = w.seg_buf.p;
+  a.x = w.x.p;
+  a.b = w.b.p;
+  a.partial = e.partial.p;
+  a.s = w.s;
+  a.rr_ref = w.st.p + 7 * K;
+  a.replacements = w.ist.p + 2 * K + 2;
+  a.max_iters = iterations;
+  a.fresh = fresh ? 1 : 0;
+  a.replace2 = FLEX_REPLACE * FLEX_REPLACE;
+  void* args[] = {&a};
+  CK(cudaLaunchCooperativeKernel((const void*)k_pcg_flex<K, V, POLY>, dim3(e.coop_blocks), dim3(PERSIST_THREADS),
+                                 args, 0, L.s));
+}
+
+// Launch the single-kernel solve for the active columns of w (x = 0 on a
+// fresh start, else continue from x); the state comes back with the
+// extraction results, as for the FP64 Jacobi kernel.
+template <int K>
+void launch_flex(DeviceEngine& e, BlockWork& w, Launch L, int iterations, bool fresh, int precision) {
+  if constexpr (flex_width<K>()) {
+    const bool poly = e.preconditioner == 3 || e.preconditioner == 4;
+    if (precision == 1) {
+      ensure_single_precision_matrix(e);
+      if (poly) ensure_flex_weights32(e);
+      const size_t nk = size_t(e.n) * K;
+      if (!w.x32.p) {
+        w.x32.alloc(nk);
+        w.r32.alloc(nk);
+        w.p32.alloc(nk);
+      }
+      if (poly && !w.z32.p) w.z32.alloc(nk);
+      if (poly) launch_flex_v<K, float, true>(e, w, L, iterations, fresh);
+      else launch_flex_v<K, float, false>(e, w, L, iterations, fresh);
+    } else {
+      if (poly) launch_flex_v<K, double, true>(e, w, L, iterations, fresh);
+      else launch_flex_v<K, double, false>(e, w, L, iterations, fresh);
+    }
+  } else {
+    fail(INTERNAL_INVARIANT_FAILED, "pcg", "the single-kernel PCG holds blocks of 32 or 64 columns");
+  }
 }
 
 // Multigrid-preconditioned blocked PCG: one iteration is q = L p with p.q,
@@ -1256,11 +1236,12 @@ int pcg_run_mg(DeviceEngine& e, BlockWork& w, Launch L, int iterations, SolveTim
 }
 
 // ---------------------------------------------------------------------------
-// PCG with the learned polynomial preconditioner: the network's pooled
-// coefficients define one symmetric degree-3 polynomial per graph, applied
-// inside the persistent kernel (k_pcg_persistent_poly).  A block whose
-// columns have not converged after LEARNED_CAP iterations, or that meets a
-// nonpositive curvature, is finished from its current iterate by Jacobi PCG.
+// Fallback of the learned stage: a block whose columns have not converged
+// after LEARNED_CAP iterations (the network's weights are positive definite
+// by construction, so this marks a stalled network, not a wrong answer), or
+// that meets a nonpositive curvature, continues from its current x with
+// CMG-preconditioned PCG.  The aggregation hierarchy is built on the first
+// fallback of the generation.
 
 constexpr int LEARNED_CAP = 300;
 
@@ -1272,49 +1253,43 @@ __global__ void k_reactivate(PcgState s) {
   if (threadIdx.x == 0) *s.breakdown = -1;
 }
 
+void ensure_multigrid(DeviceEngine& e) {
+  if (e.mg) return;
+  const size_t nnz = e.L_val.n;
+  std::vector<uint32_t> Lptr(e.n + 1), Lcol(nnz);
+  std::vector<double> Lval(nnz), Ld(e.n);
+  CK(cudaMemcpyAsync(Lptr.data(), e.L_ptr.p, Lptr.size() * 4, cudaMemcpyDeviceToHost, e.stream));
+  CK(cudaMemcpyAsync(Lcol.data(), e.L_col.p, nnz * 4, cudaMemcpyDeviceToHost, e.stream));
+  CK(cudaMemcpyAsync(Lval.data(), e.L_val.p, nnz * 8, cudaMemcpyDeviceToHost, e.stream));
+  CK(cudaMemcpyAsync(Ld.data(), e.L_diag.p, e.n * 8, cudaMemcpyDeviceToHost, e.stream));
+  CK(cudaStreamSynchronize(e.stream));
+  e.mg = build_multigrid(e.n, Lptr, Lcol, Lval, Ld, e.stream, e.stats.h2d_bytes);
+}
+
+// After a capped learned launch: returns -1 when every column converged (the
+// state comes back with the extraction results), else runs the CMG fallback
+// and returns its largest per-column iteration count.
 template <int K>
-int pcg_run_learned(DeviceEngine& e, BlockWork& w, Launch L, int iterations, SolveTimings& tm) {
-  if (!w.y1.p) {
-    w.y1.alloc(size_t(e.n) * K);
-    w.y2.alloc(size_t(e.n) * K);
-  }
-  const double* c = e.learned->scalar_coefficients();
-  PersistentPoly<K> P;
-  PersistentPcg<K>& a = P.a;
-  // matrix, balanced segment order, x, r, p, partials and state as for the Jacobi kernel
-  a = persistent_args<K>(e, w, std::min(iterations, LEARNED_CAP));
-  P.y1 = w.y1.p;
-  P.y2 = w.y2.p;
-  P.z = w.z.p;
-  P.c0 = c[0];
-  P.c1 = c[1];
-  P.c2 = c[2];
-  P.c3 = c[3];
-  void* args[] = {&P};
-  CK(cudaLaunchCooperativeKernel((const void*)k_pcg_persistent_poly<K>, dim3(e.coop_blocks), dim3(PERSIST_THREADS),
-                                 args, 0, L.s));
-  tm.kernel_launches += 1;
-  tm.spmm_launches += 1;
+int learned_fallback(DeviceEngine& e, BlockWork& w, Launch L, int budget, SolveTimings& tm) {
   int bd = -1;
-  std::vector<int> it(K);
   CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
   CK(cudaMemcpyAsync(&bd, w.s.breakdown, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+  CK(cudaStreamSynchronize(L.s));
+  if (*e.h_nactive == 0 && bd < 0) return -1;
+  tm.fallbacks += 1;
+  ensure_multigrid(e);
+  std::vector<int> it(K);
   CK(cudaMemcpyAsync(it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost, L.s));
   CK(cudaStreamSynchronize(L.s));
-  int mx = 0;
-  for (int v : it) mx = std::max(mx, v);
-  if (*e.h_nactive > 0 || bd >= 0) {
-    // fallback: finish from the current iterate with Jacobi PCG
-    tm.fallbacks += 1;
-    k_reactivate<K><<<1, 128, 0, L.s>>>(w.s);
-    int saved = e.preconditioner;
-    e.preconditioner = 1;
-    pcg_restart<K>(e, w, L, false, !two_barrier_form<K, double>());
-    mx = pcg_run<K>(e, w, L, std::max(1, iterations - mx));
-    e.preconditioner = saved;
-    tm.kernel_launches += 8;
-  }
-  return mx;
+  const int used = *std::max_element(it.begin(), it.end());
+  k_reactivate<K><<<1, 128, 0, L.s>>>(w.s);
+  const int saved = e.preconditioner;
+  e.preconditioner = 2;
+  pcg_restart<K>(e, w, L, false, true);
+  int done = pcg_run_mg<K>(e, w, L, std::max(1, budget - used), tm);
+  e.preconditioner = saved;
+  tm.kernel_launches += 10;
+  return done;
 }
 
 // Segmented firm-side gather (op as in k_seg_firm) finished per row.
@@ -1347,12 +1322,17 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
   firm_gather<K, 1, 1>(e, w, L, e.cell_scale.p, w.bW.p, nullptr, 0.0, w.bF.p, w.bW.p, nullptr, w.b.p, e.partial.p);
   finish(e.partial.p, L.grid, 2 * K, w.tot.p, L.s);
   k_pcg_init_state<K><<<1, 128, 0, L.s>>>(w.tot.p, ncols, o.pcg_tolerance, double(e.n), w.s);
+  // blocks of 32 or 64 columns in the mixed-precision or polynomial forms run
+  // the single-kernel solve, which forms its own start from x; narrower
+  // blocks of those forms run FP64 Jacobi PCG
+  const bool flex = flex_width<K>() && flex_form(e, o);
   // the multigrid and learned forms and the three-barrier Jacobi kernel take
   // p and r.z from the restart
-  const bool directions = e.preconditioner == 2 || e.preconditioner == 3 ||
-                          (o.precision != 1 && !two_barrier_form<K, double>());
-  pcg_restart<K>(e, w, L, true, directions);
-  tm.kernel_launches += directions ? 9 : 5;
+  const bool directions = e.preconditioner == 2 || !two_barrier_form<K, double>();
+  if (!flex) {
+    pcg_restart<K>(e, w, L, true, directions);
+    tm.kernel_launches += directions ? 9 : 5;
+  }
 
   const double gate = std::max(10.0 * o.pcg_tolerance, 1e-11);
   double tol = o.pcg_tolerance;
@@ -1364,12 +1344,17 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
     if (budget <= 0)
       fail(PCG_MAX_ITERATIONS, "pcg", "blocked PCG reached the iteration limit " + std::to_string(o.maximum_iterations));
     int done;
-    if (e.preconditioner == 2) {
+    if (flex) {
+      // like the Jacobi kernel below, the state comes back with the
+      // extraction results
+      const bool learned = e.preconditioner == 3;
+      launch_flex<K>(e, w, L, learned ? std::min(budget, LEARNED_CAP) : budget, ladder == 0, o.precision);
+      tm.kernel_launches += 1;
+      tm.spmm_launches += 1;
+      done = learned ? learned_fallback<K>(e, w, L, budget, tm) : -1;
+      if (done < 0) CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
+    } else if (e.preconditioner == 2) {
       done = pcg_run_mg<K>(e, w, L, budget, tm);
-    } else if (e.preconditioner == 3) {
-      done = pcg_run_learned<K>(e, w, L, budget, tm);
-    } else if (o.precision == 1) {
-      done = pcg_run_mixed<K>(e, w, L, budget, tm);
     } else {
       // the Jacobi kernel's active count and iterations come back with the
       // extraction results below (no host round trip of its own)
@@ -1445,7 +1430,7 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
     for (int j = 0; j < K; ++j) tol2[j] = tol * tol * h_bb[j];
     CK(cudaMemcpyAsync(w.s.tol2, tol2.data(), K * sizeof(double), cudaMemcpyHostToDevice, L.s));
     CK(cudaMemcpyAsync(w.s.active, h_active.data(), K * sizeof(int), cudaMemcpyHostToDevice, L.s));
-    pcg_restart<K>(e, w, L, false, directions);
+    if (!flex) pcg_restart<K>(e, w, L, false, directions);
   }
   out.block_iterations = total_iters;
   tm.pcg_iterations += total_iters;
@@ -2176,6 +2161,18 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
       // segment products written and read
       *bytes = iters * (nnz * 12 + nseg * 12 + n * (4 + 4 + 8 + 8 + 8) + n * K * 8.0 * 9 + 2 * nseg * K * 8.0);
       break;
+    case 9:
+    case 10:
+      // single-kernel FP32 solve (flex.cuh), per iteration: matrix (columns,
+      // FP32 values, segment order) and per-vertex tables once; nine passes
+      // over n x K FP32 vectors (p gathered; p, xi, r read, xi, r written; r
+      // (or z), p read, p written) and the segment products written and read.
+      // The polynomial stage adds the weighted values and weights, r gathered
+      // and read, z written, and its segment products.  Replacements are
+      // added below from the measured count.
+      *bytes = iters * (nnz * 8 + nseg * 16 + n * 16 + n * K * 4.0 * 9 + 2 * nseg * K * 4.0);
+      if (kernel == 10) *bytes += iters * (nnz * 8 + nseg * 16 + n * 16 + n * K * 4.0 * 3 + 2 * nseg * K * 4.0);
+      break;
     case 3:
       *bytes = double(e.G) * (8 + 8 + (e.observation ? 8 : K * 8)) + double(e.C) * (4 + K * 8);
       break;
@@ -2188,6 +2185,20 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
       break;
     default: fail(INVALID_INPUT, "benchmark", "unknown kernel id");
   }
+  if (kernel >= 9) {
+    if (!flex_width<K>()) fail(INVALID_INPUT, "benchmark", "the single-kernel solve holds blocks of 32 or 64 columns");
+    if (kernel == 10 && !e.flex_wa.p) {
+      e.flex_wa.alloc(e.n);
+      e.flex_ws.alloc(e.n);
+      e.flex_valw.alloc(e.L_val.n);
+      k_flex_uniform_weights<<<L.grid, THREADS, 0, L.s>>>(e.n, e.L_diag.p, FLEX_NEUMANN_A, FLEX_NEUMANN_S,
+                                                          e.flex_wa.p, e.flex_ws.p);
+      k_flex_weighted_values<<<L.grid, THREADS, 0, L.s>>>(e.L_val.n, e.L_col.p, e.L_val.p, e.flex_ws.p,
+                                                          e.flex_valw.p);
+      CK_LAUNCH();
+    }
+    CK(cudaMemsetAsync(w.ist.p + 2 * K + 2, 0, sizeof(int), L.s));
+  }
   std::vector<float> times;
   for (int i = 0; i < launches; ++i) {
     if (kernel == 1 || kernel >= 5) {
@@ -2196,7 +2207,9 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
       k_colsum_abs<K><<<L.grid, THREADS, 0, L.s>>>(e.n, w.b.p, e.partial.p);
       finish(e.partial.p, L.grid, 2 * K, w.tot.p, L.s);
       k_pcg_init_state<K><<<1, 128, 0, L.s>>>(w.tot.p, K, 0.0, double(e.n), w.s);
-      pcg_restart<K>(e, w, L, true, kernel == 5 || kernel == 7 || kernel == 8 || (kernel == 1 && !two_barrier_form<K, double>()));
+      if (kernel < 9)
+        pcg_restart<K>(e, w, L, true,
+                       kernel == 5 || kernel == 7 || kernel == 8 || (kernel == 1 && !two_barrier_form<K, double>()));
     }
     CK(cudaMemsetAsync(flush.p, i & 0xff, flush.bytes(), L.s));
     CK(cudaEventRecord(e.ev0, L.s));
@@ -2217,6 +2230,14 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
                          : two         ? (const void*)k_pcg_persistent_cg<K>
                                        : (const void*)k_pcg_persistent<K>;
         CK(cudaLaunchCooperativeKernel(fn, dim3(e.coop_blocks), dim3(PERSIST_THREADS), args, 0, L.s));
+        break;
+      }
+      case 9:
+      case 10: {
+        const int saved = e.preconditioner;
+        e.preconditioner = kernel == 10 ? 4 : 1;
+        launch_flex<K>(e, w, L, iters, true, 1);
+        e.preconditioner = saved;
         break;
       }
       case 3:
@@ -2252,6 +2273,16 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
     CK(cudaMemcpy(it.data(), w.s.iters, K * sizeof(int), cudaMemcpyDeviceToHost));
     int mx = *std::max_element(it.begin(), it.end());
     if (mx != iters) *bytes *= double(mx) / iters;
+  }
+  if (kernel >= 9) {
+    // the start (x = 0, xi = 0, r = b - mean, p = z) and the FP64 residual
+    // replacements of an average launch: x and xi read and written, x
+    // gathered, FP64 segment products written and read, b and x read, r written
+    int reps = 0;
+    CK(cudaMemcpy(&reps, w.ist.p + 2 * K + 2, sizeof(int), cudaMemcpyDeviceToHost));
+    const double per_launch = double(reps) / launches;
+    *bytes += n * K * (8.0 + 4 + 8 + 4 + 4 + 4) +
+              per_launch * (nnz * 12 + nseg * 16 + n * 16 + n * K * 52.0 + 16 * nseg * K);
   }
 }
 

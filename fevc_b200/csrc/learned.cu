@@ -1,5 +1,6 @@
-// Learned preconditioner: graph network inference and training kernels, the
-// polynomial preconditioner apply, and the pair generation by CMG-PCG.
+// Learned preconditioner: graph network inference and training kernels for
+// the per-vertex weights of the degree-1 preconditioner stage, and the pair
+// generation by CMG-PCG.
 #include "learned.h"
 
 #include <cuda_bf16.h>
@@ -49,8 +50,9 @@ std::vector<float> gnn_initial_params(uint64_t seed) {
   }
   size_t o = gnn_layer_offset(GNN_LAYERS);
   for (size_t i = 0; i < size_t(GNN_WIDTH) * GNN_OUT; ++i) p[o + i] = 0.01f * uniform();
-  // softplus(b) = 1: b = log(e - 1)
-  for (int k = 0; k < GNN_OUT; ++k) p[o + size_t(GNN_WIDTH) * GNN_OUT + k] = std::log(std::exp(1.0f) - 1.0f);
+  // untrained head: s = softplus(b_s) = 1, a = s^2 + a_min + softplus(b_a) = 1.05
+  p[o + size_t(GNN_WIDTH) * GNN_OUT + 0] = std::log(std::expm1(0.05f - GNN_A_MIN));
+  p[o + size_t(GNN_WIDTH) * GNN_OUT + 1] = std::log(std::exp(1.0f) - 1.0f);
   return p;
 }
 
@@ -179,51 +181,14 @@ __global__ void k_gnn_head(uint32_t n, const float* __restrict__ H, const __nv_b
   }
 }
 
-// Graph pooling: pooled[k] = mean over vertices of Craw[v][k] (one block,
-// fixed order), then every vertex takes c_k = softplus(pooled[k]): one
-// polynomial per graph, so the preconditioner is symmetric.
-__global__ void k_gnn_pool(uint32_t n, const float* __restrict__ Craw, float* __restrict__ pooled,
-                           float* __restrict__ C) {
-  __shared__ double red[GNN_THREADS][GNN_OUT];
-  __shared__ float cs[GNN_OUT];
-  double acc[GNN_OUT] = {0.0, 0.0, 0.0, 0.0};
-  for (size_t v = threadIdx.x; v < n; v += blockDim.x)
-#pragma unroll
-    for (int k = 0; k < GNN_OUT; ++k) acc[k] += Craw[v * GNN_OUT + k];
-#pragma unroll
-  for (int k = 0; k < GNN_OUT; ++k) red[threadIdx.x][k] = acc[k];
-  __syncthreads();
-  if (threadIdx.x < GNN_OUT) {
-    double s = 0.0;
-    for (int t = 0; t < int(blockDim.x); ++t) s += red[t][threadIdx.x];
-    float m = float(s / double(n));
-    pooled[threadIdx.x] = m;
-    cs[threadIdx.x] = softplusf(m);
+// Per-vertex weights from the head outputs: s = softplus(o_s),
+// a = s^2 + a_min + softplus(o_a); C[v] = (a, s).
+__global__ void k_gnn_weights(uint32_t n, const float* __restrict__ Craw, float* __restrict__ C) {
+  for (size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += size_t(gridDim.x) * blockDim.x) {
+    const float sv = softplusf(Craw[v * GNN_OUT + 1]);
+    C[v * GNN_OUT + 0] = sv * sv + GNN_A_MIN + softplusf(Craw[v * GNN_OUT + 0]);
+    C[v * GNN_OUT + 1] = sv;
   }
-  __syncthreads();
-  for (size_t t = threadIdx.x; t < size_t(n) * GNN_OUT; t += blockDim.x) C[t] = cs[t % GNN_OUT];
-}
-
-// Backward of the pooling: g_k = sigmoid(pooled_k) / n * sum_v dC[v][k],
-// dCraw[v][k] = g_k for every vertex (one block, fixed order).
-__global__ void k_gnn_pool_back(uint32_t n, const float* __restrict__ dC, const float* __restrict__ pooled,
-                                float* __restrict__ dCraw) {
-  __shared__ double red[GNN_THREADS][GNN_OUT];
-  __shared__ float gs[GNN_OUT];
-  double acc[GNN_OUT] = {0.0, 0.0, 0.0, 0.0};
-  for (size_t v = threadIdx.x; v < n; v += blockDim.x)
-#pragma unroll
-    for (int k = 0; k < GNN_OUT; ++k) acc[k] += dC[v * GNN_OUT + k];
-#pragma unroll
-  for (int k = 0; k < GNN_OUT; ++k) red[threadIdx.x][k] = acc[k];
-  __syncthreads();
-  if (threadIdx.x < GNN_OUT) {
-    double s = 0.0;
-    for (int t = 0; t < int(blockDim.x); ++t) s += red[t][threadIdx.x];
-    gs[threadIdx.x] = float(s) * sigmoidf(pooled[threadIdx.x]) / float(n);
-  }
-  __syncthreads();
-  for (size_t t = threadIdx.x; t < size_t(n) * GNN_OUT; t += blockDim.x) dCraw[t] = gs[t % GNN_OUT];
 }
 
 // dH[v][i] = sum_k dCraw[v][k] Wo[i][k]
@@ -334,16 +299,67 @@ __global__ void k_adam(size_t n, float* __restrict__ p, const float* __restrict_
 // M L acts on e as a multiple of the identity, which is what flexible CG
 // rewards, and it ignores the overall scale of M, to which CG is blind.
 
-// Z = sum_k C[v][k] Y[k][v][j]
-__global__ void k_pair_z(uint32_t n, int P, const float* __restrict__ C, const float* __restrict__ Y,
-                         float* __restrict__ Z) {
-  size_t total = size_t(n) * P, plane = total;
+// Forward of the degree-1 stage on the pairs (P columns, vertex-interleaved),
+// with y_0 = r / d:  U = s y_0 (= (s/d) r),  AU = A U,  Z = a y_0 + (s/d) AU.
+__global__ void k_pair_sym_u(uint32_t n, int P, const float* __restrict__ C, const float* __restrict__ Y0,
+                             float* __restrict__ U) {
+  size_t total = size_t(n) * P;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x)
+    U[t] = C[(t / P) * GNN_OUT + 1] * Y0[t];
+}
+
+__global__ void k_pair_sym_z(uint32_t n, int P, const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
+                             const double* __restrict__ val, const double* __restrict__ diag,
+                             const float* __restrict__ C, const float* __restrict__ Y0, const float* __restrict__ U,
+                             float* __restrict__ AU, float* __restrict__ Z) {
+  size_t total = size_t(n) * P;
   for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
     size_t v = t / P;
-    float z = 0.0f;
-#pragma unroll
-    for (int k = 0; k < GNN_OUT; ++k) z += C[v * GNN_OUT + k] * Y[k * plane + t];
-    Z[t] = z;
+    int j = int(t % P);
+    double acc = 0.0;
+    for (uint32_t e = ptr[v]; e < ptr[v + 1]; ++e) acc += val[e] * double(U[size_t(col[e]) * P + j]);
+    AU[t] = float(acc);
+    Z[t] = float(double(C[v * GNN_OUT]) * double(Y0[t]) + double(C[v * GNN_OUT + 1]) / diag[v] * acc);
+  }
+}
+
+// Backward, given G = dloss/dZ = s1_j R + s2_j LZ:  W = (s/d) G,  AW = A W,
+//   dloss/da_v = sum_j G y_0,  dloss/ds_v = sum_j (G AU / d + y_0 AW) + 2 s dloss/da_v
+// (a depends on s), and through the head transform
+//   dCraw[v] = (dloss/da sigmoid(o_a), dloss/ds sigmoid(o_s)).
+__global__ void k_pair_sym_g(uint32_t n, int P, const float* __restrict__ C, const double* __restrict__ diag,
+                             const float* __restrict__ R, const float* __restrict__ LZ, const float* __restrict__ s12,
+                             float* __restrict__ G, float* __restrict__ Wv) {
+  size_t total = size_t(n) * P;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
+    size_t v = t / P;
+    int j = int(t % P);
+    float g = s12[j] * R[t] + s12[P + j] * LZ[t];
+    G[t] = g;
+    Wv[t] = float(double(C[v * GNN_OUT + 1]) / diag[v] * double(g));
+  }
+}
+
+__global__ void k_pair_sym_grad(uint32_t n, int P, const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
+                                const double* __restrict__ val, const double* __restrict__ diag,
+                                const float* __restrict__ Craw, const float* __restrict__ C,
+                                const float* __restrict__ Y0, const float* __restrict__ AU,
+                                const float* __restrict__ G, const float* __restrict__ Wv,
+                                float* __restrict__ dCraw) {
+  for (size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += size_t(gridDim.x) * blockDim.x) {
+    double da = 0.0, ds = 0.0;
+    const double dv = diag[v];
+    for (int j = 0; j < P; ++j) {
+      size_t t = v * P + j;
+      double aw = 0.0;
+      for (uint32_t e = ptr[v]; e < ptr[v + 1]; ++e) aw += val[e] * double(Wv[size_t(col[e]) * P + j]);
+      da += double(G[t]) * double(Y0[t]);
+      ds += double(G[t]) * double(AU[t]) / dv + double(Y0[t]) * aw;
+    }
+    const double sv = double(C[v * GNN_OUT + 1]);
+    ds += 2.0 * sv * da;
+    dCraw[v * GNN_OUT + 0] = float(da * double(sigmoidf(Craw[v * GNN_OUT + 0])));
+    dCraw[v * GNN_OUT + 1] = float(ds * double(sigmoidf(Craw[v * GNN_OUT + 1])));
   }
 }
 
@@ -384,40 +400,12 @@ __global__ void k_pair_energy(uint32_t n, int P, const uint32_t* __restrict__ pt
   (void)total;
 }
 
-// dC[v][k] = sum_j (s1_j R[v][j] + s2_j LZ[v][j]) Y[k][v][j]
-__global__ void k_pair_grad(uint32_t n, int P, const float* __restrict__ R, const float* __restrict__ LZ,
-                            const float* __restrict__ Y, const float* __restrict__ s12, float* __restrict__ dC) {
-  size_t total = size_t(n) * GNN_OUT, plane = size_t(n) * P;
-  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
-    size_t v = t / GNN_OUT;
-    int k = int(t % GNN_OUT);
-    float acc = 0.0f;
-    for (int j = 0; j < P; ++j)
-      acc += (s12[j] * R[v * P + j] + s12[P + j] * LZ[v * P + j]) * Y[k * plane + v * P + j];
-    dC[t] = acc;
-  }
-}
-
-// y_0 = r / d; y_k = D^{-1} A y_{k-1}  (P columns, double in, float out)
+// y_0 = r / d  (P columns, double in, float out)
 __global__ void k_pair_basis0(uint32_t n, int P, const double* __restrict__ r, const double* __restrict__ diag,
                               float* __restrict__ Y0) {
   size_t total = size_t(n) * P;
   for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x)
     Y0[t] = float(r[t] / diag[t / P]);
-}
-
-__global__ void k_pair_basis_next(uint32_t n, int P, const uint32_t* __restrict__ ptr,
-                                  const uint32_t* __restrict__ col, const double* __restrict__ val,
-                                  const double* __restrict__ diag, const float* __restrict__ Yp,
-                                  float* __restrict__ Yn) {
-  size_t total = size_t(n) * P;
-  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
-    size_t v = t / P;
-    int j = int(t % P);
-    double acc = 0.0;
-    for (uint32_t e = ptr[v]; e < ptr[v + 1]; ++e) acc += val[e] * double(Yp[size_t(col[e]) * P + j]);
-    Yn[t] = float(acc / diag[v]);
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -430,8 +418,7 @@ struct GraphData {
   DBuf<float> X;                           // n x 8
   DBuf<float> S[GNN_LAYERS];               // aggregated inputs per layer
   DBuf<float> H[GNN_LAYERS];               // outputs of the layers (n x 64)
-  DBuf<float> Craw, C;                     // n x 4
-  DBuf<float> pooled;                      // 4
+  DBuf<float> Craw, C;                     // n x 2: head outputs, weights (a, s)
 };
 
 struct DeviceParams {
@@ -455,7 +442,6 @@ void upload_graph(GraphData& g, uint32_t n, const std::vector<uint32_t>& ptr, co
   }
   g.Craw.alloc(size_t(n) * GNN_OUT);
   g.C.alloc(size_t(n) * GNN_OUT);
-  g.pooled.alloc(GNN_OUT);
 }
 
 void refresh_bf16(DeviceParams& p, cudaStream_t s) {
@@ -477,89 +463,14 @@ void forward(GraphData& g, DeviceParams& p, cudaStream_t s) {
   size_t o = gnn_layer_offset(GNN_LAYERS);
   k_gnn_head<<<gnn_blocks(size_t(g.n) * GNN_OUT), GNN_THREADS, 0, s>>>(
       g.n, in, p.bf.p + o, p.master.p + o + size_t(GNN_WIDTH) * GNN_OUT, g.Craw.p);
-  k_gnn_pool<<<1, GNN_THREADS, 0, s>>>(g.n, g.Craw.p, g.pooled.p, g.C.p);
+  k_gnn_weights<<<gnn_blocks(g.n), GNN_THREADS, 0, s>>>(g.n, g.Craw.p, g.C.p);
   CK_LAUNCH();
 }
 
-// ---------------------------------------------------------------------------
-// Polynomial preconditioner apply (double vectors, K columns)
-
-template <int K, bool FIRST, bool STORE>
-__global__ void k_poly_step(uint32_t n, const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
-                            const double* __restrict__ val, const double* __restrict__ dinv,
-                            const float* __restrict__ C, int k, const double* __restrict__ yprev,
-                            double* __restrict__ ynext, double* __restrict__ z) {
-  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
-  size_t total = size_t(n) * TPR, stride = size_t(gridDim.x) * blockDim.x;
-  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
-    size_t v = t / TPR;
-    int c0 = int(t % TPR) * CPT;
-    double acc[CPT];
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
-    for (uint32_t e = ptr[v]; e < ptr[v + 1]; ++e) {
-      size_t u = col[e];
-      double w = val[e] * (FIRST ? dinv[u] : 1.0);  // FIRST: yprev is r, y_0 = r / d
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) acc[c] += w * yprev[u * K + c0 + c];
-    }
-    double di = dinv[v];
-    double ck = double(C[v * GNN_OUT + k]);
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-      size_t i = v * K + c0 + c;
-      double y = di * acc[c];
-      if (STORE) ynext[i] = y;
-      if (FIRST)
-        z[i] = double(C[v * GNN_OUT]) * di * yprev[i] + ck * y;
-      else
-        z[i] += ck * y;
-    }
-  }
-}
-
-class PolyPreconditioner final : public LearnedPreconditioner {
+class VertexWeights final : public LearnedPreconditioner {
  public:
   GraphData g;
-  DBuf<double> dinv;
-  std::map<int, std::pair<DBuf<double>, DBuf<double>>> scratch;
-
-  double scalars[GNN_OUT] = {0, 0, 0, 0};
-  int launches_per_apply() const override { return GNN_OUT - 1; }
-  const float* coefficients() const override { return g.C.p; }
-  const double* scalar_coefficients() const override { return scalars; }
-
-  void apply(int K, const double* r, double* z, cudaStream_t s) override {
-    switch (K) {
-      case 1: run<1>(r, z, s); break;
-      case 2: run<2>(r, z, s); break;
-      case 8: run<8>(r, z, s); break;
-      case 16: run<16>(r, z, s); break;
-      case 32: run<32>(r, z, s); break;
-      case 64: run<64>(r, z, s); break;
-      default: fail(INVALID_INPUT, "learned_apply", "unsupported block width");
-    }
-  }
-
- private:
-  template <int K>
-  void run(const double* r, double* z, cudaStream_t s) {
-    auto& sc = scratch[K];
-    if (!sc.first.p) {
-      sc.first.alloc(size_t(g.n) * K);
-      sc.second.alloc(size_t(g.n) * K);
-    }
-    constexpr int TPR = Cols<K>::TPR;
-    int blocks = gnn_blocks(size_t(g.n) * TPR);
-    // z = c0 y0 + c1 y1 (y1 stored), z += c2 y2 (y2 stored), z += c3 y3
-    k_poly_step<K, true, true><<<blocks, GNN_THREADS, 0, s>>>(g.n, g.ptr.p, g.col.p, g.val.p, dinv.p, g.C.p, 1, r,
-                                                              sc.first.p, z);
-    k_poly_step<K, false, true><<<blocks, GNN_THREADS, 0, s>>>(g.n, g.ptr.p, g.col.p, g.val.p, dinv.p, g.C.p, 2,
-                                                               sc.first.p, sc.second.p, z);
-    k_poly_step<K, false, false><<<blocks, GNN_THREADS, 0, s>>>(g.n, g.ptr.p, g.col.p, g.val.p, dinv.p, g.C.p, 3,
-                                                                sc.second.p, nullptr, z);
-    CK_LAUNCH();
-  }
+  const float* weights() const override { return g.C.p; }
 };
 
 }  // namespace
@@ -571,20 +482,14 @@ std::unique_ptr<LearnedPreconditioner> build_learned(const std::vector<float>& p
                                                      const std::vector<double>& diag, cudaStream_t s, uint64_t& h2d) {
   if (params.size() != gnn_param_count())
     fail(INVALID_INPUT, "learned_preconditioner", "network parameters have the wrong length");
-  auto pc = std::make_unique<PolyPreconditioner>();
+  auto pc = std::make_unique<VertexWeights>();
   upload_graph(pc->g, n, ptr, col, val, diag, s, h2d);
-  std::vector<double> di(n);
-  for (uint32_t v = 0; v < n; ++v) di[v] = 1.0 / diag[v];
-  upload(pc->dinv, di, s, h2d);
   DeviceParams p;
   upload(p.master, params, s, h2d);
   p.bf.alloc(params.size());
   refresh_bf16(p, s);
   forward(pc->g, p, s);
-  float c[GNN_OUT];
-  CK(cudaMemcpyAsync(c, pc->g.C.p, sizeof(c), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
-  for (int k = 0; k < GNN_OUT; ++k) pc->scalars[k] = double(c[k]);
+  CK(cudaStreamSynchronize(s));  // the parameter buffers are released on return
   // the activations are not needed after inference
   for (int l = 0; l < GNN_LAYERS; ++l) {
     pc->g.S[l].release();
@@ -623,7 +528,7 @@ __global__ void k_trainer_init(const double* __restrict__ partial_rz, const doub
 struct TrainGraph {
   GraphData g;
   int P = 0;                 // pairs
-  DBuf<float> Y, E, Z, LZ, R, s12, dC, dCraw;
+  DBuf<float> Y, E, Z, LZ, R, s12, U, AU, G, Wv, dCraw;
   std::vector<float> ELE;    // host copy of the energy norms
   DBuf<float> dH[2], dZ, T;  // backward temporaries (n x 64)
   DBuf<float> partial;       // weight-gradient partials
@@ -863,19 +768,12 @@ class Trainer final : public GnnTrainer {
     }
     DBuf<double> Rd;
     upload(Rd, R, s, h2d);
-    tg->Y.alloc(size_t(GNN_OUT) * n * P);
     size_t plane = size_t(n) * P;
+    tg->Y.alloc(plane);
     k_pair_basis0<<<gnn_blocks(plane), GNN_THREADS, 0, s>>>(n, P, Rd.p, tg->g.diag.p, tg->Y.p);
-    for (int k = 1; k < GNN_OUT; ++k)
-      k_pair_basis_next<<<gnn_blocks(plane), GNN_THREADS, 0, s>>>(n, P, tg->g.ptr.p, tg->g.col.p, tg->g.val.p,
-                                                                   tg->g.diag.p, tg->Y.p + (k - 1) * plane,
-                                                                   tg->Y.p + k * plane);
     upload(tg->E, E, s, h2d);
-    tg->Z.alloc(plane);
-    tg->LZ.alloc(plane);
-    tg->R.alloc(plane);
+    for (auto* b : {&tg->Z, &tg->LZ, &tg->R, &tg->U, &tg->AU, &tg->G, &tg->Wv}) b->alloc(plane);
     tg->s12.alloc(size_t(2) * P);
-    tg->dC.alloc(size_t(n) * GNN_OUT);
     tg->dCraw.alloc(size_t(n) * GNN_OUT);
     for (auto& d : tg->dH) d.alloc(size_t(n) * GNN_WIDTH);
     tg->dZ.alloc(size_t(n) * GNN_WIDTH);
@@ -903,7 +801,9 @@ class Trainer final : public GnnTrainer {
     size_t plane = size_t(n) * P;
     refresh_bf16(p, s);
     forward(g, p, s);
-    k_pair_z<<<gnn_blocks(plane), GNN_THREADS, 0, s>>>(n, P, g.C.p, tg.Y.p, tg.Z.p);
+    k_pair_sym_u<<<gnn_blocks(plane), GNN_THREADS, 0, s>>>(n, P, g.C.p, tg.Y.p, tg.U.p);
+    k_pair_sym_z<<<gnn_blocks(plane), GNN_THREADS, 0, s>>>(n, P, g.ptr.p, g.col.p, g.val.p, g.diag.p, g.C.p, tg.Y.p,
+                                                           tg.U.p, tg.AU.p, tg.Z.p);
     k_pair_energy<<<ENERGY_BLOCKS, GNN_THREADS, 2 * GNN_THREADS * sizeof(double), s>>>(
         n, P, g.ptr.p, g.col.p, g.val.p, g.diag.p, tg.Z.p, tg.Y.p, tg.LZ.p, tg.R.p, tg.epart.p);
     std::vector<double> ep(size_t(ENERGY_BLOCKS) * 2 * P);
@@ -926,11 +826,12 @@ class Trainer final : public GnnTrainer {
     }
     loss /= P;
     CK(cudaMemcpyAsync(tg.s12.p, s12.data(), s12.size() * sizeof(float), cudaMemcpyHostToDevice, s));
-    k_pair_grad<<<gnn_blocks(size_t(n) * GNN_OUT), GNN_THREADS, 0, s>>>(n, P, tg.R.p, tg.LZ.p, tg.Y.p, tg.s12.p,
-                                                                        tg.dC.p);
+    k_pair_sym_g<<<gnn_blocks(plane), GNN_THREADS, 0, s>>>(n, P, g.C.p, g.diag.p, tg.R.p, tg.LZ.p, tg.s12.p, tg.G.p,
+                                                           tg.Wv.p);
+    k_pair_sym_grad<<<gnn_blocks(n), GNN_THREADS, 0, s>>>(n, P, g.ptr.p, g.col.p, g.val.p, g.diag.p, g.Craw.p, g.C.p,
+                                                          tg.Y.p, tg.AU.p, tg.G.p, tg.Wv.p, tg.dCraw.p);
     // head
     size_t oh = gnn_layer_offset(GNN_LAYERS);
-    k_gnn_pool_back<<<1, GNN_THREADS, 0, s>>>(n, tg.dC.p, g.pooled.p, tg.dCraw.p);
     k_gnn_head_back<<<gnn_blocks(size_t(n) * GNN_WIDTH), GNN_THREADS, 0, s>>>(n, tg.dCraw.p, p.bf.p + oh,
                                                                               tg.dH[0].p);
     wgrad(n, GNN_WIDTH, GNN_OUT, g.H[GNN_LAYERS - 1].p, tg.dCraw.p, 1, tg, oh);

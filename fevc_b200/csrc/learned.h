@@ -1,19 +1,22 @@
 // Learned preconditioner stage: a message-passing graph network that maps
-// static vertex features of the hybrid Laplacian to the coefficients of a
-// degree-3 polynomial preconditioner
+// static vertex features of the hybrid Laplacian to per-vertex weights (a, s)
+// of the symmetric degree-1 preconditioner
 //
-//   z = sum_k c_k y_k,   y_0 = D^{-1} r,   y_k = D^{-1} A y_{k-1},
+//   z = (a/d) .* r + (s/d) .* (A ((s/d) .* r)),
 //
-// used inside flexible PCG.  The network (4 message-passing layers, 64 wide,
-// BF16 weights, FP32 accumulation) runs once per graph; its per-vertex
-// outputs are mean-pooled over the graph and passed through softplus, so the
-// coefficients are one positive polynomial per graph and the preconditioner
-// D^{-1/2} p(D^{-1/2} A D^{-1/2}) D^{-1/2} is symmetric.  It
-// is trained on the device by this library's own forward and backward
-// kernels on residual/error pairs (r, e = L^+ r) that CMG-PCG generates on
-// seeded panels; the loss is scale invariant, 1 - (z'r)^2 / (e'Le z'Lz)
-// with z = M r (one minus the squared energy cosine between z and e),
-// averaged over the pairs.
+// i.e. D^{-1/2} (diag(a) + diag(s) N diag(s)) D^{-1/2} with N = D^{-1/2} A
+// D^{-1/2} (spectrum in [-1, 1]), applied inside the single-kernel PCG
+// (flex.cuh).  The head gives s = softplus(o_s) and a = s^2 + a_min +
+// softplus(o_a), so a > s^2 at every vertex and the preconditioner is
+// positive definite for any parameters.  Vertex-dependent weights make it a
+// different operator from any polynomial in D^{-1} L (which CG already
+// optimises over).  The network (4 message-passing layers, 64 wide, BF16
+// weights, FP32 accumulation) runs once per graph.  It is trained on the
+// device by this library's own forward and backward kernels on
+// residual/error pairs (r, e = L^+ r) that CMG-PCG generates on seeded
+// panels; the loss is scale invariant, 1 - (z'r)^2 / (e'Le z'Lz) with
+// z = M r (one minus the squared energy cosine between z and e), averaged
+// over the pairs.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -27,15 +30,16 @@ namespace fevcb {
 constexpr int GNN_FEATURES = 8;
 constexpr int GNN_WIDTH = 64;
 constexpr int GNN_LAYERS = 4;
-constexpr int GNN_OUT = 4;  // polynomial coefficients c_0..c_3
+constexpr int GNN_OUT = 2;  // per-vertex head outputs (o_a, o_s)
+constexpr float GNN_A_MIN = 0.01f;  // a >= s^2 + GNN_A_MIN
 
 // Parameter layout (FP32 master copy, contiguous): per layer l, Ws[in][64],
 // Wn[in][64], b[64] (in = 8 for l = 0, else 64); then Wo[64][4], bo[4].
 size_t gnn_param_count();
 size_t gnn_layer_offset(int layer);  // offset of Ws of `layer`; layer = GNN_LAYERS gives Wo
-// Deterministic initial parameters (seeded, scaled uniform; output bias at
-// the inverse softplus of 1 so an untrained network is the truncated
-// Neumann series with unit coefficients).
+// Deterministic initial parameters (seeded, scaled uniform; output biases at
+// s = 1 and a = 1.05, so an untrained network is the uniform first-order
+// Neumann stage).
 std::vector<float> gnn_initial_params(uint64_t seed);
 
 // Static features of every vertex of a Laplacian given as CSR of positive
@@ -43,16 +47,11 @@ std::vector<float> gnn_initial_params(uint64_t seed);
 void gnn_features(uint32_t n, const std::vector<uint32_t>& ptr, const std::vector<uint32_t>& col,
                   const std::vector<double>& val, const std::vector<double>& diag, std::vector<float>& X);
 
-// The polynomial preconditioner of one graph with its inferred coefficients.
+// The inferred per-vertex weights of one graph.
 class LearnedPreconditioner {
  public:
   virtual ~LearnedPreconditioner() = default;
-  // z = M r for K vertex-interleaved double columns (K = 1, 8, 16, 32, 64)
-  virtual void apply(int K, const double* r, double* z, cudaStream_t s) = 0;
-  virtual int launches_per_apply() const = 0;
-  virtual const float* coefficients() const = 0;  // device, n x GNN_OUT
-  // the pooled coefficients c_0..c_3 (every vertex carries the same ones)
-  virtual const double* scalar_coefficients() const = 0;
+  virtual const float* weights() const = 0;  // device, n x 2: (a, s) per vertex
 };
 
 std::unique_ptr<LearnedPreconditioner> build_learned(const std::vector<float>& params, uint32_t n,
@@ -78,9 +77,9 @@ class GnnTrainer {
   // Adam steps over the graphs in turn; returns the loss of every step.
   virtual std::vector<double> train(int steps, double lr) = 0;
   virtual std::vector<float>& params() = 0;
-  // Host copies of graph g for an independent check: CSR, features, the pair
-  // basis y_k (GNN_OUT x n x P, vertex-interleaved), errors e (n x P) and
-  // their energy norms |e|_L^2 (P).
+  // Host copies of graph g for an independent check: CSR, features, the
+  // scaled residuals y_0 = r / d (n x P, vertex-interleaved), errors e (n x P)
+  // and their energy norms |e|_L^2 (P).
   struct Dump {
     uint32_t n = 0, pairs = 0;
     std::vector<uint32_t> ptr, col;

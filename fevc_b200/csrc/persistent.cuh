@@ -733,256 +733,6 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent_cg(Persis
 }
 
 // ---------------------------------------------------------------------------
-// Persistent PCG with a degree-3 polynomial preconditioner
-//   z = c0 y0 + c1 y1 + c2 y2 + c3 y3,  y0 = D^{-1} r,  y_k = D^{-1} A y_{k-1}
-// (scalar coefficients, so the preconditioner is symmetric and plain CG
-// applies).  Each iteration: products of p and p.q | x, r update and r.r |
-// three segmented SpMVs of the y_k (products, then a finishing pass that
-// forms y_k and accumulates z; r.z with the last) | direction.  Nine grid
-// barriers per iteration, against three for Jacobi, but several times fewer
-// iterations.
-
-template <int K>
-struct PersistentPoly {
-  PersistentPcg<K> a;  // matrix, segments, x, r, p, partials, state (a.s.rz holds r.z)
-  double* y1;
-  double* y2;
-  double* z;
-  double c0, c1, c2, c3;
-};
-
-// The k-th segment of the work order: its id (the slot of its product), row,
-// whether it is the row's first segment, and its entries [b, e).  With the
-// balanced order (segments in decreasing length) when it is given, else in
-// storage order.
-template <int K>
-__device__ __forceinline__ void ordered_segment(const PersistentPcg<K>& a, size_t k, uint32_t& id, uint32_t& row,
-                                                bool& first, uint32_t& b, uint32_t& e) {
-  if (a.ord_id != nullptr) {
-    id = __ldg(a.ord_id + k);
-    const uint32_t f = __ldg(a.ord_flag + k);
-    row = f & ~SEG_FIRST;
-    first = (f & SEG_FIRST) != 0;
-    b = __ldg(a.ord_begin + k);
-    e = __ldg(a.ord_end + k);
-  } else {
-    id = uint32_t(k);
-    row = a.seg_row[k];
-    b = a.seg_begin[k];
-    e = a.seg_end[k];
-    first = b == a.ptr[row];
-  }
-}
-
-// Segment products of a vector (R_OVER_D: of y0 = r / d, scaled on the fly)
-template <int K, bool R_OVER_D>
-__device__ __forceinline__ void poly_products(const PersistentPcg<K>& a, const double* __restrict__ y, size_t gid,
-                                              size_t ngroups, int c0) {
-  constexpr int CPT = Cols<K>::CPT;
-  for (size_t k = gid; k < a.nseg; k += ngroups) {
-    uint32_t id, row, b, e;
-    bool first;
-    ordered_segment<K>(a, k, id, row, first, b, e);
-    double acc[CPT];
-    segment_gather<K, double, R_OVER_D>(a.col, a.val, a.dinv, y, b, e, c0, acc);
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) a.seg_buf[size_t(id) * K + c0 + c] = acc[c];
-  }
-}
-
-template <int K>
-__global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_persistent_poly(PersistentPoly<K> P) {
-  namespace cg = cooperative_groups;
-  cg::grid_group grid = cg::this_grid();
-  const PersistentPcg<K>& a = P.a;
-  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
-  __shared__ double s_alpha[K], s_beta[K], s_rz[K], s_tol2[K];
-  __shared__ int s_active[K], s_iters[K];
-  __shared__ int s_nactive;
-  __shared__ double s_fin[2 * K];
-  __shared__ double s_scratch[PERSIST_THREADS];
-  __shared__ double s_red[PERSIST_THREADS / 32][2][K];
-
-  for (int j = threadIdx.x; j < K; j += blockDim.x) {
-    s_rz[j] = a.s.rz[j];
-    s_tol2[j] = a.s.tol2[j];
-    s_active[j] = a.s.active[j];
-    s_iters[j] = a.s.iters[j];
-  }
-  if (threadIdx.x == 0) s_nactive = 0;
-  __syncthreads();
-
-  const int c0 = int(threadIdx.x % TPR) * CPT;
-  const size_t gid = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) / TPR;
-  const size_t ngroups = size_t(gridDim.x) * blockDim.x / TPR;
-  int it = 0;
-  for (; it < a.max_iters; ++it) {
-    // ---- A: products of p and p.(L p)
-    {
-      double v[1][CPT];
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) v[0][c] = 0.0;
-      for (size_t k = gid; k < a.nseg; k += ngroups) {
-        uint32_t id, row, b, e;
-        bool first;
-        ordered_segment<K>(a, k, id, row, first, b, e);
-        double acc[CPT];
-        segment_gather<K, double, false>(a.col, a.val, a.dinv, a.p, b, e, c0, acc);
-        const double* pr = a.p + size_t(row) * K + c0;
-        const double d = first ? a.diag[row] : 0.0;
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-          a.seg_buf[size_t(id) * K + c0 + c] = acc[c];
-          v[0][c] += pr[c] * (d * pr[c] - acc[c]);
-        }
-      }
-      block_reduce_cols_big<K, 1>(v, a.partial_a, (double(*)[1][K])s_red);
-    }
-    grid.sync();
-    redundant_finish<1, K>(a.partial_a, gridDim.x, s_fin, s_scratch);
-    for (int j = threadIdx.x; j < K; j += blockDim.x) {
-      double pq = s_fin[j], al = 0.0;
-      if (s_active[j]) {
-        if (!(pq > 0.0) || !isfinite(pq)) {
-          if (blockIdx.x == 0) atomicCAS(a.s.breakdown, -1, j);
-          s_active[j] = 0;
-        } else {
-          al = s_rz[j] / pq;
-        }
-      }
-      s_alpha[j] = al;
-    }
-    __syncthreads();
-    // ---- B: x += alpha p, r -= alpha q, r.r
-    {
-      double w[1][CPT];
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) w[0][c] = 0.0;
-      for (size_t row = gid; row < a.n; row += ngroups) {
-        uint32_t s0 = a.row_first[row], s1 = a.row_first[row + 1];
-        double dr = a.diag[row];
-        size_t o = row * K + c0;
-        double q[CPT];
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) q[c] = dr * a.p[o + c];
-        for (uint32_t sg = s0; sg < s1; ++sg)
-#pragma unroll
-          for (int c = 0; c < CPT; ++c) q[c] -= a.seg_buf[size_t(sg) * K + c0 + c];
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-          double al = s_alpha[c0 + c];
-          a.x[o + c] += al * a.p[o + c];
-          double ri = a.r[o + c] - al * q[c];
-          a.r[o + c] = ri;
-          w[0][c] += ri * ri;
-        }
-      }
-      block_reduce_cols_big<K, 1>(w, a.partial_b, (double(*)[1][K])s_red);
-    }
-    grid.sync();
-    redundant_finish<1, K>(a.partial_b, gridDim.x, s_fin, s_scratch);
-    if (threadIdx.x == 0) s_nactive = 0;
-    __syncthreads();
-    for (int j = threadIdx.x; j < K; j += blockDim.x) {
-      double rr = s_fin[j];
-      if (s_active[j]) {
-        s_iters[j] += 1;
-        if (blockIdx.x == 0) a.s.rr[j] = rr;
-        if (rr <= s_tol2[j])
-          s_active[j] = 0;
-        else
-          atomicAdd(&s_nactive, 1);
-      }
-    }
-    __syncthreads();
-    if (s_nactive == 0) {
-      ++it;
-      break;
-    }
-    // ---- preconditioner: three segmented SpMVs
-    poly_products<K, true>(a, a.r, gid, ngroups, c0);
-    grid.sync();
-    for (size_t row = gid; row < a.n; row += ngroups) {
-      uint32_t s0 = a.row_first[row], s1 = a.row_first[row + 1];
-      double di = a.dinv[row];
-      size_t o = row * K + c0;
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) {
-        double acc = 0.0;
-        for (uint32_t sg = s0; sg < s1; ++sg) acc += a.seg_buf[size_t(sg) * K + c0 + c];
-        double y1 = di * acc;
-        P.y1[o + c] = y1;
-        P.z[o + c] = P.c0 * di * a.r[o + c] + P.c1 * y1;
-      }
-    }
-    grid.sync();
-    poly_products<K, false>(a, P.y1, gid, ngroups, c0);
-    grid.sync();
-    for (size_t row = gid; row < a.n; row += ngroups) {
-      uint32_t s0 = a.row_first[row], s1 = a.row_first[row + 1];
-      double di = a.dinv[row];
-      size_t o = row * K + c0;
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) {
-        double acc = 0.0;
-        for (uint32_t sg = s0; sg < s1; ++sg) acc += a.seg_buf[size_t(sg) * K + c0 + c];
-        double y2 = di * acc;
-        P.y2[o + c] = y2;
-        P.z[o + c] += P.c2 * y2;
-      }
-    }
-    grid.sync();
-    poly_products<K, false>(a, P.y2, gid, ngroups, c0);
-    grid.sync();
-    {
-      double w[1][CPT];
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) w[0][c] = 0.0;
-      for (size_t row = gid; row < a.n; row += ngroups) {
-        uint32_t s0 = a.row_first[row], s1 = a.row_first[row + 1];
-        double di = a.dinv[row];
-        size_t o = row * K + c0;
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-          double acc = 0.0;
-          for (uint32_t sg = s0; sg < s1; ++sg) acc += a.seg_buf[size_t(sg) * K + c0 + c];
-          double zi = P.z[o + c] + P.c3 * di * acc;
-          P.z[o + c] = zi;
-          w[0][c] += a.r[o + c] * zi;
-        }
-      }
-      block_reduce_cols_big<K, 1>(w, a.partial_a, (double(*)[1][K])s_red);
-    }
-    grid.sync();
-    redundant_finish<1, K>(a.partial_a, gridDim.x, s_fin, s_scratch);
-    for (int j = threadIdx.x; j < K; j += blockDim.x) {
-      double rz = s_fin[j], be = 0.0;
-      if (s_active[j]) {
-        be = rz / s_rz[j];
-        s_rz[j] = rz;
-      }
-      s_beta[j] = be;
-    }
-    __syncthreads();
-    // ---- C: p = z + beta p
-    for (size_t row = gid; row < a.n; row += ngroups) {
-      size_t o = row * K + c0;
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) a.p[o + c] = P.z[o + c] + s_beta[c0 + c] * a.p[o + c];
-    }
-    grid.sync();
-  }
-  if (blockIdx.x == 0) {
-    for (int j = threadIdx.x; j < K; j += blockDim.x) {
-      a.s.rz[j] = s_rz[j];
-      a.s.active[j] = s_active[j];
-      a.s.iters[j] = s_iters[j];
-    }
-    if (threadIdx.x == 0) *a.s.nactive = s_nactive;
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Segmented firm-side gathers over the firm->cell lists.
 //   op 0: sum of cell values                      (right-hand side of the firm block)
 //   op 1: sum of cell_scale[c] * bW[w(c)]          (Schur reduction of the worker block)

@@ -129,7 +129,7 @@ class Trainer:
             "val": np.ctypeslib.as_array(d.weight, shape=(nnz,)).copy(),
             "diag": np.ctypeslib.as_array(d.diagonal, shape=(n,)).copy(),
             "X": np.ctypeslib.as_array(d.features, shape=(n, 8)).copy(),
-            "Y": np.ctypeslib.as_array(d.basis, shape=(4, n, P)).copy(),
+            "Y": np.ctypeslib.as_array(d.basis, shape=(1, n, P)).copy(),
             "E": np.ctypeslib.as_array(d.error, shape=(n, P)).copy(),
             "ELE": np.ctypeslib.as_array(d.energy, shape=(P,)).copy(),
         }

@@ -662,14 +662,16 @@ const char *vckss_rust_engine_last_error(void);
 typedef struct FevcbSolveOptionsV1 {
   uint32_t struct_size;
   uint32_t block_columns;   /* right-hand sides per blocked PCG: 0 auto, 2 (one target probe per solve), 8, 16, 32, 64 */
-  uint32_t preconditioner;  /* 0 auto, 1 Jacobi, 2 aggregation multigrid, 3 learned (flexible PCG) */
+  uint32_t preconditioner;  /* 0 auto, 1 Jacobi, 2 aggregation multigrid, 3 learned (flexible PCG),
+                               4 degree-1 polynomial stage with uniform weights z = (a r + s A (s r / d)) / d */
   uint32_t keep_unit_detail;/* 1: keep per-unit leverage arrays for fevcb_engine_unit_detail_v1 */
 } FevcbSolveOptionsV1;
 
 /* Prefix-extended options (struct_size 24), accepted by the same entry. */
 typedef struct FevcbSolveOptionsV2 {
   FevcbSolveOptionsV1 v1;
-  uint32_t precision;       /* 0 double; 1 single-precision inner PCG with double iterative refinement */
+  uint32_t precision;       /* 0 double; 1 single-precision residual, direction and products with a double
+                               solution, double reductions and double residual replacement */
   uint32_t reserved;
 } FevcbSolveOptionsV2;
 
@@ -832,7 +834,10 @@ int32_t fevcb_cmg_aggregate_v1(uint32_t vertices, const uint32_t *row_ptr, const
  * 3 leverage atoms + cell sums, 4 leverage moments, 5 the three-barrier and
  * 6 the two-barrier persistent PCG, 7 the three-barrier form with per-lane
  * index loads in its gather, 8 the three-barrier form without the pipelined
- * product phase (20 iterations per launch).
+ * product phase (20 iterations per launch), 9 the single-kernel mixed-precision
+ * Jacobi solve and 10 the same with the degree-1 polynomial stage (FP32
+ * storage, FP64 residual replacement; 20 iterations per launch, blocks of 32
+ * or 64 columns).
  * Outputs the median milliseconds per launch and algorithmic bytes per launch. */
 int32_t fevcb_engine_kernel_benchmark_v1(uint64_t generation, uint32_t kernel, uint32_t block_columns,
                                          uint32_t launches, double *ms_per_launch, double *bytes_per_launch);

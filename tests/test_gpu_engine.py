@@ -242,12 +242,12 @@ def test_accounting_identity_on_a_larger_panel(lib):
     assert 0 < res["plugin"][0] < 1 and 0 < res["plugin"][1] < 1
 
 
-def solve_precision(lib, panel, *, probes, precision, centering=0, tol=1e-12, seed=8675309):
+def solve_precision(lib, panel, *, probes, precision, centering=0, tol=1e-12, seed=8675309, precond=1, block=0):
     e = abi.Engine(lib)
     e.prepare(panel)
     if centering:
         e.centering(centering)
-    e.device_options(0, 1, precision)
+    e.device_options(block, precond, precision)
     req = e.default_request()
     req.seed = seed
     req.probes = probes
@@ -257,13 +257,23 @@ def solve_precision(lib, panel, *, probes, precision, centering=0, tol=1e-12, se
     return e
 
 
+# (precision, preconditioner, block width): the single-kernel solve in FP32
+# storage with FP64 residual replacement (Jacobi and the polynomial stage) and
+# the polynomial stage in FP64, at the automatic width (64) and at 32
+SINGLE_KERNEL_FORMS = [(1, 1, 0), (0, 4, 0), (1, 4, 0), (1, 4, 32)]
+
+
+@pytest.mark.parametrize("form", SINGLE_KERNEL_FORMS)
 @pytest.mark.parametrize("name", ["small_2k", "exact_20k", "weighted_1500", "regions_4k"])
-def test_mixed_precision_matches_reference(lib, golden, name):
-    """Single-precision inner PCG with double refinement reaches the same
-    FP64 complete-residual gate, so the components agree with the plugin's."""
+def test_single_kernel_forms_match_reference(lib, golden, name, form):
+    """The single-kernel forms certify every column on an FP64 (replaced)
+    residual and pass the same FP64 complete-residual gate, so the components
+    agree with the plugin's."""
+    precision, precond, block = form
     rec = golden["jla"]["panels"][name][1]
     panel = make_golden.PANELS[name]["build"]()
-    e = solve_precision(lib, panel, probes=rec["probes"], precision=1, centering=rec["centering"], seed=rec["seed"])
+    e = solve_precision(lib, panel, probes=rec["probes"], precision=precision, centering=rec["centering"],
+                        seed=rec["seed"], precond=precond, block=block)
     res = e.result()
     rc = e.rhs_receipts(1 + 3 * rec["probes"])
     e.release()
@@ -272,19 +282,26 @@ def test_mixed_precision_matches_reference(lib, golden, name):
     assert max(r["complete_residual"] for r in rc) <= max(10 * 1e-12, 1e-11)
 
 
-def test_mixed_precision_agrees_with_double_at_scale(lib):
+def test_single_kernel_forms_agree_with_double_at_scale(lib):
     from fevc_b200.panel import generate_panel
 
     panel = generate_panel(200_000, 10_000, 5, seed=99)
-    out = {}
-    for precision in (0, 1):
-        e = solve_precision(lib, panel, probes=32, precision=precision, tol=1e-8)
-        out[precision] = e.result()
+    out, iters = {}, {}
+    for precision, precond in ((0, 1), (1, 1), (1, 4)):
+        e = solve_precision(lib, panel, probes=32, precision=precision, tol=1e-8, precond=precond)
+        out[(precision, precond)] = e.result()
+        t = e.timings()
+        iters[(precision, precond)] = t["column_iterations"] / t["rhs_columns"]
         rc = e.rhs_receipts(1 + 3 * 32)
         e.release()
         assert max(r["complete_residual"] for r in rc) <= 1e-7
-    for key in ("plugin", "correction", "corrected"):
-        assert rel(out[1][key], out[0][key]) < 1e-6, key
+    for form in ((1, 1), (1, 4)):
+        for key in ("plugin", "correction", "corrected"):
+            assert rel(out[form][key], out[(0, 1)][key]) < 1e-6, (form, key)
+    # FP32 storage with residual replacement keeps the FP64 iteration count
+    # within a few iterations, and the polynomial stage cuts it by about half
+    assert iters[(1, 1)] <= 1.15 * iters[(0, 1)] + 2, iters
+    assert iters[(1, 4)] <= 0.7 * iters[(1, 1)], iters
 
 
 @pytest.mark.parametrize("name", ["small_2k", "pareto13_4k", "regions_4k"])

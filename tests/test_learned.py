@@ -33,10 +33,10 @@ def small_problem(seed=0, n=30, P=6):
     ptr, col, val = np.array(ptr), np.array(col), np.array(val)
     diag = np.array([val[ptr[v]:ptr[v + 1]].sum() for v in range(n)])
     d = {"n": n, "pairs": P, "ptr": ptr, "col": col, "val": val, "diag": diag,
-         "X": rng.normal(size=(n, 8)), "Y": rng.normal(size=(4, n, P)), "E": rng.normal(size=(n, P))}
-    _, L = gnn_oracle.adjacency(d)
+         "X": rng.normal(size=(n, 8)), "E": rng.normal(size=(n, P))}
+    _, L, _ = gnn_oracle.adjacency(d)
     # pairs consistent with the loss: y_0 = r / d with r = L e
-    d["Y"][0] = (L @ d["E"]) / diag[:, None]
+    d["Y"] = ((L @ d["E"]) / diag[:, None])[None]
     d["ELE"] = np.einsum("vj,vj->j", d["E"], L @ d["E"])
     return d
 
@@ -68,11 +68,14 @@ def test_bf16_rounding_is_round_to_nearest_even():
 
 def test_parameter_layout_and_initial_params(lib):
     n = learned.param_count(lib)
-    assert n == gnn_oracle.layout()[2] == 26116
+    assert n == gnn_oracle.layout()[2] == 25986
     p0, p1 = learned.initial_params(lib, 1), learned.initial_params(lib, 1)
     assert np.array_equal(p0, p1) and np.all(np.isfinite(p0))
-    # untrained network: softplus(bias) = 1 for every coefficient
-    assert np.allclose(np.logaddexp(0.0, p0[-4:]), 1.0, atol=1e-6)
+    # untrained network: s = softplus(b_s) = 1 and a = s^2 + a_min + softplus(b_a)
+    # = 1.05 at every vertex (the uniform first-order Neumann stage)
+    s = np.logaddexp(0.0, p0[-1])
+    a = s * s + gnn_oracle.A_MIN + np.logaddexp(0.0, p0[-2])
+    assert abs(s - 1.0) < 1e-6 and abs(a - 1.05) < 1e-6
 
 
 def test_install_validates_parameters(lib):
