@@ -1,31 +1,42 @@
-"""Benchmark: JLA probe solves/s (and time-to-decomposition) on a seeded panel.
+"""Benchmark: JLA probe solves/s and time-to-decomposition on a seeded panel.
 
-A step is one complete leave-out decomposition of the prepared panel: the full
-fit, P leverage probes and 2P target solves (1 + 3P right-hand sides), the
-leverage adjustment, the target contraction and the four components.
+Workload (default): the 10M-worker leave-observation-out panel
+(10,000,000 workers, 1,000,000 firms, 5 periods, Pareto(1.2) firm sizes,
+4 year controls, observation deletion; seeded generator fevc_b200/panel.py),
+1000 probes (3001 right-hand sides), tolerance 1e-8.  A step is one complete
+leave-out decomposition of the prepared panel: the full fit, P leverage probes
+and 2P target solves, the leverage adjustment, the target contraction and the
+four components.
 
-* ``value``  device-resident throughput: the prepared problem is in HBM and a
-  step re-runs the solve (``fevcb_engine_resolve_v1``); CUDA events on the
-  library's stream bracket exactly K steps after W warm-up steps.
+* ``value``  device-resident throughput of the headline form: the prepared
+  problem is in HBM and a step re-runs the solve (``fevcb_engine_resolve_v1``);
+  CUDA events on the library's stream bracket exactly K steps after W warm-up
+  steps.  The headline form is the learned degree-1 preconditioner stage
+  (network weights from fevc_b200/learned_params.f32) inside the single-kernel
+  blocked PCG with FP32 storage and FP64 reductions and residual replacement
+  (blocks of 64 columns); without committed parameters, the same stage with
+  uniform weights.
 * ``e2e``    the same metric through the plugin C ABI a caller uses: each step
   is ``solve_v5`` + ``result_v1`` on a freshly prepared generation, so the
   host->device upload of the prepared problem and the device->host result read
-  are inside the timed region (host preparation is outside it and reported
-  separately as ``prepare_s``; prepare + solve is the time-to-decomposition).
-* ``roofline``  the dominant kernel (blocked SpMM on the hybrid Laplacian)
-  timed standalone with CUDA events, L2 flushed before each launch.
-* ``cpu_baseline``  the reference's own CPU implementation (its shipped plugin,
-  staged in oracle/_ref by oracle/build.py; else the C oracle) on a bounded
-  sample of the same panel, all host cores.
-
+  are inside the timed region (host preparation is outside it and reported as
+  ``prepare_s``; prepare + solve is the time-to-decomposition).
+* ``roofline``  the dominant kernel (the single-kernel blocked PCG of the
+  headline form) timed standalone with CUDA events, L2 flushed before each
+  launch; algorithmic bytes per launch from the library's formula.
 * ``forms``  the other solver forms on the same panel, one device-resident
-  step each: the plain GPU CMG-PCG form (FP64, one target probe per solve, a
-  bounded probe sample), the blocked CMG-PCG, the learned flexible PCG (with
-  the committed network parameters) and the mixed-precision solve;
-  ``speedup_vs_plain_gpu_cmg_pcg`` is ``value`` over the plain form's rate.
+  step each: FP64 Jacobi blocked PCG, mixed-precision Jacobi, the degree-1
+  stage with uniform weights (the method without the network) and the plain
+  GPU CMG-PCG (FP64, one target probe per solve) on a bounded probe sample.
+* ``parity``  the reference plugin and this engine on the same panel, seed and
+  probes at a size the plugin finishes: the largest relative difference of
+  each component group.
+* ``cpu_baseline``  the reference's own CPU implementation (its shipped
+  plugin, staged in oracle/_ref by oracle/build.py) on a bounded sample of the
+  same workload, all host cores.
 
 ``--impl reference`` times the reference plugin alone (rank 0) on the same
-panel and metric and prints its own JSON line.
+workload, metric and config and prints its own JSON line.
 """
 
 from __future__ import annotations
@@ -34,6 +45,7 @@ import argparse
 import ctypes as C
 import json
 import os
+import platform
 import subprocess
 import sys
 import threading
@@ -45,9 +57,22 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-WORKLOAD = "plain_1m"
+WORKLOAD = "learned_10m"
+PROBES = 1000
 METRIC = "JLA probe solves/s & time-to-decomposition, learned+batched vs plain GPU PCG"
 UNIT = "probe solves/s"
+PARITY_RTOL = 1e-6
+FALLBACK_HBM_GBS = 6650.0
+
+# solver forms: (preconditioner, precision, block columns, description)
+FORMS = {
+    "learned_mixed": (3, 1, 64, "learned per-vertex degree-1 stage in the single-kernel PCG, FP32 storage with "
+                                "FP64 reductions and residual replacement, blocks of 64"),
+    "polynomial_mixed": (4, 1, 64, "degree-1 stage with uniform weights (the method without the network), "
+                                   "FP32 storage with FP64 reductions and residual replacement, blocks of 64"),
+    "jacobi_mixed": (1, 1, 64, "Jacobi, FP32 storage with FP64 reductions and residual replacement, blocks of 64"),
+    "jacobi_fp64": (1, 0, 64, "Jacobi blocked PCG in FP64 (three grid barriers per iteration), blocks of 64"),
+}
 
 
 def parse():
@@ -58,14 +83,15 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--probes", type=int, default=200)
+    ap.add_argument("--probes", type=int, default=PROBES)
     ap.add_argument("--tolerance", type=float, default=1e-8)
-    ap.add_argument("--block", type=int, default=0)
-    ap.add_argument("--precond", type=int, default=0)
-    ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--cpu-probes", type=int, default=24)
+    ap.add_argument("--form", default="auto", choices=["auto"] + list(FORMS))
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-probes", type=int, default=0, help="probe sample of the CPU legs (0: per workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true")
+    ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--parity-probes", type=int, default=24)
     ap.add_argument("--sharded", action="store_true", help="use the probe-sharded path at any N (launch with torchrun)")
     ap.add_argument("--plain-probes", type=int, default=8)
     return ap.parse_args()
@@ -116,11 +142,10 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def build_panel(args):
+def build_panel(workload, scale):
     from fevc_b200.panel import named_panel
 
-    panel = named_panel(args.workload, args.scale)
-    return panel, len(panel.controls)
+    return named_panel(workload, scale)
 
 
 def deletion_mode(panel) -> int:
@@ -128,10 +153,25 @@ def deletion_mode(panel) -> int:
     return 2 if panel.info.get("deletion") == "observation" else 1
 
 
-def v5_request(engine, probes, tolerance, *, reference=False, deletion=1):
+def workload_config(args, panel):
+    """The config dict of the JSON line; the same in both arms."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    total = args.probes * world
+    return {"workload": f"{args.workload} panel ({panel.info['workers']} workers, {panel.info['firms']} firms, "
+                        f"{panel.info['periods']} periods), {total} probes, {len(panel.controls)} year controls, "
+                        f"{'observation' if deletion_mode(panel) == 2 else 'match'} deletion",
+            "probes": total, "rhs_per_step": 1 + 3 * total, "tolerance": args.tolerance,
+            "controls": len(panel.controls),
+            "parallelism": (f"probe-sharded x{world}: {args.probes} probes per GPU, {total} in the decomposition; "
+                            "NCCL all-reduce of the leverage accumulators and gather of the draws")
+            if world > 1 or args.sharded else "single GPU",
+            "l2": "inputs larger than L2 (the prepared problem and the 64-column blocks exceed 126 MB)"}
+
+
+def v5_request(engine, probes, tolerance, *, reference=False, deletion=1, route=None):
     """A V5 solve request: JLA, the panel's deletion mode, supplied tolerance.
     With controls the generic engine runs; the reference additionally selects
-    its production CMG_FULL_V2 route on all host cores."""
+    its production CMG_FULL_V2 route (or `route`) on all host cores."""
     q = engine.default_request_v5(deletion)
     if deletion == 2:
         q.v4.v3.engine = 2  # leave-observation-out runs the generic engine
@@ -143,7 +183,10 @@ def v5_request(engine, probes, tolerance, *, reference=False, deletion=1):
     q.tolerance_supplied = 1
     if reference:
         q.threads = os.cpu_count() or 1
-        q.full_cmg_v2 = 1
+        if route == "diagonal":
+            v1.solver_route = 2
+        else:
+            q.full_cmg_v2 = 1
     return q
 
 
@@ -152,43 +195,95 @@ def reference_plugin_path():
     return p if p.exists() else None
 
 
+def cpu_model() -> str:
+    try:
+        for line in subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout.splitlines():
+            if line.startswith("Model name:"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return platform.processor() or "unknown"
+
+
+def reference_solve(lib, panel, probes, tolerance, *, route=None, prepared=None):
+    """One reference solve through its V5 C ABI: production route first, its
+    diagonal PCG route when the production refinement refuses the panel (a
+    refused solve leaves the generation failed, so the retry re-prepares).
+    Returns (engine, route used, solve seconds, result, refusal text)."""
+    from fevc_b200 import abi
+
+    refused = None
+    for r in ([route] if route else ["cmg_full_v2", "diagonal"]):
+        e = prepared if prepared is not None else abi.Engine(lib)
+        prepared = None
+        if e.generation == 0:
+            e.prepare(panel, deletion_mode=deletion_mode(panel))
+        q = v5_request(e, probes, tolerance, reference=True, deletion=deletion_mode(panel), route=r)
+        t0 = time.perf_counter()
+        try:
+            e.solve_v5(q, controls_count=len(panel.controls))
+        except abi.EngineError as err:
+            refused = f"{r}: {err}"
+            e.release()
+            continue
+        res = e.result()
+        return e, r, time.perf_counter() - t0, res, refused
+    raise RuntimeError(f"the reference plugin refused the panel: {refused}")
+
+
+def cpu_probes(args) -> int:
+    if args.cpu_probes:
+        return args.cpu_probes
+    # leave-observation-out inverts 1 - P_ii per row: a sample must be large
+    # enough for every estimate to stay positive
+    return 24 if args.workload != "learned_10m" else 32
+
+
 def time_reference(panel, probes, tolerance, steps, warmup):
-    """The reference plugin's V5 full-CMG solve (CMG_FULL_V2) on all host cores."""
+    """The reference plugin prepared once, then `warmup + steps` solves of a
+    `probes`-probe sample (the route that completes: CMG_FULL_V2, else its
+    diagonal PCG), each timed solve_v5 + result_v1; median of the timed ones."""
     from fevc_b200 import abi
 
     lib = abi.load(reference_plugin_path(), bind_extensions=False)
     threads = os.cpu_count() or 1
-    times, prep_times, res = [], [], None
+    e = abi.Engine(lib)
+    t0 = time.perf_counter()
+    e.prepare(panel, deletion_mode=deletion_mode(panel))
+    prepare_s = time.perf_counter() - t0
+    e, route, first_s, res, refused = reference_solve(lib, panel, probes, tolerance, prepared=e)
+    times = []
     for i in range(warmup + steps):
-        e = abi.Engine(lib)
+        q = v5_request(e, probes, tolerance, reference=True, deletion=deletion_mode(panel), route=route)
         t0 = time.perf_counter()
-        e.prepare(panel, deletion_mode=deletion_mode(panel))
-        t1 = time.perf_counter()
-        q = v5_request(e, probes, tolerance, reference=True, deletion=deletion_mode(panel))
         e.solve_v5(q, controls_count=len(panel.controls))
         res = e.result()
-        t2 = time.perf_counter()
-        e.release()
         if i >= warmup:
-            times.append(t2 - t1)
-            prep_times.append(t1 - t0)
-    rhs = 1 + 3 * probes
-    return {"rhs_per_s": rhs / float(np.median(times)), "solve_s": float(np.median(times)),
-            "prepare_s": float(np.median(prep_times)), "threads": threads, "components": res}
+            times.append(time.perf_counter() - t0)
+    e.release()
+    solve_s = float(np.median(times)) if times else first_s
+    return {"rhs_per_s": (1 + 3 * probes) / solve_s, "solve_s": solve_s, "prepare_s": prepare_s,
+            "threads": threads, "route": route, "refused": refused, "components": res, "timed": len(times)}
 
 
-def cpu_baseline(panel, probes, tolerance):
-    if reference_plugin_path() is not None:
-        r = time_reference(panel, probes, tolerance, steps=1, warmup=0)
-        return {"value": round(r["rhs_per_s"], 3), "unit": UNIT, "cores": r["threads"], "kind": "reference",
-                "sample": f"reference plugin CMG_FULL_V2 solve of the same panel with {probes} probes "
-                          f"({1 + 3 * probes} RHS) at tol {tolerance:g}; solve phase {r['solve_s']:.2f} s, "
-                          f"prepare {r['prepare_s']:.2f} s"}
-    return None
+def cpu_baseline(args, panel):
+    """Warm median of 3 reference solves of a bounded probe sample (one
+    discarded warm-up solve), rank 0, all host cores."""
+    if reference_plugin_path() is None:
+        return None
+    probes = min(args.probes, cpu_probes(args))
+    r = time_reference(panel, probes, args.tolerance, steps=3, warmup=0)
+    return {"value": round(r["rhs_per_s"], 4), "unit": UNIT, "cores": r["threads"], "kind": "reference",
+            "cpu_model": cpu_model(),
+            "sample": f"reference plugin ({r['route']} route{'; ' + r['refused'] if r['refused'] else ''}) on the "
+                      f"same panel, {probes} probes ({1 + 3 * probes} RHS) at tol {args.tolerance:g}; prepared once "
+                      f"({r['prepare_s']:.1f} s, not in the rate), first solve discarded, median of {r['timed']} "
+                      f"solve+result of {r['solve_s']:.2f} s"}
 
 
-def time_form(lib, panel, controls, probes, tolerance, block, precond, precision, stream, barrier):
-    """One device-resident step of a solver form: (ms, RHS/s, column iterations per RHS)."""
+def time_form(lib, panel, probes, tolerance, block, precond, precision, stream, barrier, *, timed=True):
+    """One device-resident step of a solver form: ms, RHS/s, iterations per RHS
+    and the corrected components."""
     import torch
 
     from fevc_b200 import abi
@@ -196,79 +291,132 @@ def time_form(lib, panel, controls, probes, tolerance, block, precond, precision
     e = abi.Engine(lib)
     e.prepare(panel, deletion_mode=deletion_mode(panel))
     e.device_options(block, precond, precision)
-    e.solve_v5(v5_request(e, probes, tolerance, deletion=deletion_mode(panel)), controls_count=controls)
-    barrier()
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record(stream)
-    e.resolve()
-    stop.record(stream)
-    barrier()
-    ms = start.elapsed_time(stop)
+    q = v5_request(e, probes, tolerance, deletion=deletion_mode(panel))
+    t0 = time.perf_counter()
+    e.solve_v5(q, controls_count=len(panel.controls))
+    torch.cuda.synchronize()
+    first = time.perf_counter() - t0
+    ms = None
+    if timed:
+        barrier()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        e.resolve()
+        stop.record(stream)
+        barrier()
+        ms = start.elapsed_time(stop)
     t = e.timings()
     res = e.result()
     e.release()
     rhs = 1 + 3 * probes
+    ms = ms if ms is not None else first * 1000.0
     return {"ms_per_step": round(ms, 3), "value": round(rhs / (ms / 1000.0), 3), "unit": UNIT, "probes": probes,
             "iterations_per_rhs": round(t["column_iterations"] / max(t["rhs_columns"], 1), 3),
             "fallbacks": t["fallbacks"], "corrected": [round(x, 10) for x in res["corrected"]]}
 
 
-def time_forms(lib, panel, controls, args, stream, barrier):
+def plain_form_rate(lib, panel, probes, tolerance):
+    """The plain GPU CMG-PCG form (FP64, aggregation multigrid, one target
+    probe per solve) on a bounded probe sample: RHS solved per second of
+    solve wall.  A sample too small for the leave-out inverses to stay
+    positive is refused after the fit and the leverage solves; the rate then
+    counts those 1 + P solves."""
+    import torch
+
+    from fevc_b200 import abi
+
+    e = abi.Engine(lib)
+    e.prepare(panel, deletion_mode=deletion_mode(panel))
+    e.device_options(2, 2, 0)
+    q = v5_request(e, probes, tolerance, deletion=deletion_mode(panel))
+    t0 = time.perf_counter()
+    refused = None
+    try:
+        e.solve_v5(q, controls_count=len(panel.controls))
+        rhs = 1 + 3 * probes
+    except abi.EngineError as err:
+        refused = str(err)
+        rhs = 1 + probes
+    torch.cuda.synchronize()
+    s = time.perf_counter() - t0
+    e.release()
+    return {"value": round(rhs / s, 4), "unit": UNIT, "probes": probes, "rhs_solved": rhs,
+            "seconds": round(s, 3), "refused_after_leverage": refused,
+            "form": "FP64 CMG-PCG (device aggregation multigrid V-cycle), one target probe (two right-hand sides) "
+                    f"per solve, bounded sample of {probes} probes (wall of solve_v5 including the hierarchy build)"}
+
+
+def time_forms(lib, panel, args, stream, barrier, headline):
     from fevc_b200 import abi, learned
 
     def guarded(fn):
-        # a form that the estimator refuses on this panel (e.g. a leave-out
-        # inverse that a small probe sample leaves nonpositive) is reported,
-        # not fatal to the line
         try:
             return fn()
         except abi.EngineError as err:
             return {"error": str(err)}
 
     forms = {}
-    plain_probes = min(args.probes, args.plain_probes)
-    if deletion_mode(panel) == 2:
-        # leave-observation-out inverts 1 - P_ii per row: a few probes leave
-        # some estimates nonpositive, so the plain form's sample is larger
-        plain_probes = min(args.probes, max(args.plain_probes, 200))
-    forms["plain_gpu_cmg_pcg"] = {
-        **guarded(lambda: time_form(lib, panel, controls, plain_probes, args.tolerance, 2, 2, 0, stream, barrier)),
-        "form": "FP64 CMG-PCG, one target probe (two right-hand sides) per solve, "
-                f"bounded sample of {plain_probes} probes"}
-    params = learned.load_params()
-    if params is not None:
-        learned.install(lib, params)
-        forms["learned_flexible_pcg"] = {
-            **guarded(lambda: time_form(lib, panel, controls, args.probes, args.tolerance, 64, 3, 0, stream, barrier)),
-            "form": "graph-network polynomial preconditioner in flexible PCG, blocks of 64 (learned_params.f32)"}
-    forms["mixed_precision"] = {
-        **guarded(lambda: time_form(lib, panel, controls, args.probes, args.tolerance, 64, 1, 1, stream, barrier)),
-        "form": "single-precision inner PCG with double refinement, blocks of 64"}
-    forms["cmg_blocked"] = {
-        **guarded(lambda: time_form(lib, panel, controls, args.probes, args.tolerance, 64, 2, 0, stream, barrier)),
-        "form": "FP64 CMG-PCG, blocks of 64"}
+    have_params = learned.load_params() is not None
+    for name, (precond, precision, block, text) in FORMS.items():
+        if name == headline or (precond == 3 and not have_params):
+            continue
+        forms[name] = {**guarded(lambda: time_form(lib, panel, args.probes, args.tolerance, block, precond, precision,
+                                                   stream, barrier)), "form": text}
+    forms["plain_gpu_cmg_pcg"] = guarded(lambda: plain_form_rate(lib, panel, min(args.probes, args.plain_probes),
+                                                                 args.tolerance))
     return forms
+
+
+def parity(lib, headline, tolerance, workload, scale, probes):
+    """The reference plugin and this engine (headline form) on the same panel,
+    seed and probes: the largest relative difference of each component group,
+    relative to the group's largest component."""
+    from fevc_b200 import abi
+
+    panel = build_panel(workload, scale)
+    ref_lib = abi.load(reference_plugin_path(), bind_extensions=False)
+    e, route, solve_s, ref, refused = reference_solve(ref_lib, panel, probes, tolerance)
+    e.release()
+    precond, precision, block, _ = FORMS[headline]
+    g = abi.Engine(lib)
+    g.prepare(panel, deletion_mode=deletion_mode(panel))
+    g.device_options(block, precond, precision)
+    g.solve_v5(v5_request(g, probes, tolerance, deletion=deletion_mode(panel)), controls_count=len(panel.controls))
+    ours = g.result()
+    g.release()
+    diffs = {}
+    for group in ("plugin", "correction", "corrected", "numerical_mcse"):
+        a, b = np.asarray(ours[group], dtype=float), np.asarray(ref[group], dtype=float)
+        diffs[group] = float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+    return {"workload": f"{workload} panel at scale {scale:g} ({panel.info['workers']} workers, "
+                        f"{panel.info['firms']} firms)", "probes": probes, "tolerance": tolerance,
+            "reference_route": route, "reference_refused_route": refused, "reference_solve_s": round(solve_s, 2),
+            "form": headline, "max_rel_diff": diffs, "rtol": PARITY_RTOL,
+            "ok": all(v <= PARITY_RTOL for v in diffs.values()),
+            "corrected": {"ours": [float(x) for x in ours["corrected"]], "reference": [float(x) for x in ref["corrected"]]}}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    panel, controls = build_panel(args)
+    panel = build_panel(args.workload, args.scale)
     if reference_plugin_path() is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference plugin not staged (run oracle/build.py)"}))
         return
-    probes = min(args.probes, args.cpu_probes)
+    probes = min(args.probes, cpu_probes(args))
     r = time_reference(panel, probes, args.tolerance, args.steps, args.warmup)
+    sample = (f"reference plugin ({r['route']} route{'; ' + r['refused'] if r['refused'] else ''}) prepared once "
+              f"({r['prepare_s']:.1f} s, not in the rate); each step solve_v5 + result_v1 of a {probes}-probe sample "
+              f"({1 + 3 * probes} RHS) of the same panel")
     line = {"metric": METRIC, "value": round(r["rhs_per_s"], 4), "unit": UNIT, "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1000 * r["solve_s"], 2), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, fevc_b200/panel.py)",
-            "config": {"workload": f"{args.workload} panel, {probes}-probe sample", "probes": probes,
-                       "tolerance": args.tolerance, "controls": controls},
+            "config": workload_config(args, panel),
             "prepare_s": round(r["prepare_s"], 3),
             "cpu_baseline": {"value": round(r["rhs_per_s"], 4), "unit": UNIT, "cores": r["threads"],
-                             "kind": "reference", "sample": f"{probes} probes ({1 + 3 * probes} RHS) per step"},
+                             "kind": "reference", "cpu_model": cpu_model(), "sample": sample},
             "e2e": {"value": round(r["rhs_per_s"], 4), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -297,26 +445,36 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    from fevc_b200 import abi
+    from fevc_b200 import abi, learned
 
     lib = abi.load()
     stream = torch.cuda.Stream()  # the library launches on this stream; the events below record on it
     torch.cuda.set_stream(stream)
     lib.fevcb_set_stream(C.c_void_p(stream.cuda_stream))
-    panel, controls = build_panel(args)
+    panel = build_panel(args.workload, args.scale)
+    controls = len(panel.controls)
+
+    params = learned.load_params()
+    headline = args.form
+    if headline == "auto":
+        headline = "learned_mixed" if params is not None else "polynomial_mixed"
+    if FORMS[headline][0] == 3:
+        if params is None:
+            raise SystemExit("the learned form needs fevc_b200/learned_params.f32 (python -m fevc_b200.learned)")
+        learned.install(lib, params)
+    precond, precision, block, form_text = FORMS[headline]
 
     e = abi.Engine(lib)
     t0 = time.perf_counter()
     e.prepare(panel, deletion_mode=deletion_mode(panel))
     prepare_s = time.perf_counter() - t0
-    e.device_options(args.block, args.precond)
+    e.device_options(block, precond, precision)
     # N ranks: every rank contributes `probes` probes to one decomposition of
     # probes x N (weak scaling); the leverage accumulators are all-reduced and
     # the target draws gathered over NCCL (fevc_b200/sharded.py)
     total_probes = args.probes * world
     req = v5_request(e, total_probes, args.tolerance, deletion=deletion_mode(panel))
     rhs = 1 + 3 * args.probes  # right-hand sides this rank solves per step
-    collectives = None
     use_shards = world > 1 or args.sharded
     if use_shards:
         from fevc_b200 import sharded
@@ -360,32 +518,31 @@ def main():
     timings = e.timings()
     value = world * rhs * args.steps / (ms / 1000.0)
 
-    # roofline: the persistent blocked PCG kernel, standalone launches with L2 flushed
-    block = args.block or 64
+    # roofline: the headline form's single-kernel PCG, standalone launches
+    # with L2 flushed (mode 10: the polynomial stage, 9: Jacobi; both FP32
+    # storage); the FP64 Jacobi kernel beside it for comparison
+    roof_mode = 10 if precond in (3, 4) else (9 if precision == 1 else 1)
     torch.cuda.nvtx.range_push("roofline")  # the roofline kernel's standalone launches
-    spmm_ms, spmm_bytes = e.kernel_benchmark(1, block, 10)
+    roof_ms, roof_bytes = e.kernel_benchmark(roof_mode, block, 10)
     torch.cuda.nvtx.range_pop()
-    # the same iterations in both persistent forms, for comparison
-    three_ms, _ = e.kernel_benchmark(5, block, 10)
-    two_ms, _ = e.kernel_benchmark(6, block, 10)
-    two_barrier = block == 32  # the form the solver picks at this width (double, one warp per segment)
+    fp64_ms, fp64_bytes = e.kernel_benchmark(1, block, 10)
     peaks = {}
     try:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
     except Exception:
         pass
-    peak = float(peaks.get("hbm_gbs", 6650.0))
-    # DRAM traffic per launch of this kernel from the committed ncu capture
-    # (profiles/roofline_traffic.json), when it covers this kernel and workload
-    roof_kernel = f"k_pcg_persistent_cg<{block}, double>" if block == 32 else f"k_pcg_persistent<{block}, double>"
+    peak = float(peaks["hbm_gbs"]) if "hbm_gbs" in peaks else FALLBACK_HBM_GBS
+    peak_source = "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback (6.65 TB/s)"
+    roof_kernel = {10: f"k_pcg_flex<{block}, float, true>", 9: f"k_pcg_flex<{block}, float, false>",
+                   1: f"k_pcg_persistent<{block}, double, 1, 1>"}[roof_mode]
     traffic = None
     try:
         rec = json.loads((ROOT / "profiles" / "roofline_traffic.json").read_text()).get(roof_kernel)
-        if rec and rec.get("workload") == args.workload and args.scale == 1.0:
+        if rec and rec.get("workload") == args.workload and args.scale == rec.get("scale", 1.0):
             traffic = float(rec["bytes_per_launch"])
     except Exception:
         pass
-    achieved = spmm_bytes / (spmm_ms / 1000.0) / 1e9
+    achieved = roof_bytes / (roof_ms / 1000.0) / 1e9
     h2d = int(timings["h2d_bytes"])
     e.release()
 
@@ -394,7 +551,7 @@ def main():
     for i in range(max(args.e2e_steps, 1) + 1):
         g = abi.Engine(lib)
         g.prepare(panel, deletion_mode=deletion_mode(panel))
-        g.device_options(args.block, args.precond)
+        g.device_options(block, precond, precision)
         barrier()
         t0 = time.perf_counter()
         if use_shards:
@@ -414,62 +571,53 @@ def main():
         e2e_s = float(t.item())
     e2e_value = world * rhs / e2e_s
 
-    # the other solver forms on the same panel (device-resident, one timed step
-    # each): the plain GPU CMG-PCG form on a bounded probe sample, the learned
-    # flexible PCG and the mixed-precision solve
     forms = {}
     if not args.no_forms and world == 1:
-        forms = time_forms(lib, panel, controls, args, stream, barrier)
+        forms = time_forms(lib, panel, args, stream, barrier, headline)
+
+    parity_blocks = []
+    if rank == 0 and world == 1 and not args.no_parity and reference_plugin_path() is not None:
+        parity_blocks.append(parity(lib, headline, args.tolerance, "plain_1m", 1.0, args.parity_probes))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(panel, min(args.probes, args.cpu_probes), args.tolerance)
+        cpu = cpu_baseline(args, panel)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 storage / f64 reductions" if precision == 1 else "f64",
             "data": "synthetic (seeded generator, fevc_b200/panel.py)",
-            "config": {"workload": f"{args.workload} panel ({panel.info['workers']} workers, "
-                                   f"{panel.info['firms']} firms, {panel.info['periods']} periods), "
-                                   f"{total_probes} probes, {controls} year controls, "
-                                   f"{'observation' if deletion_mode(panel) == 2 else 'match'} deletion",
-                       "probes": total_probes, "rhs_per_step": rhs * world, "tolerance": args.tolerance,
-                       "block_columns": block, "preconditioner": "jacobi" if args.precond == 1 else "auto",
-                       "controls": controls,
-                       "parallelism": (f"probe-sharded x{world}: {args.probes} probes per GPU, "
-                                       f"{total_probes} in the decomposition; NCCL all-reduce of the "
-                                       "leverage accumulators and gather of the draws") if use_shards
-                       else "single GPU",
-                       "l2": "working set per step larger than L2 (126 MB)",
-                       "retained": {"workers": int(timings["vertices"]) and None}},
+            "config": workload_config(args, panel),
+            "form": {"name": headline, "description": form_text, "preconditioner": precond, "precision": precision,
+                     "block_columns": block},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": 144, "seconds_per_step": round(e2e_s, 4)},
             "time_to_decomposition_s": round(prepare_s + e2e_s, 3), "prepare_s": round(prepare_s, 3),
             "first_solve_s": round(first_solve_s, 3),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "kernel": (f"k_pcg_persistent_cg<{block}, double> (two grid barriers per iteration"
-                                    if two_barrier else
-                                    f"k_pcg_persistent<{block}, double> (three grid barriers per iteration")
-                                   + ", 20 iterations per launch, L2 flushed before each)",
-                         "bytes_per_launch": spmm_bytes,
-                         "ms_per_launch": round(spmm_ms, 5), "peak_source": "measured (MEASURED_PEAKS.json)",
-                         "three_barrier_ms_per_launch": round(three_ms, 5),
-                         "two_barrier_ms_per_launch": round(two_ms, 5)},
+                         "kernel": roof_kernel + " (20 iterations per launch, L2 flushed before each)",
+                         "bytes_per_launch": roof_bytes, "ms_per_launch": round(roof_ms, 5),
+                         "peak_source": peak_source,
+                         "fp64_jacobi_kernel": {"ms_per_launch": round(fp64_ms, 5),
+                                                "achieved": round(fp64_bytes / (fp64_ms / 1000.0) / 1e9, 1)}},
             "gpu_launches": int(timings["kernel_launches"]) * args.steps,
             "solver": {k: timings[k] for k in ("block_iterations", "column_iterations", "rhs_columns",
-                                               "vertices", "edges", "kept_workers", "levels")},
+                                               "vertices", "edges", "kept_workers", "levels", "fallbacks")},
             "phase_ms": {k: round(timings[k], 3) for k in ("fit_ms", "leverage_ms", "target_ms", "total_ms")},
             "components": {k: [round(float(x), 10) for x in v] for k, v in result.items()},
             "clocks": clocks.summary(),
         }
-        del line["config"]["retained"]
         if forms:
             line["forms"] = forms
-            plain = forms["plain_gpu_cmg_pcg"].get("value")
+            plain = forms.get("plain_gpu_cmg_pcg", {}).get("value")
             line["speedup_vs_plain_gpu_cmg_pcg"] = round(value / plain, 2) if plain else None
+            f64 = forms.get("jacobi_fp64", {}).get("value")
+            line["speedup_vs_fp64_jacobi"] = round(value / f64, 3) if f64 else None
+        if parity_blocks:
+            line["parity"] = parity_blocks
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line))

@@ -794,8 +794,11 @@ class Engine:
 
     # ---- B200 extensions
     def device_options(self, block_columns: int = 0, preconditioner: int = 0, precision: int = 0) -> None:
-        """Device solve options: block width, preconditioner (1 Jacobi, 2 CMG)
-        and precision (1: single-precision inner PCG, double refinement)."""
+        """Device solve options: block width, preconditioner (1 Jacobi, 2 CMG,
+        3 the learned per-vertex degree-1 stage, 4 the same stage with uniform
+        weights) and precision (1: single-precision residual, direction and
+        products with a double solution, double reductions and residual
+        replacement)."""
         o = FevcbSolveOptionsV2(FevcbSolveOptionsV1(C.sizeof(FevcbSolveOptionsV2), block_columns, preconditioner, 1),
                                 precision, 0)
         self.check(self.lib.fevcb_engine_solve_options_v1(self.generation, C.byref(o)))

@@ -19,6 +19,7 @@ from __future__ import annotations
 import ctypes as C
 import hashlib
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -315,15 +316,76 @@ def write_cmg_cases(lib, meta: dict) -> None:
     (HERE / "cmg_cases.json").write_text(json.dumps({"meta": meta, "panels": cmg}, indent=1))
 
 
+# Components of the plugin at reduced sizes of the configured benchmark
+# panels (fevc_b200/panel.py named panels): the same seeded generator, the
+# same probes and seed, supplied tolerance 1e-10.  The plugin's production
+# route (CMG_FULL_V2) is tried first; when its refinement ladder refuses the
+# panel the record falls back to the plugin's diagonal PCG route and says so.
+SIZED_PANELS = {
+    "plain_1m@0.1": dict(name="plain_1m", scale=0.1, probes=24),
+    "learned_10m@0.02": dict(name="learned_10m", scale=0.02, probes=48),
+}
+
+
+def sized_record(lib, name: str, scale: float, probes: int) -> dict:
+    from fevc_b200.panel import named_panel
+
+    panel = named_panel(name, scale)
+    deletion = 2 if panel.info.get("deletion") == "observation" else 1
+    last = None
+    for route in ("cmg_full_v2", "diagonal"):
+        e = abi.Engine(lib)
+        e.prepare(panel, deletion_mode=deletion)
+        q = e.default_request_v5(deletion)
+        v1 = q.v4.v3.v2.v1
+        v1.probes = probes
+        v1.pcg_tolerance = 1e-10
+        v1.maximum_iterations = 20000
+        q.v4.v3.v2.algorithm = 2
+        if deletion == 2:
+            q.v4.v3.engine = 2
+        q.tolerance_supplied = 1
+        q.threads = os.cpu_count() or 1
+        if route == "cmg_full_v2":
+            q.full_cmg_v2 = 1
+        else:
+            v1.solver_route = 2
+        try:
+            e.solve_v5(q, controls_count=len(panel.controls))
+        except abi.EngineError as err:
+            last = f"{route}: {err}"
+            e.release()
+            continue
+        res = e.result()
+        e.release()
+        return {"panel": name, "scale": scale, "rows": panel.rows, "panel_sha256": panel_digest(panel),
+                "deletion_mode": deletion, "controls": len(panel.controls), "seed": int(v1.seed), "probes": probes,
+                "pcg_tolerance": 1e-10, "route": route, "refused_route": last,
+                **{k: list(v) for k, v in res.items()}}
+    raise RuntimeError(f"the plugin refused {name}@{scale}: {last}")
+
+
+def write_sized_cases(lib, meta: dict) -> None:
+    cases = {}
+    for key, spec in SIZED_PANELS.items():
+        cases[key] = sized_record(lib, **spec)
+        print(key, cases[key]["route"], cases[key]["corrected"])
+    (HERE / "sized_cases.json").write_text(json.dumps({"meta": meta, "cases": cases}, indent=1))
+
+
 def main() -> None:
     """All fixtures; with the argument ``cmg`` only cmg_cases.json, with
-    ``receipts`` only receipt_cases.json."""
+    ``receipts`` only receipt_cases.json, with ``sized`` only sized_cases.json."""
     if not PLUGIN.exists():
         raise SystemExit(f"reference plugin not found at {PLUGIN}")
     lib = abi.load(PLUGIN, bind_extensions=False)
     if sys.argv[1:] == ["cmg"]:
         write_cmg_cases(lib, {"generator": "tests/golden/make_golden.py cmg", "reference_plugin_version":
                               lib.vckss_rust_backend_version().decode()})
+        return
+    if sys.argv[1:] == ["sized"]:
+        write_sized_cases(lib, {"generator": "tests/golden/make_golden.py sized", "reference_plugin_version":
+                                lib.vckss_rust_backend_version().decode()})
         return
     if sys.argv[1:] == ["receipts"]:
         write_receipt_cases(lib, {"generator": "tests/golden/make_golden.py receipts",
