@@ -696,7 +696,7 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the two-barrier persistent PCG kernel cannot be resident on an SM");
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_persistent_cg<64, float>, PERSIST_THREADS, 0));
     if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the single-precision persistent PCG kernel cannot be resident on an SM");
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_flex<64, float, true>, PERSIST_THREADS, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_flex<64, float, true>, FLEX_THREADS, 0));
     if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the mixed-precision persistent PCG kernel cannot be resident on an SM");
     e->coop_blocks = sms;  // one 1024-thread block per SM
   }
@@ -1149,7 +1149,7 @@ void launch_flex_v(DeviceEngine& e, BlockWork& w, Launch L, int iterations, bool
   a.fresh = fresh ? 1 : 0;
   a.replace2 = FLEX_REPLACE * FLEX_REPLACE;
   void* args[] = {&a};
-  CK(cudaLaunchCooperativeKernel((const void*)k_pcg_flex<K, V, POLY>, dim3(e.coop_blocks), dim3(PERSIST_THREADS),
+  CK(cudaLaunchCooperativeKernel((const void*)k_pcg_flex<K, V, POLY>, dim3(e.coop_blocks), dim3(FLEX_THREADS),
                                  args, 0, L.s));
 }
 

@@ -52,6 +52,10 @@
 namespace fevcb {
 
 constexpr double FLEX_REPLACE = 1e-3;  // replacement when r.r drops by FLEX_REPLACE^2
+// One block of FLEX_THREADS per SM: 512 threads leave 128 registers a thread,
+// which the batched row passes use to keep four rows' loads in flight per
+// warp (at 1024 threads the 64-register cap spills them).
+constexpr int FLEX_THREADS = 512;
 // Uniform weights of the untrained polynomial stage: a = 1.05, s = 1 (the
 // first-order Neumann series, damped by 5 % so that a > s^2 holds strictly).
 constexpr double FLEX_NEUMANN_A = 1.05;
@@ -188,12 +192,40 @@ __device__ __forceinline__ void seg_pass(const Arg& a, const VA* __restrict__ va
   }
 }
 
-// Row pass over the segment sums: f(row, sum) for every row, where sum[c] is
-// the row's segment products of column c0 + c.  Rows with many segments are
-// summed by a whole block (its warps take strided shares, warp 0 finishes);
-// the others by one warp each.  f runs on the lanes of one warp per row.
-template <int K, typename VO, typename Arg, typename F>
-__device__ __forceinline__ void row_pass(const Arg& a, Sh<K>& sh, const VO* seg, F f) {
+// Load a row's CPT columns in the storage type (no conversion; batched
+// rows hold their values in half the registers of doubles for V = float).
+template <int K, typename V>
+__device__ __forceinline__ void load_raw(const V* y, uint32_t j, int c0, V (&out)[Cols<K>::CPT]) {
+  constexpr int CPT = Cols<K>::CPT;
+  const V* src = y + size_t(j) * K + c0;
+  if constexpr (CPT == 2 && sizeof(V) == 8) {
+    double2 v = *reinterpret_cast<const double2*>(src);
+    out[0] = v.x;
+    out[1] = v.y;
+  } else if constexpr (CPT == 2 && sizeof(V) == 4) {
+    float2 v = *reinterpret_cast<const float2*>(src);
+    out[0] = v.x;
+    out[1] = v.y;
+  } else {
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) out[c] = src[c];
+  }
+}
+
+// Rows per batch of the row and vertex passes: the loads of ROW_BATCH rows
+// are issued before any of them is computed and stored, so a warp keeps
+// that many rows' reads in flight instead of one.
+constexpr int ROW_BATCH = 4;
+
+// Row pass over the segment sums: for every row, load(u, row) issues the
+// row's vector loads into batch slot u and run(u, row, sum) computes and
+// stores it, where sum[c] is the row's segment products of column c0 + c.
+// Rows with more than HEAVY_SEGMENTS segments are summed by a whole block
+// (its warps take strided shares, warp 0 finishes).  The others go in row
+// order: a warp takes 32 consecutive rows, reads their segment bounds with
+// one coalesced load and handles them ROW_BATCH at a time.
+template <int K, typename VO, int B = ROW_BATCH, typename Arg, typename LoadF, typename RunF>
+__device__ __forceinline__ void row_pass(const Arg& a, Sh<K>& sh, const VO* seg, LoadF load, RunF run) {
   constexpr int CPT = Cols<K>::CPT;
   const int lane = threadIdx.x & 31, wib = int(threadIdx.x >> 5), nwb = int(blockDim.x >> 5);
   const int c0 = lane * CPT;
@@ -221,34 +253,65 @@ __device__ __forceinline__ void row_pass(const Arg& a, Sh<K>& sh, const VO* seg,
         for (int u = 0; u < nwb; ++u) t += hs[u][c0 + c];
         sum[c] = t;
       }
-      f(row, sum);
+      load(0, row);
+      run(0, row, sum);
     }
     __syncthreads();
   }
   const size_t warp = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const size_t nw = (size_t(gridDim.x) * blockDim.x) >> 5;
-  for (size_t li = warp; li < a.nlight; li += nw) {
-    const uint32_t row = a.light_rows[li];
-    const uint32_t s0 = a.row_first[row], s1 = a.row_first[row + 1];
-    double sum[CPT];
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) sum[c] = 0.0;
-    for (uint32_t sg = s0; sg < s1; ++sg) {
-      double sv[CPT];
-      load_cols<K, VO>(seg, sg, c0, sv);
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) sum[c] += sv[c];
+  for (size_t base = warp * 32; base < a.n; base += nw * 32) {
+    uint32_t f0 = 0, f1 = 0;
+    if (base + lane < a.n) {
+      f0 = __ldg(a.row_first + base + lane);
+      f1 = __ldg(a.row_first + base + lane + 1);
     }
-    f(row, sum);
+    const int cnt = int(a.n - base < 32 ? a.n - base : 32);
+    for (int k = 0; k < cnt; k += B) {
+      uint32_t sb[B], se[B];
+      bool ok[B];
+      double sum[B][CPT];
+#pragma unroll
+      for (int u = 0; u < B; ++u) {
+        sb[u] = __shfl_sync(0xffffffffu, f0, (k + u) & 31);
+        se[u] = __shfl_sync(0xffffffffu, f1, (k + u) & 31);
+        ok[u] = k + u < cnt && se[u] - sb[u] <= HEAVY_SEGMENTS;
+      }
+#pragma unroll
+      for (int u = 0; u < B; ++u) {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) sum[u][c] = 0.0;
+        if (ok[u]) {
+          load(u, uint32_t(base + k + u));
+          for (uint32_t sg = sb[u]; sg < se[u]; ++sg) {
+            double sv[CPT];
+            load_cols<K, VO>(seg, sg, c0, sv);
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) sum[u][c] += sv[c];
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < B; ++u)
+        if (ok[u]) run(u, uint32_t(base + k + u), sum[u]);
+    }
   }
 }
 
-// Plain row pass (no segment sums): f(row) for every row, one warp per row.
-template <int K, typename F>
-__device__ __forceinline__ void vertex_pass(uint32_t n, F f) {
+// Plain row pass (no segment sums): load(u, row) then run(u, row) for every
+// row, ROW_BATCH consecutive rows per warp step with their loads first.
+template <int K, int B = ROW_BATCH, typename LoadF, typename RunF>
+__device__ __forceinline__ void vertex_pass(uint32_t n, LoadF load, RunF run) {
   const size_t warp = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const size_t nw = (size_t(gridDim.x) * blockDim.x) >> 5;
-  for (size_t row = warp; row < n; row += nw) f(uint32_t(row));
+  for (size_t base = warp * B; base < n; base += nw * B) {
+#pragma unroll
+    for (int u = 0; u < B; ++u)
+      if (base + u < n) load(u, uint32_t(base + u));
+#pragma unroll
+    for (int u = 0; u < B; ++u)
+      if (base + u < n) run(u, uint32_t(base + u));
+  }
 }
 
 template <int K, typename V>
@@ -265,66 +328,82 @@ __device__ __forceinline__ void store_cols(V* y, uint32_t j, int c0, const doubl
   }
 }
 
+// x += xi, xi = 0 for every row
+template <int K, typename V>
+__device__ void fold(const FlexPcg<K, V>& a) {
+  constexpr int CPT = Cols<K>::CPT, U = 1;
+  const int c0 = (threadIdx.x & 31) * CPT;
+  double xv[U][CPT];
+  V iv[U][CPT];
+  vertex_pass<K, 1>(
+      a.n,
+      [&](int u, uint32_t row) {
+        load_cols<K, double>(a.x, row, c0, xv[u]);
+        load_raw<K, V>(a.xi, row, c0, iv[u]);
+      },
+      [&](int u, uint32_t row) {
+        double zero[CPT];
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          xv[u][c] += double(iv[u][c]);
+          zero[c] = 0.0;
+        }
+        store_cols<K, double>(a.x, row, c0, xv[u]);
+        store_cols<K, V>(a.xi, row, c0, zero);
+      });
+}
+
 // Residual replacement: x += xi, xi = 0 (unless fresh), then r = (b - mean)
 // - L x in FP64, stored as V; sh.fin = (r.r, r.z) of the true residual
 // (r.z with the Jacobi z of the stored r; zero for the polynomial form).
 template <int K, typename V, bool POLY>
 __device__ void replace(const FlexPcg<K, V>& a, Sh<K>& sh, bool fresh, int& red,
                         cooperative_groups::grid_group& grid) {
-  constexpr int CPT = Cols<K>::CPT;
+  constexpr int CPT = Cols<K>::CPT, U = 1;
   const int c0 = (threadIdx.x & 31) * CPT;
+  double xv[U][CPT], bv[U][CPT];
   if (!fresh) {
-    vertex_pass<K>(a.n, [&](uint32_t row) {
-      double xv[CPT], iv[CPT];
-      load_cols<K, double>(a.x, row, c0, xv);
-      load_cols<K, V>(a.xi, row, c0, iv);
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) {
-        xv[c] += iv[c];
-        iv[c] = 0.0;
-      }
-      store_cols<K, double>(a.x, row, c0, xv);
-      store_cols<K, V>(a.xi, row, c0, iv);
-    });
+    fold<K, V>(a);
     grid.sync();
     double none[CPT];
     seg_pass<K, double, double, double, false>(a, a.val64, a.x, a.seg, (const double*)nullptr, none);
     grid.sync();
-  } else {
-    vertex_pass<K>(a.n, [&](uint32_t row) {
-      double zero[CPT];
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) zero[c] = 0.0;
-      store_cols<K, double>(a.x, row, c0, zero);
-      store_cols<K, V>(a.xi, row, c0, zero);
-    });
   }
   double v[2][CPT];
 #pragma unroll
   for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
-  auto fin = [&](uint32_t row, const double (&sum)[CPT]) {
-    double bv[CPT], xv[CPT], rv[CPT];
-    load_cols<K, double>(a.b, row, c0, bv);
+  auto load = [&](int u, uint32_t row) {
+    load_cols<K, double>(a.b, row, c0, bv[u]);
+    if (!fresh) load_cols<K, double>(a.x, row, c0, xv[u]);
+  };
+  auto run = [&](int u, uint32_t row, const double (&sum)[CPT]) {
     const double d = a.diag64[row];
     const double di = POLY ? 0.0 : double(a.dinv[row]);
-    if (!fresh) load_cols<K, double>(a.x, row, c0, xv);
+    double rv[CPT], zero[CPT];
 #pragma unroll
     for (int c = 0; c < CPT; ++c) {
-      double lx = fresh ? 0.0 : d * xv[c] - sum[c];
-      double r = (bv[c] - a.s.mean[c0 + c]) - lx;
+      const double lx = fresh ? 0.0 : d * xv[u][c] - sum[c];
+      const double r = (bv[u][c] - a.s.mean[c0 + c]) - lx;
       rv[c] = double(V(r));
       v[0][c] += r * r;
       v[1][c] += rv[c] * (di * rv[c]);
+      zero[c] = 0.0;
     }
     store_cols<K, V>(a.r, row, c0, rv);
+    if (fresh) {
+      store_cols<K, double>(a.x, row, c0, zero);
+      store_cols<K, V>(a.xi, row, c0, zero);
+    }
   };
   if (fresh) {
-    double zero[CPT];
+    vertex_pass<K, 1>(a.n, load, [&](int u, uint32_t row) {
+      double zero[CPT];
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) zero[c] = 0.0;
-    vertex_pass<K>(a.n, [&](uint32_t row) { fin(row, zero); });
+      for (int c = 0; c < CPT; ++c) zero[c] = 0.0;
+      run(u, row, zero);
+    });
   } else {
-    row_pass<K, double>(a, sh, a.seg, fin);
+    row_pass<K, double, 1>(a, sh, a.seg, load, run);
   }
   reduce<K, 2>(a, sh, v, red, grid);
 }
@@ -332,7 +411,7 @@ __device__ void replace(const FlexPcg<K, V>& a, Sh<K>& sh, bool fresh, int& red,
 // z = wa r + ws (A (ws r)) for the stored r; sh.fin[0..K) = r.z
 template <int K, typename V>
 __device__ void precondition(const FlexPcg<K, V>& a, Sh<K>& sh, int& red, cooperative_groups::grid_group& grid) {
-  constexpr int CPT = Cols<K>::CPT;
+  constexpr int CPT = Cols<K>::CPT, U = ROW_BATCH;
   const int c0 = (threadIdx.x & 31) * CPT;
   V* segv = reinterpret_cast<V*>(a.seg);
   double none[CPT];
@@ -341,28 +420,61 @@ __device__ void precondition(const FlexPcg<K, V>& a, Sh<K>& sh, int& red, cooper
   double v[1][CPT];
 #pragma unroll
   for (int c = 0; c < CPT; ++c) v[0][c] = 0.0;
-  row_pass<K, V>(a, sh, segv, [&](uint32_t row, const double (&sum)[CPT]) {
-    double rv[CPT], zv[CPT];
-    load_cols<K, V>(a.r, row, c0, rv);
-    const double wa = double(a.wa[row]), ws = double(a.ws[row]);
+  V rv[U][CPT], wa[U], ws[U];
+  row_pass<K, V>(
+      a, sh, segv,
+      [&](int u, uint32_t row) {
+        load_raw<K, V>(a.r, row, c0, rv[u]);
+        wa[u] = a.wa[row];
+        ws[u] = a.ws[row];
+      },
+      [&](int u, uint32_t row, const double (&sum)[CPT]) {
+        double zv[CPT];
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-      zv[c] = double(V(wa * rv[c] + ws * sum[c]));
-      v[0][c] += rv[c] * zv[c];
-    }
-    store_cols<K, V>(a.z, row, c0, zv);
-  });
+        for (int c = 0; c < CPT; ++c) {
+          zv[c] = double(V(double(wa[u]) * double(rv[u][c]) + double(ws[u]) * sum[c]));
+          v[0][c] += double(rv[u][c]) * zv[c];
+        }
+        store_cols<K, V>(a.z, row, c0, zv);
+      });
   reduce<K, 1>(a, sh, v, red, grid);
+}
+
+// p = z + beta p (beta = 0 at the start); the Jacobi form takes z = dinv r
+template <int K, typename V, bool POLY>
+__device__ void direction(const FlexPcg<K, V>& a, const double* beta) {
+  constexpr int CPT = Cols<K>::CPT, U = ROW_BATCH;
+  const int c0 = (threadIdx.x & 31) * CPT;
+  V zv[U][CPT], pv[U][CPT], di[U];
+  vertex_pass<K>(
+      a.n,
+      [&](int u, uint32_t row) {
+        load_raw<K, V>(a.p, row, c0, pv[u]);
+        if constexpr (POLY) {
+          load_raw<K, V>(a.z, row, c0, zv[u]);
+          di[u] = V(1);
+        } else {
+          load_raw<K, V>(a.r, row, c0, zv[u]);
+          di[u] = a.dinv[row];
+        }
+      },
+      [&](int u, uint32_t row) {
+        double po[CPT];
+#pragma unroll
+        for (int c = 0; c < CPT; ++c)
+          po[c] = double(di[u]) * double(zv[u][c]) + (beta ? beta[c0 + c] * double(pv[u][c]) : 0.0);
+        store_cols<K, V>(a.p, row, c0, po);
+      });
 }
 
 }  // namespace flex
 
 template <int K, typename V, bool POLY>
-__global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_flex(FlexPcg<K, V> a) {
+__global__ void __launch_bounds__(FLEX_THREADS, 1) k_pcg_flex(FlexPcg<K, V> a) {
   namespace cg = cooperative_groups;
   static_assert(Cols<K>::TPR == 32, "the flexible kernel holds one row per warp");
   cg::grid_group grid = cg::this_grid();
-  constexpr int CPT = Cols<K>::CPT;
+  constexpr int CPT = Cols<K>::CPT, U = flex::ROW_BATCH;
   __shared__ flex::Sh<K> sh;
   for (int j = threadIdx.x; j < K; j += blockDim.x) {
     sh.tol2[j] = a.s.tol2[j];
@@ -388,18 +500,7 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_flex(FlexPcg<K, V> a
     for (int j = threadIdx.x; j < K; j += blockDim.x) sh.rz[j] = sh.fin[j];
     __syncthreads();
   }
-  flex::vertex_pass<K>(a.n, [&](uint32_t row) {
-    double zv[CPT];
-    if constexpr (POLY) {
-      load_cols<K, V>(a.z, row, c0, zv);
-    } else {
-      load_cols<K, V>(a.r, row, c0, zv);
-      const double di = double(a.dinv[row]);
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) zv[c] *= di;
-    }
-    flex::store_cols<K, V>(a.p, row, c0, zv);
-  });
+  flex::direction<K, V, POLY>(a, nullptr);
   grid.sync();
 
   int it = 0;
@@ -434,24 +535,31 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_flex(FlexPcg<K, V> a
     // ---- B: q = d p - sum(seg); xi += alpha p; r -= alpha q
 #pragma unroll
     for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
-    flex::row_pass<K, V>(a, sh, reinterpret_cast<const V*>(a.seg), [&](uint32_t row, const double (&sum)[CPT]) {
-      double pv[CPT], xv[CPT], rv[CPT];
-      load_cols<K, V>(a.p, row, c0, pv);
-      load_cols<K, V>(a.xi, row, c0, xv);
-      load_cols<K, V>(a.r, row, c0, rv);
-      const double d = double(a.diag[row]);
-      const double di = POLY ? 0.0 : double(a.dinv[row]);
+    {
+      V pv[U][CPT], xv[U][CPT], rv[U][CPT], d[U], di[U];
+      flex::row_pass<K, V>(
+          a, sh, reinterpret_cast<const V*>(a.seg),
+          [&](int u, uint32_t row) {
+            flex::load_raw<K, V>(a.p, row, c0, pv[u]);
+            flex::load_raw<K, V>(a.xi, row, c0, xv[u]);
+            flex::load_raw<K, V>(a.r, row, c0, rv[u]);
+            d[u] = a.diag[row];
+            di[u] = POLY ? V(0) : a.dinv[row];
+          },
+          [&](int u, uint32_t row, const double (&sum)[CPT]) {
+            double xo[CPT], ro[CPT];
 #pragma unroll
-      for (int c = 0; c < CPT; ++c) {
-        const double al = sh.alpha[c0 + c];
-        xv[c] += al * pv[c];
-        rv[c] = double(V(rv[c] - al * (d * pv[c] - sum[c])));
-        v[0][c] += rv[c] * rv[c];
-        v[1][c] += rv[c] * (di * rv[c]);
-      }
-      flex::store_cols<K, V>(a.xi, row, c0, xv);
-      flex::store_cols<K, V>(a.r, row, c0, rv);
-    });
+            for (int c = 0; c < CPT; ++c) {
+              const double al = sh.alpha[c0 + c], pc = double(pv[u][c]);
+              xo[c] = double(xv[u][c]) + al * pc;
+              ro[c] = double(V(double(rv[u][c]) - al * (double(d[u]) * pc - sum[c])));
+              v[0][c] += ro[c] * ro[c];
+              v[1][c] += ro[c] * (double(di[u]) * ro[c]);
+            }
+            flex::store_cols<K, V>(a.xi, row, c0, xo);
+            flex::store_cols<K, V>(a.r, row, c0, ro);
+          });
+    }
     flex::reduce<K, 2>(a, sh, v, red, grid);
 
     // ---- replacement decision (identical in every block)
@@ -500,36 +608,11 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 1) k_pcg_flex(FlexPcg<K, V> a
     }
     __syncthreads();
     // ---- C: p = z + beta p
-    flex::vertex_pass<K>(a.n, [&](uint32_t row) {
-      double zv[CPT], pv[CPT];
-      load_cols<K, V>(a.p, row, c0, pv);
-      if constexpr (POLY) {
-        load_cols<K, V>(a.z, row, c0, zv);
-      } else {
-        load_cols<K, V>(a.r, row, c0, zv);
-        const double di = double(a.dinv[row]);
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) zv[c] *= di;
-      }
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) pv[c] = zv[c] + sh.beta[c0 + c] * pv[c];
-      flex::store_cols<K, V>(a.p, row, c0, pv);
-    });
+    flex::direction<K, V, POLY>(a, sh.beta);
     grid.sync();
   }
   // fold the last increment into x (columns stopped by the iteration limit)
-  flex::vertex_pass<K>(a.n, [&](uint32_t row) {
-    double xv[CPT], iv[CPT];
-    load_cols<K, double>(a.x, row, c0, xv);
-    load_cols<K, V>(a.xi, row, c0, iv);
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-      xv[c] += iv[c];
-      iv[c] = 0.0;
-    }
-    flex::store_cols<K, double>(a.x, row, c0, xv);
-    flex::store_cols<K, V>(a.xi, row, c0, iv);
-  });
+  flex::fold<K, V>(a);
   if (blockIdx.x == 0) {
     for (int j = threadIdx.x; j < K; j += blockDim.x) {
       a.s.rz[j] = sh.rz[j];
