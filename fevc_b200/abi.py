@@ -538,6 +538,7 @@ SIGNATURES = {
     "fevcb_cmg_aggregate_v1": (i32, [u32, C.POINTER(u32), C.POINTER(u32), C.POINTER(f64), f64, C.POINTER(u32),
                                      C.POINTER(u32)]),
     "fevcb_counter_atoms_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64, C.POINTER(i64)]),
+    "fevcb_engine_exact_limit_v1": (i32, [u64, u64]),
     "fevcb_counter_atoms_noalloc_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64,
                                              C.POINTER(i64)]),
 }
@@ -772,6 +773,20 @@ class Engine:
             req.v4.v3.v2.v1.deletion_mode = 2
             req.v4.v3.deletion_unit_source = 3
         return req
+
+    def exact_request_v5(self, limit: int = 2000) -> SolveRequestV5:
+        """A V5 request for the exact estimator (algorithm EXACT, no RNG
+        contract, automatic engine and route, identified-dimension limit)."""
+        req = self.default_request_v5(1)
+        req.v4.v3.v2.algorithm = 1
+        req.v4.v3.v2.v1.rng_contract = 0
+        req.v4.v3.v2.exact_estimator_limit = limit
+        return req
+
+    def exact_ceiling(self, ceiling: int) -> None:
+        """Raise this generation's exact-estimator dimension ceiling above the
+        request limit (fevcb_engine_exact_limit_v1)."""
+        self.check(self.lib.fevcb_engine_exact_limit_v1(self.generation, ceiling))
 
     def solve_v5(self, req: SolveRequestV5, controls_count: int = 0) -> None:
         req.v4.v3.request_signature = capability_signature_v3(req.v4, controls_count)

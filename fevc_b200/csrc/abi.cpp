@@ -100,6 +100,9 @@ struct Prepared {
   bool checksum_ready = false;
   uint32_t solve_version = 0;                // request version of the last solve: 1, 4, 5 or 8
   VckssEngineSolveRequestV4 last_request{};  // the last V4+ request (capability and batch fields)
+  // ceiling on the identified dimension of an exact solve above the
+  // reference's 2,000 (fevcb_engine_exact_limit_v1); 0: the request's limit
+  uint64_t exact_ceiling = 0;
 };
 
 struct Registry {
@@ -246,14 +249,15 @@ void prepare_common(const PrepareArgs& a, uint64_t* out, uint32_t cap) {
   std::memcpy(out, &r.generation, 8);
 }
 
-SolveOptions options_from_v1(const VckssEngineSolveRequestV1& q, bool observation_allowed = false) {
+SolveOptions options_from_v1(const VckssEngineSolveRequestV1& q, bool observation_allowed = false,
+                             bool exact = false) {
   require_abi(q.abi_version);
   if (q.deletion_mode != VCKSS_DELETION_MATCH &&
       !(observation_allowed && q.deletion_mode == VCKSS_DELETION_OBSERVATION))
     fail(UNSUPPORTED_FEATURE, "jla_validate", "the compressed JLA engine supports match deletion only");
-  if (q.rng_contract != VCKSS_RNG_COUNTER_V1)
+  if (!exact && q.rng_contract != VCKSS_RNG_COUNTER_V1)
     fail(UNSUPPORTED_FEATURE, "jla_validate", "the JLA engine supports VCKSS-COUNTER-V1 only");
-  if (q.probes < 2) fail(INVALID_INPUT, "jla_validate", "JLA probe count must be at least two");
+  if (!exact && q.probes < 2) fail(INVALID_INPUT, "jla_validate", "JLA probe count must be at least two");
   if (q.leverage_batch_width == 0 || q.target_batch_width == 0)
     fail(INVALID_INPUT, "jla_validate", "leverage and target batch widths must be positive");
   if (!(q.rank_tolerance >= 1e-14 && q.rank_tolerance < 0.1))
@@ -445,11 +449,41 @@ SolveOptions options_from_v4(const VckssEngineSolveRequestV4& q) {
   VckssEngineSolveRequestV1 v1 = q.v3.v2.v1;
   if (v1.leverage_batch_width == 0) v1.leverage_batch_width = 8;
   if (v1.target_batch_width == 0) v1.target_batch_width = 8;
-  if (q.v3.v2.algorithm == VCKSS_ALGORITHM_EXACT)
-    fail(UNSUPPORTED_FEATURE, "engine_solve", "the exact estimator is not provided by the device engine");
   if (q.v3.v2.nuisance_mode == VCKSS_NUISANCE_FIXED_OFFSET)
     fail(UNSUPPORTED_FEATURE, "engine_solve", "fixed-offset nuisance is not provided by the device engine");
+  if (q.v3.v2.algorithm == VCKSS_ALGORITHM_EXACT) {
+    // the reference's exact-estimator option gates
+    // (vckss-core/src/exact_estimator.rs:76-125)
+    if (q.v3.v2.exact_estimator_limit < 2 || q.v3.v2.exact_estimator_limit > 2000)
+      fail(INVALID_INPUT, "exact_estimator", "exact limit must lie in [2, 2000]");
+    if (q.v3.v2.blocksize_limit == 0 || q.v3.v2.blocksize_limit > 1000000)
+      fail(INVALID_INPUT, "exact_estimator", "block-size limit must lie in [1, 1000000]");
+    SolveOptions o = options_from_v1(v1, false, true);
+    o.algorithm = 1;
+    o.exact_limit = q.v3.v2.exact_estimator_limit;
+    o.blocksize_limit = q.v3.v2.blocksize_limit;
+    return o;
+  }
   return options_from_v1(v1, true);
+}
+
+// The exact path covers match deletion without controls: every deletion
+// block is one match whose rows share a design row.  The identified
+// dimension W + F - 1 must fit the request's exact limit (or the ceiling a
+// caller raised with fevcb_engine_exact_limit_v1), as in the reference's
+// estimator (exact_estimator.rs:511-526); so must each block's rows.
+void exact_gate(const Prepared& p, const SolveOptions& o) {
+  if (p.controls != 0 || p.plan.generic || p.deletion_mode != VCKSS_DELETION_MATCH)
+    fail(UNSUPPORTED_FEATURE, "exact_estimator",
+         "the device exact estimator covers match deletion without controls");
+  const uint64_t parameters = uint64_t(p.problem.workers) + p.problem.firms - 1;
+  const uint64_t limit = std::max<uint64_t>(o.exact_limit, p.exact_ceiling);
+  if (parameters > limit)
+    fail(RESOURCE_LIMIT, "exact_estimator", "identified coefficient dimension exceeds exact_limit()");
+  const auto& di = p.problem.deletion_index.ptr;
+  for (size_t g = 0; g + 1 < di.size(); ++g)
+    if (di[g + 1] - di[g] > o.blocksize_limit)
+      fail(RESOURCE_LIMIT, "exact_estimator", "a deletion block exceeds blocksize_limit()");
 }
 
 void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr, bool generic_allowed,
@@ -466,6 +500,7 @@ void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr, bool generi
   if (v4) reconcile_capability(p, *v4);
   if (o.deletion_mode != p.deletion_mode)
     fail(INVALID_INPUT, "engine_solve", "solve deletion mode differs from the prepared graph mode");
+  if (o.algorithm == 1) exact_gate(p, o);
   r.state = State::Solving;
   try {
     intr.check("jla_full_fit");
@@ -1491,6 +1526,15 @@ int32_t fevcb_engine_solve_options_v1(uint64_t generation, const FevcbSolveOptio
     if (p.device && o.preconditioner != p.device_options.preconditioner) p.device.reset();
     p.device_options = o;
     p.precision = o2.precision;
+  });
+}
+
+int32_t fevcb_engine_exact_limit_v1(uint64_t generation, uint64_t ceiling) {
+  return status([&] {
+    if (ceiling > 1000000) fail(INVALID_INPUT, "engine_ffi", "exact ceiling must lie in [0, 1000000]");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_exact_limit");
+    p.exact_ceiling = ceiling;
   });
 }
 

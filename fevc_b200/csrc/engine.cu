@@ -262,6 +262,7 @@ struct DeviceEngine {
   std::unique_ptr<LearnedPreconditioner> learned;
   int preconditioner = 1;
   Segments lap_seg, firm_seg;
+  PieceLevels firm_pieces;  // hierarchical finish of the hub firms' segment sums
   int coop_blocks = 0;
   std::vector<RhsReceipt> control_receipts;  // the control projections' solves (generic estimator)
   // generic (controlled) estimator: row-level data and the control geometry
@@ -302,6 +303,7 @@ DeviceStats device_stats(const DeviceEngine& e) { return e.stats; }
 struct BlockWork {
   int K;
   DBuf<double> bW, bF, b, x, r, z, p, q, alpha, cell_val, unit_atoms, dir, tot, seg_buf, fseg_out;
+  DBuf<double> piece2, piece3;  // hub firms' level-2 and level-3 partial sums
   DBuf<double> st;  // 8 * K doubles of per-column state
   DBuf<int> ist;    // 2 * K + 2 ints
   PcgState s;
@@ -429,6 +431,13 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     upload(e->firm_ptr, fptr, s, h2d);
     upload(e->firm_cells, p.firm_index.items, s, h2d);
     build_segments(fptr, e->firm_seg, s, h2d);
+    {
+      // segments per firm follow from the cell counts (SEG cells a segment)
+      std::vector<uint32_t> sfirst(fptr.size(), 0);
+      for (size_t f = 0; f + 1 < fptr.size(); ++f)
+        sfirst[f + 1] = sfirst[f] + (fptr[f + 1] - fptr[f] + SEG - 1) / SEG;
+      build_piece_levels(sfirst, e->firm_pieces, s, h2d);
+    }
     {
       std::vector<double> fd(p.firms, 0.0);
       for (size_t c = 0; c < p.cells; ++c) fd[p.cell_firm[c]] += p.cell_weight[c];
@@ -822,6 +831,8 @@ BlockWork& get_work(DeviceEngine& e) {
   w->tot.alloc(size_t(QMAX + 4) * K);
   w->seg_buf.alloc(size_t(e.lap_seg.count) * K);
   w->fseg_out.alloc(size_t(e.firm_seg.count) * K);
+  w->piece2.alloc(size_t(std::max<uint32_t>(e.firm_pieces.n2, 1)) * K);
+  w->piece3.alloc(size_t(std::max<uint32_t>(e.firm_pieces.n3, 1)) * K);
   w->st.alloc(8 * K);
   w->ist.alloc(2 * K + 4);
   double* st = w->st.p;
@@ -1300,8 +1311,15 @@ void firm_gather(DeviceEngine& e, BlockWork& w, Launch L, const double* coef, co
   k_seg_firm<K, OP><<<L.grid, THREADS, 0, L.s>>>(e.firm_seg.count, e.firm_seg.begin.p, e.firm_seg.end.p,
                                                   e.firm_cells.p, e.cell_worker.p, coef, src, total, inv_total,
                                                   w.fseg_out.p);
-  k_seg_firm_finish<K, MODE><<<L.grid, THREADS, 0, L.s>>>(e.F, e.kept, e.firm_seg.row_first.p, w.fseg_out.p, bF, bW,
-                                                          e.kept_worker.p, e.firm_diag.p, psi, out, partial);
+  const PieceLevels& pl = e.firm_pieces;
+  if (pl.rows) {
+    k_piece_sum<K><<<L.grid, THREADS, 0, L.s>>>(pl.n2, pl.begin2.p, pl.end2.p, w.fseg_out.p, w.piece2.p);
+    k_piece_sum<K><<<L.grid, THREADS, 0, L.s>>>(pl.n3, pl.begin3.p, pl.end3.p, w.piece2.p, w.piece3.p);
+  }
+  k_seg_firm_finish<K, MODE><<<L.grid, THREADS, 0, L.s>>>(e.F, e.kept, e.firm_seg.row_first.p, w.fseg_out.p,
+                                                          pl.rows ? pl.slot.p : nullptr, pl.top_first.p,
+                                                          w.piece3.p, bF, bW, e.kept_worker.p, e.firm_diag.p, psi,
+                                                          out, partial);
   CK_LAUNCH();
 }
 
@@ -1713,6 +1731,175 @@ void shard_upload(DeviceEngine& e, const double* in) {
   CK(cudaStreamSynchronize(e.stream));
 }
 
+// ---------------------------------------------------------------------------
+// Exact leverages (algorithm EXACT; match deletion without controls).  The
+// reference's dense estimator (vckss-core/src/exact_estimator.rs:1448-1600
+// match_block_action, 1698-1786 TargetMoments) deletes each match block: all
+// rows of a block share one design row x_c = (e_w, e_f), so with
+// z_c = S^+ x_c (S = X'WX) and h_c = x_c' z_c the block's leverage is n_g h_c
+// (n_g its frequency mass), its residual maker 1 - n_g h_c, and its share of
+// the correction is (sum of centred outcomes)(sum of residuals) / (1 - n_g h_c)
+// times the target bilinear forms B_c of z_c with itself:
+//   worker = sum_w s_w a_w^2 - (sum_w s_w a_w)^2,  firm likewise over firms,
+//   covariance = sum_c m_c a_{w(c)} p_{f(c)} - (sum s a)(sum s p),
+// s and m the worker, firm and cell shares of the target mass.  Here z_c
+// comes from direct blocked solves with one-hot right-hand sides, h_c and
+// B_c from reductions over the solution columns, and the block weights from
+// the leverage-adjustment kernel fed with exact moments (projection n_g h_c,
+// residual 1 - n_g h_c, no Monte Carlo bias or variance).
+
+template <int K>
+__global__ void k_exact_rhs(uint32_t first, int ncols, const uint32_t* __restrict__ cw,
+                            const uint32_t* __restrict__ cf, double* __restrict__ bW, double* __restrict__ bF) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < ncols; j += gridDim.x * blockDim.x) {
+    const uint32_t c = first + uint32_t(j);
+    bW[size_t(cw[c]) * K + j] = 1.0;
+    bF[size_t(cf[c]) * K + j] = 1.0;
+  }
+}
+
+// partial[blk][5][K] = (sum_w s_w a, sum_w s_w a^2, sum_f s_f p, sum_f s_f p^2,
+// sum_c m_c a_{w(c)} p_{f(c)}) for the block's solution columns
+template <int K>
+__global__ void k_exact_sums(uint32_t W, uint32_t F, uint32_t C, const double* __restrict__ wshare,
+                             const double* __restrict__ fshare, const double* __restrict__ cmass,
+                             const uint32_t* __restrict__ cw, const uint32_t* __restrict__ cf,
+                             const double* __restrict__ alpha, const double* __restrict__ psi,
+                             double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  double v[5][CPT];
+#pragma unroll
+  for (int m = 0; m < 5; ++m)
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) v[m][c] = 0.0;
+  const size_t rows = std::max(std::max(W, F), C);
+  const size_t N = rows * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < N; base += stride) {
+    const size_t t = base + threadIdx.x;
+    if (t < N) {
+      const size_t i = t / TPR;
+      const int c0 = int(t % TPR) * CPT;
+      if (i < W) {
+        const double sh = wshare[i];
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          const double a = alpha[i * K + c0 + c];
+          v[0][c] += sh * a;
+          v[1][c] += sh * a * a;
+        }
+      }
+      if (i < F) {
+        const double sh = fshare[i];
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          const double b = psi[i * K + c0 + c];
+          v[2][c] += sh * b;
+          v[3][c] += sh * b * b;
+        }
+      }
+      if (i < C) {
+        const double m = cmass[i];
+        const size_t wi = size_t(cw[i]) * K, fi = size_t(cf[i]) * K;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) v[4][c] += m * alpha[wi + c0 + c] * psi[fi + c0 + c];
+      }
+    }
+  }
+  block_reduce_cols<K, 5>(v, partial);
+}
+
+// h_c = a_{w(c)} + p_{f(c)} of column j (cell first + j); every unit g of the
+// cell gets the exact moments (n_g h_c, 1 - n_g h_c, 0, 0, 0)
+template <int K>
+__global__ void k_exact_moments(uint32_t first, int ncols, const uint32_t* __restrict__ cw,
+                                const uint32_t* __restrict__ cf, const double* __restrict__ alpha,
+                                const double* __restrict__ psi, const uint32_t* __restrict__ unit_ptr,
+                                const double* __restrict__ unit_count_f, double* __restrict__ moments) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < ncols; j += gridDim.x * blockDim.x) {
+    const uint32_t c = first + uint32_t(j);
+    const double h = alpha[size_t(cw[c]) * K + j] + psi[size_t(cf[c]) * K + j];
+    for (uint32_t g = unit_ptr[c]; g < unit_ptr[c + 1]; ++g) {
+      const double n = unit_count_f[g];
+      double* m = moments + size_t(g) * 5;
+      m[0] = n * h;
+      m[1] = 1.0 - n * h;
+      m[2] = m[3] = m[4] = 0.0;
+    }
+  }
+}
+
+__global__ void k_scale_copy(size_t n, const double* __restrict__ src, double s, double* __restrict__ dst) {
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    dst[i] = src[i] * s;
+}
+
+template <int K>
+void run_exact(DeviceEngine& e, const Compressed& p, const SolveOptions& o, SolveResult& res) {
+  BlockWork& w = get_work<K>(e);
+  Launch L{grid_blocks(), e.stream};
+  DBuf<double> cmass(e.C), wshare(e.W), fshare(e.F);
+  k_scale_copy<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_target.p, 1.0 / p.target_total, cmass.p);
+  k_gather<1><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, cmass.p, wshare.p);
+  k_gather<1><<<L.grid, THREADS, 0, L.s>>>(e.F, e.firm_ptr.p, e.firm_cells.p, cmass.p, fshare.p);
+  res.timings.kernel_launches += 3;
+  SolveOptions oe = o;
+  oe.pcg_tolerance = std::min(o.pcg_tolerance, 1e-10);
+  std::vector<double> B(size_t(e.C) * 3), sums(5 * K);
+  for (uint32_t first = 0; first < e.C; first += K) {
+    const int ncols = int(std::min<uint32_t>(K, e.C - first));
+    CK(cudaMemsetAsync(w.bW.p, 0, w.bW.bytes(), L.s));
+    CK(cudaMemsetAsync(w.bF.p, 0, w.bF.bytes(), L.s));
+    k_exact_rhs<K><<<1, 128, 0, L.s>>>(first, ncols, e.cell_worker.p, e.cell_firm.p, w.bW.p, w.bF.p);
+    CK_LAUNCH();
+    solve_block<K>(e, w, ncols, oe, res.timings);
+    k_exact_sums<K><<<L.grid, THREADS, 0, L.s>>>(e.W, e.F, e.C, wshare.p, fshare.p, cmass.p, e.cell_worker.p,
+                                                 e.cell_firm.p, w.alpha.p, w.x.p, e.partial.p);
+    finish(e.partial.p, L.grid, 5 * K, w.tot.p, L.s);
+    k_exact_moments<K><<<1, 128, 0, L.s>>>(first, ncols, e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p,
+                                           e.unit_ptr.p, e.unit_count_f.p, e.moments.p);
+    CK(cudaMemcpyAsync(sums.data(), w.tot.p, 5 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    res.timings.kernel_launches += 4;
+    for (int j = 0; j < ncols; ++j) {
+      const double aw = sums[j], aw2 = sums[K + j], pf = sums[2 * K + j], pf2 = sums[3 * K + j],
+                   x = sums[4 * K + j];
+      double* b = &B[size_t(first + j) * 3];
+      b[0] = aw2 - aw * aw;
+      b[1] = pf2 - pf * pf;
+      b[2] = x - aw * pf;
+    }
+  }
+  // block weights from the exact moments (one "probe": no Monte Carlo terms)
+  AdjustParams prm{e.C, 1.0, o.block_tolerance, o.rank_tolerance, outcome_mean(p, o.centering)};
+  unsigned long long init[2] = {~0ull, 0ull};
+  CK(cudaMemcpyAsync(e.error.p, init, sizeof(init), cudaMemcpyHostToDevice, L.s));
+  k_adjust<<<L.grid, THREADS, 0, L.s>>>(prm, e.unit_ptr.p, e.moments.p, e.unit_outcome.p, e.unit_count_f.p,
+                                        e.fitted.p, e.unit_out.p, e.omega.p, e.error.p, e.error.p + 1);
+  unsigned long long got[2] = {0, 0};
+  std::vector<double> omega(e.C);
+  CK(cudaMemcpyAsync(got, e.error.p, sizeof(got), cudaMemcpyDeviceToHost, L.s));
+  CK(cudaMemcpyAsync(omega.data(), e.omega.p, e.C * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+  CK(cudaStreamSynchronize(L.s));
+  res.timings.kernel_launches += 1;
+  std::memcpy(&res.max_leverage, &got[1], sizeof(double));
+  if (got[0] != ~0ull) {
+    const uint32_t code = uint32_t(got[0] & 0xff);
+    const uint32_t g = e.unit_group[got[0] >> 8];
+    fail(int32_t(code), "exact_estimator",
+         std::string(code == NONESTIMABLE_DELETION ? "a match residual block is singular"
+                                                   : "a match block correction failed") +
+             " at unit " + std::to_string(g));
+  }
+  StableSum s[3];
+  for (uint32_t c = 0; c < e.C; ++c)
+    for (int k = 0; k < 3; ++k) s[k].add(omega[c] * B[size_t(c) * 3 + k]);
+  const double cw = s[0].finish(), cf = s[1].finish(), cc = s[2].finish();
+  res.correction = finish_accounting(cw, cf, cc, cw + cf + 2.0 * cc, "exact_estimator");
+  res.corrected = Components{res.plugin.worker - cw, res.plugin.firm - cf, res.plugin.covariance - cc,
+                             res.plugin.total - res.correction.total};
+  res.mcse = Components{0.0, 0.0, 0.0, 0.0};
+}
+
 template <int K>
 void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o, SolveResult& res,
              bool detail) {
@@ -1749,6 +1936,19 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
     res.timings.kernel_launches += 6;
   }
   auto t1 = now();
+  if (o.algorithm == 1) {
+    run_exact<K>(e, p, o, res);
+    for (auto& r : res.receipts) {
+      res.max_reduced_residual = std::max(res.max_reduced_residual, r.reduced_residual);
+      res.max_complete_residual = std::max(res.max_complete_residual, r.complete_residual);
+    }
+    if (detail) device_unit_detail(e, res);
+    auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+    res.timings.fit_ms = ms(t0, t1);
+    res.timings.leverage_ms = ms(t1, now());
+    res.timings.total_ms = ms(t0, now());
+    return;
+  }
   // ---- leverage
   if (o.shard_phase != 2) {
     CK(cudaMemsetAsync(e.moments.p, 0, e.moments.bytes(), L.s));

@@ -31,6 +31,8 @@ struct SolveOptions {
   uint32_t deletion_mode = 1;  // 1 match, 2 observation (must equal the prepared mode)
   uint32_t solver_route = 0;   // the request's route: 2 diagonal PCG, 3 CMG PCG, 0 automatic
   int precision = 0;           // 0 double, 1 single-precision inner solves with double refinement
+  int algorithm = 2;           // 1 exact leverages (match deletion, no controls), 2 JLA
+  uint64_t exact_limit = 500, blocksize_limit = 5000;  // exact-estimator gates
   // Probe sharding across devices: the leverage and target probes handled
   // here are [probe_begin, probe_end) of the request's probes (end 0: all).
   // Phase 1 runs the fit and the leverage probes and returns the leverage

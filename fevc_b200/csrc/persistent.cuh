@@ -42,6 +42,76 @@ struct Segments {
 
 constexpr uint32_t HEAVY_SEGMENTS = 8;
 
+// Two further levels of partial sums for the rows of a segmented CSR with
+// more than PIECE segments (the hub firms of the firm->cell lists): level 2
+// sums each such row's segments PIECE at a time, level 3 sums its level-2
+// pieces PIECE at a time, so the row's finish reads at most a few dozen
+// level-3 pieces instead of walking thousands of segments on one warp.
+// Every sum runs in a fixed order: the results are deterministic.
+constexpr uint32_t PIECE = 32;
+
+struct PieceLevels {
+  uint32_t n2 = 0, n3 = 0, rows = 0;
+  DBuf<uint32_t> begin2, end2;  // level-2 pieces: ranges of segments
+  DBuf<uint32_t> begin3, end3;  // level-3 pieces: ranges of level-2 pieces
+  DBuf<uint32_t> top_first;     // per heavy row: its level-3 pieces [top_first[h], top_first[h+1])
+  DBuf<int32_t> slot;           // per row: its heavy-row index, or -1
+};
+
+inline void build_piece_levels(const std::vector<uint32_t>& row_first, PieceLevels& pl, cudaStream_t s,
+                               uint64_t& h2d) {
+  const size_t rows = row_first.size() - 1;
+  std::vector<uint32_t> b2, e2, b3, e3, top(1, 0);
+  std::vector<int32_t> slot(rows, -1);
+  for (size_t r = 0; r < rows; ++r) {
+    const uint32_t s0 = row_first[r], s1 = row_first[r + 1];
+    if (s1 - s0 <= PIECE) continue;
+    slot[r] = int32_t(top.size() - 1);
+    const uint32_t first2 = uint32_t(b2.size());
+    for (uint32_t x = s0; x < s1; x += PIECE) {
+      b2.push_back(x);
+      e2.push_back(std::min(s1, x + PIECE));
+    }
+    const uint32_t last2 = uint32_t(b2.size());
+    for (uint32_t x = first2; x < last2; x += PIECE) {
+      b3.push_back(x);
+      e3.push_back(std::min(last2, x + PIECE));
+    }
+    top.push_back(uint32_t(b3.size()));
+  }
+  pl.rows = uint32_t(top.size() - 1);
+  pl.n2 = uint32_t(b2.size());
+  pl.n3 = uint32_t(b3.size());
+  upload(pl.begin2, b2, s, h2d);
+  upload(pl.end2, e2, s, h2d);
+  upload(pl.begin3, b3, s, h2d);
+  upload(pl.end3, e3, s, h2d);
+  upload(pl.top_first, top, s, h2d);
+  upload(pl.slot, slot, s, h2d);
+}
+
+// dst[p] = sum of src[i] for i in [begin[p], end[p]) (K columns), in order;
+// the loads of a piece are independent, so a lane keeps them all in flight.
+template <int K>
+__global__ void k_piece_sum(uint32_t npieces, const uint32_t* __restrict__ begin, const uint32_t* __restrict__ end,
+                            const double* __restrict__ src, double* __restrict__ dst) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  const size_t N = size_t(npieces) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < N; t += stride) {
+    const size_t pc = t / TPR;
+    const int c0 = int(t % TPR) * CPT;
+    double acc[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
+    const uint32_t b = begin[pc], e = end[pc];
+    for (uint32_t i = b; i < e; ++i)
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) acc[c] += src[size_t(i) * K + c0 + c];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) dst[pc * K + c0 + c] = acc[c];
+  }
+}
+
 constexpr uint32_t SEG_FIRST = 0x80000000u;
 
 // Cut every CSR row into segments of at most SEG items.
@@ -812,9 +882,13 @@ __global__ void k_seg_firm(uint32_t nseg, const uint32_t* __restrict__ seg_begin
 //   mode 1: hybrid RHS  b[f] = bF[f] - sum; kept rows b[F+k] = -bW[kept_worker[k]];
 //           partial (sum b, sum b^2)
 //   mode 2: residual    r = bF - d_f psi_f - sum;    partial (|r|^2, |bF|^2)
+// Rows with a heavy-row slot (more than PIECE segments) sum their level-3
+// pieces (top_first / top) instead of their segments.
 template <int K, int MODE>
 __global__ void k_seg_firm_finish(uint32_t F, uint32_t kept, const uint32_t* __restrict__ row_first,
-                                  const double* __restrict__ seg_out, const double* __restrict__ bF,
+                                  const double* __restrict__ seg_out, const int32_t* __restrict__ slot,
+                                  const uint32_t* __restrict__ top_first, const double* __restrict__ top,
+                                  const double* __restrict__ bF,
                                   const double* __restrict__ bW, const uint32_t* __restrict__ kept_worker,
                                   const double* __restrict__ firm_diag, const double* __restrict__ psi,
                                   double* __restrict__ out, double* __restrict__ partial) {
@@ -833,9 +907,16 @@ __global__ void k_seg_firm_finish(uint32_t F, uint32_t kept, const uint32_t* __r
       if (f < F) {
 #pragma unroll
         for (int c = 0; c < CPT; ++c) acc[c] = 0.0;
-        for (uint32_t sg = row_first[f]; sg < row_first[f + 1]; ++sg)
+        const int32_t h = slot ? slot[f] : -1;
+        if (h < 0) {
+          for (uint32_t sg = row_first[f]; sg < row_first[f + 1]; ++sg)
 #pragma unroll
-          for (int c = 0; c < CPT; ++c) acc[c] += seg_out[size_t(sg) * K + c0 + c];
+            for (int c = 0; c < CPT; ++c) acc[c] += seg_out[size_t(sg) * K + c0 + c];
+        } else {
+          for (uint32_t q = top_first[h]; q < top_first[h + 1]; ++q)
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) acc[c] += top[size_t(q) * K + c0 + c];
+        }
         if (MODE == 1) {
 #pragma unroll
           for (int c = 0; c < CPT; ++c) acc[c] = bF[f * K + c0 + c] - acc[c];

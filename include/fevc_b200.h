@@ -842,6 +842,14 @@ int32_t fevcb_cmg_aggregate_v1(uint32_t vertices, const uint32_t *row_ptr, const
 int32_t fevcb_engine_kernel_benchmark_v1(uint64_t generation, uint32_t kernel, uint32_t block_columns,
                                          uint32_t launches, double *ms_per_launch, double *bytes_per_launch);
 
+/* Ceiling on the identified dimension (W + F - 1) of an exact-estimator solve
+ * of this generation (no counterpart in the reference, whose dense estimator
+ * refuses limits above 2,000: vckss-core/src/exact_estimator.rs:104-108).
+ * The device computes exact leverages by blocked solves instead of a dense
+ * inverse, so panels such as 20,000 workers x 1,000 firms (about 8,000
+ * parameters) fit.  0 restores the request's own limit; at most 1,000,000. */
+int32_t fevcb_engine_exact_limit_v1(uint64_t generation, uint64_t ceiling);
+
 /* Counter-V1 atoms computed on the device: out[e*columns + j] for probe first_probe + j. */
 int32_t fevcb_counter_atoms_v1(uint64_t seed, uint64_t domain_tag, uint64_t first_probe, uint32_t columns,
                                const uint64_t *entity, const uint64_t *trials, uint64_t count, int64_t *out);

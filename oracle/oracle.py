@@ -143,3 +143,77 @@ def shard(problem: OracleProblem, *, phase: int, probe_begin: int, probe_end: in
         raise RuntimeError(f"oracle failed [{code}]: {res.error.decode()}")
     draws = arrays["target_draws"].reshape(P, 4)[probe_begin:probe_end].copy()
     return {"io": io, "draws": draws, "plugin": np.array(res.plugin[:])}
+
+
+def exact(problem: OracleProblem, *, centering: int = 0, block_tolerance: float = 1e-10) -> dict:
+    """Exact leverages for match deletion without controls (dense numpy).
+
+    Restates the reference's dense estimator (rust/crates/vckss-core/src/
+    exact_estimator.rs:560-1000 full fit and match loop, 1448-1600
+    match_block_action, 1698-1786 TargetMoments::bilinear) for blocks whose
+    rows share one design row x_c = (e_w, e_f): with S = X'WX grounded at the
+    last firm, z_c = S^-1 x_c and h_c = x_c' z_c, a deletion unit g of n_g
+    frequency mass in cell c contributes (sum of centred outcomes)(sum of
+    residuals) / (1 - n_g h_c) times the target bilinear forms of z_c.
+    """
+    W, F, Cn, G = int(problem.workers), int(problem.firms), int(problem.cells), int(problem.units)
+    arr = lambda p, n: np.ctypeslib.as_array(p, shape=(n,)).copy()  # noqa: E731
+    cw = arr(problem.cell_worker, Cn).astype(np.int64)
+    cf = arr(problem.cell_firm, Cn).astype(np.int64)
+    wgt = arr(problem.cell_weight, Cn)
+    ysum = arr(problem.cell_outcome_sum, Cn)
+    tsum = arr(problem.cell_target_sum, Cn)
+    ucell = arr(problem.unit_cell, G).astype(np.int64)
+    ucount = arr(problem.unit_count, G).astype(np.float64)
+    uys = arr(problem.unit_outcome_sum, G)
+    T = float(problem.target_total)
+    dim = W + F - 1  # the last firm is grounded (the quotient's zero-sum firm block)
+    S = np.zeros((W + F, W + F))
+    np.add.at(S, (cw, cw), wgt)
+    np.add.at(S, (W + cf, W + cf), wgt)
+    np.add.at(S, (cw, W + cf), wgt)
+    np.add.at(S, (W + cf, cw), wgt)
+    Sinv = np.linalg.inv(S[:dim, :dim])
+    # S^+ in the grounded coordinates, padded with the grounded firm's zero
+    # row and column (x_c of a cell in the last firm has no coordinate there)
+    full = np.zeros((W + F, W + F))
+    full[:dim, :dim] = Sinv
+    # the fit: beta = S^+ X'Wy, effects centred by the target weights below
+    rhs = np.bincount(cw, ysum, W + F) + np.bincount(W + cf, ysum, W + F)
+    beta = full @ rhs
+    alpha_fit, psi_fit = beta[:W], beta[W:]
+    fitted = alpha_fit[cw] + psi_fit[cf]
+    ws = np.bincount(cw, tsum, W) / T
+    fs = np.bincount(cf, tsum, F) / T
+    m = tsum / T
+    am, pm = ws @ alpha_fit, fs @ psi_fit
+    plugin_w = ws @ (alpha_fit - am) ** 2
+    plugin_f = fs @ (psi_fit - pm) ** 2
+    plugin_c = m @ ((alpha_fit[cw] - am) * (psi_fit[cf] - pm))
+    plugin = np.array([plugin_w, plugin_f, plugin_c, plugin_w + plugin_f + 2 * plugin_c])
+    # exact leverages and target forms of z_c, in column chunks
+    B = np.zeros((Cn, 3))
+    h = np.zeros(Cn)
+    for lo in range(0, Cn, 2048):
+        idx = np.arange(lo, min(Cn, lo + 2048))
+        Z = full[:, cw[idx]] + full[:, W + cf[idx]]  # (W+F) x chunk: columns z_c
+        Za, Zp = Z[:W], Z[W:]
+        h[idx] = Za[cw[idx], np.arange(idx.size)] + Zp[cf[idx], np.arange(idx.size)]
+        a1, p1 = ws @ Za, fs @ Zp
+        B[idx, 0] = ws @ Za ** 2 - a1 ** 2
+        B[idx, 1] = fs @ Zp ** 2 - p1 ** 2
+        B[idx, 2] = m @ (Za[cw] * Zp[cf]) - a1 * p1
+    ybar = 0.0
+    if centering == 1:
+        rows, phys = int(problem.rows), float(problem.physical_total)
+        y = arr(problem.row_outcome, rows)
+        freq = arr(problem.row_frequency, rows).astype(np.float64)
+        ybar = y[0] + np.sum((y - y[0]) * (freq / phys))
+    maker = 1.0 - ucount * h[ucell]
+    if np.any(maker <= block_tolerance):
+        raise RuntimeError("a match residual block is singular")
+    omega = np.bincount(ucell, (uys - ybar * ucount) * (uys - ucount * fitted[ucell]) / maker, Cn)
+    corr = omega @ B
+    correction = np.array([corr[0], corr[1], corr[2], corr[0] + corr[1] + 2 * corr[2]])
+    return {"plugin": plugin, "correction": correction, "corrected": plugin - correction,
+            "mcse": np.zeros(4), "leverage": ucount * h[ucell]}

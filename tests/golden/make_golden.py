@@ -373,15 +373,65 @@ def write_sized_cases(lib, meta: dict) -> None:
     (HERE / "sized_cases.json").write_text(json.dumps({"meta": meta, "cases": cases}, indent=1))
 
 
+# The plugin's exact estimator (algorithm EXACT through its solve_v2; the
+# V4+ solves need the EXACT capability profile) on panels small enough for
+# its single-threaded dense path (identified dimension <= 2000).
+EXACT_PANELS = {
+    "kat12": dict(build=lambda: kat12()),
+    "exact_400": dict(build=lambda: generate_panel(400, 60, 5, move_p=0.3, seed=3)),
+    "exact_weighted_500": dict(build=lambda: _weighted_small(500, 50, 13)),
+}
+
+
+def _weighted_small(workers: int, firms: int, seed: int) -> Panel:
+    """Literal frequencies and uneven target weights on a small panel."""
+    p = generate_panel(workers, firms, 5, move_p=0.3, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    p.frequency = rng.integers(1, 4, p.rows).astype(np.float64)
+    p.target_weight = np.round(rng.uniform(0.5, 3.0, p.rows) * 4) / 4 * p.frequency
+    return p
+
+
+def exact_record(lib, panel: Panel, centering: int) -> dict:
+    lib.vckss_rust_engine_solve_v2.restype = C.c_int32
+    lib.vckss_rust_engine_solve_v2.argtypes = [C.c_uint64, C.c_void_p]
+    e = abi.Engine(lib)
+    e.prepare(panel)
+    if centering:
+        e.centering(centering)
+    q = abi.SolveRequestV2()
+    e.check(lib.vckss_rust_engine_default_solve_request_v2(C.byref(q), C.sizeof(q)))
+    q.algorithm = 1
+    q.exact_estimator_limit = 2000
+    e.check(lib.vckss_rust_engine_solve_v2(e.generation, C.byref(q)))
+    res = e.result()
+    e.release()
+    return {"centering": centering, "pcg_tolerance": q.v1.pcg_tolerance, **{k: list(v) for k, v in res.items()}}
+
+
+def write_exact_cases(lib, meta: dict) -> None:
+    cases = {}
+    for name, spec in EXACT_PANELS.items():
+        panel = spec["build"]()
+        cases[name] = {"panel_sha256": panel_digest(panel), "records": [exact_record(lib, panel, c) for c in (0, 1)]}
+        print(name, cases[name]["records"][0]["corrected"])
+    (HERE / "exact_cases.json").write_text(json.dumps({"meta": meta, "cases": cases}, indent=1))
+
+
 def main() -> None:
     """All fixtures; with the argument ``cmg`` only cmg_cases.json, with
-    ``receipts`` only receipt_cases.json, with ``sized`` only sized_cases.json."""
+    ``receipts`` only receipt_cases.json, with ``sized`` only sized_cases.json, with
+    ``exact`` only exact_cases.json."""
     if not PLUGIN.exists():
         raise SystemExit(f"reference plugin not found at {PLUGIN}")
     lib = abi.load(PLUGIN, bind_extensions=False)
     if sys.argv[1:] == ["cmg"]:
         write_cmg_cases(lib, {"generator": "tests/golden/make_golden.py cmg", "reference_plugin_version":
                               lib.vckss_rust_backend_version().decode()})
+        return
+    if sys.argv[1:] == ["exact"]:
+        write_exact_cases(lib, {"generator": "tests/golden/make_golden.py exact", "reference_plugin_version":
+                                lib.vckss_rust_backend_version().decode()})
         return
     if sys.argv[1:] == ["sized"]:
         write_sized_cases(lib, {"generator": "tests/golden/make_golden.py sized", "reference_plugin_version":

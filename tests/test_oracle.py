@@ -1,6 +1,9 @@
 """The oracle against the reference plugin's solved golden cases
 (tests/golden/jla_cases.json): the four components, the correction and the MCSE."""
 
+import json
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -90,3 +93,26 @@ def test_kat_unit_detail(lib, oracle_mod):
     assert np.allclose(out["projection_share"] + out["residual_share"], 1.0, atol=1e-14)
     assert out["projection_share"].shape == (8,) and out["cell_correction_weight"].shape == (4,)
     assert np.all(np.isfinite(out["deleted_mass"]))
+
+
+EXACT = json.loads((Path(__file__).resolve().parent / "golden" / "exact_cases.json").read_text())["cases"]
+
+
+@pytest.mark.parametrize("name", sorted(EXACT))
+@pytest.mark.parametrize("which", [0, 1])
+def test_exact_oracle_matches_the_plugin_exact_estimator(lib, oracle_mod, name, which):
+    """The numpy restatement of the exact estimator against the plugin's own
+    (algorithm EXACT) on the same prepared problem."""
+    case = EXACT[name]
+    rec = case["records"][which]
+    panel = make_golden.EXACT_PANELS[name]["build"]()
+    assert make_golden.panel_digest(panel) == case["panel_sha256"]
+    e = abi.Engine(lib)
+    e.prepare(panel)
+    try:
+        got = oracle_mod.exact(oracle_mod.problem_view(lib, e.generation), centering=rec["centering"])
+    finally:
+        e.release()
+    for key in ("plugin", "correction", "corrected"):
+        want = np.array(rec[key])
+        assert np.max(np.abs(got[key] - want)) <= 1e-9 * max(np.max(np.abs(want)), 1e-12), (key, got[key], want)
