@@ -1146,15 +1146,12 @@ void launch_flex_v(DeviceEngine& e, BlockWork& w, Launch L, int iterations, bool
   a.ord_end = e.lap_seg.ord_end.p;
   a.row_first = e.lap_seg.row_first.p;
   a.heavy_rows = e.lap_seg.heavy_rows.p;
-  a.light_rows = e.lap_seg.light_rows.p;
   a.nheavy = e.lap_seg.nheavy;
-  a.nlight = e.lap_seg.nlight;
   a.seg = w.seg_buf.p;
   a.x = w.x.p;
   a.b = w.b.p;
   a.partial = e.partial.p;
   a.s = w.s;
-  a.rr_ref = w.st.p + 7 * K;
   a.replacements = w.ist.p + 2 * K + 2;
   a.max_iters = iterations;
   a.fresh = fresh ? 1 : 0;
@@ -2440,6 +2437,7 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
         e.preconditioner = saved;
         break;
       }
+
       case 3:
         k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p,
                                                      e.observation ? e.unit_offset.p : nullptr, key,
