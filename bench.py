@@ -507,7 +507,7 @@ def main():
         collectives = sharded.torch_collectives(torch.device("cuda", local))
 
         def step(engine):
-            backend = sharded.DeviceBackend(engine, req, controls)
+            backend = sharded.DeviceBackend(engine, req, controls, device=torch.device("cuda", local))
             return sharded.solve_sharded(backend, total_probes, rank, world, *collectives)
     else:
         def step(engine):

@@ -1745,8 +1745,8 @@ int32_t fevcb_engine_shard_leverage_v1(uint64_t generation, const VckssEngineSol
       fail(INVALID_INPUT, "shard", "accumulator buffer has the wrong length");
     SolveOptions o = shard_options(p, request, begin, end);
     o.shard_phase = 1;
+    o.shard_output = acc;  // host or device memory: copied by unified addressing
     SolveResult res = device_solve(*p.device, p.problem, p.plan, o, false);
-    std::copy(res.shard_accumulators.begin(), res.shard_accumulators.end(), acc);
     {
       SolveTimings& t = p.shard_timings;
       t.kernel_launches += res.timings.kernel_launches;

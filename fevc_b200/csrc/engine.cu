@@ -1700,18 +1700,23 @@ double outcome_mean(const Compressed& p, Centering c) {
 }
 
 // Leverage accumulators of a shard: match units' five moment sums, or the
-// leave-observation-out per-row and per-copy sums.
-void shard_download(DeviceEngine& e, SolveResult& res) {
+// leave-observation-out per-row and per-copy sums.  With o.shard_output set
+// they are copied straight into the caller's buffer, host or device memory
+// alike (unified addressing), so a device buffer never passes through the
+// host; otherwise into res.shard_accumulators.
+void shard_download(DeviceEngine& e, const SolveOptions& o, SolveResult& res) {
+  const size_t count = e.observation ? e.obs_row_acc.n + e.obs_copy_acc.n : size_t(e.G) * 5;
+  double* dst = o.shard_output;
+  if (!dst) {
+    res.shard_accumulators.resize(count);
+    dst = res.shard_accumulators.data();
+  }
   if (e.observation) {
-    res.shard_accumulators.resize(e.obs_row_acc.n + e.obs_copy_acc.n);
-    CK(cudaMemcpyAsync(res.shard_accumulators.data(), e.obs_row_acc.p, e.obs_row_acc.bytes(), cudaMemcpyDeviceToHost,
+    CK(cudaMemcpyAsync(dst, e.obs_row_acc.p, e.obs_row_acc.bytes(), cudaMemcpyDefault, e.stream));
+    CK(cudaMemcpyAsync(dst + e.obs_row_acc.n, e.obs_copy_acc.p, e.obs_copy_acc.bytes(), cudaMemcpyDefault,
                        e.stream));
-    CK(cudaMemcpyAsync(res.shard_accumulators.data() + e.obs_row_acc.n, e.obs_copy_acc.p, e.obs_copy_acc.bytes(),
-                       cudaMemcpyDeviceToHost, e.stream));
   } else {
-    res.shard_accumulators.resize(size_t(e.G) * 5);
-    CK(cudaMemcpyAsync(res.shard_accumulators.data(), e.moments.p, size_t(e.G) * 5 * sizeof(double),
-                       cudaMemcpyDeviceToHost, e.stream));
+    CK(cudaMemcpyAsync(dst, e.moments.p, size_t(e.G) * 5 * sizeof(double), cudaMemcpyDefault, e.stream));
   }
   CK(cudaStreamSynchronize(e.stream));
 }
@@ -1719,11 +1724,11 @@ void shard_download(DeviceEngine& e, SolveResult& res) {
 void shard_upload(DeviceEngine& e, const double* in) {
   if (!in) fail(INVALID_INPUT, "shard", "the summed leverage accumulators are missing");
   if (e.observation) {
-    CK(cudaMemcpyAsync(e.obs_row_acc.p, in, e.obs_row_acc.bytes(), cudaMemcpyHostToDevice, e.stream));
-    CK(cudaMemcpyAsync(e.obs_copy_acc.p, in + e.obs_row_acc.n, e.obs_copy_acc.bytes(), cudaMemcpyHostToDevice,
+    CK(cudaMemcpyAsync(e.obs_row_acc.p, in, e.obs_row_acc.bytes(), cudaMemcpyDefault, e.stream));
+    CK(cudaMemcpyAsync(e.obs_copy_acc.p, in + e.obs_row_acc.n, e.obs_copy_acc.bytes(), cudaMemcpyDefault,
                        e.stream));
   } else {
-    CK(cudaMemcpyAsync(e.moments.p, in, size_t(e.G) * 5 * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+    CK(cudaMemcpyAsync(e.moments.p, in, size_t(e.G) * 5 * sizeof(double), cudaMemcpyDefault, e.stream));
   }
   CK(cudaStreamSynchronize(e.stream));
 }
@@ -1952,7 +1957,7 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
     run_leverage_blocks<K>(e, o, res);
   }
   if (o.shard_phase == 1) {
-    shard_download(e, res);
+    shard_download(e, o, res);
     res.timings.fit_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     return;
   }
@@ -2157,7 +2162,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     run_leverage_blocks<K>(e, o, res);
   }
   if (o.shard_phase == 1) {
-    shard_download(e, res);
+    shard_download(e, o, res);
     res.timings.fit_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     return;
   }

@@ -42,6 +42,7 @@ struct SolveOptions {
   int shard_phase = 0;
   uint32_t probe_begin = 0, probe_end = 0;
   const double* shard_input = nullptr;
+  double* shard_output = nullptr;  // phase 1: the caller's accumulator buffer (host or device)
 };
 
 // One receipt per solved right-hand side (reference `JlaRhsReceipt`,

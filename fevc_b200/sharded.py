@@ -48,7 +48,7 @@ def solve_sharded(backend, probes: int, rank: int, world: int, allreduce_sum, al
     """Run the sharded protocol; allreduce_sum(np.ndarray) -> np.ndarray and
     allgather(np.ndarray) -> list of every rank's array (rank order)."""
     b, e = probe_ranges(probes, world)[rank]
-    acc = backend.leverage(b, e) if e > b else np.zeros(backend.accumulators())
+    acc = backend.leverage(b, e) if e > b else backend.zeros()
     acc = allreduce_sum(acc)
     draws = backend.target(b, e, acc) if e > b else np.zeros((0, 4))
     all_draws = np.concatenate(allgather(draws), axis=0)
@@ -58,10 +58,13 @@ def solve_sharded(backend, probes: int, rank: int, world: int, allreduce_sum, al
 
 
 class DeviceBackend:
-    """The rank's GPU through the library's shard entry points."""
+    """The rank's GPU through the library's shard entry points.  With a torch
+    CUDA ``device`` the leverage accumulators live in a device tensor that the
+    library fills and reads directly, so the all-reduce runs on the device
+    with no host round trip; otherwise they are numpy arrays."""
 
-    def __init__(self, engine: abi.Engine, request, controls: int = 0):
-        self.e, self.req = engine, request
+    def __init__(self, engine: abi.Engine, request, controls: int = 0, device=None):
+        self.e, self.req, self.device = engine, request, device
         self.req.v4.v3.request_signature = abi.capability_signature_v3(request.v4, controls)
         n = C.c_uint64(0)
         engine.check(engine.lib.fevcb_engine_shard_size_v1(engine.generation, C.byref(n)))
@@ -70,17 +73,32 @@ class DeviceBackend:
     def accumulators(self) -> int:
         return self.count
 
-    def leverage(self, b: int, e: int) -> np.ndarray:
-        acc = np.zeros(self.count)
+    def zeros(self):
+        if self.device is None:
+            return np.zeros(self.count)
+        import torch
+
+        return torch.zeros(self.count, dtype=torch.float64, device=self.device)
+
+    def _ptr(self, acc):
+        if self.device is None:
+            return acc.ctypes.data_as(dptr)
+        return C.cast(C.c_void_p(acc.data_ptr()), dptr)
+
+    def leverage(self, b: int, e: int):
+        acc = self.zeros()
         self.e.check(self.e.lib.fevcb_engine_shard_leverage_v1(self.e.generation, C.byref(self.req), b, e,
-                                                              acc.ctypes.data_as(dptr), self.count))
+                                                              self._ptr(acc), self.count))
         return acc
 
-    def target(self, b: int, e: int, acc: np.ndarray) -> np.ndarray:
-        acc = np.ascontiguousarray(acc, dtype=np.float64)
+    def target(self, b: int, e: int, acc) -> np.ndarray:
+        if self.device is None:
+            acc = np.ascontiguousarray(acc, dtype=np.float64)
+        else:
+            acc = acc.contiguous()
         draws = np.zeros((e - b, 4))
         self.e.check(self.e.lib.fevcb_engine_shard_target_v1(self.e.generation, C.byref(self.req), b, e,
-                                                            acc.ctypes.data_as(dptr), self.count,
+                                                            self._ptr(acc), self.count,
                                                             draws.ctypes.data_as(dptr)))
         return draws
 
@@ -97,7 +115,10 @@ def torch_collectives(device=None):
     import torch
     import torch.distributed as dist
 
-    def allreduce_sum(a: np.ndarray) -> np.ndarray:
+    def allreduce_sum(a):
+        if isinstance(a, torch.Tensor):  # a device tensor: reduced in place
+            dist.all_reduce(a, op=dist.ReduceOp.SUM)
+            return a
         t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64))
         if device is not None:
             t = t.to(device)

@@ -779,7 +779,10 @@ int32_t fevcb_engine_cmg_summary_v1(uint64_t generation, uint32_t eliminate_max_
  *      (worker, firm, covariance, total draws);
  *   4. the caller gathers all probes' draws; fevcb_engine_shard_finish_v1
  *      publishes the components as the generation's result (result_v1).
- * The result equals the single-device solve of the same request. */
+ * The result equals the single-device solve of the same request.  The
+ * accumulator buffers of steps 1 and 3 may be host or device memory (copies
+ * use unified addressing), so a device buffer can go straight to a device
+ * all-reduce without passing through the host. */
 int32_t fevcb_engine_shard_size_v1(uint64_t generation, uint64_t *accumulators);
 int32_t fevcb_engine_shard_leverage_v1(uint64_t generation, const VckssEngineSolveRequestV5 *request,
                                        uint32_t probe_begin, uint32_t probe_end, double *accumulators,

@@ -51,3 +51,27 @@ def test_shards_reproduce_the_reference(lib, golden, section, name, panels, dele
     e.release()
     for key in ("plugin", "correction", "corrected", "numerical_mcse"):
         assert rel(res[key], rec[key]) < 1e-8, (key, res[key], rec[key])
+
+
+@pytest.mark.parametrize("section,name,panels,deletion", CASES[::3])
+def test_device_accumulators_reproduce_the_reference(lib, golden, section, name, panels, deletion):
+    """The accumulators in torch CUDA tensors: the library writes and reads
+    them on the device (the path an NCCL all-reduce takes)."""
+    import torch
+
+    rec = golden["jla"][section][name][0]
+    panel = panels[name]["build"]()
+    e = abi.Engine(lib)
+    e.prepare(panel, deletion_mode=deletion)
+    be = sharded.DeviceBackend(e, request(e, rec, deletion), len(panel.controls), device=torch.device("cuda"))
+    ranges = sharded.probe_ranges(rec["probes"], 2)
+    accs = [be.leverage(b, x) for b, x in ranges if x > b]
+    assert all(a.is_cuda for a in accs)
+    acc = accs[0].clone()
+    for a in accs[1:]:
+        acc += a
+    draws = np.concatenate([be.target(b, x, acc) for b, x in ranges if x > b])
+    res = be.finish(draws)
+    e.release()
+    for key in ("plugin", "correction", "corrected", "numerical_mcse"):
+        assert rel(res[key], rec[key]) < 1e-8, (key, res[key], rec[key])

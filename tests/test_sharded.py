@@ -31,6 +31,9 @@ class OracleBackend:
     def accumulators(self):
         return int(self.view.units) * 5
 
+    def zeros(self):
+        return np.zeros(self.accumulators())
+
     def leverage(self, b, e):
         io = np.zeros(self.accumulators())
         return self.o.shard(self.view, phase=1, probe_begin=b, probe_end=e, io=io, **self.kw)["io"]
