@@ -705,7 +705,7 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the two-barrier persistent PCG kernel cannot be resident on an SM");
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_persistent_cg<64, float>, PERSIST_THREADS, 0));
     if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the single-precision persistent PCG kernel cannot be resident on an SM");
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_flex<64, float, true>, FLEX_THREADS, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_flex<64, float, true>, PERSIST_THREADS, 0));
     if (per < 1) fail(RESOURCE_LIMIT, "pcg", "the mixed-precision persistent PCG kernel cannot be resident on an SM");
     e->coop_blocks = sms;  // one 1024-thread block per SM
   }
@@ -1146,18 +1146,21 @@ void launch_flex_v(DeviceEngine& e, BlockWork& w, Launch L, int iterations, bool
   a.ord_end = e.lap_seg.ord_end.p;
   a.row_first = e.lap_seg.row_first.p;
   a.heavy_rows = e.lap_seg.heavy_rows.p;
+  a.light_rows = e.lap_seg.light_rows.p;
   a.nheavy = e.lap_seg.nheavy;
+  a.nlight = e.lap_seg.nlight;
   a.seg = w.seg_buf.p;
   a.x = w.x.p;
   a.b = w.b.p;
   a.partial = e.partial.p;
   a.s = w.s;
+  a.rr_ref = w.st.p + 7 * K;
   a.replacements = w.ist.p + 2 * K + 2;
   a.max_iters = iterations;
   a.fresh = fresh ? 1 : 0;
   a.replace2 = FLEX_REPLACE * FLEX_REPLACE;
   void* args[] = {&a};
-  CK(cudaLaunchCooperativeKernel((const void*)k_pcg_flex<K, V, POLY>, dim3(e.coop_blocks), dim3(FLEX_THREADS),
+  CK(cudaLaunchCooperativeKernel((const void*)k_pcg_flex<K, V, POLY>, dim3(e.coop_blocks), dim3(PERSIST_THREADS),
                                  args, 0, L.s));
 }
 
