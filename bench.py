@@ -68,6 +68,8 @@ FALLBACK_HBM_GBS = 6650.0
 
 # solver forms: (preconditioner, precision, block columns, description)
 FORMS = {
+    "autotuned": (3, 2, 64, "autotuned per generation: the fastest of FP64 Jacobi, FP32 Jacobi and the FP32 "
+                            "learned degree-1 stage, timed on the first leverage block (fevcb_engine_tuning_v1)"),
     "learned_mixed": (3, 1, 64, "learned per-vertex degree-1 stage in the single-kernel PCG, FP32 storage with "
                                 "FP64 reductions and residual replacement, blocks of 64"),
     "polynomial_mixed": (4, 1, 64, "degree-1 stage with uniform weights (the method without the network), "
@@ -482,12 +484,14 @@ def main():
     params = learned.load_params()
     headline = args.form
     if headline == "auto":
-        headline = "learned_mixed" if params is not None else "polynomial_mixed"
-    if FORMS[headline][0] == 3:
-        if params is None:
-            raise SystemExit("the learned form needs fevc_b200/learned_params.f32 (python -m fevc_b200.learned)")
+        headline = "autotuned"
+    if params is not None:
         learned.install(lib, params)
+    elif FORMS[headline][0] == 3 and headline != "autotuned":
+        raise SystemExit("the learned form needs fevc_b200/learned_params.f32 (python -m fevc_b200.learned)")
     precond, precision, block, form_text = FORMS[headline]
+    if headline == "autotuned" and params is None:
+        precond = 4  # the degree-1 stage with uniform weights
 
     e = abi.Engine(lib)
     t0 = time.perf_counter()
@@ -546,7 +550,12 @@ def main():
     # roofline: the headline form's single-kernel PCG, standalone launches
     # with L2 flushed (mode 10: the polynomial stage, 9: Jacobi; both FP32
     # storage); the FP64 Jacobi kernel beside it for comparison
-    roof_mode = 10 if precond in (3, 4) else (9 if precision == 1 else 1)
+    eff_pre, eff_prec = precond, precision
+    if precision == 2:
+        t = e.tuning()
+        c = t["candidates"][t["chosen"]] if t["chosen"] >= 0 else {"precision": 0, "preconditioner": 1}
+        eff_pre, eff_prec = c["preconditioner"], c["precision"]
+    roof_mode = 10 if (eff_prec == 1 and eff_pre in (3, 4)) else (9 if eff_prec == 1 else 1)
     torch.cuda.nvtx.range_push("roofline")  # the roofline kernel's standalone launches
     roof_ms, roof_bytes = e.kernel_benchmark(roof_mode, block, 10)
     torch.cuda.nvtx.range_pop()
@@ -569,6 +578,7 @@ def main():
         pass
     achieved = roof_bytes / (roof_ms / 1000.0) / 1e9
     h2d = int(timings["h2d_bytes"])
+    tuning = e.tuning() if precision == 2 else None
     e.release()
 
     # e2e through the C ABI: solve + result on a fresh generation per step
@@ -614,11 +624,11 @@ def main():
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 storage / f64 reductions" if precision == 1 else "f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 storage / f64 reductions" if eff_prec == 1 else "f64",
             "data": "synthetic (seeded generator, fevc_b200/panel.py)",
             "config": workload_config(args, panel),
             "form": {"name": headline, "description": form_text, "preconditioner": precond, "precision": precision,
-                     "block_columns": block},
+                     "block_columns": block, "tuning": tuning},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": 144, "seconds_per_step": round(e2e_s, 4)},
             "time_to_decomposition_s": round(prepare_s + e2e_s, 3), "prepare_s": round(prepare_s, 3),

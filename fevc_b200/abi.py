@@ -197,6 +197,11 @@ class FevcbSolveOptionsV2(Struct):
     _fields_ = [("v1", FevcbSolveOptionsV1), ("precision", u32), ("reserved", u32)]
 
 
+class FevcbTuningV1(Struct):
+    _fields_ = [("struct_size", u32), ("chosen", C.c_int32), ("candidates", u32), ("precision", u32 * 3),
+                ("preconditioner", u32 * 3), ("reserved", u32), ("milliseconds", f64 * 3)]
+
+
 class FevcbSolveTimingsV1(Struct):
     _fields_ = [("struct_size", u32), ("fallbacks", u32), ("total_ms", f64), ("fit_ms", f64), ("leverage_ms", f64),
                 ("target_ms", f64), ("setup_ms", f64)] + [(n, u64) for n in (
@@ -539,6 +544,7 @@ SIGNATURES = {
                                      C.POINTER(u32)]),
     "fevcb_counter_atoms_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64, C.POINTER(i64)]),
     "fevcb_engine_exact_limit_v1": (i32, [u64, u64]),
+    "fevcb_engine_tuning_v1": (i32, [u64, C.c_void_p, u32]),
     "fevcb_counter_atoms_noalloc_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64,
                                              C.POINTER(i64)]),
 }
@@ -829,6 +835,15 @@ class Engine:
         t = FevcbSolveTimingsV1()
         self.check(self.lib.fevcb_engine_timings_v1(self.generation, C.byref(t), C.sizeof(t)))
         return t.as_dict()
+
+    def tuning(self) -> dict:
+        """The autotuner's candidates and choice (precision option 2)."""
+        t = FevcbTuningV1()
+        self.check(self.lib.fevcb_engine_tuning_v1(self.generation, C.byref(t), C.sizeof(t)))
+        n = t.candidates
+        return {"chosen": t.chosen, "candidates": [
+            {"precision": t.precision[c], "preconditioner": t.preconditioner[c], "ms": t.milliseconds[c]}
+            for c in range(n)]}
 
     def resolve(self) -> None:
         self.check(self.lib.fevcb_engine_resolve_v1(self.generation))

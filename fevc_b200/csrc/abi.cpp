@@ -1519,13 +1519,36 @@ int32_t fevcb_engine_solve_options_v1(uint64_t generation, const FevcbSolveOptio
         o.block_columns != 32 && o.block_columns != 64)
       fail(INVALID_INPUT, "engine_ffi", "block_columns must be 0, 2, 8, 16, 32 or 64");
     if (o.preconditioner > 4) fail(INVALID_INPUT, "engine_ffi", "preconditioner must be 0, 1, 2, 3 or 4");
-    if (o2.precision > 1) fail(INVALID_INPUT, "engine_ffi", "precision must be 0 (double) or 1 (mixed)");
+    if (o2.precision > 2) fail(INVALID_INPUT, "engine_ffi", "precision must be 0 (double), 1 (mixed) or 2 (autotuned)");
     if (o2.reserved != 0) fail(INVALID_INPUT, "engine_ffi", "reserved fields must be zero");
     std::lock_guard<std::mutex> l(reg().mu);
     Prepared& p = reg().require(generation, "engine_solve_options");
     if (p.device && o.preconditioner != p.device_options.preconditioner) p.device.reset();
     p.device_options = o;
     p.precision = o2.precision;
+  });
+}
+
+int32_t fevcb_engine_tuning_v1(uint64_t generation, FevcbTuningV1* out, uint32_t cap) {
+  return status([&] {
+    if (!out || cap < sizeof(FevcbTuningV1)) fail(INVALID_INPUT, "engine_ffi", "tuning output capacity is too small");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_tuning");
+    FevcbTuningV1 t{};
+    t.struct_size = sizeof(FevcbTuningV1);
+    t.chosen = -1;
+    if (p.device) {
+      int prec[3], pre[3], cand = 0;
+      double ms[3];
+      t.chosen = device_tuning(*p.device, prec, pre, ms, &cand);
+      t.candidates = uint32_t(cand);
+      for (int c = 0; c < 3; ++c) {
+        t.precision[c] = uint32_t(prec[c]);
+        t.preconditioner[c] = uint32_t(pre[c]);
+        t.milliseconds[c] = ms[c];
+      }
+    }
+    *out = t;
   });
 }
 

@@ -261,6 +261,12 @@ struct DeviceEngine {
   std::unique_ptr<Multigrid> mg;
   std::unique_ptr<LearnedPreconditioner> learned;
   int preconditioner = 1;
+  // autotuned solver form (precision option 2): -1 untuned, else the index
+  // of the fastest candidate timed on the first leverage block, with every
+  // candidate's milliseconds
+  int tuned = -1, tune_candidates = 0;
+  int tune_precision[3] = {0, 0, 0}, tune_preconditioner[3] = {0, 0, 0};
+  double tune_ms[3] = {0.0, 0.0, 0.0};
   Segments lap_seg, firm_seg;
   PieceLevels firm_pieces;  // hierarchical finish of the hub firms' segment sums
   int coop_blocks = 0;
@@ -298,6 +304,16 @@ struct DeviceEngine {
 };
 
 DeviceStats device_stats(const DeviceEngine& e) { return e.stats; }
+
+int device_tuning(const DeviceEngine& e, int* precision, int* preconditioner, double* ms, int* candidates) {
+  for (int c = 0; c < 3; ++c) {
+    precision[c] = e.tune_precision[c];
+    preconditioner[c] = e.tune_preconditioner[c];
+    ms[c] = e.tune_ms[c];
+  }
+  *candidates = e.tune_candidates;
+  return e.tuned;
+}
 
 // Per block-width workspace and the captured PCG iteration graph.
 struct BlockWork {
@@ -1394,7 +1410,11 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
              "blocked PCG reached the iteration limit " + std::to_string(o.maximum_iterations));
     }
     // the breakdown flag comes back with the extraction results (one host
-    // round trip per pass); nothing below is used before it is checked
+    // round trip per pass); nothing below is used before it is checked.  A
+    // block that hit the iteration limit or a curvature breakdown therefore
+    // still runs its extraction kernels, and their outputs are discarded by
+    // the fail() after the synchronisation: keep those checks ahead of any
+    // use of the extracted values
     CK(cudaMemcpyAsync(e.h_nactive + 1, w.s.breakdown, sizeof(int), cudaMemcpyDeviceToHost, L.s));
 
     // extraction and complete residual
@@ -1468,6 +1488,73 @@ Components finish_accounting(double w, double f, double c, double t, const char*
   return r;
 }
 
+// Leverage right-hand sides of probes [first, first + ncols): Counter-V1
+// atoms per unit summed per cell, then gathered to the workers and firms.
+template <int K>
+void leverage_rhs(DeviceEngine& e, BlockWork& w, Launch L, PhiloxKey key, uint32_t first, int ncols) {
+  k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p,
+                                                   e.observation ? e.unit_offset.p : nullptr, key, TAG_LEVERAGE,
+                                                   first, ncols, e.observation ? nullptr : w.unit_atoms.p,
+                                                   w.cell_val.p);
+  k_gather<K><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, w.cell_val.p, w.bW.p);
+  firm_gather<K, 0, 0>(e, w, L, nullptr, w.cell_val.p, nullptr, 0.0, nullptr, nullptr, nullptr, w.bF.p, nullptr);
+}
+
+// The solver-form autotuner (precision option 2).  On a generation's first
+// solve it builds the right-hand sides of the first K leverage probes and
+// solves them with each candidate form, timed with CUDA events on the
+// engine's stream: FP64 Jacobi (the three-barrier kernel), FP32 Jacobi and
+// the FP32 degree-1 stage (learned weights when the engine was built with
+// preconditioner 3, uniform with 4) in the single-kernel PCG.  Every form
+// meets the same FP64 tolerance, so only time decides; the fastest serves
+// every later block and resolve of the generation.  The timing solves are
+// extra work of the first solve only, and they leave no state behind (the
+// leverage loop rebuilds its right-hand sides).
+template <int K>
+void autotune(DeviceEngine& e, SolveOptions& o) {
+  if (e.tuned < 0) {
+    const int poly = (e.preconditioner == 3 || e.preconditioner == 4) && e.flex_ws.p ? e.preconditioner : 0;
+    int nc = 0;
+    auto add = [&](int precision, int pre) {
+      e.tune_precision[nc] = precision;
+      e.tune_preconditioner[nc] = pre;
+      ++nc;
+    };
+    add(0, 1);
+    if (flex_width<K>()) {
+      add(1, 1);
+      if (poly) add(1, poly);
+    }
+    e.tune_candidates = nc;
+    if (nc == 1 || o.probes < uint32_t(K)) {
+      e.tuned = 0;
+    } else {
+      BlockWork& w = get_work<K>(e);
+      Launch L{grid_blocks(), e.stream};
+      const PhiloxKey key = philox_key(o.seed);
+      int best = 0;
+      for (int c = 0; c < nc; ++c) {
+        leverage_rhs<K>(e, w, L, key, 0, K);
+        SolveOptions oc = o;
+        oc.precision = e.tune_precision[c];
+        e.preconditioner = e.tune_preconditioner[c];
+        SolveTimings scratch;
+        CK(cudaEventRecord(e.ev0, L.s));
+        solve_block<K>(e, w, K, oc, scratch);
+        CK(cudaEventRecord(e.ev1, L.s));
+        CK(cudaEventSynchronize(e.ev1));
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, e.ev0, e.ev1));
+        e.tune_ms[c] = ms;
+        if (e.tune_ms[c] < e.tune_ms[best]) best = c;
+      }
+      e.tuned = best;
+    }
+  }
+  o.precision = e.tune_precision[e.tuned];
+  e.preconditioner = e.tune_preconditioner[e.tuned];
+}
+
 template <int K>
 void run_leverage(DeviceEngine& e, const SolveOptions& o, SolveResult& res, uint64_t tag_first_probe_unused) {
   (void)tag_first_probe_unused;
@@ -1477,12 +1564,7 @@ void run_leverage(DeviceEngine& e, const SolveOptions& o, SolveResult& res, uint
   const uint32_t end = o.probe_end ? o.probe_end : o.probes;
   for (uint32_t first = o.probe_begin; first < end; first += K) {
     int ncols = int(std::min<uint32_t>(K, end - first));
-    k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p,
-                                                     e.observation ? e.unit_offset.p : nullptr, key,
-                                                     TAG_LEVERAGE, first, ncols,
-                                                     e.observation ? nullptr : w.unit_atoms.p, w.cell_val.p);
-    k_gather<K><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, w.cell_val.p, w.bW.p);
-    firm_gather<K, 0, 0>(e, w, L, nullptr, w.cell_val.p, nullptr, 0.0, nullptr, nullptr, nullptr, w.bF.p, nullptr);
+    leverage_rhs<K>(e, w, L, key, first, ncols);
     res.timings.kernel_launches += 4;
     BlockOutcome bo = solve_block<K>(e, w, ncols, o, res.timings);
     if (e.observation)
@@ -1906,8 +1988,10 @@ void run_exact(DeviceEngine& e, const Compressed& p, const SolveOptions& o, Solv
 }
 
 template <int K>
-void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o, SolveResult& res,
+void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o_request,
+             SolveResult& res,
              bool detail) {
+  SolveOptions o = o_request;  // the autotuner fixes o.precision before the leverage phase
   Launch L{grid_blocks(), e.stream};
   auto now = [] { return std::chrono::steady_clock::now(); };
   auto t0 = now();
@@ -1942,6 +2026,7 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
   }
   auto t1 = now();
   if (o.algorithm == 1) {
+    if (o.precision == 2) autotune<K>(e, o);
     run_exact<K>(e, p, o, res);
     for (auto& r : res.receipts) {
       res.max_reduced_residual = std::max(res.max_reduced_residual, r.reduced_residual);
@@ -1955,6 +2040,7 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
     return;
   }
   // ---- leverage
+  if (o.precision == 2) autotune<K>(e, o);
   if (o.shard_phase != 2) {
     CK(cudaMemsetAsync(e.moments.p, 0, e.moments.bytes(), L.s));
     run_leverage_blocks<K>(e, o, res);
@@ -2102,8 +2188,10 @@ void setup_controls(DeviceEngine& e, const SolveOptions& o, SolveTimings& tm) {
 }
 
 template <int K>
-void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o, SolveResult& res,
+void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o_request,
+             SolveResult& res,
                  bool detail) {
+  SolveOptions o = o_request;  // the autotuner fixes o.precision before the leverage phase
   Launch L{grid_blocks(), e.stream};
   auto now = [] { return std::chrono::steady_clock::now(); };
   auto t0 = now();
@@ -2155,6 +2243,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
   auto t1 = now();
   // ---- FE-only leverage probes (reference `match_leverage_moments`,
   // `observation_and_match_leverage_moments`)
+  if (o.precision == 2) autotune<K>(e, o);
   if (o.shard_phase != 2) {
     if (e.observation) {
       CK(cudaMemsetAsync(e.obs_row_acc.p, 0, e.obs_row_acc.bytes(), L.s));

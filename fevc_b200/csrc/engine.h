@@ -30,7 +30,7 @@ struct SolveOptions {
   int preconditioner = 0;     // 0 automatic, 1 Jacobi, 2 aggregation multigrid
   uint32_t deletion_mode = 1;  // 1 match, 2 observation (must equal the prepared mode)
   uint32_t solver_route = 0;   // the request's route: 2 diagonal PCG, 3 CMG PCG, 0 automatic
-  int precision = 0;           // 0 double, 1 single-precision inner solves with double refinement
+  int precision = 0;           // 0 double, 1 FP32 storage with FP64 replacement, 2 autotuned per generation
   int algorithm = 2;           // 1 exact leverages (match deletion, no controls), 2 JLA
   uint64_t exact_limit = 500, blocksize_limit = 5000;  // exact-estimator gates
   // Probe sharding across devices: the leverage and target probes handled
@@ -99,6 +99,8 @@ struct DeviceStats {
 // Upload the prepared problem and build the solver.  Throws Error.
 std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaPlan& plan, int preconditioner);
 DeviceStats device_stats(const DeviceEngine& e);
+// The autotuner's candidates (precision, preconditioner, ms) and its choice (-1: not tuned).
+int device_tuning(const DeviceEngine& e, int* precision, int* preconditioner, double* ms, int* candidates);
 SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o,
                          bool want_unit_detail);
 

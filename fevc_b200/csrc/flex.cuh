@@ -11,7 +11,7 @@
 //
 // Residual replacement.  The recursive residual of the V iteration drifts from
 // the true one by rounding.  When a column's recursive r.r falls below
-// REPLACE^2 times its value at the last replacement, or below its tolerance,
+// FLEX_REPLACE^2 times its value at the last replacement, or below its tolerance,
 // the kernel folds xi into x and recomputes r = (b - mean) - L x in FP64 for
 // the whole block (one FP64 sparse product), then continues with the same
 // direction p.  A column is declared converged only on a replaced (true)
@@ -51,7 +51,11 @@
 
 namespace fevcb {
 
-constexpr double FLEX_REPLACE = 1e-3;  // replacement when r.r drops by FLEX_REPLACE^2
+// replacement when r.r drops by FLEX_REPLACE^2: the FP32 recursion drifts by
+// about (iterations x FP32 epsilon x condition) of the residual at the last
+// replacement, a few 1e-6 here, so a 1e-4 reduction keeps the drift to a few
+// per cent of the current residual with two or three replacements a solve
+constexpr double FLEX_REPLACE = 1e-4;
 // Uniform weights of the untrained polynomial stage: a = 1.05, s = 1 (the
 // first-order Neumann series, damped by 5 % so that a > s^2 holds strictly).
 constexpr double FLEX_NEUMANN_A = 1.05;

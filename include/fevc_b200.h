@@ -671,7 +671,9 @@ typedef struct FevcbSolveOptionsV1 {
 typedef struct FevcbSolveOptionsV2 {
   FevcbSolveOptionsV1 v1;
   uint32_t precision;       /* 0 double; 1 single-precision residual, direction and products with a double
-                               solution, double reductions and double residual replacement */
+                               solution, double reductions and double residual replacement; 2 autotuned:
+                               the fastest of those forms on the generation's first leverage block
+                               (fevcb_engine_tuning_v1) */
   uint32_t reserved;
 } FevcbSolveOptionsV2;
 
@@ -844,6 +846,22 @@ int32_t fevcb_cmg_aggregate_v1(uint32_t vertices, const uint32_t *row_ptr, const
  * Outputs the median milliseconds per launch and algorithmic bytes per launch. */
 int32_t fevcb_engine_kernel_benchmark_v1(uint64_t generation, uint32_t kernel, uint32_t block_columns,
                                          uint32_t launches, double *ms_per_launch, double *bytes_per_launch);
+
+/* The solver-form autotuner of a generation solved with precision 2 (no
+ * counterpart in the reference): the candidates timed on the first leverage
+ * block (precision 0/1 and preconditioner 1 Jacobi, 3 learned or 4 uniform
+ * degree-1 stage), their milliseconds, and the index of the one kept
+ * (-1 before the first such solve). */
+typedef struct FevcbTuningV1 {
+  uint32_t struct_size;
+  int32_t chosen;
+  uint32_t candidates;
+  uint32_t precision[3];
+  uint32_t preconditioner[3];
+  uint32_t reserved;
+  double milliseconds[3];
+} FevcbTuningV1;
+int32_t fevcb_engine_tuning_v1(uint64_t generation, FevcbTuningV1 *output, uint32_t output_capacity_bytes);
 
 /* Ceiling on the identified dimension (W + F - 1) of an exact-estimator solve
  * of this generation (no counterpart in the reference, whose dense estimator

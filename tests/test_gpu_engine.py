@@ -328,3 +328,28 @@ def test_device_hybrid_assembly_with_star_workers(lib):
     kept = e.timings()["kept_workers"]
     e.release()
     assert kept > 0 and same.value == 1
+
+
+def test_autotuner_keeps_a_timed_form_with_the_same_components(lib):
+    """Precision option 2 times FP64 Jacobi, FP32 Jacobi and the FP32
+    degree-1 stage on the first leverage block, keeps the fastest for the
+    generation (its resolves included), and gives the FP64 components."""
+    from fevc_b200.panel import generate_panel
+
+    panel = generate_panel(30_000, 1_500, 5, seed=123)
+    want = solve_precision(lib, panel, probes=64, precision=0, tol=1e-10)
+    ref = want.result()
+    want.release()
+    e = solve_precision(lib, panel, probes=64, precision=2, tol=1e-10, precond=4)
+    got = e.result()
+    t = e.tuning()
+    e.resolve()
+    again = e.result()
+    assert t == e.tuning()  # the choice is kept for the generation
+    e.release()
+    assert t["chosen"] in range(len(t["candidates"])) and len(t["candidates"]) == 3
+    assert all(c["ms"] > 0 for c in t["candidates"])
+    assert {(c["precision"], c["preconditioner"]) for c in t["candidates"]} == {(0, 1), (1, 1), (1, 4)}
+    for key in ("plugin", "correction", "corrected"):
+        assert rel(got[key], ref[key]) < 1e-8, key
+        assert rel(again[key], got[key]) < 1e-12, key
