@@ -719,10 +719,10 @@ const char* vckss_rust_backend_version(void) { return "fevc-b200 0.1.0 (sm_100a)
 
 const char* vckss_rust_capabilities_json(void) {
   return "{\"backend\":\"fevc-b200\",\"abi\":1,\"device\":\"sm_100a\",\"rng\":\"VCKSS-COUNTER-V1\","
-         "\"algorithms\":[\"jla\"],\"engines\":[\"compressed\",\"generic\"],"
+         "\"algorithms\":[\"jla\",\"exact\"],\"engines\":[\"compressed\",\"generic\"],"
          "\"deletion\":[\"match\",\"observation\"],\"controls\":8,\"centering\":[\"none\",\"mean\"],"
          "\"solver\":\"blocked-pcg-hybrid-laplacian\","
-         "\"preconditioners\":[\"jacobi\",\"cmg\",\"learned\",\"polynomial\"],\"precision\":[\"f64\",\"mixed\"]}";
+         "\"preconditioners\":[\"jacobi\",\"cmg\",\"learned\",\"polynomial\"],\"precision\":[\"f64\",\"mixed\",\"autotuned\"]}";
 }
 
 const char* vckss_rust_last_error(void) { return g_last_error.c_str(); }
