@@ -497,6 +497,7 @@ def main():
     t0 = time.perf_counter()
     e.prepare(panel, deletion_mode=deletion_mode(panel))
     prepare_s = time.perf_counter() - t0
+    prepare_phases = {k: round(v / 1e3, 3) if k.endswith("_ms") else v for k, v in e.prepare_timings().items()}
     e.device_options(block, precond, precision)
     # N ranks: every rank contributes `probes` probes to one decomposition of
     # probes x N (weak scaling); the leverage accumulators are all-reduced and
@@ -632,6 +633,7 @@ def main():
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": 144, "seconds_per_step": round(e2e_s, 4)},
             "time_to_decomposition_s": round(prepare_s + e2e_s, 3), "prepare_s": round(prepare_s, 3),
+            "prepare_phases_s": {k.replace("_ms", ""): v for k, v in prepare_phases.items()},
             "first_solve_s": round(first_solve_s, 3),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,

@@ -202,6 +202,11 @@ class FevcbTuningV1(Struct):
                 ("preconditioner", u32 * 3), ("reserved", u32), ("milliseconds", f64 * 3)]
 
 
+class FevcbPrepareTimingsV1(Struct):
+    _fields_ = [("struct_size", u32), ("threads", u32), ("ingest_ms", f64), ("canonical_ms", f64),
+                ("graph_ms", f64), ("compression_ms", f64), ("plan_ms", f64), ("total_ms", f64)]
+
+
 class FevcbSolveTimingsV1(Struct):
     _fields_ = [("struct_size", u32), ("fallbacks", u32), ("total_ms", f64), ("fit_ms", f64), ("leverage_ms", f64),
                 ("target_ms", f64), ("setup_ms", f64)] + [(n, u64) for n in (
@@ -545,6 +550,7 @@ SIGNATURES = {
     "fevcb_counter_atoms_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64, C.POINTER(i64)]),
     "fevcb_engine_exact_limit_v1": (i32, [u64, u64]),
     "fevcb_engine_tuning_v1": (i32, [u64, C.c_void_p, u32]),
+    "fevcb_engine_prepare_timings_v1": (i32, [u64, C.c_void_p, u32]),
     "fevcb_counter_atoms_noalloc_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64,
                                              C.POINTER(i64)]),
 }
@@ -844,6 +850,12 @@ class Engine:
         return {"chosen": t.chosen, "candidates": [
             {"precision": t.precision[c], "preconditioner": t.preconditioner[c], "ms": t.milliseconds[c]}
             for c in range(n)]}
+
+    def prepare_timings(self) -> dict:
+        """Host preparation wall time by phase, milliseconds."""
+        t = FevcbPrepareTimingsV1()
+        self.check(self.lib.fevcb_engine_prepare_timings_v1(self.generation, C.byref(t), C.sizeof(t)))
+        return {k: getattr(t, k) for k, _ in FevcbPrepareTimingsV1._fields_ if k != "struct_size"}
 
     def resolve(self) -> None:
         self.check(self.lib.fevcb_engine_resolve_v1(self.generation))

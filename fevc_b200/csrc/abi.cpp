@@ -5,7 +5,9 @@
 // thread-local text (ffi_engine.rs:2469-2498).
 #include <algorithm>
 #include <cmath>
+#include <chrono>
 #include <cstring>
+#include <thread>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -103,6 +105,9 @@ struct Prepared {
   // ceiling on the identified dimension of an exact solve above the
   // reference's 2,000 (fevcb_engine_exact_limit_v1); 0: the request's limit
   uint64_t exact_ceiling = 0;
+  // host preparation phases, wall milliseconds: ingest copy, canonical ids,
+  // graph fixed point, compression, JLA plan
+  double prepare_ms[5] = {0, 0, 0, 0, 0};
 };
 
 struct Registry {
@@ -214,10 +219,18 @@ void prepare_common(const PrepareArgs& a, uint64_t* out, uint32_t cap) {
   }
   a.interrupt.check("engine_prepare_entry");
   auto prep = std::make_unique<Prepared>();
+  auto tick = std::chrono::steady_clock::now();
+  auto lap = [&](int phase) {
+    auto t = std::chrono::steady_clock::now();
+    prep->prepare_ms[phase] = std::chrono::duration<double, std::milli>(t - tick).count();
+    tick = t;
+  };
   InputColumns in = copy_columns(a.rows, a.v1->worker, a.v1->firm, a.v1->deletion, a.v1->outcome, a.v1->frequency,
                                  a.v1->target_weight, a.controls, a.controls_count, a.probe_order);
+  lap(0);
   a.interrupt.check("engine_ingest", a.rows);
   Canonical canon = canonicalize(std::move(in), a.implicit_match != 0);
+  lap(1);
   a.interrupt.check("canonicalize_final", a.rows);
   if (a.deletion_mode == VCKSS_DELETION_OBSERVATION)
     prep->retained = select_observation_graph(canon, prep->graph);
@@ -225,13 +238,16 @@ void prepare_common(const PrepareArgs& a, uint64_t* out, uint32_t cap) {
     prep->retained = select_implicit_match_graph(canon, prep->graph);
   else
     prep->retained = select_match_graph(canon, prep->graph);
+  lap(2);
   a.interrupt.check("graph_final", a.rows);
   prep->problem = compress(canon, prep->retained, a.implicit_match != 0);
+  lap(3);
   a.interrupt.check("compression_final", a.rows);
   if (a.deletion_mode == VCKSS_DELETION_MATCH)
     prep->plan = prep->problem.controls.empty() ? build_plan(prep->problem) : build_generic_plan(prep->problem);
   else
     prep->plan = build_generic_plan(prep->problem, Deletion::Observation);
+  lap(4);
   prep->has_plan = true;
   prep->input_rows = a.rows;
   prep->memory_limit = a.memory_limit;
@@ -1548,6 +1564,25 @@ int32_t fevcb_engine_tuning_v1(uint64_t generation, FevcbTuningV1* out, uint32_t
         t.milliseconds[c] = ms[c];
       }
     }
+    *out = t;
+  });
+}
+
+int32_t fevcb_engine_prepare_timings_v1(uint64_t generation, FevcbPrepareTimingsV1* out, uint32_t cap) {
+  return status([&] {
+    if (!out || cap < sizeof(FevcbPrepareTimingsV1))
+      fail(INVALID_INPUT, "engine_ffi", "prepare timings output capacity is too small");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_prepare_timings");
+    FevcbPrepareTimingsV1 t{};
+    t.struct_size = sizeof(FevcbPrepareTimingsV1);
+    t.threads = std::max(1u, std::thread::hardware_concurrency());
+    t.ingest_ms = p.prepare_ms[0];
+    t.canonical_ms = p.prepare_ms[1];
+    t.graph_ms = p.prepare_ms[2];
+    t.compression_ms = p.prepare_ms[3];
+    t.plan_ms = p.prepare_ms[4];
+    t.total_ms = t.ingest_ms + t.canonical_ms + t.graph_ms + t.compression_ms + t.plan_ms;
     *out = t;
   });
 }

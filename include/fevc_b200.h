@@ -863,6 +863,25 @@ typedef struct FevcbTuningV1 {
 } FevcbTuningV1;
 int32_t fevcb_engine_tuning_v1(uint64_t generation, FevcbTuningV1 *output, uint32_t output_capacity_bytes);
 
+/* Wall time of the host preparation of a generation, by phase (the split of
+ * the reference's preparation timings): ingest copy of the caller's columns,
+ * canonical ids and validation (vckss-core/src/problem.rs:102-173), graph
+ * fixed point (graph.rs:82-511), compression (problem.rs:194-606) and the
+ * JLA plan with semantic ranks (jla.rs:21-790).  threads = host threads the
+ * preparation may use. */
+typedef struct FevcbPrepareTimingsV1 {
+  uint32_t struct_size;
+  uint32_t threads;
+  double ingest_ms;
+  double canonical_ms;
+  double graph_ms;
+  double compression_ms;
+  double plan_ms;
+  double total_ms;
+} FevcbPrepareTimingsV1;
+int32_t fevcb_engine_prepare_timings_v1(uint64_t generation, FevcbPrepareTimingsV1 *output,
+                                        uint32_t output_capacity_bytes);
+
 /* Ceiling on the identified dimension (W + F - 1) of an exact-estimator solve
  * of this generation (no counterpart in the reference, whose dense estimator
  * refuses limits above 2,000: vckss-core/src/exact_estimator.rs:104-108).

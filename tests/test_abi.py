@@ -269,3 +269,26 @@ def test_entry_points_outside_the_solve_path(lib):
         assert lib.vckss_rust_session_last_error() == lib.vckss_rust_engine_last_error()
         called += 1
     assert called >= 80
+
+
+def test_prepare_timings_split_the_preparation(lib):
+    """The preparation's phase split: five non-negative phases that add up to
+    the total, which the wall clock around the prepare call bounds."""
+    import time
+
+    from fevc_b200.panel import generate_panel
+
+    e = abi.Engine(lib)
+    panel = generate_panel(20_000, 1_000, 5, seed=5)
+    t0 = time.perf_counter()
+    e.prepare(panel)
+    wall_ms = (time.perf_counter() - t0) * 1e3
+    try:
+        t = e.prepare_timings()
+        phases = [t[k] for k in ("ingest_ms", "canonical_ms", "graph_ms", "compression_ms", "plan_ms")]
+        assert all(p >= 0.0 for p in phases) and t["threads"] >= 1
+        assert abs(sum(phases) - t["total_ms"]) < 1e-6 * max(1.0, t["total_ms"])
+        assert 0.0 < t["total_ms"] <= wall_ms
+        assert lib.fevcb_engine_prepare_timings_v1(e.generation, None, 0) == 20
+    finally:
+        e.release()
