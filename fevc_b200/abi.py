@@ -160,6 +160,34 @@ class ResultV1(Struct):
                 ("correction", Components), ("corrected", Components), ("numerical_mcse", Components)]
 
 
+class NumericalRequestV1(Struct):
+    """Numerical MCSE attachment request (reference vckss_rust.h
+    VckssNumericalRequestV1, 328 bytes; the point request is a V4 solve)."""
+    _fields_ = [(n, u32) for n in ("abi_version", "struct_size", "schema_version", "threads", "tolerance_supplied",
+                                   "projection_requested", "component_requested", "reserved", "controls_count",
+                                   "reserved_2")] + [("point", SolveRequestV4)]
+
+
+class NumericalResultV1(Struct):
+    """Numerical MCSE attachment result (VckssNumericalResultV1, 512 bytes)."""
+    _fields_ = [("struct_size", u32), ("schema_version", u32), ("generation", u64)] + [
+        (n, u32) for n in ("status", "engine", "leverage_probes", "target_probes", "target_fold_a",
+                           "target_fold_b")] + [
+        (n, u64) for n in ("certified_replay_rhs", "executed_replay_rhs", "attempted_replay_rhs",
+                           "replay_generator_words", "allocation_bound_bytes")] + [
+        ("failed_replay_probe", u32), ("replay_error_code", u32)] + [
+        (n, f64) for n in ("psd_adjustment", "minimum_constrained", "minimum_residual_margin",
+                           "maximum_sensitivity_ratio")] + [
+        ("score_means", f64 * 6), ("conditional", f64 * 9), ("leverage", f64 * 9), ("raw", f64 * 9),
+        ("usable", f64 * 9), ("mcse", f64 * 4), ("point_rhs", u64), ("maximum_point_complete_residual", f64),
+        ("maximum_replay_complete_residual", f64)]
+
+
+class NumericalRhsV1(Struct):
+    _fields_ = [("schema_version", u32), ("phase", u32), ("probe", u32), ("reserved", u32),
+                ("complete_residual", f64)]
+
+
 class PreparationReceiptV2(Struct):
     _fields_ = [("struct_size", u32), ("reserved", u32)] + [(n, u64) for n in (
         "generation", "input_rows", "retained_rows", "workers", "firms", "cells", "deletion_units", "target_strata",
@@ -551,6 +579,12 @@ SIGNATURES = {
     "fevcb_engine_exact_limit_v1": (i32, [u64, u64]),
     "fevcb_engine_tuning_v1": (i32, [u64, C.c_void_p, u32]),
     "fevcb_engine_prepare_timings_v1": (i32, [u64, C.c_void_p, u32]),
+    "fevcb_numerical_finalize_v1": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u32]),
+    "vckss_rust_engine_numerical_preflight_v1": (i32, [C.c_void_p]),
+    "vckss_rust_engine_numerical_result_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_numerical_rhs_v1": (i32, [u64, C.c_void_p, u64, C.c_void_p]),
+    "vckss_rust_engine_solve_numerical_interrupt_v1": (i32, [u64, C.c_void_p, C.c_void_p, C.c_void_p, u32]),
+    "vckss_rust_engine_solve_numerical_v1": (i32, [u64, C.c_void_p]),
     "fevcb_counter_atoms_noalloc_v1": (i32, [u64, u64, u64, u32, C.POINTER(u64), C.POINTER(u64), u64,
                                              C.POINTER(i64)]),
 }
@@ -607,10 +641,7 @@ UNSUPPORTED_SIGNATURES = {
     "vckss_rust_engine_memory_forecast_v1": (i32, [u64, C.c_void_p, u32]),
     "vckss_rust_engine_memory_policy_v1": (i32, [u64, C.c_void_p, u32]),
     "vckss_rust_engine_numerical_cmg_work_v1": (i32, [u64, C.c_void_p, u32]),
-    "vckss_rust_engine_numerical_preflight_v1": (i32, [C.c_void_p]),
     "vckss_rust_engine_numerical_preflight_v2": (i32, [C.c_void_p]),
-    "vckss_rust_engine_numerical_result_v1": (i32, [u64, C.c_void_p, u32]),
-    "vckss_rust_engine_numerical_rhs_v1": (i32, [u64, C.c_void_p, u64, C.c_void_p]),
     "vckss_rust_engine_performance_receipt_v1": (i32, [u64, C.c_void_p, u32]),
     "vckss_rust_engine_prepare_interrupt_v3": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u32]),
     "vckss_rust_engine_prepare_memory_interrupt_v1": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, u32]),
@@ -629,10 +660,8 @@ UNSUPPORTED_SIGNATURES = {
     "vckss_rust_engine_solve_interrupt_v6": (i32, [u64, C.c_void_p]),
     "vckss_rust_engine_solve_interrupt_v7": (i32, [u64, C.c_void_p]),
     "vckss_rust_engine_solve_numerical_generic_legacy_v2": (i32, [u64, C.c_void_p]),
-    "vckss_rust_engine_solve_numerical_interrupt_v1": (i32, [u64, C.c_void_p, C.c_void_p, C.c_void_p, u32]),
     "vckss_rust_engine_solve_numerical_interrupt_v2": (i32, [u64, C.c_void_p, C.c_void_p, C.c_void_p, u32]),
     "vckss_rust_engine_solve_numerical_legacy_v2": (i32, [u64, C.c_void_p]),
-    "vckss_rust_engine_solve_numerical_v1": (i32, [u64, C.c_void_p]),
     "vckss_rust_engine_solve_v2": (i32, [u64, C.c_void_p]),
     "vckss_rust_engine_solve_v3": (i32, [u64, C.c_void_p]),
     "vckss_rust_engine_solve_v6": (i32, [u64, C.c_void_p]),
@@ -803,6 +832,31 @@ class Engine:
     def solve_v5(self, req: SolveRequestV5, controls_count: int = 0) -> None:
         req.v4.v3.request_signature = capability_signature_v3(req.v4, controls_count)
         self.check(self.lib.vckss_rust_engine_solve_v5(self.generation, C.byref(req)))
+
+    def numerical_request(self, point: SolveRequestV5, controls_count: int = 0) -> NumericalRequestV1:
+        """A numerical-attachment request around a V5 request's V4 point
+        (signature reconciled for controls_count)."""
+        point.v4.v3.request_signature = capability_signature_v3(point.v4, controls_count)
+        return NumericalRequestV1(1, C.sizeof(NumericalRequestV1), 1, max(1, int(point.threads)),
+                                  int(point.tolerance_supplied), 0, 0, 0, controls_count, 0, point.v4)
+
+    def solve_numerical(self, req: NumericalRequestV1) -> None:
+        self.check(self.lib.vckss_rust_engine_solve_numerical_v1(self.generation, C.byref(req)))
+
+    def numerical_result(self) -> dict:
+        r = NumericalResultV1()
+        self.check(self.lib.vckss_rust_engine_numerical_result_v1(self.generation, C.byref(r), C.sizeof(r)))
+        d = {}
+        for name, _ in NumericalResultV1._fields_:
+            v = getattr(r, name)
+            d[name] = list(v) if hasattr(v, "__len__") else v
+        return d
+
+    def numerical_rhs(self, rows: int) -> tuple[int, list[dict]]:
+        arr = (NumericalRhsV1 * max(rows, 1))()
+        count = u64(0)
+        self.check(self.lib.vckss_rust_engine_numerical_rhs_v1(self.generation, arr, rows, C.byref(count)))
+        return count.value, [arr[i].as_dict() for i in range(min(rows, count.value))]
 
     def result(self) -> dict:
         r = ResultV1()

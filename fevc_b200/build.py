@@ -21,7 +21,7 @@ INCLUDE = HERE.parent / "include"
 BUILD = HERE / "_build"
 LIB = HERE / "libfevc_b200.so"
 
-CXX_SOURCES = ["prep.cpp", "abi.cpp", "hybrid.cpp", "cmg_host.cpp", "abi_unsupported.cpp"]
+CXX_SOURCES = ["prep.cpp", "abi.cpp", "hybrid.cpp", "cmg_host.cpp", "abi_unsupported.cpp", "numerical.cpp"]
 CU_SOURCES = ["engine.cu", "multigrid.cu", "noalloc.cu", "learned.cu", "devmem.cu"]
 GENCODE = "-gencode=arch=compute_100a,code=sm_100a"
 

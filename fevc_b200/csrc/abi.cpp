@@ -16,6 +16,7 @@
 #include "fevc_b200.h"
 #include "counter_rng.h"
 #include "engine.h"
+#include "numerical.h"
 #include "cmg_host.h"
 #include "hybrid.h"
 #include "learned.h"
@@ -2068,6 +2069,211 @@ int32_t fevcb_counter_atoms_v1(uint64_t seed, uint64_t domain_tag, uint64_t firs
 }
 
 }  // extern "C"
+
+// ---- numerical MCSE attachment (reference vckss-plugin/src/numerical_api.rs)
+
+namespace {
+
+// validate_point with point_only (numerical_api.rs:113-203): schema, reserved
+// fields, JLA with Counter-V1 on the automatic / diagonal / CMG route, no
+// projection or component attachment, and a point request that reconciles
+// with its planned capability for the request's control count.
+void numerical_validate(const VckssNumericalRequestV1& q) {
+  require_abi(q.abi_version);
+  require_abi(q.point.v3.v2.v1.abi_version);
+  if (q.schema_version != 1 || q.reserved != 0 || q.reserved_2 != 0 || q.tolerance_supplied > 1 ||
+      q.projection_requested > 1 || q.component_requested > 1)
+    fail(ABI_MISMATCH, "engine_ffi", "invalid numerical V1 schema or reserved fields");
+  const VckssEngineSolveRequestV4& pt = q.point;
+  if (pt.v3.v2.v1.struct_size < sizeof(VckssEngineSolveRequestV4))
+    fail(ABI_MISMATCH, "engine_ffi", "numerical point prefix reports a short structure size");
+  if (pt.v3.reserved_3 != 0 || pt.reserved_4 != 0)
+    fail(ABI_MISMATCH, "engine_ffi", "reserved numerical point prefix fields must be zero");
+  if (q.threads == 0 || pt.v3.v2.v1.probes < 2)
+    fail(INVALID_INPUT, "numerical_preflight", "positive threads and at least two probes required");
+  const uint32_t alg = pt.v3.v2.algorithm, eng = pt.v3.engine, route = pt.v3.v2.v1.solver_route;
+  if (q.projection_requested != 0 || q.component_requested != 0 ||
+      (alg != VCKSS_ALGORITHM_JLA && alg != VCKSS_ALGORITHM_AUTO) ||
+      (eng != VCKSS_ENGINE_AUTO_OR_UNSPECIFIED && eng != VCKSS_ENGINE_GENERIC && eng != VCKSS_ENGINE_COMPRESSED) ||
+      (route != VCKSS_ROUTE_AUTO && route != VCKSS_ROUTE_DIAGONAL_PCG && route != VCKSS_ROUTE_CMG_PCG) ||
+      pt.v3.v2.v1.rng_contract != VCKSS_RNG_COUNTER_V1)
+    fail(UNSUPPORTED_FEATURE, "numerical_preflight",
+         "numerical V1 requires Counter-V1 JLA with no projection or component-inference attachment");
+  VckssEngineSolveRequestV1 v1 = pt.v3.v2.v1;  // the point's option gates (automatic widths allowed)
+  if (v1.leverage_batch_width == 0) v1.leverage_batch_width = 8;
+  if (v1.target_batch_width == 0) v1.target_batch_width = 8;
+  (void)options_from_v1(v1, true);
+  auto c = capability_request_for_solve(pt, q.controls_count);
+  const uint32_t reason = capability_reason(c);
+  if (pt.v3.capability_schema != VCKSS_REQUEST_CAPABILITY_SCHEMA_V3 ||
+      pt.v3.capability_profile != VCKSS_REQUEST_PROFILE_PLANNED_V1 || reason != VCKSS_REQUEST_REASON_SUPPORTED ||
+      capability_signature(c) != pt.v3.request_signature)
+    fail(UNSUPPORTED_FEATURE, "numerical_preflight",
+         "numerical point request does not reconcile with its planned capability");
+}
+
+void numerical_solve(uint64_t g, const VckssNumericalRequestV1& q, const Interrupt& intr) {
+  numerical_validate(q);
+  SolveOptions o = options_from_v4(q.point);
+  {
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(g, "context_solve");
+    // algorithm(auto) resolves once the retained dimensions are known
+    // (vckss-core/src/engine_plan.rs:179-240): exact within the exact limit
+    const uint64_t complexity = uint64_t(p.problem.workers) + p.problem.firms - 1 + p.problem.controls.size();
+    if (q.point.v3.v2.algorithm == VCKSS_ALGORITHM_AUTO && complexity <= q.point.v3.v2.exact_estimator_limit) {
+      o.algorithm = 1;
+      o.exact_limit = q.point.v3.v2.exact_estimator_limit;
+      o.blocksize_limit = q.point.v3.v2.blocksize_limit ? q.point.v3.v2.blocksize_limit : 5000;
+    } else if (p.has_plan && p.plan.generic) {
+      fail(UNSUPPORTED_FEATURE, "numerical_preflight",
+           "the device numerical attachment covers the compressed engine (match deletion without controls)");
+    }
+  }
+  o.numerical = true;
+  solve_common(g, o, intr, true, &q.point, 4);
+}
+
+const NumericalAttachment& numerical_of(uint64_t g, const char* phase) {
+  reg().require(g, phase);
+  if (reg().state != State::Solved || !reg().result) fail(STALE_CONTEXT, phase, "generation has no solved result");
+  const NumericalAttachment& a = reg().result->numerical;
+  if (!a.present) fail(UNSUPPORTED_FEATURE, "numerical_preflight", "result has no numerical V1 attachment");
+  return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t vckss_rust_numerical_schema_v1(void) { return 1; }
+
+int32_t vckss_rust_engine_numerical_preflight_v1(const VckssNumericalRequestV1* request) {
+  return status([&] { numerical_validate(read_struct(request, "numerical preflight")); });
+}
+
+int32_t vckss_rust_engine_solve_numerical_v1(uint64_t generation, const VckssNumericalRequestV1* request) {
+  return status([&] { numerical_solve(generation, read_struct(request, "numerical solve"), Interrupt{}); });
+}
+
+int32_t vckss_rust_engine_solve_numerical_interrupt_v1(uint64_t generation, const VckssNumericalRequestV1* request,
+                                                      VckssInterruptPollV1 poll, void* context, uint32_t interval) {
+  return status([&] {
+    auto q = read_struct(request, "numerical interrupt solve");
+    numerical_solve(generation, q, Interrupt(poll, context, interval, 0, "numerical"));
+  });
+}
+
+int32_t vckss_rust_engine_numerical_result_v1(uint64_t generation, VckssNumericalResultV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssNumericalResultV1>(out, cap, "numerical result");
+    std::lock_guard<std::mutex> l(reg().mu);
+    const NumericalAttachment& a = numerical_of(generation, "numerical_result");
+    const SolveResult& s = *reg().result;
+    VckssNumericalResultV1 v{};
+    v.struct_size = sizeof(v);
+    v.schema_version = 1;
+    v.generation = generation;
+    v.status = a.status;
+    v.engine = a.exact ? 3u : 1u;
+    v.failed_replay_probe = 0xffffffffu;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        v.conditional[i][j] = a.conditional[i][j];
+        v.leverage[i][j] = a.leverage[i][j];
+        v.raw[i][j] = a.raw[i][j];
+        v.usable[i][j] = a.usable[i][j];
+      }
+    for (int k = 0; k < 4; ++k) v.mcse[k] = a.mcse[k];
+    v.psd_adjustment = a.psd_adjustment;
+    if (!a.exact) {
+      v.leverage_probes = a.leverage_probes;
+      v.target_probes = a.target_probes;
+      v.target_fold_a = a.folds[0];
+      v.target_fold_b = a.folds[1];
+      v.certified_replay_rhs = a.replay_probe.size();
+      v.executed_replay_rhs = a.replay_probe.size();
+      v.attempted_replay_rhs = a.attempted_replay_rhs;
+      v.replay_generator_words = a.generator_words;
+      v.allocation_bound_bytes = a.allocation_bound_bytes;
+      v.failed_replay_probe = a.failed_replay_probe;
+      v.replay_error_code = a.replay_error_code;
+      for (int f = 0; f < 2; ++f)
+        for (int j = 0; j < 3; ++j) v.score_means[f][j] = a.score_means[f][j];
+      v.minimum_constrained = a.minimum_constrained;
+      v.minimum_residual_margin = a.minimum_residual_margin;
+      v.maximum_sensitivity_ratio = a.maximum_sensitivity_ratio;
+      double mx = 0.0;
+      for (double r : a.replay_residual) mx = std::max(mx, r);
+      v.maximum_replay_complete_residual = mx;
+      v.point_rhs = s.receipts.size();
+      v.maximum_point_complete_residual = s.max_complete_residual;
+    }
+    std::memcpy(out, &v, sizeof(v));
+  });
+}
+
+// The attachment's host covariance algebra on given conditional and leverage
+// matrices (row-major 3 x 3): fills status, conditional, leverage, raw,
+// usable, mcse and psd_adjustment of *out and zeroes the rest.
+int32_t fevcb_numerical_finalize_v1(const double* conditional, const double* leverage, VckssNumericalResultV1* out,
+                                    uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssNumericalResultV1>(out, cap, "numerical finalize");
+    if (!conditional || !leverage) fail(INVALID_INPUT, "numerical_mc", "null covariance input");
+    Matrix3 c{}, l{};
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        c[i][j] = conditional[3 * i + j];
+        l[i][j] = leverage[3 * i + j];
+      }
+    NumericalAttachment a;
+    finalize_covariance(c, l, a);
+    VckssNumericalResultV1 v{};
+    v.struct_size = sizeof(v);
+    v.schema_version = 1;
+    v.status = a.status;
+    v.failed_replay_probe = 0xffffffffu;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        v.conditional[i][j] = a.conditional[i][j];
+        v.leverage[i][j] = a.leverage[i][j];
+        v.raw[i][j] = a.raw[i][j];
+        v.usable[i][j] = a.usable[i][j];
+      }
+    for (int k = 0; k < 4; ++k) v.mcse[k] = a.mcse[k];
+    v.psd_adjustment = a.psd_adjustment;
+    std::memcpy(out, &v, sizeof(v));
+  });
+}
+
+int32_t vckss_rust_engine_numerical_rhs_v1(uint64_t generation, VckssNumericalRhsV1* out, uint64_t capacity,
+                                          uint64_t* written) {
+  return status([&] {
+    if (!written) fail(ABI_MISMATCH, "engine_ffi", "numerical RHS count destination is null");
+    std::lock_guard<std::mutex> l(reg().mu);
+    const NumericalAttachment& a = numerical_of(generation, "numerical_rhs");
+    const uint64_t n = a.exact ? 0 : a.replay_probe.size();
+    if (capacity > uint64_t(INT64_MAX) / sizeof(VckssNumericalRhsV1) || capacity < n || (n != 0 && !out))
+      fail(ABI_MISMATCH, "engine_ffi", "invalid or short numerical RHS destination");
+    const uintptr_t start = reinterpret_cast<uintptr_t>(out), stop = start + n * sizeof(VckssNumericalRhsV1);
+    const uintptr_t cs = reinterpret_cast<uintptr_t>(written), ce = cs + sizeof(uint64_t);
+    if (n != 0 && start < ce && cs < stop)
+      fail(ABI_MISMATCH, "engine_ffi", "numerical RHS and count destinations overlap");
+    for (uint64_t i = 0; i < n; ++i) {
+      VckssNumericalRhsV1 r{};
+      r.schema_version = 1;
+      r.phase = 1;
+      r.probe = a.replay_probe[i];
+      r.complete_residual = a.replay_residual[i];
+      std::memcpy(out + i, &r, sizeof(r));
+    }
+    *written = n;
+  });
+}
+
+}  // extern "C"
+
 
 extern "C" int32_t fevcb_counter_atoms_noalloc_v1(uint64_t seed, uint64_t domain_tag, uint64_t first_probe,
                                                   uint32_t columns, const uint64_t* entity, const uint64_t* trials,

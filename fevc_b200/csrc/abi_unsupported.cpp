@@ -58,10 +58,7 @@ int32_t vckss_rust_engine_leaveout_residual_diagnostic_v1(uint64_t, VckssLeaveou
 int32_t vckss_rust_engine_memory_forecast_v1(uint64_t, VckssMemoryForecastV1 *, uint32_t) { return fevcb::unsupported_entry("engine_memory_forecast_v1"); }
 int32_t vckss_rust_engine_memory_policy_v1(uint64_t, VckssMemoryPolicyV1 *, uint32_t) { return fevcb::unsupported_entry("engine_memory_policy_v1"); }
 int32_t vckss_rust_engine_numerical_cmg_work_v1(uint64_t, VckssFullCmgModelReceiptV1 *, uint32_t) { return fevcb::unsupported_entry("engine_numerical_cmg_work_v1"); }
-int32_t vckss_rust_engine_numerical_preflight_v1(const VckssNumericalRequestV1 *) { return fevcb::unsupported_entry("engine_numerical_preflight_v1"); }
 int32_t vckss_rust_engine_numerical_preflight_v2(const VckssNumericalRequestV2 *) { return fevcb::unsupported_entry("engine_numerical_preflight_v2"); }
-int32_t vckss_rust_engine_numerical_result_v1(uint64_t, VckssNumericalResultV1 *, uint32_t) { return fevcb::unsupported_entry("engine_numerical_result_v1"); }
-int32_t vckss_rust_engine_numerical_rhs_v1(uint64_t, VckssNumericalRhsV1 *, uint64_t, uint64_t *) { return fevcb::unsupported_entry("engine_numerical_rhs_v1"); }
 int32_t vckss_rust_engine_performance_receipt_v1(uint64_t, VckssEnginePerformanceReceiptV1 *, uint32_t) { return fevcb::unsupported_entry("engine_performance_receipt_v1"); }
 int32_t vckss_rust_engine_prepare_interrupt_v3(const VckssEnginePrepareRequestInterruptV2 *, const VckssEngineColumnsV3 *, uint64_t *, uint32_t) { return fevcb::unsupported_entry("engine_prepare_interrupt_v3"); }
 int32_t vckss_rust_engine_prepare_memory_interrupt_v1(const VckssEnginePrepareRequestInterruptV3 *, const VckssEngineColumnsV3 *, const VckssMemoryPolicyV1 *, uint64_t *, uint32_t) { return fevcb::unsupported_entry("engine_prepare_memory_interrupt_v1"); }
@@ -80,10 +77,8 @@ int32_t vckss_rust_engine_solve_interrupt_v3(uint64_t, const VckssEngineSolveReq
 int32_t vckss_rust_engine_solve_interrupt_v6(uint64_t, const VckssEngineSolveRequestInterruptV6 *) { return fevcb::unsupported_entry("engine_solve_interrupt_v6"); }
 int32_t vckss_rust_engine_solve_interrupt_v7(uint64_t, const VckssEngineSolveRequestInterruptV7 *) { return fevcb::unsupported_entry("engine_solve_interrupt_v7"); }
 int32_t vckss_rust_engine_solve_numerical_generic_legacy_v2(uint64_t, const VckssEngineSolveRequestInterruptV3 *) { return fevcb::unsupported_entry("engine_solve_numerical_generic_legacy_v2"); }
-int32_t vckss_rust_engine_solve_numerical_interrupt_v1(uint64_t, const VckssNumericalRequestV1 *, VckssInterruptPollV1, void *, uint32_t) { return fevcb::unsupported_entry("engine_solve_numerical_interrupt_v1"); }
 int32_t vckss_rust_engine_solve_numerical_interrupt_v2(uint64_t, const VckssNumericalRequestV2 *, VckssInterruptPollV1, void *, uint32_t) { return fevcb::unsupported_entry("engine_solve_numerical_interrupt_v2"); }
 int32_t vckss_rust_engine_solve_numerical_legacy_v2(uint64_t, const VckssEngineSolveRequestInterruptV2 *) { return fevcb::unsupported_entry("engine_solve_numerical_legacy_v2"); }
-int32_t vckss_rust_engine_solve_numerical_v1(uint64_t, const VckssNumericalRequestV1 *) { return fevcb::unsupported_entry("engine_solve_numerical_v1"); }
 int32_t vckss_rust_engine_solve_v2(uint64_t, const VckssEngineSolveRequestV2 *) { return fevcb::unsupported_entry("engine_solve_v2"); }
 int32_t vckss_rust_engine_solve_v3(uint64_t, const VckssEngineSolveRequestV3 *) { return fevcb::unsupported_entry("engine_solve_v3"); }
 int32_t vckss_rust_engine_solve_v6(uint64_t, const VckssEngineSolveRequestV6 *) { return fevcb::unsupported_entry("engine_solve_v6"); }
@@ -92,7 +87,6 @@ int32_t vckss_rust_engine_stayer_hybrid_result_v1(uint64_t, VckssStayerHybridRes
 uint32_t vckss_rust_exact_execution_schema_v1(void) { return 0; }  // exact execution is not provided
 uint32_t vckss_rust_exact_legacy_execution_schema_v1(void) { return 0; }  // exact execution is not provided
 uint32_t vckss_rust_exact_resolved_execution_schema_v2(void) { return 0; }  // exact execution is not provided
-uint32_t vckss_rust_numerical_schema_v1(void) { return 0; }  // the numerical attachment is not provided
 uint32_t vckss_rust_numerical_schema_v2(void) { return 0; }  // the numerical attachment is not provided
 uint32_t vckss_rust_projection_centering_schema_v1(void) { return 0; }  // the projection attachment is not provided
 int32_t vckss_rust_report_call_v1(const VckssProgressOptionsV1 *, VckssProgressOperationV1, void *) { return fevcb::unsupported_entry("report_call_v1"); }

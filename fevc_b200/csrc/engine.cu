@@ -37,6 +37,8 @@
 #include "hybrid_device.cuh"
 #include "generic.cuh"
 #include "observation.cuh"
+#include "numerical.cuh"
+#include "numerical.h"
 
 namespace fevcb {
 
@@ -288,6 +290,9 @@ struct DeviceEngine {
   bool observation = false;
   uint64_t physical = 0;
   DBuf<uint64_t> unit_offset, row_rank_d, row_copy_offset, row_phys;
+  // physical index of every unit's first copy, and the signs of the current
+  // leverage block per physical copy (bit j: probe first + j drew +1)
+  DBuf<uint64_t> unit_phys, copy_bits;
   DBuf<double> obs_row_acc, obs_copy_acc, control_lev, obs_out;
   // leave-observation-out target sums per cell (cells x (1 + q)) and the
   // cell-independent quadratic form sum_r w_r R_r R_r' (q x q, upper triangle)
@@ -296,6 +301,10 @@ struct DeviceEngine {
   // solve-long buffers
   DBuf<double> moments, unit_out, omega, fitted, fit_alpha, partial, small;
   DBuf<unsigned long long> error;
+  // numerical MCSE attachment: per-unit gradient and offset (units x 6), per-cell
+  // and per-unit target fold sums (x 6), one block's score sums, statistics
+  DBuf<double> num_coef, num_cell_fold, num_unit_fold, num_out;
+  DBuf<unsigned long long> num_stats;
   std::map<int, std::unique_ptr<BlockWork>> work;
   // pinned host scalars
   int* h_nactive = nullptr;
@@ -494,6 +503,11 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
       upload_fill(e->unit_offset, 0, R, [&](uint64_t* d) {
 #pragma omp parallel for schedule(static) if (R >= 65536)
         for (size_t i = 0; i < R; ++i) d[i] = plan.row_copy_offset[order[i]];
+      }, s, h2d);
+      e->unit_phys.alloc(R);
+      upload_fill(e->unit_phys, 0, R, [&](uint64_t* d) {
+#pragma omp parallel for schedule(static) if (R >= 65536)
+        for (size_t i = 0; i < R; ++i) d[i] = phys[order[i]];
       }, s, h2d);
       upload(e->row_rank_d, plan.row_rank, s, h2d);
       upload(e->row_copy_offset, plan.row_copy_offset, s, h2d);
@@ -1490,12 +1504,25 @@ Components finish_accounting(double w, double f, double c, double t, const char*
 
 // Leverage right-hand sides of probes [first, first + ncols): Counter-V1
 // atoms per unit summed per cell, then gathered to the workers and firms.
+//
+// Leave-observation-out blocks that start at a multiple of four also record
+// every copy's signs (k_obs_leverage_atoms), which the moment pass then reads
+// instead of drawing the Philox blocks a second time; returns whether it did.
+inline bool shared_signs(const DeviceEngine& e, uint32_t first) { return e.observation && first % 4 == 0; }
+
 template <int K>
 void leverage_rhs(DeviceEngine& e, BlockWork& w, Launch L, PhiloxKey key, uint32_t first, int ncols) {
-  k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p,
-                                                   e.observation ? e.unit_offset.p : nullptr, key, TAG_LEVERAGE,
-                                                   first, ncols, e.observation ? nullptr : w.unit_atoms.p,
-                                                   w.cell_val.p);
+  if (shared_signs(e, first)) {
+    if (!e.copy_bits.p) e.copy_bits.alloc(e.physical);
+    k_obs_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p,
+                                                         e.unit_offset.p, e.unit_phys.p, key, first, ncols,
+                                                         reinterpret_cast<uint8_t*>(e.copy_bits.p), w.cell_val.p);
+  } else {
+    k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p,
+                                                     e.observation ? e.unit_offset.p : nullptr, key, TAG_LEVERAGE,
+                                                     first, ncols, e.observation ? nullptr : w.unit_atoms.p,
+                                                     w.cell_val.p);
+  }
   k_gather<K><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, w.cell_val.p, w.bW.p);
   firm_gather<K, 0, 0>(e, w, L, nullptr, w.cell_val.p, nullptr, 0.0, nullptr, nullptr, nullptr, w.bF.p, nullptr);
 }
@@ -1570,7 +1597,8 @@ void run_leverage(DeviceEngine& e, const SolveOptions& o, SolveResult& res, uint
     if (e.observation)
       k_obs_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.rows, ncols, e.row_cell.p, e.cell_worker.p, e.cell_firm.p,
                                                     e.row_rank_d.p, e.row_copy_offset.p, e.row_phys.p, key, first,
-                                                    w.alpha.p, w.x.p, e.obs_row_acc.p, e.obs_copy_acc.p);
+                                                    shared_signs(e, first) ? e.copy_bits.p : nullptr, w.alpha.p,
+                                                    w.x.p, e.obs_row_acc.p, e.obs_copy_acc.p);
     else
       k_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.G, ncols, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
                                                 e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.moments.p);
@@ -1639,8 +1667,12 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
     CK(cudaMemcpyAsync(w.bF.p + size_t(e.F - 1) * K, lastF.data(), K * sizeof(double), cudaMemcpyHostToDevice, L.s));
     BlockOutcome bo = solve_block<K>(e, w, 2 * np, o, res.timings);
     if (!e.generic) {
-      k_contract<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, e.omega.p, w.alpha.p, w.x.p,
-                                                 e.partial.p);
+      if (o.numerical)  // the contraction plus the cells' target fold sums of the attachment
+        k_contract_folds<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, e.omega.p, w.alpha.p,
+                                                         w.x.p, uint64_t(first), e.num_cell_fold.p, e.partial.p);
+      else
+        k_contract<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, e.omega.p, w.alpha.p, w.x.p,
+                                                   e.partial.p);
       finish(e.partial.p, L.grid, 3 * K, w.tot.p, L.s);
       CK(cudaMemcpyAsync(draws.data(), w.tot.p, 3 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
       CK(cudaStreamSynchronize(L.s));
@@ -1987,6 +2019,127 @@ void run_exact(DeviceEngine& e, const Compressed& p, const SolveOptions& o, Solv
   res.mcse = Components{0.0, 0.0, 0.0, 0.0};
 }
 
+// ---------------------------------------------------------------------------
+// Numerical MCSE attachment of the compressed engine (reference
+// vckss-core/src/engine/numerical.rs).
+
+// State::new on the device: per-unit gradients and offsets; returns the
+// state's status (2 local, 5 nonsmooth adjustment, 6 nonfinite derivative)
+// and records the shares' extremes in the attachment.
+uint32_t numerical_derivative(DeviceEngine& e, const SolveOptions& o, NumericalAttachment& na) {
+  Launch L{grid_blocks(), e.stream};
+  if (e.num_coef.n < size_t(e.G) * 6) e.num_coef.alloc(size_t(e.G) * 6);
+  if (!e.num_stats.p) e.num_stats.alloc(8);
+  const unsigned long long inf = 0x7ff0000000000000ull;
+  unsigned long long init[NUM_STATS] = {0, inf, inf, 0, 0}, got[NUM_STATS];
+  CK(cudaMemcpyAsync(e.num_stats.p, init, sizeof(init), cudaMemcpyHostToDevice, L.s));
+  k_num_derivative<<<L.grid, THREADS, 0, L.s>>>(e.G, double(o.probes), e.moments.p, e.num_coef.p, e.num_stats.p);
+  CK(cudaMemcpyAsync(got, e.num_stats.p, sizeof(got), cudaMemcpyDeviceToHost, L.s));
+  CK(cudaStreamSynchronize(L.s));
+  std::memcpy(&na.minimum_constrained, &got[1], 8);
+  std::memcpy(&na.minimum_residual_margin, &got[2], 8);
+  std::memcpy(&na.maximum_sensitivity_ratio, &got[3], 8);
+  uint32_t status = got[4] ? 5u : 2u;  // a clipped adjustment variance starts nonsmooth
+  if (got[0]) status = uint32_t(got[0] & 0xff);  // the last unit that set a status wins
+  return status;
+}
+
+// Replay of the leverage probes [probe_begin, probe_end) at width K: the same
+// atoms and solves as the leverage phase, each column scored against the
+// units' target folds.  Returns false (status 7 recorded) when a solve fails
+// to certify, as the reference's replay does for PCG and residual failures.
+template <int K>
+bool numerical_replay(DeviceEngine& e, const SolveOptions& o, SolveResult& res, std::vector<Primitive> (&scores)[2]) {
+  BlockWork& w = get_work<K>(e);
+  Launch L{grid_blocks(), e.stream};
+  PhiloxKey key = philox_key(o.seed);
+  NumericalAttachment& na = res.numerical;
+  std::vector<double> out(6 * K);
+  const uint32_t end = o.probe_end ? o.probe_end : o.probes;
+  for (uint32_t first = o.probe_begin; first < end; first += K) {
+    const int ncols = int(std::min<uint32_t>(K, end - first));
+    leverage_rhs<K>(e, w, L, key, first, ncols);
+    na.attempted_replay_rhs += uint64_t(ncols);
+    BlockOutcome bo;
+    try {
+      bo = solve_block<K>(e, w, ncols, o, res.timings);
+    } catch (const Error& err) {
+      if (err.code == PCG_MAX_ITERATIONS || err.code == PCG_STAGNATION || err.code == PCG_CURVATURE_BREAKDOWN ||
+          err.code == PCG_PRECONDITIONER_BREAKDOWN || err.code == FULL_RESIDUAL_FAILED) {
+        na.failed_replay_probe = first;
+        na.replay_error_code = uint32_t(err.code);
+        return false;
+      }
+      throw;
+    }
+    k_num_scores<K><<<L.grid, THREADS, 0, L.s>>>(e.G, ncols, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
+                                                 e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.num_coef.p,
+                                                 e.num_unit_fold.p, e.partial.p);
+    finish(e.partial.p, L.grid, 6 * K, e.num_out.p, L.s);
+    CK(cudaMemcpyAsync(out.data(), e.num_out.p, 6 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    res.timings.kernel_launches += 6;
+    for (int j = 0; j < ncols; ++j) {
+      scores[0][first + j] = {out[0 * K + j], out[1 * K + j], out[2 * K + j]};
+      scores[1][first + j] = {out[3 * K + j], out[4 * K + j], out[5 * K + j]};
+      na.replay_probe.push_back(first + j);
+      na.replay_residual.push_back(bo.complete[j]);
+    }
+  }
+  return true;
+}
+
+// The replay in the leverage phase's blocks (full blocks at K, the rest at
+// the narrowest width that holds it).
+template <int K>
+bool numerical_replay_blocks(DeviceEngine& e, const SolveOptions& o, SolveResult& res,
+                             std::vector<Primitive> (&scores)[2]) {
+  SolveOptions head, tail;
+  int width = 0;
+  if (K < 16 || !split_probes(o, K, K, 1, head, tail, width)) return numerical_replay<K>(e, o, res, scores);
+  if (head.probe_end > head.probe_begin && !numerical_replay<K>(e, head, res, scores)) return false;
+  switch (width) {
+    case 8: return numerical_replay<8>(e, tail, res, scores);
+    case 16: return numerical_replay<16>(e, tail, res, scores);
+    default: return numerical_replay<32>(e, tail, res, scores);
+  }
+}
+
+// The attachment after the point solve: unit folds from the cells' target
+// fold sums, the replay, and the host covariance algebra.
+template <int K>
+void numerical_finish(DeviceEngine& e, const JlaPlan& plan, const SolveOptions& o, double outcome_mean,
+                      uint32_t state_status, SolveResult& res) {
+  Launch L{grid_blocks(), e.stream};
+  NumericalAttachment& na = res.numerical;
+  const uint32_t r = o.probes;
+  na.present = true;
+  na.leverage_probes = r;
+  na.target_probes = r;
+  na.folds[0] = (r + 1) / 2;
+  na.folds[1] = r / 2;
+  // allocation bound of the reference's attachment (engine/numerical.rs:36-49)
+  na.allocation_bound_bytes = uint64_t(e.G) * (6 * 8 + 6 * 16 + 4 * 8 + 4 * 16) + uint64_t(r) * 168 + 4096;
+  if (e.num_unit_fold.n < size_t(e.G) * 6) e.num_unit_fold.alloc(size_t(e.G) * 6);
+  k_num_unit_folds<<<L.grid, THREADS, 0, L.s>>>(e.G, e.unit_cell.p, e.unit_outcome.p, e.unit_count_f.p, e.unit_out.p,
+                                                outcome_mean, double(na.folds[0]), double(na.folds[1]),
+                                                e.num_cell_fold.p, e.num_unit_fold.p);
+  std::vector<Primitive> scores[2] = {std::vector<Primitive>(r, Primitive{0, 0, 0}),
+                                      std::vector<Primitive>(r, Primitive{0, 0, 0})};
+  uint32_t status = state_status;
+  if (status == 2) {
+    SolveOptions ro = o;
+    ro.probe_begin = 0;
+    ro.probe_end = 0;
+    if (!numerical_replay_blocks<K>(e, ro, res, scores)) status = 7;
+  }
+  // Counter-V1 words the replay addressed: ceil(copies / 64) per unit and probe
+  uint64_t words = 0;
+  for (uint64_t n : plan.del_count) words += (n + 63) / 64;
+  na.generator_words = words * na.attempted_replay_rhs;
+  finish_numerical(res.target_draws, scores, status, na);
+}
+
 template <int K>
 void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const SolveOptions& o_request,
              SolveResult& res,
@@ -1996,7 +2149,7 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
   auto now = [] { return std::chrono::steady_clock::now(); };
   auto t0 = now();
   // ---- full fit (one column); a phase-2 shard reuses the fit of its phase 1
-  if (o.shard_phase == 2) {
+  if (o.shard_phase == 2 || o.reuse_fit) {
     res.plugin = e.shard_plugin;
   } else {
     BlockWork& w = get_work<1>(e);
@@ -2028,6 +2181,15 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
   if (o.algorithm == 1) {
     if (o.precision == 2) autotune<K>(e, o);
     run_exact<K>(e, p, o, res);
+    if (o.numerical) {
+      // exact leverages leave no Monte Carlo error: the attachment is the zero
+      // covariance with status "exact zero" (numerical_api.rs:431-435)
+      res.numerical = NumericalAttachment{};
+      finalize_covariance(Matrix3{}, Matrix3{}, res.numerical);
+      res.numerical.present = true;
+      res.numerical.exact = true;
+      res.numerical.status = 1;
+    }
     for (auto& r : res.receipts) {
       res.max_reduced_residual = std::max(res.max_reduced_residual, r.reduced_residual);
       res.max_complete_residual = std::max(res.max_complete_residual, r.complete_residual);
@@ -2052,8 +2214,10 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
   }
   if (o.shard_phase == 2) shard_upload(e, o.shard_input);
   // ---- adjustment
+  const double y_mean = outcome_mean(p, o.centering);
+  uint32_t numerical_status = 0;
   {
-    AdjustParams prm{e.C, double(o.probes), o.block_tolerance, o.rank_tolerance, outcome_mean(p, o.centering)};
+    AdjustParams prm{e.C, double(o.probes), o.block_tolerance, o.rank_tolerance, y_mean};
     unsigned long long init[2] = {~0ull, 0ull};
     CK(cudaMemcpyAsync(e.error.p, init, sizeof(init), cudaMemcpyHostToDevice, L.s));
     k_adjust<<<L.grid, THREADS, 0, L.s>>>(prm, e.unit_ptr.p, e.moments.p, e.unit_outcome.p, e.unit_count_f.p,
@@ -2075,6 +2239,12 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
       fail(int32_t(code), "jla_leverage", std::string(what) + " at unit " + std::to_string(g) + ", side joint");
     }
   }
+  if (o.numerical) {
+    numerical_status = numerical_derivative(e, o, res.numerical);
+    if (e.num_cell_fold.n < size_t(e.C) * 6) e.num_cell_fold.alloc(size_t(e.C) * 6);
+    CK(cudaMemsetAsync(e.num_cell_fold.p, 0, size_t(e.C) * 6 * sizeof(double), L.s));
+    if (!e.num_out.p) e.num_out.alloc(6 * 128);
+  }
   auto t2 = now();
   // ---- target
   run_target_blocks<K>(e, o, res);
@@ -2085,6 +2255,7 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
   }
   // ---- components
   finish_draws(res, o.probes);
+  if (o.numerical) numerical_finish<K>(e, plan, o, y_mean, numerical_status, res);
   for (auto& r : res.receipts) {
     res.max_reduced_residual = std::max(res.max_reduced_residual, r.reduced_residual);
     res.max_complete_residual = std::max(res.max_complete_residual, r.complete_residual);
@@ -2199,7 +2370,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
   res.receipts.insert(res.receipts.begin(), e.control_receipts.begin(), e.control_receipts.end());
   const int q = e.q;
   // ---- joint fit: FE solve of y, then beta = S^{-1} R'W y and theta = theta_y - H beta
-  if (o.shard_phase == 2) {
+  if (o.shard_phase == 2 || o.reuse_fit) {
     res.plugin = e.shard_plugin;
   } else {
     BlockWork& w = get_work<1>(e);
@@ -2468,14 +2639,21 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
       if (kernel == 10) *bytes += iters * (nnz * 8 + nseg * 16 + n * 16 + n * K * 4.0 * 3 + 2 * nseg * K * 4.0);
       break;
     case 3:
-      *bytes = double(e.G) * (8 + 8 + (e.observation ? 8 : K * 8)) + double(e.C) * (4 + K * 8);
+      if (e.observation) {  // per unit: rank, count, offset, first copy; per copy: its signs; per cell: the sums
+        if (!e.copy_bits.p) e.copy_bits.alloc(e.physical);
+        *bytes = double(e.G) * 8 * 4 + double(e.physical) * 8 + double(e.C) * (4 + K * 8);
+      } else {
+        *bytes = double(e.G) * (8 + 8 + K * 8) + double(e.C) * (4 + K * 8);
+      }
       break;
     case 4:
-      if (e.observation)  // per row: cell, offsets, rank, two coefficient rows, row sums; per copy: its sums
-        *bytes = double(e.rows) * (4 + 8 + 8 + 8 + 2 * K * 8 + 4 * 8 * 2) + double(e.physical) * 4 * 8 * 2 +
+      if (e.observation) {  // per row: cell, offsets, rank, two coefficient rows, row sums; per copy: signs, sums
+        if (!e.copy_bits.p) e.copy_bits.alloc(e.physical);
+        *bytes = double(e.rows) * (4 + 8 + 8 + 8 + 2 * K * 8 + 4 * 8 * 2) + double(e.physical) * (8 + 4 * 8 * 2) +
                  double(e.C) * 8;
-      else
+      } else {
         *bytes = double(e.G) * (4 + 8 + K * 8 + 5 * 8 * 2) + double(e.G) * 2 * K * 8 + double(e.C) * 8;
+      }
       break;
     default: fail(INVALID_INPUT, "benchmark", "unknown kernel id");
   }
@@ -2536,16 +2714,24 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
       }
 
       case 3:
-        k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p,
-                                                     e.observation ? e.unit_offset.p : nullptr, key,
-                                                         TAG_LEVERAGE, 0, K,
-                                                         e.observation ? nullptr : w.unit_atoms.p, w.cell_val.p);
+        // the atom pass the solver runs (with the copies' signs for leave-observation-out)
+        if (e.observation)
+          k_obs_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p,
+                                                               e.unit_offset.p, e.unit_phys.p, key, 0, K,
+                                                               reinterpret_cast<uint8_t*>(e.copy_bits.p),
+                                                               w.cell_val.p);
+        else
+          k_leverage_atoms<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.unit_ptr.p, e.unit_rank.p, e.unit_count.p,
+                                                           nullptr, key, TAG_LEVERAGE, 0, K, w.unit_atoms.p,
+                                                           w.cell_val.p);
         break;
       case 4:
+        // the moment pass the solver runs (reading the recorded signs)
         if (e.observation)
           k_obs_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.rows, K, e.row_cell.p, e.cell_worker.p, e.cell_firm.p,
                                                         e.row_rank_d.p, e.row_copy_offset.p, e.row_phys.p, key, 0,
-                                                        w.alpha.p, w.x.p, e.obs_row_acc.p, e.obs_copy_acc.p);
+                                                        e.copy_bits.p, w.alpha.p, w.x.p, e.obs_row_acc.p,
+                                                        e.obs_copy_acc.p);
         else
           k_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.G, K, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
                                                     e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.moments.p);

@@ -43,6 +43,14 @@ struct SolveOptions {
   uint32_t probe_begin = 0, probe_end = 0;
   const double* shard_input = nullptr;
   double* shard_output = nullptr;  // phase 1: the caller's accumulator buffer (host or device)
+  // Probe sets: a later set of the same request on the same generation keeps
+  // the fit (plug-in components, fitted cells, residuals) of the first one,
+  // which no probe seed changes.
+  bool reuse_fit = false;
+  // Numerical MCSE attachment (reference `run_jla_no_controls_with_numerical_mc`):
+  // per-unit derivatives after the adjustment, per-unit target folds during the
+  // target phase, and a replay of the leverage probes that scores each one.
+  bool numerical = false;
 };
 
 // One receipt per solved right-hand side (reference `JlaRhsReceipt`,
@@ -68,6 +76,25 @@ struct SolveTimings {
   uint64_t fallbacks = 0;           // learned-preconditioner blocks finished by the Jacobi fallback
 };
 
+// Numerical MCSE attachment of a solve (reference `CompressedNumericalMcResult`,
+// vckss-core/src/engine/numerical.rs:13-34, and `numerical_mc::Covariance`).
+// status: 1 exact zero, 2 local, 3 local after a PSD adjustment, 4 unstable
+// (not PSD), 5 nonsmooth adjustment, 6 nonfinite derivative, 7 replay failed.
+struct NumericalAttachment {
+  bool present = false, exact = false;
+  uint32_t status = 0;
+  double conditional[3][3] = {}, leverage[3][3] = {}, raw[3][3] = {}, usable[3][3] = {};
+  double mcse[4] = {};
+  double psd_adjustment = 0;
+  uint32_t leverage_probes = 0, target_probes = 0, folds[2] = {0, 0};
+  uint64_t attempted_replay_rhs = 0, generator_words = 0, allocation_bound_bytes = 0;
+  uint32_t failed_replay_probe = 0xffffffffu, replay_error_code = 0;
+  double score_means[2][3] = {};
+  double minimum_constrained = 0, minimum_residual_margin = 0, maximum_sensitivity_ratio = 0;
+  std::vector<uint32_t> replay_probe;       // certified replay directions, in order
+  std::vector<double> replay_residual;      // their complete residuals
+};
+
 struct SolveResult {
   Components plugin, correction, corrected, mcse;
   double weighted_rss = 0;
@@ -80,6 +107,7 @@ struct SolveResult {
   double max_reduced_residual = 0, max_complete_residual = 0, max_leverage = 0;
   SolveTimings timings;
   std::vector<double> shard_accumulators;  // phase 1 output
+  NumericalAttachment numerical;
 };
 
 // Number of leverage accumulators a shard exchanges (match units: 5 moment

@@ -25,10 +25,74 @@ __device__ __forceinline__ void neumaier_add(double& sum, double& corr, double v
   sum = t;
 }
 
+// Leverage atoms of the leave-observation-out units (rows in cell order) for
+// a block of K probes that starts at a multiple of four.  Per cell the sum of
+// its rows' atoms (the right-hand side, exact integers), and per physical copy
+// the signs the block's probes draw: bit j of the copy's 64-bit word is set
+// for a +1 draw of probe first + j, so the moment pass reads one word per copy
+// instead of drawing the Philox blocks again (Counter-V1 word of the row's
+// class rank, bit = the copy's number inside its class; the row atom is
+// 2 popcount - copies, as in `rademacher_range_block_sums`).  Thread (cell, q)
+// covers the eight columns 8q .. 8q + 7 (two Philox blocks per copy word) and
+// writes byte q of each copy's word, so the threads of a cell write adjacent
+// bytes.  unit_phys[g] = physical index of unit g's first copy (copies in row
+// order).
+template <int K>
+__global__ void k_obs_leverage_atoms(uint32_t cells, const uint32_t* __restrict__ unit_ptr,
+                                     const uint64_t* __restrict__ unit_rank, const uint64_t* __restrict__ unit_count,
+                                     const uint64_t* __restrict__ unit_offset, const uint64_t* __restrict__ unit_phys,
+                                     PhiloxKey key, uint64_t first, int ncols, uint8_t* __restrict__ copy_bits,
+                                     double* __restrict__ cell_atoms) {
+  constexpr int Q = (K + 7) / 8;
+  const uint64_t pblock0 = first >> 2;
+  size_t total = size_t(cells) * Q;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
+    const uint32_t c = uint32_t(t / Q);
+    const int q = int(t % Q);
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t g = unit_ptr[c]; g < unit_ptr[c + 1]; ++g) {
+      const uint64_t ent = unit_rank[g], off = unit_offset[g], n = unit_count[g], ph = unit_phys[g];
+      int64_t pos[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      uint64_t cp = off;
+      const uint64_t end = off + n;
+      while (cp < end) {
+        const uint64_t word = cp >> 6, lo = cp & 63;
+        uint64_t hi = end - (word << 6);
+        if (hi > 64) hi = 64;
+        const uint64_t mask = (hi == 64 ? ~uint64_t(0) : ((uint64_t(1) << hi) - 1)) & ~((uint64_t(1) << lo) - 1);
+        uint64_t b0[4], b1[4] = {0, 0, 0, 0};
+        philox_block(key, ent, pblock0 + 2 * q, word, TAG_LEVERAGE, b0);
+        if (K > 4) philox_block(key, ent, pblock0 + 2 * q + 1, word, TAG_LEVERAGE, b1);
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+          pos[l] += popcount64(b0[l] & mask);
+          pos[4 + l] += popcount64(b1[l] & mask);
+        }
+        for (uint64_t k = cp; k < (word << 6) + hi; ++k) {
+          const int bit = int(k & 63);
+          uint32_t v = 0;
+#pragma unroll
+          for (int l = 0; l < 4; ++l) v |= uint32_t((b0[l] >> bit) & 1) << l | uint32_t((b1[l] >> bit) & 1) << (4 + l);
+          copy_bits[(ph + (k - off)) * 8 + q] = uint8_t(v);
+        }
+        cp = (word << 6) + hi;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[j] += double(2 * pos[j] - int64_t(n));
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int col = 8 * q + j;
+      if (col < K) cell_atoms[size_t(c) * K + col] = col < ncols ? acc[j] : 0.0;
+    }
+  }
+}
+
 // One probe block of K columns (first a multiple of 4; columns >= ncols carry a
 // zero prediction).  Each lane holds the four columns of one Counter-V1 block
 // (K / 4 lanes per row, 32 / (K / 4) rows per warp), so every Philox block a
-// copy needs is computed once.
+// copy needs is computed once; with copy_bits (the words k_obs_leverage_atoms
+// wrote for this block) the signs are read instead of drawn.
 // row_acc[r][4] = (sum P^2, its compensation, sum P^4, its compensation);
 // copy_acc[c][4] = (sum a P, compensation, sum a P^3, compensation), c the
 // copy's physical index (rows in row order, copies consecutive).
@@ -37,8 +101,9 @@ __global__ void k_obs_moments(uint32_t rows, int ncols, const uint32_t* __restri
                               const uint32_t* __restrict__ cell_worker, const uint32_t* __restrict__ cell_firm,
                               const uint64_t* __restrict__ row_rank, const uint64_t* __restrict__ row_copy_offset,
                               const uint64_t* __restrict__ row_phys, PhiloxKey key, uint64_t first,
-                              const double* __restrict__ alpha, const double* __restrict__ psi,
-                              double* __restrict__ row_acc, double* __restrict__ copy_acc) {
+                              const uint64_t* __restrict__ copy_bits, const double* __restrict__ alpha,
+                              const double* __restrict__ psi, double* __restrict__ row_acc,
+                              double* __restrict__ copy_acc) {
   constexpr int CPL = K >= 4 ? 4 : K;  // columns per lane
   constexpr int LPR = K / CPL;         // lanes per row
   static_assert(K % CPL == 0 && LPR <= 32 && 32 % LPR == 0, "rows must tile a warp");
@@ -95,7 +160,17 @@ __global__ void k_obs_moments(uint32_t rows, int ncols, const uint32_t* __restri
     for (uint64_t i = 0; i < most; ++i) {
       double f1 = 0.0, f3 = 0.0;
       bool mine = live && i < ncopy;
-      if (mine) {
+      if (mine && copy_bits) {
+        // the signs the atom pass recorded: bit c0 + c of the copy's word
+        const uint64_t m = copy_bits[ph + i] >> c0;
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) {
+          double a = ((m >> c) & 1) ? 1.0 : -1.0;
+          double p = P[c];
+          f1 += a * p;
+          f3 += a * p * p * p;
+        }
+      } else if (mine) {
         uint64_t cn = off + i, word = cn >> 6;
         if (word != word_at) {
           uint64_t blk[4];

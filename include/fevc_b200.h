@@ -298,6 +298,43 @@ typedef struct VckssEngineSolveRequestV8 {
   uint32_t tolerance_supplied;
 } VckssEngineSolveRequestV8;
 
+/* Numerical MCSE attachment (reference vckss_rust.h:2335-2388,
+ * vckss-plugin/src/numerical_api.rs:17-100): a V4 point request, and the
+ * covariance of the (worker, firm, covariance) corrections from the target
+ * draws (conditional) and from a replay of the leverage probes (leverage). */
+typedef struct VckssNumericalRequestV1 {
+  uint32_t abi_version, struct_size, schema_version, threads;
+  uint32_t tolerance_supplied, projection_requested, component_requested, reserved;
+  uint32_t controls_count, reserved_2;
+  VckssEngineSolveRequestV4 point;
+} VckssNumericalRequestV1;
+
+typedef struct VckssNumericalRequestV2 {
+  VckssNumericalRequestV1 v1;
+  uint32_t execution_mode, component_batch_mode, full_cmg, reserved;
+} VckssNumericalRequestV2;
+
+typedef struct VckssNumericalResultV1 {
+  uint32_t struct_size, schema_version;
+  uint64_t generation;
+  /* 1 exact zero, 2 local, 3 local after PSD adjustment, 4 unstable (not PSD),
+   * 5 nonsmooth adjustment, 6 nonfinite derivative, 7 replay failed */
+  uint32_t status, engine, leverage_probes, target_probes, target_fold_a, target_fold_b;
+  uint64_t certified_replay_rhs, executed_replay_rhs, attempted_replay_rhs, replay_generator_words,
+      allocation_bound_bytes;
+  uint32_t failed_replay_probe, replay_error_code;
+  double psd_adjustment, minimum_constrained, minimum_residual_margin, maximum_sensitivity_ratio;
+  double score_means[2][3];
+  double conditional[3][3], leverage[3][3], raw[3][3], usable[3][3], mcse[4];
+  uint64_t point_rhs;
+  double maximum_point_complete_residual, maximum_replay_complete_residual;
+} VckssNumericalResultV1;
+
+typedef struct VckssNumericalRhsV1 {
+  uint32_t schema_version, phase, probe, reserved;
+  double complete_residual;
+} VckssNumericalRhsV1;
+
 typedef struct VckssEngineSolveRequestInterruptV8 {
   VckssEngineSolveRequestV8 options;
   VckssInterruptPollV1 interrupt_poll;
@@ -882,6 +919,15 @@ typedef struct FevcbPrepareTimingsV1 {
 int32_t fevcb_engine_prepare_timings_v1(uint64_t generation, FevcbPrepareTimingsV1 *output,
                                         uint32_t output_capacity_bytes);
 
+/* The numerical MCSE attachment's covariance algebra on given matrices (no
+ * solve; host only): conditional and leverage are row-major 3 x 3 in the
+ * order worker, firm, covariance.  Fills status, conditional, leverage, raw,
+ * usable, mcse and psd_adjustment of *output as vckss_rust_engine_numerical_
+ * result_v1 reports them (reference numerical_mc.rs:234-354 `finalize`); the
+ * replay fields stay zero. */
+int32_t fevcb_numerical_finalize_v1(const double *conditional, const double *leverage,
+                                    VckssNumericalResultV1 *output, uint32_t output_capacity_bytes);
+
 /* Ceiling on the identified dimension (W + F - 1) of an exact-estimator solve
  * of this generation (no counterpart in the reference, whose dense estimator
  * refuses limits above 2,000: vckss-core/src/exact_estimator.rs:104-108).
@@ -1320,10 +1366,6 @@ typedef struct VckssGenericExecutionReceiptV2 VckssGenericExecutionReceiptV2;
 typedef struct VckssLeaveoutResidualDiagnosticV1 VckssLeaveoutResidualDiagnosticV1;
 typedef struct VckssMemoryForecastV1 VckssMemoryForecastV1;
 typedef struct VckssMemoryPolicyV1 VckssMemoryPolicyV1;
-typedef struct VckssNumericalRequestV1 VckssNumericalRequestV1;
-typedef struct VckssNumericalRequestV2 VckssNumericalRequestV2;
-typedef struct VckssNumericalResultV1 VckssNumericalResultV1;
-typedef struct VckssNumericalRhsV1 VckssNumericalRhsV1;
 typedef struct VckssPreparationReceiptV1 VckssPreparationReceiptV1;
 typedef struct VckssPrepareRequestV1 VckssPrepareRequestV1;
 typedef int32_t (*VckssProgressOperationV1)(void *);
@@ -1532,6 +1574,12 @@ int32_t vckss_rust_session_snapshot_v1(VckssSessionSnapshotV1 *output);
 
 #if defined(__cplusplus)
 static_assert(sizeof(VckssEnginePrepareRequestV1) == 24, "prepare request V1 layout");
+static_assert(sizeof(VckssNumericalRequestV1) == 328, "numerical request layout");
+static_assert(offsetof(VckssNumericalRequestV1, point) == 40, "numerical point offset");
+static_assert(sizeof(VckssNumericalRequestV2) == 344, "numerical V2 request layout");
+static_assert(sizeof(VckssNumericalResultV1) == 512, "numerical result layout");
+static_assert(offsetof(VckssNumericalResultV1, conditional) == 168, "numerical covariance offset");
+static_assert(sizeof(VckssNumericalRhsV1) == 24, "numerical RHS layout");
 static_assert(sizeof(FevcbCmgSummaryV1) == 688, "CMG summary layout");
 static_assert(sizeof(VckssEngineSolveRequestInterruptV4) == 312, "interrupt V4 solve layout");
 static_assert(sizeof(VckssEngineSolveRequestV8) == 320, "V8 solve layout");

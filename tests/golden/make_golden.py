@@ -418,10 +418,122 @@ def write_exact_cases(lib, meta: dict) -> None:
     (HERE / "exact_cases.json").write_text(json.dumps({"meta": meta, "cases": cases}, indent=1))
 
 
+# The plugin's numerical MCSE attachment (vckss_rust_engine_solve_numerical_v1
+# around a V4 point request, then numerical_result_v1 and numerical_rhs_v1):
+# JLA on the compressed engine at a tight diagonal-PCG tolerance, an odd probe
+# count (unequal target folds), literal frequencies, and the automatic
+# algorithm on a panel within the exact limit (the exact-zero attachment).
+NUMERICAL_PANELS = {
+    "small_2k": dict(build=lambda: generate_panel(2000, 150, 5, move_p=0.2, seed=11), probes=24, algorithm=2),
+    "odd_probes_2k": dict(build=lambda: generate_panel(2000, 150, 5, move_p=0.2, seed=12), probes=15, algorithm=2),
+    "weighted_1500": dict(build=lambda: weighted_panel(5), probes=16, algorithm=2),
+    "pareto13_4k": dict(build=lambda: generate_panel(4000, 200, 6, move_p=0.08, pareto_shape=1.3, seed=3),
+                        probes=20, algorithm=2),
+    "kat12_jla": dict(build=lambda: kat12(), probes=5, algorithm=2),
+    "kat12_auto": dict(build=lambda: kat12(), probes=5, algorithm=0),
+}
+
+NUMERICAL_FIELDS = ("status", "engine", "leverage_probes", "target_probes", "target_fold_a", "target_fold_b",
+                    "certified_replay_rhs", "executed_replay_rhs", "attempted_replay_rhs", "replay_generator_words",
+                    "allocation_bound_bytes", "failed_replay_probe", "replay_error_code", "psd_adjustment",
+                    "minimum_constrained", "minimum_residual_margin", "maximum_sensitivity_ratio", "score_means",
+                    "conditional", "leverage", "raw", "usable", "mcse", "point_rhs")
+
+
+def numerical_request(e, probes: int, algorithm: int):
+    """The numerical-attachment request the fixtures and tests use: a default
+    V5 point with the probes, JLA or the automatic algorithm, diagonal PCG at
+    1e-12 for JLA (the automatic algorithm keeps the automatic route)."""
+    q = e.default_request_v5(1)
+    v1 = q.v4.v3.v2.v1
+    v1.probes = probes
+    v1.pcg_tolerance = 1e-12
+    v1.maximum_iterations = 20000
+    q.v4.v3.v2.algorithm = algorithm
+    if algorithm == 2:
+        v1.solver_route = 2
+    q.threads = 4
+    q.tolerance_supplied = 1
+    return e.numerical_request(q)
+
+
+def numerical_record(lib, panel: Panel, probes: int, algorithm: int) -> dict:
+    e = abi.Engine(lib)
+    e.prepare(panel)
+    e.solve_numerical(numerical_request(e, probes, algorithm))
+    r = e.numerical_result()
+    point = e.result()
+    count, rhs = e.numerical_rhs(int(r["certified_replay_rhs"]))
+    e.release()
+    rec = {k: r[k] for k in NUMERICAL_FIELDS}
+    rec = {k: (str(v) if isinstance(v, float) and not np.isfinite(v) else v) for k, v in rec.items()}
+    rec["corrected"] = list(point["corrected"])
+    rec["rhs"] = [[x["probe"], x["phase"], x["complete_residual"]] for x in rhs]
+    return {"probes": probes, "algorithm": algorithm, "pcg_tolerance": 1e-12, **rec}
+
+
+# Request mutations for the preflight fixture (field path, value).
+NUMERICAL_PREFLIGHT = {
+    "base": [],
+    "schema_2": [("schema_version", 2)],
+    "reserved": [("reserved", 1)],
+    "reserved_2": [("reserved_2", 3)],
+    "tolerance_supplied_2": [("tolerance_supplied", 2)],
+    "threads_0": [("threads", 0)],
+    "probes_1": [("point.v3.v2.v1.probes", 1)],
+    "projection": [("projection_requested", 1)],
+    "component": [("component_requested", 1)],
+    "exact_algorithm": [("point.v3.v2.algorithm", 1)],
+    "exact_route": [("point.v3.v2.v1.solver_route", 1)],
+    "no_rng": [("point.v3.v2.v1.rng_contract", 0)],
+    "bad_signature": [("point.v3.request_signature", 12345)],
+    "engine_compressed": [("point.v3.engine", 1)],
+    "engine_unknown": [("point.v3.engine", 7)],
+    "controls_mismatch": [("controls_count", 2)],
+    "point_reserved": [("point.reserved_4", 1)],
+    "abi_version": [("abi_version", 2)],
+}
+
+
+def _set_path(obj, path: str, value) -> None:
+    *head, last = path.split(".")
+    for h in head:
+        obj = getattr(obj, h)
+    setattr(obj, last, value)
+
+
+def numerical_preflight_record(lib) -> dict:
+    out = {}
+    for name, muts in NUMERICAL_PREFLIGHT.items():
+        e = abi.Engine(lib)
+        req = numerical_request(e, 24, 2)
+        resign = not any(p == "point.v3.request_signature" for p, _ in muts)
+        for path, value in muts:
+            _set_path(req, path, value)
+        if resign and any(p.startswith("point.") or p == "controls_count" for p, _ in muts):
+            if not any(p == "controls_count" for p, _ in muts):
+                req.point.v3.request_signature = abi.capability_signature_v3(req.point, req.controls_count)
+        out[name] = int(lib.vckss_rust_engine_numerical_preflight_v1(C.byref(req)))
+    return out
+
+
+def write_numerical_cases(lib, meta: dict) -> None:
+    cases = {}
+    for name, spec in NUMERICAL_PANELS.items():
+        panel = spec["build"]()
+        cases[name] = {"panel_sha256": panel_digest(panel),
+                       "record": numerical_record(lib, panel, spec["probes"], spec["algorithm"])}
+        print(name, cases[name]["record"]["status"], cases[name]["record"]["mcse"])
+    pre = numerical_preflight_record(lib)
+    print(pre)
+    (HERE / "numerical_cases.json").write_text(json.dumps({"meta": meta, "cases": cases, "preflight": pre},
+                                                          indent=1))
+
+
 def main() -> None:
     """All fixtures; with the argument ``cmg`` only cmg_cases.json, with
     ``receipts`` only receipt_cases.json, with ``sized`` only sized_cases.json, with
-    ``exact`` only exact_cases.json."""
+    ``exact`` only exact_cases.json, with ``numerical`` only numerical_cases.json."""
     if not PLUGIN.exists():
         raise SystemExit(f"reference plugin not found at {PLUGIN}")
     lib = abi.load(PLUGIN, bind_extensions=False)
@@ -432,6 +544,10 @@ def main() -> None:
     if sys.argv[1:] == ["exact"]:
         write_exact_cases(lib, {"generator": "tests/golden/make_golden.py exact", "reference_plugin_version":
                                 lib.vckss_rust_backend_version().decode()})
+        return
+    if sys.argv[1:] == ["numerical"]:
+        write_numerical_cases(lib, {"generator": "tests/golden/make_golden.py numerical",
+                                    "reference_plugin_version": lib.vckss_rust_backend_version().decode()})
         return
     if sys.argv[1:] == ["sized"]:
         write_sized_cases(lib, {"generator": "tests/golden/make_golden.py sized", "reference_plugin_version":
