@@ -183,6 +183,15 @@ class NumericalResultV1(Struct):
         ("maximum_replay_complete_residual", f64)]
 
 
+class ProbeSetV1(Struct):
+    _fields_ = [("seed", u64), ("probes", u32), ("reserved", u32)]
+
+
+class ProbeSetResultV1(Struct):
+    _fields_ = [("plugin", Components), ("correction", Components), ("corrected", Components),
+                ("numerical_mcse", Components)]
+
+
 class NumericalRhsV1(Struct):
     _fields_ = [("schema_version", u32), ("phase", u32), ("probe", u32), ("reserved", u32),
                 ("complete_residual", f64)]
@@ -580,6 +589,7 @@ SIGNATURES = {
     "fevcb_engine_tuning_v1": (i32, [u64, C.c_void_p, u32]),
     "fevcb_engine_prepare_timings_v1": (i32, [u64, C.c_void_p, u32]),
     "fevcb_numerical_finalize_v1": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u32]),
+    "fevcb_engine_solve_sets_v1": (i32, [u64, C.c_void_p, C.c_void_p, u32, C.c_void_p, u32]),
     "vckss_rust_engine_numerical_preflight_v1": (i32, [C.c_void_p]),
     "vckss_rust_engine_numerical_result_v1": (i32, [u64, C.c_void_p, u32]),
     "vckss_rust_engine_numerical_rhs_v1": (i32, [u64, C.c_void_p, u64, C.c_void_p]),
@@ -832,6 +842,17 @@ class Engine:
     def solve_v5(self, req: SolveRequestV5, controls_count: int = 0) -> None:
         req.v4.v3.request_signature = capability_signature_v3(req.v4, controls_count)
         self.check(self.lib.vckss_rust_engine_solve_v5(self.generation, C.byref(req)))
+
+    def solve_sets(self, req: SolveRequestV5, sets: list[tuple[int, int]], controls_count: int = 0) -> list[dict]:
+        """Probe sets (seed, probes) in one call (fevcb_engine_solve_sets_v1);
+        the first set's result becomes the generation's result."""
+        req.v4.v3.request_signature = capability_signature_v3(req.v4, controls_count)
+        arr = (ProbeSetV1 * len(sets))(*[ProbeSetV1(int(s), int(p), 0) for s, p in sets])
+        out = (ProbeSetResultV1 * len(sets))()
+        self.check(self.lib.fevcb_engine_solve_sets_v1(self.generation, C.byref(req), arr, len(sets), out,
+                                                      C.sizeof(out)))
+        return [{k: getattr(o, k).tuple() for k in ("plugin", "correction", "corrected", "numerical_mcse")}
+                for o in out]
 
     def numerical_request(self, point: SolveRequestV5, controls_count: int = 0) -> NumericalRequestV1:
         """A numerical-attachment request around a V5 request's V4 point

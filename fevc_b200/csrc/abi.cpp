@@ -1643,6 +1643,53 @@ int32_t fevcb_engine_resolve_v1(uint64_t generation) {
   });
 }
 
+// Independent probe sets in one call: set 0 is a V5 solve with its seed and
+// probe count (its result becomes the generation's result), every later set
+// runs the leverage and target phases with its own seed and probes on the
+// same device generation, keeping set 0's fit and the autotuned form.
+int32_t fevcb_engine_solve_sets_v1(uint64_t generation, const VckssEngineSolveRequestV5* request,
+                                   const FevcbProbeSetV1* sets, uint32_t count, FevcbProbeSetResultV1* results,
+                                   uint32_t results_capacity_bytes) {
+  return status([&] {
+    auto q = read_struct(request, "V5 engine solve request");
+    if (count == 0 || !sets) fail(INVALID_INPUT, "probe_sets", "at least one probe set is required");
+    if (count > 4096) fail(RESOURCE_LIMIT, "probe_sets", "at most 4096 probe sets per call");
+    if (!results || uint64_t(results_capacity_bytes) < uint64_t(count) * sizeof(FevcbProbeSetResultV1))
+      fail(ABI_MISMATCH, "engine_ffi", "probe-set results destination is null or short");
+    std::vector<FevcbProbeSetV1> set(sets, sets + count);
+    for (const auto& st : set) {
+      if (st.reserved != 0) fail(ABI_MISMATCH, "engine_ffi", "reserved probe-set fields must be zero");
+      if (st.probes < 2) fail(INVALID_INPUT, "jla_validate", "JLA probe count must be at least two");
+    }
+    const SolveOptions base = options_from_v5(q);
+    if (base.algorithm == 1) fail(UNSUPPORTED_FEATURE, "probe_sets", "probe sets need the JLA algorithm");
+    auto put = [&](uint32_t i, const SolveResult& res) {
+      FevcbProbeSetResultV1 v{};
+      v.plugin = {res.plugin.worker, res.plugin.firm, res.plugin.covariance, res.plugin.total};
+      v.correction = {res.correction.worker, res.correction.firm, res.correction.covariance, res.correction.total};
+      v.corrected = {res.corrected.worker, res.corrected.firm, res.corrected.covariance, res.corrected.total};
+      v.numerical_mcse = {res.mcse.worker, res.mcse.firm, res.mcse.covariance, res.mcse.total};
+      std::memcpy(results + i, &v, sizeof(v));
+    };
+    SolveOptions first = base;
+    first.seed = set[0].seed;
+    first.probes = set[0].probes;
+    solve_common(generation, first, Interrupt{}, true, &q.v4, 5);
+    Registry& r = reg();
+    std::lock_guard<std::mutex> l(r.mu);
+    Prepared& p = r.require(generation, "probe_sets");
+    put(0, *r.result);
+    for (uint32_t i = 1; i < count; ++i) {
+      SolveOptions o = p.last_options;
+      o.seed = set[i].seed;
+      o.probes = set[i].probes;
+      o.reuse_fit = true;
+      SolveResult res = device_solve(*p.device, p.problem, p.plan, o, false);
+      put(i, res);
+    }
+  });
+}
+
 int32_t fevcb_engine_unit_detail_v1(uint64_t generation, uint64_t units, double* projection_share,
                                     double* residual_share, double* finite_bias, double* finite_variance,
                                     double* residual_mass, double* deleted_mass, uint64_t cells, double* fitted_cell,

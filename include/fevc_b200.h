@@ -919,6 +919,29 @@ typedef struct FevcbPrepareTimingsV1 {
 int32_t fevcb_engine_prepare_timings_v1(uint64_t generation, FevcbPrepareTimingsV1 *output,
                                         uint32_t output_capacity_bytes);
 
+/* Independent probe sets on one prepared generation in one call (no
+ * counterpart in the reference, which draws one seed per solve): set 0 is the
+ * V5 request solved with that set's seed and probe count, and its result
+ * becomes the generation's result (engine_result_v1, receipts); each later
+ * set runs the leverage and target probes of its own seed and count on the
+ * same device generation, keeping set 0's fit (which no seed changes) and
+ * the solver form chosen for the generation.  results[i] equals what a
+ * separate V5 solve of set i returns.  At most 4096 sets per call. */
+typedef struct FevcbProbeSetV1 {
+  uint64_t seed;
+  uint32_t probes;
+  uint32_t reserved;
+} FevcbProbeSetV1;
+typedef struct FevcbProbeSetResultV1 {
+  VckssComponentVectorV1 plugin;
+  VckssComponentVectorV1 correction;
+  VckssComponentVectorV1 corrected;
+  VckssComponentVectorV1 numerical_mcse;
+} FevcbProbeSetResultV1;
+int32_t fevcb_engine_solve_sets_v1(uint64_t generation, const VckssEngineSolveRequestV5 *request,
+                                   const FevcbProbeSetV1 *sets, uint32_t count, FevcbProbeSetResultV1 *results,
+                                   uint32_t results_capacity_bytes);
+
 /* The numerical MCSE attachment's covariance algebra on given matrices (no
  * solve; host only): conditional and leverage are row-major 3 x 3 in the
  * order worker, firm, covariance.  Fills status, conditional, leverage, raw,
