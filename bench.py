@@ -571,10 +571,13 @@ def main():
     roof_kernel = {10: f"k_pcg_flex<{block}, float, true>", 9: f"k_pcg_flex<{block}, float, false>",
                    1: f"k_pcg_persistent<{block}, double, 1, 1>"}[roof_mode]
     traffic = None
+    traffic_note = None
     try:
-        rec = json.loads((ROOT / "profiles" / "roofline_traffic.json").read_text()).get(roof_kernel)
-        if rec and rec.get("workload") == args.workload and args.scale == rec.get("scale", 1.0):
-            traffic = float(rec["bytes_per_launch"])
+        recs = json.loads((ROOT / "profiles" / "roofline_traffic.json").read_text()).get(roof_kernel) or []
+        for rec in recs if isinstance(recs, list) else [recs]:
+            if rec.get("workload") == args.workload and args.scale == rec.get("scale", 1.0):
+                traffic = float(rec["bytes_per_launch"])
+                traffic_note = rec.get("source")
     except Exception:
         pass
     achieved = roof_bytes / (roof_ms / 1000.0) / 1e9
@@ -636,7 +639,7 @@ def main():
             "prepare_phases_s": {k.replace("_ms", ""): v for k, v in prepare_phases.items()},
             "first_solve_s": round(first_solve_s, 3),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_source": traffic_note,
                          "kernel": roof_kernel + " (20 iterations per launch, L2 flushed before each)",
                          "bytes_per_launch": roof_bytes, "ms_per_launch": round(roof_ms, 5),
                          "peak_source": peak_source,
