@@ -1594,11 +1594,15 @@ void run_leverage(DeviceEngine& e, const SolveOptions& o, SolveResult& res, uint
     leverage_rhs<K>(e, w, L, key, first, ncols);
     res.timings.kernel_launches += 4;
     BlockOutcome bo = solve_block<K>(e, w, ncols, o, res.timings);
-    if (e.observation)
+    if (e.observation && shared_signs(e, first))
+      k_obs_moments_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, ncols, e.unit_ptr.p, e.cell_rows.p, e.cell_worker.p,
+                                                          e.cell_firm.p, e.unit_phys.p, e.unit_count.p,
+                                                          e.copy_bits.p, w.alpha.p, w.x.p, e.obs_row_acc.p,
+                                                          e.obs_copy_acc.p);
+    else if (e.observation)
       k_obs_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.rows, ncols, e.row_cell.p, e.cell_worker.p, e.cell_firm.p,
                                                     e.row_rank_d.p, e.row_copy_offset.p, e.row_phys.p, key, first,
-                                                    shared_signs(e, first) ? e.copy_bits.p : nullptr, w.alpha.p,
-                                                    w.x.p, e.obs_row_acc.p, e.obs_copy_acc.p);
+                                                    nullptr, w.alpha.p, w.x.p, e.obs_row_acc.p, e.obs_copy_acc.p);
     else
       k_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.G, ncols, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
                                                 e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.moments.p);
@@ -1753,19 +1757,24 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
 // than K.  Every column is its own PCG, so the results do not depend on the
 // width a column is solved at; a narrow last block costs a fraction of a
 // full-width one.
-inline int tail_width(uint32_t cols, int K) {
+inline int tail_width(uint32_t cols, int K, int narrowest = 8) {
   for (int k : {8, 16, 32})
-    if (k < K && uint32_t(k) >= cols) return k;
+    if (k >= narrowest && k < K && uint32_t(k) >= cols) return k;
   return 0;
 }
+
+// The narrowest tail width of a form: the single-kernel solve holds 32 or 64
+// columns, so the tails of its forms stay at 32 instead of falling back to
+// the FP64 Jacobi kernel at 8 or 16.
+inline int narrowest_width(const DeviceEngine& e, const SolveOptions& o) { return flex_form(e, o) ? 32 : 8; }
 
 // Splits [probe_begin, probe_end) into the full blocks of `per` probes and
 // the rest; `tail` is the width for the rest (0: run it all at width K).
 inline bool split_probes(const SolveOptions& o, uint32_t per, int K, int cols_per_probe, SolveOptions& head,
-                         SolveOptions& tail, int& width) {
+                         SolveOptions& tail, int& width, int narrowest = 8) {
   const uint32_t begin = o.probe_begin, end = o.probe_end ? o.probe_end : o.probes;
   const uint32_t full = end > begin ? (end - begin) / per * per : 0, rest = end > begin ? end - begin - full : 0;
-  width = rest ? tail_width(rest * uint32_t(cols_per_probe), K) : 0;
+  width = rest ? tail_width(rest * uint32_t(cols_per_probe), K, narrowest) : 0;
   if (!width) return false;
   head = o;
   tail = o;
@@ -1779,7 +1788,7 @@ template <int K>
 void run_leverage_blocks(DeviceEngine& e, const SolveOptions& o, SolveResult& res) {
   SolveOptions head, tail;
   int width = 0;
-  if (K < 16 || !split_probes(o, K, K, 1, head, tail, width)) {
+  if (K < 16 || !split_probes(o, K, K, 1, head, tail, width, narrowest_width(e, o))) {
     run_leverage<K>(e, o, res, 0);
     return;
   }
@@ -1795,7 +1804,7 @@ template <int K>
 void run_target_blocks(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double y_center = 0.0) {
   SolveOptions head, tail;
   int width = 0;
-  if (K < 16 || !split_probes(o, K / 2, K, 2, head, tail, width)) {
+  if (K < 16 || !split_probes(o, K / 2, K, 2, head, tail, width, narrowest_width(e, o))) {
     run_target<K>(e, o, res, y_center);
     return;
   }
@@ -2096,7 +2105,7 @@ bool numerical_replay_blocks(DeviceEngine& e, const SolveOptions& o, SolveResult
                              std::vector<Primitive> (&scores)[2]) {
   SolveOptions head, tail;
   int width = 0;
-  if (K < 16 || !split_probes(o, K, K, 1, head, tail, width)) return numerical_replay<K>(e, o, res, scores);
+  if (K < 16 || !split_probes(o, K, K, 1, head, tail, width, narrowest_width(e, o))) return numerical_replay<K>(e, o, res, scores);
   if (head.probe_end > head.probe_begin && !numerical_replay<K>(e, head, res, scores)) return false;
   switch (width) {
     case 8: return numerical_replay<8>(e, tail, res, scores);
@@ -2647,10 +2656,11 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
       }
       break;
     case 4:
-      if (e.observation) {  // per row: cell, offsets, rank, two coefficient rows, row sums; per copy: signs, sums
+      if (e.observation) {  // per cell: worker, firm, unit pointer, two coefficient rows; per row: its index,
+                            // first copy, copies, row sums; per copy: signs, sums (k_obs_moments_cells)
         if (!e.copy_bits.p) e.copy_bits.alloc(e.physical);
-        *bytes = double(e.rows) * (4 + 8 + 8 + 8 + 2 * K * 8 + 4 * 8 * 2) + double(e.physical) * (8 + 4 * 8 * 2) +
-                 double(e.C) * 8;
+        *bytes = double(e.C) * (8 + 4 + 2 * K * 8) + double(e.rows) * (4 + 8 + 8 + 4 * 8 * 2) +
+                 double(e.physical) * (8 + 4 * 8 * 2);
       } else {
         *bytes = double(e.G) * (4 + 8 + K * 8 + 5 * 8 * 2) + double(e.G) * 2 * K * 8 + double(e.C) * 8;
       }
@@ -2728,10 +2738,10 @@ void kernel_benchmark_k(DeviceEngine& e, int kernel, int launches, double* ms, d
       case 4:
         // the moment pass the solver runs (reading the recorded signs)
         if (e.observation)
-          k_obs_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.rows, K, e.row_cell.p, e.cell_worker.p, e.cell_firm.p,
-                                                        e.row_rank_d.p, e.row_copy_offset.p, e.row_phys.p, key, 0,
-                                                        e.copy_bits.p, w.alpha.p, w.x.p, e.obs_row_acc.p,
-                                                        e.obs_copy_acc.p);
+          k_obs_moments_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, K, e.unit_ptr.p, e.cell_rows.p, e.cell_worker.p,
+                                                              e.cell_firm.p, e.unit_phys.p, e.unit_count.p,
+                                                              e.copy_bits.p, w.alpha.p, w.x.p, e.obs_row_acc.p,
+                                                              e.obs_copy_acc.p);
         else
           k_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.G, K, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
                                                     e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.moments.p);

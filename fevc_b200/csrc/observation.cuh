@@ -205,6 +205,99 @@ __global__ void k_obs_moments(uint32_t rows, int ncols, const uint32_t* __restri
   }
 }
 
+// The same moments over cells, with the block's signs read from copy_bits
+// (k_obs_leverage_atoms wrote them): one warp per cell.  The rows of a cell
+// share its prediction P = alpha_w + psi_f, so P is loaded once per cell, every
+// row of the cell gets the same (sum P^2, sum P^4), and each copy's (sum a P,
+// sum a P^3) comes from its sign word (bit j: column j drew +1).  Lane l holds
+// columns l*CPT ..; the warp's sums are fixed xor trees, so the result is
+// deterministic.  Units are the cell's rows in cell order (unit_ptr), with
+// cell_rows[u] the row of unit u, unit_phys[u] its first copy and
+// unit_count[u] its copies.
+template <int K>
+__global__ void __launch_bounds__(THREADS) k_obs_moments_cells(
+    uint32_t cells, int ncols, const uint32_t* __restrict__ unit_ptr, const uint32_t* __restrict__ cell_rows,
+    const uint32_t* __restrict__ cell_worker, const uint32_t* __restrict__ cell_firm,
+    const uint64_t* __restrict__ unit_phys, const uint64_t* __restrict__ unit_count,
+    const uint64_t* __restrict__ copy_bits, const double* __restrict__ alpha, const double* __restrict__ psi,
+    double* __restrict__ row_acc, double* __restrict__ copy_acc) {
+  constexpr int CPT = Cols<K>::CPT;
+  constexpr int LANES = K / CPT;  // lanes that hold columns
+  static_assert(LANES <= 32, "one warp per cell");
+  const int lane = threadIdx.x & 31;
+  const int c0 = lane * CPT;
+  const size_t warp = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const size_t nw = (size_t(gridDim.x) * blockDim.x) >> 5;
+  for (size_t c = warp; c < cells; c += nw) {
+    const uint32_t u0 = unit_ptr[c], u1 = unit_ptr[c + 1];
+    const uint32_t cnt = u1 - u0;
+    // the cell's units, lane-parallel: first copy, copies and its sign word
+    uint64_t my_ph = 0, my_n = 0, my_bits = 0;
+    uint32_t my_row = 0;
+    if (uint32_t(lane) < cnt) {
+      my_ph = unit_phys[u0 + lane];
+      my_n = unit_count[u0 + lane];
+      my_row = cell_rows[u0 + lane];
+      my_bits = my_n ? copy_bits[my_ph] : 0;
+    }
+    const size_t wi = size_t(cell_worker[c]) * K, fi = size_t(cell_firm[c]) * K;
+    double P[CPT], s2 = 0.0, s4 = 0.0;
+#pragma unroll
+    for (int q = 0; q < CPT; ++q) {
+      const int col = c0 + q;
+      P[q] = (lane < LANES && col < ncols) ? alpha[wi + col] + psi[fi + col] : 0.0;
+      const double p2 = P[q] * P[q];
+      s2 += p2;
+      s4 += p2 * p2;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      s4 += __shfl_xor_sync(0xffffffffu, s4, o);
+    }
+    // row sums: every row of the cell, one lane each
+    for (uint32_t u = u0 + uint32_t(lane); u < u1; u += 32) {
+      const uint32_t r = uint32_t(u - u0) < 32 ? my_row : cell_rows[u];
+      double* a = row_acc + size_t(r) * 4;
+      neumaier_add(a[0], a[1], s2);
+      neumaier_add(a[2], a[3], s4);
+    }
+    // copies, unit after unit (the whole warp on each copy's columns)
+    for (uint32_t u = 0; u < cnt; ++u) {
+      uint64_t ph, n, bits;
+      if (u < 32) {
+        ph = __shfl_sync(0xffffffffu, my_ph, int(u));
+        n = __shfl_sync(0xffffffffu, my_n, int(u));
+        bits = __shfl_sync(0xffffffffu, my_bits, int(u));
+      } else {
+        ph = unit_phys[u0 + u];
+        n = unit_count[u0 + u];
+        bits = n ? copy_bits[ph] : 0;
+      }
+      for (uint64_t i = 0; i < n; ++i) {
+        const uint64_t m = (i == 0 ? bits : copy_bits[ph + i]) >> c0;
+        double f1 = 0.0, f3 = 0.0;
+#pragma unroll
+        for (int q = 0; q < CPT; ++q) {
+          const double a = ((m >> q) & 1) ? 1.0 : -1.0;
+          f1 += a * P[q];
+          f3 += a * P[q] * P[q] * P[q];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+          f3 += __shfl_xor_sync(0xffffffffu, f3, o);
+        }
+        if (lane == 0) {
+          double* a = copy_acc + size_t(ph + i) * 4;
+          neumaier_add(a[0], a[1], f1);
+          neumaier_add(a[2], a[3], f3);
+        }
+      }
+    }
+  }
+}
+
 // Analytic control leverage of one copy of each row, R_r' S^{-1} R_r, clipped
 // at zero; below -100 rank_tolerance or nonfinite is a moment failure
 // (reference `control_geometry`, generic_jla.rs:4493-4523).
