@@ -1481,39 +1481,48 @@ static void build_observation_units(const Compressed& p, const std::vector<doubl
   std::vector<size_t> cell_begin;
   std::vector<uint32_t> order = rows_by_cell(p, cell_begin);
   sort_within_cells(order, cell_begin, [&](uint32_t a, uint32_t b) { return sem(a, b) < 0; });
+  // class starts: the rows whose semantic key differs from the previous row's
+  // (compared on all host cores); rank = 1 + the class index
+  std::vector<uint8_t> first(R);
+#pragma omp parallel for schedule(static) if (R >= 65536)
+  for (size_t i = 0; i < R; ++i) first[i] = i == 0 || sem(order[i - 1], order[i]) != 0;
+  const std::vector<uint64_t> starts = active_indices(first);
+  const size_t classes = starts.size();
   plan.row_rank.assign(R, 0);
-  uint64_t current = 0;
-  for (size_t i = 0; i < R; ++i) {
-    if (i == 0 || sem(order[i - 1], order[i]) != 0) ++current;
-    plan.row_rank[order[i]] = current;
-  }
-  // classes: rows sorted by (rank, row); the stable sort above already holds
-  // equal ranks in row order
   plan.row_copy_offset.assign(R, 0);
-  plan.group_ptr.assign(1, 0);
+  plan.group_ptr.assign(classes + 1, 0);
   plan.group_rows.assign(order.begin(), order.end());
-  for (size_t i = 0; i < R;) {
-    size_t j = i;
+  plan.del_cell.assign(classes, 0);
+  plan.del_count.assign(classes, 0);
+  plan.del_rank.assign(classes, 0);
+  plan.del_outcome_sum.assign(classes, 0.0);
+  plan.del_target_mass.assign(classes, 0.0);
+  std::atomic<bool> bad{false};
+  // classes: rows sorted by (rank, row); the stable sort above already holds
+  // equal ranks in row order.  Every class is summed in row order by one
+  // thread, so the sums do not depend on the thread count.
+#pragma omp parallel for schedule(dynamic, 4096) if (classes >= 65536)
+  for (size_t k = 0; k < classes; ++k) {
+    const size_t i = starts[k], j = k + 1 < classes ? starts[k + 1] : R;
     uint64_t phys = 0;
     StableSum y, t;
-    while (j < R && plan.row_rank[order[j]] == plan.row_rank[order[i]]) {
-      uint32_t r = order[j];
+    for (size_t u = i; u < j; ++u) {
+      const uint32_t r = order[u];
+      plan.row_rank[r] = k + 1;
       plan.row_copy_offset[r] = phys;
       phys += p.frequency[r];
       y.add(double(p.frequency[r]) * p.outcome[r]);
       t.add(p.target[r]);
-      ++j;
     }
-    if (phys == 0 || (phys + 63) / 64 > (uint64_t(1) << 20))
-      fail(RESOURCE_LIMIT, "generic_jla_rng_preflight", "observation class has an invalid physical trial count");
-    plan.group_ptr.push_back(j);
-    plan.del_cell.push_back(p.row_cell[order[i]]);
-    plan.del_count.push_back(phys);
-    plan.del_rank.push_back(plan.row_rank[order[i]]);
-    plan.del_outcome_sum.push_back(y.finish());
-    plan.del_target_mass.push_back(t.finish());
-    i = j;
+    if (phys == 0 || (phys + 63) / 64 > (uint64_t(1) << 20)) bad = true;
+    plan.group_ptr[k + 1] = j;
+    plan.del_cell[k] = p.row_cell[order[i]];
+    plan.del_count[k] = phys;
+    plan.del_rank[k] = k + 1;
+    plan.del_outcome_sum[k] = y.finish();
+    plan.del_target_mass[k] = t.finish();
   }
+  if (bad) fail(RESOURCE_LIMIT, "generic_jla_rng_preflight", "observation class has an invalid physical trial count");
 }
 
 JlaPlan build_generic_plan(const Compressed& p, Deletion deletion) {
@@ -1604,30 +1613,41 @@ void build_target_strata(const Compressed& p, const std::vector<double>& per_cop
     if (c) return c < 0;
     return plan.row_rank[a] < plan.row_rank[b];
   });
-  for (size_t cur = 0; cur < R;) {
-    size_t begin = cur;
-    uint32_t cell = p.row_cell[tord[cur]];
-    double pc = canonical_zero(per_copy[tord[cur]]);
-    uint64_t bits;
-    std::memcpy(&bits, &pc, 8);
+  // strata: runs of equal (cell, per-copy mass bits), found on all host cores;
+  // each stratum is summed in order by one thread
+  auto bits_of = [&](uint32_t r) {
+    const double v = canonical_zero(per_copy[r]);
+    uint64_t b;
+    std::memcpy(&b, &v, 8);
+    return b;
+  };
+  std::vector<uint8_t> first(R);
+#pragma omp parallel for schedule(static) if (R >= 65536)
+  for (size_t i = 0; i < R; ++i)
+    first[i] = i == 0 || p.row_cell[tord[i]] != p.row_cell[tord[i - 1]] || bits_of(tord[i]) != bits_of(tord[i - 1]);
+  const std::vector<uint64_t> starts = active_indices(first);
+  const size_t S = starts.size();
+  plan.tgt_cell.assign(S, 0);
+  plan.tgt_per_copy.assign(S, 0.0);
+  plan.tgt_count.assign(S, 0);
+  plan.tgt_mass.assign(S, 0.0);
+  plan.tgt_rank.assign(S, 0);
+#pragma omp parallel for schedule(dynamic, 4096) if (S >= 65536)
+  for (size_t k = 0; k < S; ++k) {
+    const size_t b = starts[k], e = k + 1 < S ? starts[k + 1] : R;
     uint64_t phys = 0, ent = ~uint64_t(0);
     StableSum t;
-    while (cur < R) {
-      double v = canonical_zero(per_copy[tord[cur]]);
-      uint64_t vb;
-      std::memcpy(&vb, &v, 8);
-      if (p.row_cell[tord[cur]] != cell || vb != bits) break;
-      phys += p.frequency[tord[cur]];
-      t.add(p.target[tord[cur]]);
-      ent = std::min(ent, plan.row_rank[tord[cur]]);
-      ++cur;
+    for (size_t u = b; u < e; ++u) {
+      const uint32_t r = tord[u];
+      phys += p.frequency[r];
+      t.add(p.target[r]);
+      ent = std::min(ent, plan.row_rank[r]);
     }
-    (void)begin;
-    plan.tgt_cell.push_back(cell);
-    plan.tgt_per_copy.push_back(pc);
-    plan.tgt_count.push_back(phys);
-    plan.tgt_mass.push_back(t.finish());
-    plan.tgt_rank.push_back(ent);
+    plan.tgt_cell[k] = p.row_cell[tord[b]];
+    plan.tgt_per_copy[k] = canonical_zero(per_copy[tord[b]]);
+    plan.tgt_count[k] = phys;
+    plan.tgt_mass[k] = t.finish();
+    plan.tgt_rank[k] = ent;
   }
 }
 
