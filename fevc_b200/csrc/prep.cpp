@@ -980,6 +980,13 @@ std::vector<uint8_t> select_observation_graph(const Canonical& in, GraphReceipt&
     if (degree[in.coord_worker[c]] == 1) leaf_firm[in.coord_worker[c]] = in.coord_firm[c];
   Graph g;
   std::vector<uint32_t> edge_worker;  // worker of each traversed edge
+  // The repeated component and articulation passes run on a copy of the
+  // graph whose vertices are numbered in breadth-first order and whose edges
+  // are numbered in the order that traversal first meets them, so the passes
+  // walk their per-vertex and per-edge state nearly in sequence.  vnew maps a
+  // vertex (worker w, firm W + f) to its number in the copy.  Components,
+  // articulation points and their counts do not depend on the numbering.
+  std::vector<uint32_t> vnew;
   {
     std::vector<uint32_t> eu, ev;
     for (size_t c = 0; c < in.coord_worker.size(); ++c)
@@ -987,8 +994,39 @@ std::vector<uint8_t> select_observation_graph(const Canonical& in, GraphReceipt&
         eu.push_back(in.coord_worker[c]);
         ev.push_back(uint32_t(W + in.coord_firm[c]));
       }
-    edge_worker = eu;
-    g = make_graph(W + in.firms, eu, ev);
+    const size_t n = W + in.firms, E = eu.size();
+    Graph g0 = make_graph(n, eu, ev);
+    vnew.assign(n, MISSING);
+    std::vector<uint32_t> enew(E, MISSING), queue;
+    queue.reserve(n);
+    uint32_t nv = 0, ne = 0;
+    for (size_t root = 0; root < n; ++root) {
+      if (vnew[root] != MISSING || g0.ptr[root] == g0.ptr[root + 1]) continue;
+      vnew[root] = nv++;
+      queue.clear();
+      queue.push_back(uint32_t(root));
+      for (size_t h = 0; h < queue.size(); ++h) {
+        const uint32_t v = queue[h];
+        for (uint64_t a = g0.ptr[v]; a < g0.ptr[v + 1]; ++a) {
+          const Arc arc = g0.arc[a];
+          if (enew[arc.edge] == MISSING) enew[arc.edge] = ne++;
+          if (vnew[arc.to] == MISSING) {
+            vnew[arc.to] = nv++;
+            queue.push_back(arc.to);
+          }
+        }
+      }
+    }
+    for (size_t v = 0; v < n; ++v)
+      if (vnew[v] == MISSING) vnew[v] = nv++;  // vertices without a traversed edge
+    std::vector<uint32_t> eu2(E), ev2(E);
+    edge_worker.assign(E, 0);
+    for (size_t e = 0; e < E; ++e) {
+      eu2[enew[e]] = vnew[eu[e]];
+      ev2[enew[e]] = vnew[ev[e]];
+      edge_worker[enew[e]] = eu[e];
+    }
+    g = make_graph(n, eu2, ev2);
   }
   std::vector<uint8_t> wact(W, 0), on(edge_worker.size(), 0);
   for (size_t w = 0; w < W; ++w) wact[w] = wrows[w] > 0;
@@ -1008,27 +1046,29 @@ std::vector<uint8_t> select_observation_graph(const Canonical& in, GraphReceipt&
   // `largest_component` on the active workers: (firm count, physical mass)
   auto component = [&](size_t& comps) {
     mark();
-    std::vector<uint32_t> label(g.nodes, MISSING), queue;
+    std::vector<uint32_t> label2(g.nodes, MISSING), queue;
     queue.reserve(g.nodes);
     comps = 0;
     for (size_t root = 0; root < g.nodes; ++root) {
-      if (label[root] != MISSING) continue;
+      if (label2[root] != MISSING) continue;
       bool has_edge = false;
       for (uint64_t a = g.ptr[root]; a < g.ptr[root + 1] && !has_edge; ++a) has_edge = on[g.arc[a].edge];
       if (!has_edge) continue;
-      label[root] = uint32_t(comps);
+      label2[root] = uint32_t(comps);
       queue.clear();
       queue.push_back(uint32_t(root));
       for (size_t h = 0; h < queue.size(); ++h) {
         uint32_t v = queue[h];
         for (uint64_t a = g.ptr[v]; a < g.ptr[v + 1]; ++a)
-          if (on[g.arc[a].edge] && label[g.arc[a].to] == MISSING) {
-            label[g.arc[a].to] = uint32_t(comps);
+          if (on[g.arc[a].edge] && label2[g.arc[a].to] == MISSING) {
+            label2[g.arc[a].to] = uint32_t(comps);
             queue.push_back(g.arc[a].to);
           }
       }
       ++comps;
     }
+    std::vector<uint32_t> label(g.nodes);
+    for (size_t v = 0; v < g.nodes; ++v) label[v] = label2[vnew[v]];
     for (size_t w = 0; w < W; ++w)
       if (wact[w] && degree[w] == 1) {
         uint32_t& fl = label[W + leaf_firm[w]];
@@ -1089,9 +1129,9 @@ std::vector<uint8_t> select_observation_graph(const Canonical& in, GraphReceipt&
       continue;
     }
     mark();
-    std::vector<uint8_t> art;
-    tarjan(g, &art, nullptr, &on);
-    art.resize(W);
+    std::vector<uint8_t> art2, art(W);
+    tarjan(g, &art2, nullptr, &on);
+    for (size_t w = 0; w < W; ++w) art[w] = art2[vnew[w]];
     size_t arts = count_true(art);
     if (arts == 0) break;
     for (size_t w = 0; w < W; ++w)
