@@ -680,9 +680,10 @@ GroupIndex grouped_rows(size_t groups, const std::vector<uint32_t>& row_group) {
     gi.ptr[g + 1]++;
   }
   for (size_t g = 0; g < groups; ++g) gi.ptr[g + 1] += gi.ptr[g];
+  const size_t R = row_group.size();
   std::vector<uint64_t> cur(gi.ptr.begin(), gi.ptr.end() - 1);
-  gi.items.resize(row_group.size());
-  for (size_t r = 0; r < row_group.size(); ++r) gi.items[cur[row_group[r]]++] = uint32_t(r);
+  gi.items.resize(R);
+  for (size_t r = 0; r < R; ++r) gi.items[cur[row_group[r]]++] = uint32_t(r);
   return gi;
 }
 
@@ -1210,8 +1211,13 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
   // cell boundaries in the sorted order, then every cell's Kahan sums (in row
   // order, as a sequential walk would take them) independently
   std::vector<size_t> cell_start;
-  for (size_t i = 0; i < R; ++i)
-    if (i == 0 || key[order[i]] != key[order[i - 1]]) cell_start.push_back(i);
+  {
+    std::vector<uint8_t> first(R);
+#pragma omp parallel for schedule(static) if (R >= 65536)
+    for (size_t i = 0; i < R; ++i) first[i] = i == 0 || key[order[i]] != key[order[i - 1]];
+    const std::vector<uint64_t> at = active_indices(first);
+    cell_start.assign(at.begin(), at.end());
+  }
   const size_t NC = cell_start.size();
   cell_start.push_back(R);
   p.cell_worker.resize(NC);
@@ -1294,12 +1300,20 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
                            [&](uint32_t a, uint32_t b) { return cmp(a, b) < 0; });
     }
     p.row_target.assign(R, MISSING);
-    uint32_t current = 0;
-    for (size_t i = 0; i < R; ++i) {
-      if (i > 0 && cmp(tord[i - 1], tord[i]) != 0) ++current;
-      p.row_target[tord[i]] = current;
+    {
+      // stratum starts compared on all host cores, then every row's stratum
+      std::vector<uint8_t> first(R);
+#pragma omp parallel for schedule(static) if (R >= 65536)
+      for (size_t i = 0; i < R; ++i) first[i] = i == 0 || cmp(tord[i - 1], tord[i]) != 0;
+      const std::vector<uint64_t> starts = active_indices(first);
+      const size_t S = starts.size();
+#pragma omp parallel for schedule(static) if (S >= 65536)
+      for (size_t k = 0; k < S; ++k) {
+        const size_t e = k + 1 < S ? starts[k + 1] : R;
+        for (size_t i = starts[k]; i < e; ++i) p.row_target[tord[i]] = uint32_t(k);
+      }
+      p.exact_target_strata = S;
     }
-    p.exact_target_strata = size_t(current) + 1;
     p.target_index = grouped_from_order(p.exact_target_strata, p.row_target, std::move(tord));
   }
   p.deletion_index = grouped_rows(D, p.row_deletion);
