@@ -2172,9 +2172,10 @@ void numerical_solve(uint64_t g, const VckssNumericalRequestV1& q, const Interru
       o.algorithm = 1;
       o.exact_limit = q.point.v3.v2.exact_estimator_limit;
       o.blocksize_limit = q.point.v3.v2.blocksize_limit ? q.point.v3.v2.blocksize_limit : 5000;
-    } else if (p.has_plan && p.plan.generic) {
+    } else if (p.has_plan && p.plan.generic && !p.plan.observation) {
       fail(UNSUPPORTED_FEATURE, "numerical_preflight",
-           "the device numerical attachment covers the compressed engine (match deletion without controls)");
+           "the device numerical attachment covers the compressed engine and leave-observation-out deletion; "
+           "match deletion with controls is not provided");
     }
   }
   o.numerical = true;
@@ -2222,7 +2223,7 @@ int32_t vckss_rust_engine_numerical_result_v1(uint64_t generation, VckssNumerica
     v.schema_version = 1;
     v.generation = generation;
     v.status = a.status;
-    v.engine = a.exact ? 3u : 1u;
+    v.engine = a.exact ? 3u : a.engine;
     v.failed_replay_probe = 0xffffffffu;
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) {

@@ -304,6 +304,9 @@ struct DeviceEngine {
   // numerical MCSE attachment: per-unit gradient and offset (units x 6), per-cell
   // and per-unit target fold sums (x 6), one block's score sums, statistics
   DBuf<double> num_coef, num_cell_fold, num_unit_fold, num_out;
+  // leave-observation-out: per-row (sum p2, sum p4, offset), per-copy
+  // pullbacks (q1, q3) and per-row target folds (x 6)
+  DBuf<double> num_row_coef, num_copy_pb, num_row_fold;
   DBuf<unsigned long long> num_stats;
   std::map<int, std::unique_ptr<BlockWork>> work;
   // pinned host scalars
@@ -1699,6 +1702,12 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
           beta[k * K + j] = v;
         }
       CK(cudaMemcpyAsync(e.beta_buf.p, beta.data(), QMAX * K * sizeof(double), cudaMemcpyHostToDevice, L.s));
+      if (e.observation && o.numerical)  // the attachment's per-row target folds of this block
+        k_obs_num_folds<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.q, uint64_t(first), np, e.unit_ptr.p, e.cell_rows.p,
+                                                        e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p,
+                                                        e.beta_buf.p, e.Rd.p, e.row_y.p, y_center, e.residual.p,
+                                                        double((o.probes + 1) / 2), double(o.probes / 2),
+                                                        e.num_row_fold.p);
       if (e.observation)
         k_obs_contract_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.q, e.cell_worker.p, e.cell_firm.p,
                                                              e.obs_cell_sums.p, e.beta_buf.p, w.alpha.p, w.x.p,
@@ -2037,16 +2046,29 @@ void run_exact(DeviceEngine& e, const Compressed& p, const SolveOptions& o, Solv
 // and records the shares' extremes in the attachment.
 uint32_t numerical_derivative(DeviceEngine& e, const SolveOptions& o, NumericalAttachment& na) {
   Launch L{grid_blocks(), e.stream};
-  if (e.num_coef.n < size_t(e.G) * 6) e.num_coef.alloc(size_t(e.G) * 6);
   if (!e.num_stats.p) e.num_stats.alloc(8);
   const unsigned long long inf = 0x7ff0000000000000ull;
-  unsigned long long init[NUM_STATS] = {0, inf, inf, 0, 0}, got[NUM_STATS];
+  unsigned long long init[NUM_STATS] = {0, inf, e.observation ? order_key(INFINITY) : inf, 0, 0}, got[NUM_STATS];
   CK(cudaMemcpyAsync(e.num_stats.p, init, sizeof(init), cudaMemcpyHostToDevice, L.s));
-  k_num_derivative<<<L.grid, THREADS, 0, L.s>>>(e.G, double(o.probes), e.moments.p, e.num_coef.p, e.num_stats.p);
+  if (e.observation) {
+    // rows over their copies (generic_jla/numerical.rs `State::observation`)
+    if (e.num_row_coef.n < size_t(e.rows) * 3) e.num_row_coef.alloc(size_t(e.rows) * 3);
+    if (e.num_copy_pb.n < size_t(e.physical) * 2) e.num_copy_pb.alloc(size_t(e.physical) * 2);
+    k_obs_num_derivative<<<L.grid, THREADS, 0, L.s>>>(e.rows, double(o.probes), e.row_phys.p, e.row_rank_d.p,
+                                                      e.row_copy_offset.p, e.obs_row_acc.p, e.obs_copy_acc.p,
+                                                      e.q > 0 ? e.control_lev.p : nullptr, e.num_row_coef.p,
+                                                      e.num_copy_pb.p, e.num_stats.p);
+  } else {
+    if (e.num_coef.n < size_t(e.G) * 6) e.num_coef.alloc(size_t(e.G) * 6);
+    k_num_derivative<<<L.grid, THREADS, 0, L.s>>>(e.G, double(o.probes), e.moments.p, e.num_coef.p, e.num_stats.p);
+  }
   CK(cudaMemcpyAsync(got, e.num_stats.p, sizeof(got), cudaMemcpyDeviceToHost, L.s));
   CK(cudaStreamSynchronize(L.s));
   std::memcpy(&na.minimum_constrained, &got[1], 8);
-  std::memcpy(&na.minimum_residual_margin, &got[2], 8);
+  if (e.observation)
+    na.minimum_residual_margin = from_order_key(got[2]);
+  else
+    std::memcpy(&na.minimum_residual_margin, &got[2], 8);
   std::memcpy(&na.maximum_sensitivity_ratio, &got[3], 8);
   uint32_t status = got[4] ? 5u : 2u;  // a clipped adjustment variance starts nonsmooth
   if (got[0]) status = uint32_t(got[0] & 0xff);  // the last unit that set a status wins
@@ -2081,9 +2103,15 @@ bool numerical_replay(DeviceEngine& e, const SolveOptions& o, SolveResult& res, 
       }
       throw;
     }
-    k_num_scores<K><<<L.grid, THREADS, 0, L.s>>>(e.G, ncols, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
-                                                 e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.num_coef.p,
-                                                 e.num_unit_fold.p, e.partial.p);
+    if (e.observation)
+      k_obs_num_scores<K><<<L.grid, THREADS, 0, L.s>>>(e.C, ncols, e.unit_ptr.p, e.cell_rows.p, e.cell_worker.p,
+                                                       e.cell_firm.p, e.row_phys.p, e.copy_bits.p, w.alpha.p, w.x.p,
+                                                       e.num_row_coef.p, e.num_copy_pb.p, e.num_row_fold.p,
+                                                       e.partial.p);
+    else
+      k_num_scores<K><<<L.grid, THREADS, 0, L.s>>>(e.G, ncols, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
+                                                   e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.num_coef.p,
+                                                   e.num_unit_fold.p, e.partial.p);
     finish(e.partial.p, L.grid, 6 * K, e.num_out.p, L.s);
     CK(cudaMemcpyAsync(out.data(), e.num_out.p, 6 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
@@ -2127,12 +2155,19 @@ void numerical_finish(DeviceEngine& e, const JlaPlan& plan, const SolveOptions& 
   na.target_probes = r;
   na.folds[0] = (r + 1) / 2;
   na.folds[1] = r / 2;
-  // allocation bound of the reference's attachment (engine/numerical.rs:36-49)
-  na.allocation_bound_bytes = uint64_t(e.G) * (6 * 8 + 6 * 16 + 4 * 8 + 4 * 16) + uint64_t(r) * 168 + 4096;
-  if (e.num_unit_fold.n < size_t(e.G) * 6) e.num_unit_fold.alloc(size_t(e.G) * 6);
-  k_num_unit_folds<<<L.grid, THREADS, 0, L.s>>>(e.G, e.unit_cell.p, e.unit_outcome.p, e.unit_count_f.p, e.unit_out.p,
-                                                outcome_mean, double(na.folds[0]), double(na.folds[1]),
-                                                e.num_cell_fold.p, e.num_unit_fold.p);
+  na.engine = e.generic ? 2 : 1;
+  if (e.observation) {
+    // allocation bound of the reference's generic attachment
+    // (generic_jla/numerical.rs:88-105): copies, rows, scores and receipts
+    na.allocation_bound_bytes = e.physical * 16 + uint64_t(e.rows) * 640 + uint64_t(r) * 120 + 4096;
+  } else {
+    // allocation bound of the reference's attachment (engine/numerical.rs:36-49)
+    na.allocation_bound_bytes = uint64_t(e.G) * (6 * 8 + 6 * 16 + 4 * 8 + 4 * 16) + uint64_t(r) * 168 + 4096;
+    if (e.num_unit_fold.n < size_t(e.G) * 6) e.num_unit_fold.alloc(size_t(e.G) * 6);
+    k_num_unit_folds<<<L.grid, THREADS, 0, L.s>>>(e.G, e.unit_cell.p, e.unit_outcome.p, e.unit_count_f.p,
+                                                  e.unit_out.p, outcome_mean, double(na.folds[0]),
+                                                  double(na.folds[1]), e.num_cell_fold.p, e.num_unit_fold.p);
+  }
   std::vector<Primitive> scores[2] = {std::vector<Primitive>(r, Primitive{0, 0, 0}),
                                       std::vector<Primitive>(r, Primitive{0, 0, 0})};
   uint32_t status = state_status;
@@ -2439,6 +2474,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     return;
   }
   if (o.shard_phase == 2) shard_upload(e, o.shard_input);
+  uint32_t numerical_status = 0;
   if (e.observation) {
     // ---- deleted residual of every row from its copies
     unsigned long long init[2] = {~0ull, 0ull};
@@ -2470,6 +2506,12 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
                          : code == CORRECTION_NONFINITE  ? "observation deleted residual is nonfinite"
                                                          : "finite-projection moment failed";
       fail(int32_t(code), "generic_jla_observation_adjustment", std::string(what) + " at row " + std::to_string(row));
+    }
+    if (o.numerical) {
+      numerical_status = numerical_derivative(e, o, res.numerical);
+      if (e.num_row_fold.n < size_t(e.rows) * 6) e.num_row_fold.alloc(size_t(e.rows) * 6);
+      CK(cudaMemsetAsync(e.num_row_fold.p, 0, size_t(e.rows) * 6 * sizeof(double), L.s));
+      if (!e.num_out.p) e.num_out.alloc(6 * 128);
     }
     // the target contraction's per-cell sums of the deleted residuals
     if (!e.obs_cell_sums.p) {
@@ -2530,6 +2572,8 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     return;
   }
   finish_draws(res, o.probes);
+  if (o.numerical && e.observation)
+    numerical_finish<K>(e, plan, o, outcome_mean(p, o.centering), numerical_status, res);
   for (auto& r : res.receipts) {
     res.max_reduced_residual = std::max(res.max_reduced_residual, r.reduced_residual);
     res.max_complete_residual = std::max(res.max_complete_residual, r.complete_residual);

@@ -83,6 +83,7 @@ struct SolveTimings {
 struct NumericalAttachment {
   bool present = false, exact = false;
   uint32_t status = 0;
+  uint32_t engine = 1;  // 1 compressed, 2 generic (leave-observation-out)
   double conditional[3][3] = {}, leverage[3][3] = {}, raw[3][3] = {}, usable[3][3] = {};
   double mcse[4] = {};
   double psd_adjustment = 0;

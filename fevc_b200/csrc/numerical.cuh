@@ -1,7 +1,9 @@
 // Device kernels of the numerical MCSE attachment for the compressed engine
-// (match deletion without controls).  Reference: vckss-core/src/engine/
-// numerical.rs (State::new, State::target, State::replay) and the local
-// finite-projection derivative of vckss-core/src/numerical_mc.rs:66-135.
+// (match deletion without controls) and for leave-observation-out deletion
+// (generic engine, with or without controls).  Reference: vckss-core/src/
+// engine/numerical.rs and generic_jla/numerical.rs (State::new / observation,
+// State::target, State::replay) and the local finite-projection derivative
+// of vckss-core/src/numerical_mc.rs:66-145.
 //
 // The attachment linearises the corrected components in the leverage
 // moments: every deletion unit gets the gradient of its adjustment multiplier
@@ -15,6 +17,7 @@
 #pragma once
 
 #include "device.cuh"
+#include "generic.cuh"
 
 namespace fevcb {
 
@@ -263,6 +266,282 @@ __global__ void k_num_scores(uint32_t units, int ncols, const uint32_t* __restri
       const double A = a.finish();
 #pragma unroll
       for (int i = 0; i < 6; ++i) v[i][c] += -uf[i] * A;
+    }
+  }
+  block_reduce_cols<K, 6>(v, partial);
+}
+
+// ---------------------------------------------------------------------------
+// Leave-observation-out (generic engine; reference generic_jla/numerical.rs
+// `State::observation`, `State::target`, `State::replay`).
+
+// Unsigned keys that order like the doubles they encode (so an atomicMin of
+// keys is a minimum of doubles of either sign).
+__host__ __device__ __forceinline__ unsigned long long order_key(double x) {
+  unsigned long long b;
+  memcpy(&b, &x, 8);
+  return (b >> 63) ? ~b : b | 0x8000000000000000ull;
+}
+__host__ __device__ __forceinline__ double from_order_key(unsigned long long k) {
+  const unsigned long long b = (k >> 63) ? k & 0x7fffffffffffffffull : ~k;
+  double x;
+  memcpy(&x, &b, 8);
+  return x;
+}
+
+// copy_pullback (numerical_mc.rs:137-145): the gradient in the five raw-mean
+// moments pulled back to (row P^2, row P^4, copy aP, copy aP^3) coefficients.
+__device__ __forceinline__ void copy_pullback(const double (&g)[5], double (&out)[4]) {
+  const double p = g[0], m = g[1], a = g[2], b = g[3], c = g[4];
+  out[0] = p + m + 6.0 * b + c;
+  out[1] = a + b + c;
+  out[2] = -2.0 * m - 4.0 * b;
+  out[3] = -4.0 * b - 2.0 * c;
+}
+
+// Per row r (row order) over its physical copies: with a2 = row P^2 mean,
+// a4 = row P^4 mean, c1 / c3 = the copy's aP / aP^3 means, the copy's raw
+// moments u = (a2, 1 + a2 - 2c1, a4, 1 + 6a2 + a4 - 4c1 - 4c3, a2 + a4 - 2c3),
+// the gradient of its multiplier at the row's control leverage, and its
+// pullback: copy_pb[c] = (q1, q3); row_coef[r] = (sum p2, sum p4, offset)
+// with offset = sum (q1 c1 + q3 c3) + g2 a2 + g4 a4.  stats as in
+// k_num_derivative; the status key orders copies as the reference visits
+// them: (class rank, copy number in the class).
+__global__ void k_obs_num_derivative(uint32_t rows, double probes, const uint64_t* __restrict__ row_phys,
+                                     const uint64_t* __restrict__ row_rank, const uint64_t* __restrict__ row_copy_offset,
+                                     const double* __restrict__ row_acc, const double* __restrict__ copy_acc,
+                                     const double* __restrict__ control, double* __restrict__ row_coef,
+                                     double* __restrict__ copy_pb, unsigned long long* __restrict__ stats) {
+  unsigned long long last = 0, clipped = 0;
+  double min_c = __longlong_as_double(0x7ff0000000000000LL), min_m = min_c, max_q = 0.0;
+  const double R = probes;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+    const double pf = row_acc[size_t(r) * 4] + row_acc[size_t(r) * 4 + 1];
+    const double ps = row_acc[size_t(r) * 4 + 2] + row_acc[size_t(r) * 4 + 3];
+    const double a2 = pf / R, a4 = ps / R;
+    const double ctl = control ? control[r] : 0.0;
+    StableSumD g2, g4, off;
+    const uint64_t b = row_phys[r], e = row_phys[r + 1];
+    const unsigned long long base = (unsigned long long)row_rank[r] << 30;
+    for (uint64_t c = b; c < e; ++c) {
+      const double* acc = copy_acc + size_t(c) * 4;
+      const double first = acc[0] + acc[1], third = acc[2] + acc[3];
+      double* pb = copy_pb + size_t(c) * 2;
+      pb[0] = pb[1] = 0.0;
+      const unsigned long long key = base | (unsigned long long)(row_copy_offset[r] + (c - b)) << 3;
+      // the adjustment's variance (k_obs_adjust's expression): clipped when negative
+      {
+        const double m_res = R + pf - 2.0 * first, m_r4 = R + 6.0 * pf + ps - 4.0 * first - 4.0 * third;
+        const double m_mix = pf + ps - 2.0 * third, total = (pf + m_res) / R;
+        const double proj = (pf / R) / total, res = (m_res / R) / total;
+        const double v = (res * res * (ps / R) + proj * proj * (m_r4 / R) - 2.0 * proj * res * (m_mix / R)) / R;
+        if (v < 0.0) clipped = 1;
+      }
+      const double c1 = first / R, c3 = third / R;
+      const double u[5] = {a2, 1.0 + a2 - 2.0 * c1, a4, 1.0 + 6.0 * a2 + a4 - 4.0 * c1 - 4.0 * c3,
+                           a2 + a4 - 2.0 * c3};
+      if (!isnan(u[0] + u[1])) min_c = fmin(min_c, u[0] + u[1]);
+      double h, m, bias, var, dh[5], db[5], dv[5];
+      if (!finite_derivative(u, R, h, m, bias, var, dh, db, dv)) {
+        last = max(last, key | 6u);
+        continue;
+      }
+      const double ell = m - ctl;
+      if (!isnan(ell)) min_m = fmin(min_m, ell);
+      const double qr = sqrt(fmax(var, 0.0)) / ell;
+      if (!isnan(qr)) max_q = fmax(max_q, qr);
+      if (var < 0.0) {
+        last = max(last, key | 5u);
+        continue;
+      }
+      if (!(ell > 0.0)) {
+        last = max(last, key | 6u);
+        continue;
+      }
+      const double inv = 1.0 / ell, inv2 = inv * inv, inv3 = inv2 * inv, inv4 = inv2 * inv2;
+      const double factor = -inv2 - 2.0 * bias * inv3 + 3.0 * var * inv4;
+      double grad[5];
+      bool fin = true;
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        grad[j] = -factor * dh[j] + inv2 * db[j] - inv3 * dv[j];
+        fin &= isfinite(grad[j]);
+      }
+      if (!fin) {
+        last = max(last, key | 6u);
+        continue;
+      }
+      double pull[4];
+      copy_pullback(grad, pull);
+      g2.add(pull[0]);
+      g4.add(pull[1]);
+      off.add(pull[2] * c1);
+      off.add(pull[3] * c3);
+      pb[0] = pull[2];
+      pb[1] = pull[3];
+    }
+    const double G2 = g2.finish(), G4 = g4.finish();
+    off.add(G2 * a2);
+    off.add(G4 * a4);
+    double* rc = row_coef + size_t(r) * 3;
+    rc[0] = G2;
+    rc[1] = G4;
+    rc[2] = off.finish();
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    last = max(last, __shfl_xor_sync(0xffffffffu, last, o));
+    clipped = max(clipped, __shfl_xor_sync(0xffffffffu, clipped, o));
+    min_c = fmin(min_c, __shfl_xor_sync(0xffffffffu, min_c, o));
+    min_m = fmin(min_m, __shfl_xor_sync(0xffffffffu, min_m, o));
+    max_q = fmax(max_q, __shfl_xor_sync(0xffffffffu, max_q, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (last) atomicMax(stats + 0, last);
+    atomicMin(stats + 1, (unsigned long long)__double_as_longlong(fmax(min_c, 0.0)));
+    atomicMin(stats + 2, order_key(min_m));  // the margin can be negative
+    atomicMax(stats + 3, (unsigned long long)__double_as_longlong(fmax(max_q, 0.0)));
+    if (clipped) atomicMax(stats + 4, clipped);
+  }
+}
+
+// Target folds of one target block (K columns: column 2j the worker side,
+// 2j + 1 the firm side of probe first + j, j < np): per row r of every cell,
+// with the full-model predictions sw / sf of the two sides at the row
+// (cell prediction u plus R_r' beta of the column) and y = outcome - mean,
+// row_fold[r][fold*3 + (0, 1, 2)] += y e (sw^2, sf^2, sw sf) / fold size,
+// fold = (first + j) % 2 (State::target, generic_jla/numerical.rs:366-380).
+// One warp per cell; lane l holds columns l*CPT ...
+template <int K>
+__global__ void __launch_bounds__(THREADS) k_obs_num_folds(
+    uint32_t cells, int q, uint64_t first, int np, const uint32_t* __restrict__ unit_ptr,
+    const uint32_t* __restrict__ cell_rows, const uint32_t* __restrict__ cell_worker,
+    const uint32_t* __restrict__ cell_firm, const double* __restrict__ alpha, const double* __restrict__ psi,
+    const double* __restrict__ beta /* [QMAX][K] */, const double* __restrict__ Rd /* rows x q */,
+    const double* __restrict__ row_y, double y_mean, const double* __restrict__ residual, double count0,
+    double count1, double* __restrict__ row_fold) {
+  constexpr int CPT = Cols<K>::CPT;
+  constexpr int LANES = K / CPT;
+  static_assert(CPT <= 2 && LANES <= 32, "one warp per cell, pairs in one lane or in adjacent lanes");
+  const int lane = threadIdx.x & 31;
+  const int c0 = lane * CPT;
+  const bool act = lane < LANES;
+  double bcol[QMAX][CPT];
+#pragma unroll
+  for (int k = 0; k < QMAX; ++k)
+#pragma unroll
+    for (int cc = 0; cc < CPT; ++cc) bcol[k][cc] = (act && k < q) ? beta[k * K + c0 + cc] : 0.0;
+  // the probe of this lane's pair and its fold
+  const int j = CPT == 2 ? lane : lane >> 1;
+  const bool owner = act && j < np && (CPT == 2 || (lane & 1) == 0);
+  const int fold = int((first + uint64_t(j)) & 1);
+  const double count = fold ? count1 : count0;
+  const size_t warp = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const size_t nw = (size_t(gridDim.x) * blockDim.x) >> 5;
+  for (size_t c = warp; c < cells; c += nw) {
+    const size_t wi = size_t(cell_worker[c]) * K, fi = size_t(cell_firm[c]) * K;
+    double u[CPT];
+#pragma unroll
+    for (int cc = 0; cc < CPT; ++cc) u[cc] = act ? alpha[wi + c0 + cc] + psi[fi + c0 + cc] : 0.0;
+    for (uint32_t g = unit_ptr[c]; g < unit_ptr[c + 1]; ++g) {
+      const uint32_t r = cell_rows[g];
+      const double wgt = (row_y[r] - y_mean) * residual[r];
+      double pred[CPT];
+#pragma unroll
+      for (int cc = 0; cc < CPT; ++cc) pred[cc] = u[cc];
+#pragma unroll
+      for (int k = 0; k < QMAX; ++k)
+        if (k < q) {
+          const double x = Rd[size_t(r) * q + k];
+#pragma unroll
+          for (int cc = 0; cc < CPT; ++cc) pred[cc] += x * bcol[k][cc];
+        }
+      const double other = __shfl_xor_sync(0xffffffffu, pred[0], 1);
+      const double sw = pred[0], sf = CPT == 2 ? pred[CPT - 1] : other;
+      double v[6] = {0, 0, 0, 0, 0, 0};
+      if (owner) {
+        const double kap[3] = {sw * sw, sf * sf, sw * sf};
+#pragma unroll
+        for (int i = 0; i < 3; ++i) v[fold * 3 + i] = wgt * kap[i] / count;
+      }
+#pragma unroll
+      for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
+      if (lane == 0) {
+        double* rf = row_fold + size_t(r) * 6;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) rf[i] += v[i];
+      }
+    }
+  }
+}
+
+// Replay scores of one leverage block (State::replay, generic_jla/numerical.rs:
+// 485-640): per row, with p the block's FE prediction at the row, the copies'
+// signs a and pullbacks (q1, q3): G1 = sum q1 a, G3 = sum q3 a, and
+// A = g2 p^2 + g4 p^4 - offset + G1 p + G3 p^3; the column's six sums
+// score[fold*3 + i] += -row_fold[r][fold*3 + i] A; partial[blk][6][K].
+// One warp per cell (the rows of a cell share p), signs from copy_bits.
+template <int K>
+__global__ void __launch_bounds__(THREADS) k_obs_num_scores(
+    uint32_t cells, int ncols, const uint32_t* __restrict__ unit_ptr, const uint32_t* __restrict__ cell_rows,
+    const uint32_t* __restrict__ cell_worker, const uint32_t* __restrict__ cell_firm,
+    const uint64_t* __restrict__ row_phys, const uint64_t* __restrict__ copy_bits, const double* __restrict__ alpha,
+    const double* __restrict__ psi, const double* __restrict__ row_coef, const double* __restrict__ copy_pb,
+    const double* __restrict__ row_fold, double* __restrict__ partial) {
+  constexpr int CPT = Cols<K>::CPT;
+  constexpr int LANES = K / CPT;
+  static_assert(LANES <= 32, "one warp per cell");
+  const int lane = threadIdx.x & 31;
+  const int c0 = lane * CPT;
+  const bool act = lane < LANES;
+  double v[6][CPT];
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+#pragma unroll
+    for (int cc = 0; cc < CPT; ++cc) v[i][cc] = 0.0;
+  const size_t warp = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const size_t nw = (size_t(gridDim.x) * blockDim.x) >> 5;
+  for (size_t c = warp; c < cells; c += nw) {
+    const size_t wi = size_t(cell_worker[c]) * K, fi = size_t(cell_firm[c]) * K;
+    double P[CPT];
+    bool live[CPT];
+#pragma unroll
+    for (int cc = 0; cc < CPT; ++cc) {
+      live[cc] = act && c0 + cc < ncols;
+      P[cc] = live[cc] ? alpha[wi + c0 + cc] + psi[fi + c0 + cc] : 0.0;
+    }
+    for (uint32_t g = unit_ptr[c]; g < unit_ptr[c + 1]; ++g) {
+      const uint32_t r = cell_rows[g];
+      const double g2 = row_coef[size_t(r) * 3], g4 = row_coef[size_t(r) * 3 + 1], o = row_coef[size_t(r) * 3 + 2];
+      double fold[6];
+#pragma unroll
+      for (int i = 0; i < 6; ++i) fold[i] = row_fold[size_t(r) * 6 + i];
+      StableSumD G1[CPT], G3[CPT];
+      for (uint64_t ph = row_phys[r]; ph < row_phys[r + 1]; ++ph) {
+        const double q1 = copy_pb[ph * 2], q3 = copy_pb[ph * 2 + 1];
+        const uint64_t m = copy_bits[ph] >> c0;
+#pragma unroll
+        for (int cc = 0; cc < CPT; ++cc) {
+          const double a = ((m >> cc) & 1) ? 1.0 : -1.0;
+          G1[cc].add(q1 * a);
+          G3[cc].add(q3 * a);
+        }
+      }
+#pragma unroll
+      for (int cc = 0; cc < CPT; ++cc) {
+        if (!live[cc]) continue;
+        const double p = P[cc], p2 = p * p;
+        StableSumD A;
+        A.add(g2 * p2);
+        A.add(g4 * (p2 * p2));
+        A.add(-o);
+        A.add(G1[cc].finish() * p);
+        A.add(G3[cc].finish() * (p2 * p));
+        const double a = A.finish();
+#pragma unroll
+        for (int i = 0; i < 6; ++i) v[i][cc] += -fold[i] * a;
+      }
     }
   }
   block_reduce_cols<K, 6>(v, partial);

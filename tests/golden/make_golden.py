@@ -431,6 +431,15 @@ NUMERICAL_PANELS = {
                         probes=20, algorithm=2),
     "kat12_jla": dict(build=lambda: kat12(), probes=5, algorithm=2),
     "kat12_auto": dict(build=lambda: kat12(), probes=5, algorithm=0),
+    "obs_2k": dict(build=lambda: generate_panel(2000, 150, 5, move_p=0.2, seed=11), probes=16, algorithm=2,
+                   deletion=2),
+    "obs_odd_2k": dict(build=lambda: generate_panel(2000, 150, 5, move_p=0.2, seed=13), probes=13, algorithm=2,
+                       deletion=2),
+    "obs_controls_2k": dict(build=lambda: generate_panel(2000, 150, 5, move_p=0.2, year_controls=True, seed=11),
+                            probes=16, algorithm=2, deletion=2),
+    "obs_duplicates_1500": dict(build=lambda: duplicated_rows_panel(8, False), probes=12, algorithm=2, deletion=2),
+    "obs_controls_duplicates_1500": dict(build=lambda: duplicated_rows_panel(9, True), probes=12, algorithm=2,
+                                         deletion=2),
 }
 
 NUMERICAL_FIELDS = ("status", "engine", "leverage_probes", "target_probes", "target_fold_a", "target_fold_b",
@@ -440,11 +449,12 @@ NUMERICAL_FIELDS = ("status", "engine", "leverage_probes", "target_probes", "tar
                     "conditional", "leverage", "raw", "usable", "mcse", "point_rhs")
 
 
-def numerical_request(e, probes: int, algorithm: int):
+def numerical_request(e, probes: int, algorithm: int, deletion: int = 1, controls: int = 0):
     """The numerical-attachment request the fixtures and tests use: a default
     V5 point with the probes, JLA or the automatic algorithm, diagonal PCG at
-    1e-12 for JLA (the automatic algorithm keeps the automatic route)."""
-    q = e.default_request_v5(1)
+    1e-12 for JLA (the automatic algorithm keeps the automatic route), the
+    panel's deletion mode and control count."""
+    q = e.default_request_v5(deletion)
     v1 = q.v4.v3.v2.v1
     v1.probes = probes
     v1.pcg_tolerance = 1e-12
@@ -454,13 +464,13 @@ def numerical_request(e, probes: int, algorithm: int):
         v1.solver_route = 2
     q.threads = 4
     q.tolerance_supplied = 1
-    return e.numerical_request(q)
+    return e.numerical_request(q, controls)
 
 
-def numerical_record(lib, panel: Panel, probes: int, algorithm: int) -> dict:
+def numerical_record(lib, panel: Panel, probes: int, algorithm: int, deletion: int = 1) -> dict:
     e = abi.Engine(lib)
-    e.prepare(panel)
-    e.solve_numerical(numerical_request(e, probes, algorithm))
+    e.prepare(panel, deletion_mode=deletion)
+    e.solve_numerical(numerical_request(e, probes, algorithm, deletion, len(panel.controls)))
     r = e.numerical_result()
     point = e.result()
     count, rhs = e.numerical_rhs(int(r["certified_replay_rhs"]))
@@ -469,7 +479,7 @@ def numerical_record(lib, panel: Panel, probes: int, algorithm: int) -> dict:
     rec = {k: (str(v) if isinstance(v, float) and not np.isfinite(v) else v) for k, v in rec.items()}
     rec["corrected"] = list(point["corrected"])
     rec["rhs"] = [[x["probe"], x["phase"], x["complete_residual"]] for x in rhs]
-    return {"probes": probes, "algorithm": algorithm, "pcg_tolerance": 1e-12, **rec}
+    return {"probes": probes, "algorithm": algorithm, "deletion": deletion, "pcg_tolerance": 1e-12, **rec}
 
 
 # Request mutations for the preflight fixture (field path, value).
@@ -522,7 +532,8 @@ def write_numerical_cases(lib, meta: dict) -> None:
     for name, spec in NUMERICAL_PANELS.items():
         panel = spec["build"]()
         cases[name] = {"panel_sha256": panel_digest(panel),
-                       "record": numerical_record(lib, panel, spec["probes"], spec["algorithm"])}
+                       "record": numerical_record(lib, panel, spec["probes"], spec["algorithm"],
+                                                  spec.get("deletion", 1))}
         print(name, cases[name]["record"]["status"], cases[name]["record"]["mcse"])
     pre = numerical_preflight_record(lib)
     print(pre)

@@ -1,8 +1,10 @@
 """Numerical MCSE attachment on the device against the plugin's own
-attachment (``tests/golden/numerical_cases.json``): the replay counts, fold
-sizes and status exactly; the conditional and leverage covariances, the
-usable matrix, the MCSE and the share extremes within 1e-8 relative; the
-exact-zero attachment when the automatic algorithm resolves to exact."""
+attachment (``tests/golden/numerical_cases.json``), on the compressed engine
+and with leave-observation-out deletion (with and without controls, with
+duplicated rows and literal frequencies): the replay counts, fold sizes and
+status exactly; the conditional and leverage covariances, the usable matrix,
+the MCSE and the share extremes within 1e-8 relative; the exact-zero
+attachment when the automatic algorithm resolves to exact."""
 
 import json
 from pathlib import Path
@@ -34,9 +36,11 @@ def solved(lib):
     for name, spec in make_golden.NUMERICAL_PANELS.items():
         panel = spec["build"]()
         assert make_golden.panel_digest(panel) == CASES[name]["panel_sha256"]
+        deletion = spec.get("deletion", 1)
         e = abi.Engine(lib)
-        e.prepare(panel)
-        e.solve_numerical(make_golden.numerical_request(e, spec["probes"], spec["algorithm"]))
+        e.prepare(panel, deletion_mode=deletion)
+        e.solve_numerical(make_golden.numerical_request(e, spec["probes"], spec["algorithm"], deletion,
+                                                        len(panel.controls)))
         r = e.numerical_result()
         point = e.result()
         count, rhs = e.numerical_rhs(int(r["certified_replay_rhs"]) + 3)
