@@ -372,6 +372,38 @@ def plain_form_rate(lib, panel, probes, tolerance):
                     f"per solve, bounded sample of {probes} probes (wall of solve_v5 including the hierarchy build)"}
 
 
+def numerical_attachment(lib, panel, probes, tolerance):
+    """The numerical MCSE attachment (``vckss_rust_engine_solve_numerical_v1``)
+    on the same panel and request: wall of the point solve plus the leverage
+    replay on a fresh generation (preparation outside), the replay's share,
+    the attachment's status and MCSE beside the point estimate's."""
+    import torch
+
+    from fevc_b200 import abi, learned
+
+    e = abi.Engine(lib)
+    e.prepare(panel, deletion_mode=deletion_mode(panel))
+    # the headline's form: autotuned precision, the learned stage (uniform weights without parameters)
+    e.device_options(64, 3 if learned.load_params() is not None else 4, 2)
+    q = v5_request(e, probes, tolerance, deletion=deletion_mode(panel))
+    req = e.numerical_request(q, len(panel.controls))
+    t0 = time.perf_counter()
+    e.solve_numerical(req)
+    torch.cuda.synchronize()
+    s = time.perf_counter() - t0
+    r = e.numerical_result()
+    point = e.result()
+    t = e.timings()
+    e.release()
+    return {"seconds": round(s, 3), "status": r["status"], "engine": r["engine"],
+            "replay_rhs": r["certified_replay_rhs"], "mcse": [round(x, 12) for x in r["mcse"]],
+            "point_mcse": [round(x, 12) for x in point["numerical_mcse"]],
+            "maximum_replay_complete_residual": r["maximum_replay_complete_residual"],
+            "phase_ms": {k: round(t[k], 1) for k in ("fit_ms", "leverage_ms", "target_ms", "total_ms")},
+            "form": "numerical MCSE attachment (mcse(all)): point solve + replay of the leverage probes, through "
+                    "the C ABI, wall of solve_numerical_v1 on a fresh generation"}
+
+
 def time_forms(lib, panel, args, stream, barrier, headline):
     from fevc_b200 import abi, learned
 
@@ -390,6 +422,7 @@ def time_forms(lib, panel, args, stream, barrier, headline):
                                                    stream, barrier)), "form": text}
     forms["plain_gpu_cmg_pcg"] = guarded(lambda: plain_form_rate(lib, panel, min(args.probes, args.plain_probes),
                                                                  args.tolerance))
+    forms["numerical_attachment"] = guarded(lambda: numerical_attachment(lib, panel, args.probes, args.tolerance))
     return forms
 
 

@@ -2172,10 +2172,6 @@ void numerical_solve(uint64_t g, const VckssNumericalRequestV1& q, const Interru
       o.algorithm = 1;
       o.exact_limit = q.point.v3.v2.exact_estimator_limit;
       o.blocksize_limit = q.point.v3.v2.blocksize_limit ? q.point.v3.v2.blocksize_limit : 5000;
-    } else if (p.has_plan && p.plan.generic && !p.plan.observation) {
-      fail(UNSUPPORTED_FEATURE, "numerical_preflight",
-           "the device numerical attachment covers the compressed engine and leave-observation-out deletion; "
-           "match deletion with controls is not provided");
     }
   }
   o.numerical = true;

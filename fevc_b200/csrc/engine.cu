@@ -307,6 +307,9 @@ struct DeviceEngine {
   // leave-observation-out: per-row (sum p2, sum p4, offset), per-copy
   // pullbacks (q1, q3) and per-row target folds (x 6)
   DBuf<double> num_row_coef, num_copy_pb, num_row_fold;
+  // match deletion with controls: per-unit maker margin, per-row inverse-common
+  // action, per-unit target-fold sums
+  DBuf<double> num_unit_margin, num_row_w, num_block_sums;
   DBuf<unsigned long long> num_stats;
   std::map<int, std::unique_ptr<BlockWork>> work;
   // pinned host scalars
@@ -1716,6 +1719,12 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
         k_generic_contract_units<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.q, e.unit_cell.p, e.cell_worker.p,
                                                                  e.cell_firm.p, e.unit_sums.p, e.beta_buf.p,
                                                                  w.alpha.p, w.x.p, e.partial.p);
+      if (!e.observation && o.numerical)  // the attachment's match-unit target folds of this block
+        k_num_block_folds<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.q, uint64_t(first), np, e.unit_cell.p,
+                                                          e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p,
+                                                          e.beta_buf.p, e.num_block_sums.p,
+                                                          double((o.probes + 1) / 2), double(o.probes / 2),
+                                                          e.num_unit_fold.p);
       finish(e.partial.p, L.grid, 2 * K, w.tot.p, L.s);
       std::vector<double> g2(2 * K);
       CK(cudaMemcpyAsync(g2.data(), w.tot.p, 2 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
@@ -2048,7 +2057,7 @@ uint32_t numerical_derivative(DeviceEngine& e, const SolveOptions& o, NumericalA
   Launch L{grid_blocks(), e.stream};
   if (!e.num_stats.p) e.num_stats.alloc(8);
   const unsigned long long inf = 0x7ff0000000000000ull;
-  unsigned long long init[NUM_STATS] = {0, inf, e.observation ? order_key(INFINITY) : inf, 0, 0}, got[NUM_STATS];
+  unsigned long long init[NUM_STATS] = {0, inf, e.generic ? order_key(INFINITY) : inf, 0, 0}, got[NUM_STATS];
   CK(cudaMemcpyAsync(e.num_stats.p, init, sizeof(init), cudaMemcpyHostToDevice, L.s));
   if (e.observation) {
     // rows over their copies (generic_jla/numerical.rs `State::observation`)
@@ -2058,6 +2067,12 @@ uint32_t numerical_derivative(DeviceEngine& e, const SolveOptions& o, NumericalA
                                                       e.row_copy_offset.p, e.obs_row_acc.p, e.obs_copy_acc.p,
                                                       e.q > 0 ? e.control_lev.p : nullptr, e.num_row_coef.p,
                                                       e.num_copy_pb.p, e.num_stats.p);
+  } else if (e.generic) {
+    // match groups with controls (generic_jla/numerical.rs `State::block`)
+    if (e.num_coef.n < size_t(e.G) * 6) e.num_coef.alloc(size_t(e.G) * 6);
+    k_num_block_derivative<<<L.grid, THREADS, 0, L.s>>>(e.G, double(o.probes), e.unit_group_d.p, e.moments.p,
+                                                        e.unit_out.p, e.num_unit_margin.p, e.num_coef.p,
+                                                        e.num_stats.p);
   } else {
     if (e.num_coef.n < size_t(e.G) * 6) e.num_coef.alloc(size_t(e.G) * 6);
     k_num_derivative<<<L.grid, THREADS, 0, L.s>>>(e.G, double(o.probes), e.moments.p, e.num_coef.p, e.num_stats.p);
@@ -2065,7 +2080,7 @@ uint32_t numerical_derivative(DeviceEngine& e, const SolveOptions& o, NumericalA
   CK(cudaMemcpyAsync(got, e.num_stats.p, sizeof(got), cudaMemcpyDeviceToHost, L.s));
   CK(cudaStreamSynchronize(L.s));
   std::memcpy(&na.minimum_constrained, &got[1], 8);
-  if (e.observation)
+  if (e.generic)
     na.minimum_residual_margin = from_order_key(got[2]);
   else
     std::memcpy(&na.minimum_residual_margin, &got[2], 8);
@@ -2156,10 +2171,17 @@ void numerical_finish(DeviceEngine& e, const JlaPlan& plan, const SolveOptions& 
   na.folds[0] = (r + 1) / 2;
   na.folds[1] = r / 2;
   na.engine = e.generic ? 2 : 1;
-  if (e.observation) {
+  // Counter-V1 words one replayed probe addresses (ceil(copies / 64) per unit)
+  // and the physical copies
+  uint64_t words = 0, copies = 0;
+  for (uint64_t n : plan.del_count) {
+    words += (n + 63) / 64;
+    copies += n;
+  }
+  if (e.generic) {
     // allocation bound of the reference's generic attachment
     // (generic_jla/numerical.rs:88-105): copies, rows, scores and receipts
-    na.allocation_bound_bytes = e.physical * 16 + uint64_t(e.rows) * 640 + uint64_t(r) * 120 + 4096;
+    na.allocation_bound_bytes = copies * 16 + uint64_t(e.rows) * 640 + uint64_t(r) * 120 + 4096;
   } else {
     // allocation bound of the reference's attachment (engine/numerical.rs:36-49)
     na.allocation_bound_bytes = uint64_t(e.G) * (6 * 8 + 6 * 16 + 4 * 8 + 4 * 16) + uint64_t(r) * 168 + 4096;
@@ -2177,9 +2199,6 @@ void numerical_finish(DeviceEngine& e, const JlaPlan& plan, const SolveOptions& 
     ro.probe_end = 0;
     if (!numerical_replay_blocks<K>(e, ro, res, scores)) status = 7;
   }
-  // Counter-V1 words the replay addressed: ceil(copies / 64) per unit and probe
-  uint64_t words = 0;
-  for (uint64_t n : plan.del_count) words += (n + 63) / 64;
   na.generator_words = words * na.attempted_replay_rhs;
   finish_numerical(res.target_draws, scores, status, na);
 }
@@ -2539,9 +2558,15 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
       for (int j = 0; j < q; ++j) prm.factor.m[i * QMAX + j] = e.Lfac[i * q + j];
     unsigned long long init[2] = {~0ull, 0ull};
     CK(cudaMemcpyAsync(e.error.p, init, sizeof(init), cudaMemcpyHostToDevice, L.s));
+    if (o.numerical) {  // the attachment also needs each group's maker margin and inverse-common action
+      if (e.num_unit_margin.n < size_t(e.G)) e.num_unit_margin.alloc(e.G);
+      if (e.num_row_w.n < size_t(e.rows)) e.num_row_w.alloc(e.rows);
+    }
     k_generic_adjust<<<L.grid, THREADS, 0, L.s>>>(prm, e.unit_group_d.p, e.moments.p, e.unit_count_f.p, e.group_ptr.p,
                                                   e.group_rows.p, e.row_freq.p, e.residual.p, e.Rd.p, e.deleted.p,
-                                                  e.unit_out.p, e.error.p, e.error.p + 1);
+                                                  e.unit_out.p, e.error.p, e.error.p + 1,
+                                                  o.numerical ? e.num_unit_margin.p : nullptr,
+                                                  o.numerical ? e.num_row_w.p : nullptr);
     unsigned long long got[2] = {0, 0};
     CK(cudaMemcpyAsync(got, e.error.p, sizeof(got), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
@@ -2561,6 +2586,16 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
                                                     e.row_freq.p, e.row_y.p, outcome_mean(p, o.centering),
                                                     e.deleted.p, e.Rd.p, e.unit_sums.p);
     res.timings.kernel_launches += 1;
+    if (o.numerical) {
+      numerical_status = numerical_derivative(e, o, res.numerical);
+      if (e.num_block_sums.n < size_t(e.G) * (2 + 2 * QMAX)) e.num_block_sums.alloc(size_t(e.G) * (2 + 2 * QMAX));
+      k_num_block_sums<<<L.grid, THREADS, 0, L.s>>>(e.G, q, e.unit_group_d.p, e.group_ptr.p, e.group_rows.p,
+                                                    e.row_freq.p, e.row_y.p, outcome_mean(p, o.centering), e.Rd.p,
+                                                    e.num_row_w.p, e.unit_out.p, e.num_block_sums.p);
+      if (e.num_unit_fold.n < size_t(e.G) * 6) e.num_unit_fold.alloc(size_t(e.G) * 6);
+      CK(cudaMemsetAsync(e.num_unit_fold.p, 0, size_t(e.G) * 6 * sizeof(double), L.s));
+      if (!e.num_out.p) e.num_out.alloc(6 * 128);
+    }
   }
   }
   auto t2 = now();
@@ -2572,8 +2607,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     return;
   }
   finish_draws(res, o.probes);
-  if (o.numerical && e.observation)
-    numerical_finish<K>(e, plan, o, outcome_mean(p, o.centering), numerical_status, res);
+  if (o.numerical) numerical_finish<K>(e, plan, o, outcome_mean(p, o.centering), numerical_status, res);
   for (auto& r : res.receipts) {
     res.max_reduced_residual = std::max(res.max_reduced_residual, r.reduced_residual);
     res.max_complete_residual = std::max(res.max_complete_residual, r.complete_residual);

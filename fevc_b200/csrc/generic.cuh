@@ -221,7 +221,9 @@ __global__ void k_generic_adjust(GenericAdjustParams prm, const uint32_t* __rest
                                  const double* __restrict__ row_freq, const double* __restrict__ residual,
                                  const double* __restrict__ R, double* __restrict__ deleted,
                                  double* __restrict__ unit_out, unsigned long long* __restrict__ error,
-                                 unsigned long long* __restrict__ max_leverage) {
+                                 unsigned long long* __restrict__ max_leverage,
+                                 double* __restrict__ unit_margin = nullptr,
+                                 double* __restrict__ row_inverse_common = nullptr) {
   const int q = prm.q, rank = 1 + q;
   // the largest leverage over the groups, 1 - (lower bound of the smallest
   // eigenvalue of the maker I - V V'), as the reference's maker action reports
@@ -272,7 +274,9 @@ __global__ void k_generic_adjust(GenericAdjustParams prm, const uint32_t* __rest
           for (int k = 0; k < rank; ++k) v -= V[s][k] * V[t][k];
           a[s * RMAX + t] = v;
         }
-      lev_max = fmax(lev_max, 1.0 - sym_smallest_lower(a, width));
+      const double group_lev = 1.0 - sym_smallest_lower(a, width);
+      lev_max = fmax(lev_max, group_lev);
+      if (unit_margin) unit_margin[i] = 1.0 - group_lev;
       double piv = small_cholesky(a, width);
       if (!code && !(piv > prm.block_tolerance)) code = NONESTIMABLE_DELETION;
       if (!code) {
@@ -287,6 +291,7 @@ __global__ void k_generic_adjust(GenericAdjustParams prm, const uint32_t* __rest
       for (int l = 0; l < width; ++l) {
         uint32_t r = group_rows[b + l];
         deleted[r] = x0[l] + bias * x1[l] * ct - var * x1[l] * ci * ct;
+        if (row_inverse_common) row_inverse_common[r] = x1[l];
       }
     } else {
       // Woodbury: (I - V V')^{-1} y = y + V (I - V'V)^{-1} V'y
@@ -306,7 +311,9 @@ __global__ void k_generic_adjust(GenericAdjustParams prm, const uint32_t* __rest
           for (int t = 0; t < rank; ++t) a[s * RMAX + t] -= v[s] * v[t];
         }
       }
-      lev_max = fmax(lev_max, 1.0 - fmin(sym_smallest_lower(a, rank), 1.0));
+      const double group_lev = 1.0 - fmin(sym_smallest_lower(a, rank), 1.0);
+      lev_max = fmax(lev_max, group_lev);
+      if (unit_margin) unit_margin[i] = 1.0 - group_lev;
       double piv = small_cholesky(a, rank);
       if (!code && !(piv > prm.block_tolerance)) code = NONESTIMABLE_DELETION;
       if (!code) {
@@ -330,6 +337,7 @@ __global__ void k_generic_adjust(GenericAdjustParams prm, const uint32_t* __rest
             ci += c * t1;
           } else {
             deleted[r] = t0 + bias * t1 * ct - var * t1 * ci * ct;
+            if (row_inverse_common) row_inverse_common[r] = t1;
           }
         }
       }

@@ -547,4 +547,212 @@ __global__ void __launch_bounds__(THREADS) k_obs_num_scores(
   block_reduce_cols<K, 6>(v, partial);
 }
 
+// ---------------------------------------------------------------------------
+// Match deletion with controls (generic engine; reference generic_jla/
+// numerical.rs `State::block`, the match part of `State::target` and of
+// `State::replay`).
+
+// Per match unit i (group g = unit_group[i]): raw moments u, the block
+// gradient beta = (1 + 2 bias k - 3 var k^2) dh + db - k dv at the group's
+// k = common . inverse_common (FiniteDerivative::block, numerical_mc.rs:
+// 126-135), coef[i] = (beta, -sum beta_j u_j); t = common . transformed.
+// The status key orders events as the reference visits them: group by group,
+// the adjustment's variance clipping before the group's own status.
+__global__ void k_num_block_derivative(uint32_t units, double probes, const uint32_t* __restrict__ unit_group,
+                                       const double* __restrict__ moments, const double* __restrict__ unit_out,
+                                       const double* __restrict__ unit_margin, double* __restrict__ coef,
+                                       unsigned long long* __restrict__ stats) {
+  unsigned long long last = 0, clipped = 0;
+  double min_c = __longlong_as_double(0x7ff0000000000000LL), min_m = min_c, max_q = 0.0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < units; i += gridDim.x * blockDim.x) {
+    const double* mo = moments + size_t(i) * 5;
+    const unsigned long long key = (unsigned long long)(unit_group[i] + 1) << 4;
+    double* out = coef + size_t(i) * 6;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) out[k] = 0.0;
+    {
+      const double tm = (mo[0] + mo[1]) / probes;
+      const double pr = (mo[0] / probes) / tm, rs = (mo[1] / probes) / tm;
+      const double v = (rs * rs * (mo[2] / probes) + pr * pr * (mo[3] / probes) - 2.0 * pr * rs * (mo[4] / probes)) / probes;
+      if (v < 0.0) {
+        clipped = 1;
+        last = max(last, key | 5u);  // point clipping, before the group's own status
+      }
+    }
+    double u[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) u[k] = mo[k] / probes;
+    if (!isnan(u[0] + u[1])) min_c = fmin(min_c, u[0] + u[1]);
+    const double margin = unit_margin[i];
+    if (!isnan(margin)) min_m = fmin(min_m, margin);
+    double h, m, bias, var, dh[5], db[5], dv[5];
+    if (!finite_derivative(u, probes, h, m, bias, var, dh, db, dv)) {
+      last = max(last, key | 8u | 6u);
+      continue;
+    }
+    const double k = unit_out[size_t(i) * 6 + 5];
+    const double qr = sqrt(fmax(var, 0.0)) * k;
+    if (!isnan(qr)) max_q = fmax(max_q, qr);
+    if (var < 0.0) {
+      last = max(last, key | 8u | 5u);
+      continue;
+    }
+    if (!isfinite(k) || !(k > 0.0)) {
+      last = max(last, key | 8u | 6u);
+      continue;
+    }
+    const double lead = 1.0 + 2.0 * bias * k - 3.0 * var * k * k;
+    double beta[5];
+    bool fin = true;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      beta[j] = lead * dh[j] + db[j] - k * dv[j];
+      fin &= isfinite(beta[j]);
+    }
+    if (!fin) {
+      last = max(last, key | 8u | 6u);
+      continue;
+    }
+    StableSumD off;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) off.add(beta[j] * u[j]);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) out[j] = beta[j];
+    out[5] = -off.finish();
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    last = max(last, __shfl_xor_sync(0xffffffffu, last, o));
+    clipped = max(clipped, __shfl_xor_sync(0xffffffffu, clipped, o));
+    min_c = fmin(min_c, __shfl_xor_sync(0xffffffffu, min_c, o));
+    min_m = fmin(min_m, __shfl_xor_sync(0xffffffffu, min_m, o));
+    max_q = fmax(max_q, __shfl_xor_sync(0xffffffffu, max_q, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (last) atomicMax(stats + 0, last);
+    atomicMin(stats + 1, (unsigned long long)__double_as_longlong(fmax(min_c, 0.0)));
+    atomicMin(stats + 2, order_key(min_m));
+    atomicMax(stats + 3, (unsigned long long)__double_as_longlong(fmax(max_q, 0.0)));
+    if (clipped) atomicMax(stats + 4, clipped);
+  }
+}
+
+// Per match unit, once per solve: the sums over its rows that the target
+// folds need, with y = outcome - mean and factor_r = sqrt(f_r) w_r t
+// (w = the row's inverse-common action, t the unit's common . transformed):
+// sums[i] = (sum f y, sum f y R_r (q), sum factor, sum factor R_r (q)),
+// stride 2 + 2 QMAX.
+__global__ void k_num_block_sums(uint32_t units, int q, const uint32_t* __restrict__ unit_group,
+                                 const uint64_t* __restrict__ group_ptr, const uint32_t* __restrict__ group_rows,
+                                 const double* __restrict__ row_freq, const double* __restrict__ row_y, double y_mean,
+                                 const double* __restrict__ Rd, const double* __restrict__ row_w,
+                                 const double* __restrict__ unit_out, double* __restrict__ sums) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < units; i += gridDim.x * blockDim.x) {
+    const uint32_t g = unit_group[i];
+    const double t = unit_out[size_t(i) * 6 + 4];
+    StableSumD a0, a1[QMAX], h0, h1[QMAX];
+    for (uint64_t l = group_ptr[g]; l < group_ptr[g + 1]; ++l) {
+      const uint32_t r = group_rows[l];
+      const double f = row_freq[r], fy = f * (row_y[r] - y_mean), fac = sqrt(f) * row_w[r] * t;
+      a0.add(fy);
+      h0.add(fac);
+      for (int k = 0; k < q; ++k) {
+        const double x = Rd[size_t(r) * q + k];
+        a1[k].add(fy * x);
+        h1[k].add(fac * x);
+      }
+    }
+    double* o = sums + size_t(i) * (2 + 2 * QMAX);
+    o[0] = a0.finish();
+    o[1 + QMAX] = h0.finish();
+    for (int k = 0; k < QMAX; ++k) {
+      o[1 + k] = k < q ? a1[k].finish() : 0.0;
+      o[2 + QMAX + k] = k < q ? h1[k].finish() : 0.0;
+    }
+  }
+}
+
+// Match-unit target folds of one target block (columns 2j worker side, 2j + 1
+// firm side of probe first + j): with the full-model predictions u + R_r' beta,
+// aw = sum f y sw, af = sum f y sf, and s_w = sum factor sw, s_f = sum factor sf,
+// unit_fold[i][fold*3 + (0, 1, 2)] += (aw s_w, af s_f, (aw s_f + af s_w) / 2) / fold size.
+template <int K>
+__global__ void k_num_block_folds(uint32_t units, int q, uint64_t first, int np,
+                                  const uint32_t* __restrict__ unit_cell, const uint32_t* __restrict__ cell_worker,
+                                  const uint32_t* __restrict__ cell_firm, const double* __restrict__ alpha,
+                                  const double* __restrict__ psi, const double* __restrict__ beta /* [QMAX][K] */,
+                                  const double* __restrict__ sums, double count0, double count1,
+                                  double* __restrict__ unit_fold) {
+  constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
+  static_assert(CPT <= 2, "pairs of columns must sit in one thread or in adjacent lanes");
+  const int c0 = int(threadIdx.x % TPR) * CPT;
+  double bcol[QMAX][CPT];
+#pragma unroll
+  for (int k = 0; k < QMAX; ++k)
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) bcol[k][c] = k < q ? beta[k * K + c0 + c] : 0.0;
+  const size_t total = size_t(units) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    const size_t t = base + threadIdx.x;
+    const bool live = t < total;
+    const size_t i = live ? t / TPR : 0;
+    double a[CPT], h[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) a[c] = h[c] = 0.0;
+    if (live) {
+      const uint32_t cell = unit_cell[i];
+      const double* sm = sums + i * (2 + 2 * QMAX);
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        const double u = alpha[size_t(cell_worker[cell]) * K + c0 + c] + psi[size_t(cell_firm[cell]) * K + c0 + c];
+        double av = sm[0] * u, hv = sm[1 + QMAX] * u;
+#pragma unroll
+        for (int k = 0; k < QMAX; ++k)
+          if (k < q) {
+            av += sm[1 + k] * bcol[k][c];
+            hv += sm[2 + QMAX + k] * bcol[k][c];
+          }
+        a[c] = av;
+        h[c] = hv;
+      }
+    }
+    // the pair (worker side, firm side) of each probe
+    double aw, af, hw, hf;
+    int j;
+    bool owner;
+    if (CPT == 2) {
+      aw = a[0];
+      af = a[CPT - 1];
+      hw = h[0];
+      hf = h[CPT - 1];
+      j = c0 >> 1;
+      owner = live;
+    } else {
+      const double ao = __shfl_xor_sync(0xffffffffu, a[0], 1), ho = __shfl_xor_sync(0xffffffffu, h[0], 1);
+      aw = a[0];
+      af = ao;
+      hw = h[0];
+      hf = ho;
+      j = c0 >> 1;
+      owner = live && (c0 & 1) == 0;
+    }
+    double fv[6] = {0, 0, 0, 0, 0, 0};
+    if (owner && j < np) {
+      const int fold = int((first + uint64_t(j)) & 1);
+      const double count = fold ? count1 : count0;
+      fv[fold * 3 + 0] = aw * hw / count;
+      fv[fold * 3 + 1] = af * hf / count;
+      fv[fold * 3 + 2] = (aw * hf + af * hw) * 0.5 / count;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+#pragma unroll
+      for (int off = 1; off < TPR; off <<= 1) fv[k] += __shfl_xor_sync(0xffffffffu, fv[k], off);
+    if (live && c0 == 0) {
+      double* uf = unit_fold + i * 6;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) uf[k] += fv[k];
+    }
+  }
+}
+
 }  // namespace fevcb

@@ -440,6 +440,11 @@ NUMERICAL_PANELS = {
     "obs_duplicates_1500": dict(build=lambda: duplicated_rows_panel(8, False), probes=12, algorithm=2, deletion=2),
     "obs_controls_duplicates_1500": dict(build=lambda: duplicated_rows_panel(9, True), probes=12, algorithm=2,
                                          deletion=2),
+    "controls_2k": dict(build=lambda: generate_panel(2000, 150, 5, move_p=0.2, year_controls=True, seed=11),
+                        probes=16, algorithm=2),
+    "controls_odd_2k": dict(build=lambda: generate_panel(2000, 150, 5, move_p=0.2, year_controls=True, seed=14),
+                            probes=11, algorithm=2),
+    "controls_weighted_1500": dict(build=lambda: weighted_controls_panel(6), probes=12, algorithm=2),
 }
 
 NUMERICAL_FIELDS = ("status", "engine", "leverage_probes", "target_probes", "target_fold_a", "target_fold_b",
