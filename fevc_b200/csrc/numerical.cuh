@@ -1,6 +1,6 @@
 // Device kernels of the numerical MCSE attachment for the compressed engine
-// (match deletion without controls) and for leave-observation-out deletion
-// (generic engine, with or without controls).  Reference: vckss-core/src/
+// (match deletion without controls), for match deletion with controls and for
+// leave-observation-out deletion (generic engine).  Reference: vckss-core/src/
 // engine/numerical.rs and generic_jla/numerical.rs (State::new / observation,
 // State::target, State::replay) and the local finite-projection derivative
 // of vckss-core/src/numerical_mc.rs:66-145.
