@@ -68,13 +68,18 @@ def test_device_exact_matches_the_oracle_at_the_benchmark_size(exact_20k):
         assert rel(got[key], want[key]) < 1e-8, (key, got[key], want[key])
 
 
-def test_jla_approaches_the_exact_components(lib, exact_20k):
+@pytest.mark.parametrize("precision", [0, 1])
+def test_jla_approaches_the_exact_components(lib, exact_20k, precision):
+    """JLA (FP64, and FP32 storage with FP64 reductions and replacement) on
+    the 20,000-worker panel: each component within five numerical standard
+    errors of the exact one, the MCSE shrinking with the probes."""
     panel, got, _ = exact_20k
     exact = np.array(got["corrected"])
     errs = []
     for probes in (40, 640):
         e = abi.Engine(lib)
         e.prepare(panel)
+        e.device_options(64, 1, precision)
         e.centering(1)
         req = e.default_request()
         req.probes = probes
@@ -89,3 +94,24 @@ def test_jla_approaches_the_exact_components(lib, exact_20k):
         errs.append((float(np.max(err[:3] / np.abs(exact[:3]))), float(np.max(mcse[:3] / np.abs(exact[:3])))))
     # sixteen times the probes: the Monte Carlo error shrinks about fourfold
     assert errs[1][1] < 0.35 * errs[0][1], errs
+
+
+def test_fp32_storage_matches_fp64_on_the_exact_panel(lib, exact_20k):
+    """The mixed-precision form's components equal the FP64 form's on the same
+    probes to 1e-8 relative (both certified at the same residual in FP64),
+    so its error against the exact leverages is the Monte Carlo error."""
+    panel, _, _ = exact_20k
+    out = []
+    for precision in (0, 1):
+        e = abi.Engine(lib)
+        e.prepare(panel)
+        e.device_options(64, 1, precision)
+        e.centering(1)
+        req = e.default_request()
+        req.probes = 200
+        req.pcg_tolerance = 1e-10
+        e.solve(req)
+        out.append(e.result())
+        e.release()
+    for key in ("plugin", "correction", "corrected"):
+        assert rel(out[1][key], out[0][key]) < 1e-8, (key, out[1][key], out[0][key])
