@@ -297,6 +297,9 @@ struct DeviceEngine {
   // leave-observation-out target sums per cell (cells x (1 + q)) and the
   // cell-independent quadratic form sum_r w_r R_r R_r' (q x q, upper triangle)
   DBuf<double> obs_cell_sums, obs_s2;
+  // the fused leave-observation-out target pass: its reduced sums and a
+  // second partial buffer
+  DBuf<double> obs_fused, partial2;
   std::vector<double> obs_S2;
   // solve-long buffers
   DBuf<double> moments, unit_out, omega, fitted, fit_alpha, partial, small;
@@ -1690,46 +1693,79 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
     } else {
       // full-model solves: beta = -S^{-1} Q'W X theta_fe per column, then the
       // row-level contraction over match groups
-      std::vector<double> t(QMAX * K, 0.0), beta(QMAX * K, 0.0);
-      if (e.q > 0) {
-        k_target_control_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.q, e.cell_worker.p, e.cell_firm.p,
-                                                               e.cellQ.p, w.alpha.p, w.x.p, e.partial.p);
-        finish(e.partial.p, L.grid, QMAX * K, w.tot.p, L.s);
-        CK(cudaMemcpyAsync(t.data(), w.tot.p, QMAX * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
-        CK(cudaStreamSynchronize(L.s));
-      }
-      for (int k = 0; k < e.q; ++k)
-        for (int j = 0; j < K; ++j) {
-          double v = 0.0;
-          for (int l = 0; l < e.q; ++l) v -= e.Sinv[k * e.q + l] * t[l * K + j];
-          beta[k * K + j] = v;
+      std::vector<double> t(QMAX * K, 0.0), beta(QMAX * K, 0.0), g2(2 * K, 0.0);
+      auto solve_beta = [&] {
+        for (int k = 0; k < e.q; ++k)
+          for (int j = 0; j < K; ++j) {
+            double v = 0.0;
+            for (int l = 0; l < e.q; ++l) v -= e.Sinv[k * e.q + l] * t[l * K + j];
+            beta[k * K + j] = v;
+          }
+      };
+      if (e.observation) {
+        // one pass over the cells: the control sums and the draws' beta-free parts
+        if (!e.obs_fused.p) {
+          e.obs_fused.alloc(2 * (QMAX + 1) * 128);
+          e.partial2.alloc(size_t(L.grid) * (QMAX + 1) * 128 + 1024);
         }
-      CK(cudaMemcpyAsync(e.beta_buf.p, beta.data(), QMAX * K * sizeof(double), cudaMemcpyHostToDevice, L.s));
-      if (e.observation && o.numerical)  // the attachment's per-row target folds of this block
-        k_obs_num_folds<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.q, uint64_t(first), np, e.unit_ptr.p, e.cell_rows.p,
-                                                        e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p,
-                                                        e.beta_buf.p, e.Rd.p, e.row_y.p, y_center, e.residual.p,
-                                                        double((o.probes + 1) / 2), double(o.probes / 2),
-                                                        e.num_row_fold.p);
-      if (e.observation)
-        k_obs_contract_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.q, e.cell_worker.p, e.cell_firm.p,
-                                                             e.obs_cell_sums.p, e.beta_buf.p, w.alpha.p, w.x.p,
-                                                             e.partial.p);
-      else
+        k_obs_target_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.q, e.cell_worker.p, e.cell_firm.p,
+                                                           e.q > 0 ? e.cellQ.p : nullptr, e.obs_cell_sums.p,
+                                                           w.alpha.p, w.x.p, e.partial.p, e.partial2.p);
+        finish(e.partial.p, L.grid, (QMAX + 1) * K, e.obs_fused.p, L.s);
+        finish(e.partial2.p, L.grid, (QMAX + 1) * K, e.obs_fused.p + (QMAX + 1) * K, L.s);
+        std::vector<double> f(2 * (QMAX + 1) * K);
+        CK(cudaMemcpyAsync(f.data(), e.obs_fused.p, f.size() * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+        CK(cudaStreamSynchronize(L.s));
+        res.timings.kernel_launches += 3;
+        const double* A = f.data() + QMAX * K;
+        const double* B = f.data() + (QMAX + 1) * K;
+        const double* Atot = f.data() + (2 * QMAX + 1) * K;
+        for (int k = 0; k < e.q; ++k)
+          for (int j = 0; j < K; ++j) t[k * K + j] = f[k * K + j];
+        solve_beta();
+        for (int j = 0; j < K; ++j) {
+          double v = A[j];
+          for (int k = 0; k < e.q; ++k) v += 2.0 * B[k * K + j] * beta[k * K + j];
+          g2[j] = v;
+        }
+        for (int j = 0; j + 1 < K; j += 2) {
+          double v = Atot[j];
+          for (int k = 0; k < e.q; ++k)
+            v += 2.0 * (B[k * K + j] + B[k * K + j + 1]) * (beta[k * K + j] + beta[k * K + j + 1]);
+          g2[K + j] = v;
+        }
+        if (o.numerical) {  // the attachment's per-row target folds of this block
+          CK(cudaMemcpyAsync(e.beta_buf.p, beta.data(), QMAX * K * sizeof(double), cudaMemcpyHostToDevice, L.s));
+          k_obs_num_folds<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.q, uint64_t(first), np, e.unit_ptr.p,
+                                                          e.cell_rows.p, e.cell_worker.p, e.cell_firm.p, w.alpha.p,
+                                                          w.x.p, e.beta_buf.p, e.Rd.p, e.row_y.p, y_center,
+                                                          e.residual.p, double((o.probes + 1) / 2),
+                                                          double(o.probes / 2), e.num_row_fold.p);
+        }
+      } else {
+        if (e.q > 0) {
+          k_target_control_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.q, e.cell_worker.p, e.cell_firm.p,
+                                                                 e.cellQ.p, w.alpha.p, w.x.p, e.partial.p);
+          finish(e.partial.p, L.grid, QMAX * K, w.tot.p, L.s);
+          CK(cudaMemcpyAsync(t.data(), w.tot.p, QMAX * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+          CK(cudaStreamSynchronize(L.s));
+        }
+        solve_beta();
+        CK(cudaMemcpyAsync(e.beta_buf.p, beta.data(), QMAX * K * sizeof(double), cudaMemcpyHostToDevice, L.s));
         k_generic_contract_units<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.q, e.unit_cell.p, e.cell_worker.p,
                                                                  e.cell_firm.p, e.unit_sums.p, e.beta_buf.p,
                                                                  w.alpha.p, w.x.p, e.partial.p);
-      if (!e.observation && o.numerical)  // the attachment's match-unit target folds of this block
-        k_num_block_folds<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.q, uint64_t(first), np, e.unit_cell.p,
-                                                          e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p,
-                                                          e.beta_buf.p, e.num_block_sums.p,
-                                                          double((o.probes + 1) / 2), double(o.probes / 2),
-                                                          e.num_unit_fold.p);
-      finish(e.partial.p, L.grid, 2 * K, w.tot.p, L.s);
-      std::vector<double> g2(2 * K);
-      CK(cudaMemcpyAsync(g2.data(), w.tot.p, 2 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
-      CK(cudaStreamSynchronize(L.s));
-      res.timings.kernel_launches += 4;
+        if (o.numerical)  // the attachment's match-unit target folds of this block
+          k_num_block_folds<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.q, uint64_t(first), np, e.unit_cell.p,
+                                                            e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p,
+                                                            e.beta_buf.p, e.num_block_sums.p,
+                                                            double((o.probes + 1) / 2), double(o.probes / 2),
+                                                            e.num_unit_fold.p);
+        finish(e.partial.p, L.grid, 2 * K, w.tot.p, L.s);
+        CK(cudaMemcpyAsync(g2.data(), w.tot.p, 2 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+        CK(cudaStreamSynchronize(L.s));
+        res.timings.kernel_launches += 4;
+      }
       if (e.observation && e.q > 0) {
         // the cell-independent beta' S2 beta terms of every column and of the total
         auto quad = [&](int ja, int jb) {
@@ -2661,6 +2697,7 @@ SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& pl
   SolveResult res;
   int K = o.block_columns;
   if (K == 0) K = 64;
+  const uint64_t launches0 = kernel_launch_count();
   if (e.generic) {
     switch (K) {
       case 2: run_generic<2>(e, p, plan, o, res, want_unit_detail); break;
@@ -2670,6 +2707,7 @@ SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& pl
       case 64: run_generic<64>(e, p, plan, o, res, want_unit_detail); break;
       default: fail(INVALID_INPUT, "jla_validate", "device block width must be 2, 8, 16, 32 or 64");
     }
+    res.timings.kernel_launches = kernel_launch_count() - launches0;  // every launch of the solve
     return res;
   }
   switch (K) {
@@ -2680,6 +2718,7 @@ SolveResult device_solve(DeviceEngine& e, const Compressed& p, const JlaPlan& pl
     case 64: run_jla<64>(e, p, plan, o, res, want_unit_detail); break;
     default: fail(INVALID_INPUT, "jla_validate", "device block width must be 2, 8, 16, 32 or 64");
   }
+  res.timings.kernel_launches = kernel_launch_count() - launches0;  // every launch of the solve
   return res;
 }
 

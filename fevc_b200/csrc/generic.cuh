@@ -487,35 +487,39 @@ __global__ void k_obs_cell_target_sums(uint32_t cells, int q, const uint32_t* __
   }
 }
 
-// Leave-observation-out target draws over cells from k_obs_cell_target_sums:
-// draw_col += S0 u^2 + 2 u (S1' beta_col) per cell, the total side with
-// u = u_worker + u_firm and beta = beta_worker + beta_firm (the sum of the two
-// columns); the cell-independent beta' S2 beta terms are added by the host.
-// partial layout as in k_generic_contract.
+// Leave-observation-out target pass over cells, one read of every cell's
+// predictions u = alpha_w + psi_f per block: per column the control sums
+// t_k = sum_c CQ_ck u_c (the full-model control correction, as
+// k_target_control_cells) and the beta-free parts of the target draw from
+// k_obs_cell_target_sums' per-cell sums S0, S1: A = sum_c S0_c u_c^2,
+// B_k = sum_c u_c S1_ck, and per probe (even columns) A_tot of the total side
+// u_worker + u_firm.  With beta = -S^{-1} t the host forms the draws
+// A + 2 B'beta + beta' S2 beta (the cell sum of S0 u^2 + 2 u S1'beta plus the
+// cell-independent quadratic term).
+// partial: [blk][9][K] = (t_0 .. t_7, A); partial2: [blk][9][K] = (B_0 .. B_7, A_tot).
 template <int K>
-__global__ void k_obs_contract_cells(uint32_t cells, int q, const uint32_t* __restrict__ cell_worker,
-                                     const uint32_t* __restrict__ cell_firm, const double* __restrict__ sums,
-                                     const double* __restrict__ beta /* [QMAX][K] */, const double* __restrict__ alpha,
-                                     const double* __restrict__ psi, double* __restrict__ partial) {
+__global__ void k_obs_target_cells(uint32_t cells, int q, const uint32_t* __restrict__ cell_worker,
+                                   const uint32_t* __restrict__ cell_firm, const double* __restrict__ CQ,
+                                   const double* __restrict__ sums, const double* __restrict__ alpha,
+                                   const double* __restrict__ psi, double* __restrict__ partial,
+                                   double* __restrict__ partial2) {
   constexpr int CPT = Cols<K>::CPT, TPR = Cols<K>::TPR;
   static_assert(CPT <= 2, "pairs of columns must sit in one thread or in adjacent lanes");
-  double v[2][CPT];
+  static_assert(QMAX == 8, "nine sums per reduction");
+  double v1[QMAX + 1][CPT], v2[QMAX + 1][CPT];
 #pragma unroll
-  for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
+  for (int k = 0; k <= QMAX; ++k)
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) v1[k][c] = v2[k][c] = 0.0;
   const int c0 = int(threadIdx.x % TPR) * CPT;
-  double bcol[QMAX][CPT];
-#pragma unroll
-  for (int k = 0; k < QMAX; ++k)
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) bcol[k][c] = k < q ? beta[k * K + c0 + c] : 0.0;
   size_t total = size_t(cells) * TPR, stride = size_t(gridDim.x) * blockDim.x;
   for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
     size_t t = base + threadIdx.x;
     bool live = t < total;
     size_t c = live ? t / TPR : 0;
-    double u[CPT], b1[CPT], s0 = 0.0;
+    double u[CPT], s0 = 0.0;
 #pragma unroll
-    for (int cc = 0; cc < CPT; ++cc) u[cc] = b1[cc] = 0.0;
+    for (int cc = 0; cc < CPT; ++cc) u[cc] = 0.0;
     if (live) {
       const double* sc = sums + c * size_t(1 + q);
       s0 = sc[0];
@@ -525,24 +529,27 @@ __global__ void k_obs_contract_cells(uint32_t cells, int q, const uint32_t* __re
 #pragma unroll
       for (int k = 0; k < QMAX; ++k)
         if (k < q) {
-          const double s1 = sc[1 + k];
+          const double cq = CQ[c * QMAX + k], s1 = sc[1 + k];
 #pragma unroll
-          for (int cc = 0; cc < CPT; ++cc) b1[cc] += s1 * bcol[k][cc];
+          for (int cc = 0; cc < CPT; ++cc) {
+            v1[k][cc] += u[cc] * cq;
+            v2[k][cc] += u[cc] * s1;
+          }
         }
-    }
 #pragma unroll
-    for (int cc = 0; cc < CPT; ++cc) v[0][cc] += s0 * u[cc] * u[cc] + 2.0 * u[cc] * b1[cc];
+      for (int cc = 0; cc < CPT; ++cc) v1[QMAX][cc] += s0 * u[cc] * u[cc];
+    }
     if (CPT == 2) {
-      const double uu = u[0] + u[CPT - 1], bb = b1[0] + b1[CPT - 1];
-      v[1][0] += s0 * uu * uu + 2.0 * uu * bb;
+      const double uu = u[0] + u[CPT - 1];
+      v2[QMAX][0] += s0 * uu * uu;
     } else {
       const double uo = __shfl_xor_sync(0xffffffffu, u[0], 1);
-      const double bo = __shfl_xor_sync(0xffffffffu, b1[0], 1);
-      const double uu = u[0] + uo, bb = b1[0] + bo;
-      if ((c0 & 1) == 0) v[1][0] += s0 * uu * uu + 2.0 * uu * bb;
+      const double uu = u[0] + uo;
+      if ((c0 & 1) == 0) v2[QMAX][0] += s0 * uu * uu;
     }
   }
-  block_reduce_cols<K, 2>(v, partial);
+  block_reduce_cols<K, QMAX + 1>(v1, partial);
+  block_reduce_cols<K, QMAX + 1>(v2, partial2);
 }
 
 // Cell-level control sums of the target solutions: partial[blk][k][col] =

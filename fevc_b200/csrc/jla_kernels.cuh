@@ -25,45 +25,95 @@ __global__ void k_extract_residual(uint32_t W, uint32_t F, const uint32_t* __res
   double v[2][CPT];
 #pragma unroll
   for (int c = 0; c < CPT; ++c) v[0][c] = v[1][c] = 0.0;
-  size_t total = size_t(W) * TPR, stride = size_t(gridDim.x) * blockDim.x;
-  for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
-    size_t t = base + threadIdx.x;
-    // with one warp per worker (TPR = 32) the whole warp is live or not
-    if (t < total) {
-      size_t w = t / TPR;
-      int c0 = int(t % TPR) * CPT;
-      double acc[CPT], b[CPT];
+  auto finish_worker = [&](size_t w, int c0, int32_t k, double d, const double (&acc)[CPT], const double (&b)[CPT]) {
+    const double inv = 1.0 / d;
 #pragma unroll
-      for (int c = 0; c < CPT; ++c) acc[c] = b[c] = bW[w * K + c0 + c];
-      if constexpr (TPR == 32) {
-        // the worker's cells 32 at a time, loaded lane-parallel; acc -= w_c psi
-        const int lane = threadIdx.x & 31;
-        for (uint32_t i0 = worker_ptr[w], i1 = worker_ptr[w + 1]; i0 < i1; i0 += 32) {
-          uint32_t cnt = i1 - i0 < 32 ? i1 - i0 : 32, my_j = 0;
-          double my_a = 0.0;
-          if (uint32_t(lane) < cnt) {
-            my_j = cell_firm[i0 + lane];
-            my_a = -cell_weight[i0 + lane];
-          }
-          warp_gather<K, double>(my_j, my_a, cnt, x, c0, acc);
+    for (int c = 0; c < CPT; ++c) {
+      double al = k >= 0 ? -x[(size_t(F) + k) * K + c0 + c] : acc[c] * inv;
+      alpha[w * K + c0 + c] = al;
+      double r = acc[c] - d * al;
+      v[0][c] += r * r;
+      v[1][c] += b[c] * b[c];
+    }
+  };
+  if constexpr (TPR == 32) {
+    // one warp per 32 consecutive workers: their cell ranges, kept indices and
+    // diagonals, and their cells 32 at a time, are loaded lane-parallel and
+    // broadcast, so a worker waits only on its own row and its firms' rows;
+    // acc = bW - sum_c w_c psi_f(c) in cell order
+    const int lane = threadIdx.x & 31, c0 = lane * CPT;
+    const size_t nwarps = size_t(gridDim.x) * blockDim.x / 32;
+    for (size_t w0 = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32 * 32; w0 < W; w0 += nwarps * 32) {
+      const int nw = int(W - w0 < 32 ? W - w0 : 32);
+      uint32_t my_b = 0, my_e = 0;
+      int32_t my_k = -1;
+      double my_d = 1.0;
+      if (lane < nw) {
+        my_b = worker_ptr[w0 + lane];
+        my_e = worker_ptr[w0 + lane + 1];
+        my_k = kept_index[w0 + lane];
+        my_d = worker_diag[w0 + lane];
+      }
+      uint32_t at = __shfl_sync(0xffffffffu, my_b, 0);  // first cell of the loaded chunk
+      const uint32_t last = __shfl_sync(0xffffffffu, my_e, nw - 1);
+      uint32_t my_f = 0;
+      double my_a = 0.0;
+      auto load_chunk = [&](uint32_t from) {
+        at = from;
+        my_f = 0;
+        my_a = 0.0;
+        if (from + uint32_t(lane) < last) {
+          my_f = cell_firm[from + lane];
+          my_a = -cell_weight[from + lane];
         }
-      } else {
+      };
+      load_chunk(at);
+      for (int j = 0; j < nw; ++j) {
+        const uint32_t b = __shfl_sync(0xffffffffu, my_b, j), e = __shfl_sync(0xffffffffu, my_e, j);
+        const int32_t k = __shfl_sync(0xffffffffu, my_k, j);
+        const double d = __shfl_sync(0xffffffffu, my_d, j);
+        const size_t w = w0 + size_t(j);
+        double acc[CPT], bv[CPT];
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] = bv[c] = bW[w * K + c0 + c];
+        constexpr int U = 4;
+        for (uint32_t i = b; i < e; i += U) {
+          if (i + U > at + 32) load_chunk(i);  // the next items lie past the loaded chunk
+          double xv[U][CPT], av[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int src = int(i + u - at) & 31;
+            const uint32_t f = __shfl_sync(0xffffffffu, my_f, src);
+            av[u] = __shfl_sync(0xffffffffu, my_a, src);
+            if (i + u < e) load_cols<K, double>(x, f, c0, xv[u]);
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+            if (i + u < e) {
+#pragma unroll
+              for (int c = 0; c < CPT; ++c) acc[c] += av[u] * xv[u][c];
+            }
+        }
+        finish_worker(w, c0, k, d, acc, bv);
+      }
+    }
+  } else {
+    size_t total = size_t(W) * TPR, stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t base = size_t(blockIdx.x) * blockDim.x; base < total; base += stride) {
+      size_t t = base + threadIdx.x;
+      if (t < total) {
+        size_t w = t / TPR;
+        int c0 = int(t % TPR) * CPT;
+        double acc[CPT], b[CPT];
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] = b[c] = bW[w * K + c0 + c];
         for (uint32_t i = worker_ptr[w]; i < worker_ptr[w + 1]; ++i) {
           double a = cell_weight[i];
           size_t fb = size_t(cell_firm[i]) * K + c0;
 #pragma unroll
           for (int c = 0; c < CPT; ++c) acc[c] -= a * x[fb + c];
         }
-      }
-      int32_t k = kept_index[w];
-      double d = worker_diag[w], inv = 1.0 / d;
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) {
-        double al = k >= 0 ? -x[(size_t(F) + k) * K + c0 + c] : acc[c] * inv;
-        alpha[w * K + c0 + c] = al;
-        double r = acc[c] - d * al;
-        v[0][c] += r * r;
-        v[1][c] += b[c] * b[c];
+        finish_worker(w, c0, kept_index[w], worker_diag[w], acc, b);
       }
     }
   }

@@ -262,7 +262,20 @@ __global__ void __launch_bounds__(THREADS) k_obs_moments_cells(
       neumaier_add(a[0], a[1], s2);
       neumaier_add(a[2], a[3], s4);
     }
-    // copies, unit after unit (the whole warp on each copy's columns)
+    // copies, unit after unit (the whole warp on each copy's columns); the
+    // k-th copy's sums stay with lane k, and up to 32 copies' accumulators
+    // are updated together, one lane each
+    uint32_t held = 0;
+    uint64_t my_copy = 0;
+    double my_f1 = 0.0, my_f3 = 0.0;
+    auto flush = [&] {
+      if (uint32_t(lane) < held) {
+        double* a = copy_acc + size_t(my_copy) * 4;
+        neumaier_add(a[0], a[1], my_f1);
+        neumaier_add(a[2], a[3], my_f3);
+      }
+      held = 0;
+    };
     for (uint32_t u = 0; u < cnt; ++u) {
       uint64_t ph, n, bits;
       if (u < 32) {
@@ -288,13 +301,15 @@ __global__ void __launch_bounds__(THREADS) k_obs_moments_cells(
           f1 += __shfl_xor_sync(0xffffffffu, f1, o);
           f3 += __shfl_xor_sync(0xffffffffu, f3, o);
         }
-        if (lane == 0) {
-          double* a = copy_acc + size_t(ph + i) * 4;
-          neumaier_add(a[0], a[1], f1);
-          neumaier_add(a[2], a[3], f3);
+        if (uint32_t(lane) == held) {
+          my_copy = ph + i;
+          my_f1 = f1;
+          my_f3 = f3;
         }
+        if (++held == 32) flush();
       }
     }
+    flush();
   }
 }
 
