@@ -197,6 +197,40 @@ class NumericalRhsV1(Struct):
                 ("complete_residual", f64)]
 
 
+class ProjectionAugmentationRequestV1(Struct):
+    _fields_ = [("abi_version", u32), ("struct_size", u32), ("rows", u64), ("project_count", u32), ("effect", u32),
+                ("weight", u32), ("reserved", u32), ("rank_tolerance", f64), ("caller_copy_bytes", u64)]
+
+
+class ProjectionAugmentationRequestInterruptV1(Struct):
+    _fields_ = [("options", ProjectionAugmentationRequestV1), ("interrupt_poll", C.c_void_p),
+                ("interrupt_context", C.c_void_p), ("checkpoint_interval", u32), ("reserved", u32)]
+
+
+class ProjectionColumnsV1(Struct):
+    _fields_ = [("struct_size", u32), ("reserved", u32), ("rows", u64), ("project", C.POINTER(C.POINTER(f64))),
+                ("project_count", u32), ("reserved_2", u32)]
+
+
+class ProjectionAugmentationReceiptV1(Struct):
+    _fields_ = [("struct_size", u32), ("schema_version", u32), ("generation", u64), ("rows", u64), ("columns", u64),
+                ("effect", u32), ("weight", u32), ("caller_copy_bytes", u64),
+                ("augmentation_peak_forecast_bytes", u64), ("projection_persistent_bytes", u64),
+                ("total_prepared_resident_bytes", u64), ("gram_rcond", f64), ("gram_relres", f64),
+                ("gram_original_relres", f64)]
+
+
+class ProjectionResultReceiptV1(Struct):
+    _fields_ = [("struct_size", u32), ("schema_version", u32), ("generation", u64), ("columns", u64),
+                ("effect", u32), ("weight", u32), ("gram_rcond", f64), ("gram_relres", f64),
+                ("gram_original_relres", f64), ("covariance_smallest_eigenvalue", f64),
+                ("covariance_largest_eigenvalue", f64), ("psd_cleanup", f64), ("proxy_minimum", f64),
+                ("proxy_maximum", f64), ("maximum_iterations", u32), ("reserved", u32),
+                ("maximum_reduced_residual", f64), ("maximum_complete_residual", f64),
+                ("full_residual_tolerance", f64), ("projection_peak_forecast_bytes", u64), ("persistent_bytes", u64),
+                ("result_bytes", u64)]
+
+
 class PreparationReceiptV2(Struct):
     _fields_ = [("struct_size", u32), ("reserved", u32)] + [(n, u64) for n in (
         "generation", "input_rows", "retained_rows", "workers", "firms", "cells", "deletion_units", "target_strata",
@@ -508,6 +542,12 @@ def cmg_aggregate(lib, ptr: np.ndarray, col: np.ndarray, weight: np.ndarray, thr
 
 
 SIGNATURES = {
+    "vckss_rust_engine_augment_projection_interrupt_v1": (i32, [u64, C.c_void_p, C.c_void_p]),
+    "vckss_rust_engine_default_projection_augmentation_request_interrupt_v1": (i32, [C.c_void_p, u32]),
+    "vckss_rust_engine_projection_augmentation_receipt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_projection_result_receipt_v1": (i32, [u64, C.c_void_p, u32]),
+    "vckss_rust_engine_projection_result_v1": (i32, [u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u32]),
+    "vckss_rust_projection_centering_schema_v1": (u32, []),
     "vckss_rust_abi_version": (u32, []),
     "vckss_rust_backend_version": (C.c_char_p, []),
     "vckss_rust_capabilities_json": (C.c_char_p, []),
@@ -622,7 +662,6 @@ UNSUPPORTED_SIGNATURES = {
     "vckss_rust_engine_augment_match_component_inference_interrupt_v3": (i32, [u64, C.c_void_p]),
     "vckss_rust_engine_augment_match_component_inference_interrupt_v4": (i32, [u64, C.c_void_p, u32]),
     "vckss_rust_engine_augment_match_component_inference_interrupt_v5": (i32, [u64, C.c_void_p, u32]),
-    "vckss_rust_engine_augment_projection_interrupt_v1": (i32, [u64, C.c_void_p, C.c_void_p]),
     "vckss_rust_engine_augment_stayers_interrupt_v1": (i32, [u64, C.c_void_p, C.c_void_p]),
     "vckss_rust_engine_augment_stayers_v1": (i32, [u64, C.c_void_p, C.c_void_p]),
     "vckss_rust_engine_component_batch_receipt_v1": (i32, [u64, C.c_void_p, u32]),
@@ -634,7 +673,6 @@ UNSUPPORTED_SIGNATURES = {
     "vckss_rust_engine_component_inference_unit_receipt_v1": (i32, [u64, C.c_void_p, u32]),
     "vckss_rust_engine_component_inference_unit_receipt_v2": (i32, [u64, C.c_void_p, u32]),
     "vckss_rust_engine_default_component_inference_augmentation_request_interrupt_v1": (i32, [C.c_void_p, u32]),
-    "vckss_rust_engine_default_projection_augmentation_request_interrupt_v1": (i32, [C.c_void_p, u32]),
     "vckss_rust_engine_default_solve_request_interrupt_v2": (i32, [C.c_void_p, u32]),
     "vckss_rust_engine_default_solve_request_interrupt_v3": (i32, [C.c_void_p, u32]),
     "vckss_rust_engine_default_solve_request_interrupt_v4": (i32, [C.c_void_p, u32]),
@@ -655,9 +693,6 @@ UNSUPPORTED_SIGNATURES = {
     "vckss_rust_engine_performance_receipt_v1": (i32, [u64, C.c_void_p, u32]),
     "vckss_rust_engine_prepare_interrupt_v3": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u32]),
     "vckss_rust_engine_prepare_memory_interrupt_v1": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, u32]),
-    "vckss_rust_engine_projection_augmentation_receipt_v1": (i32, [u64, C.c_void_p, u32]),
-    "vckss_rust_engine_projection_result_receipt_v1": (i32, [u64, C.c_void_p, u32]),
-    "vckss_rust_engine_projection_result_v1": (i32, [u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, u32]),
     "vckss_rust_engine_repeat_measurement_diagnostic_v1": (i32, [u64, C.c_void_p, u32]),
     "vckss_rust_engine_repeat_measurement_leading_v1": (i32, [u64, C.c_void_p, u32]),
     "vckss_rust_engine_solve_exact_execution_interrupt_v1": (i32, [u64, C.c_void_p]),
@@ -682,7 +717,6 @@ UNSUPPORTED_SIGNATURES = {
     "vckss_rust_exact_resolved_execution_schema_v2": (u32, []),
     "vckss_rust_numerical_schema_v1": (u32, []),
     "vckss_rust_numerical_schema_v2": (u32, []),
-    "vckss_rust_projection_centering_schema_v1": (u32, []),
     "vckss_rust_report_call_v1": (i32, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "vckss_rust_session_clear_abandoned_v1": (i32, []),
     "vckss_rust_session_last_error": (C.c_char_p, []),
@@ -878,6 +912,45 @@ class Engine:
         count = u64(0)
         self.check(self.lib.vckss_rust_engine_numerical_rhs_v1(self.generation, arr, rows, C.byref(count)))
         return count.value, [arr[i].as_dict() for i in range(min(rows, count.value))]
+
+    # ---- fixed-effect projection attachment
+    def augment_projection(self, columns, effect: int = 1, weight: int = 1, rank_tolerance: float = 1e-10) -> None:
+        """Attach a projection of the worker (effect 1) or firm (2) effect on
+        the given covariates (one float64 array per covariate, one value per
+        retained row), weighted by frequency (1) or target weight (2)."""
+        cols = [np.ascontiguousarray(c, dtype=np.float64) for c in columns]
+        rows = len(cols[0])
+        q = ProjectionAugmentationRequestInterruptV1()
+        self.check(self.lib.vckss_rust_engine_default_projection_augmentation_request_interrupt_v1(
+            C.byref(q), C.sizeof(q)))
+        q.options.rows = rows
+        q.options.project_count = len(cols)
+        q.options.effect = effect
+        q.options.weight = weight
+        q.options.rank_tolerance = rank_tolerance
+        q.options.caller_copy_bytes = rows * len(cols) * 8
+        ptrs = (C.POINTER(f64) * len(cols))(*[c.ctypes.data_as(C.POINTER(f64)) for c in cols])
+        d = ProjectionColumnsV1(C.sizeof(ProjectionColumnsV1), 0, rows, ptrs, len(cols), 0)
+        self.check(self.lib.vckss_rust_engine_augment_projection_interrupt_v1(self.generation, C.byref(q), C.byref(d)))
+
+    def projection_augmentation_receipt(self) -> dict:
+        r = ProjectionAugmentationReceiptV1()
+        self.check(self.lib.vckss_rust_engine_projection_augmentation_receipt_v1(self.generation, C.byref(r),
+                                                                                C.sizeof(r)))
+        return r.as_dict()
+
+    def projection_result(self) -> dict:
+        """Coefficients, KSS and naive covariances (columns x columns) and the
+        result receipt of the last solve's projection."""
+        r = ProjectionResultReceiptV1()
+        self.check(self.lib.vckss_rust_engine_projection_result_receipt_v1(self.generation, C.byref(r), C.sizeof(r)))
+        n = int(r.columns)
+        coef, cov, naive = np.zeros(n), np.zeros(n * n), np.zeros(n * n)
+        p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        self.check(self.lib.vckss_rust_engine_projection_result_v1(self.generation, p(coef), n, p(cov), n * n,
+                                                                   p(naive), n * n, C.byref(r), C.sizeof(r)))
+        return {"coefficients": coef.tolist(), "covariance": cov.reshape(n, n).tolist(),
+                "naive_covariance": naive.reshape(n, n).tolist(), "receipt": r.as_dict()}
 
     def result(self) -> dict:
         r = ResultV1()

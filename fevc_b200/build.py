@@ -21,7 +21,8 @@ INCLUDE = HERE.parent / "include"
 BUILD = HERE / "_build"
 LIB = HERE / "libfevc_b200.so"
 
-CXX_SOURCES = ["prep.cpp", "abi.cpp", "hybrid.cpp", "cmg_host.cpp", "abi_unsupported.cpp", "numerical.cpp"]
+CXX_SOURCES = ["prep.cpp", "abi.cpp", "hybrid.cpp", "cmg_host.cpp", "abi_unsupported.cpp", "numerical.cpp",
+               "projection.cpp"]
 CU_SOURCES = ["engine.cu", "multigrid.cu", "noalloc.cu", "learned.cu", "devmem.cu"]
 GENCODE = "-gencode=arch=compute_100a,code=sm_100a"
 
@@ -77,7 +78,10 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
     if jobs or not LIB.exists():
         tmp = LIB.with_suffix(".so.tmp")
         _run([nvcc, GENCODE, "-shared", "-cudart", "static", "-o", str(tmp)] + [str(o) for o in objs]
-             + ["-Xcompiler", "-fopenmp", "-Xlinker", "--no-undefined"])
+             + ["-Xcompiler", "-fopenmp", "-Xlinker", "--no-undefined",
+                # every kernel launch passes through these two runtime calls;
+                # the wrappers in devmem.cu count them
+                "-Xlinker", "--wrap=cudaLaunchKernel", "-Xlinker", "--wrap=cudaLaunchCooperativeKernel"])
         os.replace(tmp, LIB)
     return LIB
 

@@ -109,6 +109,8 @@ struct Prepared {
   // host preparation phases, wall milliseconds: ingest copy, canonical ids,
   // graph fixed point, compression, JLA plan
   double prepare_ms[5] = {0, 0, 0, 0, 0};
+  // fixed-effect projection attached before the first solve
+  std::shared_ptr<PreparedProjection> projection;
 };
 
 struct Registry {
@@ -134,8 +136,8 @@ Registry& reg() {
 template <class T>
 void require_capacity(const void* p, uint64_t cap, const char* label) {
   if (!p) fail(INVALID_INPUT, "engine_ffi", std::string(label) + " pointer is null");
-  if (cap < sizeof(T))
-    fail(INVALID_INPUT, "engine_ffi",
+  if (cap < sizeof(T))  // a short output is an ABI mismatch (ffi_engine.rs `require_output_capacity`)
+    fail(ABI_MISMATCH, "engine_ffi",
          std::string(label) + " capacity " + std::to_string(cap) + " is below " + std::to_string(sizeof(T)));
 }
 
@@ -518,6 +520,12 @@ void solve_common(uint64_t g, SolveOptions o, const Interrupt& intr, bool generi
   if (o.deletion_mode != p.deletion_mode)
     fail(INVALID_INPUT, "engine_solve", "solve deletion mode differs from the prepared graph mode");
   if (o.algorithm == 1) exact_gate(p, o);
+  if (p.projection) {  // ffi_engine.rs:4936-4944
+    if (!p.plan.generic || o.algorithm == 1)
+      fail(UNSUPPORTED_FEATURE, "engine_solve",
+           "prepared projection or component-inference attachments require the generic JLA engine");
+    o.projection = p.projection.get();
+  }
   r.state = State::Solving;
   try {
     intr.check("jla_full_fit");
@@ -1678,6 +1686,8 @@ int32_t fevcb_engine_solve_sets_v1(uint64_t generation, const VckssEngineSolveRe
     Registry& r = reg();
     std::lock_guard<std::mutex> l(r.mu);
     Prepared& p = r.require(generation, "probe_sets");
+    if (p.projection)
+      fail(UNSUPPORTED_FEATURE, "probe_sets", "probe sets do not carry a projection attachment");
     put(0, *r.result);
     for (uint32_t i = 1; i < count; ++i) {
       SolveOptions o = p.last_options;
@@ -1849,6 +1859,7 @@ int32_t fevcb_engine_shard_leverage_v1(uint64_t generation, const VckssEngineSol
     Prepared& p = reg().require(generation, "engine_shard");
     if (!acc || count != shard_accumulator_count(p.problem, p.plan))
       fail(INVALID_INPUT, "shard", "accumulator buffer has the wrong length");
+    if (p.projection) fail(UNSUPPORTED_FEATURE, "shard", "probe shards do not carry a projection attachment");
     SolveOptions o = shard_options(p, request, begin, end);
     o.shard_phase = 1;
     o.shard_output = acc;  // host or device memory: copied by unified addressing
@@ -2117,6 +2128,204 @@ int32_t fevcb_counter_atoms_v1(uint64_t seed, uint64_t domain_tag, uint64_t firs
 
 }  // extern "C"
 
+// ---- fixed-effect projection attachment (reference ffi_engine.rs:2413-2418,
+// 2883-2899, 3679-3835, 6030-6110, 9766-9846; session_retained.rs:443-613)
+
+namespace {
+
+const ProjectionResult& projection_of(uint64_t g, const char* phase) {
+  reg().require(g, phase);
+  if (reg().state != State::Solved || !reg().result)
+    fail(CONTEXT_POISONED, "context_export", "generation " + std::to_string(g) + " has no solved result");
+  const ProjectionResult& r = reg().result->projection;
+  if (!r.present) fail(UNSUPPORTED_FEATURE, phase, "the solved generation has no projection result");
+  return r;
+}
+
+VckssProjectionResultReceiptV1 projection_receipt(uint64_t g, const ProjectionResult& r) {
+  VckssProjectionResultReceiptV1 v{};
+  v.struct_size = sizeof(v);
+  v.schema_version = VCKSS_PROJECTION_SCHEMA_V1;
+  v.generation = g;
+  v.columns = r.columns;
+  v.effect = uint32_t(r.effect);
+  v.weight = uint32_t(r.weight);
+  v.gram_rcond = r.gram_rcond;
+  v.gram_relres = r.gram_relres;
+  v.gram_original_relres = r.gram_original_relres;
+  v.covariance_smallest_eigenvalue = r.covariance_smallest_eigenvalue;
+  v.covariance_largest_eigenvalue = r.covariance_largest_eigenvalue;
+  v.psd_cleanup = r.psd_cleanup;
+  v.proxy_minimum = r.proxy_minimum;
+  v.proxy_maximum = r.proxy_maximum;
+  v.maximum_iterations = r.maximum_iterations;
+  v.maximum_reduced_residual = r.maximum_reduced_residual;
+  v.maximum_complete_residual = r.maximum_complete_residual;
+  v.full_residual_tolerance = r.full_residual_tolerance;
+  v.projection_peak_forecast_bytes = r.projection_peak_forecast_bytes;
+  v.persistent_bytes = r.persistent_bytes;
+  v.result_bytes = r.result_bytes;
+  return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t vckss_rust_projection_centering_schema_v1(void) { return 1; }
+
+int32_t vckss_rust_engine_default_projection_augmentation_request_interrupt_v1(
+    VckssProjectionAugmentationRequestInterruptV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssProjectionAugmentationRequestInterruptV1>(out, cap, "projection augmentation request");
+    VckssProjectionAugmentationRequestInterruptV1 v{};
+    v.options.abi_version = VCKSS_RUST_ABI_VERSION_V1;
+    v.options.struct_size = sizeof(VckssProjectionAugmentationRequestInterruptV1);
+    v.options.effect = VCKSS_PROJECTION_EFFECT_WORKER;
+    v.options.weight = VCKSS_PROJECTION_WEIGHT_FREQUENCY;
+    v.options.rank_tolerance = 1e-10;
+    std::memcpy(out, &v, sizeof(v));
+  });
+}
+
+int32_t vckss_rust_engine_augment_projection_interrupt_v1(uint64_t generation,
+                                                           const VckssProjectionAugmentationRequestInterruptV1* request,
+                                                           const VckssProjectionColumnsV1* columns) {
+  return status([&] {
+    auto q = read_struct(request, "projection augmentation request");
+    Interrupt intr(q.interrupt_poll, q.interrupt_context, q.checkpoint_interval, q.reserved, "projection_augmentation");
+    intr.check("engine_projection_augmentation_entry");
+    const VckssProjectionAugmentationRequestV1& o = q.options;
+    require_abi(o.abi_version);
+    if (o.struct_size < sizeof(VckssProjectionAugmentationRequestV1) || o.reserved != 0 || o.rows == 0 ||
+        o.project_count == 0 || !std::isfinite(o.rank_tolerance) || o.rank_tolerance < 1e-14 ||
+        o.rank_tolerance >= 0.1)
+      fail(INVALID_INPUT, "engine_projection_augmentation", "projection augmentation request is malformed");
+    auto c = read_struct(columns, "projection column descriptor", 0);
+    if (c.reserved != 0 || c.reserved_2 != 0 || c.rows != o.rows || c.project_count != o.project_count)
+      fail(INVALID_INPUT, "engine_projection_augmentation", "projection request and column descriptor disagree");
+    if (o.rows > (uint64_t(1) << 40) || o.caller_copy_bytes != o.rows * uint64_t(o.project_count) * 8)
+      fail(INVALID_INPUT, "engine_projection_augmentation",
+           "projection caller-copy bytes do not match the supplied dimensions");
+    if (!c.project)
+      fail(INVALID_INPUT, "engine_projection_augmentation", "positive projection count and pointer array are required");
+    std::vector<std::vector<double>> project(o.project_count);
+    for (uint32_t k = 0; k < o.project_count; ++k) {
+      intr.check("engine_copy_projection_descriptors");
+      const double* src = c.project[k];
+      if (!src) fail(INVALID_INPUT, "engine_projection_augmentation", "projection column pointer is null");
+      project[k].assign(src, src + o.rows);
+      for (double v : project[k])
+        if (!std::isfinite(v)) fail(INVALID_INPUT, "engine_projection_augmentation", "projection column has a nonfinite value");
+    }
+    if (o.effect != VCKSS_PROJECTION_EFFECT_WORKER && o.effect != VCKSS_PROJECTION_EFFECT_FIRM)
+      fail(INVALID_INPUT, "engine_projection_augmentation", "unknown projection effect");
+    if (o.weight != VCKSS_PROJECTION_WEIGHT_FREQUENCY && o.weight != VCKSS_PROJECTION_WEIGHT_TARGET)
+      fail(INVALID_INPUT, "engine_projection_augmentation", "unknown projection weight");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_projection_augmentation");
+    if (reg().state != State::Prepared)
+      fail(CONTEXT_POISONED, "context_augment",
+           "generation " + std::to_string(generation) + " is not in the prepared state");
+    // a refusal from here on fails the generation, as the reference's
+    // registry does for a failed augmentation (session_retained.rs:443-613)
+    struct Poison {
+      bool armed = true;
+      ~Poison() {
+        if (armed) reg().state = State::Failed;
+      }
+    } poison;
+    if (p.problem.rows() != o.rows)
+      fail(INVALID_INPUT, "engine_projection_augmentation", "projection rows differ from the prepared retained sample");
+    if (p.projection)
+      fail(CONTEXT_POISONED, "session_projection_augmentation", "the prepared generation already owns a projection");
+    if (o.project_count + 1 > PROJECTION_MAX_COLUMNS)
+      fail(RESOURCE_LIMIT, "session_projection_augmentation", "the device projection handles at most 31 covariates");
+    auto pp = std::make_shared<PreparedProjection>(prepare_projection(
+        p.problem, project, ProjectionEffect(o.effect), ProjectionWeight(o.weight), o.rank_tolerance));
+    // this library's resident accounting with the reference's augmentation
+    // formula: two caller-sized copies, four persistent blocks, eight
+    // q-square blocks and a header (session_retained.rs:532-553)
+    const uint64_t resident = p.problem.rows() * (4 * 6 + 8 * 3) + p.problem.cells * (4 * 2 + 8 * 3);
+    const uint64_t cols = pp->columns;
+    pp->rows = o.rows;
+    pp->caller_copy_bytes = o.caller_copy_bytes;
+    pp->augmentation_peak_forecast_bytes =
+        resident + 2 * o.caller_copy_bytes + 4 * pp->persistent_bytes + 8 * cols * cols * 8 + 4096;
+    pp->total_prepared_resident_bytes = resident + pp->persistent_bytes;
+    intr.check("session_projection_augmentation_final");
+    p.projection = std::move(pp);
+    poison.armed = false;
+  });
+}
+
+int32_t vckss_rust_engine_projection_augmentation_receipt_v1(uint64_t generation,
+                                                             VckssProjectionAugmentationReceiptV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssProjectionAugmentationReceiptV1>(out, cap, "projection augmentation receipt");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_projection_augmentation_receipt");
+    if (reg().state != State::Prepared)
+      fail(CONTEXT_POISONED, "engine_projection_augmentation_receipt",
+           "projection augmentation receipt must be read before solve");
+    if (!p.projection)
+      fail(UNSUPPORTED_FEATURE, "engine_projection_augmentation_receipt",
+           "the prepared generation has no projection attachment");
+    const PreparedProjection& pp = *p.projection;
+    VckssProjectionAugmentationReceiptV1 v{};
+    v.struct_size = sizeof(v);
+    v.schema_version = VCKSS_PROJECTION_SCHEMA_V1;
+    v.generation = generation;
+    v.rows = pp.rows;
+    v.columns = pp.columns;
+    v.effect = uint32_t(pp.effect);
+    v.weight = uint32_t(pp.weight);
+    v.caller_copy_bytes = pp.caller_copy_bytes;
+    v.augmentation_peak_forecast_bytes = pp.augmentation_peak_forecast_bytes;
+    v.projection_persistent_bytes = pp.persistent_bytes;
+    v.total_prepared_resident_bytes = pp.total_prepared_resident_bytes;
+    v.gram_rcond = pp.gram_rcond;
+    v.gram_relres = pp.gram_relres;
+    v.gram_original_relres = pp.gram_original_relres;
+    std::memcpy(out, &v, sizeof(v));
+  });
+}
+
+int32_t vckss_rust_engine_projection_result_v1(uint64_t generation, double* coefficients,
+                                               uint64_t coefficients_capacity, double* covariance,
+                                               uint64_t covariance_capacity, double* naive_covariance,
+                                               uint64_t naive_covariance_capacity,
+                                               VckssProjectionResultReceiptV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssProjectionResultReceiptV1>(out, cap, "projection result receipt");
+    std::lock_guard<std::mutex> l(reg().mu);
+    const ProjectionResult& r = projection_of(generation, "engine_projection_result");
+    auto put = [](double* dst, uint64_t capacity, const std::vector<double>& v, const char* label) {
+      if (!dst || capacity < v.size())
+        fail(INVALID_INPUT, "engine_projection_result", std::string(label) + " destination is null or short");
+      std::memcpy(dst, v.data(), v.size() * sizeof(double));
+    };
+    put(coefficients, coefficients_capacity, r.coefficients, "projection coefficients");
+    put(covariance, covariance_capacity, r.covariance, "projection covariance");
+    put(naive_covariance, naive_covariance_capacity, r.naive_covariance, "naive projection covariance");
+    VckssProjectionResultReceiptV1 v = projection_receipt(generation, r);
+    std::memcpy(out, &v, sizeof(v));
+  });
+}
+
+int32_t vckss_rust_engine_projection_result_receipt_v1(uint64_t generation, VckssProjectionResultReceiptV1* out,
+                                                       uint32_t cap) {
+  return status([&] {
+    require_capacity<VckssProjectionResultReceiptV1>(out, cap, "projection result receipt");
+    std::lock_guard<std::mutex> l(reg().mu);
+    VckssProjectionResultReceiptV1 v =
+        projection_receipt(generation, projection_of(generation, "engine_projection_result_receipt"));
+    std::memcpy(out, &v, sizeof(v));
+  });
+}
+
+}  // extern "C"
+
 // ---- numerical MCSE attachment (reference vckss-plugin/src/numerical_api.rs)
 
 namespace {
@@ -2165,6 +2374,9 @@ void numerical_solve(uint64_t g, const VckssNumericalRequestV1& q, const Interru
   {
     std::lock_guard<std::mutex> l(reg().mu);
     Prepared& p = reg().require(g, "context_solve");
+    if (p.projection)  // ffi_engine.rs:4926-4934
+      fail(UNSUPPORTED_FEATURE, "numerical_preflight",
+           "numerical V1 does not support projection or component-inference intersections");
     // algorithm(auto) resolves once the retained dimensions are known
     // (vckss-core/src/engine_plan.rs:179-240): exact within the exact limit
     const uint64_t complexity = uint64_t(p.problem.workers) + p.problem.firms - 1 + p.problem.controls.size();

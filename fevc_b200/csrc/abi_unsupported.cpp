@@ -29,7 +29,6 @@ int32_t vckss_rust_engine_augment_match_component_inference_interrupt_v2(uint64_
 int32_t vckss_rust_engine_augment_match_component_inference_interrupt_v3(uint64_t, const VckssComponentInferenceAugmentationRequestInterruptV1 *) { return fevcb::unsupported_entry("engine_augment_match_component_inference_interrupt_v3"); }
 int32_t vckss_rust_engine_augment_match_component_inference_interrupt_v4(uint64_t, const VckssComponentInferenceAugmentationRequestInterruptV1 *, uint32_t) { return fevcb::unsupported_entry("engine_augment_match_component_inference_interrupt_v4"); }
 int32_t vckss_rust_engine_augment_match_component_inference_interrupt_v5(uint64_t, const VckssComponentInferenceAugmentationRequestInterruptV1 *, uint32_t) { return fevcb::unsupported_entry("engine_augment_match_component_inference_interrupt_v5"); }
-int32_t vckss_rust_engine_augment_projection_interrupt_v1(uint64_t, const VckssProjectionAugmentationRequestInterruptV1 *, const VckssProjectionColumnsV1 *) { return fevcb::unsupported_entry("engine_augment_projection_interrupt_v1"); }
 int32_t vckss_rust_engine_augment_stayers_interrupt_v1(uint64_t, const VckssStayerAugmentationRequestInterruptV1 *, const VckssStayerAugmentationColumnsV1 *) { return fevcb::unsupported_entry("engine_augment_stayers_interrupt_v1"); }
 int32_t vckss_rust_engine_augment_stayers_v1(uint64_t, const VckssStayerAugmentationRequestV1 *, const VckssStayerAugmentationColumnsV1 *) { return fevcb::unsupported_entry("engine_augment_stayers_v1"); }
 int32_t vckss_rust_engine_component_batch_receipt_v1(uint64_t, VckssComponentBatchReceiptV1 *, uint32_t) { return fevcb::unsupported_entry("engine_component_batch_receipt_v1"); }
@@ -41,7 +40,6 @@ int32_t vckss_rust_engine_component_inference_result_v5(uint64_t, double *, uint
 int32_t vckss_rust_engine_component_inference_unit_receipt_v1(uint64_t, VckssComponentInferenceUnitReceiptV1 *, uint32_t) { return fevcb::unsupported_entry("engine_component_inference_unit_receipt_v1"); }
 int32_t vckss_rust_engine_component_inference_unit_receipt_v2(uint64_t, VckssComponentInferenceUnitReceiptV2 *, uint32_t) { return fevcb::unsupported_entry("engine_component_inference_unit_receipt_v2"); }
 int32_t vckss_rust_engine_default_component_inference_augmentation_request_interrupt_v1(VckssComponentInferenceAugmentationRequestInterruptV1 *, uint32_t) { return fevcb::unsupported_entry("engine_default_component_inference_augmentation_request_interrupt_v1"); }
-int32_t vckss_rust_engine_default_projection_augmentation_request_interrupt_v1(VckssProjectionAugmentationRequestInterruptV1 *, uint32_t) { return fevcb::unsupported_entry("engine_default_projection_augmentation_request_interrupt_v1"); }
 int32_t vckss_rust_engine_default_solve_request_interrupt_v2(VckssEngineSolveRequestInterruptV2 *, uint32_t) { return fevcb::unsupported_entry("engine_default_solve_request_interrupt_v2"); }
 int32_t vckss_rust_engine_default_solve_request_interrupt_v3(VckssEngineSolveRequestInterruptV3 *, uint32_t) { return fevcb::unsupported_entry("engine_default_solve_request_interrupt_v3"); }
 int32_t vckss_rust_engine_default_solve_request_interrupt_v4(VckssEngineSolveRequestInterruptV4 *, uint32_t) { return fevcb::unsupported_entry("engine_default_solve_request_interrupt_v4"); }
@@ -62,9 +60,6 @@ int32_t vckss_rust_engine_numerical_preflight_v2(const VckssNumericalRequestV2 *
 int32_t vckss_rust_engine_performance_receipt_v1(uint64_t, VckssEnginePerformanceReceiptV1 *, uint32_t) { return fevcb::unsupported_entry("engine_performance_receipt_v1"); }
 int32_t vckss_rust_engine_prepare_interrupt_v3(const VckssEnginePrepareRequestInterruptV2 *, const VckssEngineColumnsV3 *, uint64_t *, uint32_t) { return fevcb::unsupported_entry("engine_prepare_interrupt_v3"); }
 int32_t vckss_rust_engine_prepare_memory_interrupt_v1(const VckssEnginePrepareRequestInterruptV3 *, const VckssEngineColumnsV3 *, const VckssMemoryPolicyV1 *, uint64_t *, uint32_t) { return fevcb::unsupported_entry("engine_prepare_memory_interrupt_v1"); }
-int32_t vckss_rust_engine_projection_augmentation_receipt_v1(uint64_t, VckssProjectionAugmentationReceiptV1 *, uint32_t) { return fevcb::unsupported_entry("engine_projection_augmentation_receipt_v1"); }
-int32_t vckss_rust_engine_projection_result_receipt_v1(uint64_t, VckssProjectionResultReceiptV1 *, uint32_t) { return fevcb::unsupported_entry("engine_projection_result_receipt_v1"); }
-int32_t vckss_rust_engine_projection_result_v1(uint64_t, double *, uint64_t, double *, uint64_t, double *, uint64_t, VckssProjectionResultReceiptV1 *, uint32_t) { return fevcb::unsupported_entry("engine_projection_result_v1"); }
 int32_t vckss_rust_engine_repeat_measurement_diagnostic_v1(uint64_t, VckssRepeatMeasurementDiagnosticV1 *, uint32_t) { return fevcb::unsupported_entry("engine_repeat_measurement_diagnostic_v1"); }
 int32_t vckss_rust_engine_repeat_measurement_leading_v1(uint64_t, VckssRepeatMeasurementLeadingV1 *, uint32_t) { return fevcb::unsupported_entry("engine_repeat_measurement_leading_v1"); }
 int32_t vckss_rust_engine_solve_exact_execution_interrupt_v1(uint64_t, const VckssExactExecutionRequestInterruptV1 *) { return fevcb::unsupported_entry("engine_solve_exact_execution_interrupt_v1"); }
@@ -88,7 +83,6 @@ uint32_t vckss_rust_exact_execution_schema_v1(void) { return 0; }  // exact exec
 uint32_t vckss_rust_exact_legacy_execution_schema_v1(void) { return 0; }  // exact execution is not provided
 uint32_t vckss_rust_exact_resolved_execution_schema_v2(void) { return 0; }  // exact execution is not provided
 uint32_t vckss_rust_numerical_schema_v2(void) { return 0; }  // the numerical attachment is not provided
-uint32_t vckss_rust_projection_centering_schema_v1(void) { return 0; }  // the projection attachment is not provided
 int32_t vckss_rust_report_call_v1(const VckssProgressOptionsV1 *, VckssProgressOperationV1, void *) { return fevcb::unsupported_entry("report_call_v1"); }
 int32_t vckss_rust_session_clear_abandoned_v1(void) { return fevcb::unsupported_entry("session_clear_abandoned_v1"); }
 const char* vckss_rust_session_last_error(void) { return vckss_rust_engine_last_error(); }

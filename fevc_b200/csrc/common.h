@@ -46,6 +46,8 @@ enum Code : int32_t {
   STALE_CONTEXT = 80,
   CONTEXT_POISONED = 81,
   SINGULAR_INFORMATION = 82,
+  INVERSE_RESIDUAL_FAILED = 83,
+  SYMMETRIC_EIGENSOLVER_FAILED = 86,
   INTERNAL_INVARIANT_FAILED = 90,
   PANIC = 99,
 };
@@ -87,6 +89,8 @@ inline const char* code_name(int32_t c) {
     case STALE_CONTEXT: return "STALE_CONTEXT";
     case CONTEXT_POISONED: return "CONTEXT_POISONED";
     case SINGULAR_INFORMATION: return "SINGULAR_INFORMATION";
+    case INVERSE_RESIDUAL_FAILED: return "INVERSE_RESIDUAL_FAILED";
+    case SYMMETRIC_EIGENSOLVER_FAILED: return "SYMMETRIC_EIGENSOLVER_FAILED";
     case INTERNAL_INVARIANT_FAILED: return "INTERNAL_INVARIANT_FAILED";
     case PANIC: return "PANIC";
     default: return "UNKNOWN";

@@ -16,6 +16,7 @@
 // buffers go, and within one owner the reuse is stream-ordered.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <unordered_map>
@@ -217,4 +218,39 @@ HostStager::Bind::~Bind() { t_stager = prev; }
 
 HostStager* bound_stager() { return t_stager; }
 
+}  // namespace fevcb
+
+// ---------------------------------------------------------------------------
+// Kernel-launch count.  Every kernel this library launches goes through the
+// CUDA runtime's cudaLaunchKernel (the <<<...>>> stubs) or
+// cudaLaunchCooperativeKernel; the link wraps both symbols (ld --wrap, see
+// fevc_b200/build.py) so a solve can report exactly how many kernels it
+// launched.
+
+namespace {
+std::atomic<uint64_t> g_kernel_launches{0};
+}  // namespace
+
+extern "C" cudaError_t __real_cudaLaunchKernel(const void* fn, dim3 grid, dim3 block, void** args, size_t smem,
+                                               cudaStream_t stream);
+extern "C" cudaError_t __real_cudaLaunchCooperativeKernel(const void* fn, dim3 grid, dim3 block, void** args,
+                                                          size_t smem, cudaStream_t stream);
+
+extern "C" cudaError_t __wrap_cudaLaunchKernel(const void* fn, dim3 grid, dim3 block, void** args, size_t smem,
+                                               cudaStream_t stream) {
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  return __real_cudaLaunchKernel(fn, grid, block, args, smem, stream);
+}
+
+extern "C" cudaError_t __wrap_cudaLaunchCooperativeKernel(const void* fn, dim3 grid, dim3 block, void** args,
+                                                          size_t smem, cudaStream_t stream) {
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  return __real_cudaLaunchCooperativeKernel(fn, grid, block, args, smem, stream);
+}
+
+namespace fevcb {
+uint64_t kernel_launch_count() { return g_kernel_launches.load(std::memory_order_relaxed); }
+void count_replayed_launches(int64_t kernels) {
+  g_kernel_launches.fetch_add(uint64_t(kernels), std::memory_order_relaxed);  // modular: negative subtracts
+}
 }  // namespace fevcb

@@ -39,6 +39,7 @@
 #include "observation.cuh"
 #include "numerical.cuh"
 #include "numerical.h"
+#include "projection.cuh"
 
 namespace fevcb {
 
@@ -313,6 +314,13 @@ struct DeviceEngine {
   // match deletion with controls: per-unit maker margin, per-row inverse-common
   // action, per-unit target-fold sums
   DBuf<double> num_unit_margin, num_row_w, num_block_sums;
+  // projection attachment: loadings (uploaded once per generation), the
+  // column solutions, control coefficients, partial sums and the proxy's
+  // extremes; the coefficients of the last fit
+  DBuf<double> proj_wrhs, proj_frhs, proj_uW, proj_uF, proj_gamma, proj_partial, proj_out;
+  DBuf<unsigned long long> proj_keys;
+  const PreparedProjection* proj_loaded = nullptr;
+  std::vector<double> proj_coef;
   DBuf<unsigned long long> num_stats;
   std::map<int, std::unique_ptr<BlockWork>> work;
   // pinned host scalars
@@ -346,6 +354,7 @@ struct BlockWork {
   DBuf<float> x32, r32, p32, z32;
   cudaGraphExec_t graph = nullptr;
   int graph_iters = 0;
+  uint64_t graph_kernels = 0;  // kernels one replay of the graph launches
   ~BlockWork() {
     if (graph) cudaGraphExecDestroy(graph);
   }
@@ -1256,23 +1265,27 @@ template <int K>
 int pcg_run_mg(DeviceEngine& e, BlockWork& w, Launch L, int iterations, SolveTimings& tm) {
   if (!w.graph) {
     cudaGraph_t g = nullptr;
+    // launches recorded into the graph run only when it is replayed: take
+    // them off the launch count here and add them back per replay
+    const uint64_t captured0 = kernel_launch_count();
     CK(cudaStreamBeginCapture(L.s, cudaStreamCaptureModeThreadLocal));
     for (int i = 0; i < MG_GRAPH_ITERATIONS; ++i) mg_iteration<K>(e, w, L, L.s);
     cudaError_t end = cudaStreamEndCapture(L.s, &g);
+    w.graph_kernels = kernel_launch_count() - captured0;
+    count_replayed_launches(-int64_t(w.graph_kernels));
     CK(end);
     cudaError_t inst = cudaGraphInstantiate(&w.graph, g, 0);
     cudaGraphDestroy(g);
     CK(inst);
     w.graph_iters = MG_GRAPH_ITERATIONS;
   }
-  const int per_iteration = 6 + e.mg->launches_per_apply();
   int executed = 0;
   CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
   CK(cudaStreamSynchronize(L.s));
   while (*e.h_nactive > 0 && executed < iterations) {
     CK(cudaGraphLaunch(w.graph, L.s));
     executed += w.graph_iters;
-    tm.kernel_launches += uint64_t(w.graph_iters) * per_iteration;
+    count_replayed_launches(int64_t(w.graph_kernels));
     tm.spmm_launches += w.graph_iters;
     CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
@@ -1338,7 +1351,6 @@ int learned_fallback(DeviceEngine& e, BlockWork& w, Launch L, int budget, SolveT
   pcg_restart<K>(e, w, L, false, true);
   int done = pcg_run_mg<K>(e, w, L, std::max(1, budget - used), tm);
   e.preconditioner = saved;
-  tm.kernel_launches += 10;
   return done;
 }
 
@@ -1388,7 +1400,6 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
   const bool directions = e.preconditioner == 2 || !two_barrier_form<K, double>();
   if (!flex) {
     pcg_restart<K>(e, w, L, true, directions);
-    tm.kernel_launches += directions ? 9 : 5;
   }
 
   const double gate = std::max(10.0 * o.pcg_tolerance, 1e-11);
@@ -1406,7 +1417,6 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
       // extraction results
       const bool learned = e.preconditioner == 3;
       launch_flex<K>(e, w, L, learned ? std::min(budget, LEARNED_CAP) : budget, ladder == 0, o.precision);
-      tm.kernel_launches += 1;
       tm.spmm_launches += 1;
       done = learned ? learned_fallback<K>(e, w, L, budget, tm) : -1;
       if (done < 0) CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
@@ -1422,7 +1432,6 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
       CK(cudaLaunchCooperativeKernel(fn, dim3(e.coop_blocks), dim3(PERSIST_THREADS), args, 0, L.s));
       CK(cudaMemcpyAsync(e.h_nactive, w.s.nactive, sizeof(int), cudaMemcpyDeviceToHost, L.s));
       done = -1;
-      tm.kernel_launches += 1;
       tm.spmm_launches += 1;
     }
     const bool deferred = done < 0;
@@ -1449,7 +1458,6 @@ BlockOutcome solve_block(DeviceEngine& e, BlockWork& w, int ncols, const SolveOp
     firm_gather<K, 2, 2>(e, w, L, e.cell_weight.p, w.alpha.p, nullptr, 0.0, w.bF.p, nullptr, w.x.p, nullptr, pf);
     finish(pw, L.grid, 2 * K, w.tot.p, L.s);
     finish(pf, L.grid, 2 * K, w.tot.p + 2 * K, L.s);
-    tm.kernel_launches += 5;
     std::vector<double> tot(4 * K);
     CK(cudaMemcpyAsync(tot.data(), w.tot.p, 4 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaMemcpyAsync(h_rr.data(), w.s.rr, K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
@@ -1601,7 +1609,6 @@ void run_leverage(DeviceEngine& e, const SolveOptions& o, SolveResult& res, uint
   for (uint32_t first = o.probe_begin; first < end; first += K) {
     int ncols = int(std::min<uint32_t>(K, end - first));
     leverage_rhs<K>(e, w, L, key, first, ncols);
-    res.timings.kernel_launches += 4;
     BlockOutcome bo = solve_block<K>(e, w, ncols, o, res.timings);
     if (e.observation && shared_signs(e, first))
       k_obs_moments_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, ncols, e.unit_ptr.p, e.cell_rows.p, e.cell_worker.p,
@@ -1616,7 +1623,6 @@ void run_leverage(DeviceEngine& e, const SolveOptions& o, SolveResult& res, uint
       k_moments<K><<<L.grid, THREADS, 0, L.s>>>(e.G, ncols, e.unit_cell.p, e.unit_sqrt_n.p, e.cell_worker.p,
                                                 e.cell_firm.p, w.alpha.p, w.x.p, w.unit_atoms.p, e.moments.p);
     CK_LAUNCH();
-    res.timings.kernel_launches += 1;
     for (int j = 0; j < ncols; ++j)
       res.receipts.push_back(RhsReceipt{2, 1, int64_t(first + j), uint32_t(bo.iters[j]), uint32_t(bo.zero[j]),
                                         bo.reduced[j], bo.complete[j]});
@@ -1655,7 +1661,6 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
     CK(cudaMemcpyAsync(lastW.data(), w.bW.p + size_t(e.W - 1) * K, K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaMemcpyAsync(lastF.data(), w.bF.p + size_t(e.F - 1) * K, K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
-    res.timings.kernel_launches += 9;
     for (int q = 0; q < K; ++q) {
       int j = q / 2;
       if (j >= np) {
@@ -1689,7 +1694,6 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
       finish(e.partial.p, L.grid, 3 * K, w.tot.p, L.s);
       CK(cudaMemcpyAsync(draws.data(), w.tot.p, 3 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
       CK(cudaStreamSynchronize(L.s));
-      res.timings.kernel_launches += 2;
     } else {
       // full-model solves: beta = -S^{-1} Q'W X theta_fe per column, then the
       // row-level contraction over match groups
@@ -1716,7 +1720,6 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
         std::vector<double> f(2 * (QMAX + 1) * K);
         CK(cudaMemcpyAsync(f.data(), e.obs_fused.p, f.size() * sizeof(double), cudaMemcpyDeviceToHost, L.s));
         CK(cudaStreamSynchronize(L.s));
-        res.timings.kernel_launches += 3;
         const double* A = f.data() + QMAX * K;
         const double* B = f.data() + (QMAX + 1) * K;
         const double* Atot = f.data() + (2 * QMAX + 1) * K;
@@ -1764,7 +1767,6 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
         finish(e.partial.p, L.grid, 2 * K, w.tot.p, L.s);
         CK(cudaMemcpyAsync(g2.data(), w.tot.p, 2 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
         CK(cudaStreamSynchronize(L.s));
-        res.timings.kernel_launches += 4;
       }
       if (e.observation && e.q > 0) {
         // the cell-independent beta' S2 beta terms of every column and of the total
@@ -2023,7 +2025,6 @@ void run_exact(DeviceEngine& e, const Compressed& p, const SolveOptions& o, Solv
   k_scale_copy<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_target.p, 1.0 / p.target_total, cmass.p);
   k_gather<1><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, cmass.p, wshare.p);
   k_gather<1><<<L.grid, THREADS, 0, L.s>>>(e.F, e.firm_ptr.p, e.firm_cells.p, cmass.p, fshare.p);
-  res.timings.kernel_launches += 3;
   SolveOptions oe = o;
   oe.pcg_tolerance = std::min(o.pcg_tolerance, 1e-10);
   std::vector<double> B(size_t(e.C) * 3), sums(5 * K);
@@ -2041,7 +2042,6 @@ void run_exact(DeviceEngine& e, const Compressed& p, const SolveOptions& o, Solv
                                            e.unit_ptr.p, e.unit_count_f.p, e.moments.p);
     CK(cudaMemcpyAsync(sums.data(), w.tot.p, 5 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
-    res.timings.kernel_launches += 4;
     for (int j = 0; j < ncols; ++j) {
       const double aw = sums[j], aw2 = sums[K + j], pf = sums[2 * K + j], pf2 = sums[3 * K + j],
                    x = sums[4 * K + j];
@@ -2062,7 +2062,6 @@ void run_exact(DeviceEngine& e, const Compressed& p, const SolveOptions& o, Solv
   CK(cudaMemcpyAsync(got, e.error.p, sizeof(got), cudaMemcpyDeviceToHost, L.s));
   CK(cudaMemcpyAsync(omega.data(), e.omega.p, e.C * sizeof(double), cudaMemcpyDeviceToHost, L.s));
   CK(cudaStreamSynchronize(L.s));
-  res.timings.kernel_launches += 1;
   std::memcpy(&res.max_leverage, &got[1], sizeof(double));
   if (got[0] != ~0ull) {
     const uint32_t code = uint32_t(got[0] & 0xff);
@@ -2166,7 +2165,6 @@ bool numerical_replay(DeviceEngine& e, const SolveOptions& o, SolveResult& res, 
     finish(e.partial.p, L.grid, 6 * K, e.num_out.p, L.s);
     CK(cudaMemcpyAsync(out.data(), e.num_out.p, 6 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
-    res.timings.kernel_launches += 6;
     for (int j = 0; j < ncols; ++j) {
       scores[0][first + j] = {out[0 * K + j], out[1 * K + j], out[2 * K + j]};
       scores[1][first + j] = {out[3 * K + j], out[4 * K + j], out[5 * K + j]};
@@ -2274,7 +2272,6 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
     double T = p.target_total;
     res.plugin = finish_accounting(m[0] / T, m[1] / T, m[2] / T, m[3] / T, "jla_components");
     e.shard_plugin = res.plugin;
-    res.timings.kernel_launches += 6;
   }
   auto t1 = now();
   if (o.algorithm == 1) {
@@ -2326,7 +2323,6 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
     CK(cudaStreamSynchronize(L.s));
     const unsigned long long err = got[0];
     std::memcpy(&res.max_leverage, &got[1], sizeof(double));
-    res.timings.kernel_launches += 1;
     if (err != ~0ull) {
       uint32_t code = uint32_t(err & 0xff);
       uint32_t g = e.unit_group[err >> 8];
@@ -2425,7 +2421,6 @@ void setup_controls(DeviceEngine& e, const SolveOptions& o, SolveTimings& tm) {
   std::vector<double> S8(QMAX * QMAX);
   CK(cudaMemcpyAsync(S8.data(), e.small.p, S8.size() * sizeof(double), cudaMemcpyDeviceToHost, L.s));
   CK(cudaStreamSynchronize(L.s));
-  tm.kernel_launches += 8;
   std::vector<double> S(q * q), Lc;
   for (int i = 0; i < q; ++i)
     for (int j = 0; j < q; ++j) S[i * q + j] = 0.5 * (S8[i * QMAX + j] + S8[j * QMAX + i]);
@@ -2455,6 +2450,118 @@ void setup_controls(DeviceEngine& e, const SolveOptions& o, SolveTimings& tm) {
   if (!host_cholesky(e.Lfac, q))
     fail(BLOCK_INVERSE_FAILED, "generic_jla_control_factor", "control inverse square root failed");
   e.controls_ready = true;
+}
+
+// Projection attachment (reference generic_jla.rs:3140-3190 with
+// projection.rs:278-538): the loadings' model solutions in blocks of eight
+// columns, their control coefficients, then one streamed pass over the
+// deletion units for the KSS and naive covariances.
+void run_projection(DeviceEngine& e, const Compressed& p, const SolveOptions& o, double y_center, SolveResult& res) {
+  const PreparedProjection& pp = *o.projection;
+  const int cols = int(pp.columns), q = e.q;
+  if (cols < 2 || cols > PROJ_MAX_COLUMNS)
+    fail(RESOURCE_LIMIT, "generic_jla_projection", "the device projection handles at most 31 covariates");
+  if (e.proj_coef.size() != size_t(cols))
+    fail(INTERNAL_INVARIANT_FAILED, "generic_jla_projection", "projection coefficient state is incomplete");
+  Launch L{grid_blocks(), e.stream};
+  if (e.proj_loaded != &pp) {
+    e.proj_wrhs.alloc(pp.worker_rhs.size());
+    e.proj_frhs.alloc(pp.firm_rhs.size());
+    CK(cudaMemcpyAsync(e.proj_wrhs.p, pp.worker_rhs.data(), pp.worker_rhs.size() * sizeof(double),
+                       cudaMemcpyHostToDevice, L.s));
+    CK(cudaMemcpyAsync(e.proj_frhs.p, pp.firm_rhs.data(), pp.firm_rhs.size() * sizeof(double),
+                       cudaMemcpyHostToDevice, L.s));
+    e.proj_uW.alloc(size_t(e.W) * cols);
+    e.proj_uF.alloc(size_t(e.F) * cols);
+    e.proj_gamma.alloc(size_t(QMAX) * PROJ_MAX_COLUMNS);
+    e.proj_out.alloc(2 * PROJ_MAX_COLUMNS * (PROJ_MAX_COLUMNS + 1) / 2 + QMAX * PROJ_MAX_COLUMNS);
+    e.proj_keys.alloc(2);
+    e.proj_partial.alloc(size_t(L.grid) * PROJ_MAX_COLUMNS * (PROJ_MAX_COLUMNS + 1));
+    CK(cudaStreamSynchronize(L.s));
+    e.proj_loaded = &pp;
+  }
+  // model solutions of the columns' coefficient-space RHSs (phase 6, joint)
+  BlockWork& w8 = get_work<8>(e);
+  uint32_t max_iters = 0;
+  double max_reduced = 0.0, max_complete = 0.0;
+  for (int c0 = 0; c0 < cols; c0 += 8) {
+    const int n = std::min(8, cols - c0);
+    k_projection_rhs<8><<<L.grid, THREADS, 0, L.s>>>(e.W, e.F, c0, n, e.proj_wrhs.p, e.proj_frhs.p, w8.bW.p, w8.bF.p);
+    BlockOutcome bo = solve_block<8>(e, w8, n, o, res.timings);
+    for (int j = 0; j < n; ++j) {
+      res.receipts.push_back(RhsReceipt{6, 0, c0 + j, uint32_t(bo.iters[j]), uint32_t(bo.zero[j]), bo.reduced[j],
+                                        bo.complete[j]});
+      max_iters = std::max(max_iters, uint32_t(bo.iters[j]));
+      max_reduced = std::max(max_reduced, bo.reduced[j]);
+      max_complete = std::max(max_complete, bo.complete[j]);
+    }
+    k_projection_keep<8><<<L.grid, THREADS, 0, L.s>>>(e.W, e.F, c0, n, cols, w8.alpha.p, w8.x.p, e.proj_uW.p,
+                                                       e.proj_uF.p);
+  }
+  // gamma = -S^{-1} Q'W X u of every column (joint nuisance)
+  std::vector<double> gamma(size_t(QMAX) * cols, 0.0);
+  if (q > 0) {
+    const size_t sm = size_t(q) * cols * sizeof(double);
+    k_projection_control_dots<<<L.grid, THREADS, sm, L.s>>>(e.rows, q, cols, e.row_cell.p, e.cell_worker.p,
+                                                            e.cell_firm.p, e.row_freq.p, e.Qd.p, e.proj_uW.p,
+                                                            e.proj_uF.p, e.partial.p);
+    finish(e.partial.p, L.grid, q * cols, e.proj_out.p, L.s);
+    std::vector<double> dots(size_t(q) * cols);
+    CK(cudaMemcpyAsync(dots.data(), e.proj_out.p, dots.size() * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+    CK(cudaStreamSynchronize(L.s));
+    for (int k = 0; k < q; ++k)
+      for (int j = 0; j < cols; ++j) {
+        double v = 0.0;
+        for (int l = 0; l < q; ++l) v += e.Sinv[k * q + l] * dots[size_t(l) * cols + j];
+        gamma[size_t(k) * cols + j] = -v;
+      }
+    CK(cudaMemcpyAsync(e.proj_gamma.p, gamma.data(), size_t(q) * cols * sizeof(double), cudaMemcpyHostToDevice, L.s));
+  }
+  // the streamed covariance over the deletion units
+  ProjectionGramArgs a{};
+  a.match = !e.observation;
+  a.units = a.match ? uint32_t(e.group_ptr.n - 1) : e.rows;  // match groups in semantic order, or rows
+  a.q = q;
+  a.cols = cols;
+  a.tile = std::min(256, 6144 / (3 * cols));
+  a.y_center = y_center;
+  a.group_ptr = e.group_ptr.p;
+  a.group_rows = e.group_rows.p;
+  a.row_cell = e.row_cell.p;
+  a.cell_worker = e.cell_worker.p;
+  a.cell_firm = e.cell_firm.p;
+  a.row_freq = e.row_freq.p;
+  a.y = e.row_y.p;
+  a.deleted = e.deleted.p;
+  a.residual = e.residual.p;
+  a.R = q > 0 ? e.Rd.p : nullptr;
+  a.uW = e.proj_uW.p;
+  a.uF = e.proj_uF.p;
+  a.gamma = e.proj_gamma.p;
+  a.proxy_keys = e.proj_keys.p;
+  const unsigned long long init[2] = {~0ull, 0ull};
+  CK(cudaMemcpyAsync(e.proj_keys.p, init, sizeof(init), cudaMemcpyHostToDevice, L.s));
+  const int P = cols * (cols + 1) / 2;
+  const size_t sm = size_t(3) * a.tile * cols * sizeof(double);
+  k_projection_gram<<<L.grid, THREADS, sm, L.s>>>(a, e.proj_partial.p);
+  finish(e.proj_partial.p, L.grid, 2 * P, e.proj_out.p, L.s);
+  std::vector<double> sums(2 * P);
+  unsigned long long keys[2];
+  CK(cudaMemcpyAsync(sums.data(), e.proj_out.p, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+  CK(cudaMemcpyAsync(keys, e.proj_keys.p, sizeof(keys), cudaMemcpyDeviceToHost, L.s));
+  CK(cudaStreamSynchronize(L.s));
+  std::vector<double> cov(size_t(cols) * cols, 0.0), naive(size_t(cols) * cols, 0.0);
+  for (int l = 0, t = 0; l < cols; ++l)
+    for (int r = l; r < cols; ++r, ++t) {
+      cov[size_t(l) * cols + r] = sums[t];
+      naive[size_t(l) * cols + r] = sums[P + t];
+    }
+  finish_projection(pp, e.proj_coef, cov, naive, from_order_key(keys[0]), from_order_key(keys[1]), res.projection);
+  res.projection.maximum_iterations = max_iters;
+  res.projection.maximum_reduced_residual = max_reduced;
+  res.projection.maximum_complete_residual = max_complete;
+  res.projection.full_residual_tolerance = std::max(10.0 * o.pcg_tolerance, 1e-11);
+  (void)p;
 }
 
 template <int K>
@@ -2508,7 +2615,13 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     double T = p.target_total;
     res.plugin = finish_accounting(m[0] / T, m[1] / T, m[2] / T, m[3] / T, "generic_jla_components");
     e.shard_plugin = res.plugin;
-    res.timings.kernel_launches += 12;
+    if (o.projection) {  // projection coefficients from the working fit (projection.rs:245-276)
+      std::vector<double> a(e.W), f(e.F);
+      CK(cudaMemcpyAsync(a.data(), w.alpha.p, a.size() * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+      CK(cudaMemcpyAsync(f.data(), w.x.p, f.size() * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+      CK(cudaStreamSynchronize(L.s));
+      e.proj_coef = projection_coefficients(*o.projection, a.data(), a.size(), f.data(), f.size());
+    }
   }
   auto t1 = now();
   // ---- FE-only leverage probes (reference `match_leverage_moments`,
@@ -2540,7 +2653,6 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
         for (int j = 0; j < q; ++j) sinv.m[i * QMAX + j] = e.Sinv[i * q + j];
       k_control_leverage<<<L.grid, THREADS, 0, L.s>>>(e.rows, q, e.Rd.p, sinv, o.rank_tolerance, e.control_lev.p,
                                                       e.error.p);
-      res.timings.kernel_launches += 1;
     }
     ObservationAdjustParams prm{e.rows, double(o.probes), o.block_tolerance, o.rank_tolerance};
     k_obs_adjust<<<L.grid, THREADS, 0, L.s>>>(prm, e.row_phys.p, e.obs_row_acc.p, e.obs_copy_acc.p,
@@ -2551,7 +2663,6 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     CK(cudaStreamSynchronize(L.s));
     const unsigned long long err = got[0];
     std::memcpy(&res.max_leverage, &got[1], sizeof(double));
-    res.timings.kernel_launches += 1;
     if (err != ~0ull) {
       uint32_t code = uint32_t(err & 0xff);
       uint64_t row = err >> 8;
@@ -2580,7 +2691,6 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     e.obs_S2.assign(QMAX * QMAX, 0.0);
     CK(cudaMemcpyAsync(e.obs_S2.data(), e.obs_s2.p, QMAX * QMAX * sizeof(double), cudaMemcpyDeviceToHost, L.s));
     CK(cudaStreamSynchronize(L.s));
-    res.timings.kernel_launches += 2;
   } else {
   // ---- deleted residuals of every match group
   {
@@ -2608,7 +2718,6 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     CK(cudaStreamSynchronize(L.s));
     const unsigned long long err = got[0];
     std::memcpy(&res.max_leverage, &got[1], sizeof(double));
-    res.timings.kernel_launches += 1;
     if (err != ~0ull) {
       uint32_t code = uint32_t(err & 0xff);
       uint32_t g = e.unit_group[err >> 8];
@@ -2621,7 +2730,6 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     k_unit_target_sums<<<L.grid, THREADS, 0, L.s>>>(e.G, q, e.unit_group_d.p, e.group_ptr.p, e.group_rows.p,
                                                     e.row_freq.p, e.row_y.p, outcome_mean(p, o.centering),
                                                     e.deleted.p, e.Rd.p, e.unit_sums.p);
-    res.timings.kernel_launches += 1;
     if (o.numerical) {
       numerical_status = numerical_derivative(e, o, res.numerical);
       if (e.num_block_sums.n < size_t(e.G) * (2 + 2 * QMAX)) e.num_block_sums.alloc(size_t(e.G) * (2 + 2 * QMAX));
@@ -2644,6 +2752,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
   }
   finish_draws(res, o.probes);
   if (o.numerical) numerical_finish<K>(e, plan, o, outcome_mean(p, o.centering), numerical_status, res);
+  if (o.projection) run_projection(e, p, o, outcome_mean(p, o.centering), res);
   for (auto& r : res.receipts) {
     res.max_reduced_residual = std::max(res.max_reduced_residual, r.reduced_residual);
     res.max_complete_residual = std::max(res.max_complete_residual, r.complete_residual);

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "prep.h"
+#include "projection.h"
 
 namespace fevcb {
 
@@ -51,6 +52,10 @@ struct SolveOptions {
   // per-unit derivatives after the adjustment, per-unit target folds during the
   // target phase, and a replay of the leverage probes that scores each one.
   bool numerical = false;
+  // Fixed-effect projection attachment of the prepared generation (generic
+  // JLA only): its columns are solved on the working model after the target
+  // phase and their KSS covariance streamed over the deletion units.
+  const PreparedProjection* projection = nullptr;
 };
 
 // One receipt per solved right-hand side (reference `JlaRhsReceipt`,
@@ -109,6 +114,7 @@ struct SolveResult {
   SolveTimings timings;
   std::vector<double> shard_accumulators;  // phase 1 output
   NumericalAttachment numerical;
+  ProjectionResult projection;
 };
 
 // Number of leverage accumulators a shard exchanges (match units: 5 moment
@@ -161,6 +167,13 @@ void device_atoms_noalloc(uint64_t seed, uint64_t tag, uint64_t first_probe, uin
                           const uint64_t* trials, uint64_t count, int64_t* out);
 
 int device_count();
+// Kernels this library has launched since it was loaded (every launch passes
+// through the wrapped CUDA runtime launch calls).
+uint64_t kernel_launch_count();
+// Adjusts that count for kernels that run from a CUDA graph: a replay launches
+// them without passing through the wrapped calls, a capture passes through
+// them without launching.
+void count_replayed_launches(int64_t kernels);
 // Device allocations released by finished generations stay cached for the
 // next one (devmem.cu); the trim returns them to the driver (bytes freed).
 size_t device_cache_trim();

@@ -1356,10 +1356,129 @@ int32_t vckss_rust_engine_detailed_receipt_v7(uint64_t generation, VckssEngineDe
                                               uint32_t output_capacity_bytes);
 
 /* ---------------------------------------------------------------------------
+ * Fixed-effect projection attachment (reference vckss_rust.h:400-427,
+ * 798-838, 1721, 1820-1829, 1983-1998; ffi_engine.rs:2413-2418, 3679-3835,
+ * 6030-6110).  A prepared generation whose solve runs the generic JLA engine
+ * (controls, or leave-observation-out) takes one projection of a worker or
+ * firm effect on caller covariates (plus the automatic constant): the host
+ * builds the coefficient-space loadings at augmentation; the solve runs the
+ * loadings' model solves on the GPU after the target phase and streams the
+ * KSS covariance over the deletion units.  At most 31 covariates (32
+ * columns with the constant) on the device. */
+#define VCKSS_PROJECTION_EFFECT_WORKER 1u
+#define VCKSS_PROJECTION_EFFECT_FIRM 2u
+#define VCKSS_PROJECTION_WEIGHT_FREQUENCY 1u
+#define VCKSS_PROJECTION_WEIGHT_TARGET 2u
+#define VCKSS_PROJECTION_SCHEMA_V1 1u
+
+typedef struct VckssProjectionAugmentationRequestV1 {
+  uint32_t abi_version;
+  uint32_t struct_size;
+  uint64_t rows;
+  uint32_t project_count;
+  uint32_t effect;
+  uint32_t weight;
+  uint32_t reserved;
+  double rank_tolerance;
+  uint64_t caller_copy_bytes;
+} VckssProjectionAugmentationRequestV1;
+
+typedef struct VckssProjectionAugmentationRequestInterruptV1 {
+  VckssProjectionAugmentationRequestV1 options;
+  VckssInterruptPollV1 interrupt_poll;
+  void *interrupt_context;
+  uint32_t checkpoint_interval;
+  uint32_t reserved;
+} VckssProjectionAugmentationRequestInterruptV1;
+
+typedef struct VckssProjectionColumnsV1 {
+  uint32_t struct_size;
+  uint32_t reserved;
+  uint64_t rows;
+  const double *const *project;
+  uint32_t project_count;
+  uint32_t reserved_2;
+} VckssProjectionColumnsV1;
+
+typedef struct VckssProjectionAugmentationReceiptV1 {
+  uint32_t struct_size;
+  uint32_t schema_version;
+  uint64_t generation;
+  uint64_t rows;
+  uint64_t columns;
+  uint32_t effect;
+  uint32_t weight;
+  uint64_t caller_copy_bytes;
+  uint64_t augmentation_peak_forecast_bytes;
+  uint64_t projection_persistent_bytes;
+  uint64_t total_prepared_resident_bytes;
+  double gram_rcond;
+  double gram_relres;
+  double gram_original_relres;
+} VckssProjectionAugmentationReceiptV1;
+
+typedef struct VckssProjectionResultReceiptV1 {
+  uint32_t struct_size;
+  uint32_t schema_version;
+  uint64_t generation;
+  uint64_t columns;
+  uint32_t effect;
+  uint32_t weight;
+  double gram_rcond;
+  double gram_relres;
+  double gram_original_relres;
+  double covariance_smallest_eigenvalue;
+  double covariance_largest_eigenvalue;
+  double psd_cleanup;
+  double proxy_minimum;
+  double proxy_maximum;
+  uint32_t maximum_iterations;
+  uint32_t reserved;
+  double maximum_reduced_residual;
+  double maximum_complete_residual;
+  double full_residual_tolerance;
+  uint64_t projection_peak_forecast_bytes;
+  uint64_t persistent_bytes;
+  uint64_t result_bytes;
+} VckssProjectionResultReceiptV1;
+
+#if defined(__cplusplus)
+static_assert(sizeof(VckssProjectionAugmentationRequestV1) == 48, "projection augmentation request size");
+static_assert(sizeof(VckssProjectionAugmentationRequestInterruptV1) == 72, "interrupt projection request size");
+static_assert(sizeof(VckssProjectionColumnsV1) == 32, "projection column descriptor size");
+static_assert(sizeof(VckssProjectionAugmentationReceiptV1) == 96, "projection augmentation receipt size");
+static_assert(sizeof(VckssProjectionResultReceiptV1) == 152, "projection result receipt size");
+#endif
+
+/* 1: Mean-centred projection covariance is available. */
+uint32_t vckss_rust_projection_centering_schema_v1(void);
+/* Defaults: worker effect, frequency weight, rank tolerance 1e-10. */
+int32_t vckss_rust_engine_default_projection_augmentation_request_interrupt_v1(
+    VckssProjectionAugmentationRequestInterruptV1 *output, uint32_t output_capacity_bytes);
+/* Attach to a prepared (unsolved) generation: columns copied synchronously;
+ * INVALID_INPUT for malformed requests or nonfinite columns, SINGULAR_INFORMATION
+ * for an unidentified covariate Gram, CONTEXT_POISONED for a second projection. */
+int32_t vckss_rust_engine_augment_projection_interrupt_v1(uint64_t generation,
+                                                           const VckssProjectionAugmentationRequestInterruptV1 *request,
+                                                           const VckssProjectionColumnsV1 *columns);
+int32_t vckss_rust_engine_projection_augmentation_receipt_v1(uint64_t generation,
+                                                             VckssProjectionAugmentationReceiptV1 *output,
+                                                             uint32_t output_capacity_bytes);
+/* After a solve: the columns' coefficients, the KSS covariance (PSD-cleaned)
+ * and the naive covariance, each columns x columns row-major. */
+int32_t vckss_rust_engine_projection_result_v1(uint64_t generation, double *coefficients,
+                                               uint64_t coefficients_capacity, double *covariance,
+                                               uint64_t covariance_capacity, double *naive_covariance,
+                                               uint64_t naive_covariance_capacity,
+                                               VckssProjectionResultReceiptV1 *output, uint32_t output_capacity_bytes);
+int32_t vckss_rust_engine_projection_result_receipt_v1(uint64_t generation, VckssProjectionResultReceiptV1 *output,
+                                                       uint32_t output_capacity_bytes);
+
+/* ---------------------------------------------------------------------------
  * The rest of the reference ABI (rust/stata_backend/include/vckss_rust.h).
  * These entry points sit outside the solve path this library replaces: the
- * schema probes report what is available (centering 1; numerical, exact
- * execution, projection and component inference 0, i.e. absent), session
+ * schema probes report what is available (centering 1; exact execution and
+ * component inference 0, i.e. absent), session
  * last-error text is the engine's, and every other call returns
  * VCKSS_UNSUPPORTED_FEATURE (11) with its name in the last-error text.
  * Their argument structs are only passed through, so they are declared
@@ -1393,10 +1512,6 @@ typedef struct VckssPreparationReceiptV1 VckssPreparationReceiptV1;
 typedef struct VckssPrepareRequestV1 VckssPrepareRequestV1;
 typedef int32_t (*VckssProgressOperationV1)(void *);
 typedef struct VckssProgressOptionsV1 VckssProgressOptionsV1;
-typedef struct VckssProjectionAugmentationReceiptV1 VckssProjectionAugmentationReceiptV1;
-typedef struct VckssProjectionAugmentationRequestInterruptV1 VckssProjectionAugmentationRequestInterruptV1;
-typedef struct VckssProjectionColumnsV1 VckssProjectionColumnsV1;
-typedef struct VckssProjectionResultReceiptV1 VckssProjectionResultReceiptV1;
 typedef struct VckssRepeatMeasurementDiagnosticV1 VckssRepeatMeasurementDiagnosticV1;
 typedef struct VckssRepeatMeasurementLeadingV1 VckssRepeatMeasurementLeadingV1;
 typedef struct VckssSessionSnapshotV1 VckssSessionSnapshotV1;
@@ -1444,8 +1559,6 @@ int32_t vckss_rust_engine_augment_match_component_inference_interrupt_v3(uint64_
 int32_t vckss_rust_engine_augment_match_component_inference_interrupt_v4(uint64_t generation, const VckssComponentInferenceAugmentationRequestInterruptV1 *request, uint32_t gram_probes);
 /* vckss_rust.h:1898 */
 int32_t vckss_rust_engine_augment_match_component_inference_interrupt_v5(uint64_t generation, const VckssComponentInferenceAugmentationRequestInterruptV1 *request, uint32_t gram_probes);
-/* vckss_rust.h:1820 */
-int32_t vckss_rust_engine_augment_projection_interrupt_v1(uint64_t generation, const VckssProjectionAugmentationRequestInterruptV1 *request, const VckssProjectionColumnsV1 *columns);
 /* vckss_rust.h:1810 */
 int32_t vckss_rust_engine_augment_stayers_interrupt_v1(uint64_t generation, const VckssStayerAugmentationRequestInterruptV1 *request, const VckssStayerAugmentationColumnsV1 *columns);
 /* vckss_rust.h:1805 */
@@ -1468,8 +1581,6 @@ int32_t vckss_rust_engine_component_inference_unit_receipt_v1(uint64_t generatio
 int32_t vckss_rust_engine_component_inference_unit_receipt_v2(uint64_t generation, VckssComponentInferenceUnitReceiptV2 *output, uint32_t output_capacity_bytes);
 /* vckss_rust.h:1725 */
 int32_t vckss_rust_engine_default_component_inference_augmentation_request_interrupt_v1(VckssComponentInferenceAugmentationRequestInterruptV1 *output, uint32_t output_capacity_bytes);
-/* vckss_rust.h:1721 */
-int32_t vckss_rust_engine_default_projection_augmentation_request_interrupt_v1(VckssProjectionAugmentationRequestInterruptV1 *output, uint32_t output_capacity_bytes);
 /* vckss_rust.h:1733 */
 int32_t vckss_rust_engine_default_solve_request_interrupt_v2(VckssEngineSolveRequestInterruptV2 *output, uint32_t output_capacity_bytes);
 /* vckss_rust.h:1737 */
@@ -1516,12 +1627,6 @@ int32_t vckss_rust_engine_performance_receipt_v1(uint64_t generation, VckssEngin
 int32_t vckss_rust_engine_prepare_interrupt_v3(const VckssEnginePrepareRequestInterruptV2 *request, const VckssEngineColumnsV3 *columns, uint64_t *output_handle, uint32_t output_capacity_bytes);
 /* vckss_rust.h:2313 */
 int32_t vckss_rust_engine_prepare_memory_interrupt_v1(const VckssEnginePrepareRequestInterruptV3 *, const VckssEngineColumnsV3 *, const VckssMemoryPolicyV1 *, uint64_t *, uint32_t);
-/* vckss_rust.h:1825 */
-int32_t vckss_rust_engine_projection_augmentation_receipt_v1(uint64_t generation, VckssProjectionAugmentationReceiptV1 *output, uint32_t output_capacity_bytes);
-/* vckss_rust.h:1994 */
-int32_t vckss_rust_engine_projection_result_receipt_v1(uint64_t generation, VckssProjectionResultReceiptV1 *output, uint32_t output_capacity_bytes);
-/* vckss_rust.h:1983 */
-int32_t vckss_rust_engine_projection_result_v1(uint64_t generation, double *coefficients, uint64_t coefficients_capacity, double *covariance, uint64_t covariance_capacity, double *naive_covariance, uint64_t naive_covariance_capacity, VckssProjectionResultReceiptV1 *output, uint32_t output_capacity_bytes);
 /* vckss_rust.h:1853 */
 int32_t vckss_rust_engine_repeat_measurement_diagnostic_v1(uint64_t generation, VckssRepeatMeasurementDiagnosticV1 *output, uint32_t output_capacity_bytes);
 /* vckss_rust.h:1858 */
@@ -1574,8 +1679,6 @@ uint32_t vckss_rust_exact_resolved_execution_schema_v2(void);
 uint32_t vckss_rust_numerical_schema_v1(void);
 /* vckss_rust.h:2348 */
 uint32_t vckss_rust_numerical_schema_v2(void);
-/* vckss_rust.h:13 */
-uint32_t vckss_rust_projection_centering_schema_v1(void);
 /* vckss_rust.h:316 */
 int32_t vckss_rust_report_call_v1(const VckssProgressOptionsV1 *, VckssProgressOperationV1, void *);
 /* vckss_rust.h:1677 */

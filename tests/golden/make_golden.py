@@ -546,10 +546,159 @@ def write_numerical_cases(lib, meta: dict) -> None:
                                                           indent=1))
 
 
+# The plugin's fixed-effect projection attachment
+# (vckss_rust_engine_augment_projection_interrupt_v1 on a prepared generation,
+# a generic-engine V5 solve, then projection_result_v1): covariates are seeded
+# functions of the retained rows (a normal draw per input row, the row's
+# period index, a product of the two), restricted to the retained rows in
+# input order.  Each case names the panel, deletion mode, effect (1 worker,
+# 2 firm), weight (1 frequency, 2 target), covariates and centering.
+PROJECTION_CASES = {
+    "controls_2k_worker": dict(panel="controls_2k", deletion=1, effect=1, weight=1, covariates=2, centering=0,
+                               probes=16),
+    "controls_2k_firm_mean": dict(panel="controls_2k", deletion=1, effect=2, weight=1, covariates=3, centering=1,
+                                  probes=16),
+    "controls_weighted_1500_target": dict(panel="controls_weighted_1500", deletion=1, effect=1, weight=2,
+                                          covariates=1, centering=0, probes=12),
+    "obs_2k_worker": dict(panel="obs_2k", deletion=2, effect=1, weight=1, covariates=2, centering=0, probes=16),
+    "obs_controls_2k_firm": dict(panel="obs_controls_2k", deletion=2, effect=2, weight=2, covariates=2,
+                                 centering=1, probes=16),
+    "obs_controls_duplicates_worker": dict(panel="obs_controls_duplicates_1500", deletion=2, effect=1, weight=1,
+                                           covariates=3, centering=0, probes=12),
+}
+
+PROJECTION_RESULT_FIELDS = ("columns", "effect", "weight", "gram_rcond", "gram_relres", "gram_original_relres",
+                            "covariance_smallest_eigenvalue", "covariance_largest_eigenvalue", "psd_cleanup",
+                            "proxy_minimum", "proxy_maximum", "maximum_iterations", "full_residual_tolerance",
+                            "persistent_bytes", "result_bytes")
+PROJECTION_AUGMENTATION_FIELDS = ("rows", "columns", "effect", "weight", "caller_copy_bytes",
+                                  "projection_persistent_bytes", "gram_rcond", "gram_relres", "gram_original_relres")
+
+
+def projection_panel(name: str) -> Panel:
+    specs = {**CONTROL_PANELS, **OBSERVATION_PANELS}
+    return specs[name]["build"]()
+
+
+def projection_covariates(panel: Panel, mask: np.ndarray, count: int, seed: int) -> list:
+    """Seeded covariates for the retained rows (input order)."""
+    rng = np.random.default_rng(seed)
+    z = rng.standard_normal(panel.rows)
+    period = (np.arange(panel.rows) % 5).astype(np.float64)
+    full = [z, period, z * period + 0.5 * z * z][:count]
+    keep = mask.astype(bool)
+    return [np.ascontiguousarray(c[keep]) for c in full]
+
+
+def projection_request(e, probes: int, deletion: int, controls: int):
+    """V5 generic-engine request: diagonal PCG at 1e-12, the given probes."""
+    q = e.default_request_v5(deletion)
+    v1 = q.v4.v3.v2.v1
+    v1.probes = probes
+    v1.solver_route = 2
+    v1.pcg_tolerance = 1e-12
+    v1.maximum_iterations = 20000
+    q.v4.v3.v2.algorithm = 2
+    q.threads = 4
+    q.tolerance_supplied = 1
+    return q
+
+
+def projection_record(lib, spec: dict) -> dict:
+    panel = projection_panel(spec["panel"])
+    e = abi.Engine(lib)
+    e.prepare(panel, deletion_mode=spec["deletion"])
+    mask = e.retained_mask(panel.rows)
+    cov = projection_covariates(panel, mask, spec["covariates"], 20261204)
+    if spec["centering"]:
+        e.centering(spec["centering"])
+    e.augment_projection(cov, spec["effect"], spec["weight"])
+    aug = e.projection_augmentation_receipt()
+    e.solve_v5(projection_request(e, spec["probes"], spec["deletion"], len(panel.controls)),
+               controls_count=len(panel.controls))
+    res = e.projection_result()
+    point = e.result()
+    e.release()
+    return {"panel_sha256": panel_digest(panel), "pcg_tolerance": 1e-12, **spec,
+            "augmentation": {k: aug[k] for k in PROJECTION_AUGMENTATION_FIELDS},
+            "coefficients": res["coefficients"], "covariance": res["covariance"],
+            "naive_covariance": res["naive_covariance"],
+            "receipt": {k: res["receipt"][k] for k in PROJECTION_RESULT_FIELDS},
+            "corrected": list(point["corrected"])}
+
+
+def projection_error_record(lib) -> dict:
+    """Status codes of refused projection calls, each on a fresh generation,
+    and the status of a valid augmentation after a refused one."""
+    out = {}
+    panel = projection_panel("controls_2k")
+
+    def fresh():
+        e = abi.Engine(lib)
+        e.prepare(panel)
+        mask = e.retained_mask(panel.rows)
+        return e, projection_covariates(panel, mask, 2, 20261204), int(mask.sum())
+
+    def status(fn) -> int:
+        try:
+            fn()
+            return 0
+        except abi.EngineError as err:
+            return err.code
+
+    e, cov, rows = fresh()
+    e.release()
+    cases = {"constant_covariate": ([np.ones(rows)], 1, 1, 1e-10),
+             "rank_tolerance_high": (cov, 1, 1, 0.5),
+             "rank_tolerance_low": (cov, 1, 1, 1e-16),
+             "effect_unknown": (cov, 3, 1, 1e-10),
+             "weight_unknown": (cov, 1, 3, 1e-10),
+             "rows_short": ([c[:-1] for c in cov], 1, 1, 1e-10)}
+    for name, args in cases.items():
+        e, cov, rows = fresh()
+        out[name] = status(lambda: e.augment_projection(*args))
+        out[name + "_then_valid"] = status(lambda: e.augment_projection(cov))
+        e.release()
+    e, cov, rows = fresh()
+    e.augment_projection(cov)
+    out["second_projection"] = status(lambda: e.augment_projection(cov))
+    e.release()
+    e, cov, rows = fresh()
+    e.augment_projection(cov)
+    e.solve_v5(projection_request(e, 8, 1, len(panel.controls)), controls_count=len(panel.controls))
+    out["augmentation_receipt_after_solve"] = status(lambda: e.projection_augmentation_receipt())
+    e.release()
+    e, cov, rows = fresh()
+    e.solve_v5(projection_request(e, 8, 1, len(panel.controls)), controls_count=len(panel.controls))
+    out["result_without_projection"] = status(lambda: e.projection_result())
+    e.release()
+    # a match panel without controls runs the compressed engine: refused
+    plain = PANELS["small_2k"]["build"]()
+    e = abi.Engine(lib)
+    e.prepare(plain, use_v4=True)
+    e.augment_projection(projection_covariates(plain, e.retained_mask(plain.rows), 1, 7))
+    out["compressed_engine_solve"] = status(
+        lambda: e.solve_v5(projection_request(e, 8, 1, 0), controls_count=0))
+    e.release()
+    return out
+
+
+def write_projection_cases(lib, meta: dict) -> None:
+    cases = {}
+    for name, spec in PROJECTION_CASES.items():
+        cases[name] = projection_record(lib, spec)
+        print(name, cases[name]["coefficients"], cases[name]["receipt"]["psd_cleanup"])
+    errors = projection_error_record(lib)
+    print(errors)
+    (HERE / "projection_cases.json").write_text(json.dumps({"meta": meta, "cases": cases, "errors": errors},
+                                                           indent=1))
+
+
 def main() -> None:
     """All fixtures; with the argument ``cmg`` only cmg_cases.json, with
     ``receipts`` only receipt_cases.json, with ``sized`` only sized_cases.json, with
-    ``exact`` only exact_cases.json, with ``numerical`` only numerical_cases.json."""
+    ``exact`` only exact_cases.json, with ``numerical`` only numerical_cases.json, with
+    ``projection`` only projection_cases.json."""
     if not PLUGIN.exists():
         raise SystemExit(f"reference plugin not found at {PLUGIN}")
     lib = abi.load(PLUGIN, bind_extensions=False)
@@ -564,6 +713,10 @@ def main() -> None:
     if sys.argv[1:] == ["numerical"]:
         write_numerical_cases(lib, {"generator": "tests/golden/make_golden.py numerical",
                                     "reference_plugin_version": lib.vckss_rust_backend_version().decode()})
+        return
+    if sys.argv[1:] == ["projection"]:
+        write_projection_cases(lib, {"generator": "tests/golden/make_golden.py projection",
+                                     "reference_plugin_version": lib.vckss_rust_backend_version().decode()})
         return
     if sys.argv[1:] == ["sized"]:
         write_sized_cases(lib, {"generator": "tests/golden/make_golden.py sized", "reference_plugin_version":

@@ -64,9 +64,14 @@ def test_default_requests_match_reference(lib, name, cls):
 
 
 def test_output_capacity_checked(lib):
+    """A short output capacity is an ABI mismatch (10), a null output an
+    invalid input (20), as the plugin reports them."""
     req = abi.SolveRequestV1()
-    assert lib.vckss_rust_engine_default_solve_request_v1(C.byref(req), 8) == 20
-    assert b"capacity" in lib.vckss_rust_engine_last_error()
+    ref = abi.load(PLUGIN, bind_extensions=False)
+    for L in (lib, ref):
+        assert L.vckss_rust_engine_default_solve_request_v1(C.byref(req), 8) == 10
+        assert L.vckss_rust_engine_default_solve_request_v1(None, C.sizeof(req)) == 20
+    assert b"capacity" in lib.vckss_rust_engine_last_error() or b"pointer" in lib.vckss_rust_engine_last_error()
 
 
 def test_lifecycle_errors(lib):
@@ -253,13 +258,15 @@ def test_v4_solve_refuses_an_unreconciled_request(lib):
 
 def test_entry_points_outside_the_solve_path(lib):
     """Every other reference entry point exists: schema probes report what is
-    available (centering and the numerical attachment V1) and the rest return
+    available (centering, the numerical attachment V1 and Mean-centred
+    projection) and the rest return
     UNSUPPORTED_FEATURE naming the call."""
     assert lib.vckss_rust_centering_schema_v1() == 1
     assert lib.vckss_rust_numerical_schema_v1() == 1
+    assert lib.vckss_rust_projection_centering_schema_v1() == 1
     for probe in ("numerical_schema_v2", "exact_execution_schema_v1",
                   "exact_legacy_execution_schema_v1", "exact_resolved_execution_schema_v2",
-                  "projection_centering_schema_v1", "component_inference_interface_version"):
+                  "component_inference_interface_version"):
         assert getattr(lib, "vckss_rust_" + probe)() == 0, probe
     called = 0
     for name, (res, args) in abi.UNSUPPORTED_SIGNATURES.items():
@@ -270,7 +277,7 @@ def test_entry_points_outside_the_solve_path(lib):
         assert name[len("vckss_rust_"):].encode() in lib.vckss_rust_engine_last_error(), name
         assert lib.vckss_rust_session_last_error() == lib.vckss_rust_engine_last_error()
         called += 1
-    assert called >= 75
+    assert called >= 70
 
 
 def test_prepare_timings_split_the_preparation(lib):

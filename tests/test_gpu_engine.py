@@ -227,6 +227,29 @@ def test_receipts_and_resolve(lib):
     assert t["kernel_launches"] > 0 and t["rhs_columns"] == 1 + 3 * probes
 
 
+@pytest.mark.parametrize("precond", [1, 2, 4])
+def test_kernel_launch_count_matches_the_profiler(lib, precond):
+    """A solve's kernel-launch count (kept by wrappers around the runtime's two
+    launch calls, CUDA-graph replays added per replay) equals the number of
+    kernels the CUDA profiling interface records for the same solve: Jacobi
+    (cooperative kernel), CMG (V-cycles replayed from a graph) and the
+    single-kernel PCG with the uniform-weight degree-1 stage."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    panel = make_golden.PANELS["small_2k"]["build"]()
+    e = solve(lib, panel, probes=16, tol=1e-10, precond=precond)
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        e.resolve()
+        torch.cuda.synchronize()
+    t = e.timings()
+    e.release()
+    kernels = [ev.name for ev in prof.events()
+               if ev.device_type == torch.autograd.DeviceType.CUDA and not ev.name.startswith(("Memcpy", "Memset"))]
+    assert t["kernel_launches"] == len(kernels), (t["kernel_launches"], len(kernels), sorted(set(kernels))[:8])
+
+
 def test_accounting_identity_on_a_larger_panel(lib):
     from fevc_b200.panel import generate_panel
 
