@@ -404,6 +404,49 @@ def numerical_attachment(lib, panel, probes, tolerance):
                     "the C ABI, wall of solve_numerical_v1 on a fresh generation"}
 
 
+def projection_attachment(lib, panel, probes, tolerance):
+    """The fixed-effect projection attachment on the same panel and request:
+    the worker effect projected on three seeded covariates (a normal draw,
+    the row's period index, their product) plus the constant, frequency
+    weights, on a fresh generation.  Reports the host augmentation (loadings
+    and Gram certificates), the solve's wall and the projection's share of it
+    (its four model solves and the streamed covariance pass)."""
+    import numpy as np
+    import torch
+
+    from fevc_b200 import abi, learned
+
+    e = abi.Engine(lib)
+    e.prepare(panel, deletion_mode=deletion_mode(panel))
+    e.device_options(64, 3 if learned.load_params() is not None else 4, 2)
+    keep = e.retained_mask(panel.rows).astype(bool)
+    rng = np.random.default_rng(20261204)
+    z = rng.standard_normal(panel.rows)
+    period = (np.arange(panel.rows) % 5).astype(np.float64)
+    cov = [np.ascontiguousarray(c[keep]) for c in (z, period, z * period)]
+    t0 = time.perf_counter()
+    e.augment_projection(cov)
+    augment_s = time.perf_counter() - t0
+    q = v5_request(e, probes, tolerance, deletion=deletion_mode(panel))
+    t0 = time.perf_counter()
+    e.solve_v5(q, controls_count=len(panel.controls))
+    torch.cuda.synchronize()
+    s = time.perf_counter() - t0
+    t = e.timings()
+    res = e.projection_result()
+    e.release()
+    r = res["receipt"]
+    return {"augment_s": round(augment_s, 3), "solve_s": round(s, 3),
+            "projection_ms": round(t["total_ms"] - t["fit_ms"] - t["leverage_ms"] - t["target_ms"], 1),
+            "columns": r["columns"], "coefficients": [round(x, 9) for x in res["coefficients"]],
+            "covariance_diagonal": [res["covariance"][i][i] for i in range(r["columns"])],
+            "psd_cleanup": r["psd_cleanup"], "maximum_iterations": r["maximum_iterations"],
+            "maximum_complete_residual": r["maximum_complete_residual"],
+            "form": "projection attachment: worker effect on 3 covariates + constant, frequency weights; host "
+                    "augmentation, then solve_v5 on a fresh generation (projection solves and covariance pass "
+                    "after the target phase)"}
+
+
 def time_forms(lib, panel, args, stream, barrier, headline):
     from fevc_b200 import abi, learned
 
@@ -423,6 +466,7 @@ def time_forms(lib, panel, args, stream, barrier, headline):
     forms["plain_gpu_cmg_pcg"] = guarded(lambda: plain_form_rate(lib, panel, min(args.probes, args.plain_probes),
                                                                  args.tolerance))
     forms["numerical_attachment"] = guarded(lambda: numerical_attachment(lib, panel, args.probes, args.tolerance))
+    forms["projection_attachment"] = guarded(lambda: projection_attachment(lib, panel, args.probes, args.tolerance))
     return forms
 
 

@@ -51,7 +51,7 @@ def test_projection_matches_the_plugin(lib, name):
     try:
         got = e.projection_result()
         point = e.result()
-        receipts = e.rhs_receipts(int(e.timings()["rhs_columns"]))
+        receipts = e.rhs_receipts(int(e.timings()["rhs_columns"]) + 64)
     finally:
         e.release()
     assert rel(point["corrected"], case["corrected"]) < 1e-8
