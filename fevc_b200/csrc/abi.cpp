@@ -468,8 +468,6 @@ SolveOptions options_from_v4(const VckssEngineSolveRequestV4& q) {
   VckssEngineSolveRequestV1 v1 = q.v3.v2.v1;
   if (v1.leverage_batch_width == 0) v1.leverage_batch_width = 8;
   if (v1.target_batch_width == 0) v1.target_batch_width = 8;
-  if (q.v3.v2.nuisance_mode == VCKSS_NUISANCE_FIXED_OFFSET)
-    fail(UNSUPPORTED_FEATURE, "engine_solve", "fixed-offset nuisance is not provided by the device engine");
   if (q.v3.v2.algorithm == VCKSS_ALGORITHM_EXACT) {
     // the reference's exact-estimator option gates
     // (vckss-core/src/exact_estimator.rs:76-125)
@@ -483,7 +481,9 @@ SolveOptions options_from_v4(const VckssEngineSolveRequestV4& q) {
     o.blocksize_limit = q.v3.v2.blocksize_limit;
     return o;
   }
-  return options_from_v1(v1, true);
+  SolveOptions o = options_from_v1(v1, true);
+  o.fixed_offset = q.v3.v2.nuisance_mode == VCKSS_NUISANCE_FIXED_OFFSET;
+  return o;
 }
 
 // The exact path covers match deletion without controls: every deletion

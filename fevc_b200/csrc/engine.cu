@@ -321,6 +321,12 @@ struct DeviceEngine {
   DBuf<unsigned long long> proj_keys;
   const PreparedProjection* proj_loaded = nullptr;
   std::vector<double> proj_coef;
+  // the outcome every phase after the fit works on (y, or y - Q'beta under
+  // the fixed-offset nuisance), its centre, and the controls still active
+  DBuf<double> row_yw, cell_yw;
+  const double* y_work = nullptr;
+  double y_center = 0.0;
+  int qa = 0;
   DBuf<unsigned long long> num_stats;
   std::map<int, std::unique_ptr<BlockWork>> work;
   // pinned host scalars
@@ -1699,10 +1705,10 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
       // row-level contraction over match groups
       std::vector<double> t(QMAX * K, 0.0), beta(QMAX * K, 0.0), g2(2 * K, 0.0);
       auto solve_beta = [&] {
-        for (int k = 0; k < e.q; ++k)
+        for (int k = 0; k < e.qa; ++k)
           for (int j = 0; j < K; ++j) {
             double v = 0.0;
-            for (int l = 0; l < e.q; ++l) v -= e.Sinv[k * e.q + l] * t[l * K + j];
+            for (int l = 0; l < e.qa; ++l) v -= e.Sinv[k * e.qa + l] * t[l * K + j];
             beta[k * K + j] = v;
           }
       };
@@ -1712,8 +1718,8 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
           e.obs_fused.alloc(2 * (QMAX + 1) * 128);
           e.partial2.alloc(size_t(L.grid) * (QMAX + 1) * 128 + 1024);
         }
-        k_obs_target_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.q, e.cell_worker.p, e.cell_firm.p,
-                                                           e.q > 0 ? e.cellQ.p : nullptr, e.obs_cell_sums.p,
+        k_obs_target_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.qa, e.cell_worker.p, e.cell_firm.p,
+                                                           e.qa > 0 ? e.cellQ.p : nullptr, e.obs_cell_sums.p,
                                                            w.alpha.p, w.x.p, e.partial.p, e.partial2.p);
         finish(e.partial.p, L.grid, (QMAX + 1) * K, e.obs_fused.p, L.s);
         finish(e.partial2.p, L.grid, (QMAX + 1) * K, e.obs_fused.p + (QMAX + 1) * K, L.s);
@@ -1723,31 +1729,31 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
         const double* A = f.data() + QMAX * K;
         const double* B = f.data() + (QMAX + 1) * K;
         const double* Atot = f.data() + (2 * QMAX + 1) * K;
-        for (int k = 0; k < e.q; ++k)
+        for (int k = 0; k < e.qa; ++k)
           for (int j = 0; j < K; ++j) t[k * K + j] = f[k * K + j];
         solve_beta();
         for (int j = 0; j < K; ++j) {
           double v = A[j];
-          for (int k = 0; k < e.q; ++k) v += 2.0 * B[k * K + j] * beta[k * K + j];
+          for (int k = 0; k < e.qa; ++k) v += 2.0 * B[k * K + j] * beta[k * K + j];
           g2[j] = v;
         }
         for (int j = 0; j + 1 < K; j += 2) {
           double v = Atot[j];
-          for (int k = 0; k < e.q; ++k)
+          for (int k = 0; k < e.qa; ++k)
             v += 2.0 * (B[k * K + j] + B[k * K + j + 1]) * (beta[k * K + j] + beta[k * K + j + 1]);
           g2[K + j] = v;
         }
         if (o.numerical) {  // the attachment's per-row target folds of this block
           CK(cudaMemcpyAsync(e.beta_buf.p, beta.data(), QMAX * K * sizeof(double), cudaMemcpyHostToDevice, L.s));
-          k_obs_num_folds<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.q, uint64_t(first), np, e.unit_ptr.p,
+          k_obs_num_folds<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.qa, uint64_t(first), np, e.unit_ptr.p,
                                                           e.cell_rows.p, e.cell_worker.p, e.cell_firm.p, w.alpha.p,
-                                                          w.x.p, e.beta_buf.p, e.Rd.p, e.row_y.p, y_center,
+                                                          w.x.p, e.beta_buf.p, e.Rd.p, e.y_work, y_center,
                                                           e.residual.p, double((o.probes + 1) / 2),
                                                           double(o.probes / 2), e.num_row_fold.p);
         }
       } else {
-        if (e.q > 0) {
-          k_target_control_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.q, e.cell_worker.p, e.cell_firm.p,
+        if (e.qa > 0) {
+          k_target_control_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, e.qa, e.cell_worker.p, e.cell_firm.p,
                                                                  e.cellQ.p, w.alpha.p, w.x.p, e.partial.p);
           finish(e.partial.p, L.grid, QMAX * K, w.tot.p, L.s);
           CK(cudaMemcpyAsync(t.data(), w.tot.p, QMAX * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
@@ -1755,11 +1761,11 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
         }
         solve_beta();
         CK(cudaMemcpyAsync(e.beta_buf.p, beta.data(), QMAX * K * sizeof(double), cudaMemcpyHostToDevice, L.s));
-        k_generic_contract_units<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.q, e.unit_cell.p, e.cell_worker.p,
+        k_generic_contract_units<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.qa, e.unit_cell.p, e.cell_worker.p,
                                                                  e.cell_firm.p, e.unit_sums.p, e.beta_buf.p,
                                                                  w.alpha.p, w.x.p, e.partial.p);
         if (o.numerical)  // the attachment's match-unit target folds of this block
-          k_num_block_folds<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.q, uint64_t(first), np, e.unit_cell.p,
+          k_num_block_folds<K><<<L.grid, THREADS, 0, L.s>>>(e.G, e.qa, uint64_t(first), np, e.unit_cell.p,
                                                             e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p,
                                                             e.beta_buf.p, e.num_block_sums.p,
                                                             double((o.probes + 1) / 2), double(o.probes / 2),
@@ -1768,12 +1774,12 @@ void run_target(DeviceEngine& e, const SolveOptions& o, SolveResult& res, double
         CK(cudaMemcpyAsync(g2.data(), w.tot.p, 2 * K * sizeof(double), cudaMemcpyDeviceToHost, L.s));
         CK(cudaStreamSynchronize(L.s));
       }
-      if (e.observation && e.q > 0) {
+      if (e.observation && e.qa > 0) {
         // the cell-independent beta' S2 beta terms of every column and of the total
         auto quad = [&](int ja, int jb) {
           double acc = 0.0;
-          for (int k = 0; k < e.q; ++k)
-            for (int l = k; l < e.q; ++l) {
+          for (int k = 0; k < e.qa; ++k)
+            for (int l = k; l < e.qa; ++l) {
               const double bk = beta[k * K + ja] + (jb >= 0 ? beta[k * K + jb] : 0.0);
               const double bl = beta[l * K + ja] + (jb >= 0 ? beta[l * K + jb] : 0.0);
               acc += (l == k ? 1.0 : 2.0) * e.obs_S2[k * QMAX + l] * bk * bl;
@@ -2100,7 +2106,7 @@ uint32_t numerical_derivative(DeviceEngine& e, const SolveOptions& o, NumericalA
     if (e.num_copy_pb.n < size_t(e.physical) * 2) e.num_copy_pb.alloc(size_t(e.physical) * 2);
     k_obs_num_derivative<<<L.grid, THREADS, 0, L.s>>>(e.rows, double(o.probes), e.row_phys.p, e.row_rank_d.p,
                                                       e.row_copy_offset.p, e.obs_row_acc.p, e.obs_copy_acc.p,
-                                                      e.q > 0 ? e.control_lev.p : nullptr, e.num_row_coef.p,
+                                                      e.qa > 0 ? e.control_lev.p : nullptr, e.num_row_coef.p,
                                                       e.num_copy_pb.p, e.num_stats.p);
   } else if (e.generic) {
     // match groups with controls (generic_jla/numerical.rs `State::block`)
@@ -2458,7 +2464,7 @@ void setup_controls(DeviceEngine& e, const SolveOptions& o, SolveTimings& tm) {
 // deletion units for the KSS and naive covariances.
 void run_projection(DeviceEngine& e, const Compressed& p, const SolveOptions& o, double y_center, SolveResult& res) {
   const PreparedProjection& pp = *o.projection;
-  const int cols = int(pp.columns), q = e.q;
+  const int cols = int(pp.columns), q = e.qa;  // active controls (joint: all, fixed offset: none)
   if (cols < 2 || cols > PROJ_MAX_COLUMNS)
     fail(RESOURCE_LIMIT, "generic_jla_projection", "the device projection handles at most 31 covariates");
   if (e.proj_coef.size() != size_t(cols))
@@ -2531,7 +2537,7 @@ void run_projection(DeviceEngine& e, const Compressed& p, const SolveOptions& o,
   a.cell_worker = e.cell_worker.p;
   a.cell_firm = e.cell_firm.p;
   a.row_freq = e.row_freq.p;
-  a.y = e.row_y.p;
+  a.y = e.y_work;
   a.deleted = e.deleted.p;
   a.residual = e.residual.p;
   a.R = q > 0 ? e.Rd.p : nullptr;
@@ -2577,9 +2583,28 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
   const int q = e.q;
   // ---- joint fit: FE solve of y, then beta = S^{-1} R'W y and theta = theta_y - H beta
   if (o.shard_phase == 2 || o.reuse_fit) {
-    res.plugin = e.shard_plugin;
+    res.plugin = e.shard_plugin;  // the working outcome, centre and active controls stay
   } else {
     BlockWork& w = get_work<1>(e);
+    // plug-in components of a fit (alpha = w.alpha, psi = w.x) from the
+    // fitted cells: means first, then the centred second moments
+    auto plugin_of_fit = [&] {
+      k_fit_cells<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p, e.cell_target.p,
+                                               e.fitted.p, 0, nullptr, e.partial.p);
+      finish(e.partial.p, L.grid, 4, e.small.p, L.s);
+      std::vector<double> m(4);
+      CK(cudaMemcpyAsync(m.data(), e.small.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+      CK(cudaStreamSynchronize(L.s));
+      double means[2] = {m[0] / p.target_total, m[1] / p.target_total};
+      CK(cudaMemcpyAsync(e.small.p + 8, means, 2 * sizeof(double), cudaMemcpyHostToDevice, L.s));
+      k_fit_cells<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p, e.cell_target.p,
+                                               e.fitted.p, 1, e.small.p + 8, e.partial.p);
+      finish(e.partial.p, L.grid, 4, e.small.p, L.s);
+      CK(cudaMemcpyAsync(m.data(), e.small.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, L.s));
+      CK(cudaStreamSynchronize(L.s));
+      double T = p.target_total;
+      return finish_accounting(m[0] / T, m[1] / T, m[2] / T, m[3] / T, "generic_jla_components");
+    };
     k_gather<1><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, e.cell_outcome.p, w.bW.p);
     firm_gather<1, 0, 0>(e, w, L, nullptr, e.cell_outcome.p, nullptr, 0.0, nullptr, nullptr, nullptr, w.bF.p, nullptr);
     BlockOutcome bo = solve_block<1>(e, w, 1, o, res.timings);
@@ -2595,25 +2620,44 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
       for (int l = 0; l < q; ++l) v += e.Sinv[k * q + l] * ry[l];
       beta.m[k] = v;
     }
-    k_apply_beta<<<L.grid, THREADS, 0, L.s>>>(e.W, q, e.alphaH.p, beta, w.alpha.p);
-    k_apply_beta<<<L.grid, THREADS, 0, L.s>>>(e.F, q, e.psiH.p, beta, w.x.p);
-    k_row_residual<<<L.grid, THREADS, 0, L.s>>>(e.rows, q, e.row_cell.p, e.cell_worker.p, e.cell_firm.p, e.row_y.p,
-                                                e.Qd.p, w.alpha.p, w.x.p, beta, e.residual.p);
-    k_fit_cells<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p, e.cell_target.p,
-                                             e.fitted.p, 0, nullptr, e.partial.p);
-    finish(e.partial.p, L.grid, 4, e.small.p, L.s);
-    std::vector<double> m(4);
-    CK(cudaMemcpyAsync(m.data(), e.small.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, L.s));
-    CK(cudaStreamSynchronize(L.s));
-    double means[2] = {m[0] / p.target_total, m[1] / p.target_total};
-    CK(cudaMemcpyAsync(e.small.p + 8, means, 2 * sizeof(double), cudaMemcpyHostToDevice, L.s));
-    k_fit_cells<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_worker.p, e.cell_firm.p, w.alpha.p, w.x.p, e.cell_target.p,
-                                             e.fitted.p, 1, e.small.p + 8, e.partial.p);
-    finish(e.partial.p, L.grid, 4, e.small.p, L.s);
-    CK(cudaMemcpyAsync(m.data(), e.small.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, L.s));
-    CK(cudaStreamSynchronize(L.s));
-    double T = p.target_total;
-    res.plugin = finish_accounting(m[0] / T, m[1] / T, m[2] / T, m[3] / T, "generic_jla_components");
+    e.y_work = e.row_y.p;
+    e.qa = q;
+    e.y_center = outcome_mean(p, o.centering);
+    if (o.fixed_offset && q > 0) {
+      // fixed-offset nuisance (generic_jla.rs:2011-2046): the working outcome
+      // y - Q'beta of the joint fit, its FE-only fit (phase 4), and from here
+      // on the worker-firm model alone (no active controls)
+      if (e.row_yw.n < e.rows) e.row_yw.alloc(e.rows);
+      if (e.cell_yw.n < e.C) e.cell_yw.alloc(e.C);
+      k_offset_outcome<<<L.grid, THREADS, 0, L.s>>>(e.rows, q, e.row_y.p, e.Qd.p, beta, e.row_yw.p);
+      k_cell_row_sums<<<L.grid, THREADS, 0, L.s>>>(e.C, e.cell_rows_ptr.p, e.cell_rows.p, e.row_freq.p, e.row_yw.p,
+                                                   e.cell_yw.p);
+      k_gather<1><<<L.grid, THREADS, 0, L.s>>>(e.W, e.worker_ptr.p, nullptr, e.cell_yw.p, w.bW.p);
+      firm_gather<1, 0, 0>(e, w, L, nullptr, e.cell_yw.p, nullptr, 0.0, nullptr, nullptr, nullptr, w.bF.p, nullptr);
+      BlockOutcome bw = solve_block<1>(e, w, 1, o, res.timings);
+      res.receipts.push_back(
+          RhsReceipt{4, 1, -1, uint32_t(bw.iters[0]), uint32_t(bw.zero[0]), bw.reduced[0], bw.complete[0]});
+      k_row_residual<<<L.grid, THREADS, 0, L.s>>>(e.rows, 0, e.row_cell.p, e.cell_worker.p, e.cell_firm.p,
+                                                  e.row_yw.p, e.Qd.p, w.alpha.p, w.x.p, SmallMatrix{}, e.residual.p);
+      if (o.centering != Centering::None) {  // the centre of the working outcome (centering.rs:6-30)
+        k_centered_mass<<<L.grid, THREADS, 0, L.s>>>(e.rows, e.row_yw.p, e.row_freq.p, 1.0 / double(p.physical_total),
+                                                     e.partial.p);
+        finish(e.partial.p, L.grid, 1, e.small.p, L.s);
+        double c[2];
+        CK(cudaMemcpyAsync(c, e.small.p, sizeof(double), cudaMemcpyDeviceToHost, L.s));
+        CK(cudaMemcpyAsync(c + 1, e.row_yw.p, sizeof(double), cudaMemcpyDeviceToHost, L.s));
+        CK(cudaStreamSynchronize(L.s));
+        e.y_center = c[1] + c[0];
+      }
+      e.y_work = e.row_yw.p;
+      e.qa = 0;
+    } else {
+      k_apply_beta<<<L.grid, THREADS, 0, L.s>>>(e.W, q, e.alphaH.p, beta, w.alpha.p);
+      k_apply_beta<<<L.grid, THREADS, 0, L.s>>>(e.F, q, e.psiH.p, beta, w.x.p);
+      k_row_residual<<<L.grid, THREADS, 0, L.s>>>(e.rows, q, e.row_cell.p, e.cell_worker.p, e.cell_firm.p,
+                                                  e.row_y.p, e.Qd.p, w.alpha.p, w.x.p, beta, e.residual.p);
+    }
+    res.plugin = plugin_of_fit();
     e.shard_plugin = res.plugin;
     if (o.projection) {  // projection coefficients from the working fit (projection.rs:245-276)
       std::vector<double> a(e.W), f(e.F);
@@ -2623,6 +2667,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
       e.proj_coef = projection_coefficients(*o.projection, a.data(), a.size(), f.data(), f.size());
     }
   }
+  const int qa = e.qa;  // controls active after the fit: all (joint nuisance) or none (fixed offset)
   auto t1 = now();
   // ---- FE-only leverage probes (reference `match_leverage_moments`,
   // `observation_and_match_leverage_moments`)
@@ -2647,16 +2692,16 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     // ---- deleted residual of every row from its copies
     unsigned long long init[2] = {~0ull, 0ull};
     CK(cudaMemcpyAsync(e.error.p, init, sizeof(init), cudaMemcpyHostToDevice, L.s));
-    if (q > 0) {
+    if (qa > 0) {
       SmallMatrix sinv{};
-      for (int i = 0; i < q; ++i)
-        for (int j = 0; j < q; ++j) sinv.m[i * QMAX + j] = e.Sinv[i * q + j];
+      for (int i = 0; i < qa; ++i)
+        for (int j = 0; j < qa; ++j) sinv.m[i * QMAX + j] = e.Sinv[i * q + j];
       k_control_leverage<<<L.grid, THREADS, 0, L.s>>>(e.rows, q, e.Rd.p, sinv, o.rank_tolerance, e.control_lev.p,
                                                       e.error.p);
     }
     ObservationAdjustParams prm{e.rows, double(o.probes), o.block_tolerance, o.rank_tolerance};
     k_obs_adjust<<<L.grid, THREADS, 0, L.s>>>(prm, e.row_phys.p, e.obs_row_acc.p, e.obs_copy_acc.p,
-                                              q > 0 ? e.control_lev.p : nullptr, e.residual.p, e.deleted.p,
+                                              qa > 0 ? e.control_lev.p : nullptr, e.residual.p, e.deleted.p,
                                               e.obs_out.p, e.error.p, e.error.p + 1);
     unsigned long long got[2] = {0, 0};
     CK(cudaMemcpyAsync(got, e.error.p, sizeof(got), cudaMemcpyDeviceToHost, L.s));
@@ -2684,8 +2729,8 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
       e.obs_cell_sums.alloc(size_t(e.C) * (1 + QMAX));
       e.obs_s2.alloc(QMAX * QMAX);
     }
-    k_obs_cell_target_sums<<<L.grid, THREADS, 0, L.s>>>(e.C, q, e.cell_rows_ptr.p, e.cell_rows.p, e.row_freq.p,
-                                                        e.row_y.p, outcome_mean(p, o.centering), e.deleted.p,
+    k_obs_cell_target_sums<<<L.grid, THREADS, 0, L.s>>>(e.C, qa, e.cell_rows_ptr.p, e.cell_rows.p, e.row_freq.p,
+                                                        e.y_work, e.y_center, e.deleted.p,
                                                         e.Rd.p, e.obs_cell_sums.p, e.partial.p);
     finish(e.partial.p, L.grid, QMAX * QMAX, e.obs_s2.p, L.s);
     e.obs_S2.assign(QMAX * QMAX, 0.0);
@@ -2696,12 +2741,12 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
   {
     GenericAdjustParams prm{};
     prm.units = e.G;
-    prm.q = q;
+    prm.q = qa;
     prm.probes = double(o.probes);
     prm.block_tolerance = o.block_tolerance;
     prm.rank_tolerance = o.rank_tolerance;
-    for (int i = 0; i < q; ++i)
-      for (int j = 0; j < q; ++j) prm.factor.m[i * QMAX + j] = e.Lfac[i * q + j];
+    for (int i = 0; i < qa; ++i)
+      for (int j = 0; j < qa; ++j) prm.factor.m[i * QMAX + j] = e.Lfac[i * q + j];
     unsigned long long init[2] = {~0ull, 0ull};
     CK(cudaMemcpyAsync(e.error.p, init, sizeof(init), cudaMemcpyHostToDevice, L.s));
     if (o.numerical) {  // the attachment also needs each group's maker margin and inverse-common action
@@ -2727,14 +2772,14 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
       fail(int32_t(code), "generic_jla_leverage", std::string(what) + " at unit " + std::to_string(g));
     }
     if (!e.unit_sums.p) e.unit_sums.alloc(size_t(e.G) * 2 * (1 + QMAX));
-    k_unit_target_sums<<<L.grid, THREADS, 0, L.s>>>(e.G, q, e.unit_group_d.p, e.group_ptr.p, e.group_rows.p,
-                                                    e.row_freq.p, e.row_y.p, outcome_mean(p, o.centering),
+    k_unit_target_sums<<<L.grid, THREADS, 0, L.s>>>(e.G, qa, e.unit_group_d.p, e.group_ptr.p, e.group_rows.p,
+                                                    e.row_freq.p, e.y_work, e.y_center,
                                                     e.deleted.p, e.Rd.p, e.unit_sums.p);
     if (o.numerical) {
       numerical_status = numerical_derivative(e, o, res.numerical);
       if (e.num_block_sums.n < size_t(e.G) * (2 + 2 * QMAX)) e.num_block_sums.alloc(size_t(e.G) * (2 + 2 * QMAX));
-      k_num_block_sums<<<L.grid, THREADS, 0, L.s>>>(e.G, q, e.unit_group_d.p, e.group_ptr.p, e.group_rows.p,
-                                                    e.row_freq.p, e.row_y.p, outcome_mean(p, o.centering), e.Rd.p,
+      k_num_block_sums<<<L.grid, THREADS, 0, L.s>>>(e.G, qa, e.unit_group_d.p, e.group_ptr.p, e.group_rows.p,
+                                                    e.row_freq.p, e.y_work, e.y_center, e.Rd.p,
                                                     e.num_row_w.p, e.unit_out.p, e.num_block_sums.p);
       if (e.num_unit_fold.n < size_t(e.G) * 6) e.num_unit_fold.alloc(size_t(e.G) * 6);
       CK(cudaMemsetAsync(e.num_unit_fold.p, 0, size_t(e.G) * 6 * sizeof(double), L.s));
@@ -2744,15 +2789,15 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
   }
   auto t2 = now();
   // ---- target draws on the full model
-  run_target_blocks<K>(e, o, res, outcome_mean(p, o.centering));
+  run_target_blocks<K>(e, o, res, e.y_center);
   auto t3 = now();
   if (o.shard_phase == 2) {
     res.timings.target_ms = std::chrono::duration<double, std::milli>(t3 - t2).count();
     return;
   }
   finish_draws(res, o.probes);
-  if (o.numerical) numerical_finish<K>(e, plan, o, outcome_mean(p, o.centering), numerical_status, res);
-  if (o.projection) run_projection(e, p, o, outcome_mean(p, o.centering), res);
+  if (o.numerical) numerical_finish<K>(e, plan, o, e.y_center, numerical_status, res);
+  if (o.projection) run_projection(e, p, o, e.y_center, res);
   for (auto& r : res.receipts) {
     res.max_reduced_residual = std::max(res.max_reduced_residual, r.reduced_residual);
     res.max_complete_residual = std::max(res.max_complete_residual, r.complete_residual);

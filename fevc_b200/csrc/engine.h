@@ -56,6 +56,11 @@ struct SolveOptions {
   // JLA only): its columns are solved on the working model after the target
   // phase and their KSS covariance streamed over the deletion units.
   const PreparedProjection* projection = nullptr;
+  // Fixed-offset nuisance (generic engine with controls): the controls'
+  // coefficients of the joint fit are held fixed and everything after the
+  // fit runs on the worker-firm model with y - Q'beta (reference
+  // NuisanceMode::FixedOffset, generic_jla.rs:2011-2046)
+  bool fixed_offset = false;
 };
 
 // One receipt per solved right-hand side (reference `JlaRhsReceipt`,

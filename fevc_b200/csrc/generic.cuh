@@ -110,6 +110,41 @@ __global__ void k_row_residual(uint32_t rows, int q, const uint32_t* __restrict_
   }
 }
 
+// Fixed-offset nuisance (reference generic_jla.rs:2011-2046): the working
+// outcome y - Q'beta of every row with the full fit's control coefficients,
+// summed as the reference sums it (compensated, y first, then each -Q_k beta_k).
+__global__ void k_offset_outcome(uint32_t rows, int q, const double* __restrict__ y, const double* __restrict__ Q,
+                                 SmallMatrix beta, double* __restrict__ out) {
+  for (size_t r = size_t(blockIdx.x) * blockDim.x + threadIdx.x; r < rows; r += size_t(gridDim.x) * blockDim.x) {
+    StableSumD s;
+    s.add(y[r]);
+    for (int k = 0; k < q; ++k) s.add(-Q[r * q + k] * beta.m[k]);
+    out[r] = s.finish();
+  }
+}
+
+// Per cell sum of f * v over its rows (the FE fit's right-hand side).
+__global__ void k_cell_row_sums(uint32_t cells, const uint32_t* __restrict__ cell_ptr,
+                                const uint32_t* __restrict__ cell_rows, const double* __restrict__ row_freq,
+                                const double* __restrict__ v, double* __restrict__ out) {
+  for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < cells; c += size_t(gridDim.x) * blockDim.x) {
+    double acc = 0.0;
+    for (uint32_t i = cell_ptr[c]; i < cell_ptr[c + 1]; ++i) acc += row_freq[cell_rows[i]] * v[cell_rows[i]];
+    out[c] = acc;
+  }
+}
+
+// Sum over rows of (v - anchor) * f / total, per block (the reference's
+// `centering::mean` without its anchor, centering.rs:6-30).
+__global__ void k_centered_mass(uint32_t rows, const double* __restrict__ v, const double* __restrict__ row_freq,
+                                double inv_total, double* __restrict__ partial) {
+  double acc[1][1] = {{0.0}};
+  const double anchor = v[0];
+  for (size_t r = size_t(blockIdx.x) * blockDim.x + threadIdx.x; r < rows; r += size_t(gridDim.x) * blockDim.x)
+    acc[0][0] += (v[r] - anchor) * (row_freq[r] * inv_total);
+  block_reduce_cols<1, 1>(acc, partial);
+}
+
 struct GenericAdjustParams {
   uint32_t units;
   int q;

@@ -694,11 +694,79 @@ def write_projection_cases(lib, meta: dict) -> None:
                                                            indent=1))
 
 
+# The plugin's generic engine under the fixed-offset nuisance (nuisance_mode
+# 2: the joint fit's control coefficients held fixed, the estimator on the
+# worker-firm model of y - Q'beta): point solves through V5 at 1e-12 on the
+# diagonal route, the numerical attachment, and a projection.
+FIXED_OFFSET_CASES = {
+    "controls_2k": dict(panel="controls_2k", deletion=1, centering=0, probes=16),
+    "controls_2k_mean": dict(panel="controls_2k", deletion=1, centering=1, probes=16),
+    "controls_weighted_1500": dict(panel="controls_weighted_1500", deletion=1, centering=0, probes=12),
+    "controls_6p_4k": dict(panel="controls_6p_4k", deletion=1, centering=0, probes=12),
+    "obs_controls_2k": dict(panel="obs_controls_2k", deletion=2, centering=0, probes=16),
+    "obs_controls_2k_mean": dict(panel="obs_controls_2k", deletion=2, centering=1, probes=16),
+    "obs_controls_duplicates_1500": dict(panel="obs_controls_duplicates_1500", deletion=2, centering=0, probes=12),
+}
+
+
+def fixed_offset_record(lib, spec: dict) -> dict:
+    panel = projection_panel(spec["panel"])
+    q_count = len(panel.controls)
+    out = {"panel_sha256": panel_digest(panel), "pcg_tolerance": 1e-12, **spec}
+    e = abi.Engine(lib)
+    e.prepare(panel, deletion_mode=spec["deletion"])
+    if spec["centering"]:
+        e.centering(spec["centering"])
+    q = projection_request(e, spec["probes"], spec["deletion"], q_count)
+    q.v4.v3.v2.nuisance_mode = 2
+    e.solve_v5(q, controls_count=q_count)
+    out.update({k: list(v) for k, v in e.result().items()})
+    e.release()
+    # the numerical attachment under the same nuisance
+    e = abi.Engine(lib)
+    e.prepare(panel, deletion_mode=spec["deletion"])
+    if spec["centering"]:
+        e.centering(spec["centering"])
+    req = numerical_request(e, spec["probes"], 2, spec["deletion"], q_count)
+    req.point.v3.v2.nuisance_mode = 2
+    req.point.v3.request_signature = abi.capability_signature_v3(req.point, q_count)
+    e.solve_numerical(req)
+    r = e.numerical_result()
+    e.release()
+    out["numerical"] = {k: r[k] for k in ("status", "engine", "mcse", "raw", "usable", "psd_adjustment",
+                                          "minimum_constrained", "minimum_residual_margin",
+                                          "maximum_sensitivity_ratio")}
+    # a projection on the worker effect (two covariates)
+    e = abi.Engine(lib)
+    e.prepare(panel, deletion_mode=spec["deletion"])
+    if spec["centering"]:
+        e.centering(spec["centering"])
+    e.augment_projection(projection_covariates(panel, e.retained_mask(panel.rows), 2, 20261204))
+    q = projection_request(e, spec["probes"], spec["deletion"], q_count)
+    q.v4.v3.v2.nuisance_mode = 2
+    e.solve_v5(q, controls_count=q_count)
+    res = e.projection_result()
+    e.release()
+    out["projection"] = {"coefficients": res["coefficients"], "covariance": res["covariance"],
+                         "naive_covariance": res["naive_covariance"],
+                         "proxy": [res["receipt"]["proxy_minimum"], res["receipt"]["proxy_maximum"]]}
+    return out
+
+
+def write_fixed_offset_cases(lib, meta: dict) -> None:
+    cases = {}
+    for name, spec in FIXED_OFFSET_CASES.items():
+        cases[name] = fixed_offset_record(lib, spec)
+        print(name, cases[name]["corrected"], cases[name]["numerical"]["status"])
+    (HERE / "fixed_offset_cases.json").write_text(json.dumps({"meta": meta, "cases": cases}, indent=1))
+
+
 def main() -> None:
     """All fixtures; with the argument ``cmg`` only cmg_cases.json, with
     ``receipts`` only receipt_cases.json, with ``sized`` only sized_cases.json, with
     ``exact`` only exact_cases.json, with ``numerical`` only numerical_cases.json, with
-    ``projection`` only projection_cases.json."""
+    ``projection`` only projection_cases.json, with ``fixed_offset`` only
+    fixed_offset_cases.json."""
     if not PLUGIN.exists():
         raise SystemExit(f"reference plugin not found at {PLUGIN}")
     lib = abi.load(PLUGIN, bind_extensions=False)
@@ -713,6 +781,10 @@ def main() -> None:
     if sys.argv[1:] == ["numerical"]:
         write_numerical_cases(lib, {"generator": "tests/golden/make_golden.py numerical",
                                     "reference_plugin_version": lib.vckss_rust_backend_version().decode()})
+        return
+    if sys.argv[1:] == ["fixed_offset"]:
+        write_fixed_offset_cases(lib, {"generator": "tests/golden/make_golden.py fixed_offset",
+                                       "reference_plugin_version": lib.vckss_rust_backend_version().decode()})
         return
     if sys.argv[1:] == ["projection"]:
         write_projection_cases(lib, {"generator": "tests/golden/make_golden.py projection",
