@@ -226,29 +226,41 @@ PreparedProjection prepare_projection(const Compressed& p, const std::vector<std
   const size_t W = p.workers, F = p.firms;
   const size_t levels = effect == ProjectionEffect::Worker ? W : F - 1;
   // Gram of (1, project...) under the row masses and the per-level cross sums
-  // (projection.rs:152-191), in row order
-  std::vector<StableSum> gram(cols * cols), cross(levels * cols);
-  std::vector<double> v(cols);
+  // (projection.rs:152-191).  Every entry is its own compensated sum in row
+  // order, exactly as the reference adds it; the entries (and the cross
+  // sums' columns) are independent, so they run in parallel.
+  auto mass_of = [&](size_t r) {
+    return weight == ProjectionWeight::Frequency ? double(p.frequency[r]) : p.target[r];
+  };
+  auto value = [&](size_t k, size_t r) { return k == 0 ? 1.0 : project[k - 1][r]; };
   for (size_t r = 0; r < rows; ++r) {
-    v[0] = 1.0;
-    for (size_t k = 0; k + 1 < cols; ++k) v[k + 1] = project[k][r];
-    const double mass = weight == ProjectionWeight::Frequency ? double(p.frequency[r]) : p.target[r];
+    const double mass = mass_of(r);
     if (!std::isfinite(mass) || mass < 0.0)
       fail(INVALID_TARGET_WEIGHT, "projection_prepare", "projection mass is negative or nonfinite");
-    for (size_t a = 0; a < cols; ++a)
-      for (size_t b = 0; b < cols; ++b) gram[a * cols + b].add(mass * v[a] * v[b]);
-    size_t level;
-    if (effect == ProjectionEffect::Worker) {
-      level = p.row_worker[r];
-    } else {
-      level = p.row_firm[r];
-      if (level == F - 1) continue;  // the grounded last firm
-    }
-    for (size_t c = 0; c < cols; ++c) cross[level * cols + c].add(mass * v[c]);
   }
   std::vector<double> g(cols * cols), x(levels * cols);
-  for (size_t i = 0; i < g.size(); ++i) g[i] = gram[i].finish();
-  for (size_t i = 0; i < x.size(); ++i) x[i] = cross[i].finish();
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long long e = 0; e < (long long)(cols * cols); ++e) {
+    const size_t a = size_t(e) / cols, b = size_t(e) % cols;
+    StableSum sum;
+    for (size_t r = 0; r < rows; ++r) sum.add(mass_of(r) * value(a, r) * value(b, r));
+    g[size_t(e)] = sum.finish();
+  }
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long long c = 0; c < (long long)cols; ++c) {
+    std::vector<StableSum> cross(levels);
+    for (size_t r = 0; r < rows; ++r) {
+      size_t level;
+      if (effect == ProjectionEffect::Worker) {
+        level = p.row_worker[r];
+      } else {
+        level = p.row_firm[r];
+        if (level == F - 1) continue;  // the grounded last firm
+      }
+      cross[level].add(mass_of(r) * value(size_t(c), r));
+    }
+    for (size_t l = 0; l < levels; ++l) x[l * cols + size_t(c)] = cross[l].finish();
+  }
   const DenseInverse inv = dense_invert_scaled_spd(g, cols, rank_tolerance, "projection_gram");
   PreparedProjection out;
   out.effect = effect;
@@ -256,7 +268,9 @@ PreparedProjection prepare_projection(const Compressed& p, const std::vector<std
   out.columns = uint32_t(cols);
   out.worker_rhs.assign(W * cols, 0.0);
   out.firm_rhs.assign(F * cols, 0.0);
-  for (size_t c = 0; c < cols; ++c) {
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long long cc = 0; cc < (long long)cols; ++cc) {
+    const size_t c = size_t(cc);
     StableSum grounded;
     for (size_t l = 0; l < levels; ++l) {
       StableSum s;
