@@ -500,42 +500,20 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     // leave-observation-out every row is a unit, keyed by its class rank and
     // the number of its first copy inside the class
     if (plan.observation) {
+      // the row-keyed arrays go up; the unit (cell-order) arrays and the
+      // copy prefix are derived from them on the device after the uploads
       e->observation = true;
       size_t R = p.rows();
       e->G = uint32_t(R);
-      std::vector<uint32_t> uptr(p.cells + 1, 0);
-      for (size_t r = 0; r < R; ++r) uptr[p.row_cell[r] + 1]++;
-      for (size_t c = 0; c < p.cells; ++c) uptr[c + 1] += uptr[c];
-      std::vector<uint32_t> cur(uptr.begin(), uptr.end() - 1), order(R);
-      for (size_t r = 0; r < R; ++r) order[cur[p.row_cell[r]]++] = uint32_t(r);
-      std::vector<uint64_t> phys(R + 1, 0);
-      for (size_t r = 0; r < R; ++r) phys[r + 1] = phys[r] + p.frequency[r];
-      e->physical = phys[R];
-      upload(e->unit_ptr, uptr, s, h2d);
-      // unit arrays written straight into pinned staging blocks
+      e->physical = p.physical_total;
+      upload(e->row_rank_d, plan.row_rank, s, h2d);
+      upload(e->row_copy_offset, plan.row_copy_offset, s, h2d);
+      e->unit_ptr.alloc(p.cells + 1);
       e->unit_rank.alloc(R);
       e->unit_count.alloc(R);
       e->unit_offset.alloc(R);
-      upload_fill(e->unit_rank, 0, R, [&](uint64_t* d) {
-#pragma omp parallel for schedule(static) if (R >= 65536)
-        for (size_t i = 0; i < R; ++i) d[i] = plan.row_rank[order[i]];
-      }, s, h2d);
-      upload_fill(e->unit_count, 0, R, [&](uint64_t* d) {
-#pragma omp parallel for schedule(static) if (R >= 65536)
-        for (size_t i = 0; i < R; ++i) d[i] = p.frequency[order[i]];
-      }, s, h2d);
-      upload_fill(e->unit_offset, 0, R, [&](uint64_t* d) {
-#pragma omp parallel for schedule(static) if (R >= 65536)
-        for (size_t i = 0; i < R; ++i) d[i] = plan.row_copy_offset[order[i]];
-      }, s, h2d);
       e->unit_phys.alloc(R);
-      upload_fill(e->unit_phys, 0, R, [&](uint64_t* d) {
-#pragma omp parallel for schedule(static) if (R >= 65536)
-        for (size_t i = 0; i < R; ++i) d[i] = phys[order[i]];
-      }, s, h2d);
-      upload(e->row_rank_d, plan.row_rank, s, h2d);
-      upload(e->row_copy_offset, plan.row_copy_offset, s, h2d);
-      upload(e->row_phys, phys, s, h2d);
+      e->row_phys.alloc(R + 1);
       e->obs_row_acc.alloc(R * 4);
       e->obs_copy_acc.alloc(size_t(e->physical) * 4);
       e->control_lev.alloc(R);
@@ -627,8 +605,10 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   };
   auto groups_task = [&] {  // match groups (rows by semantic rank) and work buffers
     uint64_t& h2d = task_h2d[5];
-    upload(e->group_ptr, plan.group_ptr, s, h2d);
-    upload(e->group_rows, plan.group_rows, s, h2d);
+    if (!plan.observation) {  // leave-observation-out reads its units by cell
+      upload(e->group_ptr, plan.group_ptr, s, h2d);
+      upload(e->group_rows, plan.group_rows, s, h2d);
+    }
     e->alphaH.alloc(size_t(e->W) * QMAX);
     e->psiH.alloc(size_t(e->F) * QMAX);
     e->beta_buf.alloc(QMAX * 128);
@@ -669,6 +649,23 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   HostStager stager;
   run_parallel(tasks, &stager);
   for (uint64_t b : task_h2d) e->stats.h2d_bytes += b;
+  if (plan.observation) {
+    // units of leave-observation-out are the rows in cell order (the cell
+    // rows' stable counting sort): their class rank, copy count, first copy
+    // number and first physical copy, gathered from the row arrays; the
+    // physical-copy prefix is a scan of the frequencies
+    const size_t R = p.rows();
+    CK(cudaMemcpyAsync(e->unit_ptr.p, e->cell_rows_ptr.p, (p.cells + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                       s));
+    DBuf<uint64_t> freq(R + 1);
+    k_row_counts<<<grid_blocks(), THREADS, 0, s>>>(uint32_t(R), e->row_freq.p, freq.p);
+    device_exclusive_sum(freq.p, e->row_phys.p, R + 1, s);
+    k_obs_units<<<grid_blocks(), THREADS, 0, s>>>(uint32_t(R), e->cell_rows.p, e->row_rank_d.p, e->row_copy_offset.p,
+                                                 freq.p, e->row_phys.p, e->unit_rank.p, e->unit_count.p,
+                                                 e->unit_offset.p, e->unit_phys.p);
+    CK_LAUNCH();
+    CK(cudaStreamSynchronize(s));  // the frequency scratch is released on return
+  }
   // hybrid Laplacian, assembled on the device from the uploaded cells
   {
     DeviceHybrid h;

@@ -334,6 +334,31 @@ struct ObservationAdjustParams {
   double probes, block_tolerance, rank_tolerance;
 };
 
+// Copy counts of the rows as integers (exact: frequencies are integers below
+// 2^53), with a zero after the last row so an exclusive scan of R + 1 values
+// ends in the physical total.
+__global__ void k_row_counts(uint32_t rows, const double* __restrict__ row_freq, uint64_t* __restrict__ out) {
+  for (size_t r = size_t(blockIdx.x) * blockDim.x + threadIdx.x; r <= rows; r += size_t(gridDim.x) * blockDim.x)
+    out[r] = r < rows ? uint64_t(row_freq[r]) : 0;
+}
+
+// Leave-observation-out units in cell order: unit i is row order[i] (the
+// cell rows' stable counting sort); its class rank, copy count, first copy
+// number inside the class and first physical copy.
+__global__ void k_obs_units(uint32_t rows, const uint32_t* __restrict__ order, const uint64_t* __restrict__ row_rank,
+                            const uint64_t* __restrict__ row_copy_offset, const uint64_t* __restrict__ row_count,
+                            const uint64_t* __restrict__ row_phys, uint64_t* __restrict__ unit_rank,
+                            uint64_t* __restrict__ unit_count, uint64_t* __restrict__ unit_offset,
+                            uint64_t* __restrict__ unit_phys) {
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < rows; i += size_t(gridDim.x) * blockDim.x) {
+    const uint32_t r = order[i];
+    unit_rank[i] = row_rank[r];
+    unit_count[i] = row_count[r];
+    unit_offset[i] = row_copy_offset[r];
+    unit_phys[i] = row_phys[r];
+  }
+}
+
 // Deleted residual of every row: the mean over its copies of the
 // finite-projection inverse 1/t + bias/t^2 - var/t^3, t = residual share -
 // control leverage, times the row's full-fit residual (reference
