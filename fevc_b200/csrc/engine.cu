@@ -231,6 +231,15 @@ static int grid_blocks() {
 
 struct BlockWork;  // per-K workspace (defined below)
 
+// Per-column outcome of one blocked solve.
+struct BlockOutcome {
+  std::vector<int> iters;
+  std::vector<double> reduced, complete;
+  std::vector<int> zero;
+  int block_iterations = 0;
+};
+
+
 struct DeviceEngine {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -321,6 +330,10 @@ struct DeviceEngine {
   DBuf<unsigned long long> proj_keys;
   const PreparedProjection* proj_loaded = nullptr;
   std::vector<double> proj_coef;
+  // the autotuner's solve of the first leverage block with the chosen form,
+  // taken over by the leverage loop of the same solve (width 0: none)
+  BlockOutcome tuned_block;
+  int tuned_block_width = 0;
   // the outcome every phase after the fit works on (y, or y - Q'beta under
   // the fixed-offset nuisance), its centre, and the controls still active
   DBuf<double> row_yw, cell_yw;
@@ -1377,13 +1390,6 @@ void firm_gather(DeviceEngine& e, BlockWork& w, Launch L, const double* coef, co
   CK_LAUNCH();
 }
 
-struct BlockOutcome {
-  std::vector<int> iters;
-  std::vector<double> reduced, complete;
-  std::vector<int> zero;
-  int block_iterations = 0;
-};
-
 // Solve the K right-hand sides held in w.bW / w.bF (columns >= ncols are zero).
 // On return w.alpha holds the worker solution and w.x[0, F) the firm solution.
 template <int K>
@@ -1555,10 +1561,13 @@ void leverage_rhs(DeviceEngine& e, BlockWork& w, Launch L, PhiloxKey key, uint32
 // preconditioner 3, uniform with 4) in the single-kernel PCG.  Every form
 // meets the same FP64 tolerance, so only time decides; the fastest serves
 // every later block and resolve of the generation.  The timing solves are
-// extra work of the first solve only, and they leave no state behind (the
-// leverage loop rebuilds its right-hand sides).
+// extra work of the first solve only.  With keep_block, a winning last
+// candidate leaves its solve of the first leverage block in the block
+// workspace (right-hand sides, atoms' sign words and solution, exactly what
+// the leverage loop would recompute) for the loop to take over, its counts
+// added to tm.
 template <int K>
-void autotune(DeviceEngine& e, SolveOptions& o) {
+void autotune(DeviceEngine& e, SolveOptions& o, SolveTimings* tm = nullptr) {
   if (e.tuned < 0) {
     const int poly = (e.preconditioner == 3 || e.preconditioner == 4) && e.flex_ws.p ? e.preconditioner : 0;
     int nc = 0;
@@ -1580,14 +1589,16 @@ void autotune(DeviceEngine& e, SolveOptions& o) {
       Launch L{grid_blocks(), e.stream};
       const PhiloxKey key = philox_key(o.seed);
       int best = 0;
+      SolveTimings scratch;
+      BlockOutcome last;
       for (int c = 0; c < nc; ++c) {
         leverage_rhs<K>(e, w, L, key, 0, K);
         SolveOptions oc = o;
         oc.precision = e.tune_precision[c];
         e.preconditioner = e.tune_preconditioner[c];
-        SolveTimings scratch;
+        scratch = SolveTimings{};
         CK(cudaEventRecord(e.ev0, L.s));
-        solve_block<K>(e, w, K, oc, scratch);
+        last = solve_block<K>(e, w, K, oc, scratch);
         CK(cudaEventRecord(e.ev1, L.s));
         CK(cudaEventSynchronize(e.ev1));
         float ms = 0.0f;
@@ -1596,6 +1607,16 @@ void autotune(DeviceEngine& e, SolveOptions& o) {
         if (e.tune_ms[c] < e.tune_ms[best]) best = c;
       }
       e.tuned = best;
+      if (tm && best == nc - 1 && o.probe_begin == 0) {
+        e.tuned_block = std::move(last);
+        e.tuned_block_width = K;
+        tm->pcg_iterations += scratch.pcg_iterations;
+        tm->column_iterations += scratch.column_iterations;
+        tm->rhs_columns += scratch.rhs_columns;
+        tm->spmm_launches += scratch.spmm_launches;
+        tm->spmm_ms += scratch.spmm_ms;
+        tm->fallbacks += scratch.fallbacks;
+      }
     }
   }
   o.precision = e.tune_precision[e.tuned];
@@ -1611,8 +1632,14 @@ void run_leverage(DeviceEngine& e, const SolveOptions& o, SolveResult& res, uint
   const uint32_t end = o.probe_end ? o.probe_end : o.probes;
   for (uint32_t first = o.probe_begin; first < end; first += K) {
     int ncols = int(std::min<uint32_t>(K, end - first));
-    leverage_rhs<K>(e, w, L, key, first, ncols);
-    BlockOutcome bo = solve_block<K>(e, w, ncols, o, res.timings);
+    BlockOutcome bo;
+    if (first == 0 && ncols == K && e.tuned_block_width == K) {
+      bo = std::move(e.tuned_block);  // the autotuner's solve of this block with the chosen form
+    } else {
+      leverage_rhs<K>(e, w, L, key, first, ncols);
+      bo = solve_block<K>(e, w, ncols, o, res.timings);
+    }
+    e.tuned_block_width = 0;
     if (e.observation && shared_signs(e, first))
       k_obs_moments_cells<K><<<L.grid, THREADS, 0, L.s>>>(e.C, ncols, e.unit_ptr.p, e.cell_rows.p, e.cell_worker.p,
                                                           e.cell_firm.p, e.unit_phys.p, e.unit_count.p,
@@ -2301,11 +2328,12 @@ void run_jla(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, const So
     return;
   }
   // ---- leverage
-  if (o.precision == 2) autotune<K>(e, o);
+  if (o.precision == 2) autotune<K>(e, o, o.shard_phase != 2 ? &res.timings : nullptr);
   if (o.shard_phase != 2) {
     CK(cudaMemsetAsync(e.moments.p, 0, e.moments.bytes(), L.s));
     run_leverage_blocks<K>(e, o, res);
   }
+  e.tuned_block_width = 0;
   if (o.shard_phase == 1) {
     shard_download(e, o, res);
     res.timings.fit_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
@@ -2668,7 +2696,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
   auto t1 = now();
   // ---- FE-only leverage probes (reference `match_leverage_moments`,
   // `observation_and_match_leverage_moments`)
-  if (o.precision == 2) autotune<K>(e, o);
+  if (o.precision == 2) autotune<K>(e, o, o.shard_phase != 2 ? &res.timings : nullptr);
   if (o.shard_phase != 2) {
     if (e.observation) {
       CK(cudaMemsetAsync(e.obs_row_acc.p, 0, e.obs_row_acc.bytes(), L.s));
@@ -2678,6 +2706,7 @@ void run_generic(DeviceEngine& e, const Compressed& p, const JlaPlan& plan, cons
     }
     run_leverage_blocks<K>(e, o, res);
   }
+  e.tuned_block_width = 0;
   if (o.shard_phase == 1) {
     shard_download(e, o, res);
     res.timings.fit_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();

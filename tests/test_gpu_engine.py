@@ -356,7 +356,8 @@ def test_device_hybrid_assembly_with_star_workers(lib):
 def test_autotuner_keeps_a_timed_form_with_the_same_components(lib):
     """Precision option 2 times FP64 Jacobi, FP32 Jacobi and the FP32
     degree-1 stage on the first leverage block, keeps the fastest for the
-    generation (its resolves included), and gives the FP64 components."""
+    generation (its resolves included), and gives the FP64 components; the
+    first solve equals its resolve bit for bit."""
     from fevc_b200.panel import generate_panel
 
     panel = generate_panel(30_000, 1_500, 5, seed=123)
@@ -366,9 +367,14 @@ def test_autotuner_keeps_a_timed_form_with_the_same_components(lib):
     e = solve_precision(lib, panel, probes=64, precision=2, tol=1e-10, precond=4)
     got = e.result()
     t = e.tuning()
+    counted = e.timings()["rhs_columns"]
     e.resolve()
     again = e.result()
     assert t == e.tuning()  # the choice is kept for the generation
+    # the leverage loop takes over the winning candidate's solve of the first
+    # block: the counts and the result equal a resolve's, which solves it anew
+    assert e.timings()["rhs_columns"] == counted
+    assert again == got
     e.release()
     assert t["chosen"] in range(len(t["candidates"])) and len(t["candidates"]) == 3
     assert all(c["ms"] > 0 for c in t["candidates"])
