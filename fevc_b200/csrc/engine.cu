@@ -713,8 +713,21 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
                                                               e->flex_wa.p, e->flex_ws.p);
       CK_LAUNCH();
     }
-    if (e->preconditioner == 2 || e->preconditioner == 3) {
-      // the CMG hierarchy and the network features are built on the host
+    if (e->preconditioner == 3) {
+      // the network's features and inference on the device Laplacian
+      std::vector<float> params = learned_params();
+      if (params.empty())
+        fail(UNSUPPORTED_FEATURE, "learned_preconditioner", "no network parameters are installed");
+      e->learned = build_learned_device(params, e->n, nnz, e->L_ptr.p, e->L_col.p, e->L_val.p, e->L_diag.p, s,
+                                        e->stats.h2d_bytes);
+      e->flex_wa.alloc(e->n);
+      e->flex_ws.alloc(e->n);
+      k_flex_learned_weights<<<grid_blocks(), THREADS, 0, s>>>(e->n, e->L_diag.p, e->learned->weights(),
+                                                              e->flex_wa.p, e->flex_ws.p);
+      CK_LAUNCH();
+    }
+    if (e->preconditioner == 2) {
+      // the CMG hierarchy is built on the host
       std::vector<uint32_t> Lptr(e->n + 1), Lcol(nnz);
       std::vector<double> Lval(nnz), Ld(e->n);
       CK(cudaMemcpyAsync(Lptr.data(), e->L_ptr.p, Lptr.size() * 4, cudaMemcpyDeviceToHost, s));
@@ -723,21 +736,9 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
       CK(cudaMemcpyAsync(Ld.data(), e->L_diag.p, e->n * 8, cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
       uint64_t& h2d = e->stats.h2d_bytes;
-      if (e->preconditioner == 2) {
-        e->mg = build_multigrid(e->n, Lptr, Lcol, Lval, Ld, s, h2d);
-        e->stats.levels = e->mg->levels();
-        e->stats.terminal_vertices = e->mg->report().vertices.back();
-      } else {
-        std::vector<float> params = learned_params();
-        if (params.empty())
-          fail(UNSUPPORTED_FEATURE, "learned_preconditioner", "no network parameters are installed");
-        e->learned = build_learned(params, e->n, Lptr, Lcol, Lval, Ld, s, h2d);
-        e->flex_wa.alloc(e->n);
-        e->flex_ws.alloc(e->n);
-        k_flex_learned_weights<<<grid_blocks(), THREADS, 0, s>>>(e->n, e->L_diag.p, e->learned->weights(),
-                                                                e->flex_wa.p, e->flex_ws.p);
-        CK_LAUNCH();
-      }
+      e->mg = build_multigrid(e->n, Lptr, Lcol, Lval, Ld, s, h2d);
+      e->stats.levels = e->mg->levels();
+      e->stats.terminal_vertices = e->mg->report().vertices.back();
     }
     if (e->flex_ws.p) {
       e->flex_valw.alloc(nnz);

@@ -467,6 +467,86 @@ void forward(GraphData& g, DeviceParams& p, cudaStream_t s) {
   CK_LAUNCH();
 }
 
+// Vertex features on the device (the same eight as gnn_features): per-block
+// sums of (log d, log1p(count)), then of (log d - mean)^2, each finished by
+// one thread in block order, then one thread per vertex.
+constexpr int FEAT_THREADS = 256;
+
+__global__ void k_feat_sums(uint32_t n, const uint32_t* __restrict__ ptr, const double* __restrict__ diag,
+                            const double* __restrict__ mean, double* __restrict__ partial) {
+  __shared__ double sa[FEAT_THREADS], sb[FEAT_THREADS];
+  double a = 0.0, b = 0.0;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const double ld = log(fmax(diag[v], 1e-300));
+    if (mean) {
+      const double t = ld - mean[0];
+      a += t * t;
+    } else {
+      a += ld;
+      b += log1p(double(ptr[v + 1] - ptr[v]));
+    }
+  }
+  sa[threadIdx.x] = a;
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = FEAT_THREADS / 2; w > 0; w >>= 1) {
+    if (int(threadIdx.x) < w) {
+      sa[threadIdx.x] += sa[threadIdx.x + w];
+      sb[threadIdx.x] += sb[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = sa[0];
+    partial[2 * blockIdx.x + 1] = sb[0];
+  }
+}
+
+// stats[0] mean log d, stats[1] mean log1p(count) (pass 0); stats[2] the
+// standard deviation of log d plus 1e-12 (pass 1)
+__global__ void k_feat_finish(int blocks, uint32_t n, int pass, const double* __restrict__ partial,
+                              double* __restrict__ stats) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double a = 0.0, b = 0.0;
+  for (int i = 0; i < blocks; ++i) {
+    a += partial[2 * i];
+    b += partial[2 * i + 1];
+  }
+  const double nn = double(n > 0 ? n : 1);
+  if (pass == 0) {
+    stats[0] = a / nn;
+    stats[1] = b / nn;
+  } else {
+    stats[2] = sqrt(a / nn) + 1e-12;
+  }
+}
+
+__global__ void k_feat_vertices(uint32_t n, const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
+                                const double* __restrict__ val, const double* __restrict__ diag,
+                                const double* __restrict__ stats, float* __restrict__ X) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const double d = fmax(diag[v], 1e-300), ld = log(d);
+    double wmax = 0.0, sq = 0.0, nb = 0.0, inflow = 0.0;
+    for (uint32_t e = ptr[v]; e < ptr[v + 1]; ++e) {
+      const double a = val[e] / d, dc = fmax(diag[col[e]], 1e-300);
+      wmax = fmax(wmax, a);
+      sq += a * a;
+      nb += a * (log(dc) - ld);
+      inflow += val[e] / dc;
+    }
+    const double cnt = double(ptr[v + 1] - ptr[v]);
+    float* x = X + size_t(v) * GNN_FEATURES;
+    x[0] = float((ld - stats[0]) / stats[2]);
+    x[1] = float(log1p(cnt) - stats[1]);
+    x[2] = float(wmax);
+    x[3] = float(nb);
+    x[4] = float(sq);
+    x[5] = float(log(fmax(inflow, 1e-12)));
+    x[6] = float(1.0 / sqrt(1.0 + cnt));
+    x[7] = 1.0f;
+  }
+}
+
 class VertexWeights final : public LearnedPreconditioner {
  public:
   GraphData g;
@@ -475,25 +555,50 @@ class VertexWeights final : public LearnedPreconditioner {
 
 }  // namespace
 
-std::unique_ptr<LearnedPreconditioner> build_learned(const std::vector<float>& params, uint32_t n,
-                                                     const std::vector<uint32_t>& ptr,
-                                                     const std::vector<uint32_t>& col,
-                                                     const std::vector<double>& val,
-                                                     const std::vector<double>& diag, cudaStream_t s, uint64_t& h2d) {
+
+std::unique_ptr<LearnedPreconditioner> build_learned_device(const std::vector<float>& params, uint32_t n,
+                                                            size_t nnz, const uint32_t* ptr, const uint32_t* col,
+                                                            const double* val, const double* diag, cudaStream_t s,
+                                                            uint64_t& h2d) {
   if (params.size() != gnn_param_count())
     fail(INVALID_INPUT, "learned_preconditioner", "network parameters have the wrong length");
   auto pc = std::make_unique<VertexWeights>();
-  upload_graph(pc->g, n, ptr, col, val, diag, s, h2d);
+  GraphData& g = pc->g;
+  g.n = n;
+  g.ptr.alloc(size_t(n) + 1);
+  g.col.alloc(nnz);
+  g.val.alloc(nnz);
+  g.diag.alloc(n);
+  CK(cudaMemcpyAsync(g.ptr.p, ptr, (size_t(n) + 1) * 4, cudaMemcpyDeviceToDevice, s));
+  if (nnz) {
+    CK(cudaMemcpyAsync(g.col.p, col, nnz * 4, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(g.val.p, val, nnz * 8, cudaMemcpyDeviceToDevice, s));
+  }
+  CK(cudaMemcpyAsync(g.diag.p, diag, size_t(n) * 8, cudaMemcpyDeviceToDevice, s));
+  g.X.alloc(size_t(n) * GNN_FEATURES);
+  const int blocks = gnn_blocks(n);
+  DBuf<double> partial(size_t(2) * blocks), stats(4);
+  k_feat_sums<<<blocks, FEAT_THREADS, 0, s>>>(n, g.ptr.p, g.diag.p, nullptr, partial.p);
+  k_feat_finish<<<1, 32, 0, s>>>(blocks, n, 0, partial.p, stats.p);
+  k_feat_sums<<<blocks, FEAT_THREADS, 0, s>>>(n, g.ptr.p, g.diag.p, stats.p, partial.p);
+  k_feat_finish<<<1, 32, 0, s>>>(blocks, n, 1, partial.p, stats.p);
+  k_feat_vertices<<<blocks, FEAT_THREADS, 0, s>>>(n, g.ptr.p, g.col.p, g.val.p, g.diag.p, stats.p, g.X.p);
+  CK_LAUNCH();
+  for (int l = 0; l < GNN_LAYERS; ++l) {
+    g.S[l].alloc(size_t(n) * layer_in(l));
+    g.H[l].alloc(size_t(n) * GNN_WIDTH);
+  }
+  g.Craw.alloc(size_t(n) * GNN_OUT);
+  g.C.alloc(size_t(n) * GNN_OUT);
   DeviceParams p;
   upload(p.master, params, s, h2d);
   p.bf.alloc(params.size());
   refresh_bf16(p, s);
-  forward(pc->g, p, s);
-  CK(cudaStreamSynchronize(s));  // the parameter buffers are released on return
-  // the activations are not needed after inference
+  forward(g, p, s);
+  CK(cudaStreamSynchronize(s));  // the scratch and parameter buffers are released on return
   for (int l = 0; l < GNN_LAYERS; ++l) {
-    pc->g.S[l].release();
-    pc->g.H[l].release();
+    g.S[l].release();
+    g.H[l].release();
   }
   return pc;
 }

@@ -54,12 +54,13 @@ class LearnedPreconditioner {
   virtual const float* weights() const = 0;  // device, n x 2: (a, s) per vertex
 };
 
-std::unique_ptr<LearnedPreconditioner> build_learned(const std::vector<float>& params, uint32_t n,
-                                                     const std::vector<uint32_t>& ptr,
-                                                     const std::vector<uint32_t>& col,
-                                                     const std::vector<double>& val,
-                                                     const std::vector<double>& diag, cudaStream_t s,
-                                                     uint64_t& h2d_bytes);
+// Inference for a Laplacian already on the device (CSR of nnz positive
+// off-diagonal conductances, degree diagonal): the gnn_features features are
+// computed on the device (no host round trip), then the network runs.
+std::unique_ptr<LearnedPreconditioner> build_learned_device(const std::vector<float>& params, uint32_t n,
+                                                            size_t nnz, const uint32_t* ptr, const uint32_t* col,
+                                                            const double* val, const double* diag, cudaStream_t s,
+                                                            uint64_t& h2d);
 
 // Training on a set of graphs.
 class GnnTrainer {
