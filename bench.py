@@ -97,6 +97,9 @@ def parse():
     ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--parity-probes", type=int, default=24)
     ap.add_argument("--sharded", action="store_true", help="use the probe-sharded path at any N (launch with torchrun)")
+    ap.add_argument("--strong", action="store_true",
+                    help="strong scaling: --probes is the whole decomposition's probe count, split over the ranks "
+                         "(default: weak scaling, --probes per rank)")
     ap.add_argument("--plain-probes", type=int, default=8)
     return ap.parse_args()
 
@@ -160,13 +163,13 @@ def deletion_mode(panel) -> int:
 def workload_config(args, panel):
     """The config dict of the JSON line; the same in both arms."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    total = args.probes * world
+    total = args.probes if args.strong else args.probes * world
     return {"workload": f"{args.workload} panel ({panel.info['workers']} workers, {panel.info['firms']} firms, "
                         f"{panel.info['periods']} periods), {total} probes, {len(panel.controls)} year controls, "
                         f"{'observation' if deletion_mode(panel) == 2 else 'match'} deletion",
             "probes": total, "rhs_per_step": 1 + 3 * total, "tolerance": args.tolerance,
             "controls": len(panel.controls),
-            "parallelism": (f"probe-sharded x{world}: {args.probes} probes per GPU, {total} in the decomposition; "
+            "parallelism": (f"probe-sharded x{world}: {total / world:g} probes per GPU, {total} in the decomposition; "
                             "NCCL all-reduce of the leverage accumulators and gather of the draws")
             if world > 1 or args.sharded else "single GPU",
             "l2": "inputs larger than L2 (the prepared problem and the 64-column blocks exceed 126 MB)"}
@@ -515,7 +518,7 @@ def run_reference(args):
     sample = reference_sample_text(r, probes, scale, cpanel).replace("{tol}", f"{args.tolerance:g}")
     line = {"metric": METRIC, "value": round(r["rhs_per_s"], 4), "unit": UNIT, "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(1000 * r["solve_s"], 2), "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": round(1000 * r["solve_s"], 2), "higher_is_better": True, "scaling": "strong" if args.strong else "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, fevc_b200/panel.py)",
             "config": workload_config(args, panel),
             "prepare_s": round(r["prepare_s"], 3),
@@ -579,9 +582,10 @@ def main():
     # N ranks: every rank contributes `probes` probes to one decomposition of
     # probes x N (weak scaling); the leverage accumulators are all-reduced and
     # the target draws gathered over NCCL (fevc_b200/sharded.py)
-    total_probes = args.probes * world
+    # (--strong: `probes` in all, split over the ranks)
+    total_probes = args.probes if args.strong else args.probes * world
     req = v5_request(e, total_probes, args.tolerance, deletion=deletion_mode(panel))
-    rhs = 1 + 3 * args.probes  # right-hand sides this rank solves per step
+    rhs = 1 + 3 * total_probes / world  # right-hand sides per rank per step (every rank solves the fit)
     use_shards = world > 1 or args.sharded
     if use_shards:
         from fevc_b200 import sharded
@@ -705,7 +709,7 @@ def main():
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 storage / f64 reductions" if eff_prec == 1 else "f64",
+            "scaling": "strong" if args.strong else "weak", "vs_baseline": None, "dtype": "f32 storage / f64 reductions" if eff_prec == 1 else "f64",
             "data": "synthetic (seeded generator, fevc_b200/panel.py)",
             "config": workload_config(args, panel),
             "form": {"name": headline, "description": form_text, "preconditioner": precond, "precision": precision,
