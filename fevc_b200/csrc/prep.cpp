@@ -317,30 +317,6 @@ ComponentResult largest_component(const Canonical& in, const std::vector<uint8_t
   return out;
 }
 
-void intersect(std::vector<uint8_t>& active, const std::vector<uint8_t>& keep) {
-  for (size_t r = 0; r < active.size(); ++r) active[r] &= keep[r];
-}
-
-// Reference `distinct_deletion_counts` (graph.rs:762-781).
-std::vector<uint64_t> distinct_deletion_counts(const Canonical& in, const std::vector<uint8_t>& active) {
-  std::vector<uint8_t> seen(in.deletion_units, 0);
-  std::vector<uint64_t> counts(in.workers, 0);
-  for (size_t r = 0; r < in.rows(); ++r) {
-    if (!active[r] || seen[in.deletion[r]]) continue;
-    seen[in.deletion[r]] = 1;
-    counts[in.worker[r]]++;
-  }
-  return counts;
-}
-
-std::vector<uint64_t> worker_physical_counts(const Canonical& in, const std::vector<uint8_t>& active) {
-  validate_mask(in, active);
-  std::vector<uint64_t> counts(in.workers, 0);
-  for (size_t r = 0; r < in.rows(); ++r)
-    if (active[r]) counts[in.worker[r]] += in.frequency[r];
-  return counts;
-}
-
 // Iterative Tarjan low-link over a CSR multigraph.  The parent arc is skipped
 // by edge identity (not by endpoint), so parallel edges count as cycles.
 // Articulation vertices and bridges are properties of the graph, independent
@@ -404,46 +380,6 @@ void tarjan(const Graph& g, std::vector<uint8_t>* articulation, std::vector<uint
     }
     if (articulation) (*articulation)[root] = root_children > 1;
   }
-}
-
-std::vector<uint8_t> worker_articulations(const Canonical& in, const std::vector<uint8_t>& active) {
-  Graph g = coordinate_graph(in, active);
-  std::vector<uint8_t> art;
-  tarjan(g, &art, nullptr);
-  art.resize(in.workers);
-  return art;
-}
-
-// Active deletion units as multigraph edges (reference `deletion_bridges`,
-// graph.rs:938-1029); returns the bridge deletion ids.
-std::vector<uint32_t> deletion_bridges(const Canonical& in, const std::vector<uint8_t>& active) {
-  validate_mask(in, active);
-  std::vector<uint32_t> cw(in.deletion_units, MISSING), cf(in.deletion_units, MISSING);
-  for (size_t r = 0; r < in.rows(); ++r) {
-    if (!active[r]) continue;
-    uint32_t d = in.deletion[r];
-    if (cw[d] == MISSING) {
-      cw[d] = in.worker[r];
-      cf[d] = in.firm[r];
-    } else if (cw[d] != in.worker[r] || cf[d] != in.firm[r]) {
-      fail(INTERNAL_INVARIANT_FAILED, "graph", "deletion unit crosses worker-firm coordinates");
-    }
-  }
-  std::vector<uint32_t> ids, eu, ev;
-  for (size_t d = 0; d < in.deletion_units; ++d)
-    if (cw[d] != MISSING) {
-      ids.push_back(uint32_t(d));
-      eu.push_back(cw[d]);
-      ev.push_back(uint32_t(in.workers + cf[d]));
-    }
-  if (ids.empty()) return {};
-  Graph g = make_graph(in.workers + in.firms, eu, ev);
-  std::vector<uint8_t> br;
-  tarjan(g, nullptr, &br);
-  std::vector<uint32_t> out;
-  for (size_t e = 0; e < ids.size(); ++e)
-    if (br[e]) out.push_back(ids[e]);
-  return out;
 }
 
 // Run independent tasks on their own threads; after all finish the first
@@ -659,17 +595,6 @@ std::vector<uint32_t> unit_bridges(const std::vector<uint8_t>& act, const UnitGr
   for (size_t d = 0; d < act.size(); ++d)
     if (act[d] && br[d]) out.push_back(uint32_t(d));
   return out;
-}
-
-size_t active_deletion_count(const Canonical& in, const std::vector<uint8_t>& active) {
-  std::vector<uint8_t> seen(in.deletion_units, 0);
-  size_t c = 0;
-  for (size_t r = 0; r < in.rows(); ++r)
-    if (active[r] && !seen[in.deletion[r]]) {
-      seen[in.deletion[r]] = 1;
-      ++c;
-    }
-  return c;
 }
 
 GroupIndex grouped_rows(size_t groups, const std::vector<uint32_t>& row_group) {
