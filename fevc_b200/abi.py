@@ -197,6 +197,11 @@ class NumericalRhsV1(Struct):
                 ("complete_residual", f64)]
 
 
+class FevcbSetupTimingsV1(Struct):
+    _fields_ = [("struct_size", u32), ("builders", u32), ("builder_ms", f64 * 16), ("builders_span_ms", f64),
+                ("device_units_ms", f64), ("hybrid_ms", f64), ("preconditioner_ms", f64), ("total_ms", f64)]
+
+
 class ProjectionAugmentationRequestV1(Struct):
     _fields_ = [("abi_version", u32), ("struct_size", u32), ("rows", u64), ("project_count", u32), ("effect", u32),
                 ("weight", u32), ("reserved", u32), ("rank_tolerance", f64), ("caller_copy_bytes", u64)]
@@ -542,6 +547,7 @@ def cmg_aggregate(lib, ptr: np.ndarray, col: np.ndarray, weight: np.ndarray, thr
 
 
 SIGNATURES = {
+    "fevcb_engine_setup_timings_v1": (i32, [u64, C.c_void_p, u32]),
     "vckss_rust_engine_augment_projection_interrupt_v1": (i32, [u64, C.c_void_p, C.c_void_p]),
     "vckss_rust_engine_default_projection_augmentation_request_interrupt_v1": (i32, [C.c_void_p, u32]),
     "vckss_rust_engine_projection_augmentation_receipt_v1": (i32, [u64, C.c_void_p, u32]),
@@ -984,6 +990,16 @@ class Engine:
         self.check(getattr(self.lib, f"vckss_rust_engine_detailed_receipt_v{version}")(
             self.generation, C.byref(out), C.sizeof(out)))
         return out
+
+    def setup_timings(self) -> dict:
+        """Wall milliseconds of the device engine's setup (builders, device
+        units, hybrid assembly, preconditioner, total)."""
+        t = FevcbSetupTimingsV1()
+        self.check(self.lib.fevcb_engine_setup_timings_v1(self.generation, C.byref(t), C.sizeof(t)))
+        d = t.as_dict()
+        names = ("cells", "units", "strata", "rows", "cell_rows", "groups") + tuple(f"control_{k}" for k in range(10))
+        d["builder_ms"] = {names[i]: round(list(t.builder_ms)[i], 2) for i in range(min(t.builders, 16))}
+        return d
 
     def timings(self) -> dict:
         t = FevcbSolveTimingsV1()

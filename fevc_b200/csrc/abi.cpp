@@ -1596,6 +1596,26 @@ int32_t fevcb_engine_prepare_timings_v1(uint64_t generation, FevcbPrepareTimings
   });
 }
 
+int32_t fevcb_engine_setup_timings_v1(uint64_t generation, FevcbSetupTimingsV1* out, uint32_t cap) {
+  return status([&] {
+    require_capacity<FevcbSetupTimingsV1>(out, cap, "setup timings");
+    std::lock_guard<std::mutex> l(reg().mu);
+    Prepared& p = reg().require(generation, "engine_setup_timings");
+    if (!p.device) fail(STALE_CONTEXT, "engine_setup_timings", "the generation has no device engine yet");
+    const DeviceStats st = device_stats(*p.device);
+    FevcbSetupTimingsV1 t{};
+    t.struct_size = sizeof(t);
+    t.builders = uint32_t(st.builders);
+    for (int i = 0; i < 16; ++i) t.builder_ms[i] = st.builder_ms[i];
+    t.builders_span_ms = st.builders_span_ms;
+    t.device_units_ms = st.device_units_ms;
+    t.hybrid_ms = st.hybrid_ms;
+    t.preconditioner_ms = st.preconditioner_ms;
+    t.total_ms = st.setup_ms;
+    *out = t;
+  });
+}
+
 int32_t fevcb_engine_exact_limit_v1(uint64_t generation, uint64_t ceiling) {
   return status([&] {
     if (ceiling > 1000000) fail(INVALID_INPUT, "engine_ffi", "exact ceiling must lie in [0, 1000000]");

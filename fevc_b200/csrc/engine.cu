@@ -478,7 +478,7 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   // They run on their own threads (bound to this device); their uploads share
   // the engine's stream and fill disjoint buffers.  The hybrid Laplacian is
   // then assembled on the device.
-  uint64_t task_h2d[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  uint64_t task_h2d[16] = {};
   (void)grid_blocks();  // initialise the cached grid size before the threads use it
   auto cells_task = [&] {
     uint64_t& h2d = task_h2d[0];
@@ -592,17 +592,15 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     }, s, h2d);
     upload(e->row_y, p.outcome, s, h2d);
   };
-  // the controls row-major (r * q + k), transposed straight into pinned
-  // blocks by two tasks over halves of the rows
-  auto controls_task = [&](int half) {
-    return [&, half] {
-      uint64_t& h2d = task_h2d[6 + half];
-      const size_t q = size_t(e->q), b = half ? R / 2 : 0, end = half ? R : R / 2;
-      upload_fill(e->Qd, b * q, (end - b) * q, [&](double* d) {
-        for (size_t k = 0; k < q; ++k) {
-          const double* col = p.controls[k].data();
-          for (size_t r = b; r < end; ++r) d[(r - b) * q + k] = col[r];
-        }
+  // the controls go up column by column (one builder per column, a plain
+  // copy into pinned staging) and are transposed to row-major (r * q + k)
+  // on the device
+  DBuf<double> qcol;
+  auto controls_task = [&](int k) {
+    return [&, k] {
+      uint64_t& h2d = task_h2d[6 + k];
+      upload_fill(qcol, size_t(k) * R, R, [&](double* d) {
+        std::memcpy(d, p.controls[size_t(k)].data(), R * sizeof(double));
       }, s, h2d);
     };
   };
@@ -654,14 +652,31 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     e->residual.alloc(R);
     e->deleted.alloc(R);
     tasks.push_back(rows_task);
-    tasks.push_back(controls_task(0));
-    tasks.push_back(controls_task(1));
     tasks.push_back(cell_rows_task);
     tasks.push_back(groups_task);
+    if (e->q > 0) qcol.alloc(R * size_t(e->q));
+    for (int k = 0; k < e->q; ++k) tasks.push_back(controls_task(k));
   }
+  auto wall_ms = [](std::chrono::steady_clock::time_point a) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
+  };
+  e->stats.builders = int(tasks.size());
+  for (size_t i = 0; i < tasks.size(); ++i)
+    tasks[i] = [&, i, f = tasks[i]] {
+      const auto b = std::chrono::steady_clock::now();
+      f();
+      e->stats.builder_ms[i] = wall_ms(b);
+    };
   HostStager stager;
+  auto tb = std::chrono::steady_clock::now();
   run_parallel(tasks, &stager);
+  e->stats.builders_span_ms = wall_ms(tb);
+  tb = std::chrono::steady_clock::now();
   for (uint64_t b : task_h2d) e->stats.h2d_bytes += b;
+  if (qcol.p) {
+    k_transpose_controls<<<grid_blocks(), THREADS, 0, s>>>(uint32_t(R), e->q, qcol.p, e->Qd.p);
+    CK_LAUNCH();
+  }
   if (plan.observation) {
     // units of leave-observation-out are the rows in cell order (the cell
     // rows' stable counting sort): their class rank, copy count, first copy
@@ -679,6 +694,8 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     CK_LAUNCH();
     CK(cudaStreamSynchronize(s));  // the frequency scratch is released on return
   }
+  e->stats.device_units_ms = wall_ms(tb);
+  tb = std::chrono::steady_clock::now();
   // hybrid Laplacian, assembled on the device from the uploaded cells
   {
     DeviceHybrid h;
@@ -700,6 +717,9 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     if (nnz)
       k_scale_by_col<<<grid_blocks(), THREADS, 0, s>>>(nnz, e->L_col.p, e->L_val.p, e->L_dinv.p, e->L_vald.p);
     CK_LAUNCH();
+    CK(cudaStreamSynchronize(s));
+    e->stats.hybrid_ms = wall_ms(tb);
+    tb = std::chrono::steady_clock::now();
     e->stats.vertices = e->n;
     e->stats.terminal_vertices = e->n;
     e->stats.edges = nnz / 2;
@@ -740,6 +760,8 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
       e->stats.levels = e->mg->levels();
       e->stats.terminal_vertices = e->mg->report().vertices.back();
     }
+    CK(cudaStreamSynchronize(s));
+    e->stats.preconditioner_ms = wall_ms(tb);
     if (e->flex_ws.p) {
       e->flex_valw.alloc(nnz);
       if (nnz)

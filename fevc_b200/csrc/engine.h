@@ -134,6 +134,11 @@ struct DeviceStats {
   uint64_t h2d_bytes = 0;
   uint64_t vertices = 0, edges = 0, kept_workers = 0, levels = 0, terminal_vertices = 0;
   double setup_ms = 0;
+  // setup phases (wall ms): the host builders (in launch order), their
+  // parallel span, device-derived units, hybrid assembly, preconditioner
+  int builders = 0;
+  double builder_ms[16] = {};
+  double builders_span_ms = 0, device_units_ms = 0, hybrid_ms = 0, preconditioner_ms = 0;
 };
 
 // Upload the prepared problem and build the solver.  Throws Error.

@@ -110,6 +110,13 @@ __global__ void k_row_residual(uint32_t rows, int q, const uint32_t* __restrict_
   }
 }
 
+// Controls uploaded column-major (k * rows + r) to row-major (r * q + k).
+__global__ void k_transpose_controls(uint32_t rows, int q, const double* __restrict__ cols, double* __restrict__ Q) {
+  const size_t total = size_t(rows) * q;
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x)
+    Q[t] = cols[(t % q) * rows + t / q];
+}
+
 // Fixed-offset nuisance (reference generic_jla.rs:2011-2046): the working
 // outcome y - Q'beta of every row with the full fit's control coefficients,
 // summed as the reference sums it (compensated, y first, then each -Q_k beta_k).

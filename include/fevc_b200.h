@@ -919,6 +919,26 @@ typedef struct FevcbPrepareTimingsV1 {
 int32_t fevcb_engine_prepare_timings_v1(uint64_t generation, FevcbPrepareTimingsV1 *output,
                                         uint32_t output_capacity_bytes);
 
+/* Wall milliseconds of the device engine's setup for the generation (built
+ * on its first solve): the host builders, each on its own thread with its
+ * uploads (cells and firm segments; deletion units; target strata; row data;
+ * the rows of every cell; match groups; then one per control column),
+ * their parallel span, the unit arrays derived on the device, the hybrid
+ * Laplacian's assembly, the preconditioner's setup, and the whole setup.
+ * Builders a plan does not use report 0.  STALE_CONTEXT before a solve. */
+typedef struct FevcbSetupTimingsV1 {
+  uint32_t struct_size;
+  uint32_t builders;
+  double builder_ms[16];
+  double builders_span_ms;
+  double device_units_ms;
+  double hybrid_ms;
+  double preconditioner_ms;
+  double total_ms;
+} FevcbSetupTimingsV1;
+int32_t fevcb_engine_setup_timings_v1(uint64_t generation, FevcbSetupTimingsV1 *output,
+                                      uint32_t output_capacity_bytes);
+
 /* Independent probe sets on one prepared generation in one call (no
  * counterpart in the reference, which draws one seed per solve): set 0 is the
  * V5 request solved with that set's seed and probe count, and its result
@@ -1714,6 +1734,7 @@ static_assert(sizeof(VckssBackendRequestCapabilityRequestV3) == 120, "V3 capabil
 static_assert(sizeof(VckssBackendRequestCapabilityReceiptV3) == 160, "V3 capability receipt layout");
 static_assert(sizeof(VckssFullCmgReceiptV1) == 400, "full-CMG receipt layout");
 static_assert(sizeof(FevcbSolveOptionsV2) == 24, "device options V2 layout");
+static_assert(sizeof(FevcbSetupTimingsV1) == 176, "setup timings layout");
 static_assert(sizeof(FevcbLearnedDumpV1) == 80, "learned dump layout");
 static_assert(sizeof(VckssEnginePrepareRequestV2) == 40, "prepare request V2 layout");
 static_assert(sizeof(VckssEnginePrepareRequestV3) == 56, "prepare request V3 layout");
