@@ -109,20 +109,44 @@ int gnn_blocks(size_t work) {
   return int(std::max<size_t>(1, std::min<size_t>(b, 148 * 16)));
 }
 
-// S[v][i] = sum_u (w_uv / d_v) H[u][i]
-__global__ void k_gnn_aggregate(uint32_t n, int in, const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
+// S[v][i] = sum_u (w_uv / d_v) H[u][i]: one warp per vertex, its lanes
+// striding the vertex's edges (hub firms hold tens of thousands), every lane
+// holding all IN sums, then a fixed shuffle tree per feature.
+template <int IN>
+__global__ void k_gnn_aggregate(uint32_t n, const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
                                 const double* __restrict__ val, const double* __restrict__ diag,
                                 const float* __restrict__ H, float* __restrict__ S) {
-  size_t total = size_t(n) * in;
-  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += size_t(gridDim.x) * blockDim.x) {
-    size_t v = t / in;
-    int i = int(t % in);
-    float inv = float(1.0 / diag[v]);
-    float acc = 0.0f;
-    for (uint32_t e = ptr[v]; e < ptr[v + 1]; ++e) acc += float(val[e]) * H[size_t(col[e]) * in + i];
-    S[t] = acc * inv;
+  static_assert(IN % 4 == 0, "rows are read as float4");
+  const int lane = threadIdx.x & 31;
+  const size_t warps = (size_t(gridDim.x) * blockDim.x) >> 5;
+  for (size_t v = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+    float acc[IN];
+#pragma unroll
+    for (int i = 0; i < IN; ++i) acc[i] = 0.0f;
+    const uint32_t end = ptr[v + 1];
+    for (uint32_t e = ptr[v] + lane; e < end; e += 32) {
+      const float w = float(val[e]);
+      const float4* h = reinterpret_cast<const float4*>(H + size_t(col[e]) * IN);
+#pragma unroll
+      for (int i = 0; i < IN / 4; ++i) {
+        const float4 x = h[i];
+        acc[4 * i] += w * x.x;
+        acc[4 * i + 1] += w * x.y;
+        acc[4 * i + 2] += w * x.z;
+        acc[4 * i + 3] += w * x.w;
+      }
+    }
+    const float inv = float(1.0 / diag[v]);
+#pragma unroll
+    for (int i = 0; i < IN; ++i) {
+      float x = acc[i];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+      if (lane == (i & 31)) S[v * IN + i] = x * inv;
+    }
   }
 }
+
 
 // dH[u][i] += sum_v (w_uv / d_v) T[v][i]   (transpose of the aggregation)
 __global__ void k_gnn_aggregate_t(uint32_t n, int in, const uint32_t* __restrict__ ptr,
@@ -453,8 +477,12 @@ void forward(GraphData& g, DeviceParams& p, cudaStream_t s) {
   for (int l = 0; l < GNN_LAYERS; ++l) {
     int w = layer_in(l);
     size_t o = gnn_layer_offset(l);
-    k_gnn_aggregate<<<gnn_blocks(size_t(g.n) * w), GNN_THREADS, 0, s>>>(g.n, w, g.ptr.p, g.col.p, g.val.p, g.diag.p,
-                                                                       in, g.S[l].p);
+    if (w == GNN_FEATURES)
+      k_gnn_aggregate<GNN_FEATURES><<<gnn_blocks(size_t(g.n) * 32), GNN_THREADS, 0, s>>>(
+          g.n, g.ptr.p, g.col.p, g.val.p, g.diag.p, in, g.S[l].p);
+    else
+      k_gnn_aggregate<GNN_WIDTH><<<gnn_blocks(size_t(g.n) * 32), GNN_THREADS, 0, s>>>(
+          g.n, g.ptr.p, g.col.p, g.val.p, g.diag.p, in, g.S[l].p);
     k_gnn_dense<<<gnn_blocks(size_t(g.n) * GNN_WIDTH), GNN_THREADS, 0, s>>>(
         g.n, w, in, g.S[l].p, p.bf.p + o, p.bf.p + o + size_t(w) * GNN_WIDTH,
         p.master.p + o + size_t(w) * GNN_WIDTH * 2, g.H[l].p);
@@ -524,26 +552,39 @@ __global__ void k_feat_finish(int blocks, uint32_t n, int pass, const double* __
 __global__ void k_feat_vertices(uint32_t n, const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
                                 const double* __restrict__ val, const double* __restrict__ diag,
                                 const double* __restrict__ stats, float* __restrict__ X) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+  // one warp per vertex, its lanes striding the edges, fixed shuffle trees
+  const int lane = threadIdx.x & 31;
+  const size_t warps = (size_t(gridDim.x) * blockDim.x) >> 5;
+  for (size_t v = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
     const double d = fmax(diag[v], 1e-300), ld = log(d);
     double wmax = 0.0, sq = 0.0, nb = 0.0, inflow = 0.0;
-    for (uint32_t e = ptr[v]; e < ptr[v + 1]; ++e) {
+    const uint32_t end = ptr[v + 1];
+    for (uint32_t e = ptr[v] + lane; e < end; e += 32) {
       const double a = val[e] / d, dc = fmax(diag[col[e]], 1e-300);
       wmax = fmax(wmax, a);
       sq += a * a;
       nb += a * (log(dc) - ld);
       inflow += val[e] / dc;
     }
-    const double cnt = double(ptr[v + 1] - ptr[v]);
-    float* x = X + size_t(v) * GNN_FEATURES;
-    x[0] = float((ld - stats[0]) / stats[2]);
-    x[1] = float(log1p(cnt) - stats[1]);
-    x[2] = float(wmax);
-    x[3] = float(nb);
-    x[4] = float(sq);
-    x[5] = float(log(fmax(inflow, 1e-12)));
-    x[6] = float(1.0 / sqrt(1.0 + cnt));
-    x[7] = 1.0f;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      wmax = fmax(wmax, __shfl_xor_sync(0xffffffffu, wmax, off));
+      sq += __shfl_xor_sync(0xffffffffu, sq, off);
+      nb += __shfl_xor_sync(0xffffffffu, nb, off);
+      inflow += __shfl_xor_sync(0xffffffffu, inflow, off);
+    }
+    if (lane == 0) {
+      const double cnt = double(ptr[v + 1] - ptr[v]);
+      float* x = X + v * GNN_FEATURES;
+      x[0] = float((ld - stats[0]) / stats[2]);
+      x[1] = float(log1p(cnt) - stats[1]);
+      x[2] = float(wmax);
+      x[3] = float(nb);
+      x[4] = float(sq);
+      x[5] = float(log(fmax(inflow, 1e-12)));
+      x[6] = float(1.0 / sqrt(1.0 + cnt));
+      x[7] = 1.0f;
+    }
   }
 }
 
@@ -582,7 +623,8 @@ std::unique_ptr<LearnedPreconditioner> build_learned_device(const std::vector<fl
   k_feat_finish<<<1, 32, 0, s>>>(blocks, n, 0, partial.p, stats.p);
   k_feat_sums<<<blocks, FEAT_THREADS, 0, s>>>(n, g.ptr.p, g.diag.p, stats.p, partial.p);
   k_feat_finish<<<1, 32, 0, s>>>(blocks, n, 1, partial.p, stats.p);
-  k_feat_vertices<<<blocks, FEAT_THREADS, 0, s>>>(n, g.ptr.p, g.col.p, g.val.p, g.diag.p, stats.p, g.X.p);
+  k_feat_vertices<<<gnn_blocks(size_t(n) * 32), FEAT_THREADS, 0, s>>>(n, g.ptr.p, g.col.p, g.val.p, g.diag.p,
+                                                                       stats.p, g.X.p);
   CK_LAUNCH();
   for (int l = 0; l < GNN_LAYERS; ++l) {
     g.S[l].alloc(size_t(n) * layer_in(l));
