@@ -604,16 +604,6 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
       }, s, h2d);
     };
   };
-  auto cell_rows_task = [&] {  // rows of every cell (stable counting sort)
-    uint64_t& h2d = task_h2d[4];
-    std::vector<uint32_t> cptr(p.cells + 1, 0), crow(R);
-    for (size_t r = 0; r < R; ++r) cptr[p.row_cell[r] + 1]++;
-    for (size_t c = 0; c < p.cells; ++c) cptr[c + 1] += cptr[c];
-    std::vector<uint32_t> cur(cptr.begin(), cptr.end() - 1);
-    for (size_t r = 0; r < R; ++r) crow[cur[p.row_cell[r]]++] = uint32_t(r);
-    upload(e->cell_rows_ptr, cptr, s, h2d);
-    upload(e->cell_rows, crow, s, h2d);
-  };
   auto groups_task = [&] {  // match groups (rows by semantic rank) and work buffers
     uint64_t& h2d = task_h2d[5];
     if (!plan.observation) {  // leave-observation-out reads its units by cell
@@ -652,7 +642,6 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     e->residual.alloc(R);
     e->deleted.alloc(R);
     tasks.push_back(rows_task);
-    tasks.push_back(cell_rows_task);
     tasks.push_back(groups_task);
     if (e->q > 0) qcol.alloc(R * size_t(e->q));
     for (int k = 0; k < e->q; ++k) tasks.push_back(controls_task(k));
@@ -676,6 +665,24 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
   if (qcol.p) {
     k_transpose_controls<<<grid_blocks(), THREADS, 0, s>>>(uint32_t(R), e->q, qcol.p, e->Qd.p);
     CK_LAUNCH();
+  }
+  if (plan.generic) {
+    // the rows of every cell in row order: a stable sort of the row indices
+    // by cell (LSD radix), the cell offsets from a count and a scan
+    e->cell_rows_ptr.alloc(size_t(e->C) + 1);
+    e->cell_rows.alloc(R);
+    DBuf<uint32_t> counts(size_t(e->C) + 1), idx(R), keys(R);
+    CK(cudaMemsetAsync(counts.p, 0, counts.bytes(), s));
+    k_cell_counts<<<grid_blocks(), THREADS, 0, s>>>(uint32_t(R), e->row_cell.p, counts.p, idx.p);
+    device_exclusive_sum(counts.p, e->cell_rows_ptr.p, size_t(e->C) + 1, s);
+    int bits = 1;
+    while (bits < 32 && (uint64_t(1) << bits) <= uint64_t(e->C)) ++bits;
+    size_t bytes = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, e->row_cell.p, keys.p, idx.p, e->cell_rows.p, R, 0, bits, s));
+    DBuf<char> tmp(bytes);
+    CK(cub::DeviceRadixSort::SortPairs(tmp.p, bytes, e->row_cell.p, keys.p, idx.p, e->cell_rows.p, R, 0, bits, s));
+    CK_LAUNCH();
+    CK(cudaStreamSynchronize(s));  // the scratch is released on return
   }
   if (plan.observation) {
     // units of leave-observation-out are the rows in cell order (the cell

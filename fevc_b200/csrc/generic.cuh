@@ -110,6 +110,16 @@ __global__ void k_row_residual(uint32_t rows, int q, const uint32_t* __restrict_
   }
 }
 
+// Rows per cell (atomic counts: exact whatever the order) and the row
+// indices the stable sort by cell permutes.
+__global__ void k_cell_counts(uint32_t rows, const uint32_t* __restrict__ row_cell, uint32_t* __restrict__ counts,
+                              uint32_t* __restrict__ idx) {
+  for (size_t r = size_t(blockIdx.x) * blockDim.x + threadIdx.x; r < rows; r += size_t(gridDim.x) * blockDim.x) {
+    atomicAdd(&counts[row_cell[r]], 1u);
+    idx[r] = uint32_t(r);
+  }
+}
+
 // Controls uploaded column-major (k * rows + r) to row-major (r * q + k).
 __global__ void k_transpose_controls(uint32_t rows, int q, const double* __restrict__ cols, double* __restrict__ Q) {
   const size_t total = size_t(rows) * q;

@@ -922,8 +922,9 @@ int32_t fevcb_engine_prepare_timings_v1(uint64_t generation, FevcbPrepareTimings
 /* Wall milliseconds of the device engine's setup for the generation (built
  * on its first solve): the host builders, each on its own thread with its
  * uploads (cells and firm segments; deletion units; target strata; row data;
- * the rows of every cell; match groups; then one per control column),
- * their parallel span, the unit arrays derived on the device, the hybrid
+ * match groups; then one per control column), their parallel span, the
+ * device steps after them (controls transposed, the rows of every cell
+ * sorted, the leave-observation-out unit arrays derived), the hybrid
  * Laplacian's assembly, the preconditioner's setup, and the whole setup.
  * Builders a plan does not use report 0.  STALE_CONTEXT before a solve. */
 typedef struct FevcbSetupTimingsV1 {
