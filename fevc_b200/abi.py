@@ -997,7 +997,8 @@ class Engine:
         t = FevcbSetupTimingsV1()
         self.check(self.lib.fevcb_engine_setup_timings_v1(self.generation, C.byref(t), C.sizeof(t)))
         d = t.as_dict()
-        names = ("cells", "units", "strata", "rows", "groups") + tuple(f"control_{k}" for k in range(11))
+        names = ("cells", "units", "strata", "strata_scale", "strata_keys", "rows", "groups") + tuple(
+            f"control_{k}" for k in range(9))
         d["builder_ms"] = {names[i]: round(list(t.builder_ms)[i], 2) for i in range(min(t.builders, 16))}
         return d
 

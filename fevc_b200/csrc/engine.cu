@@ -614,28 +614,37 @@ std::shared_ptr<DeviceEngine> make_device_engine(const Compressed& p, const JlaP
     e->psiH.alloc(size_t(e->F) * QMAX);
     e->beta_buf.alloc(QMAX * 128);
   };
+  // target strata (already in cell order), in three builders: the cell
+  // offsets with the plan checks, the scales, and the Counter-V1 keys
   auto strata_task = [&] {
     uint64_t& h2d = task_h2d[2];
-    // strata (already in cell order)
-    {
-      std::vector<uint32_t> tptr(p.cells + 1, 0);
-      for (size_t k = 0; k < plan.tgt_cell.size(); ++k) {
-        if (k > 0 && plan.tgt_cell[k] < plan.tgt_cell[k - 1])
-          fail(INTERNAL_INVARIANT_FAILED, "jla_plan", "target strata are not in cell order");
-        tptr[plan.tgt_cell[k] + 1]++;
-        if (plan.tgt_count[k] == 0 || (plan.tgt_count[k] + 63) / 64 > MAX_WORDS_PER_ATOM)
-          fail(RESOURCE_LIMIT, "jla_validate", "target trial preflight failed");
-      }
-      for (size_t c = 0; c < p.cells; ++c) tptr[c + 1] += tptr[c];
-      std::vector<double> scale(plan.tgt_cell.size());
-      for (size_t k = 0; k < scale.size(); ++k) scale[k] = std::sqrt(plan.tgt_per_copy[k] / p.target_total);
-      upload(e->tgt_ptr, tptr, s, h2d);
-      upload(e->tgt_rank, plan.tgt_rank, s, h2d);
-      upload(e->tgt_count, plan.tgt_count, s, h2d);
-      upload(e->tgt_scale, scale, s, h2d);
+    std::vector<uint32_t> tptr(p.cells + 1, 0);
+    for (size_t k = 0; k < plan.tgt_cell.size(); ++k) {
+      if (k > 0 && plan.tgt_cell[k] < plan.tgt_cell[k - 1])
+        fail(INTERNAL_INVARIANT_FAILED, "jla_plan", "target strata are not in cell order");
+      tptr[plan.tgt_cell[k] + 1]++;
+      if (plan.tgt_count[k] == 0 || (plan.tgt_count[k] + 63) / 64 > MAX_WORDS_PER_ATOM)
+        fail(RESOURCE_LIMIT, "jla_validate", "target trial preflight failed");
     }
+    for (size_t c = 0; c < p.cells; ++c) tptr[c + 1] += tptr[c];
+    upload(e->tgt_ptr, tptr, s, h2d);
   };
-  std::vector<std::function<void()>> tasks = {cells_task, units_task, strata_task};
+  auto strata_scale_task = [&] {
+    uint64_t& h2d = task_h2d[4];
+    const size_t S = plan.tgt_cell.size();
+    e->tgt_scale.alloc(S);
+    upload_fill(e->tgt_scale, 0, S, [&](double* d) {
+#pragma omp parallel for schedule(static) if (S >= 65536)
+      for (size_t k = 0; k < S; ++k) d[k] = std::sqrt(plan.tgt_per_copy[k] / p.target_total);
+    }, s, h2d);
+  };
+  auto strata_keys_task = [&] {
+    uint64_t& h2d = task_h2d[14];
+    upload(e->tgt_rank, plan.tgt_rank, s, h2d);
+    upload(e->tgt_count, plan.tgt_count, s, h2d);
+  };
+  std::vector<std::function<void()>> tasks = {cells_task, units_task, strata_task, strata_scale_task,
+                                              strata_keys_task};
   if (plan.generic) {
     e->Qd.alloc(R * e->q);
     e->Rd.alloc(R * e->q);

@@ -921,8 +921,9 @@ int32_t fevcb_engine_prepare_timings_v1(uint64_t generation, FevcbPrepareTimings
 
 /* Wall milliseconds of the device engine's setup for the generation (built
  * on its first solve): the host builders, each on its own thread with its
- * uploads (cells and firm segments; deletion units; target strata; row data;
- * match groups; then one per control column), their parallel span, the
+ * uploads (cells and firm segments; deletion units; target strata offsets,
+ * scales and keys; row data; match groups; then one per control column),
+ * their parallel span, the
  * device steps after them (controls transposed, the rows of every cell
  * sorted, the leave-observation-out unit arrays derived), the hybrid
  * Laplacian's assembly, the preconditioner's setup, and the whole setup.

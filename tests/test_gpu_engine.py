@@ -251,7 +251,7 @@ def test_kernel_launch_count_matches_the_profiler(lib, precond):
 
 
 def test_setup_timings_cover_the_setup(lib):
-    """The device setup's phases: one time per host builder (three for the
+    """The device setup's phases: one time per host builder (five for the
     compressed plan), their span within the whole setup, and the later
     phases inside it as well."""
     panel = make_golden.PANELS["small_2k"]["build"]()
@@ -260,7 +260,7 @@ def test_setup_timings_cover_the_setup(lib):
         st = e.setup_timings()
     finally:
         e.release()
-    assert st["builders"] == 3 and len(st["builder_ms"]) == 3
+    assert st["builders"] == 5 and len(st["builder_ms"]) == 5
     assert all(v >= 0.0 for v in st["builder_ms"].values())
     assert 0.0 < st["builders_span_ms"] <= st["total_ms"]
     assert st["builders_span_ms"] + st["hybrid_ms"] + st["preconditioner_ms"] <= st["total_ms"] * (1 + 1e-9)
