@@ -1241,38 +1241,47 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
     }
     p.target_index = grouped_from_order(p.exact_target_strata, p.row_target, std::move(tord));
   }
-  p.deletion_index = grouped_rows(D, p.row_deletion);
-
+  // the deletion index and the retained copies of the row columns are
+  // independent: one thread each (a column's gather and its totals in row
+  // order, as a sequential walk takes them)
   KahanSum tt;
-  p.outcome.resize(R);
-  p.frequency.resize(R);
-  p.target.resize(R);
-#pragma omp parallel for schedule(static) if (R >= 65536)
-  for (size_t i = 0; i < R; ++i) {
-    uint64_t r = p.retained_rows[i];
-    p.outcome[i] = in.outcome[r];
-    p.frequency[i] = in.frequency[r];
-    p.target[i] = in.target[r];
-  }
-  // the totals in row order
-  for (size_t i = 0; i < R; ++i) {
-    p.physical_total += p.frequency[i];
-    tt.add(p.target[i]);
-  }
+  p.controls.resize(in.controls.size());
+  std::vector<std::function<void()>> tasks = {
+      [&] { p.deletion_index = grouped_rows(D, p.row_deletion); },
+      [&] {
+        p.outcome.resize(R);
+        for (size_t i = 0; i < R; ++i) p.outcome[i] = in.outcome[p.retained_rows[i]];
+      },
+      [&] {
+        p.frequency.resize(R);
+        for (size_t i = 0; i < R; ++i) {
+          p.frequency[i] = in.frequency[p.retained_rows[i]];
+          p.physical_total += p.frequency[i];
+        }
+      },
+      [&] {
+        p.target.resize(R);
+        for (size_t i = 0; i < R; ++i) {
+          p.target[i] = in.target[p.retained_rows[i]];
+          tt.add(p.target[i]);
+        }
+      }};
+  for (size_t k = 0; k < in.controls.size(); ++k)
+    tasks.push_back([&, k] {
+      std::vector<double>& col = p.controls[k];
+      col.resize(R);
+      for (size_t i = 0; i < R; ++i) col[i] = in.controls[k][p.retained_rows[i]];
+    });
+  if (!in.probe_order.empty())
+    tasks.push_back([&] {
+      p.probe_order.resize(R);
+      for (size_t i = 0; i < R; ++i) p.probe_order[i] = in.probe_order[p.retained_rows[i]];
+    });
+  run_tasks(tasks);
   p.target_total = tt.finish();
   if (!std::isfinite(p.target_total) || p.target_total <= 0.0)
     fail(INVALID_TARGET_WEIGHT, "compression", "retained target mass is not positive and finite");
   p.rows_physical = p.physical_total;
-  for (auto& ctl : in.controls) {
-    std::vector<double> col(R);
-#pragma omp parallel for schedule(static) if (R >= 65536)
-    for (size_t i = 0; i < R; ++i) col[i] = ctl[p.retained_rows[i]];
-    p.controls.push_back(std::move(col));
-  }
-  if (!in.probe_order.empty()) {
-    p.probe_order.resize(R);
-    for (size_t i = 0; i < R; ++i) p.probe_order[i] = in.probe_order[p.retained_rows[i]];
-  }
   return p;
 }
 
