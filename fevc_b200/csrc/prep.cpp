@@ -1173,6 +1173,8 @@ Compressed compress(const Canonical& in, const std::vector<uint8_t>& active, boo
     p.cell_target_sum[cell] = tsum.finish();
   }
   if (bad_moment) fail(INVALID_WEIGHT, "compression", "weighted cell moment is nonfinite");
+  p.cell_index.ptr.assign(cell_start.begin(), cell_start.end());
+  p.cell_index.items = order;
   size_t C = p.cell_worker.size();
   p.cells = C;
   {
@@ -1432,6 +1434,10 @@ void build_target_strata(const Compressed& p, const std::vector<double>& per_cop
 // rows stably when every cell's range is stable-sorted by the rest of it.
 static std::vector<uint32_t> rows_by_cell(const Compressed& p, std::vector<size_t>& begin) {
   const size_t R = p.rows(), C = p.cells;
+  if (p.cell_index.items.size() == R && p.cell_index.ptr.size() == C + 1) {  // kept by the compression
+    begin.assign(p.cell_index.ptr.begin(), p.cell_index.ptr.end());
+    return p.cell_index.items;
+  }
   begin.assign(C + 1, 0);
   for (size_t r = 0; r < R; ++r) begin[p.row_cell[r] + 1]++;
   for (size_t c = 0; c < C; ++c) begin[c + 1] += begin[c];

@@ -64,6 +64,7 @@ struct Compressed {
   std::vector<uint32_t> cell_worker, cell_firm;
   std::vector<double> cell_weight, cell_outcome_sum, cell_target_sum;
   GroupIndex worker_index, firm_index, deletion_index, target_index;
+  GroupIndex cell_index;  // rows of every cell, in row order (the compression's sort)
   uint64_t physical_total = 0;
   double target_total = 0.0;
   size_t rows() const { return row_worker.size(); }
