@@ -301,3 +301,20 @@ def test_prepare_timings_split_the_preparation(lib):
         assert lib.fevcb_engine_prepare_timings_v1(e.generation, None, 0) == 20
     finally:
         e.release()
+
+
+def test_setup_timings_need_a_device_engine(lib):
+    """The device setup timings exist only once a solve has built the
+    generation's device engine: before that the call is STALE_CONTEXT (80);
+    a short output is an ABI mismatch (10)."""
+    from make_golden import kat12
+
+    e = abi.Engine(lib)
+    e.prepare(kat12())
+    try:
+        t = abi.FevcbSetupTimingsV1()
+        assert C.sizeof(t) == 176
+        assert lib.fevcb_engine_setup_timings_v1(e.generation, C.byref(t), C.sizeof(t)) == 80
+        assert lib.fevcb_engine_setup_timings_v1(e.generation, C.byref(t), 100) == 10
+    finally:
+        e.release()
